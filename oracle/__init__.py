@@ -1,0 +1,267 @@
+"""ctypes bindings for the oracle libraries.  TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this package, and only as the checker.  The product package (vflip_b200)
+never imports it.
+
+Two libraries share one calling convention (linear layout, i fastest):
+  * ``liboracle.so``        - this project's CPU restatement (vflip_oracle.cpp);
+  * ``_ref/libvflip_ref.so`` - the reference's own code (build_ref.py), present
+    only where the reference tree was available at build time.
+
+Seven-point operators are numpy arrays of shape (7, nk, nj, ni), float64, in
+the slot order diag, -x, +x, -y, +y, -z, +z.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libvflip_ref.so")
+
+PARTICLE_DTYPE = np.dtype([("pos", "<f4", (3,)), ("vel", "<f4", (3,)), ("dens", "<f4"), ("temp", "<f4"),
+                           ("hash_idx", "<i4"), ("sub_hash_idx", "<i4")])
+assert PARTICLE_DTYPE.itemsize == 40
+
+_P = C.c_void_p
+_I = C.c_int
+_F = C.c_float
+_D = C.c_double
+
+
+def _ptr(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def build_oracle():
+    """Compile liboracle.so (and the reference library when its tree exists)."""
+    subprocess.check_call(["make", "-s", "-C", HERE, "liboracle.so"])
+    subprocess.check_call(["python3", os.path.join(HERE, "build_ref.py")])
+
+
+_libs = {}
+
+
+def _load(path, prefix):
+    if path in _libs:
+        return _libs[path]
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    p = prefix
+    if prefix == "oracle":
+        getattr(lib, p + "_levels").argtypes = [_I, _I, _I, _P, _I, _P, _P]
+        getattr(lib, p + "_rbgs").argtypes = [_I, _I, _I, _P, _P, _P, _I]
+        getattr(lib, p + "_vcycle").argtypes = [_I, _I, _I, _P, _P, _P]
+        getattr(lib, p + "_spmv").argtypes = [_I, _I, _I, _P, _P, _P]
+        getattr(lib, p + "_amgpcg").argtypes = [_I, _I, _I, _P, _P, _P, _D, _I, _P, _P]
+    else:
+        getattr(lib, p + "_levels").argtypes = [_I, _I, _I, _P, _P, _P, _I, _P, _P]
+        getattr(lib, p + "_rbgs").argtypes = [_I, _I, _I, _P, _P, _P, _P, _P, _I]
+        getattr(lib, p + "_vcycle").argtypes = [_I, _I, _I, _P, _P, _P, _P, _P]
+        getattr(lib, p + "_amgpcg").argtypes = [_I, _I, _I, _P, _P, _P, _P, _P, _D, _I, _P, _P]
+        getattr(lib, p + "_delta").argtypes = [_I, _I, _I, _P, _P, _P]
+    getattr(lib, p + "_fraction_inside4").argtypes = [_I, _P, _P, _P, _P, _P]
+    getattr(lib, p + "_face_weights").argtypes = [_I, _I, _I, _F, _P, _P, _P, _P]
+    getattr(lib, p + "_project").argtypes = [_I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                             _P, _P, _P, _P, _P]
+    getattr(lib, p + "_advect_rk2").argtypes = [_I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _P, _P]
+    getattr(lib, p + "_hash").argtypes = [_I, _I, _I, _F, _P, _I, _P]
+    getattr(lib, p + "_p2g").argtypes = [_I, _I, _I, _F, _P, _I, _I, _P, _P]
+    if prefix == "oracle":
+        getattr(lib, p + "_g2p").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _P, _P, _D]
+        getattr(lib, p + "_delta").argtypes = [_I, _I, _I, _P, _P, _P]
+    else:
+        getattr(lib, p + "_g2p").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P]
+    _libs[path] = lib
+    return lib
+
+
+# ---------------------------------------------------------------- conversions
+
+def stencil_to_csr(st):
+    """7-slot stencil (7, nk, nj, ni) -> CSR (rowstart, colindex, value) with
+    the entries of every in-grid neighbour, columns ascending."""
+    _, nk, nj, ni = st.shape
+    n = ni * nj * nk
+    flat = st.reshape(7, n)
+    idx = np.arange(n, dtype=np.int64)
+    i = idx % ni
+    j = (idx // ni) % nj
+    k = idx // (ni * nj)
+    # column order: -z, -y, -x, diag, +x, +y, +z
+    cols, vals, valid = [], [], []
+    for slot, off, ok in ((5, -ni * nj, k > 0), (3, -ni, j > 0), (1, -1, i > 0), (0, 0, np.ones(n, bool)),
+                          (2, 1, i < ni - 1), (4, ni, j < nj - 1), (6, ni * nj, k < nk - 1)):
+        cols.append(idx + off)
+        vals.append(flat[slot])
+        valid.append(ok)
+    cols = np.stack(cols, 1)
+    vals = np.stack(vals, 1)
+    valid = np.stack(valid, 1)
+    counts = valid.sum(1)
+    rowstart = np.zeros(n + 1, np.uint32)
+    rowstart[1:] = np.cumsum(counts)
+    return rowstart, cols[valid].astype(np.uint32), np.ascontiguousarray(vals[valid], dtype=np.float64)
+
+
+# ---------------------------------------------------------------- solver API
+
+class _Impl:
+    def __init__(self, lib, prefix):
+        self.lib = lib
+        self.p = prefix
+
+    def fn(self, name):
+        return getattr(self.lib, self.p + "_" + name)
+
+    def _op(self, st):
+        st = np.ascontiguousarray(st, dtype=np.float64)
+        if self.p == "oracle":
+            return (_ptr(st),), st
+        rs, ci, v = stencil_to_csr(st)
+        return (_ptr(rs), _ptr(ci), _ptr(v)), (rs, ci, v)
+
+    def levels(self, st, max_levels=16):
+        _, nk, nj, ni = st.shape
+        args, keep = self._op(st)
+        dims = np.zeros(3 * max_levels, np.int32)
+        # upper bound for all levels' stencil storage
+        total = 0
+        a, b, c = ni, nj, nk
+        for _ in range(max_levels):
+            total += 7 * a * b * c
+            a, b, c = (a + 1) // 2, (b + 1) // 2, (c + 1) // 2
+        out = np.zeros(total, np.float64)
+        nl = self.fn("levels")(ni, nj, nk, *args, max_levels, _ptr(dims), _ptr(out))
+        if nl < 0:
+            raise RuntimeError("a level left the 7-point pattern")
+        res, off = [], 0
+        for l in range(nl):
+            x, y, z = dims[3 * l:3 * l + 3]
+            m = 7 * x * y * z
+            res.append(out[off:off + m].reshape(7, z, y, x).copy())
+            off += m
+        return res
+
+    def rbgs(self, st, b, x, iters):
+        _, nk, nj, ni = st.shape
+        args, keep = self._op(st)
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.array(x, np.float64, copy=True, order="C")
+        self.fn("rbgs")(ni, nj, nk, *args, _ptr(b), _ptr(x), iters)
+        return x
+
+    def vcycle(self, st, b):
+        _, nk, nj, ni = st.shape
+        args, keep = self._op(st)
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros_like(b)
+        self.fn("vcycle")(ni, nj, nk, *args, _ptr(b), _ptr(x))
+        return x
+
+    def amgpcg(self, st, rhs, tol=1e-6, maxit=50):
+        _, nk, nj, ni = st.shape
+        args, keep = self._op(st)
+        rhs = np.ascontiguousarray(rhs, np.float64)
+        x = np.zeros_like(rhs)
+        res = C.c_double(0)
+        it = C.c_int(0)
+        ok = self.fn("amgpcg")(ni, nj, nk, *args, _ptr(rhs), _ptr(x), tol, maxit, C.byref(res), C.byref(it))
+        return x, bool(ok), res.value, it.value
+
+    def fraction_inside4(self, bl, br, tl, tr):
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (bl, br, tl, tr)]
+        out = np.zeros_like(arrs[0])
+        self.fn("fraction_inside4")(arrs[0].size, *[_ptr(a) for a in arrs], _ptr(out))
+        return out
+
+    def face_weights(self, ni, nj, nk, h, phi):
+        phi = np.ascontiguousarray(phi, np.float32)
+        uw = np.zeros((nk, nj, ni + 1), np.float32)
+        vw = np.zeros((nk, nj + 1, ni), np.float32)
+        ww = np.zeros((nk + 1, nj, ni), np.float32)
+        self.fn("face_weights")(ni, nj, nk, h, _ptr(phi), _ptr(uw), _ptr(vw), _ptr(ww))
+        return uw, vw, ww
+
+    def project(self, ni, nj, nk, h, U_in, phi, bdesc, us, vs, ws, u, v, w):
+        phi = np.ascontiguousarray(phi, np.float32)
+        bdesc = np.ascontiguousarray(bdesc, np.int8)
+        us, vs, ws = [np.ascontiguousarray(a, np.float32) for a in (us, vs, ws)]
+        u, v, w = [np.array(a, np.float32, copy=True, order="C") for a in (u, v, w)]
+        n = ni * nj * nk
+        p = np.zeros((nk, nj, ni), np.float64)
+        rhs = np.zeros((nk, nj, ni), np.float64)
+        st = np.zeros((7, nk, nj, ni), np.float64)
+        uw = np.zeros_like(us)
+        vw = np.zeros_like(vs)
+        ww = np.zeros_like(ws)
+        it = C.c_int(0)
+        res = C.c_double(0)
+        ok = self.fn("project")(ni, nj, nk, h, U_in, _ptr(phi), _ptr(bdesc), _ptr(us), _ptr(vs), _ptr(ws),
+                                _ptr(u), _ptr(v), _ptr(w), _ptr(p), _ptr(rhs), _ptr(st), _ptr(uw), _ptr(vw),
+                                _ptr(ww), C.byref(it), C.byref(res))
+        assert n == p.size
+        return dict(u=u, v=v, w=w, pressure=p, rhs=rhs, stencil=st, uw=uw, vw=vw, ww=ww, ok=bool(ok),
+                    iterations=it.value, residual=res.value)
+
+    def advect_rk2(self, ni, nj, nk, h, dt, u, v, w, field, offsets):
+        u, v, w, field = [np.ascontiguousarray(a, np.float32) for a in (u, v, w, field)]
+        fnz, fny, fnx = field.shape
+        out = np.zeros_like(field)
+        self.fn("advect_rk2")(ni, nj, nk, h, dt, _ptr(u), _ptr(v), _ptr(w), fnx, fny, fnz, float(offsets[0]),
+                              float(offsets[1]), float(offsets[2]), _ptr(field), _ptr(out))
+        return out
+
+    def hash(self, ni, nj, nk, h, particles):
+        particles = np.ascontiguousarray(particles, PARTICLE_DTYPE)
+        out = np.zeros(len(particles), np.int32)
+        self.fn("hash")(ni, nj, nk, h, _ptr(particles), len(particles), _ptr(out))
+        return out
+
+    def p2g(self, ni, nj, nk, h, particles, comp):
+        particles = np.ascontiguousarray(particles, PARTICLE_DTYPE)
+        shape = (nk + (comp == 2), nj + (comp == 1), ni + (comp == 0))
+        f = np.zeros(shape, np.float32)
+        c = np.zeros(shape, np.float32)
+        self.fn("p2g")(ni, nj, nk, h, _ptr(particles), len(particles), comp, _ptr(f), _ptr(c))
+        return f, c
+
+    def g2p(self, ni, nj, nk, h, particles, du, dv, dw, un=None, vn=None, wn=None, flip_ratio=1.0):
+        p = np.array(particles, PARTICLE_DTYPE, copy=True)
+        du, dv, dw = [np.ascontiguousarray(a, np.float32) for a in (du, dv, dw)]
+        if self.p == "oracle":
+            if un is None:
+                un, vn, wn = du, dv, dw
+            un, vn, wn = [np.ascontiguousarray(a, np.float32) for a in (un, vn, wn)]
+            self.fn("g2p")(ni, nj, nk, h, _ptr(p), len(p), _ptr(du), _ptr(dv), _ptr(dw), _ptr(un), _ptr(vn),
+                           _ptr(wn), float(flip_ratio))
+        else:
+            if flip_ratio != 1.0:
+                raise ValueError("the reference's particle_from_grid is pure FLIP")
+            self.fn("g2p")(ni, nj, nk, h, _ptr(p), len(p), _ptr(du), _ptr(dv), _ptr(dw))
+        return p
+
+    def delta(self, after, before):
+        after, before = [np.ascontiguousarray(a, np.float32) for a in (after, before)]
+        out = np.zeros_like(after)
+        nz, ny, nx = after.shape
+        self.fn("delta")(nx, ny, nz, _ptr(after), _ptr(before), _ptr(out))
+        return out
+
+
+def oracle():
+    """The CPU restatement (always available once built)."""
+    lib = _load(ORACLE_SO, "oracle")
+    if lib is None:
+        raise FileNotFoundError(f"{ORACLE_SO} missing: run `make -C oracle liboracle.so`")
+    return _Impl(lib, "oracle")
+
+
+def reference():
+    """The reference's own code, or None when it was not built here."""
+    lib = _load(REF_SO, "ref")
+    return None if lib is None else _Impl(lib, "ref")

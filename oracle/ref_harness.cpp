@@ -1,0 +1,374 @@
+// extern "C" harness over the reference solver's own CPU code.
+//
+// Test infrastructure only.  oracle/build_ref.py compiles this file together
+// with the reference translation units into oracle/_ref/libvflip_ref.so; the
+// tests use it to pin the oracle restatement (oracle/vflip_oracle.cpp) and to
+// generate the golden fixtures under tests/golden/, and bench.py times it as
+// the reference CPU arm.  Nothing in the product links it.
+//
+// Every entry point takes flat arrays in the linear layout used throughout
+// this project (index = i + ni*(j + nj*k), i fastest) and converts to/from the
+// reference's bricked Buffer3D storage (Smoke_Solver/fluid_buffer3D.h:186-202)
+// element by element, so the conversion itself cannot change a value.
+//
+// Grid shapes for an ni x nj x nk cell grid:
+//   cell  ni*nj*nk            u  (ni+1)*nj*nk
+//   v     ni*(nj+1)*nk        w  ni*nj*(nk+1)
+//   nodal (ni+1)*(nj+1)*(nk+1)
+#include <cstdint>
+#include <vector>
+
+#include "AlgebraicMultigrid.h"
+#include "GeometricLevelGen.h"
+#include "Smoke_solver3D.h"
+#include "levelset_util.h"
+#include "sub_domain.h"
+
+using namespace ivock;
+
+namespace {
+
+size_t lin(int i, int j, int k, int nx, int ny) { return (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * k); }
+
+void to_buffer(buffer3Df& b, const float* src) {
+  for (uint k = 0; k < b._nz; ++k)
+    for (uint j = 0; j < b._ny; ++j)
+      for (uint i = 0; i < b._nx; ++i) b(i, j, k) = src[lin(i, j, k, b._nx, b._ny)];
+}
+
+void from_buffer(buffer3Df& b, float* dst) {
+  for (uint k = 0; k < b._nz; ++k)
+    for (uint j = 0; j < b._ny; ++j)
+      for (uint i = 0; i < b._nx; ++i) dst[lin(i, j, k, b._nx, b._ny)] = b(i, j, k);
+}
+
+// Builds a SparseMatrix<double> from a CSR triple (rows sorted by column, as
+// the reference's own SparseMatrix keeps them, sparse_matrix.h:73-88).
+void csr_to_sparse(unsigned n, const uint32_t* rowstart, const uint32_t* colindex, const double* value,
+                   SparseMatrix<double>& m) {
+  m.resize(n);
+  m.zero();
+  for (unsigned r = 0; r < n; ++r)
+    for (uint32_t e = rowstart[r]; e < rowstart[r + 1]; ++e) m.set_element(r, colindex[e], value[e]);
+}
+
+void csr_to_fixed(unsigned n, const uint32_t* rowstart, const uint32_t* colindex, const double* value,
+                  FixedSparseMatrix<double>& f) {
+  SparseMatrix<double> m;
+  csr_to_sparse(n, rowstart, colindex, value, m);
+  f.construct_from_matrix(m);
+}
+
+// 7-array stencil view of a CSR level: diag, -x, +x, -y, +y, -z, +z.  Returns
+// the number of entries that are not on the 7-point pattern (must be 0).
+int fixed_to_stencil(const FixedSparseMatrix<double>& A, int ni, int nj, int nk, double* out) {
+  size_t n = (size_t)ni * nj * nk;
+  for (size_t q = 0; q < 7 * n; ++q) out[q] = 0.0;
+  int bad = 0;
+  for (size_t r = 0; r < n; ++r) {
+    for (unsigned e = A.rowstart[r]; e < A.rowstart[r + 1]; ++e) {
+      long long c = A.colindex[e];
+      long long d = c - (long long)r;
+      int slot = -1;
+      if (d == 0) slot = 0;
+      else if (d == -1) slot = 1;
+      else if (d == 1) slot = 2;
+      else if (d == -(long long)ni) slot = 3;
+      else if (d == (long long)ni) slot = 4;
+      else if (d == -(long long)ni * nj) slot = 5;
+      else if (d == (long long)ni * nj) slot = 6;
+      if (slot < 0) { ++bad; continue; }
+      out[slot * n + r] = A.value[e];
+    }
+  }
+  return bad;
+}
+
+void quiet_subdomain(SubDomainSolver& sd) {
+  // SubDomainSolver::bmin/bmax/_hx are never initialised unless
+  // initSubdomain() runs; park the box far outside any domain so the
+  // is_in/is_in2 tests read defined values and always fail.
+  sd._hx = sd._hy = sd._hz = 0.0f;
+  sd.bmin = Vec3f(-1.0e6f);
+  sd.bmax = Vec3f(-1.0e6f);
+}
+
+void init_solver_grids(SmokeSolver3D& s, int ni, int nj, int nk, float h) {
+  quiet_subdomain(s.sub_domain);
+  s._nx = ni; s._ny = nj; s._nz = nk;
+  s._hx = s._hy = s._hz = h;
+  s.origin = Vec3f(0.0f);
+  s._un.init(ni + 1, nj, nk, h, 0.5, 0, 0);
+  s._utemp.init(ni + 1, nj, nk, h, 0.5, 0, 0);
+  s._unp1.init(ni + 1, nj, nk, h, 0.5, 0, 0);
+  s._vn.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0);
+  s._vtemp.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0);
+  s._vnp1.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0);
+  s._wn.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5);
+  s._wtemp.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5);
+  s._wnp1.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5);
+  s._u_solid.init(ni + 1, nj, nk, h, 0.5, 0, 0);
+  s._v_solid.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0);
+  s._w_solid.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5);
+  s.u_valid.resize(ni + 1, nj, nk);
+  s.v_valid.resize(ni, nj + 1, nk);
+  s.w_valid.resize(ni, nj, nk + 1);
+  s._u_weights.init(ni + 1, nj, nk);
+  s._v_weights.init(ni, nj + 1, nk);
+  s._w_weights.init(ni, nj, nk + 1);
+  s._nodal_solid_phi.init(ni + 1, nj + 1, nk + 1, h, 0.5, 0.5, 0.5);
+  s._b_desc.init(ni, nj, nk);
+  s.particle_hash.clear();
+  s.particle_hash.resize((size_t)ni * nj * nk);  // hash_FLIP reserve-then-index UB guard
+}
+
+}  // namespace
+
+extern "C" {
+
+// levelGen::generateLevelsGalerkinCoarsening (GeometricLevelGen.h:28-71).
+// dims_out[3*l..3*l+2] = level l size; stencil_out = 7 arrays per level,
+// concatenated level after level.  Returns levels, or -1 if any level has an
+// entry off the 7-point pattern.
+int ref_levels(int ni, int nj, int nk, const uint32_t* rowstart, const uint32_t* colindex,
+               const double* value, int max_levels, int* dims_out, double* stencil_out) {
+  unsigned n = (unsigned)ni * nj * nk;
+  FixedSparseMatrix<double> A;
+  csr_to_fixed(n, rowstart, colindex, value, A);
+  std::vector<FixedSparseMatrix<double>*> A_L, R_L, P_L;
+  std::vector<Vec3i> S_L;
+  int total = 0;
+  levelGen<double> gen;
+  gen.generateLevelsGalerkinCoarsening(A_L, R_L, P_L, S_L, total, A, ni, nj, nk);
+  int bad = 0;
+  size_t off = 0;
+  for (int l = 0; l < total && l < max_levels; ++l) {
+    dims_out[3 * l + 0] = S_L[l].v[0];
+    dims_out[3 * l + 1] = S_L[l].v[1];
+    dims_out[3 * l + 2] = S_L[l].v[2];
+    if (stencil_out) {
+      bad += fixed_to_stencil(*A_L[l], S_L[l].v[0], S_L[l].v[1], S_L[l].v[2], stencil_out + off);
+      off += 7 * (size_t)S_L[l].v[0] * S_L[l].v[1] * S_L[l].v[2];
+    }
+  }
+  for (int l = 1; l < total; ++l) delete A_L[l];
+  for (int l = 0; l + 1 < total; ++l) { delete R_L[l]; delete P_L[l]; }
+  return bad ? -1 : total;
+}
+
+// ivock::RBGS (AlgebraicMultigrid.h:22-103), iters full red-black sweeps.
+void ref_rbgs(int ni, int nj, int nk, const uint32_t* rowstart, const uint32_t* colindex,
+              const double* value, const double* b, double* x, int iters) {
+  unsigned n = (unsigned)ni * nj * nk;
+  FixedSparseMatrix<double> A;
+  csr_to_fixed(n, rowstart, colindex, value, A);
+  std::vector<double> bb(b, b + n), xx(x, x + n);
+  RBGS(A, bb, xx, ni, nj, nk, iters);
+  for (unsigned q = 0; q < n; ++q) x[q] = xx[q];
+}
+
+// ivock::amgPrecond (AlgebraicMultigrid.h:177-188): x = V(4,4)-cycle applied to b.
+void ref_vcycle(int ni, int nj, int nk, const uint32_t* rowstart, const uint32_t* colindex,
+                const double* value, const double* b, double* x) {
+  unsigned n = (unsigned)ni * nj * nk;
+  FixedSparseMatrix<double> A;
+  csr_to_fixed(n, rowstart, colindex, value, A);
+  std::vector<FixedSparseMatrix<double>*> A_L, R_L, P_L;
+  std::vector<Vec3i> S_L;
+  int total = 0;
+  levelGen<double> gen;
+  gen.generateLevelsGalerkinCoarsening(A_L, R_L, P_L, S_L, total, A, ni, nj, nk);
+  std::vector<double> bb(b, b + n), xx;
+  amgPrecond(A_L, R_L, P_L, S_L, xx, bb);
+  for (unsigned q = 0; q < n; ++q) x[q] = xx[q];
+  for (int l = 1; l < total; ++l) delete A_L[l];
+  for (int l = 0; l + 1 < total; ++l) { delete R_L[l]; delete P_L[l]; }
+}
+
+// ivock::AMGPCGSolve, SparseMatrix overload (AlgebraicMultigrid.h:189-301).
+int ref_amgpcg(int ni, int nj, int nk, const uint32_t* rowstart, const uint32_t* colindex,
+               const double* value, const double* rhs, double* result, double tol, int maxit,
+               double* residual_out, int* iterations_out) {
+  unsigned n = (unsigned)ni * nj * nk;
+  SparseMatrix<double> m;
+  csr_to_sparse(n, rowstart, colindex, value, m);
+  std::vector<double> r(rhs, rhs + n), x(n, 0.0);
+  double res = 0;
+  int it = 0;
+  bool ok = AMGPCGSolve(m, r, x, tol, maxit, res, it, ni, nj, nk);
+  for (unsigned q = 0; q < n; ++q) result[q] = x[q];
+  *residual_out = res;
+  *iterations_out = it;
+  return ok ? 1 : 0;
+}
+
+// fraction_inside, 4-corner form (levelset_util.cpp:23-103), element-wise.
+void ref_fraction_inside4(int n, const float* bl, const float* br, const float* tl, const float* tr,
+                          float* out) {
+  for (int q = 0; q < n; ++q) out[q] = fraction_inside(bl[q], br[q], tl[q], tr[q]);
+}
+
+// SmokeSolver3D::compute_face_weights (Smoke_solver3D.cpp:874-944).
+void ref_face_weights(int ni, int nj, int nk, float h, const float* nodal_phi, float* uw, float* vw,
+                      float* ww) {
+  SmokeSolver3D s;
+  init_solver_grids(s, ni, nj, nk, h);
+  to_buffer(s._nodal_solid_phi, nodal_phi);
+  s.compute_face_weights();
+  from_buffer(s._u_weights, uw);
+  from_buffer(s._v_weights, vw);
+  from_buffer(s._w_weights, ww);
+}
+
+// SmokeSolver3D::pcg_projection (Smoke_solver3D.cpp:945-1202): face weights,
+// inflow overwrite, assembly, AMGPCGSolve(1e-6, 50), gradient update.
+// u/v/w are updated in place.  Optional outputs (may be null): pressure (n),
+// rhs (n), the assembled matrix as 7 stencil arrays (7n), the face weights.
+// Returns the solver's bool; iterations and residual are written.
+int ref_project(int ni, int nj, int nk, float h, float U_in, const float* nodal_phi, const int8_t* bdesc,
+                const float* us, const float* vs, const float* ws, float* u, float* v, float* w,
+                double* pressure_out, double* rhs_out, double* stencil_out, float* uw, float* vw,
+                float* ww, int* iterations_out, double* residual_out) {
+  SmokeSolver3D s;
+  init_solver_grids(s, ni, nj, nk, h);
+  s._U_in = U_in;
+  to_buffer(s._nodal_solid_phi, nodal_phi);
+  to_buffer(s._u_solid, us);
+  to_buffer(s._v_solid, vs);
+  to_buffer(s._w_solid, ws);
+  to_buffer(s._un, u);
+  to_buffer(s._vn, v);
+  to_buffer(s._wn, w);
+  for (int k = 0; k < nk; ++k)
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i < ni; ++i) s._b_desc(i, j, k) = (char)bdesc[lin(i, j, k, ni, nj)];
+  s.pcg_projection(1.0f);
+  from_buffer(s._un, u);
+  from_buffer(s._vn, v);
+  from_buffer(s._wn, w);
+  size_t n = (size_t)ni * nj * nk;
+  if (pressure_out) for (size_t q = 0; q < n; ++q) pressure_out[q] = s.pressure[q];
+  if (rhs_out) for (size_t q = 0; q < n; ++q) rhs_out[q] = s.rhs[q];
+  if (stencil_out) {
+    FixedSparseMatrix<double> A;
+    A.construct_from_matrix(s.matrix);
+    fixed_to_stencil(A, ni, nj, nk, stencil_out);
+  }
+  if (uw) from_buffer(s._u_weights, uw);
+  if (vw) from_buffer(s._v_weights, vw);
+  if (ww) from_buffer(s._w_weights, ww);
+  // pcg_projection keeps the solver's outputs in locals; re-run the same solve
+  // on the assembled system to report them (deterministic: same inputs).
+  if (iterations_out || residual_out) {
+    std::vector<double> p(n, 0.0);
+    double res = 0;
+    int it = 0;
+    bool ok = AMGPCGSolve(s.matrix, s.rhs, p, 1e-6, 50, res, it, ni, nj, nk);
+    if (iterations_out) *iterations_out = it;
+    if (residual_out) *residual_out = res;
+    return ok ? 1 : 0;
+  }
+  return 1;
+}
+
+// SubDomainSolver::advect_field (sub_domain.cpp:191-235): RK2 midpoint
+// backtrace on u,v,w + trilinear sample of `field`.  The field lives on an
+// fnx x fny x fnz grid of spacing h with grid offsets (fox, foy, foz).
+void ref_advect_rk2(int ni, int nj, int nk, float h, float dt, const float* u, const float* v,
+                    const float* w, int fnx, int fny, int fnz, double fox, double foy, double foz,
+                    const float* field, float* out) {
+  SubDomainSolver* sd = new SubDomainSolver();
+  quiet_subdomain(*sd);
+  sd->_nx = ni; sd->_ny = nj; sd->_nz = nk;
+  sd->_hx = sd->_hy = sd->_hz = h;
+  sd->_un.init(ni + 1, nj, nk, h, 0.5, 0, 0);
+  sd->_vn.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0);
+  sd->_wn.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5);
+  to_buffer(sd->_un, u);
+  to_buffer(sd->_vn, v);
+  to_buffer(sd->_wn, w);
+  buffer3Df f, fo;
+  f.init(fnx, fny, fnz, h, fox, foy, foz);
+  fo.init(fnx, fny, fnz, h, fox, foy, foz);
+  to_buffer(f, field);
+  sd->advect_field(dt, f, fo);
+  from_buffer(fo, out);
+  f.free(); fo.free();
+  sd->_un.free(); sd->_vn.free(); sd->_wn.free();
+  // SubDomainSolver's destructor frees buffers this harness never allocated;
+  // those are null and free() skips them.
+  delete sd;
+}
+
+// SmokeSolver3D::hash_FLIP (Smoke_solver3D.cpp:1327-1346): cell of each
+// particle, or -1 when out of range.  Particles are the reference's 40-byte
+// `particle` records (fluid_particle.h:14-65).
+void ref_hash(int ni, int nj, int nk, float h, const void* particles, int np, int* cell_out) {
+  const particle* p = (const particle*)particles;
+  for (int q = 0; q < np; ++q) cell_out[q] = -1;
+  SmokeSolver3D s;
+  quiet_subdomain(s.sub_domain);
+  s._nx = ni; s._ny = nj; s._nz = nk; s._hx = h;
+  s.FLIP.assign(p, p + np);
+  s.particle_hash.resize((size_t)ni * nj * nk);
+  s.hash_FLIP();
+  for (size_t c = 0; c < s.particle_hash.size(); ++c)
+    for (int q : s.particle_hash[c]) cell_out[q] = (int)c;
+}
+
+// SmokeSolver3D::particle_to_grid (Smoke_solver3D.cpp:1451-1510) after
+// hash_FLIP.  component 0/1/2 = u/v/w; field and coef have that face grid's shape.
+void ref_p2g(int ni, int nj, int nk, float h, const void* particles, int np, int component, float* field,
+             float* coef) {
+  const particle* p = (const particle*)particles;
+  SmokeSolver3D s;
+  quiet_subdomain(s.sub_domain);
+  s._nx = ni; s._ny = nj; s._nz = nk; s._hx = s._hy = s._hz = h;
+  s.FLIP.assign(p, p + np);
+  s.particle_hash.resize((size_t)ni * nj * nk);
+  s.hash_FLIP();
+  buffer3Df f, c;
+  if (component == 0) { f.init(ni + 1, nj, nk, h, 0.5, 0, 0); c.init(ni + 1, nj, nk, h, 0.5, 0, 0); }
+  else if (component == 1) { f.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0); c.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0); }
+  else { f.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5); c.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5); }
+  s.particle_to_grid(f, c, component);
+  from_buffer(f, field);
+  from_buffer(c, coef);
+  f.free(); c.free();
+}
+
+// SmokeSolver3D::particle_from_grid (Smoke_solver3D.cpp:1398-1406):
+// vel += trilinear(du, dv, dw) at each particle, in place.
+void ref_g2p(int ni, int nj, int nk, float h, void* particles, int np, const float* du, const float* dv,
+             const float* dw) {
+  particle* p = (particle*)particles;
+  SmokeSolver3D s;
+  quiet_subdomain(s.sub_domain);
+  s._nx = ni; s._ny = nj; s._nz = nk; s._hx = s._hy = s._hz = h;
+  s._utemp.init(ni + 1, nj, nk, h, 0.5, 0, 0);
+  s._vtemp.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0);
+  s._wtemp.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5);
+  to_buffer(s._utemp, du);
+  to_buffer(s._vtemp, dv);
+  to_buffer(s._wtemp, dw);
+  s.FLIP.assign(p, p + np);
+  s.particle_from_grid();
+  for (int q = 0; q < np; ++q) p[q] = s.FLIP[q];
+}
+
+// SmokeSolver3D::getDelta (Smoke_solver3D.cpp:1298-1319): delta = after - before
+// on one nx x ny x nz face grid.
+void ref_delta(int nx, int ny, int nz, const float* after, const float* before, float* delta) {
+  SmokeSolver3D s;
+  quiet_subdomain(s.sub_domain);
+  buffer3Df a, b, d;
+  a.init(nx, ny, nz); b.init(nx, ny, nz); d.init(nx, ny, nz);
+  to_buffer(a, after);
+  to_buffer(b, before);
+  s.getDelta(b, a, d);
+  from_buffer(d, delta);
+  a.free(); b.free(); d.free();
+}
+
+int ref_particle_size() { return (int)sizeof(particle); }
+}

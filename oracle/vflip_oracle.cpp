@@ -1,0 +1,695 @@
+// CPU restatement of the vFLIP hot path: the oracle.
+//
+// TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
+// cpu_baseline leg of bench.py may load this library (oracle/liboracle.so),
+// and only as the checker.  The product (vflip_b200/, libvflip_gpu.so) never
+// links, loads or falls back to it.
+//
+// Each function restates the reference algorithm in this project's own code
+// and cites the reference file:line it follows (paths inside the vFLIP
+// project, Smoke_Solver/ abbreviated SS/).  The restatement keeps the
+// reference's floating-point types and the order of every sum, so its
+// results are bit-identical to the reference's wherever the reference is
+// deterministic; tests/test_oracle_vs_ref.py pins that against the reference
+// compiled from its own sources (oracle/build_ref.py) and against the golden
+// fixtures in tests/golden/.  Build with -ffp-contract=off.
+//
+// Conventions shared with oracle/ref_harness.cpp and the CUDA library:
+//   * linear layout, index = i + ni*(j + nj*k), i fastest;
+//   * cell grid ni x nj x nk; u faces (ni+1) x nj x nk; v ni x (nj+1) x nk;
+//     w ni x nj x (nk+1); nodal solid phi (ni+1) x (nj+1) x (nk+1);
+//   * a 7-point operator is 7 arrays of n doubles, in the order
+//     diag, -x, +x, -y, +y, -z, +z (the CSR column order of one row with the
+//     diagonal moved first).
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+enum { D = 0, XM = 1, XP = 2, YM = 3, YP = 4, ZM = 5, ZP = 6 };
+
+inline size_t lin(int i, int j, int k, int nx, int ny) {
+  return (size_t)i + (size_t)nx * ((size_t)j + (size_t)ny * (size_t)k);
+}
+
+struct Stencil {
+  int ni = 0, nj = 0, nk = 0;
+  size_t n = 0;
+  std::vector<double> a;  // 7 * n
+  void init(int i, int j, int k) {
+    ni = i; nj = j; nk = k;
+    n = (size_t)i * j * k;
+    a.assign(7 * n, 0.0);
+  }
+  double& c(int s, size_t r) { return a[(size_t)s * n + r]; }
+  double c(int s, size_t r) const { return a[(size_t)s * n + r]; }
+};
+
+// Off-diagonal slots in CSR column order (ascending column index):
+// -z, -y, -x, +x, +y, +z.  SS/AlgebraicMultigrid.h:44-54 walks a row in this
+// order, skipping the diagonal.
+const int kOffOrder[6] = {ZM, YM, XM, XP, YP, ZP};
+
+inline bool nb(const Stencil& A, int i, int j, int k, int s, size_t& q) {
+  int ii = i, jj = j, kk = k;
+  switch (s) {
+    case XM: ii--; break; case XP: ii++; break;
+    case YM: jj--; break; case YP: jj++; break;
+    case ZM: kk--; break; case ZP: kk++; break;
+    default: break;
+  }
+  if (ii < 0 || jj < 0 || kk < 0 || ii >= A.ni || jj >= A.nj || kk >= A.nk) return false;
+  q = lin(ii, jj, kk, A.ni, A.nj);
+  return true;
+}
+
+// levelGen::generateLevelsGalerkinCoarsening, SS/GeometricLevelGen.h:28-71,
+// with R and P from levelGen::generateRP, SS/GeometricLevelGen.cpp:41-66
+// (R = 1/8 over the up-to-8 children, P = injection) and the two SpGEMMs
+// temp = A*P (scale 1), A_c = 0.5*R*temp (SS/sparse_matrix.h:370-405).
+// Multiplying by 0.0625 (= 0.5*0.125) is exact, so
+//   A_c(I,J) = 0.0625 * sum_{child c of I, ascending} temp(c,J),
+//   temp(c,J) = sum_{entries of row c in column order with parent J} A(c,.)
+// reproduces the SpGEMM's sums term for term.
+void coarsen(const Stencil& A, Stencil& C) {
+  int cni = C.ni, cnj = C.nj, cnk = C.nk;
+  for (int K = 0; K < cnk; ++K)
+    for (int J = 0; J < cnj; ++J)
+      for (int I = 0; I < cni; ++I) {
+        size_t rc = lin(I, J, K, cni, cnj);
+        double acc[7];
+        bool have[7] = {false, false, false, false, false, false, false};
+        for (int s = 0; s < 7; ++s) acc[s] = 0.0;
+        // children in ascending fine index: kk outer, then jj, then ii
+        for (int kk = 0; kk <= 1; ++kk)
+          for (int jj = 0; jj <= 1; ++jj)
+            for (int ii = 0; ii <= 1; ++ii) {
+              int fi = 2 * I + ii, fj = 2 * J + jj, fk = 2 * K + kk;
+              if (fi >= A.ni || fj >= A.nj || fk >= A.nk) continue;
+              size_t rf = lin(fi, fj, fk, A.ni, A.nj);
+              // temp row rf: walk the fine row in column order, bucket by parent
+              double t[7];
+              bool th[7] = {false, false, false, false, false, false, false};
+              const int order[7] = {ZM, YM, XM, D, XP, YP, ZP};
+              for (int o = 0; o < 7; ++o) {
+                int s = order[o];
+                size_t q;
+                if (s != D && !nb(A, fi, fj, fk, s, q)) continue;
+                // coarse column of the entry's column cell
+                int ci = fi, cj = fj, ck = fk;
+                if (s == XM) ci--; else if (s == XP) ci++;
+                else if (s == YM) cj--; else if (s == YP) cj++;
+                else if (s == ZM) ck--; else if (s == ZP) ck++;
+                int PI = ci / 2, PJ = cj / 2, PK = ck / 2;
+                int slot;
+                if (PI == I && PJ == J && PK == K) slot = D;
+                else if (PI == I - 1) slot = XM; else if (PI == I + 1) slot = XP;
+                else if (PJ == J - 1) slot = YM; else if (PJ == J + 1) slot = YP;
+                else if (PK == K - 1) slot = ZM; else slot = ZP;
+                double v = A.c(s, rf);
+                if (!th[slot]) { t[slot] = v; th[slot] = true; }
+                else t[slot] += v;
+              }
+              for (int s = 0; s < 7; ++s) {
+                if (!th[s]) continue;
+                double v = 0.0625 * t[s];
+                if (!have[s]) { acc[s] = v; have[s] = true; }
+                else acc[s] += v;
+              }
+            }
+        for (int s = 0; s < 7; ++s) C.c(s, rc) = acc[s];
+      }
+}
+
+void build_levels(const Stencil& A0, std::vector<Stencil>& L) {
+  L.clear();
+  L.push_back(A0);
+  int ni = A0.ni, nj = A0.nj, nk = A0.nk;
+  unsigned unknowns = (unsigned)ni * nj * nk;
+  while (unknowns > 16 * 16 * 16) {  // SS/GeometricLevelGen.h:46-58
+    ni = (int)std::ceil((float)ni / 2.0);
+    nj = (int)std::ceil((float)nj / 2.0);
+    nk = (int)std::ceil((float)nk / 2.0);
+    unknowns = (unsigned)ni * nj * nk;
+    Stencil C;
+    C.init(ni, nj, nk);
+    coarsen(L.back(), C);
+    L.push_back(std::move(C));
+  }
+}
+
+// ivock::RBGS, SS/AlgebraicMultigrid.h:22-103: colour (i+j+k) odd first,
+// then even; off-diagonal sum in CSR column order; x = 0 where diag == 0.
+void rbgs(const Stencil& A, const double* b, double* x, int iters) {
+  for (int it = 0; it < iters; ++it)
+    for (int colour = 1; colour >= 0; --colour)
+      for (int k = 0; k < A.nk; ++k)
+        for (int j = 0; j < A.nj; ++j)
+          for (int i = 0; i < A.ni; ++i) {
+            if (((i + j + k) & 1) != colour) continue;
+            size_t r = lin(i, j, k, A.ni, A.nj);
+            double sum = 0;
+            for (int o = 0; o < 6; ++o) {
+              size_t q;
+              if (!nb(A, i, j, k, kOffOrder[o], q)) continue;
+              sum += A.c(kOffOrder[o], r) * x[q];
+            }
+            double diag = A.c(D, r);
+            x[r] = (diag != 0) ? (b[r] - sum) / diag : 0;
+          }
+}
+
+// restriction, SS/AlgebraicMultigrid.h:105-117: r = b - A x with
+// multiply_and_subtract (SS/sparse_matrix.h:460-480, subtracting entry by
+// entry in column order, diagonal included), then b_c = R r.
+void restrict_residual(const Stencil& A, const double* x, const double* b, const Stencil& C, double* bc) {
+  std::vector<double> r(A.n);
+  const int order[7] = {ZM, YM, XM, D, XP, YP, ZP};
+  for (int k = 0; k < A.nk; ++k)
+    for (int j = 0; j < A.nj; ++j)
+      for (int i = 0; i < A.ni; ++i) {
+        size_t row = lin(i, j, k, A.ni, A.nj);
+        double v = b[row];
+        for (int o = 0; o < 7; ++o) {
+          size_t q = row;
+          if (order[o] != D && !nb(A, i, j, k, order[o], q)) continue;
+          v -= A.c(order[o], row) * x[q];
+        }
+        r[row] = v;
+      }
+  // b_c = R r: multiply() starts at 0 and adds 0.125*r over the children in
+  // ascending column order (SS/sparse_matrix.h:356-362, GeometricLevelGen.cpp:51-64)
+  for (int K = 0; K < C.nk; ++K)
+    for (int J = 0; J < C.nj; ++J)
+      for (int I = 0; I < C.ni; ++I) {
+        double s = 0;
+        for (int kk = 0; kk <= 1; ++kk)
+          for (int jj = 0; jj <= 1; ++jj)
+            for (int ii = 0; ii <= 1; ++ii) {
+              int fi = 2 * I + ii, fj = 2 * J + jj, fk = 2 * K + kk;
+              if (fi >= A.ni || fj >= A.nj || fk >= A.nk) continue;
+              s += 0.125 * r[lin(fi, fj, fk, A.ni, A.nj)];
+            }
+        bc[lin(I, J, K, C.ni, C.nj)] = s;
+      }
+}
+
+// prolongatoin, SS/AlgebraicMultigrid.h:118-129: x_f += P x_c (injection).
+void prolong_add(const Stencil& A, const Stencil& C, const double* xc, double* xf) {
+  for (int k = 0; k < A.nk; ++k)
+    for (int j = 0; j < A.nj; ++j)
+      for (int i = 0; i < A.ni; ++i)
+        xf[lin(i, j, k, A.ni, A.nj)] += xc[lin(i / 2, j / 2, k / 2, C.ni, C.nj)];
+}
+
+// amgVCycle / amgPrecond, SS/AlgebraicMultigrid.h:130-188: V(4,4), 200
+// sweeps on the coarsest level, all level vectors start at zero.
+void vcycle(const std::vector<Stencil>& L, const double* b, double* x) {
+  size_t nl = L.size();
+  std::vector<std::vector<double>> xs(nl), bs(nl);
+  for (size_t l = 0; l < nl; ++l) { xs[l].assign(L[l].n, 0.0); bs[l].assign(L[l].n, 0.0); }
+  std::memcpy(bs[0].data(), b, sizeof(double) * L[0].n);
+  for (size_t l = 0; l + 1 < nl; ++l) {
+    rbgs(L[l], bs[l].data(), xs[l].data(), 4);
+    restrict_residual(L[l], xs[l].data(), bs[l].data(), L[l + 1], bs[l + 1].data());
+  }
+  rbgs(L[nl - 1], bs[nl - 1].data(), xs[nl - 1].data(), 200);
+  for (int l = (int)nl - 2; l >= 0; --l) {
+    prolong_add(L[l], L[l + 1], xs[l + 1].data(), xs[l].data());
+    rbgs(L[l], bs[l].data(), xs[l].data(), 4);
+  }
+  std::memcpy(x, xs[0].data(), sizeof(double) * L[0].n);
+}
+
+// multiply, SS/sparse_matrix.h:342-366: y = A s, row sum in column order from 0.
+void spmv(const Stencil& A, const double* s, double* y) {
+  const int order[7] = {ZM, YM, XM, D, XP, YP, ZP};
+  for (int k = 0; k < A.nk; ++k)
+    for (int j = 0; j < A.nj; ++j)
+      for (int i = 0; i < A.ni; ++i) {
+        size_t row = lin(i, j, k, A.ni, A.nj);
+        double v = 0;
+        for (int o = 0; o < 7; ++o) {
+          size_t q = row;
+          if (order[o] != D && !nb(A, i, j, k, order[o], q)) continue;
+          v += A.c(order[o], row) * s[q];
+        }
+        y[row] = v;
+      }
+}
+
+// BLAS::dot (serial, index order) and BLAS::abs_max (first strict maximum of
+// |x|, NaN never wins), SS/blas_wrapper.h:13-43.
+double dot(const std::vector<double>& x, const std::vector<double>& y) {
+  double s = 0;
+  for (size_t i = 0; i < x.size(); ++i) s += x[i] * y[i];
+  return s;
+}
+double abs_max(const std::vector<double>& x) {
+  double m = 0;
+  size_t at = 0;
+  for (size_t i = 0; i < x.size(); ++i)
+    if (std::fabs(x[i]) > m) { m = std::fabs(x[i]); at = i; }
+  return x.empty() ? 0.0 : std::fabs(x[at]);
+}
+
+// AMGPCGSolve, SS/AlgebraicMultigrid.h:189-301.
+int amgpcg(const Stencil& A0, const double* rhs, double* result, double tol_factor, int maxit,
+           double* residual_out, int* iterations_out) {
+  std::vector<Stencil> L;
+  build_levels(A0, L);
+  size_t n = A0.n;
+  std::vector<double> x(n, 0.0), r(rhs, rhs + n), z(n), s(n);
+  double res = abs_max(r);
+  *residual_out = res;
+  if (res == 0) {
+    *iterations_out = 0;
+    std::memcpy(result, x.data(), sizeof(double) * n);
+    return 1;
+  }
+  double tol = tol_factor * res;
+  vcycle(L, r.data(), z.data());
+  double rho = dot(z, r);
+  if (rho == 0 || rho != rho) {
+    *iterations_out = 0;
+    std::memcpy(result, x.data(), sizeof(double) * n);
+    return 0;
+  }
+  s = z;
+  int it;
+  for (it = 0; it < maxit; ++it) {
+    spmv(A0, s.data(), z.data());
+    double alpha = rho / dot(s, z);
+    for (size_t q = 0; q < n; ++q) x[q] += alpha * s[q];
+    for (size_t q = 0; q < n; ++q) r[q] += -alpha * z[q];
+    res = abs_max(r);
+    *residual_out = res;
+    if (res <= tol) {
+      *iterations_out = it + 1;
+      std::memcpy(result, x.data(), sizeof(double) * n);
+      return 1;
+    }
+    vcycle(L, r.data(), z.data());
+    double rho_new = dot(z, r);
+    double beta = rho_new / rho;
+    for (size_t q = 0; q < n; ++q) z[q] += beta * s[q];
+    s.swap(z);
+    rho = rho_new;
+  }
+  *iterations_out = it;
+  std::memcpy(result, x.data(), sizeof(double) * n);
+  return 0;
+}
+
+Stencil from_arrays(int ni, int nj, int nk, const double* st) {
+  Stencil A;
+  A.init(ni, nj, nk);
+  std::memcpy(A.a.data(), st, sizeof(double) * 7 * A.n);
+  return A;
+}
+
+// fraction_inside, SS/levelset_util.cpp:4-13 (segment) and :23-103 (square).
+float frac2(float l, float r) {
+  if (l < 0 && r < 0) return 1;
+  if (l < 0 && r >= 0) return l / (l - r);
+  if (l >= 0 && r < 0) return r / (r - l);
+  return 0;
+}
+void rotate4(float* a) {
+  float t = a[0];
+  a[0] = a[1]; a[1] = a[2]; a[2] = a[3]; a[3] = t;
+}
+float frac4(float bl, float br, float tl, float tr) {
+  int inside = (bl <= 0) + (tl <= 0) + (br <= 0) + (tr <= 0);
+  float q[4] = {bl, br, tr, tl};
+  if (inside == 4) return 1;
+  if (inside == 3) {
+    while (q[0] < 0) rotate4(q);
+    float s0 = 1 - frac2(q[0], q[3]);
+    float s1 = 1 - frac2(q[0], q[1]);
+    return 1 - 0.5f * s0 * s1;
+  }
+  if (inside == 2) {
+    while (q[0] >= 0 || !(q[1] < 0 || q[2] < 0)) rotate4(q);
+    if (q[1] < 0) return 0.5f * (frac2(q[0], q[3]) + frac2(q[1], q[2]));
+    float mid = 0.25f * (q[0] + q[1] + q[2] + q[3]);
+    if (mid < 0) {
+      float area = 0;
+      float s1 = 1 - frac2(q[0], q[3]);
+      float s3 = 1 - frac2(q[2], q[3]);
+      area += 0.5f * s1 * s3;
+      float s2 = 1 - frac2(q[2], q[1]);
+      float s0 = 1 - frac2(q[0], q[1]);
+      area += 0.5f * s0 * s2;
+      return 1 - area;
+    }
+    float area = 0;
+    float s0 = frac2(q[0], q[1]);
+    float s1 = frac2(q[0], q[3]);
+    area += 0.5f * s0 * s1;
+    float s2 = frac2(q[2], q[1]);
+    float s3 = frac2(q[2], q[3]);
+    area += 0.5f * s2 * s3;
+    return area;
+  }
+  if (inside == 1) {
+    while (q[0] >= 0) rotate4(q);
+    float s0 = frac2(q[0], q[3]);
+    float s1 = frac2(q[0], q[1]);
+    return 0.5f * s0 * s1;
+  }
+  return 0;
+}
+inline float clamp01(float a) { return a < 0.0f ? 0.0f : (a > 1.0f ? 1.0f : a); }  // SS/util.h:172-177
+
+// SmokeSolver3D::compute_face_weights, SS/Smoke_solver3D.cpp:874-944.
+void face_weights(int ni, int nj, int nk, const float* phi, float* uw, float* vw, float* ww) {
+  int px = ni + 1, py = nj + 1;
+  auto P = [&](int i, int j, int k) { return phi[lin(i, j, k, px, py)]; };
+  for (int k = 0; k < nk; ++k)
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i <= ni; ++i)
+        uw[lin(i, j, k, ni + 1, nj)] =
+            clamp01(1 - frac4(P(i, j, k), P(i, j + 1, k), P(i, j, k + 1), P(i, j + 1, k + 1)));
+  for (int k = 0; k < nk; ++k)
+    for (int j = 0; j <= nj; ++j)
+      for (int i = 0; i < ni; ++i)
+        vw[lin(i, j, k, ni, nj + 1)] =
+            clamp01(1 - frac4(P(i, j, k), P(i, j, k + 1), P(i + 1, j, k), P(i + 1, j, k + 1)));
+  for (int k = 0; k <= nk; ++k)
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i < ni; ++i)
+        ww[lin(i, j, k, ni, nj)] =
+            clamp01(1 - frac4(P(i, j, k), P(i, j + 1, k), P(i + 1, j, k), P(i + 1, j + 1, k)));
+}
+
+// One trilinear sample of a face/cell grid, Buffer3D::sample_linear and
+// Buffer3D::at, SS/fluid_buffer3D.h:205-248: world -> grid in double,
+// clamp-to-edge indices, lerps in double, result rounded to float.
+struct Grid {
+  const float* d;
+  int nx, ny, nz;
+  double h, ox, oy, oz;
+  float at(int i, int j, int k) const {
+    i = i < 0 ? 0 : (i > nx - 1 ? nx - 1 : i);
+    j = j < 0 ? 0 : (j > ny - 1 ? ny - 1 : j);
+    k = k < 0 ? 0 : (k > nz - 1 ? nz - 1 : k);
+    return d[lin(i, j, k, nx, ny)];
+  }
+  static double lerp(double a, double b, double c) { return (1.0 - c) * a + c * b; }
+  float sample(double wx, double wy, double wz) const {
+    double gx = wx / h + ox, gy = wy / h + oy, gz = wz / h + oz;
+    int i = (int)std::floor(gx), j = (int)std::floor(gy), k = (int)std::floor(gz);
+    double cx = gx - (double)i, cy = gy - (double)j, cz = gz - (double)k;
+    double v1 = lerp(lerp(at(i, j, k), at(i + 1, j, k), cx), lerp(at(i, j + 1, k), at(i + 1, j + 1, k), cx), cy);
+    double v2 = lerp(lerp(at(i, j, k + 1), at(i + 1, j, k + 1), cx),
+                     lerp(at(i, j + 1, k + 1), at(i + 1, j + 1, k + 1), cx), cy);
+    return (float)lerp(v1, v2, cz);
+  }
+};
+
+struct Particle {  // SS/fluid_particle.h:14-20, 40 bytes
+  float pos[3];
+  float vel[3];
+  float dens, temp;
+  int hash_idx, sub_hash_idx;
+};
+static_assert(sizeof(Particle) == 40, "particle record is 40 bytes");
+
+// SmokeSolver3D::hash_FLIP, SS/Smoke_solver3D.cpp:1337-1343: cell =
+// int((pos + 0.5h)/h) per axis (truncation toward zero, float arithmetic).
+int hash_cell(const Particle& p, int ni, int nj, int nk, float h) {
+  float c = 0.5f * h;
+  int ijk[3];
+  int n[3] = {ni, nj, nk};
+  for (int a = 0; a < 3; ++a) {
+    float t = (p.pos[a] + c) / h;
+    // the reference converts with a C cast; anything outside (-1, n) or NaN
+    // lands outside [0, n) on x86 and is dropped
+    if (!(t > -1.0f && t < (float)n[a])) return -1;
+    ijk[a] = (int)t;
+  }
+  return ijk[2] * ni * nj + ijk[1] * ni + ijk[0];
+}
+
+inline float tent(float r) {  // SmokeSolver3D::H, SS/Smoke_solver3D.h:217-223
+  float res = 0;
+  if (r >= -1 && r < 0) res = 1 + r;
+  if (r >= 0 && r < 1) res = 1 - r;
+  return res;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_levels(int ni, int nj, int nk, const double* st0, int max_levels, int* dims_out, double* st_out) {
+  std::vector<Stencil> L;
+  build_levels(from_arrays(ni, nj, nk, st0), L);
+  size_t off = 0;
+  for (size_t l = 0; l < L.size() && (int)l < max_levels; ++l) {
+    dims_out[3 * l] = L[l].ni; dims_out[3 * l + 1] = L[l].nj; dims_out[3 * l + 2] = L[l].nk;
+    if (st_out) {
+      std::memcpy(st_out + off, L[l].a.data(), sizeof(double) * 7 * L[l].n);
+      off += 7 * L[l].n;
+    }
+  }
+  return (int)L.size();
+}
+
+void oracle_rbgs(int ni, int nj, int nk, const double* st, const double* b, double* x, int iters) {
+  rbgs(from_arrays(ni, nj, nk, st), b, x, iters);
+}
+
+void oracle_vcycle(int ni, int nj, int nk, const double* st, const double* b, double* x) {
+  std::vector<Stencil> L;
+  build_levels(from_arrays(ni, nj, nk, st), L);
+  vcycle(L, b, x);
+}
+
+void oracle_spmv(int ni, int nj, int nk, const double* st, const double* s, double* y) {
+  spmv(from_arrays(ni, nj, nk, st), s, y);
+}
+
+int oracle_amgpcg(int ni, int nj, int nk, const double* st, const double* rhs, double* result, double tol,
+                  int maxit, double* residual_out, int* iterations_out) {
+  return amgpcg(from_arrays(ni, nj, nk, st), rhs, result, tol, maxit, residual_out, iterations_out);
+}
+
+void oracle_fraction_inside4(int n, const float* bl, const float* br, const float* tl, const float* tr,
+                             float* out) {
+  for (int q = 0; q < n; ++q) out[q] = frac4(bl[q], br[q], tl[q], tr[q]);
+}
+
+void oracle_face_weights(int ni, int nj, int nk, float h, const float* phi, float* uw, float* vw, float* ww) {
+  (void)h;
+  face_weights(ni, nj, nk, phi, uw, vw, ww);
+}
+
+// SmokeSolver3D::pcg_projection, SS/Smoke_solver3D.cpp:945-1202.  Same
+// argument meaning as ref_project in oracle/ref_harness.cpp.
+int oracle_project(int ni, int nj, int nk, float h, float U_in, const float* phi, const int8_t* bdesc,
+                   const float* us, const float* vs, const float* ws, float* u, float* v, float* w,
+                   double* pressure_out, double* rhs_out, double* st_out, float* uw_out, float* vw_out,
+                   float* ww_out, int* iterations_out, double* residual_out) {
+  size_t n = (size_t)ni * nj * nk;
+  size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
+  std::vector<float> uw(nu), vw(nv), ww(nw);
+  face_weights(ni, nj, nk, phi, uw.data(), vw.data(), ww.data());
+  auto U = [&](int i, int j, int k) -> float& { return u[lin(i, j, k, ni + 1, nj)]; };
+  auto V = [&](int i, int j, int k) -> float& { return v[lin(i, j, k, ni, nj + 1)]; };
+  auto W = [&](int i, int j, int k) -> float& { return w[lin(i, j, k, ni, nj)]; };
+  auto UW = [&](int i, int j, int k) { return uw[lin(i, j, k, ni + 1, nj)]; };
+  auto VW = [&](int i, int j, int k) { return vw[lin(i, j, k, ni, nj + 1)]; };
+  auto WW = [&](int i, int j, int k) { return ww[lin(i, j, k, ni, nj)]; };
+  auto US = [&](int i, int j, int k) { return us[lin(i, j, k, ni + 1, nj)]; };
+  auto VS = [&](int i, int j, int k) { return vs[lin(i, j, k, ni, nj + 1)]; };
+  auto WS = [&](int i, int j, int k) { return ws[lin(i, j, k, ni, nj)]; };
+  // inflow overwrite, :964-980
+  for (int k = 0; k < nk; ++k)
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i < ni; ++i)
+        if (bdesc[lin(i, j, k, ni, nj)] == 1) {
+          U(i, j, k) = U_in; U(i + 1, j, k) = U_in;
+          V(i, j, k) = 0; V(i, j + 1, k) = 0;
+          W(i, j, k) = 0; W(i, j, k + 1) = 0;
+        }
+  // assembly over interior cells, :984-1111
+  Stencil A;
+  A.init(ni, nj, nk);
+  std::vector<double> rhs(n, 0.0);
+  float h2 = h * h;  // sqr(_hx), float
+  for (int k = 1; k < nk - 1; ++k)
+    for (int j = 1; j < nj - 1; ++j)
+      for (int i = 1; i < ni - 1; ++i) {
+        size_t r = lin(i, j, k, ni, nj);
+        double diag;
+        double b = 0;
+        float t;
+        t = UW(i + 1, j, k) / h2; diag = t; if (i < ni - 2) A.c(XP, r) = -t;
+        b -= UW(i + 1, j, k) * U(i + 1, j, k) / h;
+        t = UW(i, j, k) / h2; diag += t; if (i >= 2) A.c(XM, r) = -t;
+        b += UW(i, j, k) * U(i, j, k) / h;
+        t = VW(i, j + 1, k) / h2; diag += t; if (j < nj - 2) A.c(YP, r) = -t;
+        b -= VW(i, j + 1, k) * V(i, j + 1, k) / h;
+        t = VW(i, j, k) / h2; diag += t; if (j >= 2) A.c(YM, r) = -t;
+        b += VW(i, j, k) * V(i, j, k) / h;
+        t = WW(i, j, k + 1) / h2; diag += t; if (k < nk - 2) A.c(ZP, r) = -t;
+        b -= WW(i, j, k + 1) * W(i, j, k + 1) / h;
+        t = WW(i, j, k) / h2; diag += t; if (k >= 2) A.c(ZM, r) = -t;
+        b += WW(i, j, k) * W(i, j, k) / h;
+        A.c(D, r) = diag;
+        if (diag > 0) {
+          float sv = (UW(i + 1, j, k) - 1.0f) * US(i + 1, j, k) - (UW(i, j, k) - 1.0f) * US(i, j, k) +
+                     (VW(i, j + 1, k) - 1.0f) * VS(i, j + 1, k) - (VW(i, j, k) - 1.0f) * VS(i, j, k) +
+                     (WW(i, j, k + 1) - 1.0f) * WS(i, j, k + 1) - (WW(i, j, k) - 1.0f) * WS(i, j, k);
+          b += 1.0 / h * sv;
+        }
+        rhs[r] = b;
+      }
+  std::vector<double> p(n, 0.0);
+  double res = 0;
+  int it = 0;
+  int ok = amgpcg(A, rhs.data(), p.data(), 1e-6, 50, &res, &it);  // :1120
+  // gradient update, :1126-1200
+  for (int k = 1; k < nk - 1; ++k)
+    for (int j = 1; j < nj - 1; ++j)
+      for (int i = 2; i <= ni - 2; ++i) {
+        size_t r = lin(i, j, k, ni, nj);
+        if (UW(i, j, k) > 0) U(i, j, k) -= (float)(p[r] - p[r - 1]) / h;
+        else U(i, j, k) = US(i, j, k);
+      }
+  for (int k = 1; k < nk - 1; ++k)
+    for (int j = 2; j <= nj - 2; ++j)
+      for (int i = 1; i < ni - 1; ++i) {
+        size_t r = lin(i, j, k, ni, nj);
+        if (VW(i, j, k) > 0) V(i, j, k) -= (float)(p[r] - p[r - ni]) / h;
+        else V(i, j, k) = VS(i, j, k);
+      }
+  for (int k = 2; k <= nk - 2; ++k)
+    for (int j = 1; j < nj - 1; ++j)
+      for (int i = 1; i < ni - 1; ++i) {
+        size_t r = lin(i, j, k, ni, nj);
+        if (WW(i, j, k) > 0) W(i, j, k) -= (float)(p[r] - p[r - (size_t)ni * nj]) / h;
+        else W(i, j, k) = WS(i, j, k);
+      }
+  if (pressure_out) std::memcpy(pressure_out, p.data(), sizeof(double) * n);
+  if (rhs_out) std::memcpy(rhs_out, rhs.data(), sizeof(double) * n);
+  if (st_out) std::memcpy(st_out, A.a.data(), sizeof(double) * 7 * n);
+  if (uw_out) std::memcpy(uw_out, uw.data(), sizeof(float) * nu);
+  if (vw_out) std::memcpy(vw_out, vw.data(), sizeof(float) * nv);
+  if (ww_out) std::memcpy(ww_out, ww.data(), sizeof(float) * nw);
+  if (iterations_out) *iterations_out = it;
+  if (residual_out) *residual_out = res;
+  return ok;
+}
+
+// SubDomainSolver::advect_field, SS/sub_domain.cpp:191-235 (RK2 midpoint
+// backtrace, trilinear sample).  Same arguments as ref_advect_rk2.
+void oracle_advect_rk2(int ni, int nj, int nk, float h, float dt, const float* u, const float* v, const float* w,
+                       int fnx, int fny, int fnz, double fox, double foy, double foz, const float* field,
+                       float* out) {
+  Grid gu{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0};
+  Grid gv{v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0};
+  Grid gw{w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5};
+  Grid gf{field, fnx, fny, fnz, (double)h, fox, foy, foz};
+  for (int k = 0; k < fnz; ++k)
+    for (int j = 0; j < fny; ++j)
+      for (int i = 0; i < fnx; ++i) {
+        float wx = (float)(((double)(float)i - fox) * (double)h);
+        float wy = (float)(((double)(float)j - foy) * (double)h);
+        float wz = (float)(((double)(float)k - foz) * (double)h);
+        float a = gu.sample(wx, wy, wz), b = gv.sample(wx, wy, wz), c = gw.sample(wx, wy, wz);
+        float px = (float)((double)wx - 0.5 * (double)dt * (double)a);
+        float py = (float)((double)wy - 0.5 * (double)dt * (double)b);
+        float pz = (float)((double)wz - 0.5 * (double)dt * (double)c);
+        a = gu.sample(px, py, pz); b = gv.sample(px, py, pz); c = gw.sample(px, py, pz);
+        px = wx - dt * a; py = wy - dt * b; pz = wz - dt * c;
+        out[lin(i, j, k, fnx, fny)] = gf.sample(px, py, pz);
+      }
+}
+
+void oracle_hash(int ni, int nj, int nk, float h, const void* particles, int np, int* cell_out) {
+  const Particle* p = (const Particle*)particles;
+  for (int q = 0; q < np; ++q) cell_out[q] = hash_cell(p[q], ni, nj, nk, h);
+}
+
+// SmokeSolver3D::particle_to_grid, SS/Smoke_solver3D.cpp:1451-1510, over the
+// buckets hash_FLIP builds (particles of a cell in ascending index order).
+void oracle_p2g(int ni, int nj, int nk, float h, const void* particles, int np, int comp, float* field,
+                float* coef) {
+  const Particle* p = (const Particle*)particles;
+  size_t nc = (size_t)ni * nj * nk;
+  std::vector<int> cell(np), start(nc + 1, 0), order(np);
+  for (int q = 0; q < np; ++q) {
+    cell[q] = hash_cell(p[q], ni, nj, nk, h);
+    if (cell[q] >= 0) start[cell[q] + 1]++;
+  }
+  for (size_t c = 0; c < nc; ++c) start[c + 1] += start[c];
+  std::vector<int> fill(start.begin(), start.end() - 1);
+  for (int q = 0; q < np; ++q)
+    if (cell[q] >= 0) order[fill[cell[q]]++] = q;
+  int fx = ni + (comp == 0), fy = nj + (comp == 1), fz = nk + (comp == 2);
+  double ox = comp == 0 ? 0.5 : 0.0, oy = comp == 1 ? 0.5 : 0.0, oz = comp == 2 ? 0.5 : 0.0;
+  for (int k = 0; k < fz; ++k)
+    for (int j = 0; j < fy; ++j)
+      for (int i = 0; i < fx; ++i) {
+        float gx = (float)(((double)(float)i - ox) * (double)h);
+        float gy = (float)(((double)(float)j - oy) * (double)h);
+        float gz = (float)(((double)(float)k - oz) * (double)h);
+        float tw = 1e-5f, tv = 0;
+        for (int dk = -1; dk <= 1; ++dk)
+          for (int dj = -1; dj <= 1; ++dj)
+            for (int di = -1; di <= 1; ++di) {
+              int ci = i + di, cj = j + dj, ck = k + dk;
+              if (ci < 0 || cj < 0 || ck < 0 || ci >= ni || cj >= nj || ck >= nk) continue;
+              size_t c = lin(ci, cj, ck, ni, nj);
+              for (int e = start[c]; e < start[c + 1]; ++e) {
+                const Particle& pp = p[order[e]];
+                float wgt = tent((pp.pos[0] - gx) / h) * tent((pp.pos[1] - gy) / h) * tent((pp.pos[2] - gz) / h);
+                tw += wgt;
+                tv += wgt * pp.vel[comp];
+              }
+            }
+        coef[lin(i, j, k, fx, fy)] = tw;
+        field[lin(i, j, k, fx, fy)] = tv / tw;
+      }
+}
+
+// SmokeSolver3D::particle_from_grid, SS/Smoke_solver3D.cpp:1398-1406
+// (flip_ratio == 1: vel += trilinear(delta)); otherwise the FLIP/PIC blend of
+// fluid_particle::interpolate, SS/fluid_particle.h:315-328, in double:
+// vel = (1-f)*u_new(pos) + f*(vel + delta(pos)).
+void oracle_g2p(int ni, int nj, int nk, float h, void* particles, int np, const float* du, const float* dv,
+                const float* dw, const float* un, const float* vn, const float* wn, double flip_ratio) {
+  Particle* p = (Particle*)particles;
+  Grid g[3] = {{du, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0},
+               {dv, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0},
+               {dw, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5}};
+  Grid gn[3] = {{un, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0},
+                {vn, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0},
+                {wn, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5}};
+  for (int q = 0; q < np; ++q) {
+    double x = p[q].pos[0], y = p[q].pos[1], z = p[q].pos[2];
+    float d[3] = {g[0].sample(x, y, z), g[1].sample(x, y, z), g[2].sample(x, y, z)};
+    if (flip_ratio == 1.0) {
+      for (int a = 0; a < 3; ++a) p[q].vel[a] += d[a];
+    } else {
+      for (int a = 0; a < 3; ++a) {
+        float s = gn[a].sample(x, y, z);
+        p[q].vel[a] = (float)((1.0 - flip_ratio) * (double)s + flip_ratio * (double)(p[q].vel[a] + d[a]));
+      }
+    }
+  }
+}
+
+// SmokeSolver3D::getDelta, SS/Smoke_solver3D.cpp:1298-1319.
+void oracle_delta(int nx, int ny, int nz, const float* after, const float* before, float* delta) {
+  size_t n = (size_t)nx * ny * nz;
+  for (size_t q = 0; q < n; ++q) delta[q] = after[q] - before[q];
+}
+
+int oracle_particle_size() { return (int)sizeof(Particle); }
+}
