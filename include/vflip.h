@@ -1,0 +1,211 @@
+/* vflip.h - C ABI of the B200 (sm_100a) implementation of the vFLIP per-step
+ * hot path: the MGPCG pressure projection, RK2 semi-Lagrangian advection and
+ * the FLIP particle<->grid transfers.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and
+ * returns an int status (never aborts, never throws):
+ *     VFLIP_OK (0)              success / solver converged
+ *     VFLIP_NOT_CONVERGED (1)   solver hit max_iterations or met a zero/NaN
+ *                               rho; the reference's `false`
+ *     negative                  argument or CUDA error; vflip_last_error()
+ *                               describes it.
+ *
+ * Memory: unless a parameter is documented as a host pointer, pointers are
+ * device pointers on the context's device, and the call is ordered on the
+ * context's stream (vflip_config.stream, or a stream the context creates).
+ * Entry points that return solver statistics synchronise that stream.
+ *
+ * Grids are dense and linear, index = i + ni*(j + nj*k) (i fastest), the
+ * order of the reference's pressure vector (Smoke_solver3D.cpp:993).  For an
+ * ni x nj x nk cell grid of spacing h:
+ *     cell   ni*nj*nk                 u faces (ni+1)*nj*nk
+ *     v      ni*(nj+1)*nk             w faces ni*nj*(nk+1)
+ *     nodal solid phi (ni+1)*(nj+1)*(nk+1)
+ * A 7-point operator is passed as four FP64 arrays (diag, xp, yp, zp): the
+ * diagonal and the couplings to the +x, +y, +z neighbours; the operator is
+ * symmetric, so the -x coupling of cell c is xp[c-1].
+ *
+ * Reference file:line citations are paths inside the vFLIP project
+ * (Smoke_Solver/ abbreviated SS/).
+ */
+#ifndef VFLIP_H
+#define VFLIP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VFLIP_OK 0
+#define VFLIP_NOT_CONVERGED 1
+#define VFLIP_ERR_ARG (-1)
+#define VFLIP_ERR_CUDA (-2)
+#define VFLIP_ERR_NOT_7POINT (-3)
+#define VFLIP_ERR_NOT_SYMMETRIC (-4)
+#define VFLIP_ERR_NOMEM (-5)
+
+/* Arithmetic of the multigrid-preconditioned CG.
+ *   FP64  - everything in FP64; the V-cycle is bit-identical to the
+ *           reference's (the "FP64 GPU oracle solve").
+ *   FP32  - vectors, operator and V-cycle in FP32; PCG inner products,
+ *           residual norm and alpha/beta in FP64.
+ *   MIXED - FP32 fine level, BF16 storage of the coarse-level operators,
+ *           FP32 coarse vectors, FP64 scalars. */
+typedef enum { VFLIP_PREC_FP64 = 0, VFLIP_PREC_FP32 = 1, VFLIP_PREC_MIXED = 2 } vflip_precision;
+
+typedef struct {
+  int precision;             /* vflip_precision, default VFLIP_PREC_FP32 */
+  int pre_sweeps;            /* RBGS sweeps before restriction, default 4 (SS/AlgebraicMultigrid.h:156) */
+  int post_sweeps;           /* RBGS sweeps after prolongation, default 4 (SS/AlgebraicMultigrid.h:164) */
+  int coarse_sweeps;         /* RBGS sweeps on the coarsest level, default 200 (SS/AlgebraicMultigrid.h:160) */
+  int coarsest_max_unknowns; /* coarsen while unknowns exceed this, default 4096 (SS/GeometricLevelGen.h:46); max 4096 */
+  int device;                /* CUDA device ordinal, default 0 */
+  void* stream;              /* cudaStream_t to order work on; NULL: the context creates one */
+} vflip_config;
+
+typedef struct {
+  int iterations;   /* PCG iterations (the reference's iterations_out) */
+  int vcycles;      /* V-cycle applications, iterations + 1 when any ran */
+  int levels;       /* multigrid levels */
+  int converged;    /* 1 when |r|_inf <= tol * |rhs|_inf */
+  double residual;  /* |r|_inf at exit (the reference's residual_out) */
+  double rhs_norm;  /* |rhs|_inf */
+  double solve_ms;  /* device time of the solve, hierarchy build included */
+} vflip_solve_stats;
+
+typedef struct vflip_ctx vflip_ctx;
+
+/* Fills *cfg with the reference's defaults. */
+void vflip_config_default(vflip_config* cfg);
+
+/* Creates a context (device buffers are allocated lazily and reused across
+ * calls of the same size).  One context per host thread. */
+int vflip_create(vflip_ctx** out, const vflip_config* cfg);
+int vflip_destroy(vflip_ctx* ctx);
+/* Text of the last error on this context ("" when none). */
+const char* vflip_last_error(const vflip_ctx* ctx);
+int vflip_synchronize(vflip_ctx* ctx);
+/* Device time in milliseconds of the most recent solve or step. */
+double vflip_last_ms(const vflip_ctx* ctx);
+
+/* ---- MGPCG ------------------------------------------------------------- */
+
+/* Drop-in for
+ *   template<class T> bool ivock::AMGPCGSolve(const SparseMatrix<T>& matrix,
+ *       const std::vector<T>& rhs, std::vector<T>& result, T tolerance_factor,
+ *       int max_iterations, T& residual_out, int& iterations_out,
+ *       int ni, int nj, int nk)                 (SS/AlgebraicMultigrid.h:189-197)
+ * with the matrix as CSR (rows sorted by column, as FixedSparseMatrix holds
+ * it, SS/sparse_matrix.h:266-312).  ALL POINTERS ARE HOST POINTERS.  The
+ * matrix must be the 7-point, symmetric operator of an ni x nj x nk grid
+ * (what pcg_projection assembles); otherwise VFLIP_ERR_NOT_7POINT /
+ * VFLIP_ERR_NOT_SYMMETRIC.  result (n) is zeroed and written; the return
+ * value is VFLIP_OK where the reference returns true, VFLIP_NOT_CONVERGED
+ * where it returns false. */
+int vflip_amgpcg_solve_csr(vflip_ctx* ctx, uint32_t n, const uint32_t* rowstart, const uint32_t* colindex,
+                           const double* value, const double* rhs, double* result, double tolerance_factor,
+                           int max_iterations, double* residual_out, int* iterations_out, int ni, int nj, int nk);
+
+/* Same solve on a device-resident stencil operator and device vectors:
+ * rhs and result are FP64 arrays of ni*nj*nk.  stats may be NULL. */
+int vflip_amgpcg_solve(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const double* xp,
+                       const double* yp, const double* zp, const double* rhs, double* result,
+                       double tolerance_factor, int max_iterations, vflip_solve_stats* stats);
+
+/* Galerkin hierarchy (SS/GeometricLevelGen.h:28-71, .cpp:7-76) of an FP64
+ * stencil operator.  dims_out (HOST, 3*max_levels ints) receives each
+ * level's size; levels_out (device, may be NULL) receives, level after
+ * level, the four FP64 arrays diag, xp, yp, zp of each level.  Returns the
+ * number of levels (>= 1) or a negative status. */
+int vflip_build_levels(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const double* xp,
+                       const double* yp, const double* zp, int max_levels, int* dims_out, double* levels_out);
+
+/* `iterations` red-black Gauss-Seidel sweeps in place on x (FP64),
+ * ivock::RBGS (SS/AlgebraicMultigrid.h:22-103). */
+int vflip_rbgs(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const double* xp, const double* yp,
+               const double* zp, const double* b, double* x, int iterations);
+
+/* x = one V-cycle applied to b from x = 0, ivock::amgPrecond
+ * (SS/AlgebraicMultigrid.h:130-188), in the context's precision (b and x
+ * are FP64 either way). */
+int vflip_vcycle(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const double* xp, const double* yp,
+                 const double* zp, const double* b, double* x);
+
+/* ---- pressure projection -------------------------------------------------- */
+
+/* Face open fractions from the nodal solid level set,
+ * SmokeSolver3D::compute_face_weights (SS/Smoke_solver3D.cpp:874-944). */
+int vflip_face_weights(vflip_ctx* ctx, int ni, int nj, int nk, const float* nodal_phi, float* uw, float* vw,
+                       float* ww);
+
+/* Assembles the projection's operator and rhs without solving
+ * (SS/Smoke_solver3D.cpp:964-1111, inflow overwrite applied to u/v/w in
+ * place).  diag/xp/yp/zp/rhs are FP64 cell arrays. */
+int vflip_assemble(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, const float* nodal_phi,
+                   const int8_t* bdesc, const float* us, const float* vs, const float* ws, float* u, float* v,
+                   float* w, double* diag, double* xp, double* yp, double* zp, double* rhs);
+
+/* SmokeSolver3D::pcg_projection (SS/Smoke_solver3D.cpp:945-1202): face
+ * weights, inflow overwrite, assembly, MGPCG to tolerance_factor (the
+ * reference uses 1e-6, 50 iterations), gradient update of u/v/w in place.
+ * pressure (FP64 cells) may be NULL; stats may be NULL.  Returns the solve's
+ * status. */
+int vflip_project(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, const float* nodal_phi,
+                  const int8_t* bdesc, const float* us, const float* vs, const float* ws, float* u, float* v,
+                  float* w, double* pressure, double tolerance_factor, int max_iterations,
+                  vflip_solve_stats* stats);
+
+/* ---- advection ------------------------------------------------------------- */
+
+/* Semi-Lagrangian RK2 (midpoint) backtrace through the MAC velocity u/v/w of
+ * an ni x nj x nk grid of spacing h, then a trilinear sample of `field`,
+ * SubDomainSolver::advect_field (SS/sub_domain.cpp:191-235).  field/out are
+ * fnx x fny x fnz grids of spacing h whose node (i,j,k) sits at world
+ * ((i-ox)h, (j-oy)h, (k-oz)h): (0.5,0,0) for u, (0,0.5,0) for v, (0,0,0.5)
+ * for w, (0,0,0) for cell-centred scalars.  out must not alias field or u/v/w. */
+int vflip_advect_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                            const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
+                            double oz, const float* field, float* out);
+
+/* delta = after - before, n floats (SmokeSolver3D::getDelta, SS/Smoke_solver3D.cpp:1298-1319). */
+int vflip_delta(vflip_ctx* ctx, size_t n, const float* after, const float* before, float* delta);
+
+/* ---- FLIP transfers (particles: the reference's 40-byte `particle` records,
+ *      SS/fluid_particle.h:14-20: pos f32x3, vel f32x3, dens, temp,
+ *      hash_idx, sub_hash_idx) ------------------------------------------------ */
+
+/* Cell of each particle as SmokeSolver3D::hash_FLIP computes it
+ * (SS/Smoke_solver3D.cpp:1327-1346); -1 when outside the grid. */
+int vflip_particle_cells(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
+                         int* cell_out);
+
+/* SmokeSolver3D::particle_to_grid for u, v and w (SS/Smoke_solver3D.cpp:
+ * 1451-1510) after hash_FLIP: field = sum(w*vel)/sum(w), coef = sum(w) on
+ * each face grid, summed in the reference's bucket order (sort by cell,
+ * deterministic).  Any output pair may be NULL to skip that component. */
+int vflip_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np, float* u,
+              float* ucoef, float* v, float* vcoef, float* w, float* wcoef);
+
+/* SmokeSolver3D::particle_from_grid (SS/Smoke_solver3D.cpp:1398-1406):
+ * vel += trilinear(du, dv, dw) when flip_ratio == 1; otherwise
+ * vel = (1-flip_ratio) u_new(pos) + flip_ratio (vel + delta(pos)), the blend
+ * of fluid_particle::interpolate (SS/fluid_particle.h:315-328).  un/vn/wn
+ * may be NULL when flip_ratio == 1.  particles are updated in place. */
+int vflip_g2p(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np, const float* du,
+              const float* dv, const float* dw, const float* un, const float* vn, const float* wn,
+              double flip_ratio);
+
+/* ---- layout --------------------------------------------------------------- */
+
+/* Buffer3D's 8^3-bricked storage (SS/fluid_buffer3D.h:86-104, 186-202) <->
+ * this library's linear layout, for an nx x ny x nz float grid.  The bricked
+ * array holds ceil(n/8)*8 elements per axis. */
+int vflip_bricks_to_linear(vflip_ctx* ctx, int nx, int ny, int nz, const float* bricked, float* linear);
+int vflip_linear_to_bricks(vflip_ctx* ctx, int nx, int ny, int nz, const float* linear, float* bricked);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VFLIP_H */

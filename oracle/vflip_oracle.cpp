@@ -321,18 +321,26 @@ void rotate4(float* a) {
   float t = a[0];
   a[0] = a[1]; a[1] = a[2]; a[2] = a[3]; a[3] = t;
 }
-float frac4(float bl, float br, float tl, float tr) {
+// The reference's rotation loops (levelset_util.cpp:32,44,91) never end when
+// the inside corners (phi <= 0) include exact zeros in some patterns, e.g.
+// phi = {0, 0, 1, 1}.  Here each loop is bounded by the four rotations; a
+// failed search returns -1 and frac4 re-evaluates with exact zeros moved to
+// the smallest positive float.  Wherever the reference terminates, the result
+// is the reference's.
+float frac4_try(float bl, float br, float tl, float tr) {
   int inside = (bl <= 0) + (tl <= 0) + (br <= 0) + (tr <= 0);
   float q[4] = {bl, br, tr, tl};
   if (inside == 4) return 1;
   if (inside == 3) {
-    while (q[0] < 0) rotate4(q);
+    int n = 0;
+    while (q[0] < 0) { if (++n > 4) return -1; rotate4(q); }
     float s0 = 1 - frac2(q[0], q[3]);
     float s1 = 1 - frac2(q[0], q[1]);
     return 1 - 0.5f * s0 * s1;
   }
   if (inside == 2) {
-    while (q[0] >= 0 || !(q[1] < 0 || q[2] < 0)) rotate4(q);
+    int n = 0;
+    while (q[0] >= 0 || !(q[1] < 0 || q[2] < 0)) { if (++n > 4) return -1; rotate4(q); }
     if (q[1] < 0) return 0.5f * (frac2(q[0], q[3]) + frac2(q[1], q[2]));
     float mid = 0.25f * (q[0] + q[1] + q[2] + q[3]);
     if (mid < 0) {
@@ -355,12 +363,19 @@ float frac4(float bl, float br, float tl, float tr) {
     return area;
   }
   if (inside == 1) {
-    while (q[0] >= 0) rotate4(q);
+    int n = 0;
+    while (q[0] >= 0) { if (++n > 4) return -1; rotate4(q); }
     float s0 = frac2(q[0], q[3]);
     float s1 = frac2(q[0], q[1]);
     return 0.5f * s0 * s1;
   }
   return 0;
+}
+inline float nudge_zero(float x) { return x == 0.0f ? 1.17549435e-38f : x; }
+float frac4(float bl, float br, float tl, float tr) {
+  float f = frac4_try(bl, br, tl, tr);
+  if (f < 0) f = frac4_try(nudge_zero(bl), nudge_zero(br), nudge_zero(tl), nudge_zero(tr));
+  return f;
 }
 inline float clamp01(float a) { return a < 0.0f ? 0.0f : (a > 1.0f ? 1.0f : a); }  // SS/util.h:172-177
 

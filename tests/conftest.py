@@ -1,0 +1,62 @@
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200) and the built libvflip_gpu.so")
+
+
+@pytest.fixture(scope="session")
+def orc():
+    """The oracle restatement (built on demand; gcc is on every box)."""
+    import oracle
+
+    # make is a no-op when liboracle.so is newer than its source
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "liboracle.so"])
+    return oracle.oracle()
+
+
+@pytest.fixture(scope="session")
+def ref():
+    import oracle
+
+    r = oracle.reference()
+    if r is None:
+        pytest.skip("reference library oracle/_ref/libvflip_ref.so not built here")
+    return r
+
+
+def golden(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+def problem_from_golden(g):
+    ni, nj, nk = (int(x) for x in g["dims"])
+    pr = dict(ni=ni, nj=nj, nk=nk, h=float(g["h"]), U_in=float(g["U_in"]))
+    for k in ("phi", "bdesc", "us", "vs", "ws", "u", "v", "w"):
+        pr[k] = g["in_" + k]
+    return pr
+
+
+@pytest.fixture(scope="session")
+def gpu_solver():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from vflip_b200 import build
+    from vflip_b200.solver import Solver
+
+    build.build()
+    s = {p: Solver(precision=p) for p in (0, 1, 2)}
+    yield s
+    for v in s.values():
+        v.close()

@@ -1,0 +1,88 @@
+#!/usr/bin/env python3
+"""Generates the golden fixtures in this directory by running the
+reference's OWN code (oracle/_ref/libvflip_ref.so, compiled from the vFLIP
+sources by oracle/build_ref.py) on small seeded inputs.
+
+    python tests/golden/make_golden.py
+
+Each fixture (.npz) stores its inputs and the reference's outputs, so the
+tests need neither the reference tree nor its library: they check the
+oracle restatement (CPU) and the CUDA library (GPU) against these arrays.
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from vflip_b200 import scenes  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def main():
+    R = oracle.reference()
+    if R is None:
+        sys.exit("oracle/_ref/libvflip_ref.so is not built (python oracle/build_ref.py)")
+    # 1. projection (face weights, inflow, assembly, AMGPCG 1e-6/50, gradient)
+    #    on odd, non-cubic grids with inflow and moving solids
+    for tag, (ni, nj, nk), seed in (("proj_a", (14, 12, 11), 11), ("proj_b", (19, 17, 23), 12)):
+        pr = scenes.projection_problem(ni, nj, nk, seed=seed, inflow=True, solid_velocity=True)
+        out = R.project(**pr)
+        levels = R.levels(out["stencil"])
+        b = out["rhs"]
+        x3 = R.rbgs(out["stencil"], b, np.zeros_like(b), 3)
+        vc = R.vcycle(out["stencil"], b)
+        p, ok, res, it = R.amgpcg(out["stencil"], b)
+        arrays = {k: v for k, v in pr.items() if isinstance(v, np.ndarray)}
+        meta = np.array([ni, nj, nk], np.int32)
+        np.savez_compressed(os.path.join(OUT, f"{tag}.npz"), dims=meta, h=np.float32(pr["h"]),
+                            U_in=np.float32(pr["U_in"]), **{"in_" + k: v for k, v in arrays.items()},
+                            out_u=out["u"], out_v=out["v"], out_w=out["w"], out_pressure=out["pressure"],
+                            out_rhs=out["rhs"], out_stencil=out["stencil"], out_uw=out["uw"], out_vw=out["vw"],
+                            out_ww=out["ww"], out_iterations=np.int32(out["iterations"]),
+                            out_residual=np.float64(out["residual"]), rbgs3=x3, vcycle=vc, pcg_x=p,
+                            pcg_ok=np.int32(ok), pcg_res=np.float64(res), pcg_it=np.int32(it),
+                            n_levels=np.int32(len(levels)),
+                            **{f"level{l}": lv for l, lv in enumerate(levels)})
+    # 2. multi-level hierarchy on a grid big enough for three levels
+    st = scenes.uniform_laplacian(40, 37, 30)
+    levels = R.levels(st)
+    np.savez_compressed(os.path.join(OUT, "levels_uniform.npz"), dims=np.array([40, 37, 30], np.int32),
+                        n_levels=np.int32(len(levels)), **{f"level{l}": lv for l, lv in enumerate(levels)})
+    # 3. advection of the four grid kinds
+    rng = np.random.default_rng(21)
+    ni, nj, nk = 13, 11, 9
+    h = np.float32(1 / 13)
+    u, v, w = scenes.random_velocity(ni, nj, nk, rng, scale=3.0)
+    fields = {}
+    for name, offs, shape in (("u", (0.5, 0, 0), (nk, nj, ni + 1)), ("v", (0, 0.5, 0), (nk, nj + 1, ni)),
+                              ("w", (0, 0, 0.5), (nk + 1, nj, ni)), ("c", (0, 0, 0), (nk, nj, ni))):
+        f = rng.standard_normal(shape).astype(np.float32)
+        fields["in_" + name] = f
+        fields["out_" + name] = R.advect_rk2(ni, nj, nk, h, 0.07, u, v, w, f, offs)
+    np.savez_compressed(os.path.join(OUT, "advect.npz"), dims=np.array([ni, nj, nk], np.int32), h=h,
+                        dt=np.float32(0.07), u=u, v=v, w=w, **fields)
+    # 4. particles: hash, P2G (3 components), G2P
+    ni, nj, nk = 9, 8, 7
+    h = np.float32(1 / 9)
+    p = scenes.random_particles(ni, nj, nk, h, 4000, rng, margin=1.5)
+    du, dv, dw = scenes.random_velocity(ni, nj, nk, rng)
+    out = {"cells": R.hash(ni, nj, nk, h, p)}
+    for c in range(3):
+        f, cf = R.p2g(ni, nj, nk, h, p, c)
+        out[f"p2g_f{c}"] = f
+        out[f"p2g_c{c}"] = cf
+    g = R.g2p(ni, nj, nk, h, p, du, dv, dw)
+    np.savez_compressed(os.path.join(OUT, "transfer.npz"), dims=np.array([ni, nj, nk], np.int32), h=h,
+                        particles=p.view(np.uint8), du=du, dv=dv, dw=dw, g2p=g.view(np.uint8), **out)
+    for fn in sorted(os.listdir(OUT)):
+        if fn.endswith(".npz"):
+            print(fn, os.path.getsize(os.path.join(OUT, fn)))
+
+
+if __name__ == "__main__":
+    main()

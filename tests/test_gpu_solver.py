@@ -1,0 +1,228 @@
+"""GPU parity of the MGPCG path (calls go through the C ABI).
+
+Bar: the FP64 path reproduces the oracle (and so the reference) bit for bit
+for the hierarchy, the smoother and the V-cycle; the PCG differs only by
+the order of the tree reductions of its inner products (rel. L2 <= 1e-11,
+same iteration count).  FP32 and mixed precision meet the north-star
+tolerance: pressure within 1e-5 relative L2 of the reference solve.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, problem_from_golden
+from vflip_b200 import scenes
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+
+
+def t(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+
+
+def four(st7):
+    """(7, ...) oracle stencil -> (4, ...) device stencil: diag, +x, +y, +z."""
+    return t(np.stack([st7[0], st7[2], st7[4], st7[6]]))
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def cases():
+    return [("proj_a", None), ("proj_b", None), ("gen", (37, 33, 29)), ("gen", (64, 48, 40))]
+
+
+def system(orc, tag, dims, seed=4):
+    if tag == "gen":
+        pr = scenes.projection_problem(*dims, seed=seed, inflow=True, solid_velocity=True)
+    else:
+        pr = problem_from_golden(golden(tag))
+    out = orc.project(**pr)
+    return pr, out
+
+
+@pytest.mark.parametrize("tag,dims", cases())
+def test_levels_bit_exact(gpu_solver, orc, tag, dims):
+    _, out = system(orc, tag, dims)
+    st = out["stencil"]
+    ref_levels = orc.levels(st)
+    got = gpu_solver[0].build_levels(four(st))
+    assert len(got) == len(ref_levels)
+    for g, r in zip(got, ref_levels):
+        g = g.cpu().numpy()
+        assert np.array_equal(g, np.stack([r[0], r[2], r[4], r[6]]))
+
+
+@pytest.mark.parametrize("tag,dims", cases())
+def test_rbgs_bit_exact(gpu_solver, orc, tag, dims):
+    _, out = system(orc, tag, dims)
+    st, b = out["stencil"], out["rhs"]
+    x0 = np.random.default_rng(3).standard_normal(b.shape)
+    want = orc.rbgs(st, b, x0, 3)
+    got = gpu_solver[0].rbgs(four(st), t(b), t(x0), 3).cpu().numpy()
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("tag,dims", cases())
+def test_vcycle_bit_exact_fp64(gpu_solver, orc, tag, dims):
+    _, out = system(orc, tag, dims)
+    st, b = out["stencil"], out["rhs"]
+    want = orc.vcycle(st, b)
+    got = gpu_solver[0].vcycle(four(st), t(b)).cpu().numpy()
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.parametrize("prec,tol", [(1, 2e-5), (2, 2e-2)])
+def test_vcycle_reduced_precision(gpu_solver, orc, prec, tol):
+    _, out = system(orc, "gen", (64, 48, 40))
+    st, b = out["stencil"], out["rhs"]
+    want = orc.vcycle(st, b)
+    got = gpu_solver[prec].vcycle(four(st), t(b)).cpu().numpy()
+    assert rel_l2(got, want) < tol
+
+
+def test_vcycle_golden(gpu_solver):
+    g = golden("proj_b")
+    got = gpu_solver[0].vcycle(four(g["out_stencil"]), t(g["out_rhs"])).cpu().numpy()
+    assert np.array_equal(got, g["vcycle"])
+
+
+@pytest.mark.parametrize("tag,dims", cases())
+def test_pcg_fp64_matches_reference(gpu_solver, orc, tag, dims):
+    _, out = system(orc, tag, dims)
+    st, b = out["stencil"], out["rhs"]
+    x, ok, res, it = orc.amgpcg(st, b)
+    conv, p, stats = gpu_solver[0].amgpcg_solve(four(st), t(b), 1e-6, 50)
+    assert conv == ok and stats.iterations == it
+    assert rel_l2(p.cpu().numpy(), x) < 1e-11
+    assert abs(stats.residual - res) <= 1e-9 * abs(stats.rhs_norm)
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+@pytest.mark.parametrize("tag,dims", cases())
+def test_pcg_reduced_precision(gpu_solver, orc, prec, tag, dims):
+    _, out = system(orc, tag, dims)
+    st, b = out["stencil"], out["rhs"]
+    x, ok, res, it = orc.amgpcg(st, b)
+    conv, p, stats = gpu_solver[prec].amgpcg_solve(four(st), t(b), 1e-6, 50)
+    assert conv and ok
+    assert stats.residual <= 1e-6 * stats.rhs_norm
+    # pressure within the north-star tolerance of the reference solve
+    assert rel_l2(p.cpu().numpy(), x) < 1e-5
+    assert stats.iterations <= it + 2
+
+
+def test_csr_drop_in(gpu_solver, orc):
+    import oracle
+
+    _, out = system(orc, "proj_b", None)
+    st, b = out["stencil"], out["rhs"]
+    _, nk, nj, ni = st.shape
+    rs, ci, v = oracle.stencil_to_csr(st)
+    ok, x, res, it = gpu_solver[0].amgpcg_solve_csr(rs, ci, v, b, 1e-6, 50, ni, nj, nk)
+    want, wok, wres, wit = orc.amgpcg(st, b)
+    assert ok == wok and it == wit
+    assert rel_l2(x, want.ravel()) < 1e-11
+
+
+def test_csr_rejects_non_7point_and_asymmetric(gpu_solver):
+    import oracle
+    from vflip_b200 import VflipError
+
+    st = scenes.uniform_laplacian(8, 8, 8)
+    rs, ci, v = oracle.stencil_to_csr(st)
+    b = np.ones(512)
+    bad = ci.copy()
+    bad[rs[100] + 1] = 0  # an entry far off the 7-point pattern
+    with pytest.raises(VflipError) as e:
+        gpu_solver[1].amgpcg_solve_csr(rs, bad, v, b, 1e-6, 50, 8, 8, 8)
+    assert e.value.code == -3
+    v2 = v.copy()
+    row = 9 * 8 + 3 + 64 * 3
+    # perturb the +x coupling of one interior row only
+    for e_ in range(rs[row], rs[row + 1]):
+        if ci[e_] == row + 1:
+            v2[e_] *= 1.5
+    with pytest.raises(VflipError) as e:
+        gpu_solver[1].amgpcg_solve_csr(rs, ci, v2, b, 1e-6, 50, 8, 8, 8)
+    assert e.value.code == -4
+
+
+def test_solver_failure_modes(gpu_solver, orc):
+    """Zero rhs -> converged in 0 iterations; a NaN in the rhs -> not
+    converged with 0 iterations (rho != rho); max_iterations exhausted -> not
+    converged, as AlgebraicMultigrid.h:214-300 returns."""
+    st = scenes.uniform_laplacian(20, 19, 18)
+    s = gpu_solver[0]
+    conv, p, stats = s.amgpcg_solve(four(st), t(np.zeros((18, 19, 20))))
+    assert conv and stats.iterations == 0 and float(p.abs().max()) == 0.0
+    r = np.random.default_rng(2).standard_normal((18, 19, 20))
+    r[9, 9, 9] = np.nan
+    conv, p, stats = s.amgpcg_solve(four(st), t(r))
+    assert not conv and stats.iterations == 0
+    r = np.random.default_rng(1).standard_normal((18, 19, 20))
+    x, ok, res, it = orc.amgpcg(st, r, 1e-14, 2)
+    conv, p, stats = s.amgpcg_solve(four(st), t(r), 1e-14, 2)
+    assert not conv and not ok and stats.iterations == it == 2
+    assert rel_l2(p.cpu().numpy(), x) < 1e-12
+
+
+@pytest.mark.parametrize("dims", [(3, 3, 3), (1, 1, 1), (16, 16, 16), (5, 40, 3)])
+def test_small_and_single_level_grids(gpu_solver, orc, dims):
+    ni, nj, nk = dims
+    rng = np.random.default_rng(7)
+    st = scenes.uniform_laplacian(ni, nj, nk)
+    b = rng.standard_normal((nk, nj, ni))
+    b[st[0] == 0] = 0.0
+    x, ok, res, it = orc.amgpcg(st, b)
+    conv, p, stats = gpu_solver[0].amgpcg_solve(four(st), t(b))
+    assert conv == ok and stats.iterations == it
+    assert rel_l2(p.cpu().numpy(), x) < 1e-11 or np.abs(x).max() == 0
+
+
+@pytest.mark.parametrize("prec,tol", [(0, 1e-9), (1, 2e-5), (2, 2e-5)])
+def test_projection_matches_reference(gpu_solver, orc, prec, tol):
+    for tag in ("proj_a", "proj_b"):
+        g = golden(tag)
+        pr = problem_from_golden(g)
+        u, v, w = t(pr["u"]), t(pr["v"]), t(pr["w"])
+        conv, p, stats = gpu_solver[prec].project(pr["ni"], pr["nj"], pr["nk"], pr["h"], pr["U_in"], t(pr["phi"]),
+                                                  t(pr["bdesc"]), t(pr["us"]), t(pr["vs"]), t(pr["ws"]), u, v, w)
+        assert conv
+        assert rel_l2(p.cpu().numpy(), g["out_pressure"]) < tol
+        for name, arr in (("u", u), ("v", v), ("w", w)):
+            assert rel_l2(arr.cpu().numpy(), g["out_" + name]) < tol, name
+
+
+def test_assembly_bit_exact(gpu_solver):
+    for tag in ("proj_a", "proj_b"):
+        g = golden(tag)
+        pr = problem_from_golden(g)
+        u, v, w = t(pr["u"]), t(pr["v"]), t(pr["w"])
+        st, rhs = gpu_solver[1].assemble(pr["ni"], pr["nj"], pr["nk"], pr["h"], pr["U_in"], t(pr["phi"]),
+                                         t(pr["bdesc"]), t(pr["us"]), t(pr["vs"]), t(pr["ws"]), u, v, w)
+        ref = g["out_stencil"]
+        assert np.array_equal(st.cpu().numpy(), np.stack([ref[0], ref[2], ref[4], ref[6]]))
+        assert np.array_equal(rhs.cpu().numpy(), g["out_rhs"])
+        uw, vw, ww = gpu_solver[1].face_weights(pr["ni"], pr["nj"], pr["nk"], t(pr["phi"]))
+        for a, k in ((uw, "uw"), (vw, "vw"), (ww, "ww")):
+            assert np.array_equal(a.cpu().numpy(), g["out_" + k])
+
+
+def test_fraction_inside_zero_corners(gpu_solver, orc):
+    """Exact-zero corner patterns on which the reference loops forever: the
+    kernel terminates and agrees with the oracle's bounded restatement."""
+    ni = nj = nk = 4
+    phi = np.ones((nk + 1, nj + 1, ni + 1), np.float32)
+    phi[2, 2, :] = 0.0
+    phi[1, :, 2] = 0.0
+    phi[3, 3, 3] = -1.0
+    want = orc.face_weights(ni, nj, nk, 0.25, phi)
+    got = gpu_solver[1].face_weights(ni, nj, nk, t(phi))
+    for a, b in zip(got, want):
+        assert np.array_equal(a.cpu().numpy(), b)

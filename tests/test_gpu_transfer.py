@@ -1,0 +1,134 @@
+"""GPU parity of advection and the FLIP transfers (bit-exact: the kernels
+keep the reference's FP64 lerps and its summation order)."""
+import numpy as np
+import pytest
+
+from conftest import golden
+from vflip_b200 import scenes
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+DEV = "cuda:0"
+
+
+def t(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+
+
+def parts(p):
+    return t(p.view(np.uint8))
+
+
+def unparts(x):
+    import oracle
+
+    return x.cpu().numpy().view(oracle.PARTICLE_DTYPE)
+
+
+OFFS = {"u": (0.5, 0, 0), "v": (0, 0.5, 0), "w": (0, 0, 0.5), "c": (0, 0, 0)}
+
+
+def test_advect_golden(gpu_solver):
+    g = golden("advect")
+    ni, nj, nk = (int(x) for x in g["dims"])
+    for name, offs in OFFS.items():
+        out = gpu_solver[1].advect_rk2_linear(ni, nj, nk, float(g["h"]), float(g["dt"]), t(g["u"]), t(g["v"]),
+                                              t(g["w"]), t(g["in_" + name]), offs)
+        assert np.array_equal(out.cpu().numpy(), g["out_" + name]), name
+
+
+@pytest.mark.parametrize("dims,dt", [((40, 33, 29), 0.03), ((64, 64, 64), 0.01)])
+def test_advect_vs_oracle(gpu_solver, orc, dims, dt):
+    ni, nj, nk = dims
+    rng = np.random.default_rng(11)
+    h = np.float32(1.0 / ni)
+    u, v, w = scenes.random_velocity(ni, nj, nk, rng, scale=2.0)
+    for name, offs in OFFS.items():
+        shape = {"u": (nk, nj, ni + 1), "v": (nk, nj + 1, ni), "w": (nk + 1, nj, ni), "c": (nk, nj, ni)}[name]
+        f = rng.standard_normal(shape).astype(np.float32)
+        want = orc.advect_rk2(ni, nj, nk, h, dt, u, v, w, f, offs)
+        got = gpu_solver[1].advect_rk2_linear(ni, nj, nk, h, dt, t(u), t(v), t(w), t(f), offs).cpu().numpy()
+        assert np.array_equal(got, want), name
+
+
+def test_transfer_golden(gpu_solver):
+    g = golden("transfer")
+    ni, nj, nk = (int(x) for x in g["dims"])
+    h = float(g["h"])
+    p = t(g["particles"])
+    cells = gpu_solver[1].particle_cells(ni, nj, nk, h, p).cpu().numpy()
+    assert np.array_equal(cells, g["cells"])
+    outs = gpu_solver[1].particle_to_grid(ni, nj, nk, h, p)
+    for c in range(3):
+        assert np.array_equal(outs[c][0].cpu().numpy(), g[f"p2g_f{c}"])
+        assert np.array_equal(outs[c][1].cpu().numpy(), g[f"p2g_c{c}"])
+    gpu_solver[1].particle_from_grid(ni, nj, nk, h, p, t(g["du"]), t(g["dv"]), t(g["dw"]))
+    assert np.array_equal(p.cpu().numpy(), g["g2p"])
+
+
+@pytest.mark.parametrize("dims,n", [((33, 29, 21), 200000), ((64, 64, 64), 8 * 64 ** 3)])
+def test_p2g_vs_oracle(gpu_solver, orc, dims, n):
+    ni, nj, nk = dims
+    rng = np.random.default_rng(13)
+    h = np.float32(1.0 / ni)
+    if n == 8 * ni * nj * nk:
+        p = scenes.jittered_particles(ni, nj, nk, h, 8, rng)
+        p["vel"] = rng.standard_normal((len(p), 3)).astype(np.float32)
+        rng.shuffle(p)
+    else:
+        p = scenes.random_particles(ni, nj, nk, h, n, rng, margin=1.0)
+    outs = gpu_solver[1].particle_to_grid(ni, nj, nk, h, parts(p))
+    for c in range(3):
+        f, cf = orc.p2g(ni, nj, nk, h, p, c)
+        assert np.array_equal(outs[c][0].cpu().numpy(), f)
+        assert np.array_equal(outs[c][1].cpu().numpy(), cf)
+
+
+def test_p2g_crowded_cells_and_empty(gpu_solver, orc):
+    """Buckets far beyond 32 particles (heapsort path), particles outside the
+    grid, and an empty particle set."""
+    ni, nj, nk = 6, 5, 4
+    h = np.float32(0.2)
+    rng = np.random.default_rng(17)
+    p = scenes.random_particles(ni, nj, nk, h, 3000, rng, margin=0.0)
+    p["pos"][:2000] = (np.array([2.0, 2.0, 1.0]) * h + rng.uniform(-0.4, 0.4, (2000, 3)) * h).astype(np.float32)
+    p["pos"][2000:2100] = -5.0  # outside
+    rng.shuffle(p)
+    outs = gpu_solver[1].particle_to_grid(ni, nj, nk, h, parts(p))
+    for c in range(3):
+        f, cf = orc.p2g(ni, nj, nk, h, p, c)
+        assert np.array_equal(outs[c][0].cpu().numpy(), f)
+        assert np.array_equal(outs[c][1].cpu().numpy(), cf)
+    empty = torch.zeros((0, 40), dtype=torch.uint8, device=DEV)
+    outs = gpu_solver[1].particle_to_grid(ni, nj, nk, h, empty)
+    for c in range(3):
+        assert torch.all(outs[c][0] == 0) and torch.all(outs[c][1] == np.float32(1e-5))
+
+
+@pytest.mark.parametrize("flip", [1.0, 0.95, 0.0])
+def test_g2p_vs_oracle(gpu_solver, orc, flip):
+    ni, nj, nk = 37, 31, 23
+    rng = np.random.default_rng(19)
+    h = np.float32(1.0 / ni)
+    p = scenes.random_particles(ni, nj, nk, h, 100000, rng, margin=2.0)
+    du, dv, dw = scenes.random_velocity(ni, nj, nk, rng)
+    un, vn, wn = scenes.random_velocity(ni, nj, nk, rng)
+    want = orc.g2p(ni, nj, nk, h, p, du, dv, dw, un, vn, wn, flip_ratio=flip)
+    x = parts(p)
+    gpu_solver[1].particle_from_grid(ni, nj, nk, h, x, t(du), t(dv), t(dw), t(un), t(vn), t(wn), flip_ratio=flip)
+    assert np.array_equal(x.cpu().numpy(), want.view(np.uint8))
+
+
+def test_delta_and_bricks(gpu_solver, orc):
+    rng = np.random.default_rng(23)
+    a = rng.standard_normal((9, 10, 13)).astype(np.float32)
+    b = rng.standard_normal((9, 10, 13)).astype(np.float32)
+    assert np.array_equal(gpu_solver[1].delta(t(a), t(b)).cpu().numpy(), orc.delta(a, b))
+    br = gpu_solver[1].linear_to_bricks(13, 10, 9, t(a))
+    assert br.numel() == 16 * 16 * 16
+    # brick index of Buffer3D (fluid_buffer3D.h:186-202)
+    i, j, k = 11, 9, 7
+    idx = ((((k >> 3) * 2 * 2) + (j >> 3) * 2 + (i >> 3)) << 9) + ((k & 7) << 6) + ((j & 7) << 3) + (i & 7)
+    assert float(br[idx]) == a[k, j, i]
+    back = gpu_solver[1].bricks_to_linear(13, 10, 9, br)
+    assert np.array_equal(back.cpu().numpy(), a)

@@ -1,0 +1,152 @@
+"""CPU: the oracle restatement against the golden fixtures (made by the
+reference's own code) and, where the reference library was built here,
+against the reference directly on fresh seeded inputs."""
+import numpy as np
+import pytest
+
+from conftest import golden, problem_from_golden
+from vflip_b200 import scenes
+
+
+def same(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    assert a.shape == b.shape
+    assert np.array_equal(a, b), f"max diff {np.max(np.abs(a.astype(np.float64) - b.astype(np.float64)))}"
+
+
+@pytest.mark.parametrize("tag", ["proj_a", "proj_b"])
+def test_projection_golden(orc, tag):
+    g = golden(tag)
+    pr = problem_from_golden(g)
+    out = orc.project(**pr)
+    for k in ("u", "v", "w", "pressure", "rhs", "stencil", "uw", "vw", "ww"):
+        same(out[k], g["out_" + k])
+    assert out["iterations"] == int(g["out_iterations"])
+    assert out["residual"] == float(g["out_residual"])
+    st = g["out_stencil"]
+    b = g["out_rhs"]
+    same(orc.rbgs(st, b, np.zeros_like(b), 3), g["rbgs3"])
+    same(orc.vcycle(st, b), g["vcycle"])
+    x, ok, res, it = orc.amgpcg(st, b)
+    same(x, g["pcg_x"])
+    assert (ok, res, it) == (bool(g["pcg_ok"]), float(g["pcg_res"]), int(g["pcg_it"]))
+    levels = orc.levels(st)
+    assert len(levels) == int(g["n_levels"])
+    for l, lv in enumerate(levels):
+        same(lv, g[f"level{l}"])
+
+
+def test_levels_uniform_golden(orc):
+    g = golden("levels_uniform")
+    st = scenes.uniform_laplacian(*(int(x) for x in g["dims"]))
+    levels = orc.levels(st)
+    assert len(levels) == int(g["n_levels"]) == 3
+    for l, lv in enumerate(levels):
+        same(lv, g[f"level{l}"])
+
+
+def test_galerkin_known_answer(orc):
+    """Uniform 7-point Laplacian: interior Galerkin coefficients are
+    6/-1 -> 1.5/-0.25 -> 0.375/-0.0625 (0.5*R*A*P with R = 1/8, P = 1)."""
+    st = scenes.uniform_laplacian(64, 64, 64)
+    lv = orc.levels(st)
+    assert [l.shape[1:] for l in lv] == [(64, 64, 64), (32, 32, 32), (16, 16, 16)]
+    for l, (d, o) in enumerate(((6.0, -1.0), (1.5, -0.25), (0.375, -0.0625))):
+        s = lv[l]
+        c = s.shape[1] // 2
+        assert s[0, c, c, c] == d
+        for slot in range(1, 7):
+            assert s[slot, c, c, c] == o
+
+
+def test_advect_golden(orc):
+    g = golden("advect")
+    ni, nj, nk = (int(x) for x in g["dims"])
+    for name, offs in (("u", (0.5, 0, 0)), ("v", (0, 0.5, 0)), ("w", (0, 0, 0.5)), ("c", (0, 0, 0))):
+        out = orc.advect_rk2(ni, nj, nk, float(g["h"]), float(g["dt"]), g["u"], g["v"], g["w"], g["in_" + name], offs)
+        same(out, g["out_" + name])
+
+
+def test_transfer_golden(orc):
+    import oracle
+
+    g = golden("transfer")
+    ni, nj, nk = (int(x) for x in g["dims"])
+    h = float(g["h"])
+    p = g["particles"].view(oracle.PARTICLE_DTYPE)
+    same(orc.hash(ni, nj, nk, h, p), g["cells"])
+    for c in range(3):
+        f, cf = orc.p2g(ni, nj, nk, h, p, c)
+        same(f, g[f"p2g_f{c}"])
+        same(cf, g[f"p2g_c{c}"])
+    out = orc.g2p(ni, nj, nk, h, p, g["du"], g["dv"], g["dw"])
+    same(out.view(np.uint8), g["g2p"])
+
+
+def test_fraction_inside_zero_corners_terminate(orc):
+    """Corner patterns with exact zeros on which the reference's rotation
+    loops never end: the oracle bounds them and returns the limit from the
+    outside."""
+    cases = np.array([[0, 0, 1, 1], [-1, 0, 1, 1], [0, 1, 1, 1], [0, 0, 0, 1]], np.float32)
+    out = orc.fraction_inside4(cases[:, 0], cases[:, 1], cases[:, 2], cases[:, 3])
+    assert np.all(np.isfinite(out)) and np.all(out >= 0) and np.all(out <= 1)
+
+
+# ---------------------------------------------------------- vs the reference
+@pytest.mark.parametrize("dims,seed", [((21, 18, 17), 1), ((33, 30, 31), 2), ((12, 40, 9), 3)])
+def test_projection_vs_reference(orc, ref, dims, seed):
+    pr = scenes.projection_problem(*dims, seed=seed, inflow=True, solid_velocity=True)
+    a, b = ref.project(**pr), orc.project(**pr)
+    for k in ("u", "v", "w", "pressure", "rhs", "stencil", "uw", "vw", "ww"):
+        same(a[k], b[k])
+    assert (a["iterations"], a["residual"]) == (b["iterations"], b["residual"])
+    st = a["stencil"]
+    for la, lb in zip(ref.levels(st), orc.levels(st)):
+        same(la, lb)
+    same(ref.vcycle(st, a["rhs"]), orc.vcycle(st, a["rhs"]))
+
+
+def test_transfers_vs_reference(orc, ref):
+    rng = np.random.default_rng(5)
+    ni, nj, nk = 17, 13, 11
+    h = np.float32(1 / 17)
+    p = scenes.random_particles(ni, nj, nk, h, 30000, rng, margin=1.5)
+    same(ref.hash(ni, nj, nk, h, p), orc.hash(ni, nj, nk, h, p))
+    for c in range(3):
+        fa, ca = ref.p2g(ni, nj, nk, h, p, c)
+        fb, cb = orc.p2g(ni, nj, nk, h, p, c)
+        same(fa, fb)
+        same(ca, cb)
+    du, dv, dw = scenes.random_velocity(ni, nj, nk, rng)
+    same(ref.g2p(ni, nj, nk, h, p, du, dv, dw).view(np.uint8), orc.g2p(ni, nj, nk, h, p, du, dv, dw).view(np.uint8))
+    for offs, shape in (((0.5, 0, 0), (nk, nj, ni + 1)), ((0, 0, 0), (nk, nj, ni))):
+        f = rng.standard_normal(shape).astype(np.float32)
+        same(ref.advect_rk2(ni, nj, nk, h, 0.05, du, dv, dw, f, offs), orc.advect_rk2(ni, nj, nk, h, 0.05, du, dv, dw,
+                                                                                      f, offs))
+
+
+def test_fraction_inside_vs_reference(orc, ref):
+    rng = np.random.default_rng(9)
+    x = [rng.standard_normal(200000).astype(np.float32) for _ in range(4)]
+    same(ref.fraction_inside4(*x), orc.fraction_inside4(*x))
+
+
+def test_pcg_failure_modes_vs_reference(orc, ref):
+    """Reference error behaviour: zero rhs -> true with 0 iterations; NaN rhs
+    -> false (rho != rho); max_iterations exhausted -> false."""
+    st = scenes.uniform_laplacian(18, 17, 16)
+    n = 18 * 17 * 16
+    z = np.zeros(n)
+    for impl in (orc, ref):
+        x, ok, res, it = impl.amgpcg(st, z)
+        assert ok and it == 0 and res == 0
+    nanr = np.random.default_rng(2).standard_normal(n)
+    nanr[n // 2] = np.nan  # |r|_inf skips the NaN; rho = z.r is NaN
+    a, b = ref.amgpcg(st, nanr), orc.amgpcg(st, nanr)
+    assert (a[1], a[3]) == (b[1], b[3]) == (False, 0)
+    rhs = np.random.default_rng(1).standard_normal(n)
+    rhs = rhs.reshape(16, 17, 18)
+    a, b = ref.amgpcg(st, rhs, 1e-14, 2), orc.amgpcg(st, rhs, 1e-14, 2)
+    same(a[0], b[0])
+    assert (a[1], a[2], a[3]) == (b[1], b[2], b[3]) and a[1] is False and a[3] == 2

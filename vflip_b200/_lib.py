@@ -1,0 +1,83 @@
+"""ctypes binding of libvflip_gpu.so (the C ABI declared in include/vflip.h)."""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_NAME = "libvflip_gpu.so"
+
+_P = C.c_void_p
+_I = C.c_int
+_U32 = C.c_uint32
+_F = C.c_float
+_D = C.c_double
+_SZ = C.c_size_t
+
+
+class VflipError(RuntimeError):
+    """A negative status from the C ABI (argument or CUDA error)."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"vflip error {code}: {msg}")
+        self.code = code
+
+
+class SolveStatsC(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("vcycles", C.c_int), ("levels", C.c_int), ("converged", C.c_int),
+                ("residual", C.c_double), ("rhs_norm", C.c_double), ("solve_ms", C.c_double)]
+
+
+class ConfigC(C.Structure):
+    _fields_ = [("precision", C.c_int), ("pre_sweeps", C.c_int), ("post_sweeps", C.c_int),
+                ("coarse_sweeps", C.c_int), ("coarsest_max_unknowns", C.c_int), ("device", C.c_int),
+                ("stream", C.c_void_p)]
+
+
+# name -> (restype, argtypes); mirrors include/vflip.h one for one
+SIGNATURES = {
+    "vflip_config_default": (None, [C.POINTER(ConfigC)]),
+    "vflip_create": (_I, [C.POINTER(_P), C.POINTER(ConfigC)]),
+    "vflip_destroy": (_I, [_P]),
+    "vflip_last_error": (C.c_char_p, [_P]),
+    "vflip_synchronize": (_I, [_P]),
+    "vflip_last_ms": (_D, [_P]),
+    "vflip_amgpcg_solve_csr": (_I, [_P, _U32, _P, _P, _P, _P, _P, _D, _I, _P, _P, _I, _I, _I]),
+    "vflip_amgpcg_solve": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _D, _I, C.POINTER(SolveStatsC)]),
+    "vflip_build_levels": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _I, _P, _P]),
+    "vflip_rbgs": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _I]),
+    "vflip_vcycle": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
+    "vflip_face_weights": (_I, [_P, _I, _I, _I, _P, _P, _P, _P]),
+    "vflip_assemble": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "vflip_project": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _I,
+                           C.POINTER(SolveStatsC)]),
+    "vflip_advect_rk2_linear": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _P, _P]),
+    "vflip_delta": (_I, [_P, _SZ, _P, _P, _P]),
+    "vflip_particle_cells": (_I, [_P, _I, _I, _I, _F, _P, _I, _P]),
+    "vflip_p2g": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _P, _P]),
+    "vflip_g2p": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _P, _P, _D]),
+    "vflip_bricks_to_linear": (_I, [_P, _I, _I, _I, _P, _P]),
+    "vflip_linear_to_bricks": (_I, [_P, _I, _I, _I, _P, _P]),
+}
+
+_lib = None
+
+
+def lib_path():
+    return os.path.join(HERE, _LIB_NAME)
+
+
+def load():
+    """Load libvflip_gpu.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = lib_path()
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `python -m vflip_b200.build` "
+                                "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib

@@ -1,0 +1,85 @@
+// Shared device helpers for the vFLIP B200 kernels.
+//
+// Layout: every grid is a dense linear array, index = i + ni*(j + nj*k)
+// (i fastest), the same order the reference uses for its pressure vector
+// (Smoke_Solver/Smoke_solver3D.cpp:993).  A level's 7-point operator is
+// symmetric and stored as four arrays: diag, xp, yp, zp (the +x/+y/+z
+// couplings); the -x coupling of cell c is xp[c-1], and so on.
+//
+// The library is compiled with -fmad=false: every a*b+c is rounded twice, as
+// the reference's x86-64 build does, so kernels that follow the reference's
+// order of operations reproduce its FP64/FP32 results bit for bit.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#define VFLIP_HD __host__ __device__ __forceinline__
+
+namespace vflip {
+
+constexpr int kWarp = 32;
+
+VFLIP_HD size_t lin3(int i, int j, int k, int ni, int nj) {
+  return (size_t)i + (size_t)ni * ((size_t)j + (size_t)nj * (size_t)k);
+}
+
+// Storage-type conversions: stencils and vectors may be stored as double,
+// float or bf16 (coarse levels of the mixed-precision mode); arithmetic uses
+// Acc (double for the FP64 path, float otherwise).
+template <typename T> struct Num;
+template <> struct Num<double> {
+  using Acc = double;
+  static __device__ __forceinline__ double ld(const double* p) { return __ldg(p); }
+  static __device__ __forceinline__ double ldv(const double* p) { return *p; }
+  static __device__ __forceinline__ double to(double v) { return v; }
+};
+template <> struct Num<float> {
+  using Acc = float;
+  static __device__ __forceinline__ float ld(const float* p) { return __ldg(p); }
+  static __device__ __forceinline__ float ldv(const float* p) { return *p; }
+  static __device__ __forceinline__ float to(float v) { return v; }
+};
+template <> struct Num<__nv_bfloat16> {
+  using Acc = float;
+  static __device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
+  static __device__ __forceinline__ float ldv(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+  static __device__ __forceinline__ __nv_bfloat16 to(float v) { return __float2bfloat16_rn(v); }
+};
+
+template <typename T> __device__ __forceinline__ typename Num<T>::Acc ldg(const T* p) { return Num<T>::ld(p); }
+template <typename T> __device__ __forceinline__ typename Num<T>::Acc ldv(const T* p) { return Num<T>::ldv(p); }
+template <typename T, typename A> __device__ __forceinline__ T cvt(A v) { return Num<T>::to(v); }
+
+// Block-wide sum of one double per thread; result valid in thread 0.
+template <int BLOCK>
+__device__ __forceinline__ double block_sum(double v, double* smem /* >= BLOCK/32 */) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) smem[wid] = v;
+  __syncthreads();
+  double s = 0;
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < BLOCK / 32; ++w) s += smem[w];
+  }
+  __syncthreads();
+  return s;
+}
+
+// Block-wide max of |v| ignoring NaN (the reference's abs_max never lets a
+// NaN win, Smoke_Solver/blas_wrapper.h:25-37); result valid in thread 0.
+template <int BLOCK>
+__device__ __forceinline__ double block_absmax(double v, double* smem) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) smem[wid] = v;
+  __syncthreads();
+  double s = 0;
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < BLOCK / 32; ++w) s = fmax(s, smem[w]);
+  }
+  __syncthreads();
+  return s;
+}
+
+}  // namespace vflip

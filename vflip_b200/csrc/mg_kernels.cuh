@@ -1,0 +1,345 @@
+// Multigrid kernels: Galerkin coarsening, fused red-black Gauss-Seidel
+// sweeps, residual+restriction, coarsest-level solve.
+//
+// All of them reproduce the arithmetic of the reference's CSR routines in
+// the order the reference performs it, so the FP64 instantiation is
+// bit-identical to the reference V-cycle (Smoke_Solver/AlgebraicMultigrid.h
+// and GeometricLevelGen.*):
+//   * a row sum walks the CSR columns in ascending order: -z, -y, -x,
+//     (diag), +x, +y, +z;
+//   * red-black GS updates colour (i+j+k) odd, then even (AlgebraicMultigrid.h:39,74);
+//   * restriction adds 0.125*r over the children in ascending fine index,
+//     prolongation adds the parent's value (injection).
+#pragma once
+#include "common.cuh"
+
+namespace vflip {
+
+// ---------------------------------------------------------------------------
+// Galerkin coarsening, A_c = 0.5 R A P with R = 1/8 over the 2x2x2 children
+// and P = injection (GeometricLevelGen.cpp:41-66, GeometricLevelGen.h:60-68,
+// sparse_matrix.h:370-405).  Computed in FP64 on the stored half (diag, +x,
+// +y, +z) of the symmetric operator.  0.5*0.125 = 0.0625 is a power of two,
+// so scaling each child's partial row sum by it reproduces the two SpGEMMs
+// term for term.  One thread per coarse cell.
+__global__ void galerkin_coarsen_kernel(const double* __restrict__ fd, const double* __restrict__ fxp,
+                                        const double* __restrict__ fyp, const double* __restrict__ fzp,
+                                        double* __restrict__ cd, double* __restrict__ cxp,
+                                        double* __restrict__ cyp, double* __restrict__ czp, int ni, int nj,
+                                        int nk, int cni, int cnj, int cnk) {
+  int I = blockIdx.x * blockDim.x + threadIdx.x;
+  int J = blockIdx.y * blockDim.y + threadIdx.y;
+  int K = blockIdx.z;
+  if (I >= cni || J >= cnj || K >= cnk) return;
+  const size_t sx = 1, sy = (size_t)ni, sz = (size_t)ni * nj;
+  double aD = 0, aX = 0, aY = 0, aZ = 0;
+  bool hD = false, hX = false, hY = false, hZ = false;
+#pragma unroll
+  for (int kk = 0; kk <= 1; ++kk)
+#pragma unroll
+    for (int jj = 0; jj <= 1; ++jj)
+#pragma unroll
+      for (int ii = 0; ii <= 1; ++ii) {
+        int fi = 2 * I + ii, fj = 2 * J + jj, fk = 2 * K + kk;
+        if (fi >= ni || fj >= nj || fk >= nk) continue;
+        size_t c = lin3(fi, fj, fk, ni, nj);
+        // temp(c, parent): the child's row entries whose column has parent I,
+        // summed in column order
+        double t = 0;
+        bool th = false;
+        auto add = [&](double v) {
+          if (th) t = __dadd_rn(t, v);
+          else { t = v; th = true; }
+        };
+        if (kk == 1) add(fzp[c - sz]);
+        if (jj == 1) add(fyp[c - sy]);
+        if (ii == 1) add(fxp[c - sx]);
+        add(fd[c]);
+        if (ii == 0 && fi + 1 < ni) add(fxp[c]);
+        if (jj == 0 && fj + 1 < nj) add(fyp[c]);
+        if (kk == 0 && fk + 1 < nk) add(fzp[c]);
+        double v = __dmul_rn(0.0625, t);
+        if (hD) aD = __dadd_rn(aD, v); else { aD = v; hD = true; }
+        if (ii == 1 && fi + 1 < ni) {
+          double w = __dmul_rn(0.0625, fxp[c]);
+          if (hX) aX = __dadd_rn(aX, w); else { aX = w; hX = true; }
+        }
+        if (jj == 1 && fj + 1 < nj) {
+          double w = __dmul_rn(0.0625, fyp[c]);
+          if (hY) aY = __dadd_rn(aY, w); else { aY = w; hY = true; }
+        }
+        if (kk == 1 && fk + 1 < nk) {
+          double w = __dmul_rn(0.0625, fzp[c]);
+          if (hZ) aZ = __dadd_rn(aZ, w); else { aZ = w; hZ = true; }
+        }
+      }
+  size_t o = lin3(I, J, K, cni, cnj);
+  cd[o] = aD;
+  cxp[o] = aX;
+  cyp[o] = aY;
+  czp[o] = aZ;
+}
+
+template <typename T>
+__global__ void convert_kernel(const double* __restrict__ src, T* __restrict__ dst, size_t n) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (; i < n; i += stride) dst[i] = cvt<T>((typename Num<T>::Acc)src[i]);
+}
+
+// ---------------------------------------------------------------------------
+// One full red-black Gauss-Seidel sweep (both colours), fused, out of place.
+//
+// In a red-black sweep the red update reads only black values and the black
+// update reads only the new red values, so a sweep is a pure function of the
+// incoming black values and b.  Each CTA owns full x-rows [j0, j0+tyo) of a
+// z-chunk [k0, k0+kz) and marches k upward with a 4-plane rolling window in
+// shared memory:
+//   step p:  stage x_in plane p+1 (rows j0-2 .. j0+tyo+1)
+//            red   update of plane p   on rows j0-1 .. j0+tyo  (one-row ring)
+//            black update of plane p-1 on rows j0 .. j0+tyo-1
+//            store plane p-1
+// The ring rows and the planes k0-1 and k0+kz are recomputed redundantly by
+// the neighbouring CTAs, so no CTA ever reads a value another CTA writes and
+// x_in/x_out must be different buffers.
+//
+// Variants (compile-time):
+//   ZERO_X  - the incoming x is zero (first pre-smoothing sweep of a level,
+//             amgVCycle zero-fills x, AlgebraicMultigrid.h:145-152, 185-186);
+//   PROLONG - the incoming x is x_in + P x_coarse (prolongation fused into the
+//             first post-smoothing sweep, AlgebraicMultigrid.h:118-129,161-165);
+//   DOT     - also accumulate sum(x_out * b) over the CTA's cells (the PCG
+//             rho = dot(z, r) at the fine level, AlgebraicMultigrid.h:282).
+template <typename S, typename V>
+struct SweepArgs {
+  const V* x_in;
+  V* x_out;
+  const V* b;
+  const S* diag;
+  const S* xp;
+  const S* yp;
+  const S* zp;
+  const V* xc;  // coarse x (PROLONG)
+  int ni, nj, nk;
+  int cni, cnj;
+  int tyo, kz;
+  int plane_stride;  // elements per staged plane (>= (tyo+4)*ni)
+  double* dot_partial;
+};
+
+template <typename S, typename V, bool ZERO_X, bool PROLONG, bool DOT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) rbgs_sweep_kernel(SweepArgs<S, V> a) {
+  using A = typename Num<V>::Acc;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  A* xs = reinterpret_cast<A*>(smem_raw);
+  __shared__ double red_smem[BLOCK / 32];
+
+  const int ni = a.ni, nj = a.nj, nk = a.nk;
+  const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
+  const int j0 = blockIdx.x * a.tyo;
+  const int k0 = blockIdx.y * a.kz;
+  const int kend = min(k0 + a.kz, nk);
+  const int jout1 = min(j0 + a.tyo, nj);
+  const int jr0 = max(j0 - 2, 0);                  // first staged row
+  const int jr1 = min(j0 + a.tyo + 2, nj);         // one past the last staged row
+  const int jred0 = max(j0 - 1, 0), jred1 = min(j0 + a.tyo + 1, nj);
+  const int rows = jr1 - jr0;
+  const int pls = a.plane_stride;
+  auto X = [&](int p) -> A* { return xs + (size_t)(p & 3) * pls; };
+
+  auto stage = [&](int q) {
+    if (q < 0 || q >= nk) return;
+    A* dst = X(q);
+    const int cnt = rows * ni;
+    const size_t base = (size_t)q * sz + (size_t)jr0 * sy;
+    for (int e = threadIdx.x; e < cnt; e += BLOCK) {
+      A v;
+      if (ZERO_X) {
+        v = A(0);
+      } else {
+        v = ldg(a.x_in + base + e);
+        if (PROLONG) {
+          int i = e % ni, j = jr0 + e / ni;
+          v = v + ldg(a.xc + lin3(i >> 1, j >> 1, q >> 1, a.cni, a.cnj));
+        }
+      }
+      dst[e] = v;
+    }
+  };
+
+  // relax every cell of colour `parity` ((i+j+p)&1) on plane p, rows [r0, r1)
+  auto relax = [&](int p, int r0, int r1, int parity) {
+    A* xm1 = X(p - 1);
+    A* x0 = X(p);
+    A* xp1 = X(p + 1);
+    const int width = ni;
+    const int cnt = (r1 - r0) * width;
+    const size_t pbase = (size_t)p * sz;
+    for (int e = threadIdx.x; e < cnt; e += BLOCK) {
+      int j = r0 + e / width;
+      int i = e - (j - r0) * width;
+      if (((i + j + p) & 1) != parity) continue;
+      size_t g = pbase + (size_t)j * sy + i;
+      int s = (j - jr0) * width + i;  // staged index
+      A sum = A(0);
+      if (p > 0) sum = sum + A(ldg(a.zp + g - sz)) * xm1[s];
+      if (j > 0) sum = sum + A(ldg(a.yp + g - sy)) * x0[s - width];
+      if (i > 0) sum = sum + A(ldg(a.xp + g - 1)) * x0[s - 1];
+      if (i < ni - 1) sum = sum + A(ldg(a.xp + g)) * x0[s + 1];
+      if (j < nj - 1) sum = sum + A(ldg(a.yp + g)) * x0[s + width];
+      if (p < nk - 1) sum = sum + A(ldg(a.zp + g)) * xp1[s];
+      A d = A(ldg(a.diag + g));
+      x0[s] = (d != A(0)) ? (ldg(a.b + g) - sum) / d : A(0);
+    }
+  };
+
+  double dot = 0.0;
+  stage(k0 - 2);
+  stage(k0 - 1);
+  for (int p = k0 - 1; p <= kend; ++p) {
+    stage(p + 1);
+    __syncthreads();
+    if (p >= 0 && p < nk) relax(p, jred0, jred1, 1);
+    __syncthreads();
+    const int q = p - 1;
+    const bool out_plane = (q >= k0 && q < kend);
+    if (out_plane) relax(q, j0, jout1, 0);
+    __syncthreads();
+    if (out_plane) {
+      const A* src = X(q) + (size_t)(j0 - jr0) * ni;
+      const int cnt = (jout1 - j0) * ni;
+      const size_t base = (size_t)q * sz + (size_t)j0 * sy;
+      for (int e = threadIdx.x; e < cnt; e += BLOCK) {
+        A v = src[e];
+        V o = cvt<V>(v);
+        a.x_out[base + e] = o;
+        if (DOT) dot += (double)ldv(&o) * (double)ldg(a.b + base + e);
+      }
+    }
+  }
+  if (DOT) {
+    double s = block_sum<BLOCK>(dot, red_smem);
+    if (threadIdx.x == 0) a.dot_partial[blockIdx.x + gridDim.x * blockIdx.y] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Residual and restriction: b_c = R (b - A x), AlgebraicMultigrid.h:105-117.
+// The residual of a row subtracts entry by entry in column order, diagonal
+// included (multiply_and_subtract, sparse_matrix.h:460-480); the restriction
+// adds 0.125*r over the children in ascending fine index, starting from 0
+// (multiply, sparse_matrix.h:356-362).  One thread per coarse cell.
+template <typename S, typename V, typename VC, bool ZERO_X>
+__global__ void residual_restrict_kernel(const V* __restrict__ x, const V* __restrict__ b,
+                                         const S* __restrict__ diag, const S* __restrict__ xp,
+                                         const S* __restrict__ yp, const S* __restrict__ zp, VC* __restrict__ bc,
+                                         int ni, int nj, int nk, int cni, int cnj, int cnk) {
+  using A = typename Num<V>::Acc;
+  int I = blockIdx.x * blockDim.x + threadIdx.x;
+  int J = blockIdx.y * blockDim.y + threadIdx.y;
+  int K = blockIdx.z;
+  if (I >= cni || J >= cnj || K >= cnk) return;
+  const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
+  A s = A(0);
+#pragma unroll
+  for (int kk = 0; kk <= 1; ++kk)
+#pragma unroll
+    for (int jj = 0; jj <= 1; ++jj)
+#pragma unroll
+      for (int ii = 0; ii <= 1; ++ii) {
+        int i = 2 * I + ii, j = 2 * J + jj, k = 2 * K + kk;
+        if (i >= ni || j >= nj || k >= nk) continue;
+        size_t g = lin3(i, j, k, ni, nj);
+        A r = ldg(b + g);
+        if (!ZERO_X) {
+          if (k > 0) r = r - A(ldg(zp + g - sz)) * A(ldg(x + g - sz));
+          if (j > 0) r = r - A(ldg(yp + g - sy)) * A(ldg(x + g - sy));
+          if (i > 0) r = r - A(ldg(xp + g - 1)) * A(ldg(x + g - 1));
+          r = r - A(ldg(diag + g)) * A(ldg(x + g));
+          if (i < ni - 1) r = r - A(ldg(xp + g)) * A(ldg(x + g + 1));
+          if (j < nj - 1) r = r - A(ldg(yp + g)) * A(ldg(x + g + sy));
+          if (k < nk - 1) r = r - A(ldg(zp + g)) * A(ldg(x + g + sz));
+        }
+        s = s + A(0.125) * r;
+      }
+  bc[lin3(I, J, K, cni, cnj)] = cvt<VC>((typename Num<VC>::Acc)s);
+}
+
+// x_f += P x_c (prolongatoin, AlgebraicMultigrid.h:118-129); only used when
+// a level has no post-smoothing sweep to fuse it into.
+template <typename V, typename VC>
+__global__ void prolong_add_kernel(V* __restrict__ xf, const VC* __restrict__ xc, int ni, int nj, int nk, int cni,
+                                   int cnj) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z;
+  if (i >= ni || j >= nj) return;
+  size_t g = lin3(i, j, k, ni, nj);
+  using A = typename Num<V>::Acc;
+  xf[g] = cvt<V>(A(ldv(xf + g)) + A(ldg(xc + lin3(i >> 1, j >> 1, k >> 1, cni, cnj))));
+}
+
+// ---------------------------------------------------------------------------
+// Coarsest level: `sweeps` red-black sweeps from x = 0 (AlgebraicMultigrid.h:
+// 159-160, 200 sweeps), the whole level resident in shared memory of one
+// CTA.  Up to 4096 unknowns (the coarsening stops at <= 16^3,
+// GeometricLevelGen.h:46), six arrays of Acc.
+template <typename S, typename V, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) coarsest_rbgs_kernel(const V* __restrict__ b, const S* __restrict__ diag,
+                                                             const S* __restrict__ xp, const S* __restrict__ yp,
+                                                             const S* __restrict__ zp, V* __restrict__ x_out,
+                                                             int ni, int nj, int nk, int sweeps,
+                                                             double* dot_out) {
+  using A = typename Num<V>::Acc;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = ni * nj * nk;
+  A* xs = reinterpret_cast<A*>(smem_raw);
+  A* bs = xs + n;
+  A* ds = bs + n;
+  A* xps = ds + n;
+  A* yps = xps + n;
+  A* zps = yps + n;
+  __shared__ double red_smem[BLOCK / 32];
+  for (int e = threadIdx.x; e < n; e += BLOCK) {
+    xs[e] = A(0);
+    bs[e] = A(ldg(b + e));
+    ds[e] = A(ldg(diag + e));
+    xps[e] = A(ldg(xp + e));
+    yps[e] = A(ldg(yp + e));
+    zps[e] = A(ldg(zp + e));
+  }
+  __syncthreads();
+  const int sy = ni, sz = ni * nj;
+  for (int it = 0; it < sweeps; ++it) {
+    for (int parity = 1; parity >= 0; --parity) {
+      for (int e = threadIdx.x; e < n; e += BLOCK) {
+        int i = e % ni;
+        int j = (e / ni) % nj;
+        int k = e / sz;
+        if (((i + j + k) & 1) != parity) continue;
+        A sum = A(0);
+        if (k > 0) sum = sum + zps[e - sz] * xs[e - sz];
+        if (j > 0) sum = sum + yps[e - sy] * xs[e - sy];
+        if (i > 0) sum = sum + xps[e - 1] * xs[e - 1];
+        if (i < ni - 1) sum = sum + xps[e] * xs[e + 1];
+        if (j < nj - 1) sum = sum + yps[e] * xs[e + sy];
+        if (k < nk - 1) sum = sum + zps[e] * xs[e + sz];
+        A d = ds[e];
+        xs[e] = (d != A(0)) ? (bs[e] - sum) / d : A(0);
+      }
+      __syncthreads();
+    }
+  }
+  double dot = 0.0;
+  for (int e = threadIdx.x; e < n; e += BLOCK) {
+    V v = cvt<V>(xs[e]);
+    x_out[e] = v;
+    if (dot_out) dot += (double)ldv(&v) * (double)bs[e];
+  }
+  if (dot_out) {
+    double s = block_sum<BLOCK>(dot, red_smem);
+    if (threadIdx.x == 0) *dot_out = s;
+  }
+}
+
+}  // namespace vflip

@@ -1,0 +1,191 @@
+// PCG vector kernels and the on-device scalar recurrence of AMGPCGSolve
+// (Smoke_Solver/AlgebraicMultigrid.h:189-301).
+//
+// The PCG scalars (rho, alpha, beta, the residual norm) live in device memory
+// in FP64 for every precision mode; block partials of each reduction are
+// combined in a fixed order by the last block to finish (threadfence +
+// counter), so every reduction is deterministic run to run.
+#pragma once
+#include "common.cuh"
+
+namespace vflip {
+
+struct PcgScalars {
+  double rho;        // z.r of the current iterate
+  double rho_new;
+  double sz;         // s.(A s)
+  double alpha;
+  double beta;
+  double res;        // |r|_inf
+  double tol;        // tolerance_factor * |rhs|_inf
+  int converged;     // res <= tol
+  int bad_rho;       // rho == 0 or NaN
+  unsigned int done_blocks[4];  // last-block-done counters, one per reduction kind
+};
+
+enum ReduceKind { kReduceSZ = 0, kReduceRes = 1, kReduceRho = 2, kReduceRes0 = 3 };
+
+// Called by every thread of every block after thread 0 wrote the block's
+// partial: the last block to arrive folds all partials in index order and
+// updates the scalars.
+template <int BLOCK>
+__device__ __forceinline__ void finish_reduction(double* partials, int nblocks, PcgScalars* st, int kind,
+                                                 double tol_factor, int launched_blocks) {
+  __shared__ bool last;
+  __shared__ double sm[BLOCK / 32];
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned int ticket = atomicAdd(&st->done_blocks[kind], 1u);
+    last = (ticket == (unsigned)launched_blocks - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // fold: each thread sums a fixed strided subset, then a fixed-order tree
+  double v = 0.0;
+  for (int q = threadIdx.x; q < nblocks; q += BLOCK) {
+    double p = ((volatile double*)partials)[q];
+    if (kind == kReduceRes || kind == kReduceRes0) v = fmax(v, p);
+    else v += p;
+  }
+  double tot = (kind == kReduceRes || kind == kReduceRes0) ? block_absmax<BLOCK>(v, sm) : block_sum<BLOCK>(v, sm);
+  if (threadIdx.x == 0) {
+    st->done_blocks[kind] = 0;
+    if (kind == kReduceSZ) {
+      st->sz = tot;
+      st->alpha = st->rho / tot;
+    } else if (kind == kReduceRes) {
+      st->res = tot;
+      st->converged = (tot <= st->tol) ? 1 : 0;
+    } else if (kind == kReduceRes0) {
+      st->res = tot;
+      st->tol = tol_factor * tot;
+      st->converged = (tot == 0.0) ? 1 : 0;
+    } else {  // kReduceRho
+      st->rho_new = tot;
+      st->beta = tot / st->rho;  // unused after the first V-cycle (s = z there)
+      st->rho = tot;
+      st->bad_rho = (tot == 0.0 || tot != tot) ? 1 : 0;
+    }
+  }
+}
+
+// Folds partials already written by another kernel (the fused dot of the
+// last smoothing sweep); launched with a single block.
+template <int BLOCK>
+__global__ void fold_kernel(double* partials, int nblocks, PcgScalars* st, int kind, double tol_factor) {
+  // a single block performs the whole fold
+  finish_reduction<BLOCK>(partials, nblocks, st, kind, tol_factor, 1);
+}
+
+// r = rhs (converted to the vector type), x = 0, partial |rhs|_inf.
+template <typename T, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) pcg_init_kernel(const double* __restrict__ rhs, T* __restrict__ r,
+                                                        T* __restrict__ x, size_t n, double* partials,
+                                                        PcgScalars* st, double tol_factor) {
+  __shared__ double sm[BLOCK / 32];
+  double m = 0.0;
+  for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK) {
+    double v = rhs[i];
+    r[i] = cvt<T>((typename Num<T>::Acc)v);
+    x[i] = cvt<T>((typename Num<T>::Acc)0);
+    m = fmax(m, fabs(v));
+  }
+  double bm = block_absmax<BLOCK>(m, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = bm;
+  finish_reduction<BLOCK>(partials, gridDim.x, st, kReduceRes0, tol_factor, gridDim.x);
+}
+
+// s_new = first ? z : z + beta*s_old   (AlgebraicMultigrid.h:254, 284)
+// q = A s_new                           (multiply, sparse_matrix.h:356-362)
+// partial s_new.q                        (AlgebraicMultigrid.h:259)
+// One thread per cell of a (32 x 8) x-y tile, marching k.  The neighbours'
+// s_new are recomputed from z and s_old, so s_old is never overwritten.
+template <typename T, bool FIRST, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) pcg_spmv_dot_kernel(const T* __restrict__ z, const T* __restrict__ s_old,
+                                                            T* __restrict__ s_new, T* __restrict__ q,
+                                                            const T* __restrict__ diag, const T* __restrict__ xp,
+                                                            const T* __restrict__ yp, const T* __restrict__ zp,
+                                                            int ni, int nj, int nk, int kz, double* partials,
+                                                            PcgScalars* st) {
+  using A = typename Num<T>::Acc;
+  __shared__ double sm[BLOCK / 32];
+  const int i = blockIdx.x * 32 + (threadIdx.x & 31);
+  const int j = blockIdx.y * (BLOCK / 32) + (threadIdx.x >> 5);
+  const int kb = blockIdx.z * kz, ke = min(kb + kz, nk);
+  const size_t sy = (size_t)ni, szs = (size_t)ni * nj;
+  const double beta = FIRST ? 0.0 : st->beta;
+  double dot = 0.0;
+  if (i < ni && j < nj) {
+    for (int k = kb; k < ke; ++k) {
+      size_t g = lin3(i, j, k, ni, nj);
+      auto sv = [&](size_t gg) -> A {
+        if (FIRST) return ldg(z + gg);
+        T t = cvt<T>((A)((double)ldg(z + gg) + beta * (double)ldg(s_old + gg)));
+        return ldv(&t);
+      };
+      A sc = sv(g);
+      A acc = A(0);
+      if (k > 0) acc = acc + ldg(zp + g - szs) * sv(g - szs);
+      if (j > 0) acc = acc + ldg(yp + g - sy) * sv(g - sy);
+      if (i > 0) acc = acc + ldg(xp + g - 1) * sv(g - 1);
+      acc = acc + ldg(diag + g) * sc;
+      if (i < ni - 1) acc = acc + ldg(xp + g) * sv(g + 1);
+      if (j < nj - 1) acc = acc + ldg(yp + g) * sv(g + sy);
+      if (k < nk - 1) acc = acc + ldg(zp + g) * sv(g + szs);
+      s_new[g] = cvt<T>(sc);
+      T qq = cvt<T>(acc);
+      q[g] = qq;
+      dot += (double)sc * (double)ldv(&qq);
+    }
+  }
+  double bs = block_sum<BLOCK>(dot, sm);
+  int nb = gridDim.x * gridDim.y * gridDim.z;
+  int bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  if (threadIdx.x == 0) partials[bid] = bs;
+  finish_reduction<BLOCK>(partials, nb, st, kReduceSZ, 0.0, nb);
+}
+
+// x += alpha s, r -= alpha q, partial |r|_inf  (AlgebraicMultigrid.h:259-262)
+template <typename T, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) pcg_update_kernel(T* __restrict__ x, T* __restrict__ r,
+                                                          const T* __restrict__ s, const T* __restrict__ q, size_t n,
+                                                          double* partials, PcgScalars* st) {
+  __shared__ double sm[BLOCK / 32];
+  const double alpha = st->alpha;
+  const double nalpha = -alpha;
+  double m = 0.0;
+  for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK) {
+    double xv = (double)ldv(x + i) + alpha * (double)ldg(s + i);
+    double rv = (double)ldv(r + i) + nalpha * (double)ldg(q + i);
+    T rt = cvt<T>((typename Num<T>::Acc)rv);
+    x[i] = cvt<T>((typename Num<T>::Acc)xv);
+    r[i] = rt;
+    m = fmax(m, fabs((double)ldv(&rt)));
+  }
+  double bm = block_absmax<BLOCK>(m, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = bm;
+  finish_reduction<BLOCK>(partials, gridDim.x, st, kReduceRes, 0.0, gridDim.x);
+}
+
+// Plain z.r when the V-cycle could not fuse it (single-level hierarchies
+// produce it inside the coarsest kernel instead).
+template <typename T, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) dot_kernel(const T* __restrict__ a, const T* __restrict__ b, size_t n,
+                                                   double* partials, PcgScalars* st, int kind) {
+  __shared__ double sm[BLOCK / 32];
+  double s = 0.0;
+  for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK)
+    s += (double)ldg(a + i) * (double)ldg(b + i);
+  double bs = block_sum<BLOCK>(s, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = bs;
+  finish_reduction<BLOCK>(partials, gridDim.x, st, kind, 0.0, gridDim.x);
+}
+
+template <typename T, int BLOCK>
+__global__ void to_double_kernel(const T* __restrict__ src, double* __restrict__ dst, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK)
+    dst[i] = (double)ldg(src + i);
+}
+
+}  // namespace vflip

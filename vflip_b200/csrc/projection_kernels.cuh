@@ -1,0 +1,217 @@
+// Pressure-projection kernels around the solve: face weights, inflow
+// overwrite, matrix-free assembly of the 7-point operator and right-hand
+// side, gradient update.  Each follows SmokeSolver3D::pcg_projection
+// (Smoke_Solver/Smoke_solver3D.cpp:874-1202) with the reference's float /
+// double mix and order of operations, so the FP64 operator and rhs equal the
+// reference's SparseMatrixd/rhs entry for entry.
+#pragma once
+#include "common.cuh"
+
+namespace vflip {
+
+// fraction_inside, levelset_util.cpp:4-13
+__device__ __forceinline__ float frac2(float l, float r) {
+  if (l < 0 && r < 0) return 1.0f;
+  if (l < 0 && r >= 0) return l / (l - r);
+  if (l >= 0 && r < 0) return r / (r - l);
+  return 0.0f;
+}
+
+__device__ __forceinline__ void rot4(float& a, float& b, float& c, float& d) {
+  float t = a;
+  a = b; b = c; c = d; d = t;
+}
+
+// fraction_inside of a square, levelset_util.cpp:23-103.  The corner list is
+// (bl, br, tr, tl) and is rotated exactly as the reference rotates it.  The
+// reference's rotation loops never end when the corners that count as inside
+// (phi <= 0) include exact zeros in some patterns (e.g. phi = {0, 0, 1, 1});
+// here each loop is bounded by the four possible rotations and a failed
+// search returns -1, after which the caller re-evaluates with exact zeros
+// moved to the smallest positive float (the limit from the outside).
+__device__ __forceinline__ float frac4_try(float bl, float br, float tl, float tr) {
+  int inside = (bl <= 0) + (tl <= 0) + (br <= 0) + (tr <= 0);
+  float q0 = bl, q1 = br, q2 = tr, q3 = tl;
+  if (inside == 4) return 1.0f;
+  if (inside == 3) {
+    int n = 0;
+    while (q0 < 0) { if (++n > 4) return -1.0f; rot4(q0, q1, q2, q3); }
+    float s0 = 1 - frac2(q0, q3);
+    float s1 = 1 - frac2(q0, q1);
+    return 1 - 0.5f * s0 * s1;
+  }
+  if (inside == 2) {
+    int n = 0;
+    while (q0 >= 0 || !(q1 < 0 || q2 < 0)) { if (++n > 4) return -1.0f; rot4(q0, q1, q2, q3); }
+    if (q1 < 0) return 0.5f * (frac2(q0, q3) + frac2(q1, q2));
+    float mid = 0.25f * (q0 + q1 + q2 + q3);
+    if (mid < 0) {
+      float area = 0;
+      float s1 = 1 - frac2(q0, q3);
+      float s3 = 1 - frac2(q2, q3);
+      area += 0.5f * s1 * s3;
+      float s2 = 1 - frac2(q2, q1);
+      float s0 = 1 - frac2(q0, q1);
+      area += 0.5f * s0 * s2;
+      return 1 - area;
+    }
+    float area = 0;
+    float s0 = frac2(q0, q1);
+    float s1 = frac2(q0, q3);
+    area += 0.5f * s0 * s1;
+    float s2 = frac2(q2, q1);
+    float s3 = frac2(q2, q3);
+    area += 0.5f * s2 * s3;
+    return area;
+  }
+  if (inside == 1) {
+    int n = 0;
+    while (q0 >= 0) { if (++n > 4) return -1.0f; rot4(q0, q1, q2, q3); }
+    float s0 = frac2(q0, q3);
+    float s1 = frac2(q0, q1);
+    return 0.5f * s0 * s1;
+  }
+  return 0.0f;
+}
+
+__device__ __forceinline__ float nudge_zero(float x) { return x == 0.0f ? 1.17549435e-38f : x; }
+
+__device__ __forceinline__ float frac4(float bl, float br, float tl, float tr) {
+  float f = frac4_try(bl, br, tl, tr);
+  if (f < 0.0f) f = frac4_try(nudge_zero(bl), nudge_zero(br), nudge_zero(tl), nudge_zero(tr));
+  return f;
+}
+
+__device__ __forceinline__ float clamp01(float a) { return a < 0.0f ? 0.0f : (a > 1.0f ? 1.0f : a); }
+
+// compute_face_weights, Smoke_solver3D.cpp:874-944.  One thread per face of
+// the three face grids (flattened: u, then v, then w).
+__global__ void face_weights_kernel(const float* __restrict__ phi, float* __restrict__ uw, float* __restrict__ vw,
+                                    float* __restrict__ ww, int ni, int nj, int nk) {
+  const size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
+  const int px = ni + 1, py = nj + 1;
+  auto P = [&](int i, int j, int k) { return __ldg(phi + lin3(i, j, k, px, py)); };
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nu + nv + nw;
+       e += (size_t)gridDim.x * blockDim.x) {
+    if (e < nu) {
+      int i = (int)(e % (ni + 1)), j = (int)((e / (ni + 1)) % nj), k = (int)(e / ((size_t)(ni + 1) * nj));
+      uw[e] = clamp01(1 - frac4(P(i, j, k), P(i, j + 1, k), P(i, j, k + 1), P(i, j + 1, k + 1)));
+    } else if (e < nu + nv) {
+      size_t f = e - nu;
+      int i = (int)(f % ni), j = (int)((f / ni) % (nj + 1)), k = (int)(f / ((size_t)ni * (nj + 1)));
+      vw[f] = clamp01(1 - frac4(P(i, j, k), P(i, j, k + 1), P(i + 1, j, k), P(i + 1, j, k + 1)));
+    } else {
+      size_t f = e - nu - nv;
+      int i = (int)(f % ni), j = (int)((f / ni) % nj), k = (int)(f / ((size_t)ni * nj));
+      ww[f] = clamp01(1 - frac4(P(i, j, k), P(i, j + 1, k), P(i + 1, j, k), P(i + 1, j + 1, k)));
+    }
+  }
+}
+
+// Inflow overwrite, Smoke_solver3D.cpp:964-980: every cell with b_desc == 1
+// pins its six faces (u = U_in, v = w = 0).  Concurrent writers store the
+// same value, so the result is order independent.
+__global__ void inflow_kernel(const int8_t* __restrict__ bdesc, float* __restrict__ u, float* __restrict__ v,
+                              float* __restrict__ w, float U_in, int ni, int nj, int nk) {
+  const size_t n = (size_t)ni * nj * nk;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    if (bdesc[e] != 1) continue;
+    int i = (int)(e % ni), j = (int)((e / ni) % nj), k = (int)(e / ((size_t)ni * nj));
+    u[lin3(i, j, k, ni + 1, nj)] = U_in;
+    u[lin3(i + 1, j, k, ni + 1, nj)] = U_in;
+    v[lin3(i, j, k, ni, nj + 1)] = 0.0f;
+    v[lin3(i, j + 1, k, ni, nj + 1)] = 0.0f;
+    w[lin3(i, j, k, ni, nj)] = 0.0f;
+    w[lin3(i, j, k + 1, ni, nj)] = 0.0f;
+  }
+}
+
+// Matrix-free assembly, Smoke_solver3D.cpp:984-1111, for interior cells
+// 1..n-2 (ring rows stay empty: diag = 0, which the smoother maps to x = 0,
+// i.e. Dirichlet p = 0 on the ring).  Writes the FP64 operator (diag, +x,
+// +y, +z; the -x/-y/-z couplings the reference also stores are the +x/+y/+z
+// couplings of the neighbour, equal by construction) and the FP64 rhs.
+__global__ void assemble_kernel(const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
+                                const float* __restrict__ uw, const float* __restrict__ vw,
+                                const float* __restrict__ ww, const float* __restrict__ us,
+                                const float* __restrict__ vs, const float* __restrict__ ws, double* __restrict__ diag,
+                                double* __restrict__ xp, double* __restrict__ yp, double* __restrict__ zp,
+                                double* __restrict__ rhs, float h, int ni, int nj, int nk) {
+  const size_t n = (size_t)ni * nj * nk;
+  const float h2 = h * h;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(e % ni), j = (int)((e / ni) % nj), k = (int)(e / ((size_t)ni * nj));
+    double d = 0.0, cx = 0.0, cy = 0.0, cz = 0.0, b = 0.0;
+    if (i >= 1 && i < ni - 1 && j >= 1 && j < nj - 1 && k >= 1 && k < nk - 1) {
+      const size_t iu0 = lin3(i, j, k, ni + 1, nj), iu1 = lin3(i + 1, j, k, ni + 1, nj);
+      const size_t iv0 = lin3(i, j, k, ni, nj + 1), iv1 = lin3(i, j + 1, k, ni, nj + 1);
+      const size_t iw0 = lin3(i, j, k, ni, nj), iw1 = lin3(i, j, k + 1, ni, nj);
+      float t;
+      t = uw[iu1] / h2; d = (double)t; if (i < ni - 2) cx = (double)(-t);
+      b = b - (double)(uw[iu1] * u[iu1] / h);
+      t = uw[iu0] / h2; d = d + (double)t;
+      b = b + (double)(uw[iu0] * u[iu0] / h);
+      t = vw[iv1] / h2; d = d + (double)t; if (j < nj - 2) cy = (double)(-t);
+      b = b - (double)(vw[iv1] * v[iv1] / h);
+      t = vw[iv0] / h2; d = d + (double)t;
+      b = b + (double)(vw[iv0] * v[iv0] / h);
+      t = ww[iw1] / h2; d = d + (double)t; if (k < nk - 2) cz = (double)(-t);
+      b = b - (double)(ww[iw1] * w[iw1] / h);
+      t = ww[iw0] / h2; d = d + (double)t;
+      b = b + (double)(ww[iw0] * w[iw0] / h);
+      if (d > 0) {
+        float sv = (uw[iu1] - 1.0f) * us[iu1] - (uw[iu0] - 1.0f) * us[iu0] + (vw[iv1] - 1.0f) * vs[iv1] -
+                   (vw[iv0] - 1.0f) * vs[iv0] + (ww[iw1] - 1.0f) * ws[iw1] - (ww[iw0] - 1.0f) * ws[iw0];
+        b = b + (1.0 / (double)h) * (double)sv;
+      }
+    }
+    diag[e] = d;
+    xp[e] = cx;
+    yp[e] = cy;
+    zp[e] = cz;
+    rhs[e] = b;
+  }
+}
+
+// Gradient update, Smoke_solver3D.cpp:1126-1200: on the faces strictly
+// between two interior cells (u: i in [2, ni-2], j,k in [1, n-2]; v, w
+// analogous) u -= (float)(p_i - p_{i-1}) / h where the face is open, else
+// u = u_solid.  Other faces are left untouched, as in the reference.
+template <typename P>
+__global__ void gradient_kernel(const P* __restrict__ p, float* __restrict__ u, float* __restrict__ v,
+                                float* __restrict__ w, const float* __restrict__ uw, const float* __restrict__ vw,
+                                const float* __restrict__ ww, const float* __restrict__ us,
+                                const float* __restrict__ vs, const float* __restrict__ ws, float h, int ni, int nj,
+                                int nk) {
+  const size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
+  const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nu + nv + nw;
+       e += (size_t)gridDim.x * blockDim.x) {
+    if (e < nu) {
+      int i = (int)(e % (ni + 1)), j = (int)((e / (ni + 1)) % nj), k = (int)(e / ((size_t)(ni + 1) * nj));
+      if (k < nk - 1 && k > 0 && j < nj - 1 && j > 0 && i < ni - 1 && i > 1) {
+        size_t c = lin3(i, j, k, ni, nj);
+        if (uw[e] > 0) u[e] = u[e] - (float)((double)p[c] - (double)p[c - 1]) / h;
+        else u[e] = us[e];
+      }
+    } else if (e < nu + nv) {
+      size_t f = e - nu;
+      int i = (int)(f % ni), j = (int)((f / ni) % (nj + 1)), k = (int)(f / ((size_t)ni * (nj + 1)));
+      if (k < nk - 1 && k > 0 && j > 1 && j < nj - 1 && i < ni - 1 && i > 0) {
+        size_t c = lin3(i, j, k, ni, nj);
+        if (vw[f] > 0) v[f] = v[f] - (float)((double)p[c] - (double)p[c - sy]) / h;
+        else v[f] = vs[f];
+      }
+    } else {
+      size_t f = e - nu - nv;
+      int i = (int)(f % ni), j = (int)((f / ni) % nj), k = (int)(f / ((size_t)ni * nj));
+      if (k > 1 && k < nk - 1 && j < nj - 1 && j > 0 && i < ni - 1 && i > 0) {
+        size_t c = lin3(i, j, k, ni, nj);
+        if (ww[f] > 0) w[f] = w[f] - (float)((double)p[c] - (double)p[c - sz]) / h;
+        else w[f] = ws[f];
+      }
+    }
+  }
+}
+
+}  // namespace vflip

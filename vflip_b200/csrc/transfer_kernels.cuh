@@ -1,0 +1,311 @@
+// Grid sampling, semi-Lagrangian advection and the FLIP particle<->grid
+// transfers.
+//
+// Sampling follows Buffer3D::sample_linear/at (Smoke_Solver/fluid_buffer3D.h:
+// 205-248): world -> grid coordinates in double, floor, clamp-to-edge, three
+// levels of lerp in double, rounded to float at the end.  Keeping that FP64
+// arithmetic makes advection and G2P bit-identical to the reference.
+//
+// P2G is a sort-by-cell gather: particles are bucketed by cell with a
+// counting sort whose buckets are then put into ascending particle order, so
+// each face node sums its neighbours' contributions in exactly the order
+// SmokeSolver3D::particle_to_grid does (27 buckets in (k,j,i) order, bucket
+// contents in insertion order, Smoke_solver3D.cpp:1477-1502).  The sums are
+// deterministic and bit-identical to the reference.
+#pragma once
+#include "common.cuh"
+
+namespace vflip {
+
+struct GridView {
+  const float* d;
+  int nx, ny, nz;
+  double h, ox, oy, oz;
+};
+
+__device__ __forceinline__ float grid_at(const GridView& g, int i, int j, int k) {
+  i = i < 0 ? 0 : (i > g.nx - 1 ? g.nx - 1 : i);
+  j = j < 0 ? 0 : (j > g.ny - 1 ? g.ny - 1 : j);
+  k = k < 0 ? 0 : (k > g.nz - 1 ? g.nz - 1 : k);
+  return __ldg(g.d + lin3(i, j, k, g.nx, g.ny));
+}
+
+__device__ __forceinline__ double lerp_d(double a, double b, double c) { return (1.0 - c) * a + c * b; }
+
+__device__ __forceinline__ float sample_linear(const GridView& g, double wx, double wy, double wz) {
+  double gx = wx / g.h + g.ox, gy = wy / g.h + g.oy, gz = wz / g.h + g.oz;
+  int i = (int)floor(gx), j = (int)floor(gy), k = (int)floor(gz);
+  double cx = gx - (double)i, cy = gy - (double)j, cz = gz - (double)k;
+  double v1 = lerp_d(lerp_d(grid_at(g, i, j, k), grid_at(g, i + 1, j, k), cx),
+                     lerp_d(grid_at(g, i, j + 1, k), grid_at(g, i + 1, j + 1, k), cx), cy);
+  double v2 = lerp_d(lerp_d(grid_at(g, i, j, k + 1), grid_at(g, i + 1, j, k + 1), cx),
+                     lerp_d(grid_at(g, i, j + 1, k + 1), grid_at(g, i + 1, j + 1, k + 1), cx), cy);
+  return (float)lerp_d(v1, v2, cz);
+}
+
+// SubDomainSolver::advect_field, sub_domain.cpp:191-235: RK2 midpoint
+// backtrace through the MAC velocity, then a trilinear sample of the field.
+// The field's node (i,j,k) sits at world ((i-ox)h, (j-oy)h, (k-oz)h).
+__global__ void advect_rk2_kernel(GridView u, GridView v, GridView w, GridView f, float* __restrict__ out, float h,
+                                  float dt) {
+  const size_t n = (size_t)f.nx * f.ny * f.nz;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(e % f.nx), j = (int)((e / f.nx) % f.ny), k = (int)(e / ((size_t)f.nx * f.ny));
+    float wx = (float)(((double)(float)i - f.ox) * (double)h);
+    float wy = (float)(((double)(float)j - f.oy) * (double)h);
+    float wz = (float)(((double)(float)k - f.oz) * (double)h);
+    float a = sample_linear(u, wx, wy, wz), b = sample_linear(v, wx, wy, wz), c = sample_linear(w, wx, wy, wz);
+    const double hdt = 0.5 * (double)dt;
+    float px = (float)((double)wx - hdt * (double)a);
+    float py = (float)((double)wy - hdt * (double)b);
+    float pz = (float)((double)wz - hdt * (double)c);
+    a = sample_linear(u, px, py, pz);
+    b = sample_linear(v, px, py, pz);
+    c = sample_linear(w, px, py, pz);
+    px = wx - dt * a;
+    py = wy - dt * b;
+    pz = wz - dt * c;
+    out[e] = sample_linear(f, px, py, pz);
+  }
+}
+
+// getDelta, Smoke_solver3D.cpp:1298-1319
+__global__ void delta_kernel(const float* __restrict__ after, const float* __restrict__ before,
+                             float* __restrict__ delta, size_t n) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    delta[e] = after[e] - before[e];
+}
+
+// ------------------------------------------------------------------ P2G
+// The reference's particle record (fluid_particle.h:14-20), 40 bytes.
+struct ParticleRec {
+  float pos[3];
+  float vel[3];
+  float dens, temp;
+  int hash_idx, sub_hash_idx;
+};
+static_assert(sizeof(ParticleRec) == 40, "particle record is 40 bytes");
+
+// hash_FLIP cell, Smoke_solver3D.cpp:1337-1343: int((pos + 0.5h)/h) with
+// C truncation; values outside (-1, n) (and NaN) are out of range, as the
+// x86 conversion makes them in the reference.
+__device__ __forceinline__ int hash_cell(const float* pos, int ni, int nj, int nk, float h) {
+  const float c = 0.5f * h;
+  float tx = (pos[0] + c) / h, ty = (pos[1] + c) / h, tz = (pos[2] + c) / h;
+  if (!(tx > -1.0f && tx < (float)ni)) return -1;
+  if (!(ty > -1.0f && ty < (float)nj)) return -1;
+  if (!(tz > -1.0f && tz < (float)nk)) return -1;
+  return ((int)tz * nj + (int)ty) * ni + (int)tx;
+}
+
+__global__ void hash_count_kernel(const ParticleRec* __restrict__ p, int np, int ni, int nj, int nk, float h,
+                                  int* __restrict__ cell, int* __restrict__ slot, int* __restrict__ count) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
+    int c = hash_cell(p[q].pos, ni, nj, nk, h);
+    cell[q] = c;
+    slot[q] = (c >= 0) ? atomicAdd(count + c, 1) : -1;
+  }
+}
+
+// Exclusive scan of int counts, three-phase (block scan, scan of block
+// sums, add).  SCAN_BLOCK threads x 4 items per block.
+constexpr int kScanBlock = 512;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* sm, int& total) {
+  // warp inclusive
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sm[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int s = (lane < kScanBlock / 32) ? sm[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    if (lane < kScanBlock / 32) sm[lane] = s;
+  }
+  __syncthreads();
+  int warp_prefix = (wid > 0) ? sm[wid - 1] : 0;
+  total = sm[kScanBlock / 32 - 1];
+  __syncthreads();
+  return warp_prefix + x - v;
+}
+
+__global__ void __launch_bounds__(kScanBlock) scan_tiles_kernel(const int* __restrict__ in, int* __restrict__ out,
+                                                               int* __restrict__ tile_sums, size_t n) {
+  __shared__ int sm[32];
+  size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int local = 0;
+#pragma unroll
+  for (int t = 0; t < kScanItems; ++t) {
+    v[t] = (base + t < n) ? in[base + t] : 0;
+    local += v[t];
+  }
+  int total;
+  int pre = block_exclusive_scan(local, sm, total);
+#pragma unroll
+  for (int t = 0; t < kScanItems; ++t) {
+    if (base + t < n) out[base + t] = pre;
+    pre += v[t];
+  }
+  if (threadIdx.x == 0 && tile_sums) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void scan_add_kernel(int* __restrict__ out, const int* __restrict__ tile_prefix, size_t n) {
+  size_t base = (size_t)blockIdx.x * kScanTile;
+  int add = tile_prefix[blockIdx.x];
+  for (int t = threadIdx.x; t < kScanTile; t += blockDim.x)
+    if (base + t < n) out[base + t] += add;
+}
+
+__global__ void scatter_kernel(const int* __restrict__ cell, const int* __restrict__ slot,
+                               const int* __restrict__ start, int* __restrict__ order, int np) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
+    int c = cell[q];
+    if (c >= 0) order[start[c] + slot[q]] = q;
+  }
+}
+
+// Put every bucket into ascending particle order (the order hash_FLIP
+// pushes them in).  Insertion sort for the usual handful of particles per
+// cell, heapsort beyond 32.
+__device__ __forceinline__ void sift_down(int* a, int root, int end) {
+  while (true) {
+    int child = 2 * root + 1;
+    if (child >= end) return;
+    if (child + 1 < end && a[child] < a[child + 1]) ++child;
+    if (a[root] >= a[child]) return;
+    int t = a[root]; a[root] = a[child]; a[child] = t;
+    root = child;
+  }
+}
+
+__global__ void sort_buckets_kernel(const int* __restrict__ start, int* __restrict__ order, int ncells) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) {
+    int b = start[c], e = start[c + 1];
+    int m = e - b;
+    if (m < 2) continue;
+    int* a = order + b;
+    if (m <= 32) {
+      for (int x = 1; x < m; ++x) {
+        int key = a[x];
+        int y = x - 1;
+        while (y >= 0 && a[y] > key) { a[y + 1] = a[y]; --y; }
+        a[y + 1] = key;
+      }
+    } else {
+      for (int r = m / 2 - 1; r >= 0; --r) sift_down(a, r, m);
+      for (int end = m - 1; end > 0; --end) {
+        int t = a[0]; a[0] = a[end]; a[end] = t;
+        sift_down(a, 0, end);
+      }
+    }
+  }
+}
+
+// Sorted structure-of-arrays copy for the gather: pos.xyz + a flag in .w
+// (1 when all three velocity components are finite), vel.xyz.
+// Only the start[ncells] bucketed particles are gathered (`total` points at
+// that count on the device); particles outside the grid have no slot.
+__global__ void gather_sorted_kernel(const ParticleRec* __restrict__ p, const int* __restrict__ order,
+                                     float4* __restrict__ spos, float4* __restrict__ svel,
+                                     const int* __restrict__ total) {
+  const int nsorted = *total;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nsorted; e += gridDim.x * blockDim.x) {
+    const ParticleRec& r = p[order[e]];
+    bool fin = isfinite(r.vel[0]) && isfinite(r.vel[1]) && isfinite(r.vel[2]);
+    spos[e] = make_float4(r.pos[0], r.pos[1], r.pos[2], fin ? 1.0f : 0.0f);
+    svel[e] = make_float4(r.vel[0], r.vel[1], r.vel[2], 0.0f);
+  }
+}
+
+__device__ __forceinline__ float tent(float r) {  // SmokeSolver3D::H, Smoke_solver3D.h:217-223
+  float res = 0.0f;
+  if (r >= -1.0f && r < 0.0f) res = 1.0f + r;
+  if (r >= 0.0f && r < 1.0f) res = 1.0f - r;
+  return res;
+}
+
+// particle_to_grid for one velocity component, Smoke_solver3D.cpp:1451-1510:
+// field = sum(w v)/sum(w), coef = sum(w), with sum(w) starting at 1e-5 and
+// the weight H(dx/h)H(dy/h)H(dz/h).  A particle whose offset from the node
+// exceeds 1.0001 h on some axis has weight exactly 0 and (finite velocity)
+// contributes exactly nothing, so it is skipped without changing any sum.
+__global__ void p2g_kernel(const int* __restrict__ start, const float4* __restrict__ spos,
+                           const float4* __restrict__ svel, float* __restrict__ field, float* __restrict__ coef,
+                           int comp, int ni, int nj, int nk, float h) {
+  const int fx = ni + (comp == 0), fy = nj + (comp == 1), fz = nk + (comp == 2);
+  const double ox = comp == 0 ? 0.5 : 0.0, oy = comp == 1 ? 0.5 : 0.0, oz = comp == 2 ? 0.5 : 0.0;
+  const size_t n = (size_t)fx * fy * fz;
+  const float reach = h * 1.0001f;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(e % fx), j = (int)((e / fx) % fy), k = (int)(e / ((size_t)fx * fy));
+    float gx = (float)(((double)(float)i - ox) * (double)h);
+    float gy = (float)(((double)(float)j - oy) * (double)h);
+    float gz = (float)(((double)(float)k - oz) * (double)h);
+    float tw = 1e-5f, tv = 0.0f;
+    for (int dk = -1; dk <= 1; ++dk) {
+      int ck = k + dk;
+      if (ck < 0 || ck >= nk) continue;
+      for (int dj = -1; dj <= 1; ++dj) {
+        int cj = j + dj;
+        if (cj < 0 || cj >= nj) continue;
+        for (int di = -1; di <= 1; ++di) {
+          int ci = i + di;
+          if (ci < 0 || ci >= ni) continue;
+          int c = (ck * nj + cj) * ni + ci;
+          int b = __ldg(start + c), en = __ldg(start + c + 1);
+          for (int q = b; q < en; ++q) {
+            float4 pp = __ldg(spos + q);
+            float dx = pp.x - gx, dy = pp.y - gy, dz = pp.z - gz;
+            if (pp.w != 0.0f && (fabsf(dx) >= reach || fabsf(dy) >= reach || fabsf(dz) >= reach)) continue;
+            float wgt = tent(dx / h) * tent(dy / h) * tent(dz / h);
+            float4 vv = __ldg(svel + q);
+            float vc = comp == 0 ? vv.x : (comp == 1 ? vv.y : vv.z);
+            tw = tw + wgt;
+            tv = tv + wgt * vc;
+          }
+        }
+      }
+    }
+    coef[e] = tw;
+    field[e] = tv / tw;
+  }
+}
+
+// particle_from_grid, Smoke_solver3D.cpp:1398-1406 (flip_ratio == 1:
+// vel += trilinear(delta)); otherwise the FLIP/PIC blend of
+// fluid_particle::interpolate, fluid_particle.h:315-328, evaluated in double:
+// vel = (1 - f) u_new(pos) + f (vel + delta(pos)).
+__global__ void g2p_kernel(ParticleRec* __restrict__ p, int np, GridView du, GridView dv, GridView dw, GridView un,
+                           GridView vn, GridView wn, double flip_ratio) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
+    ParticleRec r = p[q];
+    double x = r.pos[0], y = r.pos[1], z = r.pos[2];
+    float d0 = sample_linear(du, x, y, z), d1 = sample_linear(dv, x, y, z), d2 = sample_linear(dw, x, y, z);
+    if (flip_ratio == 1.0) {
+      r.vel[0] = r.vel[0] + d0;
+      r.vel[1] = r.vel[1] + d1;
+      r.vel[2] = r.vel[2] + d2;
+    } else {
+      const double pic = 1.0 - flip_ratio;
+      float s0 = sample_linear(un, x, y, z), s1 = sample_linear(vn, x, y, z), s2 = sample_linear(wn, x, y, z);
+      r.vel[0] = (float)(pic * (double)s0 + flip_ratio * (double)(r.vel[0] + d0));
+      r.vel[1] = (float)(pic * (double)s1 + flip_ratio * (double)(r.vel[1] + d1));
+      r.vel[2] = (float)(pic * (double)s2 + flip_ratio * (double)(r.vel[2] + d2));
+    }
+    p[q].vel[0] = r.vel[0];
+    p[q].vel[1] = r.vel[1];
+    p[q].vel[2] = r.vel[2];
+  }
+}
+
+}  // namespace vflip

@@ -1,0 +1,1058 @@
+// C ABI of libvflip_gpu.so (declared in include/vflip.h): context, device
+// buffer cache, multigrid hierarchy, V-cycle and PCG orchestration, and the
+// projection / advection / transfer entry points.
+//
+// The PCG loop follows ivock::AMGPCGSolve (Smoke_Solver/AlgebraicMultigrid.h:
+// 189-301) step for step; its scalars stay on the device and the host reads
+// one small struct per iteration to test convergence.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/vflip.h"
+#include "common.cuh"
+#include "mg_kernels.cuh"
+#include "pcg_kernels.cuh"
+#include "projection_kernels.cuh"
+#include "transfer_kernels.cuh"
+
+using namespace vflip;
+
+namespace {
+
+constexpr int kSweepBlock = 256;
+constexpr int kRedBlock = 256;
+constexpr int kCoarseBlock = 1024;
+constexpr int kMaxPartials = 1 << 16;
+
+struct Dims {
+  int ni, nj, nk;
+  size_t n() const { return (size_t)ni * nj * nk; }
+};
+
+}  // namespace
+
+struct vflip_ctx {
+  vflip_config cfg;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  std::unordered_map<std::string, std::pair<void*, size_t>> bufs;
+  PcgScalars* st = nullptr;         // device
+  PcgScalars* st_host = nullptr;    // pinned
+  double* partials = nullptr;       // device, kMaxPartials
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0.0;
+  int num_sms = 148;
+
+  int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    err = buf;
+    return code;
+  }
+  // Cached device buffer of at least `bytes`, keyed by name.
+  void* buf(const std::string& name, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    auto it = bufs.find(name);
+    if (it != bufs.end() && it->second.second >= bytes) return it->second.first;
+    if (it != bufs.end()) {
+      cudaFree(it->second.first);
+      bufs.erase(it);
+    }
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    bufs[name] = {p, bytes};
+    return p;
+  }
+};
+
+#define VF_CUDA(call)                                                                         \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess) return ctx->fail(VFLIP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+#define VF_LAUNCH_CHECK()                                                                      \
+  do {                                                                                        \
+    cudaError_t e_ = cudaGetLastError();                                                      \
+    if (e_ != cudaSuccess) return ctx->fail(VFLIP_ERR_CUDA, "launch: %s", cudaGetErrorString(e_)); \
+  } while (0)
+
+#define VF_ALLOC(ptr, type, name, count)                                                     \
+  do {                                                                                        \
+    ptr = (type*)ctx->buf((name), sizeof(type) * (size_t)(count));                           \
+    if (!ptr) return ctx->fail(VFLIP_ERR_NOMEM, "cudaMalloc failed for %s", std::string(name).c_str()); \
+  } while (0)
+
+namespace {
+
+int grid_for(size_t n, int block, int num_sms) {
+  size_t g = (n + block - 1) / block;
+  size_t cap = (size_t)num_sms * 16;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+// Level sizes: ceil(n/2) per axis while the level has more than
+// `max_unknowns` unknowns (GeometricLevelGen.h:44-58).
+std::vector<Dims> level_dims(int ni, int nj, int nk, int max_unknowns) {
+  std::vector<Dims> d{{ni, nj, nk}};
+  unsigned unknowns = (unsigned)ni * nj * nk;
+  while (unknowns > (unsigned)max_unknowns) {
+    Dims c{(d.back().ni + 1) / 2, (d.back().nj + 1) / 2, (d.back().nk + 1) / 2};
+    d.push_back(c);
+    unknowns = (unsigned)c.ni * c.nj * c.nk;
+  }
+  return d;
+}
+
+// Typed view of one level: operator (S) and vectors (V).
+template <typename S, typename V>
+struct Level {
+  Dims d;
+  const S* diag;
+  const S* xp;
+  const S* yp;
+  const S* zp;
+  V* b;   // coarse levels own their rhs; level 0 reads the PCG residual
+  V* xa;
+  V* xb;
+};
+
+struct SweepShape {
+  int tyo, kz, plane_stride, grid_y, grid_z;
+  size_t smem;
+};
+
+template <typename A>
+SweepShape sweep_shape(const Dims& d, int num_sms) {
+  const int target = sizeof(A) == 8 ? 1536 : 3072;  // staged cells per plane
+  int tyo = std::max(1, target / std::max(1, d.ni) - 4);
+  tyo = std::min(tyo, d.nj);
+  int gy = (d.nj + tyo - 1) / tyo;
+  int want = num_sms * 4;
+  int nz_chunks = std::max(1, std::min(d.nk, (want + gy - 1) / gy));
+  int kz = std::max(4, (d.nk + nz_chunks - 1) / nz_chunks);
+  kz = std::min(kz, d.nk);
+  int gz = (d.nk + kz - 1) / kz;
+  int rows = std::min(tyo + 4, d.nj);
+  int pls = rows * d.ni;
+  pls = (pls + 3) & ~3;
+  SweepShape s{tyo, kz, pls, gy, gz, (size_t)4 * pls * sizeof(A)};
+  return s;
+}
+
+template <typename S, typename V, bool Z, bool P, bool D>
+int launch_sweep_t(vflip_ctx* ctx, const SweepArgs<S, V>& a, const SweepShape& sh) {
+  auto kern = rbgs_sweep_kernel<S, V, Z, P, D, kSweepBlock>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set = true;
+  }
+  dim3 grid(sh.grid_y, sh.grid_z);
+  kern<<<grid, kSweepBlock, sh.smem, ctx->stream>>>(a);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+// One sweep x_in -> x_out on a level; x_in == nullptr means x = 0.
+template <typename S, typename V>
+int sweep(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_out, const V* xc, const Dims* cd,
+          double* dot_partial, int* nblocks_out = nullptr) {
+  using A = typename Num<V>::Acc;
+  SweepShape sh = sweep_shape<A>(L.d, ctx->num_sms);
+  if (sh.smem > 200 * 1024) return ctx->fail(VFLIP_ERR_ARG, "grid row of %d cells too long for one CTA", L.d.ni);
+  SweepArgs<S, V> a;
+  a.x_in = x_in;
+  a.x_out = x_out;
+  a.b = b;
+  a.diag = L.diag;
+  a.xp = L.xp;
+  a.yp = L.yp;
+  a.zp = L.zp;
+  a.xc = xc;
+  a.ni = L.d.ni;
+  a.nj = L.d.nj;
+  a.nk = L.d.nk;
+  a.cni = cd ? cd->ni : 0;
+  a.cnj = cd ? cd->nj : 0;
+  a.tyo = sh.tyo;
+  a.kz = sh.kz;
+  a.plane_stride = sh.plane_stride;
+  a.dot_partial = dot_partial;
+  if (nblocks_out) *nblocks_out = sh.grid_y * sh.grid_z;
+  if (sh.grid_y * sh.grid_z > kMaxPartials) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
+  bool zero = (x_in == nullptr), pro = (xc != nullptr), dot = (dot_partial != nullptr);
+  if (zero && !pro && !dot) return launch_sweep_t<S, V, true, false, false>(ctx, a, sh);
+  if (zero && !pro && dot) return launch_sweep_t<S, V, true, false, true>(ctx, a, sh);
+  if (!zero && pro && !dot) return launch_sweep_t<S, V, false, true, false>(ctx, a, sh);
+  if (!zero && pro && dot) return launch_sweep_t<S, V, false, true, true>(ctx, a, sh);
+  if (!zero && !pro && !dot) return launch_sweep_t<S, V, false, false, false>(ctx, a, sh);
+  if (!zero && !pro && dot) return launch_sweep_t<S, V, false, false, true>(ctx, a, sh);
+  return ctx->fail(VFLIP_ERR_ARG, "sweep: prolongation needs an incoming x");
+}
+
+template <typename S, typename V>
+int coarsest(vflip_ctx* ctx, const Level<S, V>& L, const V* b, V* x_out, int sweeps, double* dot_out) {
+  using A = typename Num<V>::Acc;
+  size_t n = L.d.n();
+  size_t smem = 6 * n * sizeof(A);
+  auto kern = coarsest_rbgs_kernel<S, V, kCoarseBlock>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
+    attr_set = true;
+  }
+  if (smem > 220 * 1024) return ctx->fail(VFLIP_ERR_ARG, "coarsest level of %zu unknowns exceeds 4096", n);
+  kern<<<1, kCoarseBlock, smem, ctx->stream>>>(b, L.diag, L.xp, L.yp, L.zp, x_out, L.d.ni, L.d.nj, L.d.nk, sweeps,
+                                               dot_out);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+template <typename S, typename V, typename VC>
+int restrict_to(vflip_ctx* ctx, const Level<S, V>& L, const V* x, const V* b, VC* bc, const Dims& cd) {
+  dim3 blk(32, 8);
+  dim3 grid((cd.ni + 31) / 32, (cd.nj + 7) / 8, cd.nk);
+  if (x)
+    residual_restrict_kernel<S, V, VC, false><<<grid, blk, 0, ctx->stream>>>(
+        x, b, L.diag, L.xp, L.yp, L.zp, bc, L.d.ni, L.d.nj, L.d.nk, cd.ni, cd.nj, cd.nk);
+  else
+    residual_restrict_kernel<S, V, VC, true><<<grid, blk, 0, ctx->stream>>>(
+        x, b, L.diag, L.xp, L.yp, L.zp, bc, L.d.ni, L.d.nj, L.d.nk, cd.ni, cd.nj, cd.nk);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+// ---------------------------------------------------------------- hierarchy
+// Device storage of a hierarchy in FP64 (always built: the coarsening is
+// exact FP64 arithmetic) plus typed copies for the FP32/mixed modes.
+struct Hierarchy64 {
+  std::vector<Dims> dims;
+  std::vector<double*> lv;  // 4 arrays per level, contiguous: diag, xp, yp, zp
+};
+
+int build_hierarchy64(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const double* xp,
+                      const double* yp, const double* zp, Hierarchy64& H) {
+  H.dims = level_dims(ni, nj, nk, ctx->cfg.coarsest_max_unknowns);
+  H.lv.assign(H.dims.size(), nullptr);
+  for (size_t l = 1; l < H.dims.size(); ++l) {
+    double* p;
+    VF_ALLOC(p, double, "h64_" + std::to_string(l), 4 * H.dims[l].n());
+    H.lv[l] = p;
+  }
+  for (size_t l = 1; l < H.dims.size(); ++l) {
+    const Dims& f = H.dims[l - 1];
+    const Dims& c = H.dims[l];
+    const double *fd, *fx, *fy, *fz;
+    if (l == 1) {
+      fd = diag; fx = xp; fy = yp; fz = zp;
+    } else {
+      size_t fn = f.n();
+      fd = H.lv[l - 1]; fx = fd + fn; fy = fx + fn; fz = fy + fn;
+    }
+    size_t cn = c.n();
+    double* cdp = H.lv[l];
+    dim3 blk(32, 8);
+    dim3 grid((c.ni + 31) / 32, (c.nj + 7) / 8, c.nk);
+    galerkin_coarsen_kernel<<<grid, blk, 0, ctx->stream>>>(fd, fx, fy, fz, cdp, cdp + cn, cdp + 2 * cn,
+                                                           cdp + 3 * cn, f.ni, f.nj, f.nk, c.ni, c.nj, c.nk);
+    VF_LAUNCH_CHECK();
+  }
+  return VFLIP_OK;
+}
+
+template <typename T>
+int convert_array(vflip_ctx* ctx, const double* src, T* dst, size_t n) {
+  convert_kernel<T><<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(src, dst, n);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+// Typed levels: level 0 uses (S0, V), coarse levels (SC, V).
+template <typename S0, typename SC, typename V>
+struct Typed {
+  Level<S0, V> fine;
+  std::vector<Level<SC, V>> coarse;  // coarse[l-1] = level l
+};
+
+template <typename S, typename V>
+int make_level(vflip_ctx* ctx, const Hierarchy64& H, size_t l, const double* d0, const double* x0,
+               const double* y0, const double* z0, Level<S, V>& L, const char* tag) {
+  L.d = H.dims[l];
+  size_t n = L.d.n();
+  const double *d, *x, *y, *z;
+  if (l == 0) {
+    d = d0; x = x0; y = y0; z = z0;
+  } else {
+    d = H.lv[l]; x = d + n; y = x + n; z = y + n;
+  }
+  if (std::is_same<S, double>::value) {
+    L.diag = (const S*)d; L.xp = (const S*)x; L.yp = (const S*)y; L.zp = (const S*)z;
+  } else {
+    S* p;
+    VF_ALLOC(p, S, std::string(tag) + "_op_" + std::to_string(l), 4 * n);
+    int rc;
+    if ((rc = convert_array<S>(ctx, d, p, n))) return rc;
+    if ((rc = convert_array<S>(ctx, x, p + n, n))) return rc;
+    if ((rc = convert_array<S>(ctx, y, p + 2 * n, n))) return rc;
+    if ((rc = convert_array<S>(ctx, z, p + 3 * n, n))) return rc;
+    L.diag = p; L.xp = p + n; L.yp = p + 2 * n; L.zp = p + 3 * n;
+  }
+  V* v;
+  VF_ALLOC(v, V, std::string(tag) + "_vec_" + std::to_string(l), 3 * n);
+  L.b = v; L.xa = v + n; L.xb = v + 2 * n;
+  return VFLIP_OK;
+}
+
+template <typename S0, typename SC, typename V>
+int make_typed(vflip_ctx* ctx, const Hierarchy64& H, const double* d0, const double* x0, const double* y0,
+               const double* z0, Typed<S0, SC, V>& T, const char* tag) {
+  int rc;
+  if ((rc = make_level<S0, V>(ctx, H, 0, d0, x0, y0, z0, T.fine, tag))) return rc;
+  T.coarse.resize(H.dims.size() - 1);
+  for (size_t l = 1; l < H.dims.size(); ++l)
+    if ((rc = make_level<SC, V>(ctx, H, l, d0, x0, y0, z0, T.coarse[l - 1], tag))) return rc;
+  return VFLIP_OK;
+}
+
+// ---------------------------------------------------------------- V-cycle
+// amgVCycle (AlgebraicMultigrid.h:130-176) from x = 0.  Level l >= 1 runs
+// on T.coarse[l-1].  Returns the level's final x through *xout.
+template <typename S0, typename SC, typename V, typename S>
+int smooth_down(vflip_ctx* ctx, const Level<S, V>& L, const V* b, V** cur_out) {
+  const int pre = ctx->cfg.pre_sweeps;
+  V* cur = nullptr;
+  for (int s = 0; s < pre; ++s) {
+    V* out = (cur == L.xa) ? L.xb : L.xa;
+    int rc = sweep<S, V>(ctx, L, b, cur, out, nullptr, nullptr, nullptr);
+    if (rc) return rc;
+    cur = out;
+  }
+  *cur_out = cur;  // nullptr when pre == 0 (x = 0)
+  return VFLIP_OK;
+}
+
+template <typename S, typename V>
+int smooth_up(vflip_ctx* ctx, const Level<S, V>& L, const V* b, V* cur, const V* xc, const Dims& cd, V* final_out,
+              double* dot_partial, int* dot_blocks, V** result) {
+  const int post = ctx->cfg.post_sweeps;
+  int rc;
+  if (cur == nullptr) {
+    // pre == 0: x is zero before prolongation; materialise x = P x_c
+    cur = L.xa;
+    VF_CUDA(cudaMemsetAsync(cur, 0, sizeof(V) * L.d.n(), ctx->stream));
+  }
+  if (post == 0) {
+    dim3 blk(32, 8), grid((L.d.ni + 31) / 32, (L.d.nj + 7) / 8, L.d.nk);
+    prolong_add_kernel<V, V><<<grid, blk, 0, ctx->stream>>>(cur, xc, L.d.ni, L.d.nj, L.d.nk, cd.ni, cd.nj);
+    VF_LAUNCH_CHECK();
+    if (final_out && final_out != cur) VF_CUDA(cudaMemcpyAsync(final_out, cur, sizeof(V) * L.d.n(),
+                                                              cudaMemcpyDeviceToDevice, ctx->stream));
+    *result = final_out ? final_out : cur;
+    if (dot_blocks) *dot_blocks = 0;
+    return VFLIP_OK;
+  }
+  for (int s = 0; s < post; ++s) {
+    bool last = (s == post - 1);
+    V* out = (last && final_out) ? final_out : ((cur == L.xa) ? L.xb : L.xa);
+    rc = sweep<S, V>(ctx, L, b, cur, out, s == 0 ? xc : nullptr, &cd, last ? dot_partial : nullptr,
+                     last ? dot_blocks : nullptr);
+    if (rc) return rc;
+    cur = out;
+  }
+  *result = cur;
+  return VFLIP_OK;
+}
+
+// z = V(r); when want_dot, rho_new = z.r is reduced into the PCG scalars.
+template <typename S0, typename SC, typename V>
+int vcycle(vflip_ctx* ctx, Typed<S0, SC, V>& T, const V* r, V* z, bool want_dot) {
+  int rc;
+  const int nl = (int)T.coarse.size() + 1;
+  if (nl == 1) {
+    rc = coarsest<S0, V>(ctx, T.fine, r, z, ctx->cfg.coarse_sweeps, want_dot ? ctx->partials : nullptr);
+    if (rc) return rc;
+    if (want_dot) {
+      fold_kernel<kRedBlock><<<1, kRedBlock, 0, ctx->stream>>>(ctx->partials, 1, ctx->st, kReduceRho, 0.0);
+      VF_LAUNCH_CHECK();
+    }
+    return VFLIP_OK;
+  }
+  std::vector<V*> after_pre(nl, nullptr);
+  // down
+  if ((rc = smooth_down<S0, SC, V, S0>(ctx, T.fine, r, &after_pre[0]))) return rc;
+  if ((rc = restrict_to<S0, V, V>(ctx, T.fine, after_pre[0], r, T.coarse[0].b, T.coarse[0].d))) return rc;
+  for (int l = 1; l < nl - 1; ++l) {
+    Level<SC, V>& L = T.coarse[l - 1];
+    if ((rc = smooth_down<S0, SC, V, SC>(ctx, L, L.b, &after_pre[l]))) return rc;
+    if ((rc = restrict_to<SC, V, V>(ctx, L, after_pre[l], L.b, T.coarse[l].b, T.coarse[l].d))) return rc;
+  }
+  // bottom
+  Level<SC, V>& B = T.coarse[nl - 2];
+  if ((rc = coarsest<SC, V>(ctx, B, B.b, B.xa, ctx->cfg.coarse_sweeps, nullptr))) return rc;
+  V* xc = B.xa;
+  Dims cd = B.d;
+  // up
+  for (int l = nl - 2; l >= 1; --l) {
+    Level<SC, V>& L = T.coarse[l - 1];
+    V* res;
+    if ((rc = smooth_up<SC, V>(ctx, L, L.b, after_pre[l], xc, cd, nullptr, nullptr, nullptr, &res))) return rc;
+    xc = res;
+    cd = L.d;
+  }
+  int dot_blocks = 0;
+  V* res;
+  if ((rc = smooth_up<S0, V>(ctx, T.fine, r, after_pre[0], xc, cd, z, want_dot ? ctx->partials : nullptr,
+                             &dot_blocks, &res)))
+    return rc;
+  if (want_dot) {
+    if (dot_blocks > 0) {
+      fold_kernel<kRedBlock><<<1, kRedBlock, 0, ctx->stream>>>(ctx->partials, dot_blocks, ctx->st, kReduceRho, 0.0);
+    } else {
+      size_t n = T.fine.d.n();
+      dot_kernel<V, kRedBlock><<<grid_for(n, kRedBlock, ctx->num_sms), kRedBlock, 0, ctx->stream>>>(
+          z, r, n, ctx->partials, ctx->st, kReduceRho);
+    }
+    VF_LAUNCH_CHECK();
+  }
+  return VFLIP_OK;
+}
+
+// ---------------------------------------------------------------- PCG
+int read_scalars(vflip_ctx* ctx) {
+  VF_CUDA(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(PcgScalars), cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return VFLIP_OK;
+}
+
+template <typename S0, typename SC, typename V>
+int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor, int maxit,
+              vflip_solve_stats* stats) {
+  const Dims d = T.fine.d;
+  const size_t n = d.n();
+  V *x, *r, *z, *s0, *s1, *q;
+  VF_ALLOC(x, V, "pcg_x", n);
+  VF_ALLOC(r, V, "pcg_r", n);
+  VF_ALLOC(z, V, "pcg_z", n);
+  VF_ALLOC(s0, V, "pcg_s0", n);
+  VF_ALLOC(s1, V, "pcg_s1", n);
+  VF_ALLOC(q, V, "pcg_q", n);
+  VF_CUDA(cudaMemsetAsync(ctx->st, 0, sizeof(PcgScalars), ctx->stream));
+  int rc;
+  const int gb = grid_for(n, kRedBlock, ctx->num_sms);
+  pcg_init_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(rhs, r, x, n, ctx->partials, ctx->st,
+                                                                    tol_factor);
+  VF_LAUNCH_CHECK();
+  if ((rc = read_scalars(ctx))) return rc;
+  PcgScalars& h = *ctx->st_host;
+  const double rhs_norm = h.res;
+  int iterations = 0, vcycles = 0;
+  double residual = h.res;
+  auto finish = [&](int st_code) -> int {
+    to_double_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(x, result, n);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return ctx->fail(VFLIP_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+    if (stats) {
+      stats->iterations = iterations;
+      stats->vcycles = vcycles;
+      stats->levels = (int)T.coarse.size() + 1;
+      stats->converged = st_code == VFLIP_OK ? 1 : 0;
+      stats->residual = residual;
+      stats->rhs_norm = rhs_norm;
+    }
+    return st_code;
+  };
+  if (h.res == 0.0) {  // AlgebraicMultigrid.h:214-232
+    iterations = 0;
+    return finish(VFLIP_OK);
+  }
+  if ((rc = vcycle<S0, SC, V>(ctx, T, r, z, true))) return rc;
+  ++vcycles;
+  if ((rc = read_scalars(ctx))) return rc;
+  if (h.bad_rho) {  // AlgebraicMultigrid.h:236-252
+    iterations = 0;
+    return finish(VFLIP_NOT_CONVERGED);
+  }
+  dim3 sblk(kRedBlock);
+  const int kz = 8;
+  dim3 sgrid((d.ni + 31) / 32, (d.nj + kRedBlock / 32 - 1) / (kRedBlock / 32), (d.nk + kz - 1) / kz);
+  if ((size_t)sgrid.x * sgrid.y * sgrid.z > (size_t)kMaxPartials) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
+  V* s_old = s0;
+  V* s_new = s1;
+  int it;
+  for (it = 0; it < maxit; ++it) {
+    if (it == 0)
+      pcg_spmv_dot_kernel<V, true, kRedBlock><<<sgrid, sblk, 0, ctx->stream>>>(
+          z, s_old, s_new, q, T.fine.diag, T.fine.xp, T.fine.yp, T.fine.zp, d.ni, d.nj, d.nk, kz, ctx->partials,
+          ctx->st);
+    else
+      pcg_spmv_dot_kernel<V, false, kRedBlock><<<sgrid, sblk, 0, ctx->stream>>>(
+          z, s_old, s_new, q, T.fine.diag, T.fine.xp, T.fine.yp, T.fine.zp, d.ni, d.nj, d.nk, kz, ctx->partials,
+          ctx->st);
+    VF_LAUNCH_CHECK();
+    pcg_update_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(x, r, s_new, q, n, ctx->partials, ctx->st);
+    VF_LAUNCH_CHECK();
+    if ((rc = read_scalars(ctx))) return rc;
+    residual = h.res;
+    if (h.converged) {
+      iterations = it + 1;
+      return finish(VFLIP_OK);
+    }
+    if ((rc = vcycle<S0, SC, V>(ctx, T, r, z, true))) return rc;
+    ++vcycles;
+    std::swap(s_old, s_new);
+  }
+  iterations = it;
+  return finish(VFLIP_NOT_CONVERGED);
+}
+
+int check_dims(vflip_ctx* ctx, int ni, int nj, int nk) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  if (ni <= 0 || nj <= 0 || nk <= 0) return ctx->fail(VFLIP_ERR_ARG, "grid dimensions must be positive");
+  if ((double)ni * nj * nk > 2.0e9) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
+  return VFLIP_OK;
+}
+
+int solve_stencil(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const double* xp, const double* yp,
+                  const double* zp, const double* rhs, double* result, double tol, int maxit,
+                  vflip_solve_stats* stats) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (!diag || !xp || !yp || !zp || !rhs || !result) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  if (maxit < 0) return ctx->fail(VFLIP_ERR_ARG, "max_iterations < 0");
+  VF_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  Hierarchy64 H;
+  if ((rc = build_hierarchy64(ctx, ni, nj, nk, diag, xp, yp, zp, H))) return rc;
+  int status;
+  switch (ctx->cfg.precision) {
+    case VFLIP_PREC_FP64: {
+      Typed<double, double, double> T;
+      if ((rc = make_typed(ctx, H, diag, xp, yp, zp, T, "f64"))) return rc;
+      status = pcg_solve(ctx, T, rhs, result, tol, maxit, stats);
+      break;
+    }
+    case VFLIP_PREC_FP32: {
+      Typed<float, float, float> T;
+      if ((rc = make_typed(ctx, H, diag, xp, yp, zp, T, "f32"))) return rc;
+      status = pcg_solve(ctx, T, rhs, result, tol, maxit, stats);
+      break;
+    }
+    case VFLIP_PREC_MIXED: {
+      Typed<float, __nv_bfloat16, float> T;
+      if ((rc = make_typed(ctx, H, diag, xp, yp, zp, T, "mix"))) return rc;
+      status = pcg_solve(ctx, T, rhs, result, tol, maxit, stats);
+      break;
+    }
+    default:
+      return ctx->fail(VFLIP_ERR_ARG, "unknown precision %d", ctx->cfg.precision);
+  }
+  if (status < 0) return status;
+  VF_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  VF_CUDA(cudaEventSynchronize(ctx->ev1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  ctx->last_ms = ms;
+  if (stats) stats->solve_ms = ms;
+  return status;
+}
+
+}  // namespace
+
+// ============================================================== C ABI
+extern "C" {
+
+void vflip_config_default(vflip_config* cfg) {
+  if (!cfg) return;
+  cfg->precision = VFLIP_PREC_FP32;
+  cfg->pre_sweeps = 4;
+  cfg->post_sweeps = 4;
+  cfg->coarse_sweeps = 200;
+  cfg->coarsest_max_unknowns = 16 * 16 * 16;
+  cfg->device = 0;
+  cfg->stream = nullptr;
+}
+
+int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
+  if (!out) return VFLIP_ERR_ARG;
+  *out = nullptr;
+  vflip_ctx* ctx = new vflip_ctx();
+  if (cfg) ctx->cfg = *cfg;
+  else vflip_config_default(&ctx->cfg);
+  auto bad = [&](int code) {
+    delete ctx;
+    return code;
+  };
+  if (ctx->cfg.pre_sweeps < 0 || ctx->cfg.post_sweeps < 0 || ctx->cfg.coarse_sweeps < 0 ||
+      ctx->cfg.coarsest_max_unknowns < 1 || ctx->cfg.coarsest_max_unknowns > 4096 || ctx->cfg.precision < 0 ||
+      ctx->cfg.precision > 2)
+    return bad(VFLIP_ERR_ARG);
+  if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
+  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);
+  if (ctx->cfg.stream) {
+    ctx->stream = (cudaStream_t)ctx->cfg.stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
+    ctx->own_stream = true;
+  }
+  if (cudaMalloc(&ctx->st, sizeof(PcgScalars)) != cudaSuccess) return bad(VFLIP_ERR_NOMEM);
+  if (cudaMalloc(&ctx->partials, sizeof(double) * kMaxPartials) != cudaSuccess) return bad(VFLIP_ERR_NOMEM);
+  if (cudaMallocHost(&ctx->st_host, sizeof(PcgScalars)) != cudaSuccess) return bad(VFLIP_ERR_NOMEM);
+  if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
+    return bad(VFLIP_ERR_CUDA);
+  *out = ctx;
+  return VFLIP_OK;
+}
+
+int vflip_destroy(vflip_ctx* ctx) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->bufs) cudaFree(kv.second.first);
+  if (ctx->st) cudaFree(ctx->st);
+  if (ctx->partials) cudaFree(ctx->partials);
+  if (ctx->st_host) cudaFreeHost(ctx->st_host);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return VFLIP_OK;
+}
+
+const char* vflip_last_error(const vflip_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int vflip_synchronize(vflip_ctx* ctx) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return VFLIP_OK;
+}
+
+double vflip_last_ms(const vflip_ctx* ctx) { return ctx ? ctx->last_ms : 0.0; }
+
+int vflip_amgpcg_solve(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const double* xp,
+                       const double* yp, const double* zp, const double* rhs, double* result,
+                       double tolerance_factor, int max_iterations, vflip_solve_stats* stats) {
+  return solve_stencil(ctx, ni, nj, nk, diag, xp, yp, zp, rhs, result, tolerance_factor, max_iterations, stats);
+}
+
+int vflip_amgpcg_solve_csr(vflip_ctx* ctx, uint32_t n, const uint32_t* rowstart, const uint32_t* colindex,
+                           const double* value, const double* rhs, double* result, double tolerance_factor,
+                           int max_iterations, double* residual_out, int* iterations_out, int ni, int nj, int nk) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (!rowstart || !colindex || !value || !rhs || !result) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  if ((size_t)n != (size_t)ni * nj * nk) return ctx->fail(VFLIP_ERR_ARG, "n != ni*nj*nk");
+  // CSR -> 7 slots, checking the pattern (no wrap-around across rows/planes)
+  std::vector<double> st(7 * (size_t)n, 0.0);
+  const long long sy = ni, sz = (long long)ni * nj;
+  for (uint32_t r = 0; r < n; ++r) {
+    int i = (int)(r % ni), j = (int)((r / ni) % nj), k = (int)(r / sz);
+    for (uint32_t e = rowstart[r]; e < rowstart[r + 1]; ++e) {
+      long long dlt = (long long)colindex[e] - (long long)r;
+      int slot = -1;
+      if (dlt == 0) slot = 0;
+      else if (dlt == -1 && i > 0) slot = 1;
+      else if (dlt == 1 && i < ni - 1) slot = 2;
+      else if (dlt == -sy && j > 0) slot = 3;
+      else if (dlt == sy && j < nj - 1) slot = 4;
+      else if (dlt == -sz && k > 0) slot = 5;
+      else if (dlt == sz && k < nk - 1) slot = 6;
+      if (slot < 0) return ctx->fail(VFLIP_ERR_NOT_7POINT, "row %u has an entry at column %u off the 7-point pattern",
+                                     r, colindex[e]);
+      st[(size_t)slot * n + r] = value[e];
+    }
+  }
+  // symmetry: -x coupling of r equals +x coupling of r-1, etc.
+  for (uint32_t r = 0; r < n; ++r) {
+    int i = (int)(r % ni), j = (int)((r / ni) % nj), k = (int)(r / sz);
+    bool ok = true;
+    if (i > 0) ok &= st[1 * (size_t)n + r] == st[2 * (size_t)n + r - 1];
+    if (j > 0) ok &= st[3 * (size_t)n + r] == st[4 * (size_t)n + r - sy];
+    if (k > 0) ok &= st[5 * (size_t)n + r] == st[6 * (size_t)n + r - sz];
+    if (!ok) return ctx->fail(VFLIP_ERR_NOT_SYMMETRIC, "matrix is not symmetric at row %u", r);
+  }
+  double *dd, *drhs, *dres;
+  VF_ALLOC(dd, double, "csr_op", 4 * (size_t)n);
+  VF_ALLOC(drhs, double, "csr_rhs", n);
+  VF_ALLOC(dres, double, "csr_res", n);
+  VF_CUDA(cudaMemcpyAsync(dd, st.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(dd + n, st.data() + 2 * (size_t)n, sizeof(double) * n, cudaMemcpyHostToDevice,
+                          ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(dd + 2 * (size_t)n, st.data() + 4 * (size_t)n, sizeof(double) * n,
+                          cudaMemcpyHostToDevice, ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(dd + 3 * (size_t)n, st.data() + 6 * (size_t)n, sizeof(double) * n,
+                          cudaMemcpyHostToDevice, ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(drhs, rhs, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  vflip_solve_stats s{};
+  int status = solve_stencil(ctx, ni, nj, nk, dd, dd + n, dd + 2 * (size_t)n, dd + 3 * (size_t)n, drhs, dres,
+                             tolerance_factor, max_iterations, &s);
+  if (status < 0) return status;
+  VF_CUDA(cudaMemcpyAsync(result, dres, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (residual_out) *residual_out = s.residual;
+  if (iterations_out) *iterations_out = s.iterations;
+  return status;
+}
+
+int vflip_build_levels(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const double* xp,
+                       const double* yp, const double* zp, int max_levels, int* dims_out, double* levels_out) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (!diag || !xp || !yp || !zp) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  Hierarchy64 H;
+  if ((rc = build_hierarchy64(ctx, ni, nj, nk, diag, xp, yp, zp, H))) return rc;
+  int nl = (int)H.dims.size();
+  if (dims_out)
+    for (int l = 0; l < nl && l < max_levels; ++l) {
+      dims_out[3 * l] = H.dims[l].ni;
+      dims_out[3 * l + 1] = H.dims[l].nj;
+      dims_out[3 * l + 2] = H.dims[l].nk;
+    }
+  if (levels_out) {
+    size_t off = 0;
+    for (int l = 0; l < nl && l < max_levels; ++l) {
+      size_t n = H.dims[l].n();
+      if (l == 0) {
+        VF_CUDA(cudaMemcpyAsync(levels_out, diag, 8 * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        VF_CUDA(cudaMemcpyAsync(levels_out + n, xp, 8 * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        VF_CUDA(cudaMemcpyAsync(levels_out + 2 * n, yp, 8 * n, cudaMemcpyDeviceToDevice, ctx->stream));
+        VF_CUDA(cudaMemcpyAsync(levels_out + 3 * n, zp, 8 * n, cudaMemcpyDeviceToDevice, ctx->stream));
+      } else {
+        VF_CUDA(cudaMemcpyAsync(levels_out + off, H.lv[l], 32 * n, cudaMemcpyDeviceToDevice, ctx->stream));
+      }
+      off += 4 * n;
+    }
+  }
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  return nl;
+}
+
+int vflip_rbgs(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const double* xp, const double* yp,
+               const double* zp, const double* b, double* x, int iterations) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (!diag || !xp || !yp || !zp || !b || !x || iterations < 0) return ctx->fail(VFLIP_ERR_ARG, "bad argument");
+  size_t n = (size_t)ni * nj * nk;
+  double* tmp;
+  VF_ALLOC(tmp, double, "rbgs_tmp", n);
+  Level<double, double> L{{ni, nj, nk}, diag, xp, yp, zp, nullptr, nullptr, nullptr};
+  double* cur = x;
+  for (int s = 0; s < iterations; ++s) {
+    double* out = (cur == x) ? tmp : x;
+    if ((rc = sweep<double, double>(ctx, L, b, cur, out, nullptr, nullptr, nullptr))) return rc;
+    cur = out;
+  }
+  if (cur != x) VF_CUDA(cudaMemcpyAsync(x, cur, 8 * n, cudaMemcpyDeviceToDevice, ctx->stream));
+  return VFLIP_OK;
+}
+
+int vflip_vcycle(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const double* xp, const double* yp,
+                 const double* zp, const double* b, double* x) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (!diag || !xp || !yp || !zp || !b || !x) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  Hierarchy64 H;
+  if ((rc = build_hierarchy64(ctx, ni, nj, nk, diag, xp, yp, zp, H))) return rc;
+  size_t n = (size_t)ni * nj * nk;
+  const int gb = grid_for(n, 256, ctx->num_sms);
+  switch (ctx->cfg.precision) {
+    case VFLIP_PREC_FP64: {
+      Typed<double, double, double> T;
+      if ((rc = make_typed(ctx, H, diag, xp, yp, zp, T, "f64"))) return rc;
+      return vcycle(ctx, T, b, x, false);
+    }
+    case VFLIP_PREC_FP32:
+    case VFLIP_PREC_MIXED: {
+      float *bf, *xf;
+      VF_ALLOC(bf, float, "vc_b", n);
+      VF_ALLOC(xf, float, "vc_x", n);
+      convert_kernel<float><<<gb, 256, 0, ctx->stream>>>(b, bf, n);
+      VF_LAUNCH_CHECK();
+      if (ctx->cfg.precision == VFLIP_PREC_FP32) {
+        Typed<float, float, float> T;
+        if ((rc = make_typed(ctx, H, diag, xp, yp, zp, T, "f32"))) return rc;
+        if ((rc = vcycle(ctx, T, bf, xf, false))) return rc;
+      } else {
+        Typed<float, __nv_bfloat16, float> T;
+        if ((rc = make_typed(ctx, H, diag, xp, yp, zp, T, "mix"))) return rc;
+        if ((rc = vcycle(ctx, T, bf, xf, false))) return rc;
+      }
+      to_double_kernel<float, 256><<<gb, 256, 0, ctx->stream>>>(xf, x, n);
+      VF_LAUNCH_CHECK();
+      return VFLIP_OK;
+    }
+  }
+  return ctx->fail(VFLIP_ERR_ARG, "unknown precision");
+}
+
+int vflip_face_weights(vflip_ctx* ctx, int ni, int nj, int nk, const float* nodal_phi, float* uw, float* vw,
+                       float* ww) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (!nodal_phi || !uw || !vw || !ww) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  size_t tot = (size_t)(ni + 1) * nj * nk + (size_t)ni * (nj + 1) * nk + (size_t)ni * nj * (nk + 1);
+  face_weights_kernel<<<grid_for(tot, 256, ctx->num_sms), 256, 0, ctx->stream>>>(nodal_phi, uw, vw, ww, ni, nj, nk);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+int vflip_assemble(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, const float* nodal_phi,
+                   const int8_t* bdesc, const float* us, const float* vs, const float* ws, float* u, float* v,
+                   float* w, double* diag, double* xp, double* yp, double* zp, double* rhs) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (!nodal_phi || !bdesc || !us || !vs || !ws || !u || !v || !w || !diag || !xp || !yp || !zp || !rhs)
+    return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
+  float* wts;
+  VF_ALLOC(wts, float, "face_weights", nu + nv + nw);
+  if ((rc = vflip_face_weights(ctx, ni, nj, nk, nodal_phi, wts, wts + nu, wts + nu + nv))) return rc;
+  size_t n = (size_t)ni * nj * nk;
+  inflow_kernel<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(bdesc, u, v, w, U_in, ni, nj, nk);
+  VF_LAUNCH_CHECK();
+  assemble_kernel<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
+      u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, diag, xp, yp, zp, rhs, h, ni, nj, nk);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+int vflip_project(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, const float* nodal_phi,
+                  const int8_t* bdesc, const float* us, const float* vs, const float* ws, float* u, float* v,
+                  float* w, double* pressure, double tolerance_factor, int max_iterations,
+                  vflip_solve_stats* stats) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  size_t n = (size_t)ni * nj * nk;
+  double *op, *rhs, *p;
+  VF_ALLOC(op, double, "proj_op", 4 * n);
+  VF_ALLOC(rhs, double, "proj_rhs", n);
+  if (pressure) p = pressure;
+  else VF_ALLOC(p, double, "proj_p", n);
+  cudaEvent_t e0;
+  VF_CUDA(cudaEventCreate(&e0));
+  VF_CUDA(cudaEventRecord(e0, ctx->stream));
+  if ((rc = vflip_assemble(ctx, ni, nj, nk, h, U_in, nodal_phi, bdesc, us, vs, ws, u, v, w, op, op + n, op + 2 * n,
+                           op + 3 * n, rhs))) {
+    cudaEventDestroy(e0);
+    return rc;
+  }
+  vflip_solve_stats s{};
+  int status = solve_stencil(ctx, ni, nj, nk, op, op + n, op + 2 * n, op + 3 * n, rhs, p, tolerance_factor,
+                             max_iterations, &s);
+  if (status < 0) {
+    cudaEventDestroy(e0);
+    return status;
+  }
+  size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
+  float* wts = (float*)ctx->buf("face_weights", sizeof(float) * (nu + nv + nw));
+  gradient_kernel<double><<<grid_for(nu + nv + nw, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
+      p, u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, h, ni, nj, nk);
+  cudaError_t le = cudaGetLastError();
+  if (le != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return ctx->fail(VFLIP_ERR_CUDA, "launch: %s", cudaGetErrorString(le));
+  }
+  VF_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  VF_CUDA(cudaEventSynchronize(ctx->ev1));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, e0, ctx->ev1);
+  cudaEventDestroy(e0);
+  ctx->last_ms = ms;
+  if (stats) {
+    *stats = s;
+    stats->solve_ms = ms;
+  }
+  return status;
+}
+
+int vflip_advect_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                            const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
+                            double oz, const float* field, float* out) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (fnx <= 0 || fny <= 0 || fnz <= 0 || !u || !v || !w || !field || !out)
+    return ctx->fail(VFLIP_ERR_ARG, "bad argument");
+  if (out == field || out == u || out == v || out == w) return ctx->fail(VFLIP_ERR_ARG, "out aliases an input");
+  GridView gu{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0};
+  GridView gv{v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0};
+  GridView gw{w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5};
+  GridView gf{field, fnx, fny, fnz, (double)h, ox, oy, oz};
+  size_t n = (size_t)fnx * fny * fnz;
+  advect_rk2_kernel<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, h, dt);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+int vflip_delta(vflip_ctx* ctx, size_t n, const float* after, const float* before, float* delta) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  if (!after || !before || !delta) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  if (n == 0) return VFLIP_OK;
+  delta_kernel<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(after, before, delta, n);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+int vflip_particle_cells(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
+                         int* cell_out) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (np < 0 || (np > 0 && (!particles || !cell_out))) return ctx->fail(VFLIP_ERR_ARG, "bad argument");
+  if (np == 0) return VFLIP_OK;
+  size_t nc = (size_t)ni * nj * nk;
+  int *slot, *count;
+  VF_ALLOC(slot, int, "p_slot", np);
+  VF_ALLOC(count, int, "p_count", nc + 1);
+  VF_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (nc + 1), ctx->stream));
+  hash_count_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
+      (const ParticleRec*)particles, np, ni, nj, nk, h, cell_out, slot, count);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Exclusive scan of n ints (n may be large): tiles, then the tile sums
+// recursively.
+int exclusive_scan(vflip_ctx* ctx, const int* in, int* out, size_t n, int depth = 0) {
+  size_t tiles = (n + kScanTile - 1) / kScanTile;
+  int* sums = nullptr;
+  if (tiles > 1) {
+    VF_ALLOC(sums, int, "scan_sums_" + std::to_string(depth), tiles);
+  }
+  scan_tiles_kernel<<<(unsigned)tiles, kScanBlock, 0, ctx->stream>>>(in, out, sums, n);
+  VF_LAUNCH_CHECK();
+  if (tiles > 1) {
+    int* pre;
+    VF_ALLOC(pre, int, "scan_pre_" + std::to_string(depth), tiles);
+    int rc = exclusive_scan(ctx, sums, pre, tiles, depth + 1);
+    if (rc) return rc;
+    scan_add_kernel<<<(unsigned)tiles, 256, 0, ctx->stream>>>(out, pre, n);
+    VF_LAUNCH_CHECK();
+  }
+  return VFLIP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vflip_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np, float* u,
+              float* ucoef, float* v, float* vcoef, float* w, float* wcoef) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (np < 0 || (np > 0 && !particles)) return ctx->fail(VFLIP_ERR_ARG, "bad particle array");
+  if ((!u) != (!ucoef) || (!v) != (!vcoef) || (!w) != (!wcoef))
+    return ctx->fail(VFLIP_ERR_ARG, "field and coef pointers must be given in pairs");
+  size_t nc = (size_t)ni * nj * nk;
+  int *cell, *slot, *count, *start, *order;
+  float4 *spos, *svel;
+  size_t npp = np > 0 ? (size_t)np : 1;
+  VF_ALLOC(cell, int, "p_cell", npp);
+  VF_ALLOC(slot, int, "p_slot", npp);
+  VF_ALLOC(count, int, "p_count", nc + 1);
+  VF_ALLOC(start, int, "p_start", nc + 1);
+  VF_ALLOC(order, int, "p_order", npp);
+  VF_ALLOC(spos, float4, "p_spos", npp);
+  VF_ALLOC(svel, float4, "p_svel", npp);
+  VF_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (nc + 1), ctx->stream));
+  if (np > 0) {
+    hash_count_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
+        (const ParticleRec*)particles, np, ni, nj, nk, h, cell, slot, count);
+    VF_LAUNCH_CHECK();
+  }
+  if ((rc = exclusive_scan(ctx, count, start, nc + 1))) return rc;
+  if (np > 0) {
+    scatter_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(cell, slot, start, order, np);
+    VF_LAUNCH_CHECK();
+    sort_buckets_kernel<<<grid_for(nc, 256, ctx->num_sms), 256, 0, ctx->stream>>>(start, order, (int)nc);
+    VF_LAUNCH_CHECK();
+    gather_sorted_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
+        (const ParticleRec*)particles, order, spos, svel, start + nc);
+    VF_LAUNCH_CHECK();
+  }
+  float* outs[3][2] = {{u, ucoef}, {v, vcoef}, {w, wcoef}};
+  for (int c = 0; c < 3; ++c) {
+    if (!outs[c][0]) continue;
+    size_t nf = (size_t)(ni + (c == 0)) * (nj + (c == 1)) * (nk + (c == 2));
+    p2g_kernel<<<grid_for(nf, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(start, spos, svel, outs[c][0],
+                                                                             outs[c][1], c, ni, nj, nk, h);
+    VF_LAUNCH_CHECK();
+  }
+  return VFLIP_OK;
+}
+
+int vflip_g2p(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np, const float* du,
+              const float* dv, const float* dw, const float* un, const float* vn, const float* wn,
+              double flip_ratio) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (np < 0 || (np > 0 && !particles) || !du || !dv || !dw) return ctx->fail(VFLIP_ERR_ARG, "bad argument");
+  if (flip_ratio != 1.0 && (!un || !vn || !wn)) return ctx->fail(VFLIP_ERR_ARG, "blend needs u_new/v_new/w_new");
+  if (np == 0) return VFLIP_OK;
+  GridView gdu{du, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0};
+  GridView gdv{dv, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0};
+  GridView gdw{dw, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5};
+  GridView gun{un ? un : du, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0};
+  GridView gvn{vn ? vn : dv, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0};
+  GridView gwn{wn ? wn : dw, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5};
+  g2p_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>((ParticleRec*)particles, np, gdu, gdv, gdw,
+                                                                       gun, gvn, gwn, flip_ratio);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+}  // extern "C"
+
+namespace {
+__global__ void bricks_kernel(const float* __restrict__ src, float* __restrict__ dst, int nx, int ny, int nz,
+                              bool to_linear) {
+  const int bx = (nx + 7) / 8, by = (ny + 7) / 8;
+  const size_t n = (size_t)nx * ny * nz;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    unsigned i = (unsigned)(e % nx), j = (unsigned)((e / nx) % ny), k = (unsigned)(e / ((size_t)nx * ny));
+    size_t b = ((size_t)((k >> 3) * bx * by + (j >> 3) * bx + (i >> 3)) << 9) + ((k & 7) << 6) + ((j & 7) << 3) +
+               (i & 7);
+    if (to_linear) dst[e] = src[b];
+    else dst[b] = src[e];
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int vflip_bricks_to_linear(vflip_ctx* ctx, int nx, int ny, int nz, const float* bricked, float* linear) {
+  int rc;
+  if ((rc = check_dims(ctx, nx, ny, nz))) return rc;
+  if (!bricked || !linear) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  size_t n = (size_t)nx * ny * nz;
+  bricks_kernel<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(bricked, linear, nx, ny, nz, true);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+int vflip_linear_to_bricks(vflip_ctx* ctx, int nx, int ny, int nz, const float* linear, float* bricked) {
+  int rc;
+  if ((rc = check_dims(ctx, nx, ny, nz))) return rc;
+  if (!bricked || !linear) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  size_t n = (size_t)nx * ny * nz;
+  bricks_kernel<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(linear, bricked, nx, ny, nz, false);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,259 @@
+"""Host-side mirror of the reference's solver call surface over the C ABI.
+
+``Solver`` owns one ``vflip_ctx`` (device buffers, PCG scalars, a stream:
+torch's current stream by default, so the library's kernels are ordered with
+the caller's torch work).  Methods take torch CUDA tensors and return
+torch CUDA tensors; ``amgpcg_solve_csr`` is the exact drop-in of
+``ivock::AMGPCGSolve`` and takes host (numpy) arrays like the reference.
+
+Status handling mirrors the reference: the solve returns the reference's bool
+(converged or not) plus residual and iteration count; argument and CUDA
+errors raise ``VflipError``.
+"""
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from ._lib import ConfigC, SolveStatsC, VflipError, load
+from .particles import PARTICLE_BYTES
+
+
+@dataclass
+class SolveStats:
+    iterations: int
+    vcycles: int
+    levels: int
+    converged: bool
+    residual: float
+    rhs_norm: float
+    solve_ms: float
+
+    @classmethod
+    def from_c(cls, s):
+        return cls(s.iterations, s.vcycles, s.levels, bool(s.converged), s.residual, s.rhs_norm, s.solve_ms)
+
+
+def _p(t):
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        return C.c_void_p(t.ctypes.data)
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _face_shapes(ni, nj, nk):
+    return (nk, nj, ni + 1), (nk, nj + 1, ni), (nk + 1, nj, ni)
+
+
+class Solver:
+    def __init__(self, precision=1, pre_sweeps=4, post_sweeps=4, coarse_sweeps=200, coarsest_max_unknowns=4096,
+                 device=0, stream=None):
+        self.lib = load()
+        cfg = ConfigC()
+        self.lib.vflip_config_default(C.byref(cfg))
+        cfg.precision = precision
+        cfg.pre_sweeps = pre_sweeps
+        cfg.post_sweeps = post_sweeps
+        cfg.coarse_sweeps = coarse_sweeps
+        cfg.coarsest_max_unknowns = coarsest_max_unknowns
+        cfg.device = device
+        self.device = torch.device("cuda", device)
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        self.stream = stream
+        cfg.stream = C.c_void_p(stream.cuda_stream)
+        ctx = C.c_void_p()
+        rc = self.lib.vflip_create(C.byref(ctx), C.byref(cfg))
+        if rc != 0:
+            raise VflipError(rc, "vflip_create failed")
+        self.ctx = ctx
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.vflip_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------- helpers
+    def _check(self, rc):
+        if rc < 0:
+            raise VflipError(rc, self.lib.vflip_last_error(self.ctx).decode())
+        return rc
+
+    def _empty(self, shape, dtype):
+        return torch.empty(shape, dtype=dtype, device=self.device)
+
+    def synchronize(self):
+        self._check(self.lib.vflip_synchronize(self.ctx))
+
+    @property
+    def last_ms(self):
+        return self.lib.vflip_last_ms(self.ctx)
+
+    # ------------------------------------------------------------- MGPCG
+    def amgpcg_solve_csr(self, rowstart, colindex, value, rhs, tolerance_factor, max_iterations, ni, nj, nk):
+        """Drop-in of ivock::AMGPCGSolve on host CSR arrays.  Returns
+        (success, result, residual_out, iterations_out)."""
+        rowstart = np.ascontiguousarray(rowstart, np.uint32)
+        colindex = np.ascontiguousarray(colindex, np.uint32)
+        value = np.ascontiguousarray(value, np.float64)
+        rhs = np.ascontiguousarray(rhs, np.float64).ravel()
+        result = np.zeros_like(rhs)
+        res = C.c_double(0.0)
+        it = C.c_int(0)
+        rc = self.lib.vflip_amgpcg_solve_csr(self.ctx, len(rhs), _p(rowstart), _p(colindex), _p(value), _p(rhs),
+                                            _p(result), float(tolerance_factor), int(max_iterations), C.byref(res),
+                                            C.byref(it), ni, nj, nk)
+        self._check(rc)
+        return rc == 0, result, res.value, it.value
+
+    def amgpcg_solve(self, stencil, rhs, tolerance_factor=1e-6, max_iterations=50, result=None):
+        """Solve A p = rhs for a (4, nk, nj, ni) float64 stencil (diag, xp,
+        yp, zp) on the device.  Returns (converged, result, SolveStats)."""
+        _, nk, nj, ni = stencil.shape
+        if result is None:
+            result = self._empty((nk, nj, ni), torch.float64)
+        st = SolveStatsC()
+        rc = self.lib.vflip_amgpcg_solve(self.ctx, ni, nj, nk, _p(stencil[0]), _p(stencil[1]), _p(stencil[2]),
+                                        _p(stencil[3]), _p(rhs), _p(result), float(tolerance_factor),
+                                        int(max_iterations), C.byref(st))
+        self._check(rc)
+        return rc == 0, result, SolveStats.from_c(st)
+
+    def build_levels(self, stencil, max_levels=16):
+        _, nk, nj, ni = stencil.shape
+        dims = np.zeros(3 * max_levels, np.int32)
+        total, a, b, c = 0, ni, nj, nk
+        for _ in range(max_levels):
+            total += 4 * a * b * c
+            a, b, c = (a + 1) // 2, (b + 1) // 2, (c + 1) // 2
+        out = self._empty((total,), torch.float64)
+        nl = self._check(self.lib.vflip_build_levels(self.ctx, ni, nj, nk, _p(stencil[0]), _p(stencil[1]),
+                                                     _p(stencil[2]), _p(stencil[3]), max_levels, _p(dims),
+                                                     _p(out)))
+        levels, off = [], 0
+        for l in range(nl):
+            x, y, z = (int(v) for v in dims[3 * l:3 * l + 3])
+            m = 4 * x * y * z
+            levels.append(out[off:off + m].view(4, z, y, x))
+            off += m
+        return levels
+
+    def rbgs(self, stencil, b, x, iterations):
+        """In-place red-black Gauss-Seidel on float64 x."""
+        _, nk, nj, ni = stencil.shape
+        self._check(self.lib.vflip_rbgs(self.ctx, ni, nj, nk, _p(stencil[0]), _p(stencil[1]), _p(stencil[2]),
+                                        _p(stencil[3]), _p(b), _p(x), int(iterations)))
+        return x
+
+    def vcycle(self, stencil, b):
+        _, nk, nj, ni = stencil.shape
+        x = self._empty((nk, nj, ni), torch.float64)
+        self._check(self.lib.vflip_vcycle(self.ctx, ni, nj, nk, _p(stencil[0]), _p(stencil[1]), _p(stencil[2]),
+                                          _p(stencil[3]), _p(b), _p(x)))
+        return x
+
+    # ------------------------------------------------------------- projection
+    def face_weights(self, ni, nj, nk, nodal_phi):
+        su, sv, sw = _face_shapes(ni, nj, nk)
+        uw, vw, ww = self._empty(su, torch.float32), self._empty(sv, torch.float32), self._empty(sw, torch.float32)
+        self._check(self.lib.vflip_face_weights(self.ctx, ni, nj, nk, _p(nodal_phi), _p(uw), _p(vw), _p(ww)))
+        return uw, vw, ww
+
+    def assemble(self, ni, nj, nk, h, U_in, nodal_phi, bdesc, us, vs, ws, u, v, w):
+        st = self._empty((4, nk, nj, ni), torch.float64)
+        rhs = self._empty((nk, nj, ni), torch.float64)
+        self._check(self.lib.vflip_assemble(self.ctx, ni, nj, nk, float(h), float(U_in), _p(nodal_phi), _p(bdesc),
+                                            _p(us), _p(vs), _p(ws), _p(u), _p(v), _p(w), _p(st[0]), _p(st[1]),
+                                            _p(st[2]), _p(st[3]), _p(rhs)))
+        return st, rhs
+
+    def project(self, ni, nj, nk, h, U_in, nodal_phi, bdesc, us, vs, ws, u, v, w, pressure=None,
+                tolerance_factor=1e-6, max_iterations=50):
+        """SmokeSolver3D::pcg_projection on device arrays; u/v/w updated in
+        place.  Returns (converged, pressure, SolveStats)."""
+        if pressure is None:
+            pressure = self._empty((nk, nj, ni), torch.float64)
+        st = SolveStatsC()
+        rc = self.lib.vflip_project(self.ctx, ni, nj, nk, float(h), float(U_in), _p(nodal_phi), _p(bdesc), _p(us),
+                                   _p(vs), _p(ws), _p(u), _p(v), _p(w), _p(pressure), float(tolerance_factor),
+                                   int(max_iterations), C.byref(st))
+        self._check(rc)
+        return rc == 0, pressure, SolveStats.from_c(st)
+
+    # ------------------------------------------------------------- advection
+    def advect_rk2_linear(self, ni, nj, nk, h, dt, u, v, w, field, offsets, out=None):
+        fnz, fny, fnx = field.shape
+        if out is None:
+            out = torch.empty_like(field)
+        self._check(self.lib.vflip_advect_rk2_linear(self.ctx, ni, nj, nk, float(h), float(dt), _p(u), _p(v), _p(w),
+                                                     fnx, fny, fnz, float(offsets[0]), float(offsets[1]),
+                                                     float(offsets[2]), _p(field), _p(out)))
+        return out
+
+    def delta(self, after, before, out=None):
+        if out is None:
+            out = torch.empty_like(after)
+        self._check(self.lib.vflip_delta(self.ctx, after.numel(), _p(after), _p(before), _p(out)))
+        return out
+
+    # ------------------------------------------------------------- FLIP
+    @staticmethod
+    def _np(particles):
+        nbytes = particles.numel() * particles.element_size()
+        if nbytes % PARTICLE_BYTES:
+            raise ValueError("particle buffer is not a whole number of 40-byte records")
+        return nbytes // PARTICLE_BYTES
+
+    def particle_cells(self, ni, nj, nk, h, particles):
+        n = self._np(particles)
+        out = self._empty((n,), torch.int32)
+        self._check(self.lib.vflip_particle_cells(self.ctx, ni, nj, nk, float(h), _p(particles), n, _p(out)))
+        return out
+
+    def particle_to_grid(self, ni, nj, nk, h, particles, components=(0, 1, 2)):
+        """Returns {comp: (field, coef)} on the u/v/w face grids."""
+        n = self._np(particles)
+        shapes = _face_shapes(ni, nj, nk)
+        outs = {c: (self._empty(shapes[c], torch.float32), self._empty(shapes[c], torch.float32)) for c in components}
+        ptrs = []
+        for c in range(3):
+            ptrs += [_p(outs[c][0]), _p(outs[c][1])] if c in outs else [None, None]
+        self._check(self.lib.vflip_p2g(self.ctx, ni, nj, nk, float(h), _p(particles), n, *ptrs))
+        return outs
+
+    def particle_from_grid(self, ni, nj, nk, h, particles, du, dv, dw, un=None, vn=None, wn=None, flip_ratio=1.0):
+        n = self._np(particles)
+        self._check(self.lib.vflip_g2p(self.ctx, ni, nj, nk, float(h), _p(particles), n, _p(du), _p(dv), _p(dw),
+                                       _p(un), _p(vn), _p(wn), float(flip_ratio)))
+        return particles
+
+    # ------------------------------------------------------------- layout
+    def bricks_to_linear(self, nx, ny, nz, bricked):
+        out = self._empty((nz, ny, nx), torch.float32)
+        self._check(self.lib.vflip_bricks_to_linear(self.ctx, nx, ny, nz, _p(bricked), _p(out)))
+        return out
+
+    def linear_to_bricks(self, nx, ny, nz, linear):
+        pad = lambda n: (n + 7) // 8 * 8  # noqa: E731
+        out = torch.zeros((pad(nz) * pad(ny) * pad(nx),), dtype=torch.float32, device=self.device)
+        self._check(self.lib.vflip_linear_to_bricks(self.ctx, nx, ny, nz, _p(linear), _p(out)))
+        return out
