@@ -1,0 +1,319 @@
+#!/usr/bin/env python3
+"""Benchmark of the vFLIP hot path on B200: steps/s of the 256^3 smoke plume.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--n 256]
+                    [--precision fp32|fp64|mixed] [--no-cpu-baseline]
+
+A step (the unit of the metric) is one smoke-plume step on a 256^3 MAC grid
+with the centred sphere obstacle and box walls: RK2 semi-Lagrangian
+trilinear advection of u, v, w, density and temperature, the density /
+temperature source and buoyancy, and the pressure projection with plain
+MGPCG (V(4,4) red-black Gauss-Seidel, Galerkin coarsening, 200 coarsest
+sweeps) to |r|_inf <= 1e-6 |rhs|_inf, i.e. SmokeSolver3D::pcg_projection's
+solve.  Synthetic seeded state; the grid fields (335 MB) are larger than L2,
+so no L2 flush is needed between steps.
+
+Multi-GPU: the path does not shard - every rank runs an independent replica
+on its own GPU ("replicas only", weak scaling); value is the sum of the
+replicas' steps/s (N * K / max-over-ranks time).
+
+--impl reference times the reference's own CPU code (oracle/_ref, compiled
+from the vFLIP sources: SubDomainSolver::advect_field + pcg_projection) on
+the same workload on this box's host cores; when that library is absent it
+times the oracle restatement (kind "port").
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "256³ steps/s @1e-6 residual, learned-precond vs plain MGPCG; % HBM roofline"
+PREC = {"fp64": 0, "fp32": 1, "mixed": 2}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="vflip", choices=["vflip", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--dt", type=float, default=0.01)
+    ap.add_argument("--precision", default="fp32", choices=sorted(PREC))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds for the reference arm's timed steps")
+    return ap.parse_args()
+
+
+def workload(a):
+    return (f"smoke plume {a.n}^3 MAC grid, sphere obstacle r=0.15 + 5 solid walls, source sphere r=0.1 at "
+            f"(0.5,0.1,0.5); step = RK2 trilinear advection of u,v,w,rho,T + sources/buoyancy + MGPCG "
+            f"projection to 1e-6 (plain V(4,4) RBGS preconditioner)")
+
+
+def config(a, n_gpus):
+    return {"workload": workload(a), "grid": a.n, "dt": a.dt, "precision": a.precision,
+            "tolerance": 1e-6, "parallelism": f"replicas x{n_gpus}",
+            "l2": "inputs larger than L2 (5 fields x 64 MB + solver vectors), no flush"}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(n):
+    """DRAM bytes per launch of the fine-level sweep from the committed ncu
+    summary (profiles/rbgs_sweep_fp32_256.md), scaled to n^3 cells."""
+    p = os.path.join(ROOT, "profiles", "rbgs_sweep_fp32_256.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_launch:"):
+            b = float(line.split(":")[1].split()[0])
+            return b * (n / 256.0) ** 3
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.path = os.path.join("/tmp", f"vflip_clocks_{os.getpid()}.csv")
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={gpu_id}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[4:8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for _, _, r in rows for q in range(4) if r[q].lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def run_vflip(a):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from vflip_b200.plume import PlumeParams, PlumeSim
+    from vflip_b200.solver import Solver
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    solver = Solver(precision=PREC[a.precision], device=local)
+    params = PlumeParams(n=a.n, dt=a.dt)
+    sim = PlumeSim(solver, params)
+    for _ in range(a.warmup):
+        sim.step()
+    torch.cuda.synchronize()
+
+    props = torch.cuda.get_device_properties(local)
+    clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local))
+    time.sleep(0.3)
+    iters, vcycles, resid = [], [], []
+    solver.set_profiling(True)
+    launches0 = solver.launch_count
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        conv, st = sim.step()
+        iters.append(st.iterations)
+        vcycles.append(st.vcycles)
+        resid.append(st.residual / max(st.rhs_norm, 1e-300))
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    launches = solver.launch_count - launches0
+    n_sweeps, sweep_ms, cells = solver.profile_sweeps()
+    solver.set_profiling(False)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(ms)
+
+    # end to end through the public API with host-resident state
+    host = {k: torch.empty(sim.shapes[k], dtype=torch.float32, pin_memory=True) for k in sim.FIELDS}
+    for k in sim.FIELDS:
+        host[k].copy_(sim.f[k])
+    torch.cuda.synchronize()
+    barrier()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record()
+    for _ in range(a.steps):
+        sim.step_host(host)
+    e3.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e2.elapsed_time(e3))
+
+    out = None
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        avg_sweep_ms = sweep_ms / max(n_sweeps, 1)
+        alg_bytes = 7 * 4 * cells  # x_in, b, diag, xp, yp, zp read + x_out written, FP32
+        achieved = alg_bytes / (avg_sweep_ms * 1e-3) / 1e9 if n_sweeps else None
+        traffic = profile_traffic(a.n)
+        out = {
+            "metric": METRIC, "value": world * a.steps / (ms_max * 1e-3), "unit": "steps/s", "n_gpus": world,
+            "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32" if a.precision != "fp64" else "fp64",
+            "data": "synthetic (seeded plume scene, state evolved by the warm-up steps)",
+            "config": config(a, world),
+            "cells_steps_per_s": world * a.steps * a.n ** 3 / (ms_max * 1e-3),
+            "solver": {"pcg_iterations_mean": float(np.mean(iters)), "vcycles_mean": float(np.mean(vcycles)),
+                       "rel_residual_max": float(np.max(resid)), "levels": sim.last.levels},
+            "roofline": {"bound": "hbm", "kernel": "rbgs_sweep_kernel<float,float> (fine level)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_sweep_ms,
+                         "launches_timed": n_sweeps, "peak_kind": peak_kind},
+            "e2e": {"value": world * a.steps / (e2e_ms * 1e-3), "unit": "steps/s",
+                    "h2d_bytes_per_step": sim.host_bytes(), "d2h_bytes_per_step": sim.host_bytes()},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        if not a.no_cpu_baseline and world == 1:
+            out["cpu_baseline"] = cpu_baseline(a, {k: sim.f[k].cpu().numpy().copy() for k in sim.FIELDS}, params)
+    solver.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return out
+
+
+def _cpu_impl():
+    import oracle
+
+    r = oracle.reference()
+    if r is not None:
+        return r, "reference"
+    return oracle.oracle(), "port"
+
+
+def cpu_baseline(a, state, params):
+    """One reference plume step on this state (bounded: a single step)."""
+    import numpy as np
+
+    from vflip_b200.plume import nodal_phi
+
+    impl, kind = _cpu_impl()
+    phi = nodal_phi(params)
+    st = {k: np.ascontiguousarray(v) for k, v in state.items()}
+    t0 = time.time()
+    r = impl.smoke_step(a.n, params.h, params.dt, phi, st)
+    wall = time.time() - t0
+    secs = r[0] if kind == "reference" else wall
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())) if kind == "reference" else 1
+    return {"value": 1.0 / secs, "unit": "steps/s", "cores": cores, "kind": kind,
+            "sample": f"one full {a.n}^3 plume step from the GPU run's state (reference advect_field x5 + "
+                      f"pcg_projection; {secs:.1f} s in reference code, {wall:.1f} s wall)"}
+
+
+def run_reference(a):
+    import numpy as np
+
+    from vflip_b200 import scenes
+    from vflip_b200.plume import PlumeParams, nodal_phi
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    impl, kind = _cpu_impl()
+    params = PlumeParams(n=a.n, dt=a.dt)
+    n = a.n
+    su, sv, sw = scenes.face_shapes(n, n, n)
+    st = {k: np.zeros(s, np.float32) for k, s in zip(("u", "v", "w", "rho", "temp"), (su, sv, sw, (n, n, n),
+                                                                                     (n, n, n)))}
+    phi = nodal_phi(params)
+
+    def one():
+        t0 = time.time()
+        r = impl.smoke_step(n, params.h, params.dt, phi, st)
+        wall = time.time() - t0
+        return (r[0] if kind == "reference" else wall), wall
+
+    warm = []
+    for _ in range(max(1, min(a.warmup, 1))):  # one warm-up step: the reference is slow
+        warm.append(one()[0])
+    per = warm[-1]
+    k = max(1, min(a.steps, int(a.cpu_budget // max(per, 1e-3))))
+    times = [one()[0] for _ in range(k)]
+    tot = sum(times)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count())) if kind == "reference" else 1
+    value = k / tot
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": a.gpus,
+            "steps": k, "warmup": len(warm), "ms_per_step": 1e3 * tot / k, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp64+fp32 (reference: FP32 fields, FP64 solve)",
+            "data": "synthetic (seeded plume scene)", "config": config(a, 1),
+            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": cores, "kind": kind,
+                             "sample": f"{k} full {n}^3 plume steps from rest after {len(warm)} warm-up step(s) "
+                                       f"(steps requested {a.steps}, bounded to ~{a.cpu_budget:.0f} s)"},
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    a = parse()
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    out = run_reference(a) if a.impl == "reference" else run_vflip(a)
+    if out is not None:
+        print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

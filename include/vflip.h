@@ -12,7 +12,7 @@
  *
  * Memory: unless a parameter is documented as a host pointer, pointers are
  * device pointers on the context's device, and the call is ordered on the
- * context's stream (vflip_config.stream, or a stream the context creates).
+ * context's stream (vflip_config.stream; NULL is the CUDA default stream).
  * Entry points that return solver statistics synchronise that stream.
  *
  * Grids are dense and linear, index = i + ni*(j + nj*k) (i fastest), the
@@ -62,7 +62,7 @@ typedef struct {
   int coarse_sweeps;         /* RBGS sweeps on the coarsest level, default 200 (SS/AlgebraicMultigrid.h:160) */
   int coarsest_max_unknowns; /* coarsen while unknowns exceed this, default 4096 (SS/GeometricLevelGen.h:46); max 4096 */
   int device;                /* CUDA device ordinal, default 0 */
-  void* stream;              /* cudaStream_t to order work on; NULL: the context creates one */
+  void* stream;              /* cudaStream_t to order work on; NULL: the CUDA default stream */
 } vflip_config;
 
 typedef struct {
@@ -196,6 +196,30 @@ int vflip_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* parti
 int vflip_g2p(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np, const float* du,
               const float* dv, const float* dw, const float* un, const float* vn, const float* wn,
               double flip_ratio);
+
+/* ---- measurement ----------------------------------------------------------- */
+
+/* When enabled, every launch of the fine-level smoothing sweep (the
+ * dominant kernel) is bracketed by a pair of CUDA events on the context
+ * stream.  vflip_profile_sweeps synchronises the stream and returns the
+ * number of timed launches, their summed device time and the fine level's
+ * cell count, then starts a new count.  No reference counterpart. */
+int vflip_set_profiling(vflip_ctx* ctx, int enable);
+int vflip_profile_sweeps(vflip_ctx* ctx, int* launches, double* total_ms, double* cells);
+/* Number of kernels launched through this context so far. */
+unsigned long long vflip_launch_count(const vflip_ctx* ctx);
+
+/* ---- plume scenes ---------------------------------------------------------- */
+
+/* Grid analogue of the reference's smoke sources (SS/Smoke_solver3D.cpp:
+ * 1624-1668, which act on particles and 2x density/temperature grids): sets
+ * rho = dens_value and temp = heat_value in the cells whose centre (i,j,k)*h
+ * lies in the sphere (cx,cy,cz, radius), then adds
+ * dt * (-alpha * rho + beta * temp), averaged over the two adjacent cells, to
+ * every interior v face.  No reference counterpart on the grid path. */
+int vflip_plume_sources(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, float* rho, float* temp, float* v,
+                        float cx, float cy, float cz, float radius, float dens_value, float heat_value, float alpha,
+                        float beta);
 
 /* ---- layout --------------------------------------------------------------- */
 

@@ -64,6 +64,8 @@ def _load(path, prefix):
         getattr(lib, p + "_vcycle").argtypes = [_I, _I, _I, _P, _P, _P, _P, _P]
         getattr(lib, p + "_amgpcg").argtypes = [_I, _I, _I, _P, _P, _P, _P, _P, _D, _I, _P, _P]
         getattr(lib, p + "_delta").argtypes = [_I, _I, _I, _P, _P, _P]
+    getattr(lib, p + "_smoke_step").argtypes = [_I, _F, _F, _P, _P, _P, _P, _P, _P, _F, _F, _F, _F, _F, _F, _P, _P]
+    getattr(lib, p + "_smoke_step").restype = C.c_double if prefix == "ref" else C.c_int
     getattr(lib, p + "_fraction_inside4").argtypes = [_I, _P, _P, _P, _P, _P]
     getattr(lib, p + "_face_weights").argtypes = [_I, _I, _I, _F, _P, _P, _P, _P]
     getattr(lib, p + "_project").argtypes = [_I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
@@ -244,6 +246,22 @@ class _Impl:
                 raise ValueError("the reference's particle_from_grid is pure FLIP")
             self.fn("g2p")(ni, nj, nk, h, _ptr(p), len(p), _ptr(du), _ptr(dv), _ptr(dw))
         return p
+
+    def smoke_step(self, n, h, dt, phi, state, source_centre=(0.5, 0.1, 0.5), source_radius=0.1, alpha=0.1,
+                   beta=1.0):
+        """One grid plume step on numpy state {u, v, w, rho, temp} (updated in
+        place).  Returns the library's return value: the solver's bool for
+        the oracle, the seconds spent in reference code for the reference."""
+        phi = np.ascontiguousarray(phi, np.float32)
+        for k in ("u", "v", "w", "rho", "temp"):
+            assert state[k].dtype == np.float32 and state[k].flags.c_contiguous
+        it = C.c_int(0)
+        res = C.c_double(0)
+        r = self.fn("smoke_step")(n, float(h), float(dt), _ptr(phi), _ptr(state["u"]), _ptr(state["v"]),
+                                  _ptr(state["w"]), _ptr(state["rho"]), _ptr(state["temp"]),
+                                  float(source_centre[0]), float(source_centre[1]), float(source_centre[2]),
+                                  float(source_radius), float(alpha), float(beta), C.byref(it), C.byref(res))
+        return r, it.value, res.value
 
     def delta(self, after, before):
         after, before = [np.ascontiguousarray(a, np.float32) for a in (after, before)]

@@ -15,7 +15,10 @@
 //   cell  ni*nj*nk            u  (ni+1)*nj*nk
 //   v     ni*(nj+1)*nk        w  ni*nj*(nk+1)
 //   nodal (ni+1)*(nj+1)*(nk+1)
+#include <omp.h>
+
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include "AlgebraicMultigrid.h"
@@ -371,4 +374,102 @@ void ref_delta(int nx, int ny, int nz, const float* after, const float* before, 
 }
 
 int ref_particle_size() { return (int)sizeof(particle); }
+
+// Density/temperature source sphere and v-face buoyancy of the grid plume.
+// Not reference code (the reference's sources act on particles, see
+// vflip_plume_sources in include/vflip.h); the same float arithmetic as the
+// CUDA kernel and the oracle, applied between the reference's advection and
+// its projection.
+static void plume_sources_linear(int n, float h, float dt, float* rho, float* temp, float* v, float cx, float cy,
+                                 float cz, float radius, float alpha, float beta) {
+  const float r2 = radius * radius;
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        float dx = i * h - cx, dy = j * h - cy, dz = k * h - cz;
+        if (dx * dx + dy * dy + dz * dz <= r2) {
+          rho[lin(i, j, k, n, n)] = 1.0f;
+          temp[lin(i, j, k, n, n)] = 1.0f;
+        }
+      }
+  for (int k = 0; k < n; ++k)
+    for (int j = 1; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        size_t c0 = lin(i, j - 1, k, n, n), c1 = lin(i, j, k, n, n);
+        float r = 0.5f * (rho[c0] + rho[c1]);
+        float t = 0.5f * (temp[c0] + temp[c1]);
+        size_t e = lin(i, j, k, n, n + 1);
+        v[e] = v[e] + dt * (-alpha * r + beta * t);
+      }
+}
+
+// One grid smoke-plume step on the reference's own code: RK2 trilinear
+// advection of u, v, w, rho, temp (SubDomainSolver::advect_field,
+// sub_domain.cpp:191-235), the plume sources, then
+// SmokeSolver3D::pcg_projection (Smoke_solver3D.cpp:945-1202) with no
+// inflow and resting solids.  Fields are updated in place.  Returns the wall
+// seconds spent inside the reference's advect_field and pcg_projection calls
+// (set-up and layout conversion of this harness excluded); iterations and
+// residual of the solve through the pointers.
+double ref_smoke_step(int n, float h, float dt, const float* nodal_phi, float* u, float* v, float* w, float* rho,
+                      float* temp, float cx, float cy, float cz, float radius, float alpha, float beta,
+                      int* iterations_out, double* residual_out) {
+  double secs = 0.0;
+  size_t nc = (size_t)n * n * n, nu = (size_t)(n + 1) * n * n;
+  std::vector<float> u2(nu), v2(nu), w2(nu), rho2(nc), temp2(nc);
+  {
+    SubDomainSolver* sd = new SubDomainSolver();
+    quiet_subdomain(*sd);
+    sd->_nx = n; sd->_ny = n; sd->_nz = n;
+    sd->_hx = sd->_hy = sd->_hz = h;
+    sd->_un.init(n + 1, n, n, h, 0.5, 0, 0);
+    sd->_vn.init(n, n + 1, n, h, 0.0, 0.5, 0.0);
+    sd->_wn.init(n, n, n + 1, h, 0.0, 0.0, 0.5);
+    to_buffer(sd->_un, u);
+    to_buffer(sd->_vn, v);
+    to_buffer(sd->_wn, w);
+    struct F { const float* in; float* out; int nx, ny, nz; double ox, oy, oz; };
+    F fs[5] = {{u, u2.data(), n + 1, n, n, 0.5, 0, 0}, {v, v2.data(), n, n + 1, n, 0, 0.5, 0},
+               {w, w2.data(), n, n, n + 1, 0, 0, 0.5}, {rho, rho2.data(), n, n, n, 0, 0, 0},
+               {temp, temp2.data(), n, n, n, 0, 0, 0}};
+    for (auto& f : fs) {
+      buffer3Df a, b;
+      a.init(f.nx, f.ny, f.nz, h, f.ox, f.oy, f.oz);
+      b.init(f.nx, f.ny, f.nz, h, f.ox, f.oy, f.oz);
+      to_buffer(a, f.in);
+      double t0 = omp_get_wtime();
+      sd->advect_field(dt, a, b);
+      secs += omp_get_wtime() - t0;
+      from_buffer(b, f.out);
+      a.free(); b.free();
+    }
+    sd->_un.free(); sd->_vn.free(); sd->_wn.free();
+    delete sd;
+  }
+  std::memcpy(u, u2.data(), 4 * nu);
+  std::memcpy(v, v2.data(), 4 * nu);
+  std::memcpy(w, w2.data(), 4 * nu);
+  std::memcpy(rho, rho2.data(), 4 * nc);
+  std::memcpy(temp, temp2.data(), 4 * nc);
+  plume_sources_linear(n, h, dt, rho, temp, v, cx, cy, cz, radius, alpha, beta);
+  SmokeSolver3D s;
+  init_solver_grids(s, n, n, n, h);
+  s._U_in = 0.0f;
+  to_buffer(s._nodal_solid_phi, nodal_phi);
+  to_buffer(s._un, u);
+  to_buffer(s._vn, v);
+  to_buffer(s._wn, w);
+  double t0 = omp_get_wtime();
+  s.pcg_projection(1.0f);
+  secs += omp_get_wtime() - t0;
+  from_buffer(s._un, u);
+  from_buffer(s._vn, v);
+  from_buffer(s._wn, w);
+  if (iterations_out || residual_out) {
+    // pcg_projection prints but does not return its statistics
+    if (iterations_out) *iterations_out = -1;
+    if (residual_out) *residual_out = -1.0;
+  }
+  return secs;
+}
 }

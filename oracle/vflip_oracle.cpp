@@ -707,4 +707,49 @@ void oracle_delta(int nx, int ny, int nz, const float* after, const float* befor
 }
 
 int oracle_particle_size() { return (int)sizeof(Particle); }
+
+// The grid smoke-plume step (vflip_b200/plume.py): RK2 advection of the five
+// fields (SubDomainSolver::advect_field), the plume sources (this project's
+// grid analogue of SS/Smoke_solver3D.cpp:1624-1668), pcg_projection with no
+// inflow and resting solids.  Fields are updated in place; returns the
+// solver's bool.
+int oracle_smoke_step(int n, float h, float dt, const float* phi, float* u, float* v, float* w, float* rho,
+                      float* temp, float cx, float cy, float cz, float radius, float alpha, float beta,
+                      int* iterations_out, double* residual_out) {
+  size_t nc = (size_t)n * n * n, nu = (size_t)(n + 1) * n * n;
+  std::vector<float> u2(nu), v2(nu), w2(nu), rho2(nc), temp2(nc);
+  oracle_advect_rk2(n, n, n, h, dt, u, v, w, n + 1, n, n, 0.5, 0, 0, u, u2.data());
+  oracle_advect_rk2(n, n, n, h, dt, u, v, w, n, n + 1, n, 0, 0.5, 0, v, v2.data());
+  oracle_advect_rk2(n, n, n, h, dt, u, v, w, n, n, n + 1, 0, 0, 0.5, w, w2.data());
+  oracle_advect_rk2(n, n, n, h, dt, u, v, w, n, n, n, 0, 0, 0, rho, rho2.data());
+  oracle_advect_rk2(n, n, n, h, dt, u, v, w, n, n, n, 0, 0, 0, temp, temp2.data());
+  std::memcpy(u, u2.data(), 4 * nu);
+  std::memcpy(v, v2.data(), 4 * nu);
+  std::memcpy(w, w2.data(), 4 * nu);
+  std::memcpy(rho, rho2.data(), 4 * nc);
+  std::memcpy(temp, temp2.data(), 4 * nc);
+  const float r2 = radius * radius;
+  for (int k = 0; k < n; ++k)
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        float dx = i * h - cx, dy = j * h - cy, dz = k * h - cz;
+        if (dx * dx + dy * dy + dz * dz <= r2) {
+          rho[lin(i, j, k, n, n)] = 1.0f;
+          temp[lin(i, j, k, n, n)] = 1.0f;
+        }
+      }
+  for (int k = 0; k < n; ++k)
+    for (int j = 1; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        size_t c0 = lin(i, j - 1, k, n, n), c1 = lin(i, j, k, n, n);
+        float r = 0.5f * (rho[c0] + rho[c1]);
+        float t = 0.5f * (temp[c0] + temp[c1]);
+        size_t e = lin(i, j, k, n, n + 1);
+        v[e] = v[e] + dt * (-alpha * r + beta * t);
+      }
+  std::vector<int8_t> bdesc(nc, 0);
+  std::vector<float> zu(nu, 0.0f);
+  return oracle_project(n, n, n, h, 0.0f, phi, bdesc.data(), zu.data(), zu.data(), zu.data(), u, v, w, nullptr,
+                        nullptr, nullptr, nullptr, nullptr, nullptr, iterations_out, residual_out);
+}
 }

@@ -150,3 +150,20 @@ def test_pcg_failure_modes_vs_reference(orc, ref):
     a, b = ref.amgpcg(st, rhs, 1e-14, 2), orc.amgpcg(st, rhs, 1e-14, 2)
     same(a[0], b[0])
     assert (a[1], a[2], a[3]) == (b[1], b[2], b[3]) and a[1] is False and a[3] == 2
+
+
+def test_smoke_step_vs_reference(orc, ref):
+    from vflip_b200.plume import PlumeParams, nodal_phi
+
+    p = PlumeParams(n=20, dt=0.02)
+    phi = nodal_phi(p)
+    from vflip_b200 import scenes
+
+    su, sv, sw = scenes.face_shapes(20, 20, 20)
+    a = {k: np.zeros(s, np.float32) for k, s in zip(("u", "v", "w", "rho", "temp"), (su, sv, sw, (20,) * 3, (20,) * 3))}
+    b = {k: v.copy() for k, v in a.items()}
+    for _ in range(3):
+        ref.smoke_step(20, p.h, p.dt, phi, a)
+        orc.smoke_step(20, p.h, p.dt, phi, b)
+    for k in a:
+        same(a[k], b[k])

@@ -54,6 +54,10 @@ SIGNATURES = {
     "vflip_particle_cells": (_I, [_P, _I, _I, _I, _F, _P, _I, _P]),
     "vflip_p2g": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _P, _P]),
     "vflip_g2p": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _P, _P, _D]),
+    "vflip_set_profiling": (_I, [_P, _I]),
+    "vflip_profile_sweeps": (_I, [_P, C.POINTER(_I), C.POINTER(_D), C.POINTER(_D)]),
+    "vflip_launch_count": (C.c_ulonglong, [_P]),
+    "vflip_plume_sources": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _F, _F, _F, _F, _F, _F, _F, _F]),
     "vflip_bricks_to_linear": (_I, [_P, _I, _I, _I, _P, _P]),
     "vflip_linear_to_bricks": (_I, [_P, _I, _I, _I, _P, _P]),
 }

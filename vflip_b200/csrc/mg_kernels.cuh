@@ -283,7 +283,10 @@ __global__ void prolong_add_kernel(V* __restrict__ xf, const VC* __restrict__ xc
 // Coarsest level: `sweeps` red-black sweeps from x = 0 (AlgebraicMultigrid.h:
 // 159-160, 200 sweeps), the whole level resident in shared memory of one
 // CTA.  Up to 4096 unknowns (the coarsening stops at <= 16^3,
-// GeometricLevelGen.h:46), six arrays of Acc.
+// GeometricLevelGen.h:46), six arrays of Acc.  Each thread owns the cells
+// tid, tid+BLOCK, ... and decodes their coordinates, colour and neighbour
+// set once, so a colour phase is a handful of shared-memory loads per cell
+// and one barrier.
 template <typename S, typename V, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) coarsest_rbgs_kernel(const V* __restrict__ b, const S* __restrict__ diag,
                                                              const S* __restrict__ xp, const S* __restrict__ yp,
@@ -291,6 +294,7 @@ __global__ void __launch_bounds__(BLOCK) coarsest_rbgs_kernel(const V* __restric
                                                              int ni, int nj, int nk, int sweeps,
                                                              double* dot_out) {
   using A = typename Num<V>::Acc;
+  constexpr int kMaxOwn = 4096 / BLOCK;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n = ni * nj * nk;
   A* xs = reinterpret_cast<A*>(smem_raw);
@@ -308,22 +312,40 @@ __global__ void __launch_bounds__(BLOCK) coarsest_rbgs_kernel(const V* __restric
     yps[e] = A(ldg(yp + e));
     zps[e] = A(ldg(zp + e));
   }
-  __syncthreads();
   const int sy = ni, sz = ni * nj;
+  // owned cells: index, colour and which of the six neighbours exist
+  int own[kMaxOwn];
+  int colour[kMaxOwn];
+  int mask[kMaxOwn];
+#pragma unroll
+  for (int m = 0; m < kMaxOwn; ++m) {
+    int e = threadIdx.x + m * BLOCK;
+    own[m] = e;
+    colour[m] = -1;
+    mask[m] = 0;
+    if (e < n) {
+      int i = e % ni, j = (e / ni) % nj, k = e / sz;
+      colour[m] = (i + j + k) & 1;
+      mask[m] = (k > 0) | ((j > 0) << 1) | ((i > 0) << 2) | ((i < ni - 1) << 3) | ((j < nj - 1) << 4) |
+                ((k < nk - 1) << 5);
+    }
+  }
+  __syncthreads();
   for (int it = 0; it < sweeps; ++it) {
+#pragma unroll
     for (int parity = 1; parity >= 0; --parity) {
-      for (int e = threadIdx.x; e < n; e += BLOCK) {
-        int i = e % ni;
-        int j = (e / ni) % nj;
-        int k = e / sz;
-        if (((i + j + k) & 1) != parity) continue;
+#pragma unroll
+      for (int m = 0; m < kMaxOwn; ++m) {
+        if (colour[m] != parity) continue;
+        const int e = own[m];
+        const int f = mask[m];
         A sum = A(0);
-        if (k > 0) sum = sum + zps[e - sz] * xs[e - sz];
-        if (j > 0) sum = sum + yps[e - sy] * xs[e - sy];
-        if (i > 0) sum = sum + xps[e - 1] * xs[e - 1];
-        if (i < ni - 1) sum = sum + xps[e] * xs[e + 1];
-        if (j < nj - 1) sum = sum + yps[e] * xs[e + sy];
-        if (k < nk - 1) sum = sum + zps[e] * xs[e + sz];
+        if (f & 1) sum = sum + zps[e - sz] * xs[e - sz];
+        if (f & 2) sum = sum + yps[e - sy] * xs[e - sy];
+        if (f & 4) sum = sum + xps[e - 1] * xs[e - 1];
+        if (f & 8) sum = sum + xps[e] * xs[e + 1];
+        if (f & 16) sum = sum + yps[e] * xs[e + sy];
+        if (f & 32) sum = sum + zps[e] * xs[e + sz];
         A d = ds[e];
         xs[e] = (d != A(0)) ? (bs[e] - sum) / d : A(0);
       }

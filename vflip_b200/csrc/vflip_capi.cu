@@ -21,6 +21,7 @@
 #include "common.cuh"
 #include "mg_kernels.cuh"
 #include "pcg_kernels.cuh"
+#include "plume_kernels.cuh"
 #include "projection_kernels.cuh"
 #include "transfer_kernels.cuh"
 
@@ -43,7 +44,6 @@ struct Dims {
 struct vflip_ctx {
   vflip_config cfg;
   cudaStream_t stream = nullptr;
-  bool own_stream = false;
   std::string err;
   std::unordered_map<std::string, std::pair<void*, size_t>> bufs;
   PcgScalars* st = nullptr;         // device
@@ -52,6 +52,12 @@ struct vflip_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0.0;
   int num_sms = 148;
+  unsigned long long launches = 0;  // kernels launched through this context
+  // fine-level sweep timing (vflip_set_profiling)
+  bool profiling = false;
+  size_t prof_fine_n = 0;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+  size_t prof_used = 0;
 
   int fail(int code, const char* fmt, ...) {
     char buf[512];
@@ -86,6 +92,7 @@ struct vflip_ctx {
 
 #define VF_LAUNCH_CHECK()                                                                      \
   do {                                                                                        \
+    ++ctx->launches;                                                                          \
     cudaError_t e_ = cudaGetLastError();                                                      \
     if (e_ != cudaSuccess) return ctx->fail(VFLIP_ERR_CUDA, "launch: %s", cudaGetErrorString(e_)); \
   } while (0)
@@ -164,8 +171,22 @@ int launch_sweep_t(vflip_ctx* ctx, const SweepArgs<S, V>& a, const SweepShape& s
     attr_set = true;
   }
   dim3 grid(sh.grid_y, sh.grid_z);
+  const bool timed = ctx->profiling && (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n;
+  if (timed) {
+    if (ctx->prof_used == ctx->prof_events.size()) {
+      cudaEvent_t e0, e1;
+      VF_CUDA(cudaEventCreate(&e0));
+      VF_CUDA(cudaEventCreate(&e1));
+      ctx->prof_events.push_back({e0, e1});
+    }
+    VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].first, ctx->stream));
+  }
   kern<<<grid, kSweepBlock, sh.smem, ctx->stream>>>(a);
   VF_LAUNCH_CHECK();
+  if (timed) {
+    VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].second, ctx->stream));
+    ++ctx->prof_used;
+  }
   return VFLIP_OK;
 }
 
@@ -465,6 +486,7 @@ int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* re
   double residual = h.res;
   auto finish = [&](int st_code) -> int {
     to_double_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(x, result, n);
+    ++ctx->launches;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return ctx->fail(VFLIP_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
     if (stats) {
@@ -536,6 +558,7 @@ int solve_stencil(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, co
   if (!diag || !xp || !yp || !zp || !rhs || !result) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
   if (maxit < 0) return ctx->fail(VFLIP_ERR_ARG, "max_iterations < 0");
   VF_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  ctx->prof_fine_n = (size_t)ni * nj * nk;
   Hierarchy64 H;
   if ((rc = build_hierarchy64(ctx, ni, nj, nk, diag, xp, yp, zp, H))) return rc;
   int status;
@@ -603,12 +626,9 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
     return bad(VFLIP_ERR_ARG);
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);
-  if (ctx->cfg.stream) {
-    ctx->stream = (cudaStream_t)ctx->cfg.stream;
-  } else {
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
-    ctx->own_stream = true;
-  }
+  // NULL selects the CUDA default stream, so work is ordered with whatever
+  // the caller ran on it (e.g. torch's default stream)
+  ctx->stream = (cudaStream_t)ctx->cfg.stream;
   if (cudaMalloc(&ctx->st, sizeof(PcgScalars)) != cudaSuccess) return bad(VFLIP_ERR_NOMEM);
   if (cudaMalloc(&ctx->partials, sizeof(double) * kMaxPartials) != cudaSuccess) return bad(VFLIP_ERR_NOMEM);
   if (cudaMallocHost(&ctx->st_host, sizeof(PcgScalars)) != cudaSuccess) return bad(VFLIP_ERR_NOMEM);
@@ -625,9 +645,12 @@ int vflip_destroy(vflip_ctx* ctx) {
   if (ctx->st) cudaFree(ctx->st);
   if (ctx->partials) cudaFree(ctx->partials);
   if (ctx->st_host) cudaFreeHost(ctx->st_host);
+  for (auto& pe : ctx->prof_events) {
+    cudaEventDestroy(pe.first);
+    cudaEventDestroy(pe.second);
+  }
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
-  if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return VFLIP_OK;
 }
@@ -860,6 +883,7 @@ int vflip_project(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, c
   float* wts = (float*)ctx->buf("face_weights", sizeof(float) * (nu + nv + nw));
   gradient_kernel<double><<<grid_for(nu + nv + nw, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
       p, u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, h, ni, nj, nk);
+  ++ctx->launches;
   cudaError_t le = cudaGetLastError();
   if (le != cudaSuccess) {
     cudaEventDestroy(e0);
@@ -1054,5 +1078,53 @@ int vflip_linear_to_bricks(vflip_ctx* ctx, int nx, int ny, int nz, const float* 
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
 }
+
+}  // extern "C"
+
+extern "C" {
+
+int vflip_plume_sources(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, float* rho, float* temp, float* v,
+                        float cx, float cy, float cz, float radius, float dens_value, float heat_value, float alpha,
+                        float beta) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (!rho || !temp || !v) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  size_t nc = (size_t)ni * nj * nk, nv = (size_t)ni * (nj + 1) * nk;
+  plume_sources_kernel<<<grid_for(nc, 256, ctx->num_sms), 256, 0, ctx->stream>>>(rho, temp, ni, nj, nk, h, cx, cy, cz,
+                                                                                radius, dens_value, heat_value);
+  VF_LAUNCH_CHECK();
+  buoyancy_kernel<<<grid_for(nv, 256, ctx->num_sms), 256, 0, ctx->stream>>>(rho, temp, v, ni, nj, nk, dt, alpha, beta);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int vflip_set_profiling(vflip_ctx* ctx, int enable) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  ctx->profiling = enable != 0;
+  ctx->prof_used = 0;
+  return VFLIP_OK;
+}
+
+int vflip_profile_sweeps(vflip_ctx* ctx, int* launches, double* total_ms, double* cells) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  double tot = 0.0;
+  for (size_t q = 0; q < ctx->prof_used; ++q) {
+    float ms = 0.0f;
+    VF_CUDA(cudaEventElapsedTime(&ms, ctx->prof_events[q].first, ctx->prof_events[q].second));
+    tot += ms;
+  }
+  if (launches) *launches = (int)ctx->prof_used;
+  if (total_ms) *total_ms = tot;
+  if (cells) *cells = (double)ctx->prof_fine_n;
+  ctx->prof_used = 0;
+  return VFLIP_OK;
+}
+
+unsigned long long vflip_launch_count(const vflip_ctx* ctx) { return ctx ? ctx->launches : 0ull; }
 
 }  // extern "C"

@@ -1,0 +1,103 @@
+"""Grid smoke-plume stepper built from the library's kernels.
+
+One step (the unit of the benchmark) is what SURVEY-scale configs call a
+smoke step:
+  1. RK2 semi-Lagrangian trilinear advection of u, v, w, density and
+     temperature through the current velocity
+     (SubDomainSolver::advect_field, sub_domain.cpp:191-235);
+  2. density/temperature source sphere and buoyancy on the v faces (grid
+     analogue of gen_heat / add_smokeforce, Smoke_solver3D.cpp:1624-1668);
+  3. pressure projection with MGPCG to the tolerance
+     (SmokeSolver3D::pcg_projection, Smoke_solver3D.cpp:945-1202).
+
+Solids are the five box walls (open top) and optionally the centred sphere
+obstacle, as a nodal level set.
+"""
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import scenes
+
+
+@dataclass
+class PlumeParams:
+    n: int
+    dt: float = 0.01
+    obstacle: bool = True
+    obstacle_centre: tuple = (0.5, 0.5, 0.5)
+    obstacle_radius: float = 0.15
+    source_centre: tuple = (0.5, 0.1, 0.5)
+    source_radius: float = 0.1
+    alpha: float = 0.1
+    beta: float = 1.0
+    tol: float = 1e-6
+    max_iterations: int = 50
+
+    @property
+    def h(self):
+        return float(np.float32(1.0 / self.n))
+
+
+def nodal_phi(p: PlumeParams):
+    n, h = p.n, np.float32(p.h)
+    phi = scenes.box_walls_phi(n, n, n, h, open_top=True)
+    if p.obstacle:
+        phi = np.minimum(phi, scenes.sphere_phi(n, n, n, h, p.obstacle_centre, p.obstacle_radius))
+    return phi.astype(np.float32)
+
+
+class PlumeSim:
+    FIELDS = ("u", "v", "w", "rho", "temp")
+
+    def __init__(self, solver, params: PlumeParams):
+        self.s = solver
+        self.p = params
+        n = params.n
+        dev = solver.device
+        su, sv, sw = scenes.face_shapes(n, n, n)
+        shapes = {"u": su, "v": sv, "w": sw, "rho": (n, n, n), "temp": (n, n, n)}
+        self.shapes = shapes
+        self.f = {k: torch.zeros(shapes[k], dtype=torch.float32, device=dev) for k in self.FIELDS}
+        self.g = {k: torch.zeros(shapes[k], dtype=torch.float32, device=dev) for k in self.FIELDS}
+        self.phi = torch.from_numpy(nodal_phi(params)).to(dev)
+        self.bdesc = torch.zeros((n, n, n), dtype=torch.int8, device=dev)
+        self.solid = {k: torch.zeros(shapes[k], dtype=torch.float32, device=dev) for k in ("u", "v", "w")}
+        self.pressure = torch.zeros((n, n, n), dtype=torch.float64, device=dev)
+        self.last = None
+
+    def load_state(self, arrays):
+        for k in self.FIELDS:
+            self.f[k].copy_(torch.as_tensor(arrays[k]), non_blocking=True)
+
+    def state(self):
+        return {k: self.f[k] for k in self.FIELDS}
+
+    def step(self):
+        p, s, n, h = self.p, self.s, self.p.n, self.p.h
+        u, v, w = self.f["u"], self.f["v"], self.f["w"]
+        offs = {"u": (0.5, 0, 0), "v": (0, 0.5, 0), "w": (0, 0, 0.5), "rho": (0, 0, 0), "temp": (0, 0, 0)}
+        for k in self.FIELDS:
+            s.advect_rk2_linear(n, n, n, h, p.dt, u, v, w, self.f[k], offs[k], out=self.g[k])
+        self.f, self.g = self.g, self.f
+        s.plume_sources(n, n, n, h, p.dt, self.f["rho"], self.f["temp"], self.f["v"], p.source_centre,
+                        p.source_radius, 1.0, 1.0, p.alpha, p.beta)
+        conv, _, stats = s.project(n, n, n, h, 0.0, self.phi, self.bdesc, self.solid["u"], self.solid["v"],
+                                   self.solid["w"], self.f["u"], self.f["v"], self.f["w"], pressure=self.pressure,
+                                   tolerance_factor=p.tol, max_iterations=p.max_iterations)
+        self.last = stats
+        return conv, stats
+
+    def step_host(self, host):
+        """One step on host-resident state (pinned tensors): H2D copy, step,
+        D2H copy back into the same host tensors."""
+        for k in self.FIELDS:
+            self.f[k].copy_(host[k], non_blocking=True)
+        out = self.step()
+        for k in self.FIELDS:
+            host[k].copy_(self.f[k], non_blocking=True)
+        return out
+
+    def host_bytes(self):
+        return sum(int(np.prod(self.shapes[k])) * 4 for k in self.FIELDS)

@@ -246,6 +246,29 @@ class Solver:
                                        _p(un), _p(vn), _p(wn), float(flip_ratio)))
         return particles
 
+    # ------------------------------------------------------------- plume
+    def plume_sources(self, ni, nj, nk, h, dt, rho, temp, v, centre, radius, dens_value=1.0, heat_value=1.0,
+                      alpha=0.1, beta=1.0):
+        self._check(self.lib.vflip_plume_sources(self.ctx, ni, nj, nk, float(h), float(dt), _p(rho), _p(temp), _p(v),
+                                                 float(centre[0]), float(centre[1]), float(centre[2]), float(radius),
+                                                 float(dens_value), float(heat_value), float(alpha), float(beta)))
+
+    # ------------------------------------------------------------- measurement
+    def set_profiling(self, enable):
+        self._check(self.lib.vflip_set_profiling(self.ctx, 1 if enable else 0))
+
+    def profile_sweeps(self):
+        """(launches, total_ms, fine cells) of the timed fine-level sweeps."""
+        n = C.c_int(0)
+        ms = C.c_double(0.0)
+        cells = C.c_double(0.0)
+        self._check(self.lib.vflip_profile_sweeps(self.ctx, C.byref(n), C.byref(ms), C.byref(cells)))
+        return n.value, ms.value, cells.value
+
+    @property
+    def launch_count(self):
+        return int(self.lib.vflip_launch_count(self.ctx))
+
     # ------------------------------------------------------------- layout
     def bricks_to_linear(self, nx, ny, nz, bricked):
         out = self._empty((nz, ny, nx), torch.float32)
