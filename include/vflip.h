@@ -63,6 +63,8 @@ typedef struct {
   int coarsest_max_unknowns; /* coarsen while unknowns exceed this, default 4096 (SS/GeometricLevelGen.h:46); max 4096 */
   int device;                /* CUDA device ordinal, default 0 */
   void* stream;              /* cudaStream_t to order work on; NULL: the CUDA default stream */
+  int sweep_kernel;          /* smoother kernel: 0 = pipelined (cp.async plane staging) where the row length
+                                allows it, else the plain fused kernel; 1 = always the plain fused kernel */
 } vflip_config;
 
 typedef struct {

@@ -51,15 +51,22 @@ template <typename T> __device__ __forceinline__ typename Num<T>::Acc ldg(const 
 template <typename T> __device__ __forceinline__ typename Num<T>::Acc ldv(const T* p) { return Num<T>::ldv(p); }
 template <typename T, typename A> __device__ __forceinline__ T cvt(A v) { return Num<T>::to(v); }
 
-// Block-wide sum of one double per thread; result valid in thread 0.
+__device__ __forceinline__ int linear_tid() {
+  return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+}
+
+// Block-wide sum of one double per thread (1-, 2- or 3-D blocks of BLOCK
+// threads); result valid in linear thread 0.  Fixed order: warp shuffle
+// tree, then warps in index order.
 template <int BLOCK>
 __device__ __forceinline__ double block_sum(double v, double* smem /* >= BLOCK/32 */) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int tid = linear_tid();
+  int lane = tid & 31, wid = tid >> 5;
   if (lane == 0) smem[wid] = v;
   __syncthreads();
   double s = 0;
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     for (int w = 0; w < BLOCK / 32; ++w) s += smem[w];
   }
   __syncthreads();
@@ -71,11 +78,12 @@ __device__ __forceinline__ double block_sum(double v, double* smem /* >= BLOCK/3
 template <int BLOCK>
 __device__ __forceinline__ double block_absmax(double v, double* smem) {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int tid = linear_tid();
+  int lane = tid & 31, wid = tid >> 5;
   if (lane == 0) smem[wid] = v;
   __syncthreads();
   double s = 0;
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     for (int w = 0; w < BLOCK / 32; ++w) s = fmax(s, smem[w]);
   }
   __syncthreads();

@@ -190,11 +190,121 @@ int launch_sweep_t(vflip_ctx* ctx, const SweepArgs<S, V>& a, const SweepShape& s
   return VFLIP_OK;
 }
 
+// Shape of the pipelined sweep (rbgs_sweep2_kernel): rows per tile from a
+// shared-memory budget, persistent CTAs over equal shares of the level's
+// (row tile, plane) pairs.
+struct Sweep2Shape {
+  int tyo, gy, rows_max, crows_max, grid, work, bx, by;
+  size_t smem;
+};
+
+constexpr size_t kSweep2Smem = 200 * 1024;
+
+template <typename S>
+bool sweep2_shape(const Dims& d, const Dims* cd, bool prolong, int num_sms, Sweep2Shape& o) {
+  if (d.ni % 4 != 0 || (d.ni * sizeof(S)) % 16 != 0) return false;
+  if (prolong && (!cd || cd->ni % 4 != 0)) return false;
+  const size_t per_row = (size_t)d.ni * (8 * 4 + 13 * sizeof(S));
+  const int cni = cd ? cd->ni : 0;
+  int rows = (int)(kSweep2Smem / (per_row + (prolong ? 5 * 4 * (size_t)cni : 0)));
+  if (rows < 5) return false;
+  int tyo = std::min(rows - 4, d.nj);
+  o.tyo = tyo;
+  o.gy = (d.nj + tyo - 1) / tyo;
+  o.rows_max = std::min(tyo + 4, d.nj);
+  o.crows_max = prolong ? (o.rows_max + 3) / 2 : 0;
+  o.smem = (size_t)o.rows_max * d.ni * (8 * 4 + 13 * sizeof(S)) + (size_t)5 * o.crows_max * cni * 4;
+  if (o.smem > kSweep2Smem) return false;
+  const int total = o.gy * d.nk;
+  o.grid = std::max(1, std::min(num_sms, total / 8));
+  o.work = (total + o.grid - 1) / o.grid;
+  o.grid = (total + o.work - 1) / o.work;
+  int P = (d.ni + 1) / 2;
+  int bx = 1;
+  while (bx < P && bx < 128) bx <<= 1;
+  o.bx = bx;
+  o.by = 256 / bx;
+  return true;
+}
+
+template <typename S, bool Z, bool P, bool D>
+int launch_sweep2_t(vflip_ctx* ctx, const Sweep2Args<S>& a, const Sweep2Shape& sh) {
+  auto kern = rbgs_sweep2_kernel<S, Z, P, D, 256>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweep2Smem);
+    attr_set = true;
+  }
+  const bool timed = ctx->profiling && (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n;
+  if (timed) {
+    if (ctx->prof_used == ctx->prof_events.size()) {
+      cudaEvent_t e0, e1;
+      VF_CUDA(cudaEventCreate(&e0));
+      VF_CUDA(cudaEventCreate(&e1));
+      ctx->prof_events.push_back({e0, e1});
+    }
+    VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].first, ctx->stream));
+  }
+  kern<<<sh.grid, dim3(sh.bx, sh.by), sh.smem, ctx->stream>>>(a);
+  VF_LAUNCH_CHECK();
+  if (timed) {
+    VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].second, ctx->stream));
+    ++ctx->prof_used;
+  }
+  return VFLIP_OK;
+}
+
+// FP32-vector sweeps take the pipelined kernel when the row layout allows.
+template <typename S, typename V>
+int sweep2(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_out, const V* xc, const Dims* cd,
+           double* dot_partial, int* nblocks_out, bool* used) {
+  *used = false;
+  if (!std::is_same<V, float>::value || ctx->cfg.sweep_kernel == 1) return VFLIP_OK;
+  Sweep2Shape sh;
+  const bool pro = xc != nullptr;
+  if (!sweep2_shape<S>(L.d, cd, pro, ctx->num_sms, sh)) return VFLIP_OK;
+  Sweep2Args<S> a;
+  a.x_in = (const float*)x_in;
+  a.x_out = (float*)x_out;
+  a.b = (const float*)b;
+  a.diag = L.diag;
+  a.xp = L.xp;
+  a.yp = L.yp;
+  a.zp = L.zp;
+  a.xc = (const float*)xc;
+  a.ni = L.d.ni;
+  a.nj = L.d.nj;
+  a.nk = L.d.nk;
+  a.cni = cd ? cd->ni : 0;
+  a.cnj = cd ? cd->nj : 0;
+  a.tyo = sh.tyo;
+  a.gy = sh.gy;
+  a.work = sh.work;
+  a.rows_max = sh.rows_max;
+  a.crows_max = sh.crows_max;
+  a.dot_partial = dot_partial;
+  if (nblocks_out) *nblocks_out = sh.grid;
+  *used = true;
+  bool zero = (x_in == nullptr), dot = (dot_partial != nullptr);
+  if (zero && !pro && !dot) return launch_sweep2_t<S, true, false, false>(ctx, a, sh);
+  if (zero && !pro && dot) return launch_sweep2_t<S, true, false, true>(ctx, a, sh);
+  if (!zero && pro && !dot) return launch_sweep2_t<S, false, true, false>(ctx, a, sh);
+  if (!zero && pro && dot) return launch_sweep2_t<S, false, true, true>(ctx, a, sh);
+  if (!zero && !pro && !dot) return launch_sweep2_t<S, false, false, false>(ctx, a, sh);
+  if (!zero && !pro && dot) return launch_sweep2_t<S, false, false, true>(ctx, a, sh);
+  return ctx->fail(VFLIP_ERR_ARG, "sweep: prolongation needs an incoming x");
+}
+
 // One sweep x_in -> x_out on a level; x_in == nullptr means x = 0.
 template <typename S, typename V>
 int sweep(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_out, const V* xc, const Dims* cd,
           double* dot_partial, int* nblocks_out = nullptr) {
   using A = typename Num<V>::Acc;
+  {
+    bool used = false;
+    int rc = sweep2<S, V>(ctx, L, b, x_in, x_out, xc, cd, dot_partial, nblocks_out, &used);
+    if (rc || used) return rc;
+  }
   SweepShape sh = sweep_shape<A>(L.d, ctx->num_sms);
   if (sh.smem > 200 * 1024) return ctx->fail(VFLIP_ERR_ARG, "grid row of %d cells too long for one CTA", L.d.ni);
   SweepArgs<S, V> a;
@@ -608,6 +718,7 @@ void vflip_config_default(vflip_config* cfg) {
   cfg->coarsest_max_unknowns = 16 * 16 * 16;
   cfg->device = 0;
   cfg->stream = nullptr;
+  cfg->sweep_kernel = 0;
 }
 
 int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
@@ -622,7 +733,7 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
   };
   if (ctx->cfg.pre_sweeps < 0 || ctx->cfg.post_sweeps < 0 || ctx->cfg.coarse_sweeps < 0 ||
       ctx->cfg.coarsest_max_unknowns < 1 || ctx->cfg.coarsest_max_unknowns > 4096 || ctx->cfg.precision < 0 ||
-      ctx->cfg.precision > 2)
+      ctx->cfg.precision > 2 || ctx->cfg.sweep_kernel < 0 || ctx->cfg.sweep_kernel > 1)
     return bad(VFLIP_ERR_ARG);
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);

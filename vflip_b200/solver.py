@@ -53,7 +53,7 @@ def _face_shapes(ni, nj, nk):
 
 class Solver:
     def __init__(self, precision=1, pre_sweeps=4, post_sweeps=4, coarse_sweeps=200, coarsest_max_unknowns=4096,
-                 device=0, stream=None):
+                 device=0, stream=None, sweep_kernel=0):
         self.lib = load()
         cfg = ConfigC()
         self.lib.vflip_config_default(C.byref(cfg))
@@ -63,6 +63,7 @@ class Solver:
         cfg.coarse_sweeps = coarse_sweeps
         cfg.coarsest_max_unknowns = coarsest_max_unknowns
         cfg.device = device
+        cfg.sweep_kernel = sweep_kernel
         self.device = torch.device("cuda", device)
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
