@@ -263,12 +263,21 @@ struct Sweep2Args {
   const float* xc;
   int ni, nj, nk;
   int cni, cnj;
-  int tyo, gy;
-  int work;        // tile-planes per CTA
-  int rows_max;    // staged rows per plane slot (tyo + 4, clamped to nj)
+  int tyo;         // output rows per tile; blockIdx.x = row tile
+  int zlen;        // planes per CTA; blockIdx.y = plane range
   int crows_max;   // staged coarse rows per slot
   double* dot_partial;
 };
+
+// Rows staged per plane for a tile of `tyo` output rows: x needs the red ring
+// and its neighbours (tyo + 4), b/diag/xp/zp the red rows (tyo + 2), yp one
+// more row below them (tyo + 3).
+template <typename S>
+__host__ __device__ constexpr size_t sweep2_smem_bytes(int ni, int tyo, int crows, int cni) {
+  return (size_t)ni * (5 * 4 * (tyo + 4) + 3 * 4 * (tyo + 2) + 3 * 2 * sizeof(S) * (tyo + 2) +
+                       3 * sizeof(S) * (tyo + 3) + 4 * sizeof(S) * (tyo + 2)) +
+         (size_t)5 * crows * cni * 4;
+}
 
 template <typename S, bool ZERO_X, bool PROLONG, bool DOT, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) rbgs_sweep2_kernel(Sweep2Args<S> a) {
@@ -276,171 +285,153 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep2_kernel(Sweep2Args<S> a) {
   __shared__ double red_smem[BLOCK / 32];
   const int ni = a.ni, nj = a.nj, nk = a.nk;
   const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
-  const int plane_f = a.rows_max * ni;  // elements per slot
+  const int tyo = a.tyo;
+  const int xslot = (tyo + 4) * ni, cslot = (tyo + 2) * ni, yslot = (tyo + 3) * ni;
   float* X = reinterpret_cast<float*>(smem_raw);
-  float* B = X + 5 * plane_f;
-  S* Dg = reinterpret_cast<S*>(B + 3 * plane_f);
-  S* XP = Dg + 3 * plane_f;
-  S* YP = XP + 3 * plane_f;
-  S* ZP = YP + 3 * plane_f;
-  float* XC = reinterpret_cast<float*>(ZP + 4 * plane_f);
+  float* B = X + 5 * xslot;
+  S* Dg = reinterpret_cast<S*>(B + 3 * cslot);
+  S* XP = Dg + 3 * cslot;
+  S* ZP = XP + 3 * cslot;
+  S* YP = ZP + 4 * cslot;
+  float* XC = reinterpret_cast<float*>(YP + 3 * yslot);
   const int cplane = a.crows_max * a.cni;
-  auto xs = [&](int q) { return X + ((q % 5 + 5) % 5) * plane_f; };
-  auto bs = [&](int q) { return B + ((q % 3 + 3) % 3) * plane_f; };
-  auto ds = [&](int q) { return Dg + ((q % 3 + 3) % 3) * plane_f; };
-  auto xps = [&](int q) { return XP + ((q % 3 + 3) % 3) * plane_f; };
-  auto yps = [&](int q) { return YP + ((q % 3 + 3) % 3) * plane_f; };
-  auto zps = [&](int q) { return ZP + ((q % 4 + 4) % 4) * plane_f; };
-  auto xcs = [&](int q) { return XC + ((q % 5 + 5) % 5) * cplane; };
-  const int P = (ni + 1) / 2;  // cell pairs per row
+  auto m5 = [](int q) { return (q % 5 + 5) % 5; };
+  auto m3 = [](int q) { return (q % 3 + 3) % 3; };
+  auto m4 = [](int q) { return q & 3; };
+  const int P = (ni + 1) / 2;
   const int tx = threadIdx.x, ty = threadIdx.y, bx = blockDim.x, by = blockDim.y;
   double dot = 0.0;
 
-  const int total = a.gy * nk;
-  const int beg = blockIdx.x * a.work;
-  const int end = min(total, beg + a.work);
-  for (int pos = beg; pos < end;) {
-    const int t = pos / nk;
-    const int k0 = pos - t * nk;
-    const int kend = min(nk, k0 + (end - pos));
-    pos += kend - k0;
-    const int j0 = t * a.tyo;
-    const int jout1 = min(j0 + a.tyo, nj);
-    const int jr0 = max(j0 - 2, 0), jr1 = min(j0 + a.tyo + 2, nj);
-    const int jred0 = max(j0 - 1, 0), jred1 = min(j0 + a.tyo + 1, nj);
-    const int rows = jr1 - jr0;
-    const int cr0 = jr0 >> 1, cr1 = ((jr1 - 1) >> 1) + 1;
+  const int j0 = blockIdx.x * tyo;
+  const int k0 = blockIdx.y * a.zlen;
+  const int kend = min(nk, k0 + a.zlen);
+  const int jout1 = min(j0 + tyo, nj);
+  const int jr0 = max(j0 - 2, 0), jr1 = min(j0 + tyo + 2, nj);         // x rows
+  const int jred0 = max(j0 - 1, 0), jred1 = min(j0 + tyo + 1, nj);     // b, diag, xp, zp rows
+  const int jy0 = jr0;                                                  // yp rows [jy0, jred1)
+  const int xrows = jr1 - jr0, crows = jred1 - jred0, yrows = jred1 - jy0;
+  const int cr0 = jr0 >> 1, cr1 = ((jr1 - 1) >> 1) + 1;
 
-    auto issue_x = [&](int q) {
-      if (q < 0 || q >= nk || ZERO_X) return;
-      stage_bytes<BLOCK>((unsigned char*)xs(q), (const unsigned char*)(a.x_in + q * sz + jr0 * sy), rows * ni * 4);
-      if (PROLONG)
-        stage_bytes<BLOCK>((unsigned char*)xcs(q),
-                           (const unsigned char*)(a.xc + (size_t)(q >> 1) * a.cni * a.cnj + (size_t)cr0 * a.cni),
-                           (cr1 - cr0) * a.cni * 4);
-    };
-    auto issue_coef = [&](int q) {
-      if (q < 0 || q >= nk) return;
-      const size_t o = q * sz + jr0 * sy;
-      const int nb = rows * ni;
-      stage_bytes<BLOCK>((unsigned char*)bs(q), (const unsigned char*)(a.b + o), nb * 4);
-      stage_bytes<BLOCK>((unsigned char*)ds(q), (const unsigned char*)(a.diag + o), nb * (int)sizeof(S));
-      stage_bytes<BLOCK>((unsigned char*)xps(q), (const unsigned char*)(a.xp + o), nb * (int)sizeof(S));
-      stage_bytes<BLOCK>((unsigned char*)yps(q), (const unsigned char*)(a.yp + o), nb * (int)sizeof(S));
-    };
-    auto issue_zp = [&](int q) {
-      if (q < 0 || q >= nk) return;
-      stage_bytes<BLOCK>((unsigned char*)zps(q), (const unsigned char*)(a.zp + q * sz + jr0 * sy),
-                         rows * ni * (int)sizeof(S));
-    };
-    // x_in + P x_c on a freshly landed plane (prolongation, injection)
-    auto prolong_add = [&](int q) {
-      if (!PROLONG || q < 0 || q >= nk) return;
-      float* xq = xs(q);
-      const float* cq = xcs(q);
-      for (int r = ty; r < rows; r += by) {
-        const int cr = ((jr0 + r) >> 1) - cr0;
-        for (int i = tx; i < ni; i += bx) xq[r * ni + i] = xq[r * ni + i] + cq[cr * a.cni + (i >> 1)];
-      }
-    };
-    auto relax = [&](int p, int r0, int r1, int odd) {
-      float* x0 = xs(p);
-      const float* xm1 = xs(p - 1);
-      const float* xp1 = xs(p + 1);
-      const float* bq = bs(p);
-      const S* dq = ds(p);
-      const S* xq = xps(p);
-      const S* yq = yps(p);
-      const S* zq = zps(p);
-      const S* zm = zps(p - 1);
-      for (int j = r0 + ty; j < r1; j += by) {
-        const int sh = odd ? ((j + p + 1) & 1) : ((j + p) & 1);
-        for (int m = tx; m < P; m += bx) {
-          const int i = 2 * m + sh;
-          if (i >= ni) continue;
-          const int s = (j - jr0) * ni + i;
-          float sum = 0.0f;
-          if (p > 0) sum = sum + float(ldv(zm + s)) * xm1[s];
-          if (j > 0) sum = sum + float(ldv(yq + s - ni)) * x0[s - ni];
-          if (i > 0) sum = sum + float(ldv(xq + s - 1)) * x0[s - 1];
-          if (i < ni - 1) sum = sum + float(ldv(xq + s)) * x0[s + 1];
-          if (j < nj - 1) sum = sum + float(ldv(yq + s)) * x0[s + ni];
-          if (p < nk - 1) sum = sum + float(ldv(zq + s)) * xp1[s];
-          const float d = float(ldv(dq + s));
-          x0[s] = (d != 0.0f) ? (bq[s] - sum) / d : 0.0f;
-        }
-      }
-    };
-
-    // prologue: x(k0-2 .. k0), coefficients (k0-1), zp(k0-2)
-    issue_x(k0 - 2);
-    issue_x(k0 - 1);
-    issue_x(k0);
-    issue_coef(k0 - 1);
-    issue_zp(k0 - 2);
-    issue_zp(k0 - 1);
-    cp_async_commit();
-    for (int p = k0 - 1; p <= kend; ++p) {
-      issue_x(p + 2);
-      issue_coef(p + 1);
-      issue_zp(p + 1);
-      cp_async_commit();
-      cp_async_wait1();
-      __syncthreads();
-      if (PROLONG) {
-        if (p == k0 - 1) {
-          prolong_add(k0 - 2);
-          prolong_add(k0 - 1);
-        }
-        prolong_add(p + 1);
-        __syncthreads();
-      }
-      if (ZERO_X) {
-        // the incoming x is zero: zero-fill the staged plane instead of
-        // copying it (same arithmetic as relaxing against a zero array)
-        float* xq = xs(p + 1);
-        for (int r = ty; r < rows; r += by)
-          for (int i = tx; i < ni; i += bx) xq[r * ni + i] = 0.0f;
-        if (p == k0 - 1) {
-          float* xa = xs(k0 - 1);
-          float* xb = xs(k0 - 2);
-          for (int r = ty; r < rows; r += by)
-            for (int i = tx; i < ni; i += bx) {
-              xa[r * ni + i] = 0.0f;
-              xb[r * ni + i] = 0.0f;
-            }
-        }
-        __syncthreads();
-      }
-      if (p >= 0 && p < nk) relax(p, jred0, jred1, 1);
-      __syncthreads();
-      const int q = p - 1;
-      const bool out_plane = (q >= k0 && q < kend);
-      if (out_plane) relax(q, j0, jout1, 0);
-      __syncthreads();
-      if (out_plane) {
-        const float* src = xs(q) + (j0 - jr0) * ni;
-        const int cnt4 = (jout1 - j0) * ni / 4;
-        float4* dst = reinterpret_cast<float4*>(a.x_out + q * sz + j0 * sy);
-        const float4* s4 = reinterpret_cast<const float4*>(src);
-        const float4* b4 = reinterpret_cast<const float4*>(bs(q) + (j0 - jr0) * ni);
-        for (int e = ty * bx + tx; e < cnt4; e += BLOCK) {
-          float4 v = s4[e];
-          dst[e] = v;
-          if (DOT) {
-            float4 bb = b4[e];
-            dot += (double)v.x * bb.x + (double)v.y * bb.y + (double)v.z * bb.z + (double)v.w * bb.w;
-          }
-        }
-        if (DOT) __syncthreads();
+  auto issue_x = [&](int q) {
+    if (q < 0 || q >= nk || ZERO_X) return;
+    stage_bytes<BLOCK>((unsigned char*)(X + m5(q) * xslot), (const unsigned char*)(a.x_in + q * sz + jr0 * sy),
+                       xrows * ni * 4);
+    if (PROLONG)
+      stage_bytes<BLOCK>((unsigned char*)(XC + m5(q) * cplane),
+                         (const unsigned char*)(a.xc + (size_t)(q >> 1) * a.cni * a.cnj + (size_t)cr0 * a.cni),
+                         (cr1 - cr0) * a.cni * 4);
+  };
+  auto issue_coef = [&](int q) {
+    if (q < 0 || q >= nk) return;
+    const size_t o = q * sz + jred0 * sy;
+    const int nb = crows * ni;
+    stage_bytes<BLOCK>((unsigned char*)(B + m3(q) * cslot), (const unsigned char*)(a.b + o), nb * 4);
+    stage_bytes<BLOCK>((unsigned char*)(Dg + m3(q) * cslot), (const unsigned char*)(a.diag + o),
+                       nb * (int)sizeof(S));
+    stage_bytes<BLOCK>((unsigned char*)(XP + m3(q) * cslot), (const unsigned char*)(a.xp + o), nb * (int)sizeof(S));
+    stage_bytes<BLOCK>((unsigned char*)(YP + m3(q) * yslot), (const unsigned char*)(a.yp + q * sz + jy0 * sy),
+                       yrows * ni * (int)sizeof(S));
+  };
+  auto issue_zp = [&](int q) {
+    if (q < 0 || q >= nk) return;
+    stage_bytes<BLOCK>((unsigned char*)(ZP + m4(q) * cslot), (const unsigned char*)(a.zp + q * sz + jred0 * sy),
+                       crows * ni * (int)sizeof(S));
+  };
+  auto prolong_add = [&](int q) {
+    if (!PROLONG || q < 0 || q >= nk) return;
+    float* xq = X + m5(q) * xslot;
+    const float* cq = XC + m5(q) * cplane;
+    for (int r = ty; r < xrows; r += by) {
+      const int cr = ((jr0 + r) >> 1) - cr0;
+      for (int i = tx; i < ni; i += bx) xq[r * ni + i] = xq[r * ni + i] + cq[cr * a.cni + (i >> 1)];
+    }
+  };
+  auto zero_x = [&](int q) {
+    float* xq = X + m5(q) * xslot;
+    for (int e = ty * bx + tx; e < xrows * ni; e += BLOCK) xq[e] = 0.0f;
+  };
+  // relax colour `odd` of plane p on rows [r0, r1): the reference's row sum
+  // in column order (-z, -y, -x, +x, +y, +z), then (b - sum) / diag
+  auto relax = [&](int p, int r0, int r1, int odd) {
+    float* x0 = X + m5(p) * xslot;
+    const float* xm1 = X + m5(p - 1) * xslot;
+    const float* xp1 = X + m5(p + 1) * xslot;
+    const float* bq = B + m3(p) * cslot;
+    const S* dq = Dg + m3(p) * cslot;
+    const S* xq = XP + m3(p) * cslot;
+    const S* yq = YP + m3(p) * yslot;
+    const S* zq = ZP + m4(p) * cslot;
+    const S* zm = ZP + m4(p - 1) * cslot;
+    for (int j = r0 + ty; j < r1; j += by) {
+      const int sh = odd ? ((j + p + 1) & 1) : ((j + p) & 1);
+      const int xrow = (j - jr0) * ni, crow = (j - jred0) * ni, yrow = (j - jy0) * ni;
+      for (int m = tx; m < P; m += bx) {
+        const int i = 2 * m + sh;
+        if (i >= ni) continue;
+        const int s = xrow + i, c = crow + i, y = yrow + i;
+        float sum = 0.0f;
+        if (p > 0) sum = sum + float(ldv(zm + c)) * xm1[s];
+        if (j > 0) sum = sum + float(ldv(yq + y - ni)) * x0[s - ni];
+        if (i > 0) sum = sum + float(ldv(xq + c - 1)) * x0[s - 1];
+        if (i < ni - 1) sum = sum + float(ldv(xq + c)) * x0[s + 1];
+        if (j < nj - 1) sum = sum + float(ldv(yq + y)) * x0[s + ni];
+        if (p < nk - 1) sum = sum + float(ldv(zq + c)) * xp1[s];
+        const float d = float(ldv(dq + c));
+        x0[s] = (d != 0.0f) ? (bq[c] - sum) / d : 0.0f;
       }
     }
-    cp_async_wait0();
+  };
+
+  // prologue: x(k0-2 .. k0), coefficients (k0-1), zp(k0-2, k0-1)
+  issue_x(k0 - 2);
+  issue_x(k0 - 1);
+  issue_x(k0);
+  issue_coef(k0 - 1);
+  issue_zp(k0 - 2);
+  issue_zp(k0 - 1);
+  cp_async_commit();
+  for (int p = k0 - 1; p <= kend; ++p) {
+    issue_x(p + 2);
+    issue_coef(p + 1);
+    issue_zp(p + 1);
+    cp_async_commit();
+    cp_async_wait1();
     __syncthreads();
+    if (PROLONG || ZERO_X) {
+      if (p == k0 - 1) {
+        if (PROLONG) { prolong_add(k0 - 2); prolong_add(k0 - 1); }
+        if (ZERO_X) { zero_x(k0 - 2); zero_x(k0 - 1); }
+      }
+      if (PROLONG) prolong_add(p + 1);
+      if (ZERO_X) zero_x(p + 1);
+      __syncthreads();
+    }
+    if (p >= 0 && p < nk) relax(p, jred0, jred1, 1);
+    __syncthreads();
+    const int q = p - 1;
+    const bool out_plane = (q >= k0 && q < kend);
+    if (out_plane) relax(q, j0, jout1, 0);
+    __syncthreads();
+    if (out_plane) {
+      const float4* s4 = reinterpret_cast<const float4*>(X + m5(q) * xslot + (j0 - jr0) * ni);
+      const float4* b4 = reinterpret_cast<const float4*>(B + m3(q) * cslot + (j0 - jred0) * ni);
+      float4* dst = reinterpret_cast<float4*>(a.x_out + q * sz + j0 * sy);
+      const int cnt4 = (jout1 - j0) * ni / 4;
+      for (int e = ty * bx + tx; e < cnt4; e += BLOCK) {
+        float4 v = s4[e];
+        dst[e] = v;
+        if (DOT) {
+          float4 bb = b4[e];
+          dot += (double)v.x * bb.x + (double)v.y * bb.y + (double)v.z * bb.z + (double)v.w * bb.w;
+        }
+      }
+      if (DOT) __syncthreads();
+    }
   }
+  cp_async_wait0();
   if (DOT) {
     double s = block_sum<BLOCK>(dot, red_smem);
-    if (threadIdx.x == 0 && threadIdx.y == 0) a.dot_partial[blockIdx.x] = s;
+    if (threadIdx.x == 0 && threadIdx.y == 0) a.dot_partial[blockIdx.x + gridDim.x * blockIdx.y] = s;
   }
 }
 

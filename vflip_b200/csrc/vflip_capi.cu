@@ -194,37 +194,54 @@ int launch_sweep_t(vflip_ctx* ctx, const SweepArgs<S, V>& a, const SweepShape& s
 // shared-memory budget, persistent CTAs over equal shares of the level's
 // (row tile, plane) pairs.
 struct Sweep2Shape {
-  int tyo, gy, rows_max, crows_max, grid, work, bx, by;
+  int tyo, gy, zlen, gz, crows_max, bx, by;
   size_t smem;
 };
 
-constexpr size_t kSweep2Smem = 200 * 1024;
+constexpr size_t kSweep2Smem = 224 * 1024;
 
+// Tile shape: choose (rows per tile, planes per CTA) so that every CTA of a
+// launch is resident at once (one per SM) and marches in step with the CTAs
+// of the neighbouring row tiles (their halo rows then come from L2), trading
+// the 4 redundant halo planes of each plane range against load balance.
 template <typename S>
 bool sweep2_shape(const Dims& d, const Dims* cd, bool prolong, int num_sms, Sweep2Shape& o) {
   if (d.ni % 4 != 0 || (d.ni * sizeof(S)) % 16 != 0) return false;
   if (prolong && (!cd || cd->ni % 4 != 0)) return false;
-  const size_t per_row = (size_t)d.ni * (8 * 4 + 13 * sizeof(S));
-  const int cni = cd ? cd->ni : 0;
-  int rows = (int)(kSweep2Smem / (per_row + (prolong ? 5 * 4 * (size_t)cni : 0)));
-  if (rows < 5) return false;
-  int tyo = std::min(rows - 4, d.nj);
-  o.tyo = tyo;
-  o.gy = (d.nj + tyo - 1) / tyo;
-  o.rows_max = std::min(tyo + 4, d.nj);
-  o.crows_max = prolong ? (o.rows_max + 3) / 2 : 0;
-  o.smem = (size_t)o.rows_max * d.ni * (8 * 4 + 13 * sizeof(S)) + (size_t)5 * o.crows_max * cni * 4;
-  if (o.smem > kSweep2Smem) return false;
-  const int total = o.gy * d.nk;
-  o.grid = std::max(1, std::min(num_sms, total / 8));
-  o.work = (total + o.grid - 1) / o.grid;
-  o.grid = (total + o.work - 1) / o.work;
+  const int cni = prolong ? cd->ni : 0;
+  int tyo_max = 0;
+  for (int t = 1; t <= d.nj; ++t) {
+    if (sweep2_smem_bytes<S>(d.ni, t, prolong ? (t + 4 + 3) / 2 : 0, cni) > kSweep2Smem) break;
+    tyo_max = t;
+  }
+  if (tyo_max < 1) return false;
+  double best = 1e30;
+  for (int nzr = 1; nzr <= std::min(d.nk, 16); ++nzr) {
+    int gy_target = std::max(1, num_sms / nzr);
+    int tyo = std::max((d.nj + gy_target - 1) / gy_target, 1);
+    if (tyo > tyo_max) tyo = tyo_max;
+    int gy = (d.nj + tyo - 1) / tyo;
+    int zlen = (d.nk + nzr - 1) / nzr;
+    int gz = (d.nk + zlen - 1) / zlen;
+    double waves = std::ceil((double)gy * gz / num_sms);
+    double util = (double)gy * gz / (waves * num_sms);
+    double cost = (1.0 + 4.0 / zlen) * (1.0 + 4.0 / tyo * 0.15) / util;
+    if (cost < best) {
+      best = cost;
+      o.tyo = tyo;
+      o.gy = gy;
+      o.zlen = zlen;
+      o.gz = gz;
+    }
+  }
+  o.crows_max = prolong ? (o.tyo + 4 + 3) / 2 : 0;
+  o.smem = sweep2_smem_bytes<S>(d.ni, o.tyo, o.crows_max, cni);
   int P = (d.ni + 1) / 2;
   int bx = 1;
   while (bx < P && bx < 128) bx <<= 1;
   o.bx = bx;
   o.by = 256 / bx;
-  return true;
+  return o.smem <= kSweep2Smem;
 }
 
 template <typename S, bool Z, bool P, bool D>
@@ -245,7 +262,7 @@ int launch_sweep2_t(vflip_ctx* ctx, const Sweep2Args<S>& a, const Sweep2Shape& s
     }
     VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].first, ctx->stream));
   }
-  kern<<<sh.grid, dim3(sh.bx, sh.by), sh.smem, ctx->stream>>>(a);
+  kern<<<dim3(sh.gy, sh.gz), dim3(sh.bx, sh.by), sh.smem, ctx->stream>>>(a);
   VF_LAUNCH_CHECK();
   if (timed) {
     VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].second, ctx->stream));
@@ -278,12 +295,10 @@ int sweep2(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x
   a.cni = cd ? cd->ni : 0;
   a.cnj = cd ? cd->nj : 0;
   a.tyo = sh.tyo;
-  a.gy = sh.gy;
-  a.work = sh.work;
-  a.rows_max = sh.rows_max;
+  a.zlen = sh.zlen;
   a.crows_max = sh.crows_max;
   a.dot_partial = dot_partial;
-  if (nblocks_out) *nblocks_out = sh.grid;
+  if (nblocks_out) *nblocks_out = sh.gy * sh.gz;
   *used = true;
   bool zero = (x_in == nullptr), dot = (dot_partial != nullptr);
   if (zero && !pro && !dot) return launch_sweep2_t<S, true, false, false>(ctx, a, sh);
