@@ -51,6 +51,12 @@ template <typename T> __device__ __forceinline__ typename Num<T>::Acc ldg(const 
 template <typename T> __device__ __forceinline__ typename Num<T>::Acc ldv(const T* p) { return Num<T>::ldv(p); }
 template <typename T, typename A> __device__ __forceinline__ T cvt(A v) { return Num<T>::to(v); }
 
+// Gauss-Seidel division: IEEE in FP64 (reproduces the reference's
+// smoother bit for bit), the hardware fast division (2 ulp) in FP32, whose
+// smoother is not bit-exact with the FP64 reference in any case.
+__device__ __forceinline__ double gs_div(double a, double b) { return a / b; }
+__device__ __forceinline__ float gs_div(float a, float b) { return __fdividef(a, b); }
+
 __device__ __forceinline__ int linear_tid() {
   return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
 }

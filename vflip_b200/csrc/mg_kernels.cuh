@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_kernel(SweepArgs<S, V> a) {
       if (j < nj - 1) sum = sum + A(ldg(a.yp + g)) * x0[s + width];
       if (p < nk - 1) sum = sum + A(ldg(a.zp + g)) * xp1[s];
       A d = A(ldg(a.diag + g));
-      x0[s] = (d != A(0)) ? (ldg(a.b + g) - sum) / d : A(0);
+      x0[s] = (d != A(0)) ? gs_div(ldg(a.b + g) - sum, d) : A(0);
     }
   };
 
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep2_kernel(Sweep2Args<S> a) {
         if (j < nj - 1) sum = sum + float(ldv(yq + y)) * x0[s + ni];
         if (p < nk - 1) sum = sum + float(ldv(zq + c)) * xp1[s];
         const float d = float(ldv(dq + c));
-        x0[s] = (d != 0.0f) ? (bq[c] - sum) / d : 0.0f;
+        x0[s] = (d != 0.0f) ? gs_div(bq[c] - sum, d) : 0.0f;
       }
     }
   };
@@ -559,7 +559,7 @@ __global__ void __launch_bounds__(BLOCK) coarsest_rbgs_kernel(const V* __restric
         if (f & 16) sum = sum + yps[e] * xs[e + sy];
         if (f & 32) sum = sum + zps[e] * xs[e + sz];
         A d = ds[e];
-        xs[e] = (d != A(0)) ? (bs[e] - sum) / d : A(0);
+        xs[e] = (d != A(0)) ? gs_div(bs[e] - sum, d) : A(0);
       }
       __syncthreads();
     }

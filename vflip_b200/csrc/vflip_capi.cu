@@ -199,6 +199,7 @@ struct Sweep2Shape {
 };
 
 constexpr size_t kSweep2Smem = 224 * 1024;
+constexpr int kSweep2Block = 512;
 
 // Tile shape: choose (rows per tile, planes per CTA) so that every CTA of a
 // launch is resident at once (one per SM) and marches in step with the CTAs
@@ -240,13 +241,13 @@ bool sweep2_shape(const Dims& d, const Dims* cd, bool prolong, int num_sms, Swee
   int bx = 1;
   while (bx < P && bx < 128) bx <<= 1;
   o.bx = bx;
-  o.by = 256 / bx;
+  o.by = kSweep2Block / bx;
   return o.smem <= kSweep2Smem;
 }
 
 template <typename S, bool Z, bool P, bool D>
 int launch_sweep2_t(vflip_ctx* ctx, const Sweep2Args<S>& a, const Sweep2Shape& sh) {
-  auto kern = rbgs_sweep2_kernel<S, Z, P, D, 256>;
+  auto kern = rbgs_sweep2_kernel<S, Z, P, D, kSweep2Block>;
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweep2Smem);
