@@ -224,186 +224,234 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_kernel(SweepArgs<S, V> a) {
 }
 
 // ---------------------------------------------------------------------------
-// Pipelined variant of the fused sweep for rows whose byte length is a
-// multiple of 16: every array of a plane (x_in, b, diag, xp, yp, zp, and the
-// coarse x for the fused prolongation) is copied into shared memory with
-// cp.async one plane ahead of its use, so the relaxation phases read only
-// shared memory while the next plane streams in.  Same arithmetic and the
-// same schedule as rbgs_sweep_kernel (red on plane p over the one-row ring,
-// black on plane p-1, store p-1), with persistent CTAs: the (row tile,
-// plane) pairs of the level are split into equal contiguous ranges, one per
-// CTA, so every SM streams the same number of planes.
+// Pipelined FP32 variant of the fused sweep for rows whose length is a
+// multiple of 4 cells.  Every array of a plane region (x_in, b, diag, xp, yp,
+// zp, and the coarse x of the fused prolongation) is a contiguous range of
+// global memory; one thread moves each of them into shared memory with a TMA
+// bulk copy (cp.async.bulk, completion on an mbarrier) one plane ahead of its
+// use, so the relaxation phases read only shared memory while the next
+// plane streams in.  Same arithmetic and schedule as rbgs_sweep_kernel: red
+// on plane p over the tile and a one-row ring, black on plane p-1 over the
+// tile, store plane p-1.
 //
-// Shared-memory rings (plane q lives in slot q mod ring):
-//   x 5 planes (p-2 .. p+2), b/diag/xp/yp 3 planes (p-1 .. p+1), zp 4 planes
-//   (p-2 .. p+1), coarse x 5 planes.
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-template <int BLOCK>
-__device__ __forceinline__ void stage_bytes(unsigned char* dst, const unsigned char* src, int bytes) {
-  for (int c = threadIdx.y * blockDim.x + threadIdx.x; c < (bytes >> 4); c += BLOCK)
-    cp_async16(dst + 16 * c, src + 16 * c);
-}
-
-template <typename S>
-struct Sweep2Args {
+// Grid: (row tiles, plane ranges), sized so that every CTA is resident (one
+// per SM); the CTAs of neighbouring row tiles march the same planes at the
+// same time, so the halo rows one tile re-reads were just fetched by its
+// neighbour and come from L2.
+//
+// Shared-memory rings (plane q in slot q mod ring): x 5 planes (p-2 .. p+2),
+// b/diag/xp/yp 3 (p-1 .. p+1), zp 4 (p-2 .. p+1), coarse x 5.  Two mbarriers
+// alternate between consecutive copy groups.  Every wait is bounded: on a
+// timeout the CTA records the failure in *error, drains its own copies (again
+// bounded) and returns.
+struct TmaSweepArgs {
   const float* x_in;
   float* x_out;
   const float* b;
-  const S* diag;
-  const S* xp;
-  const S* yp;
-  const S* zp;
+  const float* diag;
+  const float* xp;
+  const float* yp;
+  const float* zp;
   const float* xc;
   int ni, nj, nk;
   int cni, cnj;
-  int tyo;         // output rows per tile; blockIdx.x = row tile
-  int zlen;        // planes per CTA; blockIdx.y = plane range
-  int crows_max;   // staged coarse rows per slot
+  int tyo;        // output rows per tile; blockIdx.x = row tile
+  int zlen;       // planes per CTA; blockIdx.y = plane range
+  int crows_max;  // staged coarse rows per slot
   double* dot_partial;
+  int* error;
 };
 
-// Rows staged per plane for a tile of `tyo` output rows: x needs the red ring
-// and its neighbours (tyo + 4), b/diag/xp/zp the red rows (tyo + 2), yp one
-// more row below them (tyo + 3).
-template <typename S>
-__host__ __device__ constexpr size_t sweep2_smem_bytes(int ni, int tyo, int crows, int cni) {
-  return (size_t)ni * (5 * 4 * (tyo + 4) + 3 * 4 * (tyo + 2) + 3 * 2 * sizeof(S) * (tyo + 2) +
-                       3 * sizeof(S) * (tyo + 3) + 4 * sizeof(S) * (tyo + 2)) +
-         (size_t)5 * crows * cni * 4;
+// Floats of shared memory for a tile of `tyo` output rows: x needs the red
+// ring and its neighbours (tyo + 4 rows), b/diag/xp/zp the red rows
+// (tyo + 2), yp one more row below them (tyo + 3).
+__host__ __device__ constexpr size_t tma_sweep_smem_floats(int ni, int tyo, int crows, int cni) {
+  return (size_t)ni * (5 * (tyo + 4) + 3 * 3 * (tyo + 2) + 3 * (tyo + 3) + 4 * (tyo + 2)) + (size_t)5 * crows * cni;
 }
 
-template <typename S, bool ZERO_X, bool PROLONG, bool DOT, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) rbgs_sweep2_kernel(Sweep2Args<S> a) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait: false when the phase did not complete within the limit
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
+  for (int n = 0; n < (1 << 22); ++n)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void tma_bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+template <bool ZERO_X, bool PROLONG, bool DOT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
+  extern __shared__ __align__(128) float sm[];
+  __shared__ __align__(8) unsigned long long bars[2];
   __shared__ double red_smem[BLOCK / 32];
-  const int ni = a.ni, nj = a.nj, nk = a.nk;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int ni = a.ni, nj = a.nj, nk = a.nk, tyo = a.tyo;
   const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
-  const int tyo = a.tyo;
   const int xslot = (tyo + 4) * ni, cslot = (tyo + 2) * ni, yslot = (tyo + 3) * ni;
-  float* X = reinterpret_cast<float*>(smem_raw);
-  float* B = X + 5 * xslot;
-  S* Dg = reinterpret_cast<S*>(B + 3 * cslot);
-  S* XP = Dg + 3 * cslot;
-  S* ZP = XP + 3 * cslot;
-  S* YP = ZP + 4 * cslot;
-  float* XC = reinterpret_cast<float*>(YP + 3 * yslot);
   const int cplane = a.crows_max * a.cni;
-  auto m5 = [](int q) { return (q % 5 + 5) % 5; };
-  auto m3 = [](int q) { return (q % 3 + 3) % 3; };
-  auto m4 = [](int q) { return q & 3; };
+  // slot bases (float offsets into sm)
+  const int oX = 0, oB = oX + 5 * xslot, oD = oB + 3 * cslot, oXP = oD + 3 * cslot, oYP = oXP + 3 * cslot,
+            oZP = oYP + 3 * yslot, oXC = oZP + 4 * cslot;
   const int P = (ni + 1) / 2;
   const int tx = threadIdx.x, ty = threadIdx.y, bx = blockDim.x, by = blockDim.y;
-  double dot = 0.0;
 
   const int j0 = blockIdx.x * tyo;
   const int k0 = blockIdx.y * a.zlen;
   const int kend = min(nk, k0 + a.zlen);
   const int jout1 = min(j0 + tyo, nj);
-  const int jr0 = max(j0 - 2, 0), jr1 = min(j0 + tyo + 2, nj);         // x rows
-  const int jred0 = max(j0 - 1, 0), jred1 = min(j0 + tyo + 1, nj);     // b, diag, xp, zp rows
-  const int jy0 = jr0;                                                  // yp rows [jy0, jred1)
+  const int jr0 = max(j0 - 2, 0), jr1 = min(j0 + tyo + 2, nj);      // x rows
+  const int jred0 = max(j0 - 1, 0), jred1 = min(j0 + tyo + 1, nj);  // b, diag, xp, zp rows
+  const int jy0 = jr0;                                               // yp rows [jy0, jred1)
   const int xrows = jr1 - jr0, crows = jred1 - jred0, yrows = jred1 - jy0;
   const int cr0 = jr0 >> 1, cr1 = ((jr1 - 1) >> 1) + 1;
 
-  auto issue_x = [&](int q) {
-    if (q < 0 || q >= nk || ZERO_X) return;
-    stage_bytes<BLOCK>((unsigned char*)(X + m5(q) * xslot), (const unsigned char*)(a.x_in + q * sz + jr0 * sy),
-                       xrows * ni * 4);
-    if (PROLONG)
-      stage_bytes<BLOCK>((unsigned char*)(XC + m5(q) * cplane),
-                         (const unsigned char*)(a.xc + (size_t)(q >> 1) * a.cni * a.cnj + (size_t)cr0 * a.cni),
-                         (cr1 - cr0) * a.cni * 4);
-  };
-  auto issue_coef = [&](int q) {
-    if (q < 0 || q >= nk) return;
-    const size_t o = q * sz + jred0 * sy;
-    const int nb = crows * ni;
-    stage_bytes<BLOCK>((unsigned char*)(B + m3(q) * cslot), (const unsigned char*)(a.b + o), nb * 4);
-    stage_bytes<BLOCK>((unsigned char*)(Dg + m3(q) * cslot), (const unsigned char*)(a.diag + o),
-                       nb * (int)sizeof(S));
-    stage_bytes<BLOCK>((unsigned char*)(XP + m3(q) * cslot), (const unsigned char*)(a.xp + o), nb * (int)sizeof(S));
-    stage_bytes<BLOCK>((unsigned char*)(YP + m3(q) * yslot), (const unsigned char*)(a.yp + q * sz + jy0 * sy),
-                       yrows * ni * (int)sizeof(S));
-  };
-  auto issue_zp = [&](int q) {
-    if (q < 0 || q >= nk) return;
-    stage_bytes<BLOCK>((unsigned char*)(ZP + m4(q) * cslot), (const unsigned char*)(a.zp + q * sz + jred0 * sy),
-                       crows * ni * (int)sizeof(S));
-  };
-  auto prolong_add = [&](int q) {
-    if (!PROLONG || q < 0 || q >= nk) return;
-    float* xq = X + m5(q) * xslot;
-    const float* cq = XC + m5(q) * cplane;
-    for (int r = ty; r < xrows; r += by) {
-      const int cr = ((jr0 + r) >> 1) - cr0;
-      for (int i = tx; i < ni; i += bx) xq[r * ni + i] = xq[r * ni + i] + cq[cr * a.cni + (i >> 1)];
+  const unsigned bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
+  const unsigned sbase = smem_u32(sm);
+  if (tid == 0) {
+    mbar_init(bar0, 1);
+    mbar_init(bar1, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  auto m5 = [](int q) { return (q % 5 + 5) % 5; };
+  auto m3 = [](int q) { return (q % 3 + 3) % 3; };
+  // thread 0: one copy group (x plane qx, coefficient plane qc, zp planes
+  // qz0 and qz1), completion on bars[g & 1]
+  auto issue = [&](int g, int qx, int qc, int qz0, int qz1, int qx2 = -1) {
+    const unsigned bar = (g & 1) ? bar1 : bar0;
+    unsigned bytes = 0;
+    const bool hx = !ZERO_X && qx >= 0 && qx < nk;
+    const bool hx2 = !ZERO_X && qx2 >= 0 && qx2 < nk;
+    const bool hc = qc >= 0 && qc < nk;
+    const bool hz0 = qz0 >= 0 && qz0 < nk, hz1 = qz1 >= 0 && qz1 < nk;
+    if (hx) bytes += xrows * ni * 4 + (PROLONG ? (cr1 - cr0) * a.cni * 4 : 0);
+    if (hx2) bytes += xrows * ni * 4 + (PROLONG ? (cr1 - cr0) * a.cni * 4 : 0);
+    if (hc) bytes += (3 * crows + yrows) * ni * 4;
+    if (hz0) bytes += crows * ni * 4;
+    if (hz1) bytes += crows * ni * 4;
+    fence_proxy_async();
+    mbar_expect_tx(bar, bytes);
+    if (hx) {
+      tma_bulk_g2s(sbase + 4u * (oX + m5(qx) * xslot), a.x_in + qx * sz + jr0 * sy, xrows * ni * 4, bar);
+      if (PROLONG)
+        tma_bulk_g2s(sbase + 4u * (oXC + m5(qx) * cplane),
+                     a.xc + (size_t)(qx >> 1) * a.cni * a.cnj + (size_t)cr0 * a.cni, (cr1 - cr0) * a.cni * 4, bar);
     }
+    if (hx2) {
+      tma_bulk_g2s(sbase + 4u * (oX + m5(qx2) * xslot), a.x_in + qx2 * sz + jr0 * sy, xrows * ni * 4, bar);
+      if (PROLONG)
+        tma_bulk_g2s(sbase + 4u * (oXC + m5(qx2) * cplane),
+                     a.xc + (size_t)(qx2 >> 1) * a.cni * a.cnj + (size_t)cr0 * a.cni, (cr1 - cr0) * a.cni * 4, bar);
+    }
+    if (hc) {
+      const size_t o = qc * sz + jred0 * sy;
+      const int s3 = m3(qc);
+      tma_bulk_g2s(sbase + 4u * (oB + s3 * cslot), a.b + o, crows * ni * 4, bar);
+      tma_bulk_g2s(sbase + 4u * (oD + s3 * cslot), a.diag + o, crows * ni * 4, bar);
+      tma_bulk_g2s(sbase + 4u * (oXP + s3 * cslot), a.xp + o, crows * ni * 4, bar);
+      tma_bulk_g2s(sbase + 4u * (oYP + s3 * yslot), a.yp + qc * sz + jy0 * sy, yrows * ni * 4, bar);
+    }
+    if (hz0) tma_bulk_g2s(sbase + 4u * (oZP + (qz0 & 3) * cslot), a.zp + qz0 * sz + jred0 * sy, crows * ni * 4, bar);
+    if (hz1) tma_bulk_g2s(sbase + 4u * (oZP + (qz1 & 3) * cslot), a.zp + qz1 * sz + jred0 * sy, crows * ni * 4, bar);
   };
-  auto zero_x = [&](int q) {
-    float* xq = X + m5(q) * xslot;
-    for (int e = ty * bx + tx; e < xrows * ni; e += BLOCK) xq[e] = 0.0f;
+  // all threads: wait for group g; block-uniform result
+  auto wait_group = [&](int g) -> bool {
+    const unsigned bar = (g & 1) ? bar1 : bar0;
+    const bool ok = mbar_wait_bounded(bar, (unsigned)((g >> 1) & 1));
+    return __syncthreads_and(ok) != 0;
   };
+
   // relax colour `odd` of plane p on rows [r0, r1): the reference's row sum
   // in column order (-z, -y, -x, +x, +y, +z), then (b - sum) / diag
   auto relax = [&](int p, int r0, int r1, int odd) {
-    float* x0 = X + m5(p) * xslot;
-    const float* xm1 = X + m5(p - 1) * xslot;
-    const float* xp1 = X + m5(p + 1) * xslot;
-    const float* bq = B + m3(p) * cslot;
-    const S* dq = Dg + m3(p) * cslot;
-    const S* xq = XP + m3(p) * cslot;
-    const S* yq = YP + m3(p) * yslot;
-    const S* zq = ZP + m4(p) * cslot;
-    const S* zm = ZP + m4(p - 1) * cslot;
+    const int x0 = oX + m5(p) * xslot, xm1 = oX + m5(p - 1) * xslot, xp1 = oX + m5(p + 1) * xslot;
+    const int s3 = m3(p);
+    const int cb = oB + s3 * cslot, cd = oD + s3 * cslot, cx = oXP + s3 * cslot, cy = oYP + s3 * yslot;
+    const int cz = oZP + (p & 3) * cslot, czm = oZP + ((p - 1) & 3) * cslot;
+    const bool zlo = p > 0, zhi = p < nk - 1;
     for (int j = r0 + ty; j < r1; j += by) {
       const int sh = odd ? ((j + p + 1) & 1) : ((j + p) & 1);
-      const int xrow = (j - jr0) * ni, crow = (j - jred0) * ni, yrow = (j - jy0) * ni;
+      const int xr = (j - jr0) * ni, cr = (j - jred0) * ni, yr = (j - jy0) * ni;
+      const bool ylo = j > 0, yhi = j < nj - 1;
       for (int m = tx; m < P; m += bx) {
         const int i = 2 * m + sh;
         if (i >= ni) continue;
-        const int s = xrow + i, c = crow + i, y = yrow + i;
+        const int s = xr + i, c = cr + i, y = yr + i;
         float sum = 0.0f;
-        if (p > 0) sum = sum + float(ldv(zm + c)) * xm1[s];
-        if (j > 0) sum = sum + float(ldv(yq + y - ni)) * x0[s - ni];
-        if (i > 0) sum = sum + float(ldv(xq + c - 1)) * x0[s - 1];
-        if (i < ni - 1) sum = sum + float(ldv(xq + c)) * x0[s + 1];
-        if (j < nj - 1) sum = sum + float(ldv(yq + y)) * x0[s + ni];
-        if (p < nk - 1) sum = sum + float(ldv(zq + c)) * xp1[s];
-        const float d = float(ldv(dq + c));
-        x0[s] = (d != 0.0f) ? gs_div(bq[c] - sum, d) : 0.0f;
+        if (zlo) sum = sum + sm[czm + c] * sm[xm1 + s];
+        if (ylo) sum = sum + sm[cy + y - ni] * sm[x0 + s - ni];
+        if (i > 0) sum = sum + sm[cx + c - 1] * sm[x0 + s - 1];
+        if (i < ni - 1) sum = sum + sm[cx + c] * sm[x0 + s + 1];
+        if (yhi) sum = sum + sm[cy + y] * sm[x0 + s + ni];
+        if (zhi) sum = sum + sm[cz + c] * sm[xp1 + s];
+        const float d = sm[cd + c];
+        sm[x0 + s] = (d != 0.0f) ? gs_div(sm[cb + c] - sum, d) : 0.0f;
       }
     }
   };
+  auto prolong_add = [&](int q) {
+    if (q < 0 || q >= nk) return;
+    const int xq = oX + m5(q) * xslot, cq = oXC + m5(q) * cplane;
+    for (int r = ty; r < xrows; r += by) {
+      const int crr = ((jr0 + r) >> 1) - cr0;
+      for (int i = tx; i < ni; i += bx) sm[xq + r * ni + i] = sm[xq + r * ni + i] + sm[cq + crr * a.cni + (i >> 1)];
+    }
+  };
+  auto zero_x = [&](int q) {
+    const int xq = oX + m5(q) * xslot;
+    for (int e = tid; e < xrows * ni; e += BLOCK) sm[xq + e] = 0.0f;
+  };
 
-  // prologue: x(k0-2 .. k0), coefficients (k0-1), zp(k0-2, k0-1)
-  issue_x(k0 - 2);
-  issue_x(k0 - 1);
-  issue_x(k0);
-  issue_coef(k0 - 1);
-  issue_zp(k0 - 2);
-  issue_zp(k0 - 1);
-  cp_async_commit();
+  // Copy groups: G0 = x(k0-2), x(k0-1), coefficients (k0-1), zp(k0-2),
+  // zp(k0-1); G1 = x(k0); the step for plane p waits for the group holding
+  // x(p+1) and coefficients (p), then issues x(p+2), coefficients (p+1),
+  // zp(p+1) to land during its relaxation.  Group g completes on
+  // bars[g & 1] in phase (g >> 1) & 1; a barrier is re-armed only after all
+  // threads have waited for its previous phase.
+  double dot = 0.0;
+  bool failed = false;
+  int g_next = 2;
+  if (tid == 0) {
+    issue(0, k0 - 2, k0 - 1, k0 - 2, k0 - 1, k0 - 1);
+    issue(1, k0, -1, -1, -1);
+  }
   for (int p = k0 - 1; p <= kend; ++p) {
-    issue_x(p + 2);
-    issue_coef(p + 1);
-    issue_zp(p + 1);
-    cp_async_commit();
-    cp_async_wait1();
-    __syncthreads();
+    if (p == k0 - 1) {
+      if (!wait_group(0) || !wait_group(1)) { failed = true; break; }
+    } else {
+      if (!wait_group(g_next - 1)) { failed = true; break; }
+    }
+    if (tid == 0) issue(g_next, p + 2, p + 1, p + 1, -1);
+    ++g_next;
     if (PROLONG || ZERO_X) {
       if (p == k0 - 1) {
-        if (PROLONG) { prolong_add(k0 - 2); prolong_add(k0 - 1); }
-        if (ZERO_X) { zero_x(k0 - 2); zero_x(k0 - 1); }
+        if (PROLONG) { prolong_add(k0 - 2); prolong_add(k0 - 1); prolong_add(k0); }
+        if (ZERO_X) { zero_x(k0 - 2); zero_x(k0 - 1); zero_x(k0); }
+      } else {
+        if (PROLONG) prolong_add(p + 1);
+        if (ZERO_X) zero_x(p + 1);
       }
-      if (PROLONG) prolong_add(p + 1);
-      if (ZERO_X) zero_x(p + 1);
       __syncthreads();
     }
     if (p >= 0 && p < nk) relax(p, jred0, jred1, 1);
@@ -413,11 +461,11 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep2_kernel(Sweep2Args<S> a) {
     if (out_plane) relax(q, j0, jout1, 0);
     __syncthreads();
     if (out_plane) {
-      const float4* s4 = reinterpret_cast<const float4*>(X + m5(q) * xslot + (j0 - jr0) * ni);
-      const float4* b4 = reinterpret_cast<const float4*>(B + m3(q) * cslot + (j0 - jred0) * ni);
+      const float4* s4 = reinterpret_cast<const float4*>(sm + oX + m5(q) * xslot + (j0 - jr0) * ni);
+      const float4* b4 = reinterpret_cast<const float4*>(sm + oB + m3(q) * cslot + (j0 - jred0) * ni);
       float4* dst = reinterpret_cast<float4*>(a.x_out + q * sz + j0 * sy);
       const int cnt4 = (jout1 - j0) * ni / 4;
-      for (int e = ty * bx + tx; e < cnt4; e += BLOCK) {
+      for (int e = tid; e < cnt4; e += BLOCK) {
         float4 v = s4[e];
         dst[e] = v;
         if (DOT) {
@@ -425,13 +473,22 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep2_kernel(Sweep2Args<S> a) {
           dot += (double)v.x * bb.x + (double)v.y * bb.y + (double)v.z * bb.z + (double)v.w * bb.w;
         }
       }
-      if (DOT) __syncthreads();
     }
   }
-  cp_async_wait0();
+  const int g = g_next;
+  if (failed) {
+    if (tid == 0) atomicExch(a.error, 1);
+    // drain: the last issued group (and so every earlier one) must land
+    // before the CTA's shared memory is released
+    mbar_wait_bounded(((g - 1) & 1) ? bar1 : bar0, (unsigned)(((g - 1) >> 1) & 1));
+    mbar_wait_bounded(((g - 2) & 1) ? bar1 : bar0, (unsigned)(((g - 2) >> 1) & 1));
+    return;
+  }
+  // drain the copy group issued by the last step (planes beyond the range)
+  wait_group(g - 1);
   if (DOT) {
     double s = block_sum<BLOCK>(dot, red_smem);
-    if (threadIdx.x == 0 && threadIdx.y == 0) a.dot_partial[blockIdx.x + gridDim.x * blockIdx.y] = s;
+    if (tid == 0) a.dot_partial[blockIdx.x + gridDim.x * blockIdx.y] = s;
   }
 }
 

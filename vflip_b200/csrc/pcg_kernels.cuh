@@ -20,6 +20,7 @@ struct PcgScalars {
   double tol;        // tolerance_factor * |rhs|_inf
   int converged;     // res <= tol
   int bad_rho;       // rho == 0 or NaN
+  int kernel_error;  // host copy of the smoother's timeout flag
   unsigned int done_blocks[4];  // last-block-done counters, one per reduction kind
 };
 

@@ -49,6 +49,7 @@ struct vflip_ctx {
   PcgScalars* st = nullptr;         // device
   PcgScalars* st_host = nullptr;    // pinned
   double* partials = nullptr;       // device, kMaxPartials
+  int* d_error = nullptr;           // device, set by kernels whose bounded waits timed out
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0.0;
   int num_sms = 148;
@@ -193,26 +194,26 @@ int launch_sweep_t(vflip_ctx* ctx, const SweepArgs<S, V>& a, const SweepShape& s
 // Shape of the pipelined sweep (rbgs_sweep2_kernel): rows per tile from a
 // shared-memory budget, persistent CTAs over equal shares of the level's
 // (row tile, plane) pairs.
-struct Sweep2Shape {
+struct TmaShape {
   int tyo, gy, zlen, gz, crows_max, bx, by;
   size_t smem;
 };
 
-constexpr size_t kSweep2Smem = 224 * 1024;
-constexpr int kSweep2Block = 512;
+constexpr size_t kTmaSmem = 224 * 1024;
+constexpr int kTmaBlock = 512;
 
-// Tile shape: choose (rows per tile, planes per CTA) so that every CTA of a
-// launch is resident at once (one per SM) and marches in step with the CTAs
-// of the neighbouring row tiles (their halo rows then come from L2), trading
-// the 4 redundant halo planes of each plane range against load balance.
-template <typename S>
-bool sweep2_shape(const Dims& d, const Dims* cd, bool prolong, int num_sms, Sweep2Shape& o) {
-  if (d.ni % 4 != 0 || (d.ni * sizeof(S)) % 16 != 0) return false;
+// Tile shape of the TMA-pipelined sweep: choose (rows per tile, planes per
+// CTA) so that every CTA of a launch is resident at once (one per SM) and
+// marches in step with the CTAs of the neighbouring row tiles (their halo
+// rows then come from L2), trading the 4 redundant halo planes of each plane
+// range against load balance.
+bool tma_shape(const Dims& d, const Dims* cd, bool prolong, int num_sms, TmaShape& o) {
+  if (d.ni % 4 != 0) return false;
   if (prolong && (!cd || cd->ni % 4 != 0)) return false;
   const int cni = prolong ? cd->ni : 0;
   int tyo_max = 0;
   for (int t = 1; t <= d.nj; ++t) {
-    if (sweep2_smem_bytes<S>(d.ni, t, prolong ? (t + 4 + 3) / 2 : 0, cni) > kSweep2Smem) break;
+    if (4 * tma_sweep_smem_floats(d.ni, t, prolong ? (t + 7) / 2 : 0, cni) > kTmaSmem) break;
     tyo_max = t;
   }
   if (tyo_max < 1) return false;
@@ -235,22 +236,22 @@ bool sweep2_shape(const Dims& d, const Dims* cd, bool prolong, int num_sms, Swee
       o.gz = gz;
     }
   }
-  o.crows_max = prolong ? (o.tyo + 4 + 3) / 2 : 0;
-  o.smem = sweep2_smem_bytes<S>(d.ni, o.tyo, o.crows_max, cni);
+  o.crows_max = prolong ? (o.tyo + 7) / 2 : 0;
+  o.smem = 4 * tma_sweep_smem_floats(d.ni, o.tyo, o.crows_max, cni);
   int P = (d.ni + 1) / 2;
   int bx = 1;
   while (bx < P && bx < 128) bx <<= 1;
   o.bx = bx;
-  o.by = kSweep2Block / bx;
-  return o.smem <= kSweep2Smem;
+  o.by = kTmaBlock / bx;
+  return o.smem <= kTmaSmem;
 }
 
-template <typename S, bool Z, bool P, bool D>
-int launch_sweep2_t(vflip_ctx* ctx, const Sweep2Args<S>& a, const Sweep2Shape& sh) {
-  auto kern = rbgs_sweep2_kernel<S, Z, P, D, kSweep2Block>;
+template <bool Z, bool P, bool D>
+int launch_tma_t(vflip_ctx* ctx, const TmaSweepArgs& a, const TmaShape& sh) {
+  auto kern = rbgs_sweep_tma_kernel<Z, P, D, kTmaBlock>;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSweep2Smem);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmem);
     attr_set = true;
   }
   const bool timed = ctx->profiling && (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n;
@@ -272,23 +273,24 @@ int launch_sweep2_t(vflip_ctx* ctx, const Sweep2Args<S>& a, const Sweep2Shape& s
   return VFLIP_OK;
 }
 
-// FP32-vector sweeps take the pipelined kernel when the row layout allows.
+// FP32 sweeps take the TMA-pipelined kernel when the row layout allows.
 template <typename S, typename V>
-int sweep2(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_out, const V* xc, const Dims* cd,
-           double* dot_partial, int* nblocks_out, bool* used) {
+int sweep_tma(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_out, const V* xc,
+              const Dims* cd, double* dot_partial, int* nblocks_out, bool* used) {
   *used = false;
-  if (!std::is_same<V, float>::value || ctx->cfg.sweep_kernel == 1) return VFLIP_OK;
-  Sweep2Shape sh;
+  if (!std::is_same<V, float>::value || !std::is_same<S, float>::value || ctx->cfg.sweep_kernel == 1)
+    return VFLIP_OK;
+  TmaShape sh;
   const bool pro = xc != nullptr;
-  if (!sweep2_shape<S>(L.d, cd, pro, ctx->num_sms, sh)) return VFLIP_OK;
-  Sweep2Args<S> a;
+  if (!tma_shape(L.d, cd, pro, ctx->num_sms, sh)) return VFLIP_OK;
+  TmaSweepArgs a;
   a.x_in = (const float*)x_in;
   a.x_out = (float*)x_out;
   a.b = (const float*)b;
-  a.diag = L.diag;
-  a.xp = L.xp;
-  a.yp = L.yp;
-  a.zp = L.zp;
+  a.diag = (const float*)L.diag;
+  a.xp = (const float*)L.xp;
+  a.yp = (const float*)L.yp;
+  a.zp = (const float*)L.zp;
   a.xc = (const float*)xc;
   a.ni = L.d.ni;
   a.nj = L.d.nj;
@@ -299,15 +301,16 @@ int sweep2(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x
   a.zlen = sh.zlen;
   a.crows_max = sh.crows_max;
   a.dot_partial = dot_partial;
+  a.error = ctx->d_error;
   if (nblocks_out) *nblocks_out = sh.gy * sh.gz;
   *used = true;
   bool zero = (x_in == nullptr), dot = (dot_partial != nullptr);
-  if (zero && !pro && !dot) return launch_sweep2_t<S, true, false, false>(ctx, a, sh);
-  if (zero && !pro && dot) return launch_sweep2_t<S, true, false, true>(ctx, a, sh);
-  if (!zero && pro && !dot) return launch_sweep2_t<S, false, true, false>(ctx, a, sh);
-  if (!zero && pro && dot) return launch_sweep2_t<S, false, true, true>(ctx, a, sh);
-  if (!zero && !pro && !dot) return launch_sweep2_t<S, false, false, false>(ctx, a, sh);
-  if (!zero && !pro && dot) return launch_sweep2_t<S, false, false, true>(ctx, a, sh);
+  if (zero && !pro && !dot) return launch_tma_t<true, false, false>(ctx, a, sh);
+  if (zero && !pro && dot) return launch_tma_t<true, false, true>(ctx, a, sh);
+  if (!zero && pro && !dot) return launch_tma_t<false, true, false>(ctx, a, sh);
+  if (!zero && pro && dot) return launch_tma_t<false, true, true>(ctx, a, sh);
+  if (!zero && !pro && !dot) return launch_tma_t<false, false, false>(ctx, a, sh);
+  if (!zero && !pro && dot) return launch_tma_t<false, false, true>(ctx, a, sh);
   return ctx->fail(VFLIP_ERR_ARG, "sweep: prolongation needs an incoming x");
 }
 
@@ -318,7 +321,7 @@ int sweep(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_
   using A = typename Num<V>::Acc;
   {
     bool used = false;
-    int rc = sweep2<S, V>(ctx, L, b, x_in, x_out, xc, cd, dot_partial, nblocks_out, &used);
+    int rc = sweep_tma<S, V>(ctx, L, b, x_in, x_out, xc, cd, dot_partial, nblocks_out, &used);
     if (rc || used) return rc;
   }
   SweepShape sh = sweep_shape<A>(L.d, ctx->num_sms);
@@ -581,10 +584,22 @@ int vcycle(vflip_ctx* ctx, Typed<S0, SC, V>& T, const V* r, V* z, bool want_dot)
 }
 
 // ---------------------------------------------------------------- PCG
+// Device-side failure report of the pipelined smoother (a bounded wait that
+// timed out); read after a synchronisation.
+int check_kernel_error(vflip_ctx* ctx, int err_host) {
+  if (err_host) {
+    cudaMemsetAsync(ctx->d_error, 0, sizeof(int), ctx->stream);
+    return ctx->fail(VFLIP_ERR_CUDA, "smoother copy pipeline timed out");
+  }
+  return VFLIP_OK;
+}
+
 int read_scalars(vflip_ctx* ctx) {
   VF_CUDA(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(PcgScalars), cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(&ctx->st_host->kernel_error, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost,
+                          ctx->stream));
   VF_CUDA(cudaStreamSynchronize(ctx->stream));
-  return VFLIP_OK;
+  return check_kernel_error(ctx, ctx->st_host->kernel_error);
 }
 
 template <typename S0, typename SC, typename V>
@@ -758,6 +773,8 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
   ctx->stream = (cudaStream_t)ctx->cfg.stream;
   if (cudaMalloc(&ctx->st, sizeof(PcgScalars)) != cudaSuccess) return bad(VFLIP_ERR_NOMEM);
   if (cudaMalloc(&ctx->partials, sizeof(double) * kMaxPartials) != cudaSuccess) return bad(VFLIP_ERR_NOMEM);
+  if (cudaMalloc(&ctx->d_error, sizeof(int)) != cudaSuccess) return bad(VFLIP_ERR_NOMEM);
+  if (cudaMemset(ctx->d_error, 0, sizeof(int)) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
   if (cudaMallocHost(&ctx->st_host, sizeof(PcgScalars)) != cudaSuccess) return bad(VFLIP_ERR_NOMEM);
   if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
     return bad(VFLIP_ERR_CUDA);
@@ -771,6 +788,7 @@ int vflip_destroy(vflip_ctx* ctx) {
   for (auto& kv : ctx->bufs) cudaFree(kv.second.first);
   if (ctx->st) cudaFree(ctx->st);
   if (ctx->partials) cudaFree(ctx->partials);
+  if (ctx->d_error) cudaFree(ctx->d_error);
   if (ctx->st_host) cudaFreeHost(ctx->st_host);
   for (auto& pe : ctx->prof_events) {
     cudaEventDestroy(pe.first);
@@ -786,8 +804,12 @@ const char* vflip_last_error(const vflip_ctx* ctx) { return ctx ? ctx->err.c_str
 
 int vflip_synchronize(vflip_ctx* ctx) {
   if (!ctx) return VFLIP_ERR_ARG;
+  int err = 0;
+  VF_CUDA(cudaMemcpyAsync(&ctx->st_host->kernel_error, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost,
+                          ctx->stream));
   VF_CUDA(cudaStreamSynchronize(ctx->stream));
-  return VFLIP_OK;
+  err = ctx->st_host->kernel_error;
+  return check_kernel_error(ctx, err);
 }
 
 double vflip_last_ms(const vflip_ctx* ctx) { return ctx ? ctx->last_ms : 0.0; }
