@@ -63,8 +63,16 @@ typedef struct {
   int coarsest_max_unknowns; /* coarsen while unknowns exceed this, default 4096 (SS/GeometricLevelGen.h:46); max 4096 */
   int device;                /* CUDA device ordinal, default 0 */
   void* stream;              /* cudaStream_t to order work on; NULL: the CUDA default stream */
-  int sweep_kernel;          /* smoother kernel: 0 = pipelined (cp.async plane staging) where the row length
-                                allows it, else the plain fused kernel; 1 = always the plain fused kernel */
+  int sweep_kernel;          /* smoother kernel: 0 = TMA-pipelined (bulk plane copies) for FP32 levels whose
+                                row length is a multiple of 4, else the plain fused kernel; 1 = always the
+                                plain fused kernel */
+  /* Tile shape of the TMA-pipelined smoother, 0 = automatic (tuning knobs;
+   * vflip_b200/tune.py searches them): copy groups in flight (1..3), output
+   * rows per tile, plane ranges per launch, resident CTAs per SM (1..2). */
+  int smoother_depth;
+  int smoother_tile_rows;
+  int smoother_plane_ranges;
+  int smoother_ctas_per_sm;
 } vflip_config;
 
 typedef struct {

@@ -29,7 +29,9 @@ class SolveStatsC(C.Structure):
 class ConfigC(C.Structure):
     _fields_ = [("precision", C.c_int), ("pre_sweeps", C.c_int), ("post_sweeps", C.c_int),
                 ("coarse_sweeps", C.c_int), ("coarsest_max_unknowns", C.c_int), ("device", C.c_int),
-                ("stream", C.c_void_p), ("sweep_kernel", C.c_int)]
+                ("stream", C.c_void_p), ("sweep_kernel", C.c_int), ("smoother_depth", C.c_int),
+                ("smoother_tile_rows", C.c_int), ("smoother_plane_ranges", C.c_int),
+                ("smoother_ctas_per_sm", C.c_int)]
 
 
 # name -> (restype, argtypes); mirrors include/vflip.h one for one

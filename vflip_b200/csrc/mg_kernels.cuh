@@ -257,16 +257,23 @@ struct TmaSweepArgs {
   int cni, cnj;
   int tyo;        // output rows per tile; blockIdx.x = row tile
   int zlen;       // planes per CTA; blockIdx.y = plane range
+  int depth;      // copy groups in flight (prefetch distance in planes), 1..3
   int crows_max;  // staged coarse rows per slot
   double* dot_partial;
   int* error;
 };
 
-// Floats of shared memory for a tile of `tyo` output rows: x needs the red
-// ring and its neighbours (tyo + 4 rows), b/diag/xp/zp the red rows
-// (tyo + 2), yp one more row below them (tyo + 3).
-__host__ __device__ constexpr size_t tma_sweep_smem_floats(int ni, int tyo, int crows, int cni) {
-  return (size_t)ni * (5 * (tyo + 4) + 3 * 3 * (tyo + 2) + 3 * (tyo + 3) + 4 * (tyo + 2)) + (size_t)5 * crows * cni;
+constexpr int kTmaMaxDepth = 3;
+
+// Floats of shared memory for a tile of `tyo` output rows and prefetch depth
+// D: x needs the red ring and its neighbours (tyo + 4 rows) for planes
+// p-2 .. p+1 plus D in flight; b/diag/xp (tyo + 2 rows) and yp (tyo + 3)
+// for planes p-1, p plus D; zp (tyo + 2) for p-2 .. p plus D; coarse x
+// follows the x ring.
+__host__ __device__ constexpr size_t tma_sweep_smem_floats(int ni, int tyo, int depth, int crows, int cni) {
+  return (size_t)ni * ((4 + depth) * (tyo + 4) + 3 * (2 + depth) * (tyo + 2) + (2 + depth) * (tyo + 3) +
+                       (3 + depth) * (tyo + 2)) +
+         (size_t)(4 + depth) * crows * cni;
 }
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -302,16 +309,17 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 template <bool ZERO_X, bool PROLONG, bool DOT, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
   extern __shared__ __align__(128) float sm[];
-  __shared__ __align__(8) unsigned long long bars[2];
+  constexpr int NB = kTmaMaxDepth + 2;  // mbarrier ring
+  __shared__ __align__(8) unsigned long long bars[NB];
   __shared__ double red_smem[BLOCK / 32];
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-  const int ni = a.ni, nj = a.nj, nk = a.nk, tyo = a.tyo;
+  const int ni = a.ni, nj = a.nj, nk = a.nk, tyo = a.tyo, D = a.depth;
   const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
   const int xslot = (tyo + 4) * ni, cslot = (tyo + 2) * ni, yslot = (tyo + 3) * ni;
   const int cplane = a.crows_max * a.cni;
-  // slot bases (float offsets into sm)
-  const int oX = 0, oB = oX + 5 * xslot, oD = oB + 3 * cslot, oXP = oD + 3 * cslot, oYP = oXP + 3 * cslot,
-            oZP = oYP + 3 * yslot, oXC = oZP + 4 * cslot;
+  const int RX = 4 + D, RC = 2 + D, RZ = 3 + D;  // ring lengths
+  const int oX = 0, oB = oX + RX * xslot, oD = oB + RC * cslot, oXP = oD + RC * cslot, oYP = oXP + RC * cslot,
+            oZP = oYP + RC * yslot, oXC = oZP + RZ * cslot;
   const int P = (ni + 1) / 2;
   const int tx = threadIdx.x, ty = threadIdx.y, bx = blockDim.x, by = blockDim.y;
 
@@ -325,70 +333,66 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
   const int xrows = jr1 - jr0, crows = jred1 - jred0, yrows = jred1 - jy0;
   const int cr0 = jr0 >> 1, cr1 = ((jr1 - 1) >> 1) + 1;
 
-  const unsigned bar0 = smem_u32(&bars[0]), bar1 = smem_u32(&bars[1]);
   const unsigned sbase = smem_u32(sm);
+  const unsigned bar_base = smem_u32(&bars[0]);
   if (tid == 0) {
-    mbar_init(bar0, 1);
-    mbar_init(bar1, 1);
+    for (int q = 0; q < NB; ++q) mbar_init(bar_base + 8u * q, 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
 
-  auto m5 = [](int q) { return (q % 5 + 5) % 5; };
-  auto m3 = [](int q) { return (q % 3 + 3) % 3; };
-  // thread 0: one copy group (x plane qx, coefficient plane qc, zp planes
-  // qz0 and qz1), completion on bars[g & 1]
-  auto issue = [&](int g, int qx, int qc, int qz0, int qz1, int qx2 = -1) {
-    const unsigned bar = (g & 1) ? bar1 : bar0;
-    unsigned bytes = 0;
-    const bool hx = !ZERO_X && qx >= 0 && qx < nk;
-    const bool hx2 = !ZERO_X && qx2 >= 0 && qx2 < nk;
+  // ring slots (planes may be negative before the domain)
+  auto rs = [](int q, int r) { return (q % r + r) % r; };
+  auto xo = [&](int q) { return oX + rs(q, RX) * xslot; };
+  auto xco = [&](int q) { return oXC + rs(q, RX) * cplane; };
+
+  // thread 0: copy group g, on mbarrier g % NB in phase (g / NB) & 1; x planes
+  // qx0/qx1, coefficient plane qc, zp planes qz0/qz1 (out of range: skipped)
+  auto issue = [&](int g, int qx0, int qx1, int qc, int qz0, int qz1) {
+    const unsigned bar = bar_base + 8u * (unsigned)(g % NB);
+    const bool hx0 = !ZERO_X && qx0 >= 0 && qx0 < nk, hx1 = !ZERO_X && qx1 >= 0 && qx1 < nk;
     const bool hc = qc >= 0 && qc < nk;
     const bool hz0 = qz0 >= 0 && qz0 < nk, hz1 = qz1 >= 0 && qz1 < nk;
-    if (hx) bytes += xrows * ni * 4 + (PROLONG ? (cr1 - cr0) * a.cni * 4 : 0);
-    if (hx2) bytes += xrows * ni * 4 + (PROLONG ? (cr1 - cr0) * a.cni * 4 : 0);
-    if (hc) bytes += (3 * crows + yrows) * ni * 4;
-    if (hz0) bytes += crows * ni * 4;
-    if (hz1) bytes += crows * ni * 4;
+    const unsigned xb = xrows * ni * 4 + (PROLONG ? (cr1 - cr0) * a.cni * 4 : 0);
+    unsigned bytes = (hx0 ? xb : 0) + (hx1 ? xb : 0) + (hc ? (3 * crows + yrows) * ni * 4 : 0) +
+                     (hz0 ? crows * ni * 4 : 0) + (hz1 ? crows * ni * 4 : 0);
     fence_proxy_async();
     mbar_expect_tx(bar, bytes);
-    if (hx) {
-      tma_bulk_g2s(sbase + 4u * (oX + m5(qx) * xslot), a.x_in + qx * sz + jr0 * sy, xrows * ni * 4, bar);
+    for (int h = 0; h < 2; ++h) {
+      const int qx = h ? qx1 : qx0;
+      if (!(h ? hx1 : hx0)) continue;
+      tma_bulk_g2s(sbase + 4u * xo(qx), a.x_in + qx * sz + jr0 * sy, xrows * ni * 4, bar);
       if (PROLONG)
-        tma_bulk_g2s(sbase + 4u * (oXC + m5(qx) * cplane),
-                     a.xc + (size_t)(qx >> 1) * a.cni * a.cnj + (size_t)cr0 * a.cni, (cr1 - cr0) * a.cni * 4, bar);
-    }
-    if (hx2) {
-      tma_bulk_g2s(sbase + 4u * (oX + m5(qx2) * xslot), a.x_in + qx2 * sz + jr0 * sy, xrows * ni * 4, bar);
-      if (PROLONG)
-        tma_bulk_g2s(sbase + 4u * (oXC + m5(qx2) * cplane),
-                     a.xc + (size_t)(qx2 >> 1) * a.cni * a.cnj + (size_t)cr0 * a.cni, (cr1 - cr0) * a.cni * 4, bar);
+        tma_bulk_g2s(sbase + 4u * xco(qx), a.xc + (size_t)(qx >> 1) * a.cni * a.cnj + (size_t)cr0 * a.cni,
+                     (cr1 - cr0) * a.cni * 4, bar);
     }
     if (hc) {
       const size_t o = qc * sz + jred0 * sy;
-      const int s3 = m3(qc);
-      tma_bulk_g2s(sbase + 4u * (oB + s3 * cslot), a.b + o, crows * ni * 4, bar);
-      tma_bulk_g2s(sbase + 4u * (oD + s3 * cslot), a.diag + o, crows * ni * 4, bar);
-      tma_bulk_g2s(sbase + 4u * (oXP + s3 * cslot), a.xp + o, crows * ni * 4, bar);
-      tma_bulk_g2s(sbase + 4u * (oYP + s3 * yslot), a.yp + qc * sz + jy0 * sy, yrows * ni * 4, bar);
+      const int sc = rs(qc, RC);
+      tma_bulk_g2s(sbase + 4u * (oB + sc * cslot), a.b + o, crows * ni * 4, bar);
+      tma_bulk_g2s(sbase + 4u * (oD + sc * cslot), a.diag + o, crows * ni * 4, bar);
+      tma_bulk_g2s(sbase + 4u * (oXP + sc * cslot), a.xp + o, crows * ni * 4, bar);
+      tma_bulk_g2s(sbase + 4u * (oYP + sc * yslot), a.yp + qc * sz + jy0 * sy, yrows * ni * 4, bar);
     }
-    if (hz0) tma_bulk_g2s(sbase + 4u * (oZP + (qz0 & 3) * cslot), a.zp + qz0 * sz + jred0 * sy, crows * ni * 4, bar);
-    if (hz1) tma_bulk_g2s(sbase + 4u * (oZP + (qz1 & 3) * cslot), a.zp + qz1 * sz + jred0 * sy, crows * ni * 4, bar);
+    for (int h = 0; h < 2; ++h) {
+      const int qz = h ? qz1 : qz0;
+      if (!(h ? hz1 : hz0)) continue;
+      tma_bulk_g2s(sbase + 4u * (oZP + rs(qz, RZ) * cslot), a.zp + qz * sz + jred0 * sy, crows * ni * 4, bar);
+    }
   };
   // all threads: wait for group g; block-uniform result
   auto wait_group = [&](int g) -> bool {
-    const unsigned bar = (g & 1) ? bar1 : bar0;
-    const bool ok = mbar_wait_bounded(bar, (unsigned)((g >> 1) & 1));
+    const bool ok = mbar_wait_bounded(bar_base + 8u * (unsigned)(g % NB), (unsigned)((g / NB) & 1));
     return __syncthreads_and(ok) != 0;
   };
 
   // relax colour `odd` of plane p on rows [r0, r1): the reference's row sum
   // in column order (-z, -y, -x, +x, +y, +z), then (b - sum) / diag
   auto relax = [&](int p, int r0, int r1, int odd) {
-    const int x0 = oX + m5(p) * xslot, xm1 = oX + m5(p - 1) * xslot, xp1 = oX + m5(p + 1) * xslot;
-    const int s3 = m3(p);
-    const int cb = oB + s3 * cslot, cd = oD + s3 * cslot, cx = oXP + s3 * cslot, cy = oYP + s3 * yslot;
-    const int cz = oZP + (p & 3) * cslot, czm = oZP + ((p - 1) & 3) * cslot;
+    const int x0 = xo(p), xm1 = xo(p - 1), xp1 = xo(p + 1);
+    const int sc = rs(p, RC);
+    const int cb = oB + sc * cslot, cd = oD + sc * cslot, cx = oXP + sc * cslot, cy = oYP + sc * yslot;
+    const int cz = oZP + rs(p, RZ) * cslot, czm = oZP + rs(p - 1, RZ) * cslot;
     const bool zlo = p > 0, zhi = p < nk - 1;
     for (int j = r0 + ty; j < r1; j += by) {
       const int sh = odd ? ((j + p + 1) & 1) : ((j + p) & 1);
@@ -412,46 +416,42 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
   };
   auto prolong_add = [&](int q) {
     if (q < 0 || q >= nk) return;
-    const int xq = oX + m5(q) * xslot, cq = oXC + m5(q) * cplane;
+    const int xq = xo(q), cq = xco(q);
     for (int r = ty; r < xrows; r += by) {
       const int crr = ((jr0 + r) >> 1) - cr0;
       for (int i = tx; i < ni; i += bx) sm[xq + r * ni + i] = sm[xq + r * ni + i] + sm[cq + crr * a.cni + (i >> 1)];
     }
   };
   auto zero_x = [&](int q) {
-    const int xq = oX + m5(q) * xslot;
+    const int xq = xo(q);
     for (int e = tid; e < xrows * ni; e += BLOCK) sm[xq + e] = 0.0f;
   };
 
-  // Copy groups: G0 = x(k0-2), x(k0-1), coefficients (k0-1), zp(k0-2),
-  // zp(k0-1); G1 = x(k0); the step for plane p waits for the group holding
-  // x(p+1) and coefficients (p), then issues x(p+2), coefficients (p+1),
-  // zp(p+1) to land during its relaxation.  Group g completes on
-  // bars[g & 1] in phase (g >> 1) & 1; a barrier is re-armed only after all
-  // threads have waited for its previous phase.
+  // Copy groups: G0 = x(k0-2), x(k0-1), zp(k0-2); then H(q) for q >= k0-1
+  // carries x(q+1), coefficients (q), zp(q) and is group q - k0 + 2.  The
+  // step for plane p waits for H(p) (and G0 first), then issues H(p+D), so
+  // D groups stream in during its relaxation.
   double dot = 0.0;
   bool failed = false;
-  int g_next = 2;
-  if (tid == 0) {
-    issue(0, k0 - 2, k0 - 1, k0 - 2, k0 - 1, k0 - 1);
-    issue(1, k0, -1, -1, -1);
-  }
+  int issued = 0;
+  auto issue_h = [&](int q) {
+    if (tid == 0) issue(q - k0 + 2, q + 1, -1, q, q, -1);
+    issued = q - k0 + 3;
+  };
+  if (tid == 0) issue(0, k0 - 2, k0 - 1, -1, k0 - 2, -1);
+  issued = 1;
+  for (int q = k0 - 1; q < k0 - 1 + D && q <= kend; ++q) issue_h(q);
   for (int p = k0 - 1; p <= kend; ++p) {
-    if (p == k0 - 1) {
-      if (!wait_group(0) || !wait_group(1)) { failed = true; break; }
-    } else {
-      if (!wait_group(g_next - 1)) { failed = true; break; }
-    }
-    if (tid == 0) issue(g_next, p + 2, p + 1, p + 1, -1);
-    ++g_next;
+    if (p == k0 - 1 && !wait_group(0)) { failed = true; break; }
+    if (!wait_group(p - k0 + 2)) { failed = true; break; }
+    if (p + D <= kend) issue_h(p + D);
     if (PROLONG || ZERO_X) {
       if (p == k0 - 1) {
-        if (PROLONG) { prolong_add(k0 - 2); prolong_add(k0 - 1); prolong_add(k0); }
-        if (ZERO_X) { zero_x(k0 - 2); zero_x(k0 - 1); zero_x(k0); }
-      } else {
-        if (PROLONG) prolong_add(p + 1);
-        if (ZERO_X) zero_x(p + 1);
+        if (PROLONG) { prolong_add(k0 - 2); prolong_add(k0 - 1); }
+        if (ZERO_X) { zero_x(k0 - 2); zero_x(k0 - 1); }
       }
+      if (PROLONG) prolong_add(p + 1);
+      if (ZERO_X) zero_x(p + 1);
       __syncthreads();
     }
     if (p >= 0 && p < nk) relax(p, jred0, jred1, 1);
@@ -461,8 +461,8 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
     if (out_plane) relax(q, j0, jout1, 0);
     __syncthreads();
     if (out_plane) {
-      const float4* s4 = reinterpret_cast<const float4*>(sm + oX + m5(q) * xslot + (j0 - jr0) * ni);
-      const float4* b4 = reinterpret_cast<const float4*>(sm + oB + m3(q) * cslot + (j0 - jred0) * ni);
+      const float4* s4 = reinterpret_cast<const float4*>(sm + xo(q) + (j0 - jr0) * ni);
+      const float4* b4 = reinterpret_cast<const float4*>(sm + oB + rs(q, RC) * cslot + (j0 - jred0) * ni);
       float4* dst = reinterpret_cast<float4*>(a.x_out + q * sz + j0 * sy);
       const int cnt4 = (jout1 - j0) * ni / 4;
       for (int e = tid; e < cnt4; e += BLOCK) {
@@ -475,17 +475,14 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
       }
     }
   }
-  const int g = g_next;
   if (failed) {
     if (tid == 0) atomicExch(a.error, 1);
-    // drain: the last issued group (and so every earlier one) must land
-    // before the CTA's shared memory is released
-    mbar_wait_bounded(((g - 1) & 1) ? bar1 : bar0, (unsigned)(((g - 1) >> 1) & 1));
-    mbar_wait_bounded(((g - 2) & 1) ? bar1 : bar0, (unsigned)(((g - 2) >> 1) & 1));
+    // drain: every issued group must land before the CTA's shared memory is
+    // released (bounded again)
+    for (int g = max(0, issued - NB); g < issued; ++g)
+      mbar_wait_bounded(bar_base + 8u * (unsigned)(g % NB), (unsigned)((g / NB) & 1));
     return;
   }
-  // drain the copy group issued by the last step (planes beyond the range)
-  wait_group(g - 1);
   if (DOT) {
     double s = block_sum<BLOCK>(dot, red_smem);
     if (tid == 0) a.dot_partial[blockIdx.x + gridDim.x * blockIdx.y] = s;

@@ -195,38 +195,46 @@ int launch_sweep_t(vflip_ctx* ctx, const SweepArgs<S, V>& a, const SweepShape& s
 // shared-memory budget, persistent CTAs over equal shares of the level's
 // (row tile, plane) pairs.
 struct TmaShape {
-  int tyo, gy, zlen, gz, crows_max, bx, by;
+  int tyo, gy, zlen, gz, depth, crows_max, bx, by;
   size_t smem;
 };
 
-constexpr size_t kTmaSmem = 224 * 1024;
+constexpr size_t kTmaSmemMax = 227 * 1024 - 1024;  // opt-in limit minus the static part
 constexpr int kTmaBlock = 512;
 
-// Tile shape of the TMA-pipelined sweep: choose (rows per tile, planes per
-// CTA) so that every CTA of a launch is resident at once (one per SM) and
-// marches in step with the CTAs of the neighbouring row tiles (their halo
-// rows then come from L2), trading the 4 redundant halo planes of each plane
-// range against load balance.
-bool tma_shape(const Dims& d, const Dims* cd, bool prolong, int num_sms, TmaShape& o) {
+// Tile shape of the TMA-pipelined sweep.  Rows per tile, plane ranges and
+// copy depth are chosen so that every CTA of a launch is resident at once
+// (ctas_per_sm per SM) and marches in step with the CTAs of the neighbouring
+// row tiles (their halo rows then come from L2); the 4 redundant halo planes
+// of each plane range are traded against load balance.  Fields of the
+// context configuration override the choice (0 = automatic).
+bool tma_shape(const vflip_config& cfg, const Dims& d, const Dims* cd, bool prolong, int num_sms, TmaShape& o) {
   if (d.ni % 4 != 0) return false;
   if (prolong && (!cd || cd->ni % 4 != 0)) return false;
   const int cni = prolong ? cd->ni : 0;
+  const int depth = cfg.smoother_depth > 0 ? std::min(cfg.smoother_depth, kTmaMaxDepth) : 2;
+  const int cps = cfg.smoother_ctas_per_sm > 0 ? std::min(cfg.smoother_ctas_per_sm, 2) : 1;
+  const size_t budget = cps == 1 ? kTmaSmemMax : kTmaSmemMax / 2 - 1024;
+  auto bytes = [&](int t) { return 4 * tma_sweep_smem_floats(d.ni, t, depth, prolong ? (t + 7) / 2 : 0, cni); };
   int tyo_max = 0;
   for (int t = 1; t <= d.nj; ++t) {
-    if (4 * tma_sweep_smem_floats(d.ni, t, prolong ? (t + 7) / 2 : 0, cni) > kTmaSmem) break;
+    if (bytes(t) > budget) break;
     tyo_max = t;
   }
   if (tyo_max < 1) return false;
+  const int slots = num_sms * cps;
   double best = 1e30;
   for (int nzr = 1; nzr <= std::min(d.nk, 16); ++nzr) {
-    int gy_target = std::max(1, num_sms / nzr);
+    int gy_target = std::max(1, slots / nzr);
     int tyo = std::max((d.nj + gy_target - 1) / gy_target, 1);
     if (tyo > tyo_max) tyo = tyo_max;
+    if (cfg.smoother_tile_rows > 0) tyo = std::min(cfg.smoother_tile_rows, tyo_max);
+    if (cfg.smoother_plane_ranges > 0 && nzr != std::min(cfg.smoother_plane_ranges, d.nk)) continue;
     int gy = (d.nj + tyo - 1) / tyo;
     int zlen = (d.nk + nzr - 1) / nzr;
     int gz = (d.nk + zlen - 1) / zlen;
-    double waves = std::ceil((double)gy * gz / num_sms);
-    double util = (double)gy * gz / (waves * num_sms);
+    double waves = std::ceil((double)gy * gz / slots);
+    double util = (double)gy * gz / (waves * slots);
     double cost = (1.0 + 4.0 / zlen) * (1.0 + 4.0 / tyo * 0.15) / util;
     if (cost < best) {
       best = cost;
@@ -236,14 +244,16 @@ bool tma_shape(const Dims& d, const Dims* cd, bool prolong, int num_sms, TmaShap
       o.gz = gz;
     }
   }
+  if (best >= 1e30) return false;
+  o.depth = depth;
   o.crows_max = prolong ? (o.tyo + 7) / 2 : 0;
-  o.smem = 4 * tma_sweep_smem_floats(d.ni, o.tyo, o.crows_max, cni);
+  o.smem = bytes(o.tyo);
   int P = (d.ni + 1) / 2;
   int bx = 1;
   while (bx < P && bx < 128) bx <<= 1;
   o.bx = bx;
   o.by = kTmaBlock / bx;
-  return o.smem <= kTmaSmem;
+  return o.smem <= budget;
 }
 
 template <bool Z, bool P, bool D>
@@ -251,7 +261,7 @@ int launch_tma_t(vflip_ctx* ctx, const TmaSweepArgs& a, const TmaShape& sh) {
   auto kern = rbgs_sweep_tma_kernel<Z, P, D, kTmaBlock>;
   static bool attr_set = false;
   if (!attr_set) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmem);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemMax);
     attr_set = true;
   }
   const bool timed = ctx->profiling && (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n;
@@ -282,7 +292,7 @@ int sweep_tma(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V
     return VFLIP_OK;
   TmaShape sh;
   const bool pro = xc != nullptr;
-  if (!tma_shape(L.d, cd, pro, ctx->num_sms, sh)) return VFLIP_OK;
+  if (!tma_shape(ctx->cfg, L.d, cd, pro, ctx->num_sms, sh)) return VFLIP_OK;
   TmaSweepArgs a;
   a.x_in = (const float*)x_in;
   a.x_out = (float*)x_out;
@@ -299,6 +309,7 @@ int sweep_tma(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V
   a.cnj = cd ? cd->nj : 0;
   a.tyo = sh.tyo;
   a.zlen = sh.zlen;
+  a.depth = sh.depth;
   a.crows_max = sh.crows_max;
   a.dot_partial = dot_partial;
   a.error = ctx->d_error;
@@ -750,6 +761,10 @@ void vflip_config_default(vflip_config* cfg) {
   cfg->device = 0;
   cfg->stream = nullptr;
   cfg->sweep_kernel = 0;
+  cfg->smoother_depth = 0;
+  cfg->smoother_tile_rows = 0;
+  cfg->smoother_plane_ranges = 0;
+  cfg->smoother_ctas_per_sm = 0;
 }
 
 int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
@@ -764,7 +779,9 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
   };
   if (ctx->cfg.pre_sweeps < 0 || ctx->cfg.post_sweeps < 0 || ctx->cfg.coarse_sweeps < 0 ||
       ctx->cfg.coarsest_max_unknowns < 1 || ctx->cfg.coarsest_max_unknowns > 4096 || ctx->cfg.precision < 0 ||
-      ctx->cfg.precision > 2 || ctx->cfg.sweep_kernel < 0 || ctx->cfg.sweep_kernel > 1)
+      ctx->cfg.precision > 2 || ctx->cfg.sweep_kernel < 0 || ctx->cfg.sweep_kernel > 1 ||
+      ctx->cfg.smoother_depth < 0 || ctx->cfg.smoother_tile_rows < 0 || ctx->cfg.smoother_plane_ranges < 0 ||
+      ctx->cfg.smoother_ctas_per_sm < 0)
     return bad(VFLIP_ERR_ARG);
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);

@@ -1,0 +1,103 @@
+"""Autotuner for the TMA-pipelined smoother's tile shape.
+
+    python -m vflip_b200.tune [--n 256] [--out vflip_b200/tuning.json]
+
+For one grid size it times plain-FP32 MGPCG solves of the plume operator
+(box walls + sphere obstacle) under each candidate shape - copy groups in
+flight, output rows per tile, plane ranges per launch, resident CTAs per SM -
+reading the fine-level smoother's launch times from the library's own CUDA
+events (vflip_set_profiling), and records the fastest shape per grid size in
+a JSON cache that vflip_b200.plume.PlumeSim and bench.py pass to the solver.
+"""
+import argparse
+import json
+import os
+
+import numpy as np
+import torch
+
+from . import scenes
+from .solver import Solver
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CACHE = os.path.join(HERE, "tuning.json")
+
+# (depth, tile rows, plane ranges, CTAs per SM); 0 = the library's choice
+CANDIDATES = [
+    (1, 0, 0, 1), (2, 0, 0, 1), (3, 0, 0, 1),
+    (2, 5, 3, 1), (2, 6, 3, 1), (3, 4, 4, 1), (2, 4, 4, 1),
+    (1, 2, 2, 2), (2, 2, 2, 2), (1, 3, 3, 2), (2, 1, 2, 2), (1, 2, 0, 2),
+]
+
+
+def load_cache():
+    if os.path.exists(CACHE):
+        with open(CACHE) as f:
+            return json.load(f)
+    return {}
+
+
+def tuned_kwargs(n):
+    """Solver keyword arguments recorded for an n^3 grid (empty if none)."""
+    entry = load_cache().get(str(n))
+    if not entry:
+        return {}
+    d, t, r, c = entry["shape"]
+    return dict(smoother_depth=d, smoother_tile_rows=t, smoother_plane_ranges=r, smoother_ctas_per_sm=c)
+
+
+def problem(n, dev):
+    h = np.float32(1.0 / n)
+    phi = np.minimum(scenes.box_walls_phi(n, n, n, h), scenes.sphere_phi(n, n, n, h, (0.5, 0.5, 0.5), 0.15))
+    rng = np.random.default_rng(0)
+    u, v, w = scenes.random_velocity(n, n, n, rng)
+    zs = [np.zeros(s, np.float32) for s in scenes.face_shapes(n, n, n)]
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    with Solver(precision=1) as s:
+        st, rhs = s.assemble(n, n, n, h, 0.0, T(phi), T(np.zeros((n, n, n), np.int8)), T(zs[0]), T(zs[1]),
+                             T(zs[2]), T(u), T(v), T(w))
+    return st, rhs
+
+
+def measure(st, rhs, shape, reps=2):
+    d, t, r, c = shape
+    with Solver(precision=1, smoother_depth=d, smoother_tile_rows=t, smoother_plane_ranges=r,
+                smoother_ctas_per_sm=c) as s:
+        s.amgpcg_solve(st, rhs, 1e-6, 50)  # warm (allocations)
+        s.set_profiling(True)
+        s.profile_sweeps()
+        tot = 0.0
+        for _ in range(reps):
+            ok, _, stats = s.amgpcg_solve(st, rhs, 1e-6, 50)
+            tot += stats.solve_ms
+        nl, ms, cells = s.profile_sweeps()
+        s.set_profiling(False)
+    return {"shape": list(shape), "sweep_ms": ms / max(nl, 1), "solve_ms": tot / reps, "sweeps": nl,
+            "gbs": 28 * cells / (ms / max(nl, 1)) / 1e6 if nl else None}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--out", default=CACHE)
+    a = ap.parse_args()
+    st, rhs = problem(a.n, "cuda:0")
+    results = []
+    for shape in CANDIDATES:
+        try:
+            r = measure(st, rhs, shape)
+        except Exception as e:  # a shape the library rejects
+            r = {"shape": list(shape), "error": str(e)}
+        results.append(r)
+        print(json.dumps(r), flush=True)
+    ok = [r for r in results if "sweep_ms" in r]
+    best = min(ok, key=lambda r: r["solve_ms"])
+    cache = load_cache()
+    cache[str(a.n)] = {"shape": best["shape"], "sweep_ms": best["sweep_ms"], "solve_ms": best["solve_ms"]}
+    with open(a.out, "w") as f:
+        json.dump(cache, f, indent=1, sort_keys=True)
+    print("best", json.dumps(best))
+
+
+if __name__ == "__main__":
+    main()
