@@ -341,44 +341,41 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
   }
   __syncthreads();
 
-  // ring slots (planes may be negative before the domain)
-  auto rs = [](int q, int r) { return (q % r + r) % r; };
-  auto xo = [&](int q) { return oX + rs(q, RX) * xslot; };
-  auto xco = [&](int q) { return oXC + rs(q, RX) * cplane; };
+  // Ring slots.  Plane q lives in slot q mod ring; the loop carries the slot
+  // of the current plane p in each ring and steps it by one per plane, so no
+  // division runs inside the loop.
+  auto wrap = [](int v, int r) { return v >= r ? v - r : (v < 0 ? v + r : v); };
+  const int p0 = k0 - 1;
+  int px = ((p0 % RX) + RX) % RX, pc = ((p0 % RC) + RC) % RC, pz = ((p0 % RZ) + RZ) % RZ;
 
-  // thread 0: copy group g, on mbarrier g % NB in phase (g / NB) & 1; x planes
-  // qx0/qx1, coefficient plane qc, zp planes qz0/qz1 (out of range: skipped)
-  auto issue = [&](int g, int qx0, int qx1, int qc, int qz0, int qz1) {
+  // thread 0: copy group g on mbarrier g % NB, phase (g / NB) & 1: x planes
+  // qx0/qx1 into x slots sx0/sx1, coefficient plane qc into slot sc, zp plane
+  // qz into slot szs (planes out of the domain are skipped)
+  auto issue = [&](int g, int qx0, int sx0, int qx1, int sx1, int qc, int sc, int qz, int szs) {
     const unsigned bar = bar_base + 8u * (unsigned)(g % NB);
     const bool hx0 = !ZERO_X && qx0 >= 0 && qx0 < nk, hx1 = !ZERO_X && qx1 >= 0 && qx1 < nk;
-    const bool hc = qc >= 0 && qc < nk;
-    const bool hz0 = qz0 >= 0 && qz0 < nk, hz1 = qz1 >= 0 && qz1 < nk;
+    const bool hc = qc >= 0 && qc < nk, hz = qz >= 0 && qz < nk;
     const unsigned xb = xrows * ni * 4 + (PROLONG ? (cr1 - cr0) * a.cni * 4 : 0);
-    unsigned bytes = (hx0 ? xb : 0) + (hx1 ? xb : 0) + (hc ? (3 * crows + yrows) * ni * 4 : 0) +
-                     (hz0 ? crows * ni * 4 : 0) + (hz1 ? crows * ni * 4 : 0);
+    const unsigned bytes = (hx0 ? xb : 0) + (hx1 ? xb : 0) + (hc ? (3 * crows + yrows) * ni * 4 : 0) +
+                           (hz ? crows * ni * 4 : 0);
     fence_proxy_async();
     mbar_expect_tx(bar, bytes);
     for (int h = 0; h < 2; ++h) {
-      const int qx = h ? qx1 : qx0;
+      const int qx = h ? qx1 : qx0, sx = h ? sx1 : sx0;
       if (!(h ? hx1 : hx0)) continue;
-      tma_bulk_g2s(sbase + 4u * xo(qx), a.x_in + qx * sz + jr0 * sy, xrows * ni * 4, bar);
+      tma_bulk_g2s(sbase + 4u * (oX + sx * xslot), a.x_in + qx * sz + jr0 * sy, xrows * ni * 4, bar);
       if (PROLONG)
-        tma_bulk_g2s(sbase + 4u * xco(qx), a.xc + (size_t)(qx >> 1) * a.cni * a.cnj + (size_t)cr0 * a.cni,
+        tma_bulk_g2s(sbase + 4u * (oXC + sx * cplane), a.xc + (size_t)(qx >> 1) * a.cni * a.cnj + (size_t)cr0 * a.cni,
                      (cr1 - cr0) * a.cni * 4, bar);
     }
     if (hc) {
       const size_t o = qc * sz + jred0 * sy;
-      const int sc = rs(qc, RC);
       tma_bulk_g2s(sbase + 4u * (oB + sc * cslot), a.b + o, crows * ni * 4, bar);
       tma_bulk_g2s(sbase + 4u * (oD + sc * cslot), a.diag + o, crows * ni * 4, bar);
       tma_bulk_g2s(sbase + 4u * (oXP + sc * cslot), a.xp + o, crows * ni * 4, bar);
       tma_bulk_g2s(sbase + 4u * (oYP + sc * yslot), a.yp + qc * sz + jy0 * sy, yrows * ni * 4, bar);
     }
-    for (int h = 0; h < 2; ++h) {
-      const int qz = h ? qz1 : qz0;
-      if (!(h ? hz1 : hz0)) continue;
-      tma_bulk_g2s(sbase + 4u * (oZP + rs(qz, RZ) * cslot), a.zp + qz * sz + jred0 * sy, crows * ni * 4, bar);
-    }
+    if (hz) tma_bulk_g2s(sbase + 4u * (oZP + szs * cslot), a.zp + qz * sz + jred0 * sy, crows * ni * 4, bar);
   };
   // all threads: wait for group g; block-uniform result
   auto wait_group = [&](int g) -> bool {
@@ -386,13 +383,11 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
     return __syncthreads_and(ok) != 0;
   };
 
-  // relax colour `odd` of plane p on rows [r0, r1): the reference's row sum
-  // in column order (-z, -y, -x, +x, +y, +z), then (b - sum) / diag
-  auto relax = [&](int p, int r0, int r1, int odd) {
-    const int x0 = xo(p), xm1 = xo(p - 1), xp1 = xo(p + 1);
-    const int sc = rs(p, RC);
-    const int cb = oB + sc * cslot, cd = oD + sc * cslot, cx = oXP + sc * cslot, cy = oYP + sc * yslot;
-    const int cz = oZP + rs(p, RZ) * cslot, czm = oZP + rs(p - 1, RZ) * cslot;
+  // relax colour `odd` of plane p on rows [r0, r1) (slot offsets given): the
+  // reference's row sum in column order (-z, -y, -x, +x, +y, +z), then
+  // (b - sum) / diag
+  auto relax = [&](int p, int r0, int r1, int odd, int x0, int xm1, int xp1, int cb, int cd, int cx, int cy, int cz,
+                   int czm) {
     const bool zlo = p > 0, zhi = p < nk - 1;
     for (int j = r0 + ty; j < r1; j += by) {
       const int sh = odd ? ((j + p + 1) & 1) : ((j + p) & 1);
@@ -414,16 +409,16 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
       }
     }
   };
-  auto prolong_add = [&](int q) {
+  auto prolong_add = [&](int q, int slot) {
     if (q < 0 || q >= nk) return;
-    const int xq = xo(q), cq = xco(q);
+    const int xq = oX + slot * xslot, cq = oXC + slot * cplane;
     for (int r = ty; r < xrows; r += by) {
       const int crr = ((jr0 + r) >> 1) - cr0;
       for (int i = tx; i < ni; i += bx) sm[xq + r * ni + i] = sm[xq + r * ni + i] + sm[cq + crr * a.cni + (i >> 1)];
     }
   };
-  auto zero_x = [&](int q) {
-    const int xq = xo(q);
+  auto zero_x = [&](int slot) {
+    const int xq = oX + slot * xslot;
     for (int e = tid; e < xrows * ni; e += BLOCK) sm[xq + e] = 0.0f;
   };
 
@@ -433,36 +428,46 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
   // D groups stream in during its relaxation.
   double dot = 0.0;
   bool failed = false;
-  int issued = 0;
-  auto issue_h = [&](int q) {
-    if (tid == 0) issue(q - k0 + 2, q + 1, -1, q, q, -1);
-    issued = q - k0 + 3;
-  };
-  if (tid == 0) issue(0, k0 - 2, k0 - 1, -1, k0 - 2, -1);
-  issued = 1;
-  for (int q = k0 - 1; q < k0 - 1 + D && q <= kend; ++q) issue_h(q);
-  for (int p = k0 - 1; p <= kend; ++p) {
-    if (p == k0 - 1 && !wait_group(0)) { failed = true; break; }
+  int issued = 1;
+  if (tid == 0) issue(0, p0 - 1, wrap(px - 1, RX), p0, px, -1, 0, p0 - 1, wrap(pz - 1, RZ));
+  for (int d = 0; d < D && p0 + d <= kend; ++d) {
+    if (tid == 0) issue(1 + d, p0 + d + 1, wrap(px + d + 1, RX), -1, 0, p0 + d, wrap(pc + d, RC), p0 + d,
+                        wrap(pz + d, RZ));
+    issued = 2 + d;
+  }
+  for (int p = p0; p <= kend; ++p) {
+    if (p == p0 && !wait_group(0)) { failed = true; break; }
     if (!wait_group(p - k0 + 2)) { failed = true; break; }
-    if (p + D <= kend) issue_h(p + D);
+    if (p + D <= kend) {
+      if (tid == 0) issue(p + D - k0 + 2, p + D + 1, wrap(px + D + 1, RX), -1, 0, p + D, wrap(pc + D, RC), p + D,
+                          wrap(pz + D, RZ));
+      issued = p + D - k0 + 3;
+    }
+    const int sxm2 = wrap(px - 2, RX), sxm1 = wrap(px - 1, RX), sxp1 = wrap(px + 1, RX);
+    const int scm1 = wrap(pc - 1, RC);
+    const int szm2 = wrap(pz - 2, RZ), szm1 = wrap(pz - 1, RZ);
     if (PROLONG || ZERO_X) {
-      if (p == k0 - 1) {
-        if (PROLONG) { prolong_add(k0 - 2); prolong_add(k0 - 1); }
-        if (ZERO_X) { zero_x(k0 - 2); zero_x(k0 - 1); }
+      if (p == p0) {
+        if (PROLONG) { prolong_add(p - 1, sxm1); prolong_add(p, px); }
+        if (ZERO_X) { zero_x(sxm1); zero_x(px); }
       }
-      if (PROLONG) prolong_add(p + 1);
-      if (ZERO_X) zero_x(p + 1);
+      if (PROLONG) prolong_add(p + 1, sxp1);
+      if (ZERO_X) zero_x(sxp1);
       __syncthreads();
     }
-    if (p >= 0 && p < nk) relax(p, jred0, jred1, 1);
+    if (p >= 0 && p < nk)
+      relax(p, jred0, jred1, 1, oX + px * xslot, oX + sxm1 * xslot, oX + sxp1 * xslot, oB + pc * cslot,
+            oD + pc * cslot, oXP + pc * cslot, oYP + pc * yslot, oZP + pz * cslot, oZP + szm1 * cslot);
     __syncthreads();
     const int q = p - 1;
     const bool out_plane = (q >= k0 && q < kend);
-    if (out_plane) relax(q, j0, jout1, 0);
+    if (out_plane)
+      relax(q, j0, jout1, 0, oX + sxm1 * xslot, oX + sxm2 * xslot, oX + px * xslot, oB + scm1 * cslot,
+            oD + scm1 * cslot, oXP + scm1 * cslot, oYP + scm1 * yslot, oZP + szm1 * cslot, oZP + szm2 * cslot);
     __syncthreads();
     if (out_plane) {
-      const float4* s4 = reinterpret_cast<const float4*>(sm + xo(q) + (j0 - jr0) * ni);
-      const float4* b4 = reinterpret_cast<const float4*>(sm + oB + rs(q, RC) * cslot + (j0 - jred0) * ni);
+      const float4* s4 = reinterpret_cast<const float4*>(sm + oX + sxm1 * xslot + (j0 - jr0) * ni);
+      const float4* b4 = reinterpret_cast<const float4*>(sm + oB + scm1 * cslot + (j0 - jred0) * ni);
       float4* dst = reinterpret_cast<float4*>(a.x_out + q * sz + j0 * sy);
       const int cnt4 = (jout1 - j0) * ni / 4;
       for (int e = tid; e < cnt4; e += BLOCK) {
@@ -474,6 +479,9 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
         }
       }
     }
+    px = wrap(px + 1, RX);
+    pc = wrap(pc + 1, RC);
+    pz = wrap(pz + 1, RZ);
   }
   if (failed) {
     if (tid == 0) atomicExch(a.error, 1);
