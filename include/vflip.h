@@ -179,6 +179,12 @@ int vflip_advect_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, flo
                             const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
                             double oz, const float* field, float* out);
 
+/* Same backtrace for two fields on one grid (e.g. density and temperature):
+ * out = advect(field), out2 = advect(field2); field2/out2 may be NULL. */
+int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                             const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
+                             double oz, const float* field, float* out, const float* field2, float* out2);
+
 /* delta = after - before, n floats (SmokeSolver3D::getDelta, SS/Smoke_solver3D.cpp:1298-1319). */
 int vflip_delta(vflip_ctx* ctx, size_t n, const float* after, const float* before, float* delta);
 

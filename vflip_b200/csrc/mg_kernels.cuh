@@ -587,43 +587,79 @@ __global__ void __launch_bounds__(BLOCK) coarsest_rbgs_kernel(const V* __restric
     zps[e] = A(ldg(zp + e));
   }
   const int sy = ni, sz = ni * nj;
-  // owned cells: index, colour and which of the six neighbours exist
-  int own[kMaxOwn];
-  int colour[kMaxOwn];
+  // owned cells tid + m*BLOCK: bits 0-5 say which of the six neighbours
+  // exist, bits 6-7 hold the colour (0 or 1) or 2 for "no cell"
   int mask[kMaxOwn];
 #pragma unroll
   for (int m = 0; m < kMaxOwn; ++m) {
     int e = threadIdx.x + m * BLOCK;
-    own[m] = e;
-    colour[m] = -1;
-    mask[m] = 0;
+    mask[m] = 2 << 6;
     if (e < n) {
       int i = e % ni, j = (e / ni) % nj, k = e / sz;
-      colour[m] = (i + j + k) & 1;
       mask[m] = (k > 0) | ((j > 0) << 1) | ((i > 0) << 2) | ((i < ni - 1) << 3) | ((j < nj - 1) << 4) |
-                ((k < nk - 1) << 5);
+                ((k < nk - 1) << 5) | (((i + j + k) & 1) << 6);
     }
   }
   __syncthreads();
-  for (int it = 0; it < sweeps; ++it) {
+  if (sizeof(A) == 4) {
+    // FP32: each owned cell's couplings, diagonal and rhs stay in registers
+    // (a missing neighbour gets coupling 0 and reads the cell itself), so a
+    // colour phase is six shared loads per cell and one barrier
+    A c[kMaxOwn][6], dd[kMaxOwn], bb[kMaxOwn];
 #pragma unroll
-    for (int parity = 1; parity >= 0; --parity) {
+    for (int m = 0; m < kMaxOwn; ++m) {
+      const int e = (threadIdx.x + m * BLOCK) < n ? (threadIdx.x + m * BLOCK) : 0;
+      const int f = mask[m];
+      c[m][0] = (f & 1) ? zps[e - sz] : A(0);
+      c[m][1] = (f & 2) ? yps[e - sy] : A(0);
+      c[m][2] = (f & 4) ? xps[e - 1] : A(0);
+      c[m][3] = (f & 8) ? xps[e] : A(0);
+      c[m][4] = (f & 16) ? yps[e] : A(0);
+      c[m][5] = (f & 32) ? zps[e] : A(0);
+      dd[m] = ds[e];
+      bb[m] = bs[e];
+    }
+    for (int it = 0; it < sweeps; ++it) {
 #pragma unroll
-      for (int m = 0; m < kMaxOwn; ++m) {
-        if (colour[m] != parity) continue;
-        const int e = own[m];
-        const int f = mask[m];
-        A sum = A(0);
-        if (f & 1) sum = sum + zps[e - sz] * xs[e - sz];
-        if (f & 2) sum = sum + yps[e - sy] * xs[e - sy];
-        if (f & 4) sum = sum + xps[e - 1] * xs[e - 1];
-        if (f & 8) sum = sum + xps[e] * xs[e + 1];
-        if (f & 16) sum = sum + yps[e] * xs[e + sy];
-        if (f & 32) sum = sum + zps[e] * xs[e + sz];
-        A d = ds[e];
-        xs[e] = (d != A(0)) ? gs_div(bs[e] - sum, d) : A(0);
+      for (int parity = 1; parity >= 0; --parity) {
+#pragma unroll
+        for (int m = 0; m < kMaxOwn; ++m) {
+          if ((mask[m] >> 6) != parity) continue;
+          const int e = threadIdx.x + m * BLOCK;
+          const int f = mask[m];
+          A sum = A(0);
+          sum = sum + c[m][0] * xs[(f & 1) ? e - sz : e];
+          sum = sum + c[m][1] * xs[(f & 2) ? e - sy : e];
+          sum = sum + c[m][2] * xs[(f & 4) ? e - 1 : e];
+          sum = sum + c[m][3] * xs[(f & 8) ? e + 1 : e];
+          sum = sum + c[m][4] * xs[(f & 16) ? e + sy : e];
+          sum = sum + c[m][5] * xs[(f & 32) ? e + sz : e];
+          xs[e] = (dd[m] != A(0)) ? gs_div(bb[m] - sum, dd[m]) : A(0);
+        }
+        __syncthreads();
       }
-      __syncthreads();
+    }
+  } else {
+    for (int it = 0; it < sweeps; ++it) {
+#pragma unroll
+      for (int parity = 1; parity >= 0; --parity) {
+#pragma unroll
+        for (int m = 0; m < kMaxOwn; ++m) {
+          if ((mask[m] >> 6) != parity) continue;
+          const int e = threadIdx.x + m * BLOCK;
+          const int f = mask[m];
+          A sum = A(0);
+          if (f & 1) sum = sum + zps[e - sz] * xs[e - sz];
+          if (f & 2) sum = sum + yps[e - sy] * xs[e - sy];
+          if (f & 4) sum = sum + xps[e - 1] * xs[e - 1];
+          if (f & 8) sum = sum + xps[e] * xs[e + 1];
+          if (f & 16) sum = sum + yps[e] * xs[e + sy];
+          if (f & 32) sum = sum + zps[e] * xs[e + sz];
+          A d = ds[e];
+          xs[e] = (d != A(0)) ? gs_div(bs[e] - sum, d) : A(0);
+        }
+        __syncthreads();
+      }
     }
   }
   double dot = 0.0;

@@ -21,7 +21,11 @@ struct GridView {
   const float* d;
   int nx, ny, nz;
   double h, ox, oy, oz;
+  double inv_h;  // 1/h when h is a power of two (then x*inv_h == x/h exactly), else 0
 };
+
+// x / h exactly as IEEE division; a multiplication when h is a power of two
+__device__ __forceinline__ double div_h(double x, const GridView& g) { return g.inv_h != 0.0 ? x * g.inv_h : x / g.h; }
 
 __device__ __forceinline__ float grid_at(const GridView& g, int i, int j, int k) {
   i = i < 0 ? 0 : (i > g.nx - 1 ? g.nx - 1 : i);
@@ -33,7 +37,7 @@ __device__ __forceinline__ float grid_at(const GridView& g, int i, int j, int k)
 __device__ __forceinline__ double lerp_d(double a, double b, double c) { return (1.0 - c) * a + c * b; }
 
 __device__ __forceinline__ float sample_linear(const GridView& g, double wx, double wy, double wz) {
-  double gx = wx / g.h + g.ox, gy = wy / g.h + g.oy, gz = wz / g.h + g.oz;
+  double gx = div_h(wx, g) + g.ox, gy = div_h(wy, g) + g.oy, gz = div_h(wz, g) + g.oz;
   int i = (int)floor(gx), j = (int)floor(gy), k = (int)floor(gz);
   double cx = gx - (double)i, cy = gy - (double)j, cz = gz - (double)k;
   double v1 = lerp_d(lerp_d(grid_at(g, i, j, k), grid_at(g, i + 1, j, k), cx),
@@ -45,27 +49,64 @@ __device__ __forceinline__ float sample_linear(const GridView& g, double wx, dou
 
 // SubDomainSolver::advect_field, sub_domain.cpp:191-235: RK2 midpoint
 // backtrace through the MAC velocity, then a trilinear sample of the field.
-// The field's node (i,j,k) sits at world ((i-ox)h, (j-oy)h, (k-oz)h).
-__global__ void advect_rk2_kernel(GridView u, GridView v, GridView w, GridView f, float* __restrict__ out, float h,
-                                  float dt) {
+// The field's node (i,j,k) sits at world ((i-ox)h, (j-oy)h, (k-oz)h).  A
+// second field on the same grid (f2.d != nullptr) shares the backtrace.
+// Each thread carries two nodes through the three dependent gather rounds
+// so that their loads overlap.
+struct Backtrace {
+  float px, py, pz;
+};
+
+__device__ __forceinline__ void node_world(const GridView& f, size_t e, float h, float& wx, float& wy, float& wz) {
+  int i = (int)(e % f.nx), j = (int)((e / f.nx) % f.ny), k = (int)(e / ((size_t)f.nx * f.ny));
+  wx = (float)(((double)(float)i - f.ox) * (double)h);
+  wy = (float)(((double)(float)j - f.oy) * (double)h);
+  wz = (float)(((double)(float)k - f.oz) * (double)h);
+}
+
+__global__ void advect_rk2_kernel(GridView u, GridView v, GridView w, GridView f, float* __restrict__ out,
+                                  GridView f2, float* __restrict__ out2, float h, float dt) {
   const size_t n = (size_t)f.nx * f.ny * f.nz;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    int i = (int)(e % f.nx), j = (int)((e / f.nx) % f.ny), k = (int)(e / ((size_t)f.nx * f.ny));
-    float wx = (float)(((double)(float)i - f.ox) * (double)h);
-    float wy = (float)(((double)(float)j - f.oy) * (double)h);
-    float wz = (float)(((double)(float)k - f.oz) * (double)h);
-    float a = sample_linear(u, wx, wy, wz), b = sample_linear(v, wx, wy, wz), c = sample_linear(w, wx, wy, wz);
-    const double hdt = 0.5 * (double)dt;
-    float px = (float)((double)wx - hdt * (double)a);
-    float py = (float)((double)wy - hdt * (double)b);
-    float pz = (float)((double)wz - hdt * (double)c);
-    a = sample_linear(u, px, py, pz);
-    b = sample_linear(v, px, py, pz);
-    c = sample_linear(w, px, py, pz);
-    px = wx - dt * a;
-    py = wy - dt * b;
-    pz = wz - dt * c;
-    out[e] = sample_linear(f, px, py, pz);
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const double hdt = 0.5 * (double)dt;
+  for (size_t e0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < n; e0 += 2 * stride) {
+    const size_t e1 = e0 + stride;
+    const bool two = e1 < n;
+    float wx0, wy0, wz0, wx1 = 0, wy1 = 0, wz1 = 0;
+    node_world(f, e0, h, wx0, wy0, wz0);
+    if (two) node_world(f, e1, h, wx1, wy1, wz1);
+    float a0 = sample_linear(u, wx0, wy0, wz0), b0 = sample_linear(v, wx0, wy0, wz0),
+          c0 = sample_linear(w, wx0, wy0, wz0);
+    float a1 = 0, b1 = 0, c1 = 0;
+    if (two) {
+      a1 = sample_linear(u, wx1, wy1, wz1);
+      b1 = sample_linear(v, wx1, wy1, wz1);
+      c1 = sample_linear(w, wx1, wy1, wz1);
+    }
+    float px0 = (float)((double)wx0 - hdt * (double)a0), py0 = (float)((double)wy0 - hdt * (double)b0),
+          pz0 = (float)((double)wz0 - hdt * (double)c0);
+    float px1 = (float)((double)wx1 - hdt * (double)a1), py1 = (float)((double)wy1 - hdt * (double)b1),
+          pz1 = (float)((double)wz1 - hdt * (double)c1);
+    a0 = sample_linear(u, px0, py0, pz0);
+    b0 = sample_linear(v, px0, py0, pz0);
+    c0 = sample_linear(w, px0, py0, pz0);
+    if (two) {
+      a1 = sample_linear(u, px1, py1, pz1);
+      b1 = sample_linear(v, px1, py1, pz1);
+      c1 = sample_linear(w, px1, py1, pz1);
+    }
+    px0 = wx0 - dt * a0;
+    py0 = wy0 - dt * b0;
+    pz0 = wz0 - dt * c0;
+    px1 = wx1 - dt * a1;
+    py1 = wy1 - dt * b1;
+    pz1 = wz1 - dt * c1;
+    out[e0] = sample_linear(f, px0, py0, pz0);
+    if (out2) out2[e0] = sample_linear(f2, px0, py0, pz0);
+    if (two) {
+      out[e1] = sample_linear(f, px1, py1, pz1);
+      if (out2) out2[e1] = sample_linear(f2, px1, py1, pz1);
+    }
   }
 }
 
@@ -89,9 +130,13 @@ static_assert(sizeof(ParticleRec) == 40, "particle record is 40 bytes");
 // hash_FLIP cell, Smoke_solver3D.cpp:1337-1343: int((pos + 0.5h)/h) with
 // C truncation; values outside (-1, n) (and NaN) are out of range, as the
 // x86 conversion makes them in the reference.
-__device__ __forceinline__ int hash_cell(const float* pos, int ni, int nj, int nk, float h) {
+// x / h in float, exactly as IEEE division; a multiplication when h is a
+// power of two (inv_h != 0), which is then exact
+__device__ __forceinline__ float fdiv_h(float x, float h, float inv_h) { return inv_h != 0.0f ? x * inv_h : x / h; }
+
+__device__ __forceinline__ int hash_cell(const float* pos, int ni, int nj, int nk, float h, float inv_h) {
   const float c = 0.5f * h;
-  float tx = (pos[0] + c) / h, ty = (pos[1] + c) / h, tz = (pos[2] + c) / h;
+  float tx = fdiv_h(pos[0] + c, h, inv_h), ty = fdiv_h(pos[1] + c, h, inv_h), tz = fdiv_h(pos[2] + c, h, inv_h);
   if (!(tx > -1.0f && tx < (float)ni)) return -1;
   if (!(ty > -1.0f && ty < (float)nj)) return -1;
   if (!(tz > -1.0f && tz < (float)nk)) return -1;
@@ -99,9 +144,10 @@ __device__ __forceinline__ int hash_cell(const float* pos, int ni, int nj, int n
 }
 
 __global__ void hash_count_kernel(const ParticleRec* __restrict__ p, int np, int ni, int nj, int nk, float h,
-                                  int* __restrict__ cell, int* __restrict__ slot, int* __restrict__ count) {
+                                  float inv_h, int* __restrict__ cell, int* __restrict__ slot,
+                                  int* __restrict__ count) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
-    int c = hash_cell(p[q].pos, ni, nj, nk, h);
+    int c = hash_cell(p[q].pos, ni, nj, nk, h, inv_h);
     cell[q] = c;
     slot[q] = (c >= 0) ? atomicAdd(count + c, 1) : -1;
   }
@@ -241,7 +287,7 @@ __device__ __forceinline__ float tent(float r) {  // SmokeSolver3D::H, Smoke_sol
 // contributes exactly nothing, so it is skipped without changing any sum.
 __global__ void p2g_kernel(const int* __restrict__ start, const float4* __restrict__ spos,
                            const float4* __restrict__ svel, float* __restrict__ field, float* __restrict__ coef,
-                           int comp, int ni, int nj, int nk, float h) {
+                           int comp, int ni, int nj, int nk, float h, float inv_h) {
   const int fx = ni + (comp == 0), fy = nj + (comp == 1), fz = nk + (comp == 2);
   const double ox = comp == 0 ? 0.5 : 0.0, oy = comp == 1 ? 0.5 : 0.0, oz = comp == 2 ? 0.5 : 0.0;
   const size_t n = (size_t)fx * fy * fz;
@@ -267,7 +313,7 @@ __global__ void p2g_kernel(const int* __restrict__ start, const float4* __restri
             float4 pp = __ldg(spos + q);
             float dx = pp.x - gx, dy = pp.y - gy, dz = pp.z - gz;
             if (pp.w != 0.0f && (fabsf(dx) >= reach || fabsf(dy) >= reach || fabsf(dz) >= reach)) continue;
-            float wgt = tent(dx / h) * tent(dy / h) * tent(dz / h);
+            float wgt = tent(fdiv_h(dx, h, inv_h)) * tent(fdiv_h(dy, h, inv_h)) * tent(fdiv_h(dz, h, inv_h));
             float4 vv = __ldg(svel + q);
             float vc = comp == 0 ? vv.x : (comp == 1 ? vv.y : vv.z);
             tw = tw + wgt;

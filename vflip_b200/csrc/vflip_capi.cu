@@ -106,6 +106,13 @@ struct vflip_ctx {
 
 namespace {
 
+// 1/h when h is a power of two (x*(1/h) then equals x/h exactly), else 0
+double inv_pow2(double h) {
+  int e;
+  double m = std::frexp(h, &e);
+  return (m == 0.5 && h > 0) ? 1.0 / h : 0.0;
+}
+
 int grid_for(size_t n, int block, int num_sms) {
   size_t g = (n + block - 1) / block;
   size_t cap = (size_t)num_sms * 16;
@@ -1068,22 +1075,35 @@ int vflip_project(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, c
   return status;
 }
 
-int vflip_advect_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
-                            const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
-                            double oz, const float* field, float* out) {
+int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                             const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
+                             double oz, const float* field, float* out, const float* field2, float* out2) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (fnx <= 0 || fny <= 0 || fnz <= 0 || !u || !v || !w || !field || !out)
     return ctx->fail(VFLIP_ERR_ARG, "bad argument");
   if (out == field || out == u || out == v || out == w) return ctx->fail(VFLIP_ERR_ARG, "out aliases an input");
-  GridView gu{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0};
-  GridView gv{v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0};
-  GridView gw{w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5};
-  GridView gf{field, fnx, fny, fnz, (double)h, ox, oy, oz};
+  if (field2 && (!out2 || out2 == field2 || out2 == field || out2 == out || out2 == u || out2 == v || out2 == w ||
+                 out == field2))
+    return ctx->fail(VFLIP_ERR_ARG, "second output missing or aliased");
+  const double ih = inv_pow2(h);
+  GridView gu{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0, ih};
+  GridView gv{v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0, ih};
+  GridView gw{w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5, ih};
+  GridView gf{field, fnx, fny, fnz, (double)h, ox, oy, oz, ih};
+  GridView gf2{field2, fnx, fny, fnz, (double)h, ox, oy, oz, ih};
   size_t n = (size_t)fnx * fny * fnz;
-  advect_rk2_kernel<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, h, dt);
+  advect_rk2_kernel<<<grid_for((n + 1) / 2, 256, ctx->num_sms), 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2,
+                                                                                     field2 ? out2 : nullptr, h, dt);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
+}
+
+int vflip_advect_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                            const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
+                            double oz, const float* field, float* out) {
+  return vflip_advect_rk2_linear2(ctx, ni, nj, nk, h, dt, u, v, w, fnx, fny, fnz, ox, oy, oz, field, out, nullptr,
+                                  nullptr);
 }
 
 int vflip_delta(vflip_ctx* ctx, size_t n, const float* after, const float* before, float* delta) {
@@ -1107,7 +1127,7 @@ int vflip_particle_cells(vflip_ctx* ctx, int ni, int nj, int nk, float h, const 
   VF_ALLOC(count, int, "p_count", nc + 1);
   VF_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (nc + 1), ctx->stream));
   hash_count_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
-      (const ParticleRec*)particles, np, ni, nj, nk, h, cell_out, slot, count);
+      (const ParticleRec*)particles, np, ni, nj, nk, h, (float)inv_pow2(h), cell_out, slot, count);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
 }
@@ -1162,7 +1182,7 @@ int vflip_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* parti
   VF_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (nc + 1), ctx->stream));
   if (np > 0) {
     hash_count_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
-        (const ParticleRec*)particles, np, ni, nj, nk, h, cell, slot, count);
+        (const ParticleRec*)particles, np, ni, nj, nk, h, (float)inv_pow2(h), cell, slot, count);
     VF_LAUNCH_CHECK();
   }
   if ((rc = exclusive_scan(ctx, count, start, nc + 1))) return rc;
@@ -1180,7 +1200,8 @@ int vflip_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* parti
     if (!outs[c][0]) continue;
     size_t nf = (size_t)(ni + (c == 0)) * (nj + (c == 1)) * (nk + (c == 2));
     p2g_kernel<<<grid_for(nf, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(start, spos, svel, outs[c][0],
-                                                                             outs[c][1], c, ni, nj, nk, h);
+                                                                             outs[c][1], c, ni, nj, nk, h,
+                                                                             (float)inv_pow2(h));
     VF_LAUNCH_CHECK();
   }
   return VFLIP_OK;
@@ -1194,12 +1215,13 @@ int vflip_g2p(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, 
   if (np < 0 || (np > 0 && !particles) || !du || !dv || !dw) return ctx->fail(VFLIP_ERR_ARG, "bad argument");
   if (flip_ratio != 1.0 && (!un || !vn || !wn)) return ctx->fail(VFLIP_ERR_ARG, "blend needs u_new/v_new/w_new");
   if (np == 0) return VFLIP_OK;
-  GridView gdu{du, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0};
-  GridView gdv{dv, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0};
-  GridView gdw{dw, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5};
-  GridView gun{un ? un : du, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0};
-  GridView gvn{vn ? vn : dv, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0};
-  GridView gwn{wn ? wn : dw, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5};
+  const double ih = inv_pow2(h);
+  GridView gdu{du, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0, ih};
+  GridView gdv{dv, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0, ih};
+  GridView gdw{dw, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5, ih};
+  GridView gun{un ? un : du, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0, ih};
+  GridView gvn{vn ? vn : dv, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0, ih};
+  GridView gwn{wn ? wn : dw, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5, ih};
   g2p_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>((ParticleRec*)particles, np, gdu, gdv, gdw,
                                                                        gun, gvn, gwn, flip_ratio);
   VF_LAUNCH_CHECK();

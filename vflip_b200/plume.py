@@ -77,9 +77,12 @@ class PlumeSim:
     def step(self):
         p, s, n, h = self.p, self.s, self.p.n, self.p.h
         u, v, w = self.f["u"], self.f["v"], self.f["w"]
-        offs = {"u": (0.5, 0, 0), "v": (0, 0.5, 0), "w": (0, 0, 0.5), "rho": (0, 0, 0), "temp": (0, 0, 0)}
-        for k in self.FIELDS:
+        offs = {"u": (0.5, 0, 0), "v": (0, 0.5, 0), "w": (0, 0, 0.5)}
+        for k in ("u", "v", "w"):
             s.advect_rk2_linear(n, n, n, h, p.dt, u, v, w, self.f[k], offs[k], out=self.g[k])
+        # density and temperature share the cell-centred backtrace
+        s.advect_rk2_linear2(n, n, n, h, p.dt, u, v, w, self.f["rho"], self.f["temp"], (0, 0, 0), out=self.g["rho"],
+                             out2=self.g["temp"])
         self.f, self.g = self.g, self.f
         s.plume_sources(n, n, n, h, p.dt, self.f["rho"], self.f["temp"], self.f["v"], p.source_centre,
                         p.source_radius, 1.0, 1.0, p.alpha, p.beta)

@@ -215,6 +215,16 @@ class Solver:
                                                      float(offsets[2]), _p(field), _p(out)))
         return out
 
+    def advect_rk2_linear2(self, ni, nj, nk, h, dt, u, v, w, field, field2, offsets, out=None, out2=None):
+        """Two fields on the same grid advected along one backtrace."""
+        fnz, fny, fnx = field.shape
+        out = torch.empty_like(field) if out is None else out
+        out2 = torch.empty_like(field2) if out2 is None else out2
+        self._check(self.lib.vflip_advect_rk2_linear2(self.ctx, ni, nj, nk, float(h), float(dt), _p(u), _p(v), _p(w),
+                                                      fnx, fny, fnz, float(offsets[0]), float(offsets[1]),
+                                                      float(offsets[2]), _p(field), _p(out), _p(field2), _p(out2)))
+        return out, out2
+
     def delta(self, after, before, out=None):
         if out is None:
             out = torch.empty_like(after)
