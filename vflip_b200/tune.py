@@ -80,8 +80,16 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--out", default=CACHE)
+    ap.add_argument("--solve-once", action="store_true",
+                    help="assemble the operator and run one FP32 solve (a small target for profilers)")
+    ap.add_argument("--precision", type=int, default=1)
     a = ap.parse_args()
     st, rhs = problem(a.n, "cuda:0")
+    if a.solve_once:
+        with Solver(precision=a.precision) as s:
+            ok, _, stats = s.amgpcg_solve(st, rhs, 1e-6, 50)
+        print(json.dumps({"n": a.n, "converged": ok, "iterations": stats.iterations, "solve_ms": stats.solve_ms}))
+        return
     results = []
     for shape in CANDIDATES:
         try:
