@@ -45,6 +45,7 @@ extern "C" {
 #define VFLIP_ERR_NOT_7POINT (-3)
 #define VFLIP_ERR_NOT_SYMMETRIC (-4)
 #define VFLIP_ERR_NOMEM (-5)
+#define VFLIP_ERR_TOO_LARGE (-6)
 
 /* Arithmetic of the multigrid-preconditioned CG.
  *   FP64  - everything in FP64; the V-cycle is bit-identical to the
@@ -142,6 +143,26 @@ int vflip_rbgs(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const
  * are FP64 either way). */
 int vflip_vcycle(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const double* xp, const double* yp,
                  const double* zp, const double* b, double* x);
+
+/* Same sweeps as vflip_rbgs, for callers that cannot allocate device memory:
+ * code recorded into a CUDA graph by stream capture (where cudaMalloc is not
+ * permitted), real-time loops that forbid allocation, and applications that
+ * hand every device byte to their own allocator.  No context is needed and
+ * nothing is allocated: the work runs on `stream` (NULL: the default stream)
+ * of the current device, and the second buffer of the sweeps is a fixed
+ * array of VFLIP_NOALLOC_MAX_CELLS doubles (2 MiB) inside this library, which
+ * every GPU that loads the library holds until the process exits.  Grids with
+ * more than VFLIP_NOALLOC_MAX_CELLS cells return VFLIP_ERR_TOO_LARGE.
+ * The first call on a device looks up that array's device address (once per
+ * device) and must come before any stream capture on that device.  All calls
+ * share the one array: calls that overlap on the GPU (different streams, or
+ * different host threads) race on it and must be serialised by the caller.
+ * The array keeps the last call's contents; every sweep overwrites all the
+ * cells it reads back, so nothing needs clearing.  No counterpart in the
+ * reference (its RBGS, AlgebraicMultigrid.h:22-103, allocates host vectors). */
+#define VFLIP_NOALLOC_MAX_CELLS (64 * 64 * 64)
+int vflip_rbgs_noalloc(void* stream, int ni, int nj, int nk, const double* diag, const double* xp, const double* yp,
+                       const double* zp, const double* b, double* x, int iterations);
 
 /* ---- pressure projection -------------------------------------------------- */
 

@@ -47,6 +47,7 @@ SIGNATURES = {
     "vflip_build_levels": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _I, _P, _P]),
     "vflip_rbgs": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _I]),
     "vflip_vcycle": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P]),
+    "vflip_rbgs_noalloc": (_I, [_P, _I, _I, _I, _P, _P, _P, _P, _P, _P, _I]),
     "vflip_face_weights": (_I, [_P, _I, _I, _I, _P, _P, _P, _P]),
     "vflip_assemble": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "vflip_project": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _I,

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <mutex>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -1316,3 +1317,92 @@ int vflip_profile_sweeps(vflip_ctx* ctx, int* launches, double* total_ms, double
 unsigned long long vflip_launch_count(const vflip_ctx* ctx) { return ctx ? ctx->launches : 0ull; }
 
 }  // extern "C"
+
+// ============================================================== no-allocation smoother
+// vflip_rbgs_noalloc: the red-black smoother of vflip_rbgs for callers that
+// must not allocate device memory.  Its ping-pong buffer is the file-scope
+// array below; each GPU that loads this library holds it until the process
+// exits.  Host code never dereferences the symbol: the device address is
+// fetched with cudaGetSymbolAddress once per device, with that device current,
+// the first time the entry point runs on it.
+namespace {
+
+static __device__ __align__(256) double vflip_noalloc_scratch[VFLIP_NOALLOC_MAX_CELLS];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+double* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+int g_noalloc_sms[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array and SM count for the current device,
+// looked up once per device (the first call should therefore come before any
+// stream capture).
+cudaError_t noalloc_setup(double** ptr, int* sms) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, vflip_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    int n = 0;
+    e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    g_noalloc_sms[dev] = n;
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *ptr = g_noalloc_ptr[dev];
+  *sms = g_noalloc_sms[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+extern "C" int vflip_rbgs_noalloc(void* stream, int ni, int nj, int nk, const double* diag, const double* xp,
+                                  const double* yp, const double* zp, const double* b, double* x, int iterations) {
+  if (ni <= 0 || nj <= 0 || nk <= 0 || !diag || !xp || !yp || !zp || !b || !x || iterations < 0)
+    return VFLIP_ERR_ARG;
+  const size_t n = (size_t)ni * nj * nk;
+  if (n > (size_t)VFLIP_NOALLOC_MAX_CELLS) return VFLIP_ERR_TOO_LARGE;
+  double* scratch = nullptr;
+  int sms = 0;
+  if (noalloc_setup(&scratch, &sms) != cudaSuccess) return VFLIP_ERR_CUDA;
+  if (iterations == 0) return VFLIP_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const Dims d{ni, nj, nk};
+  SweepShape sh = sweep_shape<double>(d, sms);
+  if (sh.smem > 200 * 1024 || sh.grid_y * sh.grid_z > kMaxPartials) return VFLIP_ERR_ARG;
+  auto kern = rbgs_sweep_kernel<double, double, false, false, false, kSweepBlock>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) != cudaSuccess)
+    return VFLIP_ERR_CUDA;
+  SweepArgs<double, double> a{};
+  a.b = b;
+  a.diag = diag;
+  a.xp = xp;
+  a.yp = yp;
+  a.zp = zp;
+  a.xc = nullptr;
+  a.ni = ni;
+  a.nj = nj;
+  a.nk = nk;
+  a.tyo = sh.tyo;
+  a.kz = sh.kz;
+  a.plane_stride = sh.plane_stride;
+  a.dot_partial = nullptr;
+  // ping-pong between x and the scratch array; every sweep writes all cells
+  // of its output, so the scratch needs no clearing between calls
+  double* cur = x;
+  for (int s = 0; s < iterations; ++s) {
+    double* out = (cur == x) ? scratch : x;
+    a.x_in = cur;
+    a.x_out = out;
+    kern<<<dim3(sh.grid_y, sh.grid_z), kSweepBlock, sh.smem, st>>>(a);
+    if (cudaGetLastError() != cudaSuccess) return VFLIP_ERR_CUDA;
+    cur = out;
+  }
+  if (cur != x && cudaMemcpyAsync(x, cur, sizeof(double) * n, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return VFLIP_ERR_CUDA;
+  return VFLIP_OK;
+}
