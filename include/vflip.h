@@ -188,6 +188,17 @@ int vflip_project(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, c
                   float* w, double* pressure, double tolerance_factor, int max_iterations,
                   vflip_solve_stats* stats);
 
+/* SubDomainSolver::pcg_projection (SS/sub_domain.cpp:560-821), the nested
+ * fine domain's projection: no inflow overwrite, operator terms
+ * w*dt/h^2, solid term scaled by the float 1/h, and the gradient
+ * u -= dt*(p_i - p_{i-1})/h applied on every face between two cells of the
+ * grid.  The reference solves it to tolerance 1e-9 in at most 1000
+ * iterations (SS/sub_domain.cpp:739). */
+int vflip_project_subdomain(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* nodal_phi,
+                            const float* us, const float* vs, const float* ws, float* u, float* v, float* w,
+                            double* pressure, double tolerance_factor, int max_iterations,
+                            vflip_solve_stats* stats);
+
 /* ---- advection ------------------------------------------------------------- */
 
 /* Semi-Lagrangian RK2 (midpoint) backtrace through the MAC velocity u/v/w of

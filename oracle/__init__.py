@@ -64,6 +64,12 @@ def _load(path, prefix):
         getattr(lib, p + "_vcycle").argtypes = [_I, _I, _I, _P, _P, _P, _P, _P]
         getattr(lib, p + "_amgpcg").argtypes = [_I, _I, _I, _P, _P, _P, _P, _P, _D, _I, _P, _P]
         getattr(lib, p + "_delta").argtypes = [_I, _I, _I, _P, _P, _P]
+    if prefix == "oracle":
+        getattr(lib, p + "_project_subdomain").argtypes = [_I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                                           _P, _P, _D, _I]
+    else:
+        getattr(lib, p + "_project_subdomain").argtypes = [_I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                                           _P]
     getattr(lib, p + "_smoke_step").argtypes = [_I, _F, _F, _P, _P, _P, _P, _P, _P, _F, _F, _F, _F, _F, _F, _P, _P]
     getattr(lib, p + "_smoke_step").restype = C.c_double if prefix == "ref" else C.c_int
     getattr(lib, p + "_fraction_inside4").argtypes = [_I, _P, _P, _P, _P, _P]
@@ -209,6 +215,28 @@ class _Impl:
         assert n == p.size
         return dict(u=u, v=v, w=w, pressure=p, rhs=rhs, stencil=st, uw=uw, vw=vw, ww=ww, ok=bool(ok),
                     iterations=it.value, residual=res.value)
+
+    def project_subdomain(self, ni, nj, nk, h, dt, phi, us, vs, ws, u, v, w, tol=1e-9, maxit=1000):
+        """SubDomainSolver::pcg_projection (the reference library always uses
+        1e-9 / 1000)."""
+        phi = np.ascontiguousarray(phi, np.float32)
+        us, vs, ws = [np.ascontiguousarray(a, np.float32) for a in (us, vs, ws)]
+        u, v, w = [np.array(a, np.float32, copy=True, order="C") for a in (u, v, w)]
+        p = np.zeros((nk, nj, ni), np.float64)
+        rhs = np.zeros_like(p)
+        st = np.zeros((7, nk, nj, ni), np.float64)
+        if self.p == "oracle":
+            it = C.c_int(0)
+            res = C.c_double(0)
+            ok = self.fn("project_subdomain")(ni, nj, nk, h, dt, _ptr(phi), _ptr(us), _ptr(vs), _ptr(ws), _ptr(u),
+                                              _ptr(v), _ptr(w), _ptr(p), _ptr(rhs), _ptr(st), C.byref(it),
+                                              C.byref(res), tol, maxit)
+            extra = dict(ok=bool(ok), iterations=it.value, residual=res.value)
+        else:
+            self.fn("project_subdomain")(ni, nj, nk, h, dt, _ptr(phi), _ptr(us), _ptr(vs), _ptr(ws), _ptr(u), _ptr(v),
+                                         _ptr(w), _ptr(p), _ptr(rhs), _ptr(st))
+            extra = {}
+        return dict(u=u, v=v, w=w, pressure=p, rhs=rhs, stencil=st, **extra)
 
     def advect_rk2(self, ni, nj, nk, h, dt, u, v, w, field, offsets):
         u, v, w, field = [np.ascontiguousarray(a, np.float32) for a in (u, v, w, field)]

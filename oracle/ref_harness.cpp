@@ -274,6 +274,54 @@ int ref_project(int ni, int nj, int nk, float h, float U_in, const float* nodal_
   return 1;
 }
 
+// SubDomainSolver::pcg_projection (sub_domain.cpp:560-821) on a subdomain
+// grid set up like SubDomainSolver::init (sub_domain.h:218-262): no inflow,
+// dt-scaled operator, AMGPCGSolve(1e-9, 1000).  u/v/w updated in place;
+// optional outputs as in ref_project.  Returns 1.
+int ref_project_subdomain(int ni, int nj, int nk, float h, float dt, const float* nodal_phi, const float* us,
+                          const float* vs, const float* ws, float* u, float* v, float* w, double* pressure_out,
+                          double* rhs_out, double* stencil_out) {
+  SubDomainSolver* sd = new SubDomainSolver();
+  quiet_subdomain(*sd);
+  sd->_nx = ni; sd->_ny = nj; sd->_nz = nk;
+  sd->_hx = sd->_hy = sd->_hz = h;
+  sd->_un.init(ni + 1, nj, nk, h, 0.5, 0, 0);
+  sd->_vn.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0);
+  sd->_wn.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5);
+  sd->_u_solid.init(ni + 1, nj, nk, h, 0.5, 0, 0);
+  sd->_v_solid.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0);
+  sd->_w_solid.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5);
+  sd->u_valid.resize(ni + 1, nj, nk);
+  sd->v_valid.resize(ni, nj + 1, nk);
+  sd->w_valid.resize(ni, nj, nk + 1);
+  sd->_u_weights.init(ni + 1, nj, nk);
+  sd->_v_weights.init(ni, nj + 1, nk);
+  sd->_w_weights.init(ni, nj, nk + 1);
+  sd->_nodal_solid_phi.init(ni + 1, nj + 1, nk + 1, h, 0.5, 0.5, 0.5);
+  to_buffer(sd->_nodal_solid_phi, nodal_phi);
+  to_buffer(sd->_u_solid, us);
+  to_buffer(sd->_v_solid, vs);
+  to_buffer(sd->_w_solid, ws);
+  to_buffer(sd->_un, u);
+  to_buffer(sd->_vn, v);
+  to_buffer(sd->_wn, w);
+  sd->pcg_projection(dt);
+  from_buffer(sd->_un, u);
+  from_buffer(sd->_vn, v);
+  from_buffer(sd->_wn, w);
+  size_t n = (size_t)ni * nj * nk;
+  if (pressure_out) for (size_t q = 0; q < n; ++q) pressure_out[q] = sd->pressure[q];
+  if (rhs_out) for (size_t q = 0; q < n; ++q) rhs_out[q] = sd->rhs[q];
+  if (stencil_out) {
+    FixedSparseMatrix<double> A;
+    A.construct_from_matrix(sd->matrix);
+    fixed_to_stencil(A, ni, nj, nk, stencil_out);
+  }
+  // the subdomain solver's buffers are freed by its destructor
+  delete sd;
+  return 1;
+}
+
 // SubDomainSolver::advect_field (sub_domain.cpp:191-235): RK2 midpoint
 // backtrace on u,v,w + trilinear sample of `field`.  The field lives on an
 // fnx x fny x fnz grid of spacing h with grid offsets (fox, foy, foz).

@@ -503,12 +503,20 @@ void oracle_face_weights(int ni, int nj, int nk, float h, const float* phi, floa
   face_weights(ni, nj, nk, phi, uw, vw, ww);
 }
 
-// SmokeSolver3D::pcg_projection, SS/Smoke_solver3D.cpp:945-1202.  Same
-// argument meaning as ref_project in oracle/ref_harness.cpp.
-int oracle_project(int ni, int nj, int nk, float h, float U_in, const float* phi, const int8_t* bdesc,
-                   const float* us, const float* vs, const float* ws, float* u, float* v, float* w,
-                   double* pressure_out, double* rhs_out, double* st_out, float* uw_out, float* vw_out,
-                   float* ww_out, int* iterations_out, double* residual_out) {
+}  // extern "C"
+
+namespace {
+// variant 0: SmokeSolver3D::pcg_projection, SS/Smoke_solver3D.cpp:945-1202
+// (inflow overwrite, w/h^2 terms, double 1.0/h solid term, gradient on faces
+// strictly inside the interior, AMGPCG 1e-6 / 50);
+// variant 1: SubDomainSolver::pcg_projection, SS/sub_domain.cpp:560-821 (no
+// inflow, w*dt/h^2 terms, float 1/h solid term, gradient dt*(dp)/h on every
+// face between two cells, AMGPCG with the given tolerance / iterations).
+int project_impl(int variant, int ni, int nj, int nk, float h, float dt, float U_in, const float* phi,
+                 const int8_t* bdesc, const float* us, const float* vs, const float* ws, float* u, float* v,
+                 float* w, double* pressure_out, double* rhs_out, double* st_out, float* uw_out, float* vw_out,
+                 float* ww_out, int* iterations_out, double* residual_out, double tol, int maxit) {
+  const bool sub = variant == 1;
   size_t n = (size_t)ni * nj * nk;
   size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
   std::vector<float> uw(nu), vw(nv), ww(nw);
@@ -522,8 +530,8 @@ int oracle_project(int ni, int nj, int nk, float h, float U_in, const float* phi
   auto US = [&](int i, int j, int k) { return us[lin(i, j, k, ni + 1, nj)]; };
   auto VS = [&](int i, int j, int k) { return vs[lin(i, j, k, ni, nj + 1)]; };
   auto WS = [&](int i, int j, int k) { return ws[lin(i, j, k, ni, nj)]; };
-  // inflow overwrite, :964-980
-  for (int k = 0; k < nk; ++k)
+  // inflow overwrite, :964-980 (main domain only)
+  for (int k = 0; k < nk && !sub; ++k)
     for (int j = 0; j < nj; ++j)
       for (int i = 0; i < ni; ++i)
         if (bdesc[lin(i, j, k, ni, nj)] == 1) {
@@ -543,51 +551,58 @@ int oracle_project(int ni, int nj, int nk, float h, float U_in, const float* phi
         double diag;
         double b = 0;
         float t;
-        t = UW(i + 1, j, k) / h2; diag = t; if (i < ni - 2) A.c(XP, r) = -t;
+        // the subdomain's term is w*dt/sqr(h) (SS/sub_domain.cpp:611), evaluated left to right
+        auto term = [&](float wgt) { return sub ? wgt * dt / h2 : wgt / h2; };
+        t = term(UW(i + 1, j, k)); diag = t; if (i < ni - 2) A.c(XP, r) = -t;
         b -= UW(i + 1, j, k) * U(i + 1, j, k) / h;
-        t = UW(i, j, k) / h2; diag += t; if (i >= 2) A.c(XM, r) = -t;
+        t = term(UW(i, j, k)); diag += t; if (i >= 2) A.c(XM, r) = -t;
         b += UW(i, j, k) * U(i, j, k) / h;
-        t = VW(i, j + 1, k) / h2; diag += t; if (j < nj - 2) A.c(YP, r) = -t;
+        t = term(VW(i, j + 1, k)); diag += t; if (j < nj - 2) A.c(YP, r) = -t;
         b -= VW(i, j + 1, k) * V(i, j + 1, k) / h;
-        t = VW(i, j, k) / h2; diag += t; if (j >= 2) A.c(YM, r) = -t;
+        t = term(VW(i, j, k)); diag += t; if (j >= 2) A.c(YM, r) = -t;
         b += VW(i, j, k) * V(i, j, k) / h;
-        t = WW(i, j, k + 1) / h2; diag += t; if (k < nk - 2) A.c(ZP, r) = -t;
+        t = term(WW(i, j, k + 1)); diag += t; if (k < nk - 2) A.c(ZP, r) = -t;
         b -= WW(i, j, k + 1) * W(i, j, k + 1) / h;
-        t = WW(i, j, k) / h2; diag += t; if (k >= 2) A.c(ZM, r) = -t;
+        t = term(WW(i, j, k)); diag += t; if (k >= 2) A.c(ZM, r) = -t;
         b += WW(i, j, k) * W(i, j, k) / h;
         A.c(D, r) = diag;
         if (diag > 0) {
           float sv = (UW(i + 1, j, k) - 1.0f) * US(i + 1, j, k) - (UW(i, j, k) - 1.0f) * US(i, j, k) +
                      (VW(i, j + 1, k) - 1.0f) * VS(i, j + 1, k) - (VW(i, j, k) - 1.0f) * VS(i, j, k) +
                      (WW(i, j, k + 1) - 1.0f) * WS(i, j, k + 1) - (WW(i, j, k) - 1.0f) * WS(i, j, k);
-          b += 1.0 / h * sv;
+          if (sub) b += 1 / h * sv;  // float 1/_hx, SS/sub_domain.cpp:716
+          else b += 1.0 / h * sv;
         }
         rhs[r] = b;
       }
   std::vector<double> p(n, 0.0);
   double res = 0;
   int it = 0;
-  int ok = amgpcg(A, rhs.data(), p.data(), 1e-6, 50, &res, &it);  // :1120
-  // gradient update, :1126-1200
+  int ok = amgpcg(A, rhs.data(), p.data(), tol, maxit, &res, &it);  // :1120, SS/sub_domain.cpp:739
+  // gradient update, :1126-1200 (SS/sub_domain.cpp:741-818 for the subdomain)
+  const int lo = sub ? 1 : 2, hi_i = sub ? ni - 1 : ni - 2, hi_j = sub ? nj - 1 : nj - 2, hi_k = sub ? nk - 1 : nk - 2;
+  auto grad = [&](float cur, double pc, double pm) {
+    return sub ? cur - dt * (float)(pc - pm) / h : cur - (float)(pc - pm) / h;
+  };
   for (int k = 1; k < nk - 1; ++k)
     for (int j = 1; j < nj - 1; ++j)
-      for (int i = 2; i <= ni - 2; ++i) {
+      for (int i = lo; i <= hi_i; ++i) {
         size_t r = lin(i, j, k, ni, nj);
-        if (UW(i, j, k) > 0) U(i, j, k) -= (float)(p[r] - p[r - 1]) / h;
+        if (UW(i, j, k) > 0) U(i, j, k) = grad(U(i, j, k), p[r], p[r - 1]);
         else U(i, j, k) = US(i, j, k);
       }
   for (int k = 1; k < nk - 1; ++k)
-    for (int j = 2; j <= nj - 2; ++j)
+    for (int j = lo; j <= hi_j; ++j)
       for (int i = 1; i < ni - 1; ++i) {
         size_t r = lin(i, j, k, ni, nj);
-        if (VW(i, j, k) > 0) V(i, j, k) -= (float)(p[r] - p[r - ni]) / h;
+        if (VW(i, j, k) > 0) V(i, j, k) = grad(V(i, j, k), p[r], p[r - ni]);
         else V(i, j, k) = VS(i, j, k);
       }
-  for (int k = 2; k <= nk - 2; ++k)
+  for (int k = lo; k <= hi_k; ++k)
     for (int j = 1; j < nj - 1; ++j)
       for (int i = 1; i < ni - 1; ++i) {
         size_t r = lin(i, j, k, ni, nj);
-        if (WW(i, j, k) > 0) W(i, j, k) -= (float)(p[r] - p[r - (size_t)ni * nj]) / h;
+        if (WW(i, j, k) > 0) W(i, j, k) = grad(W(i, j, k), p[r], p[r - (size_t)ni * nj]);
         else W(i, j, k) = WS(i, j, k);
       }
   if (pressure_out) std::memcpy(pressure_out, p.data(), sizeof(double) * n);
@@ -599,6 +614,29 @@ int oracle_project(int ni, int nj, int nk, float h, float U_in, const float* phi
   if (iterations_out) *iterations_out = it;
   if (residual_out) *residual_out = res;
   return ok;
+}
+}  // namespace
+
+extern "C" {
+
+// SmokeSolver3D::pcg_projection.  Same argument meaning as ref_project in
+// oracle/ref_harness.cpp.
+int oracle_project(int ni, int nj, int nk, float h, float U_in, const float* phi, const int8_t* bdesc,
+                   const float* us, const float* vs, const float* ws, float* u, float* v, float* w,
+                   double* pressure_out, double* rhs_out, double* st_out, float* uw_out, float* vw_out,
+                   float* ww_out, int* iterations_out, double* residual_out) {
+  return project_impl(0, ni, nj, nk, h, 1.0f, U_in, phi, bdesc, us, vs, ws, u, v, w, pressure_out, rhs_out, st_out,
+                      uw_out, vw_out, ww_out, iterations_out, residual_out, 1e-6, 50);
+}
+
+// SubDomainSolver::pcg_projection with the given tolerance / iterations (the
+// reference uses 1e-9 / 1000).
+int oracle_project_subdomain(int ni, int nj, int nk, float h, float dt, const float* phi, const float* us,
+                             const float* vs, const float* ws, float* u, float* v, float* w, double* pressure_out,
+                             double* rhs_out, double* st_out, int* iterations_out, double* residual_out, double tol,
+                             int maxit) {
+  return project_impl(1, ni, nj, nk, h, dt, 0.0f, phi, nullptr, us, vs, ws, u, v, w, pressure_out, rhs_out, st_out,
+                      nullptr, nullptr, nullptr, iterations_out, residual_out, tol, maxit);
 }
 
 // SubDomainSolver::advect_field, SS/sub_domain.cpp:191-235 (RK2 midpoint

@@ -48,6 +48,14 @@ def main():
                             pcg_ok=np.int32(ok), pcg_res=np.float64(res), pcg_it=np.int32(it),
                             n_levels=np.int32(len(levels)),
                             **{f"level{l}": lv for l, lv in enumerate(levels)})
+    # 1b. the nested subdomain's projection (dt-scaled, tolerance 1e-9)
+    pr = scenes.projection_problem(22, 19, 25, seed=13, solid_velocity=True)
+    out = R.project_subdomain(pr["ni"], pr["nj"], pr["nk"], pr["h"], 0.005, pr["phi"], pr["us"], pr["vs"], pr["ws"],
+                              pr["u"], pr["v"], pr["w"])
+    np.savez_compressed(os.path.join(OUT, "proj_sub.npz"), dims=np.array([22, 19, 25], np.int32),
+                        h=np.float32(pr["h"]), dt=np.float32(0.005),
+                        **{"in_" + k: pr[k] for k in ("phi", "us", "vs", "ws", "u", "v", "w")},
+                        **{"out_" + k: out[k] for k in ("u", "v", "w", "pressure", "rhs", "stencil")})
     # 2. multi-level hierarchy on a grid big enough for three levels
     st = scenes.uniform_laplacian(40, 37, 30)
     levels = R.levels(st)

@@ -167,3 +167,14 @@ def test_smoke_step_vs_reference(orc, ref):
         orc.smoke_step(20, p.h, p.dt, phi, b)
     for k in a:
         same(a[k], b[k])
+
+
+@pytest.mark.parametrize("dims,dt", [((21, 18, 17), 0.5), ((26, 30, 24), 0.005)])
+def test_subdomain_projection_vs_reference(orc, ref, dims, dt):
+    pr = scenes.projection_problem(*dims, seed=7, solid_velocity=True)
+    args = (pr["ni"], pr["nj"], pr["nk"], pr["h"], dt, pr["phi"], pr["us"], pr["vs"], pr["ws"], pr["u"], pr["v"],
+            pr["w"])
+    a, b = ref.project_subdomain(*args), orc.project_subdomain(*args)
+    for k in ("u", "v", "w", "pressure", "rhs", "stencil"):
+        same(a[k], b[k])
+    assert b["ok"]

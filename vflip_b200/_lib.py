@@ -52,6 +52,8 @@ SIGNATURES = {
     "vflip_assemble": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "vflip_project": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _I,
                            C.POINTER(SolveStatsC)]),
+    "vflip_project_subdomain": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _D, _I,
+                                     C.POINTER(SolveStatsC)]),
     "vflip_advect_rk2_linear": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _P, _P]),
     "vflip_advect_rk2_linear2": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _P, _P, _P, _P]),
     "vflip_delta": (_I, [_P, _SZ, _P, _P, _P]),

@@ -131,12 +131,16 @@ __global__ void inflow_kernel(const int8_t* __restrict__ bdesc, float* __restric
 // i.e. Dirichlet p = 0 on the ring).  Writes the FP64 operator (diag, +x,
 // +y, +z; the -x/-y/-z couplings the reference also stores are the +x/+y/+z
 // couplings of the neighbour, equal by construction) and the FP64 rhs.
+// variant 0: SmokeSolver3D::pcg_projection; variant 1:
+// SubDomainSolver::pcg_projection (sub_domain.cpp:560-729): the operator
+// terms carry the time step, w*dt/h^2, and the solid term is scaled by the
+// float 1/h instead of the double 1.0/h.
 __global__ void assemble_kernel(const float* __restrict__ u, const float* __restrict__ v, const float* __restrict__ w,
                                 const float* __restrict__ uw, const float* __restrict__ vw,
                                 const float* __restrict__ ww, const float* __restrict__ us,
                                 const float* __restrict__ vs, const float* __restrict__ ws, double* __restrict__ diag,
                                 double* __restrict__ xp, double* __restrict__ yp, double* __restrict__ zp,
-                                double* __restrict__ rhs, float h, int ni, int nj, int nk) {
+                                double* __restrict__ rhs, float h, int ni, int nj, int nk, int variant, float dt) {
   const size_t n = (size_t)ni * nj * nk;
   const float h2 = h * h;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
@@ -146,23 +150,26 @@ __global__ void assemble_kernel(const float* __restrict__ u, const float* __rest
       const size_t iu0 = lin3(i, j, k, ni + 1, nj), iu1 = lin3(i + 1, j, k, ni + 1, nj);
       const size_t iv0 = lin3(i, j, k, ni, nj + 1), iv1 = lin3(i, j + 1, k, ni, nj + 1);
       const size_t iw0 = lin3(i, j, k, ni, nj), iw1 = lin3(i, j, k + 1, ni, nj);
+      const bool sub = variant == 1;
+      auto term = [&](float wgt) { return sub ? (wgt * dt) / h2 : wgt / h2; };
       float t;
-      t = uw[iu1] / h2; d = (double)t; if (i < ni - 2) cx = (double)(-t);
+      t = term(uw[iu1]); d = (double)t; if (i < ni - 2) cx = (double)(-t);
       b = b - (double)(uw[iu1] * u[iu1] / h);
-      t = uw[iu0] / h2; d = d + (double)t;
+      t = term(uw[iu0]); d = d + (double)t;
       b = b + (double)(uw[iu0] * u[iu0] / h);
-      t = vw[iv1] / h2; d = d + (double)t; if (j < nj - 2) cy = (double)(-t);
+      t = term(vw[iv1]); d = d + (double)t; if (j < nj - 2) cy = (double)(-t);
       b = b - (double)(vw[iv1] * v[iv1] / h);
-      t = vw[iv0] / h2; d = d + (double)t;
+      t = term(vw[iv0]); d = d + (double)t;
       b = b + (double)(vw[iv0] * v[iv0] / h);
-      t = ww[iw1] / h2; d = d + (double)t; if (k < nk - 2) cz = (double)(-t);
+      t = term(ww[iw1]); d = d + (double)t; if (k < nk - 2) cz = (double)(-t);
       b = b - (double)(ww[iw1] * w[iw1] / h);
-      t = ww[iw0] / h2; d = d + (double)t;
+      t = term(ww[iw0]); d = d + (double)t;
       b = b + (double)(ww[iw0] * w[iw0] / h);
       if (d > 0) {
         float sv = (uw[iu1] - 1.0f) * us[iu1] - (uw[iu0] - 1.0f) * us[iu0] + (vw[iv1] - 1.0f) * vs[iv1] -
                    (vw[iv0] - 1.0f) * vs[iv0] + (ww[iw1] - 1.0f) * ws[iw1] - (ww[iw0] - 1.0f) * ws[iw0];
-        b = b + (1.0 / (double)h) * (double)sv;
+        if (sub) b = b + (double)((1.0f / h) * sv);
+        else b = b + (1.0 / (double)h) * (double)sv;
       }
     }
     diag[e] = d;
@@ -177,38 +184,46 @@ __global__ void assemble_kernel(const float* __restrict__ u, const float* __rest
 // between two interior cells (u: i in [2, ni-2], j,k in [1, n-2]; v, w
 // analogous) u -= (float)(p_i - p_{i-1}) / h where the face is open, else
 // u = u_solid.  Other faces are left untouched, as in the reference.
+// variant 1 (SubDomainSolver::pcg_projection, sub_domain.cpp:741-818):
+// faces i in [1, ni-1] (all faces between cells of the grid) and
+// u -= dt * (float)(p_i - p_{i-1}) / h.
 template <typename P>
 __global__ void gradient_kernel(const P* __restrict__ p, float* __restrict__ u, float* __restrict__ v,
                                 float* __restrict__ w, const float* __restrict__ uw, const float* __restrict__ vw,
                                 const float* __restrict__ ww, const float* __restrict__ us,
                                 const float* __restrict__ vs, const float* __restrict__ ws, float h, int ni, int nj,
-                                int nk) {
+                                int nk, int variant, float dt) {
   const size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
   const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nu + nv + nw;
        e += (size_t)gridDim.x * blockDim.x) {
+    const bool sub = variant == 1;
+    const int lo = sub ? 0 : 1;  // first face index excluded: faces > lo
+    const int hi = sub ? 0 : 1;  // faces < n - hi
+    auto upd = [&](float cur, double pc, double pm, float wgt, float solid) {
+      if (!(wgt > 0)) return solid;
+      float diff = (float)(pc - pm);
+      return sub ? cur - (dt * diff) / h : cur - diff / h;
+    };
     if (e < nu) {
       int i = (int)(e % (ni + 1)), j = (int)((e / (ni + 1)) % nj), k = (int)(e / ((size_t)(ni + 1) * nj));
-      if (k < nk - 1 && k > 0 && j < nj - 1 && j > 0 && i < ni - 1 && i > 1) {
+      if (k < nk - 1 && k > 0 && j < nj - 1 && j > 0 && i < ni - hi && i > lo) {
         size_t c = lin3(i, j, k, ni, nj);
-        if (uw[e] > 0) u[e] = u[e] - (float)((double)p[c] - (double)p[c - 1]) / h;
-        else u[e] = us[e];
+        u[e] = upd(u[e], (double)p[c], (double)p[c - 1], uw[e], us[e]);
       }
     } else if (e < nu + nv) {
       size_t f = e - nu;
       int i = (int)(f % ni), j = (int)((f / ni) % (nj + 1)), k = (int)(f / ((size_t)ni * (nj + 1)));
-      if (k < nk - 1 && k > 0 && j > 1 && j < nj - 1 && i < ni - 1 && i > 0) {
+      if (k < nk - 1 && k > 0 && j > lo && j < nj - hi && i < ni - 1 && i > 0) {
         size_t c = lin3(i, j, k, ni, nj);
-        if (vw[f] > 0) v[f] = v[f] - (float)((double)p[c] - (double)p[c - sy]) / h;
-        else v[f] = vs[f];
+        v[f] = upd(v[f], (double)p[c], (double)p[c - sy], vw[f], vs[f]);
       }
     } else {
       size_t f = e - nu - nv;
       int i = (int)(f % ni), j = (int)((f / ni) % nj), k = (int)(f / ((size_t)ni * nj));
-      if (k > 1 && k < nk - 1 && j < nj - 1 && j > 0 && i < ni - 1 && i > 0) {
+      if (k > lo && k < nk - hi && j < nj - 1 && j > 0 && i < ni - 1 && i > 0) {
         size_t c = lin3(i, j, k, ni, nj);
-        if (ww[f] > 0) w[f] = w[f] - (float)((double)p[c] - (double)p[c - sz]) / h;
-        else w[f] = ws[f];
+        w[f] = upd(w[f], (double)p[c], (double)p[c - sz], ww[f], ws[f]);
       }
     }
   }

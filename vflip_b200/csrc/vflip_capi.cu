@@ -1006,30 +1006,39 @@ int vflip_face_weights(vflip_ctx* ctx, int ni, int nj, int nk, const float* noda
   return VFLIP_OK;
 }
 
-int vflip_assemble(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, const float* nodal_phi,
-                   const int8_t* bdesc, const float* us, const float* vs, const float* ws, float* u, float* v,
-                   float* w, double* diag, double* xp, double* yp, double* zp, double* rhs) {
+}  // extern "C"
+
+namespace {
+
+// variant 0: SmokeSolver3D::pcg_projection (inflow overwrite, 1/h^2 terms);
+// variant 1: SubDomainSolver::pcg_projection (no inflow, dt/h^2 terms)
+int assemble_impl(vflip_ctx* ctx, int variant, int ni, int nj, int nk, float h, float dt, float U_in,
+                  const float* nodal_phi, const int8_t* bdesc, const float* us, const float* vs, const float* ws,
+                  float* u, float* v, float* w, double* diag, double* xp, double* yp, double* zp, double* rhs) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
-  if (!nodal_phi || !bdesc || !us || !vs || !ws || !u || !v || !w || !diag || !xp || !yp || !zp || !rhs)
+  if (!nodal_phi || (variant == 0 && !bdesc) || !us || !vs || !ws || !u || !v || !w || !diag || !xp || !yp || !zp ||
+      !rhs)
     return ctx->fail(VFLIP_ERR_ARG, "null pointer");
   size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
   float* wts;
   VF_ALLOC(wts, float, "face_weights", nu + nv + nw);
   if ((rc = vflip_face_weights(ctx, ni, nj, nk, nodal_phi, wts, wts + nu, wts + nu + nv))) return rc;
   size_t n = (size_t)ni * nj * nk;
-  inflow_kernel<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(bdesc, u, v, w, U_in, ni, nj, nk);
-  VF_LAUNCH_CHECK();
+  if (variant == 0) {
+    inflow_kernel<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(bdesc, u, v, w, U_in, ni, nj, nk);
+    VF_LAUNCH_CHECK();
+  }
   assemble_kernel<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
-      u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, diag, xp, yp, zp, rhs, h, ni, nj, nk);
+      u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, diag, xp, yp, zp, rhs, h, ni, nj, nk, variant, dt);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
 }
 
-int vflip_project(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, const float* nodal_phi,
-                  const int8_t* bdesc, const float* us, const float* vs, const float* ws, float* u, float* v,
-                  float* w, double* pressure, double tolerance_factor, int max_iterations,
-                  vflip_solve_stats* stats) {
+int project_impl(vflip_ctx* ctx, int variant, int ni, int nj, int nk, float h, float dt, float U_in,
+                 const float* nodal_phi, const int8_t* bdesc, const float* us, const float* vs, const float* ws,
+                 float* u, float* v, float* w, double* pressure, double tolerance_factor, int max_iterations,
+                 vflip_solve_stats* stats) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   size_t n = (size_t)ni * nj * nk;
@@ -1041,8 +1050,8 @@ int vflip_project(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, c
   cudaEvent_t e0;
   VF_CUDA(cudaEventCreate(&e0));
   VF_CUDA(cudaEventRecord(e0, ctx->stream));
-  if ((rc = vflip_assemble(ctx, ni, nj, nk, h, U_in, nodal_phi, bdesc, us, vs, ws, u, v, w, op, op + n, op + 2 * n,
-                           op + 3 * n, rhs))) {
+  if ((rc = assemble_impl(ctx, variant, ni, nj, nk, h, dt, U_in, nodal_phi, bdesc, us, vs, ws, u, v, w, op,
+                          op + n, op + 2 * n, op + 3 * n, rhs))) {
     cudaEventDestroy(e0);
     return rc;
   }
@@ -1056,7 +1065,7 @@ int vflip_project(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, c
   size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
   float* wts = (float*)ctx->buf("face_weights", sizeof(float) * (nu + nv + nw));
   gradient_kernel<double><<<grid_for(nu + nv + nw, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
-      p, u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, h, ni, nj, nk);
+      p, u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, h, ni, nj, nk, variant, dt);
   ++ctx->launches;
   cudaError_t le = cudaGetLastError();
   if (le != cudaSuccess) {
@@ -1074,6 +1083,33 @@ int vflip_project(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, c
     stats->solve_ms = ms;
   }
   return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vflip_assemble(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, const float* nodal_phi,
+                   const int8_t* bdesc, const float* us, const float* vs, const float* ws, float* u, float* v,
+                   float* w, double* diag, double* xp, double* yp, double* zp, double* rhs) {
+  return assemble_impl(ctx, 0, ni, nj, nk, h, 1.0f, U_in, nodal_phi, bdesc, us, vs, ws, u, v, w, diag, xp, yp, zp,
+                       rhs);
+}
+
+int vflip_project_subdomain(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* nodal_phi,
+                            const float* us, const float* vs, const float* ws, float* u, float* v, float* w,
+                            double* pressure, double tolerance_factor, int max_iterations,
+                            vflip_solve_stats* stats) {
+  return project_impl(ctx, 1, ni, nj, nk, h, dt, 0.0f, nodal_phi, nullptr, us, vs, ws, u, v, w, pressure,
+                      tolerance_factor, max_iterations, stats);
+}
+
+int vflip_project(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, const float* nodal_phi,
+                  const int8_t* bdesc, const float* us, const float* vs, const float* ws, float* u, float* v,
+                  float* w, double* pressure, double tolerance_factor, int max_iterations,
+                  vflip_solve_stats* stats) {
+  return project_impl(ctx, 0, ni, nj, nk, h, 1.0f, U_in, nodal_phi, bdesc, us, vs, ws, u, v, w, pressure,
+                      tolerance_factor, max_iterations, stats);
 }
 
 int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,

@@ -205,6 +205,19 @@ class Solver:
         self._check(rc)
         return rc == 0, pressure, SolveStats.from_c(st)
 
+    def project_subdomain(self, ni, nj, nk, h, dt, nodal_phi, us, vs, ws, u, v, w, pressure=None,
+                          tolerance_factor=1e-9, max_iterations=1000):
+        """SubDomainSolver::pcg_projection (dt-scaled operator, tolerance 1e-9
+        and 1000 iterations by default, as the reference calls it)."""
+        if pressure is None:
+            pressure = self._empty((nk, nj, ni), torch.float64)
+        st = SolveStatsC()
+        rc = self.lib.vflip_project_subdomain(self.ctx, ni, nj, nk, float(h), float(dt), _p(nodal_phi), _p(us),
+                                              _p(vs), _p(ws), _p(u), _p(v), _p(w), _p(pressure),
+                                              float(tolerance_factor), int(max_iterations), C.byref(st))
+        self._check(rc)
+        return rc == 0, pressure, SolveStats.from_c(st)
+
     # ------------------------------------------------------------- advection
     def advect_rk2_linear(self, ni, nj, nk, h, dt, u, v, w, field, offsets, out=None):
         fnz, fny, fnx = field.shape
