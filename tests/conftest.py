@@ -58,6 +58,7 @@ def gpu_solver():
     build.build()
     s = {p: Solver(precision=p) for p in (0, 1, 2)}
     s["f32_plain"] = Solver(precision=1, sweep_kernel=1)  # the non-pipelined smoother
+    s["mix_plain"] = Solver(precision=2, sweep_kernel=1)
     yield s
     for v in s.values():
         v.close()

@@ -95,6 +95,10 @@ def test_pipelined_sweep_matches_plain_kernel(gpu_solver, orc, dims):
     a = gpu_solver[1].vcycle(st, b).cpu().numpy()
     c = gpu_solver["f32_plain"].vcycle(st, b).cpu().numpy()
     assert np.array_equal(a, c)
+    # mixed precision: BF16 coarse operators through both smoother kernels
+    a = gpu_solver[2].vcycle(st, b).cpu().numpy()
+    c = gpu_solver["mix_plain"].vcycle(st, b).cpu().numpy()
+    assert np.array_equal(a, c)
 
 
 @pytest.mark.parametrize("shape", [(1, 0, 0, 1), (2, 0, 0, 1), (3, 0, 0, 1), (2, 2, 2, 2), (1, 3, 3, 2), (3, 1, 5, 1)])

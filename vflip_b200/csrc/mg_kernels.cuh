@@ -244,14 +244,15 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_kernel(SweepArgs<S, V> a) {
 // alternate between consecutive copy groups.  Every wait is bounded: on a
 // timeout the CTA records the failure in *error, drains its own copies (again
 // bounded) and returns.
+template <typename S>
 struct TmaSweepArgs {
   const float* x_in;
   float* x_out;
   const float* b;
-  const float* diag;
-  const float* xp;
-  const float* yp;
-  const float* zp;
+  const S* diag;
+  const S* xp;
+  const S* yp;
+  const S* zp;
   const float* xc;
   int ni, nj, nk;
   int cni, cnj;
@@ -270,10 +271,37 @@ constexpr int kTmaMaxDepth = 3;
 // p-2 .. p+1 plus D in flight; b/diag/xp (tyo + 2 rows) and yp (tyo + 3)
 // for planes p-1, p plus D; zp (tyo + 2) for p-2 .. p plus D; coarse x
 // follows the x ring.
-__host__ __device__ constexpr size_t tma_sweep_smem_floats(int ni, int tyo, int depth, int crows, int cni) {
-  return (size_t)ni * ((4 + depth) * (tyo + 4) + 3 * (2 + depth) * (tyo + 2) + (2 + depth) * (tyo + 3) +
-                       (3 + depth) * (tyo + 2)) +
-         (size_t)(4 + depth) * crows * cni;
+// Layout (4-byte units unless noted): x ring, b ring (FP32), then the
+// coefficient rings diag, xp, yp, zp in elements of S (FP32 or BF16),
+// then the coarse-x ring (FP32) at the next 16-byte boundary.
+struct TmaLayout {
+  int xslot, cslot, yslot, cplane;
+  int oX, oB, oC;        // float offsets: x ring, b ring, start of the coefficient region
+  int cD, cXP, cYP, cZP; // S-element offsets inside the coefficient region
+  int oXC;               // float offset of the coarse-x ring
+  size_t bytes;
+};
+
+template <typename S>
+__host__ __device__ inline TmaLayout tma_layout(int ni, int tyo, int depth, int crows, int cni) {
+  TmaLayout L;
+  const int RX = 4 + depth, RC = 2 + depth, RZ = 3 + depth;
+  L.xslot = (tyo + 4) * ni;
+  L.cslot = (tyo + 2) * ni;
+  L.yslot = (tyo + 3) * ni;
+  L.cplane = crows * cni;
+  L.oX = 0;
+  L.oB = L.oX + RX * L.xslot;
+  L.oC = L.oB + RC * L.cslot;
+  L.cD = 0;
+  L.cXP = L.cD + RC * L.cslot;
+  L.cYP = L.cXP + RC * L.cslot;
+  L.cZP = L.cYP + RC * L.yslot;
+  const size_t coef_bytes = (size_t)(L.cZP + RZ * L.cslot) * sizeof(S);
+  const size_t xc_byte = ((size_t)L.oC * 4 + coef_bytes + 15) / 16 * 16;
+  L.oXC = (int)(xc_byte / 4);
+  L.bytes = xc_byte + (size_t)RX * L.cplane * 4;
+  return L;
 }
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -306,8 +334,8 @@ __device__ __forceinline__ void tma_bulk_g2s(unsigned dst, const void* src, unsi
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
-template <bool ZERO_X, bool PROLONG, bool DOT, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
+template <typename S, bool ZERO_X, bool PROLONG, bool DOT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs<S> a) {
   extern __shared__ __align__(128) float sm[];
   constexpr int NB = kTmaMaxDepth + 2;  // mbarrier ring
   __shared__ __align__(8) unsigned long long bars[NB];
@@ -315,11 +343,14 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   const int ni = a.ni, nj = a.nj, nk = a.nk, tyo = a.tyo, D = a.depth;
   const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
-  const int xslot = (tyo + 4) * ni, cslot = (tyo + 2) * ni, yslot = (tyo + 3) * ni;
-  const int cplane = a.crows_max * a.cni;
+  const TmaLayout Ly = tma_layout<S>(ni, tyo, D, a.crows_max, a.cni);
+  const int xslot = Ly.xslot, cslot = Ly.cslot, yslot = Ly.yslot, cplane = Ly.cplane;
   const int RX = 4 + D, RC = 2 + D, RZ = 3 + D;  // ring lengths
-  const int oX = 0, oB = oX + RX * xslot, oD = oB + RC * cslot, oXP = oD + RC * cslot, oYP = oXP + RC * cslot,
-            oZP = oYP + RC * yslot, oXC = oZP + RZ * cslot;
+  const int oX = Ly.oX, oB = Ly.oB, oXC = Ly.oXC;
+  const int oD = Ly.cD, oXP = Ly.cXP, oYP = Ly.cYP, oZP = Ly.cZP;  // in elements of S
+  const S* cs = reinterpret_cast<const S*>(sm + Ly.oC);
+  const unsigned cbase_b = 4u * (unsigned)Ly.oC;  // byte offset of the coefficient region
+  constexpr unsigned ES = sizeof(S);
   const int P = (ni + 1) / 2;
   const int tx = threadIdx.x, ty = threadIdx.y, bx = blockDim.x, by = blockDim.y;
 
@@ -356,8 +387,8 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
     const bool hx0 = !ZERO_X && qx0 >= 0 && qx0 < nk, hx1 = !ZERO_X && qx1 >= 0 && qx1 < nk;
     const bool hc = qc >= 0 && qc < nk, hz = qz >= 0 && qz < nk;
     const unsigned xb = xrows * ni * 4 + (PROLONG ? (cr1 - cr0) * a.cni * 4 : 0);
-    const unsigned bytes = (hx0 ? xb : 0) + (hx1 ? xb : 0) + (hc ? (3 * crows + yrows) * ni * 4 : 0) +
-                           (hz ? crows * ni * 4 : 0);
+    const unsigned bytes = (hx0 ? xb : 0) + (hx1 ? xb : 0) +
+                           (hc ? crows * ni * 4 + (2 * crows + yrows) * ni * ES : 0) + (hz ? crows * ni * ES : 0);
     fence_proxy_async();
     mbar_expect_tx(bar, bytes);
     for (int h = 0; h < 2; ++h) {
@@ -371,11 +402,12 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
     if (hc) {
       const size_t o = qc * sz + jred0 * sy;
       tma_bulk_g2s(sbase + 4u * (oB + sc * cslot), a.b + o, crows * ni * 4, bar);
-      tma_bulk_g2s(sbase + 4u * (oD + sc * cslot), a.diag + o, crows * ni * 4, bar);
-      tma_bulk_g2s(sbase + 4u * (oXP + sc * cslot), a.xp + o, crows * ni * 4, bar);
-      tma_bulk_g2s(sbase + 4u * (oYP + sc * yslot), a.yp + qc * sz + jy0 * sy, yrows * ni * 4, bar);
+      tma_bulk_g2s(sbase + cbase_b + ES * (oD + sc * cslot), a.diag + o, crows * ni * ES, bar);
+      tma_bulk_g2s(sbase + cbase_b + ES * (oXP + sc * cslot), a.xp + o, crows * ni * ES, bar);
+      tma_bulk_g2s(sbase + cbase_b + ES * (oYP + sc * yslot), a.yp + qc * sz + jy0 * sy, yrows * ni * ES, bar);
     }
-    if (hz) tma_bulk_g2s(sbase + 4u * (oZP + szs * cslot), a.zp + qz * sz + jred0 * sy, crows * ni * 4, bar);
+    if (hz)
+      tma_bulk_g2s(sbase + cbase_b + ES * (oZP + szs * cslot), a.zp + qz * sz + jred0 * sy, crows * ni * ES, bar);
   };
   // all threads: wait for group g; block-uniform result
   auto wait_group = [&](int g) -> bool {
@@ -398,13 +430,13 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs a) {
         if (i >= ni) continue;
         const int s = xr + i, c = cr + i, y = yr + i;
         float sum = 0.0f;
-        if (zlo) sum = sum + sm[czm + c] * sm[xm1 + s];
-        if (ylo) sum = sum + sm[cy + y - ni] * sm[x0 + s - ni];
-        if (i > 0) sum = sum + sm[cx + c - 1] * sm[x0 + s - 1];
-        if (i < ni - 1) sum = sum + sm[cx + c] * sm[x0 + s + 1];
-        if (yhi) sum = sum + sm[cy + y] * sm[x0 + s + ni];
-        if (zhi) sum = sum + sm[cz + c] * sm[xp1 + s];
-        const float d = sm[cd + c];
+        if (zlo) sum = sum + float(ldv(cs + czm + c)) * sm[xm1 + s];
+        if (ylo) sum = sum + float(ldv(cs + cy + y - ni)) * sm[x0 + s - ni];
+        if (i > 0) sum = sum + float(ldv(cs + cx + c - 1)) * sm[x0 + s - 1];
+        if (i < ni - 1) sum = sum + float(ldv(cs + cx + c)) * sm[x0 + s + 1];
+        if (yhi) sum = sum + float(ldv(cs + cy + y)) * sm[x0 + s + ni];
+        if (zhi) sum = sum + float(ldv(cs + cz + c)) * sm[xp1 + s];
+        const float d = float(ldv(cs + cd + c));
         sm[x0 + s] = (d != 0.0f) ? gs_div(sm[cb + c] - sum, d) : 0.0f;
       }
     }

@@ -216,14 +216,15 @@ constexpr int kTmaBlock = 512;
 // row tiles (their halo rows then come from L2); the 4 redundant halo planes
 // of each plane range are traded against load balance.  Fields of the
 // context configuration override the choice (0 = automatic).
+template <typename S>
 bool tma_shape(const vflip_config& cfg, const Dims& d, const Dims* cd, bool prolong, int num_sms, TmaShape& o) {
-  if (d.ni % 4 != 0) return false;
+  if (d.ni % 4 != 0 || (d.ni * sizeof(S)) % 16 != 0) return false;
   if (prolong && (!cd || cd->ni % 4 != 0)) return false;
   const int cni = prolong ? cd->ni : 0;
   const int depth = cfg.smoother_depth > 0 ? std::min(cfg.smoother_depth, kTmaMaxDepth) : 2;
   const int cps = cfg.smoother_ctas_per_sm > 0 ? std::min(cfg.smoother_ctas_per_sm, 2) : 1;
   const size_t budget = cps == 1 ? kTmaSmemMax : kTmaSmemMax / 2 - 1024;
-  auto bytes = [&](int t) { return 4 * tma_sweep_smem_floats(d.ni, t, depth, prolong ? (t + 7) / 2 : 0, cni); };
+  auto bytes = [&](int t) { return tma_layout<S>(d.ni, t, depth, prolong ? (t + 7) / 2 : 0, cni).bytes; };
   int tyo_max = 0;
   for (int t = 1; t <= d.nj; ++t) {
     if (bytes(t) > budget) break;
@@ -264,9 +265,9 @@ bool tma_shape(const vflip_config& cfg, const Dims& d, const Dims* cd, bool prol
   return o.smem <= budget;
 }
 
-template <bool Z, bool P, bool D>
-int launch_tma_t(vflip_ctx* ctx, const TmaSweepArgs& a, const TmaShape& sh) {
-  auto kern = rbgs_sweep_tma_kernel<Z, P, D, kTmaBlock>;
+template <typename S, bool Z, bool P, bool D>
+int launch_tma_t(vflip_ctx* ctx, const TmaSweepArgs<S>& a, const TmaShape& sh) {
+  auto kern = rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlock>;
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemMax);
@@ -296,19 +297,19 @@ template <typename S, typename V>
 int sweep_tma(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_out, const V* xc,
               const Dims* cd, double* dot_partial, int* nblocks_out, bool* used) {
   *used = false;
-  if (!std::is_same<V, float>::value || !std::is_same<S, float>::value || ctx->cfg.sweep_kernel == 1)
+  if (!std::is_same<V, float>::value || std::is_same<S, double>::value || ctx->cfg.sweep_kernel == 1)
     return VFLIP_OK;
   TmaShape sh;
   const bool pro = xc != nullptr;
-  if (!tma_shape(ctx->cfg, L.d, cd, pro, ctx->num_sms, sh)) return VFLIP_OK;
-  TmaSweepArgs a;
+  if (!tma_shape<S>(ctx->cfg, L.d, cd, pro, ctx->num_sms, sh)) return VFLIP_OK;
+  TmaSweepArgs<S> a;
   a.x_in = (const float*)x_in;
   a.x_out = (float*)x_out;
   a.b = (const float*)b;
-  a.diag = (const float*)L.diag;
-  a.xp = (const float*)L.xp;
-  a.yp = (const float*)L.yp;
-  a.zp = (const float*)L.zp;
+  a.diag = L.diag;
+  a.xp = L.xp;
+  a.yp = L.yp;
+  a.zp = L.zp;
   a.xc = (const float*)xc;
   a.ni = L.d.ni;
   a.nj = L.d.nj;
@@ -324,12 +325,12 @@ int sweep_tma(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V
   if (nblocks_out) *nblocks_out = sh.gy * sh.gz;
   *used = true;
   bool zero = (x_in == nullptr), dot = (dot_partial != nullptr);
-  if (zero && !pro && !dot) return launch_tma_t<true, false, false>(ctx, a, sh);
-  if (zero && !pro && dot) return launch_tma_t<true, false, true>(ctx, a, sh);
-  if (!zero && pro && !dot) return launch_tma_t<false, true, false>(ctx, a, sh);
-  if (!zero && pro && dot) return launch_tma_t<false, true, true>(ctx, a, sh);
-  if (!zero && !pro && !dot) return launch_tma_t<false, false, false>(ctx, a, sh);
-  if (!zero && !pro && dot) return launch_tma_t<false, false, true>(ctx, a, sh);
+  if (zero && !pro && !dot) return launch_tma_t<S, true, false, false>(ctx, a, sh);
+  if (zero && !pro && dot) return launch_tma_t<S, true, false, true>(ctx, a, sh);
+  if (!zero && pro && !dot) return launch_tma_t<S, false, true, false>(ctx, a, sh);
+  if (!zero && pro && dot) return launch_tma_t<S, false, true, true>(ctx, a, sh);
+  if (!zero && !pro && !dot) return launch_tma_t<S, false, false, false>(ctx, a, sh);
+  if (!zero && !pro && dot) return launch_tma_t<S, false, false, true>(ctx, a, sh);
   return ctx->fail(VFLIP_ERR_ARG, "sweep: prolongation needs an incoming x");
 }
 
