@@ -27,23 +27,27 @@ struct GridView {
 // x / h exactly as IEEE division; a multiplication when h is a power of two
 __device__ __forceinline__ double div_h(double x, const GridView& g) { return g.inv_h != 0.0 ? x * g.inv_h : x / g.h; }
 
-__device__ __forceinline__ float grid_at(const GridView& g, int i, int j, int k) {
-  i = i < 0 ? 0 : (i > g.nx - 1 ? g.nx - 1 : i);
-  j = j < 0 ? 0 : (j > g.ny - 1 ? g.ny - 1 : j);
-  k = k < 0 ? 0 : (k > g.nz - 1 ? g.nz - 1 : k);
-  return __ldg(g.d + lin3(i, j, k, g.nx, g.ny));
-}
+__device__ __forceinline__ int clampi(int v, int hi) { return v < 0 ? 0 : (v > hi ? hi : v); }
 
 __device__ __forceinline__ double lerp_d(double a, double b, double c) { return (1.0 - c) * a + c * b; }
 
+// The eight corners share three clamped coordinate pairs; addresses are
+// 32-bit element offsets (every grid here has fewer than 2^31 elements).
 __device__ __forceinline__ float sample_linear(const GridView& g, double wx, double wy, double wz) {
   double gx = div_h(wx, g) + g.ox, gy = div_h(wy, g) + g.oy, gz = div_h(wz, g) + g.oz;
   int i = (int)floor(gx), j = (int)floor(gy), k = (int)floor(gz);
   double cx = gx - (double)i, cy = gy - (double)j, cz = gz - (double)k;
-  double v1 = lerp_d(lerp_d(grid_at(g, i, j, k), grid_at(g, i + 1, j, k), cx),
-                     lerp_d(grid_at(g, i, j + 1, k), grid_at(g, i + 1, j + 1, k), cx), cy);
-  double v2 = lerp_d(lerp_d(grid_at(g, i, j, k + 1), grid_at(g, i + 1, j, k + 1), cx),
-                     lerp_d(grid_at(g, i, j + 1, k + 1), grid_at(g, i + 1, j + 1, k + 1), cx), cy);
+  const int i0 = clampi(i, g.nx - 1), i1 = clampi(i + 1, g.nx - 1);
+  const int sy = g.nx, sz = g.nx * g.ny;
+  const int j0 = clampi(j, g.ny - 1) * sy, j1 = clampi(j + 1, g.ny - 1) * sy;
+  const int k0 = clampi(k, g.nz - 1) * sz, k1 = clampi(k + 1, g.nz - 1) * sz;
+  const float* d = g.d;
+  const double a000 = __ldg(d + (i0 + j0 + k0)), a100 = __ldg(d + (i1 + j0 + k0));
+  const double a010 = __ldg(d + (i0 + j1 + k0)), a110 = __ldg(d + (i1 + j1 + k0));
+  const double a001 = __ldg(d + (i0 + j0 + k1)), a101 = __ldg(d + (i1 + j0 + k1));
+  const double a011 = __ldg(d + (i0 + j1 + k1)), a111 = __ldg(d + (i1 + j1 + k1));
+  double v1 = lerp_d(lerp_d(a000, a100, cx), lerp_d(a010, a110, cx), cy);
+  double v2 = lerp_d(lerp_d(a001, a101, cx), lerp_d(a011, a111, cx), cy);
   return (float)lerp_d(v1, v2, cz);
 }
 
@@ -64,14 +68,19 @@ __device__ __forceinline__ void node_world(const GridView& f, size_t e, float h,
   wz = (float)(((double)(float)k - f.oz) * (double)h);
 }
 
+// Each block owns a contiguous run of `per_block` nodes (so the blocks in
+// flight cover a compact slab and the gathers of neighbouring blocks hit
+// L2), walked two nodes per thread at a time.
 __global__ void advect_rk2_kernel(GridView u, GridView v, GridView w, GridView f, float* __restrict__ out,
-                                  GridView f2, float* __restrict__ out2, float h, float dt) {
+                                  GridView f2, float* __restrict__ out2, float h, float dt, int per_block) {
   const size_t n = (size_t)f.nx * f.ny * f.nz;
-  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t stride = blockDim.x;
   const double hdt = 0.5 * (double)dt;
-  for (size_t e0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e0 < n; e0 += 2 * stride) {
+  const size_t beg = (size_t)blockIdx.x * per_block;
+  const size_t end = beg + per_block < n ? beg + per_block : n;
+  for (size_t e0 = beg + threadIdx.x; e0 < end; e0 += 2 * stride) {
     const size_t e1 = e0 + stride;
-    const bool two = e1 < n;
+    const bool two = e1 < end;
     float wx0, wy0, wz0, wx1 = 0, wy1 = 0, wz1 = 0;
     node_world(f, e0, h, wx0, wy0, wz0);
     if (two) node_world(f, e1, h, wx1, wy1, wz1);

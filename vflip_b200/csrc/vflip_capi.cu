@@ -707,7 +707,8 @@ int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* re
 int check_dims(vflip_ctx* ctx, int ni, int nj, int nk) {
   if (!ctx) return VFLIP_ERR_ARG;
   if (ni <= 0 || nj <= 0 || nk <= 0) return ctx->fail(VFLIP_ERR_ARG, "grid dimensions must be positive");
-  if ((double)ni * nj * nk > 2.0e9) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
+  // element offsets inside kernels are 32-bit for the face grids too
+  if ((double)(ni + 1) * (nj + 1) * (nk + 1) > 2147483647.0) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
   return VFLIP_OK;
 }
 
@@ -1131,8 +1132,10 @@ int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, fl
   GridView gf{field, fnx, fny, fnz, (double)h, ox, oy, oz, ih};
   GridView gf2{field2, fnx, fny, fnz, (double)h, ox, oy, oz, ih};
   size_t n = (size_t)fnx * fny * fnz;
-  advect_rk2_kernel<<<grid_for((n + 1) / 2, 256, ctx->num_sms), 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2,
-                                                                                     field2 ? out2 : nullptr, h, dt);
+  const int per_block = 256 * 8;
+  const unsigned blocks = (unsigned)((n + per_block - 1) / per_block);
+  advect_rk2_kernel<<<blocks, 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2, field2 ? out2 : nullptr, h, dt,
+                                                     per_block);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
 }
