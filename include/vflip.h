@@ -206,7 +206,9 @@ int vflip_project_subdomain(vflip_ctx* ctx, int ni, int nj, int nk, float h, flo
  * SubDomainSolver::advect_field (SS/sub_domain.cpp:191-235).  field/out are
  * fnx x fny x fnz grids of spacing h whose node (i,j,k) sits at world
  * ((i-ox)h, (j-oy)h, (k-oz)h): (0.5,0,0) for u, (0,0.5,0) for v, (0,0,0.5)
- * for w, (0,0,0) for cell-centred scalars.  out must not alias field or u/v/w. */
+ * for w, (0,0,0) for cell-centred scalars.  out must not alias field or u/v/w.
+ * A VFLIP_PREC_FP64 context reproduces the reference's FP64 sampling bit for
+ * bit; FP32/MIXED contexts sample in FP32 (a few ulp from it). */
 int vflip_advect_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
                             const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
                             double oz, const float* field, float* out);

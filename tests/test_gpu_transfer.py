@@ -32,7 +32,7 @@ def test_advect_golden(gpu_solver):
     g = golden("advect")
     ni, nj, nk = (int(x) for x in g["dims"])
     for name, offs in OFFS.items():
-        out = gpu_solver[1].advect_rk2_linear(ni, nj, nk, float(g["h"]), float(g["dt"]), t(g["u"]), t(g["v"]),
+        out = gpu_solver[0].advect_rk2_linear(ni, nj, nk, float(g["h"]), float(g["dt"]), t(g["u"]), t(g["v"]),
                                               t(g["w"]), t(g["in_" + name]), offs)
         assert np.array_equal(out.cpu().numpy(), g["out_" + name]), name
 
@@ -47,8 +47,11 @@ def test_advect_vs_oracle(gpu_solver, orc, dims, dt):
         shape = {"u": (nk, nj, ni + 1), "v": (nk, nj + 1, ni), "w": (nk + 1, nj, ni), "c": (nk, nj, ni)}[name]
         f = rng.standard_normal(shape).astype(np.float32)
         want = orc.advect_rk2(ni, nj, nk, h, dt, u, v, w, f, offs)
-        got = gpu_solver[1].advect_rk2_linear(ni, nj, nk, h, dt, t(u), t(v), t(w), t(f), offs).cpu().numpy()
+        got = gpu_solver[0].advect_rk2_linear(ni, nj, nk, h, dt, t(u), t(v), t(w), t(f), offs).cpu().numpy()
         assert np.array_equal(got, want), name
+        # FP32 sampling: within a few ulp of the reference's FP64 sampling
+        got32 = gpu_solver[1].advect_rk2_linear(ni, nj, nk, h, dt, t(u), t(v), t(w), t(f), offs).cpu().numpy()
+        assert np.max(np.abs(got32 - want)) <= 2e-5 * max(1.0, np.abs(want).max()), name
 
 
 def test_transfer_golden(gpu_solver):
@@ -143,6 +146,6 @@ def test_advect_pair_matches_single(gpu_solver, orc):
     u, v, w = scenes.random_velocity(ni, nj, nk, rng, scale=2.0)
     f = rng.standard_normal((nk, nj, ni)).astype(np.float32)
     g = rng.standard_normal((nk, nj, ni)).astype(np.float32)
-    a, b = gpu_solver[1].advect_rk2_linear2(ni, nj, nk, h, 0.02, t(u), t(v), t(w), t(f), t(g), (0, 0, 0))
+    a, b = gpu_solver[0].advect_rk2_linear2(ni, nj, nk, h, 0.02, t(u), t(v), t(w), t(f), t(g), (0, 0, 0))
     assert np.array_equal(a.cpu().numpy(), orc.advect_rk2(ni, nj, nk, h, 0.02, u, v, w, f, (0, 0, 0)))
     assert np.array_equal(b.cpu().numpy(), orc.advect_rk2(ni, nj, nk, h, 0.02, u, v, w, g, (0, 0, 0)))

@@ -51,6 +51,29 @@ __device__ __forceinline__ float sample_linear(const GridView& g, double wx, dou
   return (float)lerp_d(v1, v2, cz);
 }
 
+// FP32 variant of sample_linear for the FP32/mixed precision modes: the
+// same corners and lerp structure with the world->grid transform and the
+// lerps in float (within a few ulp of the FP64 form, not bit-identical).
+__device__ __forceinline__ float lerp_f(float a, float b, float c) { return __fmaf_rn(c, b - a, a); }
+
+__device__ __forceinline__ float sample_linear_f(const GridView& g, float wx, float wy, float wz) {
+  const float ih = (float)(g.inv_h != 0.0 ? g.inv_h : 1.0 / g.h);
+  float gx = __fmaf_rn(wx, ih, (float)g.ox), gy = __fmaf_rn(wy, ih, (float)g.oy), gz = __fmaf_rn(wz, ih, (float)g.oz);
+  float fi = floorf(gx), fj = floorf(gy), fk = floorf(gz);
+  int i = (int)fi, j = (int)fj, k = (int)fk;
+  float cx = gx - fi, cy = gy - fj, cz = gz - fk;
+  const int i0 = clampi(i, g.nx - 1), i1 = clampi(i + 1, g.nx - 1);
+  const int sy = g.nx, sz = g.nx * g.ny;
+  const int j0 = clampi(j, g.ny - 1) * sy, j1 = clampi(j + 1, g.ny - 1) * sy;
+  const int k0 = clampi(k, g.nz - 1) * sz, k1 = clampi(k + 1, g.nz - 1) * sz;
+  const float* d = g.d;
+  float v1 = lerp_f(lerp_f(__ldg(d + (i0 + j0 + k0)), __ldg(d + (i1 + j0 + k0)), cx),
+                    lerp_f(__ldg(d + (i0 + j1 + k0)), __ldg(d + (i1 + j1 + k0)), cx), cy);
+  float v2 = lerp_f(lerp_f(__ldg(d + (i0 + j0 + k1)), __ldg(d + (i1 + j0 + k1)), cx),
+                    lerp_f(__ldg(d + (i0 + j1 + k1)), __ldg(d + (i1 + j1 + k1)), cx), cy);
+  return lerp_f(v1, v2, cz);
+}
+
 // SubDomainSolver::advect_field, sub_domain.cpp:191-235: RK2 midpoint
 // backtrace through the MAC velocity, then a trilinear sample of the field.
 // The field's node (i,j,k) sits at world ((i-ox)h, (j-oy)h, (k-oz)h).  A
@@ -71,6 +94,15 @@ __device__ __forceinline__ void node_world(const GridView& f, size_t e, float h,
 // Each block owns a contiguous run of `per_block` nodes (so the blocks in
 // flight cover a compact slab and the gathers of neighbouring blocks hit
 // L2), walked two nodes per thread at a time.
+template <bool EXACT>
+__device__ __forceinline__ float smp(const GridView& g, float x, float y, float z) {
+  return EXACT ? sample_linear(g, x, y, z) : sample_linear_f(g, x, y, z);
+}
+
+// EXACT: the reference's arithmetic (FP64 transform and lerps, FP64 midpoint
+// step), bit-identical to SubDomainSolver::advect_field; otherwise the same
+// scheme in FP32.
+template <bool EXACT>
 __global__ void advect_rk2_kernel(GridView u, GridView v, GridView w, GridView f, float* __restrict__ out,
                                   GridView f2, float* __restrict__ out2, float h, float dt, int per_block) {
   const size_t n = (size_t)f.nx * f.ny * f.nz;
@@ -84,25 +116,33 @@ __global__ void advect_rk2_kernel(GridView u, GridView v, GridView w, GridView f
     float wx0, wy0, wz0, wx1 = 0, wy1 = 0, wz1 = 0;
     node_world(f, e0, h, wx0, wy0, wz0);
     if (two) node_world(f, e1, h, wx1, wy1, wz1);
-    float a0 = sample_linear(u, wx0, wy0, wz0), b0 = sample_linear(v, wx0, wy0, wz0),
-          c0 = sample_linear(w, wx0, wy0, wz0);
+    float a0 = smp<EXACT>(u, wx0, wy0, wz0), b0 = smp<EXACT>(v, wx0, wy0, wz0), c0 = smp<EXACT>(w, wx0, wy0, wz0);
     float a1 = 0, b1 = 0, c1 = 0;
     if (two) {
-      a1 = sample_linear(u, wx1, wy1, wz1);
-      b1 = sample_linear(v, wx1, wy1, wz1);
-      c1 = sample_linear(w, wx1, wy1, wz1);
+      a1 = smp<EXACT>(u, wx1, wy1, wz1);
+      b1 = smp<EXACT>(v, wx1, wy1, wz1);
+      c1 = smp<EXACT>(w, wx1, wy1, wz1);
     }
-    float px0 = (float)((double)wx0 - hdt * (double)a0), py0 = (float)((double)wy0 - hdt * (double)b0),
-          pz0 = (float)((double)wz0 - hdt * (double)c0);
-    float px1 = (float)((double)wx1 - hdt * (double)a1), py1 = (float)((double)wy1 - hdt * (double)b1),
-          pz1 = (float)((double)wz1 - hdt * (double)c1);
-    a0 = sample_linear(u, px0, py0, pz0);
-    b0 = sample_linear(v, px0, py0, pz0);
-    c0 = sample_linear(w, px0, py0, pz0);
+    float px0, py0, pz0, px1, py1, pz1;
+    if (EXACT) {
+      px0 = (float)((double)wx0 - hdt * (double)a0);
+      py0 = (float)((double)wy0 - hdt * (double)b0);
+      pz0 = (float)((double)wz0 - hdt * (double)c0);
+      px1 = (float)((double)wx1 - hdt * (double)a1);
+      py1 = (float)((double)wy1 - hdt * (double)b1);
+      pz1 = (float)((double)wz1 - hdt * (double)c1);
+    } else {
+      const float hf = 0.5f * dt;
+      px0 = wx0 - hf * a0; py0 = wy0 - hf * b0; pz0 = wz0 - hf * c0;
+      px1 = wx1 - hf * a1; py1 = wy1 - hf * b1; pz1 = wz1 - hf * c1;
+    }
+    a0 = smp<EXACT>(u, px0, py0, pz0);
+    b0 = smp<EXACT>(v, px0, py0, pz0);
+    c0 = smp<EXACT>(w, px0, py0, pz0);
     if (two) {
-      a1 = sample_linear(u, px1, py1, pz1);
-      b1 = sample_linear(v, px1, py1, pz1);
-      c1 = sample_linear(w, px1, py1, pz1);
+      a1 = smp<EXACT>(u, px1, py1, pz1);
+      b1 = smp<EXACT>(v, px1, py1, pz1);
+      c1 = smp<EXACT>(w, px1, py1, pz1);
     }
     px0 = wx0 - dt * a0;
     py0 = wy0 - dt * b0;
@@ -110,11 +150,11 @@ __global__ void advect_rk2_kernel(GridView u, GridView v, GridView w, GridView f
     px1 = wx1 - dt * a1;
     py1 = wy1 - dt * b1;
     pz1 = wz1 - dt * c1;
-    out[e0] = sample_linear(f, px0, py0, pz0);
-    if (out2) out2[e0] = sample_linear(f2, px0, py0, pz0);
+    out[e0] = smp<EXACT>(f, px0, py0, pz0);
+    if (out2) out2[e0] = smp<EXACT>(f2, px0, py0, pz0);
     if (two) {
-      out[e1] = sample_linear(f, px1, py1, pz1);
-      if (out2) out2[e1] = sample_linear(f2, px1, py1, pz1);
+      out[e1] = smp<EXACT>(f, px1, py1, pz1);
+      if (out2) out2[e1] = smp<EXACT>(f2, px1, py1, pz1);
     }
   }
 }

@@ -1134,8 +1134,12 @@ int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, fl
   size_t n = (size_t)fnx * fny * fnz;
   const int per_block = 256 * 8;
   const unsigned blocks = (unsigned)((n + per_block - 1) / per_block);
-  advect_rk2_kernel<<<blocks, 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2, field2 ? out2 : nullptr, h, dt,
-                                                     per_block);
+  if (ctx->cfg.precision == VFLIP_PREC_FP64)
+    advect_rk2_kernel<true><<<blocks, 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2, field2 ? out2 : nullptr, h, dt,
+                                                           per_block);
+  else
+    advect_rk2_kernel<false><<<blocks, 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2, field2 ? out2 : nullptr, h,
+                                                            dt, per_block);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
 }
