@@ -203,6 +203,7 @@ def run_vflip(a):
     barrier()
     e2e_ms = max_over_ranks(e2.elapsed_time(e3))
 
+    diag = solve_diagnostics(sim, local) if rank == 0 else None
     out = None
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -218,7 +219,7 @@ def run_vflip(a):
             "config": config(a, world),
             "cells_steps_per_s": world * a.steps * a.n ** 3 / (ms_max * 1e-3),
             "solver": {"pcg_iterations_mean": float(np.mean(iters)), "vcycles_mean": float(np.mean(vcycles)),
-                       "rel_residual_max": float(np.max(resid)), "levels": sim.last.levels},
+                       "rel_residual_max": float(np.max(resid)), "levels": sim.last.levels, **diag},
             "roofline": {"bound": "hbm", "kernel": "rbgs_sweep_kernel<float,float> (fine level)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
@@ -235,6 +236,32 @@ def run_vflip(a):
     if world > 1:
         dist.destroy_process_group()
     return out
+
+
+def solve_diagnostics(sim, device):
+    """One more step, outside the timed region, whose projection is solved
+    twice: by the benchmarked solver and by an FP64 context (the GPU oracle
+    solve).  Reports the pressure error against the FP64 solve, both
+    residual ratios and max |div u| after projection."""
+    import torch
+
+    from vflip_b200.solver import Solver
+
+    sim.advect_and_force()
+    pre = {k: sim.f[k].clone() for k in ("u", "v", "w")}
+    n = sim.p.n
+    before = float(sim.divergence(pre["u"], pre["v"], pre["w"]).abs().max())
+    p32 = torch.zeros((n, n, n), dtype=torch.float64, device=sim.s.device)
+    ok, _, st = sim.project(pressure=p32)
+    with Solver(precision=0, device=device) as s64:
+        u64, v64, w64 = (pre[k].clone() for k in ("u", "v", "w"))
+        p64 = torch.zeros_like(p32)
+        ok64, _, st64 = sim.project(solver=s64, u=u64, v=v64, w=w64, pressure=p64)
+    err = float(torch.linalg.vector_norm(p32 - p64) / torch.linalg.vector_norm(p64))
+    after = float(sim.divergence(sim.f["u"], sim.f["v"], sim.f["w"]).abs().max())
+    return {"rel_residual_inf": st.residual / st.rhs_norm, "iterations_last": st.iterations,
+            "pressure_rel_l2_vs_fp64_gpu_solve": err, "fp64_iterations": st64.iterations,
+            "max_abs_div_before": before, "max_abs_div_after": after}
 
 
 def _cpu_impl():

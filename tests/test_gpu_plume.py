@@ -33,3 +33,19 @@ def test_plume_matches_oracle(gpu_solver, orc, prec, n, steps, obstacle, tol):
         assert rel(sim.f[k].cpu().numpy(), state[k]) < tol, k
     # the projected field is (discretely) divergence free where the solve acts
     assert float(np.abs(state["v"]).max()) > 0.05
+
+
+@pytest.mark.parametrize("prec", [0, 1, 2])
+def test_projection_removes_divergence(gpu_solver, prec):
+    """After the projection the weighted divergence is the solve's residual:
+    at a 1e-6 inf-norm tolerance it drops by orders of magnitude."""
+    p = PlumeParams(n=48, dt=0.02, obstacle=True)
+    sim = PlumeSim(gpu_solver[prec], p)
+    for _ in range(3):
+        sim.step()
+    sim.advect_and_force()
+    before = float(sim.divergence(sim.f["u"], sim.f["v"], sim.f["w"]).abs().max())
+    conv, _, st = sim.project()
+    after = float(sim.divergence(sim.f["u"], sim.f["v"], sim.f["w"]).abs().max())
+    assert conv and before > 0.1
+    assert after < 1e-3 * before, (before, after)

@@ -74,7 +74,8 @@ class PlumeSim:
     def state(self):
         return {k: self.f[k] for k in self.FIELDS}
 
-    def step(self):
+    def advect_and_force(self):
+        """Steps 1-2 of a plume step (advection, sources, buoyancy)."""
         p, s, n, h = self.p, self.s, self.p.n, self.p.h
         u, v, w = self.f["u"], self.f["v"], self.f["w"]
         offs = {"u": (0.5, 0, 0), "v": (0, 0.5, 0), "w": (0, 0, 0.5)}
@@ -86,11 +87,34 @@ class PlumeSim:
         self.f, self.g = self.g, self.f
         s.plume_sources(n, n, n, h, p.dt, self.f["rho"], self.f["temp"], self.f["v"], p.source_centre,
                         p.source_radius, 1.0, 1.0, p.alpha, p.beta)
-        conv, _, stats = s.project(n, n, n, h, 0.0, self.phi, self.bdesc, self.solid["u"], self.solid["v"],
-                                   self.solid["w"], self.f["u"], self.f["v"], self.f["w"], pressure=self.pressure,
-                                   tolerance_factor=p.tol, max_iterations=p.max_iterations)
+
+    def project(self, solver=None, u=None, v=None, w=None, pressure=None):
+        """Step 3: the pressure projection of (u, v, w) (the state by default)."""
+        p, n, h = self.p, self.p.n, self.p.h
+        s = solver or self.s
+        u = self.f["u"] if u is None else u
+        v = self.f["v"] if v is None else v
+        w = self.f["w"] if w is None else w
+        pressure = self.pressure if pressure is None else pressure
+        return s.project(n, n, n, h, 0.0, self.phi, self.bdesc, self.solid["u"], self.solid["v"], self.solid["w"], u,
+                         v, w, pressure=pressure, tolerance_factor=p.tol, max_iterations=p.max_iterations)
+
+    def step(self):
+        self.advect_and_force()
+        conv, _, stats = self.project()
         self.last = stats
         return conv, stats
+
+    def divergence(self, u, v, w):
+        """Weighted discrete divergence sum(w_f u_f n_f)/h per cell, the
+        quantity the projection drives to zero, on the cells two or more
+        away from the Dirichlet ring (the reference leaves the faces next to
+        the ring uncorrected, Smoke_solver3D.cpp:1135)."""
+        uw, vw, ww = self.s.face_weights(self.p.n, self.p.n, self.p.n, self.phi)
+        h = self.p.h
+        fu, fv, fw = uw * u, vw * v, ww * w
+        div = (fu[:, :, 1:] - fu[:, :, :-1] + fv[:, 1:, :] - fv[:, :-1, :] + fw[1:, :, :] - fw[:-1, :, :]) / h
+        return div[2:-2, 2:-2, 2:-2]
 
     def step_host(self, host):
         """One step on host-resident state (pinned tensors): H2D copy, step,
