@@ -279,6 +279,50 @@ int vflip_plume_sources(vflip_ctx* ctx, int ni, int nj, int nk, float h, float d
 int vflip_bricks_to_linear(vflip_ctx* ctx, int nx, int ny, int nz, const float* bricked, float* linear);
 int vflip_linear_to_bricks(vflip_ctx* ctx, int nx, int ny, int nz, const float* linear, float* bricked);
 
+/* ---- learned preconditioner: the 3D U-Net --------------------------------- */
+
+/* No reference counterpart (the reference solves with plain MGPCG only).  A
+ * 3D U-Net (4 levels, 16/32/64/128 channels, 3x3x3 convolutions with ReLU,
+ * 2x2x2 average pooling, nearest upsampling, concatenated skips) maps
+ * (scaled rhs, fluid fraction) on a coarse grid to two fields: a warm-start
+ * pressure and a coarse correction.  Convolutions are BF16 tensor-core
+ * (tcgen05) kernels with FP32 accumulation; parameters are FP32 masters,
+ * trained by Adam with the library's own backward kernels.  All array
+ * arguments are device pointers ordered on `stream` (NULL = the default
+ * stream).  Network grids have dimensions that are multiples of 8; per-voxel
+ * fields are channels-last [z][y][x][c]. */
+typedef struct vflip_unet vflip_unet;
+int vflip_unet_create(vflip_unet** net, int device, void* stream, unsigned long long seed);
+int vflip_unet_destroy(vflip_unet* net);
+const char* vflip_unet_last_error(const vflip_unet* net);
+/* number of FP32 parameters: per layer W[cout][cin][27] then b[cout] */
+int vflip_unet_num_params(void);
+int vflip_unet_get_params(vflip_unet* net, float* host_params);
+int vflip_unet_set_params(vflip_unet* net, const float* host_params); /* also resets Adam */
+/* in2, out2: [Z][Y][X][2] FP32 */
+int vflip_unet_forward(vflip_unet* net, int X, int Y, int Z, const float* in2, float* out2);
+/* loss = sum_v weight[v] (cw0 (o0 - t0)^2 + cw1 (o1 - t1)^2) / (X Y Z); grad_out: nparams FP32 (or NULL) */
+int vflip_unet_gradients(vflip_unet* net, int X, int Y, int Z, const float* in2, const float* target2,
+                         const float* weight, float cw0, float cw1, float* grad_out, double* loss);
+/* one Adam step (beta 0.9 / 0.999) on that loss */
+int vflip_unet_train_step(vflip_unet* net, int X, int Y, int Z, const float* in2, const float* target2,
+                          const float* weight, float cw0, float cw1, float lr, double* loss);
+/* Single 3x3x3 convolution (zero padding) of a BF16 channel view
+ * in[v*in_ctot + in_coff + c] with FP32 weights w[layer_cout][layer_cin][27]
+ * (tap = 9 dz + 3 dy + dx, offsets -1..1).  backward_data = 0: out = conv(in)
+ * + bias, ReLU if relu; backward_data = 1: the gradient with respect to the
+ * layer's input (layer_cout channels in, layer_cin out, taps mirrored, no
+ * bias).  mask (optional) zeroes outputs where mask <= 0.  Output as BF16
+ * (out) and/or FP32 (outf, first outf_valid channels). */
+int vflip_unet_conv3(vflip_unet* net, int X, int Y, int Z, const void* in, int in_ctot, int in_coff, const float* w,
+                     int layer_cin, int layer_cout, int backward_data, const float* bias, int relu, const void* mask,
+                     int mask_ctot, int mask_coff, void* out, int out_ctot, int out_coff, float* outf, int outf_stride,
+                     int outf_valid);
+/* dw[cout][cin][27] = sum_v dy[v][co] * x[v + tap][ci] (FP32, deterministic) */
+int vflip_unet_conv3_wgrad(vflip_unet* net, int X, int Y, int Z, const void* x, int x_ctot, int x_coff, int cin,
+                           const void* dy, int dy_ctot, int dy_coff, int cout, float* dw);
+long long vflip_unet_launch_count(const vflip_unet* net);
+
 #ifdef __cplusplus
 }
 #endif

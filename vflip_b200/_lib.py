@@ -66,6 +66,19 @@ SIGNATURES = {
     "vflip_plume_sources": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _F, _F, _F, _F, _F, _F, _F, _F]),
     "vflip_bricks_to_linear": (_I, [_P, _I, _I, _I, _P, _P]),
     "vflip_linear_to_bricks": (_I, [_P, _I, _I, _I, _P, _P]),
+    "vflip_unet_create": (_I, [C.POINTER(_P), _I, _P, C.c_ulonglong]),
+    "vflip_unet_destroy": (_I, [_P]),
+    "vflip_unet_last_error": (C.c_char_p, [_P]),
+    "vflip_unet_num_params": (_I, []),
+    "vflip_unet_get_params": (_I, [_P, _P]),
+    "vflip_unet_set_params": (_I, [_P, _P]),
+    "vflip_unet_forward": (_I, [_P, _I, _I, _I, _P, _P]),
+    "vflip_unet_gradients": (_I, [_P, _I, _I, _I, _P, _P, _P, _F, _F, _P, C.POINTER(_D)]),
+    "vflip_unet_train_step": (_I, [_P, _I, _I, _I, _P, _P, _P, _F, _F, _F, C.POINTER(_D)]),
+    "vflip_unet_conv3": (_I, [_P, _I, _I, _I, _P, _I, _I, _P, _I, _I, _I, _P, _I, _P, _I, _I, _P, _I, _I, _P, _I,
+                              _I]),
+    "vflip_unet_conv3_wgrad": (_I, [_P, _I, _I, _I, _P, _I, _I, _I, _P, _I, _I, _I, _P]),
+    "vflip_unet_launch_count": (C.c_longlong, [_P]),
 }
 
 _lib = None

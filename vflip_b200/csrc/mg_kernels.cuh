@@ -12,6 +12,7 @@
 //     prolongation adds the parent's value (injection).
 #pragma once
 #include "common.cuh"
+#include "sm100.cuh"
 
 namespace vflip {
 
@@ -304,35 +305,6 @@ __host__ __device__ inline TmaLayout tma_layout(int ni, int tyo, int depth, int 
   return L;
 }
 
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait: false when the phase did not complete within the limit
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, unsigned parity) {
-  for (int n = 0; n < (1 << 22); ++n)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-__device__ __forceinline__ void tma_bulk_g2s(unsigned dst, const void* src, unsigned bytes, unsigned bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
 template <typename S, bool ZERO_X, bool PROLONG, bool DOT, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs<S> a) {
@@ -368,7 +340,7 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs<S> a
   const unsigned bar_base = smem_u32(&bars[0]);
   if (tid == 0) {
     for (int q = 0; q < NB; ++q) mbar_init(bar_base + 8u * q, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    mbar_init_fence();
   }
   __syncthreads();
 

@@ -1,0 +1,115 @@
+"""The learned preconditioner's 3D U-Net over the C ABI (vflip_unet_*).
+
+``UNet`` owns one network (FP32 master parameters, Adam state, BF16 packed
+weights, activation buffers) on a device and runs on torch's current stream.
+Inputs and outputs are torch CUDA tensors, channels last:
+``in2``/``out2``/``target2`` are [Z, Y, X, 2] float32 and ``weight`` is
+[Z, Y, X] float32.  The network has no reference counterpart; its CPU FP64
+definition is oracle/unet_oracle.py (test infrastructure).
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from ._lib import VflipError, load
+from .solver import _p
+
+
+class UNet:
+    def __init__(self, device=None, seed=0):
+        self.lib = load()
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        h = C.c_void_p()
+        rc = self.lib.vflip_unet_create(C.byref(h), self.device.index, C.c_void_p(stream or None), seed)
+        if rc < 0:
+            msg = self.lib.vflip_unet_last_error(h).decode() if h.value else "create failed"
+            if h.value:
+                self.lib.vflip_unet_destroy(h)
+            raise VflipError(rc, msg)
+        self.h = h
+        self.nparams = self.lib.vflip_unet_num_params()
+
+    def close(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.vflip_unet_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc < 0:
+            raise VflipError(rc, self.lib.vflip_unet_last_error(self.h).decode())
+        return rc
+
+    @property
+    def launch_count(self):
+        return self.lib.vflip_unet_launch_count(self.h)
+
+    # parameters
+    def get_params(self):
+        p = np.empty(self.nparams, np.float32)
+        self._check(self.lib.vflip_unet_get_params(self.h, p.ctypes.data))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.nparams
+        self._check(self.lib.vflip_unet_set_params(self.h, p.ctypes.data))
+
+    # network
+    def forward(self, in2, out2=None):
+        Z, Y, X = in2.shape[:3]
+        if out2 is None:
+            out2 = torch.empty((Z, Y, X, 2), dtype=torch.float32, device=in2.device)
+        self._check(self.lib.vflip_unet_forward(self.h, X, Y, Z, _p(in2), _p(out2)))
+        return out2
+
+    def gradients(self, in2, target2, weight, cw0=1.0, cw1=1.0):
+        Z, Y, X = in2.shape[:3]
+        g = torch.empty(self.nparams, dtype=torch.float32, device=in2.device)
+        loss = C.c_double()
+        self._check(self.lib.vflip_unet_gradients(self.h, X, Y, Z, _p(in2), _p(target2), _p(weight), cw0, cw1,
+                                                  _p(g), C.byref(loss)))
+        return loss.value, g
+
+    def train_step(self, in2, target2, weight, lr, cw0=1.0, cw1=1.0, want_loss=True):
+        Z, Y, X = in2.shape[:3]
+        loss = C.c_double()
+        self._check(self.lib.vflip_unet_train_step(self.h, X, Y, Z, _p(in2), _p(target2), _p(weight), cw0, cw1,
+                                                   float(lr), C.byref(loss) if want_loss else None))
+        return loss.value if want_loss else None
+
+    # single operations (BF16 channels-last tensors [Z, Y, X, C])
+    def conv3(self, x, w, layer_cin, layer_cout, backward_data=False, bias=None, relu=False, mask=None,
+              in_coff=0, mask_coff=0, out=None, out_coff=0, outf=None, outf_valid=None):
+        Z, Y, X, ctot = x.shape
+        cout = layer_cin if backward_data else layer_cout
+        if out is None and outf is None:
+            outf = torch.empty((Z, Y, X, cout), dtype=torch.float32, device=x.device)
+        self._check(self.lib.vflip_unet_conv3(
+            self.h, X, Y, Z, _p(x), ctot, in_coff, _p(w), layer_cin, layer_cout, int(backward_data), _p(bias),
+            int(relu), _p(mask), mask.shape[3] if mask is not None else 0, mask_coff, _p(out),
+            out.shape[3] if out is not None else 0, out_coff, _p(outf), outf.shape[3] if outf is not None else 0,
+            (outf.shape[3] if outf_valid is None else outf_valid) if outf is not None else 0))
+        return outf if outf is not None else out
+
+    def conv3_wgrad(self, x, dy, cin=None, cout=None, x_coff=0, dy_coff=0):
+        Z, Y, X = x.shape[:3]
+        cin = x.shape[3] - x_coff if cin is None else cin
+        cout = dy.shape[3] - dy_coff if cout is None else cout
+        dw = torch.empty((cout, cin, 27), dtype=torch.float32, device=x.device)
+        self._check(self.lib.vflip_unet_conv3_wgrad(self.h, X, Y, Z, _p(x), x.shape[3], x_coff, cin, _p(dy),
+                                                    dy.shape[3], dy_coff, cout, _p(dw)))
+        return dw
