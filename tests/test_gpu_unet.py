@@ -66,7 +66,8 @@ def test_conv_forward(net, dims, cin, cout, ctot, coff):
     net.conv3(x, wt, cin, cout, bias=bt, relu=True, mask=m, in_coff=coff, out=out, out_coff=16)
     o = out.float().cpu().numpy()
     ref = np.maximum(want, 0) * (mn > 0)
-    assert np.all(np.abs(o[..., 16:] - ref) <= 2.0 ** -8 * np.abs(ref) + 1e-30)
+    # one BF16 rounding, plus FP32-vs-FP64 slack where the ReLU cuts near zero
+    assert np.all(np.abs(o[..., 16:] - ref) <= 2.0 ** -8 * np.abs(ref) + 1e-5 * np.abs(want).max())
     assert np.all(o[..., :16] == 0)
 
 
@@ -130,11 +131,7 @@ def test_network_gradients_match_oracle(net):
     off = 0
     for name, ci, co, _ in uo.LAYERS:
         n = co * ci * 27 + co
-        if name == "OUT":  # only the first 2 output rows carry weights
-            gl, wl = g[off:off + n], gw[off:off + n]
-        else:
-            gl, wl = g[off:off + n], gw[off:off + n]
-        assert rel(gl, wl) < 5e-2, name
+        assert rel(g[off:off + n], gw[off:off + n]) < 5e-2, name
         off += n
     cos = float(g @ gw / (np.linalg.norm(g) * np.linalg.norm(gw)))
     assert cos > 0.999

@@ -25,7 +25,7 @@ const LayerSpec kSpec[kNumLayers] = {
 namespace {
 
 constexpr size_t kConvSmemMax = 200 * 1024;
-constexpr size_t kConvSmemFloor = 160 * 1024;   // one CTA per SM
+constexpr size_t kConvSmemFloor = 100 * 1024;   // at most two CTAs (2 x <= 256 TMEM columns) per SM
 constexpr size_t kWgradSmemMax = 200 * 1024;
 constexpr size_t kWgradSmemFloor = 116 * 1024;  // one CTA (512 TMEM columns) per SM
 
