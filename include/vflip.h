@@ -323,6 +323,47 @@ int vflip_unet_conv3_wgrad(vflip_unet* net, int X, int Y, int Z, const void* x, 
                            const void* dy, int dy_ctot, int dy_coff, int cout, float* dw);
 long long vflip_unet_launch_count(const vflip_unet* net);
 
+/* ---- learned-preconditioned projection -------------------------------------- */
+
+/* mode bits of vflip_project_learned */
+#define VFLIP_LEARNED_CAPTURE 1 /* plain MGPCG; also write this solve's training triple */
+#define VFLIP_LEARNED_SOLVE 2   /* network warm start + coarse correction, flexible PCG */
+#define VFLIP_LEARNED_NO_VB 4   /* leave V(b) out of the initial Ritz subspace */
+
+typedef struct vflip_learned_stats {
+  int fallback;          /* 1: the learned iteration stalled; plain MGPCG solved from zero */
+  int subspace;          /* vectors kept by the initial Ritz step (0-3) */
+  double gamma[3];       /* Ritz coefficients of V(b), warm start, coarse correction */
+  double init_residual;  /* |b - A x0|_inf after the Ritz step */
+  double net_ms;         /* network forward time */
+} vflip_learned_stats;
+
+/* Network grid for a fine grid and multigrid level: ceil(n / 2^level)
+ * rounded up to a multiple of 8, per axis. */
+int vflip_learned_grid(int ni, int nj, int nk, int level, int* X, int* Y, int* Z);
+
+/* vflip_project with the learned preconditioner.  No reference counterpart:
+ * an addition beside SmokeSolver3D::pcg_projection's solve, which stays the
+ * plain path and the fallback.
+ *   VFLIP_LEARNED_CAPTURE: plain MGPCG (same answer as vflip_project); the
+ *     network grid (vflip_learned_grid at `level`) receives the features
+ *     in2 = (s R^L rhs, R^L fluid) with s = 1 / |R^L rhs|_inf, the targets
+ *     target2 = (s R^L p, s R^L (p - x1)) where p is the converged pressure
+ *     and x1 plain PCG's first iterate, and weight = R^L fluid.
+ *   VFLIP_LEARNED_SOLVE: the network maps the features to a warm-start
+ *     pressure and a coarse correction (trilinear prolongation to the fine
+ *     grid); the initial iterate minimises the energy error over
+ *     span{V(b), warm start, coarse correction} (Ritz step), then flexible
+ *     (Polak-Ribiere) PCG with the V-cycle runs to the same tolerance.  When
+ *     the residual stalls (less than 2x reduction over two iterations, or
+ *     NaN) plain MGPCG restarts from zero.  stats->vcycles counts every
+ *     V-cycle, the Ritz step's and a fallback's included. */
+int vflip_project_learned(vflip_ctx* ctx, vflip_unet* net, int mode, int level, int ni, int nj, int nk, float h,
+                          float U_in, const float* nodal_phi, const int8_t* bdesc, const float* us, const float* vs,
+                          const float* ws, float* u, float* v, float* w, double* pressure, double tolerance_factor,
+                          int max_iterations, float* sample_in2, float* sample_target2, float* sample_weight,
+                          vflip_solve_stats* stats, vflip_learned_stats* lstats);
+
 #ifdef __cplusplus
 }
 #endif

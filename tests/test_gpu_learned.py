@@ -1,0 +1,100 @@
+"""GPU: the learned-preconditioned projection.  Capture mode is the plain
+solve (identical results); the learned solve converges to the same
+tolerance whatever the network outputs (random, or non-finite), and the
+answer agrees with the plain solve's."""
+import numpy as np
+import pytest
+
+from vflip_b200.learned import CAPTURE, NO_VB, SOLVE, LearnedPreconditioner, UNet
+from vflip_b200.plume import PlumeParams, PlumeSim
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def _state(prec, n=40, steps=4):
+    from vflip_b200.solver import Solver
+
+    s = Solver(precision=prec)
+    sim = PlumeSim(s, PlumeParams(n=n, dt=0.02))
+    for _ in range(steps):
+        sim.step()
+    sim.advect_and_force()
+    return s, sim
+
+
+def _rel(a, b):
+    return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_capture_is_the_plain_solve(prec):
+    s, sim = _state(prec)
+    u0 = {k: sim.f[k].clone() for k in ("u", "v", "w")}
+    conv, p_plain, st, = sim.project()[:3]
+    p_plain = p_plain.clone()
+    u_plain = {k: sim.f[k].clone() for k in ("u", "v", "w")}
+    for k in u0:
+        sim.f[k].copy_(u0[k])
+    n = sim.p.n
+    X, Y, Z = s.learned_grid(n, n, n, 1)
+    assert (X, Y, Z) == (24, 24, 24)
+    smp = (torch.empty((Z, Y, X, 2), device="cuda"), torch.empty((Z, Y, X, 2), device="cuda"),
+           torch.empty((Z, Y, X), device="cuda"))
+    conv2, p2, st2, _ = sim.project_learned(None, CAPTURE, 1, sample=smp)
+    assert conv and conv2 and st2.iterations == st.iterations
+    assert torch.equal(p2, p_plain)
+    for k in u0:
+        assert torch.equal(sim.f[k], u_plain[k])
+    in2, t2, w = (x.cpu().numpy() for x in smp)
+    assert np.array_equal(in2[..., 1], w) and w.min() >= 0 and w.max() <= 1
+    assert np.abs(in2[..., 0]).max() == pytest.approx(1.0)
+    # targets are R p and R (p - x1) scaled like the features: channel 0
+    # equals the block average of the pressure times the feature scale
+    p = p_plain.cpu().numpy()
+    pad = np.zeros((Z * 2, Y * 2, X * 2))
+    pad[:n, :n, :n] = p
+    avg = pad.reshape(Z, 2, Y, 2, X, 2).mean(axis=(1, 3, 5))
+    m = np.abs(avg) > 1e-3 * np.abs(avg).max()
+    ratio = t2[..., 0][m] / avg[m]
+    assert np.allclose(ratio, ratio.mean(), rtol=1e-4)
+    assert np.isfinite(t2).all()
+
+
+@pytest.mark.parametrize("prec,mode", [(0, SOLVE), (1, SOLVE), (1, SOLVE | NO_VB), (2, SOLVE)])
+def test_learned_solve_converges_to_plain_answer(prec, mode):
+    s, sim = _state(prec)
+    u0 = {k: sim.f[k].clone() for k in ("u", "v", "w")}
+    _, p_plain, st = sim.project()
+    p_plain = p_plain.clone()
+    for k in u0:
+        sim.f[k].copy_(u0[k])
+    with UNet(seed=7) as net:
+        conv, p, st2, ls = sim.project_learned(net, mode, 1)
+    assert conv and st2.converged
+    assert st2.residual <= 1e-6 * st2.rhs_norm
+    assert _rel(p, p_plain) < (1e-5 if prec == 0 else 2e-3)
+    assert ls.net_ms > 0
+
+
+def test_learned_solve_survives_non_finite_network():
+    s, sim = _state(1)
+    with UNet(seed=7) as net:
+        p = net.get_params()
+        p[:] = np.nan
+        net.set_params(p)
+        conv, _, st, ls = sim.project_learned(net, SOLVE, 1)
+    assert conv and st.residual <= 1e-6 * st.rhs_norm
+    assert ls.subspace <= 1 and ls.gamma[1] == 0 and ls.gamma[2] == 0
+
+
+def test_learned_mode_arguments():
+    from vflip_b200._lib import VflipError
+
+    s, sim = _state(1, n=24, steps=1)
+    with pytest.raises(VflipError):
+        sim.project_learned(None, SOLVE, 1)
+    with pytest.raises(VflipError):
+        sim.project_learned(None, CAPTURE, 1)
+    with pytest.raises(VflipError):
+        sim.project_learned(None, CAPTURE | SOLVE, 1)

@@ -34,6 +34,11 @@ class ConfigC(C.Structure):
                 ("smoother_ctas_per_sm", C.c_int)]
 
 
+class LearnedStatsC(C.Structure):
+    _fields_ = [("fallback", C.c_int), ("subspace", C.c_int), ("gamma", C.c_double * 3),
+                ("init_residual", C.c_double), ("net_ms", C.c_double)]
+
+
 # name -> (restype, argtypes); mirrors include/vflip.h one for one
 SIGNATURES = {
     "vflip_config_default": (None, [C.POINTER(ConfigC)]),
@@ -79,6 +84,9 @@ SIGNATURES = {
                               _I]),
     "vflip_unet_conv3_wgrad": (_I, [_P, _I, _I, _I, _P, _I, _I, _I, _P, _I, _I, _I, _P]),
     "vflip_unet_launch_count": (C.c_longlong, [_P]),
+    "vflip_learned_grid": (_I, [_I, _I, _I, _I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
+    "vflip_project_learned": (_I, [_P, _P, _I, _I, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _I,
+                                   _P, _P, _P, C.POINTER(SolveStatsC), C.POINTER(LearnedStatsC)]),
 }
 
 _lib = None

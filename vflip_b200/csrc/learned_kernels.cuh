@@ -1,0 +1,228 @@
+// Kernels of the learned-preconditioned solve: the network's features on a
+// coarse grid (block averages of the rhs and of the fluid indicator, scaled
+// by 1/|rhs_c|_inf), the trilinear prolongation of its two outputs back to
+// the fine grid, the Ritz step over the initial subspace, and the flexible
+// (Polak-Ribiere) PCG update.  No reference counterpart.
+#pragma once
+#include "common.cuh"
+#include "pcg_kernels.cuh"
+
+namespace vflip {
+
+// Network grid of a fine grid at multigrid level L: ceil(n / 2^L) rounded up
+// to a multiple of 8 (the network pools three times).
+inline void learned_grid_dims(int ni, int nj, int nk, int L, int& X, int& Y, int& Z) {
+  auto f = [L](int n) {
+    const int c = (n + (1 << L) - 1) >> L;
+    return (c + 7) / 8 * 8;
+  };
+  X = f(ni);
+  Y = f(nj);
+  Z = f(nk);
+}
+
+// out[v] (network grid X x Y x Z) = (1/8^L) * sum over the fine cells of the
+// 2^L block of f(a, b); blocks beyond the fine grid are 0.  This is R^L of
+// the multigrid restriction (out-of-range children add nothing).
+//   kind 0: a;  kind 1: (a > 0) (fluid indicator of the diagonal);  kind 2: a - b
+template <typename TA, typename TB>
+__global__ void block_average_kernel(const TA* __restrict__ a, const TB* __restrict__ b, int kind, int ni, int nj,
+                                     int nk, int L, float* __restrict__ out, int X, int Y, int Z) {
+  const size_t nv = (size_t)X * Y * Z;
+  const int B = 1 << L;
+  const double inv = 1.0 / (double)((size_t)B * B * B);
+  for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += (size_t)gridDim.x * blockDim.x) {
+    const int I = (int)(v % X), J = (int)((v / X) % Y), K = (int)(v / ((size_t)X * Y));
+    double s = 0.0;
+    for (int k = K * B; k < min(nk, (K + 1) * B); ++k)
+      for (int j = J * B; j < min(nj, (J + 1) * B); ++j)
+        for (int i = I * B; i < min(ni, (I + 1) * B); ++i) {
+          const size_t e = lin3(i, j, k, ni, nj);
+          const double va = (double)a[e];
+          s += kind == 0 ? va : kind == 1 ? (va > 0.0 ? 1.0 : 0.0) : va - (double)b[e];
+        }
+    out[v] = (float)(s * inv);
+  }
+}
+
+// partial max |f| per block, folded by the last block into *scale = 1/max (0 if max == 0)
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) inv_absmax_kernel(const float* __restrict__ f, size_t n, double* partials,
+                                                           unsigned int* counter, double* scale) {
+  __shared__ double sm[BLOCK / 32];
+  __shared__ bool last;
+  double m = 0.0;
+  for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK)
+    m = fmax(m, fabs((double)f[i]));
+  m = block_absmax<BLOCK>(m, sm);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = m;
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double v = 0.0;
+  for (int q = threadIdx.x; q < (int)gridDim.x; q += BLOCK) v = fmax(v, ((volatile double*)partials)[q]);
+  v = block_absmax<BLOCK>(v, sm);
+  if (threadIdx.x == 0) {
+    *scale = v > 0.0 ? 1.0 / v : 0.0;
+    *counter = 0;
+  }
+}
+
+// out2[v] = (scale * c0[v], c1 ? scale1 * c1[v] : w[v]) packs two channels
+__global__ void pack2_kernel(const float* __restrict__ c0, const float* __restrict__ c1, const double* __restrict__ scale,
+                             int scale_c1, float* __restrict__ out2, size_t n) {
+  const float s = (float)*scale;
+  for (size_t v = (size_t)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (size_t)gridDim.x * blockDim.x) {
+    out2[2 * v] = s * c0[v];
+    out2[2 * v + 1] = scale_c1 ? s * c1[v] : c1[v];
+  }
+}
+
+// w[fine] = trilinear interpolation of channel ch of the network output
+// (cell-centred coarse grid of level L) at the fine cell centre, divided by
+// the feature scale; 0 in cells outside the system (diag == 0)
+template <typename V>
+__global__ void prolong_trilinear_kernel(const float* __restrict__ out2, int ch, int X, int Y, int Z, int L,
+                                         const double* __restrict__ scale, const double* __restrict__ diag,
+                                         V* __restrict__ w, int ni, int nj, int nk) {
+  const size_t n = (size_t)ni * nj * nk;
+  const double s = *scale;
+  const double inv_s = s > 0.0 ? 1.0 / s : 0.0;
+  const float inv_b = 1.0f / (float)(1 << L);
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    if (!(diag[e] > 0.0)) {
+      w[e] = V(0);
+      continue;
+    }
+    const int i = (int)(e % ni), j = (int)((e / ni) % nj), k = (int)(e / ((size_t)ni * nj));
+    const float cx = fminf(fmaxf((i + 0.5f) * inv_b - 0.5f, 0.0f), (float)(X - 1));
+    const float cy = fminf(fmaxf((j + 0.5f) * inv_b - 0.5f, 0.0f), (float)(Y - 1));
+    const float cz = fminf(fmaxf((k + 0.5f) * inv_b - 0.5f, 0.0f), (float)(Z - 1));
+    const int x0 = min((int)cx, X - 1), y0 = min((int)cy, Y - 1), z0 = min((int)cz, Z - 1);
+    const int x1 = min(x0 + 1, X - 1), y1 = min(y0 + 1, Y - 1), z1 = min(z0 + 1, Z - 1);
+    const float fx = cx - x0, fy = cy - y0, fz = cz - z0;
+    auto at = [&](int x, int y, int z) { return out2[2 * (((size_t)z * Y + y) * X + x) + ch]; };
+    const float c00 = at(x0, y0, z0) + fx * (at(x1, y0, z0) - at(x0, y0, z0));
+    const float c10 = at(x0, y1, z0) + fx * (at(x1, y1, z0) - at(x0, y1, z0));
+    const float c01 = at(x0, y0, z1) + fx * (at(x1, y0, z1) - at(x0, y0, z1));
+    const float c11 = at(x0, y1, z1) + fx * (at(x1, y1, z1) - at(x0, y1, z1));
+    const float c0 = c00 + fy * (c10 - c00), c1 = c01 + fy * (c11 - c01);
+    w[e] = cvt<V>((typename Num<V>::Acc)((double)(c0 + fz * (c1 - c0)) * inv_s));
+  }
+}
+
+// y = A x for the 7-point operator stored as (diag, +x, +y, +z)
+template <typename S, typename V>
+__global__ void spmv_kernel(const V* __restrict__ x, V* __restrict__ y, const S* __restrict__ diag,
+                            const S* __restrict__ xp, const S* __restrict__ yp, const S* __restrict__ zp, int ni,
+                            int nj, int nk) {
+  using A = typename Num<V>::Acc;
+  const size_t n = (size_t)ni * nj * nk, sy = (size_t)ni, sz = (size_t)ni * nj;
+  for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(g % ni), j = (int)((g / ni) % nj), k = (int)(g / sz);
+    A acc = A(0);
+    if (k > 0) acc = acc + (A)ldg(zp + g - sz) * ldg(x + g - sz);
+    if (j > 0) acc = acc + (A)ldg(yp + g - sy) * ldg(x + g - sy);
+    if (i > 0) acc = acc + (A)ldg(xp + g - 1) * ldg(x + g - 1);
+    acc = acc + (A)ldg(diag + g) * ldg(x + g);
+    if (i < ni - 1) acc = acc + (A)ldg(xp + g) * ldg(x + g + 1);
+    if (j < nj - 1) acc = acc + (A)ldg(yp + g) * ldg(x + g + sy);
+    if (k < nk - 1) acc = acc + (A)ldg(zp + g) * ldg(x + g + sz);
+    y[g] = cvt<V>(acc);
+  }
+}
+
+// The nine inner products of the Ritz step over W = [w0 w1 w2], Q = A W:
+// w0.q0 w0.q1 w0.q2 w1.q1 w1.q2 w2.q2 w0.b w1.b w2.b; FP64 block partials
+// written as partials[k * gridDim.x + block]
+template <typename V, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) ritz_dots_kernel(const V* __restrict__ w0, const V* __restrict__ w1,
+                                                          const V* __restrict__ w2, const V* __restrict__ q0,
+                                                          const V* __restrict__ q1, const V* __restrict__ q2,
+                                                          const V* __restrict__ b, size_t n, double* partials) {
+  __shared__ double sm[BLOCK / 32];
+  double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK) {
+    const double a0 = (double)ldg(w0 + i), a1 = (double)ldg(w1 + i), a2 = (double)ldg(w2 + i);
+    const double c0 = (double)ldg(q0 + i), c1 = (double)ldg(q1 + i), c2 = (double)ldg(q2 + i);
+    const double bb = (double)ldg(b + i);
+    s[0] += a0 * c0;
+    s[1] += a0 * c1;
+    s[2] += a0 * c2;
+    s[3] += a1 * c1;
+    s[4] += a1 * c2;
+    s[5] += a2 * c2;
+    s[6] += a0 * bb;
+    s[7] += a1 * bb;
+    s[8] += a2 * bb;
+  }
+  for (int k = 0; k < 9; ++k) {
+    const double t = block_sum<BLOCK>(s[k], sm);
+    if (threadIdx.x == 0) partials[(size_t)k * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+// folds the nine partial rows in block order into out[9] (one block)
+template <int BLOCK>
+__global__ void ritz_fold_kernel(const double* __restrict__ partials, int nb, double* __restrict__ out) {
+  __shared__ double sm[BLOCK / 32];
+  for (int k = 0; k < 9; ++k) {
+    double v = 0.0;
+    for (int q = threadIdx.x; q < nb; q += BLOCK) v += partials[(size_t)k * nb + q];
+    v = block_sum<BLOCK>(v, sm);
+    if (threadIdx.x == 0) out[k] = v;
+  }
+}
+
+// x = sum g_i w_i, r = b - sum g_i q_i, partial |r|_inf (converged flag set
+// against the tolerance by the last block)
+template <typename V, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) ritz_combine_kernel(const V* __restrict__ w0, const V* __restrict__ w1,
+                                                             const V* __restrict__ w2, const V* __restrict__ q0,
+                                                             const V* __restrict__ q1, const V* __restrict__ q2,
+                                                             const V* __restrict__ b, double g0, double g1, double g2,
+                                                             V* __restrict__ x, V* __restrict__ r, size_t n,
+                                                             double* partials, PcgScalars* st) {
+  __shared__ double sm[BLOCK / 32];
+  double m = 0.0;
+  for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK) {
+    const double xv = g0 * (double)ldg(w0 + i) + g1 * (double)ldg(w1 + i) + g2 * (double)ldg(w2 + i);
+    const double rv =
+        (double)ldg(b + i) - (g0 * (double)ldg(q0 + i) + g1 * (double)ldg(q1 + i) + g2 * (double)ldg(q2 + i));
+    x[i] = cvt<V>((typename Num<V>::Acc)xv);
+    const V rt = cvt<V>((typename Num<V>::Acc)rv);
+    r[i] = rt;
+    m = fmax(m, fabs((double)ldv(&rt)));
+  }
+  const double bm = block_absmax<BLOCK>(m, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = bm;
+  finish_reduction<BLOCK>(partials, gridDim.x, st, kReduceRes, 0.0, gridDim.x);
+}
+
+// x += alpha s; r_out = r_in - alpha q (r_in kept for the Polak-Ribiere beta)
+template <typename T, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) fcg_update_kernel(T* __restrict__ x, const T* __restrict__ r_in,
+                                                          T* __restrict__ r_out, const T* __restrict__ s,
+                                                          const T* __restrict__ q, size_t n, double* partials,
+                                                          PcgScalars* st) {
+  __shared__ double sm[BLOCK / 32];
+  const double alpha = st->alpha;
+  double m = 0.0;
+  for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK) {
+    const double xv = (double)ldv(x + i) + alpha * (double)ldg(s + i);
+    const double rv = (double)ldg(r_in + i) - alpha * (double)ldg(q + i);
+    const T rt = cvt<T>((typename Num<T>::Acc)rv);
+    x[i] = cvt<T>((typename Num<T>::Acc)xv);
+    r_out[i] = rt;
+    m = fmax(m, fabs((double)ldv(&rt)));
+  }
+  const double bm = block_absmax<BLOCK>(m, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = bm;
+  finish_reduction<BLOCK>(partials, gridDim.x, st, kReduceRes, 0.0, gridDim.x);
+}
+
+}  // namespace vflip

@@ -13,6 +13,7 @@ namespace vflip {
 struct PcgScalars {
   double rho;        // z.r of the current iterate
   double rho_new;
+  double rho_prev;   // z.r of the previous iterate (flexible PCG)
   double sz;         // s.(A s)
   double alpha;
   double beta;
@@ -21,10 +22,10 @@ struct PcgScalars {
   int converged;     // res <= tol
   int bad_rho;       // rho == 0 or NaN
   int kernel_error;  // host copy of the smoother's timeout flag
-  unsigned int done_blocks[4];  // last-block-done counters, one per reduction kind
+  unsigned int done_blocks[5];  // last-block-done counters, one per reduction kind
 };
 
-enum ReduceKind { kReduceSZ = 0, kReduceRes = 1, kReduceRho = 2, kReduceRes0 = 3 };
+enum ReduceKind { kReduceSZ = 0, kReduceRes = 1, kReduceRho = 2, kReduceRes0 = 3, kReduceFlex = 4 };
 
 // Called by every thread of every block after thread 0 wrote the block's
 // partial: the last block to arrive folds all partials in index order and
@@ -62,9 +63,12 @@ __device__ __forceinline__ void finish_reduction(double* partials, int nblocks, 
       st->res = tot;
       st->tol = tol_factor * tot;
       st->converged = (tot == 0.0) ? 1 : 0;
+    } else if (kind == kReduceFlex) {  // z_new . r_old: Polak-Ribiere beta of flexible PCG
+      st->beta = (st->rho - tot) / st->rho_prev;
     } else {  // kReduceRho
       st->rho_new = tot;
       st->beta = tot / st->rho;  // unused after the first V-cycle (s = z there)
+      st->rho_prev = st->rho;
       st->rho = tot;
       st->bad_rho = (tot == 0.0 || tot != tot) ? 1 : 0;
     }

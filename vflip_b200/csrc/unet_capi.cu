@@ -553,10 +553,6 @@ int Net::adam(float lr, float b1, float b2, float eps) {
 using vflip::unet::Net;
 using vflip::unet::View;
 
-struct vflip_unet {
-  Net* net;
-};
-
 extern "C" {
 
 int vflip_unet_create(vflip_unet** out, int device, void* stream, unsigned long long seed) {

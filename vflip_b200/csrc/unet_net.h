@@ -84,3 +84,8 @@ class Net {
 
 }  // namespace unet
 }  // namespace vflip
+
+// the C ABI handle (include/vflip.h)
+struct vflip_unet {
+  vflip::unet::Net* net;
+};

@@ -25,6 +25,8 @@
 #include "plume_kernels.cuh"
 #include "projection_kernels.cuh"
 #include "transfer_kernels.cuh"
+#include "learned_kernels.cuh"
+#include "unet_net.h"
 
 using namespace vflip;
 
@@ -624,7 +626,7 @@ int read_scalars(vflip_ctx* ctx) {
 
 template <typename S0, typename SC, typename V>
 int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor, int maxit,
-              vflip_solve_stats* stats) {
+              vflip_solve_stats* stats, V* x1_out = nullptr) {
   const Dims d = T.fine.d;
   const size_t n = d.n();
   V *x, *r, *z, *s0, *s1, *q;
@@ -690,6 +692,7 @@ int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* re
     VF_LAUNCH_CHECK();
     pcg_update_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(x, r, s_new, q, n, ctx->partials, ctx->st);
     VF_LAUNCH_CHECK();
+    if (it == 0 && x1_out) VF_CUDA(cudaMemcpyAsync(x1_out, x, n * sizeof(V), cudaMemcpyDeviceToDevice, ctx->stream));
     if ((rc = read_scalars(ctx))) return rc;
     residual = h.res;
     if (h.converged) {
@@ -704,6 +707,306 @@ int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* re
   return finish(VFLIP_NOT_CONVERGED);
 }
 
+// ---------------------------------------------------------------- learned
+// Options of a learned-preconditioned projection (vflip_project_learned).
+struct LearnedOpts {
+  vflip::unet::Net* net = nullptr;
+  int mode = 0;
+  int level = 1;
+  const double* diag = nullptr;  // fine FP64 diagonal: fluid cells are diag > 0
+  float* s_in2 = nullptr;        // capture outputs (network grid)
+  float* s_tgt2 = nullptr;
+  float* s_w = nullptr;
+  vflip_learned_stats* lstats = nullptr;
+};
+
+// in2 = (s R^L rhs, R^L fluid), s = 1/|R^L rhs|_inf (device scalar); mc keeps R^L fluid
+int learned_features(vflip_ctx* ctx, const LearnedOpts& lo, const Dims& d, const double* rhs, int X, int Y, int Z,
+                     float* in2, float** mc_out, double** scale_out) {
+  const size_t nv = (size_t)X * Y * Z;
+  float *bc, *mc;
+  double* scale;
+  unsigned int* counter;
+  VF_ALLOC(bc, float, "lrn_bc", nv);
+  VF_ALLOC(mc, float, "lrn_mc", nv);
+  VF_ALLOC(scale, double, "lrn_scale", 1);
+  VF_ALLOC(counter, unsigned int, "lrn_counter", 1);
+  const int g = grid_for(nv, 256, ctx->num_sms);
+  block_average_kernel<double, double><<<g, 256, 0, ctx->stream>>>(rhs, nullptr, 0, d.ni, d.nj, d.nk, lo.level, bc,
+                                                                    X, Y, Z);
+  VF_LAUNCH_CHECK();
+  block_average_kernel<double, double><<<g, 256, 0, ctx->stream>>>(lo.diag, nullptr, 1, d.ni, d.nj, d.nk, lo.level,
+                                                                    mc, X, Y, Z);
+  VF_LAUNCH_CHECK();
+  VF_CUDA(cudaMemsetAsync(counter, 0, sizeof(unsigned int), ctx->stream));
+  const int gr = std::min(grid_for(nv, kRedBlock, ctx->num_sms), kMaxPartials);
+  inv_absmax_kernel<kRedBlock><<<gr, kRedBlock, 0, ctx->stream>>>(bc, nv, ctx->partials, counter, scale);
+  VF_LAUNCH_CHECK();
+  pack2_kernel<<<g, 256, 0, ctx->stream>>>(bc, mc, scale, 0, in2, nv);
+  VF_LAUNCH_CHECK();
+  *mc_out = mc;
+  *scale_out = scale;
+  return VFLIP_OK;
+}
+
+// Training triple of a converged plain solve: features, targets
+// (s R^L p, s R^L (p - x1)) and weight R^L fluid, on the network grid.
+template <typename V>
+int learned_capture(vflip_ctx* ctx, const LearnedOpts& lo, const Dims& d, const double* rhs, const double* p,
+                    const V* x1) {
+  int X, Y, Z;
+  learned_grid_dims(d.ni, d.nj, d.nk, lo.level, X, Y, Z);
+  const size_t nv = (size_t)X * Y * Z;
+  float *mc, *pc, *dc;
+  double* scale;
+  int rc;
+  if ((rc = learned_features(ctx, lo, d, rhs, X, Y, Z, lo.s_in2, &mc, &scale))) return rc;
+  VF_ALLOC(pc, float, "lrn_pc", nv);
+  VF_ALLOC(dc, float, "lrn_dc", nv);
+  const int g = grid_for(nv, 256, ctx->num_sms);
+  block_average_kernel<double, double><<<g, 256, 0, ctx->stream>>>(p, nullptr, 0, d.ni, d.nj, d.nk, lo.level, pc, X,
+                                                                    Y, Z);
+  VF_LAUNCH_CHECK();
+  block_average_kernel<double, V><<<g, 256, 0, ctx->stream>>>(p, x1, 2, d.ni, d.nj, d.nk, lo.level, dc, X, Y, Z);
+  VF_LAUNCH_CHECK();
+  pack2_kernel<<<g, 256, 0, ctx->stream>>>(pc, dc, scale, 1, lo.s_tgt2, nv);
+  VF_LAUNCH_CHECK();
+  VF_CUDA(cudaMemcpyAsync(lo.s_w, mc, nv * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
+  return VFLIP_OK;
+}
+
+// Energy-minimising coefficients over the active subset of three vectors:
+// G gamma = g with G_ij = w_i.A w_j; vectors whose pivot collapses (linearly
+// dependent, zero, or non-finite) are dropped.  Returns the kept count.
+int ritz_solve(const double* dots, bool use0, double* gamma) {
+  const double G[3][3] = {{dots[0], dots[1], dots[2]}, {dots[1], dots[3], dots[4]}, {dots[2], dots[4], dots[5]}};
+  const double g[3] = {dots[6], dots[7], dots[8]};
+  bool on[3] = {use0, true, true};
+  for (int i = 0; i < 3; ++i) {
+    gamma[i] = 0.0;
+    if (!(G[i][i] > 0.0) || !std::isfinite(G[i][i]) || !std::isfinite(g[i])) on[i] = false;
+  }
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    int idx[3], m = 0;
+    for (int i = 0; i < 3; ++i)
+      if (on[i]) idx[m++] = i;
+    if (m == 0) return 0;
+    // Cholesky of the scaled subset
+    double L[3][3] = {}, sc[3];
+    for (int a = 0; a < m; ++a) sc[a] = 1.0 / std::sqrt(G[idx[a]][idx[a]]);
+    int bad = -1;
+    for (int a = 0; a < m && bad < 0; ++a) {
+      for (int b = 0; b <= a; ++b) {
+        double v = G[idx[a]][idx[b]] * sc[a] * sc[b];
+        for (int c = 0; c < b; ++c) v -= L[a][c] * L[b][c];
+        if (a == b) {
+          if (!(v > 1e-10)) {
+            bad = a;
+            break;
+          }
+          L[a][a] = std::sqrt(v);
+        } else {
+          L[a][b] = v / L[b][b];
+        }
+      }
+    }
+    if (bad >= 0) {
+      on[idx[bad]] = false;
+      continue;
+    }
+    double y[3], t[3];
+    for (int a = 0; a < m; ++a) {
+      double v = g[idx[a]] * sc[a];
+      for (int c = 0; c < a; ++c) v -= L[a][c] * y[c];
+      y[a] = v / L[a][a];
+    }
+    for (int a = m - 1; a >= 0; --a) {
+      double v = y[a];
+      for (int c = a + 1; c < m; ++c) v -= L[c][a] * t[c];
+      t[a] = v / L[a][a];
+    }
+    for (int a = 0; a < m; ++a) gamma[idx[a]] = t[a] * sc[a];
+    return m;
+  }
+  return 0;
+}
+
+template <typename S0, typename SC, typename V>
+int learned_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor,
+                  int maxit, vflip_solve_stats* stats, const LearnedOpts& lo) {
+  const Dims d = T.fine.d;
+  const size_t n = d.n();
+  int X, Y, Z;
+  learned_grid_dims(d.ni, d.nj, d.nk, lo.level, X, Y, Z);
+  const size_t nv = (size_t)X * Y * Z;
+  float *in2, *out2;
+  double* ritz;
+  V *x, *r, *r2, *bv, *z, *w0, *w1, *w2, *q0, *q1, *q2, *s0, *s1, *q;
+  VF_ALLOC(in2, float, "lrn_in2", 2 * nv);
+  VF_ALLOC(out2, float, "lrn_out2", 2 * nv);
+  VF_ALLOC(ritz, double, "lrn_ritz", 9);
+  VF_ALLOC(x, V, "pcg_x", n);
+  VF_ALLOC(r, V, "pcg_r", n);
+  VF_ALLOC(z, V, "pcg_z", n);
+  VF_ALLOC(s0, V, "pcg_s0", n);
+  VF_ALLOC(s1, V, "pcg_s1", n);
+  VF_ALLOC(q, V, "pcg_q", n);
+  VF_ALLOC(r2, V, "lrn_r2", n);
+  VF_ALLOC(bv, V, "lrn_b", n);
+  VF_ALLOC(w0, V, "lrn_w0", n);
+  VF_ALLOC(w1, V, "lrn_w1", n);
+  VF_ALLOC(w2, V, "lrn_w2", n);
+  VF_ALLOC(q0, V, "lrn_q0", n);
+  VF_ALLOC(q1, V, "lrn_q1", n);
+  VF_ALLOC(q2, V, "lrn_q2", n);
+  vflip_learned_stats ls{};
+  int rc;
+  VF_CUDA(cudaMemsetAsync(ctx->st, 0, sizeof(PcgScalars), ctx->stream));
+  const int gb = grid_for(n, kRedBlock, ctx->num_sms);
+  pcg_init_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(rhs, r, x, n, ctx->partials, ctx->st,
+                                                                    tol_factor);
+  VF_LAUNCH_CHECK();
+  if ((rc = read_scalars(ctx))) return rc;
+  PcgScalars& h = *ctx->st_host;
+  const double rhs_norm = h.res;
+  int iterations = 0, vcycles = 0;
+  double residual = h.res;
+  auto finish = [&](int code) -> int {
+    to_double_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(x, result, n);
+    ++ctx->launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return ctx->fail(VFLIP_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+    if (stats) {
+      stats->iterations = iterations;
+      stats->vcycles = vcycles;
+      stats->levels = (int)T.coarse.size() + 1;
+      stats->converged = code == VFLIP_OK ? 1 : 0;
+      stats->residual = residual;
+      stats->rhs_norm = rhs_norm;
+    }
+    if (lo.lstats) *lo.lstats = ls;
+    return code;
+  };
+  auto fallback = [&]() -> int {
+    vflip_solve_stats st2{};
+    const int code = pcg_solve(ctx, T, rhs, result, tol_factor, maxit, &st2);
+    if (code < 0) return code;
+    ls.fallback = 1;
+    if (stats) {
+      *stats = st2;
+      stats->iterations += iterations;
+      stats->vcycles += vcycles;
+    }
+    if (lo.lstats) *lo.lstats = ls;
+    return code;
+  };
+  if (h.res == 0.0) return finish(VFLIP_OK);
+  VF_CUDA(cudaMemcpyAsync(bv, r, n * sizeof(V), cudaMemcpyDeviceToDevice, ctx->stream));
+
+  // network: features -> (warm start, coarse correction) on its grid
+  float* mc;
+  double* scale;
+  if ((rc = learned_features(ctx, lo, d, rhs, X, Y, Z, in2, &mc, &scale))) return rc;
+  vflip::unet::Net& net = *lo.net;
+  const cudaStream_t saved = net.stream;
+  net.stream = ctx->stream;
+  cudaEvent_t na, nb;
+  VF_CUDA(cudaEventCreate(&na));
+  VF_CUDA(cudaEventCreate(&nb));
+  cudaEventRecord(na, ctx->stream);
+  rc = net.forward(X, Y, Z, in2, out2);
+  cudaEventRecord(nb, ctx->stream);
+  if (!rc) rc = net.sync_error();
+  net.stream = saved;
+  if (!rc) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, na, nb);
+    ls.net_ms = ms;
+  }
+  cudaEventDestroy(na);
+  cudaEventDestroy(nb);
+  if (rc) return ctx->fail(rc, "network: %s", net.err.c_str());
+
+  // initial subspace on the fine grid
+  const int g = grid_for(n, 256, ctx->num_sms);
+  prolong_trilinear_kernel<V><<<g, 256, 0, ctx->stream>>>(out2, 0, X, Y, Z, lo.level, scale, lo.diag, w1, d.ni, d.nj,
+                                                          d.nk);
+  VF_LAUNCH_CHECK();
+  prolong_trilinear_kernel<V><<<g, 256, 0, ctx->stream>>>(out2, 1, X, Y, Z, lo.level, scale, lo.diag, w2, d.ni, d.nj,
+                                                          d.nk);
+  VF_LAUNCH_CHECK();
+  const bool use_vb = !(lo.mode & VFLIP_LEARNED_NO_VB);
+  if (use_vb) {
+    if ((rc = vcycle<S0, SC, V>(ctx, T, bv, w0, false))) return rc;
+    ++vcycles;
+  } else {
+    VF_CUDA(cudaMemsetAsync(w0, 0, n * sizeof(V), ctx->stream));
+  }
+  const Level<S0, V>& F = T.fine;
+  spmv_kernel<S0, V><<<g, 256, 0, ctx->stream>>>(w0, q0, F.diag, F.xp, F.yp, F.zp, d.ni, d.nj, d.nk);
+  VF_LAUNCH_CHECK();
+  spmv_kernel<S0, V><<<g, 256, 0, ctx->stream>>>(w1, q1, F.diag, F.xp, F.yp, F.zp, d.ni, d.nj, d.nk);
+  VF_LAUNCH_CHECK();
+  spmv_kernel<S0, V><<<g, 256, 0, ctx->stream>>>(w2, q2, F.diag, F.xp, F.yp, F.zp, d.ni, d.nj, d.nk);
+  VF_LAUNCH_CHECK();
+  const int rb = std::min(gb, kMaxPartials / 9);
+  ritz_dots_kernel<V, kRedBlock><<<rb, kRedBlock, 0, ctx->stream>>>(w0, w1, w2, q0, q1, q2, bv, n, ctx->partials);
+  VF_LAUNCH_CHECK();
+  ritz_fold_kernel<kRedBlock><<<1, kRedBlock, 0, ctx->stream>>>(ctx->partials, rb, ritz);
+  VF_LAUNCH_CHECK();
+  double dots[9];
+  VF_CUDA(cudaMemcpyAsync(dots, ritz, sizeof dots, cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  ls.subspace = ritz_solve(dots, use_vb, ls.gamma);
+  ritz_combine_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(
+      w0, w1, w2, q0, q1, q2, bv, ls.gamma[0], ls.gamma[1], ls.gamma[2], x, r, n, ctx->partials, ctx->st);
+  VF_LAUNCH_CHECK();
+  if ((rc = read_scalars(ctx))) return rc;
+  residual = ls.init_residual = h.res;
+  iterations = 1;
+  if (h.converged) return finish(VFLIP_OK);
+  if (!std::isfinite(h.res)) return fallback();
+
+  // flexible PCG from x0 (Polak-Ribiere beta)
+  if ((rc = vcycle<S0, SC, V>(ctx, T, r, z, true))) return rc;
+  ++vcycles;
+  if ((rc = read_scalars(ctx))) return rc;
+  if (h.bad_rho) return fallback();
+  dim3 sblk(kRedBlock);
+  const int kz = 8;
+  dim3 sgrid((d.ni + 31) / 32, (d.nj + kRedBlock / 32 - 1) / (kRedBlock / 32), (d.nk + kz - 1) / kz);
+  if ((size_t)sgrid.x * sgrid.y * sgrid.z > (size_t)kMaxPartials) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
+  V* s_old = s0;
+  V* s_new = s1;
+  std::vector<double> hist{h.res};
+  for (int it = 0; it < maxit; ++it) {
+    if (it == 0)
+      pcg_spmv_dot_kernel<V, true, kRedBlock><<<sgrid, sblk, 0, ctx->stream>>>(
+          z, s_old, s_new, q, F.diag, F.xp, F.yp, F.zp, d.ni, d.nj, d.nk, kz, ctx->partials, ctx->st);
+    else
+      pcg_spmv_dot_kernel<V, false, kRedBlock><<<sgrid, sblk, 0, ctx->stream>>>(
+          z, s_old, s_new, q, F.diag, F.xp, F.yp, F.zp, d.ni, d.nj, d.nk, kz, ctx->partials, ctx->st);
+    VF_LAUNCH_CHECK();
+    fcg_update_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(x, r, r2, s_new, q, n, ctx->partials,
+                                                                        ctx->st);
+    VF_LAUNCH_CHECK();
+    if ((rc = read_scalars(ctx))) return rc;
+    residual = h.res;
+    ++iterations;
+    hist.push_back(h.res);
+    if (h.converged) return finish(VFLIP_OK);
+    const size_t k = hist.size() - 1;
+    if (!std::isfinite(h.res) || (k >= 2 && h.res > 0.5 * hist[k - 2])) return fallback();
+    std::swap(r, r2);  // r: new residual, r2: previous one
+    if ((rc = vcycle<S0, SC, V>(ctx, T, r, z, true))) return rc;
+    ++vcycles;
+    dot_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(z, r2, n, ctx->partials, ctx->st, kReduceFlex);
+    VF_LAUNCH_CHECK();
+    std::swap(s_old, s_new);
+  }
+  return fallback();
+}
+
 int check_dims(vflip_ctx* ctx, int ni, int nj, int nk) {
   if (!ctx) return VFLIP_ERR_ARG;
   if (ni <= 0 || nj <= 0 || nk <= 0) return ctx->fail(VFLIP_ERR_ARG, "grid dimensions must be positive");
@@ -712,9 +1015,24 @@ int check_dims(vflip_ctx* ctx, int ni, int nj, int nk) {
   return VFLIP_OK;
 }
 
+template <typename S0, typename SC, typename V>
+int solve_typed(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol, int maxit,
+                vflip_solve_stats* stats, const LearnedOpts* lo) {
+  if (lo && (lo->mode & VFLIP_LEARNED_SOLVE)) return learned_solve(ctx, T, rhs, result, tol, maxit, stats, *lo);
+  if (lo && (lo->mode & VFLIP_LEARNED_CAPTURE)) {
+    V* x1;
+    VF_ALLOC(x1, V, "lrn_x1", T.fine.d.n());
+    const int status = pcg_solve(ctx, T, rhs, result, tol, maxit, stats, x1);
+    if (status < 0) return status;
+    const int rc = learned_capture<V>(ctx, *lo, T.fine.d, rhs, result, x1);
+    return rc ? rc : status;
+  }
+  return pcg_solve(ctx, T, rhs, result, tol, maxit, stats);
+}
+
 int solve_stencil(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, const double* xp, const double* yp,
                   const double* zp, const double* rhs, double* result, double tol, int maxit,
-                  vflip_solve_stats* stats) {
+                  vflip_solve_stats* stats, const LearnedOpts* lo = nullptr) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (!diag || !xp || !yp || !zp || !rhs || !result) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
@@ -728,19 +1046,19 @@ int solve_stencil(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, co
     case VFLIP_PREC_FP64: {
       Typed<double, double, double> T;
       if ((rc = make_typed(ctx, H, diag, xp, yp, zp, T, "f64"))) return rc;
-      status = pcg_solve(ctx, T, rhs, result, tol, maxit, stats);
+      status = solve_typed(ctx, T, rhs, result, tol, maxit, stats, lo);
       break;
     }
     case VFLIP_PREC_FP32: {
       Typed<float, float, float> T;
       if ((rc = make_typed(ctx, H, diag, xp, yp, zp, T, "f32"))) return rc;
-      status = pcg_solve(ctx, T, rhs, result, tol, maxit, stats);
+      status = solve_typed(ctx, T, rhs, result, tol, maxit, stats, lo);
       break;
     }
     case VFLIP_PREC_MIXED: {
       Typed<float, __nv_bfloat16, float> T;
       if ((rc = make_typed(ctx, H, diag, xp, yp, zp, T, "mix"))) return rc;
-      status = pcg_solve(ctx, T, rhs, result, tol, maxit, stats);
+      status = solve_typed(ctx, T, rhs, result, tol, maxit, stats, lo);
       break;
     }
     default:
@@ -1040,7 +1358,7 @@ int assemble_impl(vflip_ctx* ctx, int variant, int ni, int nj, int nk, float h, 
 int project_impl(vflip_ctx* ctx, int variant, int ni, int nj, int nk, float h, float dt, float U_in,
                  const float* nodal_phi, const int8_t* bdesc, const float* us, const float* vs, const float* ws,
                  float* u, float* v, float* w, double* pressure, double tolerance_factor, int max_iterations,
-                 vflip_solve_stats* stats) {
+                 vflip_solve_stats* stats, LearnedOpts* lo = nullptr) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   size_t n = (size_t)ni * nj * nk;
@@ -1058,8 +1376,9 @@ int project_impl(vflip_ctx* ctx, int variant, int ni, int nj, int nk, float h, f
     return rc;
   }
   vflip_solve_stats s{};
+  if (lo) lo->diag = op;
   int status = solve_stencil(ctx, ni, nj, nk, op, op + n, op + 2 * n, op + 3 * n, rhs, p, tolerance_factor,
-                             max_iterations, &s);
+                             max_iterations, &s, lo);
   if (status < 0) {
     cudaEventDestroy(e0);
     return status;
@@ -1112,6 +1431,38 @@ int vflip_project(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, c
                   vflip_solve_stats* stats) {
   return project_impl(ctx, 0, ni, nj, nk, h, 1.0f, U_in, nodal_phi, bdesc, us, vs, ws, u, v, w, pressure,
                       tolerance_factor, max_iterations, stats);
+}
+
+int vflip_learned_grid(int ni, int nj, int nk, int level, int* X, int* Y, int* Z) {
+  if (ni <= 0 || nj <= 0 || nk <= 0 || level < 0 || level > 8 || !X || !Y || !Z) return VFLIP_ERR_ARG;
+  learned_grid_dims(ni, nj, nk, level, *X, *Y, *Z);
+  return VFLIP_OK;
+}
+
+int vflip_project_learned(vflip_ctx* ctx, vflip_unet* net, int mode, int level, int ni, int nj, int nk, float h,
+                          float U_in, const float* nodal_phi, const int8_t* bdesc, const float* us, const float* vs,
+                          const float* ws, float* u, float* v, float* w, double* pressure, double tolerance_factor,
+                          int max_iterations, float* sample_in2, float* sample_target2, float* sample_weight,
+                          vflip_solve_stats* stats, vflip_learned_stats* lstats) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  if (level < 0 || level > 8) return ctx->fail(VFLIP_ERR_ARG, "level %d out of range", level);
+  const bool solve = (mode & VFLIP_LEARNED_SOLVE) != 0, capture = (mode & VFLIP_LEARNED_CAPTURE) != 0;
+  if (solve == capture) return ctx->fail(VFLIP_ERR_ARG, "mode must select exactly one of CAPTURE and SOLVE");
+  if (solve && (!net || !net->net)) return ctx->fail(VFLIP_ERR_ARG, "learned solve needs a network");
+  if (capture && (!sample_in2 || !sample_target2 || !sample_weight))
+    return ctx->fail(VFLIP_ERR_ARG, "capture needs the three sample buffers");
+  if (solve && net->net->device != ctx->cfg.device)
+    return ctx->fail(VFLIP_ERR_ARG, "network and context are on different devices");
+  LearnedOpts lo;
+  lo.net = net ? net->net : nullptr;
+  lo.mode = mode;
+  lo.level = level;
+  lo.s_in2 = sample_in2;
+  lo.s_tgt2 = sample_target2;
+  lo.s_w = sample_weight;
+  lo.lstats = lstats;
+  return project_impl(ctx, 0, ni, nj, nk, h, 1.0f, U_in, nodal_phi, bdesc, us, vs, ws, u, v, w, pressure,
+                      tolerance_factor, max_iterations, stats, &lo);
 }
 
 int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,

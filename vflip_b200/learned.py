@@ -113,3 +113,77 @@ class UNet:
         self._check(self.lib.vflip_unet_conv3_wgrad(self.h, X, Y, Z, _p(x), x.shape[3], x_coff, cin, _p(dy),
                                                     dy.shape[3], dy_coff, cout, _p(dw)))
         return dw
+
+
+CAPTURE, SOLVE, NO_VB = 1, 2, 4
+
+
+class LearnedPreconditioner:
+    """The learned warm start + coarse correction for a plume's projection.
+
+    Phase 1 (``capturing``): projections run plain MGPCG and record one
+    (features, targets, weight) triple each on the network grid of multigrid
+    level ``level``.  ``train()`` fits the U-Net to the recorded triples with
+    Adam on the GPU.  Phase 2: projections use the network inside flexible
+    PCG (``vflip_project_learned``), which converges to the same tolerance and
+    falls back to plain MGPCG when the residual stalls.
+    """
+
+    def __init__(self, solver, level=1, seed=0, net=None, use_vb=True):
+        self.s = solver
+        self.level = level
+        self.net = net if net is not None else UNet(device=solver.device.index, seed=seed)
+        self.samples = []
+        self.capturing = True
+        self.use_vb = use_vb
+        self.cw = (1.0, 1.0)
+        self.last = None
+
+    def _grid(self, sim):
+        n = sim.p.n
+        return self.s.learned_grid(n, n, n, self.level)
+
+    def project(self, sim):
+        """Projection of sim's current state; returns (converged, SolveStats)."""
+        if self.capturing:
+            X, Y, Z = self._grid(sim)
+            dev = self.s.device
+            sample = (torch.empty((Z, Y, X, 2), dtype=torch.float32, device=dev),
+                      torch.empty((Z, Y, X, 2), dtype=torch.float32, device=dev),
+                      torch.empty((Z, Y, X), dtype=torch.float32, device=dev))
+            conv, _, st, ls = sim.project_learned(None, CAPTURE, self.level, sample=sample)
+            self.samples.append(sample)
+        else:
+            mode = SOLVE | (0 if self.use_vb else NO_VB)
+            conv, _, st, ls = sim.project_learned(self.net, mode, self.level)
+        self.last = ls
+        return conv, st
+
+    def train(self, epochs=8, lr=1e-3, seed=0, log=None):
+        """Adam over the recorded triples (one sample per step, shuffled per
+        epoch, cosine-decayed learning rate).  The two target channels are
+        weighted by the inverse of their weighted mean square over the set.
+        Returns the mean loss of each epoch."""
+        if not self.samples:
+            raise RuntimeError("no captured samples to train on")
+        m0 = m1 = wsum = 0.0
+        for _, t, w in self.samples:
+            m0 += float((w * t[..., 0] ** 2).sum())
+            m1 += float((w * t[..., 1] ** 2).sum())
+            wsum += float(w.sum())
+        self.cw = (wsum / max(m0, 1e-30), wsum / max(m1, 1e-30))
+        rng = np.random.default_rng(seed)
+        total = epochs * len(self.samples)
+        losses, step = [], 0
+        for ep in range(epochs):
+            acc = 0.0
+            for i in rng.permutation(len(self.samples)):
+                in2, t, w = self.samples[i]
+                lr_t = lr * 0.5 * (1.0 + np.cos(np.pi * step / total))
+                acc += self.net.train_step(in2, t, w, lr_t, self.cw[0], self.cw[1])
+                step += 1
+            losses.append(acc / len(self.samples))
+            if log:
+                log(ep, losses[-1])
+        self.capturing = False
+        return losses

@@ -99,9 +99,22 @@ class PlumeSim:
         return s.project(n, n, n, h, 0.0, self.phi, self.bdesc, self.solid["u"], self.solid["v"], self.solid["w"], u,
                          v, w, pressure=pressure, tolerance_factor=p.tol, max_iterations=p.max_iterations)
 
-    def step(self):
+    def project_learned(self, net, mode, level, sample=None):
+        """Step 3 through vflip_project_learned (capture or learned solve)."""
+        p, n, h = self.p, self.p.n, self.p.h
+        return self.s.project_learned(net, mode, level, n, n, n, h, 0.0, self.phi, self.bdesc, self.solid["u"],
+                                      self.solid["v"], self.solid["w"], self.f["u"], self.f["v"], self.f["w"],
+                                      pressure=self.pressure, tolerance_factor=p.tol,
+                                      max_iterations=p.max_iterations, sample=sample)
+
+    def step(self, precond=None):
+        """One plume step; `precond` (a learned.LearnedPreconditioner) takes
+        over the projection when given."""
         self.advect_and_force()
-        conv, _, stats = self.project()
+        if precond is None:
+            conv, _, stats = self.project()
+        else:
+            conv, stats = precond.project(self)
         self.last = stats
         return conv, stats
 
@@ -116,12 +129,12 @@ class PlumeSim:
         div = (fu[:, :, 1:] - fu[:, :, :-1] + fv[:, 1:, :] - fv[:, :-1, :] + fw[1:, :, :] - fw[:-1, :, :]) / h
         return div[2:-2, 2:-2, 2:-2]
 
-    def step_host(self, host):
+    def step_host(self, host, precond=None):
         """One step on host-resident state (pinned tensors): H2D copy, step,
         D2H copy back into the same host tensors."""
         for k in self.FIELDS:
             self.f[k].copy_(host[k], non_blocking=True)
-        out = self.step()
+        out = self.step(precond)
         for k in self.FIELDS:
             host[k].copy_(self.f[k], non_blocking=True)
         return out

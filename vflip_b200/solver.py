@@ -16,7 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from ._lib import ConfigC, SolveStatsC, VflipError, load
+from ._lib import ConfigC, LearnedStatsC, SolveStatsC, VflipError, load
 from .particles import PARTICLE_BYTES
 
 
@@ -33,6 +33,19 @@ class SolveStats:
     @classmethod
     def from_c(cls, s):
         return cls(s.iterations, s.vcycles, s.levels, bool(s.converged), s.residual, s.rhs_norm, s.solve_ms)
+
+
+@dataclass
+class LearnedStats:
+    fallback: bool
+    subspace: int
+    gamma: tuple
+    init_residual: float
+    net_ms: float
+
+    @classmethod
+    def from_c(cls, s):
+        return cls(bool(s.fallback), s.subspace, tuple(s.gamma), s.init_residual, s.net_ms)
 
 
 def _p(t):
@@ -204,6 +217,29 @@ class Solver:
                                    int(max_iterations), C.byref(st))
         self._check(rc)
         return rc == 0, pressure, SolveStats.from_c(st)
+
+    def learned_grid(self, ni, nj, nk, level):
+        X, Y, Z = C.c_int(), C.c_int(), C.c_int()
+        self._check(self.lib.vflip_learned_grid(ni, nj, nk, level, C.byref(X), C.byref(Y), C.byref(Z)))
+        return X.value, Y.value, Z.value
+
+    def project_learned(self, net, mode, level, ni, nj, nk, h, U_in, nodal_phi, bdesc, us, vs, ws, u, v, w,
+                        pressure=None, tolerance_factor=1e-6, max_iterations=50, sample=None):
+        """vflip_project_learned.  mode: VFLIP_LEARNED_CAPTURE (1) with
+        sample = (in2, target2, weight) tensors on the network grid, or
+        VFLIP_LEARNED_SOLVE (2, | 4 to leave V(b) out of the Ritz step) with
+        a ``learned.UNet``.  Returns (converged, pressure, SolveStats,
+        LearnedStats)."""
+        if pressure is None:
+            pressure = self._empty((nk, nj, ni), torch.float64)
+        st, ls = SolveStatsC(), LearnedStatsC()
+        si, stt, sw = sample if sample is not None else (None, None, None)
+        rc = self.lib.vflip_project_learned(self.ctx, net.h if net is not None else None, int(mode), int(level), ni, nj,
+                                            nk, float(h), float(U_in), _p(nodal_phi), _p(bdesc), _p(us), _p(vs),
+                                            _p(ws), _p(u), _p(v), _p(w), _p(pressure), float(tolerance_factor),
+                                            int(max_iterations), _p(si), _p(stt), _p(sw), C.byref(st), C.byref(ls))
+        self._check(rc)
+        return rc == 0, pressure, SolveStats.from_c(st), LearnedStats.from_c(ls)
 
     def project_subdomain(self, ni, nj, nk, h, dt, nodal_phi, us, vs, ws, u, v, w, pressure=None,
                           tolerance_factor=1e-9, max_iterations=1000):
