@@ -261,13 +261,24 @@ int Net::conv(const View& in, int X, int Y, int Z, const __nv_bfloat16* wpacked,
   if (mask && (!view_ok(*mask) || mask->c != cout)) return fail(VFLIP_ERR_ARG, "conv: bad mask view");
   if (!out && !outf) return fail(VFLIP_ERR_ARG, "conv: no output");
   if (outf && (ofvalid < 0 || ofvalid > cout || ofstride < ofvalid)) return fail(VFLIP_ERR_ARG, "conv: bad fp32 output");
+  // weights resident when every tap fits beside the two slabs; else the
+  // widest channel group whose slabs leave room for a ring of >= 8 slots
   const int nch = cin / 8;
-  int cc = 0;
-  for (int c = nch; c >= 2; --c)
-    if (nch % c == 0 && c % 2 == 0 && 2 * (size_t)c * kPlane + (size_t)kRing * c * cout * 16 <= kConvSmemMax) {
+  int cc = 0, ring = 0;
+  const size_t full = 2 * (size_t)nch * kPlane + (size_t)27 * nch * cout * 16;
+  if (full <= kConvSmemMax) {
+    cc = nch;
+    ring = 27;
+  } else {
+    for (int c = nch; c >= 2; --c) {
+      if (nch % c || c % 2) continue;
+      const size_t slabs = 2 * (size_t)c * kPlane, blk = (size_t)c * cout * 16;
+      if (slabs + 8 * blk > kConvSmemMax) continue;
       cc = c;
+      ring = (int)std::min<size_t>(kMaxRing, (kConvSmemMax - slabs) / blk);
       break;
     }
+  }
   if (!cc) return fail(VFLIP_ERR_ARG, "conv: no shared-memory split for %d -> %d", cin, cout);
   CUtensorMap amap;
   if (!make_map(&amap, in, X, Y, Z, kSX, kSY, 3)) return fail(VFLIP_ERR_CUDA, "conv: tensor map encode failed");
@@ -294,9 +305,11 @@ int Net::conv(const View& in, int X, int Y, int Z, const __nv_bfloat16* wpacked,
   a.ntx = (X + kTX - 1) / kTX;
   a.nty = (Y + kTY - 1) / kTY;
   a.ntiles = a.ntx * a.nty * Z;
+  a.ring = ring;
+  a.lag = ring >= 27 * a.ngroups ? 0 : std::min(4, ring / 4);
   a.tmem_cols = pow2_cols(cout);
   a.error = d_error;
-  const size_t smem = std::max(kConvSmemFloor, 2 * (size_t)cc * kPlane + (size_t)kRing * cc * cout * 16);
+  const size_t smem = std::max(kConvSmemFloor, 2 * (size_t)cc * kPlane + (size_t)ring * cc * cout * 16);
   const int grid = std::min(a.ntiles, 2 * num_sms);
   conv3_tc_kernel<<<grid, kConvThreads, smem, stream>>>(amap, a);
   NET_LAUNCH();

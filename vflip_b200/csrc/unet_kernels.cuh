@@ -17,7 +17,8 @@
 // a row (voxel) is 16 bytes, rows 8 apart in x are one core matrix and the
 // y rows are 160 bytes apart, so the A operand of every tap is the same slab
 // with a shifted start address - the 27 taps reuse one copy of the input.
-// Weights stream per tap through a 4-deep ring of bulk copies.  One thread
+// Weights stay resident in shared memory when all 27 taps fit; otherwise
+// they stream per tap through a ring of bulk copies.  One thread
 // issues all copies and MMAs; the four warps then read the 128 x c_out
 // accumulator from TMEM (warp w owns TMEM lanes 32w..32w+31) and apply the
 // fused epilogue (bias, ReLU, or the ReLU-derivative mask of the backward
@@ -46,7 +47,7 @@ constexpr uint32_t kPlane = 8704;                 // slab plane stride in shared
 constexpr uint32_t kRowY = kSX * 16;              // bytes between slab rows in y
 constexpr uint32_t kDyPlane = 128 * 16;           // one 8-channel plane of a dY tile
 constexpr int kConvThreads = 128;
-constexpr int kRing = 4, kLag = 2;                // weight ring depth, MMA steps kept queued
+constexpr int kMaxRing = 32;                      // weight ring slots (runtime depth <= this)
 
 __host__ __device__ constexpr uint32_t tap_shift(int tap) {
   return (uint32_t)((((tap / 9) * kSY + (tap / 3) % 3) * kSX + tap % 3) * 16);
@@ -63,6 +64,7 @@ struct ConvArgs {
   int ofstride, ofvalid;
   int X, Y, Z, cin, cout, cc, ngroups, relu;
   int ntx, nty, ntiles;
+  int ring, lag;  // weight slots and MMA steps kept queued; ring == 27 * ngroups: resident
   uint32_t tmem_cols;
   int* error;
 };
@@ -94,25 +96,27 @@ __device__ __forceinline__ void load_bf16x16(const __nv_bfloat16* src, float (&v
 __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_constant__ CUtensorMap amap,
                                                                      const ConvArgs a) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) unsigned long long bars[6 + 2 * kRing];
+  __shared__ __align__(8) unsigned long long bars[6 + 2 * kMaxRing];
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int cc = a.cc, cout = a.cout, G = a.ngroups;
+  const int cc = a.cc, cout = a.cout, G = a.ngroups, R = a.ring, L = a.lag;
+  const int steps_tile = G * 27;
+  const bool resident = R >= steps_tile;
   const uint32_t sb = smem_u32(smem);
   const uint32_t slab_bytes = (uint32_t)cc * kPlane;
   const uint32_t bblk = (uint32_t)cc * cout * 16;
   const uint32_t ring0 = sb + 2 * slab_bytes;
   const uint32_t bar0 = smem_u32(bars);
-  // barriers: 0-1 slab full, 2-3 slab free, 4.. weight full, .. weight free, accumulator full, drain
-  const uint32_t ACC_FULL = bar0 + 8u * (4 + 2 * kRing), DRAIN = ACC_FULL + 8u;
+  // barriers: 0-1 slab full, 2-3 slab free, accumulator full, drain, then R weight-full, R weight-free
+  const uint32_t ACC_FULL = bar0 + 32u, DRAIN = bar0 + 40u;
   auto slab_full = [&](int b) { return bar0 + 8u * b; };
   auto slab_free = [&](int b) { return bar0 + 8u * (2 + b); };
-  auto b_full = [&](int r) { return bar0 + 8u * (4 + r); };
-  auto b_free = [&](int r) { return bar0 + 8u * (4 + kRing + r); };
+  auto b_full = [&](int r) { return bar0 + 8u * (6 + r); };
+  auto b_free = [&](int r) { return bar0 + 8u * (6 + R + r); };
 
   if (tid == 0) {
-    for (int q = 0; q < 6 + 2 * kRing; ++q) mbar_init(bar0 + 8u * q, 1);
+    for (int q = 0; q < 6 + 2 * R; ++q) mbar_init(bar0 + 8u * q, 1);
     mbar_init_fence();
     abort_sh = 0;
   }
@@ -123,7 +127,6 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_
   const uint32_t tmem = tmem_sh;
 
   const int ntiles_me = (int)blockIdx.x < a.ntiles ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-  const int steps_tile = G * 27;
   const long total_steps = (long)ntiles_me * steps_tile;
   const int total_slabs = ntiles_me * G;
   const int nch = a.cin >> 3;
@@ -150,7 +153,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_
     s_issued = q + 1;
   };
   auto issue_w = [&](long s) {
-    const int r = (int)(s % kRing);
+    const int r = (int)(s % R);
     const int blk = (int)(s % steps_tile);  // g * 27 + tap
     const int g = blk / 27, tap = blk % 27;
     mbar_expect_tx(b_full(r), bblk);
@@ -161,7 +164,8 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_
   bool ok = true;
   if (tid == 0 && total_steps > 0) {
     issue_slab(0);
-    for (long p = 0; p < kRing - kLag && p < total_steps; ++p) issue_w(p);
+    const long pre = resident ? steps_tile : R - L;
+    for (long p = 0; p < pre && p < total_steps; ++p) issue_w(p);
   }
   long s = 0;
   int q = 0;
@@ -175,24 +179,28 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_
         tc_fence_after();
         const uint32_t slab = sb + buf * slab_bytes;
         for (int tap = 0; tap < 27; ++tap, ++s) {
-          const int r = (int)(s % kRing);
-          ok = mbar_wait_bounded(b_full(r), (uint32_t)((s / kRing) & 1));
-          if (!ok) break;
-          b_done = s + 1;
+          const int r = (int)(s % R);
+          if (!resident || s < R) {
+            ok = mbar_wait_bounded(b_full(r), (uint32_t)((s / R) & 1));
+            if (!ok) break;
+            b_done = s + 1;
+          }
           const uint32_t a0 = slab + tap_shift(tap), b0 = ring0 + r * bblk;
           for (int j = 0; j < (cc >> 1); ++j) {
             const uint64_t ad = umma_sdesc(a0 + 2u * j * kPlane, kPlane, kRowY);
             const uint64_t bd = umma_sdesc(b0 + 2u * j * cout * 16, cout * 16, 128);
             umma_bf16(tmem, ad, bd, idesc, (g | tap | j) != 0);
           }
-          umma_commit(b_free(r));
-          const long nxt = s + (kRing - kLag);
-          if (nxt < total_steps) {
-            if (s >= kLag) {
-              ok = mbar_wait_bounded(b_free((int)((s - kLag) % kRing)), (uint32_t)(((s - kLag) / kRing) & 1));
-              if (!ok) break;
+          if (!resident) {
+            umma_commit(b_free(r));
+            const long nxt = s + (R - L);
+            if (nxt < total_steps) {
+              if (s >= L) {
+                ok = mbar_wait_bounded(b_free((int)((s - L) % R)), (uint32_t)(((s - L) / R) & 1));
+                if (!ok) break;
+              }
+              issue_w(nxt);
             }
-            issue_w(nxt);
           }
         }
         if (!ok) break;
@@ -212,6 +220,8 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_
         mbar_arrive(ACC_FULL);
       }
     }
+    // the producer's own warp parks here instead of spinning beside it
+    __syncwarp();
     const bool got = mbar_wait_bounded(ACC_FULL, (uint32_t)(it & 1));
     if (__syncthreads_or(!got || abort_sh)) {
       if (tid == 0) atomicExch(a.error, 1);
@@ -253,11 +263,12 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_
     tc_fence_before();
     __syncthreads();
   }
-  // on an abort, wait (bounded) for every copy and MMA still in flight
-  if (tid == 0 && abort_sh) {
+  // on an abort, or when copies are still in flight, wait (bounded) for
+  // every copy and MMA before the shared memory goes away
+  if (tid == 0 && (abort_sh || b_done < b_issued || s_done < s_issued)) {
     umma_commit(DRAIN);
     mbar_wait_bounded(DRAIN, 0);
-    for (long p = b_done; p < b_issued; ++p) mbar_wait_bounded(b_full((int)(p % kRing)), (uint32_t)((p / kRing) & 1));
+    for (long p = b_done; p < b_issued; ++p) mbar_wait_bounded(b_full((int)(p % R)), (uint32_t)((p / R) & 1));
     for (int p = s_done; p < s_issued; ++p) mbar_wait_bounded(slab_full(p & 1), (uint32_t)((p >> 1) & 1));
   }
   tc_fence_before();
@@ -373,6 +384,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_wgrad_tc_kernel(const _
       mbar_arrive(ACC_FULL);
     }
   }
+  __syncwarp();
   const bool got = mbar_wait_bounded(ACC_FULL, 0);
   if (__syncthreads_or(!got || abort_sh)) {
     if (tid == 0) {

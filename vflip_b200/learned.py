@@ -136,7 +136,7 @@ class LearnedPreconditioner:
         self.samples = []
         self.capturing = True
         self.use_vb = use_vb
-        self.cw = (1.0, 1.0)
+        self.sigma = None
         self.last = None
 
     def _grid(self, sim):
@@ -161,29 +161,41 @@ class LearnedPreconditioner:
 
     def train(self, epochs=8, lr=1e-3, seed=0, log=None):
         """Adam over the recorded triples (one sample per step, shuffled per
-        epoch, cosine-decayed learning rate).  The two target channels are
-        weighted by the inverse of their weighted mean square over the set.
-        Returns the mean loss of each epoch."""
+        epoch, cosine-decayed learning rate).  Each target channel is divided
+        by its weighted RMS over the set so the network learns O(1) outputs
+        (the solve's Ritz step is invariant to the outputs' scale).  Returns
+        the mean loss of each epoch."""
         if not self.samples:
             raise RuntimeError("no captured samples to train on")
-        m0 = m1 = wsum = 0.0
+        m = torch.zeros(2, dtype=torch.float64, device=self.s.device)
+        wsum = 0.0
         for _, t, w in self.samples:
-            m0 += float((w * t[..., 0] ** 2).sum())
-            m1 += float((w * t[..., 1] ** 2).sum())
+            m += (w[..., None].double() * t.double() ** 2).sum(dim=(0, 1, 2))
             wsum += float(w.sum())
-        self.cw = (wsum / max(m0, 1e-30), wsum / max(m1, 1e-30))
+        self.sigma = torch.sqrt(m / max(wsum, 1e-30)).clamp_min(1e-30).float()
+        targets = [(t / self.sigma).contiguous() for _, t, _ in self.samples]
         rng = np.random.default_rng(seed)
         total = epochs * len(self.samples)
         losses, step = [], 0
         for ep in range(epochs):
             acc = 0.0
             for i in rng.permutation(len(self.samples)):
-                in2, t, w = self.samples[i]
+                in2, _, w = self.samples[i]
                 lr_t = lr * 0.5 * (1.0 + np.cos(np.pi * step / total))
-                acc += self.net.train_step(in2, t, w, lr_t, self.cw[0], self.cw[1])
+                acc += self.net.train_step(in2, targets[i], w, lr_t, 1.0, 1.0)
                 step += 1
             losses.append(acc / len(self.samples))
             if log:
                 log(ep, losses[-1])
         self.capturing = False
         return losses
+
+    def prediction_error(self, sample):
+        """Weighted relative L2 error of the network's two outputs on one
+        captured triple (targets normalised as in training)."""
+        in2, t, w = sample
+        out = self.net.forward(in2)
+        tn = t / self.sigma
+        num = (w[..., None] * (out - tn) ** 2).sum(dim=(0, 1, 2))
+        den = (w[..., None] * tn ** 2).sum(dim=(0, 1, 2))
+        return tuple(float(x) for x in torch.sqrt(num / den))
