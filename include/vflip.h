@@ -322,6 +322,9 @@ int vflip_unet_conv3(vflip_unet* net, int X, int Y, int Z, const void* in, int i
 int vflip_unet_conv3_wgrad(vflip_unet* net, int X, int Y, int Z, const void* x, int x_ctot, int x_coff, int cin,
                            const void* dy, int dy_ctot, int dy_coff, int cout, float* dw);
 long long vflip_unet_launch_count(const vflip_unet* net);
+/* Multipliers of the two outputs when a learned solve uses them (training
+ * sets them to the RMS its targets were divided by); default 1. */
+int vflip_unet_set_output_scale(vflip_unet* net, float s0, float s1);
 
 /* ---- learned-preconditioned projection -------------------------------------- */
 
@@ -329,11 +332,14 @@ long long vflip_unet_launch_count(const vflip_unet* net);
 #define VFLIP_LEARNED_CAPTURE 1 /* plain MGPCG; also write this solve's training triple */
 #define VFLIP_LEARNED_SOLVE 2   /* network warm start + coarse correction, flexible PCG */
 #define VFLIP_LEARNED_NO_VB 4   /* leave V(b) out of the initial Ritz subspace */
+#define VFLIP_LEARNED_PREV 8    /* add the incoming pressure (previous solve) to the Ritz subspace */
+#define VFLIP_LEARNED_NO_NET 16 /* leave the network out (ablation; net may be NULL) */
+#define VFLIP_LEARNED_SWEEPS(k) ((k) << 8) /* k (0-15) smoothing sweeps on each network vector */
 
 typedef struct vflip_learned_stats {
   int fallback;          /* 1: the learned iteration stalled; plain MGPCG solved from zero */
-  int subspace;          /* vectors kept by the initial Ritz step (0-3) */
-  double gamma[3];       /* Ritz coefficients of V(b), warm start, coarse correction */
+  int subspace;          /* vectors kept by the initial Ritz step (0-4) */
+  double gamma[4];       /* Ritz coefficients of V(b), warm start, V(b) + coarse correction, previous pressure */
   double init_residual;  /* |b - A x0|_inf after the Ritz step */
   double net_ms;         /* network forward time */
 } vflip_learned_stats;
@@ -352,8 +358,12 @@ int vflip_learned_grid(int ni, int nj, int nk, int level, int* X, int* Y, int* Z
  *     and x1 plain PCG's first iterate, and weight = R^L fluid.
  *   VFLIP_LEARNED_SOLVE: the network maps the features to a warm-start
  *     pressure and a coarse correction (trilinear prolongation to the fine
- *     grid); the initial iterate minimises the energy error over
- *     span{V(b), warm start, coarse correction} (Ritz step), then flexible
+ *     grid, scaled by vflip_unet_set_output_scale), each smoothed by
+ *     VFLIP_LEARNED_SWEEPS(k) red-black Gauss-Seidel sweeps on A x = b (the
+ *     correction after adding V(b)); the initial iterate minimises the
+ *     energy error over span{V(b), warm start, V(b) + coarse correction}
+ *     (plus the incoming pressure with VFLIP_LEARNED_PREV) (Ritz step), then
+ *     flexible
  *     (Polak-Ribiere) PCG with the V-cycle runs to the same tolerance.  When
  *     the residual stalls (less than 2x reduction over two iterations, or
  *     NaN) plain MGPCG restarts from zero.  stats->vcycles counts every

@@ -35,7 +35,7 @@ class ConfigC(C.Structure):
 
 
 class LearnedStatsC(C.Structure):
-    _fields_ = [("fallback", C.c_int), ("subspace", C.c_int), ("gamma", C.c_double * 3),
+    _fields_ = [("fallback", C.c_int), ("subspace", C.c_int), ("gamma", C.c_double * 4),
                 ("init_residual", C.c_double), ("net_ms", C.c_double)]
 
 
@@ -84,6 +84,7 @@ SIGNATURES = {
                               _I]),
     "vflip_unet_conv3_wgrad": (_I, [_P, _I, _I, _I, _P, _I, _I, _I, _P, _I, _I, _I, _P]),
     "vflip_unet_launch_count": (C.c_longlong, [_P]),
+    "vflip_unet_set_output_scale": (_I, [_P, _F, _F]),
     "vflip_learned_grid": (_I, [_I, _I, _I, _I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
     "vflip_project_learned": (_I, [_P, _P, _I, _I, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _I,
                                    _P, _P, _P, C.POINTER(SolveStatsC), C.POINTER(LearnedStatsC)]),

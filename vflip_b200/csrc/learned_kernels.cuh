@@ -84,14 +84,16 @@ __global__ void pack2_kernel(const float* __restrict__ c0, const float* __restri
 
 // w[fine] = trilinear interpolation of channel ch of the network output
 // (cell-centred coarse grid of level L) at the fine cell centre, divided by
-// the feature scale; 0 in cells outside the system (diag == 0)
+// the feature scale and multiplied by the network's output scale (the RMS
+// its training targets were divided by); 0 in cells outside the system
+// (diag == 0)
 template <typename V>
 __global__ void prolong_trilinear_kernel(const float* __restrict__ out2, int ch, int X, int Y, int Z, int L,
-                                         const double* __restrict__ scale, const double* __restrict__ diag,
-                                         V* __restrict__ w, int ni, int nj, int nk) {
+                                         const double* __restrict__ scale, float out_scale,
+                                         const double* __restrict__ diag, V* __restrict__ w, int ni, int nj, int nk) {
   const size_t n = (size_t)ni * nj * nk;
   const double s = *scale;
-  const double inv_s = s > 0.0 ? 1.0 / s : 0.0;
+  const double inv_s = s > 0.0 ? (double)out_scale / s : 0.0;
   const float inv_b = 1.0f / (float)(1 << L);
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     if (!(diag[e] > 0.0)) {
@@ -115,6 +117,13 @@ __global__ void prolong_trilinear_kernel(const float* __restrict__ out2, int ch,
   }
 }
 
+// y += x
+template <typename V>
+__global__ void vec_add_kernel(V* __restrict__ y, const V* __restrict__ x, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    y[i] = cvt<V>((typename Num<V>::Acc)((double)ldv(y + i) + (double)ldg(x + i)));
+}
+
 // y = A x for the 7-point operator stored as (diag, +x, +y, +z)
 template <typename S, typename V>
 __global__ void spmv_kernel(const V* __restrict__ x, V* __restrict__ y, const S* __restrict__ diag,
@@ -136,41 +145,52 @@ __global__ void spmv_kernel(const V* __restrict__ x, V* __restrict__ y, const S*
   }
 }
 
-// The nine inner products of the Ritz step over W = [w0 w1 w2], Q = A W:
-// w0.q0 w0.q1 w0.q2 w1.q1 w1.q2 w2.q2 w0.b w1.b w2.b; FP64 block partials
-// written as partials[k * gridDim.x + block]
+// The Ritz step over W = [w0 .. w3] (unused vectors are all zero), Q = A W.
+constexpr int kRitzVecs = 4;
+constexpr int kRitzSums = kRitzVecs * (kRitzVecs + 1) / 2 + kRitzVecs;  // upper G, then W^T b
+template <typename V>
+struct RitzVecs {
+  const V* w[kRitzVecs];
+  const V* q[kRitzVecs];
+  double gamma[kRitzVecs];
+};
+
+// FP64 block partials of G_ij = w_i.q_j (i <= j, row-major upper triangle)
+// and g_i = w_i.b, written as partials[k * gridDim.x + block]
 template <typename V, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) ritz_dots_kernel(const V* __restrict__ w0, const V* __restrict__ w1,
-                                                          const V* __restrict__ w2, const V* __restrict__ q0,
-                                                          const V* __restrict__ q1, const V* __restrict__ q2,
-                                                          const V* __restrict__ b, size_t n, double* partials) {
+__global__ void __launch_bounds__(BLOCK) ritz_dots_kernel(const RitzVecs<V> v, const V* __restrict__ b, size_t n,
+                                                          double* partials) {
   __shared__ double sm[BLOCK / 32];
-  double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double s[kRitzSums];
+#pragma unroll
+  for (int k = 0; k < kRitzSums; ++k) s[k] = 0.0;
   for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK) {
-    const double a0 = (double)ldg(w0 + i), a1 = (double)ldg(w1 + i), a2 = (double)ldg(w2 + i);
-    const double c0 = (double)ldg(q0 + i), c1 = (double)ldg(q1 + i), c2 = (double)ldg(q2 + i);
+    double w[kRitzVecs], q[kRitzVecs];
+#pragma unroll
+    for (int a = 0; a < kRitzVecs; ++a) {
+      w[a] = (double)ldg(v.w[a] + i);
+      q[a] = (double)ldg(v.q[a] + i);
+    }
     const double bb = (double)ldg(b + i);
-    s[0] += a0 * c0;
-    s[1] += a0 * c1;
-    s[2] += a0 * c2;
-    s[3] += a1 * c1;
-    s[4] += a1 * c2;
-    s[5] += a2 * c2;
-    s[6] += a0 * bb;
-    s[7] += a1 * bb;
-    s[8] += a2 * bb;
+    int k = 0;
+#pragma unroll
+    for (int a = 0; a < kRitzVecs; ++a)
+#pragma unroll
+      for (int c = a; c < kRitzVecs; ++c) s[k++] += w[a] * q[c];
+#pragma unroll
+    for (int a = 0; a < kRitzVecs; ++a) s[k++] += w[a] * bb;
   }
-  for (int k = 0; k < 9; ++k) {
+  for (int k = 0; k < kRitzSums; ++k) {
     const double t = block_sum<BLOCK>(s[k], sm);
     if (threadIdx.x == 0) partials[(size_t)k * gridDim.x + blockIdx.x] = t;
   }
 }
 
-// folds the nine partial rows in block order into out[9] (one block)
+// folds the partial rows in block order into out[kRitzSums] (one block)
 template <int BLOCK>
 __global__ void ritz_fold_kernel(const double* __restrict__ partials, int nb, double* __restrict__ out) {
   __shared__ double sm[BLOCK / 32];
-  for (int k = 0; k < 9; ++k) {
+  for (int k = 0; k < kRitzSums; ++k) {
     double v = 0.0;
     for (int q = threadIdx.x; q < nb; q += BLOCK) v += partials[(size_t)k * nb + q];
     v = block_sum<BLOCK>(v, sm);
@@ -178,23 +198,23 @@ __global__ void ritz_fold_kernel(const double* __restrict__ partials, int nb, do
   }
 }
 
-// x = sum g_i w_i, r = b - sum g_i q_i, partial |r|_inf (converged flag set
-// against the tolerance by the last block)
+// x = sum gamma_i w_i, r = b - sum gamma_i q_i, partial |r|_inf (converged
+// flag set against the tolerance by the last block)
 template <typename V, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) ritz_combine_kernel(const V* __restrict__ w0, const V* __restrict__ w1,
-                                                             const V* __restrict__ w2, const V* __restrict__ q0,
-                                                             const V* __restrict__ q1, const V* __restrict__ q2,
-                                                             const V* __restrict__ b, double g0, double g1, double g2,
+__global__ void __launch_bounds__(BLOCK) ritz_combine_kernel(const RitzVecs<V> v, const V* __restrict__ b,
                                                              V* __restrict__ x, V* __restrict__ r, size_t n,
                                                              double* partials, PcgScalars* st) {
   __shared__ double sm[BLOCK / 32];
   double m = 0.0;
   for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK) {
-    const double xv = g0 * (double)ldg(w0 + i) + g1 * (double)ldg(w1 + i) + g2 * (double)ldg(w2 + i);
-    const double rv =
-        (double)ldg(b + i) - (g0 * (double)ldg(q0 + i) + g1 * (double)ldg(q1 + i) + g2 * (double)ldg(q2 + i));
+    double xv = 0.0, av = 0.0;
+#pragma unroll
+    for (int a = 0; a < kRitzVecs; ++a) {
+      xv += v.gamma[a] * (double)ldg(v.w[a] + i);
+      av += v.gamma[a] * (double)ldg(v.q[a] + i);
+    }
     x[i] = cvt<V>((typename Num<V>::Acc)xv);
-    const V rt = cvt<V>((typename Num<V>::Acc)rv);
+    const V rt = cvt<V>((typename Num<V>::Acc)((double)ldg(b + i) - av));
     r[i] = rt;
     m = fmax(m, fabs((double)ldv(&rt)));
   }

@@ -666,4 +666,11 @@ int vflip_unet_conv3_wgrad(vflip_unet* u, int X, int Y, int Z, const void* x, in
 
 long long vflip_unet_launch_count(const vflip_unet* u) { return u ? u->net->launches : 0; }
 
+int vflip_unet_set_output_scale(vflip_unet* u, float s0, float s1) {
+  if (!u || !(s0 > 0.0f) || !(s1 > 0.0f)) return VFLIP_ERR_ARG;
+  u->net->out_scale[0] = s0;
+  u->net->out_scale[1] = s1;
+  return VFLIP_OK;
+}
+
 }  // extern "C"

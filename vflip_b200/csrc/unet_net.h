@@ -69,6 +69,7 @@ class Net {
   float *params = nullptr, *grads = nullptr, *adam_m = nullptr, *adam_v = nullptr;
   __nv_bfloat16 *wf[kNumLayers] = {}, *wd[kNumLayers] = {};
   int adam_t = 0;
+  float out_scale[2] = {1.0f, 1.0f};  // multiplies the two outputs when the solver uses them
   long long launches = 0;
   int* d_error = nullptr;
 

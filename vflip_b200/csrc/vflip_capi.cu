@@ -775,30 +775,39 @@ int learned_capture(vflip_ctx* ctx, const LearnedOpts& lo, const Dims& d, const 
   return VFLIP_OK;
 }
 
-// Energy-minimising coefficients over the active subset of three vectors:
-// G gamma = g with G_ij = w_i.A w_j; vectors whose pivot collapses (linearly
+// Energy-minimising coefficients over the active subset of the Ritz
+// vectors: G gamma = g with G_ij = w_i.A w_j (upper triangle first in
+// `dots`, then g_i = w_i.b); vectors whose pivot collapses (linearly
 // dependent, zero, or non-finite) are dropped.  Returns the kept count.
-int ritz_solve(const double* dots, bool use0, double* gamma) {
-  const double G[3][3] = {{dots[0], dots[1], dots[2]}, {dots[1], dots[3], dots[4]}, {dots[2], dots[4], dots[5]}};
-  const double g[3] = {dots[6], dots[7], dots[8]};
-  bool on[3] = {use0, true, true};
-  for (int i = 0; i < 3; ++i) {
+int ritz_solve(const double* dots, const bool* use, double* gamma) {
+  constexpr int M = kRitzVecs;
+  double G[M][M], g[M];
+  int k = 0;
+  for (int a = 0; a < M; ++a)
+    for (int c = a; c < M; ++c) G[a][c] = G[c][a] = dots[k++];
+  for (int a = 0; a < M; ++a) g[a] = dots[k++];
+  bool on[M];
+  for (int i = 0; i < M; ++i) {
     gamma[i] = 0.0;
-    if (!(G[i][i] > 0.0) || !std::isfinite(G[i][i]) || !std::isfinite(g[i])) on[i] = false;
+    on[i] = use[i] && G[i][i] > 0.0 && std::isfinite(G[i][i]) && std::isfinite(g[i]);
   }
-  for (int attempt = 0; attempt < 3; ++attempt) {
-    int idx[3], m = 0;
-    for (int i = 0; i < 3; ++i)
+  for (int attempt = 0; attempt < M; ++attempt) {
+    int idx[M], m = 0;
+    for (int i = 0; i < M; ++i)
       if (on[i]) idx[m++] = i;
     if (m == 0) return 0;
-    // Cholesky of the scaled subset
-    double L[3][3] = {}, sc[3];
+    // Cholesky of the diagonally scaled subset
+    double L[M][M] = {}, sc[M];
     for (int a = 0; a < m; ++a) sc[a] = 1.0 / std::sqrt(G[idx[a]][idx[a]]);
     int bad = -1;
     for (int a = 0; a < m && bad < 0; ++a) {
       for (int b = 0; b <= a; ++b) {
         double v = G[idx[a]][idx[b]] * sc[a] * sc[b];
         for (int c = 0; c < b; ++c) v -= L[a][c] * L[b][c];
+        if (!std::isfinite(v)) {
+          bad = a;
+          break;
+        }
         if (a == b) {
           if (!(v > 1e-10)) {
             bad = a;
@@ -814,7 +823,7 @@ int ritz_solve(const double* dots, bool use0, double* gamma) {
       on[idx[bad]] = false;
       continue;
     }
-    double y[3], t[3];
+    double y[M], t[M];
     for (int a = 0; a < m; ++a) {
       double v = g[idx[a]] * sc[a];
       for (int c = 0; c < a; ++c) v -= L[a][c] * y[c];
@@ -841,10 +850,10 @@ int learned_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double
   const size_t nv = (size_t)X * Y * Z;
   float *in2, *out2;
   double* ritz;
-  V *x, *r, *r2, *bv, *z, *w0, *w1, *w2, *q0, *q1, *q2, *s0, *s1, *q;
+  V *x, *r, *r2, *bv, *z, *w0, *w1, *w2, *w3, *q0, *q1, *q2, *q3, *s0, *s1, *q;
   VF_ALLOC(in2, float, "lrn_in2", 2 * nv);
   VF_ALLOC(out2, float, "lrn_out2", 2 * nv);
-  VF_ALLOC(ritz, double, "lrn_ritz", 9);
+  VF_ALLOC(ritz, double, "lrn_ritz", kRitzSums);
   VF_ALLOC(x, V, "pcg_x", n);
   VF_ALLOC(r, V, "pcg_r", n);
   VF_ALLOC(z, V, "pcg_z", n);
@@ -859,7 +868,19 @@ int learned_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double
   VF_ALLOC(q0, V, "lrn_q0", n);
   VF_ALLOC(q1, V, "lrn_q1", n);
   VF_ALLOC(q2, V, "lrn_q2", n);
+  VF_ALLOC(w3, V, "lrn_w3", n);
+  VF_ALLOC(q3, V, "lrn_q3", n);
   vflip_learned_stats ls{};
+  const bool use_vb = !(lo.mode & VFLIP_LEARNED_NO_VB), use_net = !(lo.mode & VFLIP_LEARNED_NO_NET),
+             use_prev = (lo.mode & VFLIP_LEARNED_PREV) != 0;
+  const int g = grid_for(n, 256, ctx->num_sms);
+  // the incoming pressure (the previous solve's answer) before it is overwritten
+  if (use_prev) {
+    convert_kernel<V><<<g, 256, 0, ctx->stream>>>(result, w3, n);
+    VF_LAUNCH_CHECK();
+  } else {
+    VF_CUDA(cudaMemsetAsync(w3, 0, n * sizeof(V), ctx->stream));
+  }
   int rc;
   VF_CUDA(cudaMemsetAsync(ctx->st, 0, sizeof(PcgScalars), ctx->stream));
   const int gb = grid_for(n, kRedBlock, ctx->num_sms);
@@ -904,38 +925,44 @@ int learned_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double
   VF_CUDA(cudaMemcpyAsync(bv, r, n * sizeof(V), cudaMemcpyDeviceToDevice, ctx->stream));
 
   // network: features -> (warm start, coarse correction) on its grid
-  float* mc;
-  double* scale;
-  if ((rc = learned_features(ctx, lo, d, rhs, X, Y, Z, in2, &mc, &scale))) return rc;
-  vflip::unet::Net& net = *lo.net;
-  const cudaStream_t saved = net.stream;
-  net.stream = ctx->stream;
-  cudaEvent_t na, nb;
-  VF_CUDA(cudaEventCreate(&na));
-  VF_CUDA(cudaEventCreate(&nb));
-  cudaEventRecord(na, ctx->stream);
-  rc = net.forward(X, Y, Z, in2, out2);
-  cudaEventRecord(nb, ctx->stream);
-  if (!rc) rc = net.sync_error();
-  net.stream = saved;
-  if (!rc) {
-    float ms = 0.0f;
-    cudaEventElapsedTime(&ms, na, nb);
-    ls.net_ms = ms;
+  float out_scale[2] = {1.0f, 1.0f};
+  if (use_net) {
+    float* mc;
+    double* scale;
+    if ((rc = learned_features(ctx, lo, d, rhs, X, Y, Z, in2, &mc, &scale))) return rc;
+    vflip::unet::Net& net = *lo.net;
+    out_scale[0] = net.out_scale[0];
+    out_scale[1] = net.out_scale[1];
+    const cudaStream_t saved = net.stream;
+    net.stream = ctx->stream;
+    cudaEvent_t na, nb;
+    VF_CUDA(cudaEventCreate(&na));
+    VF_CUDA(cudaEventCreate(&nb));
+    cudaEventRecord(na, ctx->stream);
+    rc = net.forward(X, Y, Z, in2, out2);
+    cudaEventRecord(nb, ctx->stream);
+    if (!rc) rc = net.sync_error();
+    net.stream = saved;
+    if (!rc) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, na, nb);
+      ls.net_ms = ms;
+    }
+    cudaEventDestroy(na);
+    cudaEventDestroy(nb);
+    if (rc) return ctx->fail(rc, "network: %s", net.err.c_str());
+    prolong_trilinear_kernel<V><<<g, 256, 0, ctx->stream>>>(out2, 0, X, Y, Z, lo.level, scale, out_scale[0],
+                                                            lo.diag, w1, d.ni, d.nj, d.nk);
+    VF_LAUNCH_CHECK();
+    prolong_trilinear_kernel<V><<<g, 256, 0, ctx->stream>>>(out2, 1, X, Y, Z, lo.level, scale, out_scale[1],
+                                                            lo.diag, w2, d.ni, d.nj, d.nk);
+    VF_LAUNCH_CHECK();
+  } else {
+    VF_CUDA(cudaMemsetAsync(w1, 0, n * sizeof(V), ctx->stream));
+    VF_CUDA(cudaMemsetAsync(w2, 0, n * sizeof(V), ctx->stream));
   }
-  cudaEventDestroy(na);
-  cudaEventDestroy(nb);
-  if (rc) return ctx->fail(rc, "network: %s", net.err.c_str());
 
   // initial subspace on the fine grid
-  const int g = grid_for(n, 256, ctx->num_sms);
-  prolong_trilinear_kernel<V><<<g, 256, 0, ctx->stream>>>(out2, 0, X, Y, Z, lo.level, scale, lo.diag, w1, d.ni, d.nj,
-                                                          d.nk);
-  VF_LAUNCH_CHECK();
-  prolong_trilinear_kernel<V><<<g, 256, 0, ctx->stream>>>(out2, 1, X, Y, Z, lo.level, scale, lo.diag, w2, d.ni, d.nj,
-                                                          d.nk);
-  VF_LAUNCH_CHECK();
-  const bool use_vb = !(lo.mode & VFLIP_LEARNED_NO_VB);
   if (use_vb) {
     if ((rc = vcycle<S0, SC, V>(ctx, T, bv, w0, false))) return rc;
     ++vcycles;
@@ -943,23 +970,50 @@ int learned_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double
     VF_CUDA(cudaMemsetAsync(w0, 0, n * sizeof(V), ctx->stream));
   }
   const Level<S0, V>& F = T.fine;
-  spmv_kernel<S0, V><<<g, 256, 0, ctx->stream>>>(w0, q0, F.diag, F.xp, F.yp, F.zp, d.ni, d.nj, d.nk);
-  VF_LAUNCH_CHECK();
-  spmv_kernel<S0, V><<<g, 256, 0, ctx->stream>>>(w1, q1, F.diag, F.xp, F.yp, F.zp, d.ni, d.nj, d.nk);
-  VF_LAUNCH_CHECK();
-  spmv_kernel<S0, V><<<g, 256, 0, ctx->stream>>>(w2, q2, F.diag, F.xp, F.yp, F.zp, d.ni, d.nj, d.nk);
-  VF_LAUNCH_CHECK();
-  const int rb = std::min(gb, kMaxPartials / 9);
-  ritz_dots_kernel<V, kRedBlock><<<rb, kRedBlock, 0, ctx->stream>>>(w0, w1, w2, q0, q1, q2, bv, n, ctx->partials);
+  // the coarse correction corrects V(b); smoothing sweeps on A x = b damp
+  // the rough error the coarse prediction and its interpolation carry
+  const int ksw = (lo.mode >> 8) & 15;
+  if (use_net) {
+    vec_add_kernel<V><<<g, 256, 0, ctx->stream>>>(w2, w0, n);
+    VF_LAUNCH_CHECK();
+  }
+  if (use_net && ksw > 0) {
+    V* tmp;
+    VF_ALLOC(tmp, V, "lrn_tmp", n);
+    for (V* v : {w1, w2}) {
+      V *src = v, *dst = tmp;
+      for (int k = 0; k < ksw; ++k) {
+        if ((rc = sweep<S0, V>(ctx, F, bv, src, dst, nullptr, nullptr, nullptr))) return rc;
+        std::swap(src, dst);
+      }
+      if (src != v) VF_CUDA(cudaMemcpyAsync(v, src, n * sizeof(V), cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+  }
+  RitzVecs<V> rv;
+  V* ws[kRitzVecs] = {w0, w1, w2, w3};
+  V* qs[kRitzVecs] = {q0, q1, q2, q3};
+  const bool use[kRitzVecs] = {use_vb, use_net, use_net, use_prev};
+  for (int a = 0; a < kRitzVecs; ++a) {
+    rv.w[a] = ws[a];
+    rv.q[a] = qs[a];
+    if (use[a]) {
+      spmv_kernel<S0, V><<<g, 256, 0, ctx->stream>>>(ws[a], qs[a], F.diag, F.xp, F.yp, F.zp, d.ni, d.nj, d.nk);
+      VF_LAUNCH_CHECK();
+    } else {
+      VF_CUDA(cudaMemsetAsync(qs[a], 0, n * sizeof(V), ctx->stream));
+    }
+  }
+  const int rb = std::min(gb, kMaxPartials / kRitzSums);
+  ritz_dots_kernel<V, kRedBlock><<<rb, kRedBlock, 0, ctx->stream>>>(rv, bv, n, ctx->partials);
   VF_LAUNCH_CHECK();
   ritz_fold_kernel<kRedBlock><<<1, kRedBlock, 0, ctx->stream>>>(ctx->partials, rb, ritz);
   VF_LAUNCH_CHECK();
-  double dots[9];
+  double dots[kRitzSums];
   VF_CUDA(cudaMemcpyAsync(dots, ritz, sizeof dots, cudaMemcpyDeviceToHost, ctx->stream));
   VF_CUDA(cudaStreamSynchronize(ctx->stream));
-  ls.subspace = ritz_solve(dots, use_vb, ls.gamma);
-  ritz_combine_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(
-      w0, w1, w2, q0, q1, q2, bv, ls.gamma[0], ls.gamma[1], ls.gamma[2], x, r, n, ctx->partials, ctx->st);
+  ls.subspace = ritz_solve(dots, use, ls.gamma);
+  for (int a = 0; a < kRitzVecs; ++a) rv.gamma[a] = ls.gamma[a];
+  ritz_combine_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(rv, bv, x, r, n, ctx->partials, ctx->st);
   VF_LAUNCH_CHECK();
   if ((rc = read_scalars(ctx))) return rc;
   residual = ls.init_residual = h.res;
@@ -1448,10 +1502,11 @@ int vflip_project_learned(vflip_ctx* ctx, vflip_unet* net, int mode, int level, 
   if (level < 0 || level > 8) return ctx->fail(VFLIP_ERR_ARG, "level %d out of range", level);
   const bool solve = (mode & VFLIP_LEARNED_SOLVE) != 0, capture = (mode & VFLIP_LEARNED_CAPTURE) != 0;
   if (solve == capture) return ctx->fail(VFLIP_ERR_ARG, "mode must select exactly one of CAPTURE and SOLVE");
-  if (solve && (!net || !net->net)) return ctx->fail(VFLIP_ERR_ARG, "learned solve needs a network");
+  if (solve && !(mode & VFLIP_LEARNED_NO_NET) && (!net || !net->net))
+    return ctx->fail(VFLIP_ERR_ARG, "learned solve needs a network");
   if (capture && (!sample_in2 || !sample_target2 || !sample_weight))
     return ctx->fail(VFLIP_ERR_ARG, "capture needs the three sample buffers");
-  if (solve && net->net->device != ctx->cfg.device)
+  if (solve && net && net->net && net->net->device != ctx->cfg.device)
     return ctx->fail(VFLIP_ERR_ARG, "network and context are on different devices");
   LearnedOpts lo;
   lo.net = net ? net->net : nullptr;

@@ -63,6 +63,9 @@ class UNet:
         self._check(self.lib.vflip_unet_get_params(self.h, p.ctypes.data))
         return p
 
+    def set_output_scale(self, s0, s1):
+        self._check(self.lib.vflip_unet_set_output_scale(self.h, float(s0), float(s1)))
+
     def set_params(self, p):
         p = np.ascontiguousarray(p, np.float32)
         assert p.size == self.nparams
@@ -115,7 +118,11 @@ class UNet:
         return dw
 
 
-CAPTURE, SOLVE, NO_VB = 1, 2, 4
+CAPTURE, SOLVE, NO_VB, PREV, NO_NET = 1, 2, 4, 8, 16
+
+
+def SWEEPS(k):
+    return int(k) << 8
 
 
 class LearnedPreconditioner:
@@ -129,13 +136,16 @@ class LearnedPreconditioner:
     falls back to plain MGPCG when the residual stalls.
     """
 
-    def __init__(self, solver, level=1, seed=0, net=None, use_vb=True):
+    def __init__(self, solver, level=1, seed=0, net=None, use_vb=True, sweeps=2, use_prev=False, use_net=True):
         self.s = solver
         self.level = level
         self.net = net if net is not None else UNet(device=solver.device.index, seed=seed)
         self.samples = []
         self.capturing = True
         self.use_vb = use_vb
+        self.sweeps = sweeps
+        self.use_prev = use_prev
+        self.use_net = use_net
         self.sigma = None
         self.last = None
 
@@ -154,10 +164,14 @@ class LearnedPreconditioner:
             conv, _, st, ls = sim.project_learned(None, CAPTURE, self.level, sample=sample)
             self.samples.append(sample)
         else:
-            mode = SOLVE | (0 if self.use_vb else NO_VB)
+            mode = self.mode()
             conv, _, st, ls = sim.project_learned(self.net, mode, self.level)
         self.last = ls
         return conv, st
+
+    def mode(self):
+        return (SOLVE | (0 if self.use_vb else NO_VB) | (PREV if self.use_prev else 0) |
+                (0 if self.use_net else NO_NET) | SWEEPS(self.sweeps))
 
     def train(self, epochs=8, lr=1e-3, seed=0, log=None):
         """Adam over the recorded triples (one sample per step, shuffled per
@@ -173,6 +187,7 @@ class LearnedPreconditioner:
             m += (w[..., None].double() * t.double() ** 2).sum(dim=(0, 1, 2))
             wsum += float(w.sum())
         self.sigma = torch.sqrt(m / max(wsum, 1e-30)).clamp_min(1e-30).float()
+        self.net.set_output_scale(float(self.sigma[0]), float(self.sigma[1]))
         targets = [(t / self.sigma).contiguous() for _, t, _ in self.samples]
         rng = np.random.default_rng(seed)
         total = epochs * len(self.samples)
