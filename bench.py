@@ -47,6 +47,10 @@ def parse():
     ap.add_argument("--dt", type=float, default=0.01)
     ap.add_argument("--precision", default="fp32", choices=sorted(PREC))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner arm")
+    ap.add_argument("--learned-level", type=int, default=1)
+    ap.add_argument("--learned-capture", type=int, default=40)
+    ap.add_argument("--learned-epochs", type=int, default=16)
     ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds for the reference arm's timed steps")
     return ap.parse_args()
 
@@ -232,10 +236,59 @@ def run_vflip(a):
         }
         if not a.no_cpu_baseline and world == 1:
             out["cpu_baseline"] = cpu_baseline(a, {k: sim.f[k].cpu().numpy().copy() for k in sim.FIELDS}, params)
+        if not a.no_learned and world == 1:
+            out["learned"] = learned_arm(a, sim, solver)
     solver.close()
     if world > 1:
         dist.destroy_process_group()
     return out
+
+
+def learned_arm(a, sim, solver):
+    """The learned-preconditioned arm on the same plume: capture the next
+    `learned_capture` plain projections as training triples, train the U-Net
+    on the GPU (untimed), then time `steps` learned steps and, right after,
+    `steps` plain steps from the state they reached (CUDA events, same
+    windowing as the headline)."""
+    import numpy as np
+    import torch
+
+    from vflip_b200.learned import LearnedPreconditioner
+
+    pre = LearnedPreconditioner(solver, level=a.learned_level, seed=0, use_vb=False, sweeps=2)
+    for _ in range(a.learned_capture):
+        sim.step(pre)
+    torch.cuda.synchronize()
+    t0 = time.time()
+    losses = pre.train(epochs=a.learned_epochs, lr=1e-3)
+    torch.cuda.synchronize()
+    train_s = time.time() - t0
+
+    def timed(precond):
+        vc, net_ms, fb = [], [], 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(a.steps):
+            conv, st = sim.step(precond)
+            vc.append(st.vcycles)
+            if precond is not None:
+                net_ms.append(precond.last.net_ms)
+                fb += int(precond.last.fallback)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), vc, net_ms, fb
+
+    ms_l, vc_l, net_ms, fb = timed(pre)
+    ms_p, vc_p, _, _ = timed(None)
+    return {"steps_per_s": a.steps / (ms_l * 1e-3), "vcycles_mean": float(np.mean(vc_l)),
+            "plain_steps_per_s_adjacent": a.steps / (ms_p * 1e-3), "plain_vcycles_mean_adjacent": float(np.mean(vc_p)),
+            "vcycle_ratio_learned_over_plain": float(np.mean(vc_l) / np.mean(vc_p)),
+            "steps_per_s_ratio_learned_over_plain": ms_p / ms_l, "network_ms_mean": float(np.mean(net_ms)),
+            "fallbacks": fb, "train_s": train_s, "train_final_loss": losses[-1],
+            "config": {"network_grid_level": a.learned_level, "capture_steps": a.learned_capture,
+                       "epochs": a.learned_epochs, "ritz_subspace": "network warm start + coarse correction (no V(b)), "
+                       "2 smoothing sweeps each", "unet": "4 levels, 16/32/64/128 channels, BF16 tcgen05 convs"}}
 
 
 def solve_diagnostics(sim, device):
