@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--precision", default="fp32", choices=sorted(PREC))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner arm")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched uneven-Poisson arm")
     ap.add_argument("--learned-level", type=int, default=1)
     ap.add_argument("--learned-capture", type=int, default=40)
     ap.add_argument("--learned-epochs", type=int, default=16)
@@ -238,6 +239,8 @@ def run_vflip(a):
             out["cpu_baseline"] = cpu_baseline(a, {k: sim.f[k].cpu().numpy().copy() for k in sim.FIELDS}, params)
         if not a.no_learned and world == 1:
             out["learned"] = learned_arm(a, sim, solver)
+        if not a.no_batched and world == 1:
+            out["batched"] = batched_arm(solver)
     solver.close()
     if world > 1:
         dist.destroy_process_group()
@@ -289,6 +292,35 @@ def learned_arm(a, sim, solver):
             "config": {"network_grid_level": a.learned_level, "capture_steps": a.learned_capture,
                        "epochs": a.learned_epochs, "ritz_subspace": "network warm start + coarse correction (no V(b)), "
                        "2 smoothing sweeps each", "unet": "4 levels, 16/32/64/128 channels, BF16 tcgen05 convs"}}
+
+
+def batched_arm(solver, count=32, reps=2):
+    """32 independent systems, sides uniform from {32..192}, random solid
+    spheres, rhs = divergence of a smoothed Gaussian velocity (seeded), to
+    1e-6: the whole batch as one CUDA graph (device-side PCG loops, systems
+    as parallel branches) vs one system after another; both timed from the
+    first hierarchy build to the last result (CUDA events, best of `reps`)."""
+    import numpy as np
+
+    from vflip_b200 import scenes
+
+    systems, sides = scenes.batch_workload(solver, count=count, seed=0)
+    res = {}
+    for name, mode in (("graph", 0), ("loop", 1)):
+        best, stats = None, None
+        for _ in range(reps + 1):  # the first call also creates the per-system contexts
+            ok, _, st = solver.batched_solve(systems, 1e-6, 100, mode=mode)
+            ms = st[0].solve_ms
+            best = ms if best is None or ms < best else best
+            stats = st
+        res[name] = (best, ok, stats)
+    cells = sum(s ** 3 for s in sides)
+    g, l = res["graph"], res["loop"]
+    return {"systems": count, "sides": sides, "cells": cells, "graph_ms": g[0], "loop_ms": l[0],
+            "speedup_graph_over_loop": l[0] / g[0], "all_converged": bool(g[1] and l[1]),
+            "iterations_mean": float(np.mean([x.iterations for x in g[2]])),
+            "iterations_equal": all(x.iterations == y.iterations for x, y in zip(g[2], l[2])),
+            "cells_per_s_graph": cells / (g[0] * 1e-3)}
 
 
 def solve_diagnostics(sim, device):

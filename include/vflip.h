@@ -374,6 +374,34 @@ int vflip_project_learned(vflip_ctx* ctx, vflip_unet* net, int mode, int level, 
                           int max_iterations, float* sample_in2, float* sample_target2, float* sample_weight,
                           vflip_solve_stats* stats, vflip_learned_stats* lstats);
 
+/* ---- batched solves ---------------------------------------------------------- */
+
+/* One Poisson system of a batch: the symmetric 7-point operator (diag, +x,
+ * +y, +z couplings, FP64, as vflip_amgpcg_solve takes it), its rhs and the
+ * result array, all device pointers. */
+typedef struct vflip_system {
+  int ni, nj, nk;
+  const double *diag, *xp, *yp, *zp;
+  const double* rhs;
+  double* result;
+} vflip_system;
+
+#define VFLIP_BATCH_GRAPH 0 /* one CUDA graph: each system's PCG loop a device-side while node, systems in parallel */
+#define VFLIP_BATCH_LOOP 1  /* one system after another (vflip_amgpcg_solve per system) */
+
+/* Solves many independent systems of uneven sizes with the context's MGPCG
+ * (same hierarchy, smoother, tolerance test and precision as
+ * vflip_amgpcg_solve).  VFLIP_BATCH_GRAPH builds every system's hierarchy,
+ * then captures the batch into one CUDA graph and launches it once: per
+ * system a parallel branch whose PCG iterations run in a conditional while
+ * node whose condition a kernel sets from the device-side scalars, so no
+ * iteration returns to the host.  Returns 0 when every system converged, 1
+ * otherwise; stats[i] per system (solve_ms = the whole call).  No reference
+ * counterpart (the reference solves one system per AMGPCGSolve call,
+ * SS/AlgebraicMultigrid.h:189-301). */
+int vflip_batched_solve(vflip_ctx* ctx, int nsys, const vflip_system* systems, double tolerance_factor,
+                        int max_iterations, int mode, vflip_solve_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -34,6 +34,11 @@ class ConfigC(C.Structure):
                 ("smoother_ctas_per_sm", C.c_int)]
 
 
+class SystemC(C.Structure):
+    _fields_ = [("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int), ("diag", C.c_void_p), ("xp", C.c_void_p),
+                ("yp", C.c_void_p), ("zp", C.c_void_p), ("rhs", C.c_void_p), ("result", C.c_void_p)]
+
+
 class LearnedStatsC(C.Structure):
     _fields_ = [("fallback", C.c_int), ("subspace", C.c_int), ("gamma", C.c_double * 4),
                 ("init_residual", C.c_double), ("net_ms", C.c_double)]
@@ -85,6 +90,7 @@ SIGNATURES = {
     "vflip_unet_conv3_wgrad": (_I, [_P, _I, _I, _I, _P, _I, _I, _I, _P, _I, _I, _I, _P]),
     "vflip_unet_launch_count": (C.c_longlong, [_P]),
     "vflip_unet_set_output_scale": (_I, [_P, _F, _F]),
+    "vflip_batched_solve": (_I, [_P, _I, C.POINTER(SystemC), _D, _I, _I, C.POINTER(SolveStatsC)]),
     "vflip_learned_grid": (_I, [_I, _I, _I, _I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
     "vflip_project_learned": (_I, [_P, _P, _I, _I, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _I,
                                    _P, _P, _P, C.POINTER(SolveStatsC), C.POINTER(LearnedStatsC)]),

@@ -187,6 +187,37 @@ __global__ void __launch_bounds__(BLOCK) dot_kernel(const T* __restrict__ a, con
   finish_reduction<BLOCK>(partials, gridDim.x, st, kind, 0.0, gridDim.x);
 }
 
+// ---- graph-resident PCG (batched solves): the loop runs as a CUDA graph
+// while-node whose condition a kernel sets from the device-side scalars.
+
+// after pcg_init: rho = 1 so the first beta only scales s = 0
+__global__ void pcg_loop_init_kernel(PcgScalars* st, int* it, cudaGraphConditionalHandle h) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    st->rho = 1.0;
+    st->beta = 0.0;
+    *it = 0;
+    cudaGraphSetConditional(h, st->converged ? 0u : 1u);
+  }
+}
+
+// s = z + beta s in place (the direction update of AlgebraicMultigrid.h:284)
+template <typename T>
+__global__ void pcg_direction_kernel(const T* __restrict__ z, T* __restrict__ s, size_t n, const PcgScalars* st) {
+  using A = typename Num<T>::Acc;
+  const double beta = st->beta;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    s[i] = cvt<T>((A)((double)ldg(z + i) + beta * (double)ldv(s + i)));
+}
+
+// one iteration done: continue while not converged, rho valid, below maxit
+__global__ void pcg_loop_cond_kernel(const PcgScalars* st, int* it, int maxit, cudaGraphConditionalHandle h) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    const int k = ++*it;
+    const bool go = !st->converged && !st->bad_rho && k < maxit && st->res == st->res;
+    cudaGraphSetConditional(h, go ? 1u : 0u);
+  }
+}
+
 template <typename T, int BLOCK>
 __global__ void to_double_kernel(const T* __restrict__ src, double* __restrict__ dst, size_t n) {
   for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK)

@@ -57,6 +57,7 @@ struct vflip_ctx {
   double last_ms = 0.0;
   int num_sms = 148;
   unsigned long long launches = 0;  // kernels launched through this context
+  std::vector<vflip_ctx*> subs;     // per-system contexts of batched solves
   // fine-level sweep timing (vflip_set_profiling)
   bool profiling = false;
   size_t prof_fine_n = 0;
@@ -1128,6 +1129,187 @@ int solve_stencil(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag, co
   return status;
 }
 
+// ---------------------------------------------------------------- batched
+// Per-system state of a graph-resident batched solve; each system owns a
+// sub-context (its scalars, partials, buffers, error flag).
+template <typename S0, typename SC, typename V>
+struct BatchItem {
+  vflip_ctx* sub = nullptr;
+  Hierarchy64 H;
+  Typed<S0, SC, V> T;
+  V *x, *r, *z, *s, *q, *sd;
+  int* it;
+  cudaGraphConditionalHandle h;
+};
+
+int batch_sub(vflip_ctx* ctx, size_t i, vflip_ctx** out) {
+  while (ctx->subs.size() <= i) {
+    vflip_config c = ctx->cfg;
+    c.stream = nullptr;
+    vflip_ctx* sub = nullptr;
+    const int rc = vflip_create(&sub, &c);
+    if (rc) return ctx->fail(rc, "cannot create a per-system context");
+    ctx->subs.push_back(sub);
+  }
+  *out = ctx->subs[i];
+  return VFLIP_OK;
+}
+
+// Every system's PCG loop as one CUDA graph: per system a parallel branch
+// [init] -> while(not converged) {V-cycle; s = z + beta s; q = A s; x, r
+// update; condition} -> [FP64 result].  The loop never returns to the host.
+template <typename S0, typename SC, typename V>
+int batched_graph(vflip_ctx* ctx, int nsys, const vflip_system* sys, double tol, int maxit, vflip_solve_stats* stats,
+                  const char* tag) {
+  int rc;
+  std::vector<BatchItem<S0, SC, V>> items(nsys);
+  cudaStream_t cs = nullptr;
+  VF_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  auto cleanup = [&]() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (auto& it : items)
+      if (it.sub) it.sub->stream = nullptr;
+    cudaStreamDestroy(cs);
+  };
+  auto bail = [&](int code) {
+    cleanup();
+    return code;
+  };
+  // set-up: hierarchies and vectors (eager, on the capture stream)
+  for (int i = 0; i < nsys; ++i) {
+    BatchItem<S0, SC, V>& b = items[i];
+    if ((rc = batch_sub(ctx, i, &b.sub))) return bail(rc);
+    vflip_ctx* c = b.sub;
+    c->stream = cs;
+    c->profiling = false;
+    const vflip_system& y = sys[i];
+    if ((rc = build_hierarchy64(c, y.ni, y.nj, y.nk, y.diag, y.xp, y.yp, y.zp, b.H)) ||
+        (rc = make_typed(c, b.H, y.diag, y.xp, y.yp, y.zp, b.T, tag))) {
+      ctx->err = c->err;
+      return bail(rc);
+    }
+    const size_t n = (size_t)y.ni * y.nj * y.nk;
+    V** vs[6] = {&b.x, &b.r, &b.z, &b.s, &b.q, &b.sd};
+    const char* names[6] = {"bat_x", "bat_r", "bat_z", "bat_s", "bat_q", "bat_sd"};
+    for (int k = 0; k < 6; ++k) {
+      *vs[k] = (V*)c->buf(names[k], sizeof(V) * n);
+      if (!*vs[k]) return bail(ctx->fail(VFLIP_ERR_NOMEM, "cudaMalloc failed for %s", names[k]));
+    }
+    b.it = (int*)c->buf("bat_it", sizeof(int));
+    if (!b.it) return bail(ctx->fail(VFLIP_ERR_NOMEM, "cudaMalloc failed for bat_it"));
+  }
+  if (cudaStreamSynchronize(cs) != cudaSuccess) return bail(ctx->fail(VFLIP_ERR_CUDA, "set-up failed"));
+  // the graph
+  if (cudaGraphCreate(&graph, 0) != cudaSuccess) return bail(ctx->fail(VFLIP_ERR_CUDA, "cudaGraphCreate"));
+  auto capture_end = [&](cudaGraph_t g) -> int {
+    cudaGraph_t out = nullptr;
+    cudaError_t e = cudaStreamEndCapture(cs, &out);
+    if (e != cudaSuccess || out != g) return ctx->fail(VFLIP_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
+    return VFLIP_OK;
+  };
+  for (int i = 0; i < nsys; ++i) {
+    BatchItem<S0, SC, V>& b = items[i];
+    vflip_ctx* c = b.sub;
+    const vflip_system& y = sys[i];
+    const size_t n = (size_t)y.ni * y.nj * y.nk;
+    const int gb = grid_for(n, kRedBlock, c->num_sms);
+    if (cudaGraphConditionalHandleCreate(&b.h, graph, 0, 0) != cudaSuccess)
+      return bail(ctx->fail(VFLIP_ERR_CUDA, "cudaGraphConditionalHandleCreate"));
+    // init branch
+    if (cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+      return bail(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamBeginCaptureToGraph"));
+    cudaMemsetAsync(c->st, 0, sizeof(PcgScalars), cs);
+    cudaMemsetAsync(b.s, 0, n * sizeof(V), cs);
+    pcg_init_kernel<V, kRedBlock><<<gb, kRedBlock, 0, cs>>>(y.rhs, b.r, b.x, n, c->partials, c->st, tol);
+    pcg_loop_init_kernel<<<1, 32, 0, cs>>>(c->st, b.it, b.h);
+    cudaStreamCaptureStatus cst;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    if (cudaStreamGetCaptureInfo(cs, &cst, nullptr, nullptr, &deps, &ndeps) != cudaSuccess) {
+      cudaStreamEndCapture(cs, &graph);
+      return bail(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamGetCaptureInfo"));
+    }
+    std::vector<cudaGraphNode_t> dv(deps, deps + ndeps);
+    if ((rc = capture_end(graph))) return bail(rc);
+    // the loop
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = b.h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wn;
+    if (cudaGraphAddNode(&wn, graph, dv.data(), dv.size(), &cp) != cudaSuccess)
+      return bail(ctx->fail(VFLIP_ERR_CUDA, "cannot add the while node"));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+      return bail(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamBeginCaptureToGraph (body)"));
+    const Dims d = b.T.fine.d;
+    dim3 sblk(kRedBlock);
+    const int kz = 8;
+    dim3 sgrid((d.ni + 31) / 32, (d.nj + kRedBlock / 32 - 1) / (kRedBlock / 32), (d.nk + kz - 1) / kz);
+    int brc = vcycle<S0, SC, V>(c, b.T, b.r, b.z, true);
+    pcg_direction_kernel<V><<<grid_for(n, 256, c->num_sms), 256, 0, cs>>>(b.z, b.s, n, c->st);
+    pcg_spmv_dot_kernel<V, true, kRedBlock><<<sgrid, sblk, 0, cs>>>(b.s, nullptr, b.sd, b.q, b.T.fine.diag,
+                                                                    b.T.fine.xp, b.T.fine.yp, b.T.fine.zp, d.ni,
+                                                                    d.nj, d.nk, kz, c->partials, c->st);
+    pcg_update_kernel<V, kRedBlock><<<gb, kRedBlock, 0, cs>>>(b.x, b.r, b.s, b.q, n, c->partials, c->st);
+    pcg_loop_cond_kernel<<<1, 32, 0, cs>>>(c->st, b.it, maxit, b.h);
+    if ((rc = capture_end(body))) return bail(rc);
+    if (brc) {
+      ctx->err = c->err;
+      return bail(brc);
+    }
+    if ((size_t)sgrid.x * sgrid.y * sgrid.z > (size_t)kMaxPartials)
+      return bail(ctx->fail(VFLIP_ERR_ARG, "grid too large"));
+    // result
+    if (cudaStreamBeginCaptureToGraph(cs, graph, &wn, nullptr, 1, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+      return bail(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamBeginCaptureToGraph (result)"));
+    to_double_kernel<V, kRedBlock><<<gb, kRedBlock, 0, cs>>>(b.x, y.result, n);
+    if ((rc = capture_end(graph))) return bail(rc);
+  }
+  if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+    return bail(ctx->fail(VFLIP_ERR_CUDA, "cudaGraphInstantiate failed"));
+  VF_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  if (cudaGraphLaunch(exec, ctx->stream) != cudaSuccess) return bail(ctx->fail(VFLIP_ERR_CUDA, "cudaGraphLaunch"));
+  VF_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  if (cudaEventSynchronize(ctx->ev1) != cudaSuccess) return bail(ctx->fail(VFLIP_ERR_CUDA, "batched graph failed"));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  ctx->last_ms = ms;
+  ctx->launches += 1;
+  int status = VFLIP_OK;
+  for (int i = 0; i < nsys; ++i) {
+    BatchItem<S0, SC, V>& b = items[i];
+    vflip_ctx* c = b.sub;
+    PcgScalars h;
+    int iters = 0, kerr = 0;
+    if (cudaMemcpy(&h, c->st, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(&iters, b.it, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(&kerr, c->d_error, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return bail(ctx->fail(VFLIP_ERR_CUDA, "reading the batched results failed"));
+    if (kerr) {
+      cudaMemset(c->d_error, 0, sizeof(int));
+      return bail(ctx->fail(VFLIP_ERR_CUDA, "smoother copy pipeline timed out (system %d)", i));
+    }
+    const bool conv = h.converged != 0;
+    if (!conv) status = VFLIP_NOT_CONVERGED;
+    if (stats) {
+      stats[i].iterations = iters;
+      stats[i].vcycles = iters;
+      stats[i].levels = (int)b.T.coarse.size() + 1;
+      stats[i].converged = conv ? 1 : 0;
+      stats[i].residual = h.res;
+      stats[i].rhs_norm = tol > 0.0 ? h.tol / tol : 0.0;
+      stats[i].solve_ms = ms;
+    }
+  }
+  cleanup();
+  return status;
+}
+
 }  // namespace
 
 // ============================================================== C ABI
@@ -1184,6 +1366,7 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
 int vflip_destroy(vflip_ctx* ctx) {
   if (!ctx) return VFLIP_ERR_ARG;
   cudaStreamSynchronize(ctx->stream);
+  for (vflip_ctx* sub : ctx->subs) vflip_destroy(sub);
   for (auto& kv : ctx->bufs) cudaFree(kv.second.first);
   if (ctx->st) cudaFree(ctx->st);
   if (ctx->partials) cudaFree(ctx->partials);
@@ -1485,6 +1668,75 @@ int vflip_project(vflip_ctx* ctx, int ni, int nj, int nk, float h, float U_in, c
                   vflip_solve_stats* stats) {
   return project_impl(ctx, 0, ni, nj, nk, h, 1.0f, U_in, nodal_phi, bdesc, us, vs, ws, u, v, w, pressure,
                       tolerance_factor, max_iterations, stats);
+}
+
+int vflip_batched_solve(vflip_ctx* ctx, int nsys, const vflip_system* systems, double tolerance_factor,
+                        int max_iterations, int mode, vflip_solve_stats* stats) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  if (nsys < 0 || (nsys > 0 && !systems)) return ctx->fail(VFLIP_ERR_ARG, "bad system list");
+  if (max_iterations < 1) return ctx->fail(VFLIP_ERR_ARG, "max_iterations < 1");
+  int rc;
+  for (int i = 0; i < nsys; ++i) {
+    const vflip_system& y = systems[i];
+    if ((rc = check_dims(ctx, y.ni, y.nj, y.nk))) return rc;
+    if (!y.diag || !y.xp || !y.yp || !y.zp || !y.rhs || !y.result)
+      return ctx->fail(VFLIP_ERR_ARG, "null pointer in system %d", i);
+  }
+  if (nsys == 0) return VFLIP_OK;
+  if (mode == VFLIP_BATCH_LOOP) {
+    int status = VFLIP_OK;
+    cudaEvent_t a, b;
+    VF_CUDA(cudaEventCreate(&a));
+    VF_CUDA(cudaEventCreate(&b));
+    cudaEventRecord(a, ctx->stream);
+    for (int i = 0; i < nsys; ++i) {
+      const vflip_system& y = systems[i];
+      rc = solve_stencil(ctx, y.ni, y.nj, y.nk, y.diag, y.xp, y.yp, y.zp, y.rhs, y.result, tolerance_factor,
+                         max_iterations, stats ? &stats[i] : nullptr);
+      if (rc < 0) {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        return rc;
+      }
+      if (rc) status = rc;
+    }
+    cudaEventRecord(b, ctx->stream);
+    cudaEventSynchronize(b);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    ctx->last_ms = ms;
+    if (stats)
+      for (int i = 0; i < nsys; ++i) stats[i].solve_ms = ms;
+    return status;
+  }
+  if (mode != VFLIP_BATCH_GRAPH) return ctx->fail(VFLIP_ERR_ARG, "unknown batch mode %d", mode);
+  cudaEvent_t a;
+  VF_CUDA(cudaEventCreate(&a));
+  cudaEventRecord(a, ctx->stream);
+  switch (ctx->cfg.precision) {
+    case VFLIP_PREC_FP64:
+      rc = batched_graph<double, double, double>(ctx, nsys, systems, tolerance_factor, max_iterations, stats, "f64");
+      break;
+    case VFLIP_PREC_FP32:
+      rc = batched_graph<float, float, float>(ctx, nsys, systems, tolerance_factor, max_iterations, stats, "f32");
+      break;
+    default:
+      rc = batched_graph<float, __nv_bfloat16, float>(ctx, nsys, systems, tolerance_factor, max_iterations, stats,
+                                                      "mix");
+      break;
+  }
+  if (rc >= 0) {
+    // the whole call, set-up included, like the loop's timing
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, ctx->ev1);
+    ctx->last_ms = ms;
+    if (stats)
+      for (int i = 0; i < nsys; ++i) stats[i].solve_ms = ms;
+  }
+  cudaEventDestroy(a);
+  return rc;
 }
 
 int vflip_learned_grid(int ni, int nj, int nk, int level, int* X, int* Y, int* Z) {

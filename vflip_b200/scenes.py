@@ -135,3 +135,48 @@ def jittered_particles(ni, nj, nk, h, ppc, rng, centre=None, radius=None):
     base = np.repeat(cells, ppc, axis=0) * h
     p["pos"] = (base + rng.uniform(-0.49, 0.49, (n, 3)) * h).astype(np.float32)
     return p
+
+
+BATCH_SIDES = (32, 48, 64, 96, 128, 160, 192)
+
+
+def batch_system(solver, side, seed, device=None):
+    """One system of the batched uneven-Poisson workload: a side^3 box, 1-6
+    random solid spheres of radius 0.05-0.25 side (nodal level set), and the
+    rhs of the projection of an FP32 Gaussian velocity (sigma 1) smoothed by
+    3 Jacobi sweeps (7-point averaging), assembled by the library's own
+    projection assembly.  Returns (stencil[4, n, n, n], rhs[n, n, n]) on the
+    device.  The random fields are generated on the GPU (torch, seeded)."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    n = int(side)
+    h = np.float32(1.0 / n)
+    dev = solver.device if device is None else device
+    phi = np.full((n + 1, n + 1, n + 1), 1.0, np.float32)
+    for _ in range(int(rng.integers(1, 7))):
+        c = rng.uniform(0.15, 0.85, 3)
+        r = rng.uniform(0.05, 0.25)
+        phi = np.minimum(phi, sphere_phi(n, n, n, h, c, r))
+    g = torch.Generator(device=dev).manual_seed(int(seed))
+
+    def smooth(a):
+        for _ in range(3):
+            p = torch.nn.functional.pad(a[None, None], (1, 1, 1, 1, 1, 1), mode="replicate")[0, 0]
+            a = (p[1:-1, 1:-1, 1:-1] + p[:-2, 1:-1, 1:-1] + p[2:, 1:-1, 1:-1] + p[1:-1, :-2, 1:-1] +
+                 p[1:-1, 2:, 1:-1] + p[1:-1, 1:-1, :-2] + p[1:-1, 1:-1, 2:]) / 7.0
+        return a.contiguous()
+
+    su, sv, sw = face_shapes(n, n, n)
+    u, v, w = (smooth(torch.randn(s, generator=g, device=dev, dtype=torch.float32)) for s in (su, sv, sw))
+    zeros = [torch.zeros(s, dtype=torch.float32, device=dev) for s in (su, sv, sw)]
+    bdesc = torch.zeros((n, n, n), dtype=torch.int8, device=dev)
+    st, rhs = solver.assemble(n, n, n, float(h), 0.0, torch.from_numpy(phi).to(dev), bdesc, *zeros, u, v, w)
+    return st, rhs
+
+
+def batch_workload(solver, count=32, seed=0, sides=BATCH_SIDES):
+    """`count` systems with sides drawn uniformly from `sides` (seeded)."""
+    rng = np.random.default_rng(seed)
+    picks = rng.choice(np.asarray(sides), size=count)
+    return [batch_system(solver, int(s), seed * 1000 + i) for i, s in enumerate(picks)], [int(s) for s in picks]

@@ -16,7 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from ._lib import ConfigC, LearnedStatsC, SolveStatsC, VflipError, load
+from ._lib import ConfigC, LearnedStatsC, SolveStatsC, SystemC, VflipError, load
 from .particles import PARTICLE_BYTES
 
 
@@ -217,6 +217,25 @@ class Solver:
                                    int(max_iterations), C.byref(st))
         self._check(rc)
         return rc == 0, pressure, SolveStats.from_c(st)
+
+    def batched_solve(self, systems, tolerance_factor=1e-6, max_iterations=50, mode=0):
+        """vflip_batched_solve over [(stencil[4, nk, nj, ni] float64, rhs[nk, nj, ni] float64), ...]
+        (device tensors).  mode 0: one CUDA graph with device-side loops;
+        1: one system after another.  Returns (all_converged, [pressure], [SolveStats])."""
+        n = len(systems)
+        arr = (SystemC * max(n, 1))()
+        results = []
+        for i, (st, rhs) in enumerate(systems):
+            nk, nj, ni = rhs.shape
+            res = self._empty((nk, nj, ni), torch.float64)
+            results.append(res)
+            arr[i] = SystemC(ni, nj, nk, _p(st[0]).value, _p(st[1]).value, _p(st[2]).value, _p(st[3]).value,
+                             _p(rhs).value, _p(res).value)
+        stats = (SolveStatsC * max(n, 1))()
+        rc = self.lib.vflip_batched_solve(self.ctx, n, arr, float(tolerance_factor), int(max_iterations), int(mode),
+                                          stats)
+        self._check(rc)
+        return rc == 0, results, [SolveStats.from_c(stats[i]) for i in range(n)]
 
     def learned_grid(self, ni, nj, nk, level):
         X, Y, Z = C.c_int(), C.c_int(), C.c_int()
