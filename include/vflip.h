@@ -396,7 +396,8 @@ typedef struct vflip_system {
  * system a parallel branch whose PCG iterations run in a conditional while
  * node whose condition a kernel sets from the device-side scalars, so no
  * iteration returns to the host.  Returns 0 when every system converged, 1
- * otherwise; stats[i] per system (solve_ms = the whole call).  No reference
+ * otherwise; stats[i] per system (solve_ms = the whole call, set-up
+ * included; vflip_last_ms = the graph launch alone in graph mode).  No reference
  * counterpart (the reference solves one system per AMGPCGSolve call,
  * SS/AlgebraicMultigrid.h:189-301). */
 int vflip_batched_solve(vflip_ctx* ctx, int nsys, const vflip_system* systems, double tolerance_factor,
