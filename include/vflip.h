@@ -66,7 +66,9 @@ typedef struct {
   void* stream;              /* cudaStream_t to order work on; NULL: the CUDA default stream */
   int sweep_kernel;          /* smoother kernel: 0 = TMA-pipelined (bulk plane copies) for FP32 levels whose
                                 row length is a multiple of 4, else the plain fused kernel; 1 = always the
-                                plain fused kernel */
+                                plain fused kernel; 2 = 3-D-tiled (TMA tensor boxes, several CTAs per SM)
+                                for FP32 levels whose row length is a multiple of 4 (8 for BF16 operators),
+                                else as 0 */
   /* Tile shape of the TMA-pipelined smoother, 0 = automatic (tuning knobs;
    * vflip_b200/tune.py searches them): copy groups in flight (1..3), output
    * rows per tile, plane ranges per launch, resident CTAs per SM (1..2). */

@@ -26,6 +26,8 @@
 #include "projection_kernels.cuh"
 #include "transfer_kernels.cuh"
 #include "learned_kernels.cuh"
+#include "smoother3d.cuh"
+#include "tmap.h"
 #include "unet_net.h"
 
 using namespace vflip;
@@ -58,6 +60,7 @@ struct vflip_ctx {
   int num_sms = 148;
   unsigned long long launches = 0;  // kernels launched through this context
   std::vector<vflip_ctx*> subs;     // per-system contexts of batched solves
+  std::unordered_map<std::string, CUtensorMap> tmaps;  // encoded TMA tensor maps by (address, shape)
   // fine-level sweep timing (vflip_set_profiling)
   bool profiling = false;
   size_t prof_fine_n = 0;
@@ -337,6 +340,109 @@ int sweep_tma(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V
   return ctx->fail(VFLIP_ERR_ARG, "sweep: prolongation needs an incoming x");
 }
 
+// Cached 3-D tensor map of a dense grid array (the address and shape fully
+// determine a map, so a reused address stays valid).
+const CUtensorMap* grid_map(vflip_ctx* ctx, const void* p, int es, int nx, int ny, int nz, int bx, int by) {
+  char key[160];
+  snprintf(key, sizeof key, "%p/%d/%d/%d/%d/%d/%d", p, es, nx, ny, nz, bx, by);
+  auto it = ctx->tmaps.find(key);
+  if (it != ctx->tmaps.end()) return &it->second;
+  if (ctx->tmaps.size() > 4096) ctx->tmaps.clear();
+  CUtensorMap m;
+  if (!encode_grid_map(&m, p, es, nx, ny, nz, bx, by)) return nullptr;
+  return &(ctx->tmaps[key] = m);
+}
+
+template <typename S, bool Z, bool P, bool D>
+int launch_t3d_t(vflip_ctx* ctx, const T3dMaps<S>& mp, const T3dArgs& a, dim3 grid, size_t smem) {
+  auto kern = rbgs_sweep_t3d_kernel<S, Z, P, D, kT3dTX, kT3dTY, kT3dBlock>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemMax);
+    attr_set = true;
+  }
+  const bool timed = ctx->profiling && (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n;
+  if (timed) {
+    if (ctx->prof_used == ctx->prof_events.size()) {
+      cudaEvent_t e0, e1;
+      VF_CUDA(cudaEventCreate(&e0));
+      VF_CUDA(cudaEventCreate(&e1));
+      ctx->prof_events.push_back({e0, e1});
+    }
+    VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].first, ctx->stream));
+  }
+  kern<<<grid, kT3dBlock, smem, ctx->stream>>>(mp, a);
+  VF_LAUNCH_CHECK();
+  if (timed) {
+    VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].second, ctx->stream));
+    ++ctx->prof_used;
+  }
+  return VFLIP_OK;
+}
+
+// 3-D-tiled sweep (sweep_kernel == 2) when the level's rows meet the TMA
+// stride and alignment rules; *used says whether it ran.
+template <typename S, typename V>
+int sweep_t3d(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_out, const V* xc,
+              const Dims* cd, double* dot_partial, int* nblocks_out, bool* used) {
+  *used = false;
+  if (ctx->cfg.sweep_kernel != 2 || !std::is_same<V, float>::value || std::is_same<S, double>::value)
+    return VFLIP_OK;
+  const bool pro = xc != nullptr, zero = x_in == nullptr, dot = dot_partial != nullptr;
+  const int ni = L.d.ni, nj = L.d.nj, nk = L.d.nk;
+  if (ni % 4 || (sizeof(S) == 2 && ni % 8) || (pro && (!cd || cd->ni % 4))) return VFLIP_OK;
+  if (zero && pro) return VFLIP_OK;
+  const int D = ctx->cfg.smoother_depth > 0 ? std::min(ctx->cfg.smoother_depth, kT3dMaxDepth) : 2;
+  const size_t smem = t3d_smem_bytes<S, kT3dTX, kT3dTY>(D, pro);
+  if (smem > kTmaSmemMax) return VFLIP_OK;
+  const int ntx = (ni + kT3dTX - 1) / kT3dTX, nty = (nj + kT3dTY - 1) / kT3dTY, tiles = ntx * nty;
+  const int per_sm = std::max(1, std::min(4, (int)((228 * 1024) / (smem + 2048))));
+  int zr = ctx->cfg.smoother_plane_ranges > 0 ? ctx->cfg.smoother_plane_ranges
+                                              : std::max(1, (ctx->num_sms * per_sm) / tiles);
+  zr = std::max(1, std::min(zr, nk));
+  const int zlen = (nk + zr - 1) / zr;
+  zr = (nk + zlen - 1) / zlen;
+  if ((size_t)tiles * zr > (size_t)kMaxPartials) return VFLIP_OK;
+  using G = T3dGeom<S, kT3dTX, kT3dTY>;
+  T3dMaps<S> mp;
+  const CUtensorMap *mx = grid_map(ctx, zero ? (const void*)b : (const void*)x_in, 4, ni, nj, nk, G::WX, G::H),
+                    *mb = grid_map(ctx, b, 4, ni, nj, nk, G::WX, G::H),
+                    *md = grid_map(ctx, L.diag, sizeof(S), ni, nj, nk, G::WC, G::H),
+                    *mxp = grid_map(ctx, L.xp, sizeof(S), ni, nj, nk, G::WC, G::H),
+                    *myp = grid_map(ctx, L.yp, sizeof(S), ni, nj, nk, G::WC, G::H),
+                    *mzp = grid_map(ctx, L.zp, sizeof(S), ni, nj, nk, G::WC, G::H);
+  const CUtensorMap* mxc = pro ? grid_map(ctx, xc, 4, cd->ni, cd->nj, cd->nk, G::WXC, G::HCR) : mx;
+  if (!mx || !mb || !md || !mxp || !myp || !mzp || !mxc) return VFLIP_OK;
+  mp.x = *mx;
+  mp.b = *mb;
+  mp.d = *md;
+  mp.xp = *mxp;
+  mp.yp = *myp;
+  mp.zp = *mzp;
+  mp.xc = *mxc;
+  T3dArgs a;
+  a.x_out = (float*)x_out;
+  a.ni = ni;
+  a.nj = nj;
+  a.nk = nk;
+  a.cni = cd ? cd->ni : 0;
+  a.cnj = cd ? cd->nj : 0;
+  a.ntx = ntx;
+  a.zlen = zlen;
+  a.depth = D;
+  a.dot_partial = dot_partial;
+  a.error = ctx->d_error;
+  if (nblocks_out) *nblocks_out = tiles * zr;
+  *used = true;
+  const dim3 grid(tiles, zr);
+  if (zero && !dot) return launch_t3d_t<S, true, false, false>(ctx, mp, a, grid, smem);
+  if (zero && dot) return launch_t3d_t<S, true, false, true>(ctx, mp, a, grid, smem);
+  if (pro && !dot) return launch_t3d_t<S, false, true, false>(ctx, mp, a, grid, smem);
+  if (pro && dot) return launch_t3d_t<S, false, true, true>(ctx, mp, a, grid, smem);
+  if (!dot) return launch_t3d_t<S, false, false, false>(ctx, mp, a, grid, smem);
+  return launch_t3d_t<S, false, false, true>(ctx, mp, a, grid, smem);
+}
+
 // One sweep x_in -> x_out on a level; x_in == nullptr means x = 0.
 template <typename S, typename V>
 int sweep(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_out, const V* xc, const Dims* cd,
@@ -344,7 +450,9 @@ int sweep(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_
   using A = typename Num<V>::Acc;
   {
     bool used = false;
-    int rc = sweep_tma<S, V>(ctx, L, b, x_in, x_out, xc, cd, dot_partial, nblocks_out, &used);
+    int rc = sweep_t3d<S, V>(ctx, L, b, x_in, x_out, xc, cd, dot_partial, nblocks_out, &used);
+    if (rc || used) return rc;
+    rc = sweep_tma<S, V>(ctx, L, b, x_in, x_out, xc, cd, dot_partial, nblocks_out, &used);
     if (rc || used) return rc;
   }
   SweepShape sh = sweep_shape<A>(L.d, ctx->num_sms);
@@ -1343,7 +1451,7 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
   };
   if (ctx->cfg.pre_sweeps < 0 || ctx->cfg.post_sweeps < 0 || ctx->cfg.coarse_sweeps < 0 ||
       ctx->cfg.coarsest_max_unknowns < 1 || ctx->cfg.coarsest_max_unknowns > 4096 || ctx->cfg.precision < 0 ||
-      ctx->cfg.precision > 2 || ctx->cfg.sweep_kernel < 0 || ctx->cfg.sweep_kernel > 1 ||
+      ctx->cfg.precision > 2 || ctx->cfg.sweep_kernel < 0 || ctx->cfg.sweep_kernel > 2 ||
       ctx->cfg.smoother_depth < 0 || ctx->cfg.smoother_tile_rows < 0 || ctx->cfg.smoother_plane_ranges < 0 ||
       ctx->cfg.smoother_ctas_per_sm < 0)
     return bad(VFLIP_ERR_ARG);

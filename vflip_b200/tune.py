@@ -1,10 +1,11 @@
-"""Autotuner for the TMA-pipelined smoother's tile shape.
+"""Autotuner for the smoother kernel and its tile shape.
 
     python -m vflip_b200.tune [--n 256] [--out vflip_b200/tuning.json]
 
 For one grid size it times plain-FP32 MGPCG solves of the plume operator
-(box walls + sphere obstacle) under each candidate shape - copy groups in
-flight, output rows per tile, plane ranges per launch, resident CTAs per SM -
+(box walls + sphere obstacle) under each candidate - smoother kernel
+(0 full-row TMA, 2 3-D-tiled TMA), copy groups in flight, output rows per
+tile (full-row kernel), plane ranges per launch, resident CTAs per SM -
 reading the fine-level smoother's launch times from the library's own CUDA
 events (vflip_set_profiling), and records the fastest shape per grid size in
 a JSON cache that vflip_b200.plume.PlumeSim and bench.py pass to the solver.
@@ -22,11 +23,10 @@ from .solver import Solver
 HERE = os.path.dirname(os.path.abspath(__file__))
 CACHE = os.path.join(HERE, "tuning.json")
 
-# (depth, tile rows, plane ranges, CTAs per SM); 0 = the library's choice
+# (kernel, depth, tile rows, plane ranges, CTAs per SM); 0 = the library's choice
 CANDIDATES = [
-    (1, 0, 0, 1), (2, 0, 0, 1), (3, 0, 0, 1),
-    (2, 5, 3, 1), (2, 6, 3, 1), (3, 4, 4, 1), (2, 4, 4, 1),
-    (1, 2, 2, 2), (2, 2, 2, 2), (1, 3, 3, 2), (2, 1, 2, 2), (1, 2, 0, 2),
+    (0, 1, 0, 0, 1), (0, 2, 0, 0, 1), (0, 2, 5, 3, 1), (0, 1, 2, 0, 2),
+    (2, 1, 0, 0, 0), (2, 2, 0, 0, 0), (2, 3, 0, 0, 0), (2, 2, 0, 1, 0), (2, 2, 0, 4, 0), (2, 3, 0, 4, 0),
 ]
 
 
@@ -42,8 +42,10 @@ def tuned_kwargs(n):
     entry = load_cache().get(str(n))
     if not entry:
         return {}
-    d, t, r, c = entry["shape"]
-    return dict(smoother_depth=d, smoother_tile_rows=t, smoother_plane_ranges=r, smoother_ctas_per_sm=c)
+    shape = entry["shape"]
+    k, d, t, r, c = shape if len(shape) == 5 else [0] + list(shape)
+    return dict(sweep_kernel=k, smoother_depth=d, smoother_tile_rows=t, smoother_plane_ranges=r,
+                smoother_ctas_per_sm=c)
 
 
 def problem(n, dev):
@@ -59,10 +61,10 @@ def problem(n, dev):
     return st, rhs
 
 
-def measure(st, rhs, shape, reps=2):
-    d, t, r, c = shape
-    with Solver(precision=1, smoother_depth=d, smoother_tile_rows=t, smoother_plane_ranges=r,
-                smoother_ctas_per_sm=c) as s:
+def measure(st, rhs, shape, reps=2, precision=1):
+    k, d, t, r, c = shape
+    with Solver(precision=precision, sweep_kernel=k, smoother_depth=d, smoother_tile_rows=t,
+                smoother_plane_ranges=r, smoother_ctas_per_sm=c) as s:
         s.amgpcg_solve(st, rhs, 1e-6, 50)  # warm (allocations)
         s.set_profiling(True)
         s.profile_sweeps()
@@ -83,10 +85,11 @@ def main():
     ap.add_argument("--solve-once", action="store_true",
                     help="assemble the operator and run one FP32 solve (a small target for profilers)")
     ap.add_argument("--precision", type=int, default=1)
+    ap.add_argument("--sweep-kernel", type=int, default=0, help="smoother kernel of --solve-once")
     a = ap.parse_args()
     st, rhs = problem(a.n, "cuda:0")
     if a.solve_once:
-        with Solver(precision=a.precision) as s:
+        with Solver(precision=a.precision, sweep_kernel=a.sweep_kernel) as s:
             ok, _, stats = s.amgpcg_solve(st, rhs, 1e-6, 50)
         print(json.dumps({"n": a.n, "converged": ok, "iterations": stats.iterations, "solve_ms": stats.solve_ms}))
         return
