@@ -306,6 +306,45 @@ __host__ __device__ inline TmaLayout tma_layout(int ni, int tyo, int depth, int 
 }
 
 
+// Four consecutive elements of a shared-memory row as floats (16-byte
+// aligned FP32 or 8-byte aligned BF16).
+__device__ __forceinline__ float4 ld4f(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ float4 ld4f(const __nv_bfloat16* p) {
+  const uint2 u = *reinterpret_cast<const uint2*>(p);
+  const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&u.x), b = *reinterpret_cast<const __nv_bfloat162*>(&u.y);
+  const float2 fa = __bfloat1622float2(a), fb = __bfloat1622float2(b);
+  return make_float4(fa.x, fa.y, fb.x, fb.y);
+}
+// (the FP64 instantiation of the pipelined kernel is compiled but never launched)
+__device__ __forceinline__ float4 ld4f(const double* p) {
+  return make_float4((float)p[0], (float)p[1], (float)p[2], (float)p[3]);
+}
+template <int K>
+__device__ __forceinline__ float c4(const float4& v) {
+  return K == 0 ? v.x : K == 1 ? v.y : K == 2 ? v.z : v.w;
+}
+// Relaxation of cell K of a quad of four consecutive cells (i0 .. i0+3):
+// the reference's row sum in column order (-z, -y, -x, +x, +y, +z), then
+// (b - sum) / diag.  xl/xr are x at i0-1 / i0+4, cxl is +x coupling of i0-1.
+template <int K>
+__device__ __forceinline__ float relax_quad_cell(bool zlo, bool zhi, bool ylo, bool yhi, bool xlo, bool xhi,
+                                                 const float4& xc, const float4& xym, const float4& xyp,
+                                                 const float4& xzm, const float4& xzp, float xl, float xr,
+                                                 const float4& bb, const float4& dd, const float4& cx, float cxl,
+                                                 const float4& cyp, const float4& cym, const float4& czp,
+                                                 const float4& czm) {
+  constexpr int KL = K > 0 ? K - 1 : 0, KR = K < 3 ? K + 1 : 3;
+  float sum = 0.0f;
+  if (zlo) sum = sum + c4<K>(czm) * c4<K>(xzm);
+  if (ylo) sum = sum + c4<K>(cym) * c4<K>(xym);
+  if (xlo) sum = sum + (K == 0 ? cxl : c4<KL>(cx)) * (K == 0 ? xl : c4<KL>(xc));
+  if (xhi) sum = sum + c4<K>(cx) * (K == 3 ? xr : c4<KR>(xc));
+  if (yhi) sum = sum + c4<K>(cyp) * c4<K>(xyp);
+  if (zhi) sum = sum + c4<K>(czp) * c4<K>(xzp);
+  const float d = c4<K>(dd);
+  return (d != 0.0f) ? gs_div(c4<K>(bb) - sum, d) : 0.0f;
+}
+
 template <typename S, bool ZERO_X, bool PROLONG, bool DOT, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs<S> a) {
   extern __shared__ __align__(128) float sm[];
@@ -387,29 +426,46 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs<S> a
     return __syncthreads_and(ok) != 0;
   };
 
-  // relax colour `odd` of plane p on rows [r0, r1) (slot offsets given): the
-  // reference's row sum in column order (-z, -y, -x, +x, +y, +z), then
-  // (b - sum) / diag
+  // relax colour `odd` of plane p on rows [r0, r1) (slot offsets given).
+  // A thread takes quads of four consecutive cells (rows are multiples of 4
+  // long) and updates the quad's two cells of that colour from 16-byte
+  // loads; each cell's arithmetic is the reference's, in its order.
   auto relax = [&](int p, int r0, int r1, int odd, int x0, int xm1, int xp1, int cb, int cd, int cx, int cy, int cz,
                    int czm) {
     const bool zlo = p > 0, zhi = p < nk - 1;
+    const int Q = ni >> 2;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int j = r0 + ty; j < r1; j += by) {
-      const int sh = odd ? ((j + p + 1) & 1) : ((j + p) & 1);
+      const int sh = (j + p + odd) & 1;
       const int xr = (j - jr0) * ni, cr = (j - jred0) * ni, yr = (j - jy0) * ni;
       const bool ylo = j > 0, yhi = j < nj - 1;
-      for (int m = tx; m < P; m += bx) {
-        const int i = 2 * m + sh;
-        if (i >= ni) continue;
-        const int s = xr + i, c = cr + i, y = yr + i;
-        float sum = 0.0f;
-        if (zlo) sum = sum + float(ldv(cs + czm + c)) * sm[xm1 + s];
-        if (ylo) sum = sum + float(ldv(cs + cy + y - ni)) * sm[x0 + s - ni];
-        if (i > 0) sum = sum + float(ldv(cs + cx + c - 1)) * sm[x0 + s - 1];
-        if (i < ni - 1) sum = sum + float(ldv(cs + cx + c)) * sm[x0 + s + 1];
-        if (yhi) sum = sum + float(ldv(cs + cy + y)) * sm[x0 + s + ni];
-        if (zhi) sum = sum + float(ldv(cs + cz + c)) * sm[xp1 + s];
-        const float d = float(ldv(cs + cd + c));
-        sm[x0 + s] = (d != 0.0f) ? gs_div(sm[cb + c] - sum, d) : 0.0f;
+      for (int q = tx; q < Q; q += bx) {
+        const int i0 = 4 * q;
+        const int s = xr + i0, c = cr + i0, y = yr + i0;
+        const float4 xc = ld4f(sm + x0 + s);
+        const float4 xym = ylo ? ld4f(sm + x0 + s - ni) : z4, xyp = yhi ? ld4f(sm + x0 + s + ni) : z4;
+        const float4 xzm = zlo ? ld4f(sm + xm1 + s) : z4, xzp = zhi ? ld4f(sm + xp1 + s) : z4;
+        const float4 bb = ld4f(sm + cb + c), dd = ld4f(cs + cd + c), cxv = ld4f(cs + cx + c);
+        const float4 cyp = ld4f(cs + cy + y), cym = ylo ? ld4f(cs + cy + y - ni) : z4;
+        const float4 czp = ld4f(cs + cz + c), czmv = zlo ? ld4f(cs + czm + c) : z4;
+        if (sh == 0) {
+          const float xl = i0 > 0 ? sm[x0 + s - 1] : 0.0f;
+          const float cxl = i0 > 0 ? float(ldv(cs + cx + c - 1)) : 0.0f;
+          const float v0 = relax_quad_cell<0>(zlo, zhi, ylo, yhi, i0 > 0, i0 < ni - 1, xc, xym, xyp, xzm, xzp, xl,
+                                              0.0f, bb, dd, cxv, cxl, cyp, cym, czp, czmv);
+          const float v2 = relax_quad_cell<2>(zlo, zhi, ylo, yhi, true, i0 + 2 < ni - 1, xc, xym, xyp, xzm, xzp,
+                                              0.0f, 0.0f, bb, dd, cxv, 0.0f, cyp, cym, czp, czmv);
+          sm[x0 + s] = v0;
+          sm[x0 + s + 2] = v2;
+        } else {
+          const float xr4 = i0 + 4 < ni ? sm[x0 + s + 4] : 0.0f;
+          const float v1 = relax_quad_cell<1>(zlo, zhi, ylo, yhi, true, i0 + 1 < ni - 1, xc, xym, xyp, xzm, xzp,
+                                              0.0f, 0.0f, bb, dd, cxv, 0.0f, cyp, cym, czp, czmv);
+          const float v3 = relax_quad_cell<3>(zlo, zhi, ylo, yhi, true, i0 + 3 < ni - 1, xc, xym, xyp, xzm, xzp,
+                                              0.0f, xr4, bb, dd, cxv, 0.0f, cyp, cym, czp, czmv);
+          sm[x0 + s + 1] = v1;
+          sm[x0 + s + 3] = v3;
+        }
       }
     }
   };

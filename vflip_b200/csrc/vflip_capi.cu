@@ -263,9 +263,9 @@ bool tma_shape(const vflip_config& cfg, const Dims& d, const Dims* cd, bool prol
   o.depth = depth;
   o.crows_max = prolong ? (o.tyo + 7) / 2 : 0;
   o.smem = bytes(o.tyo);
-  int P = (d.ni + 1) / 2;
+  const int Q = (d.ni + 3) / 4;  // quads of four cells per row (one thread each)
   int bx = 1;
-  while (bx < P && bx < 128) bx <<= 1;
+  while (bx < Q && bx < 128) bx <<= 1;
   o.bx = bx;
   o.by = kTmaBlock / bx;
   return o.smem <= budget;
