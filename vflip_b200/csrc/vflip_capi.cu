@@ -227,7 +227,9 @@ bool tma_shape(const vflip_config& cfg, const Dims& d, const Dims* cd, bool prol
   if (d.ni % 4 != 0 || (d.ni * sizeof(S)) % 16 != 0) return false;
   if (prolong && (!cd || cd->ni % 4 != 0)) return false;
   const int cni = prolong ? cd->ni : 0;
-  const int depth = cfg.smoother_depth > 0 ? std::min(cfg.smoother_depth, kTmaMaxDepth) : 2;
+  // one copy group in flight measured fastest at 256^3 (vflip_b200/tune.py): deeper
+  // prefetch only shortens the tiles
+  const int depth = cfg.smoother_depth > 0 ? std::min(cfg.smoother_depth, kTmaMaxDepth) : 1;
   const int cps = cfg.smoother_ctas_per_sm > 0 ? std::min(cfg.smoother_ctas_per_sm, 2) : 1;
   const size_t budget = cps == 1 ? kTmaSmemMax : kTmaSmemMax / 2 - 1024;
   auto bytes = [&](int t) { return tma_layout<S>(d.ni, t, depth, prolong ? (t + 7) / 2 : 0, cni).bytes; };
