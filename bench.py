@@ -78,8 +78,8 @@ def measured_peaks():
 
 
 def profile_traffic(n):
-    """DRAM bytes per launch of the fine-level sweep from the committed ncu
-    summary committed under profiles/, scaled to n^3 cells."""
+    """DRAM bytes per launch of the fine-level sweep from the ncu summary
+    committed under profiles/, scaled to n^3 cells."""
     p = os.path.join(ROOT, "profiles", "rbgs_sweep_fp32_256.md")
     if not os.path.exists(p):
         return None
