@@ -430,10 +430,15 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs<S> a
   // A thread takes quads of four consecutive cells (rows are multiples of 4
   // long) and updates the quad's two cells of that colour from 16-byte
   // loads; each cell's arithmetic is the reference's, in its order.
+  // With `store` (the black pass of an output plane) each thread also writes
+  // its whole quad to x_out - two new black values and the two red values
+  // finished one step earlier - and adds the quad to the fused z.r.
+  double dot = 0.0;
   auto relax = [&](int p, int r0, int r1, int odd, int x0, int xm1, int xp1, int cb, int cd, int cx, int cy, int cz,
-                   int czm) {
+                   int czm, bool store) {
     const bool zlo = p > 0, zhi = p < nk - 1;
     const int Q = ni >> 2;
+    float* outp = a.x_out + (size_t)p * sz;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int j = r0 + ty; j < r1; j += by) {
       const int sh = (j + p + odd) & 1;
@@ -457,6 +462,11 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs<S> a
                                               0.0f, 0.0f, bb, dd, cxv, 0.0f, cyp, cym, czp, czmv);
           sm[x0 + s] = v0;
           sm[x0 + s + 2] = v2;
+          if (store) {
+            const float4 o = make_float4(v0, xc.y, v2, xc.w);
+            *reinterpret_cast<float4*>(outp + (size_t)j * sy + i0) = o;
+            if (DOT) dot += (double)o.x * bb.x + (double)o.y * bb.y + (double)o.z * bb.z + (double)o.w * bb.w;
+          }
         } else {
           const float xr4 = i0 + 4 < ni ? sm[x0 + s + 4] : 0.0f;
           const float v1 = relax_quad_cell<1>(zlo, zhi, ylo, yhi, true, i0 + 1 < ni - 1, xc, xym, xyp, xzm, xzp,
@@ -465,6 +475,11 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs<S> a
                                               0.0f, xr4, bb, dd, cxv, 0.0f, cyp, cym, czp, czmv);
           sm[x0 + s + 1] = v1;
           sm[x0 + s + 3] = v3;
+          if (store) {
+            const float4 o = make_float4(xc.x, v1, xc.z, v3);
+            *reinterpret_cast<float4*>(outp + (size_t)j * sy + i0) = o;
+            if (DOT) dot += (double)o.x * bb.x + (double)o.y * bb.y + (double)o.z * bb.z + (double)o.w * bb.w;
+          }
         }
       }
     }
@@ -486,7 +501,6 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs<S> a
   // carries x(q+1), coefficients (q), zp(q) and is group q - k0 + 2.  The
   // step for plane p waits for H(p) (and G0 first), then issues H(p+D), so
   // D groups stream in during its relaxation.
-  double dot = 0.0;
   bool failed = false;
   int issued = 1;
   if (tid == 0) issue(0, p0 - 1, wrap(px - 1, RX), p0, px, -1, 0, p0 - 1, wrap(pz - 1, RZ));
@@ -517,28 +531,14 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs<S> a
     }
     if (p >= 0 && p < nk)
       relax(p, jred0, jred1, 1, oX + px * xslot, oX + sxm1 * xslot, oX + sxp1 * xslot, oB + pc * cslot,
-            oD + pc * cslot, oXP + pc * cslot, oYP + pc * yslot, oZP + pz * cslot, oZP + szm1 * cslot);
+            oD + pc * cslot, oXP + pc * cslot, oYP + pc * yslot, oZP + pz * cslot, oZP + szm1 * cslot, false);
     __syncthreads();
+    // black pass of plane p-1 with the quads stored as they finish; the next
+    // step's wait barrier orders it before any slot it reads is refilled
     const int q = p - 1;
-    const bool out_plane = (q >= k0 && q < kend);
-    if (out_plane)
+    if (q >= k0 && q < kend)
       relax(q, j0, jout1, 0, oX + sxm1 * xslot, oX + sxm2 * xslot, oX + px * xslot, oB + scm1 * cslot,
-            oD + scm1 * cslot, oXP + scm1 * cslot, oYP + scm1 * yslot, oZP + szm1 * cslot, oZP + szm2 * cslot);
-    __syncthreads();
-    if (out_plane) {
-      const float4* s4 = reinterpret_cast<const float4*>(sm + oX + sxm1 * xslot + (j0 - jr0) * ni);
-      const float4* b4 = reinterpret_cast<const float4*>(sm + oB + scm1 * cslot + (j0 - jred0) * ni);
-      float4* dst = reinterpret_cast<float4*>(a.x_out + q * sz + j0 * sy);
-      const int cnt4 = (jout1 - j0) * ni / 4;
-      for (int e = tid; e < cnt4; e += BLOCK) {
-        float4 v = s4[e];
-        dst[e] = v;
-        if (DOT) {
-          float4 bb = b4[e];
-          dot += (double)v.x * bb.x + (double)v.y * bb.y + (double)v.z * bb.z + (double)v.w * bb.w;
-        }
-      }
-    }
+            oD + scm1 * cslot, oXP + scm1 * cslot, oYP + scm1 * yslot, oZP + szm1 * cslot, oZP + szm2 * cslot, true);
     px = wrap(px + 1, RX);
     pc = wrap(pc + 1, RC);
     pz = wrap(pz + 1, RZ);
