@@ -60,8 +60,11 @@ typedef struct {
   int precision;             /* vflip_precision, default VFLIP_PREC_FP32 */
   int pre_sweeps;            /* RBGS sweeps before restriction, default 4 (SS/AlgebraicMultigrid.h:156) */
   int post_sweeps;           /* RBGS sweeps after prolongation, default 4 (SS/AlgebraicMultigrid.h:164) */
-  int coarse_sweeps;         /* RBGS sweeps on the coarsest level, default 200 (SS/AlgebraicMultigrid.h:160) */
-  int coarsest_max_unknowns; /* coarsen while unknowns exceed this, default 4096 (SS/GeometricLevelGen.h:46); max 4096 */
+  int coarse_sweeps;         /* RBGS sweeps on the coarsest level; 0 (default) = automatic: 200 in FP64
+                                (SS/AlgebraicMultigrid.h:160), 100 in FP32/MIXED */
+  int coarsest_max_unknowns; /* coarsen while unknowns exceed this (max 4096); 0 (default) = automatic:
+                                4096 in FP64 (SS/GeometricLevelGen.h:46, the reference's hierarchy), 512 in
+                                FP32/MIXED (an 8^3 coarsest level those sweeps solve to convergence) */
   int device;                /* CUDA device ordinal, default 0 */
   void* stream;              /* cudaStream_t to order work on; NULL: the CUDA default stream */
   int sweep_kernel;          /* smoother kernel: 0 = TMA-pipelined (bulk plane copies) for FP32 levels whose

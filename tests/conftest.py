@@ -47,6 +47,9 @@ def problem_from_golden(g):
     return pr
 
 
+REF_HIERARCHY = dict(coarse_sweeps=200, coarsest_max_unknowns=4096)
+
+
 @pytest.fixture(scope="session")
 def gpu_solver():
     torch = pytest.importorskip("torch")
@@ -56,9 +59,11 @@ def gpu_solver():
     from vflip_b200.solver import Solver
 
     build.build()
-    s = {p: Solver(precision=p) for p in (0, 1, 2)}
-    s["f32_plain"] = Solver(precision=1, sweep_kernel=1)  # the non-pipelined smoother
-    s["mix_plain"] = Solver(precision=2, sweep_kernel=1)
+    # the reference's hierarchy (16^3 coarsest level, 200 sweeps) in every
+    # precision, so V-cycles compare with the oracle's
+    s = {p: Solver(precision=p, **REF_HIERARCHY) for p in (0, 1, 2)}
+    s["f32_plain"] = Solver(precision=1, sweep_kernel=1, **REF_HIERARCHY)  # the non-pipelined smoother
+    s["mix_plain"] = Solver(precision=2, sweep_kernel=1, **REF_HIERARCHY)
     yield s
     for v in s.values():
         v.close()

@@ -43,7 +43,8 @@ def test_config_defaults_are_the_reference_constants(lib):
     cfg = ConfigC()
     lib.vflip_config_default(C.byref(cfg))
     # AlgebraicMultigrid.h:156,160,164 and GeometricLevelGen.h:46
-    assert (cfg.pre_sweeps, cfg.post_sweeps, cfg.coarse_sweeps, cfg.coarsest_max_unknowns) == (4, 4, 200, 4096)
+    # 0 = automatic (the reference's 4096 / 200 in FP64, 512 / 100 in FP32 and MIXED)
+    assert (cfg.pre_sweeps, cfg.post_sweeps, cfg.coarse_sweeps, cfg.coarsest_max_unknowns) == (4, 4, 0, 0)
 
 
 def test_bad_arguments_fail_without_a_device(lib):

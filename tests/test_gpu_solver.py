@@ -9,7 +9,7 @@ tolerance: pressure within 1e-5 relative L2 of the reference solve.
 import numpy as np
 import pytest
 
-from conftest import golden, problem_from_golden
+from conftest import REF_HIERARCHY, golden, problem_from_golden
 from vflip_b200 import scenes
 
 torch = pytest.importorskip("torch")
@@ -111,7 +111,7 @@ def test_tma_smoother_shapes_match_plain_kernel(gpu_solver, orc, shape):
     st, b = four(out["stencil"]), t(out["rhs"])
     d, r, z, c = shape
     with Solver(precision=1, smoother_depth=d, smoother_tile_rows=r, smoother_plane_ranges=z,
-                smoother_ctas_per_sm=c) as s:
+                smoother_ctas_per_sm=c, **REF_HIERARCHY) as s:
         a = s.vcycle(st, b).cpu().numpy()
     ref = gpu_solver["f32_plain"].vcycle(st, b).cpu().numpy()
     assert np.array_equal(a, ref)
@@ -128,7 +128,7 @@ def test_tiled3d_smoother_matches_plain_kernel(gpu_solver, orc, dims, depth):
     _, out = system(orc, "gen", dims)
     st, b = four(out["stencil"]), t(out["rhs"])
     for prec, plain in ((1, "f32_plain"), (2, "mix_plain")):
-        with Solver(precision=prec, sweep_kernel=2, smoother_depth=depth) as s:
+        with Solver(precision=prec, sweep_kernel=2, smoother_depth=depth, **REF_HIERARCHY) as s:
             a = s.vcycle(st, b).cpu().numpy()
         ref = gpu_solver[plain].vcycle(st, b).cpu().numpy()
         assert np.array_equal(a, ref), prec
@@ -139,11 +139,28 @@ def test_tiled3d_smoother_pcg(gpu_solver, orc):
 
     _, out = system(orc, "gen", (64, 48, 40))
     st, b = four(out["stencil"]), t(out["rhs"])
-    with Solver(precision=1, sweep_kernel=2) as s:
+    with Solver(precision=1, sweep_kernel=2, **REF_HIERARCHY) as s:
         conv, p, stats = s.amgpcg_solve(st, b, 1e-6, 50)
     conv2, p2, stats2 = gpu_solver["f32_plain"].amgpcg_solve(st, b, 1e-6, 50)
     assert conv and conv2 and stats.iterations == stats2.iterations
     assert rel_l2(p.cpu().numpy(), p2.cpu().numpy()) < 1e-6
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+def test_automatic_hierarchy(gpu_solver, orc, prec):
+    """FP32/MIXED contexts coarsen to an 8^3 level by default: the solve
+    reaches the tolerance in no more iterations than with the reference's
+    hierarchy and agrees with the reference's pressure."""
+    from vflip_b200.solver import Solver
+
+    _, out = system(orc, "gen", (64, 48, 40))
+    st, b = out["stencil"], out["rhs"]
+    x, ok, res, it = orc.amgpcg(st, b)
+    with Solver(precision=prec) as s:
+        conv, p, stats = s.amgpcg_solve(four(st), t(b), 1e-6, 50)
+    assert conv and stats.residual <= 1e-6 * stats.rhs_norm
+    assert stats.levels > 3 and stats.iterations <= it
+    assert rel_l2(p.cpu().numpy(), x) < 1e-4
 
 
 def test_vcycle_golden(gpu_solver):

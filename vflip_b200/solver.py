@@ -65,7 +65,7 @@ def _face_shapes(ni, nj, nk):
 
 
 class Solver:
-    def __init__(self, precision=1, pre_sweeps=4, post_sweeps=4, coarse_sweeps=200, coarsest_max_unknowns=4096,
+    def __init__(self, precision=1, pre_sweeps=4, post_sweeps=4, coarse_sweeps=0, coarsest_max_unknowns=0,
                  device=0, stream=None, sweep_kernel=0, smoother_depth=0, smoother_tile_rows=0,
                  smoother_plane_ranges=0, smoother_ctas_per_sm=0):
         self.lib = load()
