@@ -79,6 +79,9 @@ def _load(path, prefix):
     getattr(lib, p + "_advect_rk2").argtypes = [_I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _P, _P]
     getattr(lib, p + "_hash").argtypes = [_I, _I, _I, _F, _P, _I, _P]
     getattr(lib, p + "_p2g").argtypes = [_I, _I, _I, _F, _P, _I, _I, _P, _P]
+    getattr(lib, p + "_advect_flip").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _F]
+    getattr(lib, p + "_reorder_flip").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, C.c_uint, _P, _I]
+    getattr(lib, p + "_reorder_flip").restype = _I
     if prefix == "oracle":
         getattr(lib, p + "_g2p").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _P, _P, _D]
         getattr(lib, p + "_delta").argtypes = [_I, _I, _I, _P, _P, _P]
@@ -274,6 +277,25 @@ class _Impl:
                 raise ValueError("the reference's particle_from_grid is pure FLIP")
             self.fn("g2p")(ni, nj, nk, h, _ptr(p), len(p), _ptr(du), _ptr(dv), _ptr(dw))
         return p
+
+    def advect_flip(self, ni, nj, nk, h, particles, u, v, w, nodal_phi, dt):
+        """SmokeSolver3D::advect_FLIP (RK3 + solid push-out) on a copy."""
+        p = np.array(particles, PARTICLE_DTYPE, copy=True)
+        u, v, w, phi = [np.ascontiguousarray(a, np.float32) for a in (u, v, w, nodal_phi)]
+        self.fn("advect_flip")(ni, nj, nk, h, _ptr(p), len(p), _ptr(u), _ptr(v), _ptr(w), _ptr(phi), float(dt))
+        return p
+
+    def reorder_flip(self, ni, nj, nk, h, particles, u, v, w, nodal_phi, seed=0):
+        """SmokeSolver3D::hash_FLIP + reorder_FLIP; returns the new particle array."""
+        p = np.ascontiguousarray(particles, PARTICLE_DTYPE)
+        u, v, w, phi = [np.ascontiguousarray(a, np.float32) for a in (u, v, w, nodal_phi)]
+        cap = 9 * ni * nj * nk + 16
+        out = np.zeros(cap, PARTICLE_DTYPE)
+        n = self.fn("reorder_flip")(ni, nj, nk, h, _ptr(p), len(p), _ptr(u), _ptr(v), _ptr(w), _ptr(phi), int(seed),
+                                    _ptr(out), cap)
+        if n < 0 or n > cap:
+            raise RuntimeError("reorder capacity")
+        return out[:n].copy()
 
     def smoke_step(self, n, h, dt, phi, state, source_centre=(0.5, 0.1, 0.5), source_radius=0.1, alpha=0.1,
                    beta=1.0):

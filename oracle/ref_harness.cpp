@@ -407,6 +407,45 @@ void ref_g2p(int ni, int nj, int nk, float h, void* particles, int np, const flo
   for (int q = 0; q < np; ++q) p[q] = s.FLIP[q];
 }
 
+// SmokeSolver3D::advect_FLIP (Smoke_solver3D.cpp:1407-1449) on the grid
+// velocity (u, v, w) and nodal solid phi.
+void ref_advect_flip(int ni, int nj, int nk, float h, void* particles, int np, const float* u, const float* v,
+                     const float* w, const float* nodal_phi, float dt) {
+  particle* p = (particle*)particles;
+  SmokeSolver3D s;
+  init_solver_grids(s, ni, nj, nk, h);
+  to_buffer(s._un, u);
+  to_buffer(s._vn, v);
+  to_buffer(s._wn, w);
+  to_buffer(s._nodal_solid_phi, nodal_phi);
+  s.FLIP.assign(p, p + np);
+  s.advect_FLIP(dt);
+  for (int q = 0; q < np; ++q) p[q] = s.FLIP[q];
+}
+
+// SmokeSolver3D::hash_FLIP then reorder_FLIP (Smoke_solver3D.cpp:1327-1396);
+// rand() is seeded with `seed`.  Returns the new particle count (particles
+// beyond `capacity` are not copied out).
+int ref_reorder_flip(int ni, int nj, int nk, float h, const void* particles, int np, const float* u,
+                     const float* v, const float* w, const float* nodal_phi, unsigned seed, void* out,
+                     int capacity) {
+  const particle* p = (const particle*)particles;
+  SmokeSolver3D s;
+  init_solver_grids(s, ni, nj, nk, h);
+  to_buffer(s._un, u);
+  to_buffer(s._vn, v);
+  to_buffer(s._wn, w);
+  to_buffer(s._nodal_solid_phi, nodal_phi);
+  s.FLIP.assign(p, p + np);
+  s.hash_FLIP();
+  srand(seed);
+  s.reorder_FLIP();
+  particle* o = (particle*)out;
+  const int n = (int)s.FLIP.size();
+  for (int q = 0; q < n && q < capacity; ++q) o[q] = s.FLIP[q];
+  return n;
+}
+
 // SmokeSolver3D::getDelta (Smoke_solver3D.cpp:1298-1319): delta = after - before
 // on one nx x ny x nz face grid.
 void ref_delta(int nx, int ny, int nz, const float* after, const float* before, float* delta) {

@@ -738,6 +738,135 @@ void oracle_g2p(int ni, int nj, int nk, float h, void* particles, int np, const 
   }
 }
 
+// SmokeSolver3D::traceRK3, SS/Smoke_solver3D.cpp:144-158, through
+// get_velocity (:71-87; the subdomain blend is inactive): c1 = 2/9 dt,
+// c2 = 3/9 dt computed in double and rounded to float, and - as the reference
+// writes it - c3 = (1 - c1 - c2) dt with c1, c2 already carrying dt.
+static void trace_rk3(const Grid* vel, const float pos[3], float dt, float out[3]) {
+  const float c1 = (float)(2.0 / 9.0 * (double)dt), c2 = (float)(3.0 / 9.0 * (double)dt);
+  const float c3 = (float)((1.0 - (double)c1 - (double)c2) * (double)dt);
+  auto sample = [&](const float x[3], float v[3]) {
+    for (int a = 0; a < 3; ++a) v[a] = vel[a].sample(x[0], x[1], x[2]);
+  };
+  float v1[3], v2[3], v3[3], m1[3], m2[3];
+  sample(pos, v1);
+  const float half = (float)(0.5 * (double)dt), q3 = (float)(0.75 * (double)dt);
+  for (int a = 0; a < 3; ++a) m1[a] = pos[a] + half * v1[a];
+  sample(m1, v2);
+  for (int a = 0; a < 3; ++a) m2[a] = pos[a] + q3 * v2[a];
+  sample(m2, v3);
+  for (int a = 0; a < 3; ++a) out[a] = pos[a] + c1 * v1[a] + c2 * v2[a] + c3 * v3[a];
+}
+
+// Buffer3D::sample_grad, SS/fluid_buffer3D.h:249-257, then normalize
+// (SS/vec.h:218-219 with mag = sqrt(mag2) + 1e-6, the square root taken in
+// double as the reference's build resolves it): the solid normal of
+// SmokeSolver3D::get_solid_normal, SS/Smoke_solver3D.cpp:115-124.
+static void solid_normal(const Grid& phi, const float pos[3], float n[3]) {
+  const double x = pos[0], y = pos[1], z = pos[2], h = phi.h;
+  const float r = phi.sample(x + h, y, z), l = phi.sample(x - h, y, z);
+  const float u = phi.sample(x, y + h, z), b = phi.sample(x, y - h, z);
+  const float f = phi.sample(x, y, z - h), k = phi.sample(x, y, z + h);
+  const float g[3] = {(float)((double)(r - l) / h), (float)((double)(u - b) / h), (float)((double)(k - f) / h)};
+  for (int a = 0; a < 3; ++a) n[a] = 0.5f * g[a];
+  float m2 = n[0] * n[0];
+  m2 += n[1] * n[1];
+  m2 += n[2] * n[2];
+  const float mag = (float)(std::sqrt((double)m2) + 1e-6);
+  for (int a = 0; a < 3; ++a) n[a] /= mag;
+}
+
+// SmokeSolver3D::advect_FLIP, SS/Smoke_solver3D.cpp:1407-1449: RK3 through
+// the grid velocity, then a particle that ends inside a solid (sampled nodal
+// phi < 0) moves out along the solid normal by -phi.
+void oracle_advect_flip(int ni, int nj, int nk, float h, void* particles, int np, const float* u, const float* v,
+                        const float* w, const float* nodal_phi, float dt) {
+  Particle* p = (Particle*)particles;
+  const Grid vel[3] = {{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0},
+                       {v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0},
+                       {w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5}};
+  const Grid phi = {nodal_phi, ni + 1, nj + 1, nk + 1, (double)h, 0.5, 0.5, 0.5};
+  for (int q = 0; q < np; ++q) {
+    float pos[3];
+    trace_rk3(vel, p[q].pos, dt, pos);
+    const float ph = phi.sample(pos[0], pos[1], pos[2]);
+    if (ph < 0) {
+      float n[3];
+      solid_normal(phi, pos, n);
+      for (int a = 0; a < 3; ++a) pos[a] -= ph * n[a];
+    }
+    for (int a = 0; a < 3; ++a) p[q].pos[a] = pos[a];
+  }
+}
+
+// Counter-based uniform in [-1, 1) for reseeding: a 32-bit integer mix of
+// (seed, cell, slot, axis) - the GPU kernel computes the same integers.
+// The reference draws frand(-1, 1) from rand() (SS/Smoke_solver3D.h:36-39),
+// the same distribution from a sequential generator no parallel code can
+// reproduce.
+static uint32_t mix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+static float reseed_uniform(uint32_t seed, uint32_t cell, uint32_t slot, uint32_t axis) {
+  const uint32_t r = mix32(mix32(mix32(seed ^ 0x9e3779b9u) + cell) + (slot * 3u + axis));
+  return -1.0f + 2.0f * ((float)(r >> 8) * (1.0f / 16777216.0f));
+}
+
+// SmokeSolver3D::reorder_FLIP, SS/Smoke_solver3D.cpp:1347-1396, after
+// hash_FLIP: cells in (k, j, i) order; a cell with fewer than 8 particles
+// keeps them and gains 8 - n new ones at (i, j, k) h + r 0.49 h (r uniform in
+// [-1, 1)^3, reseed_uniform) with the grid velocity there
+// (get_velocity_self, :89-97), density and temperature 0; 8 or 9 stay; 10 or
+// more keep their first 8.  Then particles with sampled solid phi < 0 are
+// dropped.  Returns the count written (or -needed when capacity is short).
+int oracle_reorder_flip(int ni, int nj, int nk, float h, const void* particles, int np, const float* u,
+                        const float* v, const float* w, const float* nodal_phi, unsigned seed, void* out,
+                        int capacity) {
+  const Particle* p = (const Particle*)particles;
+  Particle* o = (Particle*)out;
+  const size_t nc = (size_t)ni * nj * nk;
+  std::vector<std::vector<int>> bucket(nc);
+  for (int q = 0; q < np; ++q) {
+    const int c = hash_cell(p[q], ni, nj, nk, h);
+    if (c >= 0) bucket[(size_t)c].push_back(q);
+  }
+  const Grid vel[3] = {{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0},
+                       {v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0},
+                       {w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5}};
+  const Grid phi = {nodal_phi, ni + 1, nj + 1, nk + 1, (double)h, 0.5, 0.5, 0.5};
+  std::vector<Particle> all;
+  for (int k = 0; k < nk; ++k)
+    for (int j = 0; j < nj; ++j)
+      for (int i = 0; i < ni; ++i) {
+        const size_t c = lin(i, j, k, ni, nj);
+        const std::vector<int>& b = bucket[c];
+        const int cnt = (int)b.size();
+        const int keep = cnt < 10 ? cnt : 8;
+        for (int e = 0; e < keep; ++e) all.push_back(p[b[e]]);
+        for (int e = cnt; e < 8; ++e) {
+          Particle n = {};
+          const float base[3] = {(float)i * h, (float)j * h, (float)k * h};
+          for (int a = 0; a < 3; ++a)
+            n.pos[a] = base[a] + reseed_uniform(seed, (uint32_t)c, (uint32_t)e, (uint32_t)a) * 0.49f * h;
+          for (int a = 0; a < 3; ++a) n.vel[a] = vel[a].sample(n.pos[0], n.pos[1], n.pos[2]);
+          all.push_back(n);
+        }
+      }
+  int count = 0;
+  for (const Particle& q : all) {
+    if (phi.sample(q.pos[0], q.pos[1], q.pos[2]) >= 0) {
+      if (count < capacity) o[count] = q;
+      ++count;
+    }
+  }
+  return count <= capacity ? count : -count;
+}
+
 // SmokeSolver3D::getDelta, SS/Smoke_solver3D.cpp:1298-1319.
 void oracle_delta(int nx, int ny, int nz, const float* after, const float* before, float* delta) {
   size_t n = (size_t)nx * ny * nz;

@@ -178,3 +178,68 @@ def test_subdomain_projection_vs_reference(orc, ref, dims, dt):
     for k in ("u", "v", "w", "pressure", "rhs", "stencil"):
         same(a[k], b[k])
     assert b["ok"]
+
+
+def _flip_scene(ni, nj, nk, seed, n_particles=None, ppc=None):
+    from vflip_b200 import scenes
+
+    rng = np.random.default_rng(seed)
+    h = np.float32(1.0 / max(ni, nj, nk))
+    phi = scenes.random_phi(ni, nj, nk, h, rng, n_spheres=2)
+    u, v, w = scenes.random_velocity(ni, nj, nk, rng, scale=0.5)
+    if ppc is not None:
+        p = scenes.jittered_particles(ni, nj, nk, h, ppc, rng)
+    else:
+        p = scenes.random_particles(ni, nj, nk, h, n_particles, rng)
+    return h, phi, u, v, w, p
+
+
+@pytest.mark.parametrize("dims,dt", [((12, 10, 9), 0.02), ((16, 16, 16), 0.05)])
+def test_advect_flip_matches_reference(orc, ref, dims, dt):
+    """advect_FLIP (RK3 with the reference's c3 = (1 - c1 - c2) dt, then the
+    solid push-out along the normalised phi gradient): bit-identical."""
+    ni, nj, nk = dims
+    h, phi, u, v, w, p = _flip_scene(ni, nj, nk, 5, n_particles=4000)
+    a = orc.advect_flip(ni, nj, nk, h, p, u, v, w, phi, dt)
+    b = ref.advect_flip(ni, nj, nk, h, p, u, v, w, phi, dt)
+    assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+    # some particles were pushed out of a solid
+    assert (orc.advect_flip(ni, nj, nk, h, p, u * 0, v * 0, w * 0, phi, dt)["pos"] != p["pos"]).any()
+
+
+def test_reorder_flip_matches_reference_without_seeding(orc, ref):
+    """Every cell holds 8 or more particles: reorder_FLIP only keeps (8-9) or
+    caps (10+) in bucket order and drops solid particles - no random draws,
+    so the oracle equals the reference exactly."""
+    ni, nj, nk = 8, 7, 6
+    h, phi, u, v, w, p = _flip_scene(ni, nj, nk, 6, ppc=8)
+    extra = p[np.random.default_rng(1).integers(0, len(p), 900)]
+    p = np.concatenate([p, extra])
+    a = orc.reorder_flip(ni, nj, nk, h, p, u, v, w, phi)
+    b = ref.reorder_flip(ni, nj, nk, h, p, u, v, w, phi)
+    assert len(a) == len(b) and np.array_equal(a.view(np.uint8), b.view(np.uint8))
+
+
+def test_reorder_flip_seeding_structure_matches_reference(orc, ref):
+    """Sparse cells are topped up to 8: the reference draws positions from
+    rand(), the oracle from its counter-based generator, so compare what is
+    deterministic - the kept particles in order and the per-cell counts."""
+    ni, nj, nk = 9, 8, 7
+    h, phi, u, v, w, p = _flip_scene(ni, nj, nk, 7, n_particles=1500)
+    p["temp"] = np.arange(len(p), dtype=np.float32) + 1.0  # marks the input particles
+    a = orc.reorder_flip(ni, nj, nk, h, p, u, v, w, phi, seed=3)
+    b = ref.reorder_flip(ni, nj, nk, h, p, u, v, w, phi, seed=3)
+    ka, kb = a[a["temp"] > 0], b[b["temp"] > 0]
+    assert np.array_equal(ka.view(np.uint8), kb.view(np.uint8))
+    ca = orc.hash(ni, nj, nk, h, a)
+    cb = orc.hash(ni, nj, nk, h, b)
+    assert abs(len(a) - len(b)) <= 0.02 * len(b)  # new particles straddling a solid may differ
+    ha = np.bincount(ca[ca >= 0], minlength=ni * nj * nk)
+    hb = np.bincount(cb[cb >= 0], minlength=ni * nj * nk)
+    # cells whose eight nodal-phi corners share a sign filter every position alike
+    corners = np.stack([phi[dk:dk + nk, dj:dj + nj, di:di + ni] for dk in (0, 1) for dj in (0, 1) for di in (0, 1)])
+    sure = ((corners >= 0).all(axis=0) | (corners < 0).all(axis=0)).ravel()
+    assert sure.sum() > 0.5 * sure.size
+    assert np.array_equal(ha[sure], hb[sure])
+    new = a[a["temp"] == 0]
+    assert len(new) > 0 and (new["dens"] == 0).all()
