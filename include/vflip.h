@@ -252,6 +252,28 @@ int vflip_g2p(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, 
               const float* dv, const float* dw, const float* un, const float* vn, const float* wn,
               double flip_ratio);
 
+/* SmokeSolver3D::advect_FLIP (SS/Smoke_solver3D.cpp:1407-1449): RK3 trace
+ * through the grid velocity (traceRK3 :144-158, with the reference's
+ * c3 = (1 - c1 - c2) dt), then a particle whose sampled nodal solid phi is
+ * negative moves out along the normalised phi gradient by -phi
+ * (get_solid_normal :115-124).  Positions updated in place; bit-exact. */
+int vflip_advect_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np, const float* u,
+                      const float* v, const float* w, const float* nodal_phi, float dt);
+
+/* SmokeSolver3D::hash_FLIP + reorder_FLIP (SS/Smoke_solver3D.cpp:1327-1396):
+ * per cell in (k, j, i) order, fewer than 8 particles are kept and topped up
+ * to 8 with new ones at (i, j, k) h + r 0.49 h (r uniform in [-1, 1)^3, grid
+ * velocity there, density/temperature 0), 8-9 kept, 10+ cut to their first
+ * 8; then particles inside solids (sampled nodal phi < 0) are dropped.  The
+ * reference draws r from rand(); here r comes from a counter-based hash of
+ * (seed, cell, slot, axis), so new positions differ from the reference's
+ * while the kept particles, their order and the counts match.  Writes the
+ * result to `out` (device, `capacity` records) and its count to *np_out
+ * (also when it exceeds capacity: VFLIP_ERR_TOO_LARGE). */
+int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
+                       const float* u, const float* v, const float* w, const float* nodal_phi, unsigned seed,
+                       void* out, int capacity, int* np_out);
+
 /* ---- measurement ----------------------------------------------------------- */
 
 /* When enabled, every launch of the fine-level smoothing sweep (the

@@ -152,3 +152,45 @@ def test_advect_pair_matches_single(gpu_solver, orc):
     a, b = gpu_solver[0].advect_rk2_linear2(ni, nj, nk, h, 0.02, t(u), t(v), t(w), t(f), t(g), (0, 0, 0))
     assert np.array_equal(a.cpu().numpy(), orc.advect_rk2(ni, nj, nk, h, 0.02, u, v, w, f, (0, 0, 0)))
     assert np.array_equal(b.cpu().numpy(), orc.advect_rk2(ni, nj, nk, h, 0.02, u, v, w, g, (0, 0, 0)))
+
+
+def _flip_scene(ni, nj, nk, seed, n_particles):
+    rng = np.random.default_rng(seed)
+    h = np.float32(1.0 / max(ni, nj, nk))
+    phi = scenes.random_phi(ni, nj, nk, h, rng, n_spheres=2)
+    u, v, w = scenes.random_velocity(ni, nj, nk, rng, scale=0.5)
+    p = scenes.random_particles(ni, nj, nk, h, n_particles, rng)
+    return h, phi, u, v, w, p
+
+
+@pytest.mark.parametrize("dims,dt,n", [((12, 10, 9), 0.02, 5000), ((32, 24, 20), 0.05, 60000)])
+def test_advect_flip_bit_exact(gpu_solver, orc, dims, dt, n):
+    ni, nj, nk = dims
+    h, phi, u, v, w, p = _flip_scene(ni, nj, nk, 5, n)
+    x = t(p.view(np.uint8))
+    gpu_solver[1].advect_flip(ni, nj, nk, h, x, t(u), t(v), t(w), t(phi), dt)
+    want = orc.advect_flip(ni, nj, nk, h, p, u, v, w, phi, dt)
+    assert np.array_equal(x.cpu().numpy(), want.view(np.uint8))
+
+
+@pytest.mark.parametrize("dims,n,seed", [((9, 8, 7), 1500, 3), ((24, 20, 16), 40000, 11), ((16, 16, 16), 0, 2)])
+def test_reorder_flip_bit_exact(gpu_solver, orc, dims, n, seed):
+    """Same counter-based draws as the oracle: the whole reseeded set is equal
+    byte for byte (kept particles in cell order, new ones, solid filter)."""
+    ni, nj, nk = dims
+    h, phi, u, v, w, p = _flip_scene(ni, nj, nk, 9, max(n, 1))
+    p = p[:n]
+    got = gpu_solver[1].reorder_flip(ni, nj, nk, h, t(p.view(np.uint8)) if n else torch.empty(0, dtype=torch.uint8,
+                                                                                                   device=DEV),
+                                     t(u), t(v), t(w), t(phi), seed=seed).cpu().numpy()
+    want = orc.reorder_flip(ni, nj, nk, h, p, u, v, w, phi, seed=seed)
+    assert got.size == want.size * 40 and np.array_equal(got, want.view(np.uint8))
+
+
+def test_reorder_flip_capacity(gpu_solver):
+    from vflip_b200._lib import VflipError
+
+    ni = nj = nk = 8
+    h, phi, u, v, w, p = _flip_scene(ni, nj, nk, 4, 100)
+    with pytest.raises(VflipError):
+        gpu_solver[1].reorder_flip(ni, nj, nk, h, t(p.view(np.uint8)), t(u), t(v), t(w), t(phi), capacity=10)

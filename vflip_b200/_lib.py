@@ -69,6 +69,8 @@ SIGNATURES = {
     "vflip_delta": (_I, [_P, _SZ, _P, _P, _P]),
     "vflip_particle_cells": (_I, [_P, _I, _I, _I, _F, _P, _I, _P]),
     "vflip_p2g": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _P, _P]),
+    "vflip_advect_flip": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _F]),
+    "vflip_reorder_flip": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, C.c_uint, _P, _I, C.POINTER(_I)]),
     "vflip_g2p": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _P, _P, _D]),
     "vflip_set_profiling": (_I, [_P, _I]),
     "vflip_profile_sweeps": (_I, [_P, C.POINTER(_I), C.POINTER(_D), C.POINTER(_D)]),

@@ -403,4 +403,147 @@ __global__ void g2p_kernel(ParticleRec* __restrict__ p, int np, GridView du, Gri
   }
 }
 
+// ---------------------------------------------------------------------------
+// FLIP particle advection and reseeding (the steps either side of P2G/G2P)
+
+// SmokeSolver3D::traceRK3, Smoke_solver3D.cpp:144-158, through get_velocity
+// (subdomain blend inactive): c1 = 2/9 dt and c2 = 3/9 dt rounded from
+// double, and c3 = (1 - c1 - c2) dt as the reference writes it (c1, c2
+// already carry dt).
+__device__ __forceinline__ void trace_rk3(const GridView& u, const GridView& v, const GridView& w, const float p[3],
+                                          float dt, float out[3]) {
+  const float c1 = (float)(2.0 / 9.0 * (double)dt), c2 = (float)(3.0 / 9.0 * (double)dt);
+  const float c3 = (float)((1.0 - (double)c1 - (double)c2) * (double)dt);
+  const float half = (float)(0.5 * (double)dt), q3 = (float)(0.75 * (double)dt);
+  const float v1[3] = {sample_linear(u, p[0], p[1], p[2]), sample_linear(v, p[0], p[1], p[2]),
+                       sample_linear(w, p[0], p[1], p[2])};
+  const float m1[3] = {p[0] + half * v1[0], p[1] + half * v1[1], p[2] + half * v1[2]};
+  const float v2[3] = {sample_linear(u, m1[0], m1[1], m1[2]), sample_linear(v, m1[0], m1[1], m1[2]),
+                       sample_linear(w, m1[0], m1[1], m1[2])};
+  const float m2[3] = {p[0] + q3 * v2[0], p[1] + q3 * v2[1], p[2] + q3 * v2[2]};
+  const float v3[3] = {sample_linear(u, m2[0], m2[1], m2[2]), sample_linear(v, m2[0], m2[1], m2[2]),
+                       sample_linear(w, m2[0], m2[1], m2[2])};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) out[a] = p[a] + c1 * v1[a] + c2 * v2[a] + c3 * v3[a];
+}
+
+// get_solid_normal (Smoke_solver3D.cpp:115-124): Buffer3D::sample_grad
+// (fluid_buffer3D.h:249-257, differences over +-h in double world
+// coordinates) normalised by mag = sqrt(mag2) + 1e-6 (vec.h:194-219; the
+// square root in double, as the reference's build evaluates it)
+__device__ __forceinline__ void solid_normal(const GridView& phi, const float p[3], float n[3]) {
+  const double x = p[0], y = p[1], z = p[2], h = phi.h;
+  const float r = sample_linear(phi, x + h, y, z), l = sample_linear(phi, x - h, y, z);
+  const float u = sample_linear(phi, x, y + h, z), b = sample_linear(phi, x, y - h, z);
+  const float f = sample_linear(phi, x, y, z - h), k = sample_linear(phi, x, y, z + h);
+  n[0] = 0.5f * (float)((double)(r - l) / h);
+  n[1] = 0.5f * (float)((double)(u - b) / h);
+  n[2] = 0.5f * (float)((double)(k - f) / h);
+  float m2 = n[0] * n[0];
+  m2 = m2 + n[1] * n[1];
+  m2 = m2 + n[2] * n[2];
+  const float mag = (float)(sqrt((double)m2) + 1e-6);
+  n[0] = n[0] / mag;
+  n[1] = n[1] / mag;
+  n[2] = n[2] / mag;
+}
+
+// SmokeSolver3D::advect_FLIP, Smoke_solver3D.cpp:1407-1449: RK3 through the
+// grid velocity, then out of a solid along its normal by -phi.
+__global__ void advect_flip_kernel(ParticleRec* __restrict__ p, int np, GridView u, GridView v, GridView w,
+                                   GridView phi, float dt) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
+    const float pos0[3] = {p[q].pos[0], p[q].pos[1], p[q].pos[2]};
+    float pos[3];
+    trace_rk3(u, v, w, pos0, dt, pos);
+    const float ph = sample_linear(phi, pos[0], pos[1], pos[2]);
+    if (ph < 0) {
+      float n[3];
+      solid_normal(phi, pos, n);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) pos[a] = pos[a] - ph * n[a];
+    }
+    p[q].pos[0] = pos[0];
+    p[q].pos[1] = pos[1];
+    p[q].pos[2] = pos[2];
+  }
+}
+
+// Counter-based uniform in [-1, 1) for reseeding: a 32-bit integer mix of
+// (seed, cell, slot, axis).  The reference draws frand(-1, 1) from rand()
+// (Smoke_solver3D.h:36-39) - the same distribution from a sequential
+// generator that parallel code cannot reproduce.
+__host__ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+__device__ __forceinline__ float reseed_uniform(uint32_t seed, uint32_t cell, uint32_t slot, uint32_t axis) {
+  const uint32_t r = mix32(mix32(mix32(seed ^ 0x9e3779b9u) + cell) + (slot * 3u + axis));
+  return -1.0f + 2.0f * ((float)(r >> 8) * (1.0f / 16777216.0f));
+}
+
+// reorder_FLIP, Smoke_solver3D.cpp:1347-1396: particles written per cell -
+// fewer than 8: all kept + topped up to 8; 8 or 9: all; 10+: the first 8
+__global__ void reorder_count_kernel(const int* __restrict__ start, int* __restrict__ out_count, int nc) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    const int cnt = start[c + 1] - start[c];
+    out_count[c] = cnt < 8 ? 8 : (cnt < 10 ? cnt : 8);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) out_count[nc] = 0;
+}
+
+// one thread per cell: kept particles in bucket order, then the new ones at
+// (i, j, k) h + r 0.49 h with the grid velocity there, density and
+// temperature 0 (get_velocity_self, Smoke_solver3D.cpp:89-97)
+__global__ void reorder_write_kernel(const ParticleRec* __restrict__ p, const int* __restrict__ start,
+                                     const int* __restrict__ order, const int* __restrict__ base,
+                                     ParticleRec* __restrict__ tmp, int ni, int nj, int nk, float h, GridView u,
+                                     GridView v, GridView w, uint32_t seed) {
+  const int nc = ni * nj * nk;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    const int s0 = start[c], cnt = start[c + 1] - s0, b = base[c];
+    const int keep = cnt < 10 ? cnt : 8;
+    for (int e = 0; e < keep; ++e) tmp[b + e] = p[order[s0 + e]];
+    if (cnt < 8) {
+      const int i = c % ni, j = (c / ni) % nj, k = c / (ni * nj);
+      const float bx = (float)i * h, by = (float)j * h, bz = (float)k * h;
+      for (int e = cnt; e < 8; ++e) {
+        ParticleRec r;
+        r.pos[0] = bx + reseed_uniform(seed, (uint32_t)c, (uint32_t)e, 0u) * 0.49f * h;
+        r.pos[1] = by + reseed_uniform(seed, (uint32_t)c, (uint32_t)e, 1u) * 0.49f * h;
+        r.pos[2] = bz + reseed_uniform(seed, (uint32_t)c, (uint32_t)e, 2u) * 0.49f * h;
+        r.vel[0] = sample_linear(u, r.pos[0], r.pos[1], r.pos[2]);
+        r.vel[1] = sample_linear(v, r.pos[0], r.pos[1], r.pos[2]);
+        r.vel[2] = sample_linear(w, r.pos[0], r.pos[1], r.pos[2]);
+        r.dens = 0.0f;
+        r.temp = 0.0f;
+        r.hash_idx = 0;
+        r.sub_hash_idx = 0;
+        tmp[b + e] = r;
+      }
+    }
+  }
+}
+
+// keep flag: sampled solid phi >= 0 (reorder_FLIP's final filter)
+__global__ void solid_keep_kernel(const ParticleRec* __restrict__ tmp, const int* __restrict__ total,
+                                  int* __restrict__ keep, GridView phi, int cap) {
+  const int n = min(*total, cap);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+    keep[q] = sample_linear(phi, tmp[q].pos[0], tmp[q].pos[1], tmp[q].pos[2]) >= 0.0f ? 1 : 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) keep[n] = 0;
+}
+
+__global__ void compact_kernel(const ParticleRec* __restrict__ tmp, const int* __restrict__ keep,
+                               const int* __restrict__ pos, const int* __restrict__ total, ParticleRec* __restrict__ out,
+                               int cap_in, int cap_out) {
+  const int n = min(*total, cap_in);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+    if (keep[q] && pos[q] < cap_out) out[pos[q]] = tmp[q];
+}
+
 }  // namespace vflip

@@ -2026,6 +2026,84 @@ int vflip_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* parti
   return VFLIP_OK;
 }
 
+int vflip_advect_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np, const float* u,
+                      const float* v, const float* w, const float* nodal_phi, float dt) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (np < 0 || (np > 0 && !particles) || !u || !v || !w || !nodal_phi) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  if (np == 0) return VFLIP_OK;
+  const double hd = h, ih = inv_pow2(h);
+  GridView gu{u, ni + 1, nj, nk, hd, 0.5, 0.0, 0.0, ih}, gv{v, ni, nj + 1, nk, hd, 0.0, 0.5, 0.0, ih},
+      gw{w, ni, nj, nk + 1, hd, 0.0, 0.0, 0.5, ih}, gp{nodal_phi, ni + 1, nj + 1, nk + 1, hd, 0.5, 0.5, 0.5, ih};
+  advect_flip_kernel<<<grid_for(np, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>((ParticleRec*)particles, np, gu,
+                                                                                  gv, gw, gp, dt);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
+                       const float* u, const float* v, const float* w, const float* nodal_phi, unsigned seed,
+                       void* out, int capacity, int* np_out) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (np < 0 || (np > 0 && !particles) || !u || !v || !w || !nodal_phi || !out || !np_out || capacity < 0)
+    return ctx->fail(VFLIP_ERR_ARG, "null pointer or negative capacity");
+  const size_t nc = (size_t)ni * nj * nk;
+  if (9.0 * (double)nc > 2147483000.0) return ctx->fail(VFLIP_ERR_TOO_LARGE, "grid too large for reseeding");
+  const int ntmp = (int)(9 * nc);  // at most 9 particles per cell before the solid filter
+  int *cell, *slot, *count, *start, *order, *ocount, *base, *keep, *kpos;
+  ParticleRec* tmp;
+  const size_t npp = np > 0 ? (size_t)np : 1;
+  VF_ALLOC(cell, int, "p_cell", npp);
+  VF_ALLOC(slot, int, "p_slot", npp);
+  VF_ALLOC(count, int, "p_count", nc + 1);
+  VF_ALLOC(start, int, "p_start", nc + 1);
+  VF_ALLOC(order, int, "p_order", npp);
+  VF_ALLOC(ocount, int, "r_count", nc + 1);
+  VF_ALLOC(base, int, "r_base", nc + 1);
+  VF_ALLOC(tmp, ParticleRec, "r_tmp", ntmp);
+  VF_ALLOC(keep, int, "r_keep", (size_t)ntmp + 1);
+  VF_ALLOC(kpos, int, "r_kpos", (size_t)ntmp + 1);
+  VF_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (nc + 1), ctx->stream));
+  if (np > 0) {
+    hash_count_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
+        (const ParticleRec*)particles, np, ni, nj, nk, h, (float)inv_pow2(h), cell, slot, count);
+    VF_LAUNCH_CHECK();
+  }
+  if ((rc = exclusive_scan(ctx, count, start, nc + 1))) return rc;
+  if (np > 0) {
+    scatter_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(cell, slot, start, order, np);
+    VF_LAUNCH_CHECK();
+    sort_buckets_kernel<<<grid_for(nc, 256, ctx->num_sms), 256, 0, ctx->stream>>>(start, order, (int)nc);
+    VF_LAUNCH_CHECK();
+  }
+  reorder_count_kernel<<<grid_for(nc, 256, ctx->num_sms), 256, 0, ctx->stream>>>(start, ocount, (int)nc);
+  VF_LAUNCH_CHECK();
+  if ((rc = exclusive_scan(ctx, ocount, base, nc + 1))) return rc;
+  const double hd = h, ih = inv_pow2(h);
+  GridView gu{u, ni + 1, nj, nk, hd, 0.5, 0.0, 0.0, ih}, gv{v, ni, nj + 1, nk, hd, 0.0, 0.5, 0.0, ih},
+      gw{w, ni, nj, nk + 1, hd, 0.0, 0.0, 0.5, ih}, gp{nodal_phi, ni + 1, nj + 1, nk + 1, hd, 0.5, 0.5, 0.5, ih};
+  reorder_write_kernel<<<grid_for(nc, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(
+      (const ParticleRec*)particles, start, order, base, tmp, ni, nj, nk, h, gu, gv, gw, (uint32_t)seed);
+  VF_LAUNCH_CHECK();
+  solid_keep_kernel<<<grid_for(ntmp, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(tmp, base + nc, keep, gp, ntmp);
+  VF_LAUNCH_CHECK();
+  if ((rc = exclusive_scan(ctx, keep, kpos, (size_t)ntmp + 1))) return rc;
+  compact_kernel<<<grid_for(ntmp, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(tmp, keep, kpos, base + nc,
+                                                                                  (ParticleRec*)out, ntmp, capacity);
+  VF_LAUNCH_CHECK();
+  // kept count = kpos[total]; total <= ntmp by construction
+  int total = 0, kept = 0;
+  VF_CUDA(cudaMemcpyAsync(&total, base + nc, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(&kept, kpos + total, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  *np_out = kept;
+  if (kept > capacity) return ctx->fail(VFLIP_ERR_TOO_LARGE, "reseeded particles (%d) exceed the capacity %d", kept,
+                                        capacity);
+  return VFLIP_OK;
+}
+
 int vflip_g2p(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np, const float* du,
               const float* dv, const float* dw, const float* un, const float* vn, const float* wn,
               double flip_ratio) {

@@ -330,6 +330,24 @@ class Solver:
                                        _p(un), _p(vn), _p(wn), float(flip_ratio)))
         return particles
 
+    def advect_flip(self, ni, nj, nk, h, particles, u, v, w, nodal_phi, dt):
+        """SmokeSolver3D::advect_FLIP: RK3 + solid push-out, positions in place."""
+        n = self._np(particles)
+        self._check(self.lib.vflip_advect_flip(self.ctx, ni, nj, nk, float(h), _p(particles), n, _p(u), _p(v), _p(w),
+                                               _p(nodal_phi), float(dt)))
+        return particles
+
+    def reorder_flip(self, ni, nj, nk, h, particles, u, v, w, nodal_phi, seed=0, capacity=None):
+        """SmokeSolver3D::hash_FLIP + reorder_FLIP: returns a new particle
+        tensor (uint8 records) with 8 particles per open cell (8-9 kept)."""
+        n = self._np(particles)
+        cap = 9 * ni * nj * nk if capacity is None else int(capacity)
+        out = torch.empty(max(cap, 1) * PARTICLE_BYTES, dtype=torch.uint8, device=self.device)
+        cnt = C.c_int()
+        self._check(self.lib.vflip_reorder_flip(self.ctx, ni, nj, nk, float(h), _p(particles), n, _p(u), _p(v), _p(w),
+                                                _p(nodal_phi), int(seed) & 0xFFFFFFFF, _p(out), cap, C.byref(cnt)))
+        return out[:cnt.value * PARTICLE_BYTES]
+
     # ------------------------------------------------------------- plume
     def plume_sources(self, ni, nj, nk, h, dt, rho, temp, v, centre, radius, dens_value=1.0, heat_value=1.0,
                       alpha=0.1, beta=1.0):
