@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner arm")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched uneven-Poisson arm")
+    ap.add_argument("--no-flip", action="store_true", help="skip the FLIP smoke arm")
     ap.add_argument("--learned-level", type=int, default=1)
     ap.add_argument("--learned-capture", type=int, default=40)
     ap.add_argument("--learned-epochs", type=int, default=16)
@@ -241,6 +242,8 @@ def run_vflip(a):
             out["learned"] = learned_arm(a, sim, solver)
         if not a.no_batched and world == 1:
             out["batched"] = batched_arm(solver)
+        if not a.no_flip and world == 1:
+            out["flip"] = flip_arm(solver, a.steps)
     solver.close()
     if world > 1:
         dist.destroy_process_group()
@@ -292,6 +295,36 @@ def learned_arm(a, sim, solver):
             "config": {"network_grid_level": a.learned_level, "capture_steps": a.learned_capture,
                        "epochs": a.learned_epochs, "ritz_subspace": "network warm start + coarse correction (no V(b)), "
                        "2 smoothing sweeps each", "unet": "4 levels, 16/32/64/128 channels, BF16 tcgen05 convs"}}
+
+
+def flip_arm(solver, steps, n=128, warmup=3):
+    """The FLIP smoke scene at 128^3 (8 particles per cell jittered in the
+    source sphere r = 0.12, sphere obstacle r = 0.15, FLIP/PIC 0.95, dt 0.01,
+    MGPCG to 1e-6): advect_FLIP, P2G, projection, delta, G2P, reorder_FLIP
+    per step, particles resident on the device; CUDA events around `steps`
+    steps after `warmup` (reseeding fills every open cell to 8 particles)."""
+    import torch
+
+    from vflip_b200.flip import FlipParams, FlipSim
+
+    sim = FlipSim(solver, FlipParams(n=n))
+    for _ in range(warmup):
+        sim.step()
+    np0 = sim.num_particles
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    iters = []
+    for _ in range(steps):
+        conv, st = sim.step()
+        iters.append(st.iterations)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"grid": n, "steps_per_s": steps / (ms * 1e-3), "ms_per_step": ms / steps,
+            "particles": sim.num_particles, "particles_at_start": np0,
+            "particle_steps_per_s": sim.num_particles * steps / (ms * 1e-3),
+            "pcg_iterations_mean": sum(iters) / len(iters)}
 
 
 def batched_arm(solver, count=32, reps=2):
