@@ -224,6 +224,59 @@ int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, fl
                              const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
                              double oz, const float* field, float* out, const float* field2, float* out2);
 
+/* SmokeSolver3D::advect_field_cubic_clamp (SS/Smoke_solver3D.cpp:657-707):
+ * the RK2 backtrace above, then the cubic sample of Buffer3D::sample_cubic
+ * (SS/fluid_buffer3D.h:22-38, 259-326) over the clamped 4x4x4 neighbourhood,
+ * replaced by the trilinear sample where the cubic value reaches or leaves
+ * the range of the eight surrounding nodes.  Arguments as
+ * vflip_advect_rk2_linear; FP64 contexts are bit-identical to the reference,
+ * FP32/MIXED contexts run the same scheme in FP32. */
+int vflip_advect_cubic_clamp(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                             const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
+                             double oz, const float* field, float* out);
+
+/* SmokeSolver3D::advect (SS/Smoke_solver3D.cpp:8-29): cubic-clamped
+ * self-advection of the MAC velocity, all three components in one launch.
+ * The outputs must not alias the inputs. */
+int vflip_advect_velocity_cubic_clamp(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                                      const float* v, const float* w, float* u_out, float* v_out, float* w_out);
+
+/* SmokeSolver3D::advect_field (SS/Smoke_solver3D.cpp:564-610): traceRK3
+ * (SS/Smoke_solver3D.cpp:144-157) from each node with step -dt through the
+ * MAC velocity of the ni x nj x nk grid of spacing h, then a trilinear
+ * sample.  The field has its own spacing fh: node (i,j,k) sits at
+ * ((i-ox)fh, (j-oy)fh, (k-oz)fh).  The reference's density and temperature
+ * grids are 2ni x 2nj x 2nk at fh = h/2 with zero offsets
+ * (SS/Smoke_solver3D.h:313-315).  Precision as vflip_advect_cubic_clamp. */
+int vflip_advect_rk3_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                            const float* v, const float* w, int fnx, int fny, int fnz, double fh, double ox,
+                            double oy, double oz, const float* field, float* out);
+
+/* Same for two fields on one grid sharing the backtrace (density and
+ * temperature); field2/out2 may be NULL. */
+int vflip_advect_rk3_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                             const float* v, const float* w, int fnx, int fny, int fnz, double fh, double ox,
+                             double oy, double oz, const float* field, float* out, const float* field2,
+                             float* out2);
+
+/* ---- smoke scalars on the density/temperature grids ------------------------ */
+
+/* SmokeSolver3D::gen_heat (SS/Smoke_solver3D.cpp:1624-1650), in place on the
+ * fnx x fny x fnz density and temperature grids of spacing fh: divide by
+ * (1 + decay dt), then set (dens, heat) inside the source, the nodes
+ * (i,j,k) fh within `radius` of (cx, cz) horizontally and within radius/4 of
+ * cy vertically.  Bit-identical to the reference. */
+int vflip_gen_heat(vflip_ctx* ctx, int fnx, int fny, int fnz, double fh, float dt, float dens_decay,
+                   float temp_decay, float cx, float cy, float cz, float radius, float dens, float heat, float* rho,
+                   float* temp);
+
+/* SmokeSolver3D::add_smokeforce (SS/Smoke_solver3D.cpp:1652-1668): each
+ * particle's y velocity gains dt (-alpha rho + beta T), with rho and T
+ * sampled trilinearly (FP64 lerps) from the grids of spacing fh.  In place;
+ * bit-identical to the reference. */
+int vflip_add_smokeforce(vflip_ctx* ctx, void* particles, int np, int fnx, int fny, int fnz, double fh,
+                         const float* rho, const float* temp, float alpha, float beta, float dt);
+
 /* delta = after - before, n floats (SmokeSolver3D::getDelta, SS/Smoke_solver3D.cpp:1298-1319). */
 int vflip_delta(vflip_ctx* ctx, size_t n, const float* after, const float* before, float* delta);
 

@@ -82,6 +82,11 @@ def _load(path, prefix):
     getattr(lib, p + "_advect_flip").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _F]
     getattr(lib, p + "_reorder_flip").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, C.c_uint, _P, _I]
     getattr(lib, p + "_reorder_flip").restype = _I
+    getattr(lib, p + "_advect_cubic_clamp").argtypes = [_I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _P,
+                                                        _P]
+    getattr(lib, p + "_advect_rk3").argtypes = [_I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _D, _P, _P]
+    getattr(lib, p + "_gen_heat").argtypes = [_I, _I, _I, _D, _F, _F, _F, _F, _F, _F, _F, _F, _F, _P, _P]
+    getattr(lib, p + "_add_smokeforce").argtypes = [_P, _I, _I, _I, _I, _D, _P, _P, _F, _F, _F]
     if prefix == "oracle":
         getattr(lib, p + "_g2p").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _P, _P, _D]
         getattr(lib, p + "_delta").argtypes = [_I, _I, _I, _P, _P, _P]
@@ -248,6 +253,42 @@ class _Impl:
         self.fn("advect_rk2")(ni, nj, nk, h, dt, _ptr(u), _ptr(v), _ptr(w), fnx, fny, fnz, float(offsets[0]),
                               float(offsets[1]), float(offsets[2]), _ptr(field), _ptr(out))
         return out
+
+    def advect_cubic_clamp(self, ni, nj, nk, h, dt, u, v, w, field, offsets):
+        """SmokeSolver3D::advect_field_cubic_clamp (RK2 backtrace, clamped cubic sample)."""
+        u, v, w, field = [np.ascontiguousarray(a, np.float32) for a in (u, v, w, field)]
+        fnz, fny, fnx = field.shape
+        out = np.zeros_like(field)
+        self.fn("advect_cubic_clamp")(ni, nj, nk, h, dt, _ptr(u), _ptr(v), _ptr(w), fnx, fny, fnz,
+                                      float(offsets[0]), float(offsets[1]), float(offsets[2]), _ptr(field), _ptr(out))
+        return out
+
+    def advect_rk3(self, ni, nj, nk, h, dt, u, v, w, field, fh, offsets=(0.0, 0.0, 0.0)):
+        """SmokeSolver3D::advect_field (RK3 backtrace, trilinear sample) of a
+        field of spacing fh (h/2 for the density/temperature grids)."""
+        u, v, w, field = [np.ascontiguousarray(a, np.float32) for a in (u, v, w, field)]
+        fnz, fny, fnx = field.shape
+        out = np.zeros_like(field)
+        self.fn("advect_rk3")(ni, nj, nk, h, dt, _ptr(u), _ptr(v), _ptr(w), fnx, fny, fnz, float(fh),
+                              float(offsets[0]), float(offsets[1]), float(offsets[2]), _ptr(field), _ptr(out))
+        return out
+
+    def gen_heat(self, rho, temp, fh, dt, dens_decay, temp_decay, centre, radius, dens, heat):
+        """SmokeSolver3D::gen_heat on copies; returns (rho, temp)."""
+        rho = np.array(rho, np.float32, copy=True)
+        temp = np.array(temp, np.float32, copy=True)
+        fnz, fny, fnx = rho.shape
+        self.fn("gen_heat")(fnx, fny, fnz, float(fh), dt, dens_decay, temp_decay, float(centre[0]),
+                            float(centre[1]), float(centre[2]), radius, dens, heat, _ptr(rho), _ptr(temp))
+        return rho, temp
+
+    def add_smokeforce(self, particles, rho, temp, fh, alpha, beta, dt):
+        """SmokeSolver3D::add_smokeforce on a copy of the particles."""
+        p = np.array(particles, PARTICLE_DTYPE, copy=True)
+        rho, temp = [np.ascontiguousarray(a, np.float32) for a in (rho, temp)]
+        fnz, fny, fnx = rho.shape
+        self.fn("add_smokeforce")(_ptr(p), len(p), fnx, fny, fnz, float(fh), _ptr(rho), _ptr(temp), alpha, beta, dt)
+        return p
 
     def hash(self, ni, nj, nk, h, particles):
         particles = np.ascontiguousarray(particles, PARTICLE_DTYPE)

@@ -446,6 +446,83 @@ int ref_reorder_flip(int ni, int nj, int nk, float h, const void* particles, int
   return n;
 }
 
+// SmokeSolver3D::advect_field_cubic_clamp (Smoke_solver3D.cpp:657-707) of a
+// field with the velocity's spacing h and grid offsets (fox, foy, foz).
+void ref_advect_cubic_clamp(int ni, int nj, int nk, float h, float dt, const float* u, const float* v,
+                            const float* w, int fnx, int fny, int fnz, double fox, double foy, double foz,
+                            const float* field, float* out) {
+  SmokeSolver3D s;
+  init_solver_grids(s, ni, nj, nk, h);
+  to_buffer(s._un, u);
+  to_buffer(s._vn, v);
+  to_buffer(s._wn, w);
+  buffer3Df f, fo;
+  f.init(fnx, fny, fnz, h, fox, foy, foz);
+  fo.init(fnx, fny, fnz, h, fox, foy, foz);
+  to_buffer(f, field);
+  s.advect_field_cubic_clamp(dt, f, fo);
+  from_buffer(fo, out);
+  f.free(); fo.free();
+}
+
+// SmokeSolver3D::advect_field (Smoke_solver3D.cpp:564-610): traceRK3 with
+// step -dt, trilinear sample.  The field has its own spacing fh.
+void ref_advect_rk3(int ni, int nj, int nk, float h, float dt, const float* u, const float* v, const float* w,
+                    int fnx, int fny, int fnz, double fh, double fox, double foy, double foz, const float* field,
+                    float* out) {
+  SmokeSolver3D s;
+  init_solver_grids(s, ni, nj, nk, h);
+  to_buffer(s._un, u);
+  to_buffer(s._vn, v);
+  to_buffer(s._wn, w);
+  buffer3Df f, fo;
+  f.init(fnx, fny, fnz, fh, fox, foy, foz);
+  fo.init(fnx, fny, fnz, fh, fox, foy, foz);
+  to_buffer(f, field);
+  s.advect_field(dt, f, fo);
+  from_buffer(fo, out);
+  f.free(); fo.free();
+}
+
+// SmokeSolver3D::gen_heat (Smoke_solver3D.cpp:1624-1650) on density and
+// temperature grids of fnx x fny x fnz nodes at spacing fh, in place.
+void ref_gen_heat(int fnx, int fny, int fnz, double fh, float dt, float dens_decay, float temp_decay, float cx,
+                  float cy, float cz, float radius, float dens, float heat, float* rho, float* temp) {
+  SmokeSolver3D s;
+  quiet_subdomain(s.sub_domain);
+  s._rho.init(fnx, fny, fnz, fh, 0.0, 0.0, 0.0);
+  s._Temperature.init(fnx, fny, fnz, fh, 0.0, 0.0, 0.0);
+  to_buffer(s._rho, rho);
+  to_buffer(s._Temperature, temp);
+  s._dens_decay = dens_decay;
+  s._temp_decay = temp_decay;
+  s._smoke_center = Vec3f(cx, cy, cz);
+  s._smoke_radius = radius;
+  s._smoke_dens = dens;
+  s._smoke_heat = heat;
+  s.gen_heat(dt);
+  from_buffer(s._rho, rho);
+  from_buffer(s._Temperature, temp);
+}
+
+// SmokeSolver3D::add_smokeforce (Smoke_solver3D.cpp:1652-1668) on the
+// particles, in place, with density/temperature grids at spacing fh.
+void ref_add_smokeforce(void* particles, int np, int fnx, int fny, int fnz, double fh, const float* rho,
+                        const float* temp, float alpha, float beta, float dt) {
+  particle* p = (particle*)particles;
+  SmokeSolver3D s;
+  quiet_subdomain(s.sub_domain);
+  s._rho.init(fnx, fny, fnz, fh, 0.0, 0.0, 0.0);
+  s._Temperature.init(fnx, fny, fnz, fh, 0.0, 0.0, 0.0);
+  to_buffer(s._rho, rho);
+  to_buffer(s._Temperature, temp);
+  s._alpha = alpha;
+  s._beta = beta;
+  s.FLIP.assign(p, p + np);
+  s.add_smokeforce(dt);
+  for (int q = 0; q < np; ++q) p[q] = s.FLIP[q];
+}
+
 // SmokeSolver3D::getDelta (Smoke_solver3D.cpp:1298-1319): delta = after - before
 // on one nx x ny x nz face grid.
 void ref_delta(int nx, int ny, int nz, const float* after, const float* before, float* delta) {

@@ -639,28 +639,41 @@ int oracle_project_subdomain(int ni, int nj, int nk, float h, float dt, const fl
                       nullptr, nullptr, nullptr, iterations_out, residual_out, tol, maxit);
 }
 
+// The RK2 midpoint backtrace shared by SubDomainSolver::advect_field
+// (SS/sub_domain.cpp:210-222) and SmokeSolver3D::advect_field_cubic_clamp
+// (SS/Smoke_solver3D.cpp:682-691): the half step in double, the full step in
+// float.
+static void rk2_backtrace(const Grid* vel, float dt, float wx, float wy, float wz, float p[3]) {
+  float a = vel[0].sample(wx, wy, wz), b = vel[1].sample(wx, wy, wz), c = vel[2].sample(wx, wy, wz);
+  const float px = (float)((double)wx - 0.5 * (double)dt * (double)a);
+  const float py = (float)((double)wy - 0.5 * (double)dt * (double)b);
+  const float pz = (float)((double)wz - 0.5 * (double)dt * (double)c);
+  a = vel[0].sample(px, py, pz);
+  b = vel[1].sample(px, py, pz);
+  c = vel[2].sample(px, py, pz);
+  p[0] = wx - dt * a;
+  p[1] = wy - dt * b;
+  p[2] = wz - dt * c;
+}
+
 // SubDomainSolver::advect_field, SS/sub_domain.cpp:191-235 (RK2 midpoint
 // backtrace, trilinear sample).  Same arguments as ref_advect_rk2.
 void oracle_advect_rk2(int ni, int nj, int nk, float h, float dt, const float* u, const float* v, const float* w,
                        int fnx, int fny, int fnz, double fox, double foy, double foz, const float* field,
                        float* out) {
-  Grid gu{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0};
-  Grid gv{v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0};
-  Grid gw{w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5};
-  Grid gf{field, fnx, fny, fnz, (double)h, fox, foy, foz};
+  const Grid vel[3] = {{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0},
+                       {v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0},
+                       {w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5}};
+  const Grid gf{field, fnx, fny, fnz, (double)h, fox, foy, foz};
   for (int k = 0; k < fnz; ++k)
     for (int j = 0; j < fny; ++j)
       for (int i = 0; i < fnx; ++i) {
-        float wx = (float)(((double)(float)i - fox) * (double)h);
-        float wy = (float)(((double)(float)j - foy) * (double)h);
-        float wz = (float)(((double)(float)k - foz) * (double)h);
-        float a = gu.sample(wx, wy, wz), b = gv.sample(wx, wy, wz), c = gw.sample(wx, wy, wz);
-        float px = (float)((double)wx - 0.5 * (double)dt * (double)a);
-        float py = (float)((double)wy - 0.5 * (double)dt * (double)b);
-        float pz = (float)((double)wz - 0.5 * (double)dt * (double)c);
-        a = gu.sample(px, py, pz); b = gv.sample(px, py, pz); c = gw.sample(px, py, pz);
-        px = wx - dt * a; py = wy - dt * b; pz = wz - dt * c;
-        out[lin(i, j, k, fnx, fny)] = gf.sample(px, py, pz);
+        const float wx = (float)(((double)(float)i - fox) * (double)h);
+        const float wy = (float)(((double)(float)j - foy) * (double)h);
+        const float wz = (float)(((double)(float)k - foz) * (double)h);
+        float p[3];
+        rk2_backtrace(vel, dt, wx, wy, wz, p);
+        out[lin(i, j, k, fnx, fny)] = gf.sample(p[0], p[1], p[2]);
       }
 }
 
@@ -865,6 +878,145 @@ int oracle_reorder_flip(int ni, int nj, int nk, float h, const void* particles, 
     }
   }
   return count <= capacity ? count : -count;
+}
+
+// ---- smoke scalars and the grid advection forms of SmokeSolver3D
+
+// Buffer3D::cubic_interp_weights + cubic_interp, SS/fluid_buffer3D.h:22-38,
+// as Buffer3D<float>::sample_cubic instantiates them: the fraction arrives
+// as a float (T = float), the four weights are formed in float, and the
+// weighted sum of the double values is taken in double, left to right.
+static double cubic_interp(double vm, double v0, double v1, double v2, double t) {
+  const float f = (float)t, f2 = f * f, f3 = f2 * f;
+  const float wm = -(float)(1. / 3) * f + 0.5f * f2 - (float)(1. / 6) * f3;
+  const float w0 = 1.0f - f2 + 0.5f * (f3 - f);
+  const float w1 = f + 0.5f * (f2 - f3);
+  const float w2 = (float)(1. / 6) * (f3 - f);
+  return (double)wm * vm + (double)w0 * v0 + (double)w1 * v1 + (double)w2 * v2;
+}
+
+// Buffer3D::sample_cubic, SS/fluid_buffer3D.h:259-326: sixteen x-rows
+// (z outer, y inner) over the clamped 4x4x4 neighbourhood, then y, then z.
+static float sample_cubic(const Grid& g, double wx, double wy, double wz) {
+  const double gx = wx / g.h + g.ox, gy = wy / g.h + g.oy, gz = wz / g.h + g.oz;
+  const int i = (int)std::floor(gx), j = (int)std::floor(gy), k = (int)std::floor(gz);
+  const double x = gx - (double)i, y = gy - (double)j, z = gz - (double)k;
+  double fz[4];
+  for (int c = 0; c < 4; ++c) {
+    double fy[4];
+    for (int b = 0; b < 4; ++b) {
+      const int jj = j - 1 + b, kk = k - 1 + c;
+      fy[b] = cubic_interp(g.at(i - 1, jj, kk), g.at(i, jj, kk), g.at(i + 1, jj, kk), g.at(i + 2, jj, kk), x);
+    }
+    fz[c] = cubic_interp(fy[0], fy[1], fy[2], fy[3], y);
+  }
+  return (float)cubic_interp(fz[0], fz[1], fz[2], fz[3], z);
+}
+
+// The eight nodes around a point (Buffer3D::sample_cube_lerp,
+// SS/fluid_buffer3D.h:329-356) reduced to their min and max in the
+// reference's nesting order (SS/Smoke_solver3D.cpp:698-699).
+static void corner_range(const Grid& g, double wx, double wy, double wz, float& lo, float& hi) {
+  const int i = (int)std::floor(wx / g.h + g.ox), j = (int)std::floor(wy / g.h + g.oy);
+  const int k = (int)std::floor(wz / g.h + g.oz);
+  const float v[8] = {g.at(i, j, k),         g.at(i + 1, j, k),         g.at(i, j + 1, k),
+                      g.at(i + 1, j + 1, k), g.at(i, j, k + 1),         g.at(i + 1, j, k + 1),
+                      g.at(i, j + 1, k + 1), g.at(i + 1, j + 1, k + 1)};
+  lo = v[0];
+  hi = v[0];
+  for (int c = 1; c < 8; ++c) {
+    lo = std::min(lo, v[c]);
+    hi = std::max(hi, v[c]);
+  }
+}
+
+// SmokeSolver3D::advect_field_cubic_clamp, SS/Smoke_solver3D.cpp:657-707:
+// RK2 backtrace, cubic sample, replaced by the trilinear sample where it
+// reaches or leaves the range of the eight surrounding nodes.  Same
+// arguments as oracle_advect_rk2 (the field has the velocity's spacing h).
+void oracle_advect_cubic_clamp(int ni, int nj, int nk, float h, float dt, const float* u, const float* v,
+                               const float* w, int fnx, int fny, int fnz, double fox, double foy, double foz,
+                               const float* field, float* out) {
+  const Grid vel[3] = {{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0},
+                       {v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0},
+                       {w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5}};
+  const Grid gf{field, fnx, fny, fnz, (double)h, fox, foy, foz};
+  for (int k = 0; k < fnz; ++k)
+    for (int j = 0; j < fny; ++j)
+      for (int i = 0; i < fnx; ++i) {
+        const float wx = (float)(((double)(float)i - fox) * (double)h);
+        const float wy = (float)(((double)(float)j - foy) * (double)h);
+        const float wz = (float)(((double)(float)k - foz) * (double)h);
+        float p[3];
+        rk2_backtrace(vel, dt, wx, wy, wz, p);
+        float lo, hi;
+        corner_range(gf, p[0], p[1], p[2], lo, hi);
+        const float lin_v = gf.sample(p[0], p[1], p[2]);
+        const float cub_v = sample_cubic(gf, p[0], p[1], p[2]);
+        out[lin(i, j, k, fnx, fny)] = (cub_v <= lo || cub_v >= hi) ? lin_v : cub_v;
+      }
+}
+
+// SmokeSolver3D::advect_field, SS/Smoke_solver3D.cpp:564-610: traceRK3 with
+// step -dt from each node, then a trilinear sample.  The field has its own
+// spacing fh (the density and temperature grids are 2ni x 2nj x 2nk at h/2,
+// SS/Smoke_solver3D.h:313-315); node (i,j,k) sits at ((i-fox)fh, ...).
+void oracle_advect_rk3(int ni, int nj, int nk, float h, float dt, const float* u, const float* v, const float* w,
+                       int fnx, int fny, int fnz, double fh, double fox, double foy, double foz, const float* field,
+                       float* out) {
+  const Grid vel[3] = {{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0},
+                       {v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0},
+                       {w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5}};
+  const Grid gf{field, fnx, fny, fnz, fh, fox, foy, foz};
+  for (int k = 0; k < fnz; ++k)
+    for (int j = 0; j < fny; ++j)
+      for (int i = 0; i < fnx; ++i) {
+        const float pos[3] = {(float)(((double)(float)i - fox) * fh), (float)(((double)(float)j - foy) * fh),
+                              (float)(((double)(float)k - foz) * fh)};
+        float back[3];
+        trace_rk3(vel, pos, -dt, back);
+        out[lin(i, j, k, fnx, fny)] = gf.sample(back[0], back[1], back[2]);
+      }
+}
+
+// SmokeSolver3D::gen_heat, SS/Smoke_solver3D.cpp:1624-1650: decay density and
+// temperature, then set both inside the source: a vertical cylinder of
+// radius r about (cx, cz) (float distance) whose height is |y - cy| <= r/4
+// (compared in double).  Node (i,j,k) sits at (i,j,k)*fh in float.
+void oracle_gen_heat(int fnx, int fny, int fnz, double fh, float dt, float dens_decay, float temp_decay, float cx,
+                     float cy, float cz, float radius, float dens, float heat, float* rho, float* temp) {
+  const float hf = (float)fh;
+  for (int k = 0; k < fnz; ++k)
+    for (int j = 0; j < fny; ++j)
+      for (int i = 0; i < fnx; ++i) {
+        const size_t q = lin(i, j, k, fnx, fny);
+        rho[q] = rho[q] / (1.0f + dens_decay * dt);
+        temp[q] = temp[q] / (1.0f + temp_decay * dt);
+        const float px = (float)i * hf, py = (float)j * hf, pz = (float)k * hf;
+        const float dx = px - cx, dz = pz - cz;
+        const float d = std::sqrt(dx * dx + dz * dz);
+        if (d <= radius && (double)std::fabs(py - cy) <= 0.25 * (double)radius) {
+          rho[q] = dens;
+          temp[q] = heat;
+        }
+      }
+}
+
+// SmokeSolver3D::add_smokeforce, SS/Smoke_solver3D.cpp:1652-1668: each
+// particle's y velocity gains dt (-alpha rho + beta T), rho and T sampled
+// trilinearly from the fnx x fny x fnz grids of spacing fh (offsets 0).
+void oracle_add_smokeforce(void* particles, int np, int fnx, int fny, int fnz, double fh, const float* rho,
+                           const float* temp, float alpha, float beta, float dt) {
+  Particle* p = (Particle*)particles;
+  const Grid gr{rho, fnx, fny, fnz, fh, 0.0, 0.0, 0.0}, gt{temp, fnx, fny, fnz, fh, 0.0, 0.0, 0.0};
+  for (int q = 0; q < np; ++q) {
+    const float r = gr.sample(p[q].pos[0], p[q].pos[1], p[q].pos[2]);
+    const float t = gt.sample(p[q].pos[0], p[q].pos[1], p[q].pos[2]);
+    const float fy = dt * (-alpha * r + beta * t);
+    p[q].vel[0] += 0.0f;  // Vec3f(0, fy, 0) is added to all three components
+    p[q].vel[1] += fy;
+    p[q].vel[2] += 0.0f;
+  }
 }
 
 // SmokeSolver3D::getDelta, SS/Smoke_solver3D.cpp:1298-1319.

@@ -3,7 +3,8 @@
 reference's OWN code (oracle/_ref/libvflip_ref.so, compiled from the vFLIP
 sources by oracle/build_ref.py) on small seeded inputs.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py smoke      # only smoke.npz
 
 Each fixture (.npz) stores its inputs and the reference's outputs, so the
 tests need neither the reference tree nor its library: they check the
@@ -23,10 +24,45 @@ from vflip_b200 import scenes  # noqa: E402
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 
-def main():
+def make_smoke(R):
+    """The grid advection forms of SmokeSolver3D and the smoke scalars:
+    advect_field_cubic_clamp on the four grid kinds, advect_field (RK3) of
+    density and temperature on the 2x grid at h/2, gen_heat, add_smokeforce."""
+    rng = np.random.default_rng(31)
+    ni, nj, nk = 12, 10, 9
+    h = np.float32(1 / 12)  # not a power of two: exercises the true division
+    dt = np.float32(0.06)
+    u, v, w = scenes.random_velocity(ni, nj, nk, rng, scale=3.0)
+    out = {}
+    for name, offs, shape in (("u", (0.5, 0, 0), (nk, nj, ni + 1)), ("v", (0, 0.5, 0), (nk, nj + 1, ni)),
+                              ("w", (0, 0, 0.5), (nk + 1, nj, ni)), ("c", (0, 0, 0), (nk, nj, ni))):
+        f = rng.standard_normal(shape).astype(np.float32)
+        out["cubic_in_" + name] = f
+        out["cubic_out_" + name] = R.advect_cubic_clamp(ni, nj, nk, h, dt, u, v, w, f, offs)
+    fh = float(h) / 2
+    rho = rng.random((2 * nk, 2 * nj, 2 * ni)).astype(np.float32)
+    temp = rng.random((2 * nk, 2 * nj, 2 * ni)).astype(np.float32)
+    out["rk3_rho"] = R.advect_rk3(ni, nj, nk, h, dt, u, v, w, rho, fh)
+    out["rk3_temp"] = R.advect_rk3(ni, nj, nk, h, dt, u, v, w, temp, fh)
+    heat = dict(dt=0.06, dens_decay=0.1, temp_decay=0.3, centre=(0.5, 0.12, 0.45), radius=0.2, dens=1.0, heat=4.0)
+    out["heat_rho"], out["heat_temp"] = R.gen_heat(out["rk3_rho"], out["rk3_temp"], fh, **heat)
+    p = scenes.random_particles(ni, nj, nk, h, 3000, rng, margin=1.5)
+    out["force_particles"] = R.add_smokeforce(p, out["heat_rho"], out["heat_temp"], fh, 0.1, 0.35, 0.06).view(np.uint8)
+    np.savez_compressed(os.path.join(OUT, "smoke.npz"), dims=np.array([ni, nj, nk], np.int32), h=h, dt=dt, u=u, v=v,
+                        w=w, rho=rho, temp=temp, particles=p.view(np.uint8),
+                        heat_params=np.array([heat["dt"], heat["dens_decay"], heat["temp_decay"], *heat["centre"],
+                                              heat["radius"], heat["dens"], heat["heat"]], np.float32),
+                        force_params=np.array([0.1, 0.35, 0.06], np.float32), **out)
+
+
+def main(which=()):
     R = oracle.reference()
     if R is None:
         sys.exit("oracle/_ref/libvflip_ref.so is not built (python oracle/build_ref.py)")
+    if which:
+        if "smoke" in which:
+            make_smoke(R)
+        return
     # 1. projection (face weights, inflow, assembly, AMGPCG 1e-6/50, gradient)
     #    on odd, non-cubic grids with inflow and moving solids
     for tag, (ni, nj, nk), seed in (("proj_a", (14, 12, 11), 11), ("proj_b", (19, 17, 23), 12)):
@@ -87,10 +123,11 @@ def main():
     g = R.g2p(ni, nj, nk, h, p, du, dv, dw)
     np.savez_compressed(os.path.join(OUT, "transfer.npz"), dims=np.array([ni, nj, nk], np.int32), h=h,
                         particles=p.view(np.uint8), du=du, dv=dv, dw=dw, g2p=g.view(np.uint8), **out)
+    make_smoke(R)
     for fn in sorted(os.listdir(OUT)):
         if fn.endswith(".npz"):
             print(fn, os.path.getsize(os.path.join(OUT, fn)))
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

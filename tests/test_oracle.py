@@ -243,3 +243,82 @@ def test_reorder_flip_seeding_structure_matches_reference(orc, ref):
     assert np.array_equal(ha[sure], hb[sure])
     new = a[a["temp"] == 0]
     assert len(new) > 0 and (new["dens"] == 0).all()
+
+
+# ---- grid advection forms of SmokeSolver3D and the smoke scalars
+
+CUBIC_GRIDS = (("u", (0.5, 0, 0)), ("v", (0, 0.5, 0)), ("w", (0, 0, 0.5)), ("c", (0, 0, 0)))
+
+
+def _cubic_shape(name, ni, nj, nk):
+    return {"u": (nk, nj, ni + 1), "v": (nk, nj + 1, ni), "w": (nk + 1, nj, ni), "c": (nk, nj, ni)}[name]
+
+
+def test_smoke_golden(orc):
+    """advect_field_cubic_clamp on the four grid kinds, advect_field (RK3) on
+    the 2x density/temperature grid, gen_heat and add_smokeforce: the oracle
+    reproduces the reference's fixture bit for bit."""
+    from vflip_b200.particles import PARTICLE_DTYPE
+
+    g = golden("smoke")
+    ni, nj, nk = (int(x) for x in g["dims"])
+    h, dt = float(g["h"]), float(g["dt"])
+    for name, offs in CUBIC_GRIDS:
+        same(orc.advect_cubic_clamp(ni, nj, nk, h, dt, g["u"], g["v"], g["w"], g["cubic_in_" + name], offs),
+             g["cubic_out_" + name])
+    fh = h / 2
+    same(orc.advect_rk3(ni, nj, nk, h, dt, g["u"], g["v"], g["w"], g["rho"], fh), g["rk3_rho"])
+    same(orc.advect_rk3(ni, nj, nk, h, dt, g["u"], g["v"], g["w"], g["temp"], fh), g["rk3_temp"])
+    hp = [float(x) for x in g["heat_params"]]
+    r, t = orc.gen_heat(g["rk3_rho"], g["rk3_temp"], fh, hp[0], hp[1], hp[2], hp[3:6], hp[6], hp[7], hp[8])
+    same(r, g["heat_rho"])
+    same(t, g["heat_temp"])
+    assert (r == hp[7]).sum() > 0  # the source covers some nodes
+    fp = [float(x) for x in g["force_params"]]
+    p = g["particles"].view(PARTICLE_DTYPE)
+    same(orc.add_smokeforce(p, r, t, fh, *fp).view(np.uint8), g["force_particles"])
+
+
+@pytest.mark.parametrize("dims,h,dt", [((13, 11, 9), 1 / 13, 0.07), ((16, 16, 16), 1 / 16, 0.04),
+                                       ((7, 9, 5), 1 / 9, 0.0)])
+def test_cubic_clamp_vs_reference(orc, ref, dims, h, dt):
+    """Both branches of the clamp occur (cubic kept inside the corner range,
+    trilinear where it overshoots), and the oracle equals the reference."""
+    ni, nj, nk = dims
+    h = np.float32(h)
+    rng = np.random.default_rng(41)
+    u, v, w = scenes.random_velocity(ni, nj, nk, rng, scale=3.0)
+    for name, offs in CUBIC_GRIDS:
+        f = rng.standard_normal(_cubic_shape(name, ni, nj, nk)).astype(np.float32)
+        a = orc.advect_cubic_clamp(ni, nj, nk, h, dt, u, v, w, f, offs)
+        same(a, ref.advect_cubic_clamp(ni, nj, nk, h, dt, u, v, w, f, offs))
+        if dt > 0:
+            lin = orc.advect_rk2(ni, nj, nk, h, dt, u, v, w, f, offs)
+            picked_linear = (a == lin).mean()
+            assert 0.005 < picked_linear < 0.995, picked_linear
+        else:
+            # no motion: every node samples itself, up to the rounding of
+            # the node's world position and back
+            assert np.allclose(a, f, rtol=0, atol=2e-6)
+
+
+@pytest.mark.parametrize("dims,scale", [((12, 10, 9), 2.0), ((8, 8, 8), 0.0)])
+def test_rk3_and_smoke_scalars_vs_reference(orc, ref, dims, scale):
+    ni, nj, nk = dims
+    h = np.float32(1 / 16)
+    rng = np.random.default_rng(43)
+    u, v, w = scenes.random_velocity(ni, nj, nk, rng, scale=scale)
+    fh = float(h) / 2
+    rho = rng.random((2 * nk, 2 * nj, 2 * ni)).astype(np.float32)
+    same(orc.advect_rk3(ni, nj, nk, h, 0.05, u, v, w, rho, fh), ref.advect_rk3(ni, nj, nk, h, 0.05, u, v, w, rho, fh))
+    # a face-offset grid at the velocity's own spacing
+    f = rng.standard_normal((nk, nj, ni + 1)).astype(np.float32)
+    same(orc.advect_rk3(ni, nj, nk, h, 0.05, u, v, w, f, float(h), (0.5, 0, 0)),
+         ref.advect_rk3(ni, nj, nk, h, 0.05, u, v, w, f, float(h), (0.5, 0, 0)))
+    temp = rng.random(rho.shape).astype(np.float32)
+    args = (fh, 0.02, 0.05, 0.25, (0.4, 0.1, 0.6), 0.15, 0.8, 2.5)
+    for x, y in zip(orc.gen_heat(rho, temp, *args), ref.gen_heat(rho, temp, *args)):
+        same(x, y)
+    p = scenes.random_particles(ni, nj, nk, h, 2000, rng, margin=1.5)
+    same(orc.add_smokeforce(p, rho, temp, fh, 0.2, 0.4, 0.05).view(np.uint8),
+         ref.add_smokeforce(p, rho, temp, fh, 0.2, 0.4, 0.05).view(np.uint8))

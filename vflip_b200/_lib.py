@@ -66,6 +66,13 @@ SIGNATURES = {
                                      C.POINTER(SolveStatsC)]),
     "vflip_advect_rk2_linear": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _P, _P]),
     "vflip_advect_rk2_linear2": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _P, _P, _P, _P]),
+    "vflip_advect_cubic_clamp": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _P, _P]),
+    "vflip_advect_velocity_cubic_clamp": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P]),
+    "vflip_advect_rk3_linear": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _D, _P, _P]),
+    "vflip_advect_rk3_linear2": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _D, _P, _P, _P,
+                                      _P]),
+    "vflip_gen_heat": (_I, [_P, _I, _I, _I, _D, _F, _F, _F, _F, _F, _F, _F, _F, _F, _P, _P]),
+    "vflip_add_smokeforce": (_I, [_P, _P, _I, _I, _I, _I, _D, _P, _P, _F, _F, _F]),
     "vflip_delta": (_I, [_P, _SZ, _P, _P, _P]),
     "vflip_particle_cells": (_I, [_P, _I, _I, _I, _F, _P, _I, _P]),
     "vflip_p2g": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _P, _P]),

@@ -25,6 +25,7 @@
 #include "plume_kernels.cuh"
 #include "projection_kernels.cuh"
 #include "transfer_kernels.cuh"
+#include "smoke_kernels.cuh"
 #include "learned_kernels.cuh"
 #include "smoother3d.cuh"
 #include "tmap.h"
@@ -1923,6 +1924,130 @@ int vflip_advect_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, flo
                             double oz, const float* field, float* out) {
   return vflip_advect_rk2_linear2(ctx, ni, nj, nk, h, dt, u, v, w, fnx, fny, fnz, ox, oy, oz, field, out, nullptr,
                                   nullptr);
+}
+
+namespace {
+// The three MAC velocity views of an ni x nj x nk grid of spacing h.
+void velocity_views(const float* u, const float* v, const float* w, int ni, int nj, int nk, float h, GridView& gu,
+                    GridView& gv, GridView& gw) {
+  const double ih = inv_pow2(h);
+  gu = GridView{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0, ih};
+  gv = GridView{v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0, ih};
+  gw = GridView{w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5, ih};
+}
+
+int launch_cubic_clamp(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u, const float* v,
+                       const float* w, const CubicFields& job, int nfields) {
+  GridView gu, gv, gw;
+  velocity_views(u, v, w, ni, nj, nk, h, gu, gv, gw);
+  size_t most = 0;
+  for (int f = 0; f < nfields; ++f) most = std::max(most, (size_t)job.f[f].nx * job.f[f].ny * job.f[f].nz);
+  const int per_block = 256 * 4;
+  const dim3 grid((unsigned)((most + per_block - 1) / per_block), (unsigned)nfields);
+  if (ctx->cfg.precision == VFLIP_PREC_FP64)
+    advect_cubic_clamp_kernel<true><<<grid, 256, 0, ctx->stream>>>(gu, gv, gw, job, h, dt, per_block);
+  else
+    advect_cubic_clamp_kernel<false><<<grid, 256, 0, ctx->stream>>>(gu, gv, gw, job, h, dt, per_block);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+}  // namespace
+
+int vflip_advect_cubic_clamp(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                             const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
+                             double oz, const float* field, float* out) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (fnx <= 0 || fny <= 0 || fnz <= 0 || !u || !v || !w || !field || !out)
+    return ctx->fail(VFLIP_ERR_ARG, "bad argument");
+  if ((size_t)fnx * fny * fnz >= (1ull << 31)) return ctx->fail(VFLIP_ERR_ARG, "field too large");
+  if (out == field || out == u || out == v || out == w) return ctx->fail(VFLIP_ERR_ARG, "out aliases an input");
+  CubicFields job{};
+  job.f[0] = GridView{field, fnx, fny, fnz, (double)h, ox, oy, oz, inv_pow2(h)};
+  job.out[0] = out;
+  return launch_cubic_clamp(ctx, ni, nj, nk, h, dt, u, v, w, job, 1);
+}
+
+int vflip_advect_velocity_cubic_clamp(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                                      const float* v, const float* w, float* u_out, float* v_out, float* w_out) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (!u || !v || !w || !u_out || !v_out || !w_out) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  const float* ins[3] = {u, v, w};
+  float* outs[3] = {u_out, v_out, w_out};
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      if (outs[a] == ins[b] || (a != b && outs[a] == outs[b]))
+        return ctx->fail(VFLIP_ERR_ARG, "outputs alias the velocity or each other");
+  CubicFields job{};
+  velocity_views(u, v, w, ni, nj, nk, h, job.f[0], job.f[1], job.f[2]);
+  for (int a = 0; a < 3; ++a) job.out[a] = outs[a];
+  return launch_cubic_clamp(ctx, ni, nj, nk, h, dt, u, v, w, job, 3);
+}
+
+int vflip_advect_rk3_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                             const float* v, const float* w, int fnx, int fny, int fnz, double fh, double ox,
+                             double oy, double oz, const float* field, float* out, const float* field2,
+                             float* out2) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (fnx <= 0 || fny <= 0 || fnz <= 0 || !(fh > 0) || !u || !v || !w || !field || !out)
+    return ctx->fail(VFLIP_ERR_ARG, "bad argument");
+  if ((size_t)fnx * fny * fnz >= (1ull << 31)) return ctx->fail(VFLIP_ERR_ARG, "field too large");
+  if (out == field || out == u || out == v || out == w) return ctx->fail(VFLIP_ERR_ARG, "out aliases an input");
+  if (field2 && (!out2 || out2 == field2 || out2 == field || out2 == out || out2 == u || out2 == v || out2 == w ||
+                 out == field2))
+    return ctx->fail(VFLIP_ERR_ARG, "second output missing or aliased");
+  GridView gu, gv, gw;
+  velocity_views(u, v, w, ni, nj, nk, h, gu, gv, gw);
+  const double ih = inv_pow2(fh);
+  GridView gf{field, fnx, fny, fnz, fh, ox, oy, oz, ih};
+  GridView gf2{field2, fnx, fny, fnz, fh, ox, oy, oz, ih};
+  const size_t n = (size_t)fnx * fny * fnz;
+  const int per_block = 256 * 4;
+  const unsigned blocks = (unsigned)((n + per_block - 1) / per_block);
+  float* o2 = field2 ? out2 : nullptr;
+  if (ctx->cfg.precision == VFLIP_PREC_FP64)
+    advect_rk3_kernel<true><<<blocks, 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2, o2, dt, per_block);
+  else
+    advect_rk3_kernel<false><<<blocks, 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2, o2, dt, per_block);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+int vflip_advect_rk3_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                            const float* v, const float* w, int fnx, int fny, int fnz, double fh, double ox,
+                            double oy, double oz, const float* field, float* out) {
+  return vflip_advect_rk3_linear2(ctx, ni, nj, nk, h, dt, u, v, w, fnx, fny, fnz, fh, ox, oy, oz, field, out,
+                                  nullptr, nullptr);
+}
+
+int vflip_gen_heat(vflip_ctx* ctx, int fnx, int fny, int fnz, double fh, float dt, float dens_decay,
+                   float temp_decay, float cx, float cy, float cz, float radius, float dens, float heat, float* rho,
+                   float* temp) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  if (fnx <= 0 || fny <= 0 || fnz <= 0 || !(fh > 0) || !rho || !temp || rho == temp)
+    return ctx->fail(VFLIP_ERR_ARG, "bad argument");
+  const size_t n = (size_t)fnx * fny * fnz;
+  HeatSource s{dt, dens_decay, temp_decay, cx, cy, cz, radius, dens, heat};
+  gen_heat_kernel<<<grid_for(n, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(rho, temp, fnx, fny, fnz, (float)fh,
+                                                                              s);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+int vflip_add_smokeforce(vflip_ctx* ctx, void* particles, int np, int fnx, int fny, int fnz, double fh,
+                         const float* rho, const float* temp, float alpha, float beta, float dt) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  if (np < 0 || (np > 0 && !particles) || fnx <= 0 || fny <= 0 || fnz <= 0 || !(fh > 0) || !rho || !temp)
+    return ctx->fail(VFLIP_ERR_ARG, "bad argument");
+  if (np == 0) return VFLIP_OK;
+  const double ih = inv_pow2(fh);
+  GridView gr{rho, fnx, fny, fnz, fh, 0.0, 0.0, 0.0, ih}, gt{temp, fnx, fny, fnz, fh, 0.0, 0.0, 0.0, ih};
+  add_smokeforce_kernel<<<grid_for(np, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>((ParticleRec*)particles, np,
+                                                                                     gr, gt, alpha, beta, dt);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
 }
 
 int vflip_delta(vflip_ctx* ctx, size_t n, const float* after, const float* before, float* delta) {

@@ -293,6 +293,52 @@ class Solver:
                                                       float(offsets[2]), _p(field), _p(out), _p(field2), _p(out2)))
         return out, out2
 
+    def advect_cubic_clamp(self, ni, nj, nk, h, dt, u, v, w, field, offsets, out=None):
+        """SmokeSolver3D::advect_field_cubic_clamp of one field."""
+        fnz, fny, fnx = field.shape
+        if out is None:
+            out = torch.empty_like(field)
+        self._check(self.lib.vflip_advect_cubic_clamp(self.ctx, ni, nj, nk, float(h), float(dt), _p(u), _p(v), _p(w),
+                                                      fnx, fny, fnz, float(offsets[0]), float(offsets[1]),
+                                                      float(offsets[2]), _p(field), _p(out)))
+        return out
+
+    def advect_velocity_cubic_clamp(self, ni, nj, nk, h, dt, u, v, w, outs=None):
+        """SmokeSolver3D::advect: (u, v, w) advected by themselves, one launch."""
+        outs = tuple(torch.empty_like(a) for a in (u, v, w)) if outs is None else outs
+        self._check(self.lib.vflip_advect_velocity_cubic_clamp(self.ctx, ni, nj, nk, float(h), float(dt), _p(u),
+                                                               _p(v), _p(w), *[_p(o) for o in outs]))
+        return outs
+
+    def advect_rk3_linear(self, ni, nj, nk, h, dt, u, v, w, field, fh, offsets=(0.0, 0.0, 0.0), field2=None,
+                          out=None, out2=None):
+        """SmokeSolver3D::advect_field: RK3 backtrace, trilinear sample of a
+        field of spacing fh (h/2 for the density/temperature grids); a second
+        field on the same grid shares the backtrace."""
+        fnz, fny, fnx = field.shape
+        out = torch.empty_like(field) if out is None else out
+        if field2 is not None and out2 is None:
+            out2 = torch.empty_like(field2)
+        self._check(self.lib.vflip_advect_rk3_linear2(self.ctx, ni, nj, nk, float(h), float(dt), _p(u), _p(v), _p(w),
+                                                      fnx, fny, fnz, float(fh), float(offsets[0]), float(offsets[1]),
+                                                      float(offsets[2]), _p(field), _p(out),
+                                                      _p(field2) if field2 is not None else None,
+                                                      _p(out2) if field2 is not None else None))
+        return out if field2 is None else (out, out2)
+
+    def gen_heat(self, rho, temp, fh, dt, dens_decay, temp_decay, centre, radius, dens, heat):
+        """SmokeSolver3D::gen_heat, in place on the density/temperature grids."""
+        fnz, fny, fnx = rho.shape
+        self._check(self.lib.vflip_gen_heat(self.ctx, fnx, fny, fnz, float(fh), float(dt), float(dens_decay),
+                                            float(temp_decay), float(centre[0]), float(centre[1]), float(centre[2]),
+                                            float(radius), float(dens), float(heat), _p(rho), _p(temp)))
+
+    def add_smokeforce(self, particles, rho, temp, fh, alpha, beta, dt):
+        """SmokeSolver3D::add_smokeforce, in place on the particles."""
+        fnz, fny, fnx = rho.shape
+        self._check(self.lib.vflip_add_smokeforce(self.ctx, _p(particles), self._np(particles), fnx, fny, fnz,
+                                                  float(fh), _p(rho), _p(temp), float(alpha), float(beta), float(dt)))
+
     def delta(self, after, before, out=None):
         if out is None:
             out = torch.empty_like(after)
