@@ -244,6 +244,7 @@ def run_vflip(a):
             out["batched"] = batched_arm(solver)
         if not a.no_flip and world == 1:
             out["flip"] = flip_arm(solver, a.steps)
+            out["advection_forms"] = advection_arm(solver)
     solver.close()
     if world > 1:
         dist.destroy_process_group()
@@ -321,10 +322,84 @@ def flip_arm(solver, steps, n=128, warmup=3):
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    return {"grid": n, "steps_per_s": steps / (ms * 1e-3), "ms_per_step": ms / steps,
-            "particles": sim.num_particles, "particles_at_start": np0,
-            "particle_steps_per_s": sim.num_particles * steps / (ms * 1e-3),
-            "pcg_iterations_mean": sum(iters) / len(iters)}
+    out = {"grid": n, "steps_per_s": steps / (ms * 1e-3), "ms_per_step": ms / steps,
+           "particles": sim.num_particles, "particles_at_start": np0,
+           "particle_steps_per_s": sim.num_particles * steps / (ms * 1e-3),
+           "pcg_iterations_mean": sum(iters) / len(iters)}
+    del sim
+    # the same scene with density/temperature on the 256^3 grid at h/2 (RK3
+    # advection, gen_heat, buoyancy on the particles) inside every step
+    sim = FlipSim(solver, FlipParams(n=n, smoke=True, alpha=0.1, beta=1.0))
+    for _ in range(warmup):
+        sim.step()
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        sim.step()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["with_smoke_scalars"] = {"steps_per_s": steps / (ms * 1e-3), "ms_per_step": ms / steps,
+                                 "scalar_grid": 2 * n, "particles": sim.num_particles}
+    return out
+
+
+def advection_arm(solver, n=128, reps=20):
+    """The grid advection forms and smoke scalars at the FLIP scene's size:
+    SmokeSolver3D::advect (cubic-clamped u, v, w of a 128^3 MAC grid, one
+    launch), advect_field (RK3) of density and temperature on their 256^3
+    grid at h/2 (one shared backtrace) and gen_heat on that grid, each timed
+    with CUDA events on the library's stream (median of `reps` after 3
+    warm-ups), in the solver's precision.  Algorithmic bytes: every output
+    node reads its field value and writes one float (8 B), the velocity
+    (read once) adds 4 B per face; the gathers behind each node (2 x 3
+    trilinear velocity samples + 64 cubic nodes, or 3 x 3 + 2 trilinear
+    samples) hit L1/L2, so these kernels are bound by load issue, not HBM."""
+    import numpy as np
+    import torch
+
+    from vflip_b200 import scenes
+
+    rng = np.random.default_rng(0)
+    h = float(np.float32(1.0 / n))
+    u, v, w = [torch.from_numpy(x).cuda() for x in scenes.random_velocity(n, n, n, rng, scale=1.0)]
+    rho = torch.rand((2 * n,) * 3, device="cuda")
+    temp = torch.rand_like(rho)
+    r2, t2 = torch.empty_like(rho), torch.empty_like(rho)
+    outs = tuple(torch.empty_like(x) for x in (u, v, w))
+
+    def med(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    peak, _ = measured_peaks()
+    faces = 3 * (n + 1) * n * n
+    nodes2 = (2 * n) ** 3
+    res = {}
+    for name, fn, nodes, alg in (
+            ("velocity_cubic_clamp", lambda: solver.advect_velocity_cubic_clamp(n, n, n, h, 0.01, u, v, w, outs=outs),
+             faces, 8 * faces),
+            ("rk3_density_temperature", lambda: solver.advect_rk3_linear(n, n, n, h, 0.01, u, v, w, rho, h / 2,
+                                                                         field2=temp, out=r2, out2=t2),
+             nodes2, 16 * nodes2 + 4 * faces),
+            ("gen_heat", lambda: solver.gen_heat(rho, temp, h / 2, 0.01, 0.1, 0.1, (0.5, 0.1, 0.5), 0.12, 1.0, 1.0),
+             nodes2, 16 * nodes2)):
+        ms = med(fn)
+        gbs = alg / (ms * 1e-3) / 1e9
+        res[name] = {"ms": ms, "nodes": nodes, "gnodes_per_s": nodes / (ms * 1e-3) / 1e9, "alg_bytes": alg,
+                     "achieved_gbs": gbs, "hbm_frac": gbs / peak if peak else None}
+    res["grid"] = n
+    return res
 
 
 def batched_arm(solver, count=32, reps=2):

@@ -141,8 +141,9 @@ __device__ __forceinline__ void rk2_backtrace(const GridView& u, const GridView&
 
 // Node (i,j,k) of a grid at world ((i-ox)h, (j-oy)h, (k-oz)h), rounded to
 // float from double as `((float)i - field._ox) * _hx` is.
-__device__ __forceinline__ void node_world_d(const GridView& f, size_t e, double h, float p[3]) {
-  const int i = (int)(e % f.nx), j = (int)((e / f.nx) % f.ny), k = (int)(e / ((size_t)f.nx * f.ny));
+__device__ __forceinline__ void node_world_d(const GridView& f, unsigned e, double h, float p[3]) {
+  const unsigned row = e / (unsigned)f.nx;
+  const int i = (int)(e - row * (unsigned)f.nx), j = (int)(row % (unsigned)f.ny), k = (int)(row / (unsigned)f.ny);
   p[0] = (float)(((double)(float)i - f.ox) * h);
   p[1] = (float)(((double)(float)j - f.oy) * h);
   p[2] = (float)(((double)(float)k - f.oz) * h);
@@ -161,11 +162,11 @@ __global__ void __launch_bounds__(256) advect_cubic_clamp_kernel(GridView u, Gri
                                                                  float h, float dt, int per_block) {
   const GridView& f = job.f[blockIdx.y];
   float* __restrict__ out = job.out[blockIdx.y];
-  const size_t n = (size_t)f.nx * f.ny * f.nz;
-  const size_t beg = (size_t)blockIdx.x * per_block;
+  const unsigned n = (unsigned)f.nx * f.ny * f.nz;  // < 2^31, checked by the host
+  const unsigned beg = blockIdx.x * (unsigned)per_block;
   if (beg >= n) return;
-  const size_t end = beg + per_block < n ? beg + per_block : n;
-  for (size_t e = beg + threadIdx.x; e < end; e += blockDim.x) {
+  const unsigned end = n - beg > (unsigned)per_block ? beg + per_block : n;
+  for (unsigned e = beg + threadIdx.x; e < end; e += blockDim.x) {
     float wp[3], p[3];
     node_world_d(f, e, (double)h, wp);
     rk2_backtrace<EXACT>(u, v, w, dt, wp[0], wp[1], wp[2], p);
@@ -197,10 +198,10 @@ template <bool EXACT>
 __global__ void __launch_bounds__(256) advect_rk3_kernel(GridView u, GridView v, GridView w, GridView f,
                                                          float* __restrict__ out, GridView f2,
                                                          float* __restrict__ out2, float dt, int per_block) {
-  const size_t n = (size_t)f.nx * f.ny * f.nz;
-  const size_t beg = (size_t)blockIdx.x * per_block;
-  const size_t end = beg + per_block < n ? beg + per_block : n;
-  for (size_t e = beg + threadIdx.x; e < end; e += blockDim.x) {
+  const unsigned n = (unsigned)f.nx * f.ny * f.nz;  // < 2^31, checked by the host
+  const unsigned beg = blockIdx.x * (unsigned)per_block;
+  const unsigned end = n - beg > (unsigned)per_block ? beg + per_block : n;
+  for (unsigned e = beg + threadIdx.x; e < end; e += blockDim.x) {
     float p[3], b[3];
     node_world_d(f, e, f.h, p);
     if constexpr (EXACT) {
@@ -220,13 +221,15 @@ struct HeatSource {
   float dt, dens_decay, temp_decay, cx, cy, cz, radius, dens, heat;
 };
 
+// 32-bit index arithmetic (the host checks nx*ny*nz < 2^31).
 __global__ void gen_heat_kernel(float* __restrict__ rho, float* __restrict__ temp, int nx, int ny, int nz, float hf,
                                 HeatSource s) {
-  const size_t n = (size_t)nx * ny * nz;
+  const unsigned n = (unsigned)nx * ny * nz;
   const float dr = 1.0f + s.dens_decay * s.dt, dtm = 1.0f + s.temp_decay * s.dt;
   const double band = 0.25 * (double)s.radius;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(e % nx), j = (int)((e / nx) % ny), k = (int)(e / ((size_t)nx * ny));
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const unsigned row = e / (unsigned)nx;
+    const int i = (int)(e - row * (unsigned)nx), j = (int)(row % (unsigned)ny), k = (int)(row / (unsigned)ny);
     float r = __fdiv_rn(rho[e], dr), t = __fdiv_rn(temp[e], dtm);
     const float dx = (float)i * hf - s.cx, dz = (float)k * hf - s.cz;
     const float d = __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dz, dz)));

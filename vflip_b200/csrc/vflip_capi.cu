@@ -2029,6 +2029,7 @@ int vflip_gen_heat(vflip_ctx* ctx, int fnx, int fny, int fnz, double fh, float d
   if (fnx <= 0 || fny <= 0 || fnz <= 0 || !(fh > 0) || !rho || !temp || rho == temp)
     return ctx->fail(VFLIP_ERR_ARG, "bad argument");
   const size_t n = (size_t)fnx * fny * fnz;
+  if (n >= (1ull << 31)) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
   HeatSource s{dt, dens_decay, temp_decay, cx, cy, cz, radius, dens, heat};
   gen_heat_kernel<<<grid_for(n, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(rho, temp, fnx, fny, fnz, (float)fh,
                                                                               s);

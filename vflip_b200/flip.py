@@ -12,6 +12,12 @@ One step, in the reference's order:
      (vflip_delta, vflip_g2p);
   6. reorder_FLIP: 8 particles per open cell (vflip_reorder_flip).
 The particle state (40-byte records) stays on the device.
+
+With ``smoke=True`` the density/temperature block of time_step
+(Smoke_solver3D.cpp:353-369) runs between steps 1 and 2: advect_field (RK3)
+of density and temperature on their 2n^3 grid at h/2 along one shared
+backtrace (vflip_advect_rk3_linear2), gen_heat (vflip_gen_heat) and the
+buoyancy add_smokeforce on the particles (vflip_add_smokeforce).
 """
 from dataclasses import dataclass
 
@@ -36,6 +42,17 @@ class FlipParams:
     tol: float = 1e-6
     max_iterations: int = 50
     seed: int = 0
+    # density/temperature on the doubled grid (SmokeSolver3D::gen_heat and
+    # add_smokeforce parameters, Smoke_solver3D.h:165-170)
+    smoke: bool = False
+    smoke_centre: tuple = (0.5, 0.1, 0.5)
+    smoke_radius: float = 0.12
+    smoke_dens: float = 1.0
+    smoke_heat: float = 1.0
+    dens_decay: float = 0.0
+    temp_decay: float = 0.0
+    alpha: float = 0.0
+    beta: float = 1.0
 
     @property
     def h(self):
@@ -66,6 +83,11 @@ class FlipSim:
         c = params.source_centre
         d2 = (i * h - c[0]) ** 2 + ((j - 0.5) * h - c[1]) ** 2 + (k * h - c[2]) ** 2
         self.source_v = torch.from_numpy(d2 <= params.source_radius ** 2).to(dev)
+        if params.smoke:
+            self.rho = torch.zeros((2 * n,) * 3, dtype=torch.float32, device=dev)
+            self.temp = torch.zeros_like(self.rho)
+            self._rho2 = torch.empty_like(self.rho)
+            self._temp2 = torch.empty_like(self.rho)
         self.steps = 0
         self.last = None
 
@@ -80,6 +102,8 @@ class FlipSim:
         p, s, n, h = self.p, self.s, self.p.n, self.p.h
         u, v, w = self.vel
         s.advect_flip(n, n, n, h, self.particles, u, v, w, self.phi, p.dt)
+        if p.smoke:
+            self.smoke_scalars(u, v, w)
         outs = s.particle_to_grid(n, n, n, h, self.particles)
         un, vn, wn = outs[0][0], outs[1][0], outs[2][0]
         vn.masked_fill_(self.source_v, p.inflow)
@@ -93,3 +117,16 @@ class FlipSim:
         self.steps += 1
         self.last = stats
         return conv, stats
+
+    def smoke_scalars(self, u, v, w):
+        """advect_field of density and temperature, gen_heat, add_smokeforce
+        (Smoke_solver3D.cpp:358-369) through the grid velocity u, v, w."""
+        p, s, n = self.p, self.s, self.p.n
+        fh = self.p.h / 2
+        s.advect_rk3_linear(n, n, n, p.h, p.dt, u, v, w, self.rho, fh, field2=self.temp, out=self._rho2,
+                            out2=self._temp2)
+        self.rho, self._rho2 = self._rho2, self.rho
+        self.temp, self._temp2 = self._temp2, self.temp
+        s.gen_heat(self.rho, self.temp, fh, p.dt, p.dens_decay, p.temp_decay, p.smoke_centre, p.smoke_radius,
+                   p.smoke_dens, p.smoke_heat)
+        s.add_smokeforce(self.particles, self.rho, self.temp, fh, p.alpha, p.beta, p.dt)
