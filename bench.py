@@ -226,7 +226,7 @@ def run_vflip(a):
             "cells_steps_per_s": world * a.steps * a.n ** 3 / (ms_max * 1e-3),
             "solver": {"pcg_iterations_mean": float(np.mean(iters)), "vcycles_mean": float(np.mean(vcycles)),
                        "rel_residual_max": float(np.max(resid)), "levels": sim.last.levels, **diag},
-            "roofline": {"bound": "hbm", "kernel": "rbgs_sweep_kernel<float,float> (fine level)",
+            "roofline": {"bound": "hbm", "kernel": "rbgs_sweep_carry_kernel<float> (fine-level FP32 red-black sweep)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_sweep_ms,

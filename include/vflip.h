@@ -67,18 +67,25 @@ typedef struct {
                                 FP32/MIXED (an 8^3 coarsest level those sweeps solve to convergence) */
   int device;                /* CUDA device ordinal, default 0 */
   void* stream;              /* cudaStream_t to order work on; NULL: the CUDA default stream */
-  int sweep_kernel;          /* smoother kernel: 0 = TMA-pipelined (bulk plane copies) for FP32 levels whose
-                                row length is a multiple of 4, else the plain fused kernel; 1 = always the
-                                plain fused kernel; 2 = 3-D-tiled (TMA tensor boxes, several CTAs per SM)
-                                for FP32 levels whose row length is a multiple of 4 (8 for BF16 operators),
-                                else as 0 */
+  int sweep_kernel;          /* smoother kernel: 0 (default) = automatic: for FP32 levels whose row length
+                                is a multiple of 4, the TMA-pipelined kernel (bulk plane copies) in its
+                                register-carry form (one thread per quad of a row for the whole march;
+                                rows of up to 256 cells) or its plain form, else the plain fused kernel;
+                                1 = always the plain fused kernel; 2 = 3-D-tiled (TMA tensor boxes,
+                                several CTAs per SM) for FP32 levels whose row length is a multiple of 4
+                                (8 for BF16 operators), else as 0; 3 = as 0; 4 = the TMA-pipelined kernel
+                                without the register carry, else as 0.  All give the same bits. */
   /* Tile shape of the TMA-pipelined smoother, 0 = automatic (tuning knobs;
    * vflip_b200/tune.py searches them): copy groups in flight (1..3), output
-   * rows per tile, plane ranges per launch, resident CTAs per SM (1..2). */
+   * rows per tile, plane ranges per launch, resident CTAs per SM (1..2),
+   * threads per CTA (512 or 576), planes prefetched into L2 beyond the
+   * copies in flight (1..8; -1 = none). */
   int smoother_depth;
   int smoother_tile_rows;
   int smoother_plane_ranges;
   int smoother_ctas_per_sm;
+  int smoother_threads;
+  int smoother_prefetch;
 } vflip_config;
 
 typedef struct {

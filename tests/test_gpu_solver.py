@@ -101,17 +101,19 @@ def test_pipelined_sweep_matches_plain_kernel(gpu_solver, orc, dims):
     assert np.array_equal(a, c)
 
 
-@pytest.mark.parametrize("shape", [(1, 0, 0, 1), (2, 0, 0, 1), (3, 0, 0, 1), (2, 2, 2, 2), (1, 3, 3, 2), (3, 1, 5, 1)])
+@pytest.mark.parametrize("shape", [(1, 0, 0, 1, 0, 0), (2, 0, 0, 1, 0, 0), (3, 0, 0, 1, 0, 0), (2, 2, 2, 2, 0, 0),
+                                   (1, 3, 3, 2, 0, 0), (3, 1, 5, 1, 0, 0), (1, 7, 0, 1, 576, 0),
+                                   (1, 7, 0, 1, 512, -1), (2, 5, 3, 1, 576, 3), (1, 0, 0, 1, 0, 8)])
 def test_tma_smoother_shapes_match_plain_kernel(gpu_solver, orc, shape):
-    """Every copy depth / tile shape of the TMA smoother gives the plain
-    kernel's V-cycle bit for bit (odd plane counts, clipped edge tiles)."""
+    """Every copy depth / tile shape / CTA size of the TMA smoother gives the
+    plain kernel's V-cycle bit for bit (odd plane counts, clipped edge tiles)."""
     from vflip_b200.solver import Solver
 
     _, out = system(orc, "gen", (64, 40, 37))
     st, b = four(out["stencil"]), t(out["rhs"])
-    d, r, z, c = shape
-    with Solver(precision=1, smoother_depth=d, smoother_tile_rows=r, smoother_plane_ranges=z,
-                smoother_ctas_per_sm=c, **REF_HIERARCHY) as s:
+    d, r, z, c, th, pf = shape
+    with Solver(precision=1, sweep_kernel=4, smoother_depth=d, smoother_tile_rows=r, smoother_plane_ranges=z,
+                smoother_ctas_per_sm=c, smoother_threads=th, smoother_prefetch=pf, **REF_HIERARCHY) as s:
         a = s.vcycle(st, b).cpu().numpy()
     ref = gpu_solver["f32_plain"].vcycle(st, b).cpu().numpy()
     assert np.array_equal(a, ref)
@@ -132,6 +134,40 @@ def test_tiled3d_smoother_matches_plain_kernel(gpu_solver, orc, dims, depth):
             a = s.vcycle(st, b).cpu().numpy()
         ref = gpu_solver[plain].vcycle(st, b).cpu().numpy()
         assert np.array_equal(a, ref), prec
+
+
+@pytest.mark.parametrize("dims", [(64, 40, 37), (40, 37, 30), (128, 96, 64), (36, 20, 44), (16, 9, 5), (256, 23, 19),
+                                  (32, 70, 9)])
+@pytest.mark.parametrize("depth,prefetch", [(1, 0), (2, -1), (3, 4)])
+def test_carry_smoother_matches_plain_kernel(gpu_solver, orc, dims, depth, prefetch):
+    """The register-carry smoother (one thread per quad for the whole z
+    march, neighbours by warp shuffle; fused zero-x / prolongation variants,
+    clipped edge tiles, rows spanning one to two warps or several rows per
+    warp) gives the plain kernel's V-cycle bit for bit, FP32 and with BF16
+    coarse operators."""
+    from vflip_b200.solver import Solver
+
+    _, out = system(orc, "gen", dims)
+    st, b = four(out["stencil"]), t(out["rhs"])
+    for prec, plain in ((1, "f32_plain"), (2, "mix_plain")):
+        with Solver(precision=prec, sweep_kernel=3, smoother_depth=depth, smoother_prefetch=prefetch,
+                    **REF_HIERARCHY) as s:
+            a = s.vcycle(st, b).cpu().numpy()
+        ref = gpu_solver[plain].vcycle(st, b).cpu().numpy()
+        assert np.array_equal(a, ref), prec
+
+
+def test_carry_smoother_pcg(gpu_solver, orc):
+    """The fused z.r of the last post-sweep (DOT variant) through a full solve."""
+    from vflip_b200.solver import Solver
+
+    _, out = system(orc, "gen", (64, 48, 40))
+    st, b = four(out["stencil"]), t(out["rhs"])
+    with Solver(precision=1, sweep_kernel=3, **REF_HIERARCHY) as s:
+        conv, p, stats = s.amgpcg_solve(st, b, 1e-6, 50)
+    conv2, p2, stats2 = gpu_solver["f32_plain"].amgpcg_solve(st, b, 1e-6, 50)
+    assert conv and conv2 and stats.iterations == stats2.iterations
+    assert rel_l2(p.cpu().numpy(), p2.cpu().numpy()) < 1e-6
 
 
 def test_tiled3d_smoother_pcg(gpu_solver, orc):

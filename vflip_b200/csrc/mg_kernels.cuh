@@ -261,6 +261,7 @@ struct TmaSweepArgs {
   int zlen;       // planes per CTA; blockIdx.y = plane range
   int depth;      // copy groups in flight (prefetch distance in planes), 1..3
   int crows_max;  // staged coarse rows per slot
+  int l2_ahead;   // planes beyond the copy group that are prefetched into L2 (0 = none)
   double* dot_partial;
   int* error;
 };
@@ -419,6 +420,20 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs<S> a
     }
     if (hz)
       tma_bulk_g2s(sbase + cbase_b + ES * (oZP + szs * cslot), a.zp + qz * sz + jred0 * sy, crows * ni * ES, bar);
+    // The same plane region l2_ahead planes further on, into L2 only: the
+    // shared-memory ring holds one copy group in flight, which leaves HBM
+    // idle for a copy's latency every plane; the prefetches keep it busy and
+    // turn the later bulk copies into L2 hits.
+    const int qp = (hc ? qc : qx0) + a.l2_ahead;
+    if (a.l2_ahead > 0 && qp < nk && qp >= 0) {
+      if (!ZERO_X) tma_prefetch_l2(a.x_in + (qp + 1 < nk ? qp + 1 : qp) * sz + jr0 * sy, xrows * ni * 4);
+      const size_t o = qp * sz + jred0 * sy;
+      tma_prefetch_l2(a.b + o, crows * ni * 4);
+      tma_prefetch_l2(a.diag + o, crows * ni * ES);
+      tma_prefetch_l2(a.xp + o, crows * ni * ES);
+      tma_prefetch_l2(a.yp + qp * sz + jy0 * sy, yrows * ni * ES);
+      tma_prefetch_l2(a.zp + o, crows * ni * ES);
+    }
   };
   // all threads: wait for group g; block-uniform result
   auto wait_group = [&](int g) -> bool {

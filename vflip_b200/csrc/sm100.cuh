@@ -41,6 +41,11 @@ __device__ __forceinline__ void tma_bulk_g2s(unsigned dst, const void* src, unsi
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
 }
+// Bulk prefetch of a global range into L2 (no shared memory, no completion
+// signal); address and size multiples of 16 bytes.
+__device__ __forceinline__ void tma_prefetch_l2(const void* src, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"(bytes) : "memory");
+}
 // 4-D tiled tensor load (no multicast); c0 is the innermost coordinate and
 // must be a multiple of 16 bytes / element size
 __device__ __forceinline__ void tma_tile_4d(unsigned dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,

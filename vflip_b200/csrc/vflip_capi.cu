@@ -28,6 +28,7 @@
 #include "smoke_kernels.cuh"
 #include "learned_kernels.cuh"
 #include "smoother3d.cuh"
+#include "smoother_carry.cuh"
 #include "tmap.h"
 #include "unet_net.h"
 
@@ -210,12 +211,17 @@ int launch_sweep_t(vflip_ctx* ctx, const SweepArgs<S, V>& a, const SweepShape& s
 // shared-memory budget, persistent CTAs over equal shares of the level's
 // (row tile, plane) pairs.
 struct TmaShape {
-  int tyo, gy, zlen, gz, depth, crows_max, bx, by;
+  int tyo, gy, zlen, gz, depth, crows_max, bx, by, threads, l2_ahead;
+  bool carry;  // register-carry kernel (rbgs_sweep_carry_kernel)
   size_t smem;
 };
 
 constexpr size_t kTmaSmemMax = 227 * 1024 - 1024;  // opt-in limit minus the static part
-constexpr int kTmaBlock = 512;
+// CTA sizes of the TMA-pipelined sweep: 64 x 8 or 64 x 9 threads at 256
+// cells per row.  A relaxation pass walks its rows `by` at a time, so 576
+// threads take the red pass of a 7-row tile (9 rows with the ring) in one
+// round instead of two.
+constexpr int kTmaBlock = 512, kTmaBlockWide = 576;
 
 // Tile shape of the TMA-pipelined sweep.  Rows per tile, plane ranges and
 // copy depth are chosen so that every CTA of a launch is resident at once
@@ -224,14 +230,22 @@ constexpr int kTmaBlock = 512;
 // of each plane range are traded against load balance.  Fields of the
 // context configuration override the choice (0 = automatic).
 template <typename S>
-bool tma_shape(const vflip_config& cfg, const Dims& d, const Dims* cd, bool prolong, int num_sms, TmaShape& o) {
+bool tma_shape(const vflip_config& cfg, const Dims& d, const Dims* cd, bool prolong, int num_sms, TmaShape& o,
+               bool carry = false) {
   if (d.ni % 4 != 0 || (d.ni * sizeof(S)) % 16 != 0) return false;
   if (prolong && (!cd || cd->ni % 4 != 0)) return false;
+  const int Q = (d.ni + 3) / 4;  // quads of four cells per row (one thread each)
+  int bx = 1;
+  while (bx < Q && bx < 128) bx <<= 1;
+  // the register-carry kernel gives every (row, quad) of the red pass its own
+  // thread: all quads of a row in x, the tile and its two ring rows in y
+  const int carry_threads = kTmaBlockWide;
+  if (carry && (bx < Q || carry_threads % bx != 0 || carry_threads / bx < 3)) return false;
   const int cni = prolong ? cd->ni : 0;
   // one copy group in flight measured fastest at 256^3 (vflip_b200/tune.py): deeper
   // prefetch only shortens the tiles
   const int depth = cfg.smoother_depth > 0 ? std::min(cfg.smoother_depth, kTmaMaxDepth) : 1;
-  const int cps = cfg.smoother_ctas_per_sm > 0 ? std::min(cfg.smoother_ctas_per_sm, 2) : 1;
+  const int cps = carry ? 1 : (cfg.smoother_ctas_per_sm > 0 ? std::min(cfg.smoother_ctas_per_sm, 2) : 1);
   const size_t budget = cps == 1 ? kTmaSmemMax : kTmaSmemMax / 2 - 1024;
   auto bytes = [&](int t) { return tma_layout<S>(d.ni, t, depth, prolong ? (t + 7) / 2 : 0, cni).bytes; };
   int tyo_max = 0;
@@ -239,6 +253,7 @@ bool tma_shape(const vflip_config& cfg, const Dims& d, const Dims* cd, bool prol
     if (bytes(t) > budget) break;
     tyo_max = t;
   }
+  if (carry) tyo_max = std::min(tyo_max, carry_threads / bx - 2);
   if (tyo_max < 1) return false;
   const int slots = num_sms * cps;
   double best = 1e30;
@@ -266,21 +281,28 @@ bool tma_shape(const vflip_config& cfg, const Dims& d, const Dims* cd, bool prol
   o.depth = depth;
   o.crows_max = prolong ? (o.tyo + 7) / 2 : 0;
   o.smem = bytes(o.tyo);
-  const int Q = (d.ni + 3) / 4;  // quads of four cells per row (one thread each)
-  int bx = 1;
-  while (bx < Q && bx < 128) bx <<= 1;
   o.bx = bx;
-  o.by = kTmaBlock / bx;
+  o.carry = carry;
+  // 576 threads take a 7-row tile's red pass in one round instead of two but
+  // measured no faster at 256^3 (the copies bound the step), so 512 unless asked
+  o.threads = carry ? carry_threads
+                    : (cfg.smoother_threads == kTmaBlockWide && kTmaBlockWide % bx == 0 ? kTmaBlockWide : kTmaBlock);
+  o.by = o.threads / bx;
+  o.l2_ahead = cfg.smoother_prefetch < 0 ? 0 : (cfg.smoother_prefetch > 0 ? std::min(cfg.smoother_prefetch, 8) : 2);
   return o.smem <= budget;
 }
 
 template <typename S, bool Z, bool P, bool D>
 int launch_tma_t(vflip_ctx* ctx, const TmaSweepArgs<S>& a, const TmaShape& sh) {
-  auto kern = rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlock>;
-  static bool attr_set = false;
-  if (!attr_set) {
+  const bool wide = sh.threads == kTmaBlockWide;
+  const int which = sh.carry ? 2 : (wide ? 1 : 0);
+  auto kern = sh.carry ? rbgs_sweep_carry_kernel<S, Z, P, D, kTmaBlockWide>
+                       : (wide ? rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlockWide>
+                               : rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlock>);
+  static bool attr_set[3] = {false, false, false};
+  if (!attr_set[which]) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemMax);
-    attr_set = true;
+    attr_set[which] = true;
   }
   const bool timed = ctx->profiling && (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n;
   if (timed) {
@@ -310,7 +332,12 @@ int sweep_tma(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V
     return VFLIP_OK;
   TmaShape sh;
   const bool pro = xc != nullptr;
-  if (!tma_shape<S>(ctx->cfg, L.d, cd, pro, ctx->num_sms, sh)) return VFLIP_OK;
+  // automatic (0) and 3: the register-carry kernel where its thread shape
+  // fits the level, else the plain TMA kernel; 4: always the plain TMA kernel
+  const bool carry = ctx->cfg.sweep_kernel == 0 || ctx->cfg.sweep_kernel == 3;
+  if (!(carry && tma_shape<S>(ctx->cfg, L.d, cd, pro, ctx->num_sms, sh, true)) &&
+      !tma_shape<S>(ctx->cfg, L.d, cd, pro, ctx->num_sms, sh))
+    return VFLIP_OK;
   TmaSweepArgs<S> a;
   a.x_in = (const float*)x_in;
   a.x_out = (float*)x_out;
@@ -329,6 +356,7 @@ int sweep_tma(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V
   a.zlen = sh.zlen;
   a.depth = sh.depth;
   a.crows_max = sh.crows_max;
+  a.l2_ahead = sh.l2_ahead;
   a.dot_partial = dot_partial;
   a.error = ctx->d_error;
   if (nblocks_out) *nblocks_out = sh.gy * sh.gz;
@@ -1440,6 +1468,8 @@ void vflip_config_default(vflip_config* cfg) {
   cfg->smoother_tile_rows = 0;
   cfg->smoother_plane_ranges = 0;
   cfg->smoother_ctas_per_sm = 0;
+  cfg->smoother_threads = 0;
+  cfg->smoother_prefetch = 0;
 }
 
 int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
@@ -1461,9 +1491,11 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
   if (ctx->cfg.coarsest_max_unknowns == 0) ctx->cfg.coarsest_max_unknowns = f64 ? 16 * 16 * 16 : 8 * 8 * 8;
   if (ctx->cfg.pre_sweeps < 0 || ctx->cfg.post_sweeps < 0 || ctx->cfg.coarse_sweeps < 0 ||
       ctx->cfg.coarsest_max_unknowns < 1 || ctx->cfg.coarsest_max_unknowns > 4096 || ctx->cfg.precision < 0 ||
-      ctx->cfg.precision > 2 || ctx->cfg.sweep_kernel < 0 || ctx->cfg.sweep_kernel > 2 ||
+      ctx->cfg.precision > 2 || ctx->cfg.sweep_kernel < 0 || ctx->cfg.sweep_kernel > 4 ||
       ctx->cfg.smoother_depth < 0 || ctx->cfg.smoother_tile_rows < 0 || ctx->cfg.smoother_plane_ranges < 0 ||
-      ctx->cfg.smoother_ctas_per_sm < 0)
+      ctx->cfg.smoother_ctas_per_sm < 0 ||
+      (ctx->cfg.smoother_threads != 0 && ctx->cfg.smoother_threads != kTmaBlock &&
+       ctx->cfg.smoother_threads != kTmaBlockWide))
     return bad(VFLIP_ERR_ARG);
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);

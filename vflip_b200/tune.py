@@ -4,11 +4,13 @@
 
 For one grid size it times plain-FP32 MGPCG solves of the plume operator
 (box walls + sphere obstacle) under each candidate - smoother kernel
-(0 full-row TMA, 2 3-D-tiled TMA), copy groups in flight, output rows per
-tile (full-row kernel), plane ranges per launch, resident CTAs per SM -
-reading the fine-level smoother's launch times from the library's own CUDA
-events (vflip_set_profiling), and records the fastest shape per grid size in
-a JSON cache that vflip_b200.plume.PlumeSim and bench.py pass to the solver.
+(0 automatic, 2 3-D-tiled TMA, 3 full-row TMA with register carry, 4 full-row TMA without it), copy groups in flight, output rows per
+tile (full-row kernel), plane ranges per launch, resident CTAs per SM,
+threads per CTA, planes prefetched into L2 - reading the fine-level smoother's launch times from the
+library's own CUDA events (vflip_set_profiling), and records the fastest
+shape per grid size in a JSON cache (tuned_kwargs turns an entry into Solver
+keyword arguments; the library's automatic choice is what the measurements
+below selected as its default).
 """
 import argparse
 import json
@@ -23,11 +25,22 @@ from .solver import Solver
 HERE = os.path.dirname(os.path.abspath(__file__))
 CACHE = os.path.join(HERE, "tuning.json")
 
-# (kernel, depth, tile rows, plane ranges, CTAs per SM); 0 = the library's choice
+# (kernel, depth, tile rows, plane ranges, CTAs per SM, threads per CTA,
+# L2 prefetch planes); 0 = the library's choice, prefetch -1 = none
 CANDIDATES = [
-    (0, 1, 0, 0, 1), (0, 2, 0, 0, 1), (0, 2, 5, 3, 1), (0, 1, 2, 0, 2),
-    (2, 1, 0, 0, 0), (2, 2, 0, 0, 0), (2, 3, 0, 0, 0), (2, 2, 0, 1, 0), (2, 2, 0, 4, 0), (2, 3, 0, 4, 0),
+    (3, 1, 0, 0, 1, 0, -1), (3, 1, 0, 0, 1, 0, 2), (3, 1, 0, 0, 1, 0, 4), (3, 2, 0, 0, 1, 0, 2),
+    (4, 1, 0, 0, 1, 512, -1), (4, 1, 0, 0, 1, 512, 2), (4, 1, 0, 0, 1, 576, 2), (4, 2, 0, 0, 1, 0, 2),
+    (4, 2, 5, 3, 1, 0, 0), (4, 1, 2, 0, 2, 0, 0), (2, 1, 0, 0, 0, 0, 0), (2, 2, 0, 0, 0, 0, 0), (2, 2, 0, 4, 0, 0, 0),
 ]
+
+
+def _shape7(shape):
+    """Cached shapes from before the thread count and the prefetch were knobs
+    have 4 to 6 entries."""
+    shape = list(shape)
+    if len(shape) == 4:
+        shape = [0] + shape
+    return shape + [0] * (7 - len(shape))
 
 
 def load_cache():
@@ -42,10 +55,9 @@ def tuned_kwargs(n):
     entry = load_cache().get(str(n))
     if not entry:
         return {}
-    shape = entry["shape"]
-    k, d, t, r, c = shape if len(shape) == 5 else [0] + list(shape)
+    k, d, t, r, c, th, pf = _shape7(entry["shape"])
     return dict(sweep_kernel=k, smoother_depth=d, smoother_tile_rows=t, smoother_plane_ranges=r,
-                smoother_ctas_per_sm=c)
+                smoother_ctas_per_sm=c, smoother_threads=th, smoother_prefetch=pf)
 
 
 def problem(n, dev):
@@ -62,9 +74,10 @@ def problem(n, dev):
 
 
 def measure(st, rhs, shape, reps=2, precision=1):
-    k, d, t, r, c = shape
+    k, d, t, r, c, th, pf = _shape7(shape)
     with Solver(precision=precision, sweep_kernel=k, smoother_depth=d, smoother_tile_rows=t,
-                smoother_plane_ranges=r, smoother_ctas_per_sm=c) as s:
+                smoother_plane_ranges=r, smoother_ctas_per_sm=c, smoother_threads=th,
+                smoother_prefetch=pf) as s:
         s.amgpcg_solve(st, rhs, 1e-6, 50)  # warm (allocations)
         s.set_profiling(True)
         s.profile_sweeps()
@@ -86,6 +99,7 @@ def main():
                     help="assemble the operator and run one FP32 solve (a small target for profilers)")
     ap.add_argument("--precision", type=int, default=1)
     ap.add_argument("--sweep-kernel", type=int, default=0, help="smoother kernel of --solve-once")
+    ap.add_argument("--only-kernel", type=int, default=None, help="tune only the candidates of this smoother kernel")
     a = ap.parse_args()
     st, rhs = problem(a.n, "cuda:0")
     if a.solve_once:
@@ -95,6 +109,8 @@ def main():
         return
     results = []
     for shape in CANDIDATES:
+        if a.only_kernel is not None and shape[0] != a.only_kernel:
+            continue
         try:
             r = measure(st, rhs, shape)
         except Exception as e:  # a shape the library rejects
