@@ -84,6 +84,12 @@ struct vflip_ctx {
     auto it = bufs.find(name);
     if (it != bufs.end() && it->second.second >= bytes) return it->second.first;
     if (it != bufs.end()) {
+      // a buffer that has to grow gets 1/8 of headroom (rounded to 2 MiB),
+      // so sizes that creep up call after call (a particle count that
+      // reseeding raises a little every step) do not pay a synchronising
+      // cudaFree + cudaMalloc each time
+      bytes += bytes / 8;
+      bytes = (bytes + (2u << 20) - 1) / (2u << 20) * (2u << 20);
       cudaFree(it->second.first);
       bufs.erase(it);
     }
