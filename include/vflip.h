@@ -86,6 +86,15 @@ typedef struct {
   int smoother_ctas_per_sm;
   int smoother_threads;
   int smoother_prefetch;
+  /* Coarsest-level solve: 0 (default) = automatic: red-black sweeps
+   * (coarse_sweeps) in FP64 contexts, the reference's; in FP32/MIXED
+   * contexts an FP64 banded Cholesky direct solve, its factor built on the
+   * GPU with each hierarchy, when the coarsest level's band (ni*nj of that
+   * level) is at most 160 wide; the sweeps run instead where the band is
+   * wider or a pivot shows the level singular (no open boundary pins some
+   * fluid region).  1 = always the sweeps; 2 = the direct solve where it
+   * applies, in every precision. */
+  int coarsest_solver;
 } vflip_config;
 
 typedef struct {

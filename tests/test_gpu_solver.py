@@ -184,7 +184,8 @@ def test_tiled3d_smoother_pcg(gpu_solver, orc):
 
 @pytest.mark.parametrize("prec", [1, 2])
 def test_automatic_hierarchy(gpu_solver, orc, prec):
-    """FP32/MIXED contexts coarsen to an 8^3 level by default: the solve
+    """FP32/MIXED contexts coarsen to a level of <= 4^3 solved directly in FP64
+    by default (an 8^3 level relaxed by 100 sweeps without it): the solve
     reaches the tolerance in no more iterations than with the reference's
     hierarchy and agrees with the reference's pressure."""
     from vflip_b200.solver import Solver
@@ -361,3 +362,89 @@ def test_subdomain_projection_matches_reference(gpu_solver):
                                                      max_iterations=50)
     assert conv
     assert rel_l2(p.cpu().numpy(), g["out_pressure"]) < 1e-4
+
+
+# ---- FP64 direct solve of the coarsest level (FP32 / mixed V-cycles)
+
+def _dense(st4):
+    """Dense FP64 matrix of a (4, nk, nj, ni) stencil (diag, +x, +y, +z)."""
+    d, xp, yp, zp = (np.asarray(a, np.float64).ravel() for a in st4)
+    _, nk, nj, ni = st4.shape
+    n = ni * nj * nk
+    A = np.diag(d)
+    idx = np.arange(n)
+    i, j, k = idx % ni, (idx // ni) % nj, idx // (ni * nj)
+    for off, c, ok in ((1, xp, i < ni - 1), (ni, yp, j < nj - 1), (ni * nj, zp, k < nk - 1)):
+        r = idx[ok]
+        A[r, r + off] = c[ok]
+        A[r + off, r] = c[ok]
+    return A
+
+
+@pytest.mark.parametrize("dims", [(8, 8, 8), (7, 9, 6), (12, 5, 8), (16, 6, 5), (4, 4, 4), (6, 5, 4)])
+@pytest.mark.parametrize("prec", [1, 2])
+def test_coarse_direct_solve_matches_dense_solve(orc, dims, prec):
+    """A level small enough to be the whole hierarchy (coarsening stops at
+    512 unknowns here): the V-cycle is the coarsest solve, the FP64
+    band-Cholesky solve, with its factor read from global memory (8^3,
+    12x5x8, 16x6x5) or staged in shared memory (the others).  It agrees with a dense
+    FP64 solve of the same system (cells without fluid decoupled, x = 0) to
+    the FP32 rounding of its input and output."""
+    from vflip_b200.solver import Solver
+
+    _, out = system(orc, "gen", dims)
+    st7, b = out["stencil"], out["rhs"]
+    st4 = np.stack([st7[0], st7[2], st7[4], st7[6]])
+    A = _dense(st4)
+    b32 = b.astype(np.float32).astype(np.float64).ravel()
+    live = np.diag(A) != 0
+    want = np.zeros_like(b32)
+    want[live] = np.linalg.solve(A[np.ix_(live, live)], b32[live])
+    with Solver(precision=prec, coarsest_solver=2, coarsest_max_unknowns=512) as s:
+        x = s.vcycle(four(st7), t(b)).cpu().numpy().astype(np.float64).ravel()
+    assert (~live).sum() > 0 and live.sum() > 0 and np.all(x[~live] == 0)
+    assert rel_l2(x, want) < 2e-6
+    # the automatic choice takes the same path in FP32 / mixed precision
+    with Solver(precision=prec, coarsest_max_unknowns=512) as s:
+        x0 = s.vcycle(four(st7), t(b)).cpu().numpy().astype(np.float64).ravel()
+    assert np.array_equal(x0, x)
+
+
+def test_coarse_direct_singular_level_falls_back_to_sweeps():
+    """A pure-Neumann level (no cell pinned by an open boundary) is
+    singular: the factorisation flags it and the red-black sweeps run, so
+    the result equals the sweeps-only context bit for bit."""
+    from vflip_b200.solver import Solver
+
+    ni, nj, nk = 8, 7, 6
+    k, j, i = np.meshgrid(np.arange(nk), np.arange(nj), np.arange(ni), indexing="ij")
+    xp = np.where(i < ni - 1, -1.0, 0.0)
+    yp = np.where(j < nj - 1, -1.0, 0.0)
+    zp = np.where(k < nk - 1, -1.0, 0.0)
+    diag = ((i > 0).astype(float) + (i < ni - 1) + (j > 0) + (j < nj - 1) + (k > 0) + (k < nk - 1))
+    st = t(np.stack([diag, xp, yp, zp]).astype(np.float64))
+    b = np.random.default_rng(3).standard_normal((nk, nj, ni))
+    b -= b.mean()
+    with Solver(precision=1, coarsest_solver=2, coarsest_max_unknowns=512) as s:
+        a = s.vcycle(st, t(b)).cpu().numpy()
+    with Solver(precision=1, coarsest_solver=1, coarsest_max_unknowns=512) as s:
+        ref = s.vcycle(st, t(b)).cpu().numpy()
+    assert np.all(np.isfinite(a)) and np.array_equal(a, ref)
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+def test_coarse_direct_pcg(orc, prec):
+    """Full FP32 / mixed solves with the automatic coarsest level (the direct
+    solve of a <= 4^3 level) reach the tolerance in no more iterations than
+    with 100 sweeps on an 8^3 level and agree with the reference's pressure."""
+    from vflip_b200.solver import Solver
+
+    _, out = system(orc, "gen", (64, 48, 40))
+    st, b = four(out["stencil"]), t(out["rhs"])
+    x_ref, ok, res, it = orc.amgpcg(out["stencil"], out["rhs"])
+    with Solver(precision=prec) as s:
+        conv, p, stats = s.amgpcg_solve(st, b, 1e-6, 50)
+    with Solver(precision=prec, coarsest_solver=1) as s:
+        conv2, p2, stats2 = s.amgpcg_solve(st, b, 1e-6, 50)
+    assert conv and conv2 and stats.iterations <= stats2.iterations
+    assert rel_l2(p.cpu().numpy(), x_ref) < 1e-5

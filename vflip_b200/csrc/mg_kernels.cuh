@@ -641,7 +641,9 @@ __global__ void __launch_bounds__(BLOCK) coarsest_rbgs_kernel(const V* __restric
                                                              const S* __restrict__ xp, const S* __restrict__ yp,
                                                              const S* __restrict__ zp, V* __restrict__ x_out,
                                                              int ni, int nj, int nk, int sweeps,
-                                                             double* dot_out) {
+                                                             double* dot_out, const int* skip_if_set) {
+  // the FP64 direct solve of this level ran instead (coarse_direct.cuh)
+  if (skip_if_set && *skip_if_set) return;
   using A = typename Num<V>::Acc;
   constexpr int kMaxOwn = 4096 / BLOCK;
   extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -29,6 +29,7 @@
 #include "learned_kernels.cuh"
 #include "smoother3d.cuh"
 #include "smoother_carry.cuh"
+#include "coarse_direct.cuh"
 #include "tmap.h"
 #include "unet_net.h"
 
@@ -524,10 +525,39 @@ int sweep(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_
   return ctx->fail(VFLIP_ERR_ARG, "sweep: prolongation needs an incoming x");
 }
 
+// FP64 band-Cholesky factor of the coarsest level (coarse_direct.cuh); `on`
+// when built for this hierarchy.  *ok (device) is cleared by a singular pivot.
+struct CoarseDirect {
+  bool on = false;
+  int bw = 0;
+  double* L = nullptr;
+  double* rinv = nullptr;
+  int* ok = nullptr;
+};
+constexpr int kCholMaxBw = 160, kCholBlock = 1024, kCholSolveBlock = 256;
+constexpr size_t kCholStageMax = 200 * 1024;
+
 template <typename S, typename V>
-int coarsest(vflip_ctx* ctx, const Level<S, V>& L, const V* b, V* x_out, int sweeps, double* dot_out) {
+int coarsest(vflip_ctx* ctx, const Level<S, V>& L, const V* b, V* x_out, int sweeps, double* dot_out,
+             const CoarseDirect* cd = nullptr) {
   using A = typename Num<V>::Acc;
   size_t n = L.d.n();
+  const int* skip = nullptr;
+  if (cd && cd->on) {
+    auto sk = coarse_chol_solve_kernel<V, kCholSolveBlock>;
+    static bool sattr = false;
+    if (!sattr) {
+      cudaFuncSetAttribute(sk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCholStageMax);
+      sattr = true;
+    }
+    // the factor lives in shared memory for the solve when it fits
+    const size_t staged_bytes = (n + n * (cd->bw + 1) + n) * sizeof(double);
+    const int staged = staged_bytes <= kCholStageMax;
+    sk<<<1, kCholSolveBlock, staged ? staged_bytes : n * sizeof(double), ctx->stream>>>(
+        b, x_out, (int)n, cd->bw, cd->L, cd->rinv, cd->ok, dot_out, staged);
+    VF_LAUNCH_CHECK();
+    skip = cd->ok;  // the sweeps below run only if the factorisation failed
+  }
   size_t smem = 6 * n * sizeof(A);
   auto kern = coarsest_rbgs_kernel<S, V, kCoarseBlock>;
   static bool attr_set = false;
@@ -537,7 +567,7 @@ int coarsest(vflip_ctx* ctx, const Level<S, V>& L, const V* b, V* x_out, int swe
   }
   if (smem > 220 * 1024) return ctx->fail(VFLIP_ERR_ARG, "coarsest level of %zu unknowns exceeds 4096", n);
   kern<<<1, kCoarseBlock, smem, ctx->stream>>>(b, L.diag, L.xp, L.yp, L.zp, x_out, L.d.ni, L.d.nj, L.d.nk, sweeps,
-                                               dot_out);
+                                               dot_out, skip);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
 }
@@ -606,7 +636,46 @@ template <typename S0, typename SC, typename V>
 struct Typed {
   Level<S0, V> fine;
   std::vector<Level<SC, V>> coarse;  // coarse[l-1] = level l
+  CoarseDirect direct;               // factor of the coarsest level, when used
 };
+
+// Builds the FP64 band-Cholesky factor of the hierarchy's coarsest level
+// (one CTA) when the context asks for the direct solve and the band fits.
+int build_coarse_direct(vflip_ctx* ctx, const Hierarchy64& H, const double* d0, const double* x0, const double* y0,
+                        const double* z0, CoarseDirect& cd, const char* tag) {
+  cd.on = false;
+  const int mode = ctx->cfg.coarsest_solver;
+  if (mode == 1 || (mode == 0 && ctx->cfg.precision == VFLIP_PREC_FP64)) return VFLIP_OK;
+  const size_t l = H.dims.size() - 1;
+  const Dims& d = H.dims[l];
+  const int bw = d.ni * d.nj;
+  const size_t n = d.n();
+  if (bw > kCholMaxBw || n > 4096) return VFLIP_OK;
+  const double *dg, *xp, *yp, *zp;
+  if (l == 0) {
+    dg = d0; xp = x0; yp = y0; zp = z0;
+  } else {
+    dg = H.lv[l]; xp = dg + n; yp = xp + n; zp = yp + n;
+  }
+  double* p;
+  VF_ALLOC(p, double, std::string(tag) + "_chol", n * (bw + 1) + n + 1);
+  cd.L = p;
+  cd.rinv = p + n * (bw + 1);
+  cd.ok = reinterpret_cast<int*>(cd.rinv + n);
+  cd.bw = bw;
+  auto kern = coarse_chol_kernel<kCholBlock>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)((kCholMaxBw + 1) * (kCholMaxBw + 1) * sizeof(double)));
+    attr_set = true;
+  }
+  kern<<<1, kCholBlock, (size_t)(bw + 1) * (bw + 1) * sizeof(double), ctx->stream>>>(
+      dg, xp, yp, zp, d.ni, d.nj, d.nk, bw, cd.L, cd.rinv, cd.ok);
+  VF_LAUNCH_CHECK();
+  cd.on = true;
+  return VFLIP_OK;
+}
 
 template <typename S, typename V>
 int make_level(vflip_ctx* ctx, const Hierarchy64& H, size_t l, const double* d0, const double* x0,
@@ -645,7 +714,7 @@ int make_typed(vflip_ctx* ctx, const Hierarchy64& H, const double* d0, const dou
   T.coarse.resize(H.dims.size() - 1);
   for (size_t l = 1; l < H.dims.size(); ++l)
     if ((rc = make_level<SC, V>(ctx, H, l, d0, x0, y0, z0, T.coarse[l - 1], tag))) return rc;
-  return VFLIP_OK;
+  return build_coarse_direct(ctx, H, d0, x0, y0, z0, T.direct, tag);
 }
 
 // ---------------------------------------------------------------- V-cycle
@@ -703,7 +772,8 @@ int vcycle(vflip_ctx* ctx, Typed<S0, SC, V>& T, const V* r, V* z, bool want_dot)
   int rc;
   const int nl = (int)T.coarse.size() + 1;
   if (nl == 1) {
-    rc = coarsest<S0, V>(ctx, T.fine, r, z, ctx->cfg.coarse_sweeps, want_dot ? ctx->partials : nullptr);
+    rc = coarsest<S0, V>(ctx, T.fine, r, z, ctx->cfg.coarse_sweeps, want_dot ? ctx->partials : nullptr,
+                         &T.direct);
     if (rc) return rc;
     if (want_dot) {
       fold_kernel<kRedBlock><<<1, kRedBlock, 0, ctx->stream>>>(ctx->partials, 1, ctx->st, kReduceRho, 0.0);
@@ -722,7 +792,7 @@ int vcycle(vflip_ctx* ctx, Typed<S0, SC, V>& T, const V* r, V* z, bool want_dot)
   }
   // bottom
   Level<SC, V>& B = T.coarse[nl - 2];
-  if ((rc = coarsest<SC, V>(ctx, B, B.b, B.xa, ctx->cfg.coarse_sweeps, nullptr))) return rc;
+  if ((rc = coarsest<SC, V>(ctx, B, B.b, B.xa, ctx->cfg.coarse_sweeps, nullptr, &T.direct))) return rc;
   V* xc = B.xa;
   Dims cd = B.d;
   // up
@@ -1476,6 +1546,7 @@ void vflip_config_default(vflip_config* cfg) {
   cfg->smoother_ctas_per_sm = 0;
   cfg->smoother_threads = 0;
   cfg->smoother_prefetch = 0;
+  cfg->coarsest_solver = 0;
 }
 
 int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
@@ -1493,15 +1564,20 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
   // 8^3, which 100 sweeps solve to convergence (one PCG iteration fewer on the
   // 256^3 plume operator than 200 sweeps on 16^3)
   const bool f64 = ctx->cfg.precision == VFLIP_PREC_FP64;
+  // with the FP64 direct solve, FP32/MIXED coarsen on to <= 64 unknowns
+  // (4^3): its band factor then sits in shared memory for the solve
+  const bool direct = ctx->cfg.coarsest_solver == 2 || (ctx->cfg.coarsest_solver == 0 && !f64);
   if (ctx->cfg.coarse_sweeps == 0) ctx->cfg.coarse_sweeps = f64 ? 200 : 100;
-  if (ctx->cfg.coarsest_max_unknowns == 0) ctx->cfg.coarsest_max_unknowns = f64 ? 16 * 16 * 16 : 8 * 8 * 8;
+  if (ctx->cfg.coarsest_max_unknowns == 0)
+    ctx->cfg.coarsest_max_unknowns = f64 ? 16 * 16 * 16 : (direct ? 4 * 4 * 4 : 8 * 8 * 8);
   if (ctx->cfg.pre_sweeps < 0 || ctx->cfg.post_sweeps < 0 || ctx->cfg.coarse_sweeps < 0 ||
       ctx->cfg.coarsest_max_unknowns < 1 || ctx->cfg.coarsest_max_unknowns > 4096 || ctx->cfg.precision < 0 ||
       ctx->cfg.precision > 2 || ctx->cfg.sweep_kernel < 0 || ctx->cfg.sweep_kernel > 4 ||
       ctx->cfg.smoother_depth < 0 || ctx->cfg.smoother_tile_rows < 0 || ctx->cfg.smoother_plane_ranges < 0 ||
       ctx->cfg.smoother_ctas_per_sm < 0 ||
       (ctx->cfg.smoother_threads != 0 && ctx->cfg.smoother_threads != kTmaBlock &&
-       ctx->cfg.smoother_threads != kTmaBlockWide))
+       ctx->cfg.smoother_threads != kTmaBlockWide) ||
+      ctx->cfg.coarsest_solver < 0 || ctx->cfg.coarsest_solver > 2)
     return bad(VFLIP_ERR_ARG);
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);
