@@ -348,7 +348,9 @@ def advection_arm(solver, n=128, reps=20):
     """The grid advection forms and smoke scalars at the FLIP scene's size:
     SmokeSolver3D::advect (cubic-clamped u, v, w of a 128^3 MAC grid, one
     launch), advect_field (RK3) of density and temperature on their 256^3
-    grid at h/2 (one shared backtrace) and gen_heat on that grid, each timed
+    grid at h/2 (one shared backtrace), gen_heat on that grid and
+    advect_tracers on 4 M tracers (RK3 + solid test, 32 B read + written per
+    tracer), each timed
     with CUDA events on the library's stream (median of `reps` after 3
     warm-ups), in the solver's precision.  Algorithmic bytes: every output
     node reads its field value and writes one float (8 B), the velocity
@@ -382,6 +384,8 @@ def advection_arm(solver, n=128, reps=20):
             ts.append(e0.elapsed_time(e1))
         return float(np.median(ts))
 
+    tracers = solver.emit_tracers(None, h, (1.0, 1.0, 1.0), (0.5, 0.5, 0.5), 0.3, 4_000_000, seed=0)
+    phi = torch.full((n + 1,) * 3, 1.0, device="cuda")
     peak, _ = measured_peaks()
     faces = 3 * (n + 1) * n * n
     nodes2 = (2 * n) ** 3
@@ -393,7 +397,9 @@ def advection_arm(solver, n=128, reps=20):
                                                                          field2=temp, out=r2, out2=t2),
              nodes2, 16 * nodes2 + 4 * faces),
             ("gen_heat", lambda: solver.gen_heat(rho, temp, h / 2, 0.01, 0.1, 0.1, (0.5, 0.1, 0.5), 0.12, 1.0, 1.0),
-             nodes2, 16 * nodes2)):
+             nodes2, 16 * nodes2),
+            ("advect_tracers", lambda: solver.advect_tracers(n, n, n, h, tracers, u, v, w, phi, 0.001, 0.1),
+             tracers.shape[0], 32 * tracers.shape[0])):
         ms = med(fn)
         gbs = alg / (ms * 1e-3) / 1e9
         res[name] = {"ms": ms, "nodes": nodes, "gnodes_per_s": nodes / (ms * 1e-3) / 1e9, "alg_bytes": alg,

@@ -293,6 +293,35 @@ int vflip_gen_heat(vflip_ctx* ctx, int fnx, int fny, int fnz, double fh, float d
 int vflip_add_smokeforce(vflip_ctx* ctx, void* particles, int np, int fnx, int fny, int fnz, double fh,
                          const float* rho, const float* temp, float alpha, float beta, float dt);
 
+/* ---- smoke tracers (float4 records: x, y, z, density) ----------------------- */
+
+/* SmokeSolver3D::emit_tracers (SS/Smoke_solver3D.h:46-85): keeps, in order,
+ * the tracers inside [2h, L-2h] on every axis (L = lx, ly, lz) whose density
+ * exceeds 0.01, then appends `count` new ones of density 1 uniform in the
+ * sphere of radius r about (cx, cy, cz).  The reference rejection-samples
+ * rand() over a cube of half-width r + h; this library rejection-samples a
+ * counter-based hash of (seed, slot, attempt) over the sphere's bounding
+ * cube: the same law, other positions.  The nested subdomain's seeding
+ * (:86-96) is not part of this call.  `out` (capacity float4, must not alias
+ * `tracers`) receives the result and *n_out (HOST) its count; when that
+ * exceeds `capacity` nothing is written and VFLIP_ERR_TOO_LARGE returns.
+ * Synchronises the stream. */
+int vflip_emit_tracers(vflip_ctx* ctx, const float* tracers, int n, float h, float lx, float ly, float lz, float cx,
+                       float cy, float cz, float r, int count, unsigned seed, float* out, int capacity, int* n_out);
+
+/* SmokeSolver3D::advect_tracers (SS/Smoke_solver3D.h:99-120), in place:
+ * traceRK3 through the MAC velocity, out of a solid along its normal where
+ * the sampled nodal phi is <= 0, density / (1 + dens_decay dt).
+ * Bit-identical to the reference. */
+int vflip_advect_tracers(vflip_ctx* ctx, int ni, int nj, int nk, float h, float* tracers, int n, const float* u,
+                         const float* v, const float* w, const float* nodal_phi, float dt, float dens_decay);
+
+/* SmokeSolver3D::write_tracers (SS/Smoke_solver3D.h:121-160): writes
+ * <dir>/Particle_data%04d.bin (frame) holding n float4 records
+ * (x/lx - 0.5, y/lx, z/lx - 0.5, density), the reference's byte layout.
+ * `dir` is a HOST string; synchronises the stream. */
+int vflip_write_tracers(vflip_ctx* ctx, const float* tracers, int n, float lx, const char* dir, int frame);
+
 /* delta = after - before, n floats (SmokeSolver3D::getDelta, SS/Smoke_solver3D.cpp:1298-1319). */
 int vflip_delta(vflip_ctx* ctx, size_t n, const float* after, const float* before, float* delta);
 

@@ -87,6 +87,13 @@ def _load(path, prefix):
     getattr(lib, p + "_advect_rk3").argtypes = [_I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _D, _P, _P]
     getattr(lib, p + "_gen_heat").argtypes = [_I, _I, _I, _D, _F, _F, _F, _F, _F, _F, _F, _F, _F, _P, _P]
     getattr(lib, p + "_add_smokeforce").argtypes = [_P, _I, _I, _I, _I, _D, _P, _P, _F, _F, _F]
+    getattr(lib, p + "_emit_tracers").argtypes = [_P, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I, C.c_uint, _P, _I]
+    getattr(lib, p + "_emit_tracers").restype = _I
+    getattr(lib, p + "_advect_tracers").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _F, _F]
+    if prefix == "oracle":
+        getattr(lib, p + "_tracer_records").argtypes = [_P, _I, _F, _P]
+    else:
+        getattr(lib, p + "_write_tracers").argtypes = [_P, _I, _F, C.c_char_p, _I]
     if prefix == "oracle":
         getattr(lib, p + "_g2p").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _P, _P, _D]
         getattr(lib, p + "_delta").argtypes = [_I, _I, _I, _P, _P, _P]
@@ -289,6 +296,38 @@ class _Impl:
         fnz, fny, fnx = rho.shape
         self.fn("add_smokeforce")(_ptr(p), len(p), fnx, fny, fnz, float(fh), _ptr(rho), _ptr(temp), alpha, beta, dt)
         return p
+
+    def emit_tracers(self, tracers, h, lengths, centre, r, count, seed=0):
+        """SmokeSolver3D::emit_tracers on float4 tracers (n, 4); returns the new (m, 4) array."""
+        tr = np.ascontiguousarray(tracers, np.float32).reshape(-1, 4)
+        cap = len(tr) + int(count) + 16
+        out = np.zeros((cap, 4), np.float32)
+        m = self.fn("emit_tracers")(_ptr(tr), len(tr), h, float(lengths[0]), float(lengths[1]), float(lengths[2]),
+                                    float(centre[0]), float(centre[1]), float(centre[2]), r, int(count), int(seed),
+                                    _ptr(out), cap)
+        if m < 0 or m > cap:
+            raise RuntimeError("tracer capacity")
+        return out[:m].copy()
+
+    def advect_tracers(self, ni, nj, nk, h, tracers, u, v, w, nodal_phi, dt, dens_decay):
+        """SmokeSolver3D::advect_tracers on a copy of float4 tracers (n, 4)."""
+        tr = np.array(tracers, np.float32, copy=True).reshape(-1, 4)
+        u, v, w, phi = [np.ascontiguousarray(a, np.float32) for a in (u, v, w, nodal_phi)]
+        self.fn("advect_tracers")(ni, nj, nk, h, _ptr(tr), len(tr), _ptr(u), _ptr(v), _ptr(w), _ptr(phi), float(dt),
+                                  float(dens_decay))
+        return tr
+
+    def tracer_records(self, tracers, lx):
+        """The float4 records write_tracers puts on disk (oracle)."""
+        tr = np.ascontiguousarray(tracers, np.float32).reshape(-1, 4)
+        out = np.zeros_like(tr)
+        self.fn("tracer_records")(_ptr(tr), len(tr), float(lx), _ptr(out))
+        return out
+
+    def write_tracers(self, tracers, lx, directory, frame):
+        """SmokeSolver3D::write_tracers (reference): <directory>/Particle_data%04d.bin."""
+        tr = np.ascontiguousarray(tracers, np.float32).reshape(-1, 4)
+        self.fn("write_tracers")(_ptr(tr), len(tr), float(lx), str(directory).encode(), int(frame))
 
     def hash(self, ni, nj, nk, h, particles):
         particles = np.ascontiguousarray(particles, PARTICLE_DTYPE)

@@ -523,6 +523,61 @@ void ref_add_smokeforce(void* particles, int np, int fnx, int fny, int fnz, doub
   for (int q = 0; q < np; ++q) p[q] = s.FLIP[q];
 }
 
+// SmokeSolver3D::emit_tracers (Smoke_solver3D.h:46-97) with rand() seeded by
+// `seed`, an inactive nested subdomain (no subdomain seeding) and the
+// emitter (cx, cy, cz, r, count).  Returns the new number of tracers (those
+// beyond `capacity` are not copied out).
+int ref_emit_tracers(const float* tracers, int n, float h, float lx, float ly, float lz, float cx, float cy,
+                     float cz, float r, int count, unsigned seed, float* out, int capacity) {
+  SmokeSolver3D s;
+  quiet_subdomain(s.sub_domain);
+  s.sub_domain._nx = s.sub_domain._ny = s.sub_domain._nz = 0;
+  s._hx = s._hy = s._hz = h;
+  s._lx = lx; s._ly = ly; s._lz = lz;
+  s.tracers.clear();
+  for (int q = 0; q < n; ++q)
+    s.tracers.push_back(Vec4f(tracers[4 * q], tracers[4 * q + 1], tracers[4 * q + 2], tracers[4 * q + 3]));
+  Vec3f c(cx, cy, cz);
+  s.setEmitter(c, r, (uint)count);
+  srand(seed);
+  s.emit_tracers();
+  const int m = (int)s.tracers.size();
+  for (int q = 0; q < m && q < capacity; ++q)
+    for (int a = 0; a < 4; ++a) out[4 * q + a] = s.tracers[q][a];
+  return m;
+}
+
+// SmokeSolver3D::advect_tracers (Smoke_solver3D.h:99-120) on the grid
+// velocity and nodal solid phi, in place.
+void ref_advect_tracers(int ni, int nj, int nk, float h, float* tracers, int n, const float* u, const float* v,
+                        const float* w, const float* nodal_phi, float dt, float dens_decay) {
+  SmokeSolver3D s;
+  init_solver_grids(s, ni, nj, nk, h);
+  to_buffer(s._un, u);
+  to_buffer(s._vn, v);
+  to_buffer(s._wn, w);
+  to_buffer(s._nodal_solid_phi, nodal_phi);
+  s._dens_decay = dens_decay;
+  s.tracers.clear();
+  for (int q = 0; q < n; ++q)
+    s.tracers.push_back(Vec4f(tracers[4 * q], tracers[4 * q + 1], tracers[4 * q + 2], tracers[4 * q + 3]));
+  s.advect_tracers(dt);
+  for (int q = 0; q < n; ++q)
+    for (int a = 0; a < 4; ++a) tracers[4 * q + a] = s.tracers[q][a];
+}
+
+// SmokeSolver3D::write_tracers (Smoke_solver3D.h:121-160): writes
+// <dir>/Particle_data%04d.bin for `frame`.
+void ref_write_tracers(const float* tracers, int n, float lx, const char* dir, int frame) {
+  SmokeSolver3D s;
+  quiet_subdomain(s.sub_domain);
+  s._lx = lx;
+  s.tracers.clear();
+  for (int q = 0; q < n; ++q)
+    s.tracers.push_back(Vec4f(tracers[4 * q], tracers[4 * q + 1], tracers[4 * q + 2], tracers[4 * q + 3]));
+  s.write_tracers(const_cast<char*>(dir), frame);
+}
+
 // SmokeSolver3D::getDelta (Smoke_solver3D.cpp:1298-1319): delta = after - before
 // on one nx x ny x nz face grid.
 void ref_delta(int nx, int ny, int nz, const float* after, const float* before, float* delta) {

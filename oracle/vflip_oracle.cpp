@@ -1019,6 +1019,103 @@ void oracle_add_smokeforce(void* particles, int np, int fnx, int fny, int fnz, d
   }
 }
 
+// ---- smoke tracers (SmokeSolver3D::emit_tracers / advect_tracers /
+// write_tracers, SS/Smoke_solver3D.h:46-160): float4 records x, y, z, density
+
+// emit_tracers' keep test, SS/Smoke_solver3D.h:52-59: inside [2h, L-2h] on
+// every axis (float) and density > 0.01 (compared in double).
+static bool tracer_kept(const float* t, float h, float lx, float ly, float lz) {
+  const float m = 2 * h;
+  return t[0] > m && t[1] > m && t[2] > m && t[0] < lx - m && t[1] < ly - m && t[2] < lz - m && (double)t[3] > 0.01;
+}
+
+// Offset of new tracer `slot`: attempt a draws x, y, z uniform in [-r, r)
+// from the counter hash and accepts the first point with x^2 + z^2 + y^2 <=
+// r^2 (the reference's sum order).  The reference draws from rand() over the
+// cube of half-width r + h; a cube that just bounds the sphere gives the
+// same uniform law with a higher acceptance rate.  After 64 rejected
+// attempts (probability below 1e-20) the centre is used.
+static void tracer_offset(uint32_t seed, uint32_t slot, float r, float o[3]) {
+  for (uint32_t a = 0; a < 64; ++a) {
+    const float x = r * reseed_uniform(seed ^ 0x7f4a7c15u, slot, a, 0);
+    const float y = r * reseed_uniform(seed ^ 0x7f4a7c15u, slot, a, 1);
+    const float z = r * reseed_uniform(seed ^ 0x7f4a7c15u, slot, a, 2);
+    if (x * x + z * z + y * y <= r * r) {
+      o[0] = x; o[1] = y; o[2] = z;
+      return;
+    }
+  }
+  o[0] = o[1] = o[2] = 0.0f;
+}
+
+// SmokeSolver3D::emit_tracers, SS/Smoke_solver3D.h:46-85 (the nested
+// subdomain's seeding, :86-96, is not restated): the kept tracers in order,
+// then `count` new ones of density 1 about (cx, cy, cz).  Returns the new
+// number of tracers, negated when it exceeds `capacity` (nothing written).
+int oracle_emit_tracers(const float* tracers, int n, float h, float lx, float ly, float lz, float cx, float cy,
+                        float cz, float r, int count, unsigned seed, float* out, int capacity) {
+  int m = 0;
+  for (int q = 0; q < n; ++q) m += tracer_kept(tracers + 4 * (size_t)q, h, lx, ly, lz);
+  if (m + count > capacity) return -(m + count);
+  m = 0;
+  for (int q = 0; q < n; ++q)
+    if (tracer_kept(tracers + 4 * (size_t)q, h, lx, ly, lz)) {
+      for (int a = 0; a < 4; ++a) out[4 * (size_t)m + a] = tracers[4 * (size_t)q + a];
+      ++m;
+    }
+  for (int s = 0; s < count; ++s) {
+    float o[3];
+    tracer_offset(seed, (uint32_t)s, r, o);
+    float* t = out + 4 * (size_t)(m + s);
+    t[0] = cx + o[0];
+    t[1] = cy + o[1];
+    t[2] = cz + o[2];
+    t[3] = 1.0f;
+  }
+  return m + count;
+}
+
+// SmokeSolver3D::advect_tracers, SS/Smoke_solver3D.h:99-120: traceRK3 with
+// step dt, then out of a solid along its normal when the sampled nodal phi
+// is <= 0 (advect_FLIP's test is < 0), and the density divided by
+// 1 + decay*dt (the product in float, the sum and the quotient in double).
+void oracle_advect_tracers(int ni, int nj, int nk, float h, float* tracers, int n, const float* u, const float* v,
+                           const float* w, const float* nodal_phi, float dt, float dens_decay) {
+  const Grid vel[3] = {{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0},
+                       {v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0},
+                       {w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5}};
+  const Grid phi = {nodal_phi, ni + 1, nj + 1, nk + 1, (double)h, 0.5, 0.5, 0.5};
+  for (int q = 0; q < n; ++q) {
+    float* t = tracers + 4 * (size_t)q;
+    float pos[3];
+    trace_rk3(vel, t, dt, pos);
+    const float ph = phi.sample(pos[0], pos[1], pos[2]);
+    if (ph <= 0) {
+      float nrm[3];
+      solid_normal(phi, pos, nrm);
+      for (int a = 0; a < 3; ++a) pos[a] -= ph * nrm[a];
+    }
+    const float d = (float)((double)t[3] / (1.0 + (double)(dens_decay * dt)));
+    t[0] = pos[0];
+    t[1] = pos[1];
+    t[2] = pos[2];
+    t[3] = d;
+  }
+}
+
+// SmokeSolver3D::write_tracers' records, SS/Smoke_solver3D.h:128-140:
+// (x/lx - 0.5, y/lx, z/lx - 0.5, density), the subtraction in double.
+void oracle_tracer_records(const float* tracers, int n, float lx, float* out) {
+  for (int q = 0; q < n; ++q) {
+    const float* t = tracers + 4 * (size_t)q;
+    float* o = out + 4 * (size_t)q;
+    o[0] = (float)((double)(t[0] / lx) - 0.5);
+    o[1] = t[1] / lx;
+    o[2] = (float)((double)(t[2] / lx) - 0.5);
+    o[3] = t[3];
+  }
+}
+
 // SmokeSolver3D::getDelta, SS/Smoke_solver3D.cpp:1298-1319.
 void oracle_delta(int nx, int ny, int nz, const float* after, const float* before, float* delta) {
   size_t n = (size_t)nx * ny * nz;

@@ -4,7 +4,7 @@ reference's OWN code (oracle/_ref/libvflip_ref.so, compiled from the vFLIP
 sources by oracle/build_ref.py) on small seeded inputs.
 
     python tests/golden/make_golden.py            # every fixture
-    python tests/golden/make_golden.py smoke      # only smoke.npz
+    python tests/golden/make_golden.py smoke      # only smoke.npz (likewise tracers)
 
 Each fixture (.npz) stores its inputs and the reference's outputs, so the
 tests need neither the reference tree nor its library: they check the
@@ -55,6 +55,30 @@ def make_smoke(R):
                         force_params=np.array([0.1, 0.35, 0.06], np.float32), **out)
 
 
+def make_tracers(R):
+    """SmokeSolver3D tracers: emit_tracers (the kept prefix and the count;
+    new positions come from rand()), advect_tracers and write_tracers' bytes."""
+    import tempfile
+
+    rng = np.random.default_rng(37)
+    ni, nj, nk = 14, 12, 10
+    h = np.float32(1 / 14)
+    lengths = np.array([1.0, h * nj, h * nk], np.float32)
+    tr = np.concatenate([rng.uniform(-0.05, 1.05, (1500, 3)), rng.uniform(0.0, 0.05, (1500, 1))], 1)
+    tr = tr.astype(np.float32)
+    emitted = R.emit_tracers(tr, h, lengths, (0.5, 0.2, 0.4), 0.1, 300, seed=1)
+    phi = scenes.random_phi(ni, nj, nk, h, rng, n_spheres=2)
+    u, v, w = scenes.random_velocity(ni, nj, nk, rng, scale=0.6)
+    adv = R.advect_tracers(ni, nj, nk, h, tr, u, v, w, phi, 0.03, 0.7)
+    d = tempfile.mkdtemp()
+    R.write_tracers(adv, lengths[0], d, 12)
+    raw = np.fromfile(os.path.join(d, "Particle_data0012.bin"), np.uint8)
+    np.savez_compressed(os.path.join(OUT, "tracers.npz"), dims=np.array([ni, nj, nk], np.int32), h=h,
+                        lengths=lengths, tracers=tr, emit_kept=emitted[:len(emitted) - 300], emit_count=len(emitted),
+                        phi=phi, u=u, v=v, w=w, dt=np.float32(0.03), dens_decay=np.float32(0.7), advected=adv,
+                        file_bytes=raw)
+
+
 def main(which=()):
     R = oracle.reference()
     if R is None:
@@ -62,6 +86,8 @@ def main(which=()):
     if which:
         if "smoke" in which:
             make_smoke(R)
+        if "tracers" in which:
+            make_tracers(R)
         return
     # 1. projection (face weights, inflow, assembly, AMGPCG 1e-6/50, gradient)
     #    on odd, non-cubic grids with inflow and moving solids
@@ -124,6 +150,7 @@ def main(which=()):
     np.savez_compressed(os.path.join(OUT, "transfer.npz"), dims=np.array([ni, nj, nk], np.int32), h=h,
                         particles=p.view(np.uint8), du=du, dv=dv, dw=dw, g2p=g.view(np.uint8), **out)
     make_smoke(R)
+    make_tracers(R)
     for fn in sorted(os.listdir(OUT)):
         if fn.endswith(".npz"):
             print(fn, os.path.getsize(os.path.join(OUT, fn)))

@@ -145,3 +145,51 @@ def test_gen_heat_and_smokeforce_vs_oracle(gpu_solver, orc):
     # an empty particle set is a no-op
     gpu_solver[1].add_smokeforce(t(np.zeros(0, np.uint8)), r, tp, fh, 0.1, 0.3, 0.01)
     assert len(want.view(PARTICLE_DTYPE)) == 200000
+
+
+# ---- smoke tracers
+
+def test_tracers_golden_and_oracle(gpu_solver, orc, tmp_path):
+    """advect_tracers bit for bit against the reference's fixture; the
+    on-disk file byte for byte; emit_tracers byte for byte against the oracle
+    (same counter-based draws) and, in what the reference's rand() does not
+    decide (kept tracers, their order, the count), against the fixture."""
+    g = golden("tracers")
+    s = gpu_solver[1]
+    ni, nj, nk = (int(x) for x in g["dims"])
+    h = float(g["h"])
+    tr = t(g["tracers"])
+    s.advect_tracers(ni, nj, nk, h, tr, t(g["u"]), t(g["v"]), t(g["w"]), t(g["phi"]), float(g["dt"]),
+                     float(g["dens_decay"]))
+    assert np.array_equal(bits(tr.cpu().numpy()), bits(g["advected"]))
+    s.write_tracers(tr, float(g["lengths"][0]), tmp_path, 12)
+    assert np.array_equal(np.fromfile(tmp_path / "Particle_data0012.bin", np.uint8), g["file_bytes"])
+    e = s.emit_tracers(t(g["tracers"]), h, g["lengths"], (0.5, 0.2, 0.4), 0.1, 300, seed=1).cpu().numpy()
+    assert len(e) == int(g["emit_count"])
+    assert np.array_equal(bits(e[:-300]), bits(g["emit_kept"]))
+    want = orc.emit_tracers(g["tracers"], h, g["lengths"], (0.5, 0.2, 0.4), 0.1, 300, seed=1)
+    assert np.array_equal(bits(e), bits(want))
+
+
+@pytest.mark.parametrize("n,count", [(0, 1000), (200000, 50000), (3, 0)])
+def test_tracers_vs_oracle(gpu_solver, orc, n, count):
+    rng = np.random.default_rng(53)
+    ni, nj, nk = 32, 28, 24
+    h = np.float32(1 / 32)
+    lengths = (1.0, float(h * nj), float(h * nk))
+    tr = np.concatenate([rng.uniform(-0.1, 1.1, (n, 3)), rng.uniform(0.0, 0.03, (n, 1))], 1).astype(np.float32)
+    s = gpu_solver[1]
+    got = s.emit_tracers(t(tr) if n else None, h, lengths, (0.5, 0.3, 0.4), 0.06, count, seed=4).cpu().numpy()
+    want = orc.emit_tracers(tr, h, lengths, (0.5, 0.3, 0.4), 0.06, count, seed=4)
+    assert np.array_equal(bits(got), bits(want))
+    if len(want):
+        phi = scenes.random_phi(ni, nj, nk, h, rng, n_spheres=3)
+        u, v, w = scenes.random_velocity(ni, nj, nk, rng, scale=0.8)
+        g = t(want)
+        s.advect_tracers(ni, nj, nk, h, g, t(u), t(v), t(w), t(phi), 0.02, 0.5)
+        assert np.array_equal(bits(g.cpu().numpy()), bits(orc.advect_tracers(ni, nj, nk, h, want, u, v, w, phi, 0.02,
+                                                                              0.5)))
+    # a capacity the result does not fit is refused
+    if count:
+        with pytest.raises(RuntimeError):
+            s.emit_tracers(t(tr) if n else None, h, lengths, (0.5, 0.3, 0.4), 0.06, count, seed=4, capacity=count - 1)

@@ -322,3 +322,49 @@ def test_rk3_and_smoke_scalars_vs_reference(orc, ref, dims, scale):
     p = scenes.random_particles(ni, nj, nk, h, 2000, rng, margin=1.5)
     same(orc.add_smokeforce(p, rho, temp, fh, 0.2, 0.4, 0.05).view(np.uint8),
          ref.add_smokeforce(p, rho, temp, fh, 0.2, 0.4, 0.05).view(np.uint8))
+
+
+# ---- smoke tracers
+
+def test_tracers_golden(orc):
+    """advect_tracers and write_tracers' records bit for bit against the
+    reference's fixture; emit_tracers keeps the same tracers in the same
+    order and emits the same number (new positions come from rand() there)."""
+    g = golden("tracers")
+    ni, nj, nk = (int(x) for x in g["dims"])
+    h = float(g["h"])
+    adv = orc.advect_tracers(ni, nj, nk, h, g["tracers"], g["u"], g["v"], g["w"], g["phi"], float(g["dt"]),
+                             float(g["dens_decay"]))
+    same(adv.view(np.uint32), g["advected"].view(np.uint32))
+    rec = orc.tracer_records(g["advected"], float(g["lengths"][0]))
+    assert np.array_equal(rec.view(np.uint8).ravel(), g["file_bytes"])
+    e = orc.emit_tracers(g["tracers"], h, g["lengths"], (0.5, 0.2, 0.4), 0.1, 300, seed=1)
+    assert len(e) == int(g["emit_count"])
+    same(e[:len(e) - 300].view(np.uint32), g["emit_kept"].view(np.uint32))
+    new = e[len(e) - 300:]
+    assert np.all(np.sum((new[:, :3] - np.array([0.5, 0.2, 0.4], np.float32)) ** 2, 1) <= 0.1 ** 2 * 1.0001)
+    assert np.all(new[:, 3] == 1.0)
+
+
+def test_tracers_vs_reference(orc, ref, tmp_path):
+    rng = np.random.default_rng(47)
+    ni, nj, nk = 12, 10, 9
+    h = np.float32(1 / 12)
+    lengths = (np.float32(1.0), np.float32(h * nj), np.float32(h * nk))
+    tr = np.concatenate([rng.uniform(-0.1, 1.1, (4000, 3)), rng.uniform(0.0, 0.03, (4000, 1))], 1).astype(np.float32)
+    tr[::7, 3] = 0.01  # exactly at the density threshold (kept only above it)
+    a = orc.emit_tracers(tr, h, lengths, (0.5, 0.3, 0.3), 0.08, 700, seed=9)
+    b = ref.emit_tracers(tr, h, lengths, (0.5, 0.3, 0.3), 0.08, 700, seed=9)
+    assert len(a) == len(b) and np.array_equal(a[:-700].view(np.uint32), b[:-700].view(np.uint32))
+    # the new tracers follow the same law: uniform in the sphere
+    for x in (a[-700:, :3], b[-700:, :3]):
+        rr = np.sqrt(np.sum((x - np.array([0.5, 0.3, 0.3], np.float32)) ** 2, 1)) / 0.08
+        assert rr.max() <= 1.0001 and abs(np.mean(rr ** 3) - 0.5) < 0.05
+    phi = scenes.random_phi(ni, nj, nk, h, rng, n_spheres=3)
+    u, v, w = scenes.random_velocity(ni, nj, nk, rng, scale=0.8)
+    ta = orc.advect_tracers(ni, nj, nk, h, tr, u, v, w, phi, 0.04, 0.3)
+    tb = ref.advect_tracers(ni, nj, nk, h, tr, u, v, w, phi, 0.04, 0.3)
+    same(ta.view(np.uint32), tb.view(np.uint32))
+    ref.write_tracers(ta, lengths[0], tmp_path, 3)
+    raw = np.fromfile(tmp_path / "Particle_data0003.bin", np.uint8)
+    assert np.array_equal(raw, orc.tracer_records(ta, lengths[0]).view(np.uint8).ravel())

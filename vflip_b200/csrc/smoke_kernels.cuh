@@ -256,4 +256,85 @@ __global__ void add_smokeforce_kernel(ParticleRec* __restrict__ p, int np, GridV
   }
 }
 
+// ---------------------------------------------------------------------------
+// Smoke tracers, SmokeSolver3D::emit_tracers / advect_tracers / write_tracers
+// (Smoke_solver3D.h:46-160): float4 records (x, y, z, density).
+
+// emit_tracers' keep test (Smoke_solver3D.h:52-59): inside [2h, L-2h] on
+// every axis (float) and density > 0.01 (compared in double).
+__device__ __forceinline__ bool tracer_kept(const float4 t, float h, float lx, float ly, float lz) {
+  const float m = 2 * h;
+  return t.x > m && t.y > m && t.z > m && t.x < lx - m && t.y < ly - m && t.z < lz - m && (double)t.w > 0.01;
+}
+
+__global__ void tracer_keep_kernel(const float4* __restrict__ tr, int n, float h, float lx, float ly, float lz,
+                                   int* __restrict__ keep) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+    keep[q] = tracer_kept(tr[q], h, lx, ly, lz) ? 1 : 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) keep[n] = 0;
+}
+
+__global__ void tracer_compact_kernel(const float4* __restrict__ tr, int n, const int* __restrict__ keep,
+                                      const int* __restrict__ pos, float4* __restrict__ out) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
+    if (keep[q]) out[pos[q]] = tr[q];
+}
+
+// New tracer `slot` after the *base kept ones: the first of up to 64
+// attempts whose offset, uniform in [-r, r)^3 from the counter hash of
+// (seed, slot, attempt, axis), has x^2 + z^2 + y^2 <= r^2 (the reference's
+// rejection test and sum order; it samples rand() over the cube of
+// half-width r + h, which gives the same uniform law in the sphere).
+__global__ void tracer_emit_kernel(float4* __restrict__ out, const int* __restrict__ base, int count, uint32_t seed,
+                                   float r, float cx, float cy, float cz) {
+  const int m = *base;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < count; s += gridDim.x * blockDim.x) {
+    float ox = 0.0f, oy = 0.0f, oz = 0.0f;
+    for (uint32_t a = 0; a < 64; ++a) {
+      const float x = r * reseed_uniform(seed ^ 0x7f4a7c15u, (uint32_t)s, a, 0);
+      const float y = r * reseed_uniform(seed ^ 0x7f4a7c15u, (uint32_t)s, a, 1);
+      const float z = r * reseed_uniform(seed ^ 0x7f4a7c15u, (uint32_t)s, a, 2);
+      if (x * x + z * z + y * y <= r * r) {
+        ox = x;
+        oy = y;
+        oz = z;
+        break;
+      }
+    }
+    out[m + s] = make_float4(cx + ox, cy + oy, cz + oz, 1.0f);
+  }
+}
+
+// advect_tracers (Smoke_solver3D.h:99-120): traceRK3 with step dt, out of a
+// solid along its normal where the sampled phi is <= 0, density / (1 +
+// decay*dt) with the product in float and the rest in double.
+__global__ void advect_tracers_kernel(float4* __restrict__ tr, int n, GridView u, GridView v, GridView w,
+                                      GridView phi, float dt, float dens_decay) {
+  const double den = 1.0 + (double)(dens_decay * dt);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const float4 t = tr[q];
+    const float p0[3] = {t.x, t.y, t.z};
+    float pos[3];
+    trace_rk3(u, v, w, p0, dt, pos);
+    const float ph = sample_linear(phi, pos[0], pos[1], pos[2]);
+    if (ph <= 0) {
+      float nrm[3];
+      solid_normal(phi, pos, nrm);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) pos[a] = pos[a] - ph * nrm[a];
+    }
+    tr[q] = make_float4(pos[0], pos[1], pos[2], (float)((double)t.w / den));
+  }
+}
+
+// write_tracers' records (Smoke_solver3D.h:128-140): (x/lx - 0.5, y/lx,
+// z/lx - 0.5, density), the subtraction in double.
+__global__ void tracer_records_kernel(const float4* __restrict__ tr, int n, float lx, float4* __restrict__ out) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const float4 t = tr[q];
+    out[q] = make_float4((float)((double)__fdiv_rn(t.x, lx) - 0.5), __fdiv_rn(t.y, lx),
+                         (float)((double)__fdiv_rn(t.z, lx) - 0.5), t.w);
+  }
+}
+
 }  // namespace vflip

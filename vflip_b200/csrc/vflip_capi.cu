@@ -2404,6 +2404,79 @@ int vflip_linear_to_bricks(vflip_ctx* ctx, int nx, int ny, int nz, const float* 
   return VFLIP_OK;
 }
 
+int vflip_emit_tracers(vflip_ctx* ctx, const float* tracers, int n, float h, float lx, float ly, float lz, float cx,
+                       float cy, float cz, float r, int count, unsigned seed, float* out, int capacity, int* n_out) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  if (n < 0 || count < 0 || capacity < 0 || (n > 0 && !tracers) || !out || !n_out || !(h > 0) || !(r >= 0))
+    return ctx->fail(VFLIP_ERR_ARG, "bad argument");
+  if (n > 0 && out == tracers) return ctx->fail(VFLIP_ERR_ARG, "out aliases the tracers");
+  int *keep, *pos;
+  VF_ALLOC(keep, int, "tr_keep", (size_t)n + 1);
+  VF_ALLOC(pos, int, "tr_pos", (size_t)n + 1);
+  const float4* tr = reinterpret_cast<const float4*>(tracers);
+  tracer_keep_kernel<<<grid_for((size_t)n + 1, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(tr, n, h, lx, ly, lz,
+                                                                                            keep);
+  VF_LAUNCH_CHECK();
+  int rc;
+  if ((rc = exclusive_scan(ctx, keep, pos, (size_t)n + 1))) return rc;
+  int m = 0;
+  VF_CUDA(cudaMemcpyAsync(&m, pos + n, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  *n_out = m + count;
+  if ((long long)m + count > capacity)
+    return ctx->fail(VFLIP_ERR_TOO_LARGE, "%d tracers do not fit a capacity of %d", m + count, capacity);
+  float4* o = reinterpret_cast<float4*>(out);
+  if (n > 0) {
+    tracer_compact_kernel<<<grid_for(n, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(tr, n, keep, pos, o);
+    VF_LAUNCH_CHECK();
+  }
+  if (count > 0) {
+    tracer_emit_kernel<<<grid_for(count, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(o, pos + n, count, seed, r, cx,
+                                                                                      cy, cz);
+    VF_LAUNCH_CHECK();
+  }
+  return VFLIP_OK;
+}
+
+int vflip_advect_tracers(vflip_ctx* ctx, int ni, int nj, int nk, float h, float* tracers, int n, const float* u,
+                         const float* v, const float* w, const float* nodal_phi, float dt, float dens_decay) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (n < 0 || (n > 0 && !tracers) || !u || !v || !w || !nodal_phi) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  if (n == 0) return VFLIP_OK;
+  const double hd = h, ih = inv_pow2(h);
+  GridView gu{u, ni + 1, nj, nk, hd, 0.5, 0.0, 0.0, ih}, gv{v, ni, nj + 1, nk, hd, 0.0, 0.5, 0.0, ih},
+      gw{w, ni, nj, nk + 1, hd, 0.0, 0.0, 0.5, ih}, gp{nodal_phi, ni + 1, nj + 1, nk + 1, hd, 0.5, 0.5, 0.5, ih};
+  advect_tracers_kernel<<<grid_for(n, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(
+      reinterpret_cast<float4*>(tracers), n, gu, gv, gw, gp, dt, dens_decay);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+int vflip_write_tracers(vflip_ctx* ctx, const float* tracers, int n, float lx, const char* dir, int frame) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  if (n < 0 || (n > 0 && !tracers) || !dir) return ctx->fail(VFLIP_ERR_ARG, "bad argument");
+  std::vector<float> host((size_t)n * 4);
+  if (n > 0) {
+    float* rec;
+    VF_ALLOC(rec, float, "tr_rec", (size_t)n * 4);
+    tracer_records_kernel<<<grid_for(n, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(
+        reinterpret_cast<const float4*>(tracers), n, lx, reinterpret_cast<float4*>(rec));
+    VF_LAUNCH_CHECK();
+    VF_CUDA(cudaMemcpyAsync(host.data(), rec, sizeof(float) * 4 * (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  char name[4096];
+  if (snprintf(name, sizeof name, "%s/Particle_data%04d.bin", dir, frame) >= (int)sizeof name)
+    return ctx->fail(VFLIP_ERR_ARG, "path too long");
+  FILE* f = fopen(name, "wb");
+  if (!f) return ctx->fail(VFLIP_ERR_ARG, "cannot open %s for writing", name);
+  const size_t wrote = n > 0 ? fwrite(host.data(), sizeof(float) * 4, (size_t)n, f) : 0;
+  const int closed = fclose(f);
+  if (wrote != (size_t)n || closed != 0) return ctx->fail(VFLIP_ERR_ARG, "short write to %s", name);
+  return VFLIP_OK;
+}
+
 }  // extern "C"
 
 extern "C" {

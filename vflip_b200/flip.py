@@ -18,6 +18,11 @@ With ``smoke=True`` the density/temperature block of time_step
 of density and temperature on their 2n^3 grid at h/2 along one shared
 backtrace (vflip_advect_rk3_linear2), gen_heat (vflip_gen_heat) and the
 buoyancy add_smokeforce on the particles (vflip_add_smokeforce).
+
+With ``tracers_per_step > 0`` the tracer block of time_step runs first:
+emit_tracers (the emitter at the source sphere) and advect_tracers through
+the grid velocity (Smoke_solver3D.cpp:330-336, Smoke_solver3D.h:46-120);
+``write_tracers`` stores them in the reference's Particle_data%04d.bin form.
 """
 from dataclasses import dataclass
 
@@ -53,6 +58,8 @@ class FlipParams:
     temp_decay: float = 0.0
     alpha: float = 0.0
     beta: float = 1.0
+    # tracers emitted per step in the source sphere (0: no tracers)
+    tracers_per_step: int = 0
 
     @property
     def h(self):
@@ -88,6 +95,7 @@ class FlipSim:
             self.temp = torch.zeros_like(self.rho)
             self._rho2 = torch.empty_like(self.rho)
             self._temp2 = torch.empty_like(self.rho)
+        self.tracers = torch.zeros((0, 4), dtype=torch.float32, device=dev)
         self.steps = 0
         self.last = None
 
@@ -101,6 +109,11 @@ class FlipSim:
     def step(self):
         p, s, n, h = self.p, self.s, self.p.n, self.p.h
         u, v, w = self.vel
+        if p.tracers_per_step > 0:
+            L = float(np.float32(h) * n)
+            self.tracers = s.emit_tracers(self.tracers if self.tracers.shape[0] else None, h, (L, L, L),
+                                          p.source_centre, p.source_radius, p.tracers_per_step, seed=p.seed + self.steps)
+            s.advect_tracers(n, n, n, h, self.tracers, u, v, w, self.phi, p.dt, p.dens_decay)
         s.advect_flip(n, n, n, h, self.particles, u, v, w, self.phi, p.dt)
         if p.smoke:
             self.smoke_scalars(u, v, w)
@@ -130,3 +143,7 @@ class FlipSim:
         s.gen_heat(self.rho, self.temp, fh, p.dt, p.dens_decay, p.temp_decay, p.smoke_centre, p.smoke_radius,
                    p.smoke_dens, p.smoke_heat)
         s.add_smokeforce(self.particles, self.rho, self.temp, fh, p.alpha, p.beta, p.dt)
+
+    def write_tracers(self, directory, frame):
+        """The tracers as <directory>/Particle_data%04d.bin (SmokeSolver3D::write_tracers)."""
+        self.s.write_tracers(self.tracers, float(np.float32(self.p.h) * self.p.n), directory, frame)

@@ -343,6 +343,30 @@ class Solver:
         self._check(self.lib.vflip_add_smokeforce(self.ctx, _p(particles), self._np(particles), fnx, fny, fnz,
                                                   float(fh), _p(rho), _p(temp), float(alpha), float(beta), float(dt)))
 
+    # ------------------------------------------------------------- tracers
+    def emit_tracers(self, tracers, h, lengths, centre, radius, count, seed=0, capacity=None):
+        """SmokeSolver3D::emit_tracers: returns a new (m, 4) float32 tensor."""
+        n = tracers.shape[0] if tracers is not None else 0
+        cap = n + int(count) if capacity is None else int(capacity)
+        out = self._empty((max(cap, 1), 4), torch.float32)
+        m = C.c_int()
+        self._check(self.lib.vflip_emit_tracers(self.ctx, _p(tracers) if n else None, n, float(h), float(lengths[0]),
+                                                float(lengths[1]), float(lengths[2]), float(centre[0]),
+                                                float(centre[1]), float(centre[2]), float(radius), int(count),
+                                                int(seed) & 0xFFFFFFFF, _p(out), cap, C.byref(m)))
+        return out[:m.value]
+
+    def advect_tracers(self, ni, nj, nk, h, tracers, u, v, w, nodal_phi, dt, dens_decay=0.0):
+        """SmokeSolver3D::advect_tracers, in place on (n, 4) float32 tracers."""
+        self._check(self.lib.vflip_advect_tracers(self.ctx, ni, nj, nk, float(h), _p(tracers), tracers.shape[0], _p(u),
+                                                  _p(v), _p(w), _p(nodal_phi), float(dt), float(dens_decay)))
+
+    def write_tracers(self, tracers, lx, directory, frame):
+        """SmokeSolver3D::write_tracers: <directory>/Particle_data%04d.bin."""
+        n = tracers.shape[0]
+        self._check(self.lib.vflip_write_tracers(self.ctx, _p(tracers) if n else None, n, float(lx),
+                                                 str(directory).encode(), int(frame)))
+
     def delta(self, after, before, out=None):
         if out is None:
             out = torch.empty_like(after)
