@@ -57,6 +57,16 @@ template <typename T, typename A> __device__ __forceinline__ T cvt(A v) { return
 __device__ __forceinline__ double gs_div(double a, double b) { return a / b; }
 __device__ __forceinline__ float gs_div(float a, float b) { return __fdividef(a, b); }
 
+// (i, j, k) of the linear index e of an nx x ny x . grid in 32-bit unsigned
+// arithmetic: every grid here has fewer than 2^31 elements (the host checks),
+// and a 64-bit division costs several times a 32-bit one.
+__device__ __forceinline__ void decode3(size_t e, int nx, int ny, int& i, int& j, int& k) {
+  const unsigned ue = (unsigned)e, row = ue / (unsigned)nx;
+  i = (int)(ue - row * (unsigned)nx);
+  j = (int)(row % (unsigned)ny);
+  k = (int)(row / (unsigned)ny);
+}
+
 __device__ __forceinline__ int linear_tid() {
   return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
 }

@@ -100,7 +100,8 @@ __global__ void prolong_trilinear_kernel(const float* __restrict__ out2, int ch,
       w[e] = V(0);
       continue;
     }
-    const int i = (int)(e % ni), j = (int)((e / ni) % nj), k = (int)(e / ((size_t)ni * nj));
+    int i, j, k;
+    decode3(e, ni, nj, i, j, k);
     const float cx = fminf(fmaxf((i + 0.5f) * inv_b - 0.5f, 0.0f), (float)(X - 1));
     const float cy = fminf(fmaxf((j + 0.5f) * inv_b - 0.5f, 0.0f), (float)(Y - 1));
     const float cz = fminf(fmaxf((k + 0.5f) * inv_b - 0.5f, 0.0f), (float)(Z - 1));
@@ -132,7 +133,8 @@ __global__ void spmv_kernel(const V* __restrict__ x, V* __restrict__ y, const S*
   using A = typename Num<V>::Acc;
   const size_t n = (size_t)ni * nj * nk, sy = (size_t)ni, sz = (size_t)ni * nj;
   for (size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(g % ni), j = (int)((g / ni) % nj), k = (int)(g / sz);
+    int i, j, k;
+    decode3(g, ni, nj, i, j, k);
     A acc = A(0);
     if (k > 0) acc = acc + (A)ldg(zp + g - sz) * ldg(x + g - sz);
     if (j > 0) acc = acc + (A)ldg(yp + g - sy) * ldg(x + g - sy);

@@ -17,7 +17,8 @@ __global__ void plume_sources_kernel(float* __restrict__ rho, float* __restrict_
   const float r2 = radius * radius;
   // pass 1 (cells): source sphere, cell centre (i,j,k)*h
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nc; e += (size_t)gridDim.x * blockDim.x) {
-    int i = (int)(e % ni), j = (int)((e / ni) % nj), k = (int)(e / ((size_t)ni * nj));
+    int i, j, k;
+    decode3(e, ni, nj, i, j, k);
     float dx = i * h - cx, dy = j * h - cy, dz = k * h - cz;
     if (dx * dx + dy * dy + dz * dz <= r2) {
       rho[e] = dens_value;
@@ -32,7 +33,8 @@ __global__ void buoyancy_kernel(const float* __restrict__ rho, const float* __re
                                 int ni, int nj, int nk, float dt, float alpha, float beta) {
   const size_t nv = (size_t)ni * (nj + 1) * nk;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nv; e += (size_t)gridDim.x * blockDim.x) {
-    int i = (int)(e % ni), j = (int)((e / ni) % (nj + 1)), k = (int)(e / ((size_t)ni * (nj + 1)));
+    int i, j, k;
+    decode3(e, ni, nj + 1, i, j, k);
     if (j < 1 || j >= nj) continue;
     size_t c0 = lin3(i, j - 1, k, ni, nj), c1 = lin3(i, j, k, ni, nj);
     float r = 0.5f * (rho[c0] + rho[c1]);

@@ -94,15 +94,18 @@ __global__ void face_weights_kernel(const float* __restrict__ phi, float* __rest
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nu + nv + nw;
        e += (size_t)gridDim.x * blockDim.x) {
     if (e < nu) {
-      int i = (int)(e % (ni + 1)), j = (int)((e / (ni + 1)) % nj), k = (int)(e / ((size_t)(ni + 1) * nj));
+      int i, j, k;
+      decode3(e, ni + 1, nj, i, j, k);
       uw[e] = clamp01(1 - frac4(P(i, j, k), P(i, j + 1, k), P(i, j, k + 1), P(i, j + 1, k + 1)));
     } else if (e < nu + nv) {
       size_t f = e - nu;
-      int i = (int)(f % ni), j = (int)((f / ni) % (nj + 1)), k = (int)(f / ((size_t)ni * (nj + 1)));
+      int i, j, k;
+      decode3(f, ni, nj + 1, i, j, k);
       vw[f] = clamp01(1 - frac4(P(i, j, k), P(i, j, k + 1), P(i + 1, j, k), P(i + 1, j, k + 1)));
     } else {
       size_t f = e - nu - nv;
-      int i = (int)(f % ni), j = (int)((f / ni) % nj), k = (int)(f / ((size_t)ni * nj));
+      int i, j, k;
+      decode3(f, ni, nj, i, j, k);
       ww[f] = clamp01(1 - frac4(P(i, j, k), P(i, j + 1, k), P(i + 1, j, k), P(i + 1, j + 1, k)));
     }
   }
@@ -116,7 +119,8 @@ __global__ void inflow_kernel(const int8_t* __restrict__ bdesc, float* __restric
   const size_t n = (size_t)ni * nj * nk;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     if (bdesc[e] != 1) continue;
-    int i = (int)(e % ni), j = (int)((e / ni) % nj), k = (int)(e / ((size_t)ni * nj));
+    int i, j, k;
+    decode3(e, ni, nj, i, j, k);
     u[lin3(i, j, k, ni + 1, nj)] = U_in;
     u[lin3(i + 1, j, k, ni + 1, nj)] = U_in;
     v[lin3(i, j, k, ni, nj + 1)] = 0.0f;
@@ -144,7 +148,8 @@ __global__ void assemble_kernel(const float* __restrict__ u, const float* __rest
   const size_t n = (size_t)ni * nj * nk;
   const float h2 = h * h;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    int i = (int)(e % ni), j = (int)((e / ni) % nj), k = (int)(e / ((size_t)ni * nj));
+    int i, j, k;
+    decode3(e, ni, nj, i, j, k);
     double d = 0.0, cx = 0.0, cy = 0.0, cz = 0.0, b = 0.0;
     if (i >= 1 && i < ni - 1 && j >= 1 && j < nj - 1 && k >= 1 && k < nk - 1) {
       const size_t iu0 = lin3(i, j, k, ni + 1, nj), iu1 = lin3(i + 1, j, k, ni + 1, nj);
@@ -206,21 +211,24 @@ __global__ void gradient_kernel(const P* __restrict__ p, float* __restrict__ u, 
       return sub ? cur - (dt * diff) / h : cur - diff / h;
     };
     if (e < nu) {
-      int i = (int)(e % (ni + 1)), j = (int)((e / (ni + 1)) % nj), k = (int)(e / ((size_t)(ni + 1) * nj));
+      int i, j, k;
+      decode3(e, ni + 1, nj, i, j, k);
       if (k < nk - 1 && k > 0 && j < nj - 1 && j > 0 && i < ni - hi && i > lo) {
         size_t c = lin3(i, j, k, ni, nj);
         u[e] = upd(u[e], (double)p[c], (double)p[c - 1], uw[e], us[e]);
       }
     } else if (e < nu + nv) {
       size_t f = e - nu;
-      int i = (int)(f % ni), j = (int)((f / ni) % (nj + 1)), k = (int)(f / ((size_t)ni * (nj + 1)));
+      int i, j, k;
+      decode3(f, ni, nj + 1, i, j, k);
       if (k < nk - 1 && k > 0 && j > lo && j < nj - hi && i < ni - 1 && i > 0) {
         size_t c = lin3(i, j, k, ni, nj);
         v[f] = upd(v[f], (double)p[c], (double)p[c - sy], vw[f], vs[f]);
       }
     } else {
       size_t f = e - nu - nv;
-      int i = (int)(f % ni), j = (int)((f / ni) % nj), k = (int)(f / ((size_t)ni * nj));
+      int i, j, k;
+      decode3(f, ni, nj, i, j, k);
       if (k > lo && k < nk - hi && j < nj - 1 && j > 0 && i < ni - 1 && i > 0) {
         size_t c = lin3(i, j, k, ni, nj);
         w[f] = upd(w[f], (double)p[c], (double)p[c - sz], ww[f], ws[f]);

@@ -85,7 +85,8 @@ struct Backtrace {
 };
 
 __device__ __forceinline__ void node_world(const GridView& f, size_t e, float h, float& wx, float& wy, float& wz) {
-  int i = (int)(e % f.nx), j = (int)((e / f.nx) % f.ny), k = (int)(e / ((size_t)f.nx * f.ny));
+  int i, j, k;
+  decode3(e, f.nx, f.ny, i, j, k);
   wx = (float)(((double)(float)i - f.ox) * (double)h);
   wy = (float)(((double)(float)j - f.oy) * (double)h);
   wz = (float)(((double)(float)k - f.oz) * (double)h);
@@ -342,7 +343,8 @@ __global__ void p2g_kernel(const int* __restrict__ start, const float4* __restri
   const size_t n = (size_t)fx * fy * fz;
   const float reach = h * 1.0001f;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    int i = (int)(e % fx), j = (int)((e / fx) % fy), k = (int)(e / ((size_t)fx * fy));
+    int i, j, k;
+    decode3(e, fx, fy, i, j, k);
     float gx = (float)(((double)(float)i - ox) * (double)h);
     float gy = (float)(((double)(float)j - oy) * (double)h);
     float gz = (float)(((double)(float)k - oz) * (double)h);

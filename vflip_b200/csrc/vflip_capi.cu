@@ -2010,6 +2010,7 @@ int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, fl
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (fnx <= 0 || fny <= 0 || fnz <= 0 || !u || !v || !w || !field || !out)
     return ctx->fail(VFLIP_ERR_ARG, "bad argument");
+  if ((size_t)fnx * fny * fnz >= (1ull << 31)) return ctx->fail(VFLIP_ERR_ARG, "field too large");
   if (out == field || out == u || out == v || out == w) return ctx->fail(VFLIP_ERR_ARG, "out aliases an input");
   if (field2 && (!out2 || out2 == field2 || out2 == field || out2 == out || out2 == u || out2 == v || out2 == w ||
                  out == field2))
