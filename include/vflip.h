@@ -293,6 +293,41 @@ int vflip_gen_heat(vflip_ctx* ctx, int fnx, int fny, int fnz, double fh, float d
 int vflip_add_smokeforce(vflip_ctx* ctx, void* particles, int np, int fnx, int fny, int fnz, double fh,
                          const float* rho, const float* temp, float alpha, float beta, float dt);
 
+/* ---- nested subdomain particle transfers ----------------------------------
+ * A SubDomainSolver grid (SS/sub_domain.h, SS/sub_domain.cpp): ni x nj x nk
+ * cells of spacing h whose origin sits at bmin = (bx, by, bz) in world space;
+ * particles keep world positions and every sample is taken at pos - bmin
+ * (float).  Face grids have the main grid's shapes and offsets.  All four
+ * are bit-identical to the reference's (new particles: counter-based draws,
+ * as vflip_reorder_flip). */
+
+/* SubDomainSolver::hash_FLIP (SS/sub_domain.cpp:1087-1109): the cell of
+ * pos - bmin + h/2, truncated and clamped into the grid (every particle has
+ * a cell). */
+int vflip_sub_particle_cells(vflip_ctx* ctx, int ni, int nj, int nk, float h, float bx, float by, float bz,
+                             const void* particles, int np, int* cell_out);
+
+/* SubDomainSolver::particle_to_grid (SS/sub_domain.cpp:1204-1265) after
+ * hash_FLIP, for the components whose pointers are given: within 4 cells of
+ * the subdomain's boundary the tent is 4h wide over the 9^3 neighbouring
+ * cells (determineDist, SS/sub_domain.h:89-103), elsewhere h over 3^3. */
+int vflip_sub_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, float bx, float by, float bz,
+                  const void* particles, int np, float* u, float* ucoef, float* v, float* vcoef, float* w,
+                  float* wcoef);
+
+/* SubDomainSolver::particle_from_grid (SS/sub_domain.cpp:1161-1178): vel +=
+ * the delta grids sampled at pos - bmin, in place. */
+int vflip_sub_g2p(vflip_ctx* ctx, int ni, int nj, int nk, float h, float bx, float by, float bz, void* particles,
+                  int np, const float* du, const float* dv, const float* dw);
+
+/* SubDomainSolver::hash_FLIP + reorder_FLIP (SS/sub_domain.cpp:1087-1159): as
+ * vflip_reorder_flip over the interior cells (1 .. n-2 on each axis) only,
+ * new particles at bmin + (i,j,k) h + r 0.49 h with the subdomain's velocity,
+ * filtered on the subdomain's nodal solid phi. */
+int vflip_sub_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, float bx, float by, float bz,
+                           const void* particles, int np, const float* u, const float* v, const float* w,
+                           const float* nodal_phi, unsigned seed, void* out, int capacity, int* np_out);
+
 /* ---- smoke tracers (float4 records: x, y, z, density) ----------------------- */
 
 /* SmokeSolver3D::emit_tracers (SS/Smoke_solver3D.h:46-85): keeps, in order,

@@ -90,6 +90,12 @@ def _load(path, prefix):
     getattr(lib, p + "_emit_tracers").argtypes = [_P, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I, C.c_uint, _P, _I]
     getattr(lib, p + "_emit_tracers").restype = _I
     getattr(lib, p + "_advect_tracers").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _F, _F]
+    getattr(lib, p + "_sub_hash").argtypes = [_I, _I, _I, _F, _F, _F, _F, _P, _I, _P]
+    getattr(lib, p + "_sub_p2g").argtypes = [_I, _I, _I, _F, _F, _F, _F, _P, _I, _I, _P, _P]
+    getattr(lib, p + "_sub_g2p").argtypes = [_I, _I, _I, _F, _F, _F, _F, _P, _I, _P, _P, _P]
+    getattr(lib, p + "_sub_reorder_flip").argtypes = [_I, _I, _I, _F, _F, _F, _F, _P, _I, _P, _P, _P, _P, C.c_uint,
+                                                      _P, _I]
+    getattr(lib, p + "_sub_reorder_flip").restype = _I
     if prefix == "oracle":
         getattr(lib, p + "_tracer_records").argtypes = [_P, _I, _F, _P]
     else:
@@ -328,6 +334,39 @@ class _Impl:
         """SmokeSolver3D::write_tracers (reference): <directory>/Particle_data%04d.bin."""
         tr = np.ascontiguousarray(tracers, np.float32).reshape(-1, 4)
         self.fn("write_tracers")(_ptr(tr), len(tr), float(lx), str(directory).encode(), int(frame))
+
+    # nested subdomain: an ni x nj x nk grid of spacing h at bmin
+    def sub_hash(self, ni, nj, nk, h, bmin, particles):
+        particles = np.ascontiguousarray(particles, PARTICLE_DTYPE)
+        out = np.zeros(len(particles), np.int32)
+        self.fn("sub_hash")(ni, nj, nk, h, *(float(b) for b in bmin), _ptr(particles), len(particles), _ptr(out))
+        return out
+
+    def sub_p2g(self, ni, nj, nk, h, bmin, particles, comp):
+        particles = np.ascontiguousarray(particles, PARTICLE_DTYPE)
+        shape = (nk + (comp == 2), nj + (comp == 1), ni + (comp == 0))
+        f = np.zeros(shape, np.float32)
+        c = np.zeros(shape, np.float32)
+        self.fn("sub_p2g")(ni, nj, nk, h, *(float(b) for b in bmin), _ptr(particles), len(particles), comp, _ptr(f),
+                           _ptr(c))
+        return f, c
+
+    def sub_g2p(self, ni, nj, nk, h, bmin, particles, du, dv, dw):
+        p = np.array(particles, PARTICLE_DTYPE, copy=True)
+        du, dv, dw = [np.ascontiguousarray(a, np.float32) for a in (du, dv, dw)]
+        self.fn("sub_g2p")(ni, nj, nk, h, *(float(b) for b in bmin), _ptr(p), len(p), _ptr(du), _ptr(dv), _ptr(dw))
+        return p
+
+    def sub_reorder_flip(self, ni, nj, nk, h, bmin, particles, u, v, w, nodal_phi, seed=0):
+        p = np.ascontiguousarray(particles, PARTICLE_DTYPE)
+        u, v, w, phi = [np.ascontiguousarray(a, np.float32) for a in (u, v, w, nodal_phi)]
+        cap = 9 * ni * nj * nk + 16
+        out = np.zeros(cap, PARTICLE_DTYPE)
+        n = self.fn("sub_reorder_flip")(ni, nj, nk, h, *(float(b) for b in bmin), _ptr(p), len(p), _ptr(u), _ptr(v),
+                                        _ptr(w), _ptr(phi), int(seed), _ptr(out), cap)
+        if n < 0 or n > cap:
+            raise RuntimeError("reorder capacity")
+        return out[:n].copy()
 
     def hash(self, ni, nj, nk, h, particles):
         particles = np.ascontiguousarray(particles, PARTICLE_DTYPE)

@@ -578,6 +578,89 @@ void ref_write_tracers(const float* tracers, int n, float lx, const char* dir, i
   s.write_tracers(const_cast<char*>(dir), frame);
 }
 
+// A SubDomainSolver over an ni x nj x nk grid of spacing h at bmin, with the
+// grids the particle transfers touch and the particles loaded.
+static SubDomainSolver* make_sub(int ni, int nj, int nk, float h, float bx, float by, float bz, const void* particles,
+                                 int np) {
+  SubDomainSolver* sd = new SubDomainSolver();
+  sd->_nx = ni; sd->_ny = nj; sd->_nz = nk;
+  sd->_hx = sd->_hy = sd->_hz = h;
+  sd->bmin = Vec3f(bx, by, bz);
+  sd->bmax = sd->bmin + Vec3f((float)ni, (float)nj, (float)nk) * h;
+  sd->_un.init(ni + 1, nj, nk, h, 0.5, 0, 0);
+  sd->_vn.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0);
+  sd->_wn.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5);
+  sd->_utemp.init(ni + 1, nj, nk, h, 0.5, 0, 0);
+  sd->_vtemp.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0);
+  sd->_wtemp.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5);
+  sd->_nodal_solid_phi.init(ni + 1, nj + 1, nk + 1, h, 0.5, 0.5, 0.5);
+  sd->particle_hash.clear();
+  sd->particle_hash.resize((size_t)ni * nj * nk);  // hash_FLIP reserves, then indexes
+  const particle* p = (const particle*)particles;
+  sd->FLIP.assign(p, p + np);
+  return sd;
+}
+
+// SubDomainSolver::hash_FLIP (sub_domain.cpp:1087-1109): cell of each particle.
+void ref_sub_hash(int ni, int nj, int nk, float h, float bx, float by, float bz, const void* particles, int np,
+                  int* cell_out) {
+  SubDomainSolver* sd = make_sub(ni, nj, nk, h, bx, by, bz, particles, np);
+  sd->hash_FLIP();
+  for (int q = 0; q < np; ++q) cell_out[q] = -1;
+  for (size_t c = 0; c < sd->particle_hash.size(); ++c)
+    for (int q : sd->particle_hash[c]) cell_out[q] = (int)c;
+  delete sd;
+}
+
+// SubDomainSolver::particle_to_grid (sub_domain.cpp:1204-1265) after hash_FLIP.
+void ref_sub_p2g(int ni, int nj, int nk, float h, float bx, float by, float bz, const void* particles, int np,
+                 int comp, float* field, float* coef) {
+  SubDomainSolver* sd = make_sub(ni, nj, nk, h, bx, by, bz, particles, np);
+  sd->hash_FLIP();
+  buffer3Df f, c;
+  if (comp == 0) { f.init(ni + 1, nj, nk, h, 0.5, 0, 0); c.init(ni + 1, nj, nk, h, 0.5, 0, 0); }
+  else if (comp == 1) { f.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0); c.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0); }
+  else { f.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5); c.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5); }
+  sd->particle_to_grid(f, c, comp);
+  from_buffer(f, field);
+  from_buffer(c, coef);
+  f.free(); c.free();
+  delete sd;
+}
+
+// SubDomainSolver::particle_from_grid (sub_domain.cpp:1161-1178), in place.
+void ref_sub_g2p(int ni, int nj, int nk, float h, float bx, float by, float bz, void* particles, int np,
+                 const float* du, const float* dv, const float* dw) {
+  SubDomainSolver* sd = make_sub(ni, nj, nk, h, bx, by, bz, particles, np);
+  to_buffer(sd->_utemp, du);
+  to_buffer(sd->_vtemp, dv);
+  to_buffer(sd->_wtemp, dw);
+  sd->particle_from_grid();
+  particle* p = (particle*)particles;
+  for (int q = 0; q < np; ++q) p[q] = sd->FLIP[q];
+  delete sd;
+}
+
+// SubDomainSolver::hash_FLIP + reorder_FLIP (sub_domain.cpp:1087-1159) with
+// rand() seeded by `seed`; returns the new count (copied up to capacity).
+int ref_sub_reorder_flip(int ni, int nj, int nk, float h, float bx, float by, float bz, const void* particles,
+                         int np, const float* u, const float* v, const float* w, const float* nodal_phi,
+                         unsigned seed, void* out, int capacity) {
+  SubDomainSolver* sd = make_sub(ni, nj, nk, h, bx, by, bz, particles, np);
+  to_buffer(sd->_un, u);
+  to_buffer(sd->_vn, v);
+  to_buffer(sd->_wn, w);
+  to_buffer(sd->_nodal_solid_phi, nodal_phi);
+  sd->hash_FLIP();
+  srand(seed);
+  sd->reorder_FLIP();
+  const int n = (int)sd->FLIP.size();
+  particle* o = (particle*)out;
+  for (int q = 0; q < n && q < capacity; ++q) o[q] = sd->FLIP[q];
+  delete sd;
+  return n;
+}
+
 // SmokeSolver3D::getDelta (Smoke_solver3D.cpp:1298-1319): delta = after - before
 // on one nx x ny x nz face grid.
 void ref_delta(int nx, int ny, int nz, const float* after, const float* before, float* delta) {

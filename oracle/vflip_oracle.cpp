@@ -21,6 +21,7 @@
 //   * a 7-point operator is 7 arrays of n doubles, in the order
 //     diag, -x, +x, -y, +y, -z, +z (the CSR column order of one row with the
 //     diagonal moved first).
+#include <climits>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -1114,6 +1115,149 @@ void oracle_tracer_records(const float* tracers, int n, float lx, float* out) {
     o[2] = (float)((double)(t[2] / lx) - 0.5);
     o[3] = t[3];
   }
+}
+
+// ---- the nested subdomain's particle transfers (SubDomainSolver,
+// SS/sub_domain.cpp, SS/sub_domain.h): an ni x nj x nk grid of spacing h
+// whose origin sits at bmin in world space; its samples take pos - bmin
+// (float) and its face grids have the main grid's offsets.
+
+// x86's float -> int conversion: INT_MIN when out of range or NaN
+static int trunc_x86(float t) { return (t >= -2147483648.0f && t < 2147483648.0f) ? (int)t : INT_MIN; }
+
+// SubDomainSolver::hash_FLIP, SS/sub_domain.cpp:1087-1109: the cell of
+// pos - bmin + h/2, truncated and clamped into the grid (every particle is
+// hashed).
+static int sub_cell(const Particle& p, int ni, int nj, int nk, float h, const float* bmin) {
+  const int n[3] = {ni, nj, nk};
+  int c[3];
+  for (int a = 0; a < 3; ++a) {
+    float x = p.pos[a] - bmin[a];
+    x = x + 0.5f * h;
+    const int t = trunc_x86(x / h);
+    c[a] = t < 0 ? 0 : (t > n[a] - 1 ? n[a] - 1 : t);
+  }
+  return (int)lin(c[0], c[1], c[2], ni, nj);
+}
+
+void oracle_sub_hash(int ni, int nj, int nk, float h, float bx, float by, float bz, const void* particles, int np,
+                     int* cell_out) {
+  const Particle* p = (const Particle*)particles;
+  const float bmin[3] = {bx, by, bz};
+  for (int q = 0; q < np; ++q) cell_out[q] = sub_cell(p[q], ni, nj, nk, h, bmin);
+}
+
+// SubDomainSolver::H, SS/sub_domain.h:65-71
+static float sub_tent(float r) {
+  float res = 0;
+  if (r >= -1 && r < 0) res = 1 + r;
+  if (r >= 0 && r < 1) res = 1 - r;
+  return res;
+}
+
+// SubDomainSolver::particle_to_grid, SS/sub_domain.cpp:1204-1265, with
+// determineDist (SS/sub_domain.h:89-103): within 4 cells of the
+// subdomain's boundary (min of i, ni-i, j, nj-j, k, nk-k) the tent is 4h
+// wide and gathers from the 9^3 neighbouring buckets, elsewhere h and 3^3.
+// Buckets in (k, j, i) order, particles in hash order, sum(w) from 1e-5.
+void oracle_sub_p2g(int ni, int nj, int nk, float h, float bx, float by, float bz, const void* particles, int np,
+                    int comp, float* field, float* coef) {
+  const Particle* p = (const Particle*)particles;
+  const float bmin[3] = {bx, by, bz};
+  const size_t nc = (size_t)ni * nj * nk;
+  std::vector<std::vector<int>> bucket(nc);
+  for (int q = 0; q < np; ++q) bucket[(size_t)sub_cell(p[q], ni, nj, nk, h, bmin)].push_back(q);
+  const int fx = ni + (comp == 0), fy = nj + (comp == 1), fz = nk + (comp == 2);
+  const double ox = comp == 0 ? 0.5 : 0.0, oy = comp == 1 ? 0.5 : 0.0, oz = comp == 2 ? 0.5 : 0.0;
+  for (int k = 0; k < fz; ++k)
+    for (int j = 0; j < fy; ++j)
+      for (int i = 0; i < fx; ++i) {
+        const float gx = (float)(((double)(float)i - ox) * (double)h);
+        const float gy = (float)(((double)(float)j - oy) * (double)h);
+        const float gz = (float)(((double)(float)k - oz) * (double)h);
+        const int dist = std::min(std::min(std::min(i, ni - i), std::min(j, nj - j)), std::min(k, nk - k));
+        const int l = dist <= 4 ? 4 : 1;
+        const float hk = dist <= 4 ? (float)(4.0 * (double)h) : h;
+        float tw = 1e-5f, tv = 0.0f;
+        for (int dk = -l; dk <= l; ++dk)
+          for (int dj = -l; dj <= l; ++dj)
+            for (int di = -l; di <= l; ++di) {
+              const int ci = i + di, cj = j + dj, ck = k + dk;
+              if (ci < 0 || ci >= ni || cj < 0 || cj >= nj || ck < 0 || ck >= nk) continue;
+              for (int q : bucket[lin(ci, cj, ck, ni, nj)]) {
+                const float px = p[q].pos[0] - bx, py = p[q].pos[1] - by, pz = p[q].pos[2] - bz;
+                const float wgt = sub_tent((px - gx) / hk) * sub_tent((py - gy) / hk) * sub_tent((pz - gz) / hk);
+                tw += wgt;
+                tv += wgt * p[q].vel[comp];
+              }
+            }
+        const size_t e = lin(i, j, k, fx, fy);
+        coef[e] = tw;
+        field[e] = tv / tw;
+      }
+}
+
+// SubDomainSolver::particle_from_grid, SS/sub_domain.cpp:1161-1178:
+// vel += the delta grids sampled at pos - bmin.
+void oracle_sub_g2p(int ni, int nj, int nk, float h, float bx, float by, float bz, void* particles, int np,
+                    const float* du, const float* dv, const float* dw) {
+  Particle* p = (Particle*)particles;
+  const Grid d[3] = {{du, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0},
+                     {dv, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0},
+                     {dw, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5}};
+  for (int q = 0; q < np; ++q) {
+    const float x = p[q].pos[0] - bx, y = p[q].pos[1] - by, z = p[q].pos[2] - bz;
+    float s[3];
+    for (int a = 0; a < 3; ++a) s[a] = d[a].sample(x, y, z);
+    for (int a = 0; a < 3; ++a) p[q].vel[a] += s[a];
+  }
+}
+
+// SubDomainSolver::hash_FLIP + reorder_FLIP, SS/sub_domain.cpp:1110-1159:
+// as the main grid's, over the interior cells (1 .. n-2 on each axis) only,
+// new particles at bmin + (i, j, k) h + r 0.49 h with the subdomain's
+// velocity, and the final filter on the subdomain's solid phi; r from the
+// counter-based generator of oracle_reorder_flip.
+int oracle_sub_reorder_flip(int ni, int nj, int nk, float h, float bx, float by, float bz, const void* particles,
+                            int np, const float* u, const float* v, const float* w, const float* nodal_phi,
+                            unsigned seed, void* out, int capacity) {
+  const Particle* p = (const Particle*)particles;
+  Particle* o = (Particle*)out;
+  const float bmin[3] = {bx, by, bz};
+  const size_t nc = (size_t)ni * nj * nk;
+  std::vector<std::vector<int>> bucket(nc);
+  for (int q = 0; q < np; ++q) bucket[(size_t)sub_cell(p[q], ni, nj, nk, h, bmin)].push_back(q);
+  const Grid vel[3] = {{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0},
+                       {v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0},
+                       {w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5}};
+  const Grid phi = {nodal_phi, ni + 1, nj + 1, nk + 1, (double)h, 0.5, 0.5, 0.5};
+  std::vector<Particle> all;
+  for (int k = 1; k < nk - 1; ++k)
+    for (int j = 1; j < nj - 1; ++j)
+      for (int i = 1; i < ni - 1; ++i) {
+        const size_t c = lin(i, j, k, ni, nj);
+        const std::vector<int>& b = bucket[c];
+        const int cnt = (int)b.size();
+        const int keep = cnt < 10 ? cnt : 8;
+        for (int e = 0; e < keep; ++e) all.push_back(p[b[e]]);
+        for (int e = cnt; e < 8; ++e) {
+          Particle n = {};
+          const float base[3] = {bx + (float)i * h, by + (float)j * h, bz + (float)k * h};
+          for (int a = 0; a < 3; ++a)
+            n.pos[a] = base[a] + reseed_uniform(seed, (uint32_t)c, (uint32_t)e, (uint32_t)a) * 0.49f * h;
+          const float q0 = n.pos[0] - bx, q1 = n.pos[1] - by, q2 = n.pos[2] - bz;
+          for (int a = 0; a < 3; ++a) n.vel[a] = vel[a].sample(q0, q1, q2);
+          all.push_back(n);
+        }
+      }
+  int count = 0;
+  for (const Particle& q : all) {
+    if (phi.sample(q.pos[0] - bx, q.pos[1] - by, q.pos[2] - bz) >= 0) {
+      if (count < capacity) o[count] = q;
+      ++count;
+    }
+  }
+  return count <= capacity ? count : -count;
 }
 
 // SmokeSolver3D::getDelta, SS/Smoke_solver3D.cpp:1298-1319.

@@ -79,6 +79,29 @@ def make_tracers(R):
                         file_bytes=raw)
 
 
+def make_subdomain(R):
+    """The nested subdomain's particle transfers (SubDomainSolver): hash,
+    widened P2G (3 components), G2P and reorder without seeding (8 particles
+    per cell), on a 14 x 12 x 13 grid at h = 1/64 whose origin is off zero."""
+    rng = np.random.default_rng(67)
+    ni, nj, nk = 12, 10, 11
+    h = np.float32(1 / 64)
+    bmin = np.array([0.25, 0.3, 0.2], np.float32)
+    p = scenes.random_particles(ni, nj, nk, h, 3000, rng, margin=1.5)
+    p["pos"] += bmin
+    out = {"cells": R.sub_hash(ni, nj, nk, h, bmin, p)}
+    for c in range(3):
+        out[f"p2g_f{c}"], out[f"p2g_c{c}"] = R.sub_p2g(ni, nj, nk, h, bmin, p, c)
+    du, dv, dw = scenes.random_velocity(ni, nj, nk, rng)
+    out["g2p"] = R.sub_g2p(ni, nj, nk, h, bmin, p, du, dv, dw).view(np.uint8)
+    phi = scenes.random_phi(ni, nj, nk, h, rng, n_spheres=2)
+    q = scenes.jittered_particles(ni, nj, nk, h, 8, rng)
+    q["pos"] += bmin
+    out["reorder"] = R.sub_reorder_flip(ni, nj, nk, h, bmin, q, du, dv, dw, phi).view(np.uint8)
+    np.savez_compressed(os.path.join(OUT, "subdomain.npz"), dims=np.array([ni, nj, nk], np.int32), h=h, bmin=bmin,
+                        particles=p.view(np.uint8), du=du, dv=dv, dw=dw, phi=phi, jittered=q.view(np.uint8), **out)
+
+
 def main(which=()):
     R = oracle.reference()
     if R is None:
@@ -88,6 +111,8 @@ def main(which=()):
             make_smoke(R)
         if "tracers" in which:
             make_tracers(R)
+        if "subdomain" in which:
+            make_subdomain(R)
         return
     # 1. projection (face weights, inflow, assembly, AMGPCG 1e-6/50, gradient)
     #    on odd, non-cubic grids with inflow and moving solids
@@ -151,6 +176,7 @@ def main(which=()):
                         particles=p.view(np.uint8), du=du, dv=dv, dw=dw, g2p=g.view(np.uint8), **out)
     make_smoke(R)
     make_tracers(R)
+    make_subdomain(R)
     for fn in sorted(os.listdir(OUT)):
         if fn.endswith(".npz"):
             print(fn, os.path.getsize(os.path.join(OUT, fn)))

@@ -74,6 +74,11 @@ SIGNATURES = {
                                       _P]),
     "vflip_gen_heat": (_I, [_P, _I, _I, _I, _D, _F, _F, _F, _F, _F, _F, _F, _F, _F, _P, _P]),
     "vflip_add_smokeforce": (_I, [_P, _P, _I, _I, _I, _I, _D, _P, _P, _F, _F, _F]),
+    "vflip_sub_particle_cells": (_I, [_P, _I, _I, _I, _F, _F, _F, _F, _P, _I, _P]),
+    "vflip_sub_p2g": (_I, [_P, _I, _I, _I, _F, _F, _F, _F, _P, _I, _P, _P, _P, _P, _P, _P]),
+    "vflip_sub_g2p": (_I, [_P, _I, _I, _I, _F, _F, _F, _F, _P, _I, _P, _P, _P]),
+    "vflip_sub_reorder_flip": (_I, [_P, _I, _I, _I, _F, _F, _F, _F, _P, _I, _P, _P, _P, _P, C.c_uint, _P, _I,
+                                    C.POINTER(_I)]),
     "vflip_emit_tracers": (_I, [_P, _P, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I, C.c_uint, _P, _I, C.POINTER(_I)]),
     "vflip_advect_tracers": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _F, _F]),
     "vflip_write_tracers": (_I, [_P, _P, _I, _F, C.c_char_p, _I]),

@@ -13,6 +13,7 @@
 // contents in insertion order, Smoke_solver3D.cpp:1477-1502).  The sums are
 // deterministic and bit-identical to the reference.
 #pragma once
+#include <climits>
 #include "common.cuh"
 
 namespace vflip {
@@ -193,11 +194,40 @@ __device__ __forceinline__ int hash_cell(const float* pos, int ni, int nj, int n
   return ((int)tz * nj + (int)ty) * ni + (int)tx;
 }
 
+// The frame of a nested subdomain grid (SubDomainSolver): origin bmin in
+// world space; `sub` selects its clamped hash.  The main grid passes origin 0
+// and sub = 0 (x - 0.0f is x, so its arithmetic is unchanged).
+struct SubFrame {
+  float bx, by, bz;
+  int sub;
+};
+
+// SubDomainSolver::hash_FLIP, sub_domain.cpp:1087-1109: the cell of
+// pos - bmin + h/2, truncated (x86 semantics: out of range or NaN gives
+// INT_MIN) and clamped into the grid, so every particle is hashed.
+__device__ __forceinline__ int trunc_x86(float t) {
+  return (t >= -2147483648.0f && t < 2147483648.0f) ? (int)t : INT_MIN;
+}
+__device__ __forceinline__ int sub_hash_cell(const float* pos, int ni, int nj, int nk, float h, float inv_h,
+                                             const SubFrame& f) {
+  const float b[3] = {f.bx, f.by, f.bz};
+  const int n[3] = {ni, nj, nk};
+  int c[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float x = pos[a] - b[a];
+    x = x + 0.5f * h;
+    const int t = trunc_x86(fdiv_h(x, h, inv_h));
+    c[a] = t < 0 ? 0 : (t > n[a] - 1 ? n[a] - 1 : t);
+  }
+  return (c[2] * nj + c[1]) * ni + c[0];
+}
+
 __global__ void hash_count_kernel(const ParticleRec* __restrict__ p, int np, int ni, int nj, int nk, float h,
                                   float inv_h, int* __restrict__ cell, int* __restrict__ slot,
-                                  int* __restrict__ count) {
+                                  int* __restrict__ count, SubFrame sf) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
-    int c = hash_cell(p[q].pos, ni, nj, nk, h, inv_h);
+    int c = sf.sub ? sub_hash_cell(p[q].pos, ni, nj, nk, h, inv_h, sf) : hash_cell(p[q].pos, ni, nj, nk, h, inv_h);
     cell[q] = c;
     slot[q] = (c >= 0) ? atomicAdd(count + c, 1) : -1;
   }
@@ -311,14 +341,15 @@ __global__ void sort_buckets_kernel(const int* __restrict__ start, int* __restri
 // (1 when all three velocity components are finite), vel.xyz.
 // Only the start[ncells] bucketed particles are gathered (`total` points at
 // that count on the device); particles outside the grid have no slot.
+// Positions are relative to the grid's origin (pos - bmin).
 __global__ void gather_sorted_kernel(const ParticleRec* __restrict__ p, const int* __restrict__ order,
                                      float4* __restrict__ spos, float4* __restrict__ svel,
-                                     const int* __restrict__ total) {
+                                     const int* __restrict__ total, SubFrame sf) {
   const int nsorted = *total;
   for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nsorted; e += gridDim.x * blockDim.x) {
     const ParticleRec& r = p[order[e]];
     bool fin = isfinite(r.vel[0]) && isfinite(r.vel[1]) && isfinite(r.vel[2]);
-    spos[e] = make_float4(r.pos[0], r.pos[1], r.pos[2], fin ? 1.0f : 0.0f);
+    spos[e] = make_float4(r.pos[0] - sf.bx, r.pos[1] - sf.by, r.pos[2] - sf.bz, fin ? 1.0f : 0.0f);
     svel[e] = make_float4(r.vel[0], r.vel[1], r.vel[2], 0.0f);
   }
 }
@@ -335,6 +366,10 @@ __device__ __forceinline__ float tent(float r) {  // SmokeSolver3D::H, Smoke_sol
 // the weight H(dx/h)H(dy/h)H(dz/h).  A particle whose offset from the node
 // exceeds 1.0001 h on some axis has weight exactly 0 and (finite velocity)
 // contributes exactly nothing, so it is skipped without changing any sum.
+// SUB: SubDomainSolver::particle_to_grid (sub_domain.cpp:1204-1265) with
+// determineDist (sub_domain.h:89-103): within 4 cells of the grid's boundary
+// the tent is 4h wide over the 9^3 neighbouring buckets.
+template <bool SUB>
 __global__ void p2g_kernel(const int* __restrict__ start, const float4* __restrict__ spos,
                            const float4* __restrict__ svel, float* __restrict__ field, float* __restrict__ coef,
                            int comp, int ni, int nj, int nk, float h, float inv_h) {
@@ -348,14 +383,25 @@ __global__ void p2g_kernel(const int* __restrict__ start, const float4* __restri
     float gx = (float)(((double)(float)i - ox) * (double)h);
     float gy = (float)(((double)(float)j - oy) * (double)h);
     float gz = (float)(((double)(float)k - oz) * (double)h);
+    int l = 1;
+    float hk = h, ihk = inv_h, rk = reach;
+    if (SUB) {
+      const int dist = min(min(min(i, ni - i), min(j, nj - j)), min(k, nk - k));
+      if (dist <= 4) {
+        l = 4;
+        hk = (float)(4.0 * (double)h);
+        ihk = inv_h * 0.25f;  // exact: inv_h is a power of two or 0
+        rk = hk * 1.0001f;
+      }
+    }
     float tw = 1e-5f, tv = 0.0f;
-    for (int dk = -1; dk <= 1; ++dk) {
+    for (int dk = -l; dk <= l; ++dk) {
       int ck = k + dk;
       if (ck < 0 || ck >= nk) continue;
-      for (int dj = -1; dj <= 1; ++dj) {
+      for (int dj = -l; dj <= l; ++dj) {
         int cj = j + dj;
         if (cj < 0 || cj >= nj) continue;
-        for (int di = -1; di <= 1; ++di) {
+        for (int di = -l; di <= l; ++di) {
           int ci = i + di;
           if (ci < 0 || ci >= ni) continue;
           int c = (ck * nj + cj) * ni + ci;
@@ -363,8 +409,8 @@ __global__ void p2g_kernel(const int* __restrict__ start, const float4* __restri
           for (int q = b; q < en; ++q) {
             float4 pp = __ldg(spos + q);
             float dx = pp.x - gx, dy = pp.y - gy, dz = pp.z - gz;
-            if (pp.w != 0.0f && (fabsf(dx) >= reach || fabsf(dy) >= reach || fabsf(dz) >= reach)) continue;
-            float wgt = tent(fdiv_h(dx, h, inv_h)) * tent(fdiv_h(dy, h, inv_h)) * tent(fdiv_h(dz, h, inv_h));
+            if (pp.w != 0.0f && (fabsf(dx) >= rk || fabsf(dy) >= rk || fabsf(dz) >= rk)) continue;
+            float wgt = tent(fdiv_h(dx, hk, ihk)) * tent(fdiv_h(dy, hk, ihk)) * tent(fdiv_h(dz, hk, ihk));
             float4 vv = __ldg(svel + q);
             float vc = comp == 0 ? vv.x : (comp == 1 ? vv.y : vv.z);
             tw = tw + wgt;
@@ -382,11 +428,13 @@ __global__ void p2g_kernel(const int* __restrict__ start, const float4* __restri
 // vel += trilinear(delta)); otherwise the FLIP/PIC blend of
 // fluid_particle::interpolate, fluid_particle.h:315-328, evaluated in double:
 // vel = (1 - f) u_new(pos) + f (vel + delta(pos)).
+// Samples are taken at pos - bmin (SubDomainSolver::particle_from_grid,
+// sub_domain.cpp:1161-1178, for a subdomain; origin 0 for the main grid).
 __global__ void g2p_kernel(ParticleRec* __restrict__ p, int np, GridView du, GridView dv, GridView dw, GridView un,
-                           GridView vn, GridView wn, double flip_ratio) {
+                           GridView vn, GridView wn, double flip_ratio, SubFrame sf) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
     ParticleRec r = p[q];
-    double x = r.pos[0], y = r.pos[1], z = r.pos[2];
+    double x = r.pos[0] - sf.bx, y = r.pos[1] - sf.by, z = r.pos[2] - sf.bz;
     float d0 = sample_linear(du, x, y, z), d1 = sample_linear(dv, x, y, z), d2 = sample_linear(dw, x, y, z);
     if (flip_ratio == 1.0) {
       r.vel[0] = r.vel[0] + d0;
@@ -490,37 +538,49 @@ __device__ __forceinline__ float reseed_uniform(uint32_t seed, uint32_t cell, ui
 
 // reorder_FLIP, Smoke_solver3D.cpp:1347-1396: particles written per cell -
 // fewer than 8: all kept + topped up to 8; 8 or 9: all; 10+: the first 8
-__global__ void reorder_count_kernel(const int* __restrict__ start, int* __restrict__ out_count, int nc) {
+// For a subdomain (sub != 0) only the interior cells (1 .. n-2 on every
+// axis) are walked (SubDomainSolver::reorder_FLIP, sub_domain.cpp:1110-1159).
+__device__ __forceinline__ bool reorder_cell(int c, int ni, int nj, int nk, int sub) {
+  if (!sub) return true;
+  const int i = c % ni, j = (c / ni) % nj, k = c / (ni * nj);
+  return i >= 1 && i < ni - 1 && j >= 1 && j < nj - 1 && k >= 1 && k < nk - 1;
+}
+
+__global__ void reorder_count_kernel(const int* __restrict__ start, int* __restrict__ out_count, int nc, int ni,
+                                     int nj, int nk, int sub) {
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
     const int cnt = start[c + 1] - start[c];
-    out_count[c] = cnt < 8 ? 8 : (cnt < 10 ? cnt : 8);
+    out_count[c] = !reorder_cell(c, ni, nj, nk, sub) ? 0 : (cnt < 8 ? 8 : (cnt < 10 ? cnt : 8));
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) out_count[nc] = 0;
 }
 
 // one thread per cell: kept particles in bucket order, then the new ones at
-// (i, j, k) h + r 0.49 h with the grid velocity there, density and
-// temperature 0 (get_velocity_self, Smoke_solver3D.cpp:89-97)
+// bmin + (i, j, k) h + r 0.49 h with the grid velocity there (sampled at
+// pos - bmin), density and temperature 0 (get_velocity_self,
+// Smoke_solver3D.cpp:89-97; SubDomainSolver::get_velocity, sub_domain.cpp:69-76)
 __global__ void reorder_write_kernel(const ParticleRec* __restrict__ p, const int* __restrict__ start,
                                      const int* __restrict__ order, const int* __restrict__ base,
                                      ParticleRec* __restrict__ tmp, int ni, int nj, int nk, float h, GridView u,
-                                     GridView v, GridView w, uint32_t seed) {
+                                     GridView v, GridView w, uint32_t seed, SubFrame sf) {
   const int nc = ni * nj * nk;
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    if (!reorder_cell(c, ni, nj, nk, sf.sub)) continue;
     const int s0 = start[c], cnt = start[c + 1] - s0, b = base[c];
     const int keep = cnt < 10 ? cnt : 8;
     for (int e = 0; e < keep; ++e) tmp[b + e] = p[order[s0 + e]];
     if (cnt < 8) {
       const int i = c % ni, j = (c / ni) % nj, k = c / (ni * nj);
-      const float bx = (float)i * h, by = (float)j * h, bz = (float)k * h;
+      const float bx = sf.bx + (float)i * h, by = sf.by + (float)j * h, bz = sf.bz + (float)k * h;
       for (int e = cnt; e < 8; ++e) {
         ParticleRec r;
         r.pos[0] = bx + reseed_uniform(seed, (uint32_t)c, (uint32_t)e, 0u) * 0.49f * h;
         r.pos[1] = by + reseed_uniform(seed, (uint32_t)c, (uint32_t)e, 1u) * 0.49f * h;
         r.pos[2] = bz + reseed_uniform(seed, (uint32_t)c, (uint32_t)e, 2u) * 0.49f * h;
-        r.vel[0] = sample_linear(u, r.pos[0], r.pos[1], r.pos[2]);
-        r.vel[1] = sample_linear(v, r.pos[0], r.pos[1], r.pos[2]);
-        r.vel[2] = sample_linear(w, r.pos[0], r.pos[1], r.pos[2]);
+        const float q0 = r.pos[0] - sf.bx, q1 = r.pos[1] - sf.by, q2 = r.pos[2] - sf.bz;
+        r.vel[0] = sample_linear(u, q0, q1, q2);
+        r.vel[1] = sample_linear(v, q0, q1, q2);
+        r.vel[2] = sample_linear(w, q0, q1, q2);
         r.dens = 0.0f;
         r.temp = 0.0f;
         r.hash_idx = 0;
@@ -533,10 +593,11 @@ __global__ void reorder_write_kernel(const ParticleRec* __restrict__ p, const in
 
 // keep flag: sampled solid phi >= 0 (reorder_FLIP's final filter)
 __global__ void solid_keep_kernel(const ParticleRec* __restrict__ tmp, const int* __restrict__ total,
-                                  int* __restrict__ keep, GridView phi, int cap) {
+                                  int* __restrict__ keep, GridView phi, int cap, SubFrame sf) {
   const int n = min(*total, cap);
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
-    keep[q] = sample_linear(phi, tmp[q].pos[0], tmp[q].pos[1], tmp[q].pos[2]) >= 0.0f ? 1 : 0;
+    keep[q] = sample_linear(phi, tmp[q].pos[0] - sf.bx, tmp[q].pos[1] - sf.by, tmp[q].pos[2] - sf.bz) >= 0.0f ? 1
+                                                                                                             : 0;
   if (blockIdx.x == 0 && threadIdx.x == 0) keep[n] = 0;
 }
 

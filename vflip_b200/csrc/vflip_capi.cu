@@ -2175,8 +2175,8 @@ int vflip_delta(vflip_ctx* ctx, size_t n, const float* after, const float* befor
   return VFLIP_OK;
 }
 
-int vflip_particle_cells(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
-                         int* cell_out) {
+static int particle_cells_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
+                         int* cell_out, SubFrame sf) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (np < 0 || (np > 0 && (!particles || !cell_out))) return ctx->fail(VFLIP_ERR_ARG, "bad argument");
@@ -2187,9 +2187,14 @@ int vflip_particle_cells(vflip_ctx* ctx, int ni, int nj, int nk, float h, const 
   VF_ALLOC(count, int, "p_count", nc + 1);
   VF_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (nc + 1), ctx->stream));
   hash_count_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
-      (const ParticleRec*)particles, np, ni, nj, nk, h, (float)inv_pow2(h), cell_out, slot, count);
+      (const ParticleRec*)particles, np, ni, nj, nk, h, (float)inv_pow2(h), cell_out, slot, count, sf);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
+}
+
+int vflip_particle_cells(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
+                         int* cell_out) {
+  return particle_cells_impl(ctx, ni, nj, nk, h, particles, np, cell_out, SubFrame{0.0f, 0.0f, 0.0f, 0});
 }
 
 }  // extern "C"
@@ -2221,8 +2226,8 @@ int exclusive_scan(vflip_ctx* ctx, const int* in, int* out, size_t n, int depth 
 
 extern "C" {
 
-int vflip_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np, float* u,
-              float* ucoef, float* v, float* vcoef, float* w, float* wcoef) {
+static int p2g_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np, float* u,
+              float* ucoef, float* v, float* vcoef, float* w, float* wcoef, SubFrame sf) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (np < 0 || (np > 0 && !particles)) return ctx->fail(VFLIP_ERR_ARG, "bad particle array");
@@ -2242,7 +2247,7 @@ int vflip_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* parti
   VF_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (nc + 1), ctx->stream));
   if (np > 0) {
     hash_count_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
-        (const ParticleRec*)particles, np, ni, nj, nk, h, (float)inv_pow2(h), cell, slot, count);
+        (const ParticleRec*)particles, np, ni, nj, nk, h, (float)inv_pow2(h), cell, slot, count, sf);
     VF_LAUNCH_CHECK();
   }
   if ((rc = exclusive_scan(ctx, count, start, nc + 1))) return rc;
@@ -2252,19 +2257,27 @@ int vflip_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* parti
     sort_buckets_kernel<<<grid_for(nc, 256, ctx->num_sms), 256, 0, ctx->stream>>>(start, order, (int)nc);
     VF_LAUNCH_CHECK();
     gather_sorted_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
-        (const ParticleRec*)particles, order, spos, svel, start + nc);
+        (const ParticleRec*)particles, order, spos, svel, start + nc, sf);
     VF_LAUNCH_CHECK();
   }
   float* outs[3][2] = {{u, ucoef}, {v, vcoef}, {w, wcoef}};
   for (int c = 0; c < 3; ++c) {
     if (!outs[c][0]) continue;
     size_t nf = (size_t)(ni + (c == 0)) * (nj + (c == 1)) * (nk + (c == 2));
-    p2g_kernel<<<grid_for(nf, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(start, spos, svel, outs[c][0],
-                                                                             outs[c][1], c, ni, nj, nk, h,
-                                                                             (float)inv_pow2(h));
+    if (sf.sub)
+      p2g_kernel<true><<<grid_for(nf, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(
+          start, spos, svel, outs[c][0], outs[c][1], c, ni, nj, nk, h, (float)inv_pow2(h));
+    else
+      p2g_kernel<false><<<grid_for(nf, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(
+          start, spos, svel, outs[c][0], outs[c][1], c, ni, nj, nk, h, (float)inv_pow2(h));
     VF_LAUNCH_CHECK();
   }
   return VFLIP_OK;
+}
+
+int vflip_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np, float* u,
+              float* ucoef, float* v, float* vcoef, float* w, float* wcoef) {
+  return p2g_impl(ctx, ni, nj, nk, h, particles, np, u, ucoef, v, vcoef, w, wcoef, SubFrame{0.0f, 0.0f, 0.0f, 0});
 }
 
 int vflip_advect_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np, const float* u,
@@ -2282,9 +2295,9 @@ int vflip_advect_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* par
   return VFLIP_OK;
 }
 
-int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
+static int reorder_flip_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
                        const float* u, const float* v, const float* w, const float* nodal_phi, unsigned seed,
-                       void* out, int capacity, int* np_out) {
+                       void* out, int capacity, int* np_out, SubFrame sf) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (np < 0 || (np > 0 && !particles) || !u || !v || !w || !nodal_phi || !out || !np_out || capacity < 0)
@@ -2308,7 +2321,7 @@ int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const vo
   VF_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (nc + 1), ctx->stream));
   if (np > 0) {
     hash_count_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
-        (const ParticleRec*)particles, np, ni, nj, nk, h, (float)inv_pow2(h), cell, slot, count);
+        (const ParticleRec*)particles, np, ni, nj, nk, h, (float)inv_pow2(h), cell, slot, count, sf);
     VF_LAUNCH_CHECK();
   }
   if ((rc = exclusive_scan(ctx, count, start, nc + 1))) return rc;
@@ -2318,16 +2331,17 @@ int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const vo
     sort_buckets_kernel<<<grid_for(nc, 256, ctx->num_sms), 256, 0, ctx->stream>>>(start, order, (int)nc);
     VF_LAUNCH_CHECK();
   }
-  reorder_count_kernel<<<grid_for(nc, 256, ctx->num_sms), 256, 0, ctx->stream>>>(start, ocount, (int)nc);
+  reorder_count_kernel<<<grid_for(nc, 256, ctx->num_sms), 256, 0, ctx->stream>>>(start, ocount, (int)nc, ni, nj,
+                                                                                  nk, sf.sub);
   VF_LAUNCH_CHECK();
   if ((rc = exclusive_scan(ctx, ocount, base, nc + 1))) return rc;
   const double hd = h, ih = inv_pow2(h);
   GridView gu{u, ni + 1, nj, nk, hd, 0.5, 0.0, 0.0, ih}, gv{v, ni, nj + 1, nk, hd, 0.0, 0.5, 0.0, ih},
       gw{w, ni, nj, nk + 1, hd, 0.0, 0.0, 0.5, ih}, gp{nodal_phi, ni + 1, nj + 1, nk + 1, hd, 0.5, 0.5, 0.5, ih};
   reorder_write_kernel<<<grid_for(nc, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(
-      (const ParticleRec*)particles, start, order, base, tmp, ni, nj, nk, h, gu, gv, gw, (uint32_t)seed);
+      (const ParticleRec*)particles, start, order, base, tmp, ni, nj, nk, h, gu, gv, gw, (uint32_t)seed, sf);
   VF_LAUNCH_CHECK();
-  solid_keep_kernel<<<grid_for(ntmp, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(tmp, base + nc, keep, gp, ntmp);
+  solid_keep_kernel<<<grid_for(ntmp, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(tmp, base + nc, keep, gp, ntmp, sf);
   VF_LAUNCH_CHECK();
   if ((rc = exclusive_scan(ctx, keep, kpos, (size_t)ntmp + 1))) return rc;
   compact_kernel<<<grid_for(ntmp, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(tmp, keep, kpos, base + nc,
@@ -2345,9 +2359,23 @@ int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const vo
   return VFLIP_OK;
 }
 
-int vflip_g2p(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np, const float* du,
+int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
+                       const float* u, const float* v, const float* w, const float* nodal_phi, unsigned seed,
+                       void* out, int capacity, int* np_out) {
+  return reorder_flip_impl(ctx, ni, nj, nk, h, particles, np, u, v, w, nodal_phi, seed, out, capacity, np_out,
+                  SubFrame{0.0f, 0.0f, 0.0f, 0});
+}
+
+int vflip_sub_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, float bx, float by, float bz,
+                           const void* particles, int np, const float* u, const float* v, const float* w,
+                           const float* nodal_phi, unsigned seed, void* out, int capacity, int* np_out) {
+  return reorder_flip_impl(ctx, ni, nj, nk, h, particles, np, u, v, w, nodal_phi, seed, out, capacity, np_out,
+                           SubFrame{bx, by, bz, 1});
+}
+
+static int g2p_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np, const float* du,
               const float* dv, const float* dw, const float* un, const float* vn, const float* wn,
-              double flip_ratio) {
+              double flip_ratio, SubFrame sf) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (np < 0 || (np > 0 && !particles) || !du || !dv || !dw) return ctx->fail(VFLIP_ERR_ARG, "bad argument");
@@ -2361,9 +2389,33 @@ int vflip_g2p(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, 
   GridView gvn{vn ? vn : dv, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0, ih};
   GridView gwn{wn ? wn : dw, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5, ih};
   g2p_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>((ParticleRec*)particles, np, gdu, gdv, gdw,
-                                                                       gun, gvn, gwn, flip_ratio);
+                                                                       gun, gvn, gwn, flip_ratio, sf);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
+}
+
+int vflip_g2p(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np, const float* du,
+              const float* dv, const float* dw, const float* un, const float* vn, const float* wn,
+              double flip_ratio) {
+  return g2p_impl(ctx, ni, nj, nk, h, particles, np, du, dv, dw, un, vn, wn, flip_ratio,
+                  SubFrame{0.0f, 0.0f, 0.0f, 0});
+}
+
+int vflip_sub_particle_cells(vflip_ctx* ctx, int ni, int nj, int nk, float h, float bx, float by, float bz,
+                             const void* particles, int np, int* cell_out) {
+  return particle_cells_impl(ctx, ni, nj, nk, h, particles, np, cell_out, SubFrame{bx, by, bz, 1});
+}
+
+int vflip_sub_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, float bx, float by, float bz,
+                  const void* particles, int np, float* u, float* ucoef, float* v, float* vcoef, float* w,
+                  float* wcoef) {
+  return p2g_impl(ctx, ni, nj, nk, h, particles, np, u, ucoef, v, vcoef, w, wcoef, SubFrame{bx, by, bz, 1});
+}
+
+int vflip_sub_g2p(vflip_ctx* ctx, int ni, int nj, int nk, float h, float bx, float by, float bz, void* particles,
+                  int np, const float* du, const float* dv, const float* dw) {
+  return g2p_impl(ctx, ni, nj, nk, h, particles, np, du, dv, dw, nullptr, nullptr, nullptr, 1.0,
+                  SubFrame{bx, by, bz, 1});
 }
 
 }  // extern "C"

@@ -343,6 +343,42 @@ class Solver:
         self._check(self.lib.vflip_add_smokeforce(self.ctx, _p(particles), self._np(particles), fnx, fny, fnz,
                                                   float(fh), _p(rho), _p(temp), float(alpha), float(beta), float(dt)))
 
+    # ------------------------------------------------------------- nested subdomain
+    def sub_particle_cells(self, ni, nj, nk, h, bmin, particles):
+        n = self._np(particles)
+        out = self._empty((n,), torch.int32)
+        self._check(self.lib.vflip_sub_particle_cells(self.ctx, ni, nj, nk, float(h), *(float(b) for b in bmin),
+                                                      _p(particles), n, _p(out)))
+        return out
+
+    def sub_particle_to_grid(self, ni, nj, nk, h, bmin, particles, components=(0, 1, 2)):
+        """SubDomainSolver::particle_to_grid: {comp: (field, coef)} on the subdomain's face grids."""
+        n = self._np(particles)
+        shapes = _face_shapes(ni, nj, nk)
+        outs = {c: (self._empty(shapes[c], torch.float32), self._empty(shapes[c], torch.float32)) for c in components}
+        ptrs = []
+        for c in range(3):
+            ptrs += [_p(outs[c][0]), _p(outs[c][1])] if c in outs else [None, None]
+        self._check(self.lib.vflip_sub_p2g(self.ctx, ni, nj, nk, float(h), *(float(b) for b in bmin), _p(particles),
+                                           n, *ptrs))
+        return outs
+
+    def sub_particle_from_grid(self, ni, nj, nk, h, bmin, particles, du, dv, dw):
+        """SubDomainSolver::particle_from_grid, in place."""
+        self._check(self.lib.vflip_sub_g2p(self.ctx, ni, nj, nk, float(h), *(float(b) for b in bmin), _p(particles),
+                                           self._np(particles), _p(du), _p(dv), _p(dw)))
+
+    def sub_reorder_flip(self, ni, nj, nk, h, bmin, particles, u, v, w, nodal_phi, seed=0, capacity=None):
+        """SubDomainSolver::hash_FLIP + reorder_FLIP: a new particle tensor."""
+        n = self._np(particles)
+        cap = 9 * ni * nj * nk if capacity is None else int(capacity)
+        out = torch.empty(max(cap, 1) * PARTICLE_BYTES, dtype=torch.uint8, device=self.device)
+        cnt = C.c_int()
+        self._check(self.lib.vflip_sub_reorder_flip(self.ctx, ni, nj, nk, float(h), *(float(b) for b in bmin),
+                                                    _p(particles), n, _p(u), _p(v), _p(w), _p(nodal_phi),
+                                                    int(seed) & 0xFFFFFFFF, _p(out), cap, C.byref(cnt)))
+        return out[:cnt.value * PARTICLE_BYTES]
+
     # ------------------------------------------------------------- tracers
     def emit_tracers(self, tracers, h, lengths, centre, radius, count, seed=0, capacity=None):
         """SmokeSolver3D::emit_tracers: returns a new (m, 4) float32 tensor."""
