@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner arm")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched uneven-Poisson arm")
     ap.add_argument("--no-flip", action="store_true", help="skip the FLIP smoke arm")
+    ap.add_argument("--no-nested", action="store_true", help="skip the nested-subdomain arm")
     ap.add_argument("--learned-level", type=int, default=1)
     ap.add_argument("--learned-capture", type=int, default=40)
     ap.add_argument("--learned-epochs", type=int, default=16)
@@ -245,6 +246,8 @@ def run_vflip(a):
         if not a.no_flip and world == 1:
             out["flip"] = flip_arm(solver, a.steps)
             out["advection_forms"] = advection_arm(solver)
+        if not a.no_nested and world == 1:
+            out["nested"] = nested_arm(a.steps, device=local)
     solver.close()
     if world > 1:
         dist.destroy_process_group()
@@ -341,6 +344,67 @@ def flip_arm(solver, steps, n=128, warmup=3):
     ms = e0.elapsed_time(e1)
     out["with_smoke_scalars"] = {"steps_per_s": steps / (ms * 1e-3), "ms_per_step": ms / steps,
                                  "scalar_grid": 2 * n, "particles": sim.num_particles}
+    return out
+
+
+def nested_arm(steps, device, n=128, warmup=3):
+    """The nested-subdomain workload: a 128^3 FLIP plume (source sphere r =
+    0.12 at (0.5, 0.1, 0.5), walls on five faces, open top, dt 0.005) with a
+    subdomain over the central half at 2x refinement (128^3 cells at h/2, the
+    resolution of a 256^3 grid), coupled as SmokeSolver3D::time_step couples
+    its SubDomainSolver: both particle passes, the main MGPCG to 1e-6 and the
+    subdomain's to 1e-9, in the mixed-precision context (FP32 V-cycle with
+    BF16 coarse operators, FP64 PCG scalars and coarsest solve).  CUDA events
+    around `steps` steps after `warmup`.  Then one step from the reached state
+    is repeated in an FP64 context: `fp64_rel_err` is max |v - v64| / max |v64|
+    over the main and subdomain velocities."""
+    import torch
+
+    from vflip_b200.flip import NestedFlipSim, NestedParams
+    from vflip_b200.solver import Solver
+
+    prm = NestedParams(n=n, dt=0.005, obstacle_radius=0.0)
+    with Solver(precision=PREC["mixed"], device=device) as s, Solver(precision=PREC["fp64"], device=device) as s64:
+        sim = NestedFlipSim(s, prm)
+        for _ in range(warmup):
+            sim.step()
+        np0, nsp0 = sim.num_particles, sim.num_sub_particles
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        it, sit = [], []
+        for _ in range(steps):
+            conv, st, sst = sim.step()
+            it.append(st.iterations)
+            sit.append(sst.iterations)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out = {"grid": n, "subdomain_cells": list(sim.sdims), "subdomain_h": float(sim.sh),
+               "steps_per_s": steps / (ms * 1e-3), "ms_per_step": ms / steps,
+               "particles_main_pass": np0 + nsp0, "subdomain_particles": sim.num_sub_particles,
+               "pcg_iterations_mean": sum(it) / len(it), "sub_pcg_iterations_mean": sum(sit) / len(sit),
+               "precision": "mixed"}
+        # one step from this state in both precisions
+        keep = {k: getattr(sim, k).clone() for k in ("particles", "sub_particles", "tracers")}
+        keep_vel = [x.clone() for x in sim.vel] + [x.clone() for x in sim.sub_vel]
+        keep_p = (sim.pressure.clone(), sim.sub_pressure.clone(), sim.steps)
+        sim.step()
+        mixed = [x.clone() for x in sim.vel] + [x.clone() for x in sim.sub_vel]
+        for k, val in keep.items():
+            setattr(sim, k, val)
+        sim.vel, sim.sub_vel = keep_vel[:3], keep_vel[3:]
+        sim.pressure.copy_(keep_p[0])
+        sim.sub_pressure.copy_(keep_p[1])
+        sim.steps = keep_p[2]
+        sim.s = s64
+        sim.sub_desc = s64.subdomain(sim.sdims, sim.sh, sim.bmin, *sim.sub_vel, sim.sphi)
+        sim.step()
+        ref = list(sim.vel) + list(sim.sub_vel)
+        err = max(float((a - b).abs().max()) for a, b in zip(mixed, ref))
+        scale = max(float(b.abs().max()) for b in ref)
+        out["fp64_rel_err"] = err / scale if scale > 0 else None
+        del sim
     return out
 
 

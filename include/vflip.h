@@ -328,6 +328,74 @@ int vflip_sub_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, floa
                            const void* particles, int np, const float* u, const float* v, const float* w,
                            const float* nodal_phi, unsigned seed, void* out, int capacity, int* np_out);
 
+/* ---- the main grid with its nested subdomain active --------------------------
+ *
+ * SmokeSolver3D's samplers defer to its SubDomainSolver inside the
+ * subdomain's box (SS/Smoke_solver3D.cpp:61-124, SS/sub_domain.cpp:61-105):
+ *   get_velocity    inside is_in2 (5 h_s from the box faces) the main grid's
+ *                   velocity v becomes c v_sub + (1 - c) v, v_sub sampled at
+ *                   pos - bmin, c = get_boundary_coef (the distance to the box
+ *                   5 h_s inside, over 4 h_s, clamped to [0, 1]);
+ *   get_solid_phi / get_solid_normal
+ *                   inside is_in (2 h_s) the subdomain's nodal phi at
+ *                   pos - bmin (its gradient with spacing h_s).
+ * The calls below are the main solver's routines with those samplers; the
+ * subdomain's own routines are the vflip_sub_* calls above. */
+
+/* A nested subdomain: ni x nj x nk cells of spacing h at bmin (bmax =
+ * bmin + (ni, nj, nk) h), its face velocities and nodal solid phi (device,
+ * linear layout). */
+typedef struct vflip_subdomain {
+  int ni, nj, nk;
+  float h;
+  float bmin[3];
+  const float* u;
+  const float* v;
+  const float* w;
+  const float* nodal_phi;
+} vflip_subdomain;
+
+/* vflip_advect_flip through the nested samplers (advect_FLIP,
+ * SS/Smoke_solver3D.cpp:1407-1449, with the subdomain active). */
+int vflip_advect_flip_nested(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np,
+                             const float* u, const float* v, const float* w, const float* nodal_phi, float dt,
+                             const vflip_subdomain* sub);
+
+/* vflip_reorder_flip whose final solid filter is the nested get_solid_phi
+ * (reorder_FLIP, SS/Smoke_solver3D.cpp:1347-1396, with the subdomain active;
+ * new particles still take the main grid's velocity). */
+int vflip_reorder_flip_nested(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
+                              const float* u, const float* v, const float* w, const float* nodal_phi, unsigned seed,
+                              void* out, int capacity, int* np_out, const vflip_subdomain* sub);
+
+/* The halo selection of SmokeSolver3D::time_step (SS/Smoke_solver3D.cpp:390-398):
+ * copies, in order, the particles strictly inside [bmin - dx, bmax + dx] on
+ * every axis (SubDomainSolver::is_halo, SS/sub_domain.h:202-213) with
+ * dx = 0.5 h, h the MAIN grid's spacing, to `out` (device, `capacity`
+ * records); *n_out (HOST) gets the count (VFLIP_ERR_TOO_LARGE when it
+ * exceeds capacity).  Synchronises the stream. */
+int vflip_halo_select(vflip_ctx* ctx, const void* particles, int np, float h, const vflip_subdomain* sub, void* out,
+                      int capacity, int* n_out);
+
+/* vflip_advect_tracers through the nested samplers (advect_tracers,
+ * SS/Smoke_solver3D.h:99-120, with the subdomain active). */
+int vflip_advect_tracers_nested(vflip_ctx* ctx, int ni, int nj, int nk, float h, float* tracers, int n,
+                                const float* u, const float* v, const float* w, const float* nodal_phi, float dt,
+                                float dens_decay, const vflip_subdomain* sub);
+
+/* emit_tracers with the subdomain's seeding (SS/Smoke_solver3D.h:46-96):
+ * vflip_emit_tracers, then for each subdomain cell in (k, j, i) order four
+ * candidates at bmin + (i, j, k) h_s + r h_s (r uniform in [0, 1)^3) of
+ * density 1, kept where the nested solid phi over the main grid's nodal_phi
+ * (ni x nj x nk cells of spacing h) lies in (0, h_s).  The reference draws r
+ * from rand(); here r comes from a counter-based hash of (seed, cell, slot,
+ * axis).  *n_out gets the total; VFLIP_ERR_TOO_LARGE when it exceeds
+ * `capacity`.  Synchronises the stream. */
+int vflip_emit_tracers_nested(vflip_ctx* ctx, const float* tracers, int n, float h, float lx, float ly, float lz,
+                              float cx, float cy, float cz, float r, int count, unsigned seed, int ni, int nj, int nk,
+                              const float* nodal_phi, const vflip_subdomain* sub, float* out, int capacity,
+                              int* n_out);
+
 /* ---- smoke tracers (float4 records: x, y, z, density) ----------------------- */
 
 /* SmokeSolver3D::emit_tracers (SS/Smoke_solver3D.h:46-85): keeps, in order,
@@ -337,7 +405,7 @@ int vflip_sub_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, floa
  * rand() over a cube of half-width r + h; this library rejection-samples a
  * counter-based hash of (seed, slot, attempt) over the sphere's bounding
  * cube: the same law, other positions.  The nested subdomain's seeding
- * (:86-96) is not part of this call.  `out` (capacity float4, must not alias
+ * (:86-96) is vflip_emit_tracers_nested.  `out` (capacity float4, must not alias
  * `tracers`) receives the result and *n_out (HOST) its count; when that
  * exceeds `capacity` nothing is written and VFLIP_ERR_TOO_LARGE returns.
  * Synchronises the stream. */

@@ -32,6 +32,24 @@ _F = C.c_float
 _D = C.c_double
 
 
+class SubDesc(C.Structure):
+    """The nested subdomain as the main solver's samplers see it (the layout of
+    the C ABI's vflip_subdomain): cells, spacing, origin, face velocities and
+    nodal solid phi."""
+    _fields_ = [("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int), ("h", C.c_float), ("bmin", C.c_float * 3),
+                ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p), ("nodal_phi", C.c_void_p)]
+
+
+def sub_desc(sub):
+    """(SubDesc, arrays kept alive) from sub = dict(dims=(ni, nj, nk), h=, bmin=,
+    u=, v=, w=, phi=) with numpy grids in the linear layout."""
+    ni, nj, nk = (int(x) for x in sub["dims"])
+    arrs = [np.ascontiguousarray(sub[k], np.float32) for k in ("u", "v", "w", "phi")]
+    d = SubDesc(ni, nj, nk, float(sub["h"]), (C.c_float * 3)(*[float(x) for x in sub["bmin"]]),
+                *[a.ctypes.data for a in arrs])
+    return d, arrs
+
+
 def _ptr(a):
     return None if a is None else C.c_void_p(a.ctypes.data)
 
@@ -96,6 +114,21 @@ def _load(path, prefix):
     getattr(lib, p + "_sub_reorder_flip").argtypes = [_I, _I, _I, _F, _F, _F, _F, _P, _I, _P, _P, _P, _P, C.c_uint,
                                                       _P, _I]
     getattr(lib, p + "_sub_reorder_flip").restype = _I
+    sd = C.POINTER(SubDesc)
+    getattr(lib, p + "_advect_flip_nested").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _F, sd]
+    getattr(lib, p + "_reorder_flip_nested").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, C.c_uint, _P, _I,
+                                                         sd]
+    getattr(lib, p + "_reorder_flip_nested").restype = _I
+    getattr(lib, p + "_advect_tracers_nested").argtypes = [_I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _F, _F, sd]
+    getattr(lib, p + "_emit_tracers_nested").argtypes = [_P, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I, C.c_uint, _I,
+                                                         _I, _I, _P, sd, _P, _I]
+    getattr(lib, p + "_emit_tracers_nested").restype = _I
+    if prefix == "oracle":
+        getattr(lib, p + "_halo_select").argtypes = [_P, _I, sd, _F, _P, _I]
+    else:
+        getattr(lib, p + "_halo_select").argtypes = [_P, _I, _F, sd, _P, _I]
+    getattr(lib, p + "_solid_phi_nested").argtypes = [_I, _I, _I, _F, _P, sd, _P, _I, _P]
+    getattr(lib, p + "_halo_select").restype = _I
     if prefix == "oracle":
         getattr(lib, p + "_tracer_records").argtypes = [_P, _I, _F, _P]
     else:
@@ -414,6 +447,79 @@ class _Impl:
                                     _ptr(out), cap)
         if n < 0 or n > cap:
             raise RuntimeError("reorder capacity")
+        return out[:n].copy()
+
+    # ---- the main solver with its nested subdomain active; `sub` is the dict
+    # of sub_desc (dims, h, bmin, u, v, w, phi)
+
+    def advect_flip_nested(self, ni, nj, nk, h, particles, u, v, w, nodal_phi, dt, sub):
+        """advect_FLIP through the blended get_velocity and the nested solid phi / normal, on a copy."""
+        p = np.array(particles, PARTICLE_DTYPE, copy=True)
+        u, v, w, phi = [np.ascontiguousarray(a, np.float32) for a in (u, v, w, nodal_phi)]
+        d, _keep = sub_desc(sub)
+        self.fn("advect_flip_nested")(ni, nj, nk, h, _ptr(p), len(p), _ptr(u), _ptr(v), _ptr(w), _ptr(phi),
+                                      float(dt), C.byref(d))
+        return p
+
+    def reorder_flip_nested(self, ni, nj, nk, h, particles, u, v, w, nodal_phi, sub, seed=0):
+        """hash_FLIP + reorder_FLIP of the main grid with the nested solid phi in the final filter."""
+        p = np.ascontiguousarray(particles, PARTICLE_DTYPE)
+        u, v, w, phi = [np.ascontiguousarray(a, np.float32) for a in (u, v, w, nodal_phi)]
+        d, _keep = sub_desc(sub)
+        cap = 9 * ni * nj * nk + 16
+        out = np.zeros(cap, PARTICLE_DTYPE)
+        n = self.fn("reorder_flip_nested")(ni, nj, nk, h, _ptr(p), len(p), _ptr(u), _ptr(v), _ptr(w), _ptr(phi),
+                                           int(seed), _ptr(out), cap, C.byref(d))
+        if n < 0 or n > cap:
+            raise RuntimeError("reorder capacity")
+        return out[:n].copy()
+
+    def advect_tracers_nested(self, ni, nj, nk, h, tracers, u, v, w, nodal_phi, dt, dens_decay, sub):
+        """advect_tracers with the subdomain active, on a copy of float4 tracers (n, 4)."""
+        tr = np.array(tracers, np.float32, copy=True).reshape(-1, 4)
+        u, v, w, phi = [np.ascontiguousarray(a, np.float32) for a in (u, v, w, nodal_phi)]
+        d, _keep = sub_desc(sub)
+        self.fn("advect_tracers_nested")(ni, nj, nk, h, _ptr(tr), len(tr), _ptr(u), _ptr(v), _ptr(w), _ptr(phi),
+                                         float(dt), float(dens_decay), C.byref(d))
+        return tr
+
+    def emit_tracers_nested(self, tracers, h, lengths, centre, r, count, dims, nodal_phi, sub, seed=0):
+        """emit_tracers with the subdomain's seeding (main grid dims and nodal phi); new (m, 4) array."""
+        tr = np.ascontiguousarray(tracers, np.float32).reshape(-1, 4)
+        phi = np.ascontiguousarray(nodal_phi, np.float32)
+        d, _keep = sub_desc(sub)
+        sni, snj, snk = sub["dims"]
+        cap = len(tr) + int(count) + 4 * sni * snj * snk + 16
+        out = np.zeros((cap, 4), np.float32)
+        m = self.fn("emit_tracers_nested")(_ptr(tr), len(tr), h, float(lengths[0]), float(lengths[1]),
+                                           float(lengths[2]), float(centre[0]), float(centre[1]), float(centre[2]), r,
+                                           int(count), int(seed), int(dims[0]), int(dims[1]), int(dims[2]),
+                                           _ptr(phi), C.byref(d), _ptr(out), cap)
+        if m < 0 or m > cap:
+            raise RuntimeError("tracer capacity")
+        return out[:m].copy()
+
+    def solid_phi_nested(self, ni, nj, nk, h, nodal_phi, sub, pos):
+        """get_solid_phi with the subdomain active at positions (n, 3)."""
+        x = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        phi = np.ascontiguousarray(nodal_phi, np.float32)
+        d, _keep = sub_desc(sub)
+        out = np.zeros(len(x), np.float32)
+        self.fn("solid_phi_nested")(ni, nj, nk, h, _ptr(phi), C.byref(d), _ptr(x), len(x), _ptr(out))
+        return out
+
+    def halo_select(self, particles, h, sub):
+        """The particles inside the subdomain box widened by half a main cell (h = main spacing)."""
+        p = np.ascontiguousarray(particles, PARTICLE_DTYPE)
+        d, _keep = sub_desc(sub)
+        out = np.zeros(max(len(p), 1), PARTICLE_DTYPE)
+        if self.p == "oracle":
+            n = self.fn("halo_select")(_ptr(p), len(p), C.byref(d), float(np.float32(0.5 * float(np.float32(h)))),
+                                       _ptr(out), len(out))
+        else:
+            n = self.fn("halo_select")(_ptr(p), len(p), float(h), C.byref(d), _ptr(out), len(out))
+        if n < 0:
+            raise RuntimeError("halo capacity")
         return out[:n].copy()
 
     def smoke_step(self, n, h, dt, phi, state, source_centre=(0.5, 0.1, 0.5), source_radius=0.1, alpha=0.1,

@@ -661,6 +661,153 @@ int ref_sub_reorder_flip(int ni, int nj, int nk, float h, float bx, float by, fl
   return n;
 }
 
+// ---- the main solver with its nested subdomain active
+
+// vflip_subdomain's layout: an ni x nj x nk grid of spacing h at bmin, its
+// face velocities and nodal solid phi.
+struct SubDesc {
+  int ni, nj, nk;
+  float h;
+  float bmin[3];
+  const float *u, *v, *w, *nodal_phi;
+};
+
+// s.sub_domain set up as SubDomainSolver::init leaves it (bmax = bmin +
+// (nx, ny, nz) h, sub_domain.h:161-175) with the subdomain's velocity and
+// solid phi loaded.
+static void activate_subdomain(SmokeSolver3D& s, const SubDesc* d) {
+  SubDomainSolver& sd = s.sub_domain;
+  sd._nx = d->ni; sd._ny = d->nj; sd._nz = d->nk;
+  sd._hx = sd._hy = sd._hz = d->h;
+  sd.bmin = Vec3f(d->bmin[0], d->bmin[1], d->bmin[2]);
+  sd.bmax = sd.bmin + Vec3f((float)d->ni, (float)d->nj, (float)d->nk) * d->h;
+  const int ni = d->ni, nj = d->nj, nk = d->nk;
+  const float h = d->h;
+  sd._un.init(ni + 1, nj, nk, h, 0.5, 0, 0);
+  sd._vn.init(ni, nj + 1, nk, h, 0.0, 0.5, 0.0);
+  sd._wn.init(ni, nj, nk + 1, h, 0.0, 0.0, 0.5);
+  sd._nodal_solid_phi.init(ni + 1, nj + 1, nk + 1, h, 0.5, 0.5, 0.5);
+  to_buffer(sd._un, d->u);
+  to_buffer(sd._vn, d->v);
+  to_buffer(sd._wn, d->w);
+  to_buffer(sd._nodal_solid_phi, d->nodal_phi);
+}
+
+static void load_main(SmokeSolver3D& s, int ni, int nj, int nk, float h, const float* u, const float* v,
+                      const float* w, const float* nodal_phi, const SubDesc* sub) {
+  init_solver_grids(s, ni, nj, nk, h);
+  to_buffer(s._un, u);
+  to_buffer(s._vn, v);
+  to_buffer(s._wn, w);
+  to_buffer(s._nodal_solid_phi, nodal_phi);
+  activate_subdomain(s, sub);
+}
+
+// SmokeSolver3D::advect_FLIP (Smoke_solver3D.cpp:1407-1449) with the
+// subdomain's blended get_velocity and its solid phi / normal.
+void ref_advect_flip_nested(int ni, int nj, int nk, float h, void* particles, int np, const float* u,
+                            const float* v, const float* w, const float* nodal_phi, float dt, const SubDesc* sub) {
+  particle* p = (particle*)particles;
+  SmokeSolver3D s;
+  load_main(s, ni, nj, nk, h, u, v, w, nodal_phi, sub);
+  s.FLIP.assign(p, p + np);
+  s.advect_FLIP(dt);
+  for (int q = 0; q < np; ++q) p[q] = s.FLIP[q];
+}
+
+// SmokeSolver3D::hash_FLIP + reorder_FLIP with the subdomain active (its
+// solid phi in the final filter); rand() seeded by `seed`.
+int ref_reorder_flip_nested(int ni, int nj, int nk, float h, const void* particles, int np, const float* u,
+                            const float* v, const float* w, const float* nodal_phi, unsigned seed, void* out,
+                            int capacity, const SubDesc* sub) {
+  const particle* p = (const particle*)particles;
+  SmokeSolver3D s;
+  load_main(s, ni, nj, nk, h, u, v, w, nodal_phi, sub);
+  s.FLIP.assign(p, p + np);
+  s.hash_FLIP();
+  srand(seed);
+  s.reorder_FLIP();
+  particle* o = (particle*)out;
+  const int n = (int)s.FLIP.size();
+  for (int q = 0; q < n && q < capacity; ++q) o[q] = s.FLIP[q];
+  return n;
+}
+
+// SmokeSolver3D::advect_tracers (Smoke_solver3D.h:99-120) with the
+// subdomain active, in place.
+void ref_advect_tracers_nested(int ni, int nj, int nk, float h, float* tracers, int n, const float* u,
+                               const float* v, const float* w, const float* nodal_phi, float dt, float dens_decay,
+                               const SubDesc* sub) {
+  SmokeSolver3D s;
+  load_main(s, ni, nj, nk, h, u, v, w, nodal_phi, sub);
+  s._dens_decay = dens_decay;
+  s.tracers.clear();
+  for (int q = 0; q < n; ++q)
+    s.tracers.push_back(Vec4f(tracers[4 * q], tracers[4 * q + 1], tracers[4 * q + 2], tracers[4 * q + 3]));
+  s.advect_tracers(dt);
+  for (int q = 0; q < n; ++q)
+    for (int a = 0; a < 4; ++a) tracers[4 * q + a] = s.tracers[q][a];
+}
+
+// SmokeSolver3D::emit_tracers (Smoke_solver3D.h:46-97) with the subdomain's
+// seeding active; rand() seeded by `seed`.  Returns the new count (copied
+// up to capacity).
+int ref_emit_tracers_nested(const float* tracers, int n, float h, float lx, float ly, float lz, float cx, float cy,
+                            float cz, float r, int count, unsigned seed, int ni, int nj, int nk,
+                            const float* nodal_phi, const SubDesc* sub, float* out, int capacity) {
+  std::vector<float> zu((size_t)(ni + 1) * (nj + 1) * (nk + 1), 0.0f);
+  SmokeSolver3D s;
+  load_main(s, ni, nj, nk, h, zu.data(), zu.data(), zu.data(), nodal_phi, sub);
+  s._lx = lx; s._ly = ly; s._lz = lz;
+  s.tracers.clear();
+  for (int q = 0; q < n; ++q)
+    s.tracers.push_back(Vec4f(tracers[4 * q], tracers[4 * q + 1], tracers[4 * q + 2], tracers[4 * q + 3]));
+  Vec3f c(cx, cy, cz);
+  s.setEmitter(c, r, (uint)count);
+  srand(seed);
+  s.emit_tracers();
+  const int m = (int)s.tracers.size();
+  for (int q = 0; q < m && q < capacity; ++q)
+    for (int a = 0; a < 4; ++a) out[4 * q + a] = s.tracers[q][a];
+  return m;
+}
+
+// SmokeSolver3D::get_solid_phi (Smoke_solver3D.cpp:104-111) with the
+// subdomain active, at n positions (xyz triples).
+void ref_solid_phi_nested(int ni, int nj, int nk, float h, const float* nodal_phi, const SubDesc* sub,
+                          const float* pos, int n, float* out) {
+  std::vector<float> zu((size_t)(ni + 1) * (nj + 1) * (nk + 1), 0.0f);
+  SmokeSolver3D s;
+  load_main(s, ni, nj, nk, h, zu.data(), zu.data(), zu.data(), nodal_phi, sub);
+  for (int q = 0; q < n; ++q) {
+    Vec3f x(pos[3 * q], pos[3 * q + 1], pos[3 * q + 2]);
+    out[q] = s.get_solid_phi(x);
+  }
+}
+
+// The halo selection of SmokeSolver3D::time_step (Smoke_solver3D.cpp:390-398):
+// the particles SubDomainSolver::is_halo(pos, 0.5 * _hx) accepts, in order;
+// `h` is the main grid's spacing.
+int ref_halo_select(const void* particles, int np, float h, const SubDesc* sub, void* out, int capacity) {
+  SmokeSolver3D s;
+  quiet_subdomain(s.sub_domain);
+  s._hx = s._hy = s._hz = h;
+  s.sub_domain._hx = sub->h;
+  s.sub_domain.bmin = Vec3f(sub->bmin[0], sub->bmin[1], sub->bmin[2]);
+  s.sub_domain.bmax = s.sub_domain.bmin + Vec3f((float)sub->ni, (float)sub->nj, (float)sub->nk) * sub->h;
+  const particle* p = (const particle*)particles;
+  particle* o = (particle*)out;
+  int count = 0;
+  for (int q = 0; q < np; ++q) {
+    particle x = p[q];
+    if (s.sub_domain.is_halo(x.pos, 0.5 * s._hx)) {
+      if (count < capacity) o[count] = x;
+      ++count;
+    }
+  }
+  return count;
+}
+
 // SmokeSolver3D::getDelta (Smoke_solver3D.cpp:1298-1319): delta = after - before
 // on one nx x ny x nz face grid.
 void ref_delta(int nx, int ny, int nz, const float* after, const float* before, float* delta) {

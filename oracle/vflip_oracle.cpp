@@ -10,7 +10,7 @@
 // project, Smoke_Solver/ abbreviated SS/).  The restatement keeps the
 // reference's floating-point types and the order of every sum, so its
 // results are bit-identical to the reference's wherever the reference is
-// deterministic; tests/test_oracle_vs_ref.py pins that against the reference
+// deterministic; tests/test_oracle.py pins that against the reference
 // compiled from its own sources (oracle/build_ref.py) and against the golden
 // fixtures in tests/golden/.  Build with -ffp-contract=off.
 //
@@ -756,12 +756,11 @@ void oracle_g2p(int ni, int nj, int nk, float h, void* particles, int np, const 
 // get_velocity (:71-87; the subdomain blend is inactive): c1 = 2/9 dt,
 // c2 = 3/9 dt computed in double and rounded to float, and - as the reference
 // writes it - c3 = (1 - c1 - c2) dt with c1, c2 already carrying dt.
-static void trace_rk3(const Grid* vel, const float pos[3], float dt, float out[3]) {
+extern "C++" {
+template <class F>
+static void trace_rk3_f(F sample, const float pos[3], float dt, float out[3]) {
   const float c1 = (float)(2.0 / 9.0 * (double)dt), c2 = (float)(3.0 / 9.0 * (double)dt);
   const float c3 = (float)((1.0 - (double)c1 - (double)c2) * (double)dt);
-  auto sample = [&](const float x[3], float v[3]) {
-    for (int a = 0; a < 3; ++a) v[a] = vel[a].sample(x[0], x[1], x[2]);
-  };
   float v1[3], v2[3], v3[3], m1[3], m2[3];
   sample(pos, v1);
   const float half = (float)(0.5 * (double)dt), q3 = (float)(0.75 * (double)dt);
@@ -770,6 +769,13 @@ static void trace_rk3(const Grid* vel, const float pos[3], float dt, float out[3
   for (int a = 0; a < 3; ++a) m2[a] = pos[a] + q3 * v2[a];
   sample(m2, v3);
   for (int a = 0; a < 3; ++a) out[a] = pos[a] + c1 * v1[a] + c2 * v2[a] + c3 * v3[a];
+}
+}  // extern "C++"
+
+static void trace_rk3(const Grid* vel, const float pos[3], float dt, float out[3]) {
+  trace_rk3_f([&](const float x[3], float v[3]) {
+    for (int a = 0; a < 3; ++a) v[a] = vel[a].sample(x[0], x[1], x[2]);
+  }, pos, dt, out);
 }
 
 // Buffer3D::sample_grad, SS/fluid_buffer3D.h:249-257, then normalize
@@ -790,27 +796,130 @@ static void solid_normal(const Grid& phi, const float pos[3], float n[3]) {
   for (int a = 0; a < 3; ++a) n[a] /= mag;
 }
 
+// The nested subdomain as the main solver's samplers see it (vflip_subdomain's
+// layout): an ni x nj x nk grid of spacing h at bmin, its face velocities and
+// nodal solid phi.
+struct SubDesc {
+  int ni, nj, nk;
+  float h;
+  float bmin[3];
+  const float *u, *v, *w, *nodal_phi;
+};
+
+// SmokeSolver3D's samplers with the subdomain active
+// (SS/Smoke_solver3D.cpp:61-124, SS/sub_domain.cpp:61-105, SS/sub_domain.h:176-213).
+struct Nest {
+  float bmin[3], bmax[3], h;
+  Grid vel[3], phi;
+  explicit Nest(const SubDesc& s) : h(s.h) {
+    const int n[3] = {s.ni, s.nj, s.nk};
+    // SubDomainSolver::init, SS/sub_domain.h:161-175: bmax = bmin + (nx, ny, nz) dx
+    for (int a = 0; a < 3; ++a) {
+      bmin[a] = s.bmin[a];
+      bmax[a] = s.bmin[a] + (float)n[a] * s.h;
+    }
+    const double hd = s.h;
+    vel[0] = {s.u, s.ni + 1, s.nj, s.nk, hd, 0.5, 0.0, 0.0};
+    vel[1] = {s.v, s.ni, s.nj + 1, s.nk, hd, 0.0, 0.5, 0.0};
+    vel[2] = {s.w, s.ni, s.nj, s.nk + 1, hd, 0.0, 0.0, 0.5};
+    phi = {s.nodal_phi, s.ni + 1, s.nj + 1, s.nk + 1, hd, 0.5, 0.5, 0.5};
+  }
+  // is_in (m = 2) and is_in2 (m = 5), SS/sub_domain.h:176-201: strictly
+  // inside [bmin + m h, bmax - m h] on every axis, compared in double
+  bool inside(const float p[3], double m) const {
+    for (int a = 0; a < 3; ++a)
+      if (!((double)p[a] > (double)bmin[a] + m * (double)h && (double)p[a] < (double)bmax[a] - m * (double)h))
+        return false;
+    return true;
+  }
+  // get_boundary_coef, SS/sub_domain.cpp:96-105: the distance to the box
+  // 5h inside the subdomain (smallest |component| over both corners) over
+  // 4h, clamped to [0, 1]; all in float
+  float coef(const float p[3]) const {
+    const float m5 = 5.0f * h;
+    float d1 = std::fabs(p[0] - (bmin[0] + m5)), d2 = std::fabs(p[0] - (bmax[0] - m5));
+    for (int a = 1; a < 3; ++a) {
+      const float e1 = std::fabs(p[a] - (bmin[a] + m5)), e2 = std::fabs(p[a] - (bmax[a] - m5));
+      if (e1 < d1) d1 = e1;
+      if (e2 < d2) d2 = e2;
+    }
+    const float d = d2 < d1 ? d2 : d1;
+    const float c = d / (4.0f * h);
+    return c < 0.0f ? 0.0f : (c > 1.0f ? 1.0f : c);
+  }
+  // SubDomainSolver::get_velocity, SS/sub_domain.cpp:69-76: samples at pos - bmin
+  void sub_velocity(const float p[3], float out[3]) const {
+    const float q[3] = {p[0] - bmin[0], p[1] - bmin[1], p[2] - bmin[2]};
+    for (int a = 0; a < 3; ++a) out[a] = vel[a].sample(q[0], q[1], q[2]);
+  }
+};
+
+// SmokeSolver3D::get_velocity, SS/Smoke_solver3D.cpp:71-88: the main grid's
+// velocity, blended inside is_in2 as c vel_sub + (1 - c) vel (float)
+static void nested_velocity(const Grid* vel, const Nest* nest, const float p[3], float out[3]) {
+  for (int a = 0; a < 3; ++a) out[a] = vel[a].sample(p[0], p[1], p[2]);
+  if (nest && nest->inside(p, 5.0)) {
+    float v2[3];
+    nest->sub_velocity(p, v2);
+    const float c = nest->coef(p);
+    for (int a = 0; a < 3; ++a) out[a] = c * v2[a] + (1.0f - c) * out[a];
+  }
+}
+
+// get_solid_phi, SS/Smoke_solver3D.cpp:104-111: the subdomain's nodal phi
+// at pos - bmin inside is_in, the main grid's elsewhere
+static float nested_phi(const Grid& phi, const Nest* nest, const float p[3]) {
+  if (nest && nest->inside(p, 2.0))
+    return nest->phi.sample(p[0] - nest->bmin[0], p[1] - nest->bmin[1], p[2] - nest->bmin[2]);
+  return phi.sample(p[0], p[1], p[2]);
+}
+
+// get_solid_normal, SS/Smoke_solver3D.cpp:112-124: the gradient of the
+// subdomain's phi at pos - bmin (its own h) inside is_in, then normalised
+static void nested_normal(const Grid& phi, const Nest* nest, const float p[3], float n[3]) {
+  if (nest && nest->inside(p, 2.0)) {
+    const float q[3] = {p[0] - nest->bmin[0], p[1] - nest->bmin[1], p[2] - nest->bmin[2]};
+    solid_normal(nest->phi, q, n);
+  } else {
+    solid_normal(phi, p, n);
+  }
+}
+
 // SmokeSolver3D::advect_FLIP, SS/Smoke_solver3D.cpp:1407-1449: RK3 through
 // the grid velocity, then a particle that ends inside a solid (sampled nodal
-// phi < 0) moves out along the solid normal by -phi.
-void oracle_advect_flip(int ni, int nj, int nk, float h, void* particles, int np, const float* u, const float* v,
-                        const float* w, const float* nodal_phi, float dt) {
+// phi < 0) moves out along the solid normal by -phi.  With a subdomain, the
+// velocity, phi and normal are the nested samplers above.
+static void advect_flip_impl(int ni, int nj, int nk, float h, void* particles, int np, const float* u,
+                             const float* v, const float* w, const float* nodal_phi, float dt, const Nest* nest) {
   Particle* p = (Particle*)particles;
   const Grid vel[3] = {{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0},
                        {v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0},
                        {w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5}};
   const Grid phi = {nodal_phi, ni + 1, nj + 1, nk + 1, (double)h, 0.5, 0.5, 0.5};
+  auto sample = [&](const float x[3], float o[3]) { nested_velocity(vel, nest, x, o); };
   for (int q = 0; q < np; ++q) {
     float pos[3];
-    trace_rk3(vel, p[q].pos, dt, pos);
-    const float ph = phi.sample(pos[0], pos[1], pos[2]);
+    trace_rk3_f(sample, p[q].pos, dt, pos);
+    const float ph = nested_phi(phi, nest, pos);
     if (ph < 0) {
       float n[3];
-      solid_normal(phi, pos, n);
+      nested_normal(phi, nest, pos, n);
       for (int a = 0; a < 3; ++a) pos[a] -= ph * n[a];
     }
     for (int a = 0; a < 3; ++a) p[q].pos[a] = pos[a];
   }
+}
+
+void oracle_advect_flip(int ni, int nj, int nk, float h, void* particles, int np, const float* u, const float* v,
+                        const float* w, const float* nodal_phi, float dt) {
+  advect_flip_impl(ni, nj, nk, h, particles, np, u, v, w, nodal_phi, dt, nullptr);
+}
+
+void oracle_advect_flip_nested(int ni, int nj, int nk, float h, void* particles, int np, const float* u,
+                               const float* v, const float* w, const float* nodal_phi, float dt,
+                               const SubDesc* sub) {
+  const Nest nest(*sub);
+  advect_flip_impl(ni, nj, nk, h, particles, np, u, v, w, nodal_phi, dt, &nest);
 }
 
 // Counter-based uniform in [-1, 1) for reseeding: a 32-bit integer mix of
@@ -838,9 +947,11 @@ static float reseed_uniform(uint32_t seed, uint32_t cell, uint32_t slot, uint32_
 // (get_velocity_self, :89-97), density and temperature 0; 8 or 9 stay; 10 or
 // more keep their first 8.  Then particles with sampled solid phi < 0 are
 // dropped.  Returns the count written (or -needed when capacity is short).
-int oracle_reorder_flip(int ni, int nj, int nk, float h, const void* particles, int np, const float* u,
-                        const float* v, const float* w, const float* nodal_phi, unsigned seed, void* out,
-                        int capacity) {
+// With a subdomain the final filter reads the nested solid phi (get_solid_phi);
+// new particles still take the main grid's velocity.
+static int reorder_flip_impl(int ni, int nj, int nk, float h, const void* particles, int np, const float* u,
+                             const float* v, const float* w, const float* nodal_phi, unsigned seed, void* out,
+                             int capacity, const Nest* nest) {
   const Particle* p = (const Particle*)particles;
   Particle* o = (Particle*)out;
   const size_t nc = (size_t)ni * nj * nk;
@@ -873,8 +984,51 @@ int oracle_reorder_flip(int ni, int nj, int nk, float h, const void* particles, 
       }
   int count = 0;
   for (const Particle& q : all) {
-    if (phi.sample(q.pos[0], q.pos[1], q.pos[2]) >= 0) {
+    if (nested_phi(phi, nest, q.pos) >= 0) {
       if (count < capacity) o[count] = q;
+      ++count;
+    }
+  }
+  return count <= capacity ? count : -count;
+}
+
+int oracle_reorder_flip(int ni, int nj, int nk, float h, const void* particles, int np, const float* u,
+                        const float* v, const float* w, const float* nodal_phi, unsigned seed, void* out,
+                        int capacity) {
+  return reorder_flip_impl(ni, nj, nk, h, particles, np, u, v, w, nodal_phi, seed, out, capacity, nullptr);
+}
+
+int oracle_reorder_flip_nested(int ni, int nj, int nk, float h, const void* particles, int np, const float* u,
+                               const float* v, const float* w, const float* nodal_phi, unsigned seed, void* out,
+                               int capacity, const SubDesc* sub) {
+  const Nest nest(*sub);
+  return reorder_flip_impl(ni, nj, nk, h, particles, np, u, v, w, nodal_phi, seed, out, capacity, &nest);
+}
+
+// get_solid_phi with the subdomain active at n positions (xyz triples).
+void oracle_solid_phi_nested(int ni, int nj, int nk, float h, const float* nodal_phi, const SubDesc* sub,
+                             const float* pos, int n, float* out) {
+  const Nest nest(*sub);
+  const Grid phi = {nodal_phi, ni + 1, nj + 1, nk + 1, (double)h, 0.5, 0.5, 0.5};
+  for (int q = 0; q < n; ++q) out[q] = nested_phi(phi, &nest, pos + 3 * (size_t)q);
+}
+
+// SmokeSolver3D::time_step, SS/Smoke_solver3D.cpp:390-398: the particles
+// that SubDomainSolver::is_halo (SS/sub_domain.h:202-213) finds strictly
+// inside [bmin - dx, bmax + dx] on every axis (float), in order; the caller
+// passes dx = 0.5 h of the main grid.  Returns the count (negated, nothing
+// beyond capacity written, when it exceeds capacity).
+int oracle_halo_select(const void* particles, int np, const SubDesc* sub, float dx, void* out, int capacity) {
+  const Nest nest(*sub);
+  const Particle* p = (const Particle*)particles;
+  Particle* o = (Particle*)out;
+  int count = 0;
+  for (int q = 0; q < np; ++q) {
+    bool in = true;
+    for (int a = 0; a < 3; ++a)
+      in = in && p[q].pos[a] > nest.bmin[a] - dx && p[q].pos[a] < nest.bmax[a] + dx;
+    if (in) {
+      if (count < capacity) o[count] = p[q];
       ++count;
     }
   }
@@ -1076,24 +1230,83 @@ int oracle_emit_tracers(const float* tracers, int n, float h, float lx, float ly
   return m + count;
 }
 
+// Counter-based uniform in [0, 1) (frand(0, 1) of the subdomain's tracer
+// seeding): the 24 high bits of the reseeding hash of (seed, cell, slot, axis).
+static float unit_uniform(uint32_t seed, uint32_t cell, uint32_t slot, uint32_t axis) {
+  const uint32_t r = mix32(mix32(mix32(seed ^ 0x2545f491u) + cell) + (slot * 3u + axis));
+  return (float)(r >> 8) * (1.0f / 16777216.0f);
+}
+
+// The nested subdomain's tracer seeding of emit_tracers, SS/Smoke_solver3D.h:86-96:
+// for each subdomain cell in (k, j, i) order, four candidates at
+// bmin + (i, j, k) h_s + r h_s (r uniform in [0, 1)^3, unit_uniform with
+// slot 0..3) of density 1, kept where the nested solid phi is in (0, h_s).
+// Appends to out[m..] up to capacity; returns the number seeded.
+static int seed_sub_tracers(const Grid& phi, const Nest& nest, const SubDesc& sub, unsigned seed, float* out,
+                            int m, int capacity) {
+  int s = 0;
+  for (int k = 0; k < sub.nk; ++k)
+    for (int j = 0; j < sub.nj; ++j)
+      for (int i = 0; i < sub.ni; ++i) {
+        const uint32_t c = (uint32_t)lin(i, j, k, sub.ni, sub.nj);
+        const float base[3] = {nest.bmin[0] + (float)i * sub.h, nest.bmin[1] + (float)j * sub.h,
+                               nest.bmin[2] + (float)k * sub.h};
+        for (uint32_t e = 0; e < 4; ++e) {
+          float pos[3];
+          for (uint32_t a = 0; a < 3; ++a) pos[a] = base[a] + unit_uniform(seed, c, e, a) * sub.h;
+          const float ph = nested_phi(phi, &nest, pos);
+          if (ph > 0 && ph < sub.h) {
+            if (m + s < capacity) {
+              float* t = out + 4 * (size_t)(m + s);
+              t[0] = pos[0];
+              t[1] = pos[1];
+              t[2] = pos[2];
+              t[3] = 1.0f;
+            }
+            ++s;
+          }
+        }
+      }
+  return s;
+}
+
+// emit_tracers with the subdomain active (SS/Smoke_solver3D.h:46-96): the
+// kept tracers, the emitter's `count`, then the subdomain's seeds; the main
+// grid's nodal phi (ni x nj x nk cells of spacing h) and the subdomain's
+// enter the nested solid phi.  Returns the new number of tracers, negated
+// when it exceeds `capacity` (the content is then incomplete).
+int oracle_emit_tracers_nested(const float* tracers, int n, float h, float lx, float ly, float lz, float cx,
+                               float cy, float cz, float r, int count, unsigned seed, int ni, int nj, int nk,
+                               const float* nodal_phi, const SubDesc* sub, float* out, int capacity) {
+  const Nest nest(*sub);
+  const Grid phi = {nodal_phi, ni + 1, nj + 1, nk + 1, (double)h, 0.5, 0.5, 0.5};
+  const int m = oracle_emit_tracers(tracers, n, h, lx, ly, lz, cx, cy, cz, r, count, seed, out, capacity);
+  if (m < 0) return m;
+  const int s = seed_sub_tracers(phi, nest, *sub, seed, out, m, capacity);
+  return m + s <= capacity ? m + s : -(m + s);
+}
+
 // SmokeSolver3D::advect_tracers, SS/Smoke_solver3D.h:99-120: traceRK3 with
 // step dt, then out of a solid along its normal when the sampled nodal phi
 // is <= 0 (advect_FLIP's test is < 0), and the density divided by
 // 1 + decay*dt (the product in float, the sum and the quotient in double).
-void oracle_advect_tracers(int ni, int nj, int nk, float h, float* tracers, int n, const float* u, const float* v,
-                           const float* w, const float* nodal_phi, float dt, float dens_decay) {
+// With a subdomain, the nested velocity, phi and normal.
+static void advect_tracers_impl(int ni, int nj, int nk, float h, float* tracers, int n, const float* u,
+                                const float* v, const float* w, const float* nodal_phi, float dt, float dens_decay,
+                                const Nest* nest) {
   const Grid vel[3] = {{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0},
                        {v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0},
                        {w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5}};
   const Grid phi = {nodal_phi, ni + 1, nj + 1, nk + 1, (double)h, 0.5, 0.5, 0.5};
+  auto sample = [&](const float x[3], float o[3]) { nested_velocity(vel, nest, x, o); };
   for (int q = 0; q < n; ++q) {
     float* t = tracers + 4 * (size_t)q;
     float pos[3];
-    trace_rk3(vel, t, dt, pos);
-    const float ph = phi.sample(pos[0], pos[1], pos[2]);
+    trace_rk3_f(sample, t, dt, pos);
+    const float ph = nested_phi(phi, nest, pos);
     if (ph <= 0) {
       float nrm[3];
-      solid_normal(phi, pos, nrm);
+      nested_normal(phi, nest, pos, nrm);
       for (int a = 0; a < 3; ++a) pos[a] -= ph * nrm[a];
     }
     const float d = (float)((double)t[3] / (1.0 + (double)(dens_decay * dt)));
@@ -1102,6 +1315,18 @@ void oracle_advect_tracers(int ni, int nj, int nk, float h, float* tracers, int 
     t[2] = pos[2];
     t[3] = d;
   }
+}
+
+void oracle_advect_tracers(int ni, int nj, int nk, float h, float* tracers, int n, const float* u, const float* v,
+                           const float* w, const float* nodal_phi, float dt, float dens_decay) {
+  advect_tracers_impl(ni, nj, nk, h, tracers, n, u, v, w, nodal_phi, dt, dens_decay, nullptr);
+}
+
+void oracle_advect_tracers_nested(int ni, int nj, int nk, float h, float* tracers, int n, const float* u,
+                                  const float* v, const float* w, const float* nodal_phi, float dt, float dens_decay,
+                                  const SubDesc* sub) {
+  const Nest nest(*sub);
+  advect_tracers_impl(ni, nj, nk, h, tracers, n, u, v, w, nodal_phi, dt, dens_decay, &nest);
 }
 
 // SmokeSolver3D::write_tracers' records, SS/Smoke_solver3D.h:128-140:

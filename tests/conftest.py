@@ -39,6 +39,15 @@ def golden(name):
     return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
 
 
+def nested_from_golden():
+    """The nested fixture and its subdomain as the dict the oracle and the
+    library take (dims, h, bmin, u, v, w, phi)."""
+    g = golden("nested")
+    sub = dict(dims=tuple(int(x) for x in g["sub_dims"]), h=np.float32(g["sub_h"]), bmin=g["sub_bmin"],
+               u=g["sub_u"], v=g["sub_v"], w=g["sub_w"], phi=g["sub_phi"])
+    return g, sub
+
+
 def problem_from_golden(g):
     ni, nj, nk = (int(x) for x in g["dims"])
     pr = dict(ni=ni, nj=nj, nk=nk, h=float(g["h"]), U_in=float(g["U_in"]))

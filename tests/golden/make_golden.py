@@ -10,6 +10,7 @@ Each fixture (.npz) stores its inputs and the reference's outputs, so the
 tests need neither the reference tree nor its library: they check the
 oracle restatement (CPU) and the CUDA library (GPU) against these arrays.
 """
+import hashlib
 import os
 import sys
 
@@ -102,6 +103,38 @@ def make_subdomain(R):
                         particles=p.view(np.uint8), du=du, dv=dv, dw=dw, phi=phi, jittered=q.view(np.uint8), **out)
 
 
+def make_nested(R):
+    """The main solver with its nested subdomain active (SmokeSolver3D +
+    SubDomainSolver coupling): advect_FLIP through the blended velocity and
+    the nested solid phi/normal, reorder_FLIP without seeding (its solid
+    filter reads the nested phi), the halo selection, advect_tracers, the
+    nested get_solid_phi at probe points, and emit_tracers with the
+    subdomain's seeding (rand(): kept part exact, seeds recorded)."""
+    sc = scenes.nested_scene(seed=71, dims=(16, 14, 12), lo=(4, 3, 3), cells=(8, 7, 6))
+    ni, nj, nk = sc["dims"]
+    h, u, v, w, phi, sub, rng = sc["h"], sc["u"], sc["v"], sc["w"], sc["phi"], sc["sub"], sc["rng"]
+    p = scenes.random_particles(ni, nj, nk, h, 4000, rng)
+    out = {"advect": R.advect_flip_nested(ni, nj, nk, h, p, u, v, w, phi, 0.01, sub).view(np.uint8)}
+    q = scenes.jittered_particles(ni, nj, nk, h, 8, rng)
+    q = np.concatenate([q, q[rng.integers(0, len(q), 300)]])
+    r = R.reorder_flip_nested(ni, nj, nk, h, q, u, v, w, phi, sub)
+    out["reorder_count"] = np.int32(len(r))
+    out["reorder_sha256"] = np.array(hashlib.sha256(r.tobytes()).hexdigest())
+    out["halo"] = R.halo_select(p, h, sub).view(np.uint8)
+    tr = np.concatenate([p["pos"], rng.uniform(0.0, 1.0, (len(p), 1)).astype(np.float32)], 1)
+    out["tracers_advected"] = R.advect_tracers_nested(ni, nj, nk, h, tr, u, v, w, phi, 0.01, 0.1, sub)
+    probes = rng.uniform(0.0, 1.0, (4000, 3)).astype(np.float32) * np.array([ni, nj, nk], np.float32) * h
+    out["probe_phi"] = R.solid_phi_nested(ni, nj, nk, h, phi, sub, probes)
+    lengths = np.array([ni, nj, nk], np.float32) * h
+    e = R.emit_tracers_nested(tr, h, lengths, (0.3, 0.15, 0.25), 0.06, 400, (ni, nj, nk), phi, sub, seed=5)
+    kept = R.emit_tracers(tr, h, lengths, (0.3, 0.15, 0.25), 0.06, 0, seed=5)
+    sub_arrays = {"sub_" + k: np.asarray(sub[k]) for k in ("dims", "h", "bmin", "u", "v", "w", "phi")}
+    np.savez_compressed(os.path.join(OUT, "nested.npz"), dims=np.array([ni, nj, nk], np.int32), h=h, u=u, v=v, w=w,
+                        phi=phi, particles=p.view(np.uint8), jittered=q.view(np.uint8), tracers=tr, probes=probes,
+                        emit_kept=kept, emit_seeds=e[len(kept) + 400:], emit_count=np.int32(len(e)), **sub_arrays,
+                        **out)
+
+
 def main(which=()):
     R = oracle.reference()
     if R is None:
@@ -113,6 +146,8 @@ def main(which=()):
             make_tracers(R)
         if "subdomain" in which:
             make_subdomain(R)
+        if "nested" in which:
+            make_nested(R)
         return
     # 1. projection (face weights, inflow, assembly, AMGPCG 1e-6/50, gradient)
     #    on odd, non-cubic grids with inflow and moving solids
@@ -177,6 +212,7 @@ def main(which=()):
     make_smoke(R)
     make_tracers(R)
     make_subdomain(R)
+    make_nested(R)
     for fn in sorted(os.listdir(OUT)):
         if fn.endswith(".npz"):
             print(fn, os.path.getsize(os.path.join(OUT, fn)))

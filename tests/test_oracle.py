@@ -4,8 +4,9 @@ against the reference directly on fresh seeded inputs."""
 import numpy as np
 import pytest
 
-from conftest import golden, problem_from_golden
+from conftest import golden, nested_from_golden, problem_from_golden
 from vflip_b200 import scenes
+from vflip_b200.particles import PARTICLE_DTYPE
 
 
 def same(a, b):
@@ -416,3 +417,75 @@ def test_subdomain_vs_reference(orc, ref):
     ka, kb = a[a["temp"] > 0], b[b["temp"] > 0]
     same(ka.view(np.uint8), kb.view(np.uint8))
     assert abs(len(a) - len(b)) <= 0.02 * len(b)  # new particles straddling a solid may differ
+
+
+# ---- the main solver with its nested subdomain active (SmokeSolver3D's
+# samplers blend in / defer to SubDomainSolver)
+
+def _nested_args(g):
+    ni, nj, nk = (int(x) for x in g["dims"])
+    return ni, nj, nk, np.float32(g["h"])
+
+
+def test_nested_golden(orc):
+    """advect_FLIP through the blended velocity, reorder_FLIP with the nested
+    solid filter, the halo selection, advect_tracers and get_solid_phi: the
+    oracle reproduces the reference's fixture bit for bit; emit_tracers keeps
+    the same tracers and seeds where the reference's seeds lie."""
+    import hashlib
+    g, sub = nested_from_golden()
+    ni, nj, nk, h = _nested_args(g)
+    u, v, w, phi = g["u"], g["v"], g["w"], g["phi"]
+    p = g["particles"].view(PARTICLE_DTYPE)
+    same(orc.advect_flip_nested(ni, nj, nk, h, p, u, v, w, phi, 0.01, sub).view(np.uint8), g["advect"])
+    r = orc.reorder_flip_nested(ni, nj, nk, h, g["jittered"].view(PARTICLE_DTYPE), u, v, w, phi, sub)
+    assert len(r) == int(g["reorder_count"])
+    assert hashlib.sha256(r.tobytes()).hexdigest() == str(g["reorder_sha256"])
+    same(orc.halo_select(p, h, sub).view(np.uint8), g["halo"])
+    same(orc.advect_tracers_nested(ni, nj, nk, h, g["tracers"], u, v, w, phi, 0.01, 0.1, sub).view(np.uint32),
+         g["tracers_advected"].view(np.uint32))
+    same(orc.solid_phi_nested(ni, nj, nk, h, phi, sub, g["probes"]).view(np.uint32), g["probe_phi"].view(np.uint32))
+    # the blend and the subdomain's phi both change the result
+    assert not np.array_equal(orc.advect_flip(ni, nj, nk, h, p, u, v, w, phi, 0.01).view(np.uint8), g["advect"])
+    lengths = np.array([ni, nj, nk], np.float32) * h
+    e = orc.emit_tracers_nested(g["tracers"], h, lengths, (0.3, 0.15, 0.25), 0.06, 400, (ni, nj, nk), phi, sub, seed=5)
+    kept = g["emit_kept"]
+    same(e[:len(kept)].view(np.uint32), kept.view(np.uint32))
+    seeds, ref_seeds = e[len(kept) + 400:], g["emit_seeds"]
+    # every seed of the reference passes the restated acceptance test
+    sp = orc.solid_phi_nested(ni, nj, nk, h, phi, sub, ref_seeds[:, :3])
+    assert ((sp > 0) & (sp < sub["h"])).all() and (ref_seeds[:, 3] == 1).all()
+    # and both seed about as many: binomial counts over 4 candidates per subdomain cell
+    n = int(g["emit_count"]) - len(kept) - 400
+    assert len(ref_seeds) == n and abs(len(seeds) - n) <= 5 * np.sqrt(2 * n) + 5
+    # the seeds sit in their cells in (k, j, i) order: cell of each seed, floor
+    # over (pos - bmin) / h_s, never decreases (to within rounding at a face)
+    cell = np.floor((seeds[:, :3] - sub["bmin"]) / sub["h"]).astype(np.int64)
+    sni, snj, _ = sub["dims"]
+    lin = cell[:, 0] + sni * (cell[:, 1] + snj * cell[:, 2])
+    assert (np.diff(lin) >= -sni * snj - sni - 1).all()
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_nested_vs_reference(orc, ref, seed):
+    """Fresh scenes: the coupled samplers equal the reference bit for bit;
+    reorder_FLIP's kept particles match with seeding."""
+    sc = scenes.nested_scene(seed=seed, dims=(18, 16, 14), lo=(5, 4, 3), cells=(9, 8, 7))
+    ni, nj, nk = sc["dims"]
+    h, u, v, w, phi, sub, rng = sc["h"], sc["u"], sc["v"], sc["w"], sc["phi"], sc["sub"], sc["rng"]
+    p = scenes.random_particles(ni, nj, nk, h, 5000, rng, margin=2.0)
+    same(orc.advect_flip_nested(ni, nj, nk, h, p, u, v, w, phi, 0.02, sub).view(np.uint8),
+         ref.advect_flip_nested(ni, nj, nk, h, p, u, v, w, phi, 0.02, sub).view(np.uint8))
+    same(orc.halo_select(p, h, sub).view(np.uint8), ref.halo_select(p, h, sub).view(np.uint8))
+    tr = np.concatenate([p["pos"], np.ones((len(p), 1), np.float32)], 1)
+    same(orc.advect_tracers_nested(ni, nj, nk, h, tr, u, v, w, phi, 0.02, 0.3, sub).view(np.uint32),
+         ref.advect_tracers_nested(ni, nj, nk, h, tr, u, v, w, phi, 0.02, 0.3, sub).view(np.uint32))
+    x = rng.uniform(-0.1, 0.7, (3000, 3)).astype(np.float32)
+    same(orc.solid_phi_nested(ni, nj, nk, h, phi, sub, x).view(np.uint32),
+         ref.solid_phi_nested(ni, nj, nk, h, phi, sub, x).view(np.uint32))
+    sparse = p[:2500].copy()
+    sparse["temp"] = np.arange(len(sparse), dtype=np.float32) + 1.0
+    a = orc.reorder_flip_nested(ni, nj, nk, h, sparse, u, v, w, phi, sub, seed=1)
+    b = ref.reorder_flip_nested(ni, nj, nk, h, sparse, u, v, w, phi, sub, seed=1)
+    same(a[a["temp"] > 0].view(np.uint8), b[b["temp"] > 0].view(np.uint8))
+    assert abs(len(a) - len(b)) <= 0.02 * len(b)

@@ -40,6 +40,11 @@ class SystemC(C.Structure):
                 ("yp", C.c_void_p), ("zp", C.c_void_p), ("rhs", C.c_void_p), ("result", C.c_void_p)]
 
 
+class SubdomainC(C.Structure):
+    _fields_ = [("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int), ("h", C.c_float), ("bmin", C.c_float * 3),
+                ("u", C.c_void_p), ("v", C.c_void_p), ("w", C.c_void_p), ("nodal_phi", C.c_void_p)]
+
+
 class LearnedStatsC(C.Structure):
     _fields_ = [("fallback", C.c_int), ("subspace", C.c_int), ("gamma", C.c_double * 4),
                 ("init_residual", C.c_double), ("net_ms", C.c_double)]
@@ -79,6 +84,13 @@ SIGNATURES = {
     "vflip_sub_g2p": (_I, [_P, _I, _I, _I, _F, _F, _F, _F, _P, _I, _P, _P, _P]),
     "vflip_sub_reorder_flip": (_I, [_P, _I, _I, _I, _F, _F, _F, _F, _P, _I, _P, _P, _P, _P, C.c_uint, _P, _I,
                                     C.POINTER(_I)]),
+    "vflip_advect_flip_nested": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _F, C.POINTER(SubdomainC)]),
+    "vflip_reorder_flip_nested": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, C.c_uint, _P, _I, C.POINTER(_I),
+                                       C.POINTER(SubdomainC)]),
+    "vflip_halo_select": (_I, [_P, _P, _I, _F, C.POINTER(SubdomainC), _P, _I, C.POINTER(_I)]),
+    "vflip_advect_tracers_nested": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _F, _F, C.POINTER(SubdomainC)]),
+    "vflip_emit_tracers_nested": (_I, [_P, _P, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I, C.c_uint, _I, _I, _I, _P,
+                                       C.POINTER(SubdomainC), _P, _I, C.POINTER(_I)]),
     "vflip_emit_tracers": (_I, [_P, _P, _I, _F, _F, _F, _F, _F, _F, _F, _F, _I, C.c_uint, _P, _I, C.POINTER(_I)]),
     "vflip_advect_tracers": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _F, _F]),
     "vflip_write_tracers": (_I, [_P, _P, _I, _F, C.c_char_p, _I]),

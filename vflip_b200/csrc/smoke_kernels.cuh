@@ -305,21 +305,73 @@ __global__ void tracer_emit_kernel(float4* __restrict__ out, const int* __restri
   }
 }
 
+// The nested subdomain's tracer seeding of emit_tracers
+// (Smoke_solver3D.h:86-96): four candidates per subdomain cell (k, j, i
+// order) at bmin + (i, j, k) h + r h with r uniform in [0, 1)^3, kept where
+// the main grid's get_solid_phi with the subdomain active lies in (0, h).
+// The reference draws r from rand(); here it is the 24 high bits of a
+// counter-based hash of (seed, cell, slot, axis).
+__device__ __forceinline__ float unit_uniform(uint32_t seed, uint32_t cell, uint32_t slot, uint32_t axis) {
+  const uint32_t r = mix32(mix32(mix32(seed ^ 0x2545f491u) + cell) + (slot * 3u + axis));
+  return (float)(r >> 8) * (1.0f / 16777216.0f);
+}
+
+__device__ __forceinline__ bool tracer_seed(const GridView& phi, const Nest& n, int sni, int snj, uint32_t seed, int e,
+                                            float pos[3]) {
+  const int c = e >> 2, slot = e & 3;
+  int i, j, k;
+  decode3((size_t)c, sni, snj, i, j, k);
+  const float ijk[3] = {(float)i, (float)j, (float)k};
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    pos[a] = (n.bmin[a] + ijk[a] * n.h) + unit_uniform(seed, (uint32_t)c, (uint32_t)slot, (uint32_t)a) * n.h;
+  const float ph = nested_phi(phi, n, pos);
+  return ph > 0.0f && ph < n.h;
+}
+
+// flag[e] for the ncand = 4 * subdomain cells candidates; flag[ncand] = 0
+__global__ void tracer_seed_flag_kernel(GridView phi, Nest n, int sni, int snj, uint32_t seed, int ncand,
+                                        int* __restrict__ flag) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e <= ncand; e += gridDim.x * blockDim.x) {
+    float pos[3];
+    flag[e] = e < ncand && tracer_seed(phi, n, sni, snj, seed, e, pos) ? 1 : 0;
+  }
+}
+
+__global__ void tracer_seed_write_kernel(GridView phi, Nest n, int sni, int snj, uint32_t seed, int ncand,
+                                         const int* __restrict__ flag, const int* __restrict__ pos, int base,
+                                         float4* __restrict__ out) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ncand; e += gridDim.x * blockDim.x) {
+    if (!flag[e]) continue;
+    float x[3];
+    tracer_seed(phi, n, sni, snj, seed, e, x);
+    out[base + pos[e]] = make_float4(x[0], x[1], x[2], 1.0f);
+  }
+}
+
 // advect_tracers (Smoke_solver3D.h:99-120): traceRK3 with step dt, out of a
 // solid along its normal where the sampled phi is <= 0, density / (1 +
-// decay*dt) with the product in float and the rest in double.
+// decay*dt) with the product in float and the rest in double.  NEST: the
+// main grid's samplers with its subdomain active.
+template <bool NEST>
 __global__ void advect_tracers_kernel(float4* __restrict__ tr, int n, GridView u, GridView v, GridView w,
-                                      GridView phi, float dt, float dens_decay) {
+                                      GridView phi, float dt, float dens_decay, Nest nest) {
   const double den = 1.0 + (double)(dens_decay * dt);
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
     const float4 t = tr[q];
     const float p0[3] = {t.x, t.y, t.z};
     float pos[3];
-    trace_rk3(u, v, w, p0, dt, pos);
-    const float ph = sample_linear(phi, pos[0], pos[1], pos[2]);
+    if (NEST)
+      trace_rk3_f([&](const float* x, float* o) { nested_velocity(u, v, w, nest, x, o); }, p0, dt, pos);
+    else
+      trace_rk3(u, v, w, p0, dt, pos);
+    const float ph = NEST ? nested_phi(phi, nest, pos) : sample_linear(phi, pos[0], pos[1], pos[2]);
     if (ph <= 0) {
       float nrm[3];
-      solid_normal(phi, pos, nrm);
+      if (NEST)
+        nested_normal(phi, nest, pos, nrm);
+      else
+        solid_normal(phi, pos, nrm);
 #pragma unroll
       for (int a = 0; a < 3; ++a) pos[a] = pos[a] - ph * nrm[a];
     }

@@ -460,21 +460,31 @@ __global__ void g2p_kernel(ParticleRec* __restrict__ p, int np, GridView du, Gri
 // (subdomain blend inactive): c1 = 2/9 dt and c2 = 3/9 dt rounded from
 // double, and c3 = (1 - c1 - c2) dt as the reference writes it (c1, c2
 // already carry dt).
-__device__ __forceinline__ void trace_rk3(const GridView& u, const GridView& v, const GridView& w, const float p[3],
-                                          float dt, float out[3]) {
+// `vel(x, v)` writes the velocity at x into v.
+template <class F>
+__device__ __forceinline__ void trace_rk3_f(F vel, const float p[3], float dt, float out[3]) {
   const float c1 = (float)(2.0 / 9.0 * (double)dt), c2 = (float)(3.0 / 9.0 * (double)dt);
   const float c3 = (float)((1.0 - (double)c1 - (double)c2) * (double)dt);
   const float half = (float)(0.5 * (double)dt), q3 = (float)(0.75 * (double)dt);
-  const float v1[3] = {sample_linear(u, p[0], p[1], p[2]), sample_linear(v, p[0], p[1], p[2]),
-                       sample_linear(w, p[0], p[1], p[2])};
+  float v1[3], v2[3], v3[3];
+  vel(p, v1);
   const float m1[3] = {p[0] + half * v1[0], p[1] + half * v1[1], p[2] + half * v1[2]};
-  const float v2[3] = {sample_linear(u, m1[0], m1[1], m1[2]), sample_linear(v, m1[0], m1[1], m1[2]),
-                       sample_linear(w, m1[0], m1[1], m1[2])};
+  vel(m1, v2);
   const float m2[3] = {p[0] + q3 * v2[0], p[1] + q3 * v2[1], p[2] + q3 * v2[2]};
-  const float v3[3] = {sample_linear(u, m2[0], m2[1], m2[2]), sample_linear(v, m2[0], m2[1], m2[2]),
-                       sample_linear(w, m2[0], m2[1], m2[2])};
+  vel(m2, v3);
 #pragma unroll
   for (int a = 0; a < 3; ++a) out[a] = p[a] + c1 * v1[a] + c2 * v2[a] + c3 * v3[a];
+}
+
+__device__ __forceinline__ void trace_rk3(const GridView& u, const GridView& v, const GridView& w, const float p[3],
+                                          float dt, float out[3]) {
+  trace_rk3_f(
+      [&](const float* x, float* o) {
+        o[0] = sample_linear(u, x[0], x[1], x[2]);
+        o[1] = sample_linear(v, x[0], x[1], x[2]);
+        o[2] = sample_linear(w, x[0], x[1], x[2]);
+      },
+      p, dt, out);
 }
 
 // get_solid_normal (Smoke_solver3D.cpp:115-124): Buffer3D::sample_grad
@@ -498,18 +508,95 @@ __device__ __forceinline__ void solid_normal(const GridView& phi, const float p[
   n[2] = n[2] / mag;
 }
 
+// The nested subdomain as the main grid's samplers see it: SmokeSolver3D's
+// get_velocity, get_solid_phi and get_solid_normal (Smoke_solver3D.cpp:71-124)
+// defer to SubDomainSolver (sub_domain.cpp:61-105) inside its box.
+struct Nest {
+  float bmin[3], bmax[3], h;
+  GridView u, v, w, phi;  // the subdomain's face velocities and nodal phi (origin bmin)
+};
+
+// is_in (m = 2) and is_in2 (m = 5), sub_domain.h:176-201: strictly inside
+// [bmin + m h, bmax - m h] on every axis, compared in double.
+__device__ __forceinline__ bool nest_inside(const Nest& n, const float p[3], double m) {
+  bool in = true;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+    in = in && (double)p[a] > (double)n.bmin[a] + m * (double)n.h &&
+         (double)p[a] < (double)n.bmax[a] - m * (double)n.h;
+  return in;
+}
+
+// get_boundary_coef, sub_domain.cpp:96-105: the smallest |component| of the
+// offsets to the corners of the box 5h inside the subdomain, over 4h,
+// clamped to [0, 1]; float throughout.
+__device__ __forceinline__ float nest_coef(const Nest& n, const float p[3]) {
+  const float m5 = 5.0f * n.h;
+  float d1 = fabsf(p[0] - (n.bmin[0] + m5)), d2 = fabsf(p[0] - (n.bmax[0] - m5));
+#pragma unroll
+  for (int a = 1; a < 3; ++a) {
+    const float e1 = fabsf(p[a] - (n.bmin[a] + m5)), e2 = fabsf(p[a] - (n.bmax[a] - m5));
+    if (e1 < d1) d1 = e1;
+    if (e2 < d2) d2 = e2;
+  }
+  const float c = __fdiv_rn(d2 < d1 ? d2 : d1, 4.0f * n.h);
+  return c < 0.0f ? 0.0f : (c > 1.0f ? 1.0f : c);
+}
+
+// get_velocity: the main grid's sample, replaced inside is_in2 by
+// c v_sub + (1 - c) v with v_sub sampled at pos - bmin.
+__device__ __forceinline__ void nested_velocity(const GridView& u, const GridView& v, const GridView& w,
+                                                const Nest& n, const float p[3], float o[3]) {
+  o[0] = sample_linear(u, p[0], p[1], p[2]);
+  o[1] = sample_linear(v, p[0], p[1], p[2]);
+  o[2] = sample_linear(w, p[0], p[1], p[2]);
+  if (nest_inside(n, p, 5.0)) {
+    const float q0 = p[0] - n.bmin[0], q1 = p[1] - n.bmin[1], q2 = p[2] - n.bmin[2];
+    const float s[3] = {sample_linear(n.u, q0, q1, q2), sample_linear(n.v, q0, q1, q2),
+                        sample_linear(n.w, q0, q1, q2)};
+    const float c = nest_coef(n, p), c1 = 1.0f - c;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) o[a] = __fadd_rn(__fmul_rn(c, s[a]), __fmul_rn(c1, o[a]));
+  }
+}
+
+// get_solid_phi: the subdomain's nodal phi at pos - bmin inside is_in.
+__device__ __forceinline__ float nested_phi(const GridView& phi, const Nest& n, const float p[3]) {
+  if (nest_inside(n, p, 2.0)) return sample_linear(n.phi, p[0] - n.bmin[0], p[1] - n.bmin[1], p[2] - n.bmin[2]);
+  return sample_linear(phi, p[0], p[1], p[2]);
+}
+
+// get_solid_normal: the subdomain's phi gradient (its own h) inside is_in,
+// normalised like the main grid's.
+__device__ __forceinline__ void nested_normal(const GridView& phi, const Nest& n, const float p[3], float o[3]) {
+  if (nest_inside(n, p, 2.0)) {
+    const float q[3] = {p[0] - n.bmin[0], p[1] - n.bmin[1], p[2] - n.bmin[2]};
+    solid_normal(n.phi, q, o);
+  } else {
+    solid_normal(phi, p, o);
+  }
+}
+
 // SmokeSolver3D::advect_FLIP, Smoke_solver3D.cpp:1407-1449: RK3 through the
-// grid velocity, then out of a solid along its normal by -phi.
+// grid velocity, then out of a solid along its normal by -phi.  NEST: the
+// velocity, phi and normal of the main grid with its subdomain active.
+template <bool NEST>
 __global__ void advect_flip_kernel(ParticleRec* __restrict__ p, int np, GridView u, GridView v, GridView w,
-                                   GridView phi, float dt) {
+                                   GridView phi, float dt, Nest nest) {
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
     const float pos0[3] = {p[q].pos[0], p[q].pos[1], p[q].pos[2]};
     float pos[3];
-    trace_rk3(u, v, w, pos0, dt, pos);
-    const float ph = sample_linear(phi, pos[0], pos[1], pos[2]);
+    if (NEST)
+      trace_rk3_f([&](const float* x, float* o) { nested_velocity(u, v, w, nest, x, o); }, pos0, dt, pos);
+    else
+      trace_rk3(u, v, w, pos0, dt, pos);
+    const float ph = NEST ? nested_phi(phi, nest, pos) : sample_linear(phi, pos[0], pos[1], pos[2]);
     if (ph < 0) {
       float n[3];
-      solid_normal(phi, pos, n);
+      if (NEST)
+        nested_normal(phi, nest, pos, n);
+      else
+        solid_normal(phi, pos, n);
 #pragma unroll
       for (int a = 0; a < 3; ++a) pos[a] = pos[a] - ph * n[a];
     }
@@ -591,14 +678,41 @@ __global__ void reorder_write_kernel(const ParticleRec* __restrict__ p, const in
   }
 }
 
-// keep flag: sampled solid phi >= 0 (reorder_FLIP's final filter)
+// keep flag: sampled solid phi >= 0 (reorder_FLIP's final filter); with
+// `nested` the main grid's get_solid_phi with its subdomain active.
 __global__ void solid_keep_kernel(const ParticleRec* __restrict__ tmp, const int* __restrict__ total,
-                                  int* __restrict__ keep, GridView phi, int cap, SubFrame sf) {
+                                  int* __restrict__ keep, GridView phi, int cap, SubFrame sf, int nested, Nest nest) {
   const int n = min(*total, cap);
-  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x)
-    keep[q] = sample_linear(phi, tmp[q].pos[0] - sf.bx, tmp[q].pos[1] - sf.by, tmp[q].pos[2] - sf.bz) >= 0.0f ? 1
-                                                                                                             : 0;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const float x[3] = {tmp[q].pos[0] - sf.bx, tmp[q].pos[1] - sf.by, tmp[q].pos[2] - sf.bz};
+    keep[q] = (nested ? nested_phi(phi, nest, x) : sample_linear(phi, x[0], x[1], x[2])) >= 0.0f ? 1 : 0;
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) keep[n] = 0;
+}
+
+// The halo selection of SmokeSolver3D::time_step (Smoke_solver3D.cpp:390-398):
+// flag the particles strictly inside [bmin - dx, bmax + dx] on every axis
+// (SubDomainSolver::is_halo, sub_domain.h:202-213; float).
+__global__ void halo_flag_kernel(const ParticleRec* __restrict__ p, int np, Nest nest, float dx,
+                                 int* __restrict__ flag) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q <= np; q += gridDim.x * blockDim.x) {
+    int f = 0;
+    if (q < np) {
+      f = 1;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const float x = p[q].pos[a];
+        f &= (x > nest.bmin[a] - dx && x < nest.bmax[a] + dx) ? 1 : 0;
+      }
+    }
+    flag[q] = f;
+  }
+}
+
+__global__ void halo_compact_kernel(const ParticleRec* __restrict__ p, int np, const int* __restrict__ flag,
+                                    const int* __restrict__ pos, ParticleRec* __restrict__ out, int cap) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x)
+    if (flag[q] && pos[q] < cap) out[pos[q]] = p[q];
 }
 
 __global__ void compact_kernel(const ParticleRec* __restrict__ tmp, const int* __restrict__ keep,

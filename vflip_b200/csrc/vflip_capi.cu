@@ -2280,28 +2280,105 @@ int vflip_p2g(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* parti
   return p2g_impl(ctx, ni, nj, nk, h, particles, np, u, ucoef, v, vcoef, w, wcoef, SubFrame{0.0f, 0.0f, 0.0f, 0});
 }
 
-int vflip_advect_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np, const float* u,
-                      const float* v, const float* w, const float* nodal_phi, float dt) {
+}  // extern "C"
+
+// The device view of a nested subdomain (SubDomainSolver::init, sub_domain.h:161-175:
+// bmax = bmin + (nx, ny, nz) h, in float); null `sub` gives an inactive view.
+static int make_nest(vflip_ctx* ctx, const vflip_subdomain* sub, Nest* out) {
+  *out = Nest{};
+  if (!sub) return VFLIP_OK;
+  int rc;
+  if ((rc = check_dims(ctx, sub->ni, sub->nj, sub->nk))) return rc;
+  if (!(sub->h > 0.0f) || !sub->u || !sub->v || !sub->w || !sub->nodal_phi)
+    return ctx->fail(VFLIP_ERR_ARG, "bad subdomain (spacing or null grid)");
+  const int n[3] = {sub->ni, sub->nj, sub->nk};
+  for (int a = 0; a < 3; ++a) {
+    out->bmin[a] = sub->bmin[a];
+    out->bmax[a] = sub->bmin[a] + (float)n[a] * sub->h;
+  }
+  out->h = sub->h;
+  const double hd = sub->h, ih = inv_pow2(sub->h);
+  const int ni = sub->ni, nj = sub->nj, nk = sub->nk;
+  out->u = GridView{sub->u, ni + 1, nj, nk, hd, 0.5, 0.0, 0.0, ih};
+  out->v = GridView{sub->v, ni, nj + 1, nk, hd, 0.0, 0.5, 0.0, ih};
+  out->w = GridView{sub->w, ni, nj, nk + 1, hd, 0.0, 0.0, 0.5, ih};
+  out->phi = GridView{sub->nodal_phi, ni + 1, nj + 1, nk + 1, hd, 0.5, 0.5, 0.5, ih};
+  return VFLIP_OK;
+}
+
+static int advect_flip_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np,
+                            const float* u, const float* v, const float* w, const float* nodal_phi, float dt,
+                            const vflip_subdomain* sub) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (np < 0 || (np > 0 && !particles) || !u || !v || !w || !nodal_phi) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  Nest nest;
+  if ((rc = make_nest(ctx, sub, &nest))) return rc;
   if (np == 0) return VFLIP_OK;
   const double hd = h, ih = inv_pow2(h);
   GridView gu{u, ni + 1, nj, nk, hd, 0.5, 0.0, 0.0, ih}, gv{v, ni, nj + 1, nk, hd, 0.0, 0.5, 0.0, ih},
       gw{w, ni, nj, nk + 1, hd, 0.0, 0.0, 0.5, ih}, gp{nodal_phi, ni + 1, nj + 1, nk + 1, hd, 0.5, 0.5, 0.5, ih};
-  advect_flip_kernel<<<grid_for(np, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>((ParticleRec*)particles, np, gu,
-                                                                                  gv, gw, gp, dt);
+  const int grid = grid_for(np, 128, ctx->num_sms * 8);
+  if (sub)
+    advect_flip_kernel<true><<<grid, 128, 0, ctx->stream>>>((ParticleRec*)particles, np, gu, gv, gw, gp, dt, nest);
+  else
+    advect_flip_kernel<false><<<grid, 128, 0, ctx->stream>>>((ParticleRec*)particles, np, gu, gv, gw, gp, dt, nest);
   VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+extern "C" {
+
+int vflip_advect_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np, const float* u,
+                      const float* v, const float* w, const float* nodal_phi, float dt) {
+  return advect_flip_impl(ctx, ni, nj, nk, h, particles, np, u, v, w, nodal_phi, dt, nullptr);
+}
+
+int vflip_advect_flip_nested(vflip_ctx* ctx, int ni, int nj, int nk, float h, void* particles, int np,
+                             const float* u, const float* v, const float* w, const float* nodal_phi, float dt,
+                             const vflip_subdomain* sub) {
+  if (ctx && !sub) return ctx->fail(VFLIP_ERR_ARG, "null subdomain");
+  return advect_flip_impl(ctx, ni, nj, nk, h, particles, np, u, v, w, nodal_phi, dt, sub);
+}
+
+int vflip_halo_select(vflip_ctx* ctx, const void* particles, int np, float h, const vflip_subdomain* sub, void* out,
+                      int capacity, int* n_out) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  if (np < 0 || (np > 0 && !particles) || !sub || !out || !n_out || capacity < 0 || !(h > 0.0f))
+    return ctx->fail(VFLIP_ERR_ARG, "bad argument");
+  Nest nest;
+  int rc;
+  if ((rc = make_nest(ctx, sub, &nest))) return rc;
+  int *flag, *pos;
+  VF_ALLOC(flag, int, "halo_flag", (size_t)np + 1);
+  VF_ALLOC(pos, int, "halo_pos", (size_t)np + 1);
+  const float dx = (float)(0.5 * (double)h);  // the reference passes 0.5 * _hx (double) to a float
+  halo_flag_kernel<<<grid_for((size_t)np + 1, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(
+      (const ParticleRec*)particles, np, nest, dx, flag);
+  VF_LAUNCH_CHECK();
+  if ((rc = exclusive_scan(ctx, flag, pos, (size_t)np + 1))) return rc;
+  if (np > 0) {
+    halo_compact_kernel<<<grid_for(np, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(
+        (const ParticleRec*)particles, np, flag, pos, (ParticleRec*)out, capacity);
+    VF_LAUNCH_CHECK();
+  }
+  int m = 0;
+  VF_CUDA(cudaMemcpyAsync(&m, pos + np, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  *n_out = m;
+  if (m > capacity) return ctx->fail(VFLIP_ERR_TOO_LARGE, "%d halo particles exceed the capacity %d", m, capacity);
   return VFLIP_OK;
 }
 
 static int reorder_flip_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
                        const float* u, const float* v, const float* w, const float* nodal_phi, unsigned seed,
-                       void* out, int capacity, int* np_out, SubFrame sf) {
+                       void* out, int capacity, int* np_out, SubFrame sf, const vflip_subdomain* sub = nullptr) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (np < 0 || (np > 0 && !particles) || !u || !v || !w || !nodal_phi || !out || !np_out || capacity < 0)
     return ctx->fail(VFLIP_ERR_ARG, "null pointer or negative capacity");
+  Nest nest;
+  if ((rc = make_nest(ctx, sub, &nest))) return rc;
   const size_t nc = (size_t)ni * nj * nk;
   if (9.0 * (double)nc > 2147483000.0) return ctx->fail(VFLIP_ERR_TOO_LARGE, "grid too large for reseeding");
   const int ntmp = (int)(9 * nc);  // at most 9 particles per cell before the solid filter
@@ -2341,7 +2418,8 @@ static int reorder_flip_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, co
   reorder_write_kernel<<<grid_for(nc, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(
       (const ParticleRec*)particles, start, order, base, tmp, ni, nj, nk, h, gu, gv, gw, (uint32_t)seed, sf);
   VF_LAUNCH_CHECK();
-  solid_keep_kernel<<<grid_for(ntmp, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(tmp, base + nc, keep, gp, ntmp, sf);
+  solid_keep_kernel<<<grid_for(ntmp, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(tmp, base + nc, keep, gp, ntmp, sf,
+                                                                                    sub ? 1 : 0, nest);
   VF_LAUNCH_CHECK();
   if ((rc = exclusive_scan(ctx, keep, kpos, (size_t)ntmp + 1))) return rc;
   compact_kernel<<<grid_for(ntmp, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(tmp, keep, kpos, base + nc,
@@ -2364,6 +2442,14 @@ int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const vo
                        void* out, int capacity, int* np_out) {
   return reorder_flip_impl(ctx, ni, nj, nk, h, particles, np, u, v, w, nodal_phi, seed, out, capacity, np_out,
                   SubFrame{0.0f, 0.0f, 0.0f, 0});
+}
+
+int vflip_reorder_flip_nested(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np,
+                              const float* u, const float* v, const float* w, const float* nodal_phi, unsigned seed,
+                              void* out, int capacity, int* np_out, const vflip_subdomain* sub) {
+  if (ctx && !sub) return ctx->fail(VFLIP_ERR_ARG, "null subdomain");
+  return reorder_flip_impl(ctx, ni, nj, nk, h, particles, np, u, v, w, nodal_phi, seed, out, capacity, np_out,
+                           SubFrame{0.0f, 0.0f, 0.0f, 0}, sub);
 }
 
 int vflip_sub_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, float bx, float by, float bz,
@@ -2491,17 +2577,76 @@ int vflip_emit_tracers(vflip_ctx* ctx, const float* tracers, int n, float h, flo
   return VFLIP_OK;
 }
 
-int vflip_advect_tracers(vflip_ctx* ctx, int ni, int nj, int nk, float h, float* tracers, int n, const float* u,
-                         const float* v, const float* w, const float* nodal_phi, float dt, float dens_decay) {
+}  // extern "C"
+
+static int advect_tracers_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, float* tracers, int n,
+                               const float* u, const float* v, const float* w, const float* nodal_phi, float dt,
+                               float dens_decay, const vflip_subdomain* sub) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (n < 0 || (n > 0 && !tracers) || !u || !v || !w || !nodal_phi) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  Nest nest;
+  if ((rc = make_nest(ctx, sub, &nest))) return rc;
   if (n == 0) return VFLIP_OK;
   const double hd = h, ih = inv_pow2(h);
   GridView gu{u, ni + 1, nj, nk, hd, 0.5, 0.0, 0.0, ih}, gv{v, ni, nj + 1, nk, hd, 0.0, 0.5, 0.0, ih},
       gw{w, ni, nj, nk + 1, hd, 0.0, 0.0, 0.5, ih}, gp{nodal_phi, ni + 1, nj + 1, nk + 1, hd, 0.5, 0.5, 0.5, ih};
-  advect_tracers_kernel<<<grid_for(n, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(
-      reinterpret_cast<float4*>(tracers), n, gu, gv, gw, gp, dt, dens_decay);
+  float4* tr = reinterpret_cast<float4*>(tracers);
+  const int grid = grid_for(n, 128, ctx->num_sms * 8);
+  if (sub)
+    advect_tracers_kernel<true><<<grid, 128, 0, ctx->stream>>>(tr, n, gu, gv, gw, gp, dt, dens_decay, nest);
+  else
+    advect_tracers_kernel<false><<<grid, 128, 0, ctx->stream>>>(tr, n, gu, gv, gw, gp, dt, dens_decay, nest);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+extern "C" {
+
+int vflip_advect_tracers(vflip_ctx* ctx, int ni, int nj, int nk, float h, float* tracers, int n, const float* u,
+                         const float* v, const float* w, const float* nodal_phi, float dt, float dens_decay) {
+  return advect_tracers_impl(ctx, ni, nj, nk, h, tracers, n, u, v, w, nodal_phi, dt, dens_decay, nullptr);
+}
+
+int vflip_advect_tracers_nested(vflip_ctx* ctx, int ni, int nj, int nk, float h, float* tracers, int n,
+                                const float* u, const float* v, const float* w, const float* nodal_phi, float dt,
+                                float dens_decay, const vflip_subdomain* sub) {
+  if (ctx && !sub) return ctx->fail(VFLIP_ERR_ARG, "null subdomain");
+  return advect_tracers_impl(ctx, ni, nj, nk, h, tracers, n, u, v, w, nodal_phi, dt, dens_decay, sub);
+}
+
+int vflip_emit_tracers_nested(vflip_ctx* ctx, const float* tracers, int n, float h, float lx, float ly, float lz,
+                              float cx, float cy, float cz, float r, int count, unsigned seed, int ni, int nj, int nk,
+                              const float* nodal_phi, const vflip_subdomain* sub, float* out, int capacity,
+                              int* n_out) {
+  if (!ctx) return VFLIP_ERR_ARG;
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (!sub || !nodal_phi) return ctx->fail(VFLIP_ERR_ARG, "null subdomain or phi");
+  Nest nest;
+  if ((rc = make_nest(ctx, sub, &nest))) return rc;
+  const size_t snc = (size_t)sub->ni * sub->nj * sub->nk;
+  if (4.0 * (double)snc > 2147483000.0) return ctx->fail(VFLIP_ERR_TOO_LARGE, "subdomain too large for seeding");
+  if ((rc = vflip_emit_tracers(ctx, tracers, n, h, lx, ly, lz, cx, cy, cz, r, count, seed, out, capacity, n_out)))
+    return rc;
+  const int m = *n_out, ncand = (int)(4 * snc);
+  int *flag, *pos;
+  VF_ALLOC(flag, int, "ts_flag", (size_t)ncand + 1);
+  VF_ALLOC(pos, int, "ts_pos", (size_t)ncand + 1);
+  const double hd = h, ih = inv_pow2(h);
+  GridView gp{nodal_phi, ni + 1, nj + 1, nk + 1, hd, 0.5, 0.5, 0.5, ih};
+  tracer_seed_flag_kernel<<<grid_for((size_t)ncand + 1, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(
+      gp, nest, sub->ni, sub->nj, (uint32_t)seed, ncand, flag);
+  VF_LAUNCH_CHECK();
+  if ((rc = exclusive_scan(ctx, flag, pos, (size_t)ncand + 1))) return rc;
+  int s = 0;
+  VF_CUDA(cudaMemcpyAsync(&s, pos + ncand, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  *n_out = m + s;
+  if ((long long)m + s > capacity)
+    return ctx->fail(VFLIP_ERR_TOO_LARGE, "%d tracers do not fit a capacity of %d", m + s, capacity);
+  tracer_seed_write_kernel<<<grid_for(ncand, 256, ctx->num_sms * 8), 256, 0, ctx->stream>>>(
+      gp, nest, sub->ni, sub->nj, (uint32_t)seed, ncand, flag, pos, m, reinterpret_cast<float4*>(out));
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
 }

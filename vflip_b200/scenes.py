@@ -137,6 +137,30 @@ def jittered_particles(ni, nj, nk, h, ppc, rng, centre=None, radius=None):
     return p
 
 
+def nested_scene(seed=0, dims=(20, 18, 16), h=1 / 32, lo=(5, 4, 4), cells=(10, 9, 8), ratio=2, scale=1.0):
+    """A main grid with a nested subdomain (SmokeSolver3D + SubDomainSolver):
+    main cells `dims` at spacing h with walls and a solid sphere; the
+    subdomain covers main cells lo .. lo + cells at spacing h / ratio (its
+    origin bmin = lo h), with its own random velocity and the same sphere in
+    its own nodal phi.  Returns dict(dims, h, u, v, w, phi, sub) where sub is
+    dict(dims, h, bmin, u, v, w, phi)."""
+    rng = np.random.default_rng(seed)
+    ni, nj, nk = dims
+    h = np.float32(h)
+    u, v, w = random_velocity(ni, nj, nk, rng, scale)
+    bmin = (np.asarray(lo, np.float64) * h).astype(np.float32)
+    sh = np.float32(h / ratio)
+    sdims = tuple(int(c) * ratio for c in cells)
+    # a sphere cutting the subdomain's box near one corner
+    centre = bmin + np.float32(0.35) * np.asarray(cells, np.float32) * h
+    radius = 0.22 * min(cells) * float(h)
+    phi = np.minimum(box_walls_phi(ni, nj, nk, h), sphere_phi(ni, nj, nk, h, centre, radius)).astype(np.float32)
+    su, sv, sw = random_velocity(*sdims, rng, scale)
+    sphi = sphere_phi(*sdims, sh, centre - bmin, radius)
+    sub = dict(dims=sdims, h=sh, bmin=bmin, u=su, v=sv, w=sw, phi=sphi)
+    return dict(dims=(ni, nj, nk), h=h, u=u, v=v, w=w, phi=phi, sub=sub, rng=rng)
+
+
 BATCH_SIDES = (32, 48, 64, 96, 128, 160, 192)
 
 

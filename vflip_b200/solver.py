@@ -16,7 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from ._lib import ConfigC, LearnedStatsC, SolveStatsC, SystemC, VflipError, load
+from ._lib import ConfigC, LearnedStatsC, SolveStatsC, SubdomainC, SystemC, VflipError, load
 from .particles import PARTICLE_BYTES
 
 
@@ -378,6 +378,67 @@ class Solver:
                                                     _p(particles), n, _p(u), _p(v), _p(w), _p(nodal_phi),
                                                     int(seed) & 0xFFFFFFFF, _p(out), cap, C.byref(cnt)))
         return out[:cnt.value * PARTICLE_BYTES]
+
+    # ------------------------------------------------------------- main grid with its subdomain active
+    @staticmethod
+    def subdomain(dims, h, bmin, u, v, w, nodal_phi):
+        """The nested subdomain the *_nested calls take: dims cells of spacing h
+        at bmin, its face velocities and nodal solid phi (device tensors, kept
+        referenced by the returned object)."""
+        ni, nj, nk = (int(x) for x in dims)
+        d = SubdomainC(ni, nj, nk, float(h), (C.c_float * 3)(*(float(b) for b in bmin)), _p(u), _p(v), _p(w),
+                       _p(nodal_phi))
+        d._tensors = (u, v, w, nodal_phi)
+        return d
+
+    def advect_flip_nested(self, ni, nj, nk, h, particles, u, v, w, nodal_phi, dt, sub):
+        """advect_FLIP through the main grid's samplers with its subdomain active."""
+        n = self._np(particles)
+        self._check(self.lib.vflip_advect_flip_nested(self.ctx, ni, nj, nk, float(h), _p(particles), n, _p(u), _p(v),
+                                                      _p(w), _p(nodal_phi), float(dt), C.byref(sub)))
+        return particles
+
+    def reorder_flip_nested(self, ni, nj, nk, h, particles, u, v, w, nodal_phi, sub, seed=0, capacity=None):
+        """reorder_FLIP of the main grid with the nested solid filter: a new particle tensor."""
+        n = self._np(particles)
+        cap = 9 * ni * nj * nk if capacity is None else int(capacity)
+        out = torch.empty(max(cap, 1) * PARTICLE_BYTES, dtype=torch.uint8, device=self.device)
+        cnt = C.c_int()
+        self._check(self.lib.vflip_reorder_flip_nested(self.ctx, ni, nj, nk, float(h), _p(particles), n, _p(u),
+                                                       _p(v), _p(w), _p(nodal_phi), int(seed) & 0xFFFFFFFF, _p(out),
+                                                       cap, C.byref(cnt), C.byref(sub)))
+        return out[:cnt.value * PARTICLE_BYTES]
+
+    def halo_select(self, particles, h, sub, capacity=None):
+        """The particles inside the subdomain's box widened by half a main cell
+        (h = main spacing): a new particle tensor."""
+        n = self._np(particles)
+        cap = n if capacity is None else int(capacity)
+        out = torch.empty(max(cap, 1) * PARTICLE_BYTES, dtype=torch.uint8, device=self.device)
+        cnt = C.c_int()
+        self._check(self.lib.vflip_halo_select(self.ctx, _p(particles) if n else None, n, float(h), C.byref(sub),
+                                               _p(out), cap, C.byref(cnt)))
+        return out[:cnt.value * PARTICLE_BYTES]
+
+    def advect_tracers_nested(self, ni, nj, nk, h, tracers, u, v, w, nodal_phi, dt, dens_decay, sub):
+        """advect_tracers with the subdomain active, in place on (n, 4) float32 tracers."""
+        self._check(self.lib.vflip_advect_tracers_nested(self.ctx, ni, nj, nk, float(h), _p(tracers),
+                                                         tracers.shape[0], _p(u), _p(v), _p(w), _p(nodal_phi),
+                                                         float(dt), float(dens_decay), C.byref(sub)))
+
+    def emit_tracers_nested(self, tracers, h, lengths, centre, radius, count, dims, nodal_phi, sub, seed=0,
+                            capacity=None):
+        """emit_tracers with the subdomain's seeding: a new (m, 4) float32 tensor."""
+        n = tracers.shape[0] if tracers is not None else 0
+        cap = n + int(count) + 4 * sub.ni * sub.nj * sub.nk if capacity is None else int(capacity)
+        out = self._empty((max(cap, 1), 4), torch.float32)
+        m = C.c_int()
+        self._check(self.lib.vflip_emit_tracers_nested(
+            self.ctx, _p(tracers) if n else None, n, float(h), float(lengths[0]), float(lengths[1]),
+            float(lengths[2]), float(centre[0]), float(centre[1]), float(centre[2]), float(radius), int(count),
+            int(seed) & 0xFFFFFFFF, int(dims[0]), int(dims[1]), int(dims[2]), _p(nodal_phi), C.byref(sub), _p(out),
+            cap, C.byref(m)))
+        return out[:m.value]
 
     # ------------------------------------------------------------- tracers
     def emit_tracers(self, tracers, h, lengths, centre, radius, count, seed=0, capacity=None):
