@@ -54,6 +54,13 @@ template <typename T, typename A> __device__ __forceinline__ T cvt(A v) { return
 // Gauss-Seidel division: IEEE in FP64 (reproduces the reference's
 // smoother bit for bit), the hardware fast division (2 ulp) in FP32, whose
 // smoother is not bit-exact with the FP64 reference in any case.
+// One term of a Gauss-Seidel row sum, sum + c x.  FP64 keeps the two
+// roundings of the reference's x86-64 build (its order of operations is the
+// parity bar); FP32 smoothers, which approximate the FP64 V-cycle to a
+// tolerance, take one fused multiply-add - every FP32 smoother uses this same
+// form, so they stay bit-identical to one another.
+__device__ __forceinline__ double gs_madd(double sum, double c, double x) { return sum + c * x; }
+__device__ __forceinline__ float gs_madd(float sum, float c, float x) { return __fmaf_rn(c, x, sum); }
 __device__ __forceinline__ double gs_div(double a, double b) { return a / b; }
 __device__ __forceinline__ float gs_div(float a, float b) { return __fdividef(a, b); }
 

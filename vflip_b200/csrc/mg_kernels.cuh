@@ -183,12 +183,12 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_kernel(SweepArgs<S, V> a) {
       size_t g = pbase + (size_t)j * sy + i;
       int s = (j - jr0) * width + i;  // staged index
       A sum = A(0);
-      if (p > 0) sum = sum + A(ldg(a.zp + g - sz)) * xm1[s];
-      if (j > 0) sum = sum + A(ldg(a.yp + g - sy)) * x0[s - width];
-      if (i > 0) sum = sum + A(ldg(a.xp + g - 1)) * x0[s - 1];
-      if (i < ni - 1) sum = sum + A(ldg(a.xp + g)) * x0[s + 1];
-      if (j < nj - 1) sum = sum + A(ldg(a.yp + g)) * x0[s + width];
-      if (p < nk - 1) sum = sum + A(ldg(a.zp + g)) * xp1[s];
+      if (p > 0) sum = gs_madd(sum, A(ldg(a.zp + g - sz)), xm1[s]);
+      if (j > 0) sum = gs_madd(sum, A(ldg(a.yp + g - sy)), x0[s - width]);
+      if (i > 0) sum = gs_madd(sum, A(ldg(a.xp + g - 1)), x0[s - 1]);
+      if (i < ni - 1) sum = gs_madd(sum, A(ldg(a.xp + g)), x0[s + 1]);
+      if (j < nj - 1) sum = gs_madd(sum, A(ldg(a.yp + g)), x0[s + width]);
+      if (p < nk - 1) sum = gs_madd(sum, A(ldg(a.zp + g)), xp1[s]);
       A d = A(ldg(a.diag + g));
       x0[s] = (d != A(0)) ? gs_div(ldg(a.b + g) - sum, d) : A(0);
     }
@@ -336,12 +336,12 @@ __device__ __forceinline__ float relax_quad_cell(bool zlo, bool zhi, bool ylo, b
                                                  const float4& czm) {
   constexpr int KL = K > 0 ? K - 1 : 0, KR = K < 3 ? K + 1 : 3;
   float sum = 0.0f;
-  if (zlo) sum = sum + c4<K>(czm) * c4<K>(xzm);
-  if (ylo) sum = sum + c4<K>(cym) * c4<K>(xym);
-  if (xlo) sum = sum + (K == 0 ? cxl : c4<KL>(cx)) * (K == 0 ? xl : c4<KL>(xc));
-  if (xhi) sum = sum + c4<K>(cx) * (K == 3 ? xr : c4<KR>(xc));
-  if (yhi) sum = sum + c4<K>(cyp) * c4<K>(xyp);
-  if (zhi) sum = sum + c4<K>(czp) * c4<K>(xzp);
+  if (zlo) sum = gs_madd(sum, c4<K>(czm), c4<K>(xzm));
+  if (ylo) sum = gs_madd(sum, c4<K>(cym), c4<K>(xym));
+  if (xlo) sum = gs_madd(sum, (K == 0 ? cxl : c4<KL>(cx)), (K == 0 ? xl : c4<KL>(xc)));
+  if (xhi) sum = gs_madd(sum, c4<K>(cx), (K == 3 ? xr : c4<KR>(xc)));
+  if (yhi) sum = gs_madd(sum, c4<K>(cyp), c4<K>(xyp));
+  if (zhi) sum = gs_madd(sum, c4<K>(czp), c4<K>(xzp));
   const float d = c4<K>(dd);
   return (d != 0.0f) ? gs_div(c4<K>(bb) - sum, d) : 0.0f;
 }
@@ -705,12 +705,12 @@ __global__ void __launch_bounds__(BLOCK) coarsest_rbgs_kernel(const V* __restric
           const int e = threadIdx.x + m * BLOCK;
           const int f = mask[m];
           A sum = A(0);
-          sum = sum + c[m][0] * xs[(f & 1) ? e - sz : e];
-          sum = sum + c[m][1] * xs[(f & 2) ? e - sy : e];
-          sum = sum + c[m][2] * xs[(f & 4) ? e - 1 : e];
-          sum = sum + c[m][3] * xs[(f & 8) ? e + 1 : e];
-          sum = sum + c[m][4] * xs[(f & 16) ? e + sy : e];
-          sum = sum + c[m][5] * xs[(f & 32) ? e + sz : e];
+          sum = gs_madd(sum, c[m][0], xs[(f & 1) ? e - sz : e]);
+          sum = gs_madd(sum, c[m][1], xs[(f & 2) ? e - sy : e]);
+          sum = gs_madd(sum, c[m][2], xs[(f & 4) ? e - 1 : e]);
+          sum = gs_madd(sum, c[m][3], xs[(f & 8) ? e + 1 : e]);
+          sum = gs_madd(sum, c[m][4], xs[(f & 16) ? e + sy : e]);
+          sum = gs_madd(sum, c[m][5], xs[(f & 32) ? e + sz : e]);
           xs[e] = (dd[m] != A(0)) ? gs_div(bb[m] - sum, dd[m]) : A(0);
         }
         __syncthreads();
@@ -726,12 +726,12 @@ __global__ void __launch_bounds__(BLOCK) coarsest_rbgs_kernel(const V* __restric
           const int e = threadIdx.x + m * BLOCK;
           const int f = mask[m];
           A sum = A(0);
-          if (f & 1) sum = sum + zps[e - sz] * xs[e - sz];
-          if (f & 2) sum = sum + yps[e - sy] * xs[e - sy];
-          if (f & 4) sum = sum + xps[e - 1] * xs[e - 1];
-          if (f & 8) sum = sum + xps[e] * xs[e + 1];
-          if (f & 16) sum = sum + yps[e] * xs[e + sy];
-          if (f & 32) sum = sum + zps[e] * xs[e + sz];
+          if (f & 1) sum = gs_madd(sum, zps[e - sz], xs[e - sz]);
+          if (f & 2) sum = gs_madd(sum, yps[e - sy], xs[e - sy]);
+          if (f & 4) sum = gs_madd(sum, xps[e - 1], xs[e - 1]);
+          if (f & 8) sum = gs_madd(sum, xps[e], xs[e + 1]);
+          if (f & 16) sum = gs_madd(sum, yps[e], xs[e + sy]);
+          if (f & 32) sum = gs_madd(sum, zps[e], xs[e + sz]);
           A d = ds[e];
           xs[e] = (d != A(0)) ? gs_div(bs[e] - sum, d) : A(0);
         }

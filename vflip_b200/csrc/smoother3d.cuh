@@ -152,12 +152,12 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_t3d_kernel(const __grid_cons
       const int fy = j - ys;
       const int s = fy * G::WX + (i - xs), c = fy * G::WC + (i - cxs);
       float sum = 0.0f;
-      if (zlo) sum = sum + float(ldv(czm + c)) * xm[s];
-      if (j > 0) sum = sum + float(ldv(cy + c - G::WC)) * x[s - G::WX];
-      if (i > 0) sum = sum + float(ldv(cx + c - 1)) * x[s - 1];
-      if (i < ni - 1) sum = sum + float(ldv(cx + c)) * x[s + 1];
-      if (j < nj - 1) sum = sum + float(ldv(cy + c)) * x[s + G::WX];
-      if (zhi) sum = sum + float(ldv(cz + c)) * xq[s];
+      if (zlo) sum = gs_madd(sum, float(ldv(czm + c)), xm[s]);
+      if (j > 0) sum = gs_madd(sum, float(ldv(cy + c - G::WC)), x[s - G::WX]);
+      if (i > 0) sum = gs_madd(sum, float(ldv(cx + c - 1)), x[s - 1]);
+      if (i < ni - 1) sum = gs_madd(sum, float(ldv(cx + c)), x[s + 1]);
+      if (j < nj - 1) sum = gs_madd(sum, float(ldv(cy + c)), x[s + G::WX]);
+      if (zhi) sum = gs_madd(sum, float(ldv(cz + c)), xq[s]);
       const float dv = float(ldv(dd + c));
       x[s] = (dv != 0.0f) ? gs_div(bb[s] - sum, dv) : 0.0f;
     }

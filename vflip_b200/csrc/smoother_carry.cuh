@@ -47,12 +47,12 @@ __device__ __forceinline__ float relax_quad_cell_m(const float4& xc, const float
                                                    const float4& czm) {
   constexpr int KL = K > 0 ? K - 1 : 0, KR = K < 3 ? K + 1 : 3;
   float sum = 0.0f;
-  sum = sum + c4<K>(czm) * c4<K>(xzm);
-  sum = sum + c4<K>(C.cym) * c4<K>(xym);
-  sum = sum + (K == 0 ? cxl : c4<KL>(C.cx)) * (K == 0 ? xl : c4<KL>(xc));
-  sum = sum + c4<K>(C.cx) * (K == 3 ? xr : c4<KR>(xc));
-  sum = sum + c4<K>(C.cyp) * c4<K>(xyp);
-  sum = sum + c4<K>(czp) * c4<K>(xzp);
+  sum = gs_madd(sum, c4<K>(czm), c4<K>(xzm));
+  sum = gs_madd(sum, c4<K>(C.cym), c4<K>(xym));
+  sum = gs_madd(sum, (K == 0 ? cxl : c4<KL>(C.cx)), (K == 0 ? xl : c4<KL>(xc)));
+  sum = gs_madd(sum, c4<K>(C.cx), (K == 3 ? xr : c4<KR>(xc)));
+  sum = gs_madd(sum, c4<K>(C.cyp), c4<K>(xyp));
+  sum = gs_madd(sum, c4<K>(czp), c4<K>(xzp));
   const float d = c4<K>(C.dd);
   return (d != 0.0f) ? gs_div(c4<K>(C.bb) - sum, d) : 0.0f;
 }
