@@ -157,6 +157,25 @@ def test_carry_smoother_matches_plain_kernel(gpu_solver, orc, dims, depth, prefe
         assert np.array_equal(a, ref), prec
 
 
+@pytest.mark.parametrize("dims", [(256, 40, 37), (256, 16, 70)])
+def test_fixed_layout_carry_smoother_matches_plain_kernel(gpu_solver, orc, dims):
+    """The instance compiled for 256-cell rows, 7-row tiles and one copy
+    group (the tuned 256^3 fine-level shape) gives the plain kernel's V-cycle
+    bit for bit, with its zero-x, prolongation and z.r variants in a solve."""
+    from vflip_b200.solver import Solver
+
+    _, out = system(orc, "gen", dims)
+    st, b = four(out["stencil"]), t(out["rhs"])
+    for prec, plain in ((1, "f32_plain"), (2, "mix_plain")):
+        with Solver(precision=prec, sweep_kernel=3, smoother_depth=1, smoother_tile_rows=7, **REF_HIERARCHY) as s:
+            a = s.vcycle(st, b).cpu().numpy()
+            conv, p, stats = s.amgpcg_solve(st, b, 1e-6, 50)
+        ref = gpu_solver[plain].vcycle(st, b).cpu().numpy()
+        assert np.array_equal(a, ref), prec
+        conv2, p2, stats2 = gpu_solver[plain].amgpcg_solve(st, b, 1e-6, 50)
+        assert conv and conv2 and stats.iterations == stats2.iterations
+
+
 def test_carry_smoother_pcg(gpu_solver, orc):
     """The fused z.r of the last post-sweep (DOT variant) through a full solve."""
     from vflip_b200.solver import Solver

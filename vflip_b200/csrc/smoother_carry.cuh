@@ -24,6 +24,11 @@
 // Shape: blockDim = (bx, by) with bx >= quads per row and by >= tile rows +
 // 2 (the host checks), so every (row, quad) of the red pass has exactly one
 // owner.  Every wait is bounded as in rbgs_sweep_tma_kernel.
+//
+// NI, TYO, DEPTH (0: read from the arguments) fix the row width, the tile
+// rows and the copy depth at compile time; the shared-memory layout's
+// offsets then fold into the load addresses (the host launches such an
+// instance only for arguments with those values).
 #pragma once
 #include "mg_kernels.cuh"
 
@@ -57,7 +62,7 @@ __device__ __forceinline__ float relax_quad_cell_m(const float4& xc, const float
   return (d != 0.0f) ? gs_div(c4<K>(C.bb) - sum, d) : 0.0f;
 }
 
-template <typename S, bool ZERO_X, bool PROLONG, bool DOT, int BLOCK>
+template <typename S, bool ZERO_X, bool PROLONG, bool DOT, int BLOCK, int NI = 0, int TYO = 0, int DEPTH = 0>
 __global__ void __launch_bounds__(BLOCK, 1) rbgs_sweep_carry_kernel(TmaSweepArgs<S> a) {
   extern __shared__ __align__(128) float sm[];
   constexpr int NB = kTmaMaxDepth + 2;
@@ -65,9 +70,9 @@ __global__ void __launch_bounds__(BLOCK, 1) rbgs_sweep_carry_kernel(TmaSweepArgs
   __shared__ double red_smem[BLOCK / 32];
   constexpr unsigned FULL = 0xffffffffu;
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-  const int ni = a.ni, nj = a.nj, nk = a.nk, tyo = a.tyo, D = a.depth;
+  const int ni = NI ? NI : a.ni, nj = a.nj, nk = a.nk, tyo = TYO ? TYO : a.tyo, D = DEPTH ? DEPTH : a.depth;
   const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
-  const TmaLayout Ly = tma_layout<S>(ni, tyo, D, a.crows_max, a.cni);
+  const TmaLayout Ly = tma_layout<S>(ni, tyo, D, PROLONG ? a.crows_max : 0, PROLONG ? a.cni : 0);
   const int xslot = Ly.xslot, cslot = Ly.cslot, yslot = Ly.yslot, cplane = Ly.cplane;
   const int RX = 4 + D, RC = 2 + D, RZ = 3 + D;
   const int oX = Ly.oX, oB = Ly.oB, oXC = Ly.oXC;

@@ -302,11 +302,15 @@ bool tma_shape(const vflip_config& cfg, const Dims& d, const Dims* cd, bool prol
 template <typename S, bool Z, bool P, bool D>
 int launch_tma_t(vflip_ctx* ctx, const TmaSweepArgs<S>& a, const TmaShape& sh) {
   const bool wide = sh.threads == kTmaBlockWide;
-  const int which = sh.carry ? 2 : (wide ? 1 : 0);
-  auto kern = sh.carry ? rbgs_sweep_carry_kernel<S, Z, P, D, kTmaBlockWide>
-                       : (wide ? rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlockWide>
-                               : rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlock>);
-  static bool attr_set[3] = {false, false, false};
+  // the tuned shape of a 256-cell-row fine level (7-row tiles, one copy group
+  // in flight) runs an instance with that layout compiled in
+  const bool fixed = sh.carry && a.ni == 256 && a.tyo == 7 && a.depth == 1;
+  const int which = fixed ? 3 : (sh.carry ? 2 : (wide ? 1 : 0));
+  auto kern = fixed ? rbgs_sweep_carry_kernel<S, Z, P, D, kTmaBlockWide, 256, 7, 1>
+                    : sh.carry ? rbgs_sweep_carry_kernel<S, Z, P, D, kTmaBlockWide>
+                               : (wide ? rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlockWide>
+                                       : rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlock>);
+  static bool attr_set[4] = {false, false, false, false};
   if (!attr_set[which]) {
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemMax);
     attr_set[which] = true;
