@@ -361,28 +361,40 @@ __device__ __forceinline__ float tent(float r) {  // SmokeSolver3D::H, Smoke_sol
   return res;
 }
 
-// particle_to_grid for one velocity component, Smoke_solver3D.cpp:1451-1510:
-// field = sum(w v)/sum(w), coef = sum(w), with sum(w) starting at 1e-5 and
-// the weight H(dx/h)H(dy/h)H(dz/h).  A particle whose offset from the node
-// exceeds 1.0001 h on some axis has weight exactly 0 and (finite velocity)
-// contributes exactly nothing, so it is skipped without changing any sum.
+// particle_to_grid, Smoke_solver3D.cpp:1451-1510, for the three velocity
+// components in one pass: at each face node, field = sum(w v)/sum(w),
+// coef = sum(w), sum(w) starting at 1e-5, weight H(dx/h)H(dy/h)H(dz/h).  One
+// thread takes index (i, j, k) of all three face grids (u: (ni+1) x nj x nk,
+// v: ni x (nj+1) x nk, w: ni x nj x (nk+1); a component whose output is null
+// or whose grid does not hold (i, j, k) is skipped): the three nodes gather
+// from the same buckets in the same order, so each particle is loaded once
+// and every component's sums are those of its own pass, bit for bit.  A
+// particle whose offset from a node exceeds 1.0001 h on some axis has weight
+// exactly 0 and (finite velocity) contributes exactly nothing to that node,
+// so it is skipped there without changing any sum.
 // SUB: SubDomainSolver::particle_to_grid (sub_domain.cpp:1204-1265) with
 // determineDist (sub_domain.h:89-103): within 4 cells of the grid's boundary
 // the tent is 4h wide over the 9^3 neighbouring buckets.
 template <bool SUB>
-__global__ void p2g_kernel(const int* __restrict__ start, const float4* __restrict__ spos,
-                           const float4* __restrict__ svel, float* __restrict__ field, float* __restrict__ coef,
-                           int comp, int ni, int nj, int nk, float h, float inv_h) {
-  const int fx = ni + (comp == 0), fy = nj + (comp == 1), fz = nk + (comp == 2);
-  const double ox = comp == 0 ? 0.5 : 0.0, oy = comp == 1 ? 0.5 : 0.0, oz = comp == 2 ? 0.5 : 0.0;
-  const size_t n = (size_t)fx * fy * fz;
+__global__ void p2g3_kernel(const int* __restrict__ start, const float4* __restrict__ spos,
+                            const float4* __restrict__ svel, float* __restrict__ fu, float* __restrict__ cu,
+                            float* __restrict__ fv, float* __restrict__ cv, float* __restrict__ fw,
+                            float* __restrict__ cw, int ni, int nj, int nk, float h, float inv_h) {
+  const size_t n = (size_t)(ni + 1) * (nj + 1) * (nk + 1);
   const float reach = h * 1.0001f;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     int i, j, k;
-    decode3(e, fx, fy, i, j, k);
-    float gx = (float)(((double)(float)i - ox) * (double)h);
-    float gy = (float)(((double)(float)j - oy) * (double)h);
-    float gz = (float)(((double)(float)k - oz) * (double)h);
+    decode3(e, ni + 1, nj + 1, i, j, k);
+    const bool act0 = fu != nullptr && j < nj && k < nk;
+    const bool act1 = fv != nullptr && i < ni && k < nk;
+    const bool act2 = fw != nullptr && i < ni && j < nj;
+    if (!(act0 || act1 || act2)) continue;
+    // node positions: the component's own axis sits half a cell lower
+    const float xi = (float)((double)(float)i * (double)h), xh = (float)(((double)(float)i - 0.5) * (double)h);
+    const float yj = (float)((double)(float)j * (double)h), yh = (float)(((double)(float)j - 0.5) * (double)h);
+    const float zk = (float)((double)(float)k * (double)h), zh = (float)(((double)(float)k - 0.5) * (double)h);
+    const float gx[3] = {xh, xi, xi}, gy[3] = {yj, yh, yj}, gz[3] = {zk, zk, zh};
+    const bool act[3] = {act0, act1, act2};
     int l = 1;
     float hk = h, ihk = inv_h, rk = reach;
     if (SUB) {
@@ -394,33 +406,55 @@ __global__ void p2g_kernel(const int* __restrict__ start, const float4* __restri
         rk = hk * 1.0001f;
       }
     }
-    float tw = 1e-5f, tv = 0.0f;
+    float tw[3] = {1e-5f, 1e-5f, 1e-5f}, tv[3] = {0.0f, 0.0f, 0.0f};
     for (int dk = -l; dk <= l; ++dk) {
-      int ck = k + dk;
+      const int ck = k + dk;
       if (ck < 0 || ck >= nk) continue;
       for (int dj = -l; dj <= l; ++dj) {
-        int cj = j + dj;
+        const int cj = j + dj;
         if (cj < 0 || cj >= nj) continue;
         for (int di = -l; di <= l; ++di) {
-          int ci = i + di;
+          const int ci = i + di;
           if (ci < 0 || ci >= ni) continue;
-          int c = (ck * nj + cj) * ni + ci;
-          int b = __ldg(start + c), en = __ldg(start + c + 1);
+          const int c = (ck * nj + cj) * ni + ci;
+          const int b = __ldg(start + c), en = __ldg(start + c + 1);
           for (int q = b; q < en; ++q) {
-            float4 pp = __ldg(spos + q);
-            float dx = pp.x - gx, dy = pp.y - gy, dz = pp.z - gz;
-            if (pp.w != 0.0f && (fabsf(dx) >= rk || fabsf(dy) >= rk || fabsf(dz) >= rk)) continue;
-            float wgt = tent(fdiv_h(dx, hk, ihk)) * tent(fdiv_h(dy, hk, ihk)) * tent(fdiv_h(dz, hk, ihk));
-            float4 vv = __ldg(svel + q);
-            float vc = comp == 0 ? vv.x : (comp == 1 ? vv.y : vv.z);
-            tw = tw + wgt;
-            tv = tv + wgt * vc;
+            const float4 pp = __ldg(spos + q);
+            float4 vv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            bool have_v = false;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              if (!act[a]) continue;
+              const float dx = pp.x - gx[a], dy = pp.y - gy[a], dz = pp.z - gz[a];
+              if (pp.w != 0.0f && (fabsf(dx) >= rk || fabsf(dy) >= rk || fabsf(dz) >= rk)) continue;
+              const float wgt = tent(fdiv_h(dx, hk, ihk)) * tent(fdiv_h(dy, hk, ihk)) * tent(fdiv_h(dz, hk, ihk));
+              if (!have_v) {
+                vv = __ldg(svel + q);
+                have_v = true;
+              }
+              const float vc = a == 0 ? vv.x : (a == 1 ? vv.y : vv.z);
+              tw[a] = tw[a] + wgt;
+              tv[a] = tv[a] + wgt * vc;
+            }
           }
         }
       }
     }
-    coef[e] = tw;
-    field[e] = tv / tw;
+    if (act0) {
+      const size_t o = (size_t)i + (size_t)(ni + 1) * ((size_t)j + (size_t)nj * k);
+      cu[o] = tw[0];
+      fu[o] = tv[0] / tw[0];
+    }
+    if (act1) {
+      const size_t o = (size_t)i + (size_t)ni * ((size_t)j + (size_t)(nj + 1) * k);
+      cv[o] = tw[1];
+      fv[o] = tv[1] / tw[1];
+    }
+    if (act2) {
+      const size_t o = (size_t)i + (size_t)ni * ((size_t)j + (size_t)nj * k);
+      cw[o] = tw[2];
+      fw[o] = tv[2] / tw[2];
+    }
   }
 }
 

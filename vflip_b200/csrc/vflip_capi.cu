@@ -2264,18 +2264,16 @@ static int p2g_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void*
         (const ParticleRec*)particles, order, spos, svel, start + nc, sf);
     VF_LAUNCH_CHECK();
   }
-  float* outs[3][2] = {{u, ucoef}, {v, vcoef}, {w, wcoef}};
-  for (int c = 0; c < 3; ++c) {
-    if (!outs[c][0]) continue;
-    size_t nf = (size_t)(ni + (c == 0)) * (nj + (c == 1)) * (nk + (c == 2));
-    if (sf.sub)
-      p2g_kernel<true><<<grid_for(nf, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(
-          start, spos, svel, outs[c][0], outs[c][1], c, ni, nj, nk, h, (float)inv_pow2(h));
-    else
-      p2g_kernel<false><<<grid_for(nf, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(
-          start, spos, svel, outs[c][0], outs[c][1], c, ni, nj, nk, h, (float)inv_pow2(h));
-    VF_LAUNCH_CHECK();
-  }
+  if (!u && !v && !w) return VFLIP_OK;
+  const size_t nn = (size_t)(ni + 1) * (nj + 1) * (nk + 1);
+  const int grid = grid_for(nn, 128, ctx->num_sms * 8);
+  if (sf.sub)
+    p2g3_kernel<true><<<grid, 128, 0, ctx->stream>>>(start, spos, svel, u, ucoef, v, vcoef, w, wcoef, ni, nj, nk, h,
+                                                    (float)inv_pow2(h));
+  else
+    p2g3_kernel<false><<<grid, 128, 0, ctx->stream>>>(start, spos, svel, u, ucoef, v, vcoef, w, wcoef, ni, nj, nk, h,
+                                                     (float)inv_pow2(h));
+  VF_LAUNCH_CHECK();
   return VFLIP_OK;
 }
 
