@@ -363,7 +363,6 @@ __global__ void __launch_bounds__(BLOCK) rbgs_sweep_tma_kernel(TmaSweepArgs<S> a
   const S* cs = reinterpret_cast<const S*>(sm + Ly.oC);
   const unsigned cbase_b = 4u * (unsigned)Ly.oC;  // byte offset of the coefficient region
   constexpr unsigned ES = sizeof(S);
-  const int P = (ni + 1) / 2;
   const int tx = threadIdx.x, ty = threadIdx.y, bx = blockDim.x, by = blockDim.y;
 
   const int j0 = blockIdx.x * tyo;
