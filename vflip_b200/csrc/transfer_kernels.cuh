@@ -367,8 +367,9 @@ __device__ __forceinline__ float tent(float r) {  // SmokeSolver3D::H, Smoke_sol
 // thread takes index (i, j, k) of all three face grids (u: (ni+1) x nj x nk,
 // v: ni x (nj+1) x nk, w: ni x nj x (nk+1); a component whose output is null
 // or whose grid does not hold (i, j, k) is skipped): the three nodes gather
-// from the same buckets in the same order, so each particle is loaded once
-// and every component's sums are those of its own pass, bit for bit.  A
+// from the same buckets in the same order and share their offsets pairwise,
+// so each particle is loaded once, six one-dimensional tents give the three
+// weights, and every component's sums are those of its own pass, bit for bit.  A
 // particle whose offset from a node exceeds 1.0001 h on some axis has weight
 // exactly 0 and (finite velocity) contributes exactly nothing to that node,
 // so it is skipped there without changing any sum.
@@ -393,8 +394,6 @@ __global__ void p2g3_kernel(const int* __restrict__ start, const float4* __restr
     const float xi = (float)((double)(float)i * (double)h), xh = (float)(((double)(float)i - 0.5) * (double)h);
     const float yj = (float)((double)(float)j * (double)h), yh = (float)(((double)(float)j - 0.5) * (double)h);
     const float zk = (float)((double)(float)k * (double)h), zh = (float)(((double)(float)k - 0.5) * (double)h);
-    const float gx[3] = {xh, xi, xi}, gy[3] = {yj, yh, yj}, gz[3] = {zk, zk, zh};
-    const bool act[3] = {act0, act1, act2};
     int l = 1;
     float hk = h, ihk = inv_h, rk = reach;
     if (SUB) {
@@ -420,21 +419,36 @@ __global__ void p2g3_kernel(const int* __restrict__ start, const float4* __restr
           const int b = __ldg(start + c), en = __ldg(start + c + 1);
           for (int q = b; q < en; ++q) {
             const float4 pp = __ldg(spos + q);
-            float4 vv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            bool have_v = false;
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-              if (!act[a]) continue;
-              const float dx = pp.x - gx[a], dy = pp.y - gy[a], dz = pp.z - gz[a];
-              if (pp.w != 0.0f && (fabsf(dx) >= rk || fabsf(dy) >= rk || fabsf(dz) >= rk)) continue;
-              const float wgt = tent(fdiv_h(dx, hk, ihk)) * tent(fdiv_h(dy, hk, ihk)) * tent(fdiv_h(dz, hk, ihk));
-              if (!have_v) {
-                vv = __ldg(svel + q);
-                have_v = true;
-              }
-              const float vc = a == 0 ? vv.x : (a == 1 ? vv.y : vv.z);
-              tw[a] = tw[a] + wgt;
-              tv[a] = tv[a] + wgt * vc;
+            // the nodes share offsets pairwise: x of v and w, y of u and w,
+            // z of u and v - six one-dimensional tents serve the three weights
+            const float dxu = pp.x - xh, dxv = pp.x - xi;
+            const float dyu = pp.y - yj, dyv = pp.y - yh;
+            const float dzu = pp.z - zk, dzw = pp.z - zh;
+            const bool fin = pp.w != 0.0f;
+            const bool ox = fabsf(dxu) >= rk, oxv = fabsf(dxv) >= rk, oy = fabsf(dyu) >= rk, oyv = fabsf(dyv) >= rk;
+            const bool oz = fabsf(dzu) >= rk, ozw = fabsf(dzw) >= rk;
+            const bool ok0 = act0 && !(fin && (ox || oy || oz));
+            const bool ok1 = act1 && !(fin && (oxv || oyv || oz));
+            const bool ok2 = act2 && !(fin && (oxv || oy || ozw));
+            if (!(ok0 || ok1 || ok2)) continue;
+            const float txu = tent(fdiv_h(dxu, hk, ihk)), txv = tent(fdiv_h(dxv, hk, ihk));
+            const float tyu = tent(fdiv_h(dyu, hk, ihk)), tyv = tent(fdiv_h(dyv, hk, ihk));
+            const float tzu = tent(fdiv_h(dzu, hk, ihk)), tzw = tent(fdiv_h(dzw, hk, ihk));
+            const float4 vv = __ldg(svel + q);
+            if (ok0) {
+              const float wgt = txu * tyu * tzu;
+              tw[0] = tw[0] + wgt;
+              tv[0] = tv[0] + wgt * vv.x;
+            }
+            if (ok1) {
+              const float wgt = txv * tyv * tzu;
+              tw[1] = tw[1] + wgt;
+              tv[1] = tv[1] + wgt * vv.y;
+            }
+            if (ok2) {
+              const float wgt = txv * tyu * tzw;
+              tw[2] = tw[2] + wgt;
+              tv[2] = tv[2] + wgt * vv.z;
             }
           }
         }
