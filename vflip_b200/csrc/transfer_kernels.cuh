@@ -412,44 +412,42 @@ __global__ void p2g3_kernel(const int* __restrict__ start, const float4* __restr
       for (int dj = -l; dj <= l; ++dj) {
         const int cj = j + dj;
         if (cj < 0 || cj >= nj) continue;
-        for (int di = -l; di <= l; ++di) {
-          const int ci = i + di;
-          if (ci < 0 || ci >= ni) continue;
-          const int c = (ck * nj + cj) * ni + ci;
-          const int b = __ldg(start + c), en = __ldg(start + c + 1);
-          for (int q = b; q < en; ++q) {
-            const float4 pp = __ldg(spos + q);
-            // the nodes share offsets pairwise: x of v and w, y of u and w,
-            // z of u and v - six one-dimensional tents serve the three weights
-            const float dxu = pp.x - xh, dxv = pp.x - xi;
-            const float dyu = pp.y - yj, dyv = pp.y - yh;
-            const float dzu = pp.z - zk, dzw = pp.z - zh;
-            const bool fin = pp.w != 0.0f;
-            const bool ox = fabsf(dxu) >= rk, oxv = fabsf(dxv) >= rk, oy = fabsf(dyu) >= rk, oyv = fabsf(dyv) >= rk;
-            const bool oz = fabsf(dzu) >= rk, ozw = fabsf(dzw) >= rk;
-            const bool ok0 = act0 && !(fin && (ox || oy || oz));
-            const bool ok1 = act1 && !(fin && (oxv || oyv || oz));
-            const bool ok2 = act2 && !(fin && (oxv || oy || ozw));
-            if (!(ok0 || ok1 || ok2)) continue;
-            const float txu = tent(fdiv_h(dxu, hk, ihk)), txv = tent(fdiv_h(dxv, hk, ihk));
-            const float tyu = tent(fdiv_h(dyu, hk, ihk)), tyv = tent(fdiv_h(dyv, hk, ihk));
-            const float tzu = tent(fdiv_h(dzu, hk, ihk)), tzw = tent(fdiv_h(dzw, hk, ihk));
-            const float4 vv = __ldg(svel + q);
-            if (ok0) {
-              const float wgt = txu * tyu * tzu;
-              tw[0] = tw[0] + wgt;
-              tv[0] = tv[0] + wgt * vv.x;
-            }
-            if (ok1) {
-              const float wgt = txv * tyv * tzu;
-              tw[1] = tw[1] + wgt;
-              tv[1] = tv[1] + wgt * vv.y;
-            }
-            if (ok2) {
-              const float wgt = txv * tyu * tzw;
-              tw[2] = tw[2] + wgt;
-              tv[2] = tv[2] + wgt * vv.z;
-            }
+        // the buckets i-l .. i+l of this row are consecutive in the sorted
+        // order: one run of particles, visited in bucket order as before
+        const int row = (ck * nj + cj) * ni;
+        const int b = __ldg(start + row + max(i - l, 0)), en = __ldg(start + row + min(i + l, ni - 1) + 1);
+        for (int q = b; q < en; ++q) {
+          const float4 pp = __ldg(spos + q);
+          // the nodes share offsets pairwise: x of v and w, y of u and w,
+          // z of u and v - six one-dimensional tents serve the three weights
+          const float dxu = pp.x - xh, dxv = pp.x - xi;
+          const float dyu = pp.y - yj, dyv = pp.y - yh;
+          const float dzu = pp.z - zk, dzw = pp.z - zh;
+          const bool fin = pp.w != 0.0f;
+          const bool ox = fabsf(dxu) >= rk, oxv = fabsf(dxv) >= rk, oy = fabsf(dyu) >= rk, oyv = fabsf(dyv) >= rk;
+          const bool oz = fabsf(dzu) >= rk, ozw = fabsf(dzw) >= rk;
+          const bool ok0 = act0 && !(fin && (ox || oy || oz));
+          const bool ok1 = act1 && !(fin && (oxv || oyv || oz));
+          const bool ok2 = act2 && !(fin && (oxv || oy || ozw));
+          if (!(ok0 || ok1 || ok2)) continue;
+          const float txu = tent(fdiv_h(dxu, hk, ihk)), txv = tent(fdiv_h(dxv, hk, ihk));
+          const float tyu = tent(fdiv_h(dyu, hk, ihk)), tyv = tent(fdiv_h(dyv, hk, ihk));
+          const float tzu = tent(fdiv_h(dzu, hk, ihk)), tzw = tent(fdiv_h(dzw, hk, ihk));
+          const float4 vv = __ldg(svel + q);
+          if (ok0) {
+            const float wgt = txu * tyu * tzu;
+            tw[0] = tw[0] + wgt;
+            tv[0] = tv[0] + wgt * vv.x;
+          }
+          if (ok1) {
+            const float wgt = txv * tyv * tzu;
+            tw[1] = tw[1] + wgt;
+            tv[1] = tv[1] + wgt * vv.y;
+          }
+          if (ok2) {
+            const float wgt = txv * tyu * tzw;
+            tw[2] = tw[2] + wgt;
+            tv[2] = tv[2] + wgt * vv.z;
           }
         }
       }
