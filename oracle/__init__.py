@@ -1,7 +1,7 @@
 """ctypes bindings for the oracle libraries.  TEST INFRASTRUCTURE ONLY.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
-this package, and only as the checker.  The product package (vflip_b200)
+this package, and only to compare against.  The product package (vflip_b200)
 never imports it.
 
 Two libraries share one calling convention (linear layout, i fastest):

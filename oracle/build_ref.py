@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Build the reference solver's own CPU code into oracle/_ref/libvflip_ref.so.
 
-Test infrastructure only: the library this makes is the checker that pins the
+Test infrastructure only: the library this makes is the comparison that pins the
 oracle restatement (oracle/vflip_oracle.cpp) and the timed "reference" CPU arm
 of bench.py.  It is never linked into the product.
 

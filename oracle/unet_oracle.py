@@ -1,5 +1,5 @@
 """CPU FP64 restatement of the learned preconditioner's 3D U-Net - test
-infrastructure only (the checker for the tensor-core kernels; never called by
+infrastructure only (the comparison for the tensor-core kernels; never called by
 the product path).
 
 The network has no counterpart in the reference (which solves with plain

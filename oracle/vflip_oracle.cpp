@@ -2,7 +2,7 @@
 //
 // TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
 // cpu_baseline leg of bench.py may load this library (oracle/liboracle.so),
-// and only as the checker.  The product (vflip_b200/, libvflip_gpu.so) never
+// and only to compare against.  The product (vflip_b200/, libvflip_gpu.so) never
 // links, loads or falls back to it.
 //
 // Each function restates the reference algorithm in this project's own code

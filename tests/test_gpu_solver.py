@@ -3,7 +3,7 @@
 Bar: the FP64 path reproduces the oracle (and so the reference) bit for bit
 for the hierarchy, the smoother and the V-cycle; the PCG differs only by
 the order of the tree reductions of its inner products (rel. L2 <= 1e-11,
-same iteration count).  FP32 and mixed precision meet the north-star
+same iteration count).  FP32 and mixed precision meet the reduced-precision
 tolerance: pressure within 1e-5 relative L2 of the reference solve.
 """
 import numpy as np
@@ -245,7 +245,7 @@ def test_pcg_reduced_precision(gpu_solver, orc, prec, tag, dims):
     conv, p, stats = gpu_solver[prec].amgpcg_solve(four(st), t(b), 1e-6, 50)
     assert conv and ok
     assert stats.residual <= 1e-6 * stats.rhs_norm
-    # pressure within the north-star tolerance of the reference solve
+    # pressure within 1e-5 relative L2 of the reference solve
     assert rel_l2(p.cpu().numpy(), x) < 1e-5
     assert stats.iterations <= it + 2
 

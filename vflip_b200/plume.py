@@ -1,7 +1,6 @@
 """Grid smoke-plume stepper built from the library's kernels.
 
-One step (the unit of the benchmark) is what SURVEY-scale configs call a
-smoke step:
+One step (the unit of the benchmark) is one smoke step:
   1. RK2 semi-Lagrangian trilinear advection of u, v, w, density and
      temperature through the current velocity
      (SubDomainSolver::advect_field, sub_domain.cpp:191-235);
