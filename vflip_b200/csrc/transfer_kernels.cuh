@@ -376,16 +376,56 @@ __device__ __forceinline__ float tent(float r) {  // SmokeSolver3D::H, Smoke_sol
 // SUB: SubDomainSolver::particle_to_grid (sub_domain.cpp:1204-1265) with
 // determineDist (sub_domain.h:89-103): within 4 cells of the grid's boundary
 // the tent is 4h wide over the 9^3 neighbouring buckets.
+//
+// `part` picks the nodes a launch takes: P2G_ALL every index; for a
+// subdomain P2G_SHELL the indices within 4 of the boundary on some axis
+// (the 9^3 gathers) and P2G_INNER the box between, so that no warp mixes the
+// two costs.  The shell is enumerated as the end planes (k), then the end
+// rows (j) of the inner planes, then the end nodes (i) of the inner rows;
+// per axis the inner range is [5, n - 5] (m = max(0, n - 9) indices) and an
+// end index t in [0, n + 1 - m) is t below 5, else t + m.
+enum { P2G_ALL = 0, P2G_INNER = 1, P2G_SHELL = 2 };
+
+__host__ __device__ inline size_t p2g_part_size(int part, int ni, int nj, int nk) {
+  const size_t X = (size_t)ni + 1, Y = (size_t)nj + 1, Z = (size_t)nk + 1;
+  const size_t mi = ni > 9 ? ni - 9 : 0, mj = nj > 9 ? nj - 9 : 0, mk = nk > 9 ? nk - 9 : 0;
+  if (part == P2G_ALL) return X * Y * Z;
+  if (part == P2G_INNER) return mi * mj * mk;
+  return (Z - mk) * X * Y + mk * (Y - mj) * X + mk * mj * (X - mi);
+}
+
 template <bool SUB>
 __global__ void p2g3_kernel(const int* __restrict__ start, const float4* __restrict__ spos,
                             const float4* __restrict__ svel, float* __restrict__ fu, float* __restrict__ cu,
                             float* __restrict__ fv, float* __restrict__ cv, float* __restrict__ fw,
-                            float* __restrict__ cw, int ni, int nj, int nk, float h, float inv_h) {
-  const size_t n = (size_t)(ni + 1) * (nj + 1) * (nk + 1);
+                            float* __restrict__ cw, int ni, int nj, int nk, float h, float inv_h, int part) {
+  const size_t n = p2g_part_size(part, ni, nj, nk);
+  const int X = ni + 1, Y = nj + 1, Z = nk + 1;
+  const int mi = max(ni - 9, 0), mj = max(nj - 9, 0), mk = max(nk - 9, 0);
+  const size_t p1 = (size_t)(Z - mk) * X * Y, p2 = (size_t)mk * (Y - mj) * X;
   const float reach = h * 1.0001f;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     int i, j, k;
-    decode3(e, ni + 1, nj + 1, i, j, k);
+    if (part == P2G_ALL) {
+      decode3(e, X, Y, i, j, k);
+    } else if (part == P2G_INNER) {
+      decode3(e, mi, mj, i, j, k);
+      i += 5;
+      j += 5;
+      k += 5;
+    } else if (e < p1) {  // end planes
+      decode3(e, X, Y, i, j, k);
+      k = k < 5 ? k : k + mk;
+    } else if (e < p1 + p2) {  // end rows of the inner planes
+      decode3(e - p1, X, Y - mj, i, j, k);
+      j = j < 5 ? j : j + mj;
+      k += 5;
+    } else {  // end nodes of the inner rows
+      decode3(e - p1 - p2, X - mi, mj, i, j, k);
+      i = i < 5 ? i : i + mi;
+      j += 5;
+      k += 5;
+    }
     const bool act0 = fu != nullptr && j < nj && k < nk;
     const bool act1 = fv != nullptr && i < ni && k < nk;
     const bool act2 = fw != nullptr && i < ni && j < nj;

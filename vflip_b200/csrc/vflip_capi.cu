@@ -2265,15 +2265,23 @@ static int p2g_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void*
     VF_LAUNCH_CHECK();
   }
   if (!u && !v && !w) return VFLIP_OK;
-  const size_t nn = (size_t)(ni + 1) * (nj + 1) * (nk + 1);
-  const int grid = grid_for(nn, 128, ctx->num_sms * 8);
-  if (sf.sub)
-    p2g3_kernel<true><<<grid, 128, 0, ctx->stream>>>(start, spos, svel, u, ucoef, v, vcoef, w, wcoef, ni, nj, nk, h,
-                                                    (float)inv_pow2(h));
-  else
-    p2g3_kernel<false><<<grid, 128, 0, ctx->stream>>>(start, spos, svel, u, ucoef, v, vcoef, w, wcoef, ni, nj, nk, h,
-                                                     (float)inv_pow2(h));
-  VF_LAUNCH_CHECK();
+  const float ih = (float)inv_pow2(h);
+  if (sf.sub) {
+    // the 9^3 gathers of the boundary shell and the 3^3 ones of the inner box
+    // in separate launches, so that no warp mixes the two
+    for (int part : {P2G_SHELL, P2G_INNER}) {
+      const size_t nn = p2g_part_size(part, ni, nj, nk);
+      if (nn == 0) continue;
+      p2g3_kernel<true><<<grid_for(nn, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(
+          start, spos, svel, u, ucoef, v, vcoef, w, wcoef, ni, nj, nk, h, ih, part);
+      VF_LAUNCH_CHECK();
+    }
+  } else {
+    const size_t nn = p2g_part_size(P2G_ALL, ni, nj, nk);
+    p2g3_kernel<false><<<grid_for(nn, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(
+        start, spos, svel, u, ucoef, v, vcoef, w, wcoef, ni, nj, nk, h, ih, P2G_ALL);
+    VF_LAUNCH_CHECK();
+  }
   return VFLIP_OK;
 }
 
