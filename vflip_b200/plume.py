@@ -73,13 +73,16 @@ class PlumeSim:
     def state(self):
         return {k: self.f[k] for k in self.FIELDS}
 
-    def advect_and_force(self):
-        """Steps 1-2 of a plume step (advection, sources, buoyancy)."""
+    def advect_and_force(self, before_scalars=None):
+        """Steps 1-2 of a plume step (advection, sources, buoyancy);
+        `before_scalars` runs between the velocity and the scalar advection."""
         p, s, n, h = self.p, self.s, self.p.n, self.p.h
         u, v, w = self.f["u"], self.f["v"], self.f["w"]
         offs = {"u": (0.5, 0, 0), "v": (0, 0.5, 0), "w": (0, 0, 0.5)}
         for k in ("u", "v", "w"):
             s.advect_rk2_linear(n, n, n, h, p.dt, u, v, w, self.f[k], offs[k], out=self.g[k])
+        if before_scalars is not None:
+            before_scalars()
         # density and temperature share the cell-centred backtrace
         s.advect_rk2_linear2(n, n, n, h, p.dt, u, v, w, self.f["rho"], self.f["temp"], (0, 0, 0), out=self.g["rho"],
                              out2=self.g["temp"])
@@ -106,10 +109,13 @@ class PlumeSim:
                                       pressure=self.pressure, tolerance_factor=p.tol,
                                       max_iterations=p.max_iterations, sample=sample)
 
-    def step(self, precond=None):
+    def step(self, precond=None, before_scalars=None, after_force=None):
         """One plume step; `precond` (a learned.LearnedPreconditioner) takes
-        over the projection when given."""
-        self.advect_and_force()
+        over the projection when given.  `before_scalars` / `after_force` run
+        before the scalar advection / before the projection."""
+        self.advect_and_force(before_scalars)
+        if after_force is not None:
+            after_force()
         if precond is None:
             conv, _, stats = self.project()
         else:
@@ -129,13 +135,35 @@ class PlumeSim:
         return div[2:-2, 2:-2, 2:-2]
 
     def step_host(self, host, precond=None):
-        """One step on host-resident state (pinned tensors): H2D copy, step,
-        D2H copy back into the same host tensors."""
-        for k in self.FIELDS:
+        """One step on host-resident state (pinned tensors): every field is
+        copied in at the start of the step and back into the same host
+        tensors at its end.  Density and temperature travel on a second
+        stream: their upload follows the velocity's and overlaps the velocity
+        advection, their download leaves once the sources are applied and
+        overlaps the projection.  The step ends when both streams have."""
+        main = torch.cuda.current_stream(self.s.device)
+        if getattr(self, "_copy_stream", None) is None:
+            self._copy_stream = torch.cuda.Stream(self.s.device)
+        cs = self._copy_stream
+        for k in ("u", "v", "w"):
             self.f[k].copy_(host[k], non_blocking=True)
-        out = self.step(precond)
-        for k in self.FIELDS:
+        cs.wait_stream(main)  # after the velocity upload and all earlier work
+        with torch.cuda.stream(cs):
+            for k in ("rho", "temp"):
+                self.f[k].copy_(host[k], non_blocking=True)
+        uploaded = torch.cuda.Event()
+        uploaded.record(cs)
+
+        def download_scalars():
+            cs.wait_stream(main)
+            with torch.cuda.stream(cs):
+                for k in ("rho", "temp"):
+                    host[k].copy_(self.f[k], non_blocking=True)
+
+        out = self.step(precond, before_scalars=lambda: main.wait_event(uploaded), after_force=download_scalars)
+        for k in ("u", "v", "w"):
             host[k].copy_(self.f[k], non_blocking=True)
+        main.wait_stream(cs)
         return out
 
     def host_bytes(self):
