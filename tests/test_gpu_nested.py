@@ -179,3 +179,24 @@ def test_nested_sim_invariants_mixed():
             assert np.isfinite(sp["vel"]).all() and np.isfinite(sim.particles_host()["vel"]).all()
         assert sim.tracers.shape[0] > 300
         assert float(sim.sub_vel[1].abs().max()) > 0.0
+
+
+def test_nested_empty_inputs(gpu_solver):
+    """No particles and no tracers: every nested call returns cleanly and
+    emission seeds only the subdomain's cells."""
+    s = gpu_solver[1]
+    sc = scenes.nested_scene(seed=2)
+    ni, nj, nk = sc["dims"]
+    h = sc["h"]
+    u, v, w, phi = t(sc["u"]), t(sc["v"]), t(sc["w"]), t(sc["phi"])
+    ds = device_sub(s, sc["sub"])
+    empty = torch.zeros(0, dtype=torch.uint8, device=DEV)
+    assert s.halo_select(empty, h, ds).numel() == 0
+    s.advect_flip_nested(ni, nj, nk, h, empty, u, v, w, phi, 0.01, ds)
+    r = s.reorder_flip_nested(ni, nj, nk, h, empty, u, v, w, phi, ds, seed=1)
+    assert r.numel() > 0 and r.numel() % 40 == 0  # every open cell seeded with 8
+    lengths = np.array([ni, nj, nk], np.float32) * h
+    e = s.emit_tracers_nested(None, h, lengths, (0.3, 0.2, 0.3), 0.05, 0, (ni, nj, nk), phi, ds, seed=4)
+    assert e.shape[1] == 4 and (e[:, 3] == 1).all()
+    tr = torch.zeros((0, 4), dtype=torch.float32, device=DEV)
+    s.advect_tracers_nested(ni, nj, nk, h, tr, u, v, w, phi, 0.01, 0.1, ds)
