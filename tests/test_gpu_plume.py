@@ -53,8 +53,8 @@ def test_projection_removes_divergence(gpu_solver, prec):
 
 def test_step_host_matches_device_steps(gpu_solver):
     """Steps on host-resident state (the end-to-end path: fields copied in and
-    out every step, density and temperature on a second stream) give the
-    device-resident steps' fields bit for bit."""
+    out every step on three copy streams) give the device-resident steps'
+    fields bit for bit."""
     p = PlumeParams(n=48, dt=0.02, obstacle=True)
     a = PlumeSim(gpu_solver[1], p)
     b = PlumeSim(gpu_solver[1], p)
@@ -62,6 +62,7 @@ def test_step_host_matches_device_steps(gpu_solver):
     for _ in range(4):
         a.step()
         b.step_host(host)
+    b.host_join()
     torch.cuda.synchronize()
     for k in a.FIELDS:
         assert np.array_equal(a.f[k].cpu().numpy(), host[k].numpy()), k

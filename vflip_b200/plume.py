@@ -136,23 +136,40 @@ class PlumeSim:
 
     def step_host(self, host, precond=None):
         """One step on host-resident state (pinned tensors): every field is
-        copied in at the start of the step and back into the same host
-        tensors at its end.  Density and temperature travel on a second
-        stream: their upload follows the velocity's and overlaps the velocity
-        advection, their download leaves once the sources are applied and
-        overlaps the projection.  The step ends when both streams have."""
-        main = torch.cuda.current_stream(self.s.device)
-        if getattr(self, "_copy_stream", None) is None:
-            self._copy_stream = torch.cuda.Stream(self.s.device)
-        cs = self._copy_stream
-        for k in ("u", "v", "w"):
-            self.f[k].copy_(host[k], non_blocking=True)
-        cs.wait_stream(main)  # after the velocity upload and all earlier work
+        copied in at the start of the step and its result copied back into
+        the same host tensors.  The copies overlap the compute where the data
+        allows:
+          * u, v, w download in order on one stream and each field's next
+            upload waits only for its own download, so the upload of one
+            field runs beside the download of the next (the host link is full
+            duplex);
+          * density and temperature travel on a third stream: their upload
+            follows the velocity's and overlaps the velocity advection, their
+            download leaves once the sources are applied and overlaps the
+            projection.
+        The step returns with its velocity downloads in flight: call
+        host_join() before reading the host state or stopping a clock."""
+        dev = self.s.device
+        main = torch.cuda.current_stream(dev)
+        if getattr(self, "_up", None) is None:
+            self._up, self._down, self._cs = (torch.cuda.Stream(dev) for _ in range(3))
+            self._downloaded = {}
+        up, down, cs = self._up, self._down, self._cs
+        up.wait_stream(main)  # the device buffers are free of earlier work
+        with torch.cuda.stream(up):
+            for k in ("u", "v", "w"):
+                if k in self._downloaded:
+                    up.wait_event(self._downloaded[k])
+                self.f[k].copy_(host[k], non_blocking=True)
+        vel_in = torch.cuda.Event()
+        vel_in.record(up)
+        main.wait_event(vel_in)
+        cs.wait_event(vel_in)
         with torch.cuda.stream(cs):
             for k in ("rho", "temp"):
                 self.f[k].copy_(host[k], non_blocking=True)
-        uploaded = torch.cuda.Event()
-        uploaded.record(cs)
+        scal_in = torch.cuda.Event()
+        scal_in.record(cs)
 
         def download_scalars():
             cs.wait_stream(main)
@@ -160,11 +177,22 @@ class PlumeSim:
                 for k in ("rho", "temp"):
                     host[k].copy_(self.f[k], non_blocking=True)
 
-        out = self.step(precond, before_scalars=lambda: main.wait_event(uploaded), after_force=download_scalars)
-        for k in ("u", "v", "w"):
-            host[k].copy_(self.f[k], non_blocking=True)
-        main.wait_stream(cs)
+        out = self.step(precond, before_scalars=lambda: main.wait_event(scal_in), after_force=download_scalars)
+        down.wait_stream(main)
+        with torch.cuda.stream(down):
+            for k in ("u", "v", "w"):
+                host[k].copy_(self.f[k], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(down)
+                self._downloaded[k] = ev
         return out
+
+    def host_join(self):
+        """Make the current stream wait for step_host's copies in flight."""
+        main = torch.cuda.current_stream(self.s.device)
+        for st in (getattr(self, "_down", None), getattr(self, "_cs", None), getattr(self, "_up", None)):
+            if st is not None:
+                main.wait_stream(st)
 
     def host_bytes(self):
         return sum(int(np.prod(self.shapes[k])) * 4 for k in self.FIELDS)
