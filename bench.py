@@ -135,33 +135,60 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+class Ranks:
+    """One process per GPU: rank, world size and the two collectives the
+    timing needs (a barrier, the max over ranks).  NCCL reduces a CUDA
+    tensor, gloo (CPU tests) a CPU one; world size 1 needs no process group."""
+
+    def __init__(self, backend="nccl", timeout_s=300):
+        import datetime
+
+        import torch.distributed as dist
+
+        self.dist = dist
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
+        if self.world > 1:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max_over_ranks(self, x):
+        if self.world == 1:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device="cuda" if self.backend == "nccl" else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+def replica_throughput(world, steps, ms_max):
+    """Whole-job steps/s of `world` replicas that each ran `steps` steps, the
+    slowest in `ms_max` milliseconds."""
+    return world * steps / (ms_max * 1e-3)
+
+
 def run_vflip(a):
     import numpy as np
     import torch
-    import torch.distributed as dist
 
     from vflip_b200.plume import PlumeParams, PlumeSim
     from vflip_b200.solver import Solver
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks("nccl")
+    world, rank = ranks.world, ranks.rank
+    barrier, max_over_ranks = ranks.barrier, ranks.max_over_ranks
 
     solver = Solver(precision=PREC[a.precision], device=local)
     params = PlumeParams(n=a.n, dt=a.dt)
@@ -222,7 +249,7 @@ def run_vflip(a):
         achieved = alg_bytes / (avg_sweep_ms * 1e-3) / 1e9 if n_sweeps else None
         traffic = profile_traffic(a.n)
         out = {
-            "metric": METRIC, "value": world * a.steps / (ms_max * 1e-3), "unit": "steps/s", "n_gpus": world,
+            "metric": METRIC, "value": replica_throughput(world, a.steps, ms_max), "unit": "steps/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "fp32" if a.precision != "fp64" else "fp64",
             "data": "synthetic (seeded plume scene, state evolved by the warm-up steps)",
@@ -235,7 +262,7 @@ def run_vflip(a):
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": avg_sweep_ms,
                          "launches_timed": n_sweeps, "peak_kind": peak_kind},
-            "e2e": {"value": world * a.steps / (e2e_ms * 1e-3), "unit": "steps/s",
+            "e2e": {"value": replica_throughput(world, a.steps, e2e_ms), "unit": "steps/s",
                     "h2d_bytes_per_step": sim.host_bytes(), "d2h_bytes_per_step": sim.host_bytes()},
             "gpu_launches": launches,
             "clocks": clk,
@@ -252,8 +279,7 @@ def run_vflip(a):
         if not a.no_nested and world == 1:
             out["nested"] = nested_arm(a.steps, device=local)
     solver.close()
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
     return out
 
 
