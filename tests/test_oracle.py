@@ -489,3 +489,36 @@ def test_nested_vs_reference(orc, ref, seed):
     b = ref.reorder_flip_nested(ni, nj, nk, h, sparse, u, v, w, phi, sub, seed=1)
     same(a[a["temp"] > 0].view(np.uint8), b[b["temp"] > 0].view(np.uint8))
     assert abs(len(a) - len(b)) <= 0.02 * len(b)
+
+
+def test_nested_thresholds_vs_reference(orc, ref):
+    """Points exactly on, and one float step either side of, the subdomain's
+    thresholds: bmin/bmax +- 0.5 h_main (is_halo, float), bmin + 2 h_s / bmax - 2 h_s
+    (is_in, double) and bmin + 5 h_s / bmax - 5 h_s (is_in2, double, and the
+    boundary coefficient's 4 h_s ramp).  The oracle's halo selection, solid phi
+    and blended advection equal the reference's bit for bit there."""
+    sc = scenes.nested_scene(seed=9, dims=(16, 14, 12), lo=(4, 3, 3), cells=(8, 7, 6))
+    ni, nj, nk = sc["dims"]
+    h, u, v, w, phi, sub = sc["h"], sc["u"], sc["v"], sc["w"], sc["phi"], sc["sub"]
+    sh = np.float32(sub["h"])
+    bmin = sub["bmin"].astype(np.float32)
+    bmax = (bmin + np.array(sub["dims"], np.float32) * sh).astype(np.float32)
+    centre = ((bmin + bmax) / 2).astype(np.float32)
+    cuts = []
+    for lo, hi in ((bmin - np.float32(0.5 * h), bmax + np.float32(0.5 * h)), (bmin + 2 * sh, bmax - 2 * sh),
+                   (bmin + 5 * sh, bmax - 5 * sh), (bmin + 9 * sh, bmax - 9 * sh)):
+        for edge in (lo.astype(np.float32), hi.astype(np.float32)):
+            for a in range(3):
+                for d in (-1, 0, 1):
+                    p = centre.copy()
+                    p[a] = np.nextafter(edge[a], np.float32(np.inf if d > 0 else -np.inf)) if d else edge[a]
+                    cuts.append(p)
+    x = np.array(cuts, np.float32)
+    same(orc.solid_phi_nested(ni, nj, nk, h, phi, sub, x).view(np.uint32),
+         ref.solid_phi_nested(ni, nj, nk, h, phi, sub, x).view(np.uint32))
+    p = np.zeros(len(x), PARTICLE_DTYPE)
+    p["pos"] = x
+    p["temp"] = np.arange(len(x), dtype=np.float32)
+    same(orc.halo_select(p, h, sub).view(np.uint8), ref.halo_select(p, h, sub).view(np.uint8))
+    same(orc.advect_flip_nested(ni, nj, nk, h, p, u, v, w, phi, 1e-4, sub).view(np.uint8),
+         ref.advect_flip_nested(ni, nj, nk, h, p, u, v, w, phi, 1e-4, sub).view(np.uint8))
