@@ -59,6 +59,25 @@ def test_bad_arguments_fail_without_a_device(lib):
     assert lib.vflip_create(C.byref(ctx), C.byref(cfg)) < 0
 
 
+def test_nested_and_subdomain_calls_reject_a_null_context(lib):
+    """The nested-subdomain and subdomain entry points fail with an argument
+    error before touching the device when the context is missing."""
+    from vflip_b200._lib import SubdomainC
+
+    sub = SubdomainC(8, 8, 8, 0.125, (C.c_float * 3)(0.0, 0.0, 0.0), None, None, None, None)
+    n = C.c_int(0)
+    assert lib.vflip_halo_select(None, None, 0, 0.1, C.byref(sub), None, 0, C.byref(n)) < 0
+    assert lib.vflip_advect_flip_nested(None, 8, 8, 8, 0.1, None, 0, None, None, None, None, 0.01, C.byref(sub)) < 0
+    assert lib.vflip_reorder_flip_nested(None, 8, 8, 8, 0.1, None, 0, None, None, None, None, 0, None, 0,
+                                         C.byref(n), C.byref(sub)) < 0
+    assert lib.vflip_advect_tracers_nested(None, 8, 8, 8, 0.1, None, 0, None, None, None, None, 0.01, 0.0,
+                                           C.byref(sub)) < 0
+    assert lib.vflip_emit_tracers_nested(None, None, 0, 0.1, 1.0, 1.0, 1.0, 0.5, 0.5, 0.5, 0.1, 0, 0, 8, 8, 8, None,
+                                         C.byref(sub), None, 0, C.byref(n)) < 0
+    assert lib.vflip_sub_particle_cells(None, 8, 8, 8, 0.1, 0.0, 0.0, 0.0, None, 0, None) < 0
+    assert lib.vflip_sub_g2p(None, 8, 8, 8, 0.1, 0.0, 0.0, 0.0, None, 0, None, None, None) < 0
+
+
 def test_no_cpu_fallback_without_library(monkeypatch, tmp_path):
     import vflip_b200._lib as L
 
