@@ -172,6 +172,11 @@ __global__ void __launch_bounds__(BLOCK, 1) rbgs_sweep_carry_kernel(TmaSweepArgs
   };
 
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  // ZERO_X without a prolongation: the old x is zero everywhere, so the red
+  // pass takes zeros instead of loading them; the red store writes whole
+  // quads, so every x the black pass reads from shared memory is written
+  // first and the x ring needs no zero fill
+  constexpr bool XZ = ZERO_X && !PROLONG;
   // carried state of the thread's quad (see the header comment)
   float4 X2 = z4, X1 = z4, X0 = z4;  // x of p-2, p-1 (red-updated), p
   CarryCoef P{z4, z4, z4, z4, z4};   // coefficients of p-1
@@ -199,7 +204,7 @@ __global__ void __launch_bounds__(BLOCK, 1) rbgs_sweep_carry_kernel(TmaSweepArgs
     const int sxm1 = wrap(px - 1, RX), sxp1 = wrap(px + 1, RX);
     const int scm1 = wrap(pc - 1, RC);
     const int szm1 = wrap(pz - 1, RZ);
-    if (PROLONG || ZERO_X) {
+    if (PROLONG) {
       if (p == p0) {
         if (PROLONG) { prolong_add(p - 1, sxm1); prolong_add(p, px); }
         if (ZERO_X) { zero_x(sxm1); zero_x(px); }
@@ -212,8 +217,8 @@ __global__ void __launch_bounds__(BLOCK, 1) rbgs_sweep_carry_kernel(TmaSweepArgs
     if (p == p0 && act_red) {
       // entering the march: the planes before p0 come from shared memory
       // (old values; only their black cells are read by red(p0))
-      if (p >= 1) X1 = ld4f(sm + xm + xo);
-      if (p >= 0 && p < nk) X0 = ld4f(sm + x0 + xo);
+      if (!XZ && p >= 1) X1 = ld4f(sm + xm + xo);
+      if (!XZ && p >= 0 && p < nk) X0 = ld4f(sm + x0 + xo);
       if (p >= 1) pczp = ld4f(cs + oZP + szm1 * cslot + co);
     }
 
@@ -223,10 +228,10 @@ __global__ void __launch_bounds__(BLOCK, 1) rbgs_sweep_carry_kernel(TmaSweepArgs
     // is outside the domain (p = -1), so X0 holds x(p) on every entry
     float4 xn = z4, xym = z4, xyp = z4, czp = z4;
     CarryCoef C{z4, z4, z4, z4, z4};
-    if (act_red && p + 1 >= 0 && p + 1 < nk) xn = ld4f(sm + oX + sxp1 * xslot + xo);
+    if (!XZ && act_red && p + 1 >= 0 && p + 1 < nk) xn = ld4f(sm + oX + sxp1 * xslot + xo);
     if (do_red && act_red) {
-      if (ylo) xym = ld4f(sm + x0 + xo - ni);
-      if (yhi) xyp = ld4f(sm + x0 + xo + ni);
+      if (!XZ && ylo) xym = ld4f(sm + x0 + xo - ni);
+      if (!XZ && yhi) xyp = ld4f(sm + x0 + xo + ni);
       C.bb = ld4f(sm + oB + pc * cslot + co);
       C.dd = ld4f(cs + oD + pc * cslot + co);
       C.cx = ld4f(cs + oXP + pc * cslot + co);
@@ -239,10 +244,10 @@ __global__ void __launch_bounds__(BLOCK, 1) rbgs_sweep_carry_kernel(TmaSweepArgs
       float xr = __shfl_down_sync(FULL, X0.x, 1);
       if (do_red && act_red) {
         if (warp_l && xlo) {
-          xl = sm[x0 + xo - 1];
+          xl = XZ ? 0.0f : sm[x0 + xo - 1];
           cxl = float(ldv(cs + oXP + pc * cslot + co - 1));
         }
-        if (warp_r && need_r) xr = sm[x0 + xo + 4];
+        if (warp_r && need_r) xr = XZ ? 0.0f : sm[x0 + xo + 4];
         xl = xlo ? xl : 0.0f;
         xr = need_r ? xr : 0.0f;
         if (((j + p + 1) & 1) == 0) {
