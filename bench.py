@@ -245,7 +245,10 @@ def run_vflip(a):
     if rank == 0:
         peak, peak_kind = measured_peaks()
         avg_sweep_ms = sweep_ms / max(n_sweeps, 1)
-        alg_bytes = 7 * 4 * cells  # x_in, b, diag, xp, yp, zp read + x_out written, FP32
+        # the fine-level launches of one V(4,4) cycle: a zero-x sweep (no x read, 6 x 4 B per cell),
+        # five plain sweeps and the fused z.r sweep (x_in, b, diag, xp, yp, zp read + x_out written,
+        # 7 x 4 B) and the fused-prolongation sweep (+ the coarse x, 4 B per 8 cells), all FP32
+        alg_bytes = (24 + 5 * 28 + 28 + 28.5) / 8 * cells
         achieved = alg_bytes / (avg_sweep_ms * 1e-3) / 1e9 if n_sweeps else None
         traffic = profile_traffic(a.n)
         out = {
