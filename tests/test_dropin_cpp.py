@@ -45,3 +45,11 @@ def test_dropin_solves_like_the_reference(tmp_path, orc):
     x, ok, res, it = orc.amgpcg(st, rhs.reshape(n, n, n))
     assert bool(tail[0]) == ok and int(tail[1]) == it
     assert np.linalg.norm(p - x.ravel()) <= 1e-11 * np.linalg.norm(x)
+
+
+def test_nested_step_sequence_compiles_as_c():
+    """The coupled time_step sequence (C ABI only, tests/cpp/nested_step.c)
+    compiles as C99 against include/vflip.h with warnings as errors."""
+    src = os.path.join(ROOT, "tests", "cpp", "nested_step.c")
+    subprocess.check_call(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-I",
+                           os.path.join(ROOT, "include"), src])
