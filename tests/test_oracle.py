@@ -522,3 +522,20 @@ def test_nested_thresholds_vs_reference(orc, ref):
     same(orc.halo_select(p, h, sub).view(np.uint8), ref.halo_select(p, h, sub).view(np.uint8))
     same(orc.advect_flip_nested(ni, nj, nk, h, p, u, v, w, phi, 1e-4, sub).view(np.uint8),
          ref.advect_flip_nested(ni, nj, nk, h, p, u, v, w, phi, 1e-4, sub).view(np.uint8))
+
+
+@pytest.mark.parametrize("dims,seed", [((13, 11, 9), 21), ((20, 7, 16), 22)])
+def test_face_weights_and_delta_vs_reference(orc, ref, dims, seed):
+    """compute_face_weights (fraction_inside of the four nodal phi of every
+    face, the three face grids) and getDelta on fresh seeded inputs: the oracle
+    equals the reference bit for bit; the particle record is 40 bytes in both."""
+    ni, nj, nk = dims
+    rng = np.random.default_rng(seed)
+    h = np.float32(1.0 / max(dims))
+    phi = scenes.random_phi(ni, nj, nk, h, rng, n_spheres=4)
+    for a, b in zip(orc.face_weights(ni, nj, nk, h, phi), ref.face_weights(ni, nj, nk, h, phi)):
+        same(a.view(np.uint32), b.view(np.uint32))
+    after = rng.standard_normal((nk, nj, ni + 1)).astype(np.float32)
+    before = rng.standard_normal((nk, nj, ni + 1)).astype(np.float32)
+    same(orc.delta(after, before).view(np.uint32), ref.delta(after, before).view(np.uint32))
+    assert orc.fn("particle_size")() == ref.fn("particle_size")() == 40
