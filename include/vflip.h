@@ -63,8 +63,9 @@ typedef struct {
   int coarse_sweeps;         /* RBGS sweeps on the coarsest level; 0 (default) = automatic: 200 in FP64
                                 (SS/AlgebraicMultigrid.h:160), 100 in FP32/MIXED */
   int coarsest_max_unknowns; /* coarsen while unknowns exceed this (max 4096); 0 (default) = automatic:
-                                4096 in FP64 (SS/GeometricLevelGen.h:46, the reference's hierarchy), 512 in
-                                FP32/MIXED (an 8^3 coarsest level those sweeps solve to convergence) */
+                                4096 in FP64 (SS/GeometricLevelGen.h:46, the reference's hierarchy); in
+                                FP32/MIXED 64 (a 4^3 coarsest level) with the direct coarsest solve, 512
+                                (8^3) with the sweeps */
   int device;                /* CUDA device ordinal, default 0 */
   void* stream;              /* cudaStream_t to order work on; NULL: the CUDA default stream */
   int sweep_kernel;          /* smoother kernel: 0 (default) = automatic: for FP32 levels whose row length
@@ -95,6 +96,13 @@ typedef struct {
    * fluid region).  1 = always the sweeps; 2 = the direct solve where it
    * applies, in every precision. */
   int coarsest_solver;
+  /* PCG direction/SpMV kernel: 0 (default) = automatic: for fine levels
+   * whose rows are whole warps of quads (ni a multiple of 128, at most 1024)
+   * a plane-marching kernel (each s = z + beta s formed once, neighbours from
+   * registers and a shared-memory plane ring), else the column kernel;
+   * 1 = always the column kernel.  Both give the same q and s bit for bit;
+   * their s.q partial sums are grouped differently. */
+  int spmv_kernel;
 } vflip_config;
 
 typedef struct {

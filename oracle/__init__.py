@@ -7,7 +7,9 @@ never imports it.
 Two libraries share one calling convention (linear layout, i fastest):
   * ``liboracle.so``        - this project's CPU restatement (vflip_oracle.cpp);
   * ``_ref/libvflip_ref.so`` - the reference's own code (build_ref.py), present
-    only where the reference tree was available at build time.
+    only where the reference tree was available at build time;
+  * ``_ref/libvflip_ref_dropin.so`` - the same code with the GPU drop-in
+    (include/vflip/amgpcg_dropin.hpp) as its ivock::AMGPCGSolve.
 
 Seven-point operators are numpy arrays of shape (7, nk, nj, ni), float64, in
 the slot order diag, -x, +x, -y, +y, -z, +z.
@@ -21,6 +23,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libvflip_ref.so")
+REF_DROPIN_SO = os.path.join(HERE, "_ref", "libvflip_ref_dropin.so")
 
 PARTICLE_DTYPE = np.dtype([("pos", "<f4", (3,)), ("vel", "<f4", (3,)), ("dens", "<f4"), ("temp", "<f4"),
                            ("hash_idx", "<i4"), ("sub_hash_idx", "<i4")])
@@ -78,8 +81,9 @@ def _load(path, prefix):
         getattr(lib, p + "_amgpcg").argtypes = [_I, _I, _I, _P, _P, _P, _D, _I, _P, _P]
     else:
         getattr(lib, p + "_levels").argtypes = [_I, _I, _I, _P, _P, _P, _I, _P, _P]
-        getattr(lib, p + "_rbgs").argtypes = [_I, _I, _I, _P, _P, _P, _P, _P, _I]
-        getattr(lib, p + "_vcycle").argtypes = [_I, _I, _I, _P, _P, _P, _P, _P]
+        if hasattr(lib, p + "_rbgs"):  # absent from the drop-in build (the GPU solve replaces them)
+            getattr(lib, p + "_rbgs").argtypes = [_I, _I, _I, _P, _P, _P, _P, _P, _I]
+            getattr(lib, p + "_vcycle").argtypes = [_I, _I, _I, _P, _P, _P, _P, _P]
         getattr(lib, p + "_amgpcg").argtypes = [_I, _I, _I, _P, _P, _P, _P, _P, _D, _I, _P, _P]
         getattr(lib, p + "_delta").argtypes = [_I, _I, _I, _P, _P, _P]
     if prefix == "oracle":
@@ -557,4 +561,11 @@ def oracle():
 def reference():
     """The reference's own code, or None when it was not built here."""
     lib = _load(REF_SO, "ref")
+    return None if lib is None else _Impl(lib, "ref")
+
+
+def reference_dropin():
+    """The reference's own code with include/vflip/amgpcg_dropin.hpp as its
+    AMGPCGSolve (pressure solves on the GPU), or None when it was not built."""
+    lib = _load(REF_DROPIN_SO, "ref")
     return None if lib is None else _Impl(lib, "ref")

@@ -20,8 +20,17 @@ oracle/_ref/, which git ignores):
      and -ffp-contract=off so no FMA contraction changes rounding, together
      with the extern "C" harness oracle/ref_harness.cpp.
 
-Usage: python oracle/build_ref.py [--src /path/to/reference] [--force]
-Exit status 0 with a message when the reference tree is absent (nothing built).
+Where vflip_b200/libvflip_gpu.so is built, a second library,
+oracle/_ref/libvflip_ref_dropin.so, compiles the same reference sources and
+harness with oracle/dropin/AlgebraicMultigrid.h in place of the reference's
+AlgebraicMultigrid.h: its ivock::AMGPCGSolve is include/vflip/amgpcg_dropin.hpp,
+so SmokeSolver3D::pcg_projection and SubDomainSolver::pcg_projection run
+unchanged with their pressure solve on the GPU (the drop-in test).
+
+Usage: python oracle/build_ref.py [--src /path/to/vFLIP] [--force]
+The reference tree is --src, else $VFLIP_REF_SRC, else a checkout named
+"reference" beside this repository.  Exit status 0 with a message when the
+reference tree is absent (nothing built).
 """
 import argparse
 import os
@@ -31,8 +40,22 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
+
+
+def default_src():
+    """The reference tree: $VFLIP_REF_SRC, else ../reference beside the repository."""
+    env = os.environ.get("VFLIP_REF_SRC")
+    if env:
+        return env
+    return os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
+
+
 SRC_OUT = os.path.join(OUT, "src")
 LIB = os.path.join(OUT, "libvflip_ref.so")
+DROPIN_SRC = os.path.join(OUT, "dropin_src")
+DROPIN_LIB = os.path.join(OUT, "libvflip_ref_dropin.so")
+REPO = os.path.dirname(HERE)
+GPU_LIB_DIR = os.path.join(REPO, "vflip_b200")
 TUS = ["GeometricLevelGen.cpp", "levelset_util.cpp", "Smoke_solver3D.cpp", "sub_domain.cpp"]
 
 
@@ -86,11 +109,40 @@ def build(src_root, force=False):
     return LIB
 
 
+def build_dropin(force=False):
+    """The reference sources (patched copy in oracle/_ref/src) with the GPU
+    drop-in as their AMGPCGSolve, linked against libvflip_gpu.so."""
+    if not os.path.isdir(SRC_OUT) or not os.path.exists(os.path.join(GPU_LIB_DIR, "libvflip_gpu.so")):
+        return None
+    shim = os.path.join(HERE, "dropin", "AlgebraicMultigrid.h")
+    deps = [os.path.join(HERE, "ref_harness.cpp"), os.path.abspath(__file__), shim, LIB,
+            os.path.join(REPO, "include", "vflip", "amgpcg_dropin.hpp"), os.path.join(REPO, "include", "vflip.h")]
+    if (not force and os.path.exists(DROPIN_LIB)
+            and all(os.path.getmtime(DROPIN_LIB) >= os.path.getmtime(d) for d in deps)):
+        return DROPIN_LIB
+    # a separate copy: the units include "AlgebraicMultigrid.h" with quotes,
+    # which finds the file beside them first
+    os.makedirs(DROPIN_SRC, exist_ok=True)
+    for fn in os.listdir(SRC_OUT):
+        shutil.copyfile(os.path.join(SRC_OUT, fn), os.path.join(DROPIN_SRC, fn))
+    shutil.copyfile(shim, os.path.join(DROPIN_SRC, "AlgebraicMultigrid.h"))
+    cmd = ["g++", "-O2", "-fopenmp", "-std=c++14", "-fpermissive", "-ffp-contract=off",
+           "-fPIC", "-shared", "-w", "-DVFLIP_REF_DROPIN", "-Wl,-Bsymbolic",
+           "-include", os.path.join(DROPIN_SRC, "vflip_lvalue.h"),
+           "-I", os.path.join(HERE, "tbb_shim"), "-I", DROPIN_SRC, "-I", os.path.join(REPO, "include"),
+           os.path.join(HERE, "ref_harness.cpp")] + [os.path.join(DROPIN_SRC, t) for t in TUS] + [
+           "-L", GPU_LIB_DIR, "-l:libvflip_gpu.so", "-Wl,-rpath,$ORIGIN/../../vflip_b200", "-o", DROPIN_LIB]
+    subprocess.check_call(cmd)
+    return DROPIN_LIB
+
+
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default="/root/reference")
+    ap.add_argument("--src", default=None, help="the vFLIP source tree (default: $VFLIP_REF_SRC or ../reference)")
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
-    lib = build(a.src, a.force)
+    lib = build(a.src or default_src(), a.force)
     print(lib or "not built")
+    if lib:
+        print(build_dropin(a.force) or "drop-in build skipped (libvflip_gpu.so not built)")
     sys.exit(0)

@@ -159,6 +159,10 @@ int ref_levels(int ni, int nj, int nk, const uint32_t* rowstart, const uint32_t*
   return bad ? -1 : total;
 }
 
+#ifndef VFLIP_REF_DROPIN
+// (the drop-in build replaces AlgebraicMultigrid.h, which defines RBGS and
+// amgPrecond, by the GPU solve; only its AMGPCGSolve is on the path)
+
 // ivock::RBGS (AlgebraicMultigrid.h:22-103), iters full red-black sweeps.
 void ref_rbgs(int ni, int nj, int nk, const uint32_t* rowstart, const uint32_t* colindex,
               const double* value, const double* b, double* x, int iters) {
@@ -187,6 +191,8 @@ void ref_vcycle(int ni, int nj, int nk, const uint32_t* rowstart, const uint32_t
   for (int l = 1; l < total; ++l) delete A_L[l];
   for (int l = 0; l + 1 < total; ++l) { delete R_L[l]; delete P_L[l]; }
 }
+
+#endif  // VFLIP_REF_DROPIN
 
 // ivock::AMGPCGSolve, SparseMatrix overload (AlgebraicMultigrid.h:189-301).
 int ref_amgpcg(int ni, int nj, int nk, const uint32_t* rowstart, const uint32_t* colindex,

@@ -32,7 +32,7 @@ class ConfigC(C.Structure):
                 ("stream", C.c_void_p), ("sweep_kernel", C.c_int), ("smoother_depth", C.c_int),
                 ("smoother_tile_rows", C.c_int), ("smoother_plane_ranges", C.c_int),
                 ("smoother_ctas_per_sm", C.c_int), ("smoother_threads", C.c_int),
-                ("smoother_prefetch", C.c_int), ("coarsest_solver", C.c_int)]
+                ("smoother_prefetch", C.c_int), ("coarsest_solver", C.c_int), ("spmv_kernel", C.c_int)]
 
 
 class SystemC(C.Structure):

@@ -151,6 +151,152 @@ __global__ void __launch_bounds__(BLOCK) pcg_spmv_dot_kernel(const T* __restrict
   finish_reduction<BLOCK>(partials, nb, st, kReduceSZ, 0.0, nb);
 }
 
+// The same step as pcg_spmv_dot_kernel for grids whose rows are whole
+// quads (ni % 4 == 0): one thread per quad of 4 consecutive cells, a block
+// per (TY rows + one halo row either side) x (a range of planes), marching k.
+// Each cell's s_new is formed once per block: z-neighbours ride in
+// registers (three planes), x- and y-neighbours and the -y couplings come
+// from a three-plane shared-memory ring that every thread writes once per
+// plane, so one barrier per plane suffices.  The halo rows only form s and
+// yp.  q of plane k-1 is computed in the step that forms plane k.  Each
+// cell's q sums its terms in pcg_spmv_dot_kernel's order (-z, -y, -x, diag,
+// +x, +y, +z) with the same roundings, so q and s_new are bitwise those of
+// that kernel; the partial dots are grouped differently (deterministic).
+template <typename T>
+struct alignas(4 * sizeof(T)) Quad {
+  T v[4];
+};
+
+template <typename T>
+__device__ __forceinline__ Quad<T> ldq(const T* p) {
+  return *reinterpret_cast<const Quad<T>*>(p);
+}
+
+template <typename T, bool FIRST>
+__global__ void __launch_bounds__(1024) pcg_spmv_dot_plane_kernel(
+    const T* __restrict__ z, const T* __restrict__ s_old, T* __restrict__ s_new, T* __restrict__ q,
+    const T* __restrict__ diag, const T* __restrict__ xp, const T* __restrict__ yp, const T* __restrict__ zp,
+    int ni, int nj, int nk, int ty, int kz, double* partials, PcgScalars* st) {
+  using A = typename Num<T>::Acc;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int qx = threadIdx.x, ry = threadIdx.y, nq = blockDim.x, rows = blockDim.y;  // rows = ty + 2
+  Quad<T>* sbuf = reinterpret_cast<Quad<T>*>(smem_raw);  // [3][rows][nq]
+  Quad<T>* ybuf = sbuf + 3 * rows * nq;                   // [3][rows][nq]
+  __shared__ double red[32];
+  const int j = blockIdx.x * ty - 1 + ry;
+  const bool in_row = j >= 0 && j < nj;
+  const bool interior = ry >= 1 && ry <= ty && in_row;
+  const int kb = blockIdx.y * kz, ke = min(kb + kz, nk);
+  const size_t sy = (size_t)ni, szs = (size_t)ni * nj;
+  const int i0 = 4 * qx;
+  const double beta = FIRST ? 0.0 : st->beta;
+  Quad<T> sm{}, sc{}, sp{};  // s of planes k-1, k, k+1 (relative to the q plane)
+  Quad<T> zprev{};           // zp of the plane below the q plane
+  double dot = 0.0;
+  for (int kk = kb - 1; kk <= ke; ++kk) {
+    // s_new of plane kk on this thread's row
+    Quad<T> snew{};
+    Quad<T> ypk{};
+    if (in_row && kk >= 0 && kk < nk) {
+      const size_t g = (size_t)i0 + sy * j + szs * kk;
+      const Quad<T> zq = ldq(z + g);
+      if (FIRST) {
+        snew = zq;
+      } else {
+        const Quad<T> so = ldq(s_old + g);
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          snew.v[c] = cvt<T>((A)((double)ldv(&zq.v[c]) + beta * (double)ldv(&so.v[c])));
+      }
+      if (ry <= ty) ypk = ldq(yp + g);
+    }
+    const int bw = (kk + 3) % 3;  // kk >= -1
+    sbuf[(bw * rows + ry) * nq + qx] = snew;
+    ybuf[(bw * rows + ry) * nq + qx] = ypk;
+    sm = sc;
+    sc = sp;
+    sp = snew;
+    __syncthreads();
+    const int k = kk - 1;  // the q plane
+    if (interior && k >= kb && k < ke) {
+      const size_t g = (size_t)i0 + sy * j + szs * k;
+      const int br = (k + 3) % 3;
+      const Quad<T> dq = ldq(diag + g), xq = ldq(xp + g), zq = ldq(zp + g);
+      const Quad<T> yq = ybuf[(br * rows + ry) * nq + qx];
+      const Quad<T> sdn = sbuf[(br * rows + ry - 1) * nq + qx], ydn = ybuf[(br * rows + ry - 1) * nq + qx];
+      const Quad<T> sup = sbuf[(br * rows + ry + 1) * nq + qx];
+      // x-neighbours: the left and right cells of each cell of the quad, and
+      // the -x coupling (xp of the cell to the left)
+      A sleft[4], sright[4], xleft[4];
+      sleft[0] = qx > 0 ? ldv(&sbuf[(br * rows + ry) * nq + qx - 1].v[3]) : A(0);
+      xleft[0] = qx > 0 ? ldg(xp + g - 1) : A(0);
+      sright[3] = qx + 1 < nq ? ldv(&sbuf[(br * rows + ry) * nq + qx + 1].v[0]) : A(0);
+#pragma unroll
+      for (int c = 1; c < 4; ++c) {
+        sleft[c] = ldv(&sc.v[c - 1]);
+        xleft[c] = ldv(&xq.v[c - 1]);
+        sright[c - 1] = ldv(&sc.v[c]);
+      }
+      Quad<T> qo;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int i = i0 + c;
+        A acc = A(0);
+        if (k > 0) acc = acc + ldv(&zprev.v[c]) * ldv(&sm.v[c]);
+        if (j > 0) acc = acc + ldv(&ydn.v[c]) * ldv(&sdn.v[c]);
+        if (i > 0) acc = acc + xleft[c] * sleft[c];
+        acc = acc + ldv(&dq.v[c]) * ldv(&sc.v[c]);
+        if (i < ni - 1) acc = acc + ldv(&xq.v[c]) * sright[c];
+        if (j < nj - 1) acc = acc + ldv(&yq.v[c]) * ldv(&sup.v[c]);
+        if (k < nk - 1) acc = acc + ldv(&zq.v[c]) * ldv(&sp.v[c]);
+        qo.v[c] = cvt<T>(acc);
+        dot += (double)ldv(&sc.v[c]) * (double)ldv(&qo.v[c]);
+      }
+      *reinterpret_cast<Quad<T>*>(q + g) = qo;
+      *reinterpret_cast<Quad<T>*>(s_new + g) = sc;
+      zprev = zq;
+    } else if (interior && k == kb - 1 && k >= 0) {
+      // the plane below the first q plane: only its zp is carried
+      zprev = ldq(zp + (size_t)i0 + sy * j + szs * k);
+    }
+  }
+  // block sum in a fixed order: warp trees, then warps in index order
+  const int tid = qx + nq * ry, nthreads = nq * rows;
+  for (int o = 16; o > 0; o >>= 1) dot += __shfl_down_sync(0xffffffffu, dot, o);
+  if ((tid & 31) == 0) red[tid >> 5] = dot;
+  __syncthreads();
+  const int bid = blockIdx.x + gridDim.x * blockIdx.y, nb = gridDim.x * gridDim.y;
+  if (tid == 0) {
+    double b = 0.0;
+    for (int w = 0; w < (nthreads + 31) / 32; ++w) b += red[w];
+    partials[bid] = b;
+  }
+  // finish_reduction's fold needs a 1-D view of the block: thread 0 arrives
+  // for the block, the last block's threads fold
+  __shared__ bool last;
+  if (tid == 0) {
+    __threadfence();
+    const unsigned int ticket = atomicAdd(&st->done_blocks[kReduceSZ], 1u);
+    last = (ticket == (unsigned)nb - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double v = 0.0;
+  for (int p = tid; p < nb; p += nthreads) v += ((volatile double*)partials)[p];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((tid & 31) == 0) red[tid >> 5] = v;
+  __syncthreads();
+  if (tid == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < (nthreads + 31) / 32; ++w) tot += red[w];
+    st->done_blocks[kReduceSZ] = 0;
+    st->sz = tot;
+    st->alpha = st->rho / tot;
+  }
+}
+
 // x += alpha s, r -= alpha q, partial |r|_inf  (AlgebraicMultigrid.h:259-262)
 template <typename T, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) pcg_update_kernel(T* __restrict__ x, T* __restrict__ r,

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <mutex>
 #include <cstring>
+#include <map>
 #include <string>
 #include <type_traits>
 #include <unordered_map>
@@ -46,6 +47,25 @@ struct Dims {
   int ni, nj, nk;
   size_t n() const { return (size_t)ni * nj * nk; }
 };
+
+// Raises a kernel's dynamic shared-memory limit on the current device, once
+// per (kernel, device) pair.  The attribute is per device, so a process that
+// drives several GPUs (or creates contexts from several threads) opts every
+// device in; the table is guarded by a mutex.
+cudaError_t smem_optin(const void* func, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> g(mu);
+  const auto key = std::make_pair(func, dev);
+  auto it = done.find(key);
+  if (it != done.end() && it->second >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done[key] = bytes;
+  return e;
+}
 
 }  // namespace
 
@@ -189,11 +209,8 @@ SweepShape sweep_shape(const Dims& d, int num_sms) {
 template <typename S, typename V, bool Z, bool P, bool D>
 int launch_sweep_t(vflip_ctx* ctx, const SweepArgs<S, V>& a, const SweepShape& sh) {
   auto kern = rbgs_sweep_kernel<S, V, Z, P, D, kSweepBlock>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
+  if (smem_optin((const void*)kern, 200 * 1024) != cudaSuccess)
+    return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the sweep's shared memory limit");
   dim3 grid(sh.grid_y, sh.grid_z);
   const bool timed = ctx->profiling && (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n;
   if (timed) {
@@ -305,16 +322,12 @@ int launch_tma_t(vflip_ctx* ctx, const TmaSweepArgs<S>& a, const TmaShape& sh) {
   // the tuned shape of a 256-cell-row fine level (7-row tiles, one copy group
   // in flight) runs an instance with that layout compiled in
   const bool fixed = sh.carry && a.ni == 256 && a.tyo == 7 && a.depth == 1;
-  const int which = fixed ? 3 : (sh.carry ? 2 : (wide ? 1 : 0));
   auto kern = fixed ? rbgs_sweep_carry_kernel<S, Z, P, D, kTmaBlockWide, 256, 7, 1>
                     : sh.carry ? rbgs_sweep_carry_kernel<S, Z, P, D, kTmaBlockWide>
                                : (wide ? rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlockWide>
                                        : rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlock>);
-  static bool attr_set[4] = {false, false, false, false};
-  if (!attr_set[which]) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemMax);
-    attr_set[which] = true;
-  }
+  if (smem_optin((const void*)kern, (int)kTmaSmemMax) != cudaSuccess)
+    return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the sweep's shared memory limit");
   const bool timed = ctx->profiling && (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n;
   if (timed) {
     if (ctx->prof_used == ctx->prof_events.size()) {
@@ -398,11 +411,8 @@ const CUtensorMap* grid_map(vflip_ctx* ctx, const void* p, int es, int nx, int n
 template <typename S, bool Z, bool P, bool D>
 int launch_t3d_t(vflip_ctx* ctx, const T3dMaps<S>& mp, const T3dArgs& a, dim3 grid, size_t smem) {
   auto kern = rbgs_sweep_t3d_kernel<S, Z, P, D, kT3dTX, kT3dTY, kT3dBlock>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTmaSmemMax);
-    attr_set = true;
-  }
+  if (smem_optin((const void*)kern, (int)kTmaSmemMax) != cudaSuccess)
+    return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the sweep's shared memory limit");
   const bool timed = ctx->profiling && (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n;
   if (timed) {
     if (ctx->prof_used == ctx->prof_events.size()) {
@@ -549,11 +559,8 @@ int coarsest(vflip_ctx* ctx, const Level<S, V>& L, const V* b, V* x_out, int swe
   const int* skip = nullptr;
   if (cd && cd->on) {
     auto sk = coarse_chol_solve_kernel<V, kCholSolveBlock>;
-    static bool sattr = false;
-    if (!sattr) {
-      cudaFuncSetAttribute(sk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCholStageMax);
-      sattr = true;
-    }
+    if (smem_optin((const void*)sk, (int)kCholStageMax) != cudaSuccess)
+      return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the coarsest solve's shared memory limit");
     // the factor lives in shared memory for the solve when it fits
     const size_t staged_bytes = (n + n * (cd->bw + 1) + n) * sizeof(double);
     const int staged = staged_bytes <= kCholStageMax;
@@ -564,11 +571,8 @@ int coarsest(vflip_ctx* ctx, const Level<S, V>& L, const V* b, V* x_out, int swe
   }
   size_t smem = 6 * n * sizeof(A);
   auto kern = coarsest_rbgs_kernel<S, V, kCoarseBlock>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024);
-    attr_set = true;
-  }
+  if (smem_optin((const void*)kern, 220 * 1024) != cudaSuccess)
+    return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the coarsest sweeps' shared memory limit");
   if (smem > 220 * 1024) return ctx->fail(VFLIP_ERR_ARG, "coarsest level of %zu unknowns exceeds 4096", n);
   kern<<<1, kCoarseBlock, smem, ctx->stream>>>(b, L.diag, L.xp, L.yp, L.zp, x_out, L.d.ni, L.d.nj, L.d.nk, sweeps,
                                                dot_out, skip);
@@ -668,12 +672,8 @@ int build_coarse_direct(vflip_ctx* ctx, const Hierarchy64& H, const double* d0, 
   cd.ok = reinterpret_cast<int*>(cd.rinv + n);
   cd.bw = bw;
   auto kern = coarse_chol_kernel<kCholBlock>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)((kCholMaxBw + 1) * (kCholMaxBw + 1) * sizeof(double)));
-    attr_set = true;
-  }
+  if (smem_optin((const void*)kern, (int)((kCholMaxBw + 1) * (kCholMaxBw + 1) * sizeof(double))) != cudaSuccess)
+    return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the coarsest factorisation's shared memory limit");
   kern<<<1, kCholBlock, (size_t)(bw + 1) * (bw + 1) * sizeof(double), ctx->stream>>>(
       dg, xp, yp, zp, d.ni, d.nj, d.nk, bw, cd.L, cd.rinv, cd.ok);
   VF_LAUNCH_CHECK();
@@ -844,6 +844,51 @@ int read_scalars(vflip_ctx* ctx) {
   return check_kernel_error(ctx, ctx->st_host->kernel_error);
 }
 
+// s_new = z + beta s_old (s_new = z on the first iteration), q = A s_new on
+// the fine level and the s.q reduction (alpha).  The plane-marching kernel
+// runs where the fine rows are whole warps of quads (unless the context asks
+// for the column kernel, or `plane` is false: the batched graph keeps the
+// column kernel); both give the same q and s_new bits.
+template <typename V>
+int launch_spmv_dot(vflip_ctx* ctx, cudaStream_t stream, bool first, const V* z, const V* s_old, V* s_new, V* q,
+                    const V* diag, const V* xp, const V* yp, const V* zp, const Dims& d, bool plane = true) {
+  const int nq = d.ni / 4;
+  if (plane && ctx->cfg.spmv_kernel == 0 && d.ni % 128 == 0 && nq <= 256) {
+    const int ty = std::min(8, 1024 / nq - 2);
+    const int rows = ty + 2;
+    const size_t smem = 6 * (size_t)rows * nq * sizeof(Quad<V>);
+    auto kern = first ? pcg_spmv_dot_plane_kernel<V, true> : pcg_spmv_dot_plane_kernel<V, false>;
+    if (smem_optin((const void*)kern, (int)smem) != cudaSuccess)
+      return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the SpMV kernel's shared memory limit");
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nq * rows, smem) != cudaSuccess || per_sm < 1)
+      per_sm = 1;
+    // one wave of resident blocks: row tiles x plane ranges
+    const int rt = (d.nj + ty - 1) / ty;
+    int kr = std::max(1, std::min(d.nk, per_sm * ctx->num_sms / rt));
+    const int kz = (d.nk + kr - 1) / kr;
+    kr = (d.nk + kz - 1) / kz;
+    if ((size_t)rt * kr <= (size_t)kMaxPartials) {
+      kern<<<dim3(rt, kr), dim3(nq, rows), smem, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp, d.ni, d.nj, d.nk,
+                                                           ty, kz, ctx->partials, ctx->st);
+      VF_LAUNCH_CHECK();
+      return VFLIP_OK;
+    }
+  }
+  dim3 sblk(kRedBlock);
+  const int kz = 8;
+  dim3 sgrid((d.ni + 31) / 32, (d.nj + kRedBlock / 32 - 1) / (kRedBlock / 32), (d.nk + kz - 1) / kz);
+  if ((size_t)sgrid.x * sgrid.y * sgrid.z > (size_t)kMaxPartials) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
+  if (first)
+    pcg_spmv_dot_kernel<V, true, kRedBlock><<<sgrid, sblk, 0, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp, d.ni,
+                                                                        d.nj, d.nk, kz, ctx->partials, ctx->st);
+  else
+    pcg_spmv_dot_kernel<V, false, kRedBlock><<<sgrid, sblk, 0, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp, d.ni,
+                                                                         d.nj, d.nk, kz, ctx->partials, ctx->st);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
 template <typename S0, typename SC, typename V>
 int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor, int maxit,
               vflip_solve_stats* stats, V* x1_out = nullptr) {
@@ -893,23 +938,13 @@ int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* re
     iterations = 0;
     return finish(VFLIP_NOT_CONVERGED);
   }
-  dim3 sblk(kRedBlock);
-  const int kz = 8;
-  dim3 sgrid((d.ni + 31) / 32, (d.nj + kRedBlock / 32 - 1) / (kRedBlock / 32), (d.nk + kz - 1) / kz);
-  if ((size_t)sgrid.x * sgrid.y * sgrid.z > (size_t)kMaxPartials) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
   V* s_old = s0;
   V* s_new = s1;
   int it;
   for (it = 0; it < maxit; ++it) {
-    if (it == 0)
-      pcg_spmv_dot_kernel<V, true, kRedBlock><<<sgrid, sblk, 0, ctx->stream>>>(
-          z, s_old, s_new, q, T.fine.diag, T.fine.xp, T.fine.yp, T.fine.zp, d.ni, d.nj, d.nk, kz, ctx->partials,
-          ctx->st);
-    else
-      pcg_spmv_dot_kernel<V, false, kRedBlock><<<sgrid, sblk, 0, ctx->stream>>>(
-          z, s_old, s_new, q, T.fine.diag, T.fine.xp, T.fine.yp, T.fine.zp, d.ni, d.nj, d.nk, kz, ctx->partials,
-          ctx->st);
-    VF_LAUNCH_CHECK();
+    if ((rc = launch_spmv_dot<V>(ctx, ctx->stream, it == 0, z, s_old, s_new, q, T.fine.diag, T.fine.xp, T.fine.yp,
+                                 T.fine.zp, d)))
+      return rc;
     pcg_update_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(x, r, s_new, q, n, ctx->partials, ctx->st);
     VF_LAUNCH_CHECK();
     if (it == 0 && x1_out) VF_CUDA(cudaMemcpyAsync(x1_out, x, n * sizeof(V), cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1246,21 +1281,12 @@ int learned_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double
   ++vcycles;
   if ((rc = read_scalars(ctx))) return rc;
   if (h.bad_rho) return fallback();
-  dim3 sblk(kRedBlock);
-  const int kz = 8;
-  dim3 sgrid((d.ni + 31) / 32, (d.nj + kRedBlock / 32 - 1) / (kRedBlock / 32), (d.nk + kz - 1) / kz);
-  if ((size_t)sgrid.x * sgrid.y * sgrid.z > (size_t)kMaxPartials) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
   V* s_old = s0;
   V* s_new = s1;
   std::vector<double> hist{h.res};
   for (int it = 0; it < maxit; ++it) {
-    if (it == 0)
-      pcg_spmv_dot_kernel<V, true, kRedBlock><<<sgrid, sblk, 0, ctx->stream>>>(
-          z, s_old, s_new, q, F.diag, F.xp, F.yp, F.zp, d.ni, d.nj, d.nk, kz, ctx->partials, ctx->st);
-    else
-      pcg_spmv_dot_kernel<V, false, kRedBlock><<<sgrid, sblk, 0, ctx->stream>>>(
-          z, s_old, s_new, q, F.diag, F.xp, F.yp, F.zp, d.ni, d.nj, d.nk, kz, ctx->partials, ctx->st);
-    VF_LAUNCH_CHECK();
+    if ((rc = launch_spmv_dot<V>(ctx, ctx->stream, it == 0, z, s_old, s_new, q, F.diag, F.xp, F.yp, F.zp, d)))
+      return rc;
     fcg_update_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(x, r, r2, s_new, q, n, ctx->partials,
                                                                         ctx->st);
     VF_LAUNCH_CHECK();
@@ -1551,6 +1577,7 @@ void vflip_config_default(vflip_config* cfg) {
   cfg->smoother_threads = 0;
   cfg->smoother_prefetch = 0;
   cfg->coarsest_solver = 0;
+  cfg->spmv_kernel = 0;
 }
 
 int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
@@ -1581,7 +1608,8 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
       ctx->cfg.smoother_ctas_per_sm < 0 ||
       (ctx->cfg.smoother_threads != 0 && ctx->cfg.smoother_threads != kTmaBlock &&
        ctx->cfg.smoother_threads != kTmaBlockWide) ||
-      ctx->cfg.coarsest_solver < 0 || ctx->cfg.coarsest_solver > 2)
+      ctx->cfg.coarsest_solver < 0 || ctx->cfg.coarsest_solver > 2 || ctx->cfg.spmv_kernel < 0 ||
+      ctx->cfg.spmv_kernel > 1)
     return bad(VFLIP_ERR_ARG);
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);

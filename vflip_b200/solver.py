@@ -68,7 +68,7 @@ class Solver:
     def __init__(self, precision=1, pre_sweeps=4, post_sweeps=4, coarse_sweeps=0, coarsest_max_unknowns=0,
                  device=0, stream=None, sweep_kernel=0, smoother_depth=0, smoother_tile_rows=0,
                  smoother_plane_ranges=0, smoother_ctas_per_sm=0, smoother_threads=0,
-                 smoother_prefetch=0, coarsest_solver=0):
+                 smoother_prefetch=0, coarsest_solver=0, spmv_kernel=0):
         self.lib = load()
         cfg = ConfigC()
         self.lib.vflip_config_default(C.byref(cfg))
@@ -86,6 +86,7 @@ class Solver:
         cfg.smoother_threads = smoother_threads
         cfg.smoother_prefetch = smoother_prefetch
         cfg.coarsest_solver = coarsest_solver
+        cfg.spmv_kernel = spmv_kernel
         self.device = torch.device("cuda", device)
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
