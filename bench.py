@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched uneven-Poisson arm")
     ap.add_argument("--no-flip", action="store_true", help="skip the FLIP smoke arm")
     ap.add_argument("--no-nested", action="store_true", help="skip the nested-subdomain arm")
+    ap.add_argument("--no-precisions", action="store_true", help="skip the fp64/mixed plain arms")
     ap.add_argument("--learned-level", type=int, default=1)
     ap.add_argument("--learned-capture", type=int, default=40)
     ap.add_argument("--learned-epochs", type=int, default=16)
@@ -201,7 +202,6 @@ def run_vflip(a):
     clocks = ClockSampler(f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local))
     time.sleep(0.3)
     iters, vcycles, resid = [], [], []
-    solver.set_profiling(True)
     launches0 = solver.launch_count
     barrier()
     torch.cuda.synchronize()
@@ -217,10 +217,17 @@ def run_vflip(a):
     barrier()
     ms = e0.elapsed_time(e1)
     launches = solver.launch_count - launches0
-    n_sweeps, sweep_ms, cells = solver.profile_sweeps()
-    solver.set_profiling(False)
     clk = clocks.stop()
     ms_max = max_over_ranks(ms)
+    # the roofline's per-launch times: a separate pass of a few steps with the
+    # library's events around every fine-level sweep (that pass runs the host
+    # PCG loop, whose launches can carry events; the kernels are the same)
+    solver.set_profiling(True)
+    for _ in range(min(a.steps, 5)):
+        sim.step()
+    torch.cuda.synchronize()
+    n_sweeps, sweep_ms, cells = solver.profile_sweeps()
+    solver.set_profiling(False)
 
     # end to end through the public API with host-resident state
     host = {k: torch.empty(sim.shapes[k], dtype=torch.float32, pin_memory=True) for k in sim.FIELDS}
@@ -270,6 +277,8 @@ def run_vflip(a):
             "gpu_launches": launches,
             "clocks": clk,
         }
+        if not a.no_precisions and world == 1:
+            out["precisions"] = precision_arm(a, sim, local, a.steps)
         if not a.no_cpu_baseline and world == 1:
             out["cpu_baseline"] = cpu_baseline(a, {k: sim.f[k].cpu().numpy().copy() for k in sim.FIELDS}, params)
         if not a.no_learned and world == 1:
@@ -534,30 +543,106 @@ def batched_arm(solver, count=32, reps=2):
             "cells_per_s_graph": cells / (g[0] * 1e-3)}
 
 
+# the reference's own hierarchy (16^3 coarsest level, 200 red-black sweeps):
+# in an FP64 context the V-cycle is the reference's bit for bit
+REF_HIERARCHY = dict(coarse_sweeps=200, coarsest_max_unknowns=4096, coarsest_solver=1)
+
+
 def solve_diagnostics(sim, device):
     """One more step, outside the timed region, whose projection is solved
-    twice: by the benchmarked solver and by an FP64 context (the GPU oracle
-    solve).  Reports the pressure error against the FP64 solve, both
-    residual ratios and max |div u| after projection."""
+    four ways on the same assembled system:
+      * the benchmarked context (its precision and hierarchy);
+      * an FP64 context with the reference's hierarchy to the same 1e-6: the
+        reference's own answer (its V-cycle bit for bit, its iteration count);
+      * an FP64 context to 1e-12: the converged solution;
+      * an FP32 context with the reference's hierarchy, to 1e-6.
+    The pressure errors split what FP32 arithmetic changes from what
+    stopping at 1e-6 with another preconditioner changes: the reference's
+    answer itself sits `ref_fp64_vs_converged` from the converged solution.
+    Also both residual ratios and max |div u| before/after the projection."""
     import torch
 
     from vflip_b200.solver import Solver
 
     sim.advect_and_force()
     pre = {k: sim.f[k].clone() for k in ("u", "v", "w")}
-    n = sim.p.n
+    n, p = sim.p.n, sim.p
     before = float(sim.divergence(pre["u"], pre["v"], pre["w"]).abs().max())
     p32 = torch.zeros((n, n, n), dtype=torch.float64, device=sim.s.device)
     ok, _, st = sim.project(pressure=p32)
-    with Solver(precision=0, device=device) as s64:
-        u64, v64, w64 = (pre[k].clone() for k in ("u", "v", "w"))
-        p64 = torch.zeros_like(p32)
-        ok64, _, st64 = sim.project(solver=s64, u=u64, v=v64, w=w64, pressure=p64)
-    err = float(torch.linalg.vector_norm(p32 - p64) / torch.linalg.vector_norm(p64))
     after = float(sim.divergence(sim.f["u"], sim.f["v"], sim.f["w"]).abs().max())
+    bench_u = [sim.f[k].clone() for k in ("u", "v", "w")]
+
+    def solve(solver, tol, maxit=p.max_iterations):
+        vel = [pre[k].clone() for k in ("u", "v", "w")]
+        pr = torch.zeros_like(p32)
+        ok_, _, st_ = solver.project(n, n, n, p.h, 0.0, sim.phi, sim.bdesc, sim.solid["u"], sim.solid["v"],
+                                     sim.solid["w"], *vel, pressure=pr, tolerance_factor=tol, max_iterations=maxit)
+        return pr, vel, st_
+
+    with Solver(precision=0, device=device, **REF_HIERARCHY) as s64:
+        p_ref, u_ref, st_ref = solve(s64, p.tol)
+        p_conv, _, st_conv = solve(s64, 1e-12, 400)
+    with Solver(precision=1, device=device, **REF_HIERARCHY) as s32r:
+        p_r32, _, st_r32 = solve(s32r, p.tol)
+
+    def rel(a, b):
+        return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+    vel_err = max(float((a - b).abs().max()) for a, b in zip(bench_u, u_ref)) / max(
+        float(b.abs().max()) for b in u_ref)
     return {"rel_residual_inf": st.residual / st.rhs_norm, "iterations_last": st.iterations,
-            "pressure_rel_l2_vs_fp64_gpu_solve": err, "fp64_iterations": st64.iterations,
+            "pressure_rel_l2_vs_reference_fp64_solve": rel(p32, p_ref),
+            "pressure_rel_l2_vs_converged": rel(p32, p_conv),
+            "ref_fp64_vs_converged": rel(p_ref, p_conv),
+            "fp32_ref_hierarchy_vs_reference_fp64_solve": rel(p_r32, p_ref),
+            "velocity_rel_max_vs_reference_fp64_solve": vel_err,
+            "reference_iterations": st_ref.iterations, "fp32_ref_hierarchy_iterations": st_r32.iterations,
+            "converged_iterations": st_conv.iterations,
             "max_abs_div_before": before, "max_abs_div_after": after}
+
+
+def precision_arm(a, sim, device, steps):
+    """The same plume, continued from the headline run's state, in the other
+    precision modes of the plain MGPCG: steps/s (CUDA events, `steps` steps
+    each after one untimed step), PCG iterations and V-cycles.  fp64 runs the
+    reference's hierarchy (its bit-exact V-cycle): the like-for-like
+    counterpart of the reference's FP64 solve."""
+    import numpy as np
+    import torch
+
+    from vflip_b200.solver import Solver
+
+    state = {k: sim.f[k].clone() for k in sim.FIELDS}
+    out = {}
+    for name, kw in (("fp64", dict(precision=0, **REF_HIERARCHY)), ("mixed", dict(precision=2)),
+                     ("fp32", dict(precision=1))):
+        if name == a.precision:
+            continue
+        with Solver(device=device, **kw) as s:
+            old = sim.s
+            sim.s = s
+            for k in sim.FIELDS:
+                sim.f[k].copy_(state[k])
+            sim.step()
+            its, vcs = [], []
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(steps):
+                _, st = sim.step()
+                its.append(st.iterations)
+                vcs.append(st.vcycles)
+            e1.record()
+            torch.cuda.synchronize()
+            sim.s = old
+            ms = e0.elapsed_time(e1)
+            out[name] = {"steps_per_s": steps / (ms * 1e-3), "ms_per_step": ms / steps,
+                         "pcg_iterations_mean": float(np.mean(its)), "vcycles_mean": float(np.mean(vcs)),
+                         "config": {k: v for k, v in kw.items()}}
+    for k in sim.FIELDS:
+        sim.f[k].copy_(state[k])
+    return out
 
 
 def _cpu_impl():

@@ -103,6 +103,21 @@ typedef struct {
    * 1 = always the column kernel.  Both give the same q and s bit for bit;
    * their s.q partial sums are grouped differently. */
   int spmv_kernel;
+  /* RK2 advection kernel (vflip_advect_rk2_linear, _linear2): 0 (default) =
+   * automatic: the tiled kernel (velocity grids, and a field that is not one
+   * of them, staged in shared memory around each block's 32 x 8 x 8 nodes;
+   * samples beyond the staged halo read global memory); 1 = the per-node
+   * gather kernel.  Both give the same bits. */
+  int advect_kernel;
+  /* PCG loop: 0 (default) = automatic: the loop runs on the device, a CUDA
+   * graph (captured once per hierarchy layout and reused) whose conditional
+   * while node repeats V-cycle, direction, SpMV and update until the
+   * device-side stop test holds, with one read of the scalars per solve -
+   * unless per-launch profiling is on; 1 = the host loop, which reads the
+   * scalars after every iteration.  Same iterates; a solve that does not
+   * converge on the device is repeated by the host loop, so the failure
+   * results (zero-rho exit, max_iterations) are the host loop's. */
+  int pcg_loop;
 } vflip_config;
 
 typedef struct {
@@ -247,6 +262,13 @@ int vflip_advect_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, flo
 int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
                              const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
                              double oz, const float* field, float* out, const float* field2, float* out2);
+
+/* The velocity's self-advection of SubDomainSolver::advect_field
+ * (SS/sub_domain.cpp:191-235) for u, v and w in one launch: uo, vo, wo (the
+ * face grids, which must not alias u/v/w) receive what three
+ * vflip_advect_rk2_linear calls give, bit for bit. */
+int vflip_advect_velocity_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                                     const float* v, const float* w, float* uo, float* vo, float* wo);
 
 /* SmokeSolver3D::advect_field_cubic_clamp (SS/Smoke_solver3D.cpp:657-707):
  * the RK2 backtrace above, then the cubic sample of Buffer3D::sample_cubic
@@ -485,13 +507,23 @@ int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const vo
 
 /* ---- measurement ----------------------------------------------------------- */
 
-/* When enabled, every launch of the fine-level smoothing sweep (the
- * dominant kernel) is bracketed by a pair of CUDA events on the context
- * stream.  vflip_profile_sweeps synchronises the stream and returns the
- * number of timed launches, their summed device time and the fine level's
- * cell count, then starts a new count.  No reference counterpart. */
+/* When enabled, every launch of the kinds below is bracketed by a pair of
+ * CUDA events on its stream (the PCG loop then runs on the host, whose
+ * launches can carry events): the fine-level smoothing sweep (the dominant
+ * kernel), the fine-level PCG SpMV and update, and the RK2 advection
+ * launches.  vflip_profile_kernels synchronises the stream and returns the
+ * number of timed launches of one kind and their summed device time;
+ * vflip_profile_sweeps returns the fine sweeps' figures and the fine level's
+ * cell count, then starts a new count for every kind.  Enabling (again)
+ * also starts a new count.  No reference counterpart. */
+#define VFLIP_PROF_FINE_SWEEP 0
+#define VFLIP_PROF_SPMV 1
+#define VFLIP_PROF_UPDATE 2
+#define VFLIP_PROF_ADVECT_VELOCITY 3
+#define VFLIP_PROF_ADVECT_FIELD 4
 int vflip_set_profiling(vflip_ctx* ctx, int enable);
 int vflip_profile_sweeps(vflip_ctx* ctx, int* launches, double* total_ms, double* cells);
+int vflip_profile_kernels(vflip_ctx* ctx, int kind, int* launches, double* total_ms);
 /* Number of kernels launched through this context so far. */
 unsigned long long vflip_launch_count(const vflip_ctx* ctx);
 

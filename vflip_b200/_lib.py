@@ -32,7 +32,8 @@ class ConfigC(C.Structure):
                 ("stream", C.c_void_p), ("sweep_kernel", C.c_int), ("smoother_depth", C.c_int),
                 ("smoother_tile_rows", C.c_int), ("smoother_plane_ranges", C.c_int),
                 ("smoother_ctas_per_sm", C.c_int), ("smoother_threads", C.c_int),
-                ("smoother_prefetch", C.c_int), ("coarsest_solver", C.c_int), ("spmv_kernel", C.c_int)]
+                ("smoother_prefetch", C.c_int), ("coarsest_solver", C.c_int), ("spmv_kernel", C.c_int),
+                ("advect_kernel", C.c_int), ("pcg_loop", C.c_int)]
 
 
 class SystemC(C.Structure):
@@ -74,6 +75,7 @@ SIGNATURES = {
     "vflip_advect_rk2_linear2": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _P, _P, _P, _P]),
     "vflip_advect_cubic_clamp": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _P, _P]),
     "vflip_advect_velocity_cubic_clamp": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P]),
+    "vflip_advect_velocity_rk2_linear": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _P, _P, _P]),
     "vflip_advect_rk3_linear": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _D, _P, _P]),
     "vflip_advect_rk3_linear2": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _I, _I, _I, _D, _D, _D, _D, _P, _P, _P,
                                       _P]),
@@ -102,6 +104,7 @@ SIGNATURES = {
     "vflip_g2p": (_I, [_P, _I, _I, _I, _F, _P, _I, _P, _P, _P, _P, _P, _P, _D]),
     "vflip_set_profiling": (_I, [_P, _I]),
     "vflip_profile_sweeps": (_I, [_P, C.POINTER(_I), C.POINTER(_D), C.POINTER(_D)]),
+    "vflip_profile_kernels": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_D)]),
     "vflip_launch_count": (C.c_ulonglong, [_P]),
     "vflip_plume_sources": (_I, [_P, _I, _I, _I, _F, _F, _P, _P, _P, _F, _F, _F, _F, _F, _F, _F, _F]),
     "vflip_bricks_to_linear": (_I, [_P, _I, _I, _I, _P, _P]),

@@ -19,6 +19,7 @@ struct PcgScalars {
   double beta;
   double res;        // |r|_inf
   double tol;        // tolerance_factor * |rhs|_inf
+  double rhs_norm;   // |rhs|_inf
   int converged;     // res <= tol
   int bad_rho;       // rho == 0 or NaN
   int kernel_error;  // host copy of the smoother's timeout flag
@@ -61,6 +62,7 @@ __device__ __forceinline__ void finish_reduction(double* partials, int nblocks, 
       st->converged = (tot <= st->tol) ? 1 : 0;
     } else if (kind == kReduceRes0) {
       st->res = tot;
+      st->rhs_norm = tot;
       st->tol = tol_factor * tot;
       st->converged = (tot == 0.0) ? 1 : 0;
     } else if (kind == kReduceFlex) {  // z_new . r_old: Polak-Ribiere beta of flexible PCG
@@ -138,7 +140,7 @@ __global__ void __launch_bounds__(BLOCK) pcg_spmv_dot_kernel(const T* __restrict
       if (i < ni - 1) acc = acc + ldg(xp + g) * sv(g + 1);
       if (j < nj - 1) acc = acc + ldg(yp + g) * sv(g + sy);
       if (k < nk - 1) acc = acc + ldg(zp + g) * sv(g + szs);
-      s_new[g] = cvt<T>(sc);
+      if (s_new) s_new[g] = cvt<T>(sc);
       T qq = cvt<T>(acc);
       q[g] = qq;
       dot += (double)sc * (double)ldv(&qq);
@@ -253,7 +255,7 @@ __global__ void __launch_bounds__(1024) pcg_spmv_dot_plane_kernel(
         dot += (double)ldv(&sc.v[c]) * (double)ldv(&qo.v[c]);
       }
       *reinterpret_cast<Quad<T>*>(q + g) = qo;
-      *reinterpret_cast<Quad<T>*>(s_new + g) = sc;
+      if (s_new) *reinterpret_cast<Quad<T>*>(s_new + g) = sc;
       zprev = zq;
     } else if (interior && k == kb - 1 && k >= 0) {
       // the plane below the first q plane: only its zp is carried

@@ -83,11 +83,21 @@ struct vflip_ctx {
   int num_sms = 148;
   unsigned long long launches = 0;  // kernels launched through this context
   std::vector<vflip_ctx*> subs;     // per-system contexts of batched solves
+  // the device-resident PCG loop: its graph, kept while the buffers it names stay the same
+  cudaStream_t pg_stream = nullptr;
+  cudaGraph_t pg_graph = nullptr;
+  cudaGraphExec_t pg_exec = nullptr;
+  std::vector<uintptr_t> pg_key;
+  unsigned long long pg_init_launches = 0, pg_body_launches = 0, pg_tail_launches = 0;
   std::unordered_map<std::string, CUtensorMap> tmaps;  // encoded TMA tensor maps by (address, shape)
   // fine-level sweep timing (vflip_set_profiling)
   bool profiling = false;
   size_t prof_fine_n = 0;
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_events;
+  struct ProfEvent {
+    cudaEvent_t a, b;
+    int tag;
+  };
+  std::vector<ProfEvent> prof_events;
   size_t prof_used = 0;
 
   int fail(int code, const char* fmt, ...) {
@@ -126,6 +136,29 @@ struct vflip_ctx {
     cudaError_t e_ = (call);                                                                  \
     if (e_ != cudaSuccess) return ctx->fail(VFLIP_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
   } while (0)
+
+// Per-launch timing (vflip_set_profiling): events around the launches of
+// one kind, read back by vflip_profile_kernels.  Kinds: VFLIP_PROF_*.
+int prof_start(vflip_ctx* ctx, int tag, cudaStream_t stream) {
+  if (!ctx->profiling) return -1;
+  if (ctx->prof_used == ctx->prof_events.size()) {
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess) return -1;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+      cudaEventDestroy(e0);
+      return -1;
+    }
+    ctx->prof_events.push_back({e0, e1, tag});
+  }
+  vflip_ctx::ProfEvent& pe = ctx->prof_events[ctx->prof_used];
+  pe.tag = tag;
+  if (cudaEventRecord(pe.a, stream) != cudaSuccess) return -1;
+  return (int)ctx->prof_used++;
+}
+
+void prof_stop(vflip_ctx* ctx, int slot, cudaStream_t stream) {
+  if (slot >= 0) cudaEventRecord(ctx->prof_events[slot].b, stream);
+}
 
 #define VF_LAUNCH_CHECK()                                                                      \
   do {                                                                                        \
@@ -212,22 +245,11 @@ int launch_sweep_t(vflip_ctx* ctx, const SweepArgs<S, V>& a, const SweepShape& s
   if (smem_optin((const void*)kern, 200 * 1024) != cudaSuccess)
     return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the sweep's shared memory limit");
   dim3 grid(sh.grid_y, sh.grid_z);
-  const bool timed = ctx->profiling && (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n;
-  if (timed) {
-    if (ctx->prof_used == ctx->prof_events.size()) {
-      cudaEvent_t e0, e1;
-      VF_CUDA(cudaEventCreate(&e0));
-      VF_CUDA(cudaEventCreate(&e1));
-      ctx->prof_events.push_back({e0, e1});
-    }
-    VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].first, ctx->stream));
-  }
+  const int slot =
+      (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n ? prof_start(ctx, VFLIP_PROF_FINE_SWEEP, ctx->stream) : -1;
   kern<<<grid, kSweepBlock, sh.smem, ctx->stream>>>(a);
   VF_LAUNCH_CHECK();
-  if (timed) {
-    VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].second, ctx->stream));
-    ++ctx->prof_used;
-  }
+  prof_stop(ctx, slot, ctx->stream);
   return VFLIP_OK;
 }
 
@@ -328,22 +350,11 @@ int launch_tma_t(vflip_ctx* ctx, const TmaSweepArgs<S>& a, const TmaShape& sh) {
                                        : rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlock>);
   if (smem_optin((const void*)kern, (int)kTmaSmemMax) != cudaSuccess)
     return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the sweep's shared memory limit");
-  const bool timed = ctx->profiling && (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n;
-  if (timed) {
-    if (ctx->prof_used == ctx->prof_events.size()) {
-      cudaEvent_t e0, e1;
-      VF_CUDA(cudaEventCreate(&e0));
-      VF_CUDA(cudaEventCreate(&e1));
-      ctx->prof_events.push_back({e0, e1});
-    }
-    VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].first, ctx->stream));
-  }
+  const int slot =
+      (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n ? prof_start(ctx, VFLIP_PROF_FINE_SWEEP, ctx->stream) : -1;
   kern<<<dim3(sh.gy, sh.gz), dim3(sh.bx, sh.by), sh.smem, ctx->stream>>>(a);
   VF_LAUNCH_CHECK();
-  if (timed) {
-    VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].second, ctx->stream));
-    ++ctx->prof_used;
-  }
+  prof_stop(ctx, slot, ctx->stream);
   return VFLIP_OK;
 }
 
@@ -413,22 +424,11 @@ int launch_t3d_t(vflip_ctx* ctx, const T3dMaps<S>& mp, const T3dArgs& a, dim3 gr
   auto kern = rbgs_sweep_t3d_kernel<S, Z, P, D, kT3dTX, kT3dTY, kT3dBlock>;
   if (smem_optin((const void*)kern, (int)kTmaSmemMax) != cudaSuccess)
     return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the sweep's shared memory limit");
-  const bool timed = ctx->profiling && (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n;
-  if (timed) {
-    if (ctx->prof_used == ctx->prof_events.size()) {
-      cudaEvent_t e0, e1;
-      VF_CUDA(cudaEventCreate(&e0));
-      VF_CUDA(cudaEventCreate(&e1));
-      ctx->prof_events.push_back({e0, e1});
-    }
-    VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].first, ctx->stream));
-  }
+  const int slot =
+      (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n ? prof_start(ctx, VFLIP_PROF_FINE_SWEEP, ctx->stream) : -1;
   kern<<<grid, kT3dBlock, smem, ctx->stream>>>(mp, a);
   VF_LAUNCH_CHECK();
-  if (timed) {
-    VF_CUDA(cudaEventRecord(ctx->prof_events[ctx->prof_used].second, ctx->stream));
-    ++ctx->prof_used;
-  }
+  prof_stop(ctx, slot, ctx->stream);
   return VFLIP_OK;
 }
 
@@ -869,8 +869,10 @@ int launch_spmv_dot(vflip_ctx* ctx, cudaStream_t stream, bool first, const V* z,
     const int kz = (d.nk + kr - 1) / kr;
     kr = (d.nk + kz - 1) / kz;
     if ((size_t)rt * kr <= (size_t)kMaxPartials) {
+      const int slot = prof_start(ctx, VFLIP_PROF_SPMV, stream);
       kern<<<dim3(rt, kr), dim3(nq, rows), smem, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp, d.ni, d.nj, d.nk,
                                                            ty, kz, ctx->partials, ctx->st);
+      prof_stop(ctx, slot, stream);
       VF_LAUNCH_CHECK();
       return VFLIP_OK;
     }
@@ -879,19 +881,177 @@ int launch_spmv_dot(vflip_ctx* ctx, cudaStream_t stream, bool first, const V* z,
   const int kz = 8;
   dim3 sgrid((d.ni + 31) / 32, (d.nj + kRedBlock / 32 - 1) / (kRedBlock / 32), (d.nk + kz - 1) / kz);
   if ((size_t)sgrid.x * sgrid.y * sgrid.z > (size_t)kMaxPartials) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
+  const int slot = prof_start(ctx, VFLIP_PROF_SPMV, stream);
   if (first)
     pcg_spmv_dot_kernel<V, true, kRedBlock><<<sgrid, sblk, 0, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp, d.ni,
                                                                         d.nj, d.nk, kz, ctx->partials, ctx->st);
   else
     pcg_spmv_dot_kernel<V, false, kRedBlock><<<sgrid, sblk, 0, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp, d.ni,
                                                                          d.nj, d.nk, kz, ctx->partials, ctx->st);
+  prof_stop(ctx, slot, stream);
   VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
+// AMGPCGSolve's loop on the device (AlgebraicMultigrid.h:253-286): a CUDA
+// graph of [r = rhs, x = 0, |rhs|] -> while node {V-cycle with the fused z.r
+// (beta), s = z + beta s, q = A s with s.q (alpha), x/r update with |r|_inf,
+// stop test} -> x to FP64, captured once and relaunched while the buffers
+// and the hierarchy's layout stay the same; the host reads the scalars once.
+// The loop body rotates the host loop (the V-cycle first, s = 0 on entry),
+// so the iterates are the host loop's.  *done is false when the solve did
+// not converge (zero or NaN rho, max_iterations): the caller then repeats it
+// with the host loop, whose early exits set the result as the reference's.
+template <typename S0, typename SC, typename V>
+int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor,
+                    int maxit, vflip_solve_stats* stats, bool* done) {
+  *done = false;
+  const Dims d = T.fine.d;
+  const size_t n = d.n();
+  V *x, *r, *z, *s, *q;
+  int* itp;
+  VF_ALLOC(x, V, "pcg_x", n);
+  VF_ALLOC(r, V, "pcg_r", n);
+  VF_ALLOC(z, V, "pcg_z", n);
+  VF_ALLOC(s, V, "pcg_s0", n);
+  VF_ALLOC(q, V, "pcg_q", n);
+  VF_ALLOC(itp, int, "pcg_it", 1);
+  // everything the captured launches name
+  std::vector<uintptr_t> key;
+  auto kp = [&](const void* p) { key.push_back((uintptr_t)p); };
+  auto kl = [&](const auto& L) {
+    kp(L.diag); kp(L.xp); kp(L.yp); kp(L.zp); kp(L.b); kp(L.xa); kp(L.xb);
+    key.push_back((uintptr_t)L.d.ni); key.push_back((uintptr_t)L.d.nj); key.push_back((uintptr_t)L.d.nk);
+  };
+  kp(rhs); kp(result); kp(x); kp(r); kp(z); kp(s); kp(q); kp(itp); kp(ctx->st); kp(ctx->partials);
+  kl(T.fine);
+  for (const auto& L : T.coarse) kl(L);
+  kp(T.direct.L); kp(T.direct.rinv); kp(T.direct.ok);
+  key.push_back((uintptr_t)T.direct.on); key.push_back((uintptr_t)T.direct.bw); key.push_back((uintptr_t)maxit);
+  uint64_t tb;
+  std::memcpy(&tb, &tol_factor, sizeof tb);
+  key.push_back((uintptr_t)tb);
+  const int gb = grid_for(n, kRedBlock, ctx->num_sms);
+  if (key != ctx->pg_key || !ctx->pg_exec) {
+    if (ctx->pg_exec) cudaGraphExecDestroy(ctx->pg_exec);
+    if (ctx->pg_graph) cudaGraphDestroy(ctx->pg_graph);
+    ctx->pg_exec = nullptr;
+    ctx->pg_graph = nullptr;
+    ctx->pg_key.clear();
+    if (!ctx->pg_stream) VF_CUDA(cudaStreamCreateWithFlags(&ctx->pg_stream, cudaStreamNonBlocking));
+    const cudaStream_t cs = ctx->pg_stream;
+    cudaGraph_t graph = nullptr;
+    VF_CUDA(cudaGraphCreate(&graph, 0));
+    ctx->pg_graph = graph;
+    cudaGraphConditionalHandle hnd;
+    VF_CUDA(cudaGraphConditionalHandleCreate(&hnd, graph, 0, 0));
+    const cudaStream_t saved = ctx->stream;
+    const bool prof = ctx->profiling;
+    ctx->stream = cs;
+    ctx->profiling = false;
+    auto restore = [&](int code) {
+      ctx->stream = saved;
+      ctx->profiling = prof;
+      return code;
+    };
+    auto end_capture = [&](cudaGraph_t g) -> int {
+      cudaGraph_t out = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(cs, &out);
+      if (e != cudaSuccess || out != g)
+        return ctx->fail(VFLIP_ERR_CUDA, "PCG loop capture failed: %s", cudaGetErrorString(e));
+      return VFLIP_OK;
+    };
+    int rc;
+    const unsigned long long before_capture = ctx->launches;
+    if (cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+      return restore(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamBeginCaptureToGraph"));
+    cudaMemsetAsync(ctx->st, 0, sizeof(PcgScalars), cs);
+    cudaMemsetAsync(s, 0, n * sizeof(V), cs);
+    pcg_init_kernel<V, kRedBlock><<<gb, kRedBlock, 0, cs>>>(rhs, r, x, n, ctx->partials, ctx->st, tol_factor);
+    pcg_loop_init_kernel<<<1, 32, 0, cs>>>(ctx->st, itp, hnd);
+    cudaStreamCaptureStatus cst;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    if (cudaStreamGetCaptureInfo(cs, &cst, nullptr, nullptr, &deps, &ndeps) != cudaSuccess) {
+      end_capture(graph);
+      return restore(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamGetCaptureInfo"));
+    }
+    std::vector<cudaGraphNode_t> dv(deps, deps + ndeps);
+    if ((rc = end_capture(graph))) return restore(rc);
+    ctx->pg_init_launches = 2;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hnd;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wn;
+    if (cudaGraphAddNode(&wn, graph, dv.data(), dv.size(), &cp) != cudaSuccess)
+      return restore(ctx->fail(VFLIP_ERR_CUDA, "cannot add the while node"));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+      return restore(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamBeginCaptureToGraph (body)"));
+    const unsigned long long l0 = ctx->launches;
+    int brc = vcycle<S0, SC, V>(ctx, T, r, z, true);
+    if (!brc) {
+      pcg_direction_kernel<V><<<grid_for(n, 256, ctx->num_sms), 256, 0, cs>>>(z, s, n, ctx->st);
+      ++ctx->launches;
+      brc = launch_spmv_dot<V>(ctx, cs, true, s, nullptr, nullptr, q, T.fine.diag, T.fine.xp, T.fine.yp, T.fine.zp,
+                               d);
+    }
+    if (!brc) {
+      pcg_update_kernel<V, kRedBlock><<<gb, kRedBlock, 0, cs>>>(x, r, s, q, n, ctx->partials, ctx->st);
+      pcg_loop_cond_kernel<<<1, 32, 0, cs>>>(ctx->st, itp, maxit, hnd);
+      ctx->launches += 2;
+    }
+    if ((rc = end_capture(body))) return restore(rc);
+    if (brc) return restore(brc);
+    ctx->pg_body_launches = ctx->launches - l0;
+    if (cudaStreamBeginCaptureToGraph(cs, graph, &wn, nullptr, 1, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+      return restore(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamBeginCaptureToGraph (result)"));
+    to_double_kernel<V, kRedBlock><<<gb, kRedBlock, 0, cs>>>(x, result, n);
+    if ((rc = end_capture(graph))) return restore(rc);
+    ctx->pg_tail_launches = 1;
+    restore(VFLIP_OK);
+    ctx->launches = before_capture;  // captured launches count when the graph runs
+    if (cudaGraphInstantiate(&ctx->pg_exec, graph, 0) != cudaSuccess) {
+      ctx->pg_exec = nullptr;
+      return ctx->fail(VFLIP_ERR_CUDA, "cudaGraphInstantiate failed (PCG loop)");
+    }
+    ctx->pg_key = key;
+  }
+  if (cudaGraphLaunch(ctx->pg_exec, ctx->stream) != cudaSuccess)
+    return ctx->fail(VFLIP_ERR_CUDA, "cudaGraphLaunch (PCG loop)");
+  int iters = 0;
+  VF_CUDA(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(PcgScalars), cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(&ctx->st_host->kernel_error, ctx->d_error, sizeof(int), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(&iters, itp, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  int rc;
+  if ((rc = check_kernel_error(ctx, ctx->st_host->kernel_error))) return rc;
+  const PcgScalars& h = *ctx->st_host;
+  ctx->launches += ctx->pg_init_launches + (unsigned long long)iters * ctx->pg_body_launches + ctx->pg_tail_launches;
+  if (!h.converged || h.bad_rho) return VFLIP_OK;  // the host loop repeats the solve
+  if (stats) {
+    stats->iterations = iters;
+    stats->vcycles = iters;
+    stats->levels = (int)T.coarse.size() + 1;
+    stats->converged = 1;
+    stats->residual = h.res;
+    stats->rhs_norm = h.rhs_norm;
+  }
+  *done = true;
   return VFLIP_OK;
 }
 
 template <typename S0, typename SC, typename V>
 int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor, int maxit,
               vflip_solve_stats* stats, V* x1_out = nullptr) {
+  if (ctx->cfg.pcg_loop == 0 && !ctx->profiling && !x1_out) {
+    bool done = false;
+    const int grc = pcg_solve_graph(ctx, T, rhs, result, tol_factor, maxit, stats, &done);
+    if (grc < 0 || done) return grc;
+  }
   const Dims d = T.fine.d;
   const size_t n = d.n();
   V *x, *r, *z, *s0, *s1, *q;
@@ -945,7 +1105,9 @@ int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* re
     if ((rc = launch_spmv_dot<V>(ctx, ctx->stream, it == 0, z, s_old, s_new, q, T.fine.diag, T.fine.xp, T.fine.yp,
                                  T.fine.zp, d)))
       return rc;
+    const int uslot = prof_start(ctx, VFLIP_PROF_UPDATE, ctx->stream);
     pcg_update_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(x, r, s_new, q, n, ctx->partials, ctx->st);
+    prof_stop(ctx, uslot, ctx->stream);
     VF_LAUNCH_CHECK();
     if (it == 0 && x1_out) VF_CUDA(cudaMemcpyAsync(x1_out, x, n * sizeof(V), cudaMemcpyDeviceToDevice, ctx->stream));
     if ((rc = read_scalars(ctx))) return rc;
@@ -1578,6 +1740,8 @@ void vflip_config_default(vflip_config* cfg) {
   cfg->smoother_prefetch = 0;
   cfg->coarsest_solver = 0;
   cfg->spmv_kernel = 0;
+  cfg->advect_kernel = 0;
+  cfg->pcg_loop = 0;
 }
 
 int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
@@ -1609,7 +1773,8 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
       (ctx->cfg.smoother_threads != 0 && ctx->cfg.smoother_threads != kTmaBlock &&
        ctx->cfg.smoother_threads != kTmaBlockWide) ||
       ctx->cfg.coarsest_solver < 0 || ctx->cfg.coarsest_solver > 2 || ctx->cfg.spmv_kernel < 0 ||
-      ctx->cfg.spmv_kernel > 1)
+      ctx->cfg.spmv_kernel > 1 || ctx->cfg.advect_kernel < 0 || ctx->cfg.advect_kernel > 1 ||
+      ctx->cfg.pcg_loop < 0 || ctx->cfg.pcg_loop > 1)
     return bad(VFLIP_ERR_ARG);
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);
@@ -1631,14 +1796,17 @@ int vflip_destroy(vflip_ctx* ctx) {
   if (!ctx) return VFLIP_ERR_ARG;
   cudaStreamSynchronize(ctx->stream);
   for (vflip_ctx* sub : ctx->subs) vflip_destroy(sub);
+  if (ctx->pg_exec) cudaGraphExecDestroy(ctx->pg_exec);
+  if (ctx->pg_graph) cudaGraphDestroy(ctx->pg_graph);
+  if (ctx->pg_stream) cudaStreamDestroy(ctx->pg_stream);
   for (auto& kv : ctx->bufs) cudaFree(kv.second.first);
   if (ctx->st) cudaFree(ctx->st);
   if (ctx->partials) cudaFree(ctx->partials);
   if (ctx->d_error) cudaFree(ctx->d_error);
   if (ctx->st_host) cudaFreeHost(ctx->st_host);
   for (auto& pe : ctx->prof_events) {
-    cudaEventDestroy(pe.first);
-    cudaEventDestroy(pe.second);
+    cudaEventDestroy(pe.a);
+    cudaEventDestroy(pe.b);
   }
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
@@ -2054,6 +2222,27 @@ int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, fl
   GridView gf{field, fnx, fny, fnz, (double)h, ox, oy, oz, ih};
   GridView gf2{field2, fnx, fny, fnz, (double)h, ox, oy, oz, ih};
   size_t n = (size_t)fnx * fny * fnz;
+  if (ctx->cfg.advect_kernel == 0) {
+    // the field is one of the velocity grids (self-advection): its window is shared
+    auto same = [&](const GridView& g) {
+      return g.d == field && g.nx == fnx && g.ny == fny && g.nz == fnz && g.ox == ox && g.oy == oy && g.oz == oz;
+    };
+    int fsrc = !field2 && same(gu) ? 0 : (!field2 && same(gv) ? 1 : (!field2 && same(gw) ? 2 : 3));
+    const int windows = fsrc < 3 ? 3 : (field2 ? 5 : 4);
+    const size_t smem = (size_t)windows * kAdvWin * sizeof(float);
+    auto kern = ctx->cfg.precision == VFLIP_PREC_FP64 ? advect_rk2_tile_kernel<true> : advect_rk2_tile_kernel<false>;
+    if (smem_optin((const void*)kern, (int)smem) != cudaSuccess)
+      return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the advection kernel's shared memory limit");
+    // a face grid's last node along x rides with the previous tile
+    const int tiles_x = std::max(1, (fnx - 1 + kAdvTX - 1) / kAdvTX);
+    dim3 grid(tiles_x, (fny + kAdvTY - 1) / kAdvTY, (fnz + kAdvTZ - 1) / kAdvTZ);
+    const int slot = prof_start(ctx, VFLIP_PROF_ADVECT_FIELD, ctx->stream);
+    kern<<<grid, dim3(kAdvTX, kAdvTY), smem, ctx->stream>>>(gu, gv, gw, gf, out, gf2, field2 ? out2 : nullptr, h, dt,
+                                                            fsrc);
+    prof_stop(ctx, slot, ctx->stream);
+    VF_LAUNCH_CHECK();
+    return VFLIP_OK;
+  }
   const int per_block = 256 * 8;
   const unsigned blocks = (unsigned)((n + per_block - 1) / per_block);
   if (ctx->cfg.precision == VFLIP_PREC_FP64)
@@ -2071,6 +2260,37 @@ int vflip_advect_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, flo
                             double oz, const float* field, float* out) {
   return vflip_advect_rk2_linear2(ctx, ni, nj, nk, h, dt, u, v, w, fnx, fny, fnz, ox, oy, oz, field, out, nullptr,
                                   nullptr);
+}
+
+int vflip_advect_velocity_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
+                                     const float* v, const float* w, float* uo, float* vo, float* wo) {
+  int rc;
+  if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
+  if (!u || !v || !w || !uo || !vo || !wo) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
+  for (const float* o : {(const float*)uo, (const float*)vo, (const float*)wo})
+    if (o == u || o == v || o == w) return ctx->fail(VFLIP_ERR_ARG, "an output aliases the velocity");
+  if (uo == vo || uo == wo || vo == wo) return ctx->fail(VFLIP_ERR_ARG, "outputs alias each other");
+  if (ctx->cfg.advect_kernel != 0) {
+    if ((rc = vflip_advect_rk2_linear(ctx, ni, nj, nk, h, dt, u, v, w, ni + 1, nj, nk, 0.5, 0.0, 0.0, u, uo)) ||
+        (rc = vflip_advect_rk2_linear(ctx, ni, nj, nk, h, dt, u, v, w, ni, nj + 1, nk, 0.0, 0.5, 0.0, v, vo)) ||
+        (rc = vflip_advect_rk2_linear(ctx, ni, nj, nk, h, dt, u, v, w, ni, nj, nk + 1, 0.0, 0.0, 0.5, w, wo)))
+      return rc;
+    return VFLIP_OK;
+  }
+  const double ih = inv_pow2(h);
+  GridView gu{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0, ih};
+  GridView gv{v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0, ih};
+  GridView gw{w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5, ih};
+  const size_t smem = 3 * (size_t)kAdvWin * sizeof(float);
+  auto kern = ctx->cfg.precision == VFLIP_PREC_FP64 ? advect_vel3_tile_kernel<true> : advect_vel3_tile_kernel<false>;
+  if (smem_optin((const void*)kern, (int)smem) != cudaSuccess)
+    return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the advection kernel's shared memory limit");
+  dim3 grid((ni + kAdvTX - 1) / kAdvTX, (nj + kAdvTY - 1) / kAdvTY, (nk + kAdvTZ - 1) / kAdvTZ);
+  const int slot = prof_start(ctx, VFLIP_PROF_ADVECT_VELOCITY, ctx->stream);
+  kern<<<grid, dim3(kAdvTX, kAdvTY), smem, ctx->stream>>>(gu, gv, gw, uo, vo, wo, h, dt, ni, nj, nk);
+  prof_stop(ctx, slot, ctx->stream);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
 }
 
 namespace {
@@ -2745,17 +2965,27 @@ int vflip_set_profiling(vflip_ctx* ctx, int enable) {
 
 int vflip_profile_sweeps(vflip_ctx* ctx, int* launches, double* total_ms, double* cells) {
   if (!ctx) return VFLIP_ERR_ARG;
+  const double fine = (double)ctx->prof_fine_n;
+  int rc = vflip_profile_kernels(ctx, VFLIP_PROF_FINE_SWEEP, launches, total_ms);
+  if (cells) *cells = fine;
+  if (rc == VFLIP_OK) ctx->prof_used = 0;
+  return rc;
+}
+
+int vflip_profile_kernels(vflip_ctx* ctx, int kind, int* launches, double* total_ms) {
+  if (!ctx) return VFLIP_ERR_ARG;
   VF_CUDA(cudaStreamSynchronize(ctx->stream));
   double tot = 0.0;
+  int cnt = 0;
   for (size_t q = 0; q < ctx->prof_used; ++q) {
+    if (ctx->prof_events[q].tag != kind) continue;
     float ms = 0.0f;
-    VF_CUDA(cudaEventElapsedTime(&ms, ctx->prof_events[q].first, ctx->prof_events[q].second));
+    VF_CUDA(cudaEventElapsedTime(&ms, ctx->prof_events[q].a, ctx->prof_events[q].b));
     tot += ms;
+    ++cnt;
   }
-  if (launches) *launches = (int)ctx->prof_used;
+  if (launches) *launches = cnt;
   if (total_ms) *total_ms = tot;
-  if (cells) *cells = (double)ctx->prof_fine_n;
-  ctx->prof_used = 0;
   return VFLIP_OK;
 }
 

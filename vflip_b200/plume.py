@@ -1,9 +1,9 @@
 """Grid smoke-plume stepper built from the library's kernels.
 
 One step (the unit of the benchmark) is one smoke step:
-  1. RK2 semi-Lagrangian trilinear advection of u, v, w, density and
-     temperature through the current velocity
-     (SubDomainSolver::advect_field, sub_domain.cpp:191-235);
+  1. RK2 semi-Lagrangian trilinear advection of u, v, w (one launch) and of
+     density and temperature (one launch, one shared backtrace) through the
+     current velocity (SubDomainSolver::advect_field, sub_domain.cpp:191-235);
   2. density/temperature source sphere and buoyancy on the v faces (grid
      analogue of gen_heat / add_smokeforce, Smoke_solver3D.cpp:1624-1668);
   3. pressure projection with MGPCG to the tolerance
@@ -78,9 +78,7 @@ class PlumeSim:
         `before_scalars` runs between the velocity and the scalar advection."""
         p, s, n, h = self.p, self.s, self.p.n, self.p.h
         u, v, w = self.f["u"], self.f["v"], self.f["w"]
-        offs = {"u": (0.5, 0, 0), "v": (0, 0.5, 0), "w": (0, 0, 0.5)}
-        for k in ("u", "v", "w"):
-            s.advect_rk2_linear(n, n, n, h, p.dt, u, v, w, self.f[k], offs[k], out=self.g[k])
+        s.advect_velocity_rk2_linear(n, n, n, h, p.dt, u, v, w, outs=(self.g["u"], self.g["v"], self.g["w"]))
         if before_scalars is not None:
             before_scalars()
         # density and temperature share the cell-centred backtrace

@@ -68,7 +68,7 @@ class Solver:
     def __init__(self, precision=1, pre_sweeps=4, post_sweeps=4, coarse_sweeps=0, coarsest_max_unknowns=0,
                  device=0, stream=None, sweep_kernel=0, smoother_depth=0, smoother_tile_rows=0,
                  smoother_plane_ranges=0, smoother_ctas_per_sm=0, smoother_threads=0,
-                 smoother_prefetch=0, coarsest_solver=0, spmv_kernel=0):
+                 smoother_prefetch=0, coarsest_solver=0, spmv_kernel=0, advect_kernel=0, pcg_loop=0):
         self.lib = load()
         cfg = ConfigC()
         self.lib.vflip_config_default(C.byref(cfg))
@@ -87,6 +87,8 @@ class Solver:
         cfg.smoother_prefetch = smoother_prefetch
         cfg.coarsest_solver = coarsest_solver
         cfg.spmv_kernel = spmv_kernel
+        cfg.advect_kernel = advect_kernel
+        cfg.pcg_loop = pcg_loop
         self.device = torch.device("cuda", device)
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
@@ -297,6 +299,13 @@ class Solver:
                                                       fnx, fny, fnz, float(offsets[0]), float(offsets[1]),
                                                       float(offsets[2]), _p(field), _p(out), _p(field2), _p(out2)))
         return out, out2
+
+    def advect_velocity_rk2_linear(self, ni, nj, nk, h, dt, u, v, w, outs=None):
+        """SubDomainSolver::advect_field of u, v and w through themselves, one launch."""
+        outs = tuple(torch.empty_like(a) for a in (u, v, w)) if outs is None else outs
+        self._check(self.lib.vflip_advect_velocity_rk2_linear(self.ctx, ni, nj, nk, float(h), float(dt), _p(u), _p(v),
+                                                              _p(w), *[_p(o) for o in outs]))
+        return outs
 
     def advect_cubic_clamp(self, ni, nj, nk, h, dt, u, v, w, field, offsets, out=None):
         """SmokeSolver3D::advect_field_cubic_clamp of one field."""
@@ -538,6 +547,15 @@ class Solver:
         cells = C.c_double(0.0)
         self._check(self.lib.vflip_profile_sweeps(self.ctx, C.byref(n), C.byref(ms), C.byref(cells)))
         return n.value, ms.value, cells.value
+
+    PROF_KINDS = {"fine_sweep": 0, "spmv": 1, "update": 2, "advect_velocity": 3, "advect_field": 4}
+
+    def profile_kernels(self, kind):
+        """(launches, total_ms) of the timed launches of one kind (PROF_KINDS)."""
+        n = C.c_int(0)
+        ms = C.c_double(0.0)
+        self._check(self.lib.vflip_profile_kernels(self.ctx, self.PROF_KINDS[kind], C.byref(n), C.byref(ms)))
+        return n.value, ms.value
 
     @property
     def launch_count(self):
