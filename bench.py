@@ -56,6 +56,12 @@ def parse():
     ap.add_argument("--learned-capture", type=int, default=40)
     ap.add_argument("--learned-epochs", type=int, default=16)
     ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds for the reference arm's timed steps")
+    ap.add_argument("--kernels", default=None,
+                    help="instead of the step: per-kernel timings (comma list of advect, p2g, g2p, unet) at --n, "
+                         "one JSON line each")
+    ap.add_argument("--reps", type=int, default=5, help="timed repetitions per kernel (--kernels)")
+    ap.add_argument("--unet-sizes", type=int, nargs="+", default=[32, 64, 128], help="network grids (--kernels unet)")
+    ap.add_argument("--no-train", action="store_true", help="--kernels unet: forward only")
     return ap.parse_args()
 
 
@@ -516,31 +522,42 @@ def advection_arm(solver, n=128, reps=20):
 def batched_arm(solver, count=32, reps=2):
     """32 independent systems, sides uniform from {32..192}, random solid
     spheres, rhs = divergence of a smoothed Gaussian velocity (seeded), to
-    1e-6: the whole batch as one CUDA graph (device-side PCG loops, systems
-    as parallel branches) vs one system after another; both timed from the
-    first hierarchy build to the last result (CUDA events, best of `reps`)."""
+    1e-6, three ways: the whole batch as ONE persistent cooperative kernel
+    (its work items autotuned on this batch first, untimed, and cached), as
+    one CUDA graph of per-system device-side PCG loops, and one system after
+    another; each timed from the first hierarchy build to the last result
+    (CUDA events, best of `reps` after one untimed call)."""
     import numpy as np
 
-    from vflip_b200 import scenes
+    from vflip_b200 import scenes, tune
+    from vflip_b200.solver import Solver
 
     systems, sides = scenes.batch_workload(solver, count=count, seed=0)
+    best_cfg, table = tune.tune_batch(systems, sides, precision=solver.precision)
     res = {}
-    for name, mode in (("graph", 0), ("loop", 1)):
-        best, stats, launch = None, None, None
+    pkw = {"batch_chunk": best_cfg["chunk"], "batch_ctas_per_sm": best_cfg["ctas_per_sm"]} if best_cfg else {}
+    for name, mode, kw in (("persistent", 2, pkw), ("graph", 0, None), ("loop", 1, None)):
+        s = Solver(precision=solver.precision, **kw) if kw is not None else solver
+        best, stats, launch, ok = None, None, None, False
         for _ in range(reps + 1):  # the first call also creates the per-system contexts
-            ok, _, st = solver.batched_solve(systems, 1e-6, 100, mode=mode)
+            ok, _, st = s.batched_solve(systems, 1e-6, 100, mode=mode)
             ms = st[0].solve_ms
             if best is None or ms < best:
-                best, launch = ms, solver.last_ms
+                best, launch = ms, s.last_ms
             stats = st
+        if s is not solver:
+            s.close()
         res[name] = (best, ok, stats, launch)
-    cells = sum(s ** 3 for s in sides)
-    g, l = res["graph"], res["loop"]
-    return {"systems": count, "sides": sides, "cells": cells, "graph_ms": g[0], "loop_ms": l[0],
-            "graph_launch_ms": g[3], "speedup_graph_over_loop": l[0] / g[0], "all_converged": bool(g[1] and l[1]),
+    cells = sum(x ** 3 for x in sides)
+    p, g, l = res["persistent"], res["graph"], res["loop"]
+    return {"systems": count, "sides": sides, "cells": cells, "persistent_ms": p[0], "persistent_kernel_ms": p[3],
+            "graph_ms": g[0], "loop_ms": l[0], "graph_launch_ms": g[3],
+            "speedup_persistent_over_graph": g[0] / p[0], "speedup_persistent_over_loop": l[0] / p[0],
+            "speedup_graph_over_loop": l[0] / g[0], "all_converged": bool(p[1] and g[1] and l[1]),
             "iterations_mean": float(np.mean([x.iterations for x in g[2]])),
-            "iterations_equal": all(x.iterations == y.iterations for x, y in zip(g[2], l[2])),
-            "cells_per_s_graph": cells / (g[0] * 1e-3)}
+            "persistent_iterations_mean": float(np.mean([x.iterations for x in p[2]])),
+            "iterations_equal_graph_loop": all(x.iterations == y.iterations for x, y in zip(g[2], l[2])),
+            "cells_per_s_persistent": cells / (p[0] * 1e-3), "tuned": best_cfg, "tuning": table}
 
 
 # the reference's own hierarchy (16^3 coarsest level, 200 red-black sweeps):
@@ -715,9 +732,157 @@ def run_reference(a):
             "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def kernel_lines(a):
+    """Per-kernel timings on seeded synthetic inputs (CUDA events on the
+    library's stream after a warm-up call, L2 flushed between repetitions),
+    each with its algorithmic bytes (or FLOPs) and the fraction of the
+    measured peak:
+      advect  the one-launch u, v, w advection (24 B/cell: u, v, w read once,
+              written once) and the density/temperature pair (28 B/cell:
+              u, v, w + both fields read, both written), n^3 cells, a smooth
+              velocity field of peak |u| 0.4 (about 1 cell per step at dt 0.01);
+      p2g     sort-by-cell P2G of 8 jittered particles per cell, all three
+              components, sort included (24 B/particle + 24 B/cell);
+      g2p     the FLIP update of the same particles (24 B/particle + 12 B/cell);
+      unet    the U-Net forward (and a training step) on S^3 network grids
+              (2 x 27 x c_in x c_out FLOP per voxel and layer)."""
+    import numpy as np
+    import torch
+
+    from vflip_b200 import scenes
+    from vflip_b200.solver import Solver
+
+    n, dev = a.n, "cuda:0"
+    peak, peak_kind = measured_peaks()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for r in range(a.reps):
+            flush.fill_(r & 0xFF)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / a.reps
+
+    def line(kernel, ms, alg, **kw):
+        gbs = alg / (ms * 1e-3) / 1e9
+        print(json.dumps({"kernel": kernel, "n": n, "ms": ms, "alg_bytes": alg, "achieved_gbs": gbs,
+                          "hbm_frac": gbs / peak, "peak_gbs": peak, "peak_kind": peak_kind, **kw}), flush=True)
+
+    what = a.kernels.split(",")
+    h = np.float32(1.0 / n)
+    rng = np.random.default_rng(0)
+    T = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
+    with Solver(precision=PREC[a.precision]) as s:
+        if "advect" in what:
+            vel = []
+            for q, sh in enumerate(scenes.face_shapes(n, n, n)):
+                k, j, i = np.meshgrid(*(np.arange(x, dtype=np.float32) for x in sh), indexing="ij")
+                vel.append((0.4 * np.sin(0.05 * i + q) * np.cos(0.07 * j - q) * np.sin(0.03 * k + 2 * q)).astype(
+                    np.float32))
+            u, v, w = (T(x) for x in vel)
+            outs = tuple(torch.empty_like(x) for x in (u, v, w))
+            ms = timed(lambda: s.advect_velocity_rk2_linear(n, n, n, h, 0.01, u, v, w, outs=outs))
+            line("advect_rk2_kernel x3 (u, v, w)", ms, 24 * n ** 3)
+            rho = T(rng.standard_normal((n, n, n)).astype(np.float32))
+            tmp = T(rng.standard_normal((n, n, n)).astype(np.float32))
+            o1, o2 = torch.empty_like(rho), torch.empty_like(tmp)
+            ms = timed(lambda: s.advect_rk2_linear2(n, n, n, h, 0.01, u, v, w, rho, tmp, (0, 0, 0), out=o1, out2=o2))
+            line("advect_rk2_kernel (density + temperature pair)", ms, 28 * n ** 3)
+        if "p2g" in what or "g2p" in what:
+            part = scenes.jittered_particles(n, n, n, h, 8, rng)
+            part["vel"] = rng.standard_normal((len(part), 3)).astype(np.float32)
+            rng.shuffle(part)
+            parts = T(part.view(np.uint8))
+            npart = len(part)
+            if "p2g" in what:
+                ms = timed(lambda: s.particle_to_grid(n, n, n, h, parts))
+                line("p2g (hash, sort, p2g3_kernel)", ms, npart * 24 + 24 * n ** 3, particles=npart)
+            if "g2p" in what:
+                du, dv, dw = (T(x) for x in scenes.random_velocity(n, n, n, rng, scale=0.1))
+                ms = timed(lambda: s.particle_from_grid(n, n, n, h, parts, du, dv, dw))
+                line("g2p_kernel", ms, npart * 24 + 12 * n ** 3, particles=npart)
+    if "unet" in what:
+        unet_lines(a)
+
+
+UNET_LEVEL = {"E0A": 0, "E0B": 0, "E1A": 1, "E1B": 1, "E2A": 2, "E2B": 2, "B1": 3, "B2": 3, "D2A": 2, "D2B": 2,
+              "D1A": 1, "D1B": 1, "D0A": 0, "D0B": 0, "OUT": 0}
+UNET_LAYERS = [("E0A", 16, 16), ("E0B", 16, 16), ("E1A", 16, 32), ("E1B", 32, 32), ("E2A", 32, 64), ("E2B", 64, 64),
+               ("B1", 64, 128), ("B2", 128, 128), ("D2A", 192, 64), ("D2B", 64, 64), ("D1A", 96, 32), ("D1B", 32, 32),
+               ("D0A", 48, 16), ("D0B", 16, 16), ("OUT", 16, 16)]
+
+
+def unet_forward_flops(S):
+    """2 x 27 x c_in x c_out per voxel and layer (OUT counted at its 16 computed channels)."""
+    return sum(2 * 27 * ci * co * (S >> UNET_LEVEL[nm]) ** 3 for nm, ci, co in UNET_LAYERS)
+
+
+def measured_tflops():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+def unet_lines(a):
+    """U-Net forward (and training step) time on S^3 grids: 3 untimed
+    forwards, then `reps` timed ones; also the program the convolution
+    kernels' ncu profiles capture."""
+    import torch
+
+    from vflip_b200.learned import UNet
+
+    peak = measured_tflops()
+    net = UNet(seed=0)
+    ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))  # noqa: E731
+    for S in a.unet_sizes:
+        g = torch.Generator(device="cuda").manual_seed(S)
+        in2 = torch.randn((S, S, S, 2), device="cuda", generator=g)
+        for _ in range(3):
+            net.forward(in2)
+        torch.cuda.synchronize()
+        e0, e1 = ev()
+        e0.record()
+        for _ in range(a.reps):
+            net.forward(in2)
+        e1.record()
+        torch.cuda.synchronize()
+        fwd = e0.elapsed_time(e1) / a.reps
+        tf = unet_forward_flops(S) / (fwd * 1e-3) / 1e12
+        out = {"kernel": "unet forward (conv3_tc_kernel + pooling/upsampling)", "grid": S, "ms": fwd,
+               "flops": unet_forward_flops(S), "achieved_tflops": tf, "tensor_frac": tf / peak[0],
+               "peak_tflops": peak[0], "peak_kind": peak[1]}
+        if not a.no_train:
+            t2 = torch.randn((S, S, S, 2), device="cuda", generator=g)
+            w = torch.ones((S, S, S), device="cuda")
+            for _ in range(2):
+                net.train_step(in2, t2, w, 1e-5, want_loss=False)
+            torch.cuda.synchronize()
+            e0.record()
+            for _ in range(a.reps):
+                net.train_step(in2, t2, w, 1e-5, want_loss=False)
+            e1.record()
+            torch.cuda.synchronize()
+            out["train_step_ms"] = e0.elapsed_time(e1) / a.reps
+        print(json.dumps(out), flush=True)
+    net.close()
+
+
 def main():
     a = parse()
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    if a.kernels:
+        kernel_lines(a)
+        return
     out = run_reference(a) if a.impl == "reference" else run_vflip(a)
     if out is not None:
         print(json.dumps(out))

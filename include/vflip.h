@@ -103,12 +103,6 @@ typedef struct {
    * 1 = always the column kernel.  Both give the same q and s bit for bit;
    * their s.q partial sums are grouped differently. */
   int spmv_kernel;
-  /* RK2 advection kernel (vflip_advect_rk2_linear, _linear2): 0 (default) =
-   * automatic: the tiled kernel (velocity grids, and a field that is not one
-   * of them, staged in shared memory around each block's 32 x 8 x 8 nodes;
-   * samples beyond the staged halo read global memory); 1 = the per-node
-   * gather kernel.  Both give the same bits. */
-  int advect_kernel;
   /* PCG loop: 0 (default) = automatic: the loop runs on the device, a CUDA
    * graph (captured once per hierarchy layout and reused) whose conditional
    * while node repeats V-cycle, direction, SpMV and update until the
@@ -118,6 +112,19 @@ typedef struct {
    * converge on the device is repeated by the host loop, so the failure
    * results (zero-rho exit, max_iterations) are the host loop's. */
   int pcg_loop;
+  /* PCG vectors of FP32/MIXED contexts: 0 (default) = FP64: x, r, the
+   * search direction and A s in FP64 and the SpMV on the FP64 operator as
+   * assembled, around the FP32 (or BF16-coarse) V-cycle, which reads r
+   * rounded to FP32; the |r|_inf <= tol |rhs|_inf test then holds for the
+   * FP64 system.  1 = the working precision (vectors and SpMV in FP32: the
+   * solve converges on the FP32-rounded system, whose FP64 residual stalls
+   * near 2e-5 |rhs|_inf on the 256^3 plume operator). */
+  int pcg_vectors;
+  /* VFLIP_BATCH_PERSISTENT work items: cells per (system, level, chunk)
+   * item (0 = automatic, 4096) and resident CTAs per SM of the persistent
+   * kernel (0 = as many as fit).  vflip_b200/tune.py picks both per batch. */
+  int batch_chunk;
+  int batch_ctas_per_sm;
 } vflip_config;
 
 typedef struct {
@@ -264,9 +271,9 @@ int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, fl
                              double oz, const float* field, float* out, const float* field2, float* out2);
 
 /* The velocity's self-advection of SubDomainSolver::advect_field
- * (SS/sub_domain.cpp:191-235) for u, v and w in one launch: uo, vo, wo (the
+ * (SS/sub_domain.cpp:191-235) for u, v and w in one call: uo, vo, wo (the
  * face grids, which must not alias u/v/w) receive what three
- * vflip_advect_rk2_linear calls give, bit for bit. */
+ * vflip_advect_rk2_linear calls give (it makes those three launches). */
 int vflip_advect_velocity_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
                                      const float* v, const float* w, float* uo, float* vo, float* wo);
 
@@ -511,7 +518,7 @@ int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const vo
  * CUDA events on its stream (the PCG loop then runs on the host, whose
  * launches can carry events): the fine-level smoothing sweep (the dominant
  * kernel), the fine-level PCG SpMV and update, and the RK2 advection
- * launches.  vflip_profile_kernels synchronises the stream and returns the
+ * launches (one field; a pair of fields on one backtrace).  vflip_profile_kernels synchronises the stream and returns the
  * number of timed launches of one kind and their summed device time;
  * vflip_profile_sweeps returns the fine sweeps' figures and the fine level's
  * cell count, then starts a new count for every kind.  Enabling (again)
@@ -519,8 +526,8 @@ int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const vo
 #define VFLIP_PROF_FINE_SWEEP 0
 #define VFLIP_PROF_SPMV 1
 #define VFLIP_PROF_UPDATE 2
-#define VFLIP_PROF_ADVECT_VELOCITY 3
-#define VFLIP_PROF_ADVECT_FIELD 4
+#define VFLIP_PROF_ADVECT_FIELD 3
+#define VFLIP_PROF_ADVECT_PAIR 4
 int vflip_set_profiling(vflip_ctx* ctx, int enable);
 int vflip_profile_sweeps(vflip_ctx* ctx, int* launches, double* total_ms, double* cells);
 int vflip_profile_kernels(vflip_ctx* ctx, int kind, int* launches, double* total_ms);
@@ -656,6 +663,8 @@ typedef struct vflip_system {
 
 #define VFLIP_BATCH_GRAPH 0 /* one CUDA graph: each system's PCG loop a device-side while node, systems in parallel */
 #define VFLIP_BATCH_LOOP 1  /* one system after another (vflip_amgpcg_solve per system) */
+#define VFLIP_BATCH_PERSISTENT 2 /* one persistent cooperative kernel over a (system, level, chunk) work list, in a
+                                    CUDA graph (FP32/MIXED contexts; FP64 runs VFLIP_BATCH_GRAPH) */
 
 /* Solves many independent systems of uneven sizes with the context's MGPCG
  * (same hierarchy, smoother, tolerance test and precision as
@@ -663,7 +672,15 @@ typedef struct vflip_system {
  * then captures the batch into one CUDA graph and launches it once: per
  * system a parallel branch whose PCG iterations run in a conditional while
  * node whose condition a kernel sets from the device-side scalars, so no
- * iteration returns to the host.  Returns 0 when every system converged, 1
+ * iteration returns to the host.  VFLIP_BATCH_PERSISTENT builds the
+ * hierarchies the same way, then runs every system's PCG loop in ONE launch
+ * of a persistent cooperative kernel (captured in a graph): each phase of
+ * the V-cycle and of the PCG step is a work list of (system, chunk) items
+ * taken by all resident CTAs, grid barriers between dependent phases, the
+ * coarsest levels one CTA per system; systems leave the loop as they
+ * converge.  Same stopping test and per-cell arithmetic; its reductions are
+ * grouped per item, so its iterates agree with graph mode's to rounding.
+ * Returns 0 when every system converged, 1
  * otherwise; stats[i] per system (solve_ms = the whole call, set-up
  * included; vflip_last_ms = the graph launch alone in graph mode).  No reference
  * counterpart (the reference solves one system per AMGPCGSolve call,

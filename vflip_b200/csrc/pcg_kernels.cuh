@@ -108,8 +108,10 @@ __global__ void __launch_bounds__(BLOCK) pcg_init_kernel(const double* __restric
 // partial s_new.q                        (AlgebraicMultigrid.h:259)
 // One thread per cell of a (32 x 8) x-y tile, marching k.  The neighbours'
 // s_new are recomputed from z and s_old, so s_old is never overwritten.
-template <typename T, bool FIRST, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) pcg_spmv_dot_kernel(const T* __restrict__ z, const T* __restrict__ s_old,
+// TZ: the preconditioned residual's type (the V-cycle's vectors), which
+// may be narrower than the PCG vectors' T.
+template <typename T, bool FIRST, int BLOCK, typename TZ = T>
+__global__ void __launch_bounds__(BLOCK) pcg_spmv_dot_kernel(const TZ* __restrict__ z, const T* __restrict__ s_old,
                                                             T* __restrict__ s_new, T* __restrict__ q,
                                                             const T* __restrict__ diag, const T* __restrict__ xp,
                                                             const T* __restrict__ yp, const T* __restrict__ zp,
@@ -127,7 +129,7 @@ __global__ void __launch_bounds__(BLOCK) pcg_spmv_dot_kernel(const T* __restrict
     for (int k = kb; k < ke; ++k) {
       size_t g = lin3(i, j, k, ni, nj);
       auto sv = [&](size_t gg) -> A {
-        if (FIRST) return ldg(z + gg);
+        if (FIRST) return A(ldg(z + gg));
         T t = cvt<T>((A)((double)ldg(z + gg) + beta * (double)ldg(s_old + gg)));
         return ldv(&t);
       };
@@ -174,9 +176,9 @@ __device__ __forceinline__ Quad<T> ldq(const T* p) {
   return *reinterpret_cast<const Quad<T>*>(p);
 }
 
-template <typename T, bool FIRST>
+template <typename T, bool FIRST, typename TZ = T>
 __global__ void __launch_bounds__(1024) pcg_spmv_dot_plane_kernel(
-    const T* __restrict__ z, const T* __restrict__ s_old, T* __restrict__ s_new, T* __restrict__ q,
+    const TZ* __restrict__ z, const T* __restrict__ s_old, T* __restrict__ s_new, T* __restrict__ q,
     const T* __restrict__ diag, const T* __restrict__ xp, const T* __restrict__ yp, const T* __restrict__ zp,
     int ni, int nj, int nk, int ty, int kz, double* partials, PcgScalars* st) {
   using A = typename Num<T>::Acc;
@@ -201,9 +203,10 @@ __global__ void __launch_bounds__(1024) pcg_spmv_dot_plane_kernel(
     Quad<T> ypk{};
     if (in_row && kk >= 0 && kk < nk) {
       const size_t g = (size_t)i0 + sy * j + szs * kk;
-      const Quad<T> zq = ldq(z + g);
+      const Quad<TZ> zq = ldq(z + g);
       if (FIRST) {
-        snew = zq;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) snew.v[c] = cvt<T>(A(ldv(&zq.v[c])));
       } else {
         const Quad<T> so = ldq(s_old + g);
 #pragma unroll
@@ -321,6 +324,49 @@ __global__ void __launch_bounds__(BLOCK) pcg_update_kernel(T* __restrict__ x, T*
   finish_reduction<BLOCK>(partials, gridDim.x, st, kReduceRes, 0.0, gridDim.x);
 }
 
+// FP64 outer loop around a narrower V-cycle (vectors of type V):
+// r = rhs, its copy rv in V for the V-cycle, x = 0, partial |rhs|_inf.
+template <typename V, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) pcg_init_outer_kernel(const double* __restrict__ rhs, double* __restrict__ r,
+                                                              V* __restrict__ rv, double* __restrict__ x, size_t n,
+                                                              double* partials, PcgScalars* st, double tol_factor) {
+  __shared__ double sm[BLOCK / 32];
+  double m = 0.0;
+  for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK) {
+    const double v = rhs[i];
+    r[i] = v;
+    rv[i] = cvt<V>((typename Num<V>::Acc)v);
+    x[i] = 0.0;
+    m = fmax(m, fabs(v));
+  }
+  double bm = block_absmax<BLOCK>(m, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = bm;
+  finish_reduction<BLOCK>(partials, gridDim.x, st, kReduceRes0, tol_factor, gridDim.x);
+}
+
+// x += alpha s, r -= alpha q in FP64, the V-cycle's copy rv = r, partial |r|_inf
+template <typename V, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) pcg_update_outer_kernel(double* __restrict__ x, double* __restrict__ r,
+                                                                V* __restrict__ rv, const double* __restrict__ s,
+                                                                const double* __restrict__ q, size_t n,
+                                                                double* partials, PcgScalars* st) {
+  __shared__ double sm[BLOCK / 32];
+  const double alpha = st->alpha;
+  const double nalpha = -alpha;
+  double m = 0.0;
+  for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK) {
+    const double xv = x[i] + alpha * __ldg(s + i);
+    const double rr = r[i] + nalpha * __ldg(q + i);
+    x[i] = xv;
+    r[i] = rr;
+    rv[i] = cvt<V>((typename Num<V>::Acc)rr);
+    m = fmax(m, fabs(rr));
+  }
+  double bm = block_absmax<BLOCK>(m, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = bm;
+  finish_reduction<BLOCK>(partials, gridDim.x, st, kReduceRes, 0.0, gridDim.x);
+}
+
 // Plain z.r when the V-cycle could not fuse it (single-level hierarchies
 // produce it inside the coarsest kernel instead).
 template <typename T, int BLOCK>
@@ -349,8 +395,8 @@ __global__ void pcg_loop_init_kernel(PcgScalars* st, int* it, cudaGraphCondition
 }
 
 // s = z + beta s in place (the direction update of AlgebraicMultigrid.h:284)
-template <typename T>
-__global__ void pcg_direction_kernel(const T* __restrict__ z, T* __restrict__ s, size_t n, const PcgScalars* st) {
+template <typename T, typename TZ = T>
+__global__ void pcg_direction_kernel(const TZ* __restrict__ z, T* __restrict__ s, size_t n, const PcgScalars* st) {
   using A = typename Num<T>::Acc;
   const double beta = st->beta;
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)

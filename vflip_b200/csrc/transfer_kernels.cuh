@@ -161,234 +161,6 @@ __global__ void advect_rk2_kernel(GridView u, GridView v, GridView w, GridView f
   }
 }
 
-// ---- tiled RK2 advection: the same scheme and arithmetic as
-// advect_rk2_kernel, with the velocity grids (and the advected fields) staged
-// in shared memory around a block's tile of nodes.  A block owns 32 x 8 x 8
-// nodes of the field grid (a thread: one x-y position, eight z); each staged
-// grid is copied over a window that covers every trilinear stencil a
-// backtrace of up to kAdvHalo cells reaches, with the grid's clamp-to-edge
-// applied while staging, so a sample whose corners lie in the window reads
-// the same values the global sampler reads and rounds the same way.  Samples
-// that leave the window (faster flow) take the global sampler: the results
-// are bitwise those of advect_rk2_kernel whatever the velocity.
-constexpr int kAdvTX = 32, kAdvTY = 8, kAdvTZ = 8, kAdvHalo = 2;
-// a node of index i (any of the MAC grids, or a cell) has its stencil's low
-// corner at index i - 1 or i of every staged grid; a backtrace moves it by
-// up to kAdvHalo, the corner pair adds one, and a face grid's last node rides
-// with the last tile: windows span [x0 - 1 - kAdvHalo, x0 + T + kAdvHalo + 1]
-constexpr int kAdvSX = kAdvTX + 2 * kAdvHalo + 3, kAdvSY = kAdvTY + 2 * kAdvHalo + 3,
-              kAdvSZ = kAdvTZ + 2 * kAdvHalo + 3;
-constexpr int kAdvWin = kAdvSX * kAdvSY * kAdvSZ;
-constexpr int kAdvThreads = kAdvTX * kAdvTY;
-
-struct AdvWin {
-  const float* s;  // shared-memory window
-  int x0, y0, z0;  // its origin in the grid's index space
-};
-
-// the window of a grid for the tile whose first node is (x0, y0, z0)
-__device__ __forceinline__ AdvWin adv_window(const float* s, int x0, int y0, int z0) {
-  return AdvWin{s, x0 - 1 - kAdvHalo, y0 - 1 - kAdvHalo, z0 - 1 - kAdvHalo};
-}
-
-__device__ __forceinline__ void adv_stage(float* s, const GridView& g, const AdvWin& w) {
-  for (int e = threadIdx.x + kAdvTX * threadIdx.y; e < kAdvWin; e += kAdvThreads) {
-    const int a = e % kAdvSX, r = e / kAdvSX, b = r % kAdvSY, c = r / kAdvSY;
-    const int gi = clampi(w.x0 + a, g.nx - 1), gj = clampi(w.y0 + b, g.ny - 1), gk = clampi(w.z0 + c, g.nz - 1);
-    s[e] = __ldg(g.d + (gi + g.nx * (gj + g.ny * gk)));
-  }
-}
-
-// sample_linear / sample_linear_f through a window; outside it the global sampler
-template <bool EXACT>
-__device__ __forceinline__ float smp_win(const GridView& g, const AdvWin& w, float ihf, float x, float y, float z) {
-  int i, j, k;
-  if (EXACT) {
-    const double gx = div_h(x, g) + g.ox, gy = div_h(y, g) + g.oy, gz = div_h(z, g) + g.oz;
-    i = (int)floor(gx);
-    j = (int)floor(gy);
-    k = (int)floor(gz);
-    const unsigned a = (unsigned)i - (unsigned)w.x0, b = (unsigned)j - (unsigned)w.y0, c = (unsigned)k - (unsigned)w.z0;
-    if (a > kAdvSX - 2 || b > kAdvSY - 2 || c > kAdvSZ - 2) return sample_linear(g, x, y, z);
-    const double cx = gx - (double)i, cy = gy - (double)j, cz = gz - (double)k;
-    const float* p = w.s + (a + kAdvSX * (b + kAdvSY * c));
-    constexpr int X = 1, Y = kAdvSX, Z = kAdvSX * kAdvSY;
-    const double a000 = p[0], a100 = p[X], a010 = p[Y], a110 = p[X + Y];
-    const double a001 = p[Z], a101 = p[X + Z], a011 = p[Y + Z], a111 = p[X + Y + Z];
-    const double v1 = lerp_d(lerp_d(a000, a100, cx), lerp_d(a010, a110, cx), cy);
-    const double v2 = lerp_d(lerp_d(a001, a101, cx), lerp_d(a011, a111, cx), cy);
-    return (float)lerp_d(v1, v2, cz);
-  } else {
-    const float gx = __fmaf_rn(x, ihf, (float)g.ox), gy = __fmaf_rn(y, ihf, (float)g.oy),
-                gz = __fmaf_rn(z, ihf, (float)g.oz);
-    const float fi = floorf(gx), fj = floorf(gy), fk = floorf(gz);
-    i = (int)fi;
-    j = (int)fj;
-    k = (int)fk;
-    const unsigned a = (unsigned)i - (unsigned)w.x0, b = (unsigned)j - (unsigned)w.y0, c = (unsigned)k - (unsigned)w.z0;
-    if (a > kAdvSX - 2 || b > kAdvSY - 2 || c > kAdvSZ - 2) return sample_linear_f(g, x, y, z);
-    const float cx = gx - fi, cy = gy - fj, cz = gz - fk;
-    const float* p = w.s + (a + kAdvSX * (b + kAdvSY * c));
-    constexpr int X = 1, Y = kAdvSX, Z = kAdvSX * kAdvSY;
-    const float v1 = lerp_f(lerp_f(p[0], p[X], cx), lerp_f(p[Y], p[X + Y], cx), cy);
-    const float v2 = lerp_f(lerp_f(p[Z], p[X + Z], cx), lerp_f(p[Y + Z], p[X + Y + Z], cx), cy);
-    return lerp_f(v1, v2, cz);
-  }
-}
-
-__device__ __forceinline__ float adv_ihf(const GridView& g) {
-  return (float)(g.inv_h != 0.0 ? g.inv_h : 1.0 / g.h);
-}
-
-// fsrc: which staged grid the advected field is (0, 1, 2: u, v, w - the
-// field is that velocity grid, self-advection), or 3: stage the field (and
-// f2) in windows of their own, or 4: sample them from global memory.
-template <bool EXACT>
-__global__ void __launch_bounds__(kAdvThreads) advect_rk2_tile_kernel(GridView u, GridView v, GridView w, GridView f,
-                                                                      float* __restrict__ out, GridView f2,
-                                                                      float* __restrict__ out2, float h, float dt,
-                                                                      int fsrc) {
-  extern __shared__ float adv_smem[];
-  const int x0 = blockIdx.x * kAdvTX, y0 = blockIdx.y * kAdvTY, z0 = blockIdx.z * kAdvTZ;
-  const AdvWin wu = adv_window(adv_smem, x0, y0, z0);
-  const AdvWin wv = adv_window(adv_smem + kAdvWin, x0, y0, z0);
-  const AdvWin ww = adv_window(adv_smem + 2 * kAdvWin, x0, y0, z0);
-  adv_stage(adv_smem, u, wu);
-  adv_stage(adv_smem + kAdvWin, v, wv);
-  adv_stage(adv_smem + 2 * kAdvWin, w, ww);
-  AdvWin wf = fsrc == 0 ? wu : (fsrc == 1 ? wv : ww);
-  AdvWin wf2 = wf;
-  if (fsrc == 3) {
-    wf = adv_window(adv_smem + 3 * kAdvWin, x0, y0, z0);
-    adv_stage(adv_smem + 3 * kAdvWin, f, wf);
-    if (out2) {
-      wf2 = adv_window(adv_smem + 4 * kAdvWin, x0, y0, z0);
-      adv_stage(adv_smem + 4 * kAdvWin, f2, wf2);
-    }
-  } else if (fsrc == 4) {
-    wf.x0 = wf2.x0 = INT_MIN / 2;  // no window: every sample takes the global sampler
-  }
-  __syncthreads();
-  const float ihu = adv_ihf(u), ihv = adv_ihf(v), ihw = adv_ihf(w), ihf = adv_ihf(f), ihf2 = adv_ihf(f2);
-  const double hdt = 0.5 * (double)dt;
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  // a face grid's last node along x belongs to the last x tile (its thread 31)
-  const int nxs = (x0 + kAdvTX + 1 == f.nx && tx == kAdvTX - 1) ? 2 : 1;
-  const int j = y0 + ty;
-  if (j >= f.ny) return;
-  for (int xs = 0; xs < nxs; ++xs) {
-    const int i = x0 + tx + xs;
-    if (i >= f.nx) break;
-    for (int t = 0; t < kAdvTZ; ++t) {
-      const int k = z0 + t;
-      if (k >= f.nz) break;
-      const size_t e = (size_t)i + (size_t)f.nx * ((size_t)j + (size_t)f.ny * (size_t)k);
-      float wx, wy, wz;
-      node_world(f, e, h, wx, wy, wz);
-      float a = smp_win<EXACT>(u, wu, ihu, wx, wy, wz), b = smp_win<EXACT>(v, wv, ihv, wx, wy, wz),
-            c = smp_win<EXACT>(w, ww, ihw, wx, wy, wz);
-      float px, py, pz;
-      if (EXACT) {
-        px = (float)((double)wx - hdt * (double)a);
-        py = (float)((double)wy - hdt * (double)b);
-        pz = (float)((double)wz - hdt * (double)c);
-      } else {
-        const float hf = 0.5f * dt;
-        px = wx - hf * a;
-        py = wy - hf * b;
-        pz = wz - hf * c;
-      }
-      a = smp_win<EXACT>(u, wu, ihu, px, py, pz);
-      b = smp_win<EXACT>(v, wv, ihv, px, py, pz);
-      c = smp_win<EXACT>(w, ww, ihw, px, py, pz);
-      px = wx - dt * a;
-      py = wy - dt * b;
-      pz = wz - dt * c;
-      out[e] = smp_win<EXACT>(f, wf, ihf, px, py, pz);
-      if (out2) out2[e] = smp_win<EXACT>(f2, wf2, ihf2, px, py, pz);
-    }
-  }
-}
-
-// One node of the RK2 advection through the staged windows (the per-node
-// arithmetic of advect_rk2_kernel): the field f at node e of f's grid.
-template <bool EXACT>
-__device__ __forceinline__ float adv_node(const GridView& u, const GridView& v, const GridView& w, const AdvWin& wu,
-                                          const AdvWin& wv, const AdvWin& ww, float ihu, float ihv, float ihw,
-                                          const GridView& f, const AdvWin& wf, float ihf, size_t e, float h,
-                                          float dt) {
-  float wx, wy, wz;
-  node_world(f, e, h, wx, wy, wz);
-  float a = smp_win<EXACT>(u, wu, ihu, wx, wy, wz), b = smp_win<EXACT>(v, wv, ihv, wx, wy, wz),
-        c = smp_win<EXACT>(w, ww, ihw, wx, wy, wz);
-  float px, py, pz;
-  if (EXACT) {
-    const double hdt = 0.5 * (double)dt;
-    px = (float)((double)wx - hdt * (double)a);
-    py = (float)((double)wy - hdt * (double)b);
-    pz = (float)((double)wz - hdt * (double)c);
-  } else {
-    const float hf = 0.5f * dt;
-    px = wx - hf * a;
-    py = wy - hf * b;
-    pz = wz - hf * c;
-  }
-  a = smp_win<EXACT>(u, wu, ihu, px, py, pz);
-  b = smp_win<EXACT>(v, wv, ihv, px, py, pz);
-  c = smp_win<EXACT>(w, ww, ihw, px, py, pz);
-  px = wx - dt * a;
-  py = wy - dt * b;
-  pz = wz - dt * c;
-  return smp_win<EXACT>(f, wf, ihf, px, py, pz);
-}
-
-// SubDomainSolver::advect_field of u, v and w through (u, v, w) in one
-// launch (the velocity advection of a smoke step): the tiles run over the
-// cells, each thread advects the u, v and w nodes of its cells (and the last
-// face node of a grid along its own axis), all from the same three staged
-// windows.  Per node the arithmetic of advect_rk2_kernel: bitwise the three
-// separate launches.
-template <bool EXACT>
-__global__ void __launch_bounds__(kAdvThreads) advect_vel3_tile_kernel(GridView u, GridView v, GridView w,
-                                                                       float* __restrict__ uo, float* __restrict__ vo,
-                                                                       float* __restrict__ wo, float h, float dt,
-                                                                       int ni, int nj, int nk) {
-  extern __shared__ float adv_smem[];
-  const int x0 = blockIdx.x * kAdvTX, y0 = blockIdx.y * kAdvTY, z0 = blockIdx.z * kAdvTZ;
-  const AdvWin wu = adv_window(adv_smem, x0, y0, z0);
-  const AdvWin wv = adv_window(adv_smem + kAdvWin, x0, y0, z0);
-  const AdvWin ww = adv_window(adv_smem + 2 * kAdvWin, x0, y0, z0);
-  adv_stage(adv_smem, u, wu);
-  adv_stage(adv_smem + kAdvWin, v, wv);
-  adv_stage(adv_smem + 2 * kAdvWin, w, ww);
-  __syncthreads();
-  const float ihu = adv_ihf(u), ihv = adv_ihf(v), ihw = adv_ihf(w);
-  const int i = x0 + threadIdx.x, j = y0 + threadIdx.y;
-  if (i >= ni || j >= nj) return;
-  for (int t = 0; t < kAdvTZ; ++t) {
-    const int k = z0 + t;
-    if (k >= nk) break;
-    size_t e = (size_t)i + (size_t)u.nx * ((size_t)j + (size_t)u.ny * (size_t)k);
-    uo[e] = adv_node<EXACT>(u, v, w, wu, wv, ww, ihu, ihv, ihw, u, wu, ihu, e, h, dt);
-    if (i == ni - 1) {
-      e += 1;
-      uo[e] = adv_node<EXACT>(u, v, w, wu, wv, ww, ihu, ihv, ihw, u, wu, ihu, e, h, dt);
-    }
-    e = (size_t)i + (size_t)v.nx * ((size_t)j + (size_t)v.ny * (size_t)k);
-    vo[e] = adv_node<EXACT>(u, v, w, wu, wv, ww, ihu, ihv, ihw, v, wv, ihv, e, h, dt);
-    if (j == nj - 1) {
-      e += (size_t)v.nx;
-      vo[e] = adv_node<EXACT>(u, v, w, wu, wv, ww, ihu, ihv, ihw, v, wv, ihv, e, h, dt);
-    }
-    e = (size_t)i + (size_t)w.nx * ((size_t)j + (size_t)w.ny * (size_t)k);
-    wo[e] = adv_node<EXACT>(u, v, w, wu, wv, ww, ihu, ihv, ihw, w, ww, ihw, e, h, dt);
-    if (k == nk - 1) {
-      e += (size_t)w.nx * (size_t)w.ny;
-      wo[e] = adv_node<EXACT>(u, v, w, wu, wv, ww, ihu, ihv, ihw, w, ww, ihw, e, h, dt);
-    }
-  }
-}
-
 // getDelta, Smoke_solver3D.cpp:1298-1319
 __global__ void delta_kernel(const float* __restrict__ after, const float* __restrict__ before,
                              float* __restrict__ delta, size_t n) {

@@ -31,6 +31,7 @@
 #include "smoother3d.cuh"
 #include "smoother_carry.cuh"
 #include "coarse_direct.cuh"
+#include "batch_kernels.cuh"
 #include "tmap.h"
 #include "unet_net.h"
 
@@ -643,6 +644,11 @@ int convert_array(vflip_ctx* ctx, const double* src, T* dst, size_t n) {
 template <typename S0, typename SC, typename V>
 struct Typed {
   Level<S0, V> fine;
+  // the fine operator in FP64 as assembled (the outer PCG's SpMV in FP64)
+  const double* d64 = nullptr;
+  const double* x64 = nullptr;
+  const double* y64 = nullptr;
+  const double* z64 = nullptr;
   std::vector<Level<SC, V>> coarse;  // coarse[l-1] = level l
   CoarseDirect direct;               // factor of the coarsest level, when used
 };
@@ -715,6 +721,10 @@ int make_typed(vflip_ctx* ctx, const Hierarchy64& H, const double* d0, const dou
                const double* z0, Typed<S0, SC, V>& T, const char* tag) {
   int rc;
   if ((rc = make_level<S0, V>(ctx, H, 0, d0, x0, y0, z0, T.fine, tag))) return rc;
+  T.d64 = d0;
+  T.x64 = x0;
+  T.y64 = y0;
+  T.z64 = z0;
   T.coarse.resize(H.dims.size() - 1);
   for (size_t l = 1; l < H.dims.size(); ++l)
     if ((rc = make_level<SC, V>(ctx, H, l, d0, x0, y0, z0, T.coarse[l - 1], tag))) return rc;
@@ -849,23 +859,25 @@ int read_scalars(vflip_ctx* ctx) {
 // runs where the fine rows are whole warps of quads (unless the context asks
 // for the column kernel, or `plane` is false: the batched graph keeps the
 // column kernel); both give the same q and s_new bits.
-template <typename V>
-int launch_spmv_dot(vflip_ctx* ctx, cudaStream_t stream, bool first, const V* z, const V* s_old, V* s_new, V* q,
-                    const V* diag, const V* xp, const V* yp, const V* zp, const Dims& d, bool plane = true) {
+template <typename W, typename Z = W>
+int launch_spmv_dot(vflip_ctx* ctx, cudaStream_t stream, bool first, const Z* z, const W* s_old, W* s_new, W* q,
+                    const W* diag, const W* xp, const W* yp, const W* zp, const Dims& d, bool plane = true) {
   const int nq = d.ni / 4;
   if (plane && ctx->cfg.spmv_kernel == 0 && d.ni % 128 == 0 && nq <= 256) {
-    const int ty = std::min(8, 1024 / nq - 2);
+    // about 384 threads a block (at 256 cells a row: 4 rows + 2 halo rows,
+    // three blocks per SM) and two waves of blocks measured fastest
+    const int ty = std::max(2, 384 / nq - 2);
     const int rows = ty + 2;
-    const size_t smem = 6 * (size_t)rows * nq * sizeof(Quad<V>);
-    auto kern = first ? pcg_spmv_dot_plane_kernel<V, true> : pcg_spmv_dot_plane_kernel<V, false>;
+    const size_t smem = 6 * (size_t)rows * nq * sizeof(Quad<W>);
+    auto kern = first ? pcg_spmv_dot_plane_kernel<W, true, Z> : pcg_spmv_dot_plane_kernel<W, false, Z>;
     if (smem_optin((const void*)kern, (int)smem) != cudaSuccess)
       return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the SpMV kernel's shared memory limit");
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nq * rows, smem) != cudaSuccess || per_sm < 1)
       per_sm = 1;
-    // one wave of resident blocks: row tiles x plane ranges
+    // row tiles x plane ranges
     const int rt = (d.nj + ty - 1) / ty;
-    int kr = std::max(1, std::min(d.nk, per_sm * ctx->num_sms / rt));
+    int kr = std::max(1, std::min(d.nk, 2 * per_sm * ctx->num_sms / rt));
     const int kz = (d.nk + kr - 1) / kr;
     kr = (d.nk + kz - 1) / kz;
     if ((size_t)rt * kr <= (size_t)kMaxPartials) {
@@ -883,14 +895,79 @@ int launch_spmv_dot(vflip_ctx* ctx, cudaStream_t stream, bool first, const V* z,
   if ((size_t)sgrid.x * sgrid.y * sgrid.z > (size_t)kMaxPartials) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
   const int slot = prof_start(ctx, VFLIP_PROF_SPMV, stream);
   if (first)
-    pcg_spmv_dot_kernel<V, true, kRedBlock><<<sgrid, sblk, 0, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp, d.ni,
-                                                                        d.nj, d.nk, kz, ctx->partials, ctx->st);
+    pcg_spmv_dot_kernel<W, true, kRedBlock, Z><<<sgrid, sblk, 0, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp,
+                                                                           d.ni, d.nj, d.nk, kz, ctx->partials,
+                                                                           ctx->st);
   else
-    pcg_spmv_dot_kernel<V, false, kRedBlock><<<sgrid, sblk, 0, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp, d.ni,
-                                                                         d.nj, d.nk, kz, ctx->partials, ctx->st);
+    pcg_spmv_dot_kernel<W, false, kRedBlock, Z><<<sgrid, sblk, 0, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp,
+                                                                            d.ni, d.nj, d.nk, kz, ctx->partials,
+                                                                            ctx->st);
   prof_stop(ctx, slot, stream);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
+}
+
+// The outer PCG's vectors: W = V (everything in the working precision) or
+// W = double around a narrower V-cycle (FP32/MIXED contexts by default).
+// In the second case x is the caller's FP64 result itself, r/s/q are FP64,
+// the SpMV uses the FP64 fine operator, and rv is r rounded to V for the
+// V-cycle (written by the update).
+template <typename W, typename V>
+struct OuterVecs {
+  W *x = nullptr, *r = nullptr, *s0 = nullptr, *s1 = nullptr, *q = nullptr;
+  V *rv = nullptr, *z = nullptr;
+  const W *od = nullptr, *ox = nullptr, *oy = nullptr, *oz = nullptr;
+};
+
+template <typename W, typename S0, typename SC, typename V>
+int outer_vecs(vflip_ctx* ctx, Typed<S0, SC, V>& T, double* result, OuterVecs<W, V>& o) {
+  const size_t n = T.fine.d.n();
+  constexpr bool same = std::is_same<W, V>::value;
+  VF_ALLOC(o.z, V, "pcg_z", n);
+  VF_ALLOC(o.s0, W, same ? "pcg_s0" : "pcg_s0_64", n);
+  VF_ALLOC(o.s1, W, same ? "pcg_s1" : "pcg_s1_64", n);
+  VF_ALLOC(o.q, W, same ? "pcg_q" : "pcg_q_64", n);
+  if constexpr (same) {
+    VF_ALLOC(o.x, W, "pcg_x", n);
+    VF_ALLOC(o.r, W, "pcg_r", n);
+    o.rv = o.r;
+    o.od = reinterpret_cast<const W*>(T.fine.diag);
+    o.ox = reinterpret_cast<const W*>(T.fine.xp);
+    o.oy = reinterpret_cast<const W*>(T.fine.yp);
+    o.oz = reinterpret_cast<const W*>(T.fine.zp);
+  } else {
+    o.x = result;
+    VF_ALLOC(o.r, W, "pcg_r_64", n);
+    VF_ALLOC(o.rv, V, "pcg_r", n);
+    o.od = T.d64;
+    o.ox = T.x64;
+    o.oy = T.y64;
+    o.oz = T.z64;
+  }
+  return VFLIP_OK;
+}
+
+// r = rhs, x = 0, |rhs|_inf
+template <typename W, typename V>
+void launch_pcg_init(vflip_ctx* ctx, cudaStream_t st, const OuterVecs<W, V>& o, const double* rhs, size_t n,
+                     double tol_factor) {
+  const int gb = grid_for(n, kRedBlock, ctx->num_sms);
+  if constexpr (std::is_same<W, V>::value)
+    pcg_init_kernel<V, kRedBlock><<<gb, kRedBlock, 0, st>>>(rhs, o.r, o.x, n, ctx->partials, ctx->st, tol_factor);
+  else
+    pcg_init_outer_kernel<V, kRedBlock><<<gb, kRedBlock, 0, st>>>(rhs, o.r, o.rv, o.x, n, ctx->partials, ctx->st,
+                                                                  tol_factor);
+}
+
+// x += alpha s, r -= alpha q, |r|_inf (and the V-cycle's copy of r)
+template <typename W, typename V>
+void launch_pcg_update(vflip_ctx* ctx, cudaStream_t st, const OuterVecs<W, V>& o, const W* s, size_t n) {
+  const int gb = grid_for(n, kRedBlock, ctx->num_sms);
+  if constexpr (std::is_same<W, V>::value)
+    pcg_update_kernel<V, kRedBlock><<<gb, kRedBlock, 0, st>>>(o.x, o.r, s, o.q, n, ctx->partials, ctx->st);
+  else
+    pcg_update_outer_kernel<V, kRedBlock><<<gb, kRedBlock, 0, st>>>(o.x, o.r, o.rv, s, o.q, n, ctx->partials,
+                                                                    ctx->st);
 }
 
 // AMGPCGSolve's loop on the device (AlgebraicMultigrid.h:253-286): a CUDA
@@ -902,19 +979,18 @@ int launch_spmv_dot(vflip_ctx* ctx, cudaStream_t stream, bool first, const V* z,
 // so the iterates are the host loop's.  *done is false when the solve did
 // not converge (zero or NaN rho, max_iterations): the caller then repeats it
 // with the host loop, whose early exits set the result as the reference's.
-template <typename S0, typename SC, typename V>
+template <typename W, typename S0, typename SC, typename V>
 int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor,
                     int maxit, vflip_solve_stats* stats, bool* done) {
   *done = false;
   const Dims d = T.fine.d;
   const size_t n = d.n();
-  V *x, *r, *z, *s, *q;
+  OuterVecs<W, V> o;
+  int rc0;
+  if ((rc0 = outer_vecs<W>(ctx, T, result, o))) return rc0;
+  W *x = o.x, *r = o.r, *s = o.s0, *q = o.q;
+  V* z = o.z;
   int* itp;
-  VF_ALLOC(x, V, "pcg_x", n);
-  VF_ALLOC(r, V, "pcg_r", n);
-  VF_ALLOC(z, V, "pcg_z", n);
-  VF_ALLOC(s, V, "pcg_s0", n);
-  VF_ALLOC(q, V, "pcg_q", n);
   VF_ALLOC(itp, int, "pcg_it", 1);
   // everything the captured launches name
   std::vector<uintptr_t> key;
@@ -923,7 +999,8 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
     kp(L.diag); kp(L.xp); kp(L.yp); kp(L.zp); kp(L.b); kp(L.xa); kp(L.xb);
     key.push_back((uintptr_t)L.d.ni); key.push_back((uintptr_t)L.d.nj); key.push_back((uintptr_t)L.d.nk);
   };
-  kp(rhs); kp(result); kp(x); kp(r); kp(z); kp(s); kp(q); kp(itp); kp(ctx->st); kp(ctx->partials);
+  kp(rhs); kp(result); kp(x); kp(r); kp(o.rv); kp(z); kp(s); kp(q); kp(itp); kp(ctx->st); kp(ctx->partials);
+  kp(o.od); kp(o.ox); kp(o.oy); kp(o.oz);
   kl(T.fine);
   for (const auto& L : T.coarse) kl(L);
   kp(T.direct.L); kp(T.direct.rinv); kp(T.direct.ok);
@@ -966,8 +1043,8 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
     if (cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
       return restore(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamBeginCaptureToGraph"));
     cudaMemsetAsync(ctx->st, 0, sizeof(PcgScalars), cs);
-    cudaMemsetAsync(s, 0, n * sizeof(V), cs);
-    pcg_init_kernel<V, kRedBlock><<<gb, kRedBlock, 0, cs>>>(rhs, r, x, n, ctx->partials, ctx->st, tol_factor);
+    cudaMemsetAsync(s, 0, n * sizeof(W), cs);
+    launch_pcg_init(ctx, cs, o, rhs, n, tol_factor);
     pcg_loop_init_kernel<<<1, 32, 0, cs>>>(ctx->st, itp, hnd);
     cudaStreamCaptureStatus cst;
     const cudaGraphNode_t* deps = nullptr;
@@ -991,15 +1068,15 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
     if (cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
       return restore(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamBeginCaptureToGraph (body)"));
     const unsigned long long l0 = ctx->launches;
-    int brc = vcycle<S0, SC, V>(ctx, T, r, z, true);
+    int brc = vcycle<S0, SC, V>(ctx, T, o.rv, z, true);
     if (!brc) {
-      pcg_direction_kernel<V><<<grid_for(n, 256, ctx->num_sms), 256, 0, cs>>>(z, s, n, ctx->st);
+      pcg_direction_kernel<W, V><<<grid_for(n, 256, ctx->num_sms), 256, 0, cs>>>(z, s, n, ctx->st);
       ++ctx->launches;
-      brc = launch_spmv_dot<V>(ctx, cs, true, s, nullptr, nullptr, q, T.fine.diag, T.fine.xp, T.fine.yp, T.fine.zp,
-                               d);
+      brc = launch_spmv_dot<W>(ctx, cs, true, (const W*)s, (const W*)nullptr, (W*)nullptr, q, o.od, o.ox, o.oy,
+                               o.oz, d);
     }
     if (!brc) {
-      pcg_update_kernel<V, kRedBlock><<<gb, kRedBlock, 0, cs>>>(x, r, s, q, n, ctx->partials, ctx->st);
+      launch_pcg_update(ctx, cs, o, s, n);
       pcg_loop_cond_kernel<<<1, 32, 0, cs>>>(ctx->st, itp, maxit, hnd);
       ctx->launches += 2;
     }
@@ -1008,9 +1085,13 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
     ctx->pg_body_launches = ctx->launches - l0;
     if (cudaStreamBeginCaptureToGraph(cs, graph, &wn, nullptr, 1, cudaStreamCaptureModeRelaxed) != cudaSuccess)
       return restore(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamBeginCaptureToGraph (result)"));
-    to_double_kernel<V, kRedBlock><<<gb, kRedBlock, 0, cs>>>(x, result, n);
+    if constexpr (std::is_same<W, V>::value) {
+      to_double_kernel<V, kRedBlock><<<gb, kRedBlock, 0, cs>>>(x, result, n);
+      ctx->pg_tail_launches = 1;
+    } else {
+      ctx->pg_tail_launches = 0;  // x is the result
+    }
     if ((rc = end_capture(graph))) return restore(rc);
-    ctx->pg_tail_launches = 1;
     restore(VFLIP_OK);
     ctx->launches = before_capture;  // captured launches count when the graph runs
     if (cudaGraphInstantiate(&ctx->pg_exec, graph, 0) != cudaSuccess) {
@@ -1044,28 +1125,24 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
   return VFLIP_OK;
 }
 
-template <typename S0, typename SC, typename V>
-int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor, int maxit,
-              vflip_solve_stats* stats, V* x1_out = nullptr) {
+// AMGPCGSolve (AlgebraicMultigrid.h:189-301) with the outer vectors in W.
+template <typename W, typename S0, typename SC, typename V>
+int pcg_solve_w(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor,
+                int maxit, vflip_solve_stats* stats, V* x1_out) {
+  constexpr bool same = std::is_same<W, V>::value;
   if (ctx->cfg.pcg_loop == 0 && !ctx->profiling && !x1_out) {
     bool done = false;
-    const int grc = pcg_solve_graph(ctx, T, rhs, result, tol_factor, maxit, stats, &done);
+    const int grc = pcg_solve_graph<W>(ctx, T, rhs, result, tol_factor, maxit, stats, &done);
     if (grc < 0 || done) return grc;
   }
   const Dims d = T.fine.d;
   const size_t n = d.n();
-  V *x, *r, *z, *s0, *s1, *q;
-  VF_ALLOC(x, V, "pcg_x", n);
-  VF_ALLOC(r, V, "pcg_r", n);
-  VF_ALLOC(z, V, "pcg_z", n);
-  VF_ALLOC(s0, V, "pcg_s0", n);
-  VF_ALLOC(s1, V, "pcg_s1", n);
-  VF_ALLOC(q, V, "pcg_q", n);
-  VF_CUDA(cudaMemsetAsync(ctx->st, 0, sizeof(PcgScalars), ctx->stream));
+  OuterVecs<W, V> o;
   int rc;
+  if ((rc = outer_vecs<W>(ctx, T, result, o))) return rc;
+  VF_CUDA(cudaMemsetAsync(ctx->st, 0, sizeof(PcgScalars), ctx->stream));
   const int gb = grid_for(n, kRedBlock, ctx->num_sms);
-  pcg_init_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(rhs, r, x, n, ctx->partials, ctx->st,
-                                                                    tol_factor);
+  launch_pcg_init(ctx, ctx->stream, o, rhs, n, tol_factor);
   VF_LAUNCH_CHECK();
   if ((rc = read_scalars(ctx))) return rc;
   PcgScalars& h = *ctx->st_host;
@@ -1073,10 +1150,12 @@ int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* re
   int iterations = 0, vcycles = 0;
   double residual = h.res;
   auto finish = [&](int st_code) -> int {
-    to_double_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(x, result, n);
-    ++ctx->launches;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return ctx->fail(VFLIP_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+    if constexpr (same) {
+      to_double_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(o.x, result, n);
+      ++ctx->launches;
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return ctx->fail(VFLIP_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+    }
     if (stats) {
       stats->iterations = iterations;
       stats->vcycles = vcycles;
@@ -1091,37 +1170,54 @@ int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* re
     iterations = 0;
     return finish(VFLIP_OK);
   }
-  if ((rc = vcycle<S0, SC, V>(ctx, T, r, z, true))) return rc;
+  if ((rc = vcycle<S0, SC, V>(ctx, T, o.rv, o.z, true))) return rc;
   ++vcycles;
   if ((rc = read_scalars(ctx))) return rc;
   if (h.bad_rho) {  // AlgebraicMultigrid.h:236-252
     iterations = 0;
     return finish(VFLIP_NOT_CONVERGED);
   }
-  V* s_old = s0;
-  V* s_new = s1;
+  W* s_old = o.s0;
+  W* s_new = o.s1;
   int it;
   for (it = 0; it < maxit; ++it) {
-    if ((rc = launch_spmv_dot<V>(ctx, ctx->stream, it == 0, z, s_old, s_new, q, T.fine.diag, T.fine.xp, T.fine.yp,
-                                 T.fine.zp, d)))
+    if ((rc = launch_spmv_dot<W, V>(ctx, ctx->stream, it == 0, o.z, s_old, s_new, o.q, o.od, o.ox, o.oy, o.oz, d)))
       return rc;
     const int uslot = prof_start(ctx, VFLIP_PROF_UPDATE, ctx->stream);
-    pcg_update_kernel<V, kRedBlock><<<gb, kRedBlock, 0, ctx->stream>>>(x, r, s_new, q, n, ctx->partials, ctx->st);
+    launch_pcg_update(ctx, ctx->stream, o, s_new, n);
     prof_stop(ctx, uslot, ctx->stream);
     VF_LAUNCH_CHECK();
-    if (it == 0 && x1_out) VF_CUDA(cudaMemcpyAsync(x1_out, x, n * sizeof(V), cudaMemcpyDeviceToDevice, ctx->stream));
+    if (it == 0 && x1_out) {
+      if constexpr (same) {
+        VF_CUDA(cudaMemcpyAsync(x1_out, o.x, n * sizeof(V), cudaMemcpyDeviceToDevice, ctx->stream));
+      } else {
+        convert_kernel<V><<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(o.x, x1_out, n);
+        VF_LAUNCH_CHECK();
+      }
+    }
     if ((rc = read_scalars(ctx))) return rc;
     residual = h.res;
     if (h.converged) {
       iterations = it + 1;
       return finish(VFLIP_OK);
     }
-    if ((rc = vcycle<S0, SC, V>(ctx, T, r, z, true))) return rc;
+    if ((rc = vcycle<S0, SC, V>(ctx, T, o.rv, o.z, true))) return rc;
     ++vcycles;
     std::swap(s_old, s_new);
   }
   iterations = it;
   return finish(VFLIP_NOT_CONVERGED);
+}
+
+// The outer loop runs in FP64 around an FP32/MIXED V-cycle unless the
+// context asks for the working precision (pcg_vectors = 1).
+template <typename S0, typename SC, typename V>
+int pcg_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor, int maxit,
+              vflip_solve_stats* stats, V* x1_out = nullptr) {
+  if constexpr (!std::is_same<V, double>::value) {
+    if (ctx->cfg.pcg_vectors == 0) return pcg_solve_w<double>(ctx, T, rhs, result, tol_factor, maxit, stats, x1_out);
+  }
+  return pcg_solve_w<V>(ctx, T, rhs, result, tol_factor, maxit, stats, x1_out);
 }
 
 // ---------------------------------------------------------------- learned
@@ -1717,7 +1813,182 @@ int batched_graph(vflip_ctx* ctx, int nsys, const vflip_system* sys, double tol,
   return status;
 }
 
+// The whole batch as one persistent cooperative kernel (batch_kernels.cuh)
+// inside a captured CUDA graph: the hierarchies are built first (eagerly,
+// one per-system context each, as in graph mode), then one launch runs every
+// system's PCG loop over a (system, level, chunk) work list.  The cells per
+// work item and the resident CTAs per SM come from the context's
+// configuration (batch_chunk, batch_ctas_per_sm; vflip_b200/tune.py picks
+// them per batch).  A batch the kernel does not take (a system with a single
+// level or more levels than it holds) is left to graph mode (*taken false).
+template <typename S0, typename SC, typename V>
+int batched_persistent(vflip_ctx* ctx, int nsys, const vflip_system* sys, double tol, int maxit,
+                       vflip_solve_stats* stats, const char* tag, bool* taken) {
+  using A = typename Num<V>::Acc;
+  *taken = false;
+  int rc;
+  std::vector<BatchItem<S0, SC, V>> items(nsys);
+  std::vector<BatchSys<S0, SC, V>> desc(nsys);
+  const int CH = ctx->cfg.batch_chunk > 0 ? ctx->cfg.batch_chunk : 4096;
+  int lmax = 0, part_stride = 1, smem_doubles = 1;
+  for (int i = 0; i < nsys; ++i) {
+    BatchItem<S0, SC, V>& b = items[i];
+    if ((rc = batch_sub(ctx, i, &b.sub))) return rc;
+    vflip_ctx* c = b.sub;
+    c->stream = ctx->stream;
+    c->profiling = false;
+    const vflip_system& y = sys[i];
+    if ((rc = build_hierarchy64(c, y.ni, y.nj, y.nk, y.diag, y.xp, y.yp, y.zp, b.H)) ||
+        (rc = make_typed(c, b.H, y.diag, y.xp, y.yp, y.zp, b.T, tag))) {
+      ctx->err = c->err;
+      return rc;
+    }
+    const int nl = (int)b.T.coarse.size() + 1;
+    if (nl < 2 || nl > kBatchMaxLevels) return VFLIP_OK;  // not taken
+    const size_t n = (size_t)y.ni * y.nj * y.nk;
+    V** vs[5] = {&b.x, &b.r, &b.z, &b.s, &b.q};
+    const char* names[5] = {"bat_x", "bat_r", "bat_z", "bat_s", "bat_q"};
+    for (int k = 0; k < 5; ++k) {
+      *vs[k] = (V*)c->buf(names[k], sizeof(V) * n);
+      if (!*vs[k]) return ctx->fail(VFLIP_ERR_NOMEM, "cudaMalloc failed for %s", names[k]);
+    }
+    b.it = (int*)c->buf("bat_it2", 2 * sizeof(int));  // iterations, state
+    if (!b.it) return ctx->fail(VFLIP_ERR_NOMEM, "cudaMalloc failed for bat_it2");
+    BatchSys<S0, SC, V>& d = desc[i];
+    std::memset(&d, 0, sizeof d);
+    d.nl = nl;
+    const Level<S0, V>& F = b.T.fine;
+    d.fine = BatchLevel<S0, V>{F.d.ni, F.d.nj, F.d.nk, F.diag, F.xp, F.yp, F.zp, b.r, b.z};
+    for (int l = 1; l < nl; ++l) {
+      const Level<SC, V>& L = b.T.coarse[l - 1];
+      d.lv[l] = BatchLevel<SC, V>{L.d.ni, L.d.nj, L.d.nk, L.diag, L.xp, L.yp, L.zp, L.b, L.xa};
+    }
+    d.x = b.x;
+    d.s = b.s;
+    d.q = b.q;
+    d.rhs = y.rhs;
+    d.result = y.result;
+    d.st = c->st;
+    d.it = b.it;
+    d.state = b.it + 1;
+    d.direct = b.T.direct.on ? 1 : 0;
+    d.bw = b.T.direct.bw;
+    d.L = b.T.direct.L;
+    d.rinv = b.T.direct.rinv;
+    d.ok = b.T.direct.ok;
+    d.sweeps = ctx->cfg.coarse_sweeps;
+    d.tol_factor = tol;
+    lmax = std::max(lmax, nl);
+    part_stride = std::max(part_stride, (int)((n + CH - 1) / CH));
+    const Level<SC, V>& C = b.T.coarse[nl - 2];
+    const int nc = C.d.ni * C.d.nj * C.d.nk;
+    smem_doubles = std::max(smem_doubles, d.direct ? nc : (int)((2 * (size_t)nc * sizeof(A) + 7) / 8));
+  }
+  smem_doubles = std::min(smem_doubles, 6144);  // 48 KB; larger coarsest sweeps run in global memory
+  // work lists: cell items of level 0 for every system and of a coarser
+  // level where the system smooths there; restriction items into level l+1
+  const size_t tab = (size_t)lmax * (nsys + 1);
+  std::vector<int> cell_pre(tab, 0), rest_pre(tab, 0);
+  for (int l = 0; l < lmax; ++l)
+    for (int i = 0; i < nsys; ++i) {
+      const BatchSys<S0, SC, V>& d = desc[i];
+      long long ci = 0, ri = 0;
+      if (l == 0) ci = ((long long)d.fine.ni * d.fine.nj * d.fine.nk + CH - 1) / CH;
+      else if (l + 1 < d.nl) ci = ((long long)d.lv[l].ni * d.lv[l].nj * d.lv[l].nk + CH - 1) / CH;
+      if (l + 1 < d.nl) ri = ((long long)d.lv[l + 1].ni * d.lv[l + 1].nj * d.lv[l + 1].nk + CH - 1) / CH;
+      cell_pre[(size_t)l * (nsys + 1) + i + 1] = cell_pre[(size_t)l * (nsys + 1) + i] + (int)ci;
+      rest_pre[(size_t)l * (nsys + 1) + i + 1] = rest_pre[(size_t)l * (nsys + 1) + i] + (int)ri;
+    }
+  const size_t sys_bytes = ((sizeof(BatchSys<S0, SC, V>) * nsys + 255) / 256) * 256;
+  const size_t part_bytes = (size_t)nsys * part_stride * sizeof(double);
+  char* dev = (char*)ctx->buf("bp_plan", sys_bytes + part_bytes + (2 * tab + 4) * sizeof(int));
+  if (!dev) return ctx->fail(VFLIP_ERR_NOMEM, "cudaMalloc failed for the batch plan");
+  auto* dsys = reinterpret_cast<BatchSys<S0, SC, V>*>(dev);
+  double* part = reinterpret_cast<double*>(dev + sys_bytes);
+  int* dcell = reinterpret_cast<int*>(dev + sys_bytes + part_bytes);
+  int* drest = dcell + tab;
+  int* dactive = drest + tab;
+  VF_CUDA(cudaMemcpyAsync(dsys, desc.data(), sizeof(BatchSys<S0, SC, V>) * nsys, cudaMemcpyHostToDevice,
+                          ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(dcell, cell_pre.data(), tab * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(drest, rest_pre.data(), tab * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  // the host vectors above are read by the copies: wait for them before they go
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  BatchPlan plan{nsys, lmax, maxit, CH, dcell, drest, part, part_stride, dactive, smem_doubles};
+  auto kern = batch_pcg_kernel<S0, SC, V>;
+  const size_t smem = (size_t)smem_doubles * sizeof(double);
+  if (smem_optin((const void*)kern, (int)smem) != cudaSuccess)
+    return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the batch kernel's shared memory limit");
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBatchThreads, smem) != cudaSuccess || per_sm < 1)
+    return ctx->fail(VFLIP_ERR_CUDA, "the batch kernel cannot be resident");
+  if (ctx->cfg.batch_ctas_per_sm > 0) per_sm = std::min(per_sm, ctx->cfg.batch_ctas_per_sm);
+  const int grid = per_sm * ctx->num_sms;
+  // the launch, captured into a graph (a cooperative kernel node) on a private stream
+  cudaStream_t cs = nullptr;
+  VF_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  auto done = [&](int code) {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(cs);
+    return code;
+  };
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(grid);
+  lc.blockDim = dim3(kBatchThreads);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = cs;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  lc.attrs = at;
+  lc.numAttrs = 1;
+  if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+    return done(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamBeginCapture (batch)"));
+  const cudaError_t le = cudaLaunchKernelEx(&lc, kern, (const BatchSys<S0, SC, V>*)dsys, plan);
+  const cudaError_t ce = cudaStreamEndCapture(cs, &graph);
+  if (le != cudaSuccess || ce != cudaSuccess)
+    return done(ctx->fail(VFLIP_ERR_CUDA, "capturing the persistent batch kernel: %s",
+                          cudaGetErrorString(le != cudaSuccess ? le : ce)));
+  if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+    return done(ctx->fail(VFLIP_ERR_CUDA, "cudaGraphInstantiate (batch)"));
+  *taken = true;
+  VF_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+  if (cudaGraphLaunch(exec, ctx->stream) != cudaSuccess)
+    return done(ctx->fail(VFLIP_ERR_CUDA, "cudaGraphLaunch (batch)"));
+  VF_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+  if (cudaEventSynchronize(ctx->ev1) != cudaSuccess) return done(ctx->fail(VFLIP_ERR_CUDA, "persistent batch failed"));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  ctx->last_ms = ms;
+  ctx->launches += 1;
+  int status = VFLIP_OK;
+  for (int i = 0; i < nsys; ++i) {
+    PcgScalars h;
+    int itst[2] = {0, 0};
+    if (cudaMemcpy(&h, desc[i].st, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(itst, items[i].it, sizeof itst, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return done(ctx->fail(VFLIP_ERR_CUDA, "reading the batched results failed"));
+    const bool conv = itst[1] == 0 && h.converged != 0;
+    if (!conv) status = VFLIP_NOT_CONVERGED;
+    if (stats) {
+      stats[i].iterations = itst[1] == 2 ? 0 : itst[0];
+      stats[i].vcycles = itst[0] + (itst[1] == 2 ? 1 : 0);
+      stats[i].levels = desc[i].nl;
+      stats[i].converged = conv ? 1 : 0;
+      stats[i].residual = h.res;
+      stats[i].rhs_norm = h.rhs_norm;
+      stats[i].solve_ms = ms;
+    }
+  }
+  return done(status);
+}
+
 }  // namespace
+
+// ============================================================== C ABI}  // namespace
 
 // ============================================================== C ABI
 extern "C" {
@@ -1740,8 +2011,10 @@ void vflip_config_default(vflip_config* cfg) {
   cfg->smoother_prefetch = 0;
   cfg->coarsest_solver = 0;
   cfg->spmv_kernel = 0;
-  cfg->advect_kernel = 0;
   cfg->pcg_loop = 0;
+  cfg->pcg_vectors = 0;
+  cfg->batch_chunk = 0;
+  cfg->batch_ctas_per_sm = 0;
 }
 
 int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
@@ -1773,8 +2046,8 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
       (ctx->cfg.smoother_threads != 0 && ctx->cfg.smoother_threads != kTmaBlock &&
        ctx->cfg.smoother_threads != kTmaBlockWide) ||
       ctx->cfg.coarsest_solver < 0 || ctx->cfg.coarsest_solver > 2 || ctx->cfg.spmv_kernel < 0 ||
-      ctx->cfg.spmv_kernel > 1 || ctx->cfg.advect_kernel < 0 || ctx->cfg.advect_kernel > 1 ||
-      ctx->cfg.pcg_loop < 0 || ctx->cfg.pcg_loop > 1)
+      ctx->cfg.spmv_kernel > 1 ||
+      ctx->cfg.pcg_loop < 0 || ctx->cfg.pcg_loop > 1 || ctx->cfg.pcg_vectors < 0 || ctx->cfg.pcg_vectors > 1 || ctx->cfg.batch_chunk < 0 || ctx->cfg.batch_ctas_per_sm < 0)
     return bad(VFLIP_ERR_ARG);
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);
@@ -2143,10 +2416,36 @@ int vflip_batched_solve(vflip_ctx* ctx, int nsys, const vflip_system* systems, d
       for (int i = 0; i < nsys; ++i) stats[i].solve_ms = ms;
     return status;
   }
-  if (mode != VFLIP_BATCH_GRAPH) return ctx->fail(VFLIP_ERR_ARG, "unknown batch mode %d", mode);
+  if (mode != VFLIP_BATCH_GRAPH && mode != VFLIP_BATCH_PERSISTENT)
+    return ctx->fail(VFLIP_ERR_ARG, "unknown batch mode %d", mode);
   cudaEvent_t a;
   VF_CUDA(cudaEventCreate(&a));
   cudaEventRecord(a, ctx->stream);
+  if (mode == VFLIP_BATCH_PERSISTENT && ctx->cfg.precision != VFLIP_PREC_FP64) {
+    bool taken = false;
+    if (ctx->cfg.precision == VFLIP_PREC_FP32)
+      rc = batched_persistent<float, float, float>(ctx, nsys, systems, tolerance_factor, max_iterations, stats, "f32",
+                                                   &taken);
+    else
+      rc = batched_persistent<float, __nv_bfloat16, float>(ctx, nsys, systems, tolerance_factor, max_iterations,
+                                                           stats, "mix", &taken);
+    if (rc < 0 || taken) {
+      if (rc >= 0 && stats) {
+        // stats: the whole call, set-up included; vflip_last_ms keeps the kernel's graph launch
+        cudaEvent_t b;
+        float ms = 0.0f;
+        if (cudaEventCreate(&b) == cudaSuccess) {
+          cudaEventRecord(b, ctx->stream);
+          cudaEventSynchronize(b);
+          cudaEventElapsedTime(&ms, a, b);
+          cudaEventDestroy(b);
+        }
+        for (int i = 0; i < nsys; ++i) stats[i].solve_ms = ms;
+      }
+      cudaEventDestroy(a);
+      return rc;
+    }
+  }
   switch (ctx->cfg.precision) {
     case VFLIP_PREC_FP64:
       rc = batched_graph<double, double, double>(ctx, nsys, systems, tolerance_factor, max_iterations, stats, "f64");
@@ -2222,35 +2521,16 @@ int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, fl
   GridView gf{field, fnx, fny, fnz, (double)h, ox, oy, oz, ih};
   GridView gf2{field2, fnx, fny, fnz, (double)h, ox, oy, oz, ih};
   size_t n = (size_t)fnx * fny * fnz;
-  if (ctx->cfg.advect_kernel == 0) {
-    // the field is one of the velocity grids (self-advection): its window is shared
-    auto same = [&](const GridView& g) {
-      return g.d == field && g.nx == fnx && g.ny == fny && g.nz == fnz && g.ox == ox && g.oy == oy && g.oz == oz;
-    };
-    int fsrc = !field2 && same(gu) ? 0 : (!field2 && same(gv) ? 1 : (!field2 && same(gw) ? 2 : 3));
-    const int windows = fsrc < 3 ? 3 : (field2 ? 5 : 4);
-    const size_t smem = (size_t)windows * kAdvWin * sizeof(float);
-    auto kern = ctx->cfg.precision == VFLIP_PREC_FP64 ? advect_rk2_tile_kernel<true> : advect_rk2_tile_kernel<false>;
-    if (smem_optin((const void*)kern, (int)smem) != cudaSuccess)
-      return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the advection kernel's shared memory limit");
-    // a face grid's last node along x rides with the previous tile
-    const int tiles_x = std::max(1, (fnx - 1 + kAdvTX - 1) / kAdvTX);
-    dim3 grid(tiles_x, (fny + kAdvTY - 1) / kAdvTY, (fnz + kAdvTZ - 1) / kAdvTZ);
-    const int slot = prof_start(ctx, VFLIP_PROF_ADVECT_FIELD, ctx->stream);
-    kern<<<grid, dim3(kAdvTX, kAdvTY), smem, ctx->stream>>>(gu, gv, gw, gf, out, gf2, field2 ? out2 : nullptr, h, dt,
-                                                            fsrc);
-    prof_stop(ctx, slot, ctx->stream);
-    VF_LAUNCH_CHECK();
-    return VFLIP_OK;
-  }
   const int per_block = 256 * 8;
   const unsigned blocks = (unsigned)((n + per_block - 1) / per_block);
+  const int slot = prof_start(ctx, field2 ? VFLIP_PROF_ADVECT_PAIR : VFLIP_PROF_ADVECT_FIELD, ctx->stream);
   if (ctx->cfg.precision == VFLIP_PREC_FP64)
     advect_rk2_kernel<true><<<blocks, 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2, field2 ? out2 : nullptr, h, dt,
                                                            per_block);
   else
     advect_rk2_kernel<false><<<blocks, 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2, field2 ? out2 : nullptr, h,
                                                             dt, per_block);
+  prof_stop(ctx, slot, ctx->stream);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
 }
@@ -2270,26 +2550,10 @@ int vflip_advect_velocity_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, flo
   for (const float* o : {(const float*)uo, (const float*)vo, (const float*)wo})
     if (o == u || o == v || o == w) return ctx->fail(VFLIP_ERR_ARG, "an output aliases the velocity");
   if (uo == vo || uo == wo || vo == wo) return ctx->fail(VFLIP_ERR_ARG, "outputs alias each other");
-  if (ctx->cfg.advect_kernel != 0) {
-    if ((rc = vflip_advect_rk2_linear(ctx, ni, nj, nk, h, dt, u, v, w, ni + 1, nj, nk, 0.5, 0.0, 0.0, u, uo)) ||
-        (rc = vflip_advect_rk2_linear(ctx, ni, nj, nk, h, dt, u, v, w, ni, nj + 1, nk, 0.0, 0.5, 0.0, v, vo)) ||
-        (rc = vflip_advect_rk2_linear(ctx, ni, nj, nk, h, dt, u, v, w, ni, nj, nk + 1, 0.0, 0.0, 0.5, w, wo)))
-      return rc;
-    return VFLIP_OK;
-  }
-  const double ih = inv_pow2(h);
-  GridView gu{u, ni + 1, nj, nk, (double)h, 0.5, 0.0, 0.0, ih};
-  GridView gv{v, ni, nj + 1, nk, (double)h, 0.0, 0.5, 0.0, ih};
-  GridView gw{w, ni, nj, nk + 1, (double)h, 0.0, 0.0, 0.5, ih};
-  const size_t smem = 3 * (size_t)kAdvWin * sizeof(float);
-  auto kern = ctx->cfg.precision == VFLIP_PREC_FP64 ? advect_vel3_tile_kernel<true> : advect_vel3_tile_kernel<false>;
-  if (smem_optin((const void*)kern, (int)smem) != cudaSuccess)
-    return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the advection kernel's shared memory limit");
-  dim3 grid((ni + kAdvTX - 1) / kAdvTX, (nj + kAdvTY - 1) / kAdvTY, (nk + kAdvTZ - 1) / kAdvTZ);
-  const int slot = prof_start(ctx, VFLIP_PROF_ADVECT_VELOCITY, ctx->stream);
-  kern<<<grid, dim3(kAdvTX, kAdvTY), smem, ctx->stream>>>(gu, gv, gw, uo, vo, wo, h, dt, ni, nj, nk);
-  prof_stop(ctx, slot, ctx->stream);
-  VF_LAUNCH_CHECK();
+  if ((rc = vflip_advect_rk2_linear(ctx, ni, nj, nk, h, dt, u, v, w, ni + 1, nj, nk, 0.5, 0.0, 0.0, u, uo)) ||
+      (rc = vflip_advect_rk2_linear(ctx, ni, nj, nk, h, dt, u, v, w, ni, nj + 1, nk, 0.0, 0.5, 0.0, v, vo)) ||
+      (rc = vflip_advect_rk2_linear(ctx, ni, nj, nk, h, dt, u, v, w, ni, nj, nk + 1, 0.0, 0.0, 0.5, w, wo)))
+    return rc;
   return VFLIP_OK;
 }
 

@@ -68,7 +68,8 @@ class Solver:
     def __init__(self, precision=1, pre_sweeps=4, post_sweeps=4, coarse_sweeps=0, coarsest_max_unknowns=0,
                  device=0, stream=None, sweep_kernel=0, smoother_depth=0, smoother_tile_rows=0,
                  smoother_plane_ranges=0, smoother_ctas_per_sm=0, smoother_threads=0,
-                 smoother_prefetch=0, coarsest_solver=0, spmv_kernel=0, advect_kernel=0, pcg_loop=0):
+                 smoother_prefetch=0, coarsest_solver=0, spmv_kernel=0, pcg_loop=0, pcg_vectors=0,
+                 batch_chunk=0, batch_ctas_per_sm=0):
         self.lib = load()
         cfg = ConfigC()
         self.lib.vflip_config_default(C.byref(cfg))
@@ -87,8 +88,10 @@ class Solver:
         cfg.smoother_prefetch = smoother_prefetch
         cfg.coarsest_solver = coarsest_solver
         cfg.spmv_kernel = spmv_kernel
-        cfg.advect_kernel = advect_kernel
         cfg.pcg_loop = pcg_loop
+        cfg.pcg_vectors = pcg_vectors
+        cfg.batch_chunk = batch_chunk
+        cfg.batch_ctas_per_sm = batch_ctas_per_sm
         self.device = torch.device("cuda", device)
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
@@ -228,7 +231,7 @@ class Solver:
     def batched_solve(self, systems, tolerance_factor=1e-6, max_iterations=50, mode=0):
         """vflip_batched_solve over [(stencil[4, nk, nj, ni] float64, rhs[nk, nj, ni] float64), ...]
         (device tensors).  mode 0: one CUDA graph with device-side loops;
-        1: one system after another.  Returns (all_converged, [pressure], [SolveStats])."""
+        1: one system after another; 2: one persistent cooperative kernel.  Returns (all_converged, [pressure], [SolveStats])."""
         n = len(systems)
         arr = (SystemC * max(n, 1))()
         results = []
@@ -301,7 +304,7 @@ class Solver:
         return out, out2
 
     def advect_velocity_rk2_linear(self, ni, nj, nk, h, dt, u, v, w, outs=None):
-        """SubDomainSolver::advect_field of u, v and w through themselves, one launch."""
+        """SubDomainSolver::advect_field of u, v and w through themselves, one call."""
         outs = tuple(torch.empty_like(a) for a in (u, v, w)) if outs is None else outs
         self._check(self.lib.vflip_advect_velocity_rk2_linear(self.ctx, ni, nj, nk, float(h), float(dt), _p(u), _p(v),
                                                               _p(w), *[_p(o) for o in outs]))
@@ -548,7 +551,7 @@ class Solver:
         self._check(self.lib.vflip_profile_sweeps(self.ctx, C.byref(n), C.byref(ms), C.byref(cells)))
         return n.value, ms.value, cells.value
 
-    PROF_KINDS = {"fine_sweep": 0, "spmv": 1, "update": 2, "advect_velocity": 3, "advect_field": 4}
+    PROF_KINDS = {"fine_sweep": 0, "spmv": 1, "update": 2, "advect_field": 3, "advect_pair": 4}
 
     def profile_kernels(self, kind):
         """(launches, total_ms) of the timed launches of one kind (PROF_KINDS)."""

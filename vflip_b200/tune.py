@@ -1,6 +1,13 @@
-"""Autotuner for the smoother kernel and its tile shape.
+"""Autotuners: the smoother kernel and its tile shape, and the persistent
+batched solve's work items.
 
     python -m vflip_b200.tune [--n 256] [--out vflip_b200/tuning.json]
+
+Batched solves (VFLIP_BATCH_PERSISTENT): tune_batch times the persistent
+kernel on a batch under each (cells per work item, CTAs per SM) candidate and
+records the fastest per batch signature (precision + sorted sides) in a JSON
+cache (BATCH_CACHE, or $VFLIP_BATCH_TUNE); tuned_batch_kwargs returns the
+recorded choice as Solver keyword arguments.
 
 For one grid size it times plain-FP32 MGPCG solves of the plume operator
 (box walls + sphere obstacle) under each candidate - smoother kernel
@@ -89,6 +96,60 @@ def measure(st, rhs, shape, reps=2, precision=1):
         s.set_profiling(False)
     return {"shape": list(shape), "sweep_ms": ms / max(nl, 1), "solve_ms": tot / reps, "sweeps": nl,
             "gbs": 28 * cells / (ms / max(nl, 1)) / 1e6 if nl else None}
+
+
+BATCH_CACHE = os.environ.get("VFLIP_BATCH_TUNE", os.path.join(HERE, "batch_tuning.json"))
+BATCH_CANDIDATES = [(chunk, ctas) for chunk in (1024, 2048, 4096, 8192, 16384) for ctas in (0, 1, 2)]
+
+
+def batch_key(precision, sides):
+    return f"p{int(precision)}:" + ",".join(str(int(x)) for x in sorted(sides))
+
+
+def load_batch_cache(path=None):
+    path = path or BATCH_CACHE
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
+def tuned_batch_kwargs(precision, sides, path=None):
+    """Solver keyword arguments recorded for this batch signature (empty if none)."""
+    e = load_batch_cache(path).get(batch_key(precision, sides))
+    return dict(batch_chunk=e["chunk"], batch_ctas_per_sm=e["ctas_per_sm"]) if e else {}
+
+
+def tune_batch(systems, sides, precision=1, tol=1e-6, maxit=100, reps=1, candidates=None, path=None):
+    """Times VFLIP_BATCH_PERSISTENT on `systems` (the (stencil, rhs) device
+    pairs of Solver.batched_solve) under each (chunk, CTAs per SM)
+    candidate - the whole call, hierarchy set-up included, best of `reps`
+    after one untimed call - and records the fastest for this batch's
+    signature in the JSON cache.  Returns (best entry, all measurements)."""
+    rows = []
+    for chunk, ctas in candidates or BATCH_CANDIDATES:
+        with Solver(precision=precision, batch_chunk=chunk, batch_ctas_per_sm=ctas) as s:
+            ok, _, st = s.batched_solve(systems, tol, maxit, mode=2)
+            best = None
+            for _ in range(reps):
+                ok, _, st = s.batched_solve(systems, tol, maxit, mode=2)
+                ms = st[0].solve_ms if st else 0.0
+                best = ms if best is None else min(best, ms)
+            rows.append({"chunk": chunk, "ctas_per_sm": ctas, "ms": best, "kernel_ms": s.last_ms,
+                         "converged": bool(ok)})
+    good = [r for r in rows if r["converged"]]
+    if not good:
+        return None, rows
+    best = min(good, key=lambda r: r["ms"])
+    path = path or BATCH_CACHE
+    cache = load_batch_cache(path)
+    cache[batch_key(precision, sides)] = best
+    try:
+        with open(path, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+    except OSError:  # a read-only install keeps the choice for this call only
+        pass
+    return best, rows
 
 
 def main():
