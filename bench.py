@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--no-flip", action="store_true", help="skip the FLIP smoke arm")
     ap.add_argument("--no-nested", action="store_true", help="skip the nested-subdomain arm")
     ap.add_argument("--no-precisions", action="store_true", help="skip the fp64/mixed plain arms")
-    ap.add_argument("--learned-level", type=int, default=1)
+    ap.add_argument("--learned-level", type=int, default=2)
+    ap.add_argument("--learned-sweeps", type=int, default=2)
     ap.add_argument("--learned-capture", type=int, default=40)
     ap.add_argument("--learned-epochs", type=int, default=16)
     ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds for the reference arm's timed steps")
@@ -302,17 +303,22 @@ def run_vflip(a):
 
 
 def learned_arm(a, sim, solver):
-    """The learned-preconditioned arm on the same plume: capture the next
-    `learned_capture` plain projections as training triples, train the U-Net
-    on the GPU (untimed), then time `steps` learned steps and, right after,
-    `steps` plain steps from the state they reached (CUDA events, same
-    windowing as the headline)."""
+    """The learned arm on the same plume: the network corrects the previous
+    pressure from its residual (VFLIP_LEARNED_RESID).  The next
+    `learned_capture` projections run plain MGPCG and record training
+    triples; the U-Net trains on the GPU (untimed); then `steps` steps each
+    of three projections from the same states, interleaved step by step so
+    that all three see the same flow: plain MGPCG from zero (the
+    reference's solve), the warm start alone (the previous pressure scaled by
+    the Ritz step, no network) and the learned warm start (previous pressure
+    + the network's smoothed correction).  CUDA events around each step."""
     import numpy as np
     import torch
 
-    from vflip_b200.learned import LearnedPreconditioner
+    from vflip_b200.learned import NO_NET, RESID, SOLVE, SWEEPS, LearnedPreconditioner
 
-    pre = LearnedPreconditioner(solver, level=a.learned_level, seed=0, use_vb=False, sweeps=2)
+    lvl = a.learned_level
+    pre = LearnedPreconditioner(solver, level=lvl, seed=0, sweeps=a.learned_sweeps, residual=True)
     for _ in range(a.learned_capture):
         sim.step(pre)
     torch.cuda.synchronize()
@@ -320,32 +326,56 @@ def learned_arm(a, sim, solver):
     losses = pre.train(epochs=a.learned_epochs, lr=1e-3)
     torch.cuda.synchronize()
     train_s = time.time() - t0
-
-    def timed(precond):
-        vc, net_ms, fb = [], [], 0
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record()
-        for _ in range(a.steps):
-            conv, st = sim.step(precond)
-            vc.append(st.vcycles)
-            if precond is not None:
-                net_ms.append(precond.last.net_ms)
-                fb += int(precond.last.fallback)
-        e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1), vc, net_ms, fb
-
-    ms_l, vc_l, net_ms, fb = timed(pre)
-    ms_p, vc_p, _, _ = timed(None)
-    return {"steps_per_s": a.steps / (ms_l * 1e-3), "vcycles_mean": float(np.mean(vc_l)),
-            "plain_steps_per_s_adjacent": a.steps / (ms_p * 1e-3), "plain_vcycles_mean_adjacent": float(np.mean(vc_p)),
-            "vcycle_ratio_learned_over_plain": float(np.mean(vc_l) / np.mean(vc_p)),
-            "steps_per_s_ratio_learned_over_plain": ms_p / ms_l, "network_ms_mean": float(np.mean(net_ms)),
-            "fallbacks": fb, "train_s": train_s, "train_final_loss": losses[-1],
-            "config": {"network_grid_level": a.learned_level, "capture_steps": a.learned_capture,
-                       "epochs": a.learned_epochs, "ritz_subspace": "network warm start + coarse correction (no V(b)), "
-                       "2 smoothing sweeps each", "unet": "4 levels, 16/32/64/128 channels, BF16 tcgen05 convs"}}
+    modes = {"plain": None, "warm_start_only": SOLVE | RESID | NO_NET,
+             "learned": SOLVE | RESID | SWEEPS(a.learned_sweeps)}
+    res = {k: {"ms": [], "vc": [], "it": [], "net_ms": [], "fb": 0} for k in modes}
+    for _ in range(a.steps):
+        sim.advect_and_force()
+        u0 = {k: sim.f[k].clone() for k in ("u", "v", "w")}
+        p0 = sim.pressure.clone()
+        out = {}
+        for name, mode in modes.items():
+            for k in u0:
+                sim.f[k].copy_(u0[k])
+            sim.pressure.copy_(p0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            if mode is None:
+                conv, _, st = sim.project()
+            else:
+                conv, _, st, ls = sim.project_learned(pre.net, mode, lvl)
+                res[name]["net_ms"].append(ls.net_ms)
+                res[name]["fb"] += int(ls.fallback)
+            e1.record()
+            torch.cuda.synchronize()
+            res[name]["ms"].append(e0.elapsed_time(e1))
+            res[name]["vc"].append(st.vcycles)
+            res[name]["it"].append(st.iterations)
+            out[name] = {k: sim.f[k].clone() for k in ("u", "v", "w")}, sim.pressure.clone()
+        # the state continues from the learned projection
+        for k in u0:
+            sim.f[k].copy_(out["learned"][0][k])
+        sim.pressure.copy_(out["learned"][1])
+    # the rest of a step (advection, sources) is the same in every arm: the
+    # plain step's time from the headline split into advection and projection
+    summ = {k: {"projection_ms_mean": float(np.mean(v["ms"])), "vcycles_mean": float(np.mean(v["vc"])),
+                "pcg_iterations_mean": float(np.mean(v["it"])),
+                "network_ms_mean": float(np.mean(v["net_ms"])) if v["net_ms"] else 0.0, "fallbacks": v["fb"]}
+            for k, v in res.items()}
+    pl, ws, ln = summ["plain"], summ["warm_start_only"], summ["learned"]
+    return {"arms": summ,
+            "vcycle_ratio_learned_over_plain": ln["vcycles_mean"] / pl["vcycles_mean"],
+            "projection_speedup_learned_over_plain": pl["projection_ms_mean"] / ln["projection_ms_mean"],
+            "vcycle_ratio_learned_over_warm_start_only": ln["vcycles_mean"] / ws["vcycles_mean"],
+            "projection_speedup_learned_over_warm_start_only": ws["projection_ms_mean"] / ln["projection_ms_mean"],
+            "train_s": train_s, "train_final_loss": losses[-1], "train_first_loss": losses[0],
+            "config": {"network_grid_level": lvl, "capture_steps": a.learned_capture, "epochs": a.learned_epochs,
+                       "smoothing_sweeps": a.learned_sweeps,
+                       "network": "4-level U-Net, 16/32/64/128 channels, BF16 tcgen05 convolutions",
+                       "input": "residual of the previous pressure (level-L block averages) + fluid fraction",
+                       "output": "correction of the previous pressure (Ritz-weighted with it)",
+                       "steps": a.steps}}
 
 
 def flip_arm(solver, steps, n=128, warmup=3):

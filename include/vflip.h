@@ -610,6 +610,11 @@ int vflip_unet_set_output_scale(vflip_unet* net, float s0, float s1);
 #define VFLIP_LEARNED_PREV 8    /* add the incoming pressure (previous solve) to the Ritz subspace */
 #define VFLIP_LEARNED_NO_NET 16 /* leave the network out (ablation; net may be NULL) */
 #define VFLIP_LEARNED_SWEEPS(k) ((k) << 8) /* k (0-15) smoothing sweeps on each network vector */
+#define VFLIP_LEARNED_RESID 32  /* warm-start correction: the network maps the residual r0 = b - A p of the
+                                   previous pressure p (the pressure array on entry) to a correction of p; capture
+                                   records (r0 features, R^L(p_new - p)); solve takes the energy-optimal
+                                   combination of p and the smoothed correction (p alone with NO_NET), then PCG
+                                   with the plain V-cycle; needs FP64 PCG vectors (pcg_vectors = 0) */
 
 typedef struct vflip_learned_stats {
   int fallback;          /* 1: the learned iteration stalled; plain MGPCG solved from zero */

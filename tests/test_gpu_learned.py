@@ -142,3 +142,76 @@ def test_training_improves_the_warm_start():
                 vv.append(st.vcycles)
     assert np.mean(r_tr) < 0.6 * np.mean(r_un), (r_tr, r_un)
     assert np.mean(vc_tr) <= np.mean(vc_un), (vc_tr, vc_un)
+
+
+# ---- the warm-start correction (VFLIP_LEARNED_RESID)
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_resid_capture_is_the_plain_solve(prec):
+    """Capture in residual mode solves like the plain projection (same bits)
+    and records target = R^L (p_new - p_prev) scaled like the features."""
+    from vflip_b200.learned import RESID
+
+    s, sim = _state(prec)
+    p_prev = sim.pressure.clone()
+    u0 = {k: sim.f[k].clone() for k in ("u", "v", "w")}
+    conv, p_plain, st = sim.project()
+    p_plain = p_plain.clone()
+    for k in u0:
+        sim.f[k].copy_(u0[k])
+    sim.pressure.copy_(p_prev)
+    n = sim.p.n
+    X, Y, Z = s.learned_grid(n, n, n, 1)
+    smp = (torch.empty((Z, Y, X, 2), device="cuda"), torch.empty((Z, Y, X, 2), device="cuda"),
+           torch.empty((Z, Y, X), device="cuda"))
+    conv2, p2, st2, _ = sim.project_learned(None, CAPTURE | RESID, 1, sample=smp)
+    assert conv and conv2 and st2.iterations == st.iterations
+    assert torch.equal(p2, p_plain)
+    in2, t2, w = (x.cpu().numpy() for x in smp)
+    assert np.abs(in2[..., 0]).max() == pytest.approx(1.0)
+    d = (p_plain - p_prev).cpu().numpy()
+    pad = np.zeros((Z * 2, Y * 2, X * 2))
+    pad[:n, :n, :n] = d
+    avg = pad.reshape(Z, 2, Y, 2, X, 2).mean(axis=(1, 3, 5))
+    m = np.abs(avg) > 1e-3 * np.abs(avg).max()
+    ratio = t2[..., 0][m] / avg[m]
+    assert np.allclose(ratio, ratio.mean(), rtol=1e-4)
+    assert np.array_equal(t2[..., 0], t2[..., 1])
+
+
+@pytest.mark.parametrize("prec,net_on,sweeps", [(1, False, 0), (1, True, 2), (2, True, 2), (0, True, 0)])
+def test_resid_solve_converges_to_plain_answer(prec, net_on, sweeps):
+    """Whatever the network says (here an untrained one), the residual-mode
+    solve reaches the plain solve's tolerance and answer (both with FP64
+    PCG vectors, so they agree to the tolerance, not to FP32 rounding)."""
+    from vflip_b200.learned import NO_NET, RESID, SWEEPS
+
+    s, sim = _state(prec)
+    p_prev = sim.pressure.clone()
+    u0 = {k: sim.f[k].clone() for k in ("u", "v", "w")}
+    _, p_plain, st = sim.project()
+    p_plain = p_plain.clone()
+    for k in u0:
+        sim.f[k].copy_(u0[k])
+    sim.pressure.copy_(p_prev)
+    with UNet(seed=7) as net:
+        mode = SOLVE | RESID | SWEEPS(sweeps) | (0 if net_on else NO_NET)
+        conv, p, st2, ls = sim.project_learned(net if net_on else None, mode, 1)
+    assert conv and st2.converged
+    assert st2.residual <= 1e-6 * st2.rhs_norm
+    assert _rel(p, p_plain) < 2e-5
+    assert (ls.net_ms > 0) == net_on
+    if not net_on:
+        assert ls.gamma[1] == 0
+
+
+def test_resid_mode_needs_fp64_vectors():
+    from vflip_b200._lib import VflipError
+    from vflip_b200.learned import NO_NET, RESID
+    from vflip_b200.solver import Solver
+
+    s = Solver(precision=1, pcg_vectors=1)
+    sim = PlumeSim(s, PlumeParams(n=24, dt=0.02))
+    sim.advect_and_force()
+    with pytest.raises(VflipError):
+        sim.project_learned(None, SOLVE | RESID | NO_NET, 1)

@@ -225,6 +225,77 @@ __global__ void __launch_bounds__(BLOCK) ritz_combine_kernel(const RitzVecs<V> v
   finish_reduction<BLOCK>(partials, gridDim.x, st, kReduceRes, 0.0, gridDim.x);
 }
 
+// ---- the warm-start correction (residual mode): the previous pressure p
+// and the network's correction e of its residual r0 = b - A p.
+
+// r -= q (r0 = b - A p in place of r = b), its copy rv in the V-cycle's type
+template <typename V>
+__global__ void resid_sub_kernel(double* __restrict__ r, const double* __restrict__ q, V* __restrict__ rv, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double v = r[i] - q[i];
+    r[i] = v;
+    rv[i] = cvt<V>((typename Num<V>::Acc)v);
+  }
+}
+
+// FP64 block partials of the 2 x 2 Ritz system over {p, e}: p.Ap, p.Ae,
+// e.Ae, p.b, e.b, written as partials[k * gridDim.x + block]
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) ritz2_dots_kernel(const double* __restrict__ p, const double* __restrict__ ap,
+                                                           const double* __restrict__ e, const double* __restrict__ ae,
+                                                           const double* __restrict__ b, size_t n, double* partials) {
+  __shared__ double sm[BLOCK / 32];
+  double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK) {
+    const double pv = __ldg(p + i), ev = __ldg(e + i), bv = __ldg(b + i), aev = __ldg(ae + i);
+    s[0] += pv * __ldg(ap + i);
+    s[1] += pv * aev;
+    s[2] += ev * aev;
+    s[3] += pv * bv;
+    s[4] += ev * bv;
+  }
+  for (int k = 0; k < 5; ++k) {
+    const double t = block_sum<BLOCK>(s[k], sm);
+    if (threadIdx.x == 0) partials[(size_t)k * gridDim.x + blockIdx.x] = t;
+  }
+}
+
+template <int BLOCK>
+__global__ void ritz2_fold_kernel(const double* __restrict__ partials, int nb, double* __restrict__ out) {
+  __shared__ double sm[BLOCK / 32];
+  for (int k = 0; k < 5; ++k) {
+    double v = 0.0;
+    for (int q = threadIdx.x; q < nb; q += BLOCK) v += partials[(size_t)k * nb + q];
+    v = block_sum<BLOCK>(v, sm);
+    if (threadIdx.x == 0) out[k] = v;
+  }
+}
+
+// x = g0 p + g1 e, r = b - g0 Ap - g1 Ae, rv = r in V, partial |r|_inf
+// (the converged flag against the tolerance set by the last block)
+template <typename V, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) ritz2_combine_kernel(const double* __restrict__ p,
+                                                              const double* __restrict__ ap,
+                                                              const double* __restrict__ e,
+                                                              const double* __restrict__ ae,
+                                                              const double* __restrict__ b, double g0, double g1,
+                                                              double* __restrict__ x, double* __restrict__ r,
+                                                              V* __restrict__ rv, size_t n, double* partials,
+                                                              PcgScalars* st) {
+  __shared__ double sm[BLOCK / 32];
+  double m = 0.0;
+  for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK) {
+    x[i] = g0 * __ldg(p + i) + g1 * __ldg(e + i);
+    const double rr = __ldg(b + i) - (g0 * __ldg(ap + i) + g1 * __ldg(ae + i));
+    r[i] = rr;
+    rv[i] = cvt<V>((typename Num<V>::Acc)rr);
+    m = fmax(m, fabs(rr));
+  }
+  const double bm = block_absmax<BLOCK>(m, sm);
+  if (threadIdx.x == 0) partials[blockIdx.x] = bm;
+  finish_reduction<BLOCK>(partials, gridDim.x, st, kReduceRes, 0.0, gridDim.x);
+}
+
 // x += alpha s; r_out = r_in - alpha q (r_in kept for the Polak-Ribiere beta)
 template <typename T, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) fcg_update_kernel(T* __restrict__ x, const T* __restrict__ r_in,

@@ -1126,11 +1126,13 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
 }
 
 // AMGPCGSolve (AlgebraicMultigrid.h:189-301) with the outer vectors in W.
+// warm: the caller has set x (the result), r, its V copy and the scalars
+// (tolerance from |rhs|_inf, |r|_inf of the initial guess); host loop.
 template <typename W, typename S0, typename SC, typename V>
 int pcg_solve_w(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor,
-                int maxit, vflip_solve_stats* stats, V* x1_out) {
+                int maxit, vflip_solve_stats* stats, V* x1_out, bool warm = false) {
   constexpr bool same = std::is_same<W, V>::value;
-  if (ctx->cfg.pcg_loop == 0 && !ctx->profiling && !x1_out) {
+  if (ctx->cfg.pcg_loop == 0 && !ctx->profiling && !x1_out && !warm) {
     bool done = false;
     const int grc = pcg_solve_graph<W>(ctx, T, rhs, result, tol_factor, maxit, stats, &done);
     if (grc < 0 || done) return grc;
@@ -1140,13 +1142,15 @@ int pcg_solve_w(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* 
   OuterVecs<W, V> o;
   int rc;
   if ((rc = outer_vecs<W>(ctx, T, result, o))) return rc;
-  VF_CUDA(cudaMemsetAsync(ctx->st, 0, sizeof(PcgScalars), ctx->stream));
   const int gb = grid_for(n, kRedBlock, ctx->num_sms);
-  launch_pcg_init(ctx, ctx->stream, o, rhs, n, tol_factor);
-  VF_LAUNCH_CHECK();
+  if (!warm) {
+    VF_CUDA(cudaMemsetAsync(ctx->st, 0, sizeof(PcgScalars), ctx->stream));
+    launch_pcg_init(ctx, ctx->stream, o, rhs, n, tol_factor);
+    VF_LAUNCH_CHECK();
+  }
   if ((rc = read_scalars(ctx))) return rc;
   PcgScalars& h = *ctx->st_host;
-  const double rhs_norm = h.res;
+  const double rhs_norm = warm ? h.rhs_norm : h.res;
   int iterations = 0, vcycles = 0;
   double residual = h.res;
   auto finish = [&](int st_code) -> int {
@@ -1166,7 +1170,7 @@ int pcg_solve_w(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* 
     }
     return st_code;
   };
-  if (h.res == 0.0) {  // AlgebraicMultigrid.h:214-232
+  if (h.res == 0.0 || (warm && h.converged)) {  // AlgebraicMultigrid.h:214-232
     iterations = 0;
     return finish(VFLIP_OK);
   }
@@ -1565,6 +1569,179 @@ int learned_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double
   return fallback();
 }
 
+// ---- the warm-start correction (VFLIP_LEARNED_RESID).  The previous
+// pressure p (the result array on entry) is the warm start; the network maps
+// its residual r0 = b - A p (features on the level-L grid) to a correction e
+// of p; a Ritz step takes x0 = g0 p + g1 e with the energy-optimal g, and
+// PCG with the plain V-cycle continues from x0 to |r|_inf <= tol |b|_inf (the
+// outer vectors in FP64).  Without the network (NO_NET) the Ritz step scales
+// p alone.  A solve that does not converge is repeated by plain MGPCG from
+// zero.
+template <typename S0, typename SC, typename V>
+int learned_resid_prep(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor,
+                       OuterVecs<double, V>& o, double** pp_out, double** q1_out) {
+  const Dims d = T.fine.d;
+  const size_t n = d.n();
+  int rc;
+  if ((rc = outer_vecs<double>(ctx, T, result, o))) return rc;
+  double *pp, *q1;
+  VF_ALLOC(pp, double, "lrn_pp", n);
+  VF_ALLOC(q1, double, "lrn_q1", n);
+  const int g = grid_for(n, 256, ctx->num_sms);
+  VF_CUDA(cudaMemcpyAsync(pp, result, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  VF_CUDA(cudaMemsetAsync(ctx->st, 0, sizeof(PcgScalars), ctx->stream));
+  launch_pcg_init(ctx, ctx->stream, o, rhs, n, tol_factor);  // r = b, x = 0, tolerance from |b|
+  VF_LAUNCH_CHECK();
+  spmv_kernel<double, double><<<g, 256, 0, ctx->stream>>>(pp, q1, T.d64, T.x64, T.y64, T.z64, d.ni, d.nj, d.nk);
+  VF_LAUNCH_CHECK();
+  resid_sub_kernel<V><<<g, 256, 0, ctx->stream>>>(o.r, q1, o.rv, n);  // r0 = b - A p
+  VF_LAUNCH_CHECK();
+  *pp_out = pp;
+  *q1_out = q1;
+  return VFLIP_OK;
+}
+
+template <typename S0, typename SC, typename V>
+int learned_resid_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor,
+                        int maxit, vflip_solve_stats* stats, const LearnedOpts& lo) {
+  const Dims d = T.fine.d;
+  const size_t n = d.n();
+  int rc;
+  OuterVecs<double, V> o;
+  double *pp, *q1;
+  if ((rc = learned_resid_prep(ctx, T, rhs, result, tol_factor, o, &pp, &q1))) return rc;
+  vflip_learned_stats ls{};
+  const bool use_net = !(lo.mode & VFLIP_LEARNED_NO_NET);
+  const int g = grid_for(n, 256, ctx->num_sms);
+  double *e, *q2, *dots;
+  VF_ALLOC(e, double, "lrn_e", n);
+  VF_ALLOC(q2, double, "lrn_q2", n);
+  VF_ALLOC(dots, double, "lrn_dots", 8);
+  if (use_net) {
+    int X, Y, Z;
+    learned_grid_dims(d.ni, d.nj, d.nk, lo.level, X, Y, Z);
+    const size_t nv = (size_t)X * Y * Z;
+    float *in2, *out2, *mc;
+    double* scale;
+    V *ev, *et;
+    VF_ALLOC(in2, float, "lrn_in2", 2 * nv);
+    VF_ALLOC(out2, float, "lrn_out2", 2 * nv);
+    VF_ALLOC(ev, V, "lrn_ev", n);
+    VF_ALLOC(et, V, "lrn_et", n);
+    if ((rc = learned_features(ctx, lo, d, o.r, X, Y, Z, in2, &mc, &scale))) return rc;
+    vflip::unet::Net& net = *lo.net;
+    const cudaStream_t saved = net.stream;
+    net.stream = ctx->stream;
+    cudaEvent_t na, nb;
+    VF_CUDA(cudaEventCreate(&na));
+    VF_CUDA(cudaEventCreate(&nb));
+    cudaEventRecord(na, ctx->stream);
+    rc = net.forward(X, Y, Z, in2, out2);
+    cudaEventRecord(nb, ctx->stream);
+    if (!rc) rc = net.sync_error();
+    net.stream = saved;
+    if (!rc) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, na, nb);
+      ls.net_ms = ms;
+    }
+    cudaEventDestroy(na);
+    cudaEventDestroy(nb);
+    if (rc) return ctx->fail(rc, "network: %s", net.err.c_str());
+    prolong_trilinear_kernel<V><<<g, 256, 0, ctx->stream>>>(out2, 0, X, Y, Z, lo.level, scale, net.out_scale[0],
+                                                            T.d64, ev, d.ni, d.nj, d.nk);
+    VF_LAUNCH_CHECK();
+    // red-black sweeps on A e = r0 damp the rough error of the interpolated prediction
+    const int ksw = (lo.mode >> 8) & 15;
+    V *src = ev, *dst = et;
+    for (int k = 0; k < ksw; ++k) {
+      if ((rc = sweep<S0, V>(ctx, T.fine, o.rv, src, dst, nullptr, nullptr, nullptr))) return rc;
+      std::swap(src, dst);
+    }
+    to_double_kernel<V, kRedBlock><<<grid_for(n, kRedBlock, ctx->num_sms), kRedBlock, 0, ctx->stream>>>(src, e, n);
+    VF_LAUNCH_CHECK();
+    spmv_kernel<double, double><<<g, 256, 0, ctx->stream>>>(e, q2, T.d64, T.x64, T.y64, T.z64, d.ni, d.nj, d.nk);
+    VF_LAUNCH_CHECK();
+  } else {
+    VF_CUDA(cudaMemsetAsync(e, 0, n * sizeof(double), ctx->stream));
+    VF_CUDA(cudaMemsetAsync(q2, 0, n * sizeof(double), ctx->stream));
+  }
+  const int rb = std::min(grid_for(n, kRedBlock, ctx->num_sms), kMaxPartials / 5);
+  ritz2_dots_kernel<kRedBlock><<<rb, kRedBlock, 0, ctx->stream>>>(pp, q1, e, q2, rhs, n, ctx->partials);
+  VF_LAUNCH_CHECK();
+  ritz2_fold_kernel<kRedBlock><<<1, kRedBlock, 0, ctx->stream>>>(ctx->partials, rb, dots);
+  VF_LAUNCH_CHECK();
+  double h5[5];
+  VF_CUDA(cudaMemcpyAsync(h5, dots, sizeof h5, cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  // the 2 x 2 system in ritz_solve's layout (upper G row by row, then W^T b)
+  double full[kRitzSums] = {};
+  full[0] = h5[0];                 // G00
+  full[1] = h5[1];                 // G01
+  full[kRitzVecs] = h5[2];         // G11
+  full[kRitzSums - kRitzVecs] = h5[3];      // g0
+  full[kRitzSums - kRitzVecs + 1] = h5[4];  // g1
+  const bool use[kRitzVecs] = {true, use_net, false, false};
+  ls.subspace = ritz_solve(full, use, ls.gamma);
+  ritz2_combine_kernel<V, kRedBlock><<<grid_for(n, kRedBlock, ctx->num_sms), kRedBlock, 0, ctx->stream>>>(
+      pp, q1, e, q2, rhs, ls.gamma[0], ls.gamma[1], o.x, o.r, o.rv, n, ctx->partials, ctx->st);
+  VF_LAUNCH_CHECK();
+  if ((rc = read_scalars(ctx))) return rc;
+  ls.init_residual = ctx->st_host->res;
+  vflip_solve_stats st2{};
+  rc = std::isfinite(ls.init_residual)
+           ? pcg_solve_w<double>(ctx, T, rhs, result, tol_factor, maxit, &st2, (V*)nullptr, true)
+           : VFLIP_NOT_CONVERGED;
+  if (rc < 0) return rc;
+  if (rc != VFLIP_OK) {  // plain MGPCG from zero decides
+    vflip_solve_stats st3{};
+    const int code = pcg_solve(ctx, T, rhs, result, tol_factor, maxit, &st3);
+    if (code < 0) return code;
+    ls.fallback = 1;
+    st3.iterations += st2.iterations;
+    st3.vcycles += st2.vcycles;
+    st2 = st3;
+    rc = code;
+  }
+  if (stats) *stats = st2;
+  if (lo.lstats) *lo.lstats = ls;
+  return rc;
+}
+
+// Training triple of the warm-start correction: features of r0 = b - A p
+// (p the previous pressure, the result on entry), target R^L (p_new - p) in
+// both output channels, weight R^L fluid; the projection itself is plain
+// MGPCG (the same answer as without capture).
+template <typename S0, typename SC, typename V>
+int learned_resid_capture(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol,
+                          int maxit, vflip_solve_stats* stats, const LearnedOpts& lo) {
+  const Dims d = T.fine.d;
+  const size_t n = d.n();
+  int rc;
+  OuterVecs<double, V> o;
+  double *pp, *q1, *r0;
+  if ((rc = learned_resid_prep(ctx, T, rhs, result, tol, o, &pp, &q1))) return rc;
+  VF_ALLOC(r0, double, "lrn_r0", n);
+  VF_CUDA(cudaMemcpyAsync(r0, o.r, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  const int status = pcg_solve(ctx, T, rhs, result, tol, maxit, stats);
+  if (status < 0) return status;
+  int X, Y, Z;
+  learned_grid_dims(d.ni, d.nj, d.nk, lo.level, X, Y, Z);
+  const size_t nv = (size_t)X * Y * Z;
+  float *mc, *pc;
+  double* scale;
+  if ((rc = learned_features(ctx, lo, d, r0, X, Y, Z, lo.s_in2, &mc, &scale))) return rc;
+  VF_ALLOC(pc, float, "lrn_pc", nv);
+  const int gv = grid_for(nv, 256, ctx->num_sms);
+  block_average_kernel<double, double><<<gv, 256, 0, ctx->stream>>>(result, pp, 2, d.ni, d.nj, d.nk, lo.level, pc,
+                                                                     X, Y, Z);
+  VF_LAUNCH_CHECK();
+  pack2_kernel<<<gv, 256, 0, ctx->stream>>>(pc, pc, scale, 1, lo.s_tgt2, nv);
+  VF_LAUNCH_CHECK();
+  VF_CUDA(cudaMemcpyAsync(lo.s_w, mc, nv * sizeof(float), cudaMemcpyDeviceToDevice, ctx->stream));
+  return status;
+}
+
 int check_dims(vflip_ctx* ctx, int ni, int nj, int nk) {
   if (!ctx) return VFLIP_ERR_ARG;
   if (ni <= 0 || nj <= 0 || nk <= 0) return ctx->fail(VFLIP_ERR_ARG, "grid dimensions must be positive");
@@ -1576,6 +1753,12 @@ int check_dims(vflip_ctx* ctx, int ni, int nj, int nk) {
 template <typename S0, typename SC, typename V>
 int solve_typed(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol, int maxit,
                 vflip_solve_stats* stats, const LearnedOpts* lo) {
+  if (lo && (lo->mode & VFLIP_LEARNED_RESID)) {
+    if (!std::is_same<V, double>::value && ctx->cfg.pcg_vectors != 0)
+      return ctx->fail(VFLIP_ERR_ARG, "the residual mode runs with FP64 PCG vectors (pcg_vectors = 0)");
+    if (lo->mode & VFLIP_LEARNED_SOLVE) return learned_resid_solve(ctx, T, rhs, result, tol, maxit, stats, *lo);
+    return learned_resid_capture(ctx, T, rhs, result, tol, maxit, stats, *lo);
+  }
   if (lo && (lo->mode & VFLIP_LEARNED_SOLVE)) return learned_solve(ctx, T, rhs, result, tol, maxit, stats, *lo);
   if (lo && (lo->mode & VFLIP_LEARNED_CAPTURE)) {
     V* x1;

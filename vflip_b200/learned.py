@@ -118,7 +118,7 @@ class UNet:
         return dw
 
 
-CAPTURE, SOLVE, NO_VB, PREV, NO_NET = 1, 2, 4, 8, 16
+CAPTURE, SOLVE, NO_VB, PREV, NO_NET, RESID = 1, 2, 4, 8, 16, 32
 
 
 def SWEEPS(k):
@@ -136,7 +136,8 @@ class LearnedPreconditioner:
     falls back to plain MGPCG when the residual stalls.
     """
 
-    def __init__(self, solver, level=1, seed=0, net=None, use_vb=True, sweeps=2, use_prev=False, use_net=True):
+    def __init__(self, solver, level=1, seed=0, net=None, use_vb=True, sweeps=2, use_prev=False, use_net=True,
+                 residual=False):
         self.s = solver
         self.level = level
         self.net = net if net is not None else UNet(device=solver.device.index, seed=seed)
@@ -146,6 +147,9 @@ class LearnedPreconditioner:
         self.sweeps = sweeps
         self.use_prev = use_prev
         self.use_net = use_net
+        # residual: the network corrects the previous pressure from its
+        # residual (VFLIP_LEARNED_RESID) instead of predicting the pressure
+        self.residual = residual
         self.sigma = None
         self.last = None
 
@@ -161,7 +165,8 @@ class LearnedPreconditioner:
             sample = (torch.empty((Z, Y, X, 2), dtype=torch.float32, device=dev),
                       torch.empty((Z, Y, X, 2), dtype=torch.float32, device=dev),
                       torch.empty((Z, Y, X), dtype=torch.float32, device=dev))
-            conv, _, st, ls = sim.project_learned(None, CAPTURE, self.level, sample=sample)
+            conv, _, st, ls = sim.project_learned(None, CAPTURE | (RESID if self.residual else 0), self.level,
+                                                  sample=sample)
             self.samples.append(sample)
         else:
             mode = self.mode()
@@ -170,6 +175,8 @@ class LearnedPreconditioner:
         return conv, st
 
     def mode(self):
+        if self.residual:
+            return SOLVE | RESID | (0 if self.use_net else NO_NET) | SWEEPS(self.sweeps)
         return (SOLVE | (0 if self.use_vb else NO_VB) | (PREV if self.use_prev else 0) |
                 (0 if self.use_net else NO_NET) | SWEEPS(self.sweeps))
 
