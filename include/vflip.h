@@ -121,7 +121,8 @@ typedef struct {
    * near 2e-5 |rhs|_inf on the 256^3 plume operator). */
   int pcg_vectors;
   /* VFLIP_BATCH_PERSISTENT work items: cells per (system, level, chunk)
-   * item (0 = automatic, 4096) and resident CTAs per SM of the persistent
+   * item and about the cells of a sweep tile (0 = automatic, 4096) and
+   * resident CTAs per SM of the persistent
    * kernel (0 = as many as fit).  vflip_b200/tune.py picks both per batch. */
   int batch_chunk;
   int batch_ctas_per_sm;

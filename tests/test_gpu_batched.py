@@ -49,7 +49,7 @@ def test_graph_batch_edge_cases():
 
 
 @pytest.mark.parametrize("prec", [1, 2])
-@pytest.mark.parametrize("chunk,ctas", [(0, 0), (1024, 1), (8192, 2)])
+@pytest.mark.parametrize("chunk,ctas", [(0, 0), (1024, 1), (65536, 2)])
 def test_persistent_batch_matches_graph(prec, chunk, ctas):
     from vflip_b200.solver import Solver
 

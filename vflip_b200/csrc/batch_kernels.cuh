@@ -7,17 +7,18 @@
 // of one level of one system - and the CTAs take items grid-stride; a grid
 // barrier separates dependent phases, and every CTA meets every barrier (no
 // CTA leaves the program early).  Per PCG iteration:
-//   V-cycle: for each level l: red pass (the first one with x = 0 folded in:
-//            amgPrecond zero-fills x), black pass, three more sweeps, then
-//            b_{l+1} = R (b_l - A_l x_l); the coarsest level of each system
-//            (one CTA per system: the FP64 band-Cholesky solve, or red-black
-//            sweeps in shared memory); up: x_l += P x_{l+1}, four sweeps;
-//            the last black pass of level 0 also forms z.r (rho, beta);
+//   V-cycle: for each level l: four fused red-black sweeps (sweep tiles of
+//            rows x planes, out of place, the first from x = 0: amgPrecond
+//            zero-fills x), then b_{l+1} = R (b_l - A_l x_l); the coarsest
+//            level of each system (one CTA per system: the FP64
+//            band-Cholesky solve, or red-black sweeps in shared memory); up:
+//            four sweeps, the first on x + P x_{l+1}; the last sweep of
+//            level 0 also forms z.r (rho, beta);
 //   s = z + beta s; q = A s with s.q (alpha); x += alpha s, r -= alpha q
 //   with |r|_inf (the stop test); systems that converged drop out.
-// Red-black Gauss-Seidel is done in place, one colour per pass: the values
-// the fused out-of-place kernels produce (a colour's update reads only the
-// other colour), cell by cell in the reference's term order.
+// A sweep tile follows rbgs_sweep_kernel's schedule and arithmetic, so the
+// V-cycle's values are the single-system kernels' (the reductions are
+// grouped per item instead).
 //
 // Reductions are deterministic: every item writes its partial to a slot of
 // its own, and after the barrier one CTA per system folds that system's
@@ -48,7 +49,9 @@ struct BatchLevel {
   const S* yp;
   const S* zp;
   V* b;  // level rhs (level 0: the PCG residual r)
-  V* x;  // level solution (level 0: z)
+  V* x;  // level solution (level 0: z); every sweep sequence ends here
+  V* t;  // the other buffer of the out-of-place sweeps
+  int tyo, kz, ntj;  // sweep tiles: tyo rows x kz planes, ntj row tiles per plane range
 };
 
 template <typename S0, typename SC, typename V>
@@ -75,12 +78,13 @@ struct BatchPlan {
   // items of each level's cell phases and of the restriction into level
   // l+1, as prefix sums over the systems: the items of system s at level l
   // are [cell_pre[l][s], cell_pre[l][s+1]); a system without that level has none
-  const int* cell_pre;  // [lmax][nsys+1]
-  const int* rest_pre;  // [lmax][nsys+1]
+  const int* cell_pre;   // [lmax][nsys+1] (level 0: the PCG vector phases)
+  const int* rest_pre;   // [lmax][nsys+1]
+  const int* sweep_pre;  // [lmax][nsys+1] sweep tiles of the levels a system smooths
   double* part;         // [nsys][part_stride] reduction slots
   int part_stride;
   int* active;          // [2] systems still iterating, alternating per iteration
-  int smem_doubles;     // dynamic shared memory of the coarsest phase
+  int smem_doubles;     // dynamic shared memory (doubles): the sweeps' plane window, the coarsest phase
 };
 
 // the system whose item range holds `item` (pre is non-decreasing)
@@ -99,39 +103,93 @@ __device__ __forceinline__ bool batch_live(const BatchSys<S0, SC, V>& y) {
   return __ldcg(y.state) == 1;
 }
 
-// One red-black colour pass over the cells [c0, c1) of a level, in place.
-// ZERO: the first pass of a sweep from x = 0 (red cells from b alone, black
-// cells set to 0); dot: also the partial sum(x * b) of the range's cells.
-template <typename S, typename V, bool ZERO>
-__device__ __forceinline__ double batch_colour(const BatchLevel<S, V>& L, int parity, size_t c0, size_t c1,
-                                               bool dot) {
+// One fused red-black sweep (both colours, out of place) of one tile of a
+// level: rbgs_sweep_kernel's schedule and arithmetic for the rows
+// [tj*tyo, +tyo) of the planes [tk*kz, +kz) - a rolling window of four
+// staged planes (xs, shared memory), red on plane p over the tile and a
+// one-row ring, black on plane p-1 over the tile, store plane p-1; the ring
+// rows and end planes are recomputed by the neighbouring tiles.  ZERO: the
+// incoming x is 0; PROLONG: it is x_in + P x_c; DOT: returns this thread's
+// part of sum(x_out * b).
+template <typename S, typename V, bool ZERO, bool PROLONG, bool DOT>
+__device__ double batch_sweep(const BatchLevel<S, V>& L, const V* x_in, V* x_out, const V* xc, int cni, int cnj,
+                              int tj, int tk, typename Num<V>::Acc* xs) {
   using A = typename Num<V>::Acc;
-  const int ni = L.ni, nj = L.nj, nk = L.nk;
+  const int ni = L.ni, nj = L.nj, nk = L.nk, tyo = L.tyo;
   const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
-  double acc = 0.0;
-  for (size_t g = c0 + threadIdx.x; g < c1; g += kBatchThreads) {
-    int i, j, k;
-    decode3(g, ni, nj, i, j, k);
-    if (((i + j + k) & 1) == parity) {
-      A sum = A(0);
-      if (!ZERO) {
-        if (k > 0) sum = gs_madd(sum, A(ldg(L.zp + g - sz)), ldcg(L.x + g - sz));
-        if (j > 0) sum = gs_madd(sum, A(ldg(L.yp + g - sy)), ldcg(L.x + g - sy));
-        if (i > 0) sum = gs_madd(sum, A(ldg(L.xp + g - 1)), ldcg(L.x + g - 1));
-        if (i < ni - 1) sum = gs_madd(sum, A(ldg(L.xp + g)), ldcg(L.x + g + 1));
-        if (j < nj - 1) sum = gs_madd(sum, A(ldg(L.yp + g)), ldcg(L.x + g + sy));
-        if (k < nk - 1) sum = gs_madd(sum, A(ldg(L.zp + g)), ldcg(L.x + g + sz));
+  const int j0 = tj * tyo, k0 = tk * L.kz;
+  const int kend = min(k0 + L.kz, nk), jout1 = min(j0 + tyo, nj);
+  const int jr0 = max(j0 - 2, 0), jr1 = min(j0 + tyo + 2, nj);
+  const int jred0 = max(j0 - 1, 0), jred1 = min(j0 + tyo + 1, nj);
+  const int rows = jr1 - jr0, pls = (tyo + 4) * ni;
+  auto X = [&](int p) -> A* { return xs + (size_t)(p & 3) * pls; };
+  auto stage = [&](int q) {
+    if (q < 0 || q >= nk) return;
+    A* dst = X(q);
+    const int cnt = rows * ni;
+    const size_t base = (size_t)q * sz + (size_t)jr0 * sy;
+    for (int e = threadIdx.x; e < cnt; e += kBatchThreads) {
+      A v;
+      if (ZERO) {
+        v = A(0);
+      } else {
+        v = ldcg(x_in + base + e);
+        if (PROLONG) {
+          const int i = e % ni, j = jr0 + e / ni;
+          v = v + ldcg(xc + lin3(i >> 1, j >> 1, q >> 1, cni, cnj));
+        }
       }
+      dst[e] = v;
+    }
+  };
+  auto relax = [&](int p, int r0, int r1, int parity) {
+    A* xm1 = X(p - 1);
+    A* x0 = X(p);
+    A* xp1 = X(p + 1);
+    const int cnt = (r1 - r0) * ni;
+    const size_t pbase = (size_t)p * sz;
+    for (int e = threadIdx.x; e < cnt; e += kBatchThreads) {
+      const int j = r0 + e / ni;
+      const int i = e - (j - r0) * ni;
+      if (((i + j + p) & 1) != parity) continue;
+      const size_t g = pbase + (size_t)j * sy + i;
+      const int sidx = (j - jr0) * ni + i;
+      A sum = A(0);
+      if (p > 0) sum = gs_madd(sum, A(ldg(L.zp + g - sz)), xm1[sidx]);
+      if (j > 0) sum = gs_madd(sum, A(ldg(L.yp + g - sy)), x0[sidx - ni]);
+      if (i > 0) sum = gs_madd(sum, A(ldg(L.xp + g - 1)), x0[sidx - 1]);
+      if (i < ni - 1) sum = gs_madd(sum, A(ldg(L.xp + g)), x0[sidx + 1]);
+      if (j < nj - 1) sum = gs_madd(sum, A(ldg(L.yp + g)), x0[sidx + ni]);
+      if (p < nk - 1) sum = gs_madd(sum, A(ldg(L.zp + g)), xp1[sidx]);
       const A d = A(ldg(L.diag + g));
-      const V o = cvt<V>((d != A(0)) ? gs_div(ldcg(L.b + g) - sum, d) : A(0));
-      L.x[g] = o;
-      if (dot) acc += (double)ldv(&o) * (double)ldcg(L.b + g);
-    } else {
-      if (ZERO) L.x[g] = cvt<V>(A(0));
-      if (dot) acc += (double)ldcg(L.x + g) * (double)ldcg(L.b + g);
+      x0[sidx] = (d != A(0)) ? gs_div(ldcg(L.b + g) - sum, d) : A(0);
+    }
+  };
+  double dot = 0.0;
+  stage(k0 - 2);
+  stage(k0 - 1);
+  for (int p = k0 - 1; p <= kend; ++p) {
+    stage(p + 1);
+    __syncthreads();
+    if (p >= 0 && p < nk) relax(p, jred0, jred1, 1);
+    __syncthreads();
+    const int q = p - 1;
+    const bool out_plane = q >= k0 && q < kend;
+    if (out_plane) relax(q, j0, jout1, 0);
+    __syncthreads();
+    if (out_plane) {
+      const A* src = X(q) + (size_t)(j0 - jr0) * ni;
+      const int cnt = (jout1 - j0) * ni;
+      const size_t base = (size_t)q * sz + (size_t)j0 * sy;
+      for (int e = threadIdx.x; e < cnt; e += kBatchThreads) {
+        const V o = cvt<V>(src[e]);
+        x_out[base + e] = o;
+        if (DOT) dot += (double)ldv(&o) * (double)ldcg(L.b + base + e);
+      }
     }
   }
-  return acc;
+  __syncthreads();  // the next tile restages the window
+  return dot;
 }
 
 // b_c = R (b - A x) over the coarse cells [c0, c1) (residual_restrict_kernel's arithmetic)
@@ -165,17 +223,6 @@ __device__ __forceinline__ void batch_restrict(const BatchLevel<S, V>& F, const 
           s = s + A(0.125) * r;
         }
     Cl.b[e] = cvt<V>(s);
-  }
-}
-
-// x_l += P x_{l+1} (injection) over the fine cells [c0, c1)
-template <typename S, typename V, typename SN>
-__device__ __forceinline__ void batch_prolong(const BatchLevel<S, V>& F, const BatchLevel<SN, V>& Cl, size_t c0,
-                                              size_t c1) {
-  for (size_t g = c0 + threadIdx.x; g < c1; g += kBatchThreads) {
-    int i, j, k;
-    decode3(g, F.ni, F.nj, i, j, k);
-    F.x[g] = cvt<V>(ldcg(F.x + g) + ldcg(Cl.x + lin3(i >> 1, j >> 1, k >> 1, Cl.ni, Cl.nj)));
   }
 }
 
@@ -344,13 +391,29 @@ __global__ void __launch_bounds__(kBatchThreads) batch_pcg_kernel(const BatchSys
       fn(y, s, local, (size_t)local * CH);
     }
   };
+  // every sweep tile of level l of the systems that smooth there (live ones):
+  // fn(system, its index, tile index within the system, row tile, plane range)
+  auto tiles = [&](int l, auto&& fn) {
+    const int* pre = p.sweep_pre + (size_t)l * (nsys + 1);
+    const int total = __ldg(pre + nsys);
+    for (int item = B; item < total; item += G) {
+      const int s = batch_find(pre, nsys, item);
+      const BatchSys<S0, SC, V>& y = sys[s];
+      if (!batch_live(y)) continue;
+      const int local = item - __ldg(pre + s);
+      const int ntj = l == 0 ? y.fine.ntj : y.lv[l].ntj;
+      fn(y, s, local, local % ntj, local / ntj);
+    }
+  };
+  A* xs = reinterpret_cast<A*>(bsm);  // the sweeps' plane window
   auto slot = [&](int s, int local) -> double* { return p.part + (size_t)s * p.part_stride + local; };
   // one CTA per system folds that system's level-0 slots in index order
   auto fold = [&](int kind) {
     for (int s = B; s < nsys; s += G) {
       const BatchSys<S0, SC, V>& y = sys[s];
       if (kind != kFoldInit && !batch_live(y)) continue;
-      const int cnt = __ldg(p.cell_pre + s + 1) - __ldg(p.cell_pre + s);
+      const int* cpre = kind == kFoldRho ? p.sweep_pre : p.cell_pre;
+      const int cnt = __ldg(cpre + s + 1) - __ldg(cpre + s);
       const bool mx = kind == kFoldInit || kind == kFoldRes;
       double v = 0.0;
       for (int q = threadIdx.x; q < cnt; q += kBatchThreads) {
@@ -423,26 +486,23 @@ __global__ void __launch_bounds__(kBatchThreads) batch_pcg_kernel(const BatchSys
 
   for (int iter = 0; iter < p.maxit; ++iter) {
     if (__ldcg(p.active + (iter & 1)) == 0) break;  // every CTA reads the same count after the barrier
-    // ---- V-cycle, down
+    // ---- V-cycle, down: four sweeps from x = 0 ending in x (t, x, t, x)
     for (int l = 0; l + 1 < p.lmax; ++l) {
       for (int sw = 0; sw < 4; ++sw) {
-        for (int parity = 1; parity >= 0; --parity) {
-          const bool zero = sw == 0 && parity == 1;
-          cells(l, [&](const BatchSys<S0, SC, V>& y, int, int, size_t c0) {
-            if (l + 1 >= y.nl) return;  // the system's coarsest level
-            if (l == 0) {
-              const size_t c1 = min(c0 + CH, (size_t)y.fine.ni * y.fine.nj * y.fine.nk);
-              if (zero) batch_colour<S0, V, true>(y.fine, parity, c0, c1, false);
-              else batch_colour<S0, V, false>(y.fine, parity, c0, c1, false);
-            } else {
-              const BatchLevel<SC, V>& L = y.lv[l];
-              const size_t c1 = min(c0 + CH, (size_t)L.ni * L.nj * L.nk);
-              if (zero) batch_colour<SC, V, true>(L, parity, c0, c1, false);
-              else batch_colour<SC, V, false>(L, parity, c0, c1, false);
-            }
-          });
-          grid.sync();
-        }
+        tiles(l, [&](const BatchSys<S0, SC, V>& y, int, int, int tj, int tk) {
+          if (l == 0) {
+            const BatchLevel<S0, V>& L = y.fine;
+            if (sw == 0) batch_sweep<S0, V, true, false, false>(L, nullptr, L.t, nullptr, 0, 0, tj, tk, xs);
+            else batch_sweep<S0, V, false, false, false>(L, sw & 1 ? L.t : L.x, sw & 1 ? L.x : L.t, nullptr, 0, 0,
+                                                         tj, tk, xs);
+          } else {
+            const BatchLevel<SC, V>& L = y.lv[l];
+            if (sw == 0) batch_sweep<SC, V, true, false, false>(L, nullptr, L.t, nullptr, 0, 0, tj, tk, xs);
+            else batch_sweep<SC, V, false, false, false>(L, sw & 1 ? L.t : L.x, sw & 1 ? L.x : L.t, nullptr, 0, 0,
+                                                         tj, tk, xs);
+          }
+        });
+        grid.sync();
       }
       {
         const int* pre = p.rest_pre + (size_t)l * (nsys + 1);
@@ -467,37 +527,32 @@ __global__ void __launch_bounds__(kBatchThreads) batch_pcg_kernel(const BatchSys
       batch_coarsest<SC, V>(y.lv[y.nl - 1], y.direct, y.bw, y.L, y.rinv, y.ok, y.sweeps, bsm, p.smem_doubles);
     }
     grid.sync();
-    // ---- V-cycle, up; the last black pass of level 0 forms the partial z.r
+    // ---- V-cycle, up: x + P x_c, then four sweeps ending in x; the last
+    // sweep of level 0 forms the partial z.r
     for (int l = p.lmax - 2; l >= 0; --l) {
-      cells(l, [&](const BatchSys<S0, SC, V>& y, int, int, size_t c0) {
-        if (l + 1 >= y.nl) return;
-        if (l == 0) {
-          batch_prolong<S0, V, SC>(y.fine, y.lv[1], c0, min(c0 + CH, (size_t)y.fine.ni * y.fine.nj * y.fine.nk));
-        } else {
-          const BatchLevel<SC, V>& L = y.lv[l];
-          batch_prolong<SC, V, SC>(L, y.lv[l + 1], c0, min(c0 + CH, (size_t)L.ni * L.nj * L.nk));
-        }
-      });
-      grid.sync();
       for (int sw = 0; sw < 4; ++sw) {
-        for (int parity = 1; parity >= 0; --parity) {
-          const bool last = l == 0 && sw == 3 && parity == 0;
-          cells(l, [&](const BatchSys<S0, SC, V>& y, int s, int local, size_t c0) {
-            if (l + 1 >= y.nl) return;
-            if (l == 0) {
-              const size_t c1 = min(c0 + CH, (size_t)y.fine.ni * y.fine.nj * y.fine.nk);
-              const double d = batch_colour<S0, V, false>(y.fine, parity, c0, c1, last);
-              if (last) {
-                const double bs = batch_block_sum(d, red);
-                if (threadIdx.x == 0) *slot(s, local) = bs;
-              }
-            } else {
-              const BatchLevel<SC, V>& L = y.lv[l];
-              batch_colour<SC, V, false>(L, parity, c0, min(c0 + CH, (size_t)L.ni * L.nj * L.nk), false);
+        const bool last = l == 0 && sw == 3;
+        tiles(l, [&](const BatchSys<S0, SC, V>& y, int s, int local, int tj, int tk) {
+          const BatchLevel<SC, V>& C = y.lv[l + 1];
+          if (l == 0) {
+            const BatchLevel<S0, V>& L = y.fine;
+            double d = 0.0;
+            if (sw == 0) batch_sweep<S0, V, false, true, false>(L, L.x, L.t, C.x, C.ni, C.nj, tj, tk, xs);
+            else if (last) d = batch_sweep<S0, V, false, false, true>(L, L.t, L.x, nullptr, 0, 0, tj, tk, xs);
+            else batch_sweep<S0, V, false, false, false>(L, sw & 1 ? L.t : L.x, sw & 1 ? L.x : L.t, nullptr, 0, 0,
+                                                         tj, tk, xs);
+            if (last) {
+              const double bs = batch_block_sum(d, red);
+              if (threadIdx.x == 0) *slot(s, local) = bs;
             }
-          });
-          grid.sync();
-        }
+          } else {
+            const BatchLevel<SC, V>& L = y.lv[l];
+            if (sw == 0) batch_sweep<SC, V, false, true, false>(L, L.x, L.t, C.x, C.ni, C.nj, tj, tk, xs);
+            else batch_sweep<SC, V, false, false, false>(L, sw & 1 ? L.t : L.x, sw & 1 ? L.x : L.t, nullptr, 0, 0,
+                                                         tj, tk, xs);
+          }
+        });
+        grid.sync();
       }
     }
     fold(kFoldRho);

@@ -2029,9 +2029,9 @@ int batched_persistent(vflip_ctx* ctx, int nsys, const vflip_system* sys, double
     const int nl = (int)b.T.coarse.size() + 1;
     if (nl < 2 || nl > kBatchMaxLevels) return VFLIP_OK;  // not taken
     const size_t n = (size_t)y.ni * y.nj * y.nk;
-    V** vs[5] = {&b.x, &b.r, &b.z, &b.s, &b.q};
-    const char* names[5] = {"bat_x", "bat_r", "bat_z", "bat_s", "bat_q"};
-    for (int k = 0; k < 5; ++k) {
+    V** vs[6] = {&b.x, &b.r, &b.z, &b.s, &b.q, &b.sd};
+    const char* names[6] = {"bat_x", "bat_r", "bat_z", "bat_s", "bat_q", "bat_z2"};
+    for (int k = 0; k < 6; ++k) {
       *vs[k] = (V*)c->buf(names[k], sizeof(V) * n);
       if (!*vs[k]) return ctx->fail(VFLIP_ERR_NOMEM, "cudaMalloc failed for %s", names[k]);
     }
@@ -2040,11 +2040,21 @@ int batched_persistent(vflip_ctx* ctx, int nsys, const vflip_system* sys, double
     BatchSys<S0, SC, V>& d = desc[i];
     std::memset(&d, 0, sizeof d);
     d.nl = nl;
+    // sweep tiles: up to 8 rows, plane ranges of about `CH` cells (at least 4 planes)
+    auto shape = [&](int ni_, int nj_, int nk_, int& tyo, int& kz, int& ntj) {
+      tyo = std::min(8, nj_);
+      kz = std::max(4, CH / std::max(1, ni_ * tyo));
+      kz = std::min(kz, nk_);
+      ntj = (nj_ + tyo - 1) / tyo;
+      smem_doubles = std::max(smem_doubles, (int)((4 * (size_t)(tyo + 4) * ni_ * sizeof(A) + 7) / 8));
+    };
     const Level<S0, V>& F = b.T.fine;
-    d.fine = BatchLevel<S0, V>{F.d.ni, F.d.nj, F.d.nk, F.diag, F.xp, F.yp, F.zp, b.r, b.z};
+    d.fine = BatchLevel<S0, V>{F.d.ni, F.d.nj, F.d.nk, F.diag, F.xp, F.yp, F.zp, b.r, b.z, b.sd, 0, 0, 0};
+    shape(F.d.ni, F.d.nj, F.d.nk, d.fine.tyo, d.fine.kz, d.fine.ntj);
     for (int l = 1; l < nl; ++l) {
       const Level<SC, V>& L = b.T.coarse[l - 1];
-      d.lv[l] = BatchLevel<SC, V>{L.d.ni, L.d.nj, L.d.nk, L.diag, L.xp, L.yp, L.zp, L.b, L.xa};
+      d.lv[l] = BatchLevel<SC, V>{L.d.ni, L.d.nj, L.d.nk, L.diag, L.xp, L.yp, L.zp, L.b, L.xa, L.xb, 0, 0, 0};
+      shape(L.d.ni, L.d.nj, L.d.nk, d.lv[l].tyo, d.lv[l].kz, d.lv[l].ntj);
     }
     d.x = b.x;
     d.s = b.s;
@@ -2067,37 +2077,46 @@ int batched_persistent(vflip_ctx* ctx, int nsys, const vflip_system* sys, double
     const int nc = C.d.ni * C.d.nj * C.d.nk;
     smem_doubles = std::max(smem_doubles, d.direct ? nc : (int)((2 * (size_t)nc * sizeof(A) + 7) / 8));
   }
-  smem_doubles = std::min(smem_doubles, 6144);  // 48 KB; larger coarsest sweeps run in global memory
+  if (smem_doubles > 26 * 1024) return VFLIP_OK;  // plane window over 208 KB (rows of > 1300 cells): not taken
+  if (ctx->cfg.pre_sweeps != 4 || ctx->cfg.post_sweeps != 4) return VFLIP_OK;  // the kernel runs V(4,4)
   // work lists: cell items of level 0 for every system and of a coarser
   // level where the system smooths there; restriction items into level l+1
   const size_t tab = (size_t)lmax * (nsys + 1);
-  std::vector<int> cell_pre(tab, 0), rest_pre(tab, 0);
+  std::vector<int> cell_pre(tab, 0), rest_pre(tab, 0), sweep_pre(tab, 0);
   for (int l = 0; l < lmax; ++l)
     for (int i = 0; i < nsys; ++i) {
       const BatchSys<S0, SC, V>& d = desc[i];
-      long long ci = 0, ri = 0;
+      long long ci = 0, ri = 0, si = 0;
       if (l == 0) ci = ((long long)d.fine.ni * d.fine.nj * d.fine.nk + CH - 1) / CH;
-      else if (l + 1 < d.nl) ci = ((long long)d.lv[l].ni * d.lv[l].nj * d.lv[l].nk + CH - 1) / CH;
-      if (l + 1 < d.nl) ri = ((long long)d.lv[l + 1].ni * d.lv[l + 1].nj * d.lv[l + 1].nk + CH - 1) / CH;
-      cell_pre[(size_t)l * (nsys + 1) + i + 1] = cell_pre[(size_t)l * (nsys + 1) + i] + (int)ci;
-      rest_pre[(size_t)l * (nsys + 1) + i + 1] = rest_pre[(size_t)l * (nsys + 1) + i] + (int)ri;
+      if (l + 1 < d.nl) {
+        ri = ((long long)d.lv[l + 1].ni * d.lv[l + 1].nj * d.lv[l + 1].nk + CH - 1) / CH;
+        const int nk_ = l == 0 ? d.fine.nk : d.lv[l].nk, kz = l == 0 ? d.fine.kz : d.lv[l].kz;
+        si = (long long)(l == 0 ? d.fine.ntj : d.lv[l].ntj) * ((nk_ + kz - 1) / kz);
+      }
+      const size_t o = (size_t)l * (nsys + 1) + i;
+      cell_pre[o + 1] = cell_pre[o] + (int)ci;
+      rest_pre[o + 1] = rest_pre[o] + (int)ri;
+      sweep_pre[o + 1] = sweep_pre[o] + (int)si;
     }
+  for (int i = 0; i < nsys; ++i) part_stride = std::max(part_stride, sweep_pre[i + 1] - sweep_pre[i]);
   const size_t sys_bytes = ((sizeof(BatchSys<S0, SC, V>) * nsys + 255) / 256) * 256;
   const size_t part_bytes = (size_t)nsys * part_stride * sizeof(double);
-  char* dev = (char*)ctx->buf("bp_plan", sys_bytes + part_bytes + (2 * tab + 4) * sizeof(int));
+  char* dev = (char*)ctx->buf("bp_plan", sys_bytes + part_bytes + (3 * tab + 4) * sizeof(int));
   if (!dev) return ctx->fail(VFLIP_ERR_NOMEM, "cudaMalloc failed for the batch plan");
   auto* dsys = reinterpret_cast<BatchSys<S0, SC, V>*>(dev);
   double* part = reinterpret_cast<double*>(dev + sys_bytes);
   int* dcell = reinterpret_cast<int*>(dev + sys_bytes + part_bytes);
   int* drest = dcell + tab;
-  int* dactive = drest + tab;
+  int* dsweep = drest + tab;
+  int* dactive = dsweep + tab;
   VF_CUDA(cudaMemcpyAsync(dsys, desc.data(), sizeof(BatchSys<S0, SC, V>) * nsys, cudaMemcpyHostToDevice,
                           ctx->stream));
   VF_CUDA(cudaMemcpyAsync(dcell, cell_pre.data(), tab * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   VF_CUDA(cudaMemcpyAsync(drest, rest_pre.data(), tab * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(dsweep, sweep_pre.data(), tab * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   // the host vectors above are read by the copies: wait for them before they go
   VF_CUDA(cudaStreamSynchronize(ctx->stream));
-  BatchPlan plan{nsys, lmax, maxit, CH, dcell, drest, part, part_stride, dactive, smem_doubles};
+  BatchPlan plan{nsys, lmax, maxit, CH, dcell, drest, dsweep, part, part_stride, dactive, smem_doubles};
   auto kern = batch_pcg_kernel<S0, SC, V>;
   const size_t smem = (size_t)smem_doubles * sizeof(double);
   if (smem_optin((const void*)kern, (int)smem) != cudaSuccess)

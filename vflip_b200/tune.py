@@ -99,7 +99,7 @@ def measure(st, rhs, shape, reps=2, precision=1):
 
 
 BATCH_CACHE = os.environ.get("VFLIP_BATCH_TUNE", os.path.join(HERE, "batch_tuning.json"))
-BATCH_CANDIDATES = [(chunk, ctas) for chunk in (1024, 2048, 4096, 8192, 16384) for ctas in (0, 1, 2)]
+BATCH_CANDIDATES = [(chunk, ctas) for chunk in (4096, 8192, 16384, 32768, 65536) for ctas in (0, 1, 2)]
 
 
 def batch_key(precision, sides):
