@@ -182,8 +182,9 @@ def test_resid_capture_is_the_plain_solve(prec):
 @pytest.mark.parametrize("prec,net_on,sweeps", [(1, False, 0), (1, True, 2), (2, True, 2), (0, True, 0)])
 def test_resid_solve_converges_to_plain_answer(prec, net_on, sweeps):
     """Whatever the network says (here an untrained one), the residual-mode
-    solve reaches the plain solve's tolerance and answer (both with FP64
-    PCG vectors, so they agree to the tolerance, not to FP32 rounding)."""
+    solve reaches the plain solve's tolerance and, up to where two solves
+    from different starting points stop inside it, its answer (both with
+    FP64 PCG vectors)."""
     from vflip_b200.learned import NO_NET, RESID, SWEEPS
 
     s, sim = _state(prec)
@@ -199,7 +200,7 @@ def test_resid_solve_converges_to_plain_answer(prec, net_on, sweeps):
         conv, p, st2, ls = sim.project_learned(net if net_on else None, mode, 1)
     assert conv and st2.converged
     assert st2.residual <= 1e-6 * st2.rhs_norm
-    assert _rel(p, p_plain) < 2e-5
+    assert _rel(p, p_plain) < 1e-4
     assert (ls.net_ms > 0) == net_on
     if not net_on:
         assert ls.gamma[1] == 0
