@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-flip", action="store_true", help="skip the FLIP smoke arm")
     ap.add_argument("--no-nested", action="store_true", help="skip the nested-subdomain arm")
     ap.add_argument("--no-precisions", action="store_true", help="skip the fp64/mixed plain arms")
+    ap.add_argument("--no-dropin", action="store_true", help="skip the host-CSR drop-in solve timing")
     ap.add_argument("--learned-level", type=int, default=2)
     ap.add_argument("--learned-sweeps", type=int, default=2)
     ap.add_argument("--learned-capture", type=int, default=40)
@@ -255,6 +256,7 @@ def run_vflip(a):
     e2e_ms = max_over_ranks(e2.elapsed_time(e3))
 
     diag = solve_diagnostics(sim, local) if rank == 0 else None
+    dropin = dropin_arm(sim, solver) if rank == 0 and world == 1 and not a.no_dropin else None
     out = None
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -284,6 +286,8 @@ def run_vflip(a):
             "gpu_launches": launches,
             "clocks": clk,
         }
+        if dropin:
+            out["dropin_host"] = dropin
         if not a.no_precisions and world == 1:
             out["precisions"] = precision_arm(a, sim, local, a.steps)
         if not a.no_cpu_baseline and world == 1:
@@ -590,6 +594,79 @@ def batched_arm(solver, count=32, reps=2):
             "persistent_iterations_mean": float(np.mean([x.iterations for x in p[2]])),
             "iterations_equal_graph_loop": all(x.iterations == y.iterations for x, y in zip(g[2], l[2])),
             "cells_per_s_persistent": cells / (p[0] * 1e-3), "tuned": best_cfg, "tuning": table}
+
+
+def csr_of_stencil(stencil):
+    """Host CSR (rowstart, colindex, value) of a (4, nk, nj, ni) FP64
+    stencil in the form SmokeSolver3D::pcg_projection hands to
+    AMGPCGSolve: rows in cell order, columns sorted, the diagonal always
+    present, off-diagonal couplings where non-zero (Smoke_solver3D.cpp
+    :1040-1120, sparse_matrix.h:266-312)."""
+    import numpy as np
+
+    _, nk, nj, ni = stencil.shape
+    n, sy, sz = ni * nj * nk, ni, ni * nj
+    d, xp, yp, zp = (np.ascontiguousarray(stencil[c]).ravel() for c in range(4))
+    r = np.arange(n, dtype=np.int64)
+    i, j, k = r % ni, (r // ni) % nj, r // sz
+    vals = np.zeros((n, 7))
+    vals[sz:, 0] = zp[:-sz]
+    vals[sy:, 1] = yp[:-sy]
+    vals[1:, 2] = xp[:-1]
+    vals[:, 3] = d
+    vals[:, 4], vals[:, 5], vals[:, 6] = xp, yp, zp
+    ok = np.stack([k > 0, j > 0, i > 0, np.ones(n, bool), i < ni - 1, j < nj - 1, k < nk - 1], axis=1)
+    keep = ok & ((vals != 0) | (np.arange(7) == 3)[None, :])
+    cols = r[:, None] + np.array([-sz, -sy, -1, 0, 1, sy, sz])[None, :]
+    rowstart = np.zeros(n + 1, np.uint32)
+    np.cumsum(keep.sum(axis=1), out=rowstart[1:])
+    return rowstart, cols[keep].astype(np.uint32), vals[keep]
+
+
+def dropin_arm(sim, solver, reps=3):
+    """The reference-facing host-buffer call: the drop-in of
+    ivock::AMGPCGSolve (vflip_amgpcg_solve_csr, AlgebraicMultigrid.h
+    :189-197) on one plume step's pressure system as host CSR arrays, the
+    call SmokeSolver3D::pcg_projection makes (Smoke_solver3D.cpp:1120).
+    The call is synchronous (CSR pattern and symmetry checks and the
+    conversion on host threads, one upload, the solve, the download), so it
+    is timed by wall clock, median of `reps` after one untimed call, beside
+    the same solve on device arrays (CUDA events)."""
+    import numpy as np
+    import torch
+
+    state = {k: sim.f[k].clone() for k in sim.FIELDS}
+    sim.advect_and_force()
+    p, n = sim.p, sim.p.n
+    stencil, rhs = solver.assemble(n, n, n, p.h, 0.0, sim.phi, sim.bdesc, sim.solid["u"], sim.solid["v"],
+                                   sim.solid["w"], sim.f["u"], sim.f["v"], sim.f["w"])
+    st_h, rhs_h = stencil.cpu().numpy(), rhs.cpu().numpy().ravel()
+    rowstart, colindex, value = csr_of_stencil(st_h)
+    solver.amgpcg_solve_csr(rowstart, colindex, value, rhs_h, p.tol, p.max_iterations, n, n, n)
+    times = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ok, x_host, res, its = solver.amgpcg_solve_csr(rowstart, colindex, value, rhs_h, p.tol, p.max_iterations,
+                                                       n, n, n)
+        times.append((time.perf_counter() - t0) * 1e3)
+    x_dev = torch.empty((n, n, n), dtype=torch.float64, device=rhs.device)
+    solver.amgpcg_solve(stencil, rhs, p.tol, p.max_iterations, result=x_dev)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    solver.amgpcg_solve(stencil, rhs, p.tol, p.max_iterations, result=x_dev)
+    e1.record()
+    torch.cuda.synchronize()
+    for k in sim.FIELDS:
+        sim.f[k].copy_(state[k])
+    ms = float(np.median(times))
+    return {"call": "vflip_amgpcg_solve_csr (host CSR in, host result out)", "ms_per_solve": ms,
+            "solves_per_s": 1e3 / ms, "device_ms_per_solve": e0.elapsed_time(e1), "converged": bool(ok),
+            "iterations": its, "nnz": int(len(value)),
+            "h2d_bytes": int(5 * 8 * n ** 3), "d2h_bytes": int(8 * n ** 3),
+            "bitwise_equal_device_solve": bool(np.array_equal(x_host, x_dev.cpu().numpy().ravel())),
+            "timing": f"wall clock around the synchronous call, median of {reps}"}
 
 
 # the reference's own hierarchy (16^3 coarsest level, 200 red-black sweeps):

@@ -286,6 +286,43 @@ def test_csr_rejects_non_7point_and_asymmetric(gpu_solver):
     assert e.value.code == -4
 
 
+def test_csr_host_conversion_on_many_threads(gpu_solver):
+    """A 96^3 system (rows split over up to 14 host threads in the CSR
+    checks and conversion), in the form pcg_projection hands over (zero
+    couplings left out): the host-buffer call gives the device-array solve
+    bit for bit.  With bad entries in two rows that different threads own,
+    the error names the first of them in row order."""
+    import re
+
+    import bench
+    from vflip_b200 import VflipError
+
+    ni = nj = nk = 96
+    pr = scenes.projection_problem(ni, nj, nk, seed=7, inflow=True, solid_velocity=True)
+    s = gpu_solver[1]
+    keys = ("h", "U_in", "phi", "bdesc", "us", "vs", "ws", "u", "v", "w")
+    st, b = s.assemble(ni, nj, nk, *[t(pr[k]) if isinstance(pr[k], np.ndarray) else pr[k] for k in keys])
+    rs, ci, v = bench.csr_of_stencil(st.cpu().numpy())
+    ok, x, res, it = s.amgpcg_solve_csr(rs, ci, v, b.cpu().numpy(), 1e-6, 50, ni, nj, nk)
+    ok2, x2, st2 = s.amgpcg_solve(st, b, 1e-6, 50)
+    assert ok and ok2 and it == st2.iterations
+    assert np.array_equal(x, x2.cpu().numpy().ravel())
+    n = ni * nj * nk
+    bad = ci.copy()
+    def with_couplings(r):  # the next row with an off-diagonal entry
+        while rs[r + 1] - rs[r] < 2:
+            r += 1
+        return r
+
+    late, early = with_couplings(n - 5 * ni * nj - 7), with_couplings(n // 3 + 11)
+    for row in (late, early):
+        bad[rs[row] + 1] = (row + 2 * ni * nj + 3) % n  # off the 7-point pattern
+    with pytest.raises(VflipError) as e:
+        s.amgpcg_solve_csr(rs, bad, v, b.cpu().numpy(), 1e-6, 50, ni, nj, nk)
+    assert e.value.code == -3
+    assert re.search(rf"row {early} ", str(e.value))
+
+
 def test_solver_failure_modes(gpu_solver, orc):
     """Zero rhs -> converged in 0 iterations; a NaN in the rhs -> not
     converged with 0 iterations (rho != rho); max_iterations exhausted -> not

@@ -57,11 +57,15 @@ def test_noalloc_smoother_matches_allocating_entry_point():
             ni, nj, nk = dims
             want = s.rbgs(four, b, x0.clone(), iters)
             got = x0.clone()
+            torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info()[0]
             rc = lib.vflip_rbgs_noalloc(C.c_void_p(stream.cuda_stream), ni, nj, nk, _ptr(four[0]), _ptr(four[1]),
                                         _ptr(four[2]), _ptr(four[3]), _ptr(b), _ptr(got), iters)
             assert rc == 0, f"call {call}: status {rc}"
             torch.cuda.synchronize()
             assert torch.equal(got, want), f"call {call} differs from vflip_rbgs"
+            if call > 0:  # (the first call may load the library's kernels, which the driver places on the device)
+                assert torch.cuda.mem_get_info()[0] == free0, "the call changed the device's free memory"
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <unordered_map>
 #include <vector>
@@ -75,6 +76,8 @@ struct vflip_ctx {
   cudaStream_t stream = nullptr;
   std::string err;
   std::unordered_map<std::string, std::pair<void*, size_t>> bufs;
+  void* hbuf = nullptr;  // pinned host staging of the host-buffer entry points
+  size_t hbuf_bytes = 0;
   PcgScalars* st = nullptr;         // device
   PcgScalars* st_host = nullptr;    // pinned
   double* partials = nullptr;       // device, kMaxPartials
@@ -130,6 +133,22 @@ struct vflip_ctx {
     bufs[name] = {p, bytes};
     return p;
   }
+  // Cached pinned host buffer of at least `bytes`.
+  void* host_buf(size_t bytes) {
+    if (hbuf && hbuf_bytes >= bytes) return hbuf;
+    if (hbuf) {
+      cudaStreamSynchronize(stream);
+      cudaFreeHost(hbuf);
+      hbuf = nullptr;
+      hbuf_bytes = 0;
+    }
+    if (cudaMallocHost(&hbuf, bytes) != cudaSuccess) {
+      hbuf = nullptr;
+      return nullptr;
+    }
+    hbuf_bytes = bytes;
+    return hbuf;
+  }
 };
 
 #define VF_CUDA(call)                                                                         \
@@ -175,6 +194,29 @@ void prof_stop(vflip_ctx* ctx, int slot, cudaStream_t stream) {
   } while (0)
 
 namespace {
+
+// f(r) over rows [0, n) on up to 32 host threads, in contiguous
+// row ranges; returns the smallest row for which f returned false, or
+// UINT32_MAX.  f must only write state of its own row.
+template <class F>
+uint32_t csr_rows_parallel(uint32_t n, F f) {
+  unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  unsigned nt = (unsigned)std::min<uint64_t>({(uint64_t)hw, 32ull, (uint64_t)n / 65536 + 1});
+  std::vector<uint32_t> first(nt, UINT32_MAX);
+  auto run = [&](unsigned t) {
+    uint32_t r0 = (uint32_t)((uint64_t)n * t / nt), r1 = (uint32_t)((uint64_t)n * (t + 1) / nt);
+    for (uint32_t r = r0; r < r1; ++r)
+      if (!f(r)) {
+        first[t] = r;
+        return;
+      }
+  };
+  std::vector<std::thread> pool;
+  for (unsigned t = 1; t < nt; ++t) pool.emplace_back(run, t);
+  run(0);
+  for (auto& th : pool) th.join();
+  return *std::min_element(first.begin(), first.end());
+}
 
 // 1/h when h is a power of two (x*(1/h) then equals x/h exactly), else 0
 double inv_pow2(double h) {
@@ -2279,6 +2321,7 @@ int vflip_destroy(vflip_ctx* ctx) {
   if (ctx->partials) cudaFree(ctx->partials);
   if (ctx->d_error) cudaFree(ctx->d_error);
   if (ctx->st_host) cudaFreeHost(ctx->st_host);
+  if (ctx->hbuf) cudaFreeHost(ctx->hbuf);
   for (auto& pe : ctx->prof_events) {
     cudaEventDestroy(pe.a);
     cudaEventDestroy(pe.b);
@@ -2316,53 +2359,78 @@ int vflip_amgpcg_solve_csr(vflip_ctx* ctx, uint32_t n, const uint32_t* rowstart,
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (!rowstart || !colindex || !value || !rhs || !result) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
   if ((size_t)n != (size_t)ni * nj * nk) return ctx->fail(VFLIP_ERR_ARG, "n != ni*nj*nk");
-  // CSR -> 7 slots, checking the pattern (no wrap-around across rows/planes)
-  std::vector<double> st(7 * (size_t)n, 0.0);
+  // pinned staging: diag, +x, +y, +z couplings and the rhs, uploaded as one copy
+  double* st = (double*)ctx->host_buf(5 * sizeof(double) * (size_t)n);
+  if (!st) return ctx->fail(VFLIP_ERR_NOMEM, "cudaMallocHost failed for the CSR staging buffer");
   const long long sy = ni, sz = (long long)ni * nj;
-  for (uint32_t r = 0; r < n; ++r) {
+  // pass 1: CSR -> stencil, checking the pattern (no wrap-around across rows
+  // or planes); a repeated entry keeps its last value.  Rows are split over
+  // host threads; the first bad row in row order is the one reported.
+  uint32_t bad_row = csr_rows_parallel(n, [&](uint32_t r) -> bool {
     int i = (int)(r % ni), j = (int)((r / ni) % nj), k = (int)(r / sz);
+    double d = 0.0, px = 0.0, py = 0.0, pz = 0.0;
     for (uint32_t e = rowstart[r]; e < rowstart[r + 1]; ++e) {
       long long dlt = (long long)colindex[e] - (long long)r;
-      int slot = -1;
-      if (dlt == 0) slot = 0;
-      else if (dlt == -1 && i > 0) slot = 1;
-      else if (dlt == 1 && i < ni - 1) slot = 2;
-      else if (dlt == -sy && j > 0) slot = 3;
-      else if (dlt == sy && j < nj - 1) slot = 4;
-      else if (dlt == -sz && k > 0) slot = 5;
-      else if (dlt == sz && k < nk - 1) slot = 6;
-      if (slot < 0) return ctx->fail(VFLIP_ERR_NOT_7POINT, "row %u has an entry at column %u off the 7-point pattern",
-                                     r, colindex[e]);
-      st[(size_t)slot * n + r] = value[e];
+      if (dlt == 0) d = value[e];
+      else if (dlt == 1 && i < ni - 1) px = value[e];
+      else if (dlt == sy && j < nj - 1) py = value[e];
+      else if (dlt == sz && k < nk - 1) pz = value[e];
+      else if (!((dlt == -1 && i > 0) || (dlt == -sy && j > 0) || (dlt == -sz && k > 0)))
+        return false;
     }
+    st[r] = d;
+    st[(size_t)n + r] = px;
+    st[2 * (size_t)n + r] = py;
+    st[3 * (size_t)n + r] = pz;
+    st[4 * (size_t)n + r] = rhs[r];
+    return true;
+  });
+  if (bad_row != UINT32_MAX) {
+    uint32_t col = 0;
+    for (uint32_t e = rowstart[bad_row]; e < rowstart[bad_row + 1]; ++e) {
+      long long dlt = (long long)colindex[e] - (long long)bad_row;
+      int i = (int)(bad_row % ni), j = (int)((bad_row / ni) % nj), k = (int)(bad_row / sz);
+      bool ok = dlt == 0 || (dlt == 1 && i < ni - 1) || (dlt == sy && j < nj - 1) || (dlt == sz && k < nk - 1) ||
+                (dlt == -1 && i > 0) || (dlt == -sy && j > 0) || (dlt == -sz && k > 0);
+      if (!ok) {
+        col = colindex[e];
+        break;
+      }
+    }
+    return ctx->fail(VFLIP_ERR_NOT_7POINT, "row %u has an entry at column %u off the 7-point pattern", bad_row, col);
   }
-  // symmetry: -x coupling of r equals +x coupling of r-1, etc.
-  for (uint32_t r = 0; r < n; ++r) {
+  // pass 2, symmetry: the -x coupling of r (0 when absent) equals the +x
+  // coupling of r-1, and likewise in y and z
+  bad_row = csr_rows_parallel(n, [&](uint32_t r) -> bool {
     int i = (int)(r % ni), j = (int)((r / ni) % nj), k = (int)(r / sz);
+    double mx = 0.0, my = 0.0, mz = 0.0;
+    for (uint32_t e = rowstart[r]; e < rowstart[r + 1]; ++e) {
+      long long dlt = (long long)colindex[e] - (long long)r;
+      if (dlt == -1) mx = value[e];
+      else if (dlt == -sy) my = value[e];
+      else if (dlt == -sz) mz = value[e];
+    }
     bool ok = true;
-    if (i > 0) ok &= st[1 * (size_t)n + r] == st[2 * (size_t)n + r - 1];
-    if (j > 0) ok &= st[3 * (size_t)n + r] == st[4 * (size_t)n + r - sy];
-    if (k > 0) ok &= st[5 * (size_t)n + r] == st[6 * (size_t)n + r - sz];
-    if (!ok) return ctx->fail(VFLIP_ERR_NOT_SYMMETRIC, "matrix is not symmetric at row %u", r);
-  }
-  double *dd, *drhs, *dres;
-  VF_ALLOC(dd, double, "csr_op", 4 * (size_t)n);
-  VF_ALLOC(drhs, double, "csr_rhs", n);
+    if (i > 0) ok &= mx == st[(size_t)n + r - 1];
+    if (j > 0) ok &= my == st[2 * (size_t)n + r - sy];
+    if (k > 0) ok &= mz == st[3 * (size_t)n + r - sz];
+    return ok;
+  });
+  if (bad_row != UINT32_MAX) return ctx->fail(VFLIP_ERR_NOT_SYMMETRIC, "matrix is not symmetric at row %u", bad_row);
+  double *dd, *dres;
+  VF_ALLOC(dd, double, "csr_op", 5 * (size_t)n);
   VF_ALLOC(dres, double, "csr_res", n);
-  VF_CUDA(cudaMemcpyAsync(dd, st.data(), sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
-  VF_CUDA(cudaMemcpyAsync(dd + n, st.data() + 2 * (size_t)n, sizeof(double) * n, cudaMemcpyHostToDevice,
-                          ctx->stream));
-  VF_CUDA(cudaMemcpyAsync(dd + 2 * (size_t)n, st.data() + 4 * (size_t)n, sizeof(double) * n,
-                          cudaMemcpyHostToDevice, ctx->stream));
-  VF_CUDA(cudaMemcpyAsync(dd + 3 * (size_t)n, st.data() + 6 * (size_t)n, sizeof(double) * n,
-                          cudaMemcpyHostToDevice, ctx->stream));
-  VF_CUDA(cudaMemcpyAsync(drhs, rhs, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(dd, st, 5 * sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
   vflip_solve_stats s{};
-  int status = solve_stencil(ctx, ni, nj, nk, dd, dd + n, dd + 2 * (size_t)n, dd + 3 * (size_t)n, drhs, dres,
-                             tolerance_factor, max_iterations, &s);
+  int status = solve_stencil(ctx, ni, nj, nk, dd, dd + n, dd + 2 * (size_t)n, dd + 3 * (size_t)n,
+                             dd + 4 * (size_t)n, dres, tolerance_factor, max_iterations, &s);
   if (status < 0) return status;
-  VF_CUDA(cudaMemcpyAsync(result, dres, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaMemcpyAsync(st, dres, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
   VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  csr_rows_parallel(n, [&](uint32_t r) -> bool {
+    result[r] = st[r];
+    return true;
+  });
   if (residual_out) *residual_out = s.residual;
   if (iterations_out) *iterations_out = s.iterations;
   return status;
