@@ -216,3 +216,43 @@ def test_resid_mode_needs_fp64_vectors():
     sim.advect_and_force()
     with pytest.raises(VflipError):
         sim.project_learned(None, SOLVE | RESID | NO_NET, 1)
+
+
+@pytest.mark.parametrize("prec,net_on", [(1, False), (1, True), (2, True)])
+def test_resid_solve_device_loop_equals_host_loop(prec, net_on):
+    """The warm-started PCG runs as the device-resident loop (a CUDA graph
+    with a conditional while node); the host loop (pcg_loop=1) gives the
+    same bits, iterations and Ritz coefficients.  Plain and warm-started
+    solves alternating on one context keep their own graphs."""
+    from vflip_b200.learned import NO_NET, RESID, SWEEPS
+    from vflip_b200.solver import Solver
+
+    out = []
+    for loop in (0, 1):
+        s = Solver(precision=prec, pcg_loop=loop)
+        sim = PlumeSim(s, PlumeParams(n=40, dt=0.02))
+        for _ in range(4):
+            sim.step()
+        sim.advect_and_force()
+        p_prev = sim.pressure.clone()
+        u0 = {k: sim.f[k].clone() for k in ("u", "v", "w")}
+        res = []
+        with UNet(seed=7) as net:
+            mode = SOLVE | RESID | SWEEPS(2) | (0 if net_on else NO_NET)
+            for rep in range(2):
+                for k in u0:
+                    sim.f[k].copy_(u0[k])
+                sim.pressure.copy_(p_prev)
+                _, p_plain, st_plain = sim.project()
+                p_plain = p_plain.clone()
+                for k in u0:
+                    sim.f[k].copy_(u0[k])
+                sim.pressure.copy_(p_prev)
+                conv, p, st, ls = sim.project_learned(net if net_on else None, mode, 1)
+                res.append((p.clone(), st.iterations, tuple(ls.gamma[:2]), p_plain, st_plain.iterations))
+        out.append(res)
+        s.close()
+    for (pa, ia, ga, qa, ja), (pb, ib, gb, qb, jb) in zip(*out):
+        assert torch.equal(pa, pb) and ia == ib and ga == gb
+        assert torch.equal(qa, qb) and ja == jb
+    assert torch.equal(out[0][0][0], out[0][1][0])

@@ -272,17 +272,20 @@ __global__ void ritz2_fold_kernel(const double* __restrict__ partials, int nb, d
 }
 
 // x = g0 p + g1 e, r = b - g0 Ap - g1 Ae, rv = r in V, partial |r|_inf
+// (g0, g1 = gam[0], gam[1], the device-side Ritz step's result)
 // (the converged flag against the tolerance set by the last block)
 template <typename V, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) ritz2_combine_kernel(const double* __restrict__ p,
                                                               const double* __restrict__ ap,
                                                               const double* __restrict__ e,
                                                               const double* __restrict__ ae,
-                                                              const double* __restrict__ b, double g0, double g1,
+                                                              const double* __restrict__ b,
+                                                              const double* __restrict__ gam,
                                                               double* __restrict__ x, double* __restrict__ r,
                                                               V* __restrict__ rv, size_t n, double* partials,
                                                               PcgScalars* st) {
   __shared__ double sm[BLOCK / 32];
+  const double g0 = gam[0], g1 = gam[1];
   double m = 0.0;
   for (size_t i = (size_t)blockIdx.x * BLOCK + threadIdx.x; i < n; i += (size_t)gridDim.x * BLOCK) {
     x[i] = g0 * __ldg(p + i) + g1 * __ldg(e + i);

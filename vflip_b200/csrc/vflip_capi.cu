@@ -44,6 +44,7 @@ constexpr int kSweepBlock = 256;
 constexpr int kRedBlock = 256;
 constexpr int kCoarseBlock = 1024;
 constexpr int kMaxPartials = 1 << 16;
+constexpr int kPcgGraphs = 4;  // PCG loop graphs kept per context
 
 struct Dims {
   int ni, nj, nk;
@@ -89,10 +90,15 @@ struct vflip_ctx {
   std::vector<vflip_ctx*> subs;     // per-system contexts of batched solves
   // the device-resident PCG loop: its graph, kept while the buffers it names stay the same
   cudaStream_t pg_stream = nullptr;
-  cudaGraph_t pg_graph = nullptr;
-  cudaGraphExec_t pg_exec = nullptr;
-  std::vector<uintptr_t> pg_key;
-  unsigned long long pg_init_launches = 0, pg_body_launches = 0, pg_tail_launches = 0;
+  struct PcgGraph {
+    std::vector<uintptr_t> key;  // every buffer and size the captured launches name
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long init_launches = 0, body_launches = 0, tail_launches = 0;
+    unsigned long long used = 0;  // last use, for replacing the least recently used
+  };
+  std::vector<PcgGraph> pgs;  // at most kPcgGraphs (a plain and a warm-started loop, their precisions)
+  unsigned long long pg_clock = 0;
   std::unordered_map<std::string, CUtensorMap> tmaps;  // encoded TMA tensor maps by (address, shape)
   // fine-level sweep timing (vflip_set_profiling)
   bool profiling = false;
@@ -1023,7 +1029,7 @@ void launch_pcg_update(vflip_ctx* ctx, cudaStream_t st, const OuterVecs<W, V>& o
 // with the host loop, whose early exits set the result as the reference's.
 template <typename W, typename S0, typename SC, typename V>
 int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor,
-                    int maxit, vflip_solve_stats* stats, bool* done) {
+                    int maxit, vflip_solve_stats* stats, bool* done, bool warm = false) {
   *done = false;
   const Dims d = T.fine.d;
   const size_t n = d.n();
@@ -1047,21 +1053,30 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
   for (const auto& L : T.coarse) kl(L);
   kp(T.direct.L); kp(T.direct.rinv); kp(T.direct.ok);
   key.push_back((uintptr_t)T.direct.on); key.push_back((uintptr_t)T.direct.bw); key.push_back((uintptr_t)maxit);
+  key.push_back((uintptr_t)warm);
   uint64_t tb;
   std::memcpy(&tb, &tol_factor, sizeof tb);
   key.push_back((uintptr_t)tb);
   const int gb = grid_for(n, kRedBlock, ctx->num_sms);
-  if (key != ctx->pg_key || !ctx->pg_exec) {
-    if (ctx->pg_exec) cudaGraphExecDestroy(ctx->pg_exec);
-    if (ctx->pg_graph) cudaGraphDestroy(ctx->pg_graph);
-    ctx->pg_exec = nullptr;
-    ctx->pg_graph = nullptr;
-    ctx->pg_key.clear();
+  vflip_ctx::PcgGraph* E = nullptr;
+  for (auto& g : ctx->pgs)
+    if (g.exec && g.key == key) E = &g;
+  if (!E) {
+    if (ctx->pgs.size() < (size_t)kPcgGraphs) {
+      ctx->pgs.emplace_back();
+      E = &ctx->pgs.back();
+    } else {
+      E = &*std::min_element(ctx->pgs.begin(), ctx->pgs.end(),
+                             [](const vflip_ctx::PcgGraph& a, const vflip_ctx::PcgGraph& b) { return a.used < b.used; });
+      if (E->exec) cudaGraphExecDestroy(E->exec);
+      if (E->graph) cudaGraphDestroy(E->graph);
+      *E = vflip_ctx::PcgGraph{};
+    }
     if (!ctx->pg_stream) VF_CUDA(cudaStreamCreateWithFlags(&ctx->pg_stream, cudaStreamNonBlocking));
     const cudaStream_t cs = ctx->pg_stream;
     cudaGraph_t graph = nullptr;
     VF_CUDA(cudaGraphCreate(&graph, 0));
-    ctx->pg_graph = graph;
+    E->graph = graph;
     cudaGraphConditionalHandle hnd;
     VF_CUDA(cudaGraphConditionalHandleCreate(&hnd, graph, 0, 0));
     const cudaStream_t saved = ctx->stream;
@@ -1084,9 +1099,11 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
     const unsigned long long before_capture = ctx->launches;
     if (cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
       return restore(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamBeginCaptureToGraph"));
-    cudaMemsetAsync(ctx->st, 0, sizeof(PcgScalars), cs);
+    // warm: the caller has set x, r, its V copy and the scalars (tolerance
+    // and |r|_inf of the initial guess); otherwise r = b, x = 0
+    if (!warm) cudaMemsetAsync(ctx->st, 0, sizeof(PcgScalars), cs);
     cudaMemsetAsync(s, 0, n * sizeof(W), cs);
-    launch_pcg_init(ctx, cs, o, rhs, n, tol_factor);
+    if (!warm) launch_pcg_init(ctx, cs, o, rhs, n, tol_factor);
     pcg_loop_init_kernel<<<1, 32, 0, cs>>>(ctx->st, itp, hnd);
     cudaStreamCaptureStatus cst;
     const cudaGraphNode_t* deps = nullptr;
@@ -1097,7 +1114,7 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
     }
     std::vector<cudaGraphNode_t> dv(deps, deps + ndeps);
     if ((rc = end_capture(graph))) return restore(rc);
-    ctx->pg_init_launches = 2;
+    E->init_launches = warm ? 1 : 2;
     cudaGraphNodeParams cp = {};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = hnd;
@@ -1124,25 +1141,26 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
     }
     if ((rc = end_capture(body))) return restore(rc);
     if (brc) return restore(brc);
-    ctx->pg_body_launches = ctx->launches - l0;
+    E->body_launches = ctx->launches - l0;
     if (cudaStreamBeginCaptureToGraph(cs, graph, &wn, nullptr, 1, cudaStreamCaptureModeRelaxed) != cudaSuccess)
       return restore(ctx->fail(VFLIP_ERR_CUDA, "cudaStreamBeginCaptureToGraph (result)"));
     if constexpr (std::is_same<W, V>::value) {
       to_double_kernel<V, kRedBlock><<<gb, kRedBlock, 0, cs>>>(x, result, n);
-      ctx->pg_tail_launches = 1;
+      E->tail_launches = 1;
     } else {
-      ctx->pg_tail_launches = 0;  // x is the result
+      E->tail_launches = 0;  // x is the result
     }
     if ((rc = end_capture(graph))) return restore(rc);
     restore(VFLIP_OK);
     ctx->launches = before_capture;  // captured launches count when the graph runs
-    if (cudaGraphInstantiate(&ctx->pg_exec, graph, 0) != cudaSuccess) {
-      ctx->pg_exec = nullptr;
+    if (cudaGraphInstantiate(&E->exec, graph, 0) != cudaSuccess) {
+      E->exec = nullptr;
       return ctx->fail(VFLIP_ERR_CUDA, "cudaGraphInstantiate failed (PCG loop)");
     }
-    ctx->pg_key = key;
+    E->key = key;
   }
-  if (cudaGraphLaunch(ctx->pg_exec, ctx->stream) != cudaSuccess)
+  E->used = ++ctx->pg_clock;
+  if (cudaGraphLaunch(E->exec, ctx->stream) != cudaSuccess)
     return ctx->fail(VFLIP_ERR_CUDA, "cudaGraphLaunch (PCG loop)");
   int iters = 0;
   VF_CUDA(cudaMemcpyAsync(ctx->st_host, ctx->st, sizeof(PcgScalars), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1153,30 +1171,33 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
   int rc;
   if ((rc = check_kernel_error(ctx, ctx->st_host->kernel_error))) return rc;
   const PcgScalars& h = *ctx->st_host;
-  ctx->launches += ctx->pg_init_launches + (unsigned long long)iters * ctx->pg_body_launches + ctx->pg_tail_launches;
-  if (!h.converged || h.bad_rho) return VFLIP_OK;  // the host loop repeats the solve
+  ctx->launches += E->init_launches + (unsigned long long)iters * E->body_launches + E->tail_launches;
+  const bool ok = h.converged && !h.bad_rho;
+  // a failed plain solve is repeated by the host loop (its exact statistics);
+  // a failed warm start is reported as such (the caller decides what follows)
+  if (!ok && !warm) return VFLIP_OK;
   if (stats) {
     stats->iterations = iters;
     stats->vcycles = iters;
     stats->levels = (int)T.coarse.size() + 1;
-    stats->converged = 1;
+    stats->converged = ok ? 1 : 0;
     stats->residual = h.res;
     stats->rhs_norm = h.rhs_norm;
   }
   *done = true;
-  return VFLIP_OK;
+  return ok ? VFLIP_OK : VFLIP_NOT_CONVERGED;
 }
 
 // AMGPCGSolve (AlgebraicMultigrid.h:189-301) with the outer vectors in W.
 // warm: the caller has set x (the result), r, its V copy and the scalars
-// (tolerance from |rhs|_inf, |r|_inf of the initial guess); host loop.
+// (tolerance from |rhs|_inf, |r|_inf of the initial guess).
 template <typename W, typename S0, typename SC, typename V>
 int pcg_solve_w(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* result, double tol_factor,
                 int maxit, vflip_solve_stats* stats, V* x1_out, bool warm = false) {
   constexpr bool same = std::is_same<W, V>::value;
-  if (ctx->cfg.pcg_loop == 0 && !ctx->profiling && !x1_out && !warm) {
+  if (ctx->cfg.pcg_loop == 0 && !ctx->profiling && !x1_out) {
     bool done = false;
-    const int grc = pcg_solve_graph<W>(ctx, T, rhs, result, tol_factor, maxit, stats, &done);
+    const int grc = pcg_solve_graph<W>(ctx, T, rhs, result, tol_factor, maxit, stats, &done, warm);
     if (grc < 0 || done) return grc;
   }
   const Dims d = T.fine.d;
@@ -1338,7 +1359,13 @@ int learned_capture(vflip_ctx* ctx, const LearnedOpts& lo, const Dims& d, const 
 // vectors: G gamma = g with G_ij = w_i.A w_j (upper triangle first in
 // `dots`, then g_i = w_i.b); vectors whose pivot collapses (linearly
 // dependent, zero, or non-finite) are dropped.  Returns the kept count.
-int ritz_solve(const double* dots, const bool* use, double* gamma) {
+__host__ __device__ inline bool finite_d(double v) { return (v - v) == 0.0; }
+
+// gamma = argmin of the energy over the subspace of the vectors in use:
+// G gamma = W^T b by Cholesky of the diagonally scaled Gram matrix, dropping
+// a vector whose pivot is not positive or not finite and starting again.
+// Returns the subspace dimension (0: gamma = 0).
+__host__ __device__ int ritz_solve(const double* dots, const bool* use, double* gamma) {
   constexpr int M = kRitzVecs;
   double G[M][M], g[M];
   int k = 0;
@@ -1348,7 +1375,7 @@ int ritz_solve(const double* dots, const bool* use, double* gamma) {
   bool on[M];
   for (int i = 0; i < M; ++i) {
     gamma[i] = 0.0;
-    on[i] = use[i] && G[i][i] > 0.0 && std::isfinite(G[i][i]) && std::isfinite(g[i]);
+    on[i] = use[i] && G[i][i] > 0.0 && finite_d(G[i][i]) && finite_d(g[i]);
   }
   for (int attempt = 0; attempt < M; ++attempt) {
     int idx[M], m = 0;
@@ -1357,13 +1384,13 @@ int ritz_solve(const double* dots, const bool* use, double* gamma) {
     if (m == 0) return 0;
     // Cholesky of the diagonally scaled subset
     double L[M][M] = {}, sc[M];
-    for (int a = 0; a < m; ++a) sc[a] = 1.0 / std::sqrt(G[idx[a]][idx[a]]);
+    for (int a = 0; a < m; ++a) sc[a] = 1.0 / sqrt(G[idx[a]][idx[a]]);
     int bad = -1;
     for (int a = 0; a < m && bad < 0; ++a) {
       for (int b = 0; b <= a; ++b) {
         double v = G[idx[a]][idx[b]] * sc[a] * sc[b];
         for (int c = 0; c < b; ++c) v -= L[a][c] * L[b][c];
-        if (!std::isfinite(v)) {
+        if (!finite_d(v)) {
           bad = a;
           break;
         }
@@ -1372,7 +1399,7 @@ int ritz_solve(const double* dots, const bool* use, double* gamma) {
             bad = a;
             break;
           }
-          L[a][a] = std::sqrt(v);
+          L[a][a] = sqrt(v);
         } else {
           L[a][b] = v / L[b][b];
         }
@@ -1397,6 +1424,24 @@ int ritz_solve(const double* dots, const bool* use, double* gamma) {
     return m;
   }
   return 0;
+}
+
+// The 2 x 2 Ritz step of the warm-start correction on the device: dots =
+// (p.Ap, p.Ae, e.Ae, p.b, e.b); out = (gamma_p, gamma_e, subspace dim).
+__global__ void ritz2_solve_kernel(const double* __restrict__ dots, int use_net, double* __restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double full[kRitzSums] = {};
+  full[0] = dots[0];                          // G00
+  full[1] = dots[1];                          // G01
+  full[kRitzVecs] = dots[2];                  // G11
+  full[kRitzSums - kRitzVecs] = dots[3];      // g0
+  full[kRitzSums - kRitzVecs + 1] = dots[4];  // g1
+  const bool use[kRitzVecs] = {true, use_net != 0, false, false};
+  double gamma[kRitzVecs];
+  const int m = ritz_solve(full, use, gamma);
+  out[0] = gamma[0];
+  out[1] = gamma[1];
+  out[2] = (double)m;
 }
 
 template <typename S0, typename SC, typename V>
@@ -1713,28 +1758,24 @@ int learned_resid_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, 
   VF_LAUNCH_CHECK();
   ritz2_fold_kernel<kRedBlock><<<1, kRedBlock, 0, ctx->stream>>>(ctx->partials, rb, dots);
   VF_LAUNCH_CHECK();
-  double h5[5];
-  VF_CUDA(cudaMemcpyAsync(h5, dots, sizeof h5, cudaMemcpyDeviceToHost, ctx->stream));
-  VF_CUDA(cudaStreamSynchronize(ctx->stream));
-  // the 2 x 2 system in ritz_solve's layout (upper G row by row, then W^T b)
-  double full[kRitzSums] = {};
-  full[0] = h5[0];                 // G00
-  full[1] = h5[1];                 // G01
-  full[kRitzVecs] = h5[2];         // G11
-  full[kRitzSums - kRitzVecs] = h5[3];      // g0
-  full[kRitzSums - kRitzVecs + 1] = h5[4];  // g1
-  const bool use[kRitzVecs] = {true, use_net, false, false};
-  ls.subspace = ritz_solve(full, use, ls.gamma);
-  ritz2_combine_kernel<V, kRedBlock><<<grid_for(n, kRedBlock, ctx->num_sms), kRedBlock, 0, ctx->stream>>>(
-      pp, q1, e, q2, rhs, ls.gamma[0], ls.gamma[1], o.x, o.r, o.rv, n, ctx->partials, ctx->st);
+  // the Ritz step and the combination stay on the device (no host round trip)
+  ritz2_solve_kernel<<<1, 32, 0, ctx->stream>>>(dots, use_net ? 1 : 0, dots + 5);
   VF_LAUNCH_CHECK();
-  if ((rc = read_scalars(ctx))) return rc;
-  ls.init_residual = ctx->st_host->res;
+  ritz2_combine_kernel<V, kRedBlock><<<grid_for(n, kRedBlock, ctx->num_sms), kRedBlock, 0, ctx->stream>>>(
+      pp, q1, e, q2, rhs, dots + 5, o.x, o.r, o.rv, n, ctx->partials, ctx->st);
+  VF_LAUNCH_CHECK();
+  // the initial residual, kept for the statistics before the loop overwrites it
+  VF_CUDA(cudaMemcpyAsync(dots + 3, &ctx->st->res, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
   vflip_solve_stats st2{};
-  rc = std::isfinite(ls.init_residual)
-           ? pcg_solve_w<double>(ctx, T, rhs, result, tol_factor, maxit, &st2, (V*)nullptr, true)
-           : VFLIP_NOT_CONVERGED;
+  rc = pcg_solve_w<double>(ctx, T, rhs, result, tol_factor, maxit, &st2, (V*)nullptr, true);
   if (rc < 0) return rc;
+  double h4[5];
+  VF_CUDA(cudaMemcpyAsync(h4, dots + 3, sizeof h4, cudaMemcpyDeviceToHost, ctx->stream));
+  VF_CUDA(cudaStreamSynchronize(ctx->stream));
+  ls.init_residual = h4[0];
+  ls.gamma[0] = h4[2];
+  ls.gamma[1] = h4[3];
+  ls.subspace = (int)h4[4];
   if (rc != VFLIP_OK) {  // plain MGPCG from zero decides
     vflip_solve_stats st3{};
     const int code = pcg_solve(ctx, T, rhs, result, tol_factor, maxit, &st3);
@@ -2313,8 +2354,10 @@ int vflip_destroy(vflip_ctx* ctx) {
   if (!ctx) return VFLIP_ERR_ARG;
   cudaStreamSynchronize(ctx->stream);
   for (vflip_ctx* sub : ctx->subs) vflip_destroy(sub);
-  if (ctx->pg_exec) cudaGraphExecDestroy(ctx->pg_exec);
-  if (ctx->pg_graph) cudaGraphDestroy(ctx->pg_graph);
+  for (auto& g : ctx->pgs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+  }
   if (ctx->pg_stream) cudaStreamDestroy(ctx->pg_stream);
   for (auto& kv : ctx->bufs) cudaFree(kv.second.first);
   if (ctx->st) cudaFree(ctx->st);
