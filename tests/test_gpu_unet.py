@@ -117,6 +117,35 @@ def test_network_forward_matches_oracle(net):
     assert np.array_equal(got, again)  # deterministic
 
 
+def test_network_forward_replay_follows_inputs_and_weights(net):
+    """vflip_unet_forward replays a captured graph when the grid and the
+    buffers repeat: new input values and new weights in the same buffers
+    give the eager forward's bits (the training path's forward), and the
+    oracle's answer for the new weights."""
+    rng = np.random.default_rng(12)
+    S = 16
+    a, t2, wgt = _sample(S, rng)
+    b, _, _ = _sample(S, rng)
+    in2 = torch.from_numpy(a).cuda()
+    out2 = torch.empty((S, S, S, 2), dtype=torch.float32, device="cuda")
+    p0 = net.get_params()
+    try:
+        net.forward(in2, out2)
+        in2.copy_(torch.from_numpy(b))
+        got_b = net.forward(in2, out2).clone()
+        net.set_params(p0 * 0.9)
+        got_b2 = net.forward(in2, out2).clone()
+        want, _ = uo.forward(net.get_params().astype(np.float64), b.astype(np.float64), round_acts=True)
+        assert rel(got_b2.cpu().numpy(), want) < 2e-2
+        assert not torch.equal(got_b, got_b2)
+        # the training path runs the same forward eagerly: the same output
+        net.gradients(in2, torch.from_numpy(t2).cuda(), torch.from_numpy(wgt).cuda())
+        again = net.forward(in2, out2)
+        assert torch.equal(again, got_b2)
+    finally:
+        net.set_params(p0)
+
+
 def test_network_gradients_match_oracle(net):
     rng = np.random.default_rng(12)
     S = 16

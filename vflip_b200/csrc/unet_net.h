@@ -42,6 +42,11 @@ class Net {
   int init_status() const { return init_rc; }
 
   int forward(int X, int Y, int Z, const float* in2, float* out2);
+  // The same forward pass replayed as a CUDA graph, captured once per
+  // (grid, buffers) and launched on `stream`: the inference path, whose
+  // ~30 launches would otherwise each pay a host-side launch and
+  // tensor-map encode.  Bitwise the eager pass.
+  int forward_replay(int X, int Y, int Z, const float* in2, float* out2);
   int backward(const float* target2, const float* weight, float cw0, float cw1, double* loss);
   int adam(float lr, float b1 = 0.9f, float b2 = 0.999f, float eps = 1e-8f);
   int repack();
@@ -81,6 +86,11 @@ class Net {
   std::vector<std::pair<void*, size_t>> scratch_;
   void* act_mem = nullptr;
   size_t act_bytes = 0;
+  cudaStream_t cap_stream = nullptr;  // capture stream of forward_replay
+  cudaGraph_t fwd_graph = nullptr;
+  cudaGraphExec_t fwd_exec = nullptr;
+  std::vector<uintptr_t> fwd_key;
+  long long fwd_launches = 0;
 };
 
 }  // namespace unet

@@ -1543,7 +1543,7 @@ int learned_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double
     VF_CUDA(cudaEventCreate(&na));
     VF_CUDA(cudaEventCreate(&nb));
     cudaEventRecord(na, ctx->stream);
-    rc = net.forward(X, Y, Z, in2, out2);
+    rc = net.forward_replay(X, Y, Z, in2, out2);
     cudaEventRecord(nb, ctx->stream);
     if (!rc) rc = net.sync_error();
     net.stream = saved;
@@ -1723,7 +1723,7 @@ int learned_resid_solve(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, 
     VF_CUDA(cudaEventCreate(&na));
     VF_CUDA(cudaEventCreate(&nb));
     cudaEventRecord(na, ctx->stream);
-    rc = net.forward(X, Y, Z, in2, out2);
+    rc = net.forward_replay(X, Y, Z, in2, out2);
     cudaEventRecord(nb, ctx->stream);
     if (!rc) rc = net.sync_error();
     net.stream = saved;
