@@ -231,9 +231,19 @@ def run_vflip(a):
     # library's events around every fine-level sweep (that pass runs the host
     # PCG loop, whose launches can carry events; the kernels are the same)
     solver.set_profiling(True)
-    for _ in range(min(a.steps, 5)):
+    nprof = min(a.steps, 5)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record()
+    for _ in range(nprof):
         sim.step()
+    p1.record()
     torch.cuda.synchronize()
+    # where a step's device time goes (per step, from the same events; spans
+    # nest: the V-cycle holds the fine sweeps and the coarse part)
+    breakdown = {"steps": nprof, "step_ms_with_events": p0.elapsed_time(p1) / nprof}
+    for kind in ("vcycle", "coarse", "fine_sweep", "spmv", "update", "advect_field", "advect_pair"):
+        cnt, kms = solver.profile_kernels(kind)
+        breakdown[kind] = {"per_step": cnt / nprof, "ms_per_step": kms / nprof}
     n_sweeps, sweep_ms, cells = solver.profile_sweeps()
     solver.set_profiling(False)
 
@@ -285,6 +295,7 @@ def run_vflip(a):
                     "h2d_bytes_per_step": sim.host_bytes(), "d2h_bytes_per_step": sim.host_bytes()},
             "gpu_launches": launches,
             "clocks": clk,
+            "step_breakdown": breakdown,
         }
         if dropin:
             out["dropin_host"] = dropin

@@ -519,7 +519,10 @@ int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const vo
  * CUDA events on its stream (the PCG loop then runs on the host, whose
  * launches can carry events): the fine-level smoothing sweep (the dominant
  * kernel), the fine-level PCG SpMV and update, and the RK2 advection
- * launches (one field; a pair of fields on one backtrace).  vflip_profile_kernels synchronises the stream and returns the
+ * launches (one field; a pair of fields on one backtrace); and, as spans of
+ * several launches, each V-cycle of the PCG (VCYCLE) and its part below the
+ * fine level (COARSE: the levels >= 1, from after the fine restriction to
+ * the fine prolongation).  vflip_profile_kernels synchronises the stream and returns the
  * number of timed launches of one kind and their summed device time;
  * vflip_profile_sweeps returns the fine sweeps' figures and the fine level's
  * cell count, then starts a new count for every kind.  Enabling (again)
@@ -529,6 +532,8 @@ int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const vo
 #define VFLIP_PROF_UPDATE 2
 #define VFLIP_PROF_ADVECT_FIELD 3
 #define VFLIP_PROF_ADVECT_PAIR 4
+#define VFLIP_PROF_VCYCLE 5
+#define VFLIP_PROF_COARSE 6
 int vflip_set_profiling(vflip_ctx* ctx, int enable);
 int vflip_profile_sweeps(vflip_ctx* ctx, int* launches, double* total_ms, double* cells);
 int vflip_profile_kernels(vflip_ctx* ctx, int kind, int* launches, double* total_ms);

@@ -844,9 +844,11 @@ int vcycle(vflip_ctx* ctx, Typed<S0, SC, V>& T, const V* r, V* z, bool want_dot)
     return VFLIP_OK;
   }
   std::vector<V*> after_pre(nl, nullptr);
+  const int vslot = prof_start(ctx, VFLIP_PROF_VCYCLE, ctx->stream);
   // down
   if ((rc = smooth_down<S0, SC, V, S0>(ctx, T.fine, r, &after_pre[0]))) return rc;
   if ((rc = restrict_to<S0, V, V>(ctx, T.fine, after_pre[0], r, T.coarse[0].b, T.coarse[0].d))) return rc;
+  const int cslot = prof_start(ctx, VFLIP_PROF_COARSE, ctx->stream);
   for (int l = 1; l < nl - 1; ++l) {
     Level<SC, V>& L = T.coarse[l - 1];
     if ((rc = smooth_down<S0, SC, V, SC>(ctx, L, L.b, &after_pre[l]))) return rc;
@@ -865,11 +867,13 @@ int vcycle(vflip_ctx* ctx, Typed<S0, SC, V>& T, const V* r, V* z, bool want_dot)
     xc = res;
     cd = L.d;
   }
+  prof_stop(ctx, cslot, ctx->stream);
   int dot_blocks = 0;
   V* res;
   if ((rc = smooth_up<S0, V>(ctx, T.fine, r, after_pre[0], xc, cd, z, want_dot ? ctx->partials : nullptr,
                              &dot_blocks, &res)))
     return rc;
+  prof_stop(ctx, vslot, ctx->stream);
   if (want_dot) {
     if (dot_blocks > 0) {
       fold_kernel<kRedBlock><<<1, kRedBlock, 0, ctx->stream>>>(ctx->partials, dot_blocks, ctx->st, kReduceRho, 0.0);

@@ -551,7 +551,8 @@ class Solver:
         self._check(self.lib.vflip_profile_sweeps(self.ctx, C.byref(n), C.byref(ms), C.byref(cells)))
         return n.value, ms.value, cells.value
 
-    PROF_KINDS = {"fine_sweep": 0, "spmv": 1, "update": 2, "advect_field": 3, "advect_pair": 4}
+    PROF_KINDS = {"fine_sweep": 0, "spmv": 1, "update": 2, "advect_field": 3, "advect_pair": 4, "vcycle": 5,
+                  "coarse": 6}
 
     def profile_kernels(self, kind):
         """(launches, total_ms) of the timed launches of one kind (PROF_KINDS)."""
