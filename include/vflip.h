@@ -126,6 +126,13 @@ typedef struct {
    * kernel (0 = as many as fit).  vflip_b200/tune.py picks both per batch. */
   int batch_chunk;
   int batch_ctas_per_sm;
+  /* Small end of the V-cycle in FP32/MIXED contexts: 0 (default) =
+   * automatic: every level from the first coarse level of at most 4096
+   * cells down to the coarsest runs in ONE launch of one CTA (the levels in
+   * shared memory, colour passes separated by CTA barriers), where that
+   * level is not itself the coarsest; 1 = one launch per sweep, restriction
+   * and coarsest solve.  Same bits. */
+  int coarse_tail;
 } vflip_config;
 
 typedef struct {

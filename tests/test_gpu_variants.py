@@ -1,7 +1,8 @@
 """Entry points and kernel variants that must agree with the ones they stand for:
   * the one-call u, v, w advection gives the three single calls' bits;
   * the plane-marching PCG SpMV gives the column kernel's iterations and,
-    up to the grouping of its s.q partial sums, its solution."""
+    up to the grouping of its s.q partial sums, its solution;
+  * the one-CTA V-cycle tail gives the per-level launches' bits."""
 import numpy as np
 import pytest
 
@@ -60,3 +61,31 @@ def test_plane_spmv_matches_column_kernel(prec):
     (a, ia), (b, ib) = res
     assert ia == ib
     assert float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b)) < (1e-10 if prec == 0 else 1e-5)
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+@pytest.mark.parametrize("dims,direct", [((64, 64, 64), 0), ((80, 72, 64), 0), ((64, 64, 64), 1),
+                                         ((128, 96, 72), 0)])
+def test_vcycle_tail_matches_per_level_launches(prec, dims, direct):
+    """The levels from the first one of <= 4096 cells down run in one CTA
+    (coarse_tail 0); one launch per sweep (coarse_tail 1) gives the same
+    V-cycle bit for bit, with the FP64 direct coarsest solve or with the
+    coarsest sweeps (coarsest_solver 1), and so the same solve."""
+    from vflip_b200.solver import Solver
+
+    ni, nj, nk = dims
+    pr = scenes.projection_problem(ni, nj, nk, seed=11, inflow=True, solid_velocity=True)
+    st = rhs = None
+    out = []
+    for tail in (0, 1):
+        with Solver(precision=prec, coarse_tail=tail, coarsest_solver=direct) as s:
+            if st is None:
+                st, rhs = s.assemble(ni, nj, nk, pr["h"], pr["U_in"], t(pr["phi"]), t(pr["bdesc"]), t(pr["us"]),
+                                     t(pr["vs"]), t(pr["ws"]), t(pr["u"]), t(pr["v"]), t(pr["w"]))
+            z = s.vcycle(st, rhs).clone()
+            ok, x, stats = s.amgpcg_solve(st, rhs, 1e-6, 100)
+            assert ok
+            out.append((z, x.clone(), stats.iterations))
+    (za, xa, ia), (zb, xb, ib) = out
+    assert torch.equal(za, zb)
+    assert torch.equal(xa, xb) and ia == ib

@@ -93,36 +93,14 @@ __global__ void __launch_bounds__(BLOCK) coarse_chol_kernel(const double* __rest
   if (tid == 0) *ok_flag = ok;
 }
 
-// One CTA: x = A^-1 b from the band factor, in FP64, blocked by 32 columns.
-// With `staged`, the factor and the reciprocal pivots are first copied into
-// shared memory (the whole solve then reads no global memory but b).
-// Forward (L y = b): warp 0 solves each 32 x 32 diagonal block with
-// shuffles, then all threads subtract the block's contribution from the
-// next bw rows.  Backward (L^T x = y), blocks from the last: all threads
-// first subtract the contributions of the rows already solved, then warp 0
-// solves the block's transposed triangle.  With `dot_out`, also writes
-// sum(x * b) (the PCG z.r when this level is the whole V-cycle).
-// Returns at once unless *ok_flag is set.
-template <typename V, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) coarse_chol_solve_kernel(const V* __restrict__ b, V* __restrict__ x_out,
-                                                                  int n, int bw, const double* Lc,
-                                                                  const double* rinv,
-                                                                  const int* __restrict__ ok_flag,
-                                                                  double* __restrict__ dot_out, int staged) {
-  if (*ok_flag == 0) return;
-  extern __shared__ double y[];  // n values: y, then x in place; then the staged factor
-  __shared__ double red[BLOCK / 32];
+// The band solve of coarse_chol_solve_kernel on y (shared memory, n
+// values: b in, x out) by the whole CTA (nthreads >= 256 threads; the
+// column sums of the backward pass use 8 threads per column of a 32-column
+// block).  Every thread of the CTA calls it; it ends with a barrier.
+__device__ __forceinline__ void chol_band_solve_block(double* y, int n, int bw, const double* Lc, const double* rinv,
+                                                      int nthreads) {
   constexpr unsigned FULL = 0xffffffffu;
   const int B1 = bw + 1, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int e = tid; e < n; e += BLOCK) y[e] = (double)ldv(b + e);
-  if (staged) {
-    double* sL = y + n;
-    for (int e = tid; e < n * B1; e += BLOCK) sL[e] = Lc[e];
-    for (int e = tid; e < n; e += BLOCK) sL[n * B1 + e] = rinv[e];
-    Lc = sL;
-    rinv = sL + (size_t)n * B1;
-  }
-  __syncthreads();
   // ---- forward
   for (int kb = 0; kb < n; kb += 32) {
     const int nb = min(32, n - kb);
@@ -139,7 +117,7 @@ __global__ void __launch_bounds__(BLOCK) coarse_chol_solve_kernel(const V* __res
     __syncthreads();
     // rows below the block that the band reaches
     const int r0 = kb + nb, r1 = min(n, kb + nb + bw);
-    for (int i = r0 + tid; i < r1; i += BLOCK) {
+    for (int i = r0 + tid; i < r1; i += nthreads) {
       double s = y[i];
       for (int c = 0; c < nb; ++c) {
         const int d = i - (kb + c);
@@ -181,6 +159,39 @@ __global__ void __launch_bounds__(BLOCK) coarse_chol_solve_kernel(const V* __res
     }
     __syncthreads();
   }
+}
+
+// One CTA: x = A^-1 b from the band factor, in FP64, blocked by 32 columns.
+// With `staged`, the factor and the reciprocal pivots are first copied into
+// shared memory (the whole solve then reads no global memory but b).
+// Forward (L y = b): warp 0 solves each 32 x 32 diagonal block with
+// shuffles, then all threads subtract the block's contribution from the
+// next bw rows.  Backward (L^T x = y), blocks from the last: all threads
+// first subtract the contributions of the rows already solved, then warp 0
+// solves the block's transposed triangle.  With `dot_out`, also writes
+// sum(x * b) (the PCG z.r when this level is the whole V-cycle).
+// Returns at once unless *ok_flag is set.
+template <typename V, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) coarse_chol_solve_kernel(const V* __restrict__ b, V* __restrict__ x_out,
+                                                                  int n, int bw, const double* Lc,
+                                                                  const double* rinv,
+                                                                  const int* __restrict__ ok_flag,
+                                                                  double* __restrict__ dot_out, int staged) {
+  if (*ok_flag == 0) return;
+  extern __shared__ double y[];  // n values: y, then x in place; then the staged factor
+  __shared__ double red[BLOCK / 32];
+  constexpr unsigned FULL = 0xffffffffu;
+  const int B1 = bw + 1, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < n; e += BLOCK) y[e] = (double)ldv(b + e);
+  if (staged) {
+    double* sL = y + n;
+    for (int e = tid; e < n * B1; e += BLOCK) sL[e] = Lc[e];
+    for (int e = tid; e < n; e += BLOCK) sL[n * B1 + e] = rinv[e];
+    Lc = sL;
+    rinv = sL + (size_t)n * B1;
+  }
+  __syncthreads();
+  chol_band_solve_block(y, n, bw, Lc, rinv, BLOCK);
   double dot = 0.0;
   for (int e = tid; e < n; e += BLOCK) {
     const V o = cvt<V>(y[e]);

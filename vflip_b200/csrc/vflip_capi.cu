@@ -33,6 +33,7 @@
 #include "smoother_carry.cuh"
 #include "coarse_direct.cuh"
 #include "batch_kernels.cuh"
+#include "tail_kernels.cuh"
 #include "tmap.h"
 #include "unet_net.h"
 
@@ -45,6 +46,7 @@ constexpr int kRedBlock = 256;
 constexpr int kCoarseBlock = 1024;
 constexpr int kMaxPartials = 1 << 16;
 constexpr int kPcgGraphs = 4;  // PCG loop graphs kept per context
+constexpr size_t kTailSmemMax = 220 * 1024;
 
 struct Dims {
   int ni, nj, nk;
@@ -780,6 +782,55 @@ int make_typed(vflip_ctx* ctx, const Hierarchy64& H, const double* d0, const dou
 }
 
 // ---------------------------------------------------------------- V-cycle
+// The first level of the one-CTA tail (tail_kernels.cuh): the first coarse
+// level of at most kTailMaxCells cells, when the context runs FP32 vectors
+// in the V-cycle, the tail is on, that level is not the coarsest and its
+// levels fit the CTA's shared memory; else -1.
+template <typename S0, typename SC, typename V>
+int tail_start(const vflip_ctx* ctx, const Typed<S0, SC, V>& T, size_t* smem_bytes) {
+  if (!std::is_same<V, float>::value || ctx->cfg.coarse_tail != 0) return -1;
+  const int nl = (int)T.coarse.size() + 1;
+  for (int l = 1; l < nl - 1; ++l) {
+    if (T.coarse[l - 1].d.n() > (size_t)kTailMaxCells) continue;
+    if (nl - l > kTailMaxLevels) return -1;
+    size_t fl = 0;
+    for (int k = l; k < nl; ++k) fl += tail_level_floats((int)T.coarse[k - 1].d.n());
+    const size_t bytes = ((fl + 1) & ~(size_t)1) * sizeof(float) + T.coarse[nl - 2].d.n() * sizeof(double);
+    if (bytes > kTailSmemMax) return -1;
+    *smem_bytes = bytes;
+    return l;
+  }
+  return -1;
+}
+
+// Levels t .. nl-1 in one launch: b = level t's right-hand side, x its result.
+template <typename S0, typename SC, typename V>
+int launch_tail(vflip_ctx* ctx, const Typed<S0, SC, V>& T, int t, size_t smem, const V* b, V* x) {
+  const int nl = (int)T.coarse.size() + 1;
+  TailArgs<SC, V> a{};
+  a.nlev = nl - t;
+  for (int k = t; k < nl; ++k) {
+    const Level<SC, V>& L = T.coarse[k - 1];
+    a.lv[k - t] = TailLevel<SC>{L.d.ni, L.d.nj, L.d.nk, L.diag, L.xp, L.yp, L.zp};
+  }
+  a.b = b;
+  a.x = x;
+  a.pre = ctx->cfg.pre_sweeps;
+  a.post = ctx->cfg.post_sweeps;
+  a.coarse_sweeps = ctx->cfg.coarse_sweeps;
+  a.direct = T.direct.on ? 1 : 0;
+  a.bw = T.direct.bw;
+  a.L = T.direct.L;
+  a.rinv = T.direct.rinv;
+  a.ok = T.direct.ok;
+  auto kern = tail_vcycle_kernel<SC, V>;
+  if (smem_optin((const void*)kern, (int)kTailSmemMax) != cudaSuccess)
+    return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the V-cycle tail's shared memory limit");
+  kern<<<1, kTailThreads, smem, ctx->stream>>>(a);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
 // amgVCycle (AlgebraicMultigrid.h:130-176) from x = 0.  Level l >= 1 runs
 // on T.coarse[l-1].  Returns the level's final x through *xout.
 template <typename S0, typename SC, typename V, typename S>
@@ -844,23 +895,30 @@ int vcycle(vflip_ctx* ctx, Typed<S0, SC, V>& T, const V* r, V* z, bool want_dot)
     return VFLIP_OK;
   }
   std::vector<V*> after_pre(nl, nullptr);
+  size_t tail_smem = 0;
+  const int t = tail_start(ctx, T, &tail_smem);
+  const int bottom = t > 0 ? t : nl - 1;  // the levels from here down run as one unit
   const int vslot = prof_start(ctx, VFLIP_PROF_VCYCLE, ctx->stream);
   // down
   if ((rc = smooth_down<S0, SC, V, S0>(ctx, T.fine, r, &after_pre[0]))) return rc;
   if ((rc = restrict_to<S0, V, V>(ctx, T.fine, after_pre[0], r, T.coarse[0].b, T.coarse[0].d))) return rc;
   const int cslot = prof_start(ctx, VFLIP_PROF_COARSE, ctx->stream);
-  for (int l = 1; l < nl - 1; ++l) {
+  for (int l = 1; l < bottom; ++l) {
     Level<SC, V>& L = T.coarse[l - 1];
     if ((rc = smooth_down<S0, SC, V, SC>(ctx, L, L.b, &after_pre[l]))) return rc;
     if ((rc = restrict_to<SC, V, V>(ctx, L, after_pre[l], L.b, T.coarse[l].b, T.coarse[l].d))) return rc;
   }
-  // bottom
-  Level<SC, V>& B = T.coarse[nl - 2];
-  if ((rc = coarsest<SC, V>(ctx, B, B.b, B.xa, ctx->cfg.coarse_sweeps, nullptr, &T.direct))) return rc;
+  // bottom: the coarsest level, or the one-CTA tail from level t down
+  Level<SC, V>& B = T.coarse[bottom - 1];
+  if (t > 0) {
+    if ((rc = launch_tail(ctx, T, t, tail_smem, B.b, B.xa))) return rc;
+  } else if ((rc = coarsest<SC, V>(ctx, B, B.b, B.xa, ctx->cfg.coarse_sweeps, nullptr, &T.direct))) {
+    return rc;
+  }
   V* xc = B.xa;
   Dims cd = B.d;
   // up
-  for (int l = nl - 2; l >= 1; --l) {
+  for (int l = bottom - 1; l >= 1; --l) {
     Level<SC, V>& L = T.coarse[l - 1];
     V* res;
     if ((rc = smooth_up<SC, V>(ctx, L, L.b, after_pre[l], xc, cd, nullptr, nullptr, nullptr, &res))) return rc;
@@ -2304,6 +2362,7 @@ void vflip_config_default(vflip_config* cfg) {
   cfg->pcg_vectors = 0;
   cfg->batch_chunk = 0;
   cfg->batch_ctas_per_sm = 0;
+  cfg->coarse_tail = 0;
 }
 
 int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
@@ -2336,7 +2395,8 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
        ctx->cfg.smoother_threads != kTmaBlockWide) ||
       ctx->cfg.coarsest_solver < 0 || ctx->cfg.coarsest_solver > 2 || ctx->cfg.spmv_kernel < 0 ||
       ctx->cfg.spmv_kernel > 1 ||
-      ctx->cfg.pcg_loop < 0 || ctx->cfg.pcg_loop > 1 || ctx->cfg.pcg_vectors < 0 || ctx->cfg.pcg_vectors > 1 || ctx->cfg.batch_chunk < 0 || ctx->cfg.batch_ctas_per_sm < 0)
+      ctx->cfg.pcg_loop < 0 || ctx->cfg.pcg_loop > 1 || ctx->cfg.pcg_vectors < 0 || ctx->cfg.pcg_vectors > 1 || ctx->cfg.batch_chunk < 0 || ctx->cfg.batch_ctas_per_sm < 0 ||
+      ctx->cfg.coarse_tail < 0 || ctx->cfg.coarse_tail > 1)
     return bad(VFLIP_ERR_ARG);
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);
