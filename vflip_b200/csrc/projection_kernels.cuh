@@ -144,9 +144,15 @@ __global__ void assemble_kernel(const float* __restrict__ u, const float* __rest
                                 const float* __restrict__ ww, const float* __restrict__ us,
                                 const float* __restrict__ vs, const float* __restrict__ ws, double* __restrict__ diag,
                                 double* __restrict__ xp, double* __restrict__ yp, double* __restrict__ zp,
-                                double* __restrict__ rhs, float h, int ni, int nj, int nk, int variant, float dt) {
+                                double* __restrict__ rhs, float h, int ni, int nj, int nk, int variant, float dt,
+                                float inv_h) {
   const size_t n = (size_t)ni * nj * nk;
   const float h2 = h * h;
+  // x / h and x / h^2 as products when h is a power of two (inv_h != 0):
+  // the same correctly rounded quotients without the division sequence
+  const float inv_h2 = inv_h * inv_h;
+  auto div_h = [&](float x) { return inv_h != 0.0f ? x * inv_h : x / h; };
+  auto div_h2 = [&](float x) { return inv_h != 0.0f ? x * inv_h2 : x / h2; };
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     int i, j, k;
     decode3(e, ni, nj, i, j, k);
@@ -156,20 +162,20 @@ __global__ void assemble_kernel(const float* __restrict__ u, const float* __rest
       const size_t iv0 = lin3(i, j, k, ni, nj + 1), iv1 = lin3(i, j + 1, k, ni, nj + 1);
       const size_t iw0 = lin3(i, j, k, ni, nj), iw1 = lin3(i, j, k + 1, ni, nj);
       const bool sub = variant == 1;
-      auto term = [&](float wgt) { return sub ? (wgt * dt) / h2 : wgt / h2; };
+      auto term = [&](float wgt) { return sub ? div_h2(wgt * dt) : div_h2(wgt); };
       float t;
       t = term(uw[iu1]); d = (double)t; if (i < ni - 2) cx = (double)(-t);
-      b = b - (double)(uw[iu1] * u[iu1] / h);
+      b = b - (double)div_h(uw[iu1] * u[iu1]);
       t = term(uw[iu0]); d = d + (double)t;
-      b = b + (double)(uw[iu0] * u[iu0] / h);
+      b = b + (double)div_h(uw[iu0] * u[iu0]);
       t = term(vw[iv1]); d = d + (double)t; if (j < nj - 2) cy = (double)(-t);
-      b = b - (double)(vw[iv1] * v[iv1] / h);
+      b = b - (double)div_h(vw[iv1] * v[iv1]);
       t = term(vw[iv0]); d = d + (double)t;
-      b = b + (double)(vw[iv0] * v[iv0] / h);
+      b = b + (double)div_h(vw[iv0] * v[iv0]);
       t = term(ww[iw1]); d = d + (double)t; if (k < nk - 2) cz = (double)(-t);
-      b = b - (double)(ww[iw1] * w[iw1] / h);
+      b = b - (double)div_h(ww[iw1] * w[iw1]);
       t = term(ww[iw0]); d = d + (double)t;
-      b = b + (double)(ww[iw0] * w[iw0] / h);
+      b = b + (double)div_h(ww[iw0] * w[iw0]);
       if (d > 0) {
         float sv = (uw[iu1] - 1.0f) * us[iu1] - (uw[iu0] - 1.0f) * us[iu0] + (vw[iv1] - 1.0f) * vs[iv1] -
                    (vw[iv0] - 1.0f) * vs[iv0] + (ww[iw1] - 1.0f) * ws[iw1] - (ww[iw0] - 1.0f) * ws[iw0];
@@ -197,7 +203,7 @@ __global__ void gradient_kernel(const P* __restrict__ p, float* __restrict__ u, 
                                 float* __restrict__ w, const float* __restrict__ uw, const float* __restrict__ vw,
                                 const float* __restrict__ ww, const float* __restrict__ us,
                                 const float* __restrict__ vs, const float* __restrict__ ws, float h, int ni, int nj,
-                                int nk, int variant, float dt) {
+                                int nk, int variant, float dt, float inv_h) {
   const size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
   const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nu + nv + nw;
@@ -208,7 +214,9 @@ __global__ void gradient_kernel(const P* __restrict__ p, float* __restrict__ u, 
     auto upd = [&](float cur, double pc, double pm, float wgt, float solid) {
       if (!(wgt > 0)) return solid;
       float diff = (float)(pc - pm);
-      return sub ? cur - (dt * diff) / h : cur - diff / h;
+      // x / h as x * (1/h) when h is a power of two (inv_h != 0): the same bits
+      const float q = sub ? dt * diff : diff;
+      return cur - (inv_h != 0.0f ? q * inv_h : q / h);
     };
     if (e < nu) {
       int i, j, k;

@@ -2669,7 +2669,8 @@ int assemble_impl(vflip_ctx* ctx, int variant, int ni, int nj, int nk, float h, 
     VF_LAUNCH_CHECK();
   }
   assemble_kernel<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
-      u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, diag, xp, yp, zp, rhs, h, ni, nj, nk, variant, dt);
+      u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, diag, xp, yp, zp, rhs, h, ni, nj, nk, variant, dt,
+      (float)inv_pow2(h));
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
 }
@@ -2705,7 +2706,7 @@ int project_impl(vflip_ctx* ctx, int variant, int ni, int nj, int nk, float h, f
   size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
   float* wts = (float*)ctx->buf("face_weights", sizeof(float) * (nu + nv + nw));
   gradient_kernel<double><<<grid_for(nu + nv + nw, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
-      p, u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, h, ni, nj, nk, variant, dt);
+      p, u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, h, ni, nj, nk, variant, dt, (float)inv_pow2(h));
   ++ctx->launches;
   cudaError_t le = cudaGetLastError();
   if (le != cudaSuccess) {
