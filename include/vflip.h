@@ -133,6 +133,13 @@ typedef struct {
    * level is not itself the coarsest; 1 = one launch per sweep, restriction
    * and coarsest solve.  Same bits. */
   int coarse_tail;
+  /* Levels of at most this many cells (FP32/MIXED) sweep as independent 3-D
+   * tiles of 16 x 8 x 4 cells, each staged with a two-cell halo and relaxed
+   * in two barriers (no plane march: small levels live in L2 and the march's
+   * per-plane latency dominated them); 0 (default) = automatic: 262144
+   * (64^3); -1 = never.  The fine level's last sweep (which also forms z.r)
+   * always marches.  Same bits. */
+  int tile_sweep_max_cells;
 } vflip_config;
 
 typedef struct {

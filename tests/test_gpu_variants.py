@@ -2,7 +2,10 @@
   * the one-call u, v, w advection gives the three single calls' bits;
   * the plane-marching PCG SpMV gives the column kernel's iterations and,
     up to the grouping of its s.q partial sums, its solution;
-  * the one-CTA V-cycle tail gives the per-level launches' bits."""
+  * the one-CTA V-cycle tail gives the per-level launches' bits;
+  * the tiled sweep of the small levels gives the marching sweeps' bits;
+  * the projection's PCG, which reads the FP32 copies of the couplings it
+    assembled, gives the bits of the same solve on the FP64 operator."""
 import numpy as np
 import pytest
 
@@ -79,6 +82,51 @@ def test_vcycle_tail_matches_per_level_launches(prec, dims, direct):
     out = []
     for tail in (0, 1):
         with Solver(precision=prec, coarse_tail=tail, coarsest_solver=direct) as s:
+            if st is None:
+                st, rhs = s.assemble(ni, nj, nk, pr["h"], pr["U_in"], t(pr["phi"]), t(pr["bdesc"]), t(pr["us"]),
+                                     t(pr["vs"]), t(pr["ws"]), t(pr["u"]), t(pr["v"]), t(pr["w"]))
+            z = s.vcycle(st, rhs).clone()
+            ok, x, stats = s.amgpcg_solve(st, rhs, 1e-6, 100)
+            assert ok
+            out.append((z, x.clone(), stats.iterations))
+    (za, xa, ia), (zb, xb, ib) = out
+    assert torch.equal(za, zb)
+    assert torch.equal(xa, xb) and ia == ib
+
+
+@pytest.mark.parametrize("prec,loop", [(1, 0), (2, 0), (1, 1)])
+def test_projection_spmv_on_fp32_couplings(prec, loop):
+    """vflip_project's outer PCG reads the FP32 fine operator's couplings
+    (exact: the assembly writes every coupling as a float value) where
+    vflip_amgpcg_solve on the same FP64 operator reads the FP64 ones: the
+    same pressure bit for bit, and the same iterations."""
+    from vflip_b200.solver import Solver
+
+    ni, nj, nk = 128, 64, 48
+    pr = scenes.projection_problem(ni, nj, nk, seed=13, inflow=True, solid_velocity=True)
+    with Solver(precision=prec, pcg_loop=loop) as s:
+        args = [t(pr[k]) for k in ("phi", "bdesc", "us", "vs", "ws", "u", "v", "w")]
+        st, rhs = s.assemble(ni, nj, nk, pr["h"], pr["U_in"], *[a.clone() for a in args])
+        ok1, x1, st1 = s.amgpcg_solve(st, rhs, 1e-6, 100)
+        ok2, p2, st2 = s.project(ni, nj, nk, pr["h"], pr["U_in"], *args)
+        assert ok1 and ok2 and st1.iterations == st2.iterations
+        assert torch.equal(x1, p2)
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+@pytest.mark.parametrize("dims", [(128, 128, 128), (72, 40, 36), (64, 48, 17)])
+def test_tiled_sweep_matches_marching_sweeps(prec, dims):
+    """Levels of <= 64^3 cells sweep as independent halo tiles; with the tiles
+    off (tile_sweep_max_cells -1) every level marches: the same V-cycle bit
+    for bit (ragged last tiles on every axis included) and the same solve."""
+    from vflip_b200.solver import Solver
+
+    ni, nj, nk = dims
+    pr = scenes.projection_problem(ni, nj, nk, seed=17, inflow=True, solid_velocity=True)
+    st = rhs = None
+    out = []
+    for cells in (0, -1):
+        with Solver(precision=prec, tile_sweep_max_cells=cells) as s:
             if st is None:
                 st, rhs = s.assemble(ni, nj, nk, pr["h"], pr["U_in"], t(pr["phi"]), t(pr["bdesc"]), t(pr["us"]),
                                      t(pr["vs"]), t(pr["ws"]), t(pr["u"]), t(pr["v"]), t(pr["w"]))

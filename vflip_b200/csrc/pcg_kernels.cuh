@@ -110,11 +110,14 @@ __global__ void __launch_bounds__(BLOCK) pcg_init_kernel(const double* __restric
 // s_new are recomputed from z and s_old, so s_old is never overwritten.
 // TZ: the preconditioned residual's type (the V-cycle's vectors), which
 // may be narrower than the PCG vectors' T.
-template <typename T, bool FIRST, int BLOCK, typename TZ = T>
+// TO: storage of the off-diagonal couplings (T, or float where the FP64
+// operator's couplings are exactly FP32 values: products and sums then run
+// in T on the same values).
+template <typename T, bool FIRST, int BLOCK, typename TZ = T, typename TO = T>
 __global__ void __launch_bounds__(BLOCK) pcg_spmv_dot_kernel(const TZ* __restrict__ z, const T* __restrict__ s_old,
                                                             T* __restrict__ s_new, T* __restrict__ q,
-                                                            const T* __restrict__ diag, const T* __restrict__ xp,
-                                                            const T* __restrict__ yp, const T* __restrict__ zp,
+                                                            const T* __restrict__ diag, const TO* __restrict__ xp,
+                                                            const TO* __restrict__ yp, const TO* __restrict__ zp,
                                                             int ni, int nj, int nk, int kz, double* partials,
                                                             PcgScalars* st) {
   using A = typename Num<T>::Acc;
@@ -176,16 +179,16 @@ __device__ __forceinline__ Quad<T> ldq(const T* p) {
   return *reinterpret_cast<const Quad<T>*>(p);
 }
 
-template <typename T, bool FIRST, typename TZ = T>
+template <typename T, bool FIRST, typename TZ = T, typename TO = T>
 __global__ void __launch_bounds__(1024) pcg_spmv_dot_plane_kernel(
     const TZ* __restrict__ z, const T* __restrict__ s_old, T* __restrict__ s_new, T* __restrict__ q,
-    const T* __restrict__ diag, const T* __restrict__ xp, const T* __restrict__ yp, const T* __restrict__ zp,
+    const T* __restrict__ diag, const TO* __restrict__ xp, const TO* __restrict__ yp, const TO* __restrict__ zp,
     int ni, int nj, int nk, int ty, int kz, double* partials, PcgScalars* st) {
   using A = typename Num<T>::Acc;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int qx = threadIdx.x, ry = threadIdx.y, nq = blockDim.x, rows = blockDim.y;  // rows = ty + 2
-  Quad<T>* sbuf = reinterpret_cast<Quad<T>*>(smem_raw);  // [3][rows][nq]
-  Quad<T>* ybuf = sbuf + 3 * rows * nq;                   // [3][rows][nq]
+  Quad<T>* sbuf = reinterpret_cast<Quad<T>*>(smem_raw);                      // [3][rows][nq]
+  Quad<TO>* ybuf = reinterpret_cast<Quad<TO>*>(sbuf + 3 * rows * nq);        // [3][rows][nq]
   __shared__ double red[32];
   const int j = blockIdx.x * ty - 1 + ry;
   const bool in_row = j >= 0 && j < nj;
@@ -195,12 +198,12 @@ __global__ void __launch_bounds__(1024) pcg_spmv_dot_plane_kernel(
   const int i0 = 4 * qx;
   const double beta = FIRST ? 0.0 : st->beta;
   Quad<T> sm{}, sc{}, sp{};  // s of planes k-1, k, k+1 (relative to the q plane)
-  Quad<T> zprev{};           // zp of the plane below the q plane
+  Quad<TO> zprev{};          // zp of the plane below the q plane
   double dot = 0.0;
   for (int kk = kb - 1; kk <= ke; ++kk) {
     // s_new of plane kk on this thread's row
     Quad<T> snew{};
-    Quad<T> ypk{};
+    Quad<TO> ypk{};
     if (in_row && kk >= 0 && kk < nk) {
       const size_t g = (size_t)i0 + sy * j + szs * kk;
       const Quad<TZ> zq = ldq(z + g);
@@ -226,9 +229,11 @@ __global__ void __launch_bounds__(1024) pcg_spmv_dot_plane_kernel(
     if (interior && k >= kb && k < ke) {
       const size_t g = (size_t)i0 + sy * j + szs * k;
       const int br = (k + 3) % 3;
-      const Quad<T> dq = ldq(diag + g), xq = ldq(xp + g), zq = ldq(zp + g);
-      const Quad<T> yq = ybuf[(br * rows + ry) * nq + qx];
-      const Quad<T> sdn = sbuf[(br * rows + ry - 1) * nq + qx], ydn = ybuf[(br * rows + ry - 1) * nq + qx];
+      const Quad<T> dq = ldq(diag + g);
+      const Quad<TO> xq = ldq(xp + g), zq = ldq(zp + g);
+      const Quad<TO> yq = ybuf[(br * rows + ry) * nq + qx];
+      const Quad<T> sdn = sbuf[(br * rows + ry - 1) * nq + qx];
+      const Quad<TO> ydn = ybuf[(br * rows + ry - 1) * nq + qx];
       const Quad<T> sup = sbuf[(br * rows + ry + 1) * nq + qx];
       // x-neighbours: the left and right cells of each cell of the quad, and
       // the -x coupling (xp of the cell to the left)

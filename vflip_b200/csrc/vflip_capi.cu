@@ -34,6 +34,7 @@
 #include "coarse_direct.cuh"
 #include "batch_kernels.cuh"
 #include "tail_kernels.cuh"
+#include "sweep_tile.cuh"
 #include "tmap.h"
 #include "unet_net.h"
 
@@ -79,6 +80,7 @@ struct vflip_ctx {
   cudaStream_t stream = nullptr;
   std::string err;
   std::unordered_map<std::string, std::pair<void*, size_t>> bufs;
+  bool offdiag_f32 = false;  // the operator being solved was assembled here: its couplings are FP32 values
   void* hbuf = nullptr;  // pinned host staging of the host-buffer entry points
   size_t hbuf_bytes = 0;
   PcgScalars* st = nullptr;         // device
@@ -546,6 +548,54 @@ int sweep_t3d(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V
   return launch_t3d_t<S, false, false, true>(ctx, mp, a, grid, smem);
 }
 
+template <typename S, typename V, bool Z, bool P>
+int launch_tile_t(vflip_ctx* ctx, const SweepTileArgs<S, V>& a, int tiles) {
+  const int slot =
+      (size_t)a.ni * a.nj * a.nk == ctx->prof_fine_n ? prof_start(ctx, VFLIP_PROF_FINE_SWEEP, ctx->stream) : -1;
+  rbgs_sweep_tile_kernel<S, V, Z, P><<<tiles, kTileThreads, 0, ctx->stream>>>(a);
+  VF_LAUNCH_CHECK();
+  prof_stop(ctx, slot, ctx->stream);
+  return VFLIP_OK;
+}
+
+// The tiled sweep (sweep_tile.cuh) on FP32 levels of at most
+// tile_sweep_max_cells cells; not for a sweep that also forms z.r.
+template <typename S, typename V>
+int sweep_tile(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_out, const V* xc,
+               const Dims* cd, double* dot_partial, bool* used) {
+  *used = false;
+  if constexpr (!std::is_same<V, float>::value || std::is_same<S, double>::value) {
+    return VFLIP_OK;
+  } else {
+    const long long n = (long long)L.d.n();
+    if (dot_partial || ctx->cfg.tile_sweep_max_cells < 0 || n > ctx->cfg.tile_sweep_max_cells) return VFLIP_OK;
+    const bool zero = x_in == nullptr, pro = xc != nullptr;
+    if (zero && pro) return VFLIP_OK;
+    SweepTileArgs<S, V> a{};
+    a.x_in = x_in;
+    a.x_out = x_out;
+    a.b = b;
+    a.diag = L.diag;
+    a.xp = L.xp;
+    a.yp = L.yp;
+    a.zp = L.zp;
+    a.xc = xc;
+    a.ni = L.d.ni;
+    a.nj = L.d.nj;
+    a.nk = L.d.nk;
+    a.cni = cd ? cd->ni : 0;
+    a.cnj = cd ? cd->nj : 0;
+    a.ntx = (L.d.ni + kTileTX - 1) / kTileTX;
+    a.nty = (L.d.nj + kTileTY - 1) / kTileTY;
+    const long long tiles = (long long)a.ntx * a.nty * ((L.d.nk + kTileTZ - 1) / kTileTZ);
+    if (tiles > (1ll << 30)) return VFLIP_OK;
+    *used = true;
+    if (zero) return launch_tile_t<S, V, true, false>(ctx, a, (int)tiles);
+    if (pro) return launch_tile_t<S, V, false, true>(ctx, a, (int)tiles);
+    return launch_tile_t<S, V, false, false>(ctx, a, (int)tiles);
+  }
+}
+
 // One sweep x_in -> x_out on a level; x_in == nullptr means x = 0.
 template <typename S, typename V>
 int sweep(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_out, const V* xc, const Dims* cd,
@@ -553,6 +603,8 @@ int sweep(vflip_ctx* ctx, const Level<S, V>& L, const V* b, const V* x_in, V* x_
   using A = typename Num<V>::Acc;
   {
     bool used = false;
+    int trc = sweep_tile<S, V>(ctx, L, b, x_in, x_out, xc, cd, dot_partial, &used);
+    if (trc || used) return trc;
     int rc = sweep_t3d<S, V>(ctx, L, b, x_in, x_out, xc, cd, dot_partial, nblocks_out, &used);
     if (rc || used) return rc;
     rc = sweep_tma<S, V>(ctx, L, b, x_in, x_out, xc, cd, dot_partial, nblocks_out, &used);
@@ -969,17 +1021,17 @@ int read_scalars(vflip_ctx* ctx) {
 // runs where the fine rows are whole warps of quads (unless the context asks
 // for the column kernel, or `plane` is false: the batched graph keeps the
 // column kernel); both give the same q and s_new bits.
-template <typename W, typename Z = W>
+template <typename W, typename Z = W, typename O = W>
 int launch_spmv_dot(vflip_ctx* ctx, cudaStream_t stream, bool first, const Z* z, const W* s_old, W* s_new, W* q,
-                    const W* diag, const W* xp, const W* yp, const W* zp, const Dims& d, bool plane = true) {
+                    const W* diag, const O* xp, const O* yp, const O* zp, const Dims& d, bool plane = true) {
   const int nq = d.ni / 4;
   if (plane && ctx->cfg.spmv_kernel == 0 && d.ni % 128 == 0 && nq <= 256) {
     // about 384 threads a block (at 256 cells a row: 4 rows + 2 halo rows,
     // three blocks per SM) and two waves of blocks measured fastest
     const int ty = std::max(2, 384 / nq - 2);
     const int rows = ty + 2;
-    const size_t smem = 6 * (size_t)rows * nq * sizeof(Quad<W>);
-    auto kern = first ? pcg_spmv_dot_plane_kernel<W, true, Z> : pcg_spmv_dot_plane_kernel<W, false, Z>;
+    const size_t smem = 3 * (size_t)rows * nq * (sizeof(Quad<W>) + sizeof(Quad<O>));
+    auto kern = first ? pcg_spmv_dot_plane_kernel<W, true, Z, O> : pcg_spmv_dot_plane_kernel<W, false, Z, O>;
     if (smem_optin((const void*)kern, (int)smem) != cudaSuccess)
       return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the SpMV kernel's shared memory limit");
     int per_sm = 0;
@@ -1005,11 +1057,11 @@ int launch_spmv_dot(vflip_ctx* ctx, cudaStream_t stream, bool first, const Z* z,
   if ((size_t)sgrid.x * sgrid.y * sgrid.z > (size_t)kMaxPartials) return ctx->fail(VFLIP_ERR_ARG, "grid too large");
   const int slot = prof_start(ctx, VFLIP_PROF_SPMV, stream);
   if (first)
-    pcg_spmv_dot_kernel<W, true, kRedBlock, Z><<<sgrid, sblk, 0, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp,
+    pcg_spmv_dot_kernel<W, true, kRedBlock, Z, O><<<sgrid, sblk, 0, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp,
                                                                            d.ni, d.nj, d.nk, kz, ctx->partials,
                                                                            ctx->st);
   else
-    pcg_spmv_dot_kernel<W, false, kRedBlock, Z><<<sgrid, sblk, 0, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp,
+    pcg_spmv_dot_kernel<W, false, kRedBlock, Z, O><<<sgrid, sblk, 0, stream>>>(z, s_old, s_new, q, diag, xp, yp, zp,
                                                                             d.ni, d.nj, d.nk, kz, ctx->partials,
                                                                             ctx->st);
   prof_stop(ctx, slot, stream);
@@ -1027,6 +1079,10 @@ struct OuterVecs {
   W *x = nullptr, *r = nullptr, *s0 = nullptr, *s1 = nullptr, *q = nullptr;
   V *rv = nullptr, *z = nullptr;
   const W *od = nullptr, *ox = nullptr, *oy = nullptr, *oz = nullptr;
+  // the FP32 fine operator's couplings, read instead of ox/oy/oz when they
+  // equal the FP64 ones (an operator the library assembled: every coupling
+  // is a float value, so its FP32 copy is exact)
+  const float *fx = nullptr, *fy = nullptr, *fz = nullptr;
 };
 
 template <typename W, typename S0, typename SC, typename V>
@@ -1053,8 +1109,26 @@ int outer_vecs(vflip_ctx* ctx, Typed<S0, SC, V>& T, double* result, OuterVecs<W,
     o.ox = T.x64;
     o.oy = T.y64;
     o.oz = T.z64;
+    if constexpr (std::is_same<S0, float>::value) {
+      if (ctx->offdiag_f32) {
+        o.fx = T.fine.xp;
+        o.fy = T.fine.yp;
+        o.fz = T.fine.zp;
+      }
+    }
   }
   return VFLIP_OK;
+}
+
+// The outer PCG's s = z + beta s, q = A s and s.q, on the FP32 couplings
+// where they are exact (bitwise the same q).
+template <typename W, typename V>
+int outer_spmv(vflip_ctx* ctx, cudaStream_t stream, bool first, const OuterVecs<W, V>& o, const W* s_old, W* s_new,
+               W* q, const Dims& d) {
+  if constexpr (!std::is_same<W, float>::value) {
+    if (o.fx) return launch_spmv_dot<W, V, float>(ctx, stream, first, o.z, s_old, s_new, q, o.od, o.fx, o.fy, o.fz, d);
+  }
+  return launch_spmv_dot<W, V>(ctx, stream, first, o.z, s_old, s_new, q, o.od, o.ox, o.oy, o.oz, d);
 }
 
 // r = rhs, x = 0, |rhs|_inf
@@ -1110,7 +1184,7 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
     key.push_back((uintptr_t)L.d.ni); key.push_back((uintptr_t)L.d.nj); key.push_back((uintptr_t)L.d.nk);
   };
   kp(rhs); kp(result); kp(x); kp(r); kp(o.rv); kp(z); kp(s); kp(q); kp(itp); kp(ctx->st); kp(ctx->partials);
-  kp(o.od); kp(o.ox); kp(o.oy); kp(o.oz);
+  kp(o.od); kp(o.ox); kp(o.oy); kp(o.oz); kp(o.fx); kp(o.fy); kp(o.fz);
   kl(T.fine);
   for (const auto& L : T.coarse) kl(L);
   kp(T.direct.L); kp(T.direct.rinv); kp(T.direct.ok);
@@ -1193,8 +1267,12 @@ int pcg_solve_graph(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, doub
     if (!brc) {
       pcg_direction_kernel<W, V><<<grid_for(n, 256, ctx->num_sms), 256, 0, cs>>>(z, s, n, ctx->st);
       ++ctx->launches;
-      brc = launch_spmv_dot<W>(ctx, cs, true, (const W*)s, (const W*)nullptr, (W*)nullptr, q, o.od, o.ox, o.oy,
-                               o.oz, d);
+      if (o.fx)
+        brc = launch_spmv_dot<W, W, float>(ctx, cs, true, (const W*)s, (const W*)nullptr, (W*)nullptr, q, o.od, o.fx,
+                                           o.fy, o.fz, d);
+      else
+        brc = launch_spmv_dot<W>(ctx, cs, true, (const W*)s, (const W*)nullptr, (W*)nullptr, q, o.od, o.ox, o.oy,
+                                 o.oz, d);
     }
     if (!brc) {
       launch_pcg_update(ctx, cs, o, s, n);
@@ -1310,7 +1388,7 @@ int pcg_solve_w(vflip_ctx* ctx, Typed<S0, SC, V>& T, const double* rhs, double* 
   W* s_new = o.s1;
   int it;
   for (it = 0; it < maxit; ++it) {
-    if ((rc = launch_spmv_dot<W, V>(ctx, ctx->stream, it == 0, o.z, s_old, s_new, o.q, o.od, o.ox, o.oy, o.oz, d)))
+    if ((rc = outer_spmv<W, V>(ctx, ctx->stream, it == 0, o, s_old, s_new, o.q, d)))
       return rc;
     const int uslot = prof_start(ctx, VFLIP_PROF_UPDATE, ctx->stream);
     launch_pcg_update(ctx, ctx->stream, o, s_new, n);
@@ -2363,6 +2441,7 @@ void vflip_config_default(vflip_config* cfg) {
   cfg->batch_chunk = 0;
   cfg->batch_ctas_per_sm = 0;
   cfg->coarse_tail = 0;
+  cfg->tile_sweep_max_cells = 0;
 }
 
 int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
@@ -2396,8 +2475,9 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
       ctx->cfg.coarsest_solver < 0 || ctx->cfg.coarsest_solver > 2 || ctx->cfg.spmv_kernel < 0 ||
       ctx->cfg.spmv_kernel > 1 ||
       ctx->cfg.pcg_loop < 0 || ctx->cfg.pcg_loop > 1 || ctx->cfg.pcg_vectors < 0 || ctx->cfg.pcg_vectors > 1 || ctx->cfg.batch_chunk < 0 || ctx->cfg.batch_ctas_per_sm < 0 ||
-      ctx->cfg.coarse_tail < 0 || ctx->cfg.coarse_tail > 1)
+      ctx->cfg.coarse_tail < 0 || ctx->cfg.coarse_tail > 1 || ctx->cfg.tile_sweep_max_cells < -1)
     return bad(VFLIP_ERR_ARG);
+  if (ctx->cfg.tile_sweep_max_cells == 0) ctx->cfg.tile_sweep_max_cells = 64 * 64 * 64;
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
   cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device);
   // NULL selects the CUDA default stream, so work is ordered with whatever
@@ -2697,8 +2777,10 @@ int project_impl(vflip_ctx* ctx, int variant, int ni, int nj, int nk, float h, f
   }
   vflip_solve_stats s{};
   if (lo) lo->diag = op;
+  ctx->offdiag_f32 = true;  // assemble_kernel writes every coupling as (double) of a float
   int status = solve_stencil(ctx, ni, nj, nk, op, op + n, op + 2 * n, op + 3 * n, rhs, p, tolerance_factor,
                              max_iterations, &s, lo);
+  ctx->offdiag_f32 = false;
   if (status < 0) {
     cudaEventDestroy(e0);
     return status;

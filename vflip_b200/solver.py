@@ -69,7 +69,7 @@ class Solver:
                  device=0, stream=None, sweep_kernel=0, smoother_depth=0, smoother_tile_rows=0,
                  smoother_plane_ranges=0, smoother_ctas_per_sm=0, smoother_threads=0,
                  smoother_prefetch=0, coarsest_solver=0, spmv_kernel=0, pcg_loop=0, pcg_vectors=0,
-                 batch_chunk=0, batch_ctas_per_sm=0, coarse_tail=0):
+                 batch_chunk=0, batch_ctas_per_sm=0, coarse_tail=0, tile_sweep_max_cells=0):
         self.lib = load()
         cfg = ConfigC()
         self.lib.vflip_config_default(C.byref(cfg))
@@ -93,6 +93,7 @@ class Solver:
         cfg.batch_chunk = batch_chunk
         cfg.batch_ctas_per_sm = batch_ctas_per_sm
         cfg.coarse_tail = coarse_tail
+        cfg.tile_sweep_max_cells = tile_sweep_max_cells
         self.device = torch.device("cuda", device)
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
