@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-nested", action="store_true", help="skip the nested-subdomain arm")
     ap.add_argument("--no-precisions", action="store_true", help="skip the fp64/mixed plain arms")
     ap.add_argument("--no-dropin", action="store_true", help="skip the host-CSR drop-in solve timing")
+    ap.add_argument("--nested-ratio", type=int, default=4, choices=[2, 4],
+                    help="refinement of the nested subdomain (4: a 256^3 subdomain over a 128^3 plume)")
     ap.add_argument("--learned-level", type=int, default=2)
     ap.add_argument("--learned-sweeps", type=int, default=2)
     ap.add_argument("--learned-capture", type=int, default=40)
@@ -311,7 +313,7 @@ def run_vflip(a):
             out["flip"] = flip_arm(solver, a.steps)
             out["advection_forms"] = advection_arm(solver)
         if not a.no_nested and world == 1:
-            out["nested"] = nested_arm(a.steps, device=local)
+            out["nested"] = nested_arm(a.steps, device=local, ratio=a.nested_ratio)
     solver.close()
     ranks.close()
     return out
@@ -441,11 +443,12 @@ def flip_arm(solver, steps, n=128, warmup=3):
     return out
 
 
-def nested_arm(steps, device, n=128, warmup=3):
+def nested_arm(steps, device, n=128, warmup=3, ratio=4):
     """The nested-subdomain workload: a 128^3 FLIP plume (source sphere r =
     0.12 at (0.5, 0.1, 0.5), walls on five faces, open top, dt 0.005) with a
-    subdomain over the central half at 2x refinement (128^3 cells at h/2, the
-    resolution of a 256^3 grid), coupled as SmokeSolver3D::time_step couples
+    subdomain over the central half at `ratio` x refinement (4: 256^3 cells at
+    h/4, the refinement of the reference's own scene, main.cpp:63,71; 2:
+    128^3 cells at h/2), coupled as SmokeSolver3D::time_step couples
     its SubDomainSolver: both particle passes, the main MGPCG to 1e-6 and the
     subdomain's to 1e-9, in the mixed-precision context (FP32 V-cycle with
     BF16 coarse operators, FP64 PCG scalars and coarsest solve).  CUDA events
@@ -457,7 +460,7 @@ def nested_arm(steps, device, n=128, warmup=3):
     from vflip_b200.flip import NestedFlipSim, NestedParams
     from vflip_b200.solver import Solver
 
-    prm = NestedParams(n=n, dt=0.005, obstacle_radius=0.0)
+    prm = NestedParams(n=n, dt=0.005, obstacle_radius=0.0, ratio=ratio)
     with Solver(precision=PREC["mixed"], device=device) as s, Solver(precision=PREC["fp64"], device=device) as s64:
         sim = NestedFlipSim(s, prm)
         for _ in range(warmup):
@@ -474,7 +477,7 @@ def nested_arm(steps, device, n=128, warmup=3):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
-        out = {"grid": n, "subdomain_cells": list(sim.sdims), "subdomain_h": float(sim.sh),
+        out = {"grid": n, "refinement": ratio, "subdomain_cells": list(sim.sdims), "subdomain_h": float(sim.sh),
                "steps_per_s": steps / (ms * 1e-3), "ms_per_step": ms / steps,
                "particles_main_pass": np0 + nsp0, "subdomain_particles": sim.num_sub_particles,
                "pcg_iterations_mean": sum(it) / len(it), "sub_pcg_iterations_mean": sum(sit) / len(sit),
