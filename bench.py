@@ -61,7 +61,7 @@ def parse():
     ap.add_argument("--learned-epochs", type=int, default=16)
     ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds for the reference arm's timed steps")
     ap.add_argument("--kernels", default=None,
-                    help="instead of the step: per-kernel timings (comma list of advect, p2g, g2p, unet) at --n, "
+                    help="instead of the step: per-kernel timings (comma list of advect, p2g, g2p, vcycle, unet) at --n, "
                          "one JSON line each")
     ap.add_argument("--reps", type=int, default=5, help="timed repetitions per kernel (--kernels)")
     ap.add_argument("--unet-sizes", type=int, nargs="+", default=[32, 64, 128], help="network grids (--kernels unet)")
@@ -931,8 +931,40 @@ def kernel_lines(a):
                 du, dv, dw = (T(x) for x in scenes.random_velocity(n, n, n, rng, scale=0.1))
                 ms = timed(lambda: s.particle_from_grid(n, n, n, h, parts, du, dv, dw))
                 line("g2p_kernel", ms, npart * 24 + 12 * n ** 3, particles=npart)
+        if "vcycle" in what:
+            vcycle_lines(a, s, timed, line)
     if "unet" in what:
         unet_lines(a)
+
+
+def vcycle_lines(a, s, timed, line):
+    """One V(4,4)-cycle of the plume's own operator (the scene of the step,
+    state evolved by a few steps), launched level by level from the host
+    (vflip_vcycle), with the fine level's share: the V-cycle's device time,
+    and its fine-level sweeps' algorithmic bytes over that time."""
+    from vflip_b200.plume import PlumeParams, PlumeSim
+
+    n = a.n
+    sim = PlumeSim(s, PlumeParams(n=n, dt=a.dt))
+    for _ in range(3):
+        sim.step()
+    sim.advect_and_force()
+    p = sim.p
+    st, rhs = s.assemble(n, n, n, p.h, 0.0, sim.phi, sim.bdesc, sim.solid["u"], sim.solid["v"], sim.solid["w"],
+                         sim.f["u"], sim.f["v"], sim.f["w"])
+    import torch
+
+    s.vcycle(st, rhs)  # untimed: buffers and tensor maps
+    s.set_profiling(True)
+    for _ in range(a.reps):
+        s.vcycle(st, rhs)
+    torch.cuda.synchronize()
+    cnt, ms = s.profile_kernels("vcycle")
+    _, coarse_ms = s.profile_kernels("coarse")
+    s.set_profiling(False)
+    line("V(4,4)-cycle of the plume operator (all levels; CUDA events around the cycle, hierarchy build outside)",
+         ms / max(cnt, 1), (24 + 6 * 28 + 28.5 + 24) * n ** 3, coarse_levels_ms=coarse_ms / max(cnt, 1),
+         note="alg_bytes: the fine level's 8 sweeps and its restriction (FP32); the coarse levels add 1/7 of that")
 
 
 UNET_LEVEL = {"E0A": 0, "E0B": 0, "E1A": 1, "E1B": 1, "E2A": 2, "E2B": 2, "B1": 3, "B2": 3, "D2A": 2, "D2B": 2,
