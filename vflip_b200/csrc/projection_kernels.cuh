@@ -84,31 +84,27 @@ __device__ __forceinline__ float frac4(float bl, float br, float tl, float tr) {
 
 __device__ __forceinline__ float clamp01(float a) { return a < 0.0f ? 0.0f : (a > 1.0f ? 1.0f : a); }
 
-// compute_face_weights, Smoke_solver3D.cpp:874-944.  One thread per face of
-// the three face grids (flattened: u, then v, then w).
-__global__ void face_weights_kernel(const float* __restrict__ phi, float* __restrict__ uw, float* __restrict__ vw,
-                                    float* __restrict__ ww, int ni, int nj, int nk) {
-  const size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
+// compute_face_weights, Smoke_solver3D.cpp:874-944: weight = 1 - the
+// fraction of each face inside the solid, from the nodal phi at its four
+// corners (the reference's corner order per face grid).  One thread per node
+// (i, j, k) of the (ni+1) x (nj+1) x (nk+1) lattice writes the u, v and w
+// faces whose lower corner that node is, so seven nodal phi loads serve the
+// three faces, and the 2-D block over (i, j) with z over the grid needs no
+// index division.
+__global__ void face_weights3_kernel(const float* __restrict__ phi, float* __restrict__ uw, float* __restrict__ vw,
+                                     float* __restrict__ ww, int ni, int nj, int nk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+  if (i > ni || j > nj || k > nk) return;
   const int px = ni + 1, py = nj + 1;
-  auto P = [&](int i, int j, int k) { return __ldg(phi + lin3(i, j, k, px, py)); };
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nu + nv + nw;
-       e += (size_t)gridDim.x * blockDim.x) {
-    if (e < nu) {
-      int i, j, k;
-      decode3(e, ni + 1, nj, i, j, k);
-      uw[e] = clamp01(1 - frac4(P(i, j, k), P(i, j + 1, k), P(i, j, k + 1), P(i, j + 1, k + 1)));
-    } else if (e < nu + nv) {
-      size_t f = e - nu;
-      int i, j, k;
-      decode3(f, ni, nj + 1, i, j, k);
-      vw[f] = clamp01(1 - frac4(P(i, j, k), P(i, j, k + 1), P(i + 1, j, k), P(i + 1, j, k + 1)));
-    } else {
-      size_t f = e - nu - nv;
-      int i, j, k;
-      decode3(f, ni, nj, i, j, k);
-      ww[f] = clamp01(1 - frac4(P(i, j, k), P(i, j + 1, k), P(i + 1, j, k), P(i + 1, j + 1, k)));
-    }
-  }
+  auto P = [&](int a, int b, int c) { return __ldg(phi + lin3(a, b, c, px, py)); };
+  const bool xi = i < ni, yj = j < nj, zk = k < nk;
+  const float p000 = P(i, j, k);
+  const float p010 = (yj) ? P(i, j + 1, k) : 0.0f;
+  const float p001 = (zk) ? P(i, j, k + 1) : 0.0f;
+  const float p100 = (xi) ? P(i + 1, j, k) : 0.0f;
+  if (yj && zk) uw[lin3(i, j, k, ni + 1, nj)] = clamp01(1 - frac4(p000, p010, p001, P(i, j + 1, k + 1)));
+  if (xi && zk) vw[lin3(i, j, k, ni, nj + 1)] = clamp01(1 - frac4(p000, p001, p100, P(i + 1, j, k + 1)));
+  if (xi && yj) ww[lin3(i, j, k, ni, nj)] = clamp01(1 - frac4(p000, p010, p100, P(i + 1, j + 1, k)));
 }
 
 // Inflow overwrite, Smoke_solver3D.cpp:964-980: every cell with b_desc == 1
