@@ -88,6 +88,21 @@ __global__ void convert_kernel(const double* __restrict__ src, T* __restrict__ d
   for (; i < n; i += stride) dst[i] = cvt<T>((typename Num<T>::Acc)src[i]);
 }
 
+// The four operator arrays of a level in one launch (convert_kernel's
+// rounding): dst = [diag | xp | yp | zp], n each.
+template <typename T>
+__global__ void convert4_kernel(const double* __restrict__ d, const double* __restrict__ x,
+                                const double* __restrict__ y, const double* __restrict__ z, T* __restrict__ dst,
+                                size_t n) {
+  using A = typename Num<T>::Acc;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    dst[i] = cvt<T>((A)d[i]);
+    dst[n + i] = cvt<T>((A)x[i]);
+    dst[2 * n + i] = cvt<T>((A)y[i]);
+    dst[3 * n + i] = cvt<T>((A)z[i]);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // One full red-black Gauss-Seidel sweep (both colours), fused, out of place.
 //

@@ -141,7 +141,7 @@ __global__ void assemble_kernel(const float* __restrict__ u, const float* __rest
                                 const float* __restrict__ vs, const float* __restrict__ ws, double* __restrict__ diag,
                                 double* __restrict__ xp, double* __restrict__ yp, double* __restrict__ zp,
                                 double* __restrict__ rhs, float h, int ni, int nj, int nk, int variant, float dt,
-                                float inv_h) {
+                                float inv_h, float* __restrict__ op32) {
   const size_t n = (size_t)ni * nj * nk;
   const float h2 = h * h;
   // x / h and x / h^2 as products when h is a power of two (inv_h != 0):
@@ -184,6 +184,12 @@ __global__ void assemble_kernel(const float* __restrict__ u, const float* __rest
     yp[e] = cy;
     zp[e] = cz;
     rhs[e] = b;
+    if (op32) {  // the FP32 copy convert4_kernel would make: [diag | xp | yp | zp]
+      op32[e] = (float)d;
+      op32[n + e] = (float)cx;
+      op32[2 * n + e] = (float)cy;
+      op32[3 * n + e] = (float)cz;
+    }
   }
 }
 

@@ -81,6 +81,7 @@ struct vflip_ctx {
   std::string err;
   std::unordered_map<std::string, std::pair<void*, size_t>> bufs;
   bool offdiag_f32 = false;  // the operator being solved was assembled here: its couplings are FP32 values
+  const void* fine_op_ready = nullptr;  // its FP32 fine-level copy, written by the assembly
   void* hbuf = nullptr;  // pinned host staging of the host-buffer entry points
   size_t hbuf_bytes = 0;
   PcgScalars* st = nullptr;         // device
@@ -735,13 +736,6 @@ int build_hierarchy64(vflip_ctx* ctx, int ni, int nj, int nk, const double* diag
   return VFLIP_OK;
 }
 
-template <typename T>
-int convert_array(vflip_ctx* ctx, const double* src, T* dst, size_t n) {
-  convert_kernel<T><<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(src, dst, n);
-  VF_LAUNCH_CHECK();
-  return VFLIP_OK;
-}
-
 // Typed levels: level 0 uses (S0, V), coarse levels (SC, V).
 template <typename S0, typename SC, typename V>
 struct Typed {
@@ -805,11 +799,11 @@ int make_level(vflip_ctx* ctx, const Hierarchy64& H, size_t l, const double* d0,
   } else {
     S* p;
     VF_ALLOC(p, S, std::string(tag) + "_op_" + std::to_string(l), 4 * n);
-    int rc;
-    if ((rc = convert_array<S>(ctx, d, p, n))) return rc;
-    if ((rc = convert_array<S>(ctx, x, p + n, n))) return rc;
-    if ((rc = convert_array<S>(ctx, y, p + 2 * n, n))) return rc;
-    if ((rc = convert_array<S>(ctx, z, p + 3 * n, n))) return rc;
+    // the assembly may have written the fine level's FP32 copy already
+    if (!(l == 0 && (const void*)p == ctx->fine_op_ready)) {
+      convert4_kernel<S><<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(d, x, y, z, p, n);
+      VF_LAUNCH_CHECK();
+    }
     L.diag = p; L.xp = p + n; L.yp = p + 2 * n; L.zp = p + 3 * n;
   }
   V* v;
@@ -2733,7 +2727,8 @@ namespace {
 // variant 1: SubDomainSolver::pcg_projection (no inflow, dt/h^2 terms)
 int assemble_impl(vflip_ctx* ctx, int variant, int ni, int nj, int nk, float h, float dt, float U_in,
                   const float* nodal_phi, const int8_t* bdesc, const float* us, const float* vs, const float* ws,
-                  float* u, float* v, float* w, double* diag, double* xp, double* yp, double* zp, double* rhs) {
+                  float* u, float* v, float* w, double* diag, double* xp, double* yp, double* zp, double* rhs,
+                  float* op32 = nullptr) {
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (!nodal_phi || (variant == 0 && !bdesc) || !us || !vs || !ws || !u || !v || !w || !diag || !xp || !yp || !zp ||
@@ -2750,7 +2745,7 @@ int assemble_impl(vflip_ctx* ctx, int variant, int ni, int nj, int nk, float h, 
   }
   assemble_kernel<<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
       u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, diag, xp, yp, zp, rhs, h, ni, nj, nk, variant, dt,
-      (float)inv_pow2(h));
+      (float)inv_pow2(h), op32);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
 }
@@ -2770,17 +2765,26 @@ int project_impl(vflip_ctx* ctx, int variant, int ni, int nj, int nk, float h, f
   cudaEvent_t e0;
   VF_CUDA(cudaEventCreate(&e0));
   VF_CUDA(cudaEventRecord(e0, ctx->stream));
+  // FP32/MIXED contexts: the assembly also writes the fine level's FP32
+  // operator into the buffer the solve's hierarchy uses for it
+  float* op32 = nullptr;
+  if (ctx->cfg.precision == VFLIP_PREC_FP32 || ctx->cfg.precision == VFLIP_PREC_MIXED) {
+    const char* tag = ctx->cfg.precision == VFLIP_PREC_FP32 ? "f32" : "mix";
+    VF_ALLOC(op32, float, std::string(tag) + "_op_0", 4 * n);
+  }
   if ((rc = assemble_impl(ctx, variant, ni, nj, nk, h, dt, U_in, nodal_phi, bdesc, us, vs, ws, u, v, w, op,
-                          op + n, op + 2 * n, op + 3 * n, rhs))) {
+                          op + n, op + 2 * n, op + 3 * n, rhs, op32))) {
     cudaEventDestroy(e0);
     return rc;
   }
   vflip_solve_stats s{};
   if (lo) lo->diag = op;
   ctx->offdiag_f32 = true;  // assemble_kernel writes every coupling as (double) of a float
+  ctx->fine_op_ready = op32;
   int status = solve_stencil(ctx, ni, nj, nk, op, op + n, op + 2 * n, op + 3 * n, rhs, p, tolerance_factor,
                              max_iterations, &s, lo);
   ctx->offdiag_f32 = false;
+  ctx->fine_op_ready = nullptr;
   if (status < 0) {
     cudaEventDestroy(e0);
     return status;
