@@ -137,10 +137,10 @@ class PlumeSim:
         copied in at the start of the step and its result copied back into
         the same host tensors.  The copies overlap the compute where the data
         allows:
-          * u, v, w download in order on one stream and each field's next
-            upload waits only for its own download, so the upload of one
-            field runs beside the download of the next (the host link is full
-            duplex);
+          * u, v, w download in order on one stream, in HOST_CHUNKS pieces
+            each, and each piece's next upload waits only for its own
+            download, so uploads run one piece behind the downloads (the host
+            link is full duplex);
           * density and temperature travel on a third stream: their upload
             follows the velocity's and overlaps the velocity advection, their
             download leaves once the sources are applied and overlaps the
@@ -156,9 +156,10 @@ class PlumeSim:
         up.wait_stream(main)  # the device buffers are free of earlier work
         with torch.cuda.stream(up):
             for k in ("u", "v", "w"):
-                if k in self._downloaded:
-                    up.wait_event(self._downloaded[k])
-                self.f[k].copy_(host[k], non_blocking=True)
+                for c, (d, h) in enumerate(zip(self._pieces(self.f[k]), self._pieces(host[k]))):
+                    if (k, c) in self._downloaded:
+                        up.wait_event(self._downloaded[(k, c)])
+                    d.copy_(h, non_blocking=True)
         vel_in = torch.cuda.Event()
         vel_in.record(up)
         main.wait_event(vel_in)
@@ -179,11 +180,21 @@ class PlumeSim:
         down.wait_stream(main)
         with torch.cuda.stream(down):
             for k in ("u", "v", "w"):
-                host[k].copy_(self.f[k], non_blocking=True)
-                ev = torch.cuda.Event()
-                ev.record(down)
-                self._downloaded[k] = ev
+                for c, (d, h) in enumerate(zip(self._pieces(self.f[k]), self._pieces(host[k]))):
+                    h.copy_(d, non_blocking=True)
+                    ev = torch.cuda.Event()
+                    ev.record(down)
+                    self._downloaded[(k, c)] = ev
         return out
+
+    HOST_CHUNKS = 8
+
+    def _pieces(self, t):
+        """HOST_CHUNKS contiguous pieces of a field (flat views)."""
+        flat = t.view(-1)
+        n = flat.numel()
+        bounds = [n * c // self.HOST_CHUNKS for c in range(self.HOST_CHUNKS + 1)]
+        return [flat[a:b] for a, b in zip(bounds[:-1], bounds[1:])]
 
     def host_join(self):
         """Make the current stream wait for step_host's copies in flight."""
