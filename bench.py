@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-nested", action="store_true", help="skip the nested-subdomain arm")
     ap.add_argument("--no-precisions", action="store_true", help="skip the fp64/mixed plain arms")
     ap.add_argument("--no-dropin", action="store_true", help="skip the host-CSR drop-in solve timing")
+    ap.add_argument("--solver-opts", default="",
+                    help="extra integer options of the headline Solver, e.g. coarse_tail=1,tile_sweep_max_cells=-1")
     ap.add_argument("--nested-ratio", type=int, default=4, choices=[2, 4],
                     help="refinement of the nested subdomain (4: a 256^3 subdomain over a 128^3 plume)")
     ap.add_argument("--learned-level", type=int, default=2)
@@ -76,9 +78,12 @@ def workload(a):
 
 
 def config(a, n_gpus):
-    return {"workload": workload(a), "grid": a.n, "dt": a.dt, "precision": a.precision,
-            "tolerance": 1e-6, "parallelism": f"replicas x{n_gpus}",
-            "l2": "inputs larger than L2 (5 fields x 64 MB + solver vectors), no flush"}
+    out = {"workload": workload(a), "grid": a.n, "dt": a.dt, "precision": a.precision,
+           "tolerance": 1e-6, "parallelism": f"replicas x{n_gpus}",
+           "l2": "inputs larger than L2 (5 fields x 64 MB + solver vectors), no flush"}
+    if a.solver_opts:
+        out["solver_opts"] = a.solver_opts
+    return out
 
 
 def measured_peaks():
@@ -201,7 +206,8 @@ def run_vflip(a):
     world, rank = ranks.world, ranks.rank
     barrier, max_over_ranks = ranks.barrier, ranks.max_over_ranks
 
-    solver = Solver(precision=PREC[a.precision], device=local)
+    opts = {k: int(v) for k, v in (kv.split("=") for kv in a.solver_opts.split(",") if kv)}
+    solver = Solver(precision=PREC[a.precision], device=local, **opts)
     params = PlumeParams(n=a.n, dt=a.dt)
     sim = PlumeSim(solver, params)
     for _ in range(a.warmup):

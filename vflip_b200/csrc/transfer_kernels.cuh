@@ -103,7 +103,8 @@ __device__ __forceinline__ float smp(const GridView& g, float x, float y, float 
 
 // EXACT: the reference's arithmetic (FP64 transform and lerps, FP64 midpoint
 // step), bit-identical to SubDomainSolver::advect_field; otherwise the same
-// scheme in FP32.
+// scheme in FP32 (FP32 contexts launch advect_rk2_f_kernel, its values bit
+// for bit with less work per sample).
 template <bool EXACT>
 __global__ void advect_rk2_kernel(GridView u, GridView v, GridView w, GridView f, float* __restrict__ out,
                                   GridView f2, float* __restrict__ out2, float h, float dt, int per_block) {
@@ -157,6 +158,98 @@ __global__ void advect_rk2_kernel(GridView u, GridView v, GridView w, GridView f
     if (two) {
       out[e1] = smp<EXACT>(f, px1, py1, pz1);
       if (out2) out2[e1] = smp<EXACT>(f2, px1, py1, pz1);
+    }
+  }
+}
+
+// ---- the FP32 form (advect_rk2_kernel<false>'s values bit for bit) with
+// the per-sample work cut down: each grid's float transform (1/h, offsets)
+// is computed once on the host, and the staggered u, v, w grids share the
+// axis coordinates they have in common (x of v and w, y of u and w, z of u
+// and v: same offset and extent), so a velocity sample at one point takes
+// six floor/clamp axis evaluations instead of nine.
+struct GridF {
+  const float* d;
+  int nx, ny, nz;
+  float ox, oy, oz;  // (float) of the grid's offsets
+};
+
+struct AxisF {
+  int i0, i1;  // clamped corner indices
+  float c;     // fraction
+};
+
+__device__ __forceinline__ AxisF axis_f(float w, float ih, float o, int n) {
+  const float g = __fmaf_rn(w, ih, o);
+  const float f = floorf(g);
+  const int i = (int)f;
+  return AxisF{clampi(i, n - 1), clampi(i + 1, n - 1), g - f};
+}
+
+// sample_linear_f's corners and lerps from precomputed axes (sy, sz: strides)
+__device__ __forceinline__ float tri_f(const float* __restrict__ d, int sy, int sz, const AxisF& x, const AxisF& y,
+                                       const AxisF& z) {
+  const int i0 = x.i0, i1 = x.i1, j0 = y.i0 * sy, j1 = y.i1 * sy, k0 = z.i0 * sz, k1 = z.i1 * sz;
+  float v1 = lerp_f(lerp_f(__ldg(d + (i0 + j0 + k0)), __ldg(d + (i1 + j0 + k0)), x.c),
+                    lerp_f(__ldg(d + (i0 + j1 + k0)), __ldg(d + (i1 + j1 + k0)), x.c), y.c);
+  float v2 = lerp_f(lerp_f(__ldg(d + (i0 + j0 + k1)), __ldg(d + (i1 + j0 + k1)), x.c),
+                    lerp_f(__ldg(d + (i0 + j1 + k1)), __ldg(d + (i1 + j1 + k1)), x.c), y.c);
+  return lerp_f(v1, v2, z.c);
+}
+
+__device__ __forceinline__ float grid_f(const GridF& g, float ih, float wx, float wy, float wz) {
+  return tri_f(g.d, g.nx, g.nx * g.ny, axis_f(wx, ih, g.ox, g.nx), axis_f(wy, ih, g.oy, g.ny),
+               axis_f(wz, ih, g.oz, g.nz));
+}
+
+// u, v, w of the MAC grid of ni x nj x nk cells at one point (u: offsets
+// (0.5, 0, 0), extent (ni+1, nj, nk); v: (0, 0.5, 0); w: (0, 0, 0.5))
+__device__ __forceinline__ void mac_f(const float* __restrict__ u, const float* __restrict__ v,
+                                      const float* __restrict__ w, int ni, int nj, int nk, float ih, float x, float y,
+                                      float z, float& a, float& b, float& c) {
+  const AxisF xu = axis_f(x, ih, 0.5f, ni + 1), xvw = axis_f(x, ih, 0.0f, ni);
+  const AxisF yv = axis_f(y, ih, 0.5f, nj + 1), yuw = axis_f(y, ih, 0.0f, nj);
+  const AxisF zw = axis_f(z, ih, 0.5f, nk + 1), zuv = axis_f(z, ih, 0.0f, nk);
+  a = tri_f(u, ni + 1, (ni + 1) * nj, xu, yuw, zuv);
+  b = tri_f(v, ni, ni * (nj + 1), xvw, yv, zuv);
+  c = tri_f(w, ni, ni * nj, xvw, yuw, zw);
+}
+
+// node_world's coordinates without the integer division: the block's run of
+// nodes is walked with (i, j, k) carried along
+__global__ void advect_rk2_f_kernel(const float* __restrict__ u, const float* __restrict__ v,
+                                    const float* __restrict__ w, int ni, int nj, int nk, float ih, GridView f,
+                                    GridF ff, float* __restrict__ out, GridF ff2, float* __restrict__ out2, float h,
+                                    float dt, int per_block) {
+  const size_t n = (size_t)f.nx * f.ny * f.nz;
+  const size_t stride = blockDim.x;
+  const size_t beg = (size_t)blockIdx.x * per_block;
+  const size_t end = beg + per_block < n ? beg + per_block : n;
+  const float hf = 0.5f * dt;
+  for (size_t e0 = beg + threadIdx.x; e0 < end; e0 += 2 * stride) {
+    const size_t e1 = e0 + stride;
+    const bool two = e1 < end;
+    float wx0, wy0, wz0, wx1 = 0, wy1 = 0, wz1 = 0;
+    node_world(f, e0, h, wx0, wy0, wz0);
+    if (two) node_world(f, e1, h, wx1, wy1, wz1);
+    float a0, b0, c0, a1 = 0, b1 = 0, c1 = 0;
+    mac_f(u, v, w, ni, nj, nk, ih, wx0, wy0, wz0, a0, b0, c0);
+    if (two) mac_f(u, v, w, ni, nj, nk, ih, wx1, wy1, wz1, a1, b1, c1);
+    float px0 = wx0 - hf * a0, py0 = wy0 - hf * b0, pz0 = wz0 - hf * c0;
+    float px1 = wx1 - hf * a1, py1 = wy1 - hf * b1, pz1 = wz1 - hf * c1;
+    mac_f(u, v, w, ni, nj, nk, ih, px0, py0, pz0, a0, b0, c0);
+    if (two) mac_f(u, v, w, ni, nj, nk, ih, px1, py1, pz1, a1, b1, c1);
+    px0 = wx0 - dt * a0;
+    py0 = wy0 - dt * b0;
+    pz0 = wz0 - dt * c0;
+    px1 = wx1 - dt * a1;
+    py1 = wy1 - dt * b1;
+    pz1 = wz1 - dt * c1;
+    out[e0] = grid_f(ff, ih, px0, py0, pz0);
+    if (out2) out2[e0] = grid_f(ff2, ih, px0, py0, pz0);
+    if (two) {
+      out[e1] = grid_f(ff, ih, px1, py1, pz1);
+      if (out2) out2[e1] = grid_f(ff2, ih, px1, py1, pz1);
     }
   }
 }

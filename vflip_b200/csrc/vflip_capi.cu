@@ -2991,9 +2991,14 @@ int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, fl
   if (ctx->cfg.precision == VFLIP_PREC_FP64)
     advect_rk2_kernel<true><<<blocks, 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2, field2 ? out2 : nullptr, h, dt,
                                                            per_block);
-  else
-    advect_rk2_kernel<false><<<blocks, 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2, field2 ? out2 : nullptr, h,
-                                                            dt, per_block);
+  else {
+    // sample_linear_f's float transform, computed once
+    const float ihf = (float)(ih != 0.0 ? ih : 1.0 / (double)h);
+    const GridF ff{field, fnx, fny, fnz, (float)ox, (float)oy, (float)oz};
+    const GridF ff2{field2, fnx, fny, fnz, (float)ox, (float)oy, (float)oz};
+    advect_rk2_f_kernel<<<blocks, 256, 0, ctx->stream>>>(u, v, w, ni, nj, nk, ihf, gf, ff, out, ff2,
+                                                         field2 ? out2 : nullptr, h, dt, per_block);
+  }
   prof_stop(ctx, slot, ctx->stream);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
