@@ -50,24 +50,28 @@ struct TailArgs {
   const int* ok;
 };
 
-// shared-memory floats of one level: x, b, diag, xp, yp, zp
-__host__ __device__ inline size_t tail_level_floats(int n) { return 6 * (size_t)n; }
+// shared-memory floats of one level: x, b, diag, xp, yp, zp, then one
+// mask byte per cell (bits 0-5: which of the six neighbours exist, in the
+// row-sum order -z, -y, -x, +x, +y, +z; bit 6: the cell's colour), packed
+// four to a float slot
+__host__ __device__ inline size_t tail_level_floats(int n) { return 6 * (size_t)n + ((size_t)n + 3) / 4; }
 
-// One red-black sweep in place on a level held in shared memory.
+// One red-black sweep in place on a level held in shared memory; the masks
+// spare the index arithmetic (sy = ni, sz = ni * nj).
 __device__ __forceinline__ void tail_sweep(float* xs, const float* bs, const float* ds, const float* xps,
-                                           const float* yps, const float* zps, int ni, int nj, int nk) {
-  const int n = ni * nj * nk, sy = ni, sz = ni * nj;
+                                           const float* yps, const float* zps, const unsigned char* mk, int n,
+                                           int sy, int sz) {
   for (int parity = 1; parity >= 0; --parity) {
     for (int e = threadIdx.x; e < n; e += kTailThreads) {
-      const int i = e % ni, j = (e / ni) % nj, k = e / sz;
-      if (((i + j + k) & 1) != parity) continue;
+      const int f = mk[e];
+      if ((f >> 6) != parity) continue;
       float sum = 0.0f;
-      if (k > 0) sum = gs_madd(sum, zps[e - sz], xs[e - sz]);
-      if (j > 0) sum = gs_madd(sum, yps[e - sy], xs[e - sy]);
-      if (i > 0) sum = gs_madd(sum, xps[e - 1], xs[e - 1]);
-      if (i < ni - 1) sum = gs_madd(sum, xps[e], xs[e + 1]);
-      if (j < nj - 1) sum = gs_madd(sum, yps[e], xs[e + sy]);
-      if (k < nk - 1) sum = gs_madd(sum, zps[e], xs[e + sz]);
+      if (f & 1) sum = gs_madd(sum, zps[e - sz], xs[e - sz]);
+      if (f & 2) sum = gs_madd(sum, yps[e - sy], xs[e - sy]);
+      if (f & 4) sum = gs_madd(sum, xps[e - 1], xs[e - 1]);
+      if (f & 8) sum = gs_madd(sum, xps[e], xs[e + 1]);
+      if (f & 16) sum = gs_madd(sum, yps[e], xs[e + sy]);
+      if (f & 32) sum = gs_madd(sum, zps[e], xs[e + sz]);
       const float d = ds[e];
       xs[e] = (d != 0.0f) ? gs_div(bs[e] - sum, d) : 0.0f;
     }
@@ -94,6 +98,8 @@ __global__ void __launch_bounds__(kTailThreads) tail_vcycle_kernel(const TailArg
     const int n = cnt(l);
     float* p = base[l];
     const TailLevel<S>& v = a.lv[l];
+    unsigned char* mk = reinterpret_cast<unsigned char*>(p + 6 * n);
+    const int ni = v.ni, nj = v.nj, nk = v.nk;
     for (int e = tid; e < n; e += kTailThreads) {
       p[e] = 0.0f;
       p[n + e] = l == 0 ? (float)ldv(a.b + e) : 0.0f;
@@ -101,13 +107,17 @@ __global__ void __launch_bounds__(kTailThreads) tail_vcycle_kernel(const TailArg
       p[3 * n + e] = (float)ldv(v.xp + e);
       p[4 * n + e] = (float)ldv(v.yp + e);
       p[5 * n + e] = (float)ldv(v.zp + e);
+      const int i = e % ni, j = (e / ni) % nj, k = e / (ni * nj);
+      mk[e] = (unsigned char)((k > 0) | ((j > 0) << 1) | ((i > 0) << 2) | ((i < ni - 1) << 3) |
+                              ((j < nj - 1) << 4) | ((k < nk - 1) << 5) | (((i + j + k) & 1) << 6));
     }
   }
   __syncthreads();
   auto sweep_level = [&](int l) {
     const int n = cnt(l);
     float* p = base[l];
-    tail_sweep(p, p + n, p + 2 * n, p + 3 * n, p + 4 * n, p + 5 * n, a.lv[l].ni, a.lv[l].nj, a.lv[l].nk);
+    tail_sweep(p, p + n, p + 2 * n, p + 3 * n, p + 4 * n, p + 5 * n, reinterpret_cast<const unsigned char*>(p + 6 * n),
+               n, a.lv[l].ni, a.lv[l].ni * a.lv[l].nj);
   };
   // ---- down: x = 0, pre-sweeps, b_{l+1} = R (b - A x)
   for (int l = 0; l + 1 < L; ++l) {
