@@ -26,7 +26,6 @@ namespace {
 
 constexpr size_t kConvSmemMax = 200 * 1024;
 constexpr size_t kConvSmemFloor = 100 * 1024;   // at most two CTAs (2 x <= 256 TMEM columns) per SM
-constexpr size_t kConvSmem2 = 110 * 1024;       // the most two CTAs per SM may each take
 constexpr size_t kWgradSmemMax = 200 * 1024;
 constexpr size_t kWgradSmemFloor = 116 * 1024;  // one CTA (512 TMEM columns) per SM
 
@@ -265,46 +264,21 @@ int Net::conv(const View& in, int X, int Y, int Z, const __nv_bfloat16* wpacked,
   if (mask && (!view_ok(*mask) || mask->c != cout)) return fail(VFLIP_ERR_ARG, "conv: bad mask view");
   if (!out && !outf) return fail(VFLIP_ERR_ARG, "conv: no output");
   if (outf && (ofvalid < 0 || ofvalid > cout || ofstride < ofvalid)) return fail(VFLIP_ERR_ARG, "conv: bad fp32 output");
-  // Shared memory holds two buffers of TB tiles' input slabs and the
-  // weights: resident when every tap fits, else a ring of >= 8 slots over
-  // the widest channel group that fits.  TB tiles run at once with their own
-  // TMEM accumulators (a tile's MMAs accumulate into one accumulator and so
-  // wait on each other; other tiles' MMAs fill those gaps).  Among two CTAs
-  // per SM (<= 112 KB and 256 TMEM columns each) and one (<= 200 KB, 512
-  // columns), the choice with the most tiles in flight per SM wins.
+  // weights resident when every tap fits beside the two slabs; else the
+  // widest channel group whose slabs leave room for a ring of >= 8 slots
   const int nch = cin / 8;
-  const uint32_t cols = pow2_cols(cout);
-  int cc = 0, ring = 0, tb = 0, per_sm = 0;
-  size_t smem = 0;
-  for (int ctas = 2; ctas >= 1; --ctas) {
-    const size_t budget = ctas == 2 ? kConvSmem2 : kConvSmemMax;
-    for (int t = 4; t >= 1; t >>= 1) {
-      if ((uint32_t)t * cols > (ctas == 2 ? 256u : 512u)) continue;
-      if (t * ctas <= tb * per_sm) break;
-      int c_ = 0, r_ = 0;
-      size_t need = 0;
-      const size_t full = 2 * (size_t)t * nch * kPlane + (size_t)27 * nch * cout * 16;
-      if (full <= budget) {
-        c_ = nch;
-        r_ = 27;
-        need = full;
-      } else {
-        for (int c = nch; c >= 2; --c) {
-          if (nch % c || c % 2) continue;
-          const size_t slabs = 2 * (size_t)t * c * kPlane, blk = (size_t)c * cout * 16;
-          if (slabs + 8 * blk > budget) continue;
-          c_ = c;
-          r_ = (int)std::min<size_t>(kMaxRing, (budget - slabs) / blk);
-          need = slabs + (size_t)r_ * blk;
-          break;
-        }
-      }
-      if (!c_) continue;
-      cc = c_;
-      ring = r_;
-      tb = t;
-      per_sm = ctas;
-      smem = std::max(ctas == 2 ? kConvSmemFloor : kConvSmem2 + 1024, need);
+  int cc = 0, ring = 0;
+  const size_t full = 2 * (size_t)nch * kPlane + (size_t)27 * nch * cout * 16;
+  if (full <= kConvSmemMax) {
+    cc = nch;
+    ring = 27;
+  } else {
+    for (int c = nch; c >= 2; --c) {
+      if (nch % c || c % 2) continue;
+      const size_t slabs = 2 * (size_t)c * kPlane, blk = (size_t)c * cout * 16;
+      if (slabs + 8 * blk > kConvSmemMax) continue;
+      cc = c;
+      ring = (int)std::min<size_t>(kMaxRing, (kConvSmemMax - slabs) / blk);
       break;
     }
   }
@@ -336,11 +310,10 @@ int Net::conv(const View& in, int X, int Y, int Z, const __nv_bfloat16* wpacked,
   a.ntiles = a.ntx * a.nty * Z;
   a.ring = ring;
   a.lag = ring >= 27 * a.ngroups ? 0 : std::min(4, ring / 4);
-  a.tb = tb;
-  a.cols = cols;
-  a.tmem_cols = pow2_cols((int)(tb * cols));
+  a.tmem_cols = pow2_cols(cout);
   a.error = d_error;
-  const int grid = std::min((a.ntiles + tb - 1) / tb, per_sm * num_sms);
+  const size_t smem = std::max(kConvSmemFloor, 2 * (size_t)cc * kPlane + (size_t)ring * cc * cout * 16);
+  const int grid = std::min(a.ntiles, 2 * num_sms);
   conv3_tc_kernel<<<grid, kConvThreads, smem, stream>>>(amap, a);
   NET_LAUNCH();
   return VFLIP_OK;

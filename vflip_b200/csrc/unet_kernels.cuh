@@ -65,8 +65,6 @@ struct ConvArgs {
   int X, Y, Z, cin, cout, cc, ngroups, relu;
   int ntx, nty, ntiles;
   int ring, lag;  // weight slots and MMA steps kept queued; ring == 27 * ngroups: resident
-  int tb;         // tiles in flight per CTA (1, 2 or 4): each has its own accumulator of `cols` columns
-  uint32_t cols;  // TMEM columns per tile's accumulator
   uint32_t tmem_cols;
   int* error;
 };
@@ -102,22 +100,20 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int cc = a.cc, cout = a.cout, G = a.ngroups, R = a.ring, L = a.lag, TB = a.tb;
+  const int cc = a.cc, cout = a.cout, G = a.ngroups, R = a.ring, L = a.lag;
   const int steps_tile = G * 27;
   const bool resident = R >= steps_tile;
   const uint32_t sb = smem_u32(smem);
   const uint32_t slab_bytes = (uint32_t)cc * kPlane;
   const uint32_t bblk = (uint32_t)cc * cout * 16;
-  // slabs: two buffers of TB tiles each, then the weight ring
-  const uint32_t ring0 = sb + 2 * (uint32_t)TB * slab_bytes;
+  const uint32_t ring0 = sb + 2 * slab_bytes;
   const uint32_t bar0 = smem_u32(bars);
-  // barriers: 0-1 slab batch full, 2-3 slab batch free, accumulators full, drain, then R weight-full, R weight-free
+  // barriers: 0-1 slab full, 2-3 slab free, accumulator full, drain, then R weight-full, R weight-free
   const uint32_t ACC_FULL = bar0 + 32u, DRAIN = bar0 + 40u;
   auto slab_full = [&](int b) { return bar0 + 8u * b; };
   auto slab_free = [&](int b) { return bar0 + 8u * (2 + b); };
   auto b_full = [&](int r) { return bar0 + 8u * (6 + r); };
   auto b_free = [&](int r) { return bar0 + 8u * (6 + R + r); };
-  auto slab_at = [&](int buf, int t) { return sb + (uint32_t)(buf * TB + t) * slab_bytes; };
 
   if (tid == 0) {
     for (int q = 0; q < 6 + 2 * R; ++q) mbar_init(bar0 + 8u * q, 1);
@@ -130,35 +126,30 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_
   tc_fence_after();
   const uint32_t tmem = tmem_sh;
 
-  // this CTA's tiles: blockIdx.x + t * gridDim.x, taken TB at a time (a batch)
   const int ntiles_me = (int)blockIdx.x < a.ntiles ? (a.ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
-  const int nbatch = (ntiles_me + TB - 1) / TB;
-  const long total_steps = (long)nbatch * steps_tile;
-  const int total_slabs = nbatch * G;
+  const long total_steps = (long)ntiles_me * steps_tile;
+  const int total_slabs = ntiles_me * G;
   const int nch = a.cin >> 3;
   const uint32_t idesc = umma_idesc_bf16(128, cout, 0, 0);
-  auto in_batch = [&](int bt) { return min(TB, ntiles_me - bt * TB); };
 
-  auto tile_of = [&](int t, int& tx, int& ty, int& tz) {
-    const int g = (int)blockIdx.x + t * (int)gridDim.x;
-    tx = g % a.ntx;
-    const int r = g / a.ntx;
+  auto tile_of = [&](int it, int& tx, int& ty, int& tz) {
+    const int t = (int)blockIdx.x + it * (int)gridDim.x;
+    tx = t % a.ntx;
+    const int r = t / a.ntx;
     ty = r % a.nty;
     tz = r / a.nty;
   };
   // producer state (thread 0)
   long b_issued = 0, b_done = 0;
   int s_issued = 0, s_done = 0;
-  auto issue_slab = [&](int q) {  // channel group q % G of batch q / G, into buffer q & 1
-    const int bt = q / G, g = q % G, buf = q & 1, nt = in_batch(bt);
-    mbar_expect_tx(slab_full(buf), (uint32_t)(nt * cc) * kSlabBox);
-    for (int t = 0; t < nt; ++t) {
-      int tx, ty, tz;
-      tile_of(bt * TB + t, tx, ty, tz);
-      for (int k = 0; k < cc; ++k)
-        tma_tile_4d(slab_at(buf, t) + k * kPlane, &amap, 8 * (g * cc + k), tx * kTX - 1, ty * kTY - 1, tz - 1,
-                    slab_full(buf));
-    }
+  auto issue_slab = [&](int q) {
+    int tx, ty, tz;
+    tile_of(q / G, tx, ty, tz);
+    const int g = q % G, buf = q & 1;
+    mbar_expect_tx(slab_full(buf), (uint32_t)cc * kSlabBox);
+    for (int k = 0; k < cc; ++k)
+      tma_tile_4d(sb + buf * slab_bytes + k * kPlane, &amap, 8 * (g * cc + k), tx * kTX - 1, ty * kTY - 1, tz - 1,
+                  slab_full(buf));
     s_issued = q + 1;
   };
   auto issue_w = [&](long s) {
@@ -178,8 +169,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_
   }
   long s = 0;
   int q = 0;
-  for (int bt = 0; bt < nbatch; ++bt) {
-    const int nt = in_batch(bt);
+  for (int it = 0; it < ntiles_me; ++it) {
     if (tid == 0) {
       for (int g = 0; g < G && ok; ++g, ++q) {
         const int buf = q & 1;
@@ -187,6 +177,7 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_
         if (!ok) break;
         s_done = q + 1;
         tc_fence_after();
+        const uint32_t slab = sb + buf * slab_bytes;
         for (int tap = 0; tap < 27; ++tap, ++s) {
           const int r = (int)(s % R);
           if (!resident || s < R) {
@@ -194,16 +185,11 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_
             if (!ok) break;
             b_done = s + 1;
           }
-          const uint32_t b0 = ring0 + r * bblk;
+          const uint32_t a0 = slab + tap_shift(tap), b0 = ring0 + r * bblk;
           for (int j = 0; j < (cc >> 1); ++j) {
+            const uint64_t ad = umma_sdesc(a0 + 2u * j * kPlane, kPlane, kRowY);
             const uint64_t bd = umma_sdesc(b0 + 2u * j * cout * 16, cout * 16, 128);
-            // one MMA per tile of the batch: independent accumulators, so
-            // the tensor pipe overlaps them; each tile's own MMAs keep the
-            // (group, tap, k-step) order
-            for (int t = 0; t < nt; ++t) {
-              const uint64_t ad = umma_sdesc(slab_at(buf, t) + tap_shift(tap) + 2u * j * kPlane, kPlane, kRowY);
-              umma_bf16(tmem + (uint32_t)t * a.cols, ad, bd, idesc, (g | tap | j) != 0);
-            }
+            umma_bf16(tmem, ad, bd, idesc, (g | tap | j) != 0);
           }
           if (!resident) {
             umma_commit(b_free(r));
@@ -236,43 +222,41 @@ __global__ void __launch_bounds__(kConvThreads, 1) conv3_tc_kernel(const __grid_
     }
     // the producer's own warp parks here instead of spinning beside it
     __syncwarp();
-    const bool got = mbar_wait_bounded(ACC_FULL, (uint32_t)(bt & 1));
+    const bool got = mbar_wait_bounded(ACC_FULL, (uint32_t)(it & 1));
     if (__syncthreads_or(!got || abort_sh)) {
       if (tid == 0) atomicExch(a.error, 1);
       break;
     }
     tc_fence_after();
+    int tx, ty, tz;
+    tile_of(it, tx, ty, tz);
     const int m = warp * 32 + lane;
-    for (int t = 0; t < nt; ++t) {
-      int tx, ty, tz;
-      tile_of(bt * TB + t, tx, ty, tz);
-      const int x = tx * kTX + (m & 7), y = ty * kTY + (m >> 3);
-      const bool valid = x < a.X && y < a.Y;
-      const size_t vox = ((size_t)tz * a.Y + (valid ? y : 0)) * a.X + (valid ? x : 0);
-      for (int c0 = 0; c0 < cout; c0 += 16) {
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)t * a.cols + (uint32_t)c0, v);
-        if (valid) {
-          if (a.bias) {
+    const int x = tx * kTX + (m & 7), y = ty * kTY + (m >> 3);
+    const bool valid = x < a.X && y < a.Y;
+    const size_t vox = ((size_t)tz * a.Y + (valid ? y : 0)) * a.X + (valid ? x : 0);
+    for (int c0 = 0; c0 < cout; c0 += 16) {
+      float v[16];
+      tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      if (valid) {
+        if (a.bias) {
 #pragma unroll
-            for (int k = 0; k < 16; ++k) v[k] += a.bias[c0 + k];
-          }
-          if (a.relu) {
+          for (int k = 0; k < 16; ++k) v[k] += a.bias[c0 + k];
+        }
+        if (a.relu) {
 #pragma unroll
-            for (int k = 0; k < 16; ++k) v[k] = fmaxf(v[k], 0.0f);
-          }
-          if (a.mask) {
-            float mk[16];
-            load_bf16x16(a.mask + vox * a.mstride + a.moff + c0, mk);
+          for (int k = 0; k < 16; ++k) v[k] = fmaxf(v[k], 0.0f);
+        }
+        if (a.mask) {
+          float mk[16];
+          load_bf16x16(a.mask + vox * a.mstride + a.moff + c0, mk);
 #pragma unroll
-            for (int k = 0; k < 16; ++k) v[k] = mk[k] > 0.0f ? v[k] : 0.0f;
-          }
-          if (a.out) store_bf16x16(a.out + vox * a.ostride + a.ooff + c0, v);
-          if (a.outf) {
+          for (int k = 0; k < 16; ++k) v[k] = mk[k] > 0.0f ? v[k] : 0.0f;
+        }
+        if (a.out) store_bf16x16(a.out + vox * a.ostride + a.ooff + c0, v);
+        if (a.outf) {
 #pragma unroll
-            for (int k = 0; k < 16; ++k)
-              if (c0 + k < a.ofvalid) a.outf[vox * a.ofstride + c0 + k] = v[k];
-          }
+          for (int k = 0; k < 16; ++k)
+            if (c0 + k < a.ofvalid) a.outf[vox * a.ofstride + c0 + k] = v[k];
         }
       }
     }
