@@ -157,18 +157,24 @@ __global__ void __launch_bounds__(BLOCK, 1) rbgs_sweep_carry_kernel(TmaSweepArgs
     const bool ok = mbar_wait_bounded(bar_base + 8u * (unsigned)(g % NB), (unsigned)((g / NB) & 1));
     return __syncthreads_and(ok) != 0;
   };
-  auto prolong_add = [&](int q, int slot) {
-    if (q < 0 || q >= nk) return;
-    const int xq = oX + slot * xslot, cq = oXC + slot * cplane;
-    for (int e = tid; e < xrows * ni; e += BLOCK) {
-      const int r = e / ni, i = e - r * ni;
-      const int crr = ((jr0 + r) >> 1) - cr0;
-      sm[xq + e] = sm[xq + e] + sm[cq + crr * a.cni + (i >> 1)];
-    }
+  static_assert(!(ZERO_X && PROLONG), "the prolongation needs an incoming x");
+  // PROLONG: the staged x planes hold x_in; x_in + P x_c (injection of the
+  // staged coarse plane of the same slot) is formed where an old x value is
+  // read - the thread's own quad when it enters the registers, the y and
+  // x-edge neighbours of the red pass - and the red pass stores only the red
+  // cells, so the shared-memory black cells stay x_in for every reader
+  auto cadd4 = [&](float4 v, int slot, int jj) -> float4 {
+    if (!PROLONG) return v;
+    const float2 c = *reinterpret_cast<const float2*>(sm + oXC + slot * cplane + ((jj >> 1) - cr0) * a.cni +
+                                                      (i0 >> 1));
+    v.x = v.x + c.x;
+    v.y = v.y + c.x;
+    v.z = v.z + c.y;
+    v.w = v.w + c.y;
+    return v;
   };
-  auto zero_x = [&](int slot) {
-    const int xq = oX + slot * xslot;
-    for (int e = tid; e < xrows * ni; e += BLOCK) sm[xq + e] = 0.0f;
+  auto cadd1 = [&](float v, int slot, int jj, int ii) -> float {
+    return PROLONG ? v + sm[oXC + slot * cplane + ((jj >> 1) - cr0) * a.cni + (ii >> 1)] : v;
   };
 
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -204,21 +210,12 @@ __global__ void __launch_bounds__(BLOCK, 1) rbgs_sweep_carry_kernel(TmaSweepArgs
     const int sxm1 = wrap(px - 1, RX), sxp1 = wrap(px + 1, RX);
     const int scm1 = wrap(pc - 1, RC);
     const int szm1 = wrap(pz - 1, RZ);
-    if (PROLONG) {
-      if (p == p0) {
-        if (PROLONG) { prolong_add(p - 1, sxm1); prolong_add(p, px); }
-        if (ZERO_X) { zero_x(sxm1); zero_x(px); }
-      }
-      if (PROLONG) prolong_add(p + 1, sxp1);
-      if (ZERO_X) zero_x(sxp1);
-      __syncthreads();
-    }
     const int x0 = oX + px * xslot, xm = oX + sxm1 * xslot;
     if (p == p0 && act_red) {
       // entering the march: the planes before p0 come from shared memory
       // (old values; only their black cells are read by red(p0))
-      if (!XZ && p >= 1) X1 = ld4f(sm + xm + xo);
-      if (!XZ && p >= 0 && p < nk) X0 = ld4f(sm + x0 + xo);
+      if (!XZ && p >= 1) X1 = cadd4(ld4f(sm + xm + xo), sxm1, j);
+      if (!XZ && p >= 0 && p < nk) X0 = cadd4(ld4f(sm + x0 + xo), px, j);
       if (p >= 1) pczp = ld4f(cs + oZP + szm1 * cslot + co);
     }
 
@@ -228,10 +225,10 @@ __global__ void __launch_bounds__(BLOCK, 1) rbgs_sweep_carry_kernel(TmaSweepArgs
     // is outside the domain (p = -1), so X0 holds x(p) on every entry
     float4 xn = z4, xym = z4, xyp = z4, czp = z4;
     CarryCoef C{z4, z4, z4, z4, z4};
-    if (!XZ && act_red && p + 1 >= 0 && p + 1 < nk) xn = ld4f(sm + oX + sxp1 * xslot + xo);
+    if (!XZ && act_red && p + 1 >= 0 && p + 1 < nk) xn = cadd4(ld4f(sm + oX + sxp1 * xslot + xo), sxp1, j);
     if (do_red && act_red) {
-      if (!XZ && ylo) xym = ld4f(sm + x0 + xo - ni);
-      if (!XZ && yhi) xyp = ld4f(sm + x0 + xo + ni);
+      if (!XZ && ylo) xym = cadd4(ld4f(sm + x0 + xo - ni), px, j - 1);
+      if (!XZ && yhi) xyp = cadd4(ld4f(sm + x0 + xo + ni), px, j + 1);
       C.bb = ld4f(sm + oB + pc * cslot + co);
       C.dd = ld4f(cs + oD + pc * cslot + co);
       C.cx = ld4f(cs + oXP + pc * cslot + co);
@@ -244,20 +241,28 @@ __global__ void __launch_bounds__(BLOCK, 1) rbgs_sweep_carry_kernel(TmaSweepArgs
       float xr = __shfl_down_sync(FULL, X0.x, 1);
       if (do_red && act_red) {
         if (warp_l && xlo) {
-          xl = XZ ? 0.0f : sm[x0 + xo - 1];
+          xl = XZ ? 0.0f : cadd1(sm[x0 + xo - 1], px, j, i0 - 1);
           cxl = float(ldv(cs + oXP + pc * cslot + co - 1));
         }
-        if (warp_r && need_r) xr = XZ ? 0.0f : sm[x0 + xo + 4];
+        if (warp_r && need_r) xr = XZ ? 0.0f : cadd1(sm[x0 + xo + 4], px, j, i0 + 4);
         xl = xlo ? xl : 0.0f;
         xr = need_r ? xr : 0.0f;
         if (((j + p + 1) & 1) == 0) {
           X0.x = relax_quad_cell_m<0>(X0, xym, xyp, X1, xn, xl, xr, C, cxl, czp, pczp);
           X0.z = relax_quad_cell_m<2>(X0, xym, xyp, X1, xn, xl, xr, C, cxl, czp, pczp);
+          if (PROLONG) {
+            sm[x0 + xo] = X0.x;
+            sm[x0 + xo + 2] = X0.z;
+          }
         } else {
           X0.y = relax_quad_cell_m<1>(X0, xym, xyp, X1, xn, xl, xr, C, cxl, czp, pczp);
           X0.w = relax_quad_cell_m<3>(X0, xym, xyp, X1, xn, xl, xr, C, cxl, czp, pczp);
+          if (PROLONG) {
+            sm[x0 + xo + 1] = X0.y;
+            sm[x0 + xo + 3] = X0.w;
+          }
         }
-        *reinterpret_cast<float4*>(sm + x0 + xo) = X0;
+        if (!PROLONG) *reinterpret_cast<float4*>(sm + x0 + xo) = X0;
       }
     }
     // No barrier here: the black pass of plane p-1 reads its own quad's red
