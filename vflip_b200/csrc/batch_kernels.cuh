@@ -7,18 +7,18 @@
 // of one level of one system - and the CTAs take items grid-stride; a grid
 // barrier separates dependent phases, and every CTA meets every barrier (no
 // CTA leaves the program early).  Per PCG iteration:
-//   V-cycle: for each level l: four fused red-black sweeps (sweep tiles of
-//            rows x planes, out of place, the first from x = 0: amgPrecond
-//            zero-fills x), then b_{l+1} = R (b_l - A_l x_l); the coarsest
+//   V-cycle: for each level l: four fused red-black sweeps (16 x 8 x 4
+//            cell tiles with a two-cell halo, out of place, the first from
+//            x = 0: amgPrecond zero-fills x), then b_{l+1} = R (b_l - A_l x_l); the coarsest
 //            level of each system (one CTA per system: the FP64
 //            band-Cholesky solve, or red-black sweeps in shared memory); up:
 //            four sweeps, the first on x + P x_{l+1}; the last sweep of
 //            level 0 also forms z.r (rho, beta);
 //   s = z + beta s; q = A s with s.q (alpha); x += alpha s, r -= alpha q
 //   with |r|_inf (the stop test); systems that converged drop out.
-// A sweep tile follows rbgs_sweep_kernel's schedule and arithmetic, so the
-// V-cycle's values are the single-system kernels' (the reductions are
-// grouped per item instead).
+// A sweep tile follows rbgs_sweep_tile_kernel's scheme and every smoother's
+// arithmetic, so the V-cycle's values are the single-system kernels' (the
+// reductions are grouped per item instead).
 //
 // Reductions are deterministic: every item writes its partial to a slot of
 // its own, and after the barrier one CTA per system folds that system's
@@ -51,7 +51,7 @@ struct BatchLevel {
   V* b;  // level rhs (level 0: the PCG residual r)
   V* x;  // level solution (level 0: z); every sweep sequence ends here
   V* t;  // the other buffer of the out-of-place sweeps
-  int tyo, kz, ntj;  // sweep tiles: tyo rows x kz planes, ntj row tiles per plane range
+  int ntx, nty;  // sweep tiles (kBTX x kBTY x kBTZ cells) along x and y; tile t = tx + ntx (ty + nty tz)
 };
 
 template <typename S0, typename SC, typename V>
@@ -103,92 +103,86 @@ __device__ __forceinline__ bool batch_live(const BatchSys<S0, SC, V>& y) {
   return __ldcg(y.state) == 1;
 }
 
-// One fused red-black sweep (both colours, out of place) of one tile of a
-// level: rbgs_sweep_kernel's schedule and arithmetic for the rows
-// [tj*tyo, +tyo) of the planes [tk*kz, +kz) - a rolling window of four
-// staged planes (xs, shared memory), red on plane p over the tile and a
-// one-row ring, black on plane p-1 over the tile, store plane p-1; the ring
-// rows and end planes are recomputed by the neighbouring tiles.  ZERO: the
-// incoming x is 0; PROLONG: it is x_in + P x_c; DOT: returns this thread's
-// part of sum(x_out * b).
+// One fused red-black sweep (both colours, out of place) of one kBTX x kBTY
+// x kBTZ tile of a level, as rbgs_sweep_tile_kernel does it: x, b and the
+// operator over the tile and a two-cell halo are staged at once, the red
+// pass runs over the tile and a one-cell ring, the black pass over the tile,
+// and the tile is stored (the halo is recomputed by the neighbouring tiles).
+// The same values as every other smoother bit for bit.  ZERO: the incoming
+// x is 0; PROLONG: it is x_in + P x_c; DOT: returns this thread's part of
+// sum(x_out * b).  Vectors written inside the kernel are read through L2.
+constexpr int kBTX = 16, kBTY = 8, kBTZ = 4;
+constexpr int kBRX = kBTX + 4, kBRY = kBTY + 4, kBRZ = kBTZ + 4, kBRegion = kBRX * kBRY * kBRZ;
+
 template <typename S, typename V, bool ZERO, bool PROLONG, bool DOT>
 __device__ double batch_sweep(const BatchLevel<S, V>& L, const V* x_in, V* x_out, const V* xc, int cni, int cnj,
-                              int tj, int tk, typename Num<V>::Acc* xs) {
+                              int ti, int tj, int tk, typename Num<V>::Acc* sm) {
   using A = typename Num<V>::Acc;
-  const int ni = L.ni, nj = L.nj, nk = L.nk, tyo = L.tyo;
+  A *xs = sm, *bs = sm + kBRegion, *ds = sm + 2 * kBRegion, *xps = sm + 3 * kBRegion, *yps = sm + 4 * kBRegion,
+    *zps = sm + 5 * kBRegion;
+  const int ni = L.ni, nj = L.nj, nk = L.nk;
   const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
-  const int j0 = tj * tyo, k0 = tk * L.kz;
-  const int kend = min(k0 + L.kz, nk), jout1 = min(j0 + tyo, nj);
-  const int jr0 = max(j0 - 2, 0), jr1 = min(j0 + tyo + 2, nj);
-  const int jred0 = max(j0 - 1, 0), jred1 = min(j0 + tyo + 1, nj);
-  const int rows = jr1 - jr0, pls = (tyo + 4) * ni;
-  auto X = [&](int p) -> A* { return xs + (size_t)(p & 3) * pls; };
-  auto stage = [&](int q) {
-    if (q < 0 || q >= nk) return;
-    A* dst = X(q);
-    const int cnt = rows * ni;
-    const size_t base = (size_t)q * sz + (size_t)jr0 * sy;
-    for (int e = threadIdx.x; e < cnt; e += kBatchThreads) {
-      A v;
-      if (ZERO) {
-        v = A(0);
-      } else {
-        v = ldcg(x_in + base + e);
-        if (PROLONG) {
-          const int i = e % ni, j = jr0 + e / ni;
-          v = v + ldcg(xc + lin3(i >> 1, j >> 1, q >> 1, cni, cnj));
-        }
+  const int oi = ti * kBTX - 2, oj = tj * kBTY - 2, ok = tk * kBTZ - 2;
+  for (int e = threadIdx.x; e < kBRegion; e += kBatchThreads) {
+    const int ri = e % kBRX, rj = (e / kBRX) % kBRY, rk = e / (kBRX * kBRY);
+    const int i = oi + ri, j = oj + rj, k = ok + rk;
+    A x = A(0), bb = A(0), d = A(0), cx = A(0), cy = A(0), cz = A(0);
+    if (i >= 0 && i < ni && j >= 0 && j < nj && k >= 0 && k < nk) {
+      const size_t g = (size_t)i + sy * j + sz * k;
+      if (!ZERO) {
+        x = ldcg(x_in + g);
+        if (PROLONG) x = x + ldcg(xc + lin3(i >> 1, j >> 1, k >> 1, cni, cnj));
       }
-      dst[e] = v;
+      bb = ldcg(L.b + g);
+      d = A(ldg(L.diag + g));
+      cx = A(ldg(L.xp + g));
+      cy = A(ldg(L.yp + g));
+      cz = A(ldg(L.zp + g));
     }
-  };
-  auto relax = [&](int p, int r0, int r1, int parity) {
-    A* xm1 = X(p - 1);
-    A* x0 = X(p);
-    A* xp1 = X(p + 1);
-    const int cnt = (r1 - r0) * ni;
-    const size_t pbase = (size_t)p * sz;
-    for (int e = threadIdx.x; e < cnt; e += kBatchThreads) {
-      const int j = r0 + e / ni;
-      const int i = e - (j - r0) * ni;
-      if (((i + j + p) & 1) != parity) continue;
-      const size_t g = pbase + (size_t)j * sy + i;
-      const int sidx = (j - jr0) * ni + i;
-      A sum = A(0);
-      if (p > 0) sum = gs_madd(sum, A(ldg(L.zp + g - sz)), xm1[sidx]);
-      if (j > 0) sum = gs_madd(sum, A(ldg(L.yp + g - sy)), x0[sidx - ni]);
-      if (i > 0) sum = gs_madd(sum, A(ldg(L.xp + g - 1)), x0[sidx - 1]);
-      if (i < ni - 1) sum = gs_madd(sum, A(ldg(L.xp + g)), x0[sidx + 1]);
-      if (j < nj - 1) sum = gs_madd(sum, A(ldg(L.yp + g)), x0[sidx + ni]);
-      if (p < nk - 1) sum = gs_madd(sum, A(ldg(L.zp + g)), xp1[sidx]);
-      const A d = A(ldg(L.diag + g));
-      x0[sidx] = (d != A(0)) ? gs_div(ldcg(L.b + g) - sum, d) : A(0);
-    }
-  };
-  double dot = 0.0;
-  stage(k0 - 2);
-  stage(k0 - 1);
-  for (int p = k0 - 1; p <= kend; ++p) {
-    stage(p + 1);
-    __syncthreads();
-    if (p >= 0 && p < nk) relax(p, jred0, jred1, 1);
-    __syncthreads();
-    const int q = p - 1;
-    const bool out_plane = q >= k0 && q < kend;
-    if (out_plane) relax(q, j0, jout1, 0);
-    __syncthreads();
-    if (out_plane) {
-      const A* src = X(q) + (size_t)(j0 - jr0) * ni;
-      const int cnt = (jout1 - j0) * ni;
-      const size_t base = (size_t)q * sz + (size_t)j0 * sy;
-      for (int e = threadIdx.x; e < cnt; e += kBatchThreads) {
-        const V o = cvt<V>(src[e]);
-        x_out[base + e] = o;
-        if (DOT) dot += (double)ldv(&o) * (double)ldcg(L.b + base + e);
-      }
-    }
+    xs[e] = x;
+    bs[e] = bb;
+    ds[e] = d;
+    xps[e] = cx;
+    yps[e] = cy;
+    zps[e] = cz;
   }
-  __syncthreads();  // the next tile restages the window
+  __syncthreads();
+  constexpr int SY = kBRX, SZ = kBRX * kBRY;
+  auto pass = [&](int lo, int hx, int hy, int hz, int parity) {
+    const int wx = hx - lo, wy = hy - lo, cnt = wx * wy * (hz - lo);
+    for (int q = threadIdx.x; q < cnt; q += kBatchThreads) {
+      const int ri = lo + q % wx, rj = lo + (q / wx) % wy, rk = lo + q / (wx * wy);
+      const int i = oi + ri, j = oj + rj, k = ok + rk;
+      if (i < 0 || i >= ni || j < 0 || j >= nj || k < 0 || k >= nk) continue;
+      if (((i + j + k) & 1) != parity) continue;
+      const int e = ri + SY * rj + SZ * rk;
+      A sum = A(0);
+      if (k > 0) sum = gs_madd(sum, zps[e - SZ], xs[e - SZ]);
+      if (j > 0) sum = gs_madd(sum, yps[e - SY], xs[e - SY]);
+      if (i > 0) sum = gs_madd(sum, xps[e - 1], xs[e - 1]);
+      if (i < ni - 1) sum = gs_madd(sum, xps[e], xs[e + 1]);
+      if (j < nj - 1) sum = gs_madd(sum, yps[e], xs[e + SY]);
+      if (k < nk - 1) sum = gs_madd(sum, zps[e], xs[e + SZ]);
+      const A d = ds[e];
+      xs[e] = (d != A(0)) ? gs_div(bs[e] - sum, d) : A(0);
+    }
+  };
+  pass(1, kBRX - 1, kBRY - 1, kBRZ - 1, 1);  // red: the tile and a one-cell ring
+  __syncthreads();
+  pass(2, kBRX - 2, kBRY - 2, kBRZ - 2, 0);  // black: the tile
+  __syncthreads();
+  double dot = 0.0;
+  constexpr int cnt = kBTX * kBTY * kBTZ;
+  for (int q = threadIdx.x; q < cnt; q += kBatchThreads) {
+    const int ri = 2 + q % kBTX, rj = 2 + (q / kBTX) % kBTY, rk = 2 + q / (kBTX * kBTY);
+    const int i = oi + ri, j = oj + rj, k = ok + rk;
+    if (i >= ni || j >= nj || k >= nk) continue;
+    const int e = ri + SY * rj + SZ * rk;
+    const V o = cvt<V>(xs[e]);
+    x_out[(size_t)i + sy * j + sz * k] = o;
+    if (DOT) dot += (double)ldv(&o) * (double)bs[e];
+  }
+  __syncthreads();  // the next tile restages the region
   return dot;
 }
 
@@ -392,7 +386,7 @@ __global__ void __launch_bounds__(kBatchThreads) batch_pcg_kernel(const BatchSys
     }
   };
   // every sweep tile of level l of the systems that smooth there (live ones):
-  // fn(system, its index, tile index within the system, row tile, plane range)
+  // fn(system, its index, tile index within the system, tile x, y, z)
   auto tiles = [&](int l, auto&& fn) {
     const int* pre = p.sweep_pre + (size_t)l * (nsys + 1);
     const int total = __ldg(pre + nsys);
@@ -401,8 +395,8 @@ __global__ void __launch_bounds__(kBatchThreads) batch_pcg_kernel(const BatchSys
       const BatchSys<S0, SC, V>& y = sys[s];
       if (!batch_live(y)) continue;
       const int local = item - __ldg(pre + s);
-      const int ntj = l == 0 ? y.fine.ntj : y.lv[l].ntj;
-      fn(y, s, local, local % ntj, local / ntj);
+      const int ntx = l == 0 ? y.fine.ntx : y.lv[l].ntx, nty = l == 0 ? y.fine.nty : y.lv[l].nty;
+      fn(y, s, local, local % ntx, (local / ntx) % nty, local / (ntx * nty));
     }
   };
   A* xs = reinterpret_cast<A*>(bsm);  // the sweeps' plane window
@@ -489,17 +483,17 @@ __global__ void __launch_bounds__(kBatchThreads) batch_pcg_kernel(const BatchSys
     // ---- V-cycle, down: four sweeps from x = 0 ending in x (t, x, t, x)
     for (int l = 0; l + 1 < p.lmax; ++l) {
       for (int sw = 0; sw < 4; ++sw) {
-        tiles(l, [&](const BatchSys<S0, SC, V>& y, int, int, int tj, int tk) {
+        tiles(l, [&](const BatchSys<S0, SC, V>& y, int, int, int ti, int tj, int tk) {
           if (l == 0) {
             const BatchLevel<S0, V>& L = y.fine;
-            if (sw == 0) batch_sweep<S0, V, true, false, false>(L, nullptr, L.t, nullptr, 0, 0, tj, tk, xs);
+            if (sw == 0) batch_sweep<S0, V, true, false, false>(L, nullptr, L.t, nullptr, 0, 0, ti, tj, tk, xs);
             else batch_sweep<S0, V, false, false, false>(L, sw & 1 ? L.t : L.x, sw & 1 ? L.x : L.t, nullptr, 0, 0,
-                                                         tj, tk, xs);
+                                                         ti, tj, tk, xs);
           } else {
             const BatchLevel<SC, V>& L = y.lv[l];
-            if (sw == 0) batch_sweep<SC, V, true, false, false>(L, nullptr, L.t, nullptr, 0, 0, tj, tk, xs);
+            if (sw == 0) batch_sweep<SC, V, true, false, false>(L, nullptr, L.t, nullptr, 0, 0, ti, tj, tk, xs);
             else batch_sweep<SC, V, false, false, false>(L, sw & 1 ? L.t : L.x, sw & 1 ? L.x : L.t, nullptr, 0, 0,
-                                                         tj, tk, xs);
+                                                         ti, tj, tk, xs);
           }
         });
         grid.sync();
@@ -532,24 +526,24 @@ __global__ void __launch_bounds__(kBatchThreads) batch_pcg_kernel(const BatchSys
     for (int l = p.lmax - 2; l >= 0; --l) {
       for (int sw = 0; sw < 4; ++sw) {
         const bool last = l == 0 && sw == 3;
-        tiles(l, [&](const BatchSys<S0, SC, V>& y, int s, int local, int tj, int tk) {
+        tiles(l, [&](const BatchSys<S0, SC, V>& y, int s, int local, int ti, int tj, int tk) {
           const BatchLevel<SC, V>& C = y.lv[l + 1];
           if (l == 0) {
             const BatchLevel<S0, V>& L = y.fine;
             double d = 0.0;
-            if (sw == 0) batch_sweep<S0, V, false, true, false>(L, L.x, L.t, C.x, C.ni, C.nj, tj, tk, xs);
-            else if (last) d = batch_sweep<S0, V, false, false, true>(L, L.t, L.x, nullptr, 0, 0, tj, tk, xs);
+            if (sw == 0) batch_sweep<S0, V, false, true, false>(L, L.x, L.t, C.x, C.ni, C.nj, ti, tj, tk, xs);
+            else if (last) d = batch_sweep<S0, V, false, false, true>(L, L.t, L.x, nullptr, 0, 0, ti, tj, tk, xs);
             else batch_sweep<S0, V, false, false, false>(L, sw & 1 ? L.t : L.x, sw & 1 ? L.x : L.t, nullptr, 0, 0,
-                                                         tj, tk, xs);
+                                                         ti, tj, tk, xs);
             if (last) {
               const double bs = batch_block_sum(d, red);
               if (threadIdx.x == 0) *slot(s, local) = bs;
             }
           } else {
             const BatchLevel<SC, V>& L = y.lv[l];
-            if (sw == 0) batch_sweep<SC, V, false, true, false>(L, L.x, L.t, C.x, C.ni, C.nj, tj, tk, xs);
+            if (sw == 0) batch_sweep<SC, V, false, true, false>(L, L.x, L.t, C.x, C.ni, C.nj, ti, tj, tk, xs);
             else batch_sweep<SC, V, false, false, false>(L, sw & 1 ? L.t : L.x, sw & 1 ? L.x : L.t, nullptr, 0, 0,
-                                                         tj, tk, xs);
+                                                         ti, tj, tk, xs);
           }
         });
         grid.sync();

@@ -2257,21 +2257,16 @@ int batched_persistent(vflip_ctx* ctx, int nsys, const vflip_system* sys, double
     BatchSys<S0, SC, V>& d = desc[i];
     std::memset(&d, 0, sizeof d);
     d.nl = nl;
-    // sweep tiles: up to 8 rows, plane ranges of about `CH` cells (at least 4 planes)
-    auto shape = [&](int ni_, int nj_, int nk_, int& tyo, int& kz, int& ntj) {
-      tyo = std::min(8, nj_);
-      kz = std::max(4, CH / std::max(1, ni_ * tyo));
-      kz = std::min(kz, nk_);
-      ntj = (nj_ + tyo - 1) / tyo;
-      smem_doubles = std::max(smem_doubles, (int)((4 * (size_t)(tyo + 4) * ni_ * sizeof(A) + 7) / 8));
-    };
+    // sweep tiles of kBTX x kBTY x kBTZ cells; their staged region (6 arrays
+    // over the tile and a two-cell halo) sets the shared memory
+    smem_doubles = std::max(smem_doubles, (int)((6 * (size_t)kBRegion * sizeof(A) + 7) / 8));
     const Level<S0, V>& F = b.T.fine;
-    d.fine = BatchLevel<S0, V>{F.d.ni, F.d.nj, F.d.nk, F.diag, F.xp, F.yp, F.zp, b.r, b.z, b.sd, 0, 0, 0};
-    shape(F.d.ni, F.d.nj, F.d.nk, d.fine.tyo, d.fine.kz, d.fine.ntj);
+    d.fine = BatchLevel<S0, V>{F.d.ni, F.d.nj, F.d.nk, F.diag, F.xp, F.yp, F.zp, b.r, b.z, b.sd,
+                               (F.d.ni + kBTX - 1) / kBTX, (F.d.nj + kBTY - 1) / kBTY};
     for (int l = 1; l < nl; ++l) {
       const Level<SC, V>& L = b.T.coarse[l - 1];
-      d.lv[l] = BatchLevel<SC, V>{L.d.ni, L.d.nj, L.d.nk, L.diag, L.xp, L.yp, L.zp, L.b, L.xa, L.xb, 0, 0, 0};
-      shape(L.d.ni, L.d.nj, L.d.nk, d.lv[l].tyo, d.lv[l].kz, d.lv[l].ntj);
+      d.lv[l] = BatchLevel<SC, V>{L.d.ni, L.d.nj, L.d.nk, L.diag, L.xp, L.yp, L.zp, L.b, L.xa, L.xb,
+                                  (L.d.ni + kBTX - 1) / kBTX, (L.d.nj + kBTY - 1) / kBTY};
     }
     d.x = b.x;
     d.s = b.s;
@@ -2307,8 +2302,8 @@ int batched_persistent(vflip_ctx* ctx, int nsys, const vflip_system* sys, double
       if (l == 0) ci = ((long long)d.fine.ni * d.fine.nj * d.fine.nk + CH - 1) / CH;
       if (l + 1 < d.nl) {
         ri = ((long long)d.lv[l + 1].ni * d.lv[l + 1].nj * d.lv[l + 1].nk + CH - 1) / CH;
-        const int nk_ = l == 0 ? d.fine.nk : d.lv[l].nk, kz = l == 0 ? d.fine.kz : d.lv[l].kz;
-        si = (long long)(l == 0 ? d.fine.ntj : d.lv[l].ntj) * ((nk_ + kz - 1) / kz);
+        const int nk_ = l == 0 ? d.fine.nk : d.lv[l].nk;
+        si = (long long)(l == 0 ? d.fine.ntx * d.fine.nty : d.lv[l].ntx * d.lv[l].nty) * ((nk_ + kBTZ - 1) / kBTZ);
       }
       const size_t o = (size_t)l * (nsys + 1) + i;
       cell_pre[o + 1] = cell_pre[o] + (int)ci;
