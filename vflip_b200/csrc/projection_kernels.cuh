@@ -149,7 +149,9 @@ __global__ void assemble_kernel(const float* __restrict__ u, const float* __rest
   const float inv_h2 = inv_h * inv_h;
   auto div_h = [&](float x) { return inv_h != 0.0f ? x * inv_h : x / h; };
   auto div_h2 = [&](float x) { return inv_h != 0.0f ? x * inv_h2 : x / h2; };
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+  // two cells per thread and round, so each thread has both cells' loads in
+  // flight at once (the loop was bound by memory latency)
+  auto cell = [&](size_t e) {
     int i, j, k;
     decode3(e, ni, nj, i, j, k);
     double d = 0.0, cx = 0.0, cy = 0.0, cz = 0.0, b = 0.0;
@@ -190,6 +192,11 @@ __global__ void assemble_kernel(const float* __restrict__ u, const float* __rest
       op32[2 * n + e] = (float)cy;
       op32[3 * n + e] = (float)cz;
     }
+  };
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += 2 * stride) {
+    cell(e);
+    if (e + stride < n) cell(e + stride);
   }
 }
 
@@ -208,8 +215,8 @@ __global__ void gradient_kernel(const P* __restrict__ p, float* __restrict__ u, 
                                 int nk, int variant, float dt, float inv_h) {
   const size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
   const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nu + nv + nw;
-       e += (size_t)gridDim.x * blockDim.x) {
+  // two faces per thread and round, both faces' loads in flight at once
+  auto face = [&](size_t e) {
     const bool sub = variant == 1;
     const int lo = sub ? 0 : 1;  // first face index excluded: faces > lo
     const int hi = sub ? 0 : 1;  // faces < n - hi
@@ -244,6 +251,11 @@ __global__ void gradient_kernel(const P* __restrict__ p, float* __restrict__ u, 
         w[f] = upd(w[f], (double)p[c], (double)p[c - sz], ww[f], ws[f]);
       }
     }
+  };
+  const size_t nf = nu + nv + nw, stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nf; e += 2 * stride) {
+    face(e);
+    if (e + stride < nf) face(e + stride);
   }
 }
 
