@@ -63,7 +63,8 @@ def parse():
     ap.add_argument("--learned-epochs", type=int, default=16)
     ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds for the reference arm's timed steps")
     ap.add_argument("--kernels", default=None,
-                    help="instead of the step: per-kernel timings (comma list of advect, p2g, g2p, vcycle, unet) at --n, "
+                    help="instead of the step: per-kernel timings (comma list of advect, p2g, g2p, vcycle, unet, "
+                         "hostlink) at --n, "
                          "one JSON line each")
     ap.add_argument("--reps", type=int, default=5, help="timed repetitions per kernel (--kernels)")
     ap.add_argument("--unet-sizes", type=int, nargs="+", default=[32, 64, 128], help="network grids (--kernels unet)")
@@ -941,6 +942,52 @@ def kernel_lines(a):
             vcycle_lines(a, s, timed, line)
     if "unet" in what:
         unet_lines(a)
+    if "hostlink" in what:
+        hostlink_lines(a)
+
+
+def hostlink_lines(a):
+    """The host link the end-to-end step crosses: one step's worth of fields
+    (5 x n^3 FP32, pinned host memory) copied host to device, device to host,
+    and both directions at once on two streams (CUDA events)."""
+    import torch
+
+    n = 5 * a.n ** 3
+    h_in = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    h_out = torch.empty(n, dtype=torch.float32, pin_memory=True)
+    d_in = torch.empty(n, dtype=torch.float32, device="cuda")
+    d_out = torch.empty(n, dtype=torch.float32, device="cuda")
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(a.reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / a.reps
+
+    def both():
+        cur = torch.cuda.current_stream()
+        s1.wait_stream(cur)
+        s2.wait_stream(cur)
+        with torch.cuda.stream(s1):
+            d_in.copy_(h_in, non_blocking=True)
+        with torch.cuda.stream(s2):
+            h_out.copy_(d_out, non_blocking=True)
+        cur.wait_stream(s1)
+        cur.wait_stream(s2)
+
+    gb = n * 4 / 1e9
+    up = timed(lambda: d_in.copy_(h_in, non_blocking=True))
+    down = timed(lambda: h_out.copy_(d_out, non_blocking=True))
+    duplex = timed(both)
+    print(json.dumps({"kernel": "host link (pinned, 5 fields)", "n": a.n, "bytes_each_way": n * 4,
+                      "h2d_ms": up, "h2d_gbs": gb / up * 1e3, "d2h_ms": down, "d2h_gbs": gb / down * 1e3,
+                      "both_ms": duplex, "both_gbs_each_way": gb / duplex * 1e3}), flush=True)
 
 
 def vcycle_lines(a, s, timed, line):

@@ -4,6 +4,8 @@
     up to the grouping of its s.q partial sums, its solution;
   * the one-CTA V-cycle tail gives the per-level launches' bits;
   * the tiled sweep of the small levels gives the marching sweeps' bits;
+  * the two-CTA register-carry sweep of rows <= 128 cells gives the plain
+    fused kernel's bits;
   * the projection's PCG, which reads the FP32 copies of the couplings it
     assembled, gives the bits of the same solve on the FP64 operator."""
 import numpy as np
@@ -137,3 +139,30 @@ def test_tiled_sweep_matches_marching_sweeps(prec, dims):
     (za, xa, ia), (zb, xb, ib) = out
     assert torch.equal(za, zb)
     assert torch.equal(xa, xb) and ia == ib
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+@pytest.mark.parametrize("dims", [(128, 96, 72), (100, 64, 50)])
+def test_narrow_carry_sweep_matches_plain_kernel(prec, dims):
+    """Levels whose rows hold 68..128 cells sweep with the 256-thread,
+    two-CTA-per-SM register-carry kernel (the fine level here, with its
+    fused prolongation and z.r variants); the plain fused kernel
+    (sweep_kernel 1) gives the same V-cycle and the same solve."""
+    from vflip_b200.solver import Solver
+
+    ni, nj, nk = dims
+    pr = scenes.projection_problem(ni, nj, nk, seed=19, inflow=True, solid_velocity=True)
+    st = rhs = None
+    out = []
+    for kern in (0, 1):
+        with Solver(precision=prec, sweep_kernel=kern, tile_sweep_max_cells=-1) as s:
+            if st is None:
+                st, rhs = s.assemble(ni, nj, nk, pr["h"], pr["U_in"], t(pr["phi"]), t(pr["bdesc"]), t(pr["us"]),
+                                     t(pr["vs"]), t(pr["ws"]), t(pr["u"]), t(pr["v"]), t(pr["w"]))
+            z = s.vcycle(st, rhs).clone()
+            ok, x, stats = s.amgpcg_solve(st, rhs, 1e-6, 100)
+            assert ok
+            out.append((z, x.clone(), stats.iterations))
+    (za, xa, ia), (zb, xb, ib) = out
+    assert torch.equal(za, zb)
+    assert ia == ib

@@ -63,7 +63,7 @@ __device__ __forceinline__ float relax_quad_cell_m(const float4& xc, const float
 }
 
 template <typename S, bool ZERO_X, bool PROLONG, bool DOT, int BLOCK, int NI = 0, int TYO = 0, int DEPTH = 0>
-__global__ void __launch_bounds__(BLOCK, 1) rbgs_sweep_carry_kernel(TmaSweepArgs<S> a) {
+__global__ void __launch_bounds__(BLOCK, BLOCK <= 256 ? 2 : 1) rbgs_sweep_carry_kernel(TmaSweepArgs<S> a) {
   extern __shared__ __align__(128) float sm[];
   constexpr int NB = kTmaMaxDepth + 2;
   __shared__ __align__(8) unsigned long long bars[NB];

@@ -311,7 +311,7 @@ int launch_sweep_t(vflip_ctx* ctx, const SweepArgs<S, V>& a, const SweepShape& s
 // shared-memory budget, persistent CTAs over equal shares of the level's
 // (row tile, plane) pairs.
 struct TmaShape {
-  int tyo, gy, zlen, gz, depth, crows_max, bx, by, threads, l2_ahead;
+  int tyo, gy, zlen, gz, depth, crows_max, bx, by, threads, l2_ahead, cps;
   bool carry;  // register-carry kernel (rbgs_sweep_carry_kernel)
   size_t smem;
 };
@@ -322,6 +322,7 @@ constexpr size_t kTmaSmemMax = 227 * 1024 - 1024;  // opt-in limit minus the sta
 // threads take the red pass of a 7-row tile (9 rows with the ring) in one
 // round instead of two.
 constexpr int kTmaBlock = 512, kTmaBlockWide = 576;
+constexpr int kCarryNarrow = 256;  // the carry kernel on rows of <= 128 cells: 32 quads x (6 tile + 2 ring) rows
 
 // Tile shape of the TMA-pipelined sweep.  Rows per tile, plane ranges and
 // copy depth are chosen so that every CTA of a launch is resident at once
@@ -339,15 +340,20 @@ bool tma_shape(const vflip_config& cfg, const Dims& d, const Dims* cd, bool prol
   while (bx < Q && bx < 128) bx <<= 1;
   // the register-carry kernel gives every (row, quad) of the red pass its own
   // thread: all quads of a row in x, the tile and its two ring rows in y
-  const int carry_threads = kTmaBlockWide;
-  if (carry && (bx < Q || carry_threads % bx != 0 || carry_threads / bx < 3)) return false;
   const int cni = prolong ? cd->ni : 0;
   // one copy group in flight measured fastest at 256^3 (vflip_b200/tune.py): deeper
   // prefetch only shortens the tiles
   const int depth = cfg.smoother_depth > 0 ? std::min(cfg.smoother_depth, kTmaMaxDepth) : 1;
-  const int cps = carry ? 1 : (cfg.smoother_ctas_per_sm > 0 ? std::min(cfg.smoother_ctas_per_sm, 2) : 1);
-  const size_t budget = cps == 1 ? kTmaSmemMax : kTmaSmemMax / 2 - 1024;
   auto bytes = [&](int t) { return tma_layout<S>(d.ni, t, depth, prolong ? (t + 7) / 2 : 0, cni).bytes; };
+  // rows of at most 128 cells (levels that live in L2, where a CTA's march of
+  // plane steps is latency-bound): the carry kernel as two 256-thread CTAs
+  // per SM with 6-row tiles, so twice the CTAs each march half the planes
+  const bool narrow = carry && bx == 32 && Q <= 32 && cfg.smoother_tile_rows == 0 &&
+                      cfg.smoother_ctas_per_sm == 0 && bytes(kCarryNarrow / 32 - 2) <= kTmaSmemMax / 2 - 1024;
+  const int carry_threads = narrow ? kCarryNarrow : kTmaBlockWide;
+  if (carry && (bx < Q || carry_threads % bx != 0 || carry_threads / bx < 3)) return false;
+  const int cps = narrow ? 2 : carry ? 1 : (cfg.smoother_ctas_per_sm > 0 ? std::min(cfg.smoother_ctas_per_sm, 2) : 1);
+  const size_t budget = cps == 1 ? kTmaSmemMax : kTmaSmemMax / 2 - 1024;
   int tyo_max = 0;
   for (int t = 1; t <= d.nj; ++t) {
     if (bytes(t) > budget) break;
@@ -387,6 +393,7 @@ bool tma_shape(const vflip_config& cfg, const Dims& d, const Dims* cd, bool prol
   // measured no faster at 256^3 (the copies bound the step), so 512 unless asked
   o.threads = carry ? carry_threads
                     : (cfg.smoother_threads == kTmaBlockWide && kTmaBlockWide % bx == 0 ? kTmaBlockWide : kTmaBlock);
+  o.cps = cps;
   o.by = o.threads / bx;
   o.l2_ahead = cfg.smoother_prefetch < 0 ? 0 : (cfg.smoother_prefetch > 0 ? std::min(cfg.smoother_prefetch, 8) : 2);
   return o.smem <= budget;
@@ -399,6 +406,7 @@ int launch_tma_t(vflip_ctx* ctx, const TmaSweepArgs<S>& a, const TmaShape& sh) {
   // in flight) runs an instance with that layout compiled in
   const bool fixed = sh.carry && a.ni == 256 && a.tyo == 7 && a.depth == 1;
   auto kern = fixed ? rbgs_sweep_carry_kernel<S, Z, P, D, kTmaBlockWide, 256, 7, 1>
+                    : (sh.carry && sh.threads == kCarryNarrow) ? rbgs_sweep_carry_kernel<S, Z, P, D, kCarryNarrow>
                     : sh.carry ? rbgs_sweep_carry_kernel<S, Z, P, D, kTmaBlockWide>
                                : (wide ? rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlockWide>
                                        : rbgs_sweep_tma_kernel<S, Z, P, D, kTmaBlock>);
