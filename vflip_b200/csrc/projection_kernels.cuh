@@ -161,22 +161,27 @@ __global__ void assemble_kernel(const float* __restrict__ u, const float* __rest
       const size_t iw0 = lin3(i, j, k, ni, nj), iw1 = lin3(i, j, k + 1, ni, nj);
       const bool sub = variant == 1;
       auto term = [&](float wgt) { return sub ? div_h2(wgt * dt) : div_h2(wgt); };
+      // every load up front (one round of memory latency; the solid
+      // velocities are read whether or not the cell turns out fluid)
+      const float uw1 = uw[iu1], uw0 = uw[iu0], vw1 = vw[iv1], vw0 = vw[iv0], ww1 = ww[iw1], ww0 = ww[iw0];
+      const float u1 = u[iu1], u0 = u[iu0], v1 = v[iv1], v0 = v[iv0], w1 = w[iw1], w0 = w[iw0];
+      const float us1 = us[iu1], us0 = us[iu0], vs1 = vs[iv1], vs0 = vs[iv0], ws1 = ws[iw1], ws0 = ws[iw0];
       float t;
-      t = term(uw[iu1]); d = (double)t; if (i < ni - 2) cx = (double)(-t);
-      b = b - (double)div_h(uw[iu1] * u[iu1]);
-      t = term(uw[iu0]); d = d + (double)t;
-      b = b + (double)div_h(uw[iu0] * u[iu0]);
-      t = term(vw[iv1]); d = d + (double)t; if (j < nj - 2) cy = (double)(-t);
-      b = b - (double)div_h(vw[iv1] * v[iv1]);
-      t = term(vw[iv0]); d = d + (double)t;
-      b = b + (double)div_h(vw[iv0] * v[iv0]);
-      t = term(ww[iw1]); d = d + (double)t; if (k < nk - 2) cz = (double)(-t);
-      b = b - (double)div_h(ww[iw1] * w[iw1]);
-      t = term(ww[iw0]); d = d + (double)t;
-      b = b + (double)div_h(ww[iw0] * w[iw0]);
+      t = term(uw1); d = (double)t; if (i < ni - 2) cx = (double)(-t);
+      b = b - (double)div_h(uw1 * u1);
+      t = term(uw0); d = d + (double)t;
+      b = b + (double)div_h(uw0 * u0);
+      t = term(vw1); d = d + (double)t; if (j < nj - 2) cy = (double)(-t);
+      b = b - (double)div_h(vw1 * v1);
+      t = term(vw0); d = d + (double)t;
+      b = b + (double)div_h(vw0 * v0);
+      t = term(ww1); d = d + (double)t; if (k < nk - 2) cz = (double)(-t);
+      b = b - (double)div_h(ww1 * w1);
+      t = term(ww0); d = d + (double)t;
+      b = b + (double)div_h(ww0 * w0);
       if (d > 0) {
-        float sv = (uw[iu1] - 1.0f) * us[iu1] - (uw[iu0] - 1.0f) * us[iu0] + (vw[iv1] - 1.0f) * vs[iv1] -
-                   (vw[iv0] - 1.0f) * vs[iv0] + (ww[iw1] - 1.0f) * ws[iw1] - (ww[iw0] - 1.0f) * ws[iw0];
+        float sv = (uw1 - 1.0f) * us1 - (uw0 - 1.0f) * us0 + (vw1 - 1.0f) * vs1 -
+                   (vw0 - 1.0f) * vs0 + (ww1 - 1.0f) * ws1 - (ww0 - 1.0f) * ws0;
         if (sub) b = b + (double)((1.0f / h) * sv);
         else b = b + (1.0 / (double)h) * (double)sv;
       }
