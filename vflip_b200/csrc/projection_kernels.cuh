@@ -98,13 +98,17 @@ __global__ void face_weights3_kernel(const float* __restrict__ phi, float* __res
   const int px = ni + 1, py = nj + 1;
   auto P = [&](int a, int b, int c) { return __ldg(phi + lin3(a, b, c, px, py)); };
   const bool xi = i < ni, yj = j < nj, zk = k < nk;
+  // all seven corners loaded up front (one round of memory latency)
   const float p000 = P(i, j, k);
-  const float p010 = (yj) ? P(i, j + 1, k) : 0.0f;
-  const float p001 = (zk) ? P(i, j, k + 1) : 0.0f;
-  const float p100 = (xi) ? P(i + 1, j, k) : 0.0f;
-  if (yj && zk) uw[lin3(i, j, k, ni + 1, nj)] = clamp01(1 - frac4(p000, p010, p001, P(i, j + 1, k + 1)));
-  if (xi && zk) vw[lin3(i, j, k, ni, nj + 1)] = clamp01(1 - frac4(p000, p001, p100, P(i + 1, j, k + 1)));
-  if (xi && yj) ww[lin3(i, j, k, ni, nj)] = clamp01(1 - frac4(p000, p010, p100, P(i + 1, j + 1, k)));
+  const float p010 = yj ? P(i, j + 1, k) : 0.0f;
+  const float p001 = zk ? P(i, j, k + 1) : 0.0f;
+  const float p100 = xi ? P(i + 1, j, k) : 0.0f;
+  const float p011 = (yj && zk) ? P(i, j + 1, k + 1) : 0.0f;
+  const float p101 = (xi && zk) ? P(i + 1, j, k + 1) : 0.0f;
+  const float p110 = (xi && yj) ? P(i + 1, j + 1, k) : 0.0f;
+  if (yj && zk) uw[lin3(i, j, k, ni + 1, nj)] = clamp01(1 - frac4(p000, p010, p001, p011));
+  if (xi && zk) vw[lin3(i, j, k, ni, nj + 1)] = clamp01(1 - frac4(p000, p001, p100, p101));
+  if (xi && yj) ww[lin3(i, j, k, ni, nj)] = clamp01(1 - frac4(p000, p010, p100, p110));
 }
 
 // Inflow overwrite, Smoke_solver3D.cpp:964-980: every cell with b_desc == 1
