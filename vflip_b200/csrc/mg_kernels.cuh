@@ -615,13 +615,25 @@ __global__ void residual_restrict_kernel(const V* __restrict__ x, const V* __res
         size_t g = lin3(i, j, k, ni, nj);
         A r = ldg(b + g);
         if (!ZERO_X) {
-          if (k > 0) r = r - A(ldg(zp + g - sz)) * A(ldg(x + g - sz));
-          if (j > 0) r = r - A(ldg(yp + g - sy)) * A(ldg(x + g - sy));
-          if (i > 0) r = r - A(ldg(xp + g - 1)) * A(ldg(x + g - 1));
-          r = r - A(ldg(diag + g)) * A(ldg(x + g));
-          if (i < ni - 1) r = r - A(ldg(xp + g)) * A(ldg(x + g + 1));
-          if (j < nj - 1) r = r - A(ldg(yp + g)) * A(ldg(x + g + sy));
-          if (k < nk - 1) r = r - A(ldg(zp + g)) * A(ldg(x + g + sz));
+          // every operand loaded before the row's subtractions (neighbours
+          // outside the level at a clamped, in-range address, then unused),
+          // so a child's loads are in flight together; the subtractions keep
+          // their order and roundings
+          const bool zl = k > 0, yl = j > 0, xl = i > 0, xh = i < ni - 1, yh = j < nj - 1, zh = k < nk - 1;
+          const A czm = A(ldg(zp + (zl ? g - sz : g))), xzm = A(ldg(x + (zl ? g - sz : g)));
+          const A cym = A(ldg(yp + (yl ? g - sy : g))), xym = A(ldg(x + (yl ? g - sy : g)));
+          const A cxm = A(ldg(xp + (xl ? g - 1 : g))), xxm = A(ldg(x + (xl ? g - 1 : g)));
+          const A cd = A(ldg(diag + g)), xc = A(ldg(x + g));
+          const A cxp = A(ldg(xp + g)), xxp = A(ldg(x + (xh ? g + 1 : g)));
+          const A cyp = A(ldg(yp + g)), xyp = A(ldg(x + (yh ? g + sy : g)));
+          const A czp = A(ldg(zp + g)), xzp = A(ldg(x + (zh ? g + sz : g)));
+          if (zl) r = r - czm * xzm;
+          if (yl) r = r - cym * xym;
+          if (xl) r = r - cxm * xxm;
+          r = r - cd * xc;
+          if (xh) r = r - cxp * xxp;
+          if (yh) r = r - cyp * xyp;
+          if (zh) r = r - czp * xzp;
         }
         s = s + A(0.125) * r;
       }
