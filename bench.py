@@ -928,16 +928,23 @@ def kernel_lines(a):
         if "p2g" in what or "g2p" in what:
             part = scenes.jittered_particles(n, n, n, h, 8, rng)
             part["vel"] = rng.standard_normal((len(part), 3)).astype(np.float32)
-            rng.shuffle(part)
-            parts = T(part.view(np.uint8))
             npart = len(part)
-            if "p2g" in what:
-                ms = timed(lambda: s.particle_to_grid(n, n, n, h, parts))
-                line("p2g (hash, sort, p2g3_kernel)", ms, npart * 24 + 24 * n ** 3, particles=npart)
-            if "g2p" in what:
-                du, dv, dw = (T(x) for x in scenes.random_velocity(n, n, n, rng, scale=0.1))
-                ms = timed(lambda: s.particle_from_grid(n, n, n, h, parts, du, dv, dw))
-                line("g2p_kernel", ms, npart * 24 + 12 * n ** 3, particles=npart)
+            du, dv, dw = (T(x) for x in scenes.random_velocity(n, n, n, rng, scale=0.1))
+            # two particle orders: shuffled (the worst case for the gathers)
+            # and by cell (the order the FLIP step's reseeding leaves them in)
+            cell = np.floor(part["pos"] / h + 0.5).astype(np.int64).clip(0, n - 1)
+            by_cell = np.argsort(cell[:, 0] + n * (cell[:, 1] + n * cell[:, 2]), kind="stable")
+            shuffled = rng.permutation(npart)
+            for order, idx in (("shuffled", shuffled), ("cell order", by_cell)):
+                parts = T(np.ascontiguousarray(part[idx]).view(np.uint8))
+                if "p2g" in what:
+                    ms = timed(lambda: s.particle_to_grid(n, n, n, h, parts))
+                    line(f"p2g (hash, sort, p2g3_kernel), particles in {order}", ms, npart * 24 + 24 * n ** 3,
+                         particles=npart)
+                if "g2p" in what:
+                    ms = timed(lambda: s.particle_from_grid(n, n, n, h, parts, du, dv, dw))
+                    line(f"g2p_kernel, particles in {order}", ms, npart * 24 + 12 * n ** 3, particles=npart)
+                del parts
         if "vcycle" in what:
             vcycle_lines(a, s, timed, line)
     if "unet" in what:
