@@ -156,6 +156,11 @@ typedef struct vflip_ctx vflip_ctx;
 
 /* Fills *cfg with the reference's defaults. */
 void vflip_config_default(vflip_config* cfg);
+/* sizeof(vflip_config) in this build of the library.  vflip_config grows by
+ * fields appended at its end; code compiled against another version of this
+ * header compares it with its own sizeof(vflip_config) and must not pass its
+ * struct to the library when they differ. */
+size_t vflip_config_size(void);
 
 /* Creates a context (device buffers are allocated lazily and reused across
  * calls of the same size).  One context per host thread. */

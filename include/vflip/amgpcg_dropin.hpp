@@ -51,6 +51,11 @@ struct ThreadContext {
     if (ctx && precision == precision_setting()) return ctx;
     if (ctx) vflip_destroy(ctx);
     ctx = nullptr;
+    if (vflip_config_size() != sizeof(vflip_config)) {  // a library built from another vflip.h
+      std::fprintf(stderr, "vflip: libvflip_gpu.so was built from another vflip.h (config %zu vs %zu bytes)\n",
+                   vflip_config_size(), sizeof(vflip_config));
+      return nullptr;
+    }
     vflip_config cfg;
     vflip_config_default(&cfg);
     cfg.precision = precision_setting();

@@ -56,6 +56,7 @@ class LearnedStatsC(C.Structure):
 # name -> (restype, argtypes); mirrors include/vflip.h one for one
 SIGNATURES = {
     "vflip_config_default": (None, [C.POINTER(ConfigC)]),
+    "vflip_config_size": (C.c_size_t, []),
     "vflip_create": (_I, [C.POINTER(_P), C.POINTER(ConfigC)]),
     "vflip_destroy": (_I, [_P]),
     "vflip_last_error": (C.c_char_p, [_P]),
@@ -152,5 +153,8 @@ def load():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
+    if lib.vflip_config_size() != C.sizeof(ConfigC):
+        raise RuntimeError(f"{path} was built from another include/vflip.h: vflip_config is "
+                           f"{lib.vflip_config_size()} bytes there, {C.sizeof(ConfigC)} here")
     _lib = lib
     return lib

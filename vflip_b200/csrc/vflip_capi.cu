@@ -2415,6 +2415,8 @@ int batched_persistent(vflip_ctx* ctx, int nsys, const vflip_system* sys, double
 // ============================================================== C ABI
 extern "C" {
 
+size_t vflip_config_size(void) { return sizeof(vflip_config); }
+
 void vflip_config_default(vflip_config* cfg) {
   if (!cfg) return;
   cfg->precision = VFLIP_PREC_FP32;
