@@ -37,6 +37,11 @@ METRIC = "256³ steps/s @1e-6 residual, learned-precond vs plain MGPCG; % HBM ro
 PREC = {"fp64": 0, "fp32": 1, "mixed": 2}
 
 
+def solver_opts(a):
+    """--solver-opts "key=value,...": extra Solver keyword arguments (ints)."""
+    return {k: int(v) for k, v in (kv.split("=") for kv in a.solver_opts.split(",") if kv)}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -207,8 +212,7 @@ def run_vflip(a):
     world, rank = ranks.world, ranks.rank
     barrier, max_over_ranks = ranks.barrier, ranks.max_over_ranks
 
-    opts = {k: int(v) for k, v in (kv.split("=") for kv in a.solver_opts.split(",") if kv)}
-    solver = Solver(precision=PREC[a.precision], device=local, **opts)
+    solver = Solver(precision=PREC[a.precision], device=local, **solver_opts(a))
     params = PlumeParams(n=a.n, dt=a.dt)
     sim = PlumeSim(solver, params)
     for _ in range(a.warmup):
@@ -404,6 +408,19 @@ def learned_arm(a, sim, solver):
                        "steps": a.steps}}
 
 
+def p2g_split(solver, sim, steps=2):
+    """Device time per step of the P2G bucketing (histogram, scan, scatter,
+    bucket sort, sorted copies) and of the gathers: CUDA events around them
+    over `steps` further steps (with profiling on, the PCG loop runs from
+    the host)."""
+    solver.set_profiling(True)
+    for _ in range(steps):
+        sim.step()
+    out = {k + "_ms": solver.profile_kernels(k)[1] / steps for k in ("p2g_sort", "p2g_gather")}
+    solver.set_profiling(False)
+    return out
+
+
 def flip_arm(solver, steps, n=128, warmup=3):
     """The FLIP smoke scene at 128^3 (8 particles per cell jittered in the
     source sphere r = 0.12, sphere obstacle r = 0.15, FLIP/PIC 0.95, dt 0.01,
@@ -432,6 +449,7 @@ def flip_arm(solver, steps, n=128, warmup=3):
            "particles": sim.num_particles, "particles_at_start": np0,
            "particle_steps_per_s": sim.num_particles * steps / (ms * 1e-3),
            "pcg_iterations_mean": sum(iters) / len(iters)}
+    out["p2g_per_step"] = p2g_split(solver, sim)
     del sim
     # the same scene with density/temperature on the 256^3 grid at h/2 (RK3
     # advection, gen_heat, buoyancy on the particles) inside every step
@@ -489,6 +507,7 @@ def nested_arm(steps, device, n=128, warmup=3, ratio=4):
                "particles_main_pass": np0 + nsp0, "subdomain_particles": sim.num_sub_particles,
                "pcg_iterations_mean": sum(it) / len(it), "sub_pcg_iterations_mean": sum(sit) / len(sit),
                "precision": "mixed"}
+        out["p2g_per_step"] = p2g_split(s, sim)
         # one step from this state in both precisions
         keep = {k: getattr(sim, k).clone() for k in ("particles", "sub_particles", "tracers")}
         keep_vel = [x.clone() for x in sim.vel] + [x.clone() for x in sim.sub_vel]
@@ -909,7 +928,7 @@ def kernel_lines(a):
     h = np.float32(1.0 / n)
     rng = np.random.default_rng(0)
     T = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)  # noqa: E731
-    with Solver(precision=PREC[a.precision]) as s:
+    with Solver(precision=PREC[a.precision], **solver_opts(a)) as s:
         if "advect" in what:
             vel = []
             for q, sh in enumerate(scenes.face_shapes(n, n, n)):

@@ -140,6 +140,13 @@ typedef struct {
    * (64^3); -1 = never.  The fine level's last sweep (which also forms z.r)
    * always marches.  Same bits. */
   int tile_sweep_max_cells;
+  /* P2G gather on the main grid: 0 (default) = automatic, as 2; 1 = every
+   * node gathers from global memory; 2 = tiled: a CTA stages the particles
+   * of an 8 x 8 x 8 tile of face nodes and its one-cell ring in shared
+   * memory (in chunks where they do not fit at once), one CTA per SM, and
+   * its threads gather from there, two nodes each; 3 = the same with
+   * 8 x 8 x 4 tiles, two CTAs per SM.  Same bits. */
+  int p2g_kernel;
 } vflip_config;
 
 typedef struct {
@@ -541,7 +548,9 @@ int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const vo
  * launches (one field; a pair of fields on one backtrace); and, as spans of
  * several launches, each V-cycle of the PCG (VCYCLE) and its part below the
  * fine level (COARSE: the levels >= 1, from after the fine restriction to
- * the fine prolongation).  vflip_profile_kernels synchronises the stream and returns the
+ * the fine prolongation); P2G_SORT spans a P2G's bucketing (histogram,
+ * scan, scatter, bucket sort, sorted copies), P2G_GATHER its gathers.
+ * vflip_profile_kernels synchronises the stream and returns the
  * number of timed launches of one kind and their summed device time;
  * vflip_profile_sweeps returns the fine sweeps' figures and the fine level's
  * cell count, then starts a new count for every kind.  Enabling (again)
@@ -553,6 +562,8 @@ int vflip_reorder_flip(vflip_ctx* ctx, int ni, int nj, int nk, float h, const vo
 #define VFLIP_PROF_ADVECT_PAIR 4
 #define VFLIP_PROF_VCYCLE 5
 #define VFLIP_PROF_COARSE 6
+#define VFLIP_PROF_P2G_SORT 7
+#define VFLIP_PROF_P2G_GATHER 8
 int vflip_set_profiling(vflip_ctx* ctx, int enable);
 int vflip_profile_sweeps(vflip_ctx* ctx, int* launches, double* total_ms, double* cells);
 int vflip_profile_kernels(vflip_ctx* ctx, int kind, int* launches, double* total_ms);

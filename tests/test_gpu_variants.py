@@ -7,7 +7,8 @@
   * the two-CTA register-carry sweep of rows <= 128 cells gives the plain
     fused kernel's bits;
   * the projection's PCG, which reads the FP32 copies of the couplings it
-    assembled, gives the bits of the same solve on the FP64 operator."""
+    assembled, gives the bits of the same solve on the FP64 operator;
+  * the tiled P2G gives the per-node global gather's bits."""
 import numpy as np
 import pytest
 
@@ -166,3 +167,64 @@ def test_narrow_carry_sweep_matches_plain_kernel(prec, dims):
     (za, xa, ia), (zb, xb, ib) = out
     assert torch.equal(za, zb)
     assert ia == ib
+
+
+def _p2g_cases():
+    rng = np.random.default_rng(23)
+    out = []
+    # 8 particles per cell, shuffled: every tile stages its buckets
+    ni, nj, nk = 41, 35, 30
+    h = np.float32(1.0 / ni)
+    p = scenes.jittered_particles(ni, nj, nk, h, 8, rng)
+    p["vel"] = rng.standard_normal((len(p), 3)).astype(np.float32)
+    rng.shuffle(p)
+    out.append(("jittered", (ni, nj, nk), h, p, (0, 1, 2)))
+    # a blob of 40000 particles in a few cells: its tiles hold more than fit
+    # in shared memory and stage them in chunks; some particles outside
+    ni, nj, nk = 24, 20, 16
+    h = np.float32(0.05)
+    p = scenes.random_particles(ni, nj, nk, h, 60000, rng, margin=0.0)
+    p["pos"][:40000] = (np.array([9.0, 7.0, 5.0]) * h + rng.uniform(-1.2, 1.2, (40000, 3)) * h).astype(np.float32)
+    p["pos"][40000:40100] = -3.0
+    rng.shuffle(p)
+    out.append(("dense blob", (ni, nj, nk), h, p, (0, 1, 2)))
+    # non-finite velocities (NaN sums wherever the window holds one)
+    ni, nj, nk = 30, 26, 22
+    h = np.float32(1.0 / 32)
+    p = scenes.jittered_particles(ni, nj, nk, h, 4, rng)
+    p["vel"] = rng.standard_normal((len(p), 3)).astype(np.float32)
+    bad = rng.choice(len(p), 40, replace=False)
+    p["vel"][bad[:20], 0] = np.nan
+    p["vel"][bad[20:], 2] = np.inf
+    out.append(("non-finite", (ni, nj, nk), h, p, (0, 1, 2)))
+    # thin grids, one component, and the three spacings the tents take:
+    # not a power of two (above), a power of two <= 1, and one above 1
+    for dims, comps, hh in (((1, 9, 70), (0, 1, 2), 1.0 / 16), ((70, 1, 3), (1,), 1.0 / 16),
+                            ((17, 16, 8), (2,), 1.0 / 16), ((12, 10, 9), (0, 1, 2), 2.0)):
+        h = np.float32(hh)
+        p = scenes.jittered_particles(*dims, h, 6, rng)
+        p["vel"] = rng.standard_normal((len(p), 3)).astype(np.float32)
+        rng.shuffle(p)
+        out.append((f"{dims} {comps}", dims, h, p, comps))
+    return out
+
+
+def test_tiled_p2g_matches_global_gather():
+    """The tiled P2G (8 x 8 x 8 and 8 x 8 x 4 node tiles, particles staged
+    in shared memory, every window particle added) gives the per-node global
+    gather's bits (p2g_kernel 1): with one chunk per tile, with tiles staged in
+    several chunks, with non-finite velocities, on thin grids and for
+    single components."""
+    from vflip_b200.solver import Solver
+
+    for name, (ni, nj, nk), h, p, comps in _p2g_cases():
+        res = []
+        for kern in (1, 0, 2, 3):
+            with Solver(precision=1, p2g_kernel=kern) as s:
+                outs = s.particle_to_grid(ni, nj, nk, h, t(p.view(np.uint8)), components=comps)
+                res.append({c: (outs[c][0].view(torch.int32).clone(), outs[c][1].view(torch.int32).clone())
+                            for c in comps})
+        for r in res[1:]:
+            for c in comps:
+                assert torch.equal(res[0][c][0], r[c][0]), (name, c)
+                assert torch.equal(res[0][c][1], r[c][1]), (name, c)

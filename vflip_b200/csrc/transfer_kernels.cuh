@@ -447,12 +447,11 @@ __global__ void gather_sorted_kernel(const ParticleRec* __restrict__ p, const in
   }
 }
 
-__device__ __forceinline__ float tent(float r) {  // SmokeSolver3D::H, Smoke_solver3D.h:217-223
-  float res = 0.0f;
-  if (r >= -1.0f && r < 0.0f) res = 1.0f + r;
-  if (r >= 0.0f && r < 1.0f) res = 1.0f - r;
-  return res;
-}
+// SmokeSolver3D::H, Smoke_solver3D.h:217-223: 1 + r on [-1, 0), 1 - r on
+// [0, 1), else 0 (NaN included).  Written as max(1 - |r|, 0): on [-1, 0)
+// 1 - (-r) is the same rounded sum as 1 + r; for |r| >= 1 (and r = +-inf)
+// 1 - |r| <= 0 and the maximum is +0; fmaxf returns 0 for a NaN r.
+__device__ __forceinline__ float tent(float r) { return fmaxf(1.0f - fabsf(r), 0.0f); }
 
 // particle_to_grid, Smoke_solver3D.cpp:1451-1510, for the three velocity
 // components in one pass: at each face node, field = sum(w v)/sum(w),
@@ -487,6 +486,177 @@ __host__ __device__ inline size_t p2g_part_size(int part, int ni, int nj, int nk
   return (Z - mk) * X * Y + mk * (Y - mj) * X + mk * mj * (X - mi);
 }
 
+// The face-node triple (i, j, k) of the u, v, w grids during a gather:
+// node coordinates, which components it holds, and the running sums.
+struct P2gNode {
+  float xi, xh, yj, yh, zk, zh;
+  bool act0, act1, act2;
+  float tw[3], tv[3];
+};
+
+__device__ __forceinline__ P2gNode p2g_node(int i, int j, int k, int ni, int nj, int nk, float h, bool hu, bool hv,
+                                            bool hw) {
+  P2gNode n;
+  n.act0 = hu && j < nj && k < nk;
+  n.act1 = hv && i < ni && k < nk;
+  n.act2 = hw && i < ni && j < nj;
+  // node positions: the component's own axis sits half a cell lower
+  n.xi = (float)((double)(float)i * (double)h);
+  n.xh = (float)(((double)(float)i - 0.5) * (double)h);
+  n.yj = (float)((double)(float)j * (double)h);
+  n.yh = (float)(((double)(float)j - 0.5) * (double)h);
+  n.zk = (float)((double)(float)k * (double)h);
+  n.zh = (float)(((double)(float)k - 0.5) * (double)h);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    n.tw[c] = 1e-5f;
+    n.tv[c] = 0.0f;
+  }
+  return n;
+}
+
+// One particle's step of the gather at node n: the particle at (px, py, pz)
+// (grid-relative), `fin` when its velocity is finite; `vel()` fetches the
+// velocity, called only when some component takes the particle.  The nodes
+// share offsets pairwise (x of v and w, y of u and w, z of u and v): six
+// one-dimensional tents serve the three weights.
+template <typename VelF>
+__device__ __forceinline__ void p2g_visit(P2gNode& n, float px, float py, float pz, bool fin, float hk, float ihk,
+                                          float rk, VelF vel) {
+  const float dxu = px - n.xh, dxv = px - n.xi;
+  const float dyu = py - n.yj, dyv = py - n.yh;
+  const float dzu = pz - n.zk, dzw = pz - n.zh;
+  const bool ox = fabsf(dxu) >= rk, oxv = fabsf(dxv) >= rk, oy = fabsf(dyu) >= rk, oyv = fabsf(dyv) >= rk;
+  const bool oz = fabsf(dzu) >= rk, ozw = fabsf(dzw) >= rk;
+  const bool ok0 = n.act0 && !(fin && (ox || oy || oz));
+  const bool ok1 = n.act1 && !(fin && (oxv || oyv || oz));
+  const bool ok2 = n.act2 && !(fin && (oxv || oy || ozw));
+  if (!(ok0 || ok1 || ok2)) return;
+  const float txu = tent(fdiv_h(dxu, hk, ihk)), txv = tent(fdiv_h(dxv, hk, ihk));
+  const float tyu = tent(fdiv_h(dyu, hk, ihk)), tyv = tent(fdiv_h(dyv, hk, ihk));
+  const float tzu = tent(fdiv_h(dzu, hk, ihk)), tzw = tent(fdiv_h(dzw, hk, ihk));
+  const float3 vv = vel();
+  if (ok0) {
+    const float wgt = txu * tyu * tzu;
+    n.tw[0] = n.tw[0] + wgt;
+    n.tv[0] = n.tv[0] + wgt * vv.x;
+  }
+  if (ok1) {
+    const float wgt = txv * tyv * tzu;
+    n.tw[1] = n.tw[1] + wgt;
+    n.tv[1] = n.tv[1] + wgt * vv.y;
+  }
+  if (ok2) {
+    const float wgt = txv * tyu * tzw;
+    n.tw[2] = n.tw[2] + wgt;
+    n.tv[2] = n.tv[2] + wgt * vv.z;
+  }
+}
+
+// The tent of an offset d from a node, in units of h.  M = 0: d / h; M = 1:
+// h a power of two, d * inv_h (exact); M = 2: h a power of two <= 1 and the
+// positions and node coordinates already multiplied by inv_h: scaling by a
+// power of two >= 1 is exact and commutes with the rounded difference, so d
+// is the scaled offset itself (an overflow to inf gives tent 0 either way).
+template <int M>
+__device__ __forceinline__ float p2g_tent(float d, float h, float inv_h) {
+  return tent(M == 0 ? d / h : (M == 1 ? d * inv_h : d));
+}
+
+// One particle of node n's window added as the reference's loop adds it,
+// with no reach test: a particle out of reach has weight exactly 0 and adds
+// +0 to sum(w) and +-0 to sum(w v) (which never holds -0), so the sums are
+// those of p2g_visit; a non-finite velocity makes sum(w v) NaN in both.
+// Inactive components are summed and not stored.
+template <int M>
+__device__ __forceinline__ void p2g_add(P2gNode& n, float px, float py, float pz, float vx, float vy, float vz,
+                                        float h, float inv_h) {
+  const float txu = p2g_tent<M>(px - n.xh, h, inv_h), txv = p2g_tent<M>(px - n.xi, h, inv_h);
+  const float tyu = p2g_tent<M>(py - n.yj, h, inv_h), tyv = p2g_tent<M>(py - n.yh, h, inv_h);
+  const float tzu = p2g_tent<M>(pz - n.zk, h, inv_h), tzw = p2g_tent<M>(pz - n.zh, h, inv_h);
+  const float w0 = txu * tyu * tzu, w1 = txv * tyv * tzu, w2 = txv * tyu * tzw;
+  n.tw[0] = n.tw[0] + w0;
+  n.tv[0] = n.tv[0] + w0 * vx;
+  n.tw[1] = n.tw[1] + w1;
+  n.tv[1] = n.tv[1] + w1 * vy;
+  n.tw[2] = n.tw[2] + w2;
+  n.tv[2] = n.tv[2] + w2 * vz;
+}
+
+// p2g_add for the nodes (i, j, k) and (i, j, k + 1) at once: they share the
+// x and y tents and the products tx * ty, so each weight is the same
+// product as p2g_add forms, with the node's own z tent.
+template <int M>
+__device__ __forceinline__ void p2g_add2(P2gNode& a, P2gNode& b, float px, float py, float pz, float vx, float vy,
+                                         float vz, float h, float inv_h) {
+  const float txu = p2g_tent<M>(px - a.xh, h, inv_h), txv = p2g_tent<M>(px - a.xi, h, inv_h);
+  const float tyu = p2g_tent<M>(py - a.yj, h, inv_h), tyv = p2g_tent<M>(py - a.yh, h, inv_h);
+  const float uu = txu * tyu, vv = txv * tyv, ww = txv * tyu;
+  const float tzua = p2g_tent<M>(pz - a.zk, h, inv_h), tzwa = p2g_tent<M>(pz - a.zh, h, inv_h);
+  const float tzub = p2g_tent<M>(pz - b.zk, h, inv_h), tzwb = p2g_tent<M>(pz - b.zh, h, inv_h);
+  const float a0 = uu * tzua, a1 = vv * tzua, a2 = ww * tzwa;
+  const float b0 = uu * tzub, b1 = vv * tzub, b2 = ww * tzwb;
+  a.tw[0] = a.tw[0] + a0;
+  a.tv[0] = a.tv[0] + a0 * vx;
+  a.tw[1] = a.tw[1] + a1;
+  a.tv[1] = a.tv[1] + a1 * vy;
+  a.tw[2] = a.tw[2] + a2;
+  a.tv[2] = a.tv[2] + a2 * vz;
+  b.tw[0] = b.tw[0] + b0;
+  b.tv[0] = b.tv[0] + b0 * vx;
+  b.tw[1] = b.tw[1] + b1;
+  b.tv[1] = b.tv[1] + b1 * vy;
+  b.tw[2] = b.tw[2] + b2;
+  b.tv[2] = b.tv[2] + b2 * vz;
+}
+
+// field = sum(w v) / sum(w), coef = sum(w) at the components node n holds
+__device__ __forceinline__ void p2g_store(const P2gNode& n, int i, int j, int k, int ni, int nj, float* fu,
+                                          float* cu, float* fv, float* cv, float* fw, float* cw) {
+  if (n.act0) {
+    const size_t o = (size_t)i + (size_t)(ni + 1) * ((size_t)j + (size_t)nj * k);
+    cu[o] = n.tw[0];
+    fu[o] = n.tv[0] / n.tw[0];
+  }
+  if (n.act1) {
+    const size_t o = (size_t)i + (size_t)ni * ((size_t)j + (size_t)(nj + 1) * k);
+    cv[o] = n.tw[1];
+    fv[o] = n.tv[1] / n.tw[1];
+  }
+  if (n.act2) {
+    const size_t o = (size_t)i + (size_t)ni * ((size_t)j + (size_t)nj * k);
+    cw[o] = n.tw[2];
+    fw[o] = n.tv[2] / n.tw[2];
+  }
+}
+
+// The gather of node n from the global sorted arrays: the buckets i-l..i+l
+// of each row (ck, cj) of the (2l+1)^2 neighbouring rows, rows in order of
+// k then j, each row's buckets one consecutive run of particles in the
+// sorted order, visited in that order.
+__device__ __forceinline__ void p2g_gather_global(P2gNode& n, int i, int j, int k, int l, int ni, int nj, int nk,
+                                                  float hk, float ihk, float rk, const int* __restrict__ start,
+                                                  const float4* __restrict__ spos,
+                                                  const float4* __restrict__ svel) {
+  for (int dk = -l; dk <= l; ++dk) {
+    const int ck = k + dk;
+    if (ck < 0 || ck >= nk) continue;
+    for (int dj = -l; dj <= l; ++dj) {
+      const int cj = j + dj;
+      if (cj < 0 || cj >= nj) continue;
+      const int row = (ck * nj + cj) * ni;
+      const int b = __ldg(start + row + max(i - l, 0)), en = __ldg(start + row + min(i + l, ni - 1) + 1);
+      for (int q = b; q < en; ++q) {
+        const float4 pp = __ldg(spos + q);
+        p2g_visit(n, pp.x, pp.y, pp.z, pp.w != 0.0f, hk, ihk, rk, [&] {
+          const float4 vv = __ldg(svel + q);
+          return make_float3(vv.x, vv.y, vv.z);
+        });
+      }
+    }
+  }
+}
+
 template <bool SUB>
 __global__ void p2g3_kernel(const int* __restrict__ start, const float4* __restrict__ spos,
                             const float4* __restrict__ svel, float* __restrict__ fu, float* __restrict__ cu,
@@ -519,14 +689,8 @@ __global__ void p2g3_kernel(const int* __restrict__ start, const float4* __restr
       j += 5;
       k += 5;
     }
-    const bool act0 = fu != nullptr && j < nj && k < nk;
-    const bool act1 = fv != nullptr && i < ni && k < nk;
-    const bool act2 = fw != nullptr && i < ni && j < nj;
-    if (!(act0 || act1 || act2)) continue;
-    // node positions: the component's own axis sits half a cell lower
-    const float xi = (float)((double)(float)i * (double)h), xh = (float)(((double)(float)i - 0.5) * (double)h);
-    const float yj = (float)((double)(float)j * (double)h), yh = (float)(((double)(float)j - 0.5) * (double)h);
-    const float zk = (float)((double)(float)k * (double)h), zh = (float)(((double)(float)k - 0.5) * (double)h);
+    P2gNode nd = p2g_node(i, j, k, ni, nj, nk, h, fu != nullptr, fv != nullptr, fw != nullptr);
+    if (!(nd.act0 || nd.act1 || nd.act2)) continue;
     int l = 1;
     float hk = h, ihk = inv_h, rk = reach;
     if (SUB) {
@@ -538,69 +702,247 @@ __global__ void p2g3_kernel(const int* __restrict__ start, const float4* __restr
         rk = hk * 1.0001f;
       }
     }
-    float tw[3] = {1e-5f, 1e-5f, 1e-5f}, tv[3] = {0.0f, 0.0f, 0.0f};
-    for (int dk = -l; dk <= l; ++dk) {
-      const int ck = k + dk;
-      if (ck < 0 || ck >= nk) continue;
-      for (int dj = -l; dj <= l; ++dj) {
-        const int cj = j + dj;
-        if (cj < 0 || cj >= nj) continue;
-        // the buckets i-l .. i+l of this row are consecutive in the sorted
-        // order: one run of particles, visited in bucket order as before
-        const int row = (ck * nj + cj) * ni;
-        const int b = __ldg(start + row + max(i - l, 0)), en = __ldg(start + row + min(i + l, ni - 1) + 1);
-        for (int q = b; q < en; ++q) {
-          const float4 pp = __ldg(spos + q);
-          // the nodes share offsets pairwise: x of v and w, y of u and w,
-          // z of u and v - six one-dimensional tents serve the three weights
-          const float dxu = pp.x - xh, dxv = pp.x - xi;
-          const float dyu = pp.y - yj, dyv = pp.y - yh;
-          const float dzu = pp.z - zk, dzw = pp.z - zh;
-          const bool fin = pp.w != 0.0f;
-          const bool ox = fabsf(dxu) >= rk, oxv = fabsf(dxv) >= rk, oy = fabsf(dyu) >= rk, oyv = fabsf(dyv) >= rk;
-          const bool oz = fabsf(dzu) >= rk, ozw = fabsf(dzw) >= rk;
-          const bool ok0 = act0 && !(fin && (ox || oy || oz));
-          const bool ok1 = act1 && !(fin && (oxv || oyv || oz));
-          const bool ok2 = act2 && !(fin && (oxv || oy || ozw));
-          if (!(ok0 || ok1 || ok2)) continue;
-          const float txu = tent(fdiv_h(dxu, hk, ihk)), txv = tent(fdiv_h(dxv, hk, ihk));
-          const float tyu = tent(fdiv_h(dyu, hk, ihk)), tyv = tent(fdiv_h(dyv, hk, ihk));
-          const float tzu = tent(fdiv_h(dzu, hk, ihk)), tzw = tent(fdiv_h(dzw, hk, ihk));
-          const float4 vv = __ldg(svel + q);
-          if (ok0) {
-            const float wgt = txu * tyu * tzu;
-            tw[0] = tw[0] + wgt;
-            tv[0] = tv[0] + wgt * vv.x;
+    p2g_gather_global(nd, i, j, k, l, ni, nj, nk, hk, ihk, rk, start, spos, svel);
+    p2g_store(nd, i, j, k, ni, nj, fu, cu, fv, cv, fw, cw);
+  }
+}
+
+// The tiled gather (main grid, every node index): a CTA owns an 8 x 8 x TZ
+// tile of face-node indices (i, j, k), two nodes (k, k + 1) per thread, and
+// stages the particles its nodes gather from - the buckets of the tile's
+// cells and a one-cell ring, each row of them one consecutive run of the
+// sorted order - in shared memory, positions and velocities as six float
+// arrays; the threads then gather from there.  In the global form each
+// thread streams its own runs through L1, the 32 threads of a warp reading
+// 32 runs about a bucket apart; here the loads are coalesced once per tile,
+// and a thread's two nodes share the x run and the x and y tents of the
+// planes both windows hold.  A region holding more than `cap` particles is
+// staged in chunks of `cap`: the staged sequence is the row runs in row
+// order and a node's window is a sub-run of each of its rows, taken in that
+// order, so chunk by chunk each node adds the part of its window the chunk
+// holds and its visiting order is unchanged.  Every particle of a window is
+// added (p2g_add: no reach test, no divergence between the threads of a
+// warp), which gives p2g_visit's sums bit for bit.
+// Tile shapes: TZ = 8 node layers (one CTA of 256 threads per SM, a
+// 10 x 10 x 10-cell region) or TZ = 4 (two CTAs of 128 threads per SM, each
+// half the shared memory, so that one CTA's staging overlaps the other's
+// gathers; a 10 x 10 x 6-cell region).
+constexpr int kP2gTX = 8, kP2gTY = 8;
+constexpr int kP2gRX = kP2gTX + 2;  // bucket columns of the staged region
+constexpr int kP2gBatch = 4;        // particles a thread loads before staging them
+template <int TZ>
+struct P2gTile {
+  static constexpr int threads = kP2gTX * kP2gTY * (TZ / 2);  // two nodes (k, k + 1) per thread
+  static constexpr int rows = (kP2gTY + 2) * (TZ + 2);        // bucket rows of the staged region
+  static constexpr int rows_pad = rows < 64 ? 64 : 128;       // the row scan's width
+  static constexpr int fixed_ints = rows * (kP2gRX + 1) + 2 * rows_pad;
+  static constexpr int ctas_per_sm = TZ == 8 ? 1 : 2;
+  static_assert(rows < rows_pad && fixed_ints % 4 == 0 && threads >= rows_pad, "p2g tile tables");
+};
+
+// shared-memory slot of staged particle s: one pad word per 32 spreads the
+// reads of neighbouring nodes, about a bucket apart, over the banks
+__host__ __device__ inline int p2g_slot(int s) { return s + (s >> 5); }
+
+// particles a CTA with `smem_bytes` of dynamic shared memory stages
+template <int TZ>
+__host__ __device__ inline int p2g_tile_cap(size_t smem_bytes) {
+  const size_t fixed = sizeof(int) * (size_t)P2gTile<TZ>::fixed_ints;
+  if (smem_bytes <= fixed + 6 * sizeof(float) * 2) return 0;
+  const long a = (long)((smem_bytes - fixed) / (6 * sizeof(float)));  // floats per array
+  long cap = (a - 1) * 32 / 33;
+  while (cap > 0 && p2g_slot((int)cap - 1) + 1 > a) --cap;
+  return (int)cap;
+}
+
+// node (i, j, k)'s window in row (ck, cj) of the staged region, clipped to
+// the chunk [c0, c1) and made chunk-relative
+__device__ __forceinline__ int2 p2g_window(const int* cs, int row, int i, int ni, int clo, int c0, int c1) {
+  const int* c = cs + row * (kP2gRX + 1);
+  return make_int2(max(c[max(i - 1, 0) - clo], c0) - c0, min(c[min(i + 1, ni - 1) + 1 - clo], c1) - c0);
+}
+
+template <int M>
+__device__ __forceinline__ void p2g_run1(P2gNode& n, int b, int e, const float* px, const float* py,
+                                         const float* pz, const float* vx, const float* vy, const float* vz,
+                                         float h, float inv_h) {
+#pragma unroll 2
+  for (int s = b; s < e; ++s) {
+    const int P = p2g_slot(s);
+    p2g_add<M>(n, px[P], py[P], pz[P], vx[P], vy[P], vz[P], h, inv_h);
+  }
+}
+
+template <int M>
+__device__ __forceinline__ void p2g_run2(P2gNode& n0, P2gNode& n1, int b, int e, const float* px, const float* py,
+                                         const float* pz, const float* vx, const float* vy, const float* vz,
+                                         float h, float inv_h) {
+#pragma unroll 2
+  for (int s = b; s < e; ++s) {
+    const int P = p2g_slot(s);
+    p2g_add2<M>(n0, n1, px[P], py[P], pz[P], vx[P], vy[P], vz[P], h, inv_h);
+  }
+}
+
+// One chunk's gathers of the thread's nodes (i, j, k) and (i, j, k + 1):
+// planes k - 1 .. k + 2 in order, rows j - 1 .. j + 1 in each; planes k
+// and k + 1 belong to both windows (the same x run), k - 1 to the first
+// node's only, k + 2 to the second's.
+template <int M>
+__device__ __forceinline__ void p2g_chunk2(P2gNode& n0, P2gNode& n1, bool on0, bool on1, int i, int j, int k,
+                                           int ni, int nj, int nk, int clo, int cjlo, int cklo, int nry,
+                                           const int* cs, int c0, int c1, const float* px, const float* py,
+                                           const float* pz, const float* vx, const float* vy, const float* vz,
+                                           float h, float inv_h) {
+  for (int dk = -1; dk <= 2; ++dk) {
+    const int ck = k + dk;
+    const bool a0 = on0 && dk <= 1, a1 = on1 && dk >= 0;
+    if (ck < 0 || ck >= nk || !(a0 || a1)) continue;
+    for (int dj = -1; dj <= 1; ++dj) {
+      const int cj = j + dj;
+      if (cj < 0 || cj >= nj) continue;
+      const int2 w = p2g_window(cs, (ck - cklo) * nry + (cj - cjlo), i, ni, clo, c0, c1);
+      if (a0 && a1)
+        p2g_run2<M>(n0, n1, w.x, w.y, px, py, pz, vx, vy, vz, h, inv_h);
+      else if (a0)
+        p2g_run1<M>(n0, w.x, w.y, px, py, pz, vx, vy, vz, h, inv_h);
+      else
+        p2g_run1<M>(n1, w.x, w.y, px, py, pz, vx, vy, vz, h, inv_h);
+    }
+  }
+}
+
+template <int TZ>
+__global__ void __launch_bounds__(P2gTile<TZ>::threads, P2gTile<TZ>::ctas_per_sm)
+    p2g3_tile_kernel(const int* __restrict__ start, const float4* __restrict__ spos,
+                     const float4* __restrict__ svel, float* __restrict__ fu, float* __restrict__ cu,
+                     float* __restrict__ fv, float* __restrict__ cv, float* __restrict__ fw, float* __restrict__ cw,
+                     int ni, int nj, int nk, float h, float inv_h, int ntx, int nty, int cap) {
+  using T = P2gTile<TZ>;
+  constexpr int R = T::rows_pad / 32;  // rows per lane of the scan
+  extern __shared__ __align__(16) int psm[];
+  int* cs = psm;                                   // [row][c]: staged index of bucket clo + c's first particle
+  int* rbeg = cs + T::rows * (kP2gRX + 1);         // [row]: sorted index of the row run's first particle
+  int* roff = rbeg + T::rows_pad;                  // [row]: staged index of the row run's first particle
+  const int A = p2g_slot(cap - 1) + 1;
+  float* px = reinterpret_cast<float*>(psm + T::fixed_ints);
+  float *py = px + A, *pz = py + A, *vx = pz + A, *vy = vx + A, *vz = vy + A;
+  const int tid = threadIdx.x, t = blockIdx.x;
+  const int i0 = (t % ntx) * kP2gTX, j0 = ((t / ntx) % nty) * kP2gTY, k0 = (t / (ntx * nty)) * TZ;
+  // the staged cells: [clo, chi] x [cjlo, cjhi] x [cklo, ckhi]
+  const int clo = max(i0 - 1, 0), chi = min(i0 + kP2gTX, ni - 1), nrx = chi - clo + 1;
+  const int cjlo = max(j0 - 1, 0), nry = min(j0 + kP2gTY, nj - 1) - cjlo + 1;
+  const int cklo = max(k0 - 1, 0), nrz = min(k0 + TZ, nk - 1) - cklo + 1;
+  const int nrows = nry * nrz;
+  auto row_base = [&](int r) { return ((cklo + r / nry) * nj + cjlo + r % nry) * ni; };
+  // the region's bucket starts in one round of loads, then each row's run
+  for (int e = tid; e < nrows * (nrx + 1); e += T::threads) {
+    const int r = e / (nrx + 1), c = e - r * (nrx + 1);
+    cs[r * (kP2gRX + 1) + c] = __ldg(start + row_base(r) + clo + c);
+  }
+  __syncthreads();
+  if (tid < T::rows_pad) {
+    int len = 0;
+    if (tid < nrows) {
+      const int b = cs[tid * (kP2gRX + 1)];
+      rbeg[tid] = b;
+      len = cs[tid * (kP2gRX + 1) + nrx] - b;
+    }
+    roff[tid] = len;
+  }
+  __syncthreads();
+  if (tid < 32) {  // exclusive scan of the run lengths, R rows per lane
+    int v[R], x = 0;
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      v[q] = roff[R * tid + q];
+      x += v[q];
+    }
+    const int own = x;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (tid >= o) x += y;
+    }
+    int pre = x - own;
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      roff[R * tid + q] = pre;
+      pre += v[q];
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < nrows * (nrx + 1); e += T::threads) {
+    const int r = e / (nrx + 1), c = e - r * (nrx + 1);
+    cs[r * (kP2gRX + 1) + c] += roff[r] - rbeg[r];
+  }
+  const int total = roff[nrows];  // the rows past nrows have length 0
+  // tent mode (p2g_tent): 2 scales positions and node coordinates by inv_h
+  const int mode = inv_h == 0.0f ? 0 : (inv_h >= 1.0f ? 2 : 1);
+  const float sc = mode == 2 ? inv_h : 1.0f;
+  const int i = i0 + tid % kP2gTX, j = j0 + (tid / kP2gTX) % kP2gTY, k = k0 + 2 * (tid / (kP2gTX * kP2gTY));
+  const bool on0 = i <= ni && j <= nj && k <= nk, on1 = on0 && k + 1 <= nk;
+  P2gNode n0 = p2g_node(i, j, k, ni, nj, nk, h, fu != nullptr, fv != nullptr, fw != nullptr);
+  P2gNode n1 = p2g_node(i, j, k + 1, ni, nj, nk, h, fu != nullptr, fv != nullptr, fw != nullptr);
+  if (mode == 2) {
+    for (P2gNode* n : {&n0, &n1}) {
+      n->xi *= sc;
+      n->xh *= sc;
+      n->yj *= sc;
+      n->yh *= sc;
+      n->zk *= sc;
+      n->zh *= sc;
+    }
+  }
+  // the staged sequence is the row runs in row order (k, then j), and a
+  // node's window is a sub-run of each of its rows, taken in that order:
+  // chunk by chunk, each node adds the part of its window the chunk holds
+  for (int c0 = 0; c0 < total; c0 += cap) {
+    const int c1 = min(c0 + cap, total);
+    __syncthreads();  // the previous chunk is consumed (and cs is written)
+    // each warp copies whole rows, kP2gBatch steps of 32 particles with
+    // their loads in flight before the stores
+    for (int r = tid >> 5; r < nrows; r += T::threads / 32) {
+      const int lo = max(roff[r], c0), hi = min(roff[r + 1], c1);
+      const int g = rbeg[r] - roff[r];
+      for (int s0 = lo + (tid & 31); s0 < hi; s0 += 32 * kP2gBatch) {
+        float4 a[kP2gBatch], v[kP2gBatch];
+#pragma unroll
+        for (int q = 0; q < kP2gBatch; ++q) {
+          const int s = s0 + 32 * q;
+          if (s < hi) {
+            a[q] = __ldg(spos + g + s);
+            v[q] = __ldg(svel + g + s);
           }
-          if (ok1) {
-            const float wgt = txv * tyv * tzu;
-            tw[1] = tw[1] + wgt;
-            tv[1] = tv[1] + wgt * vv.y;
-          }
-          if (ok2) {
-            const float wgt = txv * tyu * tzw;
-            tw[2] = tw[2] + wgt;
-            tv[2] = tv[2] + wgt * vv.z;
+        }
+#pragma unroll
+        for (int q = 0; q < kP2gBatch; ++q) {
+          const int s = s0 + 32 * q;
+          if (s < hi) {
+            const int P = p2g_slot(s - c0);
+            px[P] = a[q].x * sc;
+            py[P] = a[q].y * sc;
+            pz[P] = a[q].z * sc;
+            vx[P] = v[q].x;
+            vy[P] = v[q].y;
+            vz[P] = v[q].z;
           }
         }
       }
     }
-    if (act0) {
-      const size_t o = (size_t)i + (size_t)(ni + 1) * ((size_t)j + (size_t)nj * k);
-      cu[o] = tw[0];
-      fu[o] = tv[0] / tw[0];
-    }
-    if (act1) {
-      const size_t o = (size_t)i + (size_t)ni * ((size_t)j + (size_t)(nj + 1) * k);
-      cv[o] = tw[1];
-      fv[o] = tv[1] / tw[1];
-    }
-    if (act2) {
-      const size_t o = (size_t)i + (size_t)ni * ((size_t)j + (size_t)nj * k);
-      cw[o] = tw[2];
-      fw[o] = tv[2] / tw[2];
-    }
+    __syncthreads();
+    if (!on0) continue;
+    if (mode == 2)
+      p2g_chunk2<2>(n0, n1, on0, on1, i, j, k, ni, nj, nk, clo, cjlo, cklo, nry, cs, c0, c1, px, py, pz, vx, vy, vz,
+                    h, inv_h);
+    else if (mode == 1)
+      p2g_chunk2<1>(n0, n1, on0, on1, i, j, k, ni, nj, nk, clo, cjlo, cklo, nry, cs, c0, c1, px, py, pz, vx, vy, vz,
+                    h, inv_h);
+    else
+      p2g_chunk2<0>(n0, n1, on0, on1, i, j, k, ni, nj, nk, clo, cjlo, cklo, nry, cs, c0, c1, px, py, pz, vx, vy, vz,
+                    h, inv_h);
   }
+  if (on0) p2g_store(n0, i, j, k, ni, nj, fu, cu, fv, cv, fw, cw);
+  if (on1) p2g_store(n1, i, j, k + 1, ni, nj, fu, cu, fv, cv, fw, cw);
 }
 
 // particle_from_grid, Smoke_solver3D.cpp:1398-1406 (flip_ratio == 1:

@@ -2441,6 +2441,7 @@ void vflip_config_default(vflip_config* cfg) {
   cfg->batch_ctas_per_sm = 0;
   cfg->coarse_tail = 0;
   cfg->tile_sweep_max_cells = 0;
+  cfg->p2g_kernel = 0;
 }
 
 int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
@@ -2474,7 +2475,8 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
       ctx->cfg.coarsest_solver < 0 || ctx->cfg.coarsest_solver > 2 || ctx->cfg.spmv_kernel < 0 ||
       ctx->cfg.spmv_kernel > 1 ||
       ctx->cfg.pcg_loop < 0 || ctx->cfg.pcg_loop > 1 || ctx->cfg.pcg_vectors < 0 || ctx->cfg.pcg_vectors > 1 || ctx->cfg.batch_chunk < 0 || ctx->cfg.batch_ctas_per_sm < 0 ||
-      ctx->cfg.coarse_tail < 0 || ctx->cfg.coarse_tail > 1 || ctx->cfg.tile_sweep_max_cells < -1)
+      ctx->cfg.coarse_tail < 0 || ctx->cfg.coarse_tail > 1 || ctx->cfg.tile_sweep_max_cells < -1 ||
+      ctx->cfg.p2g_kernel < 0 || ctx->cfg.p2g_kernel > 3)
     return bad(VFLIP_ERR_ARG);
   if (ctx->cfg.tile_sweep_max_cells == 0) ctx->cfg.tile_sweep_max_cells = 64 * 64 * 64;
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
@@ -3214,6 +3216,30 @@ int exclusive_scan(vflip_ctx* ctx, const int* in, int* out, size_t n, int depth 
 
 }  // namespace
 
+// The tiled P2G gather over (ni+1) x (nj+1) x (nk+1) node indices in tiles
+// of 8 x 8 x TZ: TZ = 8 one CTA per SM, TZ = 4 two, each with the shared
+// memory that residency leaves it.
+template <int TZ>
+static int launch_p2g_tile(vflip_ctx* ctx, int ni, int nj, int nk, float h, float ih, const int* start,
+                           const float4* spos, const float4* svel, float* u, float* ucoef, float* v, float* vcoef,
+                           float* w, float* wcoef) {
+  int per_sm = 0, per_block = 0;
+  VF_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->cfg.device));
+  VF_CUDA(cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device));
+  // the runtime reserves 1 KB of each resident CTA's shared memory
+  const int smem = std::min(per_block, per_sm / P2gTile<TZ>::ctas_per_sm - 1024) & ~15;
+  VF_CUDA(smem_optin((const void*)p2g3_tile_kernel<TZ>, smem));
+  const int cap = p2g_tile_cap<TZ>(smem);
+  if (cap < 1) return ctx->fail(VFLIP_ERR_CUDA, "no shared memory for the tiled P2G");
+  const int ntx = (ni + kP2gTX) / kP2gTX, nty = (nj + kP2gTY) / kP2gTY, ntz = (nk + TZ) / TZ;
+  const size_t tiles = (size_t)ntx * nty * ntz;
+  if (tiles > 0x7fffffff) return ctx->fail(VFLIP_ERR_ARG, "grid too large for the tiled P2G");
+  p2g3_tile_kernel<TZ><<<(unsigned)tiles, P2gTile<TZ>::threads, smem, ctx->stream>>>(
+      start, spos, svel, u, ucoef, v, vcoef, w, wcoef, ni, nj, nk, h, ih, ntx, nty, cap);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
 extern "C" {
 
 static int p2g_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void* particles, int np, float* u,
@@ -3234,6 +3260,7 @@ static int p2g_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void*
   VF_ALLOC(order, int, "p_order", npp);
   VF_ALLOC(spos, float4, "p_spos", npp);
   VF_ALLOC(svel, float4, "p_svel", npp);
+  const int sslot = prof_start(ctx, VFLIP_PROF_P2G_SORT, ctx->stream);
   VF_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * (nc + 1), ctx->stream));
   if (np > 0) {
     hash_count_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
@@ -3250,8 +3277,10 @@ static int p2g_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void*
         (const ParticleRec*)particles, order, spos, svel, start + nc, sf);
     VF_LAUNCH_CHECK();
   }
+  prof_stop(ctx, sslot, ctx->stream);
   if (!u && !v && !w) return VFLIP_OK;
   const float ih = (float)inv_pow2(h);
+  const int gslot = prof_start(ctx, VFLIP_PROF_P2G_GATHER, ctx->stream);
   if (sf.sub) {
     // the 9^3 gathers of the boundary shell and the 3^3 ones of the inner box
     // in separate launches, so that no warp mixes the two
@@ -3262,12 +3291,18 @@ static int p2g_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void*
           start, spos, svel, u, ucoef, v, vcoef, w, wcoef, ni, nj, nk, h, ih, part);
       VF_LAUNCH_CHECK();
     }
+  } else if (ctx->cfg.p2g_kernel != 1) {
+    const int rc2 = ctx->cfg.p2g_kernel == 3
+                        ? launch_p2g_tile<4>(ctx, ni, nj, nk, h, ih, start, spos, svel, u, ucoef, v, vcoef, w, wcoef)
+                        : launch_p2g_tile<8>(ctx, ni, nj, nk, h, ih, start, spos, svel, u, ucoef, v, vcoef, w, wcoef);
+    if (rc2) return rc2;
   } else {
     const size_t nn = p2g_part_size(P2G_ALL, ni, nj, nk);
     p2g3_kernel<false><<<grid_for(nn, 128, ctx->num_sms * 8), 128, 0, ctx->stream>>>(
         start, spos, svel, u, ucoef, v, vcoef, w, wcoef, ni, nj, nk, h, ih, P2G_ALL);
     VF_LAUNCH_CHECK();
   }
+  prof_stop(ctx, gslot, ctx->stream);
   return VFLIP_OK;
 }
 

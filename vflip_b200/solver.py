@@ -69,7 +69,8 @@ class Solver:
                  device=0, stream=None, sweep_kernel=0, smoother_depth=0, smoother_tile_rows=0,
                  smoother_plane_ranges=0, smoother_ctas_per_sm=0, smoother_threads=0,
                  smoother_prefetch=0, coarsest_solver=0, spmv_kernel=0, pcg_loop=0, pcg_vectors=0,
-                 batch_chunk=0, batch_ctas_per_sm=0, coarse_tail=0, tile_sweep_max_cells=0):
+                 batch_chunk=0, batch_ctas_per_sm=0, coarse_tail=0, tile_sweep_max_cells=0,
+                 p2g_kernel=0):
         self.lib = load()
         cfg = ConfigC()
         self.lib.vflip_config_default(C.byref(cfg))
@@ -94,6 +95,7 @@ class Solver:
         cfg.batch_ctas_per_sm = batch_ctas_per_sm
         cfg.coarse_tail = coarse_tail
         cfg.tile_sweep_max_cells = tile_sweep_max_cells
+        cfg.p2g_kernel = p2g_kernel
         self.device = torch.device("cuda", device)
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
@@ -554,7 +556,7 @@ class Solver:
         return n.value, ms.value, cells.value
 
     PROF_KINDS = {"fine_sweep": 0, "spmv": 1, "update": 2, "advect_field": 3, "advect_pair": 4, "vcycle": 5,
-                  "coarse": 6}
+                  "coarse": 6, "p2g_sort": 7, "p2g_gather": 8}
 
     def profile_kernels(self, kind):
         """(launches, total_ms) of the timed launches of one kind (PROF_KINDS)."""
