@@ -91,14 +91,16 @@ def test_p2g_vs_oracle(gpu_solver, orc, dims, n):
 
 
 def test_p2g_crowded_cells_and_empty(gpu_solver, orc):
-    """Buckets far beyond 32 particles (heapsort path), particles outside the
-    grid, and an empty particle set."""
+    """Buckets far beyond 32 particles (2600 in one cell: heapsort; 700 in
+    another: a warp's bitonic sort), particles outside the grid, and an
+    empty particle set."""
     ni, nj, nk = 6, 5, 4
     h = np.float32(0.2)
     rng = np.random.default_rng(17)
-    p = scenes.random_particles(ni, nj, nk, h, 3000, rng, margin=0.0)
-    p["pos"][:2000] = (np.array([2.0, 2.0, 1.0]) * h + rng.uniform(-0.4, 0.4, (2000, 3)) * h).astype(np.float32)
-    p["pos"][2000:2100] = -5.0  # outside
+    p = scenes.random_particles(ni, nj, nk, h, 4300, rng, margin=0.0)
+    p["pos"][:2600] = (np.array([2.0, 2.0, 1.0]) * h + rng.uniform(-0.4, 0.4, (2600, 3)) * h).astype(np.float32)
+    p["pos"][3000:3700] = (np.array([4.0, 1.0, 2.0]) * h + rng.uniform(-0.4, 0.4, (700, 3)) * h).astype(np.float32)
+    p["pos"][2600:2700] = -5.0  # outside
     rng.shuffle(p)
     outs = gpu_solver[1].particle_to_grid(ni, nj, nk, h, parts(p))
     for c in range(3):
@@ -185,6 +187,20 @@ def test_reorder_flip_bit_exact(gpu_solver, orc, dims, n, seed):
                                      t(u), t(v), t(w), t(phi), seed=seed).cpu().numpy()
     want = orc.reorder_flip(ni, nj, nk, h, p, u, v, w, phi, seed=seed)
     assert got.size == want.size * 40 and np.array_equal(got, want.view(np.uint8))
+
+
+def test_reorder_flip_crowded_cells(gpu_solver, orc):
+    """Reseeding keeps the first particles of each bucket in index order:
+    buckets of 2500 (heapsort) and 900 (a warp's bitonic sort) particles."""
+    ni, nj, nk = 9, 8, 7
+    h, phi, u, v, w, p = _flip_scene(ni, nj, nk, 21, 5000)
+    rng = np.random.default_rng(4)
+    p["pos"][:2500] = (np.array([4.0, 4.0, 3.0]) * h + rng.uniform(-0.45, 0.45, (2500, 3)) * h).astype(np.float32)
+    p["pos"][2500:3400] = (np.array([2.0, 5.0, 4.0]) * h + rng.uniform(-0.45, 0.45, (900, 3)) * h).astype(np.float32)
+    rng.shuffle(p)
+    got = gpu_solver[1].reorder_flip(ni, nj, nk, h, t(p.view(np.uint8)), t(u), t(v), t(w), t(phi), seed=5)
+    want = orc.reorder_flip(ni, nj, nk, h, p, u, v, w, phi, seed=5)
+    assert np.array_equal(got.cpu().numpy(), want.view(np.uint8))
 
 
 def test_reorder_flip_capacity(gpu_solver):

@@ -8,7 +8,8 @@
     fused kernel's bits;
   * the projection's PCG, which reads the FP32 copies of the couplings it
     assembled, gives the bits of the same solve on the FP64 operator;
-  * the tiled P2G gives the per-node global gather's bits."""
+  * the tiled P2G, on the main grid and on a subdomain's, gives the
+    per-node global gather's bits."""
 import numpy as np
 import pytest
 
@@ -228,3 +229,42 @@ def test_tiled_p2g_matches_global_gather():
             for c in comps:
                 assert torch.equal(res[0][c][0], r[c][0]), (name, c)
                 assert torch.equal(res[0][c][1], r[c][1]), (name, c)
+
+
+def test_tiled_subdomain_p2g_matches_global_gather():
+    """A subdomain's tiled P2G (tiles near its boundary stage a 4-cell ring;
+    nodes within 4 cells of the boundary gather 9^3 buckets with the 4h
+    tent, the rest 3^3) gives the global shell and inner-box launches' bits
+    (p2g_kernel 1), for the three spacing forms, a dense blob staged in
+    chunks and particles outside the subdomain (clamped into its edge
+    buckets)."""
+    from vflip_b200.solver import Solver
+
+    rng = np.random.default_rng(29)
+    cases = []
+    for dims, hh, ppc in (((40, 36, 30), 1.0 / 64, 8), ((27, 22, 19), 0.03, 6), ((18, 13, 21), 2.0, 5)):
+        h = np.float32(hh)
+        bmin = tuple(np.float32(x) for x in rng.uniform(-1.0, 1.0, 3) * h * 7)
+        p = scenes.jittered_particles(*dims, h, ppc, rng)
+        p["pos"] += np.array(bmin, np.float32)
+        p["vel"] = rng.standard_normal((len(p), 3)).astype(np.float32)
+        out = scenes.random_particles(*dims, h, 500, rng, margin=3.0)
+        out["pos"] += np.array(bmin, np.float32)
+        p = np.concatenate([p, out])
+        rng.shuffle(p)
+        cases.append((dims, h, bmin, p))
+    dims, h, bmin, p = cases[0]
+    blob = p[:30000].copy()
+    blob["pos"] = (np.array([3.0, 30.0, 12.0]) * h + rng.uniform(-1.5, 1.5, (30000, 3)) * h + bmin).astype(np.float32)
+    cases.append((dims, h, bmin, np.concatenate([p, blob])))
+    for dims, h, bmin, p in cases:
+        res = []
+        for kern in (1, 0, 3):
+            with Solver(precision=1, p2g_kernel=kern) as s:
+                outs = s.sub_particle_to_grid(*dims, h, bmin, t(p.view(np.uint8)))
+                res.append([(outs[c][0].view(torch.int32).clone(), outs[c][1].view(torch.int32).clone())
+                            for c in range(3)])
+        for r in res[1:]:
+            for c in range(3):
+                assert torch.equal(res[0][c][0], r[c][0]), (dims, h, c)
+                assert torch.equal(res[0][c][1], r[c][1]), (dims, h, c)

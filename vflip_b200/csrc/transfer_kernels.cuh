@@ -407,12 +407,21 @@ __device__ __forceinline__ void sift_down(int* a, int root, int end) {
   }
 }
 
-__global__ void sort_buckets_kernel(const int* __restrict__ start, int* __restrict__ order, int ncells) {
+// Buckets of 33 .. kBigBucket particles are listed in `big` (big_n counts
+// them) for sort_big_buckets_kernel; larger ones are heapsorted here.
+constexpr int kBigBucket = 2048;
+
+__global__ void sort_buckets_kernel(const int* __restrict__ start, int* __restrict__ order, int ncells,
+                                    int* __restrict__ big, int* __restrict__ big_n) {
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncells; c += gridDim.x * blockDim.x) {
     int b = start[c], e = start[c + 1];
     int m = e - b;
     if (m < 2) continue;
     int* a = order + b;
+    if (m > 32 && m <= kBigBucket) {
+      big[atomicAdd(big_n, 1)] = c;
+      continue;
+    }
     if (m <= 32) {
       for (int x = 1; x < m; ++x) {
         int key = a[x];
@@ -427,6 +436,48 @@ __global__ void sort_buckets_kernel(const int* __restrict__ start, int* __restri
         sift_down(a, 0, end);
       }
     }
+  }
+}
+
+// The listed buckets, one warp each: the particle indices in shared memory,
+// padded with INT_MAX to a power of two, put in ascending order by a
+// bitonic network (within a stage the compare-exchange pairs are disjoint;
+// the warp synchronises between stages).  Particle indices are distinct, so
+// the order is the one the heapsort gives.
+constexpr int kBigWarps = 4;
+
+__global__ void __launch_bounds__(32 * kBigWarps) sort_big_buckets_kernel(const int* __restrict__ start,
+                                                                       int* __restrict__ order,
+                                                                       const int* __restrict__ big,
+                                                                       const int* __restrict__ big_n) {
+  __shared__ int sm[kBigWarps][kBigBucket];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int* v = sm[wid];
+  const int nbig = *big_n;
+  for (int e = blockIdx.x * kBigWarps + wid; e < nbig; e += gridDim.x * kBigWarps) {
+    const int c = big[e];
+    const int b = start[c], m = start[c + 1] - b;
+    int P = 64;
+    while (P < m) P <<= 1;
+    for (int i = lane; i < P; i += 32) v[i] = i < m ? order[b + i] : INT_MAX;
+    __syncwarp();
+    for (int k = 2; k <= P; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int i = lane; i < P; i += 32) {
+          const int x = i ^ j;
+          if (x > i) {
+            const int p = v[i], q = v[x];
+            if ((p > q) == ((i & k) == 0)) {
+              v[i] = q;
+              v[x] = p;
+            }
+          }
+        }
+        __syncwarp();
+      }
+    }
+    for (int i = lane; i < m; i += 32) order[b + i] = v[i];
+    __syncwarp();
   }
 }
 
@@ -723,21 +774,23 @@ __global__ void p2g3_kernel(const int* __restrict__ start, const float4* __restr
 // holds and its visiting order is unchanged.  Every particle of a window is
 // added (p2g_add: no reach test, no divergence between the threads of a
 // warp), which gives p2g_visit's sums bit for bit.
-// Tile shapes: TZ = 8 node layers (one CTA of 256 threads per SM, a
-// 10 x 10 x 10-cell region) or TZ = 4 (two CTAs of 128 threads per SM, each
-// half the shared memory, so that one CTA's staging overlaps the other's
-// gathers; a 10 x 10 x 6-cell region).
+// Tile shapes: TZ = 8 node layers (one CTA of 256 threads per SM) or TZ = 4
+// (two CTAs of 128 threads per SM, each half the shared memory, so that one
+// CTA's staging overlaps the other's gathers).  SUB: a subdomain's grid,
+// whose nodes within 4 of its boundary gather from 9^3 buckets: the tables
+// hold a 4-cell ring.
 constexpr int kP2gTX = 8, kP2gTY = 8;
-constexpr int kP2gRX = kP2gTX + 2;  // bucket columns of the staged region
-constexpr int kP2gBatch = 4;        // particles a thread loads before staging them
-template <int TZ>
+constexpr int kP2gBatch = 4;  // 32-particle steps a warp loads before staging them
+template <int TZ, bool SUB>
 struct P2gTile {
-  static constexpr int threads = kP2gTX * kP2gTY * (TZ / 2);  // two nodes (k, k + 1) per thread
-  static constexpr int rows = (kP2gTY + 2) * (TZ + 2);        // bucket rows of the staged region
-  static constexpr int rows_pad = rows < 64 ? 64 : 128;       // the row scan's width
-  static constexpr int fixed_ints = rows * (kP2gRX + 1) + 2 * rows_pad;
+  static constexpr int ring = SUB ? 4 : 1;                          // widest window half-width
+  static constexpr int threads = kP2gTX * kP2gTY * (TZ / 2);         // two nodes (k, k + 1) per thread
+  static constexpr int rx = kP2gTX + 2 * ring;                       // bucket columns of the staged region
+  static constexpr int rows = (kP2gTY + 2 * ring) * (TZ + 2 * ring);  // bucket rows of the staged region
+  static constexpr int rows_pad = (rows + 1 + 31) / 32 * 32;          // the row scan's width
+  static constexpr int fixed_ints = rows * (rx + 1) + 2 * rows_pad;
   static constexpr int ctas_per_sm = TZ == 8 ? 1 : 2;
-  static_assert(rows < rows_pad && fixed_ints % 4 == 0 && threads >= rows_pad, "p2g tile tables");
+  static_assert(fixed_ints % 4 == 0, "p2g tile tables");
 };
 
 // shared-memory slot of staged particle s: one pad word per 32 spreads the
@@ -745,9 +798,9 @@ struct P2gTile {
 __host__ __device__ inline int p2g_slot(int s) { return s + (s >> 5); }
 
 // particles a CTA with `smem_bytes` of dynamic shared memory stages
-template <int TZ>
+template <int TZ, bool SUB>
 __host__ __device__ inline int p2g_tile_cap(size_t smem_bytes) {
-  const size_t fixed = sizeof(int) * (size_t)P2gTile<TZ>::fixed_ints;
+  const size_t fixed = sizeof(int) * (size_t)P2gTile<TZ, SUB>::fixed_ints;
   if (smem_bytes <= fixed + 6 * sizeof(float) * 2) return 0;
   const long a = (long)((smem_bytes - fixed) / (6 * sizeof(float)));  // floats per array
   long cap = (a - 1) * 32 / 33;
@@ -755,100 +808,142 @@ __host__ __device__ inline int p2g_tile_cap(size_t smem_bytes) {
   return (int)cap;
 }
 
-// node (i, j, k)'s window in row (ck, cj) of the staged region, clipped to
-// the chunk [c0, c1) and made chunk-relative
-__device__ __forceinline__ int2 p2g_window(const int* cs, int row, int i, int ni, int clo, int c0, int c1) {
-  const int* c = cs + row * (kP2gRX + 1);
-  return make_int2(max(c[max(i - 1, 0) - clo], c0) - c0, min(c[min(i + 1, ni - 1) + 1 - clo], c1) - c0);
+// The staged particles of one chunk and where each row's buckets start.
+struct P2gStage {
+  const int* cs;  // [row][c]: staged index of bucket clo + c's first particle (row stride `stride`)
+  int stride, clo, cjlo, cklo, nry;
+  int c0, c1;  // the chunk: staged indices [c0, c1)
+  const float *px, *py, *pz, *vx, *vy, *vz;
+};
+
+// the window i - l .. i + l (clipped to the grid) of row (ck, cj), clipped
+// to the chunk and made chunk-relative
+__device__ __forceinline__ int2 p2g_window(const P2gStage& g, int ck, int cj, int i, int l, int ni) {
+  const int* c = g.cs + ((ck - g.cklo) * g.nry + (cj - g.cjlo)) * g.stride;
+  return make_int2(max(c[max(i - l, 0) - g.clo], g.c0) - g.c0, min(c[min(i + l, ni - 1) + 1 - g.clo], g.c1) - g.c0);
 }
 
 template <int M>
-__device__ __forceinline__ void p2g_run1(P2gNode& n, int b, int e, const float* px, const float* py,
-                                         const float* pz, const float* vx, const float* vy, const float* vz,
-                                         float h, float inv_h) {
+__device__ __forceinline__ void p2g_run1(P2gNode& n, int b, int e, const P2gStage& g, float hk, float ihk) {
 #pragma unroll 2
   for (int s = b; s < e; ++s) {
     const int P = p2g_slot(s);
-    p2g_add<M>(n, px[P], py[P], pz[P], vx[P], vy[P], vz[P], h, inv_h);
+    p2g_add<M>(n, g.px[P], g.py[P], g.pz[P], g.vx[P], g.vy[P], g.vz[P], hk, ihk);
   }
 }
 
 template <int M>
-__device__ __forceinline__ void p2g_run2(P2gNode& n0, P2gNode& n1, int b, int e, const float* px, const float* py,
-                                         const float* pz, const float* vx, const float* vy, const float* vz,
-                                         float h, float inv_h) {
+__device__ __forceinline__ void p2g_run2(P2gNode& n0, P2gNode& n1, int b, int e, const P2gStage& g, float hk,
+                                         float ihk) {
 #pragma unroll 2
   for (int s = b; s < e; ++s) {
     const int P = p2g_slot(s);
-    p2g_add2<M>(n0, n1, px[P], py[P], pz[P], vx[P], vy[P], vz[P], h, inv_h);
+    p2g_add2<M>(n0, n1, g.px[P], g.py[P], g.pz[P], g.vx[P], g.vy[P], g.vz[P], hk, ihk);
   }
 }
 
-// One chunk's gathers of the thread's nodes (i, j, k) and (i, j, k + 1):
-// planes k - 1 .. k + 2 in order, rows j - 1 .. j + 1 in each; planes k
-// and k + 1 belong to both windows (the same x run), k - 1 to the first
-// node's only, k + 2 to the second's.
+// One chunk's gathers of the nodes (i, j, k) and (i, j, k + 1), both of
+// window half-width l: planes k - l .. k + 1 + l in order, rows j - l ..
+// j + l in each; the planes both windows hold are visited once for both
+// (the same x run), k - l only by the first node, k + 1 + l only by the
+// second.  on1 false: the first node alone.
 template <int M>
-__device__ __forceinline__ void p2g_chunk2(P2gNode& n0, P2gNode& n1, bool on0, bool on1, int i, int j, int k,
-                                           int ni, int nj, int nk, int clo, int cjlo, int cklo, int nry,
-                                           const int* cs, int c0, int c1, const float* px, const float* py,
-                                           const float* pz, const float* vx, const float* vy, const float* vz,
-                                           float h, float inv_h) {
-  for (int dk = -1; dk <= 2; ++dk) {
-    const int ck = k + dk;
-    const bool a0 = on0 && dk <= 1, a1 = on1 && dk >= 0;
+__device__ __forceinline__ void p2g_chunk2(P2gNode& n0, P2gNode& n1, bool on1, int l, int i, int j, int k, int ni,
+                                           int nj, int nk, const P2gStage& g, float hk, float ihk) {
+  for (int ck = k - l; ck <= k + 1 + l; ++ck) {
+    const bool a0 = ck <= k + l, a1 = on1 && ck >= k + 1 - l;
     if (ck < 0 || ck >= nk || !(a0 || a1)) continue;
-    for (int dj = -1; dj <= 1; ++dj) {
-      const int cj = j + dj;
+    for (int cj = j - l; cj <= j + l; ++cj) {
       if (cj < 0 || cj >= nj) continue;
-      const int2 w = p2g_window(cs, (ck - cklo) * nry + (cj - cjlo), i, ni, clo, c0, c1);
+      const int2 w = p2g_window(g, ck, cj, i, l, ni);
       if (a0 && a1)
-        p2g_run2<M>(n0, n1, w.x, w.y, px, py, pz, vx, vy, vz, h, inv_h);
+        p2g_run2<M>(n0, n1, w.x, w.y, g, hk, ihk);
       else if (a0)
-        p2g_run1<M>(n0, w.x, w.y, px, py, pz, vx, vy, vz, h, inv_h);
+        p2g_run1<M>(n0, w.x, w.y, g, hk, ihk);
       else
-        p2g_run1<M>(n1, w.x, w.y, px, py, pz, vx, vy, vz, h, inv_h);
+        p2g_run1<M>(n1, w.x, w.y, g, hk, ihk);
     }
   }
 }
 
-template <int TZ>
-__global__ void __launch_bounds__(P2gTile<TZ>::threads, P2gTile<TZ>::ctas_per_sm)
+// The same for a single node of half-width l.
+template <int M>
+__device__ __forceinline__ void p2g_chunk1(P2gNode& n, int l, int i, int j, int k, int ni, int nj, int nk,
+                                           const P2gStage& g, float hk, float ihk) {
+  for (int ck = max(k - l, 0); ck <= min(k + l, nk - 1); ++ck)
+    for (int cj = max(j - l, 0); cj <= min(j + l, nj - 1); ++cj) {
+      const int2 w = p2g_window(g, ck, cj, i, l, ni);
+      p2g_run1<M>(n, w.x, w.y, g, hk, ihk);
+    }
+}
+
+// The tent mode and scale for window half-width l (tent width l == 4 ? 4h
+// : h): mode 2 (positions and node coordinates scaled by inv_h) takes the
+// scaled offset itself for l = 1 and a quarter of it for l = 4 (exact);
+// mode 1 multiplies by inv_h (/ 4); mode 0 divides by h (4h: exact in float).
+template <bool PAIR>
+__device__ __forceinline__ void p2g_chunk(P2gNode& n0, P2gNode& n1, bool on1, int l, int mode, int i, int j, int k,
+                                          int ni, int nj, int nk, const P2gStage& g, float h, float inv_h) {
+  const bool w4 = l == 4;
+  if (mode == 2 && !w4) {
+    if (PAIR) p2g_chunk2<2>(n0, n1, on1, l, i, j, k, ni, nj, nk, g, h, inv_h);
+    else p2g_chunk1<2>(n0, l, i, j, k, ni, nj, nk, g, h, inv_h);
+  } else if (mode != 0) {
+    const float ihk = mode == 2 ? 0.25f : (w4 ? inv_h * 0.25f : inv_h);
+    if (PAIR) p2g_chunk2<1>(n0, n1, on1, l, i, j, k, ni, nj, nk, g, h, ihk);
+    else p2g_chunk1<1>(n0, l, i, j, k, ni, nj, nk, g, h, ihk);
+  } else {
+    const float hk = w4 ? (float)(4.0 * (double)h) : h;
+    if (PAIR) p2g_chunk2<0>(n0, n1, on1, l, i, j, k, ni, nj, nk, g, hk, inv_h);
+    else p2g_chunk1<0>(n0, l, i, j, k, ni, nj, nk, g, hk, inv_h);
+  }
+}
+
+template <int TZ, bool SUB>
+__global__ void __launch_bounds__(P2gTile<TZ, SUB>::threads, P2gTile<TZ, SUB>::ctas_per_sm)
     p2g3_tile_kernel(const int* __restrict__ start, const float4* __restrict__ spos,
                      const float4* __restrict__ svel, float* __restrict__ fu, float* __restrict__ cu,
                      float* __restrict__ fv, float* __restrict__ cv, float* __restrict__ fw, float* __restrict__ cw,
                      int ni, int nj, int nk, float h, float inv_h, int ntx, int nty, int cap) {
-  using T = P2gTile<TZ>;
+  using T = P2gTile<TZ, SUB>;
   constexpr int R = T::rows_pad / 32;  // rows per lane of the scan
+  constexpr int S = T::rx + 1;         // the bucket table's row stride
   extern __shared__ __align__(16) int psm[];
-  int* cs = psm;                                   // [row][c]: staged index of bucket clo + c's first particle
-  int* rbeg = cs + T::rows * (kP2gRX + 1);         // [row]: sorted index of the row run's first particle
-  int* roff = rbeg + T::rows_pad;                  // [row]: staged index of the row run's first particle
+  int* cs = psm;                       // [row][c]: staged index of bucket clo + c's first particle
+  int* rbeg = cs + T::rows * S;        // [row]: sorted index of the row run's first particle
+  int* roff = rbeg + T::rows_pad;      // [row]: staged index of the row run's first particle
   const int A = p2g_slot(cap - 1) + 1;
   float* px = reinterpret_cast<float*>(psm + T::fixed_ints);
   float *py = px + A, *pz = py + A, *vx = pz + A, *vy = vx + A, *vz = vy + A;
   const int tid = threadIdx.x, t = blockIdx.x;
   const int i0 = (t % ntx) * kP2gTX, j0 = ((t / ntx) % nty) * kP2gTY, k0 = (t / (ntx * nty)) * TZ;
+  // the widest window of the tile's nodes: 4 where one lies within 4 of a
+  // subdomain's boundary (some axis of the tile comes that close)
+  int L = 1;
+  if (SUB) {
+    auto near = [](int a0, int n, int w) { return a0 <= 4 || min(a0 + w - 1, n) >= n - 4; };
+    if (near(i0, ni, kP2gTX) || near(j0, nj, kP2gTY) || near(k0, nk, TZ)) L = 4;
+  }
   // the staged cells: [clo, chi] x [cjlo, cjhi] x [cklo, ckhi]
-  const int clo = max(i0 - 1, 0), chi = min(i0 + kP2gTX, ni - 1), nrx = chi - clo + 1;
-  const int cjlo = max(j0 - 1, 0), nry = min(j0 + kP2gTY, nj - 1) - cjlo + 1;
-  const int cklo = max(k0 - 1, 0), nrz = min(k0 + TZ, nk - 1) - cklo + 1;
+  const int clo = max(i0 - L, 0), chi = min(i0 + kP2gTX - 1 + L, ni - 1), nrx = chi - clo + 1;
+  const int cjlo = max(j0 - L, 0), nry = min(j0 + kP2gTY - 1 + L, nj - 1) - cjlo + 1;
+  const int cklo = max(k0 - L, 0), nrz = min(k0 + TZ - 1 + L, nk - 1) - cklo + 1;
   const int nrows = nry * nrz;
   auto row_base = [&](int r) { return ((cklo + r / nry) * nj + cjlo + r % nry) * ni; };
   // the region's bucket starts in one round of loads, then each row's run
   for (int e = tid; e < nrows * (nrx + 1); e += T::threads) {
     const int r = e / (nrx + 1), c = e - r * (nrx + 1);
-    cs[r * (kP2gRX + 1) + c] = __ldg(start + row_base(r) + clo + c);
+    cs[r * S + c] = __ldg(start + row_base(r) + clo + c);
   }
   __syncthreads();
-  if (tid < T::rows_pad) {
+  for (int r = tid; r < T::rows_pad; r += T::threads) {
     int len = 0;
-    if (tid < nrows) {
-      const int b = cs[tid * (kP2gRX + 1)];
-      rbeg[tid] = b;
-      len = cs[tid * (kP2gRX + 1) + nrx] - b;
+    if (r < nrows) {
+      const int b = cs[r * S];
+      rbeg[r] = b;
+      len = cs[r * S + nrx] - b;
     }
-    roff[tid] = len;
+    roff[r] = len;
   }
   __syncthreads();
   if (tid < 32) {  // exclusive scan of the run lengths, R rows per lane
@@ -873,7 +968,7 @@ __global__ void __launch_bounds__(P2gTile<TZ>::threads, P2gTile<TZ>::ctas_per_sm
   __syncthreads();
   for (int e = tid; e < nrows * (nrx + 1); e += T::threads) {
     const int r = e / (nrx + 1), c = e - r * (nrx + 1);
-    cs[r * (kP2gRX + 1) + c] += roff[r] - rbeg[r];
+    cs[r * S + c] += roff[r] - rbeg[r];
   }
   const int total = roff[nrows];  // the rows past nrows have length 0
   // tent mode (p2g_tent): 2 scales positions and node coordinates by inv_h
@@ -881,6 +976,13 @@ __global__ void __launch_bounds__(P2gTile<TZ>::threads, P2gTile<TZ>::ctas_per_sm
   const float sc = mode == 2 ? inv_h : 1.0f;
   const int i = i0 + tid % kP2gTX, j = j0 + (tid / kP2gTX) % kP2gTY, k = k0 + 2 * (tid / (kP2gTX * kP2gTY));
   const bool on0 = i <= ni && j <= nj && k <= nk, on1 = on0 && k + 1 <= nk;
+  // window half-widths: SubDomainSolver::determineDist, 4 within 4 cells of the boundary
+  auto half = [&](int kk) {
+    if (!SUB) return 1;
+    const int d = min(min(min(i, ni - i), min(j, nj - j)), min(kk, nk - kk));
+    return d <= 4 ? 4 : 1;
+  };
+  const int l0 = half(k), l1 = half(k + 1);
   P2gNode n0 = p2g_node(i, j, k, ni, nj, nk, h, fu != nullptr, fv != nullptr, fw != nullptr);
   P2gNode n1 = p2g_node(i, j, k + 1, ni, nj, nk, h, fu != nullptr, fv != nullptr, fw != nullptr);
   if (mode == 2) {
@@ -931,15 +1033,13 @@ __global__ void __launch_bounds__(P2gTile<TZ>::threads, P2gTile<TZ>::ctas_per_sm
     }
     __syncthreads();
     if (!on0) continue;
-    if (mode == 2)
-      p2g_chunk2<2>(n0, n1, on0, on1, i, j, k, ni, nj, nk, clo, cjlo, cklo, nry, cs, c0, c1, px, py, pz, vx, vy, vz,
-                    h, inv_h);
-    else if (mode == 1)
-      p2g_chunk2<1>(n0, n1, on0, on1, i, j, k, ni, nj, nk, clo, cjlo, cklo, nry, cs, c0, c1, px, py, pz, vx, vy, vz,
-                    h, inv_h);
-    else
-      p2g_chunk2<0>(n0, n1, on0, on1, i, j, k, ni, nj, nk, clo, cjlo, cklo, nry, cs, c0, c1, px, py, pz, vx, vy, vz,
-                    h, inv_h);
+    const P2gStage g{cs, S, clo, cjlo, cklo, nry, c0, c1, px, py, pz, vx, vy, vz};
+    if (l0 == l1 || !on1) {
+      p2g_chunk<true>(n0, n1, on1 && l0 == l1, l0, mode, i, j, k, ni, nj, nk, g, h, inv_h);
+    } else {  // a subdomain node pair across the shell's edge: each alone
+      p2g_chunk<false>(n0, n0, false, l0, mode, i, j, k, ni, nj, nk, g, h, inv_h);
+      p2g_chunk<false>(n1, n1, false, l1, mode, i, j, k + 1, ni, nj, nk, g, h, inv_h);
+    }
   }
   if (on0) p2g_store(n0, i, j, k, ni, nj, fu, cu, fv, cv, fw, cw);
   if (on1) p2g_store(n1, i, j, k + 1, ni, nj, fu, cu, fv, cv, fw, cw);

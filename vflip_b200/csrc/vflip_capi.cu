@@ -3216,25 +3216,41 @@ int exclusive_scan(vflip_ctx* ctx, const int* in, int* out, size_t n, int depth 
 
 }  // namespace
 
+// Each bucket of `order` (start[c] .. start[c+1]) into ascending particle
+// order: insertion sort of up to 32, a warp's bitonic sort in shared memory
+// of up to kBigBucket (the buckets listed by sort_buckets_kernel), heapsort
+// beyond.
+static int sort_buckets(vflip_ctx* ctx, const int* start, int* order, size_t nc, int np) {
+  int* big;
+  VF_ALLOC(big, int, "p_big", (size_t)np / 33 + 2);  // [0]: the count; at most np / 33 buckets exceed 32
+  VF_CUDA(cudaMemsetAsync(big, 0, sizeof(int), ctx->stream));
+  sort_buckets_kernel<<<grid_for(nc, 256, ctx->num_sms), 256, 0, ctx->stream>>>(start, order, (int)nc, big + 1, big);
+  VF_LAUNCH_CHECK();
+  sort_big_buckets_kernel<<<ctx->num_sms * 6, 32 * kBigWarps, 0, ctx->stream>>>(start, order, big + 1, big);
+  VF_LAUNCH_CHECK();
+  return VFLIP_OK;
+}
+
 // The tiled P2G gather over (ni+1) x (nj+1) x (nk+1) node indices in tiles
 // of 8 x 8 x TZ: TZ = 8 one CTA per SM, TZ = 4 two, each with the shared
-// memory that residency leaves it.
-template <int TZ>
+// memory that residency leaves it; SUB: a subdomain's grid.
+template <int TZ, bool SUB>
 static int launch_p2g_tile(vflip_ctx* ctx, int ni, int nj, int nk, float h, float ih, const int* start,
                            const float4* spos, const float4* svel, float* u, float* ucoef, float* v, float* vcoef,
                            float* w, float* wcoef) {
+  using T = P2gTile<TZ, SUB>;
   int per_sm = 0, per_block = 0;
   VF_CUDA(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->cfg.device));
   VF_CUDA(cudaDeviceGetAttribute(&per_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->cfg.device));
   // the runtime reserves 1 KB of each resident CTA's shared memory
-  const int smem = std::min(per_block, per_sm / P2gTile<TZ>::ctas_per_sm - 1024) & ~15;
-  VF_CUDA(smem_optin((const void*)p2g3_tile_kernel<TZ>, smem));
-  const int cap = p2g_tile_cap<TZ>(smem);
+  const int smem = std::min(per_block, per_sm / T::ctas_per_sm - 1024) & ~15;
+  VF_CUDA(smem_optin((const void*)p2g3_tile_kernel<TZ, SUB>, smem));
+  const int cap = p2g_tile_cap<TZ, SUB>(smem);
   if (cap < 1) return ctx->fail(VFLIP_ERR_CUDA, "no shared memory for the tiled P2G");
   const int ntx = (ni + kP2gTX) / kP2gTX, nty = (nj + kP2gTY) / kP2gTY, ntz = (nk + TZ) / TZ;
   const size_t tiles = (size_t)ntx * nty * ntz;
   if (tiles > 0x7fffffff) return ctx->fail(VFLIP_ERR_ARG, "grid too large for the tiled P2G");
-  p2g3_tile_kernel<TZ><<<(unsigned)tiles, P2gTile<TZ>::threads, smem, ctx->stream>>>(
+  p2g3_tile_kernel<TZ, SUB><<<(unsigned)tiles, T::threads, smem, ctx->stream>>>(
       start, spos, svel, u, ucoef, v, vcoef, w, wcoef, ni, nj, nk, h, ih, ntx, nty, cap);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
@@ -3271,8 +3287,7 @@ static int p2g_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void*
   if (np > 0) {
     scatter_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(cell, slot, start, order, np);
     VF_LAUNCH_CHECK();
-    sort_buckets_kernel<<<grid_for(nc, 256, ctx->num_sms), 256, 0, ctx->stream>>>(start, order, (int)nc);
-    VF_LAUNCH_CHECK();
+    if ((rc = sort_buckets(ctx, start, order, nc, np))) return rc;
     gather_sorted_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
         (const ParticleRec*)particles, order, spos, svel, start + nc, sf);
     VF_LAUNCH_CHECK();
@@ -3281,7 +3296,13 @@ static int p2g_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void*
   if (!u && !v && !w) return VFLIP_OK;
   const float ih = (float)inv_pow2(h);
   const int gslot = prof_start(ctx, VFLIP_PROF_P2G_GATHER, ctx->stream);
-  if (sf.sub) {
+  if (sf.sub && ctx->cfg.p2g_kernel != 1) {
+    const int rc2 =
+        ctx->cfg.p2g_kernel == 3
+            ? launch_p2g_tile<4, true>(ctx, ni, nj, nk, h, ih, start, spos, svel, u, ucoef, v, vcoef, w, wcoef)
+            : launch_p2g_tile<8, true>(ctx, ni, nj, nk, h, ih, start, spos, svel, u, ucoef, v, vcoef, w, wcoef);
+    if (rc2) return rc2;
+  } else if (sf.sub) {
     // the 9^3 gathers of the boundary shell and the 3^3 ones of the inner box
     // in separate launches, so that no warp mixes the two
     for (int part : {P2G_SHELL, P2G_INNER}) {
@@ -3293,8 +3314,10 @@ static int p2g_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, const void*
     }
   } else if (ctx->cfg.p2g_kernel != 1) {
     const int rc2 = ctx->cfg.p2g_kernel == 3
-                        ? launch_p2g_tile<4>(ctx, ni, nj, nk, h, ih, start, spos, svel, u, ucoef, v, vcoef, w, wcoef)
-                        : launch_p2g_tile<8>(ctx, ni, nj, nk, h, ih, start, spos, svel, u, ucoef, v, vcoef, w, wcoef);
+                        ? launch_p2g_tile<4, false>(ctx, ni, nj, nk, h, ih, start, spos, svel, u, ucoef, v, vcoef, w,
+                                                    wcoef)
+                        : launch_p2g_tile<8, false>(ctx, ni, nj, nk, h, ih, start, spos, svel, u, ucoef, v, vcoef, w,
+                                                    wcoef);
     if (rc2) return rc2;
   } else {
     const size_t nn = p2g_part_size(P2G_ALL, ni, nj, nk);
@@ -3436,8 +3459,7 @@ static int reorder_flip_impl(vflip_ctx* ctx, int ni, int nj, int nk, float h, co
   if (np > 0) {
     scatter_kernel<<<grid_for(np, 256, ctx->num_sms), 256, 0, ctx->stream>>>(cell, slot, start, order, np);
     VF_LAUNCH_CHECK();
-    sort_buckets_kernel<<<grid_for(nc, 256, ctx->num_sms), 256, 0, ctx->stream>>>(start, order, (int)nc);
-    VF_LAUNCH_CHECK();
+    if ((rc = sort_buckets(ctx, start, order, nc, np))) return rc;
   }
   reorder_count_kernel<<<grid_for(nc, 256, ctx->num_sms), 256, 0, ctx->stream>>>(start, ocount, (int)nc, ni, nj,
                                                                                   nk, sf.sub);
