@@ -90,10 +90,12 @@ def test_p2g_vs_oracle(gpu_solver, orc, dims, n):
         assert np.array_equal(outs[c][1].cpu().numpy(), cf)
 
 
-def test_p2g_crowded_cells_and_empty(gpu_solver, orc):
+@pytest.mark.parametrize("order", ["shuffled", "by cell"])
+def test_p2g_crowded_cells_and_empty(gpu_solver, orc, order):
     """Buckets far beyond 32 particles (2600 in one cell: heapsort; 700 in
-    another: a warp's bitonic sort), particles outside the grid, and an
-    empty particle set."""
+    another: a warp's radix sort when shuffled, its runs of consecutive
+    indices when the particles come by cell), particles outside the grid,
+    and an empty particle set."""
     ni, nj, nk = 6, 5, 4
     h = np.float32(0.2)
     rng = np.random.default_rng(17)
@@ -102,6 +104,9 @@ def test_p2g_crowded_cells_and_empty(gpu_solver, orc):
     p["pos"][3000:3700] = (np.array([4.0, 1.0, 2.0]) * h + rng.uniform(-0.4, 0.4, (700, 3)) * h).astype(np.float32)
     p["pos"][2600:2700] = -5.0  # outside
     rng.shuffle(p)
+    if order == "by cell":
+        c = np.clip(np.floor(p["pos"] / h + 0.5).astype(np.int64), 0, [ni - 1, nj - 1, nk - 1])
+        p = p[np.argsort(c[:, 0] + ni * (c[:, 1] + nj * c[:, 2]), kind="stable")]
     outs = gpu_solver[1].particle_to_grid(ni, nj, nk, h, parts(p))
     for c in range(3):
         f, cf = orc.p2g(ni, nj, nk, h, p, c)
@@ -111,6 +116,23 @@ def test_p2g_crowded_cells_and_empty(gpu_solver, orc):
     outs = gpu_solver[1].particle_to_grid(ni, nj, nk, h, empty)
     for c in range(3):
         assert torch.all(outs[c][0] == 0) and torch.all(outs[c][1] == np.float32(1e-5))
+
+
+def test_p2g_dense_tiles_vs_oracle(gpu_solver, orc):
+    """A blob of 110 000 particles over a few cells: the tiles around it hold
+    many shared-memory chunks and keep their nodes' sums in shared memory
+    between chunks."""
+    ni, nj, nk = 12, 10, 9
+    h = np.float32(1.0 / 16)
+    rng = np.random.default_rng(31)
+    p = scenes.random_particles(ni, nj, nk, h, 130000, rng, margin=0.5)
+    p["pos"][:110000] = (np.array([5.0, 4.0, 4.0]) * h + rng.uniform(-1.5, 1.5, (110000, 3)) * h).astype(np.float32)
+    rng.shuffle(p)
+    outs = gpu_solver[1].particle_to_grid(ni, nj, nk, h, parts(p))
+    for c in range(3):
+        f, cf = orc.p2g(ni, nj, nk, h, p, c)
+        assert np.array_equal(outs[c][0].cpu().numpy(), f)
+        assert np.array_equal(outs[c][1].cpu().numpy(), cf)
 
 
 @pytest.mark.parametrize("flip", [1.0, 0.95, 0.0])
@@ -191,7 +213,7 @@ def test_reorder_flip_bit_exact(gpu_solver, orc, dims, n, seed):
 
 def test_reorder_flip_crowded_cells(gpu_solver, orc):
     """Reseeding keeps the first particles of each bucket in index order:
-    buckets of 2500 (heapsort) and 900 (a warp's bitonic sort) particles."""
+    buckets of 2500 (heapsort) and 900 (a warp's radix sort) particles."""
     ni, nj, nk = 9, 8, 7
     h, phi, u, v, w, p = _flip_scene(ni, nj, nk, 21, 5000)
     rng = np.random.default_rng(4)

@@ -189,6 +189,13 @@ def _p2g_cases():
     p["pos"][40000:40100] = -3.0
     rng.shuffle(p)
     out.append(("dense blob", (ni, nj, nk), h, p, (0, 1, 2)))
+    # 120000 in a few cells: beyond 8 chunks, the nodes' sums in shared memory
+    q = scenes.random_particles(ni, nj, nk, h, 20000, rng, margin=0.5)
+    blob = scenes.random_particles(ni, nj, nk, h, 120000, rng, margin=0.0)
+    blob["pos"] = (np.array([15.0, 8.0, 9.0]) * h + rng.uniform(-1.4, 1.4, (120000, 3)) * h).astype(np.float32)
+    q = np.concatenate([q, blob])
+    rng.shuffle(q)
+    out.append(("very dense blob", (ni, nj, nk), h, q, (0, 1, 2)))
     # non-finite velocities (NaN sums wherever the window holds one)
     ni, nj, nk = 30, 26, 22
     h = np.float32(1.0 / 32)
@@ -235,9 +242,9 @@ def test_tiled_subdomain_p2g_matches_global_gather():
     """A subdomain's tiled P2G (tiles near its boundary stage a 4-cell ring;
     nodes within 4 cells of the boundary gather 9^3 buckets with the 4h
     tent, the rest 3^3) gives the global shell and inner-box launches' bits
-    (p2g_kernel 1), for the three spacing forms, a dense blob staged in
-    chunks and particles outside the subdomain (clamped into its edge
-    buckets)."""
+    (p2g_kernel 1), for the three spacing forms, a dense blob (tiles of
+    many chunks, node sums in shared memory) and particles outside the
+    subdomain (clamped into its edge buckets)."""
     from vflip_b200.solver import Solver
 
     rng = np.random.default_rng(29)
@@ -254,8 +261,8 @@ def test_tiled_subdomain_p2g_matches_global_gather():
         rng.shuffle(p)
         cases.append((dims, h, bmin, p))
     dims, h, bmin, p = cases[0]
-    blob = p[:30000].copy()
-    blob["pos"] = (np.array([3.0, 30.0, 12.0]) * h + rng.uniform(-1.5, 1.5, (30000, 3)) * h + bmin).astype(np.float32)
+    blob = np.concatenate([p] * 6)[:100000].copy()
+    blob["pos"] = (np.array([3.0, 30.0, 12.0]) * h + rng.uniform(-1.5, 1.5, (100000, 3)) * h + bmin).astype(np.float32)
     cases.append((dims, h, bmin, np.concatenate([p, blob])))
     for dims, h, bmin, p in cases:
         res = []

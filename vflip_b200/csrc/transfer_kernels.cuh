@@ -322,7 +322,15 @@ __global__ void hash_count_kernel(const ParticleRec* __restrict__ p, int np, int
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) {
     int c = sf.sub ? sub_hash_cell(p[q].pos, ni, nj, nk, h, inv_h, sf) : hash_cell(p[q].pos, ni, nj, nk, h, inv_h);
     cell[q] = c;
-    slot[q] = (c >= 0) ? atomicAdd(count + c, 1) : -1;
+    // the lanes of a warp that share a cell take consecutive slots in lane
+    // (particle) order with one atomic, so a bucket is a few runs of
+    // consecutive particle indices where the particles come in cell order
+    const unsigned grp = __match_any_sync(__activemask(), c);
+    const int lane = threadIdx.x & 31, leader = __ffs(grp) - 1;
+    int base = 0;
+    if (lane == leader && c >= 0) base = atomicAdd(count + c, __popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    slot[q] = (c >= 0) ? base + __popc(grp & ((1u << lane) - 1u)) : -1;
   }
 }
 
@@ -439,44 +447,153 @@ __global__ void sort_buckets_kernel(const int* __restrict__ start, int* __restri
   }
 }
 
-// The listed buckets, one warp each: the particle indices in shared memory,
-// padded with INT_MAX to a power of two, put in ascending order by a
-// bitonic network (within a stage the compare-exchange pairs are disjoint;
-// the warp synchronises between stages).  Particle indices are distinct, so
-// the order is the one the heapsort gives.
-constexpr int kBigWarps = 4;
+// Bitonic sort (ascending) of P keys in shared memory by one warp, P a
+// power of two >= 32; `pay`, when given, moves with the keys.  Within a
+// stage the compare-exchange pairs are disjoint; the warp synchronises
+// between stages.
+__device__ __forceinline__ void warp_bitonic(int* key, int* pay, int P, int lane) {
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < P; i += 32) {
+        const int x = i ^ j;
+        if (x > i) {
+          const int p = key[i], q = key[x];
+          if ((p > q) == ((i & k) == 0)) {
+            key[i] = q;
+            key[x] = p;
+            if (pay) {
+              const int t = pay[i];
+              pay[i] = pay[x];
+              pay[x] = t;
+            }
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// The listed buckets, one warp each, into ascending particle order.  A
+// bucket is read as runs of consecutive particle indices (hash_count_kernel
+// gives a warp's particles of one cell consecutive slots, so particles that
+// come in cell order leave few runs); the runs are disjoint integer ranges,
+// so the bucket in order is the runs sorted by their first index and
+// written out as ranges.  A bucket of more than kBigRuns runs is sorted by
+// a least-significant-digit radix sort of (index - the bucket's smallest)
+// in 8-bit digits, as many passes as that range needs: per pass a
+// shared-memory histogram, its scan, and a stable scatter of 32 entries at
+// a time in order (each entry's rank among the earlier equal digits of its
+// 32 from __match_any_sync).  Particle indices are distinct, so either
+// gives the order the heapsort gives.
+constexpr int kBigWarps = 2;
+constexpr int kBigRuns = 128;
 
 __global__ void __launch_bounds__(32 * kBigWarps) sort_big_buckets_kernel(const int* __restrict__ start,
                                                                        int* __restrict__ order,
                                                                        const int* __restrict__ big,
                                                                        const int* __restrict__ big_n) {
-  __shared__ int sm[kBigWarps][kBigBucket];
+  __shared__ int sm[kBigWarps][2][kBigBucket];
+  __shared__ int hist[kBigWarps][256];
+  __shared__ int rkey[kBigWarps][kBigRuns], rlen[kBigWarps][kBigRuns];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int* v = sm[wid];
+  const unsigned lt = (1u << lane) - 1u;
+  int *v = sm[wid][0], *u = sm[wid][1], *cnt = hist[wid], *rk = rkey[wid], *rl = rlen[wid];
   const int nbig = *big_n;
   for (int e = blockIdx.x * kBigWarps + wid; e < nbig; e += gridDim.x * kBigWarps) {
     const int c = big[e];
     const int b = start[c], m = start[c + 1] - b;
-    int P = 64;
-    while (P < m) P <<= 1;
-    for (int i = lane; i < P; i += 32) v[i] = i < m ? order[b + i] : INT_MAX;
+    int lo = INT_MAX, hi = 0;
+    for (int i = lane; i < m; i += 32) {
+      const int x = order[b + i];
+      v[i] = x;
+      lo = min(lo, x);
+      hi = max(hi, x);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
     __syncwarp();
-    for (int k = 2; k <= P; k <<= 1) {
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        for (int i = lane; i < P; i += 32) {
-          const int x = i ^ j;
-          if (x > i) {
-            const int p = v[i], q = v[x];
-            if ((p > q) == ((i & k) == 0)) {
-              v[i] = q;
-              v[x] = p;
-            }
+    // run heads: position x starts a run unless v[x] == v[x - 1] + 1
+    int nrun = 0;
+    for (int x0 = 0; x0 < m; x0 += 32) {
+      const int x = x0 + lane;
+      const bool head = x < m && (x == 0 || v[x] != v[x - 1] + 1);
+      const unsigned hm = __ballot_sync(0xffffffffu, head);
+      const int idx = nrun + __popc(hm & lt);
+      if (head && idx < kBigRuns) rk[idx] = x;
+      nrun += __popc(hm);
+    }
+    __syncwarp();
+    if (nrun <= kBigRuns) {
+      for (int r = lane; r < nrun; r += 32) rl[r] = (r + 1 < nrun ? rk[r + 1] : m) - rk[r];
+      __syncwarp();
+      int P = 32;
+      while (P < nrun) P <<= 1;
+      for (int r = lane; r < P; r += 32) {
+        if (r < nrun) {
+          rk[r] = v[rk[r]];
+        } else {
+          rk[r] = INT_MAX;
+          rl[r] = 0;
+        }
+      }
+      __syncwarp();
+      warp_bitonic(rk, rl, P, lane);
+      int off = 0;
+      for (int r = 0; r < nrun; ++r) {
+        const int k0 = rk[r], len = rl[r];
+        for (int x = lane; x < len; x += 32) order[b + off + x] = k0 + x;
+        off += len;
+      }
+    } else {
+      const unsigned span = (unsigned)(hi - lo);
+      for (int shift = 0; shift == 0 || (shift < 32 && (span >> shift) != 0u); shift += 8) {
+        for (int d = lane; d < 256; d += 32) cnt[d] = 0;
+        __syncwarp();
+        for (int i = lane; i < m; i += 32) atomicAdd(cnt + ((unsigned)(v[i] - lo) >> shift & 255u), 1);
+        __syncwarp();
+        {  // exclusive scan of the 256 counts, 8 consecutive bins per lane
+          int t[8], sum = 0;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            t[q] = cnt[8 * lane + q];
+            sum += t[q];
+          }
+          int x = sum;
+          for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+          }
+          int pre = x - sum;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            cnt[8 * lane + q] = pre;
+            pre += t[q];
           }
         }
         __syncwarp();
+        for (int x0 = 0; x0 < m; x0 += 32) {
+          const int x = x0 + lane;
+          const bool ok = x < m;
+          const int val = ok ? v[x] : 0;
+          const int d = ok ? (int)((unsigned)(val - lo) >> shift & 255u) : 256;
+          const unsigned peers = __match_any_sync(0xffffffffu, d);
+          const int base = ok ? cnt[d] : 0;
+          if (ok) u[base + __popc(peers & lt)] = val;
+          __syncwarp();
+          if (ok && (peers & lt) == 0u) cnt[d] = base + __popc(peers);
+          __syncwarp();
+        }
+        int* w = v;
+        v = u;
+        u = w;
       }
+      for (int i = lane; i < m; i += 32) order[b + i] = v[i];
+      v = sm[wid][0];
+      u = sm[wid][1];
     }
-    for (int i = lane; i < m; i += 32) order[b + i] = v[i];
     __syncwarp();
   }
 }
@@ -974,35 +1091,10 @@ __global__ void __launch_bounds__(P2gTile<TZ, SUB>::threads, P2gTile<TZ, SUB>::c
   // tent mode (p2g_tent): 2 scales positions and node coordinates by inv_h
   const int mode = inv_h == 0.0f ? 0 : (inv_h >= 1.0f ? 2 : 1);
   const float sc = mode == 2 ? inv_h : 1.0f;
-  const int i = i0 + tid % kP2gTX, j = j0 + (tid / kP2gTX) % kP2gTY, k = k0 + 2 * (tid / (kP2gTX * kP2gTY));
-  const bool on0 = i <= ni && j <= nj && k <= nk, on1 = on0 && k + 1 <= nk;
-  // window half-widths: SubDomainSolver::determineDist, 4 within 4 cells of the boundary
-  auto half = [&](int kk) {
-    if (!SUB) return 1;
-    const int d = min(min(min(i, ni - i), min(j, nj - j)), min(kk, nk - kk));
-    return d <= 4 ? 4 : 1;
-  };
-  const int l0 = half(k), l1 = half(k + 1);
-  P2gNode n0 = p2g_node(i, j, k, ni, nj, nk, h, fu != nullptr, fv != nullptr, fw != nullptr);
-  P2gNode n1 = p2g_node(i, j, k + 1, ni, nj, nk, h, fu != nullptr, fv != nullptr, fw != nullptr);
-  if (mode == 2) {
-    for (P2gNode* n : {&n0, &n1}) {
-      n->xi *= sc;
-      n->xh *= sc;
-      n->yj *= sc;
-      n->yh *= sc;
-      n->zk *= sc;
-      n->zh *= sc;
-    }
-  }
-  // the staged sequence is the row runs in row order (k, then j), and a
-  // node's window is a sub-run of each of its rows, taken in that order:
-  // chunk by chunk, each node adds the part of its window the chunk holds
-  for (int c0 = 0; c0 < total; c0 += cap) {
-    const int c1 = min(c0 + cap, total);
-    __syncthreads();  // the previous chunk is consumed (and cs is written)
-    // each warp copies whole rows, kP2gBatch steps of 32 particles with
-    // their loads in flight before the stores
+  // copy staged indices [c0, c1) into the six arrays (positions scaled by
+  // sc): each warp copies whole rows, kP2gBatch steps of 32 particles with
+  // their loads in flight before the stores
+  auto stage = [&](int c0, int c1, float* qx, float* qy, float* qz, float* wx, float* wy, float* wz) {
     for (int r = tid >> 5; r < nrows; r += T::threads / 32) {
       const int lo = max(roff[r], c0), hi = min(roff[r + 1], c1);
       const int g = rbeg[r] - roff[r];
@@ -1021,16 +1113,48 @@ __global__ void __launch_bounds__(P2gTile<TZ, SUB>::threads, P2gTile<TZ, SUB>::c
           const int s = s0 + 32 * q;
           if (s < hi) {
             const int P = p2g_slot(s - c0);
-            px[P] = a[q].x * sc;
-            py[P] = a[q].y * sc;
-            pz[P] = a[q].z * sc;
-            vx[P] = v[q].x;
-            vy[P] = v[q].y;
-            vz[P] = v[q].z;
+            qx[P] = a[q].x * sc;
+            qy[P] = a[q].y * sc;
+            qz[P] = a[q].z * sc;
+            wx[P] = v[q].x;
+            wy[P] = v[q].y;
+            wz[P] = v[q].z;
           }
         }
       }
     }
+  };
+  auto scale = [&](P2gNode& n) {
+    n.xi *= sc;
+    n.xh *= sc;
+    n.yj *= sc;
+    n.yh *= sc;
+    n.zk *= sc;
+    n.zh *= sc;
+  };
+  // window half-widths: SubDomainSolver::determineDist, 4 within 4 cells of the boundary
+  auto half = [&](int ii, int jj, int kk) {
+    if (!SUB) return 1;
+    const int d = min(min(min(ii, ni - ii), min(jj, nj - jj)), min(kk, nk - kk));
+    return d <= 4 ? 4 : 1;
+  };
+  const bool hu = fu != nullptr, hv = fv != nullptr, hw = fw != nullptr;
+  const int i = i0 + tid % kP2gTX, j = j0 + (tid / kP2gTX) % kP2gTY, k = k0 + 2 * (tid / (kP2gTX * kP2gTY));
+  const bool on0 = i <= ni && j <= nj && k <= nk, on1 = on0 && k + 1 <= nk;
+  const int l0 = half(i, j, k), l1 = half(i, j, k + 1);
+  P2gNode n0 = p2g_node(i, j, k, ni, nj, nk, h, hu, hv, hw);
+  P2gNode n1 = p2g_node(i, j, k + 1, ni, nj, nk, h, hu, hv, hw);
+  if (mode == 2) {
+    scale(n0);
+    scale(n1);
+  }
+  // the staged sequence is the row runs in row order (k, then j), and a
+  // node's window is a sub-run of each of its rows, taken in that order:
+  // chunk by chunk, each node adds the part of its window the chunk holds
+  for (int c0 = 0; c0 < total; c0 += cap) {
+    const int c1 = min(c0 + cap, total);
+    __syncthreads();  // the previous chunk is consumed (and cs is written)
+    stage(c0, c1, px, py, pz, vx, vy, vz);
     __syncthreads();
     if (!on0) continue;
     const P2gStage g{cs, S, clo, cjlo, cklo, nry, c0, c1, px, py, pz, vx, vy, vz};
