@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds for the reference arm's timed steps")
     ap.add_argument("--kernels", default=None,
                     help="instead of the step: per-kernel timings (comma list of advect, p2g, g2p, vcycle, unet, "
-                         "hostlink) at --n, "
+                         "hostlink, nested) at --n, "
                          "one JSON line each")
     ap.add_argument("--reps", type=int, default=5, help="timed repetitions per kernel (--kernels)")
     ap.add_argument("--unet-sizes", type=int, nargs="+", default=[32, 64, 128], help="network grids (--kernels unet)")
@@ -958,8 +958,19 @@ def kernel_lines(a):
                 parts = T(np.ascontiguousarray(part[idx]).view(np.uint8))
                 if "p2g" in what:
                     ms = timed(lambda: s.particle_to_grid(n, n, n, h, parts))
+                    # the split, from CUDA events around the bucketing and the
+                    # gathers of one more call; the gathers' algorithmic bytes:
+                    # the sorted positions and velocities read once (32 B per
+                    # particle), six floats written per node index
+                    s.set_profiling(True)
+                    s.particle_to_grid(n, n, n, h, parts)
+                    sort_ms = s.profile_kernels("p2g_sort")[1]
+                    gather_ms = s.profile_kernels("p2g_gather")[1]
+                    s.set_profiling(False)
+                    gather_bytes = npart * 32 + 24 * (n + 1) ** 3
                     line(f"p2g (hash, sort, p2g3_kernel), particles in {order}", ms, npart * 24 + 24 * n ** 3,
-                         particles=npart)
+                         particles=npart, sort_ms=sort_ms, gather_ms=gather_ms,
+                         gather_hbm_frac=gather_bytes / (gather_ms * 1e-3) / 1e9 / peak)
                 if "g2p" in what:
                     ms = timed(lambda: s.particle_from_grid(n, n, n, h, parts, du, dv, dw))
                     line(f"g2p_kernel, particles in {order}", ms, npart * 24 + 12 * n ** 3, particles=npart)
@@ -970,6 +981,35 @@ def kernel_lines(a):
         unet_lines(a)
     if "hostlink" in what:
         hostlink_lines(a)
+    if "nested" in what:
+        nested_lines(a)
+
+
+def nested_lines(a):
+    """The nested arm's step (128^3 plume, 256^3 subdomain at 4x, mixed
+    precision) alone: 3 warm-up steps, then --reps steps, each with its
+    P2G split (CUDA events around the bucketing and the gathers)."""
+    import torch
+
+    from vflip_b200.flip import NestedFlipSim, NestedParams
+    from vflip_b200.solver import Solver
+
+    with Solver(precision=PREC["mixed"]) as s:
+        sim = NestedFlipSim(s, NestedParams(n=128, dt=0.005, obstacle_radius=0.0, ratio=4))
+        for _ in range(3):
+            sim.step()
+        for _ in range(a.reps):
+            s.set_profiling(True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            sim.step()
+            e1.record()
+            torch.cuda.synchronize()
+            print(json.dumps({"kernel": "nested step (128^3 + 256^3 subdomain at 4x)", "ms": e0.elapsed_time(e1),
+                              "p2g_sort_ms": s.profile_kernels("p2g_sort")[1],
+                              "p2g_gather_ms": s.profile_kernels("p2g_gather")[1],
+                              "particles_main_pass": sim.num_particles + sim.num_sub_particles}), flush=True)
+            s.set_profiling(False)
 
 
 def hostlink_lines(a):
