@@ -938,12 +938,15 @@ def kernel_lines(a):
             u, v, w = (T(x) for x in vel)
             outs = tuple(torch.empty_like(x) for x in (u, v, w))
             ms = timed(lambda: s.advect_velocity_rk2_linear(n, n, n, h, 0.01, u, v, w, outs=outs))
-            line("advect_rk2_kernel x3 (u, v, w)", ms, 24 * n ** 3)
+            gen = solver_opts(a).get("advect_kernel", 0) == 1
+            line("advect_rk2_f_kernel x3 (u, v, w)" if gen else "advect_rk2_node_kernel (u, v, w, one launch)", ms,
+                 24 * n ** 3)
             rho = T(rng.standard_normal((n, n, n)).astype(np.float32))
             tmp = T(rng.standard_normal((n, n, n)).astype(np.float32))
             o1, o2 = torch.empty_like(rho), torch.empty_like(tmp)
             ms = timed(lambda: s.advect_rk2_linear2(n, n, n, h, 0.01, u, v, w, rho, tmp, (0, 0, 0), out=o1, out2=o2))
-            line("advect_rk2_kernel (density + temperature pair)", ms, 28 * n ** 3)
+            line(("advect_rk2_f_kernel" if gen else "advect_rk2_node_kernel") + " (density + temperature pair)", ms,
+                 28 * n ** 3)
         if "p2g" in what or "g2p" in what:
             part = scenes.jittered_particles(n, n, n, h, 8, rng)
             part["vel"] = rng.standard_normal((len(part), 3)).astype(np.float32)

@@ -147,6 +147,13 @@ typedef struct {
    * its threads gather from there, two nodes each; 3 = the same with
    * 8 x 8 x 4 tiles, two CTAs per SM.  Same bits. */
   int p2g_kernel;
+  /* RK2 trilinear advection in FP32/MIXED contexts: 0 (default) =
+   * automatic: when h is a power of two and the field lies on the u, v, w or
+   * cell-centre lattice, the backtrace's first stage is read straight from
+   * the node's neighbours (its axis fractions are exactly 0 or 1/2) and
+   * u, v, w advect in one launch; otherwise as 1; 1 = every sample through
+   * the general trilinear transform, one launch per field.  Same bits. */
+  int advect_kernel;
 } vflip_config;
 
 typedef struct {

@@ -1,5 +1,6 @@
 """Entry points and kernel variants that must agree with the ones they stand for:
   * the one-call u, v, w advection gives the three single calls' bits;
+  * the node-specialised RK2 advection gives the general kernel's bits;
   * the plane-marching PCG SpMV gives the column kernel's iterations and,
     up to the grouping of its s.q partial sums, its solution;
   * the one-CTA V-cycle tail gives the per-level launches' bits;
@@ -47,6 +48,38 @@ def test_velocity_advection_one_call(prec, dims):
         got = s.advect_velocity_rk2_linear(ni, nj, nk, h, 0.03, U, V, W)
         for name, f, o, g in zip("uvw", (U, V, W), ((0.5, 0, 0), (0, 0.5, 0), (0, 0, 0.5)), got):
             assert torch.equal(g, s.advect_rk2_linear(ni, nj, nk, h, 0.03, U, V, W, f, o)), name
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+@pytest.mark.parametrize("dims", [(64, 48, 40), (5, 9, 70), (128, 1, 3)])
+def test_node_advection_matches_general_kernel(prec, dims):
+    """With h a power of two, the node-specialised RK2 advection
+    (advect_kernel 0: the first stage read from the node's neighbours, u, v,
+    w in one launch) gives the general per-sample kernel's bits
+    (advect_kernel 1) on every lattice and for the field pair, including
+    velocities of +0 and -0 and backtraces that leave the grid."""
+    from vflip_b200.solver import Solver
+
+    ni, nj, nk = dims
+    h = np.float32(1.0 / 64)
+    vel = smooth_velocity(ni, nj, nk, 2.0, seed=7)
+    for a, z in zip(vel, (0.0, -0.0, 0.0)):
+        a[:, :, :2] = z
+        a[: max(1, a.shape[0] // 3)] *= -1
+    U, V, W = (t(x) for x in vel)
+    rng = np.random.default_rng(3)
+    rho, temp = (t(rng.standard_normal((nk, nj, ni)).astype(np.float32)) for _ in range(2))
+    offs = ((0.5, 0, 0), (0, 0.5, 0), (0, 0, 0.5), (0, 0, 0))
+    res = []
+    for kern in (0, 1):
+        with Solver(precision=prec, advect_kernel=kern) as s:
+            got = list(s.advect_velocity_rk2_linear(ni, nj, nk, h, 0.03, U, V, W))
+            for f, o in zip((U, V, W), offs):
+                got.append(s.advect_rk2_linear(ni, nj, nk, h, 0.03, U, V, W, f, o))
+            got += list(s.advect_rk2_linear2(ni, nj, nk, h, 0.03, U, V, W, rho, temp, offs[3]))
+            res.append(got)
+    for i, (a, b) in enumerate(zip(*res)):
+        assert torch.equal(a.view(torch.int32), b.view(torch.int32)), i
 
 
 @pytest.mark.parametrize("prec", [1, 2, 0])

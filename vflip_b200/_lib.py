@@ -35,7 +35,8 @@ class ConfigC(C.Structure):
                 ("smoother_prefetch", C.c_int), ("coarsest_solver", C.c_int), ("spmv_kernel", C.c_int),
                 ("pcg_loop", C.c_int), ("pcg_vectors", C.c_int), ("batch_chunk", C.c_int),
                 ("batch_ctas_per_sm", C.c_int), ("coarse_tail", C.c_int),
-                ("tile_sweep_max_cells", C.c_int), ("p2g_kernel", C.c_int)]
+                ("tile_sweep_max_cells", C.c_int), ("p2g_kernel", C.c_int),
+                ("advect_kernel", C.c_int)]
 
 
 class SystemC(C.Structure):

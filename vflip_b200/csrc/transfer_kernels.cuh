@@ -254,6 +254,165 @@ __global__ void advect_rk2_f_kernel(const float* __restrict__ u, const float* __
   }
 }
 
+// ---- the FP32 form again (the same values), specialised to lattice nodes
+// when h is a power of two.  A node of the u, v, w or cell-centre lattice
+// sits at whole or half-cell coordinates of every MAC velocity grid, so the
+// backtrace's first stage (the velocity at the node itself) has axis
+// fractions of exactly 0 or 1/2: along an axis where the node and the
+// sampled component share their staggering the fraction is 0 and the lerp
+// keeps its first corner (lerp_f(a, b, 0) == a for finite values; only the
+// sign of a zero can differ, and a zero velocity's sign cannot change
+// x - (dt/2) a); where they differ the fraction is 1/2 and the corners are
+// (i, i+1) for a staggered component at an unstaggered node, or
+// (clamp(i-1), clamp(i)) the other way round.  That stage then reads 9
+// values (u-, v-, w-faces) or 6 (cell centres) instead of 24, with no
+// coordinate transform; the node's world position is formed in float
+// ((i - o) h is exact for a power-of-two h), and node indices are carried
+// along the block's run instead of divided out.  The midpoint and final
+// samples are advect_rk2_f_kernel's, so outputs are bit for bit its own.
+
+// sampled component C at a node of lattice G (0..2: u, v, w faces, 3: cell
+// centres), along axis A: 0 = same staggering, 1 = (i, i+1), 2 = (i-1, i)
+__host__ __device__ constexpr int node_axis_mode(int C, int A, int G) {
+  return (C == A && G != A) ? 1 : ((C != A && G == A) ? 2 : 0);
+}
+
+template <int M>
+__device__ __forceinline__ void node_pair(int i, int n, int& a, int& b) {
+  if (M == 2) {
+    a = i > 0 ? i - 1 : 0;
+    b = i < n - 1 ? i : n - 1;
+  } else {
+    a = i;
+    b = i + 1;
+  }
+}
+
+// component C (extent ni+[C==0], nj+[C==1], nk+[C==2]) at node (i,j,k) of G
+template <int C, int G>
+__device__ __forceinline__ float node_velocity(const float* __restrict__ d, int ni, int nj, int nk, int i, int j,
+                                               int k) {
+  constexpr int MX = node_axis_mode(C, 0, G), MY = node_axis_mode(C, 1, G), MZ = node_axis_mode(C, 2, G);
+  const int nx = ni + (C == 0), ny = nj + (C == 1), nz = nk + (C == 2);
+  const int sy = nx, sz = nx * ny;
+  int i0, i1, j0, j1, k0, k1;
+  node_pair<MX>(i, nx, i0, i1);
+  node_pair<MY>(j, ny, j0, j1);
+  node_pair<MZ>(k, nz, k0, k1);
+  j0 *= sy;
+  j1 *= sy;
+  k0 *= sz;
+  k1 *= sz;
+  auto X = [&](int jk) -> float {
+    if constexpr (MX == 0) return __ldg(d + (i0 + jk));
+    else return lerp_f(__ldg(d + (i0 + jk)), __ldg(d + (i1 + jk)), 0.5f);
+  };
+  auto Y = [&](int kk) -> float {
+    if constexpr (MY == 0) return X(j0 + kk);
+    else return lerp_f(X(j0 + kk), X(j1 + kk), 0.5f);
+  };
+  if constexpr (MZ == 0) return Y(k0);
+  else return lerp_f(Y(k0), Y(k1), 0.5f);
+}
+
+__device__ __forceinline__ void node_advance(int& i, int& j, int& k, int by, int nx, int ny) {
+  i += by;
+  while (i >= nx) {
+    i -= nx;
+    if (++j == ny) {
+      j = 0;
+      ++k;
+    }
+  }
+}
+
+struct NodeJob {
+  const float* f;  // field on lattice G and its output
+  float* out;
+  const float* f2;  // optional second field on the same lattice (nullptr: none)
+  float* out2;
+};
+
+struct NodeJobs {
+  NodeJob j[3];
+};
+
+template <int G>
+__device__ __forceinline__ void advect_nodes(const float* __restrict__ u, const float* __restrict__ v,
+                                             const float* __restrict__ w, int ni, int nj, int nk, float ih, float h,
+                                             float dt, const NodeJob& job, unsigned blk, int per_block) {
+  const int nx = ni + (G == 0), ny = nj + (G == 1), nz = nk + (G == 2);
+  const float ox = G == 0 ? 0.5f : 0.0f, oy = G == 1 ? 0.5f : 0.0f, oz = G == 2 ? 0.5f : 0.0f;
+  const GridF ff{job.f, nx, ny, nz, ox, oy, oz}, ff2{job.f2, nx, ny, nz, ox, oy, oz};
+  float* __restrict__ out = job.out;
+  float* __restrict__ out2 = job.out2;
+  const size_t n = (size_t)nx * ny * nz;
+  const int stride = blockDim.x;
+  const size_t beg = (size_t)blk * per_block;
+  if (beg >= n) return;
+  const size_t end = beg + per_block < n ? beg + per_block : n;
+  const float hf = 0.5f * dt;
+  int i, j, k;
+  decode3(beg + threadIdx.x, nx, ny, i, j, k);
+  for (size_t e0 = beg + threadIdx.x; e0 < end; e0 += 2 * (size_t)stride) {
+    const size_t e1 = e0 + stride;
+    const bool two = e1 < end;
+    int i1 = i, j1 = j, k1 = k;
+    node_advance(i1, j1, k1, stride, nx, ny);
+    const float wx0 = ((float)i - ox) * h, wy0 = ((float)j - oy) * h, wz0 = ((float)k - oz) * h;
+    const float wx1 = two ? ((float)i1 - ox) * h : 0.0f, wy1 = two ? ((float)j1 - oy) * h : 0.0f,
+                wz1 = two ? ((float)k1 - oz) * h : 0.0f;
+    float a0 = node_velocity<0, G>(u, ni, nj, nk, i, j, k), b0 = node_velocity<1, G>(v, ni, nj, nk, i, j, k),
+          c0 = node_velocity<2, G>(w, ni, nj, nk, i, j, k);
+    float a1 = 0, b1 = 0, c1 = 0;
+    if (two) {
+      a1 = node_velocity<0, G>(u, ni, nj, nk, i1, j1, k1);
+      b1 = node_velocity<1, G>(v, ni, nj, nk, i1, j1, k1);
+      c1 = node_velocity<2, G>(w, ni, nj, nk, i1, j1, k1);
+    }
+    float px0 = wx0 - hf * a0, py0 = wy0 - hf * b0, pz0 = wz0 - hf * c0;
+    float px1 = wx1 - hf * a1, py1 = wy1 - hf * b1, pz1 = wz1 - hf * c1;
+    mac_f(u, v, w, ni, nj, nk, ih, px0, py0, pz0, a0, b0, c0);
+    if (two) mac_f(u, v, w, ni, nj, nk, ih, px1, py1, pz1, a1, b1, c1);
+    px0 = wx0 - dt * a0;
+    py0 = wy0 - dt * b0;
+    pz0 = wz0 - dt * c0;
+    px1 = wx1 - dt * a1;
+    py1 = wy1 - dt * b1;
+    pz1 = wz1 - dt * c1;
+    out[e0] = grid_f(ff, ih, px0, py0, pz0);
+    if (out2) out2[e0] = grid_f(ff2, ih, px0, py0, pz0);
+    if (two) {
+      out[e1] = grid_f(ff, ih, px1, py1, pz1);
+      if (out2) out2[e1] = grid_f(ff2, ih, px1, py1, pz1);
+    }
+    i = i1;
+    j = j1;
+    k = k1;
+    node_advance(i, j, k, stride, nx, ny);
+  }
+}
+
+// Block b runs job b % njobs on run b / njobs of its lattice, g0 + job (one
+// launch advects u, v and w with g0 = 0 and three jobs, or one lattice's
+// field or field pair with a single job).  Interleaving the jobs block by
+// block keeps the three components' blocks in flight over the same region,
+// so the velocity they all sample is read from DRAM about once.
+__global__ void __launch_bounds__(256) advect_rk2_node_kernel(const float* __restrict__ u,
+                                                              const float* __restrict__ v,
+                                                              const float* __restrict__ w, int ni, int nj, int nk,
+                                                              float ih, float h, float dt, NodeJobs jobs, int g0,
+                                                              int njobs, int per_block) {
+  const unsigned q = blockIdx.x % (unsigned)njobs, blk = blockIdx.x / (unsigned)njobs;
+  const NodeJob job = q == 0 ? jobs.j[0] : (q == 1 ? jobs.j[1] : jobs.j[2]);
+  switch (g0 + (int)q) {
+    case 0: advect_nodes<0>(u, v, w, ni, nj, nk, ih, h, dt, job, blk, per_block); break;
+    case 1: advect_nodes<1>(u, v, w, ni, nj, nk, ih, h, dt, job, blk, per_block); break;
+    case 2: advect_nodes<2>(u, v, w, ni, nj, nk, ih, h, dt, job, blk, per_block); break;
+    default: advect_nodes<3>(u, v, w, ni, nj, nk, ih, h, dt, job, blk, per_block); break;
+  }
+}
+
 // getDelta, Smoke_solver3D.cpp:1298-1319
 __global__ void delta_kernel(const float* __restrict__ after, const float* __restrict__ before,
                              float* __restrict__ delta, size_t n) {

@@ -2442,6 +2442,7 @@ void vflip_config_default(vflip_config* cfg) {
   cfg->coarse_tail = 0;
   cfg->tile_sweep_max_cells = 0;
   cfg->p2g_kernel = 0;
+  cfg->advect_kernel = 0;
 }
 
 int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
@@ -2476,7 +2477,8 @@ int vflip_create(vflip_ctx** out, const vflip_config* cfg) {
       ctx->cfg.spmv_kernel > 1 ||
       ctx->cfg.pcg_loop < 0 || ctx->cfg.pcg_loop > 1 || ctx->cfg.pcg_vectors < 0 || ctx->cfg.pcg_vectors > 1 || ctx->cfg.batch_chunk < 0 || ctx->cfg.batch_ctas_per_sm < 0 ||
       ctx->cfg.coarse_tail < 0 || ctx->cfg.coarse_tail > 1 || ctx->cfg.tile_sweep_max_cells < -1 ||
-      ctx->cfg.p2g_kernel < 0 || ctx->cfg.p2g_kernel > 3)
+      ctx->cfg.p2g_kernel < 0 || ctx->cfg.p2g_kernel > 3 || ctx->cfg.advect_kernel < 0 ||
+      ctx->cfg.advect_kernel > 1)
     return bad(VFLIP_ERR_ARG);
   if (ctx->cfg.tile_sweep_max_cells == 0) ctx->cfg.tile_sweep_max_cells = 64 * 64 * 64;
   if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return bad(VFLIP_ERR_CUDA);
@@ -2973,6 +2975,21 @@ int vflip_project_learned(vflip_ctx* ctx, vflip_unet* net, int mode, int level, 
                       tolerance_factor, max_iterations, stats, &lo);
 }
 
+namespace {
+// The lattice (0..2: u, v, w faces, 3: cell centres) of an ni x nj x nk MAC
+// grid that a field of fnx x fny x fnz nodes at grid offsets (ox, oy, oz)
+// lies on, or -1.
+int node_lattice(int ni, int nj, int nk, int fnx, int fny, int fnz, double ox, double oy, double oz) {
+  // (float)i - 0.5f is exact below 2^22
+  if (std::max(ni, std::max(nj, nk)) >= (1 << 22)) return -1;
+  for (int g = 0; g < 4; ++g)
+    if (fnx == ni + (g == 0) && fny == nj + (g == 1) && fnz == nk + (g == 2) && ox == (g == 0 ? 0.5 : 0.0) &&
+        oy == (g == 1 ? 0.5 : 0.0) && oz == (g == 2 ? 0.5 : 0.0))
+      return g;
+  return -1;
+}
+}  // namespace
+
 int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, float dt, const float* u,
                              const float* v, const float* w, int fnx, int fny, int fnz, double ox, double oy,
                              double oz, const float* field, float* out, const float* field2, float* out2) {
@@ -2998,7 +3015,12 @@ int vflip_advect_rk2_linear2(vflip_ctx* ctx, int ni, int nj, int nk, float h, fl
   if (ctx->cfg.precision == VFLIP_PREC_FP64)
     advect_rk2_kernel<true><<<blocks, 256, 0, ctx->stream>>>(gu, gv, gw, gf, out, gf2, field2 ? out2 : nullptr, h, dt,
                                                            per_block);
-  else {
+  else if (ih != 0.0 && ctx->cfg.advect_kernel == 0 && node_lattice(ni, nj, nk, fnx, fny, fnz, ox, oy, oz) >= 0) {
+    // the field lies on a lattice whose nodes the first stage reads directly
+    const NodeJobs jobs{{NodeJob{field, out, field2, field2 ? out2 : nullptr}, NodeJob{}, NodeJob{}}};
+    advect_rk2_node_kernel<<<blocks, 256, 0, ctx->stream>>>(
+        u, v, w, ni, nj, nk, (float)ih, h, dt, jobs, node_lattice(ni, nj, nk, fnx, fny, fnz, ox, oy, oz), 1, per_block);
+  } else {
     // sample_linear_f's float transform, computed once
     const float ihf = (float)(ih != 0.0 ? ih : 1.0 / (double)h);
     const GridF ff{field, fnx, fny, fnz, (float)ox, (float)oy, (float)oz};
@@ -3026,6 +3048,23 @@ int vflip_advect_velocity_rk2_linear(vflip_ctx* ctx, int ni, int nj, int nk, flo
   for (const float* o : {(const float*)uo, (const float*)vo, (const float*)wo})
     if (o == u || o == v || o == w) return ctx->fail(VFLIP_ERR_ARG, "an output aliases the velocity");
   if (uo == vo || uo == wo || vo == wo) return ctx->fail(VFLIP_ERR_ARG, "outputs alias each other");
+  const double ih = inv_pow2(h);
+  if (ctx->cfg.precision != VFLIP_PREC_FP64 && ctx->cfg.advect_kernel == 0 && ih != 0.0 &&
+      node_lattice(ni, nj, nk, ni, nj, nk, 0.0, 0.0, 0.0) == 3) {
+    // one launch: blocks 3b, 3b+1, 3b+2 advect run b of u, v and w
+    const int per_block = 256 * 8;
+    size_t most = 0;
+    for (size_t c : {(size_t)(ni + 1) * nj * nk, (size_t)ni * (nj + 1) * nk, (size_t)ni * nj * (nk + 1)})
+      most = std::max(most, c);
+    const NodeJobs jobs{{NodeJob{u, uo, nullptr, nullptr}, NodeJob{v, vo, nullptr, nullptr},
+                         NodeJob{w, wo, nullptr, nullptr}}};
+    const int slot = prof_start(ctx, VFLIP_PROF_ADVECT_FIELD, ctx->stream);
+    advect_rk2_node_kernel<<<3 * (unsigned)((most + per_block - 1) / per_block), 256, 0, ctx->stream>>>(
+        u, v, w, ni, nj, nk, (float)ih, h, dt, jobs, 0, 3, per_block);
+    prof_stop(ctx, slot, ctx->stream);
+    VF_LAUNCH_CHECK();
+    return VFLIP_OK;
+  }
   if ((rc = vflip_advect_rk2_linear(ctx, ni, nj, nk, h, dt, u, v, w, ni + 1, nj, nk, 0.5, 0.0, 0.0, u, uo)) ||
       (rc = vflip_advect_rk2_linear(ctx, ni, nj, nk, h, dt, u, v, w, ni, nj + 1, nk, 0.0, 0.5, 0.0, v, vo)) ||
       (rc = vflip_advect_rk2_linear(ctx, ni, nj, nk, h, dt, u, v, w, ni, nj, nk + 1, 0.0, 0.0, 0.5, w, wo)))

@@ -70,7 +70,7 @@ class Solver:
                  smoother_plane_ranges=0, smoother_ctas_per_sm=0, smoother_threads=0,
                  smoother_prefetch=0, coarsest_solver=0, spmv_kernel=0, pcg_loop=0, pcg_vectors=0,
                  batch_chunk=0, batch_ctas_per_sm=0, coarse_tail=0, tile_sweep_max_cells=0,
-                 p2g_kernel=0):
+                 p2g_kernel=0, advect_kernel=0):
         self.lib = load()
         cfg = ConfigC()
         self.lib.vflip_config_default(C.byref(cfg))
@@ -96,6 +96,7 @@ class Solver:
         cfg.coarse_tail = coarse_tail
         cfg.tile_sweep_max_cells = tile_sweep_max_cells
         cfg.p2g_kernel = p2g_kernel
+        cfg.advect_kernel = advect_kernel
         self.device = torch.device("cuda", device)
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
