@@ -216,55 +216,52 @@ __global__ void assemble_kernel(const float* __restrict__ u, const float* __rest
 // variant 1 (SubDomainSolver::pcg_projection, sub_domain.cpp:741-818):
 // faces i in [1, ni-1] (all faces between cells of the grid) and
 // u -= dt * (float)(p_i - p_{i-1}) / h.
+// One thread per cell (i, j, k) updates the three faces with that index
+// (u(i,j,k), v(i,j,k), w(i,j,k)): every face the update touches has an index
+// inside the cell range, the cell's own pressure is read once for all three,
+// and the neighbours' (i-1, j-1, k-1) come from the lines the adjacent
+// threads, rows and planes just read.  A face's solid velocity is read only
+// where its weight is not positive and its velocity only where it is.
 template <typename P>
-__global__ void gradient_kernel(const P* __restrict__ p, float* __restrict__ u, float* __restrict__ v,
-                                float* __restrict__ w, const float* __restrict__ uw, const float* __restrict__ vw,
-                                const float* __restrict__ ww, const float* __restrict__ us,
-                                const float* __restrict__ vs, const float* __restrict__ ws, float h, int ni, int nj,
-                                int nk, int variant, float dt, float inv_h) {
-  const size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
+__global__ void gradient3_kernel(const P* __restrict__ p, float* __restrict__ u, float* __restrict__ v,
+                                 float* __restrict__ w, const float* __restrict__ uw, const float* __restrict__ vw,
+                                 const float* __restrict__ ww, const float* __restrict__ us,
+                                 const float* __restrict__ vs, const float* __restrict__ ws, float h, int ni, int nj,
+                                 int nk, int variant, float dt, float inv_h) {
+  const size_t n = (size_t)ni * nj * nk;
   const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
-  // two faces per thread and round, both faces' loads in flight at once
-  auto face = [&](size_t e) {
-    const bool sub = variant == 1;
-    const int lo = sub ? 0 : 1;  // first face index excluded: faces > lo
-    const int hi = sub ? 0 : 1;  // faces < n - hi
-    auto upd = [&](float cur, double pc, double pm, float wgt, float solid) {
-      if (!(wgt > 0)) return solid;
-      float diff = (float)(pc - pm);
-      // x / h as x * (1/h) when h is a power of two (inv_h != 0): the same bits
-      const float q = sub ? dt * diff : diff;
-      return cur - (inv_h != 0.0f ? q * inv_h : q / h);
-    };
-    if (e < nu) {
-      int i, j, k;
-      decode3(e, ni + 1, nj, i, j, k);
-      if (k < nk - 1 && k > 0 && j < nj - 1 && j > 0 && i < ni - hi && i > lo) {
-        size_t c = lin3(i, j, k, ni, nj);
-        u[e] = upd(u[e], (double)p[c], (double)p[c - 1], uw[e], us[e]);
-      }
-    } else if (e < nu + nv) {
-      size_t f = e - nu;
-      int i, j, k;
-      decode3(f, ni, nj + 1, i, j, k);
-      if (k < nk - 1 && k > 0 && j > lo && j < nj - hi && i < ni - 1 && i > 0) {
-        size_t c = lin3(i, j, k, ni, nj);
-        v[f] = upd(v[f], (double)p[c], (double)p[c - sy], vw[f], vs[f]);
-      }
-    } else {
-      size_t f = e - nu - nv;
-      int i, j, k;
-      decode3(f, ni, nj, i, j, k);
-      if (k > lo && k < nk - hi && j < nj - 1 && j > 0 && i < ni - 1 && i > 0) {
-        size_t c = lin3(i, j, k, ni, nj);
-        w[f] = upd(w[f], (double)p[c], (double)p[c - sz], ww[f], ws[f]);
-      }
-    }
+  const bool sub = variant == 1;
+  const int lo = sub ? 0 : 1;  // first face index excluded: faces > lo
+  const int hi = sub ? 0 : 1;  // faces < n - hi
+  auto upd = [&](float cur, double pc, double pm) {
+    float diff = (float)(pc - pm);
+    // x / h as x * (1/h) when h is a power of two (inv_h != 0): the same bits
+    const float q = sub ? dt * diff : diff;
+    return cur - (inv_h != 0.0f ? q * inv_h : q / h);
   };
-  const size_t nf = nu + nv + nw, stride = (size_t)gridDim.x * blockDim.x;
-  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < nf; e += 2 * stride) {
-    face(e);
-    if (e + stride < nf) face(e + stride);
+  auto cell = [&](size_t c) {
+    int i, j, k;
+    decode3(c, ni, nj, i, j, k);
+    const bool jin = j < nj - 1 && j > 0, kin = k < nk - 1 && k > 0, iin = i < ni - 1 && i > 0;
+    const bool fu = kin && jin && i < ni - hi && i > lo;
+    const bool fv = kin && j > lo && j < nj - hi && iin;
+    const bool fw = k > lo && k < nk - hi && jin && iin;
+    if (!(fu || fv || fw)) return;
+    const size_t eu = lin3(i, j, k, ni + 1, nj), ev = lin3(i, j, k, ni, nj + 1), ew = c;
+    // the weights, velocities and pressures of the three faces in flight at once
+    const float wu = fu ? uw[eu] : 0.0f, wv = fv ? vw[ev] : 0.0f, wwt = fw ? ww[ew] : 0.0f;
+    const float cu = fu ? u[eu] : 0.0f, cv = fv ? v[ev] : 0.0f, cw = fw ? w[ew] : 0.0f;
+    const double pc = (double)p[c];
+    const double pu = fu ? (double)p[c - 1] : 0.0, pv = fv ? (double)p[c - sy] : 0.0,
+                 pw = fw ? (double)p[c - sz] : 0.0;
+    if (fu) u[eu] = wu > 0 ? upd(cu, pc, pu) : us[eu];
+    if (fv) v[ev] = wv > 0 ? upd(cv, pc, pv) : vs[ev];
+    if (fw) w[ew] = wwt > 0 ? upd(cw, pc, pw) : ws[ew];
+  };
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += 2 * stride) {
+    cell(c);
+    if (c + stride < n) cell(c + stride);
   }
 }
 

@@ -2800,7 +2800,7 @@ int project_impl(vflip_ctx* ctx, int variant, int ni, int nj, int nk, float h, f
   }
   size_t nu = (size_t)(ni + 1) * nj * nk, nv = (size_t)ni * (nj + 1) * nk, nw = (size_t)ni * nj * (nk + 1);
   float* wts = (float*)ctx->buf("face_weights", sizeof(float) * (nu + nv + nw));
-  gradient_kernel<double><<<grid_for(nu + nv + nw, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
+  gradient3_kernel<double><<<grid_for(n, 256, ctx->num_sms), 256, 0, ctx->stream>>>(
       p, u, v, w, wts, wts + nu, wts + nu + nv, us, vs, ws, h, ni, nj, nk, variant, dt, (float)inv_pow2(h));
   ++ctx->launches;
   cudaError_t le = cudaGetLastError();
