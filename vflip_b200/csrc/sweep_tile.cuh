@@ -52,11 +52,17 @@ __global__ void __launch_bounds__(kTileThreads) rbgs_sweep_tile_kernel(const Swe
   const int ti = t % a.ntx, tj = (t / a.ntx) % a.nty, tk = t / (a.ntx * a.nty);
   // region origin: the tile's first cell minus the two-cell halo
   const int oi = ti * kTileTX - 2, oj = tj * kTileTY - 2, ok = tk * kTileTZ - 2;
-  for (int e = threadIdx.x; e < kTileRegion; e += kTileThreads) {
+  // staging: every load of the thread's region cells is issued before the
+  // first shared-memory store (one round of L2 latency, not one per cell)
+  constexpr int kIt = (kTileRegion + kTileThreads - 1) / kTileThreads;
+  A xv[kIt], bv[kIt], dv[kIt], cxv[kIt], cyv[kIt], czv[kIt];
+#pragma unroll
+  for (int q = 0; q < kIt; ++q) {
+    const int e = threadIdx.x + q * kTileThreads;
     const int ri = e % kTileRX, rj = (e / kTileRX) % kTileRY, rk = e / (kTileRX * kTileRY);
     const int i = oi + ri, j = oj + rj, k = ok + rk;
     A x = A(0), bb = A(0), d = A(0), cx = A(0), cy = A(0), cz = A(0);
-    if (i >= 0 && i < ni && j >= 0 && j < nj && k >= 0 && k < nk) {
+    if (e < kTileRegion && i >= 0 && i < ni && j >= 0 && j < nj && k >= 0 && k < nk) {
       const size_t g = (size_t)i + sy * j + sz * k;
       if (!ZERO) {
         x = ldv(a.x_in + g);
@@ -68,12 +74,24 @@ __global__ void __launch_bounds__(kTileThreads) rbgs_sweep_tile_kernel(const Swe
       cy = A(ldv(a.yp + g));
       cz = A(ldv(a.zp + g));
     }
-    xs[e] = x;
-    bs[e] = bb;
-    ds[e] = d;
-    xps[e] = cx;
-    yps[e] = cy;
-    zps[e] = cz;
+    xv[q] = x;
+    bv[q] = bb;
+    dv[q] = d;
+    cxv[q] = cx;
+    cyv[q] = cy;
+    czv[q] = cz;
+  }
+#pragma unroll
+  for (int q = 0; q < kIt; ++q) {
+    const int e = threadIdx.x + q * kTileThreads;
+    if (e < kTileRegion) {
+      xs[e] = xv[q];
+      bs[e] = bv[q];
+      ds[e] = dv[q];
+      xps[e] = cxv[q];
+      yps[e] = cyv[q];
+      zps[e] = czv[q];
+    }
   }
   __syncthreads();
   constexpr int SY = kTileRX, SZ = kTileRX * kTileRY;
