@@ -123,28 +123,50 @@ __device__ double batch_sweep(const BatchLevel<S, V>& L, const V* x_in, V* x_out
   const int ni = L.ni, nj = L.nj, nk = L.nk;
   const size_t sy = (size_t)ni, sz = (size_t)ni * nj;
   const int oi = ti * kBTX - 2, oj = tj * kBTY - 2, ok = tk * kBTZ - 2;
-  for (int e = threadIdx.x; e < kBRegion; e += kBatchThreads) {
-    const int ri = e % kBRX, rj = (e / kBRX) % kBRY, rk = e / (kBRX * kBRY);
-    const int i = oi + ri, j = oj + rj, k = ok + rk;
-    A x = A(0), bb = A(0), d = A(0), cx = A(0), cy = A(0), cz = A(0);
-    if (i >= 0 && i < ni && j >= 0 && j < nj && k >= 0 && k < nk) {
-      const size_t g = (size_t)i + sy * j + sz * k;
-      if (!ZERO) {
-        x = ldcg(x_in + g);
-        if (PROLONG) x = x + ldcg(xc + lin3(i >> 1, j >> 1, k >> 1, cni, cnj));
+  // the staging loads are issued kGrp cells at a time before their
+  // shared-memory stores (a few rounds of memory latency, not one per cell;
+  // groups keep the registers of this persistent kernel in bounds)
+  constexpr int kIt = (kBRegion + kBatchThreads - 1) / kBatchThreads, kGrp = 4;
+#pragma unroll 1
+  for (int q0 = 0; q0 < kIt; q0 += kGrp) {
+    A xv[kGrp], bv[kGrp], dv[kGrp], cxv[kGrp], cyv[kGrp], czv[kGrp];
+#pragma unroll
+    for (int u = 0; u < kGrp; ++u) {
+      const int e = threadIdx.x + (q0 + u) * kBatchThreads;
+      const int ri = e % kBRX, rj = (e / kBRX) % kBRY, rk = e / (kBRX * kBRY);
+      const int i = oi + ri, j = oj + rj, k = ok + rk;
+      A x = A(0), bb = A(0), d = A(0), cx = A(0), cy = A(0), cz = A(0);
+      if (q0 + u < kIt && e < kBRegion && i >= 0 && i < ni && j >= 0 && j < nj && k >= 0 && k < nk) {
+        const size_t g = (size_t)i + sy * j + sz * k;
+        if (!ZERO) {
+          x = ldcg(x_in + g);
+          if (PROLONG) x = x + ldcg(xc + lin3(i >> 1, j >> 1, k >> 1, cni, cnj));
+        }
+        bb = ldcg(L.b + g);
+        d = A(ldg(L.diag + g));
+        cx = A(ldg(L.xp + g));
+        cy = A(ldg(L.yp + g));
+        cz = A(ldg(L.zp + g));
       }
-      bb = ldcg(L.b + g);
-      d = A(ldg(L.diag + g));
-      cx = A(ldg(L.xp + g));
-      cy = A(ldg(L.yp + g));
-      cz = A(ldg(L.zp + g));
+      xv[u] = x;
+      bv[u] = bb;
+      dv[u] = d;
+      cxv[u] = cx;
+      cyv[u] = cy;
+      czv[u] = cz;
     }
-    xs[e] = x;
-    bs[e] = bb;
-    ds[e] = d;
-    xps[e] = cx;
-    yps[e] = cy;
-    zps[e] = cz;
+#pragma unroll
+    for (int u = 0; u < kGrp; ++u) {
+      const int e = threadIdx.x + (q0 + u) * kBatchThreads;
+      if (q0 + u < kIt && e < kBRegion) {
+        xs[e] = xv[u];
+        bs[e] = bv[u];
+        ds[e] = dv[u];
+        xps[e] = cxv[u];
+        yps[e] = cyv[u];
+        zps[e] = czv[u];
+      }
+    }
   }
   __syncthreads();
   constexpr int SY = kBRX, SZ = kBRX * kBRY;
