@@ -39,17 +39,27 @@ __device__ __forceinline__ double band_entry(const double* diag, const double* x
 // shared-memory ring (column c in slot c mod (bw+1)): step k takes the pivot
 // of column k, subtracts the rank-1 update of the scaled column k from
 // columns k+1 .. k+bw, writes column k out and loads column k+bw+1 into its
-// slot.  Two barriers per column.
+// slot.  Two barriers per column.  FULL: the whole band (n columns of the
+// original operator) is first staged in shared memory after the ring, so
+// the loop's column loads and pivot tests read shared memory instead of
+// waiting on a global load per column; the same arithmetic.
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK) coarse_chol_kernel(const double* __restrict__ diag,
                                                             const double* __restrict__ xp,
                                                             const double* __restrict__ yp,
                                                             const double* __restrict__ zp, int ni, int nj, int nk,
                                                             int bw, double* __restrict__ Lc,
-                                                            double* __restrict__ rinv, int* __restrict__ ok_flag) {
+                                                            double* __restrict__ rinv, int* __restrict__ ok_flag,
+                                                            int full) {
   extern __shared__ double W[];
   __shared__ int ok;
   const int n = ni * nj * nk, B1 = bw + 1, tid = threadIdx.x;
+  double* F = W + B1 * B1;  // FULL: column c of the band at F + c * B1
+  if (full)
+    for (int e = tid; e < n * B1; e += BLOCK) {
+      const int c = e / B1, d = e - c * B1;
+      F[e] = band_entry(diag, xp, yp, zp, ni, nj, nk, c, d);
+    }
   for (int e = tid; e < B1 * B1; e += BLOCK) {
     const int c = e / B1, d = e - c * B1;
     W[e] = band_entry(diag, xp, yp, zp, ni, nj, nk, c, d);  // columns 0..bw in slots 0..bw
@@ -59,7 +69,7 @@ __global__ void __launch_bounds__(BLOCK) coarse_chol_kernel(const double* __rest
   int sk = 0;  // slot of column k
   for (int k = 0; k < n; ++k) {
     double* col = W + sk * B1;
-    const double a = col[0], orig = diag[k];
+    const double a = col[0], orig = full ? F[k * B1] : diag[k];
     const bool zero = orig == 0.0;
     const bool good = zero || (orig > 0.0 && a > 1e-12 * orig);
     const double l = (zero || !good) ? 1.0 : sqrt(a);
@@ -81,7 +91,7 @@ __global__ void __launch_bounds__(BLOCK) coarse_chol_kernel(const double* __rest
       if (d == 0) v = zero ? 1.0 : l;
       else v = (zero || k + d >= n) ? 0.0 : col[d] * il;
       Lc[(size_t)k * B1 + d] = v;
-      col[d] = band_entry(diag, xp, yp, zp, ni, nj, nk, k + B1, d);
+      col[d] = full ? (k + B1 < n ? F[(k + B1) * B1 + d] : 0.0) : band_entry(diag, xp, yp, zp, ni, nj, nk, k + B1, d);
     }
     if (tid == 0) {
       rinv[k] = zero ? 0.0 : il;

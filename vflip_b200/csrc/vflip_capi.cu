@@ -784,8 +784,11 @@ int build_coarse_direct(vflip_ctx* ctx, const Hierarchy64& H, const double* d0, 
   auto kern = coarse_chol_kernel<kCholBlock>;
   if (smem_optin((const void*)kern, (int)((kCholMaxBw + 1) * (kCholMaxBw + 1) * sizeof(double))) != cudaSuccess)
     return ctx->fail(VFLIP_ERR_CUDA, "cannot raise the coarsest factorisation's shared memory limit");
-  kern<<<1, kCholBlock, (size_t)(bw + 1) * (bw + 1) * sizeof(double), ctx->stream>>>(
-      dg, xp, yp, zp, d.ni, d.nj, d.nk, bw, cd.L, cd.rinv, cd.ok);
+  // the whole band staged beside the ring where both fit the opted-in limit
+  const size_t ring = (size_t)(bw + 1) * (bw + 1), band = (size_t)n * (bw + 1);
+  const bool full = ring + band <= (size_t)(kCholMaxBw + 1) * (kCholMaxBw + 1);
+  kern<<<1, kCholBlock, (ring + (full ? band : 0)) * sizeof(double), ctx->stream>>>(
+      dg, xp, yp, zp, d.ni, d.nj, d.nk, bw, cd.L, cd.rinv, cd.ok, full ? 1 : 0);
   VF_LAUNCH_CHECK();
   cd.on = true;
   return VFLIP_OK;
