@@ -86,45 +86,29 @@ __device__ __forceinline__ float clamp01(float a) { return a < 0.0f ? 0.0f : (a 
 
 // compute_face_weights, Smoke_solver3D.cpp:874-944: weight = 1 - the
 // fraction of each face inside the solid, from the nodal phi at its four
-// corners (the reference's corner order per face grid).  One thread per
-// column of kFaceWeightsZ nodes (i, j, k..) of the (ni+1) x (nj+1) x (nk+1)
-// lattice writes the u, v and w faces whose lower corner each node is: the
-// four corners of layer k+1 it loads are layer k's corners of the next node,
-// so a node costs four phi loads for its three faces, and the 2-D block over
-// (i, j) with columns along z needs no index division.
-constexpr int kFaceWeightsZ = 4;
-
+// corners (the reference's corner order per face grid).  One thread per node
+// (i, j, k) of the (ni+1) x (nj+1) x (nk+1) lattice writes the u, v and w
+// faces whose lower corner that node is, so seven nodal phi loads serve the
+// three faces, and the 2-D block over (i, j) with z over the grid needs no
+// index division.
 __global__ void face_weights3_kernel(const float* __restrict__ phi, float* __restrict__ uw, float* __restrict__ vw,
                                      float* __restrict__ ww, int ni, int nj, int nk) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int k0 = blockIdx.z * kFaceWeightsZ;
-  if (i > ni || j > nj || k0 > nk) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+  if (i > ni || j > nj || k > nk) return;
   const int px = ni + 1, py = nj + 1;
   auto P = [&](int a, int b, int c) { return __ldg(phi + lin3(a, b, c, px, py)); };
-  const bool xi = i < ni, yj = j < nj;
-  // corners of layer k: (i, j), (i, j+1), (i+1, j), (i+1, j+1)
-  float p000 = P(i, j, k0);
-  float p010 = yj ? P(i, j + 1, k0) : 0.0f;
-  float p100 = xi ? P(i + 1, j, k0) : 0.0f;
-  float p110 = (xi && yj) ? P(i + 1, j + 1, k0) : 0.0f;
-  const int k1 = k0 + kFaceWeightsZ < nk + 1 ? k0 + kFaceWeightsZ : nk + 1;
-#pragma unroll
-  for (int q = 0; q < kFaceWeightsZ; ++q) {
-    const int k = k0 + q;
-    if (k >= k1) break;
-    const bool zk = k < nk;
-    const float p001 = zk ? P(i, j, k + 1) : 0.0f;
-    const float p011 = (yj && zk) ? P(i, j + 1, k + 1) : 0.0f;
-    const float p101 = (xi && zk) ? P(i + 1, j, k + 1) : 0.0f;
-    const float p111 = (xi && yj && zk) ? P(i + 1, j + 1, k + 1) : 0.0f;
-    if (yj && zk) uw[lin3(i, j, k, ni + 1, nj)] = clamp01(1 - frac4(p000, p010, p001, p011));
-    if (xi && zk) vw[lin3(i, j, k, ni, nj + 1)] = clamp01(1 - frac4(p000, p001, p100, p101));
-    if (xi && yj) ww[lin3(i, j, k, ni, nj)] = clamp01(1 - frac4(p000, p010, p100, p110));
-    p000 = p001;
-    p010 = p011;
-    p100 = p101;
-    p110 = p111;
-  }
+  const bool xi = i < ni, yj = j < nj, zk = k < nk;
+  // all seven corners loaded up front (one round of memory latency)
+  const float p000 = P(i, j, k);
+  const float p010 = yj ? P(i, j + 1, k) : 0.0f;
+  const float p001 = zk ? P(i, j, k + 1) : 0.0f;
+  const float p100 = xi ? P(i + 1, j, k) : 0.0f;
+  const float p011 = (yj && zk) ? P(i, j + 1, k + 1) : 0.0f;
+  const float p101 = (xi && zk) ? P(i + 1, j, k + 1) : 0.0f;
+  const float p110 = (xi && yj) ? P(i + 1, j + 1, k) : 0.0f;
+  if (yj && zk) uw[lin3(i, j, k, ni + 1, nj)] = clamp01(1 - frac4(p000, p010, p001, p011));
+  if (xi && zk) vw[lin3(i, j, k, ni, nj + 1)] = clamp01(1 - frac4(p000, p001, p100, p101));
+  if (xi && yj) ww[lin3(i, j, k, ni, nj)] = clamp01(1 - frac4(p000, p010, p100, p110));
 }
 
 // Inflow overwrite, Smoke_solver3D.cpp:964-980: every cell with b_desc == 1

@@ -2725,7 +2725,7 @@ int vflip_face_weights(vflip_ctx* ctx, int ni, int nj, int nk, const float* noda
   int rc;
   if ((rc = check_dims(ctx, ni, nj, nk))) return rc;
   if (!nodal_phi || !uw || !vw || !ww) return ctx->fail(VFLIP_ERR_ARG, "null pointer");
-  dim3 blk(32, 8), grid((ni + 1 + 31) / 32, (nj + 1 + 7) / 8, (nk + 1 + kFaceWeightsZ - 1) / kFaceWeightsZ);
+  dim3 blk(32, 8), grid((ni + 1 + 31) / 32, (nj + 1 + 7) / 8, nk + 1);
   face_weights3_kernel<<<grid, blk, 0, ctx->stream>>>(nodal_phi, uw, vw, ww, ni, nj, nk);
   VF_LAUNCH_CHECK();
   return VFLIP_OK;
